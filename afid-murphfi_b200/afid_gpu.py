@@ -1,0 +1,334 @@
+"""Python mirror of the reference's TimeMarcher call sequence over the C ABI of ``libafidgpu.so``.
+
+The reference drives the substep from ``main.F90:281-313``: ``CalcMaxCFL`` → dt rule →
+``TimeMarcher`` → ``time += dt`` (with ``CheckDivergence`` on step 1 and every TOUT).  This
+module exposes the same calls — :meth:`Solver.calc_max_cfl`, :meth:`Solver.time_marcher`,
+:meth:`Solver.check_divergence` — on a GPU-resident state, plus the host set-up the reference
+does in ``ReadInputFile`` / ``CreateGrid`` / ``InitPressureSolver`` / ``SetTempBCs`` through the
+library's C++ host code (``include/afid_host.h``).
+
+The CUDA library is required: importing this module without ``libafidgpu.so`` raises, and
+every compute call goes to the sm_100a kernels (there is no CPU path).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "libafidgpu.so")
+
+AFID_OK = 0
+AFID_E_ALLOC = 8
+AFID_E_CFL = 165
+AFID_E_DTMIN = 166
+AFID_E_DIVERGENCE = 169
+AFID_E_FFTSIZE = 444
+AFID_E_SINGULAR = 601
+AFID_E_TIMEOUT = 602
+AFID_E_INVALID = 603
+AFID_E_CUDA = 604
+AFID_E_CAPACITY = 605
+PREC_FP64 = 0
+PREC_MIXED = 1
+
+_dp = C.POINTER(C.c_double)
+
+
+class GridT(C.Structure):
+    _fields_ = [("nxm", C.c_int), ("nym", C.c_int), ("nzm", C.c_int),
+                ("alx3", C.c_double), ("ylen", C.c_double), ("zlen", C.c_double)] + [
+        (n, _dp) for n in ("xc", "xm", "g3rc", "udx3c", "udx3m", "ap3ck", "ac3ck", "am3ck",
+                           "ap3sk", "ac3sk", "am3sk", "ap3ssk", "ac3ssk", "am3ssk",
+                           "amphk", "acphk", "apphk", "ak1", "ak2")]
+
+
+class ParamsT(C.Structure):
+    _fields_ = [("ren", C.c_double), ("pect", C.c_double), ("byct", C.c_double),
+                ("active_t", C.c_int), ("gaxis", C.c_int), ("inslws", C.c_int),
+                ("inslwn", C.c_int), ("tfixs", C.c_int), ("tfixn", C.c_int),
+                ("xplusu", C.c_double), ("xminusu", C.c_double), ("dpdy", C.c_double),
+                ("dpdz", C.c_double), ("nsst", C.c_int), ("precision", C.c_int),
+                ("tempbp", _dp), ("temptp", _dp)]
+
+
+class InputT(C.Structure):
+    _fields_ = [
+        ("nxm", C.c_int), ("nym", C.c_int), ("nzm", C.c_int), ("nsst", C.c_int),
+        ("multires", C.c_int), ("nxmr", C.c_int), ("nymr", C.c_int), ("nzmr", C.c_int),
+        ("flagsal", C.c_int), ("flagpf", C.c_int), ("nread", C.c_int), ("ireset", C.c_int),
+        ("ntst", C.c_int), ("walltimemax", C.c_double), ("tmax", C.c_double),
+        ("tout", C.c_double), ("tframe", C.c_double), ("save_3d", C.c_double),
+        ("alx3", C.c_double), ("ylen", C.c_double), ("zlen", C.c_double),
+        ("istr3", C.c_int), ("str3", C.c_double), ("istr3r", C.c_int),
+        ("rayt", C.c_double), ("prat", C.c_double), ("rays", C.c_double), ("pras", C.c_double),
+        ("ffscales", C.c_int), ("idtv", C.c_int),
+        ("dt", C.c_double), ("resid", C.c_double), ("limit_cfl", C.c_double),
+        ("dtmin", C.c_double), ("dtmax", C.c_double),
+        ("inslws", C.c_int), ("inslwn", C.c_int), ("tfixs", C.c_int), ("tfixn", C.c_int),
+        ("sfixs", C.c_int), ("sfixn", C.c_int),
+        ("active_t", C.c_int), ("active_s", C.c_int), ("gaxis", C.c_int),
+        ("xplusu", C.c_double), ("xminusu", C.c_double), ("dpdy", C.c_double),
+        ("dpdz", C.c_double), ("melt", C.c_int)]
+
+
+class RunStatsT(C.Structure):
+    _fields_ = [("steps_done", C.c_int), ("errorcode", C.c_int), ("time", C.c_double),
+                ("dt", C.c_double), ("cfl", C.c_double), ("divmax", C.c_double),
+                ("nu_vol", C.c_double), ("ke", C.c_double), ("seconds", C.c_double)]
+
+
+# Every symbol declared in include/afid_gpu.h and include/afid_host.h
+EXPORTS = [
+    "afid_gpu_create", "afid_gpu_destroy", "afid_gpu_set_stream", "afid_gpu_get_stream",
+    "afid_gpu_synchronize", "afid_gpu_upload", "afid_gpu_download", "afid_gpu_timemarcher",
+    "afid_gpu_substep", "afid_gpu_cfl", "afid_gpu_divmax", "afid_gpu_globals",
+    "afid_gpu_status_string", "afid_gpu_cuda_error", "afid_gpu_field_device_ptr",
+    "afid_gpu_launch_count",
+    "afid_parse_bou_in", "afid_read_bou_in", "afid_tables_create", "afid_tables_destroy",
+    "afid_tables_grid", "afid_tables_params", "afid_tables_array", "afid_philox_uniform",
+    "afid_initial_temperature", "afid_next_dt", "afid_run",
+]
+
+
+def load_library(path: str = _LIB_PATH) -> C.CDLL:
+    if not os.path.exists(path):
+        raise ImportError(f"libafidgpu.so not built ({path}); run afid-murphfi_b200/build.py")
+    lib = C.CDLL(path)
+    vp = C.c_void_p
+    i = C.c_int
+    d = C.c_double
+    sig = {
+        "afid_gpu_create": (i, [C.POINTER(GridT), C.POINTER(ParamsT), C.POINTER(vp)]),
+        "afid_gpu_destroy": (i, [vp]),
+        "afid_gpu_set_stream": (i, [vp, vp]),
+        "afid_gpu_get_stream": (vp, [vp]),
+        "afid_gpu_synchronize": (i, [vp]),
+        "afid_gpu_upload": (i, [vp, _dp, _dp, _dp, _dp, _dp, i, i]),
+        "afid_gpu_download": (i, [vp, _dp, _dp, _dp, _dp, _dp, i, i]),
+        "afid_gpu_timemarcher": (i, [vp, d, i]),
+        "afid_gpu_substep": (i, [vp, i, d, d, d, d, d]),
+        "afid_gpu_cfl": (i, [vp, _dp]),
+        "afid_gpu_divmax": (i, [vp, _dp]),
+        "afid_gpu_globals": (i, [vp, d, _dp, _dp, _dp]),
+        "afid_gpu_status_string": (C.c_char_p, [i]),
+        "afid_gpu_cuda_error": (i, [vp]),
+        "afid_gpu_field_device_ptr": (i, [vp, i, C.POINTER(vp), C.POINTER(i)]),
+        "afid_gpu_launch_count": (C.c_longlong, [vp]),
+        "afid_parse_bou_in": (i, [C.c_char_p, C.POINTER(InputT)]),
+        "afid_read_bou_in": (i, [C.c_char_p, C.POINTER(InputT)]),
+        "afid_tables_create": (i, [C.POINTER(InputT), i, C.POINTER(vp)]),
+        "afid_tables_destroy": (None, [vp]),
+        "afid_tables_grid": (C.POINTER(GridT), [vp]),
+        "afid_tables_params": (C.POINTER(ParamsT), [vp]),
+        "afid_tables_array": (_dp, [vp, C.c_char_p, C.POINTER(i)]),
+        "afid_philox_uniform": (d, [C.c_uint64, C.c_uint64]),
+        "afid_initial_temperature": (i, [vp, C.c_uint64, d, _dp, i, i]),
+        "afid_next_dt": (i, [C.POINTER(InputT), i, _dp, d, _dp]),
+        "afid_run": (i, [C.POINTER(InputT), i, C.c_uint64, i, i, vp, vp, C.POINTER(RunStatsT)]),
+    }
+    for name, (res, args) in sig.items():
+        f = getattr(lib, name)
+        f.restype = res
+        f.argtypes = args
+    return lib
+
+
+_lib = None
+
+
+def lib() -> C.CDLL:
+    global _lib
+    if _lib is None:
+        _lib = load_library()
+    return _lib
+
+
+class AfidError(RuntimeError):
+    def __init__(self, status: int, what: str = ""):
+        msg = lib().afid_gpu_status_string(status).decode()
+        super().__init__(f"{what}: status {status} ({msg})")
+        self.status = status
+
+
+def _check(status: int, what: str) -> None:
+    if status != AFID_OK:
+        raise AfidError(status, what)
+
+
+def _ptr(a: np.ndarray):
+    return a.ctypes.data_as(_dp)
+
+
+def parse_bou_in(text: str) -> InputT:
+    inp = InputT()
+    _check(lib().afid_parse_bou_in(text.encode(), C.byref(inp)), "afid_parse_bou_in")
+    return inp
+
+
+class Tables:
+    """Host-side set-up (CreateGrid + InitPressureSolver + SetTempBCs) built by the C++ code."""
+
+    def __init__(self, inp: InputT, precision: int = PREC_FP64):
+        self.inp = inp
+        self._h = C.c_void_p()
+        _check(lib().afid_tables_create(C.byref(inp), precision, C.byref(self._h)), "afid_tables_create")
+
+    def array(self, name: str) -> np.ndarray:
+        n = C.c_int()
+        p = lib().afid_tables_array(self._h, name.encode(), C.byref(n))
+        if not p:
+            raise KeyError(name)
+        return np.ctypeslib.as_array(p, shape=(n.value,)).copy()
+
+    @property
+    def grid(self) -> GridT:
+        return lib().afid_tables_grid(self._h).contents
+
+    @property
+    def params(self) -> ParamsT:
+        return lib().afid_tables_params(self._h).contents
+
+    def initial_temperature(self, seed: int, eps: float = 1e-3) -> np.ndarray:
+        i = self.inp
+        t = np.zeros((i.nzm, i.nym, i.nxm + 1))
+        _check(lib().afid_initial_temperature(self._h, seed, eps, _ptr(t), i.nxm + 1, i.nym),
+               "afid_initial_temperature")
+        return t
+
+    def close(self):
+        if self._h:
+            lib().afid_tables_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Solver:
+    """GPU-resident AFiD flow + temperature state.
+
+    Arrays cross the boundary in the reference's Fortran layout: numpy shape (nzm, nym, nx)
+    C-order == Fortran (nx, nym, nzm), x fastest.  ``grid`` / ``params`` are ``GridT`` /
+    ``ParamsT`` (e.g. from :class:`Tables`); the arrays they point to must outlive creation.
+    """
+
+    FIELDS = ("vx", "vy", "vz", "temp", "pr")
+
+    def __init__(self, grid: GridT, params: ParamsT):
+        self.nxm, self.nym, self.nzm = grid.nxm, grid.nym, grid.nzm
+        self.nx = self.nxm + 1
+        self._h = C.c_void_p()
+        _check(lib().afid_gpu_create(C.byref(grid), C.byref(params), C.byref(self._h)), "afid_gpu_create")
+
+    @property
+    def shape(self):
+        return (self.nzm, self.nym, self.nx)
+
+    def _arr(self, a):
+        if a is None:
+            return None
+        a = np.ascontiguousarray(a, dtype=np.float64)
+        if a.shape != self.shape:
+            raise ValueError(f"expected shape {self.shape}, got {a.shape}")
+        return a
+
+    def upload(self, vx=None, vy=None, vz=None, temp=None, pr=None):
+        arrs = [self._arr(a) for a in (vx, vy, vz, temp, pr)]
+        ptrs = [(_ptr(a) if a is not None else None) for a in arrs]
+        _check(lib().afid_gpu_upload(self._h, *ptrs, self.nx, self.nym), "afid_gpu_upload")
+
+    def download(self) -> dict:
+        out = {f: np.zeros(self.shape) for f in self.FIELDS}
+        _check(lib().afid_gpu_download(self._h, *(_ptr(out[f]) for f in self.FIELDS), self.nx, self.nym),
+               "afid_gpu_download")
+        return out
+
+    def time_marcher(self, dt: float, ntime: int = 0) -> None:
+        _check(lib().afid_gpu_timemarcher(self._h, dt, ntime), "afid_gpu_timemarcher")
+
+    def substep(self, ns: int, al: float, ga: float, ro: float, dt: float, beta: float) -> None:
+        _check(lib().afid_gpu_substep(self._h, ns, al, ga, ro, dt, beta), "afid_gpu_substep")
+
+    def calc_max_cfl(self) -> float:
+        v = C.c_double()
+        _check(lib().afid_gpu_cfl(self._h, C.byref(v)), "afid_gpu_cfl")
+        return v.value
+
+    def check_divergence(self) -> float:
+        v = C.c_double()
+        _check(lib().afid_gpu_divmax(self._h, C.byref(v)), "afid_gpu_divmax")
+        return v.value
+
+    def global_quantities(self, ra_pr: float):
+        nu, ke, tm = C.c_double(), C.c_double(), C.c_double()
+        _check(lib().afid_gpu_globals(self._h, ra_pr, C.byref(nu), C.byref(ke), C.byref(tm)),
+               "afid_gpu_globals")
+        return nu.value, ke.value, tm.value
+
+    def synchronize(self) -> None:
+        _check(lib().afid_gpu_synchronize(self._h), "afid_gpu_synchronize")
+
+    def set_stream(self, stream_handle: int | None) -> None:
+        _check(lib().afid_gpu_set_stream(self._h, C.c_void_p(stream_handle or 0)), "afid_gpu_set_stream")
+
+    def stream(self) -> int:
+        return lib().afid_gpu_get_stream(self._h) or 0
+
+    def launch_count(self) -> int:
+        return int(lib().afid_gpu_launch_count(self._h))
+
+    def device_ptr(self, which: int):
+        p, ld = C.c_void_p(), C.c_int()
+        _check(lib().afid_gpu_field_device_ptr(self._h, which, C.byref(p), C.byref(ld)), "field_device_ptr")
+        return p.value, ld.value
+
+    def close(self):
+        if self._h:
+            lib().afid_gpu_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def grid_from_arrays(nxm, nym, nzm, alx3, ylen, zlen, arrays: dict, keep: list) -> GridT:
+    """Build a GridT from named numpy tables (0-based copies of the reference arrays);
+    ``keep`` collects the contiguous copies, which must outlive the solver creation."""
+    g = GridT()
+    g.nxm, g.nym, g.nzm = nxm, nym, nzm
+    g.alx3, g.ylen, g.zlen = alx3, ylen, zlen
+    for name, _ in GridT._fields_[6:]:
+        a = np.ascontiguousarray(arrays[name], dtype=np.float64)
+        keep.append(a)
+        setattr(g, name, _ptr(a))
+    return g
+
+
+def params_from_values(ren, pect, byct, active_t, gaxis, inslws, inslwn, tfixs, tfixn,
+                       xplusu, xminusu, dpdy, dpdz, nsst, precision, tempbp, temptp,
+                       keep: list) -> ParamsT:
+    p = ParamsT()
+    p.ren, p.pect, p.byct = ren, pect, byct
+    p.active_t, p.gaxis, p.inslws, p.inslwn, p.tfixs, p.tfixn = active_t, gaxis, inslws, inslwn, tfixs, tfixn
+    p.xplusu, p.xminusu, p.dpdy, p.dpdz = xplusu, xminusu, dpdy, dpdz
+    p.nsst, p.precision = nsst, precision
+    for name, a in (("tempbp", tempbp), ("temptp", temptp)):
+        a = np.ascontiguousarray(a, dtype=np.float64)
+        keep.append(a)
+        setattr(p, name, _ptr(a))
+    return p

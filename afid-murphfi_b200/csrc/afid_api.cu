@@ -1,0 +1,561 @@
+// afid_api.cu — the C ABI of include/afid_gpu.h: context lifetime, state transfer, and the
+// TimeMarcher call sequence (TimeMarcher.F90:28-133) issued as sm_100a kernels on one stream.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include "afid_gpu.h"
+#include "afid_internal.h"
+
+using namespace afid;
+
+struct afid_ctx {
+  int dev = 0;
+  cudaStream_t own_stream = nullptr;
+  cudaStream_t stream = nullptr;
+  cudaError_t last_cuda = cudaSuccess;
+  long long launches = 0;
+  int nsst = 3;
+  double alx3 = 1.0;
+  LaunchCtx L{};
+  // device allocations
+  std::vector<void *> allocs;
+  double *vx = nullptr, *vy = nullptr, *vz = nullptr, *temp = nullptr, *pr = nullptr;
+  double *vx_o = nullptr, *vy_o = nullptr, *vz_o = nullptr, *temp_o = nullptr;
+  void *rux = nullptr, *ruy = nullptr, *ruz = nullptr, *rut = nullptr;
+  void *spec = nullptr, *phi = nullptr;
+  double *cn_tab = nullptr;
+  StepCoef *sc = nullptr;
+  int *err = nullptr;
+  unsigned long long *red = nullptr;
+  double *partial = nullptr, *gsum = nullptr;
+  double *host_scratch = nullptr;  // pinned, 8 doubles
+  // device tables for the CN builder
+  const double *am[3], *ac[3], *ap[3];
+  size_t field_elems = 0;
+};
+
+namespace {
+
+int fail_cuda(afid_ctx_t *ctx, cudaError_t e) {
+  if (ctx) ctx->last_cuda = e;
+  return AFID_E_CUDA;
+}
+
+#define AFID_CUDA(ctx, call)                       \
+  do {                                             \
+    cudaError_t e_ = (call);                       \
+    if (e_ != cudaSuccess) return fail_cuda(ctx, e_); \
+  } while (0)
+
+bool make_plan(int n, FftPlan *p) {
+  p->n = n;
+  p->npass = 0;
+  int m = n;
+  while (m % 4 == 0 && p->npass < kMaxFftPasses) { p->radix[p->npass++] = 4; m /= 4; }
+  while (m % 2 == 0 && p->npass < kMaxFftPasses) { p->radix[p->npass++] = 2; m /= 2; }
+  while (m % 3 == 0 && p->npass < kMaxFftPasses) { p->radix[p->npass++] = 3; m /= 3; }
+  while (m % 5 == 0 && p->npass < kMaxFftPasses) { p->radix[p->npass++] = 5; m /= 5; }
+  return m == 1;
+}
+
+// exp(-2 pi i m / n) for m = 0..n-1
+template <typename C>
+std::vector<C> twiddles(int n) {
+  std::vector<C> t(n);
+  const double two_pi = 2.0 * 3.14159265358979323846264338327950288;
+  for (int m = 0; m < n; ++m) {
+    const double a = two_pi * (double)m / (double)n;
+    t[m].x = (decltype(t[m].x))std::cos(a);
+    t[m].y = (decltype(t[m].y))(-std::sin(a));
+  }
+  return t;
+}
+
+int round_up(int a, int b) { return (a + b - 1) / b * b; }
+
+template <typename T>
+cudaError_t dalloc(afid_ctx_t *ctx, T **p, size_t count) {
+  void *q = nullptr;
+  cudaError_t e = cudaMalloc(&q, std::max<size_t>(count, 1) * sizeof(T));
+  if (e != cudaSuccess) return e;
+  ctx->allocs.push_back(q);
+  *p = static_cast<T *>(q);
+  return cudaMemset(q, 0, std::max<size_t>(count, 1) * sizeof(T));
+}
+
+// Copy a Fortran-layout host field (pointer at (1,1,1), leading dims ld_x, ld_y) into the
+// device layout (ldx, nym); nx doubles per x-column.
+int copy_field(afid_ctx_t *ctx, double *dst, const double *src, int ld_x, int ld_y, bool to_dev,
+               double *hdst = nullptr) {
+  const Geom &g = ctx->L.g;
+  const size_t w = (size_t)g.nx * sizeof(double);
+  cudaMemcpyKind kind = to_dev ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToHost;
+  if (ld_y == g.nym) {
+    if (to_dev)
+      AFID_CUDA(ctx, cudaMemcpy2DAsync(dst, (size_t)g.ldx * sizeof(double), src, (size_t)ld_x * sizeof(double),
+                                       w, (size_t)g.nym * g.nzm, kind, ctx->stream));
+    else
+      AFID_CUDA(ctx, cudaMemcpy2DAsync(hdst, (size_t)ld_x * sizeof(double), dst, (size_t)g.ldx * sizeof(double),
+                                       w, (size_t)g.nym * g.nzm, kind, ctx->stream));
+    return AFID_OK;
+  }
+  for (int i = 0; i < g.nzm; ++i) {
+    const size_t hoff = (size_t)i * ld_x * ld_y;
+    const size_t doff = (size_t)i * g.ldx * g.nym;
+    if (to_dev)
+      AFID_CUDA(ctx, cudaMemcpy2DAsync(dst + doff, (size_t)g.ldx * sizeof(double), src + hoff,
+                                       (size_t)ld_x * sizeof(double), w, g.nym, kind, ctx->stream));
+    else
+      AFID_CUDA(ctx, cudaMemcpy2DAsync(hdst + hoff, (size_t)ld_x * sizeof(double), dst + doff,
+                                       (size_t)g.ldx * sizeof(double), w, g.nym, kind, ctx->stream));
+  }
+  return AFID_OK;
+}
+
+int check_err_flag(afid_ctx_t *ctx) {
+  int h = 0;
+  AFID_CUDA(ctx, cudaMemcpyAsync(&h, ctx->err, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+  AFID_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  if (h & 1) return AFID_E_SINGULAR;
+  if (h & 2) return AFID_E_TIMEOUT;
+  return AFID_OK;
+}
+
+SubstepBuffers buffers(afid_ctx_t *ctx) {
+  SubstepBuffers b;
+  b.sc = ctx->sc;
+  b.cn_tab = ctx->cn_tab;
+  b.vx = ctx->vx;
+  b.vy = ctx->vy;
+  b.vz = ctx->vz;
+  b.temp = ctx->temp;
+  b.pr = ctx->pr;
+  b.rux = ctx->rux;
+  b.ruy = ctx->ruy;
+  b.ruz = ctx->ruz;
+  b.rut = ctx->rut;
+  b.vx_o = ctx->vx_o;
+  b.vy_o = ctx->vy_o;
+  b.vz_o = ctx->vz_o;
+  b.temp_o = ctx->temp_o;
+  b.spec = ctx->spec;
+  b.phi = ctx->phi;
+  b.err = ctx->err;
+  return b;
+}
+
+int build_cn(afid_ctx_t *ctx, int ns0, int nsub, const double *al, const double *ga, const double *ro,
+             double dt, double beta) {
+  const Geom &g = ctx->L.g;
+  CnInputs in;
+  for (int m = 0; m < 3; ++m) {
+    in.am[m] = ctx->am[m];
+    in.ac[m] = ctx->ac[m];
+    in.ap[m] = ctx->ap[m];
+  }
+  in.off[0] = 1;
+  in.n[0] = g.nxm - 1;
+  in.off[1] = 0;
+  in.n[1] = g.nxm;
+  in.off[2] = 0;
+  in.n[2] = g.nxm;
+  for (int s = 0; s < 3; ++s) {
+    in.al[s] = s < nsub ? al[s] : 0.0;
+    in.ga[s] = s < nsub ? ga[s] : 0.0;
+    in.ro[s] = s < nsub ? ro[s] : 0.0;
+  }
+  in.dt = dt;
+  in.beta = beta;
+  in.pect = g.pect;
+  in.ns0 = ns0;
+  in.nsub = nsub;
+  in.M = ctx->L.M;
+  in.tab = ctx->cn_tab;
+  in.sc = ctx->sc;
+  AFID_CUDA(ctx, launch_cn_tables(ctx->L, in));
+  ctx->launches += 1;
+  return AFID_OK;
+}
+
+int run_substep(afid_ctx_t *ctx, int ns) {
+  SubstepBuffers b = buffers(ctx);
+  AFID_CUDA(ctx, launch_explicit_implicit(ctx->L, b, ns));
+  AFID_CUDA(ctx, launch_pressure(ctx->L, b, ns));
+  ctx->launches += (ctx->L.g.nzm > 1) ? 7 : 5;
+  std::swap(ctx->temp, ctx->temp_o);  // temperature is final after K1; the state moves buffers
+  return AFID_OK;
+}
+
+void rk3(int nsst, double gam[3], double rom[3], double alm[3]) {
+  // InitTimeMarchScheme.F90:16-49
+  if (nsst > 1) {
+    gam[0] = 8.0 / 15.0; gam[1] = 5.0 / 12.0; gam[2] = 3.0 / 4.0;
+    rom[0] = 0.0; rom[1] = -17.0 / 60.0; rom[2] = -5.0 / 12.0;
+  } else {
+    gam[0] = 1.5; gam[1] = 0.0; gam[2] = 0.0;
+    rom[0] = -0.5; rom[1] = 0.0; rom[2] = 0.0;
+  }
+  for (int n = 0; n < 3; ++n) alm[n] = gam[n] + rom[n];
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *afid_gpu_status_string(int s) {
+  switch (s) {
+    case AFID_OK: return "ok";
+    case AFID_E_ALLOC: return "allocation failure";
+    case AFID_E_CFL: return "CFL number exceeds CFLMAX with fixed time step";
+    case AFID_E_DTMIN: return "time step below DTMIN";
+    case AFID_E_DIVERGENCE: return "maximum divergence exceeds RESID";
+    case AFID_E_FFTSIZE: return "FFT size has a prime factor other than 2, 3, 5";
+    case AFID_E_SINGULAR: return "singular Poisson mode (zero pivot)";
+    case AFID_E_TIMEOUT: return "bounded device wait timed out";
+    case AFID_E_INVALID: return "invalid argument or unsupported configuration";
+    case AFID_E_CUDA: return "CUDA runtime error";
+    case AFID_E_CAPACITY: return "capacity exhausted";
+  }
+  return "unknown status";
+}
+
+int afid_gpu_create(const afid_grid_t *grid, const afid_params_t *prm, afid_ctx_t **out) {
+  if (!grid || !prm || !out) return AFID_E_INVALID;
+  *out = nullptr;
+  const int nxm = grid->nxm, nym = grid->nym, nzm = grid->nzm;
+  if (nxm < 2 || nym < 1 || nzm < 1) return AFID_E_INVALID;
+  if (prm->dpdz != 0.0) return AFID_E_INVALID;  // bulk-flux forcing (CorrectVelocity.F90:29-59) not on this path
+  if (prm->gaxis == 2 && prm->inslwn == 1) return AFID_E_INVALID;  // mean-flux removal branch (CorrectVelocity.F90:62)
+  if (prm->precision != AFID_PREC_FP64 && prm->precision != AFID_PREC_MIXED) return AFID_E_INVALID;
+  const int M = cn_choose_M(nxm);
+  if (M < 0) return AFID_E_INVALID;
+  FftPlan py, pz;
+  if (!make_plan(nym, &py) || !make_plan(nzm, &pz)) return AFID_E_FFTSIZE;
+
+  afid_ctx_t *ctx = new (std::nothrow) afid_ctx_t();
+  if (!ctx) return AFID_E_ALLOC;
+  cudaGetDevice(&ctx->dev);
+  ctx->nsst = prm->nsst > 1 ? 3 : 1;
+  ctx->alx3 = grid->alx3;
+  const bool mixed = prm->precision == AFID_PREC_MIXED;
+
+  Geom g{};
+  g.nxm = nxm;
+  g.nym = nym;
+  g.nzm = nzm;
+  g.nx = nxm + 1;
+  g.ldx = round_up(g.nx, 8);
+  g.nyh = nym / 2 + 1;
+  g.ldxc = round_up(nxm, 4);
+  g.dx = (double)nxm / grid->alx3;  // CreateGrid.F90:100-106
+  g.dy = (double)nym / grid->ylen;
+  g.dz = (double)nzm / grid->zlen;
+  g.dyq = g.dy * g.dy;
+  g.dzq = g.dz * g.dz;
+  g.ren = prm->ren;
+  g.pect = prm->pect;
+  g.byct = prm->byct;
+  // ExplicitTermsVY.F90:30-34
+  g.gy = (prm->inslwn == 0 || prm->inslws == 0) ? prm->dpdy * prm->dpdy / (prm->ren * prm->ren)
+                                                 : 8.0 * (prm->dpdy * prm->dpdy) / (prm->ren * prm->ren);
+  g.xplusu = prm->xplusu;
+  g.xminusu = prm->xminusu;
+  g.active_t = prm->active_t;
+  g.gaxis = prm->gaxis;
+  g.inslws = prm->inslws;
+  g.inslwn = prm->inslwn;
+  g.tfixs = prm->tfixs;
+  g.tfixn = prm->tfixn;
+
+  const size_t nf = (size_t)g.ldx * nym * nzm;
+  ctx->field_elems = nf;
+  const size_t nspec = (size_t)g.ldxc * g.nyh * nzm;
+  const size_t tsz = mixed ? sizeof(float) : sizeof(double);
+  cudaError_t e = cudaSuccess;
+  auto chk = [&](cudaError_t r) { if (e == cudaSuccess) e = r; };
+  chk(cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking));
+  ctx->stream = ctx->own_stream;
+  chk(dalloc(ctx, &ctx->vx, nf));
+  chk(dalloc(ctx, &ctx->vy, nf));
+  chk(dalloc(ctx, &ctx->vz, nf));
+  chk(dalloc(ctx, &ctx->temp, nf));
+  chk(dalloc(ctx, &ctx->pr, nf));
+  chk(dalloc(ctx, &ctx->vx_o, nf));
+  chk(dalloc(ctx, &ctx->vy_o, nf));
+  chk(dalloc(ctx, &ctx->vz_o, nf));
+  chk(dalloc(ctx, &ctx->temp_o, nf));
+  unsigned char *ru = nullptr;
+  chk(dalloc(ctx, &ru, 4 * nf * tsz));
+  ctx->rux = ru;
+  ctx->ruy = ru + nf * tsz;
+  ctx->ruz = ru + 2 * nf * tsz;
+  ctx->rut = ru + 3 * nf * tsz;
+  unsigned char *ph = nullptr;
+  chk(dalloc(ctx, &ph, nf * tsz));
+  ctx->phi = ph;
+  unsigned char *sp = nullptr;
+  chk(dalloc(ctx, &sp, nspec * 2 * tsz));
+  ctx->spec = sp;
+  chk(dalloc(ctx, &ctx->cn_tab, cn_tab_doubles(M, 3)));
+  chk(dalloc(ctx, &ctx->sc, 3));
+  chk(dalloc(ctx, &ctx->err, 1));
+  chk(dalloc(ctx, &ctx->red, 1));
+  const int nb = globals_partial_blocks(g);
+  chk(dalloc(ctx, &ctx->partial, (size_t)nb * 3));
+  chk(dalloc(ctx, &ctx->gsum, 3));
+  if (e == cudaSuccess) e = cudaMallocHost(&ctx->host_scratch, 8 * sizeof(double));
+
+  // 1-D tables in one device block
+  const int nx = g.nx;
+  std::vector<double> h;
+  auto put = [&](const double *src, int n, int len) -> size_t {
+    size_t off = h.size();
+    for (int k = 0; k < len; ++k) h.push_back((src && k < n) ? src[k] : 0.0);
+    return off;
+  };
+  const int L1 = nx + 8;
+  size_t o_udx3c = put(grid->udx3c, nx, L1), o_udx3m = put(grid->udx3m, nxm, L1);
+  std::vector<double> idx(nxm);
+  for (int k = 0; k < nxm; ++k) idx[k] = 1.0 / grid->udx3m[k];  // ExplicitTermsVX.F90:194-196
+  size_t o_idx = put(idx.data(), nxm, L1);
+  size_t o_ap3ck = put(grid->ap3ck, nx, L1), o_ac3ck = put(grid->ac3ck, nx, L1), o_am3ck = put(grid->am3ck, nx, L1);
+  size_t o_ap3sk = put(grid->ap3sk, nxm, L1), o_ac3sk = put(grid->ac3sk, nxm, L1), o_am3sk = put(grid->am3sk, nxm, L1);
+  size_t o_ap3ssk = put(grid->ap3ssk, nxm, L1), o_ac3ssk = put(grid->ac3ssk, nxm, L1),
+         o_am3ssk = put(grid->am3ssk, nxm, L1);
+  size_t o_amphk = put(grid->amphk, nxm, L1), o_acphk = put(grid->acphk, nxm, L1), o_apphk = put(grid->apphk, nxm, L1);
+  size_t o_ak1 = put(grid->ak1, nzm, nzm), o_ak2 = put(grid->ak2, nym, nym);
+  size_t o_g3rc = put(grid->g3rc, nx, L1);
+  std::vector<double> tbp((size_t)nym * nzm, 0.5), ttp((size_t)nym * nzm, -0.5);
+  if (prm->tempbp) std::memcpy(tbp.data(), prm->tempbp, tbp.size() * sizeof(double));
+  if (prm->temptp) std::memcpy(ttp.data(), prm->temptp, ttp.size() * sizeof(double));
+  size_t o_tbp = put(tbp.data(), (int)tbp.size(), (int)tbp.size());
+  size_t o_ttp = put(ttp.data(), (int)ttp.size(), (int)ttp.size());
+  double *dtab = nullptr;
+  if (e == cudaSuccess) e = dalloc(ctx, &dtab, h.size());
+  if (e == cudaSuccess) e = cudaMemcpy(dtab, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice);
+  Tables t{};
+  if (dtab) {
+    t.udx3c = dtab + o_udx3c;
+    t.udx3m = dtab + o_udx3m;
+    t.idx = dtab + o_idx;
+    t.ap3ck = dtab + o_ap3ck;
+    t.ac3ck = dtab + o_ac3ck;
+    t.am3ck = dtab + o_am3ck;
+    t.ap3sk = dtab + o_ap3sk;
+    t.ac3sk = dtab + o_ac3sk;
+    t.am3sk = dtab + o_am3sk;
+    t.ap3ssk = dtab + o_ap3ssk;
+    t.ac3ssk = dtab + o_ac3ssk;
+    t.am3ssk = dtab + o_am3ssk;
+    t.amphk = dtab + o_amphk;
+    t.acphk = dtab + o_acphk;
+    t.apphk = dtab + o_apphk;
+    t.ak1 = dtab + o_ak1;
+    t.ak2 = dtab + o_ak2;
+    t.g3rc = dtab + o_g3rc;
+    t.tempbp = dtab + o_tbp;
+    t.temptp = dtab + o_ttp;
+    ctx->am[0] = t.am3ck; ctx->ac[0] = t.ac3ck; ctx->ap[0] = t.ap3ck;
+    ctx->am[1] = t.am3sk; ctx->ac[1] = t.ac3sk; ctx->ap[1] = t.ap3sk;
+    ctx->am[2] = t.am3ssk; ctx->ac[2] = t.ac3ssk; ctx->ap[2] = t.ap3ssk;
+  }
+  // twiddles
+  void *twy = nullptr, *twz = nullptr;
+  if (e == cudaSuccess) {
+    if (mixed) {
+      auto a = twiddles<float2>(nym), b = twiddles<float2>(nzm);
+      float2 *dy_ = nullptr, *dz_ = nullptr;
+      e = dalloc(ctx, &dy_, a.size());
+      if (e == cudaSuccess) e = dalloc(ctx, &dz_, b.size());
+      if (e == cudaSuccess) e = cudaMemcpy(dy_, a.data(), a.size() * sizeof(float2), cudaMemcpyHostToDevice);
+      if (e == cudaSuccess) e = cudaMemcpy(dz_, b.data(), b.size() * sizeof(float2), cudaMemcpyHostToDevice);
+      twy = dy_;
+      twz = dz_;
+    } else {
+      auto a = twiddles<double2>(nym), b = twiddles<double2>(nzm);
+      double2 *dy_ = nullptr, *dz_ = nullptr;
+      e = dalloc(ctx, &dy_, a.size());
+      if (e == cudaSuccess) e = dalloc(ctx, &dz_, b.size());
+      if (e == cudaSuccess) e = cudaMemcpy(dy_, a.data(), a.size() * sizeof(double2), cudaMemcpyHostToDevice);
+      if (e == cudaSuccess) e = cudaMemcpy(dz_, b.data(), b.size() * sizeof(double2), cudaMemcpyHostToDevice);
+      twy = dy_;
+      twz = dz_;
+    }
+  }
+  if (e != cudaSuccess) {
+    ctx->last_cuda = e;
+    afid_gpu_destroy(ctx);
+    return (e == cudaErrorMemoryAllocation) ? AFID_E_ALLOC : AFID_E_CUDA;
+  }
+  LaunchCtx &L = ctx->L;
+  L.g = g;
+  L.t = t;
+  L.stream = ctx->stream;
+  L.M = M;
+  L.mixed = mixed;
+  const size_t csz = mixed ? sizeof(float2) : sizeof(double2);
+  const size_t smem_cap = 96 * 1024;
+  L.tx_y = 8;
+  while (L.tx_y > 2 && (size_t)L.tx_y * nym * csz > smem_cap) L.tx_y /= 2;
+  L.tx_z = 8;
+  while (L.tx_z > 2 && (size_t)2 * L.tx_z * nzm * csz > smem_cap) L.tx_z /= 2;
+  if ((size_t)L.tx_y * nym * csz > 200 * 1024 || (size_t)2 * L.tx_z * nzm * csz > 200 * 1024) {
+    afid_gpu_destroy(ctx);
+    return AFID_E_INVALID;
+  }
+  L.plan_y = py;
+  L.plan_z = pz;
+  L.twy = twy;
+  L.twz = twz;
+  *out = ctx;
+  return AFID_OK;
+}
+
+int afid_gpu_destroy(afid_ctx_t *ctx) {
+  if (!ctx) return AFID_OK;
+  cudaSetDevice(ctx->dev);
+  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  for (void *p : ctx->allocs) cudaFree(p);
+  if (ctx->host_scratch) cudaFreeHost(ctx->host_scratch);
+  if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
+  delete ctx;
+  return AFID_OK;
+}
+
+int afid_gpu_set_stream(afid_ctx_t *ctx, void *stream) {
+  if (!ctx) return AFID_E_INVALID;
+  ctx->stream = stream ? static_cast<cudaStream_t>(stream) : ctx->own_stream;
+  ctx->L.stream = ctx->stream;
+  return AFID_OK;
+}
+
+void *afid_gpu_get_stream(afid_ctx_t *ctx) { return ctx ? (void *)ctx->stream : nullptr; }
+
+int afid_gpu_synchronize(afid_ctx_t *ctx) {
+  if (!ctx) return AFID_E_INVALID;
+  cudaSetDevice(ctx->dev);
+  return check_err_flag(ctx);
+}
+
+int afid_gpu_upload(afid_ctx_t *ctx, const double *vx, const double *vy, const double *vz,
+                    const double *temp, const double *pr, int ld_x, int ld_y) {
+  if (!ctx) return AFID_E_INVALID;
+  const Geom &g = ctx->L.g;
+  if (ld_x < g.nx || ld_y < g.nym) return AFID_E_INVALID;
+  cudaSetDevice(ctx->dev);
+  int s;
+  if (vx && (s = copy_field(ctx, ctx->vx, vx, ld_x, ld_y, true)) != AFID_OK) return s;
+  if (vy && (s = copy_field(ctx, ctx->vy, vy, ld_x, ld_y, true)) != AFID_OK) return s;
+  if (vz && (s = copy_field(ctx, ctx->vz, vz, ld_x, ld_y, true)) != AFID_OK) return s;
+  if (temp && (s = copy_field(ctx, ctx->temp, temp, ld_x, ld_y, true)) != AFID_OK) return s;
+  if (pr && (s = copy_field(ctx, ctx->pr, pr, ld_x, ld_y, true)) != AFID_OK) return s;
+  const size_t tsz = ctx->L.mixed ? sizeof(float) : sizeof(double);
+  AFID_CUDA(ctx, cudaMemsetAsync(ctx->rux, 0, 4 * ctx->field_elems * tsz, ctx->stream));
+  AFID_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return AFID_OK;
+}
+
+int afid_gpu_download(afid_ctx_t *ctx, double *vx, double *vy, double *vz, double *temp, double *pr,
+                      int ld_x, int ld_y) {
+  if (!ctx) return AFID_E_INVALID;
+  const Geom &g = ctx->L.g;
+  if (ld_x < g.nx || ld_y < g.nym) return AFID_E_INVALID;
+  cudaSetDevice(ctx->dev);
+  int s;
+  if (vx && (s = copy_field(ctx, ctx->vx, nullptr, ld_x, ld_y, false, vx)) != AFID_OK) return s;
+  if (vy && (s = copy_field(ctx, ctx->vy, nullptr, ld_x, ld_y, false, vy)) != AFID_OK) return s;
+  if (vz && (s = copy_field(ctx, ctx->vz, nullptr, ld_x, ld_y, false, vz)) != AFID_OK) return s;
+  if (temp && (s = copy_field(ctx, ctx->temp, nullptr, ld_x, ld_y, false, temp)) != AFID_OK) return s;
+  if (pr && (s = copy_field(ctx, ctx->pr, nullptr, ld_x, ld_y, false, pr)) != AFID_OK) return s;
+  return check_err_flag(ctx);
+}
+
+int afid_gpu_timemarcher(afid_ctx_t *ctx, double dt, int ntime) {
+  (void)ntime;
+  if (!ctx || !(dt > 0.0)) return AFID_E_INVALID;
+  cudaSetDevice(ctx->dev);
+  double gam[3], rom[3], alm[3];
+  rk3(ctx->nsst, gam, rom, alm);
+  const double beta = dt / ctx->L.g.ren * 0.5;  // TimeMarcher.F90:28
+  int s;
+  if ((s = build_cn(ctx, 0, ctx->nsst, alm, gam, rom, dt, beta)) != AFID_OK) return s;
+  for (int ns = 0; ns < ctx->nsst; ++ns)
+    if ((s = run_substep(ctx, ns)) != AFID_OK) return s;
+  return AFID_OK;
+}
+
+int afid_gpu_substep(afid_ctx_t *ctx, int ns, double al, double ga, double ro, double dt, double beta) {
+  if (!ctx || ns < 0 || ns > 2 || !(dt > 0.0)) return AFID_E_INVALID;
+  cudaSetDevice(ctx->dev);
+  int s;
+  if ((s = build_cn(ctx, ns, 1, &al, &ga, &ro, dt, beta)) != AFID_OK) return s;
+  return run_substep(ctx, ns);
+}
+
+int afid_gpu_cfl(afid_ctx_t *ctx, double *cflm) {
+  if (!ctx || !cflm) return AFID_E_INVALID;
+  cudaSetDevice(ctx->dev);
+  AFID_CUDA(ctx, launch_max_reduce(ctx->L, false, ctx->vx, ctx->vy, ctx->vz, ctx->red));
+  ctx->launches += 1;
+  AFID_CUDA(ctx, cudaMemcpyAsync(ctx->host_scratch, ctx->red, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  int s = check_err_flag(ctx);
+  const double v = ctx->host_scratch[0];
+  *cflm = std::max(0.00000001, v);  // CalcMaxCFL.F90:22
+  return s;
+}
+
+int afid_gpu_divmax(afid_ctx_t *ctx, double *dmax) {
+  if (!ctx || !dmax) return AFID_E_INVALID;
+  cudaSetDevice(ctx->dev);
+  AFID_CUDA(ctx, launch_max_reduce(ctx->L, true, ctx->vx, ctx->vy, ctx->vz, ctx->red));
+  ctx->launches += 1;
+  AFID_CUDA(ctx, cudaMemcpyAsync(ctx->host_scratch, ctx->red, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  int s = check_err_flag(ctx);
+  *dmax = ctx->host_scratch[0];
+  return s;
+}
+
+int afid_gpu_globals(afid_ctx_t *ctx, double ra_pr, double *nu_vol, double *ke, double *tmean) {
+  if (!ctx) return AFID_E_INVALID;
+  cudaSetDevice(ctx->dev);
+  const Geom &g = ctx->L.g;
+  AFID_CUDA(ctx, launch_globals(ctx->L, ctx->vx, ctx->vy, ctx->vz, ctx->temp, ctx->partial, ctx->gsum));
+  ctx->launches += 2;
+  AFID_CUDA(ctx, cudaMemcpyAsync(ctx->host_scratch, ctx->gsum, 3 * sizeof(double), cudaMemcpyDeviceToHost,
+                                 ctx->stream));
+  int s = check_err_flag(ctx);
+  // GlobalQuantities.F90:27,63-74
+  const double vol = 1.0 / (ctx->alx3 * g.dx * (double)g.nzm * (double)g.nym);
+  if (nu_vol) *nu_vol = 1.0 + std::sqrt(ra_pr) * ctx->host_scratch[0] * vol;
+  if (ke) *ke = 0.5 * ctx->host_scratch[1] * vol;
+  if (tmean) *tmean = ctx->host_scratch[2] * vol;
+  return s;
+}
+
+int afid_gpu_cuda_error(afid_ctx_t *ctx) { return ctx ? (int)ctx->last_cuda : 0; }
+
+int afid_gpu_field_device_ptr(afid_ctx_t *ctx, int which, void **dptr, int *ldx) {
+  if (!ctx || !dptr) return AFID_E_INVALID;
+  double *p = nullptr;
+  switch (which) {
+    case 0: p = ctx->vx; break;
+    case 1: p = ctx->vy; break;
+    case 2: p = ctx->vz; break;
+    case 3: p = ctx->temp; break;
+    case 4: p = ctx->pr; break;
+    default: return AFID_E_INVALID;
+  }
+  *dptr = p;
+  if (ldx) *ldx = ctx->L.g.ldx;
+  return AFID_OK;
+}
+
+long long afid_gpu_launch_count(afid_ctx_t *ctx) { return ctx ? ctx->launches : 0; }
+
+}  // extern "C"

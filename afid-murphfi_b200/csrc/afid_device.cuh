@@ -1,0 +1,201 @@
+// afid_device.cuh — device-side building blocks shared by the substep kernels.
+//
+// Layout in HBM (one context = one domain): every 3-D field is x-fastest like the reference's
+// Fortran arrays (param.F90:100-108) without halos: element (k, j, i) (0-based) sits at
+// k + ldx * (j + nym * i) with ldx >= nx = nxm + 1 padded to a multiple of 8 elements so that
+// each x-column starts on a 64-byte boundary.  Periodic y/z neighbours are reached by index
+// wrap instead of the reference's halo copies (update_halo, halo_common.F90:43-109).
+// The Poisson spectrum is complex, x-fastest: (k, ky, i|kz) at k + ldxc * (ky + nyh * i),
+// nyh = nym/2 + 1 — the reference's dphc / cz1 arrays (pressure.F90:120-134) in one layout.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace afid {
+
+constexpr int kWarp = 32;
+constexpr int kMaxFftPasses = 24;
+
+struct Geom {
+  int nxm, nym, nzm, nx;
+  int ldx;    // x stride of real fields (elements)
+  int nyh;    // nym/2 + 1
+  int ldxc;   // x stride of the complex spectrum (elements)
+  double dx, dy, dz, dyq, dzq;
+  double ren, pect, byct, gy;
+  double xplusu, xminusu;
+  int active_t, gaxis, inslws, inslwn, tfixs, tfixn;
+};
+
+// Device-resident per-substep scalars (written by the coefficient kernel, read by every
+// kernel of the substep, so a captured step graph does not depend on dt).
+struct StepCoef {
+  double al, ga, ro, dt, beta;
+};
+
+// 1-D metric tables on the device (0-based copies of the reference's arrays).
+struct Tables {
+  const double *udx3c, *udx3m, *idx;  // idx = 1/udx3m (ExplicitTermsVX.F90:194-196)
+  const double *ap3ck, *ac3ck, *am3ck;
+  const double *ap3sk, *ac3sk, *am3sk;
+  const double *ap3ssk, *ac3ssk, *am3ssk;
+  const double *amphk, *acphk, *apphk;
+  const double *ak1, *ak2;
+  const double *g3rc;
+  const double *tempbp, *temptp;  // nym*nzm, y fastest
+};
+
+struct FftPlan {
+  int n;
+  int npass;
+  int radix[kMaxFftPasses];
+};
+
+__device__ __forceinline__ int wrap_inc(int a, int n) { return (a + 1 == n) ? 0 : a + 1; }
+__device__ __forceinline__ int wrap_dec(int a, int n) { return (a == 0) ? n - 1 : a - 1; }
+
+__device__ __forceinline__ size_t col_off(const Geom &g, int j, int i) {
+  return (size_t)(j + (size_t)g.nym * i) * (size_t)g.ldx;
+}
+
+template <typename T> struct Cplx;
+template <> struct Cplx<double> { using type = double2; };
+template <> struct Cplx<float> { using type = float2; };
+
+template <typename C> __device__ __forceinline__ C cmul(C a, C b) {
+  C r;
+  r.x = a.x * b.x - a.y * b.y;
+  r.y = a.x * b.y + a.y * b.x;
+  return r;
+}
+template <typename C> __device__ __forceinline__ C cadd(C a, C b) {
+  C r;
+  r.x = a.x + b.x;
+  r.y = a.y + b.y;
+  return r;
+}
+template <typename C> __device__ __forceinline__ C csub(C a, C b) {
+  C r;
+  r.x = a.x - b.x;
+  r.y = a.y - b.y;
+  return r;
+}
+// multiply by -i (forward) or +i (inverse)
+template <bool INV, typename C> __device__ __forceinline__ C mul_mi(C a) {
+  C r;
+  if (INV) { r.x = -a.y; r.y = a.x; } else { r.x = a.y; r.y = -a.x; }
+  return r;
+}
+
+// ------------------------------------------------------------------------------------------
+// Shared-memory Stockham FFT (auto-sort), radices 2, 3, 4, 5, batch of B sequences of length
+// N stored contiguously (seq s at buf[s*N]).  Forward uses exp(-2 pi i m/N) twiddles from the
+// table tw[m] = (cos(2 pi m/N), -sin(2 pi m/N)); the inverse conjugates them and is
+// unnormalised, the FFTW_BACKWARD convention the reference uses (pressure.F90:189,193).
+// Pass p with radix R and Ns = product of earlier radices reads x[j + q*N/R] and writes
+// y[(j/Ns)*Ns*R + (j%Ns) + q*Ns] after twiddling input q by w^(q*(j%Ns)*N/(Ns*R)).
+// Returns the buffer holding the result.  All threads of the block must call it.
+// ------------------------------------------------------------------------------------------
+template <bool INV, typename T>
+__device__ typename Cplx<T>::type *fft_block(typename Cplx<T>::type *buf0,
+                                             typename Cplx<T>::type *buf1, int B,
+                                             const FftPlan &pl,
+                                             const typename Cplx<T>::type *__restrict__ tw) {
+  using C = typename Cplx<T>::type;
+  const int N = pl.n;
+  C *in = buf0, *out = buf1;
+  int Ns = 1;
+  for (int p = 0; p < pl.npass; ++p) {
+    const int R = pl.radix[p];
+    const int NR = N / R;
+    const int tstride = N / (Ns * R);
+    const int total = B * NR;
+    for (int b = threadIdx.x; b < total; b += blockDim.x) {
+      const int s = b / NR;
+      const int jj = b - s * NR;
+      const int k = jj % Ns;
+      const C *src = in + (size_t)s * N + jj;
+      C *dst = out + (size_t)s * N + (jj / Ns) * Ns * R + k;
+      C a[5];
+#pragma unroll
+      for (int q = 0; q < 5; ++q)
+        if (q < R) a[q] = src[q * NR];
+      if (Ns > 1) {
+#pragma unroll
+        for (int q = 1; q < 5; ++q) {
+          if (q < R) {
+            C w = tw[q * k * tstride];
+            if (INV) w.y = -w.y;
+            a[q] = cmul(a[q], w);
+          }
+        }
+      }
+      if (R == 2) {
+        dst[0] = cadd(a[0], a[1]);
+        dst[Ns] = csub(a[0], a[1]);
+      } else if (R == 4) {
+        C t0 = cadd(a[0], a[2]), t1 = csub(a[0], a[2]);
+        C t2 = cadd(a[1], a[3]), t3 = mul_mi<INV>(csub(a[1], a[3]));
+        dst[0] = cadd(t0, t2);
+        dst[Ns] = cadd(t1, t3);
+        dst[2 * Ns] = csub(t0, t2);
+        dst[3 * Ns] = csub(t1, t3);
+      } else if (R == 3) {
+        // y1,2 = a0 - (a1+a2)/2 -/+ i (sqrt(3)/2)(a1-a2) for the forward sign
+        const T s3 = (T)0.86602540378443864676;  // sqrt(3)/2
+        C t1 = cadd(a[1], a[2]);
+        C t2;
+        t2.x = a[0].x - (T)0.5 * t1.x;
+        t2.y = a[0].y - (T)0.5 * t1.y;
+        C d = csub(a[1], a[2]);
+        C t3 = mul_mi<INV>(d);
+        t3.x *= s3;
+        t3.y *= s3;
+        dst[0] = cadd(a[0], t1);
+        dst[Ns] = cadd(t2, t3);
+        dst[2 * Ns] = csub(t2, t3);
+      } else {  // R == 5
+        const T c1 = (T)0.30901699437494742410;   // cos(2 pi/5)
+        const T c2 = (T)-0.80901699437494742410;  // cos(4 pi/5)
+        const T s1 = (T)0.95105651629515357212;   // sin(2 pi/5)
+        const T s2 = (T)0.58778525229247312917;   // sin(4 pi/5)
+        C b1 = cadd(a[1], a[4]), b4 = csub(a[1], a[4]);
+        C b2 = cadd(a[2], a[3]), b3 = csub(a[2], a[3]);
+        C r1, r2;
+        r1.x = a[0].x + c1 * b1.x + c2 * b2.x;
+        r1.y = a[0].y + c1 * b1.y + c2 * b2.y;
+        r2.x = a[0].x + c2 * b1.x + c1 * b2.x;
+        r2.y = a[0].y + c2 * b1.y + c1 * b2.y;
+        C i1, i2;  // (s1*b4 + s2*b3) and (s2*b4 - s1*b3), then times -i (fwd)
+        i1.x = s1 * b4.x + s2 * b3.x;
+        i1.y = s1 * b4.y + s2 * b3.y;
+        i2.x = s2 * b4.x - s1 * b3.x;
+        i2.y = s2 * b4.y - s1 * b3.y;
+        i1 = mul_mi<INV>(i1);
+        i2 = mul_mi<INV>(i2);
+        C y0;
+        y0.x = a[0].x + b1.x + b2.x;
+        y0.y = a[0].y + b1.y + b2.y;
+        dst[0] = y0;
+        dst[Ns] = cadd(r1, i1);
+        dst[4 * Ns] = csub(r1, i1);
+        dst[2 * Ns] = cadd(r2, i2);
+        dst[3 * Ns] = csub(r2, i2);
+      }
+    }
+    __syncthreads();
+    C *t = in;
+    in = out;
+    out = t;
+    Ns *= R;
+  }
+  return in;
+}
+
+// ------------------------------------------------------------------------------------------
+// Bounded device-side waits: every spin in this library counts iterations and gives up with
+// an error flag instead of hanging (no trap, no unbounded loop).
+// ------------------------------------------------------------------------------------------
+constexpr long long kSpinLimit = 1LL << 26;
+
+}  // namespace afid

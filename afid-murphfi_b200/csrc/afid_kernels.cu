@@ -1,0 +1,1093 @@
+// afid_kernels.cu — sm_100a kernels of the RK3 flow + temperature substep.
+//
+// One substep (TimeMarcher.F90:38-133) is seven launches:
+//   K1 k_explicit_implicit  ExplicitTerms{VX,VY,VZ,Temp} + ImplicitAndUpdate* + SolveImpEqnUpdate_*
+//                           fused per x-column: one warp owns a (j,i) column, computes the four
+//                           explicit terms and RHS, stores rux/ruy/ruz/rutemp and solves the four
+//                           constant-matrix CN tridiagonals with a 32-chunk partition + PCR solve.
+//   K2 k_div_fft_y          CalcLocalDivergence (pressure.F90:141-162) fused with the forward
+//                           y r2c FFT (pressure.F90:174) and the 1/(nym*nzm) scaling (:179).
+//   K3 k_fft_z<fwd>         forward z c2c FFT (pressure.F90:176).
+//   K4 k_tridiag_pressure   SolveTridiagonalPressure (pressure.F90:201-236), warp per mode.
+//   K5 k_fft_z<inv>         backward z c2c FFT (pressure.F90:189).
+//   K6 k_ifft_y             backward y c2r FFT (pressure.F90:193) → phi.
+//   K7 k_correct            RemoveDivergence + CorrectPressure (pressure.F90:240-301).
+// plus k_cn_tables (once per step: CN factor tables for the three matrices and three substeps)
+// and the reductions k_cfl / k_divmax / k_globals.
+//
+// Template parameter TE is the type of the explicit terms and of the stored RK3 history
+// (double, or float for the mixed path); TS is the type of the spectral transforms.  The
+// state (vx, vy, vz, temp, pr), the RHS assembly and every tridiagonal solve are FP64.
+#include "afid_device.cuh"
+#include "afid_internal.h"
+
+namespace afid {
+
+// ------------------------------------------------------------------------------------------
+// CN tridiagonal factor tables.
+//
+// The matrices of SolveImpEqnUpdate_X.F90:27-42, SolveImpEqnUpdate_YZ.F90:96-105 and
+// SolveImpEqnUpdate_Temp.F90:154-165 are identical for every (j,i) column: rows normalised by
+// ackl_b = 1/(1 - ac*betadx), unit diagonal, a = -am*betadx*ackl_b, c = -ap*betadx*ackl_b.
+// For vx the identity rows 1 and nx (whose RHS is zeroed, SolveImpEqnUpdate_X.F90:56-57) are
+// eliminated, leaving rows k = 2..nxm.  Rows are split into 32 chunks of M (lane l owns rows
+// l*M .. l*M+M-1, padded with identity rows); the first row of each chunk is an interface
+// unknown.  Per lane the table holds the Thomas factors of the M-1 interior rows, their
+// responses v/w to unit interface values, and the coefficients of the 32-unknown reduced
+// system in PCR form.  Layout (doubles): [sc 32M][a 32M][inv 32M][cp 32M][v 32M][w 32M]
+// [as 32][cs 32][rinvB 32][pa 5x32][pg 5x32][pn 5x32], interior arrays as [q][lane].
+// ------------------------------------------------------------------------------------------
+__host__ __device__ inline size_t cn_table_size(int M) { return 192 * (size_t)M + 18 * 32; }
+
+struct CnMatrixDesc {
+  const double *am, *ac, *ap;
+  int off, n;          // first reference row (0-based) and number of unknowns
+  int temperature;     // betadx = 0.5*al*dt/pect instead of beta*al
+};
+
+struct CnBuildArgs {
+  CnMatrixDesc mat[3];
+  double al[3], ga[3], ro[3];
+  double dt, beta, pect;
+  int ns0, nsub;       // substeps ns0 .. ns0+nsub-1 are built
+};
+
+__global__ void k_cn_tables(CnBuildArgs args, int M, double *__restrict__ tab,
+                            StepCoef *__restrict__ sc) {
+  const int lane = threadIdx.x;
+  const int m = blockIdx.x % 3;
+  const int sub = blockIdx.x / 3;
+  const int ns = args.ns0 + sub;
+  const double al = args.al[sub];
+  if (m == 0 && lane == 0) {
+    StepCoef c;
+    c.al = al;
+    c.ga = args.ga[sub];
+    c.ro = args.ro[sub];
+    c.dt = args.dt;
+    c.beta = args.beta;
+    sc[ns] = c;
+  }
+  const CnMatrixDesc d = args.mat[m];
+  const double betadx = d.temperature ? 0.5 * al * args.dt / args.pect : args.beta * al;
+  double *T = tab + (size_t)(ns * 3 + m) * cn_table_size(M);
+  double *Tsc = T, *Ta = T + 32 * M, *Tinv = T + 64 * M, *Tcp = T + 96 * M, *Tv = T + 128 * M,
+         *Tw = T + 160 * M, *Tl = T + 192 * M;
+  const int n = d.n;
+  auto coef = [&](int r, double &a, double &c, double &s) {
+    if (r >= n) { a = 0.0; c = 0.0; s = 0.0; return; }
+    const int k = r + d.off;
+    const double ackl_b = 1.0 / (1.0 - d.ac[k] * betadx);
+    a = (r == 0) ? 0.0 : -d.am[k] * betadx * ackl_b;
+    c = (r == n - 1) ? 0.0 : -d.ap[k] * betadx * ackl_b;
+    s = ackl_b;
+  };
+  const int s0 = lane * M;
+  double as_, cs_, scl;
+  coef(s0, as_, cs_, scl);
+  Tsc[s0] = scl;
+  double cp_prev = 0.0, v_prev = 0.0;
+  for (int q = 1; q < M; ++q) {
+    double a, c, s;
+    coef(s0 + q, a, c, s);
+    Tsc[s0 + q] = s;
+    const double den = (q > 1) ? 1.0 - a * cp_prev : 1.0;
+    const double inv = 1.0 / den;
+    const double cp = c * inv;
+    const double vp = ((q == 1) ? -a : -a * v_prev) * inv;
+    const double wp = (q == M - 1) ? -c * inv : 0.0;
+    Ta[q * 32 + lane] = a;
+    Tinv[q * 32 + lane] = inv;
+    Tcp[q * 32 + lane] = cp;
+    Tv[q * 32 + lane] = vp;
+    Tw[q * 32 + lane] = wp;
+    cp_prev = cp;
+    v_prev = vp;
+  }
+  for (int q = M - 2; q >= 1; --q) {
+    Tv[q * 32 + lane] -= Tcp[q * 32 + lane] * Tv[(q + 1) * 32 + lane];
+    Tw[q * 32 + lane] -= Tcp[q * 32 + lane] * Tw[(q + 1) * 32 + lane];
+  }
+  double A, B, C;
+  if (M == 1) {
+    A = as_;
+    B = 1.0;
+    C = cs_;
+  } else {
+    double vl = __shfl_up_sync(0xffffffffu, Tv[(M - 1) * 32 + lane], 1);
+    double wl = __shfl_up_sync(0xffffffffu, Tw[(M - 1) * 32 + lane], 1);
+    if (lane == 0) { vl = 0.0; wl = 0.0; }
+    A = as_ * vl;
+    B = 1.0 + as_ * wl + cs_ * Tv[32 + lane];
+    C = (lane == 31) ? 0.0 : cs_ * Tw[32 + lane];
+  }
+  const double rinvB = 1.0 / B;
+  Tl[lane] = as_;
+  Tl[32 + lane] = cs_;
+  Tl[64 + lane] = rinvB;
+  double al_ = A * rinvB, ga_ = C * rinvB;
+  for (int lev = 0, h = 1; lev < 5; ++lev, h <<= 1) {
+    double am = __shfl_up_sync(0xffffffffu, al_, h);
+    double gm = __shfl_up_sync(0xffffffffu, ga_, h);
+    double ap = __shfl_down_sync(0xffffffffu, al_, h);
+    double gp = __shfl_down_sync(0xffffffffu, ga_, h);
+    if (lane < h) { am = 0.0; gm = 0.0; }
+    if (lane + h >= 32) { ap = 0.0; gp = 0.0; }
+    const double nrm = 1.0 / (1.0 - al_ * gm - ga_ * ap);
+    Tl[96 + lev * 32 + lane] = al_;
+    Tl[256 + lev * 32 + lane] = ga_;
+    Tl[416 + lev * 32 + lane] = nrm;
+    const double na = -al_ * am * nrm, ng = -ga_ * gp * nrm;
+    al_ = na;
+    ga_ = ng;
+  }
+}
+
+// Solve one column whose scaled RHS sits in s[q*32 + lane] (chunk layout); the solution
+// overwrites it.  Constant-matrix version using the tables above.
+template <int M>
+__device__ __forceinline__ void cn_solve_chunk(double *__restrict__ s, const double *__restrict__ T,
+                                               int lane) {
+  const double *Ta = T + 32 * M, *Tinv = T + 64 * M, *Tcp = T + 96 * M, *Tv = T + 128 * M,
+               *Tw = T + 160 * M, *Tl = T + 192 * M;
+  double y[M];
+#pragma unroll
+  for (int q = 0; q < M; ++q) y[q] = s[q * 32 + lane];
+  if constexpr (M > 1) {
+    y[1] = y[1] * __ldg(Tinv + 32 + lane);
+#pragma unroll
+    for (int q = 2; q < M; ++q)
+      y[q] = (y[q] - __ldg(Ta + q * 32 + lane) * y[q - 1]) * __ldg(Tinv + q * 32 + lane);
+#pragma unroll
+    for (int q = M - 2; q >= 1; --q) y[q] = y[q] - __ldg(Tcp + q * 32 + lane) * y[q + 1];
+  }
+  double D;
+  if constexpr (M > 1) {
+    double yprev = __shfl_up_sync(0xffffffffu, y[M - 1], 1);
+    if (lane == 0) yprev = 0.0;
+    D = y[0] - __ldg(Tl + lane) * yprev - __ldg(Tl + 32 + lane) * y[1];
+  } else {
+    D = y[0];
+  }
+  double delta = D * __ldg(Tl + 64 + lane);
+#pragma unroll
+  for (int lev = 0, h = 1; lev < 5; ++lev, h <<= 1) {
+    double dm = __shfl_up_sync(0xffffffffu, delta, h);
+    double dp = __shfl_down_sync(0xffffffffu, delta, h);
+    if (lane < h) dm = 0.0;
+    if (lane + h >= 32) dp = 0.0;
+    delta = (delta - __ldg(Tl + 96 + lev * 32 + lane) * dm - __ldg(Tl + 256 + lev * 32 + lane) * dp) *
+            __ldg(Tl + 416 + lev * 32 + lane);
+  }
+  double xnext = __shfl_down_sync(0xffffffffu, delta, 1);
+  if (lane == 31) xnext = 0.0;
+  s[lane] = delta;
+#pragma unroll
+  for (int q = 1; q < M; ++q)
+    s[q * 32 + lane] = y[q] + __ldg(Tv + q * 32 + lane) * delta + __ldg(Tw + q * 32 + lane) * xnext;
+}
+
+// ------------------------------------------------------------------------------------------
+// Explicit terms + RHS, one (k, j, i) point each.  Expressions follow the reference loop
+// bodies term by term; TE is the arithmetic type of the explicit terms.
+// ------------------------------------------------------------------------------------------
+struct Cols {
+  size_t c, jp, jm, ip, im, jmip, jpim;
+  int j, i;
+};
+
+template <typename TE> __device__ __forceinline__ TE ldc(const double *p) { return (TE)__ldg(p); }
+
+// ExplicitTermsVX.F90:194-291 + ImplicitAndUpdateVX.F90:124-150, k = 1..nxm-1 (0-based)
+template <typename TE, typename TR>
+__device__ __forceinline__ double rhs_vx(const Geom &g, const Tables &t, const StepCoef &sc,
+                                         const Cols &o, int k, const double *__restrict__ vx,
+                                         const double *__restrict__ vy,
+                                         const double *__restrict__ vz,
+                                         const double *__restrict__ temp,
+                                         const double *__restrict__ pr, TR *__restrict__ rux) {
+  const int km = k - 1, kp = k + 1;
+  const TE udy = (TE)(g.dy * 0.25), udz = (TE)(g.dz * 0.25);
+  const TE udyq = (TE)(g.dyq / g.ren), udzq = (TE)(g.dzq / g.ren);
+  const TE idxm = ldc<TE>(t.idx + km), idxc = ldc<TE>(t.idx + k);
+  const TE udx3c = ldc<TE>(t.udx3c + k);
+  const TE vxc = ldc<TE>(vx + o.c + k);
+  const TE vxkp = ldc<TE>(vx + o.c + kp), vxkm = ldc<TE>(vx + o.c + km);
+  const TE vxip = ldc<TE>(vx + o.ip + k), vxim = ldc<TE>(vx + o.im + k);
+  const TE vxjp = ldc<TE>(vx + o.jp + k), vxjm = ldc<TE>(vx + o.jm + k);
+  const TE hxz = udx3c * udz *
+                 ((idxm * ldc<TE>(vz + o.ip + km) + idxc * ldc<TE>(vz + o.ip + k)) * (vxip + vxc) -
+                  (idxm * ldc<TE>(vz + o.c + km) + idxc * ldc<TE>(vz + o.c + k)) * (vxc + vxim));
+  const TE hxy = udx3c * udy *
+                 ((idxm * ldc<TE>(vy + o.jp + km) + idxc * ldc<TE>(vy + o.jp + k)) * (vxjp + vxc) -
+                  (idxm * ldc<TE>(vy + o.c + km) + idxc * ldc<TE>(vy + o.c + k)) * (vxc + vxjm));
+  const TE hxx = ((vxkp + vxc) * (vxkp + vxc) - (vxc + vxkm) * (vxc + vxkm)) * udx3c * (TE)0.25;
+  const TE dzzvx = (vxim - (TE)2.0 * vxc + vxip) * udzq;
+  const TE dyyvx = (vxjm - (TE)2.0 * vxc + vxjp) * udyq;
+  TE qcap = -(hxx + hxy + hxz) + dyyvx + dzzvx;
+  if (g.gaxis == 1) {
+    const TE tempit = (TE)g.active_t * (TE)0.5 * (ldc<TE>(temp + o.c + k) + ldc<TE>(temp + o.c + km));
+    qcap = qcap + (TE)g.byct * tempit;
+  }
+  const double alre = sc.al / g.ren;
+  const double udx3 = sc.al * __ldg(t.udx3c + k);
+  const double dxxvx = __ldg(vx + o.c + kp) * __ldg(t.ap3ck + k) + __ldg(vx + o.c + k) * __ldg(t.ac3ck + k) +
+                       __ldg(vx + o.c + km) * __ldg(t.am3ck + k);
+  const double dxp = (__ldg(pr + o.c + k) - __ldg(pr + o.c + km)) * udx3;
+  const double rhs = (sc.ga * (double)qcap + sc.ro * (double)rux[o.c + k] + alre * dxxvx - dxp) * sc.dt;
+  rux[o.c + k] = (TR)qcap;
+  return rhs;
+}
+
+// ExplicitTermsVY.F90:23-122 + ImplicitAndUpdateVY.F90:28-80, k = 0..nxm-1
+template <typename TE, typename TR>
+__device__ __forceinline__ double rhs_vy(const Geom &g, const Tables &t, const StepCoef &sc,
+                                         const Cols &o, int k, const double *__restrict__ vx,
+                                         const double *__restrict__ vy,
+                                         const double *__restrict__ vz,
+                                         const double *__restrict__ temp,
+                                         const double *__restrict__ pr, TR *__restrict__ ruy) {
+  const int kmm = (k == 0) ? 0 : k - 1;
+  const int kpp = (k == g.nxm - 1) ? k : k + 1;
+  const int kp = k + 1;
+  const TE udy = (TE)(g.dy * 0.25), udz = (TE)(g.dz * 0.25);
+  const TE udyq = (TE)(g.dyq / g.ren), udzq = (TE)(g.dzq / g.ren);
+  const TE c = ldc<TE>(vy + o.c + k);
+  const TE vyjp = ldc<TE>(vy + o.jp + k), vyjm = ldc<TE>(vy + o.jm + k);
+  const TE vyip = ldc<TE>(vy + o.ip + k), vyim = ldc<TE>(vy + o.im + k);
+  const TE hyx = ((ldc<TE>(vx + o.c + kp) + ldc<TE>(vx + o.jm + kp)) * (ldc<TE>(vy + o.c + kpp) + c) -
+                  (ldc<TE>(vx + o.c + k) + ldc<TE>(vx + o.jm + k)) * (c + ldc<TE>(vy + o.c + kmm))) *
+                 ldc<TE>(t.udx3m + k) * (TE)0.25;
+  const TE hyy = ((vyjp + c) * (vyjp + c) - (vyjm + c) * (vyjm + c)) * udy;
+  const TE hyz = ((vyip + c) * (ldc<TE>(vz + o.ip + k) + ldc<TE>(vz + o.jmip + k)) -
+                  (c + vyim) * (ldc<TE>(vz + o.c + k) + ldc<TE>(vz + o.jm + k))) *
+                 udz;
+  const TE dyyvy = (vyjp - (TE)2.0 * c + vyjm) * udyq;
+  const TE dzzvy = (vyip - (TE)2.0 * c + vyim) * udzq;
+  TE dph = -(hyx + hyy + hyz) + dyyvy + dzzvy + (TE)g.gy;
+  if (g.gaxis == 2) {
+    const TE tempit = (TE)g.active_t * (TE)0.5 * (ldc<TE>(temp + o.c + k) + ldc<TE>(temp + o.jm + k));
+    dph = dph + (TE)g.byct * tempit;
+  }
+  const double alre = sc.al / g.ren;
+  const double udyp = g.dy * sc.al;
+  const double amm = __ldg(t.am3sk + k), acc = __ldg(t.ac3sk + k), app = __ldg(t.ap3sk + k);
+  const double cd = __ldg(vy + o.c + k);
+  double dxxvy;
+  if (k == 0)
+    dxxvy = __ldg(vy + o.c + kpp) * app + cd * acc - (acc + app) * g.xminusu * g.inslws;
+  else if (k == g.nxm - 1)
+    dxxvy = -(acc + amm) * g.xplusu * g.inslwn + cd * acc + __ldg(vy + o.c + kmm) * amm;
+  else
+    dxxvy = __ldg(vy + o.c + kpp) * app + cd * acc + __ldg(vy + o.c + kmm) * amm;
+  const double dyp = (__ldg(pr + o.c + k) - __ldg(pr + o.jm + k)) * udyp;
+  const double rhs = (sc.ga * (double)dph + sc.ro * (double)ruy[o.c + k] + alre * dxxvy - dyp) * sc.dt;
+  ruy[o.c + k] = (TR)dph;
+  return rhs;
+}
+
+// ExplicitTermsVZ.F90:149-244 + ImplicitAndUpdateVZ.F90:121-161, k = 0..nxm-1
+template <typename TE, typename TR>
+__device__ __forceinline__ double rhs_vz(const Geom &g, const Tables &t, const StepCoef &sc,
+                                         const Cols &o, int k, const double *__restrict__ vx,
+                                         const double *__restrict__ vy,
+                                         const double *__restrict__ vz,
+                                         const double *__restrict__ temp,
+                                         const double *__restrict__ pr, TR *__restrict__ ruz) {
+  const int kmm = (k == 0) ? 0 : k - 1;
+  const int kpp = (k == g.nxm - 1) ? k : k + 1;
+  const int kp = k + 1;
+  const TE udy = (TE)(g.dy * 0.25), udz = (TE)(g.dz * 0.25);
+  const TE udyq = (TE)(g.dyq / g.ren), udzq = (TE)(g.dzq / g.ren);
+  const TE c = ldc<TE>(vz + o.c + k);
+  const TE vzip = ldc<TE>(vz + o.ip + k), vzim = ldc<TE>(vz + o.im + k);
+  const TE vzjp = ldc<TE>(vz + o.jp + k), vzjm = ldc<TE>(vz + o.jm + k);
+  const TE hzz = ((vzip + c) * (vzip + c) - (vzim + c) * (vzim + c)) * udz;
+  const TE hzy = ((ldc<TE>(vy + o.jp + k) + ldc<TE>(vy + o.jpim + k)) * (vzjp + c) -
+                  (ldc<TE>(vy + o.c + k) + ldc<TE>(vy + o.im + k)) * (c + vzjm)) *
+                 udy;
+  const TE hzx = ((ldc<TE>(vx + o.c + kp) + ldc<TE>(vx + o.im + kp)) * (ldc<TE>(vz + o.c + kpp) + c) -
+                  (ldc<TE>(vx + o.c + k) + ldc<TE>(vx + o.im + k)) * (c + ldc<TE>(vz + o.c + kmm))) *
+                 ldc<TE>(t.udx3m + k) * (TE)0.25;
+  const TE dzzvz = (vzip - (TE)2.0 * c + vzim) * udzq;
+  const TE dyyvz = (vzjp - (TE)2.0 * c + vzjm) * udyq;
+  TE dq = -(hzx + hzy + hzz) + dyyvz + dzzvz;
+  if (g.gaxis == 3) {
+    const TE tempit = (TE)g.active_t * (TE)0.5 * (ldc<TE>(temp + o.c + k) + ldc<TE>(temp + o.im + k));
+    dq = dq + (TE)g.byct * tempit;
+  }
+  const double alre = sc.al / g.ren;
+  const double amm = __ldg(t.am3sk + k), acc = __ldg(t.ac3sk + k), app = __ldg(t.ap3sk + k);
+  const double dxxvz = __ldg(vz + o.c + kpp) * app + __ldg(vz + o.c + k) * acc + __ldg(vz + o.c + kmm) * amm;
+  const double dzp = (__ldg(pr + o.c + k) - __ldg(pr + o.im + k)) * g.dz * sc.al;
+  const double rhs = (sc.ga * (double)dq + sc.ro * (double)ruz[o.c + k] + alre * dxxvz - dzp) * sc.dt;
+  ruz[o.c + k] = (TR)dq;
+  return rhs;
+}
+
+// ExplicitTermsTemp.F90:22-77 + ImplicitAndUpdateTemp.F90:197-237, k = 0..nxm-1
+template <typename TE, typename TR>
+__device__ __forceinline__ double rhs_temp(const Geom &g, const Tables &t, const StepCoef &sc,
+                                           const Cols &o, int k, const double *__restrict__ vx,
+                                           const double *__restrict__ vy,
+                                           const double *__restrict__ vz,
+                                           const double *__restrict__ temp,
+                                           TR *__restrict__ rut) {
+  const TE udz = (TE)(g.dz * 0.5), udy = (TE)(g.dy * 0.5);
+  const TE udzq = (TE)(g.dzq / g.pect), udyq = (TE)(g.dyq / g.pect);
+  const size_t pl = (size_t)o.j + (size_t)g.nym * o.i;
+  const double tbp = __ldg(t.tempbp + pl), ttp = __ldg(t.temptp + pl);
+  const TE tc = ldc<TE>(temp + o.c + k);
+  const TE ux = ldc<TE>(t.udx3m + k);
+  TE htx;
+  if (k == 0)
+    htx = (ldc<TE>(vx + o.c + 1) * (ldc<TE>(temp + o.c + 1) + tc) - ldc<TE>(vx + o.c) * (TE)2.0 * (TE)tbp) *
+          (TE)0.5 * ux;
+  else if (k == g.nxm - 1)
+    htx = (ldc<TE>(vx + o.c + k + 1) * (TE)2.0 * (TE)ttp -
+           ldc<TE>(vx + o.c + k) * (tc + ldc<TE>(temp + o.c + k - 1))) *
+          (TE)0.5 * ux;
+  else
+    htx = (ldc<TE>(vx + o.c + k + 1) * (ldc<TE>(temp + o.c + k + 1) + tc) -
+           ldc<TE>(vx + o.c + k) * (tc + ldc<TE>(temp + o.c + k - 1))) *
+          (TE)0.5 * ux;
+  const TE tip = ldc<TE>(temp + o.ip + k), tim = ldc<TE>(temp + o.im + k);
+  const TE tjp = ldc<TE>(temp + o.jp + k), tjm = ldc<TE>(temp + o.jm + k);
+  const TE htz = (ldc<TE>(vz + o.ip + k) * (tip + tc) - ldc<TE>(vz + o.c + k) * (tc + tim)) * udz;
+  const TE hty = (ldc<TE>(vy + o.jp + k) * (tjp + tc) - ldc<TE>(vy + o.c + k) * (tc + tjm)) * udy;
+  const TE dzzt = (tip - (TE)2.0 * tc + tim) * udzq;
+  const TE dyyt = (tjp - (TE)2.0 * tc + tjm) * udyq;
+  const TE hro = -(htx + hty + htz) + dyyt + dzzt;
+  const double alpec = sc.al / g.pect;
+  const double tcd = __ldg(temp + o.c + k);
+  double dxxt;
+  if (k == 0)
+    dxxt = __ldg(temp + o.c + 1) * __ldg(t.ap3ssk) + tcd * __ldg(t.ac3ssk) -
+           (__ldg(t.ap3ssk) + __ldg(t.ac3ssk)) * tbp * g.tfixs;
+  else if (k == g.nxm - 1)
+    dxxt = tcd * __ldg(t.ac3ssk + k) + __ldg(temp + o.c + k - 1) * __ldg(t.am3ssk + k) -
+           (__ldg(t.am3ssk + k) + __ldg(t.ac3ssk + k)) * ttp * g.tfixn;
+  else
+    dxxt = __ldg(temp + o.c + k + 1) * __ldg(t.ap3ssk + k) + tcd * __ldg(t.ac3ssk + k) +
+           __ldg(temp + o.c + k - 1) * __ldg(t.am3ssk + k);
+  const double rhs = (sc.ga * (double)hro + sc.ro * (double)rut[o.c + k] + alpec * dxxt) * sc.dt;
+  rut[o.c + k] = (TR)hro;
+  return rhs;
+}
+
+// K1: one warp per (j,i) column, WPB columns per block.  Per warp shared memory holds the four
+// scaled RHS columns in chunk layout ([q][lane], row r at (r%M)*32 + r/M).
+template <int M, int WPB, typename TE>
+__global__ void __launch_bounds__(WPB * 32)
+    k_explicit_implicit(Geom g, Tables t, const StepCoef *__restrict__ sc_all, int ns,
+                        const double *__restrict__ cn_tab, const double *__restrict__ vx,
+                        const double *__restrict__ vy, const double *__restrict__ vz,
+                        const double *__restrict__ temp, const double *__restrict__ pr,
+                        TE *__restrict__ rux, TE *__restrict__ ruy, TE *__restrict__ ruz,
+                        TE *__restrict__ rut, double *__restrict__ vx_o, double *__restrict__ vy_o,
+                        double *__restrict__ vz_o, double *__restrict__ temp_o) {
+  extern __shared__ double smem_k1[];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int colid = blockIdx.x * WPB + warp;
+  if (colid >= g.nym * g.nzm) return;  // whole warp leaves; no block-wide barrier below
+  double *s_x = smem_k1 + warp * (4 * 32 * M);
+  double *s_y = s_x + 32 * M, *s_z = s_x + 64 * M, *s_t = s_x + 96 * M;
+  Cols o;
+  o.j = colid % g.nym;
+  o.i = colid / g.nym;
+  const int jp = wrap_inc(o.j, g.nym), jm = wrap_dec(o.j, g.nym);
+  const int ip = wrap_inc(o.i, g.nzm), im = wrap_dec(o.i, g.nzm);
+  o.c = col_off(g, o.j, o.i);
+  o.jp = col_off(g, jp, o.i);
+  o.jm = col_off(g, jm, o.i);
+  o.ip = col_off(g, o.j, ip);
+  o.im = col_off(g, o.j, im);
+  o.jmip = col_off(g, jm, ip);
+  o.jpim = col_off(g, jp, im);
+  const StepCoef sc = sc_all[ns];
+  const size_t tsz = cn_table_size(M);
+  const double *TX = cn_tab + (size_t)(ns * 3 + 0) * tsz;
+  const double *TY = cn_tab + (size_t)(ns * 3 + 1) * tsz;
+  const double *TT = cn_tab + (size_t)(ns * 3 + 2) * tsz;
+  const int nxm = g.nxm;
+
+#pragma unroll 1
+  for (int tt = 0; tt < M; ++tt) {
+    const int r = lane + 32 * tt;
+    const int sidx = (r % M) * 32 + r / M;
+    double dx_ = 0.0, dy_ = 0.0, dz_ = 0.0, dt_ = 0.0;
+    if (r < nxm - 1)
+      dx_ = rhs_vx<TE, TE>(g, t, sc, o, r + 1, vx, vy, vz, temp, pr, rux) * __ldg(TX + r);
+    if (r < nxm) {
+      const double syz = __ldg(TY + r);
+      dy_ = rhs_vy<TE, TE>(g, t, sc, o, r, vx, vy, vz, temp, pr, ruy) * syz;
+      dz_ = rhs_vz<TE, TE>(g, t, sc, o, r, vx, vy, vz, temp, pr, ruz) * syz;
+      dt_ = rhs_temp<TE, TE>(g, t, sc, o, r, vx, vy, vz, temp, rut) * __ldg(TT + r);
+    }
+    s_x[sidx] = dx_;
+    s_y[sidx] = dy_;
+    s_z[sidx] = dz_;
+    s_t[sidx] = dt_;
+  }
+  __syncwarp();
+  cn_solve_chunk<M>(s_x, TX, lane);
+  cn_solve_chunk<M>(s_y, TY, lane);
+  cn_solve_chunk<M>(s_z, TY, lane);
+  cn_solve_chunk<M>(s_t, TT, lane);
+  __syncwarp();
+#pragma unroll 1
+  for (int tt = 0; tt < M; ++tt) {
+    const int r = lane + 32 * tt;
+    const int sidx = (r % M) * 32 + r / M;
+    if (r < nxm - 1) vx_o[o.c + r + 1] = __ldg(vx + o.c + r + 1) + s_x[sidx];
+    if (r < nxm) {
+      vy_o[o.c + r] = __ldg(vy + o.c + r) + s_y[sidx];
+      vz_o[o.c + r] = __ldg(vz + o.c + r) + s_z[sidx];
+      temp_o[o.c + r] = __ldg(temp + o.c + r) + s_t[sidx];
+    }
+  }
+  // ImplicitAndUpdateVX.F90:171-172: vx(1) = vx(nx) = 0
+  if (lane == 0) vx_o[o.c] = 0.0;
+  if (lane == 1) vx_o[o.c + g.nx - 1] = 0.0;
+}
+
+// ------------------------------------------------------------------------------------------
+// K2: divergence (pressure.F90:147-158) fused with the forward y r2c FFT (pressure.F90:174)
+// and the 1/(nym*nzm) normalisation (pressure.F90:179).  Block = (x tile of TX points, z
+// index i).  Pairs of x points are packed as one complex sequence (re, im), transformed, and
+// split with X_k = (Z_k + conj Z_{N-k})/2, Y_k = (Z_k - conj Z_{N-k})/(2i).
+// ------------------------------------------------------------------------------------------
+template <int TX, typename TS>
+__global__ void __launch_bounds__(256)
+    k_div_fft_y(Geom g, Tables t, const StepCoef *__restrict__ sc_all, int ns,
+                const double *__restrict__ vx, const double *__restrict__ vy,
+                const double *__restrict__ vz, typename Cplx<TS>::type *__restrict__ spec,
+                FftPlan pl, const typename Cplx<TS>::type *__restrict__ tw) {
+  using C = typename Cplx<TS>::type;
+  extern __shared__ __align__(16) unsigned char smem_raw_k2[];
+  C *b0 = reinterpret_cast<C *>(smem_raw_k2);
+  const int N = g.nym, B = TX / 2;
+  C *b1 = b0 + (size_t)B * N;
+  const int k0 = blockIdx.x * TX, i = blockIdx.y;
+  const int ip = wrap_inc(i, g.nzm);
+  const StepCoef sc = sc_all[ns];
+  const double usdtal = 1.0 / (sc.dt * sc.al);
+  const int tx = threadIdx.x % TX;
+  const int k = k0 + tx;
+  for (int j = threadIdx.x / TX; j < N; j += blockDim.x / TX) {
+    double dv = 0.0;
+    if (k < g.nxm) {
+      const int jp = wrap_inc(j, N);
+      const size_t c = col_off(g, j, i), cjp = col_off(g, jp, i), cip = col_off(g, j, ip);
+      const double dqcap = (__ldg(vz + cip + k) - __ldg(vz + c + k)) * g.dz +
+                           (__ldg(vy + cjp + k) - __ldg(vy + c + k)) * g.dy +
+                           (__ldg(vx + c + k + 1) - __ldg(vx + c + k)) * __ldg(t.udx3m + k);
+      dv = dqcap * usdtal;
+    }
+    TS *d = reinterpret_cast<TS *>(&b0[(size_t)(tx >> 1) * N + j]);
+    d[tx & 1] = (TS)dv;
+  }
+  __syncthreads();
+  C *res = fft_block<false, TS>(b0, b1, B, pl, tw);
+  const TS norm = (TS)(1.0 / ((double)g.nzm * (double)g.nym));
+  const TS half = (TS)0.5;
+  for (int e = threadIdx.x; e < g.nyh * TX; e += blockDim.x) {
+    const int ex = e % TX, ky = e / TX;
+    const int kk = k0 + ex;
+    if (kk >= g.nxm) continue;
+    const int p = ex >> 1;
+    const C zk = res[(size_t)p * N + ky];
+    const C zn = res[(size_t)p * N + (ky == 0 ? 0 : N - ky)];
+    C X;
+    if ((ex & 1) == 0) {
+      X.x = (zk.x + zn.x) * half;
+      X.y = (zk.y - zn.y) * half;
+    } else {
+      X.x = (zk.y + zn.y) * half;
+      X.y = (zn.x - zk.x) * half;
+    }
+    X.x *= norm;
+    X.y *= norm;
+    spec[(size_t)(ky + (size_t)g.nyh * i) * g.ldxc + kk] = X;
+  }
+}
+
+// K3 / K5: z c2c FFT in place on the spectrum.  Block = (x tile of TXZ points, ky).
+template <int TXZ, bool INV, typename TS>
+__global__ void __launch_bounds__(256)
+    k_fft_z(Geom g, typename Cplx<TS>::type *__restrict__ spec, FftPlan pl,
+            const typename Cplx<TS>::type *__restrict__ tw) {
+  using C = typename Cplx<TS>::type;
+  extern __shared__ __align__(16) unsigned char smem_raw_k3[];
+  C *b0 = reinterpret_cast<C *>(smem_raw_k3);
+  const int N = g.nzm;
+  C *b1 = b0 + (size_t)TXZ * N;
+  const int k0 = blockIdx.x * TXZ, ky = blockIdx.y;
+  const size_t zstride = (size_t)g.nyh * g.ldxc;
+  C *base = spec + (size_t)ky * g.ldxc + k0;
+  for (int e = threadIdx.x; e < N * TXZ; e += blockDim.x) {
+    const int ex = e % TXZ, iz = e / TXZ;
+    C v;
+    v.x = 0;
+    v.y = 0;
+    if (k0 + ex < g.nxm) v = base[(size_t)iz * zstride + ex];
+    b0[(size_t)ex * N + iz] = v;
+  }
+  __syncthreads();
+  C *res = fft_block<INV, TS>(b0, b1, TXZ, pl, tw);
+  for (int e = threadIdx.x; e < N * TXZ; e += blockDim.x) {
+    const int ex = e % TXZ, iz = e / TXZ;
+    if (k0 + ex < g.nxm) base[(size_t)iz * zstride + ex] = res[(size_t)ex * N + iz];
+  }
+}
+
+// ------------------------------------------------------------------------------------------
+// K4: per (ky, kz) mode, the normalised complex tridiagonal of pressure.F90:209-232:
+// a_k = amphk(k)/(acphk(k)-ak2(j)-ak1(i)), c_k = apphk(k)/(...), diagonal 1+1e-15, RHS scaled
+// by the same factor.  One warp per mode; rows are split into 32 chunks of M (partition +
+// PCR as in the CN solve, with factors computed per mode).  The (0,0) mode is singular up to
+// the 1e-15 shift (the reference lets LAPACK return an arbitrary constant); here its last
+// equation is replaced by phi = 0, which fixes that constant without changing gradients.
+// A zero pivot sets AFID_E_SINGULAR (the reference aborts, pressure.F90:225-229).
+// ------------------------------------------------------------------------------------------
+template <int M, int WPB, typename TS>
+__global__ void __launch_bounds__(WPB * 32)
+    k_tridiag_pressure(Geom g, Tables t, typename Cplx<TS>::type *__restrict__ spec,
+                       int *__restrict__ err) {
+  using C = typename Cplx<TS>::type;
+  extern __shared__ double smem_k4[];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int sys = blockIdx.x * WPB + warp;
+  if (sys >= g.nyh * g.nzm) return;
+  const int ky = sys % g.nyh, kz = sys / g.nyh;
+  const bool pin = (ky == 0 && kz == 0);
+  double *sa = smem_k4 + warp * (4 * 32 * M);
+  double *sc_ = sa + 32 * M, *sdr = sa + 64 * M, *sdi = sa + 96 * M;
+  C *colp = spec + (size_t)sys * g.ldxc;
+  const int n = g.nxm;
+  const double akj = __ldg(t.ak2 + ky), aki = __ldg(t.ak1 + kz);
+#pragma unroll 1
+  for (int tt = 0; tt < M; ++tt) {
+    const int r = lane + 32 * tt;
+    const int s = (r % M) * 32 + r / M;
+    double a = 0.0, c = 0.0, dr = 0.0, di = 0.0;
+    if (r < n) {
+      const double f = 1.0 / (__ldg(t.acphk + r) - akj - aki);
+      a = (r > 0) ? __ldg(t.amphk + r) * f : 0.0;
+      c = (r < n - 1) ? __ldg(t.apphk + r) * f : 0.0;
+      const C v = colp[r];
+      dr = (double)v.x * f;
+      di = (double)v.y * f;
+      if (pin && r == n - 1) { a = 0.0; dr = 0.0; di = 0.0; }
+    }
+    sa[s] = a;
+    sc_[s] = c;
+    sdr[s] = dr;
+    sdi[s] = di;
+  }
+  __syncwarp();
+  const int s0 = lane * M;
+  auto diag = [&](int r) -> double { return (r < n && !(pin && r == n - 1)) ? 1.0 + 1.0e-15 : 1.0; };
+  double cp[M], yr[M], yi[M], v[M], w[M];
+  bool bad = false;
+  cp[0] = 0.0; yr[0] = 0.0; yi[0] = 0.0; v[0] = 0.0; w[0] = 0.0;
+#pragma unroll
+  for (int q = 1; q < M; ++q) {
+    const double a = sa[q * 32 + lane], c = sc_[q * 32 + lane];
+    const double den = (q > 1) ? diag(s0 + q) - a * cp[q - 1] : diag(s0 + q);
+    bad |= (den == 0.0);
+    const double inv = 1.0 / den;
+    cp[q] = c * inv;
+    const double dr = sdr[q * 32 + lane], di = sdi[q * 32 + lane];
+    if (q > 1) {
+      yr[q] = (dr - a * yr[q - 1]) * inv;
+      yi[q] = (di - a * yi[q - 1]) * inv;
+      v[q] = -a * v[q - 1] * inv;
+    } else {
+      yr[q] = dr * inv;
+      yi[q] = di * inv;
+      v[q] = -a * inv;
+    }
+    w[q] = (q == M - 1) ? -c * inv : 0.0;
+  }
+#pragma unroll
+  for (int q = M - 2; q >= 1; --q) {
+    yr[q] -= cp[q] * yr[q + 1];
+    yi[q] -= cp[q] * yi[q + 1];
+    v[q] -= cp[q] * v[q + 1];
+    w[q] -= cp[q] * w[q + 1];
+  }
+  const double as_ = sa[lane], cs_ = sc_[lane];
+  double A, B, Cc, Dr, Di;
+  if constexpr (M == 1) {
+    A = as_;
+    B = diag(s0);
+    Cc = cs_;
+    Dr = sdr[lane];
+    Di = sdi[lane];
+  } else {
+    double vl = __shfl_up_sync(0xffffffffu, v[M - 1], 1);
+    double wl = __shfl_up_sync(0xffffffffu, w[M - 1], 1);
+    double yl_r = __shfl_up_sync(0xffffffffu, yr[M - 1], 1);
+    double yl_i = __shfl_up_sync(0xffffffffu, yi[M - 1], 1);
+    if (lane == 0) { vl = 0.0; wl = 0.0; yl_r = 0.0; yl_i = 0.0; }
+    A = as_ * vl;
+    B = diag(s0) + as_ * wl + cs_ * v[1];
+    Cc = (lane == 31) ? 0.0 : cs_ * w[1];
+    Dr = sdr[lane] - as_ * yl_r - cs_ * yr[1];
+    Di = sdi[lane] - as_ * yl_i - cs_ * yi[1];
+  }
+  bad |= (B == 0.0);
+  const double rB = 1.0 / B;
+  double al_ = A * rB, ga_ = Cc * rB, er = Dr * rB, ei = Di * rB;
+#pragma unroll
+  for (int h = 1; h < 32; h <<= 1) {
+    double am = __shfl_up_sync(0xffffffffu, al_, h), gm = __shfl_up_sync(0xffffffffu, ga_, h);
+    double ap = __shfl_down_sync(0xffffffffu, al_, h), gp = __shfl_down_sync(0xffffffffu, ga_, h);
+    double erm = __shfl_up_sync(0xffffffffu, er, h), eim = __shfl_up_sync(0xffffffffu, ei, h);
+    double erp = __shfl_down_sync(0xffffffffu, er, h), eip = __shfl_down_sync(0xffffffffu, ei, h);
+    if (lane < h) { am = 0.0; gm = 0.0; erm = 0.0; eim = 0.0; }
+    if (lane + h >= 32) { ap = 0.0; gp = 0.0; erp = 0.0; eip = 0.0; }
+    const double dd = 1.0 - al_ * gm - ga_ * ap;
+    bad |= (dd == 0.0);
+    const double nrm = 1.0 / dd;
+    er = (er - al_ * erm - ga_ * erp) * nrm;
+    ei = (ei - al_ * eim - ga_ * eip) * nrm;
+    const double na = -al_ * am * nrm, ng = -ga_ * gp * nrm;
+    al_ = na;
+    ga_ = ng;
+  }
+  double xnr = __shfl_down_sync(0xffffffffu, er, 1), xni = __shfl_down_sync(0xffffffffu, ei, 1);
+  if (lane == 31) { xnr = 0.0; xni = 0.0; }
+  sdr[lane] = er;
+  sdi[lane] = ei;
+#pragma unroll
+  for (int q = 1; q < M; ++q) {
+    sdr[q * 32 + lane] = yr[q] + v[q] * er + w[q] * xnr;
+    sdi[q * 32 + lane] = yi[q] + v[q] * ei + w[q] * xni;
+  }
+  if (bad) atomicOr(err, 1);
+  __syncwarp();
+#pragma unroll 1
+  for (int tt = 0; tt < M; ++tt) {
+    const int r = lane + 32 * tt;
+    if (r < n) {
+      const int s = (r % M) * 32 + r / M;
+      C o;
+      o.x = (TS)sdr[s];
+      o.y = (TS)sdi[s];
+      colp[r] = o;
+    }
+  }
+}
+
+// K6: backward y c2r FFT (pressure.F90:193), unnormalised.  The half spectrum of two x
+// points is extended Hermitian-symmetrically (imaginary parts of the DC and Nyquist bins are
+// ignored, as a c2r transform does), packed as Z = X + iY, transformed, and split into
+// Re -> phi(k0), Im -> phi(k0+1).
+template <int TX, typename TS>
+__global__ void __launch_bounds__(256)
+    k_ifft_y(Geom g, const typename Cplx<TS>::type *__restrict__ spec, TS *__restrict__ phi,
+             FftPlan pl, const typename Cplx<TS>::type *__restrict__ tw) {
+  using C = typename Cplx<TS>::type;
+  extern __shared__ __align__(16) unsigned char smem_raw_k6[];
+  C *b0 = reinterpret_cast<C *>(smem_raw_k6);
+  const int N = g.nym, B = TX / 2;
+  C *b1 = b0 + (size_t)B * N;
+  const int k0 = blockIdx.x * TX, i = blockIdx.y;
+  for (int e = threadIdx.x; e < N * B; e += blockDim.x) {
+    const int p = e % B, j = e / B;
+    const bool cj = (2 * j > N);
+    const int jj = cj ? N - j : j;
+    const int ka = k0 + 2 * p, kb = ka + 1;
+    const C *src = spec + (size_t)(jj + (size_t)g.nyh * i) * g.ldxc;
+    C X, Y;
+    X.x = 0; X.y = 0; Y.x = 0; Y.y = 0;
+    if (ka < g.nxm) X = src[ka];
+    if (kb < g.nxm) Y = src[kb];
+    if (cj) { X.y = -X.y; Y.y = -Y.y; }
+    if (jj == 0 || 2 * jj == N) { X.y = 0; Y.y = 0; }
+    C Z;
+    Z.x = X.x - Y.y;
+    Z.y = X.y + Y.x;
+    b0[(size_t)p * N + j] = Z;
+  }
+  __syncthreads();
+  const C *res = fft_block<true, TS>(b0, b1, B, pl, tw);
+  for (int e = threadIdx.x; e < N * TX; e += blockDim.x) {
+    const int ex = e % TX, j = e / TX;
+    const int k = k0 + ex;
+    if (k >= g.nxm) continue;
+    const C z = res[(size_t)(ex >> 1) * N + j];
+    phi[col_off(g, j, i) + k] = (ex & 1) ? z.y : z.x;
+  }
+}
+
+// K7: RemoveDivergence (pressure.F90:245-266) out of place (intermediate velocities -> state)
+// and CorrectPressure (pressure.F90:276-300) in place.  Thread per (k, j, i).
+template <typename TS>
+__global__ void __launch_bounds__(256)
+    k_correct(Geom g, Tables t, const StepCoef *__restrict__ sc_all, int ns,
+              const double *__restrict__ vxh, const double *__restrict__ vyh,
+              const double *__restrict__ vzh, double *__restrict__ vx, double *__restrict__ vy,
+              double *__restrict__ vz, double *__restrict__ pr, const TS *__restrict__ phi) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int i = blockIdx.z;
+  if (k >= g.nxm || j >= g.nym) return;
+  const StepCoef sc = sc_all[ns];
+  const int jm = wrap_dec(j, g.nym), jp = wrap_inc(j, g.nym);
+  const int im = wrap_dec(i, g.nzm), ip = wrap_inc(i, g.nzm);
+  const int km = (k == 0) ? 0 : k - 1;
+  const int kp = (k == g.nxm - 1) ? k : k + 1;
+  const size_t c = col_off(g, j, i);
+  const double ph = (double)phi[c + k];
+  const double phkm = (double)phi[c + km], phkp = (double)phi[c + kp];
+  const double phjm = (double)phi[col_off(g, jm, i) + k], phjp = (double)phi[col_off(g, jp, i) + k];
+  const double phim = (double)phi[col_off(g, j, im) + k], phip = (double)phi[col_off(g, j, ip) + k];
+  const double aldt = sc.al * sc.dt;
+  const double udy = aldt * g.dy, udz = aldt * g.dz;
+  const double usukm = aldt * __ldg(t.udx3c + k);
+  vx[c + k] = __ldg(vxh + c + k) - (ph - phkm) * usukm;
+  vy[c + k] = __ldg(vyh + c + k) - (ph - phjm) * udy;
+  vz[c + k] = __ldg(vzh + c + k) - (ph - phim) * udz;
+  if (k == g.nxm - 1) vx[c + k + 1] = __ldg(vxh + c + k + 1);
+  const double be = sc.al * sc.beta;
+  const double amm = __ldg(t.amphk + k), acc = __ldg(t.acphk + k), app = __ldg(t.apphk + k);
+  pr[c + k] = pr[c + k] + ph -
+              be * ((phip - 2.0 * ph + phim) * g.dzq + (phjp - 2.0 * ph + phjm) * g.dyq +
+                    (phkp * app + ph * acc + phkm * amm));
+}
+
+// ------------------------------------------------------------------------------------------
+// Reductions.  Maxima of non-negative doubles are combined with atomicMax on their bit
+// patterns (order-preserving for x >= 0), so the result does not depend on block order.
+// ------------------------------------------------------------------------------------------
+__device__ __forceinline__ double warp_max(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+template <bool DIV>
+__global__ void __launch_bounds__(256)
+    k_max_reduce(Geom g, Tables t, const double *__restrict__ vx, const double *__restrict__ vy,
+                 const double *__restrict__ vz, unsigned long long *__restrict__ out) {
+  __shared__ double red[8];
+  double m = 0.0;
+  const int lane = threadIdx.x & 31;
+  const int ncol = g.nym * g.nzm;
+  const int wstride = gridDim.x * (blockDim.x >> 5);
+  for (int cidx = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); cidx < ncol; cidx += wstride) {
+    const int j = cidx % g.nym, i = cidx / g.nym;
+    const int jp = wrap_inc(j, g.nym), ip = wrap_inc(i, g.nzm);
+    const size_t c = col_off(g, j, i), cjp = col_off(g, jp, i), cip = col_off(g, j, ip);
+    for (int k = lane; k < g.nxm; k += 32) {
+      double q;
+      if (DIV) {  // CheckDivergence.F90:36-39
+        const double dq = (vz[cip + k] - vz[c + k]) * g.dz + (vy[cjp + k] - vy[c + k]) * g.dy +
+                          (vx[c + k + 1] - vx[c + k]) * t.udx3m[k];
+        q = fabs(dq);
+      } else {  // CalcMaxCFL.F90:36-40
+        q = fabs((vz[c + k] + vz[cip + k]) * 0.5 * g.dz) + fabs((vy[c + k] + vy[cjp + k]) * 0.5 * g.dy) +
+            fabs((vx[c + k] + vx[c + k + 1]) * 0.5 * t.udx3m[k]);
+      }
+      m = fmax(m, q);
+    }
+  }
+  m = warp_max(m);
+  if (lane == 0) red[threadIdx.x >> 5] = m;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    double v = (threadIdx.x < (blockDim.x >> 5)) ? red[threadIdx.x] : 0.0;
+    v = warp_max(v);
+    if (threadIdx.x == 0) atomicMax(out, (unsigned long long)__double_as_longlong(v));
+  }
+}
+
+// Volume sums of GlobalQuantities.F90:31-47 per block, written to partial[block*3 + {0,1,2}]
+// (T*vx_centre*g3rc, (vx^2+vy^2+vz^2)*g3rc, T*g3rc) and summed in fixed order afterwards.
+__global__ void __launch_bounds__(256)
+    k_globals_partial(Geom g, Tables t, const double *__restrict__ vx, const double *__restrict__ vy,
+                      const double *__restrict__ vz, const double *__restrict__ temp,
+                      double *__restrict__ partial) {
+  __shared__ double red[3][8];
+  double s0 = 0.0, s1 = 0.0, s2 = 0.0;
+  const int lane = threadIdx.x & 31;
+  const int ncol = g.nym * g.nzm;
+  const int wstride = gridDim.x * (blockDim.x >> 5);
+  for (int cidx = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); cidx < ncol; cidx += wstride) {
+    const size_t c = (size_t)cidx * g.ldx;
+    for (int k = lane; k < g.nxm; k += 32) {
+      const double fac2 = t.g3rc[k];
+      const double vxcen = (vx[c + k] + vx[c + k + 1]) * 0.5;
+      const double tc = temp[c + k];
+      s0 += tc * vxcen * fac2;
+      s1 += fac2 * (vz[c + k] * vz[c + k] + vy[c + k] * vy[c + k] + vx[c + k] * vx[c + k]);
+      s2 += tc * fac2;
+    }
+  }
+  s0 = warp_sum(s0);
+  s1 = warp_sum(s1);
+  s2 = warp_sum(s2);
+  if (lane == 0) {
+    red[0][threadIdx.x >> 5] = s0;
+    red[1][threadIdx.x >> 5] = s1;
+    red[2][threadIdx.x >> 5] = s2;
+  }
+  __syncthreads();
+  if (threadIdx.x < 3) {
+    double v = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) v += red[threadIdx.x][w];
+    partial[blockIdx.x * 3 + threadIdx.x] = v;
+  }
+}
+
+__global__ void k_sum_partials(const double *__restrict__ partial, int nblocks, double *__restrict__ out) {
+  __shared__ double red[3][8];
+  double s[3] = {0.0, 0.0, 0.0};
+  for (int b = threadIdx.x; b < nblocks; b += blockDim.x)
+    for (int q = 0; q < 3; ++q) s[q] += partial[b * 3 + q];
+  for (int q = 0; q < 3; ++q) {
+    s[q] = warp_sum(s[q]);
+    if ((threadIdx.x & 31) == 0) red[q][threadIdx.x >> 5] = s[q];
+  }
+  __syncthreads();
+  if (threadIdx.x < 3) {
+    double v = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) v += red[threadIdx.x][w];
+    out[threadIdx.x] = v;
+  }
+}
+
+// ==========================================================================================
+// Host-side launchers
+// ==========================================================================================
+static int pick_M(int nxm) {
+  const int need = (nxm + 31) / 32;
+  const int opts[] = {1, 2, 4, 8, 12, 16, 24, 32};
+  for (int m : opts)
+    if (m >= need) return m;
+  return -1;
+}
+
+int cn_choose_M(int nxm) { return pick_M(nxm); }
+size_t cn_tab_doubles(int M, int nsst) { return cn_table_size(M) * 3 * (size_t)nsst; }
+
+cudaError_t launch_cn_tables(const LaunchCtx &L, const CnInputs &in) {
+  CnBuildArgs a;
+  for (int m = 0; m < 3; ++m) {
+    a.mat[m].am = in.am[m];
+    a.mat[m].ac = in.ac[m];
+    a.mat[m].ap = in.ap[m];
+    a.mat[m].off = in.off[m];
+    a.mat[m].n = in.n[m];
+    a.mat[m].temperature = (m == 2);
+  }
+  for (int s = 0; s < 3; ++s) {
+    a.al[s] = in.al[s];
+    a.ga[s] = in.ga[s];
+    a.ro[s] = in.ro[s];
+  }
+  a.dt = in.dt;
+  a.beta = in.beta;
+  a.pect = in.pect;
+  a.ns0 = in.ns0;
+  a.nsub = in.nsub;
+  k_cn_tables<<<3 * in.nsub, 32, 0, L.stream>>>(a, in.M, in.tab, in.sc);
+  return cudaGetLastError();
+}
+
+template <int M, typename TE>
+static cudaError_t launch_k1_M(const LaunchCtx &L, const SubstepBuffers &b, int ns) {
+  constexpr int WPB = (M >= 16) ? 64 / M : 8;
+  constexpr int W = (WPB < 1) ? 1 : WPB;
+  const int ncol = L.g.nym * L.g.nzm;
+  const size_t smem = (size_t)W * 4 * 32 * M * sizeof(double);
+  auto kern = k_explicit_implicit<M, W, TE>;
+  cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  kern<<<(ncol + W - 1) / W, W * 32, smem, L.stream>>>(
+      L.g, L.t, b.sc, ns, b.cn_tab, b.vx, b.vy, b.vz, b.temp, b.pr, (TE *)b.rux, (TE *)b.ruy,
+      (TE *)b.ruz, (TE *)b.rut, b.vx_o, b.vy_o, b.vz_o, b.temp_o);
+  return cudaGetLastError();
+}
+
+template <typename TE>
+static cudaError_t launch_k1_T(const LaunchCtx &L, const SubstepBuffers &b, int ns) {
+  switch (L.M) {
+    case 1: return launch_k1_M<1, TE>(L, b, ns);
+    case 2: return launch_k1_M<2, TE>(L, b, ns);
+    case 4: return launch_k1_M<4, TE>(L, b, ns);
+    case 8: return launch_k1_M<8, TE>(L, b, ns);
+    case 12: return launch_k1_M<12, TE>(L, b, ns);
+    case 16: return launch_k1_M<16, TE>(L, b, ns);
+    case 24: return launch_k1_M<24, TE>(L, b, ns);
+    case 32: return launch_k1_M<32, TE>(L, b, ns);
+  }
+  return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_explicit_implicit(const LaunchCtx &L, const SubstepBuffers &b, int ns) {
+  return L.mixed ? launch_k1_T<float>(L, b, ns) : launch_k1_T<double>(L, b, ns);
+}
+
+template <int M, typename TS>
+static cudaError_t launch_k4_M(const LaunchCtx &L, void *spec, int *err) {
+  constexpr int W = (M >= 16) ? 2 : 4;
+  const int nsys = L.g.nyh * L.g.nzm;
+  const size_t smem = (size_t)W * 4 * 32 * M * sizeof(double);
+  auto kern = k_tridiag_pressure<M, W, TS>;
+  cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  kern<<<(nsys + W - 1) / W, W * 32, smem, L.stream>>>(L.g, L.t, (typename Cplx<TS>::type *)spec, err);
+  return cudaGetLastError();
+}
+
+template <typename TS>
+static cudaError_t launch_k4_T(const LaunchCtx &L, void *spec, int *err) {
+  switch (L.M) {
+    case 1: return launch_k4_M<1, TS>(L, spec, err);
+    case 2: return launch_k4_M<2, TS>(L, spec, err);
+    case 4: return launch_k4_M<4, TS>(L, spec, err);
+    case 8: return launch_k4_M<8, TS>(L, spec, err);
+    case 12: return launch_k4_M<12, TS>(L, spec, err);
+    case 16: return launch_k4_M<16, TS>(L, spec, err);
+    case 24: return launch_k4_M<24, TS>(L, spec, err);
+    case 32: return launch_k4_M<32, TS>(L, spec, err);
+  }
+  return cudaErrorInvalidValue;
+}
+
+template <typename TS>
+static cudaError_t launch_pressure_T(const LaunchCtx &L, const SubstepBuffers &b, int ns) {
+  using C = typename Cplx<TS>::type;
+  const Geom &g = L.g;
+  C *spec = (C *)b.spec;
+  const C *twy = (const C *)L.twy;
+  const C *twz = (const C *)L.twz;
+  cudaError_t e;
+  // K2 divergence + forward y FFT
+  {
+    const int TX = L.tx_y;
+    const size_t smem = (size_t)TX * g.nym * sizeof(C);  // 2 buffers of TX/2 sequences
+    dim3 grid((g.nxm + TX - 1) / TX, g.nzm);
+    if (TX == 8) {
+      cudaFuncSetAttribute(k_div_fft_y<8, TS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      k_div_fft_y<8, TS><<<grid, 256, smem, L.stream>>>(g, L.t, b.sc, ns, b.vx_o, b.vy_o, b.vz_o, spec,
+                                                        L.plan_y, twy);
+    } else if (TX == 4) {
+      cudaFuncSetAttribute(k_div_fft_y<4, TS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      k_div_fft_y<4, TS><<<grid, 256, smem, L.stream>>>(g, L.t, b.sc, ns, b.vx_o, b.vy_o, b.vz_o, spec,
+                                                        L.plan_y, twy);
+    } else {
+      cudaFuncSetAttribute(k_div_fft_y<2, TS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      k_div_fft_y<2, TS><<<grid, 256, smem, L.stream>>>(g, L.t, b.sc, ns, b.vx_o, b.vy_o, b.vz_o, spec,
+                                                        L.plan_y, twy);
+    }
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  }
+  // K3 forward z FFT
+  if (g.nzm > 1) {
+    const int TXZ = L.tx_z;
+    const size_t smem = (size_t)2 * TXZ * g.nzm * sizeof(C);
+    dim3 grid((g.nxm + TXZ - 1) / TXZ, g.nyh);
+    if (TXZ == 8) {
+      cudaFuncSetAttribute(k_fft_z<8, false, TS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      k_fft_z<8, false, TS><<<grid, 256, smem, L.stream>>>(g, spec, L.plan_z, twz);
+    } else if (TXZ == 4) {
+      cudaFuncSetAttribute(k_fft_z<4, false, TS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      k_fft_z<4, false, TS><<<grid, 256, smem, L.stream>>>(g, spec, L.plan_z, twz);
+    } else {
+      cudaFuncSetAttribute(k_fft_z<2, false, TS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      k_fft_z<2, false, TS><<<grid, 256, smem, L.stream>>>(g, spec, L.plan_z, twz);
+    }
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  }
+  // K4 tridiagonal per mode
+  if ((e = launch_k4_T<TS>(L, b.spec, b.err)) != cudaSuccess) return e;
+  // K5 backward z FFT
+  if (g.nzm > 1) {
+    const int TXZ = L.tx_z;
+    const size_t smem = (size_t)2 * TXZ * g.nzm * sizeof(C);
+    dim3 grid((g.nxm + TXZ - 1) / TXZ, g.nyh);
+    if (TXZ == 8) {
+      cudaFuncSetAttribute(k_fft_z<8, true, TS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      k_fft_z<8, true, TS><<<grid, 256, smem, L.stream>>>(g, spec, L.plan_z, twz);
+    } else if (TXZ == 4) {
+      cudaFuncSetAttribute(k_fft_z<4, true, TS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      k_fft_z<4, true, TS><<<grid, 256, smem, L.stream>>>(g, spec, L.plan_z, twz);
+    } else {
+      cudaFuncSetAttribute(k_fft_z<2, true, TS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      k_fft_z<2, true, TS><<<grid, 256, smem, L.stream>>>(g, spec, L.plan_z, twz);
+    }
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  }
+  // K6 backward y FFT -> phi
+  {
+    const int TX = L.tx_y;
+    const size_t smem = (size_t)TX * g.nym * sizeof(C);
+    dim3 grid((g.nxm + TX - 1) / TX, g.nzm);
+    TS *phi = (TS *)b.phi;
+    if (TX == 8) {
+      cudaFuncSetAttribute(k_ifft_y<8, TS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      k_ifft_y<8, TS><<<grid, 256, smem, L.stream>>>(g, spec, phi, L.plan_y, twy);
+    } else if (TX == 4) {
+      cudaFuncSetAttribute(k_ifft_y<4, TS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      k_ifft_y<4, TS><<<grid, 256, smem, L.stream>>>(g, spec, phi, L.plan_y, twy);
+    } else {
+      cudaFuncSetAttribute(k_ifft_y<2, TS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      k_ifft_y<2, TS><<<grid, 256, smem, L.stream>>>(g, spec, phi, L.plan_y, twy);
+    }
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  }
+  // K7 projection + pressure update
+  {
+    const int bx = (g.nxm >= 256) ? 256 : ((g.nxm + 31) / 32) * 32;
+    const int by = 256 / bx;
+    dim3 block(bx, by);
+    dim3 grid((g.nxm + bx - 1) / bx, (g.nym + by - 1) / by, g.nzm);
+    k_correct<TS><<<grid, block, 0, L.stream>>>(g, L.t, b.sc, ns, b.vx_o, b.vy_o, b.vz_o, b.vx, b.vy,
+                                                b.vz, b.pr, (const TS *)b.phi);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
+cudaError_t launch_pressure(const LaunchCtx &L, const SubstepBuffers &b, int ns) {
+  return L.mixed ? launch_pressure_T<float>(L, b, ns) : launch_pressure_T<double>(L, b, ns);
+}
+
+static int reduce_blocks(const Geom &g) {
+  const long long ncol = (long long)g.nym * g.nzm;
+  long long nb = (ncol + 7) / 8;  // 8 warps per block, one column per warp per pass
+  if (nb > 148 * 8) nb = 148 * 8;
+  if (nb < 1) nb = 1;
+  return (int)nb;
+}
+
+cudaError_t launch_max_reduce(const LaunchCtx &L, bool div, const double *vx, const double *vy,
+                              const double *vz, unsigned long long *out) {
+  cudaMemsetAsync(out, 0, sizeof(unsigned long long), L.stream);
+  const int nb = reduce_blocks(L.g);
+  if (div)
+    k_max_reduce<true><<<nb, 256, 0, L.stream>>>(L.g, L.t, vx, vy, vz, out);
+  else
+    k_max_reduce<false><<<nb, 256, 0, L.stream>>>(L.g, L.t, vx, vy, vz, out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_globals(const LaunchCtx &L, const double *vx, const double *vy, const double *vz,
+                           const double *temp, double *partial, double *out3) {
+  const int nb = reduce_blocks(L.g);
+  k_globals_partial<<<nb, 256, 0, L.stream>>>(L.g, L.t, vx, vy, vz, temp, partial);
+  k_sum_partials<<<1, 256, 0, L.stream>>>(partial, nb, out3);
+  return cudaGetLastError();
+}
+
+int globals_partial_blocks(const Geom &g) { return reduce_blocks(g); }
+
+}  // namespace afid

@@ -1,0 +1,135 @@
+/*
+ * afid_gpu.h — C ABI of the B200 (sm_100a) implementation of AFiD's RK3 flow + temperature
+ * substep.  Plain C types and pointers only; every entry point returns an int status.
+ *
+ * The reference (chowland/AFiD-MuRPhFi, Fortran 90) runs the path as argument-less
+ * subroutines over module state: TimeMarcher (src/flow_solver/TimeMarcher.F90:13) called from
+ * the main loop (src/main.F90:306), CalcMaxCFL (src/main.F90:285,350) and CheckDivergence
+ * (src/main.F90:249,351).  This ABI replaces those calls: the caller owns the host arrays and
+ * builds the metric tables exactly as the reference does (CreateGrid.F90, InitPressureSolver
+ * in pressure.F90:61-114); the library owns device buffers and keeps the state resident on
+ * the GPU between calls.  The precedent for binding C from the reference is its FFTW
+ * interface block (src/flow_solver/param.F90:184-226); INTEGRATION.md shows the
+ * ISO_C_BINDING interface a maintainer adds.
+ *
+ * Array conventions: all 1-D tables are 0-based copies of the reference's 1-based arrays
+ * (table[k-1] == fortran(k)).  3-D host arrays are Fortran column-major (x fastest, then y,
+ * then z) and are passed as a pointer to element (1,1,1) plus the leading dimensions ld_x
+ * (>= nx) and ld_y (>= nym), so arrays with the reference's 2-cell y/z halos
+ * (InitVariables.F90:68-73) are passed as &vx(1,1,1) with ld_x = nx, ld_y = nym + 4.
+ *
+ * Threading: one host thread per context; contexts are independent and may be used from
+ * different threads.  No call aborts or throws; errors come back as status codes.
+ */
+#ifndef AFID_GPU_H
+#define AFID_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes: the reference's errorcode values where one matches ----------------- */
+#define AFID_OK 0
+#define AFID_E_ALLOC 8           /* allocation failure (AuxiliaryRoutines.F90:88-91)          */
+#define AFID_E_CFL 165           /* CFL*dt > CFLMAX with fixed dt (main.F90:297-298)          */
+#define AFID_E_DTMIN 166         /* dt < dtmin with variable dt (main.F90:302)                */
+#define AFID_E_DIVERGENCE 169    /* max|div u| > resid (main.F90:357)                         */
+#define AFID_E_FFTSIZE 444       /* nym/nzm with a prime factor > 5 (main.F90:272-279)        */
+#define AFID_E_SINGULAR 601      /* zero pivot in a Poisson mode (pressure.F90:225-229)       */
+#define AFID_E_TIMEOUT 602       /* a bounded device-side wait ran out                        */
+#define AFID_E_INVALID 603       /* bad argument / unsupported configuration                  */
+#define AFID_E_CUDA 604          /* CUDA runtime error (afid_gpu_cuda_error gives the code)   */
+#define AFID_E_CAPACITY 605      /* batch / server slot or HBM budget exhausted               */
+
+/* precision of the explicit terms and transforms (the implicit solves are always FP64) */
+#define AFID_PREC_FP64 0
+#define AFID_PREC_MIXED 1        /* FP32 explicit terms, FFTs and pressure transforms        */
+
+typedef struct afid_ctx afid_ctx_t;
+
+/* Grid sizes and metric tables.  Lengths: nx = nxm + 1. */
+typedef struct afid_grid {
+  int nxm, nym, nzm;             /* cells in x (wall-normal), y, z (periodic)  param.F90:67  */
+  double alx3, ylen, zlen;       /* domain size                                 bou.in       */
+  const double *xc;              /* [nx]  cell faces       CreateGrid.F90:76, grid.F90:29-53 */
+  const double *xm;              /* [nx]  cell centres     CreateGrid.F90:114-117            */
+  const double *g3rc;            /* [nx]  face metric      CreateGrid.F90:118-125            */
+  const double *udx3c;           /* [nx]  dx/g3rc          CreateGrid.F90:134-138            */
+  const double *udx3m;           /* [nxm] dx/d3xc          CreateGrid.F90:134-137            */
+  const double *ap3ck, *ac3ck, *am3ck;    /* [nx]  d2/dx2 at faces    CreateGrid.F90:165     */
+  const double *ap3sk, *ac3sk, *am3sk;    /* [nxm] d2/dx2, velocity   CreateGrid.F90:171     */
+  const double *ap3ssk, *ac3ssk, *am3ssk; /* [nxm] d2/dx2, temperature CreateGrid.F90:177    */
+  const double *amphk, *acphk, *apphk;    /* [nxm] Poisson x-coeffs   pressure.F90:103-114   */
+  const double *ak1;             /* [nzm] modified wavenumbers in z            pressure.F90:78-86 */
+  const double *ak2;             /* [nym] modified wavenumbers in y            pressure.F90:89-97 */
+} afid_grid_t;
+
+/* Physics and options (ReadInputFile.F90:109-123, bou.in). */
+typedef struct afid_params {
+  double ren;                    /* sqrt(|Ra|/Pr)                                             */
+  double pect;                   /* ren * Pr                                                  */
+  double byct;                   /* buoyancy prefactor (1 unless salinity sets free-fall)     */
+  int active_t;                  /* 1 = temperature is buoyant                                */
+  int gaxis;                     /* gravity axis 1 (x), 2 (y), 3 (z)                          */
+  int inslws, inslwn;            /* no-slip (1) / free-slip (0) lower and upper walls          */
+  int tfixs, tfixn;              /* fixed-T (1) / zero-flux (0) lower and upper plates         */
+  double xplusu, xminusu;        /* wall velocities (ImplicitAndUpdateVY.F90:54-61)           */
+  double dpdy, dpdz;             /* mean pressure gradients; dpdz must be 0 on this path      */
+  int nsst;                      /* 3 = RK3 (Rai-Moin), 1 = AB2 (InitTimeMarchScheme.F90)     */
+  int precision;                 /* AFID_PREC_FP64 or AFID_PREC_MIXED                         */
+  const double *tempbp;          /* [nym*nzm] plate temperature at x = 0 (SetTempBCs.F90), y fastest */
+  const double *temptp;          /* [nym*nzm] plate temperature at x = alx3                   */
+} afid_params_t;
+
+/* ---- context lifetime ------------------------------------------------------------------ */
+/* Replaces InitVariables + InitPressureSolver device-side: allocates the resident state,
+ * uploads the tables, plans the FFTs.  State starts at zero. */
+int afid_gpu_create(const afid_grid_t *grid, const afid_params_t *params, afid_ctx_t **out);
+int afid_gpu_destroy(afid_ctx_t *ctx);
+/* Use a caller stream (cudaStream_t passed as void*); NULL restores the context's own. */
+int afid_gpu_set_stream(afid_ctx_t *ctx, void *stream);
+void *afid_gpu_get_stream(afid_ctx_t *ctx);
+int afid_gpu_synchronize(afid_ctx_t *ctx);
+
+/* ---- state transfer -------------------------------------------------------------------- */
+/* Copy vx, vy, vz, temp, pr from host (Fortran layout, see top) to the device and zero the
+ * RK3 history rux/ruy/ruz/rutemp, as a restart does (ReadFlowInterp.F90:143-171; the
+ * history is not saved because rom(1) = 0).  Any pointer may be NULL to leave that field. */
+int afid_gpu_upload(afid_ctx_t *ctx, const double *vx, const double *vy, const double *vz,
+                    const double *temp, const double *pr, int ld_x, int ld_y);
+/* Copy the resident fields back (what WriteFlowField / CalcMeanProfiles need on the host). */
+int afid_gpu_download(afid_ctx_t *ctx, double *vx, double *vy, double *vz, double *temp,
+                      double *pr, int ld_x, int ld_y);
+
+/* ---- the hot path ---------------------------------------------------------------------- */
+/* One full time step: nsst substeps with the reference's gam/rom/alm and beta = dt/ren/2.
+ * Replaces `call TimeMarcher` (main.F90:306, TimeMarcher.F90:28-133).  ntime is accepted for
+ * call-sequence compatibility (the reference only uses it for the IBM aldto). */
+int afid_gpu_timemarcher(afid_ctx_t *ctx, double dt, int ntime);
+/* One substep with explicit coefficients (TimeMarcher.F90:38-133 body). */
+int afid_gpu_substep(afid_ctx_t *ctx, int ns, double al, double ga, double ro, double dt,
+                     double beta);
+/* max over cells of |u|/dx summed over directions, at least 1e-8 (CalcMaxCFL.F90:22-46). */
+int afid_gpu_cfl(afid_ctx_t *ctx, double *cflm);
+/* max over cells of |div u| (CheckDivergence.F90:22-45). */
+int afid_gpu_divmax(afid_ctx_t *ctx, double *dmax);
+/* Volume Nusselt number, volume-mean kinetic energy and mean temperature, g3rc-weighted as
+ * GlobalQuantities.F90:27-80 (nu_vol = 1 + sqrt(Pr|Ra|) <vx T>).  ra_pr = Pr*|Ra|. */
+int afid_gpu_globals(afid_ctx_t *ctx, double ra_pr, double *nu_vol, double *ke, double *tmean);
+
+/* ---- diagnostics ------------------------------------------------------------------------ */
+const char *afid_gpu_status_string(int status);
+int afid_gpu_cuda_error(afid_ctx_t *ctx);   /* last cudaError_t seen by this context */
+/* Device pointer and x-stride (elements) of a resident field, for zero-copy interop.
+ * which: 0 vx, 1 vy, 2 vz, 3 temp, 4 pr. */
+int afid_gpu_field_device_ptr(afid_ctx_t *ctx, int which, void **dptr, int *ldx);
+/* Kernels launched by this context since creation (all are this library's own kernels). */
+long long afid_gpu_launch_count(afid_ctx_t *ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* AFID_GPU_H */

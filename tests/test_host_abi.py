@@ -1,0 +1,113 @@
+"""CPU-only checks of the C ABI library: it loads, exports every symbol that include/*.h
+declares, and its host-side set-up (bou.in reader, CreateGrid port, Philox IC, dt rule) agrees
+with the oracle.  No CUDA call is made here."""
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+
+import afid_gpu as ag
+from helpers import Case, bou_text
+from oracle import afid_oracle as o
+from oracle.philox import uniform_from_counter
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _declared_functions():
+    names = set()
+    for h in ("afid_gpu.h", "afid_host.h"):
+        text = open(os.path.join(ROOT, "include", h)).read()
+        text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+        names |= set(re.findall(r"\b(afid_\w+)\s*\(", text))
+    return {n for n in names if not n.endswith("_t")}
+
+
+def test_library_exports_every_declared_symbol():
+    lib = ag.lib()
+    declared = _declared_functions()
+    assert declared, "no declarations parsed"
+    missing = [n for n in sorted(declared) if not hasattr(lib, n)]
+    assert not missing, missing
+    assert declared <= set(ag.EXPORTS)
+
+
+def test_status_strings():
+    for s in (0, 8, 165, 166, 169, 444, 601, 602, 603, 604, 605):
+        assert ag.lib().afid_gpu_status_string(s).decode() != "unknown status"
+
+
+@pytest.mark.parametrize("kw", [dict(istr3=4, str3=2.0), dict(istr3=0), dict(istr3=6, str3=4.0),
+                                dict(istr3=7, str3=3.0), dict(istr3=1, str3=1.5),
+                                dict(istr3=2), dict(istr3=3)])
+def test_tables_match_oracle_grid(kw):
+    case = Case(48, 24, 12, ylen=2.0, zlen=0.5, **kw)
+    g = case.g
+    for name in ("xc", "xm", "g3rc", "udx3c", "udx3m", "ap3ck", "ac3ck", "am3ck", "ap3sk", "ac3sk",
+                 "am3sk", "ap3ssk", "ac3ssk", "am3ssk", "amphk", "acphk", "apphk", "ak1", "ak2"):
+        a = case.tables.array(name)
+        ref = getattr(g, name)
+        n = min(a.size, ref.size)
+        np.testing.assert_allclose(a[:n], ref[:n], rtol=1e-13, atol=1e-13 * np.abs(ref).max(),
+                                   err_msg=name)
+    prm = case.tables.params
+    assert prm.ren == pytest.approx(g.ren, rel=1e-15)
+    assert prm.pect == pytest.approx(g.pect, rel=1e-15)
+
+
+def test_bou_in_parse_matches_oracle():
+    text = bou_text(64, 32, 16, rayt=1e9, prat=0.7, idtv=1, dt=1e-4, cflmax=1.2, dtmax=1e-2,
+                    xplusu=0.25, gaxis=1)
+    inp = ag.parse_bou_in(text)
+    p = o.parse_bou_in(text)
+    assert (inp.nxm, inp.nym, inp.nzm, inp.nsst) == (p.nxm, p.nym, p.nzm, p.nsst)
+    assert inp.rayt == p.rayt and inp.prat == p.prat and inp.dt == p.dt
+    assert inp.limit_cfl == p.limit_cfl and inp.dtmax == p.dtmax and inp.xplusu == p.xplusu
+
+
+def test_reference_example_bou_in_parses():
+    """A bou.in in the reference's own layout (examples/*/bou.in shape)."""
+    text = bou_text(128, 256, 1, ylen=2.0, zlen=0.01, dt=5e-4, dtmax=5e-4, cflmax=1.2, rayt=1e8,
+                    ntst=999)
+    inp = ag.parse_bou_in(text)
+    assert inp.ntst == 999 and inp.zlen == 0.01 and inp.nzm == 1
+
+
+def test_bad_bou_in_rejected():
+    with pytest.raises(ag.AfidError) as e:
+        ag.parse_bou_in("garbage\n")
+    assert e.value.status == ag.AFID_E_INVALID
+
+
+def test_philox_c_matches_numpy():
+    ns = np.array([0, 1, 2, 12345, 2**32 + 7, 2**40 + 3], dtype=np.uint64)
+    for seed in (0, 1234, 20261203, 2**33 + 5):
+        ref = uniform_from_counter(ns, seed)
+        got = np.array([ag.lib().afid_philox_uniform(seed, int(n)) for n in ns])
+        np.testing.assert_array_equal(got, ref)
+
+
+def test_initial_temperature_matches_oracle():
+    case = Case(32, 16, 8)
+    t = case.tables.initial_temperature(777)
+    s = o.initial_state(case.g, 777)
+    np.testing.assert_allclose(t[..., :32], s.temp[..., :32], rtol=0, atol=1e-15)
+
+
+@pytest.mark.parametrize("idtv,ntime,cflm", [(1, 0, 3.0), (1, 2, 3.0), (1, 2, 1e-9), (1, 3, 1e3),
+                                             (0, 0, 100.0), (0, 5, 2e4)])
+def test_next_dt_matches_oracle(idtv, ntime, cflm):
+    text = bou_text(16, 8, 4, idtv=idtv, dt=1e-3, cflmax=1.2, dtmax=5e-3)
+    inp = ag.parse_bou_in(text)
+    inp.dtmin = 1e-3 if cflm > 100 and idtv == 1 else inp.dtmin
+    p = o.parse_bou_in(text)
+    p.dtmin = inp.dtmin
+    dt = ctypes.c_double(1e-3)
+    rep = ctypes.c_double()
+    err = ag.lib().afid_next_dt(ctypes.byref(inp), ntime, ctypes.byref(dt), cflm, ctypes.byref(rep))
+    dto, erro, repo = o.next_dt(p, ntime, 1e-3, cflm)
+    assert err == erro
+    assert dt.value == dto
+    assert rep.value == repo
