@@ -86,7 +86,7 @@ EXPORTS = [
     "afid_gpu_synchronize", "afid_gpu_upload", "afid_gpu_download", "afid_gpu_timemarcher",
     "afid_gpu_substep", "afid_gpu_cfl", "afid_gpu_divmax", "afid_gpu_globals",
     "afid_gpu_status_string", "afid_gpu_cuda_error", "afid_gpu_field_device_ptr",
-    "afid_gpu_launch_count",
+    "afid_gpu_launch_count", "afid_gpu_profile_enable", "afid_gpu_profile_report",
     "afid_parse_bou_in", "afid_read_bou_in", "afid_tables_create", "afid_tables_destroy",
     "afid_tables_grid", "afid_tables_params", "afid_tables_array", "afid_philox_uniform",
     "afid_initial_temperature", "afid_next_dt", "afid_run",
@@ -117,6 +117,8 @@ def load_library(path: str = _LIB_PATH) -> C.CDLL:
         "afid_gpu_cuda_error": (i, [vp]),
         "afid_gpu_field_device_ptr": (i, [vp, i, C.POINTER(vp), C.POINTER(i)]),
         "afid_gpu_launch_count": (C.c_longlong, [vp]),
+        "afid_gpu_profile_enable": (i, [vp, i]),
+        "afid_gpu_profile_report": (i, [vp, _dp, C.POINTER(C.c_longlong), i]),
         "afid_parse_bou_in": (i, [C.c_char_p, C.POINTER(InputT)]),
         "afid_read_bou_in": (i, [C.c_char_p, C.POINTER(InputT)]),
         "afid_tables_create": (i, [C.POINTER(InputT), i, C.POINTER(vp)]),
@@ -282,6 +284,19 @@ class Solver:
 
     def launch_count(self) -> int:
         return int(lib().afid_gpu_launch_count(self._h))
+
+    PROFILE_CLASSES = ("cn_tables", "explicit_implicit", "div_fft_y", "fft_z_fwd", "tridiag_pressure",
+                       "fft_z_inv", "ifft_y", "correct", "reductions")
+
+    def profile(self, enable: bool = True) -> None:
+        _check(lib().afid_gpu_profile_enable(self._h, int(enable)), "afid_gpu_profile_enable")
+
+    def profile_report(self) -> dict:
+        n = len(self.PROFILE_CLASSES)
+        ms = (C.c_double * n)()
+        cnt = (C.c_longlong * n)()
+        _check(lib().afid_gpu_profile_report(self._h, ms, cnt, n), "afid_gpu_profile_report")
+        return {k: (ms[i], int(cnt[i])) for i, k in enumerate(self.PROFILE_CLASSES)}
 
     def device_ptr(self, which: int):
         p, ld = C.c_void_p(), C.c_int()

@@ -38,6 +38,12 @@ struct afid_ctx {
   // device tables for the CN builder
   const double *am[3], *ac[3], *ap[3];
   size_t field_elems = 0;
+  // optional per-kernel event timing
+  bool prof = false;
+  std::vector<cudaEvent_t> ev_pool;
+  size_t ev_used = 0;
+  struct Rec { int cls; size_t a, b; };
+  std::vector<Rec> recs;
 };
 
 namespace {
@@ -150,6 +156,30 @@ SubstepBuffers buffers(afid_ctx_t *ctx) {
   return b;
 }
 
+cudaEvent_t next_event(afid_ctx_t *ctx, size_t *idx) {
+  if (ctx->ev_used == ctx->ev_pool.size()) {
+    cudaEvent_t e;
+    if (cudaEventCreate(&e) != cudaSuccess) return nullptr;
+    ctx->ev_pool.push_back(e);
+  }
+  *idx = ctx->ev_used;
+  return ctx->ev_pool[ctx->ev_used++];
+}
+
+// Launch fn() and, when profiling, bracket it with events on the context stream.
+template <typename F>
+cudaError_t timed(afid_ctx_t *ctx, int cls, F fn) {
+  if (!ctx->prof) return fn();
+  size_t ia = 0, ib = 0;
+  cudaEvent_t a = next_event(ctx, &ia);
+  if (a) cudaEventRecord(a, ctx->stream);
+  cudaError_t e = fn();
+  cudaEvent_t b = next_event(ctx, &ib);
+  if (b) cudaEventRecord(b, ctx->stream);
+  if (a && b) ctx->recs.push_back({cls, ia, ib});
+  return e;
+}
+
 int build_cn(afid_ctx_t *ctx, int ns0, int nsub, const double *al, const double *ga, const double *ro,
              double dt, double beta) {
   const Geom &g = ctx->L.g;
@@ -173,21 +203,25 @@ int build_cn(afid_ctx_t *ctx, int ns0, int nsub, const double *al, const double 
   in.dt = dt;
   in.beta = beta;
   in.pect = g.pect;
+  in.ren = g.ren;
   in.ns0 = ns0;
   in.nsub = nsub;
   in.M = ctx->L.M;
   in.tab = ctx->cn_tab;
   in.sc = ctx->sc;
-  AFID_CUDA(ctx, launch_cn_tables(ctx->L, in));
+  AFID_CUDA(ctx, timed(ctx, 0, [&] { return launch_cn_tables(ctx->L, in); }));
   ctx->launches += 1;
   return AFID_OK;
 }
 
 int run_substep(afid_ctx_t *ctx, int ns) {
   SubstepBuffers b = buffers(ctx);
-  AFID_CUDA(ctx, launch_explicit_implicit(ctx->L, b, ns));
-  AFID_CUDA(ctx, launch_pressure(ctx->L, b, ns));
-  ctx->launches += (ctx->L.g.nzm > 1) ? 7 : 5;
+  for (int st = 0; st < kNumStages; ++st) {
+    const Stage stage = static_cast<Stage>(st);
+    if (ctx->L.g.nzm == 1 && (stage == Stage::FftZFwd || stage == Stage::FftZInv)) continue;
+    AFID_CUDA(ctx, timed(ctx, 1 + st, [&] { return launch_stage(ctx->L, b, ns, stage); }));
+    ctx->launches += 1;
+  }
   std::swap(ctx->temp, ctx->temp_o);  // temperature is final after K1; the state moves buffers
   return AFID_OK;
 }
@@ -261,6 +295,12 @@ int afid_gpu_create(const afid_grid_t *grid, const afid_params_t *prm, afid_ctx_
   g.ren = prm->ren;
   g.pect = prm->pect;
   g.byct = prm->byct;
+  g.rren = 1.0 / prm->ren;
+  g.rpect = 1.0 / prm->pect;
+  g.udyq_re = g.dyq / prm->ren;  // ExplicitTermsVX.F90:191-192
+  g.udzq_re = g.dzq / prm->ren;
+  g.udyq_pe = g.dyq / prm->pect;  // ExplicitTermsTemp.F90:24-25
+  g.udzq_pe = g.dzq / prm->pect;
   // ExplicitTermsVY.F90:30-34
   g.gy = (prm->inslwn == 0 || prm->inslws == 0) ? prm->dpdy * prm->dpdy / (prm->ren * prm->ren)
                                                  : 8.0 * (prm->dpdy * prm->dpdy) / (prm->ren * prm->ren);
@@ -422,6 +462,7 @@ int afid_gpu_destroy(afid_ctx_t *ctx) {
   cudaSetDevice(ctx->dev);
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   for (void *p : ctx->allocs) cudaFree(p);
+  for (cudaEvent_t e : ctx->ev_pool) cudaEventDestroy(e);
   if (ctx->host_scratch) cudaFreeHost(ctx->host_scratch);
   if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
   delete ctx;
@@ -501,7 +542,7 @@ int afid_gpu_substep(afid_ctx_t *ctx, int ns, double al, double ga, double ro, d
 int afid_gpu_cfl(afid_ctx_t *ctx, double *cflm) {
   if (!ctx || !cflm) return AFID_E_INVALID;
   cudaSetDevice(ctx->dev);
-  AFID_CUDA(ctx, launch_max_reduce(ctx->L, false, ctx->vx, ctx->vy, ctx->vz, ctx->red));
+  AFID_CUDA(ctx, timed(ctx, 8, [&] { return launch_max_reduce(ctx->L, false, ctx->vx, ctx->vy, ctx->vz, ctx->red); }));
   ctx->launches += 1;
   AFID_CUDA(ctx, cudaMemcpyAsync(ctx->host_scratch, ctx->red, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
   int s = check_err_flag(ctx);
@@ -513,7 +554,7 @@ int afid_gpu_cfl(afid_ctx_t *ctx, double *cflm) {
 int afid_gpu_divmax(afid_ctx_t *ctx, double *dmax) {
   if (!ctx || !dmax) return AFID_E_INVALID;
   cudaSetDevice(ctx->dev);
-  AFID_CUDA(ctx, launch_max_reduce(ctx->L, true, ctx->vx, ctx->vy, ctx->vz, ctx->red));
+  AFID_CUDA(ctx, timed(ctx, 8, [&] { return launch_max_reduce(ctx->L, true, ctx->vx, ctx->vy, ctx->vz, ctx->red); }));
   ctx->launches += 1;
   AFID_CUDA(ctx, cudaMemcpyAsync(ctx->host_scratch, ctx->red, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
   int s = check_err_flag(ctx);
@@ -525,7 +566,9 @@ int afid_gpu_globals(afid_ctx_t *ctx, double ra_pr, double *nu_vol, double *ke, 
   if (!ctx) return AFID_E_INVALID;
   cudaSetDevice(ctx->dev);
   const Geom &g = ctx->L.g;
-  AFID_CUDA(ctx, launch_globals(ctx->L, ctx->vx, ctx->vy, ctx->vz, ctx->temp, ctx->partial, ctx->gsum));
+  AFID_CUDA(ctx, timed(ctx, 8, [&] {
+    return launch_globals(ctx->L, ctx->vx, ctx->vy, ctx->vz, ctx->temp, ctx->partial, ctx->gsum);
+  }));
   ctx->launches += 2;
   AFID_CUDA(ctx, cudaMemcpyAsync(ctx->host_scratch, ctx->gsum, 3 * sizeof(double), cudaMemcpyDeviceToHost,
                                  ctx->stream));
@@ -557,5 +600,31 @@ int afid_gpu_field_device_ptr(afid_ctx_t *ctx, int which, void **dptr, int *ldx)
 }
 
 long long afid_gpu_launch_count(afid_ctx_t *ctx) { return ctx ? ctx->launches : 0; }
+
+int afid_gpu_profile_enable(afid_ctx_t *ctx, int enable) {
+  if (!ctx) return AFID_E_INVALID;
+  ctx->prof = enable != 0;
+  return AFID_OK;
+}
+
+int afid_gpu_profile_report(afid_ctx_t *ctx, double *ms, long long *count, int n) {
+  if (!ctx) return AFID_E_INVALID;
+  cudaSetDevice(ctx->dev);
+  AFID_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  for (int c = 0; c < n; ++c) {
+    if (ms) ms[c] = 0.0;
+    if (count) count[c] = 0;
+  }
+  for (const auto &r : ctx->recs) {
+    if (r.cls >= n) continue;
+    float t = 0.f;
+    AFID_CUDA(ctx, cudaEventElapsedTime(&t, ctx->ev_pool[r.a], ctx->ev_pool[r.b]));
+    if (ms) ms[r.cls] += t;
+    if (count) count[r.cls] += 1;
+  }
+  ctx->recs.clear();
+  ctx->ev_used = 0;
+  return AFID_OK;
+}
 
 }  // extern "C"

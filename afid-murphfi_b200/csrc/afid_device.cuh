@@ -23,6 +23,8 @@ struct Geom {
   int ldxc;   // x stride of the complex spectrum (elements)
   double dx, dy, dz, dyq, dzq;
   double ren, pect, byct, gy;
+  double rren, rpect;                 // 1/ren, 1/pect
+  double udyq_re, udzq_re, udyq_pe, udzq_pe;  // dyq/ren, dzq/ren, dyq/pect, dzq/pect
   double xplusu, xminusu;
   int active_t, gaxis, inslws, inslwn, tfixs, tfixn;
 };
@@ -31,6 +33,7 @@ struct Geom {
 // kernel of the substep, so a captured step graph does not depend on dt).
 struct StepCoef {
   double al, ga, ro, dt, beta;
+  double alre, alpec;  // al/ren (ImplicitAndUpdateVX.F90:111), al/pect (ImplicitAndUpdateTemp.F90:197)
 };
 
 // 1-D metric tables on the device (0-based copies of the reference's arrays).
@@ -196,6 +199,44 @@ __device__ typename Cplx<T>::type *fft_block(typename Cplx<T>::type *buf0,
 // Bounded device-side waits: every spin in this library counts iterations and gives up with
 // an error flag instead of hanging (no trap, no unbounded loop).
 // ------------------------------------------------------------------------------------------
-constexpr long long kSpinLimit = 1LL << 26;
+constexpr long long kSpinLimit = 1LL << 22;
+
+// 1-D TMA bulk copies global -> shared, completed on an mbarrier (sm_90+ PTX, no tensor map,
+// no multicast).  Source and destination must be 16-byte aligned, size a multiple of 16.
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void fence_mbar_init() {
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+          smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
+// Wait for the given phase parity; gives up after `limit` polls and returns false.
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, long long limit) {
+  const uint32_t addr = smem_u32(bar);
+  for (long long it = 0; it < limit; ++it) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(done)
+        : "r"(addr), "r"(parity)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
 
 }  // namespace afid

@@ -36,7 +36,7 @@ struct CnInputs {
   const double *am[3], *ac[3], *ap[3];
   int off[3], n[3];
   double al[3], ga[3], ro[3];
-  double dt, beta, pect;
+  double dt, beta, pect, ren;
   int ns0, nsub, M;
   double *tab;
   StepCoef *sc;
@@ -46,7 +46,10 @@ int cn_choose_M(int nxm);
 size_t cn_tab_doubles(int M, int nsst);
 cudaError_t launch_cn_tables(const LaunchCtx &L, const CnInputs &in);
 cudaError_t launch_explicit_implicit(const LaunchCtx &L, const SubstepBuffers &b, int ns);
-cudaError_t launch_pressure(const LaunchCtx &L, const SubstepBuffers &b, int ns);
+// The kernels of one substep, in launch order (K1 .. K7).
+enum class Stage { ExplicitImplicit = 0, DivFftY, FftZFwd, Tridiag, FftZInv, IfftY, Correct };
+constexpr int kNumStages = 7;
+cudaError_t launch_stage(const LaunchCtx &L, const SubstepBuffers &b, int ns, Stage st);
 cudaError_t launch_max_reduce(const LaunchCtx &L, bool div, const double *vx, const double *vy,
                               const double *vz, unsigned long long *out);
 cudaError_t launch_globals(const LaunchCtx &L, const double *vx, const double *vy,

@@ -48,7 +48,7 @@ struct CnMatrixDesc {
 struct CnBuildArgs {
   CnMatrixDesc mat[3];
   double al[3], ga[3], ro[3];
-  double dt, beta, pect;
+  double dt, beta, pect, ren;
   int ns0, nsub;       // substeps ns0 .. ns0+nsub-1 are built
 };
 
@@ -66,6 +66,8 @@ __global__ void k_cn_tables(CnBuildArgs args, int M, double *__restrict__ tab,
     c.ro = args.ro[sub];
     c.dt = args.dt;
     c.beta = args.beta;
+    c.alre = al / args.ren;
+    c.alpec = al / args.pect;
     sc[ns] = c;
   }
   const CnMatrixDesc d = args.mat[m];
@@ -145,14 +147,14 @@ __global__ void k_cn_tables(CnBuildArgs args, int M, double *__restrict__ tab,
 
 // Solve one column whose scaled RHS sits in s[q*32 + lane] (chunk layout); the solution
 // overwrites it.  Constant-matrix version using the tables above.
-template <int M>
+template <int M, int LD = 32>
 __device__ __forceinline__ void cn_solve_chunk(double *__restrict__ s, const double *__restrict__ T,
                                                int lane) {
   const double *Ta = T + 32 * M, *Tinv = T + 64 * M, *Tcp = T + 96 * M, *Tv = T + 128 * M,
                *Tw = T + 160 * M, *Tl = T + 192 * M;
   double y[M];
 #pragma unroll
-  for (int q = 0; q < M; ++q) y[q] = s[q * 32 + lane];
+  for (int q = 0; q < M; ++q) y[q] = s[q * LD + lane];
   if constexpr (M > 1) {
     y[1] = y[1] * __ldg(Tinv + 32 + lane);
 #pragma unroll
@@ -184,271 +186,309 @@ __device__ __forceinline__ void cn_solve_chunk(double *__restrict__ s, const dou
   s[lane] = delta;
 #pragma unroll
   for (int q = 1; q < M; ++q)
-    s[q * 32 + lane] = y[q] + __ldg(Tv + q * 32 + lane) * delta + __ldg(Tw + q * 32 + lane) * xnext;
+    s[q * LD + lane] = y[q] + __ldg(Tv + q * 32 + lane) * delta + __ldg(Tw + q * 32 + lane) * xnext;
 }
 
 // ------------------------------------------------------------------------------------------
 // Explicit terms + RHS, one (k, j, i) point each.  Expressions follow the reference loop
-// bodies term by term; TE is the arithmetic type of the explicit terms.
+// bodies term by term; TE is the arithmetic type of the explicit terms.  The operands are
+// x-columns staged in shared memory: c = (j,i), jp/jm = (j+-1,i), ip/im = (j,i+-1),
+// d = the diagonal neighbour (j+1,i-1) for vy and (j-1,i+1) for vz.
 // ------------------------------------------------------------------------------------------
-struct Cols {
-  size_t c, jp, jm, ip, im, jmip, jpim;
-  int j, i;
+struct ColV {
+  const double *c, *jp, *jm, *ip, *im, *d;
 };
 
-template <typename TE> __device__ __forceinline__ TE ldc(const double *p) { return (TE)__ldg(p); }
+template <typename TE> __device__ __forceinline__ TE cv(double v) { return (TE)v; }
 
 // ExplicitTermsVX.F90:194-291 + ImplicitAndUpdateVX.F90:124-150, k = 1..nxm-1 (0-based)
-template <typename TE, typename TR>
-__device__ __forceinline__ double rhs_vx(const Geom &g, const Tables &t, const StepCoef &sc,
-                                         const Cols &o, int k, const double *__restrict__ vx,
-                                         const double *__restrict__ vy,
-                                         const double *__restrict__ vz,
-                                         const double *__restrict__ temp,
-                                         const double *__restrict__ pr, TR *__restrict__ rux) {
+template <typename TE>
+__device__ __forceinline__ double rhs_vx(const Geom &g, const Tables &t, const StepCoef &sc, int k,
+                                         const ColV &X, const ColV &Y, const ColV &Z, const ColV &T,
+                                         const ColV &P, double ru, TE &qout) {
   const int km = k - 1, kp = k + 1;
   const TE udy = (TE)(g.dy * 0.25), udz = (TE)(g.dz * 0.25);
-  const TE udyq = (TE)(g.dyq / g.ren), udzq = (TE)(g.dzq / g.ren);
-  const TE idxm = ldc<TE>(t.idx + km), idxc = ldc<TE>(t.idx + k);
-  const TE udx3c = ldc<TE>(t.udx3c + k);
-  const TE vxc = ldc<TE>(vx + o.c + k);
-  const TE vxkp = ldc<TE>(vx + o.c + kp), vxkm = ldc<TE>(vx + o.c + km);
-  const TE vxip = ldc<TE>(vx + o.ip + k), vxim = ldc<TE>(vx + o.im + k);
-  const TE vxjp = ldc<TE>(vx + o.jp + k), vxjm = ldc<TE>(vx + o.jm + k);
+  const TE udyq = (TE)g.udyq_re, udzq = (TE)g.udzq_re;
+  const TE idxm = cv<TE>(__ldg(t.idx + km)), idxc = cv<TE>(__ldg(t.idx + k));
+  const TE udx3c = cv<TE>(__ldg(t.udx3c + k));
+  const TE vxc = cv<TE>(X.c[k]);
+  const TE vxkp = cv<TE>(X.c[kp]), vxkm = cv<TE>(X.c[km]);
+  const TE vxip = cv<TE>(X.ip[k]), vxim = cv<TE>(X.im[k]);
+  const TE vxjp = cv<TE>(X.jp[k]), vxjm = cv<TE>(X.jm[k]);
   const TE hxz = udx3c * udz *
-                 ((idxm * ldc<TE>(vz + o.ip + km) + idxc * ldc<TE>(vz + o.ip + k)) * (vxip + vxc) -
-                  (idxm * ldc<TE>(vz + o.c + km) + idxc * ldc<TE>(vz + o.c + k)) * (vxc + vxim));
+                 ((idxm * cv<TE>(Z.ip[km]) + idxc * cv<TE>(Z.ip[k])) * (vxip + vxc) -
+                  (idxm * cv<TE>(Z.c[km]) + idxc * cv<TE>(Z.c[k])) * (vxc + vxim));
   const TE hxy = udx3c * udy *
-                 ((idxm * ldc<TE>(vy + o.jp + km) + idxc * ldc<TE>(vy + o.jp + k)) * (vxjp + vxc) -
-                  (idxm * ldc<TE>(vy + o.c + km) + idxc * ldc<TE>(vy + o.c + k)) * (vxc + vxjm));
+                 ((idxm * cv<TE>(Y.jp[km]) + idxc * cv<TE>(Y.jp[k])) * (vxjp + vxc) -
+                  (idxm * cv<TE>(Y.c[km]) + idxc * cv<TE>(Y.c[k])) * (vxc + vxjm));
   const TE hxx = ((vxkp + vxc) * (vxkp + vxc) - (vxc + vxkm) * (vxc + vxkm)) * udx3c * (TE)0.25;
   const TE dzzvx = (vxim - (TE)2.0 * vxc + vxip) * udzq;
   const TE dyyvx = (vxjm - (TE)2.0 * vxc + vxjp) * udyq;
   TE qcap = -(hxx + hxy + hxz) + dyyvx + dzzvx;
   if (g.gaxis == 1) {
-    const TE tempit = (TE)g.active_t * (TE)0.5 * (ldc<TE>(temp + o.c + k) + ldc<TE>(temp + o.c + km));
+    const TE tempit = (TE)g.active_t * (TE)0.5 * (cv<TE>(T.c[k]) + cv<TE>(T.c[km]));
     qcap = qcap + (TE)g.byct * tempit;
   }
-  const double alre = sc.al / g.ren;
+  const double alre = sc.alre;
   const double udx3 = sc.al * __ldg(t.udx3c + k);
-  const double dxxvx = __ldg(vx + o.c + kp) * __ldg(t.ap3ck + k) + __ldg(vx + o.c + k) * __ldg(t.ac3ck + k) +
-                       __ldg(vx + o.c + km) * __ldg(t.am3ck + k);
-  const double dxp = (__ldg(pr + o.c + k) - __ldg(pr + o.c + km)) * udx3;
-  const double rhs = (sc.ga * (double)qcap + sc.ro * (double)rux[o.c + k] + alre * dxxvx - dxp) * sc.dt;
-  rux[o.c + k] = (TR)qcap;
-  return rhs;
+  const double dxxvx = X.c[kp] * __ldg(t.ap3ck + k) + X.c[k] * __ldg(t.ac3ck + k) + X.c[km] * __ldg(t.am3ck + k);
+  const double dxp = (P.c[k] - P.c[km]) * udx3;
+  qout = qcap;
+  return (sc.ga * (double)qcap + sc.ro * ru + alre * dxxvx - dxp) * sc.dt;
 }
 
 // ExplicitTermsVY.F90:23-122 + ImplicitAndUpdateVY.F90:28-80, k = 0..nxm-1
-template <typename TE, typename TR>
-__device__ __forceinline__ double rhs_vy(const Geom &g, const Tables &t, const StepCoef &sc,
-                                         const Cols &o, int k, const double *__restrict__ vx,
-                                         const double *__restrict__ vy,
-                                         const double *__restrict__ vz,
-                                         const double *__restrict__ temp,
-                                         const double *__restrict__ pr, TR *__restrict__ ruy) {
+template <typename TE>
+__device__ __forceinline__ double rhs_vy(const Geom &g, const Tables &t, const StepCoef &sc, int k,
+                                         const ColV &X, const ColV &Y, const ColV &Z, const ColV &T,
+                                         const ColV &P, double ru, TE &qout) {
   const int kmm = (k == 0) ? 0 : k - 1;
   const int kpp = (k == g.nxm - 1) ? k : k + 1;
   const int kp = k + 1;
   const TE udy = (TE)(g.dy * 0.25), udz = (TE)(g.dz * 0.25);
-  const TE udyq = (TE)(g.dyq / g.ren), udzq = (TE)(g.dzq / g.ren);
-  const TE c = ldc<TE>(vy + o.c + k);
-  const TE vyjp = ldc<TE>(vy + o.jp + k), vyjm = ldc<TE>(vy + o.jm + k);
-  const TE vyip = ldc<TE>(vy + o.ip + k), vyim = ldc<TE>(vy + o.im + k);
-  const TE hyx = ((ldc<TE>(vx + o.c + kp) + ldc<TE>(vx + o.jm + kp)) * (ldc<TE>(vy + o.c + kpp) + c) -
-                  (ldc<TE>(vx + o.c + k) + ldc<TE>(vx + o.jm + k)) * (c + ldc<TE>(vy + o.c + kmm))) *
-                 ldc<TE>(t.udx3m + k) * (TE)0.25;
+  const TE udyq = (TE)g.udyq_re, udzq = (TE)g.udzq_re;
+  const TE c = cv<TE>(Y.c[k]);
+  const TE vyjp = cv<TE>(Y.jp[k]), vyjm = cv<TE>(Y.jm[k]);
+  const TE vyip = cv<TE>(Y.ip[k]), vyim = cv<TE>(Y.im[k]);
+  const TE hyx = ((cv<TE>(X.c[kp]) + cv<TE>(X.jm[kp])) * (cv<TE>(Y.c[kpp]) + c) -
+                  (cv<TE>(X.c[k]) + cv<TE>(X.jm[k])) * (c + cv<TE>(Y.c[kmm]))) *
+                 cv<TE>(__ldg(t.udx3m + k)) * (TE)0.25;
   const TE hyy = ((vyjp + c) * (vyjp + c) - (vyjm + c) * (vyjm + c)) * udy;
-  const TE hyz = ((vyip + c) * (ldc<TE>(vz + o.ip + k) + ldc<TE>(vz + o.jmip + k)) -
-                  (c + vyim) * (ldc<TE>(vz + o.c + k) + ldc<TE>(vz + o.jm + k))) *
+  const TE hyz = ((vyip + c) * (cv<TE>(Z.ip[k]) + cv<TE>(Z.d[k])) - (c + vyim) * (cv<TE>(Z.c[k]) + cv<TE>(Z.jm[k]))) *
                  udz;
   const TE dyyvy = (vyjp - (TE)2.0 * c + vyjm) * udyq;
   const TE dzzvy = (vyip - (TE)2.0 * c + vyim) * udzq;
   TE dph = -(hyx + hyy + hyz) + dyyvy + dzzvy + (TE)g.gy;
   if (g.gaxis == 2) {
-    const TE tempit = (TE)g.active_t * (TE)0.5 * (ldc<TE>(temp + o.c + k) + ldc<TE>(temp + o.jm + k));
+    const TE tempit = (TE)g.active_t * (TE)0.5 * (cv<TE>(T.c[k]) + cv<TE>(T.jm[k]));
     dph = dph + (TE)g.byct * tempit;
   }
-  const double alre = sc.al / g.ren;
+  const double alre = sc.alre;
   const double udyp = g.dy * sc.al;
   const double amm = __ldg(t.am3sk + k), acc = __ldg(t.ac3sk + k), app = __ldg(t.ap3sk + k);
-  const double cd = __ldg(vy + o.c + k);
+  const double cd = Y.c[k];
   double dxxvy;
   if (k == 0)
-    dxxvy = __ldg(vy + o.c + kpp) * app + cd * acc - (acc + app) * g.xminusu * g.inslws;
+    dxxvy = Y.c[kpp] * app + cd * acc - (acc + app) * g.xminusu * g.inslws;
   else if (k == g.nxm - 1)
-    dxxvy = -(acc + amm) * g.xplusu * g.inslwn + cd * acc + __ldg(vy + o.c + kmm) * amm;
+    dxxvy = -(acc + amm) * g.xplusu * g.inslwn + cd * acc + Y.c[kmm] * amm;
   else
-    dxxvy = __ldg(vy + o.c + kpp) * app + cd * acc + __ldg(vy + o.c + kmm) * amm;
-  const double dyp = (__ldg(pr + o.c + k) - __ldg(pr + o.jm + k)) * udyp;
-  const double rhs = (sc.ga * (double)dph + sc.ro * (double)ruy[o.c + k] + alre * dxxvy - dyp) * sc.dt;
-  ruy[o.c + k] = (TR)dph;
-  return rhs;
+    dxxvy = Y.c[kpp] * app + cd * acc + Y.c[kmm] * amm;
+  const double dyp = (P.c[k] - P.jm[k]) * udyp;
+  qout = dph;
+  return (sc.ga * (double)dph + sc.ro * ru + alre * dxxvy - dyp) * sc.dt;
 }
 
 // ExplicitTermsVZ.F90:149-244 + ImplicitAndUpdateVZ.F90:121-161, k = 0..nxm-1
-template <typename TE, typename TR>
-__device__ __forceinline__ double rhs_vz(const Geom &g, const Tables &t, const StepCoef &sc,
-                                         const Cols &o, int k, const double *__restrict__ vx,
-                                         const double *__restrict__ vy,
-                                         const double *__restrict__ vz,
-                                         const double *__restrict__ temp,
-                                         const double *__restrict__ pr, TR *__restrict__ ruz) {
+template <typename TE>
+__device__ __forceinline__ double rhs_vz(const Geom &g, const Tables &t, const StepCoef &sc, int k,
+                                         const ColV &X, const ColV &Y, const ColV &Z, const ColV &T,
+                                         const ColV &P, double ru, TE &qout) {
   const int kmm = (k == 0) ? 0 : k - 1;
   const int kpp = (k == g.nxm - 1) ? k : k + 1;
   const int kp = k + 1;
   const TE udy = (TE)(g.dy * 0.25), udz = (TE)(g.dz * 0.25);
-  const TE udyq = (TE)(g.dyq / g.ren), udzq = (TE)(g.dzq / g.ren);
-  const TE c = ldc<TE>(vz + o.c + k);
-  const TE vzip = ldc<TE>(vz + o.ip + k), vzim = ldc<TE>(vz + o.im + k);
-  const TE vzjp = ldc<TE>(vz + o.jp + k), vzjm = ldc<TE>(vz + o.jm + k);
+  const TE udyq = (TE)g.udyq_re, udzq = (TE)g.udzq_re;
+  const TE c = cv<TE>(Z.c[k]);
+  const TE vzip = cv<TE>(Z.ip[k]), vzim = cv<TE>(Z.im[k]);
+  const TE vzjp = cv<TE>(Z.jp[k]), vzjm = cv<TE>(Z.jm[k]);
   const TE hzz = ((vzip + c) * (vzip + c) - (vzim + c) * (vzim + c)) * udz;
-  const TE hzy = ((ldc<TE>(vy + o.jp + k) + ldc<TE>(vy + o.jpim + k)) * (vzjp + c) -
-                  (ldc<TE>(vy + o.c + k) + ldc<TE>(vy + o.im + k)) * (c + vzjm)) *
+  const TE hzy = ((cv<TE>(Y.jp[k]) + cv<TE>(Y.d[k])) * (vzjp + c) - (cv<TE>(Y.c[k]) + cv<TE>(Y.im[k])) * (c + vzjm)) *
                  udy;
-  const TE hzx = ((ldc<TE>(vx + o.c + kp) + ldc<TE>(vx + o.im + kp)) * (ldc<TE>(vz + o.c + kpp) + c) -
-                  (ldc<TE>(vx + o.c + k) + ldc<TE>(vx + o.im + k)) * (c + ldc<TE>(vz + o.c + kmm))) *
-                 ldc<TE>(t.udx3m + k) * (TE)0.25;
+  const TE hzx = ((cv<TE>(X.c[kp]) + cv<TE>(X.im[kp])) * (cv<TE>(Z.c[kpp]) + c) -
+                  (cv<TE>(X.c[k]) + cv<TE>(X.im[k])) * (c + cv<TE>(Z.c[kmm]))) *
+                 cv<TE>(__ldg(t.udx3m + k)) * (TE)0.25;
   const TE dzzvz = (vzip - (TE)2.0 * c + vzim) * udzq;
   const TE dyyvz = (vzjp - (TE)2.0 * c + vzjm) * udyq;
   TE dq = -(hzx + hzy + hzz) + dyyvz + dzzvz;
   if (g.gaxis == 3) {
-    const TE tempit = (TE)g.active_t * (TE)0.5 * (ldc<TE>(temp + o.c + k) + ldc<TE>(temp + o.im + k));
+    const TE tempit = (TE)g.active_t * (TE)0.5 * (cv<TE>(T.c[k]) + cv<TE>(T.im[k]));
     dq = dq + (TE)g.byct * tempit;
   }
-  const double alre = sc.al / g.ren;
+  const double alre = sc.alre;
   const double amm = __ldg(t.am3sk + k), acc = __ldg(t.ac3sk + k), app = __ldg(t.ap3sk + k);
-  const double dxxvz = __ldg(vz + o.c + kpp) * app + __ldg(vz + o.c + k) * acc + __ldg(vz + o.c + kmm) * amm;
-  const double dzp = (__ldg(pr + o.c + k) - __ldg(pr + o.im + k)) * g.dz * sc.al;
-  const double rhs = (sc.ga * (double)dq + sc.ro * (double)ruz[o.c + k] + alre * dxxvz - dzp) * sc.dt;
-  ruz[o.c + k] = (TR)dq;
-  return rhs;
+  const double dxxvz = Z.c[kpp] * app + Z.c[k] * acc + Z.c[kmm] * amm;
+  const double dzp = (P.c[k] - P.im[k]) * g.dz * sc.al;
+  qout = dq;
+  return (sc.ga * (double)dq + sc.ro * ru + alre * dxxvz - dzp) * sc.dt;
 }
 
 // ExplicitTermsTemp.F90:22-77 + ImplicitAndUpdateTemp.F90:197-237, k = 0..nxm-1
-template <typename TE, typename TR>
-__device__ __forceinline__ double rhs_temp(const Geom &g, const Tables &t, const StepCoef &sc,
-                                           const Cols &o, int k, const double *__restrict__ vx,
-                                           const double *__restrict__ vy,
-                                           const double *__restrict__ vz,
-                                           const double *__restrict__ temp,
-                                           TR *__restrict__ rut) {
+template <typename TE>
+__device__ __forceinline__ double rhs_temp(const Geom &g, const Tables &t, const StepCoef &sc, int k,
+                                           const ColV &X, const ColV &Y, const ColV &Z, const ColV &T,
+                                           double tbp, double ttp, double ru, TE &qout) {
   const TE udz = (TE)(g.dz * 0.5), udy = (TE)(g.dy * 0.5);
-  const TE udzq = (TE)(g.dzq / g.pect), udyq = (TE)(g.dyq / g.pect);
-  const size_t pl = (size_t)o.j + (size_t)g.nym * o.i;
-  const double tbp = __ldg(t.tempbp + pl), ttp = __ldg(t.temptp + pl);
-  const TE tc = ldc<TE>(temp + o.c + k);
-  const TE ux = ldc<TE>(t.udx3m + k);
+  const TE udzq = (TE)g.udzq_pe, udyq = (TE)g.udyq_pe;
+  const TE tc = cv<TE>(T.c[k]);
+  const TE ux = cv<TE>(__ldg(t.udx3m + k));
   TE htx;
   if (k == 0)
-    htx = (ldc<TE>(vx + o.c + 1) * (ldc<TE>(temp + o.c + 1) + tc) - ldc<TE>(vx + o.c) * (TE)2.0 * (TE)tbp) *
-          (TE)0.5 * ux;
+    htx = (cv<TE>(X.c[1]) * (cv<TE>(T.c[1]) + tc) - cv<TE>(X.c[0]) * (TE)2.0 * (TE)tbp) * (TE)0.5 * ux;
   else if (k == g.nxm - 1)
-    htx = (ldc<TE>(vx + o.c + k + 1) * (TE)2.0 * (TE)ttp -
-           ldc<TE>(vx + o.c + k) * (tc + ldc<TE>(temp + o.c + k - 1))) *
-          (TE)0.5 * ux;
+    htx = (cv<TE>(X.c[k + 1]) * (TE)2.0 * (TE)ttp - cv<TE>(X.c[k]) * (tc + cv<TE>(T.c[k - 1]))) * (TE)0.5 * ux;
   else
-    htx = (ldc<TE>(vx + o.c + k + 1) * (ldc<TE>(temp + o.c + k + 1) + tc) -
-           ldc<TE>(vx + o.c + k) * (tc + ldc<TE>(temp + o.c + k - 1))) *
+    htx = (cv<TE>(X.c[k + 1]) * (cv<TE>(T.c[k + 1]) + tc) - cv<TE>(X.c[k]) * (tc + cv<TE>(T.c[k - 1]))) *
           (TE)0.5 * ux;
-  const TE tip = ldc<TE>(temp + o.ip + k), tim = ldc<TE>(temp + o.im + k);
-  const TE tjp = ldc<TE>(temp + o.jp + k), tjm = ldc<TE>(temp + o.jm + k);
-  const TE htz = (ldc<TE>(vz + o.ip + k) * (tip + tc) - ldc<TE>(vz + o.c + k) * (tc + tim)) * udz;
-  const TE hty = (ldc<TE>(vy + o.jp + k) * (tjp + tc) - ldc<TE>(vy + o.c + k) * (tc + tjm)) * udy;
+  const TE tip = cv<TE>(T.ip[k]), tim = cv<TE>(T.im[k]);
+  const TE tjp = cv<TE>(T.jp[k]), tjm = cv<TE>(T.jm[k]);
+  const TE htz = (cv<TE>(Z.ip[k]) * (tip + tc) - cv<TE>(Z.c[k]) * (tc + tim)) * udz;
+  const TE hty = (cv<TE>(Y.jp[k]) * (tjp + tc) - cv<TE>(Y.c[k]) * (tc + tjm)) * udy;
   const TE dzzt = (tip - (TE)2.0 * tc + tim) * udzq;
   const TE dyyt = (tjp - (TE)2.0 * tc + tjm) * udyq;
   const TE hro = -(htx + hty + htz) + dyyt + dzzt;
-  const double alpec = sc.al / g.pect;
-  const double tcd = __ldg(temp + o.c + k);
+  const double alpec = sc.alpec;
+  const double tcd = T.c[k];
   double dxxt;
   if (k == 0)
-    dxxt = __ldg(temp + o.c + 1) * __ldg(t.ap3ssk) + tcd * __ldg(t.ac3ssk) -
-           (__ldg(t.ap3ssk) + __ldg(t.ac3ssk)) * tbp * g.tfixs;
+    dxxt = T.c[1] * __ldg(t.ap3ssk) + tcd * __ldg(t.ac3ssk) - (__ldg(t.ap3ssk) + __ldg(t.ac3ssk)) * tbp * g.tfixs;
   else if (k == g.nxm - 1)
-    dxxt = tcd * __ldg(t.ac3ssk + k) + __ldg(temp + o.c + k - 1) * __ldg(t.am3ssk + k) -
+    dxxt = tcd * __ldg(t.ac3ssk + k) + T.c[k - 1] * __ldg(t.am3ssk + k) -
            (__ldg(t.am3ssk + k) + __ldg(t.ac3ssk + k)) * ttp * g.tfixn;
   else
-    dxxt = __ldg(temp + o.c + k + 1) * __ldg(t.ap3ssk + k) + tcd * __ldg(t.ac3ssk + k) +
-           __ldg(temp + o.c + k - 1) * __ldg(t.am3ssk + k);
-  const double rhs = (sc.ga * (double)hro + sc.ro * (double)rut[o.c + k] + alpec * dxxt) * sc.dt;
-  rut[o.c + k] = (TR)hro;
-  return rhs;
+    dxxt = T.c[k + 1] * __ldg(t.ap3ssk + k) + tcd * __ldg(t.ac3ssk + k) + T.c[k - 1] * __ldg(t.am3ssk + k);
+  qout = hro;
+  return (sc.ga * (double)hro + sc.ro * ru + alpec * dxxt) * sc.dt;
 }
 
-// K1: one warp per (j,i) column, WPB columns per block.  Per warp shared memory holds the four
-// scaled RHS columns in chunk layout ([q][lane], row r at (r%M)*32 + r/M).
-template <int M, int WPB, typename TE>
-__global__ void __launch_bounds__(WPB * 32)
+// Number of x-columns K1 stages per (j,i) column: vx 5, vy 6, vz 6, temp 5, pr 3 (FP64) + 4 RK3
+// histories (TE).
+constexpr int kK1StateCols = 25;
+constexpr int kK1RuCols = 4;
+
+__host__ __device__ inline size_t k1_stage_bytes(int ldx, size_t te_size) {
+  return (size_t)kK1StateCols * ldx * sizeof(double) + (size_t)kK1RuCols * ldx * te_size;
+}
+
+// K1: a block owns one (j,i) column.  One thread issues 1-D TMA bulk copies of the 29 needed
+// x-columns (contiguous runs of ldx elements) into shared memory, completing on an mbarrier;
+// then TPC threads each compute the four explicit terms and RHS of RPT cells from shared
+// memory, write the new RK3 histories, and put the scaled RHS in the solver's chunk layout
+// (row r at (r%M)*33 + r/M).  Four warps run the partitioned CN solves, and every thread adds
+// the increments to the staged centre values and stores the intermediate fields.
+template <int M, int TPC, int RPT, typename TE>
+__global__ void __launch_bounds__(TPC)
     k_explicit_implicit(Geom g, Tables t, const StepCoef *__restrict__ sc_all, int ns,
                         const double *__restrict__ cn_tab, const double *__restrict__ vx,
                         const double *__restrict__ vy, const double *__restrict__ vz,
                         const double *__restrict__ temp, const double *__restrict__ pr,
                         TE *__restrict__ rux, TE *__restrict__ ruy, TE *__restrict__ ruz,
                         TE *__restrict__ rut, double *__restrict__ vx_o, double *__restrict__ vy_o,
-                        double *__restrict__ vz_o, double *__restrict__ temp_o) {
-  extern __shared__ double smem_k1[];
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int colid = blockIdx.x * WPB + warp;
-  if (colid >= g.nym * g.nzm) return;  // whole warp leaves; no block-wide barrier below
-  double *s_x = smem_k1 + warp * (4 * 32 * M);
-  double *s_y = s_x + 32 * M, *s_z = s_x + 64 * M, *s_t = s_x + 96 * M;
-  Cols o;
-  o.j = colid % g.nym;
-  o.i = colid / g.nym;
-  const int jp = wrap_inc(o.j, g.nym), jm = wrap_dec(o.j, g.nym);
-  const int ip = wrap_inc(o.i, g.nzm), im = wrap_dec(o.i, g.nzm);
-  o.c = col_off(g, o.j, o.i);
-  o.jp = col_off(g, jp, o.i);
-  o.jm = col_off(g, jm, o.i);
-  o.ip = col_off(g, o.j, ip);
-  o.im = col_off(g, o.j, im);
-  o.jmip = col_off(g, jm, ip);
-  o.jpim = col_off(g, jp, im);
+                        double *__restrict__ vz_o, double *__restrict__ temp_o, int *__restrict__ err) {
+  constexpr int LD = 33;
+  constexpr int FLD = LD * M;
+  extern __shared__ __align__(128) unsigned char smem_k1[];
+  __shared__ uint64_t bar;
+  const int ldx = g.ldx;
+  double *cols = reinterpret_cast<double *>(smem_k1);
+  TE *rcols = reinterpret_cast<TE *>(cols + (size_t)kK1StateCols * ldx);
+  double *s_rhs = reinterpret_cast<double *>(smem_k1 + k1_stage_bytes(ldx, sizeof(TE)));
+  const int tc = threadIdx.x;
+  const int colid = blockIdx.x;
+  const int j = colid % g.nym, i = colid / g.nym;
+  const int jp = wrap_inc(j, g.nym), jm = wrap_dec(j, g.nym);
+  const int ip = wrap_inc(i, g.nzm), im = wrap_dec(i, g.nzm);
+  const size_t c0 = col_off(g, j, i);
+  if (tc == 0) {
+    mbar_init(&bar, 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+  if (tc == 0) {
+    const size_t oc = c0, ojp = col_off(g, jp, i), ojm = col_off(g, jm, i), oip = col_off(g, j, ip),
+                 oim = col_off(g, j, im), ojpim = col_off(g, jp, im), ojmip = col_off(g, jm, ip);
+    const uint32_t cb = (uint32_t)ldx * sizeof(double), rb = (uint32_t)ldx * sizeof(TE);
+    mbar_arrive_expect_tx(&bar, (uint32_t)k1_stage_bytes(ldx, sizeof(TE)));
+    const double *src[kK1StateCols] = {vx + oc,   vx + ojp, vx + ojm, vx + oip, vx + oim,  // 0-4
+                                       vy + oc,   vy + ojp, vy + ojm, vy + oip, vy + oim, vy + ojpim,  // 5-10
+                                       vz + oc,   vz + ojp, vz + ojm, vz + oip, vz + oim, vz + ojmip,  // 11-16
+                                       temp + oc, temp + ojp, temp + ojm, temp + oip, temp + oim,      // 17-21
+                                       pr + oc,   pr + ojm, pr + oim};                                // 22-24
+#pragma unroll
+    for (int q = 0; q < kK1StateCols; ++q) bulk_g2s(cols + (size_t)q * ldx, src[q], cb, &bar);
+    bulk_g2s(rcols, rux + oc, rb, &bar);
+    bulk_g2s(rcols + ldx, ruy + oc, rb, &bar);
+    bulk_g2s(rcols + 2 * ldx, ruz + oc, rb, &bar);
+    bulk_g2s(rcols + 3 * ldx, rut + oc, rb, &bar);
+  }
+  const bool ok = mbar_wait(&bar, 0, kSpinLimit);
+  if (!__syncthreads_and(ok)) {
+    if (tc == 0) atomicOr(err, 2);
+    mbar_wait(&bar, 0, kSpinLimit);  // let copies in flight land before the block exits
+    return;
+  }
+  auto C = [&](int q) { return (const double *)(cols + (size_t)q * ldx); };
+  const ColV X{C(0), C(1), C(2), C(3), C(4), nullptr};
+  const ColV Y{C(5), C(6), C(7), C(8), C(9), C(10)};
+  const ColV Z{C(11), C(12), C(13), C(14), C(15), C(16)};
+  const ColV T{C(17), C(18), C(19), C(20), C(21), nullptr};
+  const ColV P{C(22), nullptr, C(23), nullptr, C(24), nullptr};
   const StepCoef sc = sc_all[ns];
   const size_t tsz = cn_table_size(M);
   const double *TX = cn_tab + (size_t)(ns * 3 + 0) * tsz;
   const double *TY = cn_tab + (size_t)(ns * 3 + 1) * tsz;
   const double *TT = cn_tab + (size_t)(ns * 3 + 2) * tsz;
   const int nxm = g.nxm;
-
-#pragma unroll 1
-  for (int tt = 0; tt < M; ++tt) {
-    const int r = lane + 32 * tt;
-    const int sidx = (r % M) * 32 + r / M;
-    double dx_ = 0.0, dy_ = 0.0, dz_ = 0.0, dt_ = 0.0;
-    if (r < nxm - 1)
-      dx_ = rhs_vx<TE, TE>(g, t, sc, o, r + 1, vx, vy, vz, temp, pr, rux) * __ldg(TX + r);
-    if (r < nxm) {
-      const double syz = __ldg(TY + r);
-      dy_ = rhs_vy<TE, TE>(g, t, sc, o, r, vx, vy, vz, temp, pr, ruy) * syz;
-      dz_ = rhs_vz<TE, TE>(g, t, sc, o, r, vx, vy, vz, temp, pr, ruz) * syz;
-      dt_ = rhs_temp<TE, TE>(g, t, sc, o, r, vx, vy, vz, temp, rut) * __ldg(TT + r);
-    }
-    s_x[sidx] = dx_;
-    s_y[sidx] = dy_;
-    s_z[sidx] = dz_;
-    s_t[sidx] = dt_;
-  }
-  __syncwarp();
-  cn_solve_chunk<M>(s_x, TX, lane);
-  cn_solve_chunk<M>(s_y, TY, lane);
-  cn_solve_chunk<M>(s_z, TY, lane);
-  cn_solve_chunk<M>(s_t, TT, lane);
-  __syncwarp();
-#pragma unroll 1
-  for (int tt = 0; tt < M; ++tt) {
-    const int r = lane + 32 * tt;
-    const int sidx = (r % M) * 32 + r / M;
-    if (r < nxm - 1) vx_o[o.c + r + 1] = __ldg(vx + o.c + r + 1) + s_x[sidx];
-    if (r < nxm) {
-      vy_o[o.c + r] = __ldg(vy + o.c + r) + s_y[sidx];
-      vz_o[o.c + r] = __ldg(vz + o.c + r) + s_z[sidx];
-      temp_o[o.c + r] = __ldg(temp + o.c + r) + s_t[sidx];
+  const size_t pl = (size_t)j + (size_t)g.nym * i;
+  const double tbp = __ldg(t.tempbp + pl), ttp = __ldg(t.temptp + pl);
+#pragma unroll
+  for (int p = 0; p < RPT; ++p) {
+    const int k = tc + TPC * p;
+    if (k < nxm) {
+      const double syz = __ldg(TY + k);
+      const int sk = (k % M) * LD + k / M;
+      TE q;
+      if (k >= 1) {
+        const int r = k - 1;
+        s_rhs[(r % M) * LD + r / M] = rhs_vx<TE>(g, t, sc, k, X, Y, Z, T, P, (double)rcols[k], q) * __ldg(TX + r);
+        rux[c0 + k] = q;
+      }
+      s_rhs[FLD + sk] = rhs_vy<TE>(g, t, sc, k, X, Y, Z, T, P, (double)rcols[ldx + k], q) * syz;
+      ruy[c0 + k] = q;
+      s_rhs[2 * FLD + sk] = rhs_vz<TE>(g, t, sc, k, X, Y, Z, T, P, (double)rcols[2 * ldx + k], q) * syz;
+      ruz[c0 + k] = q;
+      s_rhs[3 * FLD + sk] = rhs_temp<TE>(g, t, sc, k, X, Y, Z, T, tbp, ttp, (double)rcols[3 * ldx + k], q) *
+                            __ldg(TT + k);
+      rut[c0 + k] = q;
     }
   }
-  // ImplicitAndUpdateVX.F90:171-172: vx(1) = vx(nx) = 0
-  if (lane == 0) vx_o[o.c] = 0.0;
-  if (lane == 1) vx_o[o.c + g.nx - 1] = 0.0;
+  // identity padding rows: vx rows nxm-1 .. 32M-1, the others nxm .. 32M-1
+  for (int r = nxm - 1 + tc; r < 32 * M; r += TPC) {
+    const int sr = (r % M) * LD + r / M;
+    s_rhs[sr] = 0.0;
+    if (r >= nxm) {
+      s_rhs[FLD + sr] = 0.0;
+      s_rhs[2 * FLD + sr] = 0.0;
+      s_rhs[3 * FLD + sr] = 0.0;
+    }
+  }
+  __syncthreads();
+  {
+    const int warp = tc >> 5, lane = tc & 31;
+    constexpr int NW = TPC / 32;
+    for (int f = warp; f < 4; f += NW) {
+      const double *Tb = (f == 0) ? TX : ((f == 3) ? TT : TY);
+      cn_solve_chunk<M, LD>(s_rhs + f * FLD, Tb, lane);
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int p = 0; p < RPT; ++p) {
+    const int k = tc + TPC * p;
+    if (k < nxm) {
+      const int sk = (k % M) * LD + k / M;
+      if (k >= 1) {
+        const int r = k - 1;
+        vx_o[c0 + k] = X.c[k] + s_rhs[(r % M) * LD + r / M];
+      } else {
+        vx_o[c0] = 0.0;  // ImplicitAndUpdateVX.F90:171-172: vx(1) = vx(nx) = 0
+        vx_o[c0 + nxm] = 0.0;
+      }
+      vy_o[c0 + k] = Y.c[k] + s_rhs[FLD + sk];
+      vz_o[c0 + k] = Z.c[k] + s_rhs[2 * FLD + sk];
+      temp_o[c0 + k] = T.c[k] + s_rhs[3 * FLD + sk];
+    }
+  }
 }
 
 // ------------------------------------------------------------------------------------------
@@ -474,6 +514,7 @@ __global__ void __launch_bounds__(256)
   const double usdtal = 1.0 / (sc.dt * sc.al);
   const int tx = threadIdx.x % TX;
   const int k = k0 + tx;
+#pragma unroll 4
   for (int j = threadIdx.x / TX; j < N; j += blockDim.x / TX) {
     double dv = 0.0;
     if (k < g.nxm) {
@@ -525,6 +566,7 @@ __global__ void __launch_bounds__(256)
   const int k0 = blockIdx.x * TXZ, ky = blockIdx.y;
   const size_t zstride = (size_t)g.nyh * g.ldxc;
   C *base = spec + (size_t)ky * g.ldxc + k0;
+#pragma unroll 8
   for (int e = threadIdx.x; e < N * TXZ; e += blockDim.x) {
     const int ex = e % TXZ, iz = e / TXZ;
     C v;
@@ -566,7 +608,7 @@ __global__ void __launch_bounds__(WPB * 32)
   C *colp = spec + (size_t)sys * g.ldxc;
   const int n = g.nxm;
   const double akj = __ldg(t.ak2 + ky), aki = __ldg(t.ak1 + kz);
-#pragma unroll 1
+#pragma unroll
   for (int tt = 0; tt < M; ++tt) {
     const int r = lane + 32 * tt;
     const int s = (r % M) * 32 + r / M;
@@ -695,6 +737,7 @@ __global__ void __launch_bounds__(256)
   const int N = g.nym, B = TX / 2;
   C *b1 = b0 + (size_t)B * N;
   const int k0 = blockIdx.x * TX, i = blockIdx.y;
+#pragma unroll 4
   for (int e = threadIdx.x; e < N * B; e += blockDim.x) {
     const int p = e % B, j = e / B;
     const bool cj = (2 * j > N);
@@ -897,24 +940,34 @@ cudaError_t launch_cn_tables(const LaunchCtx &L, const CnInputs &in) {
   a.dt = in.dt;
   a.beta = in.beta;
   a.pect = in.pect;
+  a.ren = in.ren;
   a.ns0 = in.ns0;
   a.nsub = in.nsub;
   k_cn_tables<<<3 * in.nsub, 32, 0, L.stream>>>(a, in.M, in.tab, in.sc);
   return cudaGetLastError();
 }
 
+template <int M, int TPC, int RPT, typename TE>
+static cudaError_t launch_k1_cfg(const LaunchCtx &L, const SubstepBuffers &b, int ns) {
+  const int ncol = L.g.nym * L.g.nzm;
+  const size_t smem = k1_stage_bytes(L.g.ldx, sizeof(TE)) + (size_t)4 * 33 * M * sizeof(double);
+  auto kern = k_explicit_implicit<M, TPC, RPT, TE>;
+  cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  kern<<<ncol, TPC, smem, L.stream>>>(L.g, L.t, b.sc, ns, b.cn_tab, b.vx, b.vy, b.vz, b.temp, b.pr,
+                                      (TE *)b.rux, (TE *)b.ruy, (TE *)b.ruz, (TE *)b.rut, b.vx_o, b.vy_o,
+                                      b.vz_o, b.temp_o, b.err);
+  return cudaGetLastError();
+}
+
+// M = ceil(nxm/32) rounded to {1,2,4,8,12,16,24,32}; TPC threads cover nxm in RPT rows each.
 template <int M, typename TE>
 static cudaError_t launch_k1_M(const LaunchCtx &L, const SubstepBuffers &b, int ns) {
-  constexpr int WPB = (M >= 16) ? 64 / M : 8;
-  constexpr int W = (WPB < 1) ? 1 : WPB;
-  const int ncol = L.g.nym * L.g.nzm;
-  const size_t smem = (size_t)W * 4 * 32 * M * sizeof(double);
-  auto kern = k_explicit_implicit<M, W, TE>;
-  cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  kern<<<(ncol + W - 1) / W, W * 32, smem, L.stream>>>(
-      L.g, L.t, b.sc, ns, b.cn_tab, b.vx, b.vy, b.vz, b.temp, b.pr, (TE *)b.rux, (TE *)b.ruy,
-      (TE *)b.ruz, (TE *)b.rut, b.vx_o, b.vy_o, b.vz_o, b.temp_o);
-  return cudaGetLastError();
+  if constexpr (M <= 1) return launch_k1_cfg<M, 32, 1, TE>(L, b, ns);          // nxm <= 32
+  else if constexpr (M <= 2) return launch_k1_cfg<M, 64, 1, TE>(L, b, ns);     // <= 64
+  else if constexpr (M <= 4) return launch_k1_cfg<M, 128, 1, TE>(L, b, ns);    // <= 128
+  else if constexpr (M <= 8) return launch_k1_cfg<M, 256, 1, TE>(L, b, ns);    // <= 256
+  else if constexpr (M <= 16) return launch_k1_cfg<M, 256, 2, TE>(L, b, ns);   // <= 512
+  else return launch_k1_cfg<M, 256, 4, TE>(L, b, ns);                          // <= 1024
 }
 
 template <typename TE>
@@ -963,102 +1016,87 @@ static cudaError_t launch_k4_T(const LaunchCtx &L, void *spec, int *err) {
 }
 
 template <typename TS>
-static cudaError_t launch_pressure_T(const LaunchCtx &L, const SubstepBuffers &b, int ns) {
+static cudaError_t launch_stage_T(const LaunchCtx &L, const SubstepBuffers &b, int ns, Stage st) {
   using C = typename Cplx<TS>::type;
   const Geom &g = L.g;
   C *spec = (C *)b.spec;
   const C *twy = (const C *)L.twy;
   const C *twz = (const C *)L.twz;
-  cudaError_t e;
-  // K2 divergence + forward y FFT
-  {
-    const int TX = L.tx_y;
-    const size_t smem = (size_t)TX * g.nym * sizeof(C);  // 2 buffers of TX/2 sequences
-    dim3 grid((g.nxm + TX - 1) / TX, g.nzm);
-    if (TX == 8) {
-      cudaFuncSetAttribute(k_div_fft_y<8, TS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-      k_div_fft_y<8, TS><<<grid, 256, smem, L.stream>>>(g, L.t, b.sc, ns, b.vx_o, b.vy_o, b.vz_o, spec,
-                                                        L.plan_y, twy);
-    } else if (TX == 4) {
-      cudaFuncSetAttribute(k_div_fft_y<4, TS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-      k_div_fft_y<4, TS><<<grid, 256, smem, L.stream>>>(g, L.t, b.sc, ns, b.vx_o, b.vy_o, b.vz_o, spec,
-                                                        L.plan_y, twy);
-    } else {
-      cudaFuncSetAttribute(k_div_fft_y<2, TS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-      k_div_fft_y<2, TS><<<grid, 256, smem, L.stream>>>(g, L.t, b.sc, ns, b.vx_o, b.vy_o, b.vz_o, spec,
-                                                        L.plan_y, twy);
+  switch (st) {
+    case Stage::DivFftY: {  // K2 divergence + forward y FFT
+      const int TX = L.tx_y;
+      const size_t smem = (size_t)TX * g.nym * sizeof(C);  // 2 buffers of TX/2 sequences
+      dim3 grid((g.nxm + TX - 1) / TX, g.nzm);
+      if (TX == 8) {
+        cudaFuncSetAttribute(k_div_fft_y<8, TS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        k_div_fft_y<8, TS><<<grid, 256, smem, L.stream>>>(g, L.t, b.sc, ns, b.vx_o, b.vy_o, b.vz_o, spec,
+                                                          L.plan_y, twy);
+      } else if (TX == 4) {
+        cudaFuncSetAttribute(k_div_fft_y<4, TS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        k_div_fft_y<4, TS><<<grid, 256, smem, L.stream>>>(g, L.t, b.sc, ns, b.vx_o, b.vy_o, b.vz_o, spec,
+                                                          L.plan_y, twy);
+      } else {
+        cudaFuncSetAttribute(k_div_fft_y<2, TS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        k_div_fft_y<2, TS><<<grid, 256, smem, L.stream>>>(g, L.t, b.sc, ns, b.vx_o, b.vy_o, b.vz_o, spec,
+                                                          L.plan_y, twy);
+      }
+      return cudaGetLastError();
     }
-    if ((e = cudaGetLastError()) != cudaSuccess) return e;
-  }
-  // K3 forward z FFT
-  if (g.nzm > 1) {
-    const int TXZ = L.tx_z;
-    const size_t smem = (size_t)2 * TXZ * g.nzm * sizeof(C);
-    dim3 grid((g.nxm + TXZ - 1) / TXZ, g.nyh);
-    if (TXZ == 8) {
-      cudaFuncSetAttribute(k_fft_z<8, false, TS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-      k_fft_z<8, false, TS><<<grid, 256, smem, L.stream>>>(g, spec, L.plan_z, twz);
-    } else if (TXZ == 4) {
-      cudaFuncSetAttribute(k_fft_z<4, false, TS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-      k_fft_z<4, false, TS><<<grid, 256, smem, L.stream>>>(g, spec, L.plan_z, twz);
-    } else {
-      cudaFuncSetAttribute(k_fft_z<2, false, TS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-      k_fft_z<2, false, TS><<<grid, 256, smem, L.stream>>>(g, spec, L.plan_z, twz);
+    case Stage::FftZFwd:
+    case Stage::FftZInv: {  // K3 / K5 z FFT
+      if (g.nzm == 1) return cudaSuccess;
+      const int TXZ = L.tx_z;
+      const size_t smem = (size_t)2 * TXZ * g.nzm * sizeof(C);
+      dim3 grid((g.nxm + TXZ - 1) / TXZ, g.nyh);
+      const bool inv = (st == Stage::FftZInv);
+#define AFID_FFTZ(TXv, INVv)                                                                       \
+  do {                                                                                             \
+    cudaFuncSetAttribute(k_fft_z<TXv, INVv, TS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem); \
+    k_fft_z<TXv, INVv, TS><<<grid, 256, smem, L.stream>>>(g, spec, L.plan_z, twz);                 \
+  } while (0)
+      if (TXZ == 8) { if (inv) AFID_FFTZ(8, true); else AFID_FFTZ(8, false); }
+      else if (TXZ == 4) { if (inv) AFID_FFTZ(4, true); else AFID_FFTZ(4, false); }
+      else { if (inv) AFID_FFTZ(2, true); else AFID_FFTZ(2, false); }
+#undef AFID_FFTZ
+      return cudaGetLastError();
     }
-    if ((e = cudaGetLastError()) != cudaSuccess) return e;
-  }
-  // K4 tridiagonal per mode
-  if ((e = launch_k4_T<TS>(L, b.spec, b.err)) != cudaSuccess) return e;
-  // K5 backward z FFT
-  if (g.nzm > 1) {
-    const int TXZ = L.tx_z;
-    const size_t smem = (size_t)2 * TXZ * g.nzm * sizeof(C);
-    dim3 grid((g.nxm + TXZ - 1) / TXZ, g.nyh);
-    if (TXZ == 8) {
-      cudaFuncSetAttribute(k_fft_z<8, true, TS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-      k_fft_z<8, true, TS><<<grid, 256, smem, L.stream>>>(g, spec, L.plan_z, twz);
-    } else if (TXZ == 4) {
-      cudaFuncSetAttribute(k_fft_z<4, true, TS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-      k_fft_z<4, true, TS><<<grid, 256, smem, L.stream>>>(g, spec, L.plan_z, twz);
-    } else {
-      cudaFuncSetAttribute(k_fft_z<2, true, TS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-      k_fft_z<2, true, TS><<<grid, 256, smem, L.stream>>>(g, spec, L.plan_z, twz);
+    case Stage::Tridiag:  // K4
+      return launch_k4_T<TS>(L, b.spec, b.err);
+    case Stage::IfftY: {  // K6 backward y FFT -> phi
+      const int TX = L.tx_y;
+      const size_t smem = (size_t)TX * g.nym * sizeof(C);
+      dim3 grid((g.nxm + TX - 1) / TX, g.nzm);
+      TS *phi = (TS *)b.phi;
+      if (TX == 8) {
+        cudaFuncSetAttribute(k_ifft_y<8, TS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        k_ifft_y<8, TS><<<grid, 256, smem, L.stream>>>(g, spec, phi, L.plan_y, twy);
+      } else if (TX == 4) {
+        cudaFuncSetAttribute(k_ifft_y<4, TS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        k_ifft_y<4, TS><<<grid, 256, smem, L.stream>>>(g, spec, phi, L.plan_y, twy);
+      } else {
+        cudaFuncSetAttribute(k_ifft_y<2, TS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        k_ifft_y<2, TS><<<grid, 256, smem, L.stream>>>(g, spec, phi, L.plan_y, twy);
+      }
+      return cudaGetLastError();
     }
-    if ((e = cudaGetLastError()) != cudaSuccess) return e;
-  }
-  // K6 backward y FFT -> phi
-  {
-    const int TX = L.tx_y;
-    const size_t smem = (size_t)TX * g.nym * sizeof(C);
-    dim3 grid((g.nxm + TX - 1) / TX, g.nzm);
-    TS *phi = (TS *)b.phi;
-    if (TX == 8) {
-      cudaFuncSetAttribute(k_ifft_y<8, TS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-      k_ifft_y<8, TS><<<grid, 256, smem, L.stream>>>(g, spec, phi, L.plan_y, twy);
-    } else if (TX == 4) {
-      cudaFuncSetAttribute(k_ifft_y<4, TS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-      k_ifft_y<4, TS><<<grid, 256, smem, L.stream>>>(g, spec, phi, L.plan_y, twy);
-    } else {
-      cudaFuncSetAttribute(k_ifft_y<2, TS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-      k_ifft_y<2, TS><<<grid, 256, smem, L.stream>>>(g, spec, phi, L.plan_y, twy);
+    case Stage::Correct: {  // K7 projection + pressure update
+      const int bx = (g.nxm >= 256) ? 256 : ((g.nxm + 31) / 32) * 32;
+      const int by = 256 / bx;
+      dim3 block(bx, by);
+      dim3 grid((g.nxm + bx - 1) / bx, (g.nym + by - 1) / by, g.nzm);
+      k_correct<TS><<<grid, block, 0, L.stream>>>(g, L.t, b.sc, ns, b.vx_o, b.vy_o, b.vz_o, b.vx, b.vy,
+                                                  b.vz, b.pr, (const TS *)b.phi);
+      return cudaGetLastError();
     }
-    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    case Stage::ExplicitImplicit:
+      return L.mixed ? launch_k1_T<float>(L, b, ns) : launch_k1_T<double>(L, b, ns);
   }
-  // K7 projection + pressure update
-  {
-    const int bx = (g.nxm >= 256) ? 256 : ((g.nxm + 31) / 32) * 32;
-    const int by = 256 / bx;
-    dim3 block(bx, by);
-    dim3 grid((g.nxm + bx - 1) / bx, (g.nym + by - 1) / by, g.nzm);
-    k_correct<TS><<<grid, block, 0, L.stream>>>(g, L.t, b.sc, ns, b.vx_o, b.vy_o, b.vz_o, b.vx, b.vy,
-                                                b.vz, b.pr, (const TS *)b.phi);
-    if ((e = cudaGetLastError()) != cudaSuccess) return e;
-  }
-  return cudaSuccess;
+  return cudaErrorInvalidValue;
 }
 
-cudaError_t launch_pressure(const LaunchCtx &L, const SubstepBuffers &b, int ns) {
-  return L.mixed ? launch_pressure_T<float>(L, b, ns) : launch_pressure_T<double>(L, b, ns);
+cudaError_t launch_stage(const LaunchCtx &L, const SubstepBuffers &b, int ns, Stage st) {
+  if (st == Stage::ExplicitImplicit) return launch_explicit_implicit(L, b, ns);
+  return L.mixed ? launch_stage_T<float>(L, b, ns, st) : launch_stage_T<double>(L, b, ns, st);
 }
 
 static int reduce_blocks(const Geom &g) {

@@ -1,0 +1,378 @@
+#!/usr/bin/env python
+"""Throughput of AFiD's RK3 flow + temperature step on a B200.
+
+Workload (default ``rbc3d``): 3-D Rayleigh-Benard convection, FP64, Ra=1e9, Pr=1, aspect ratio
+1, 384 x 384 periodic horizontal x 256 tanh-clustered (STR3=2) wall-normal cells, no-slip walls
+at T = +0.5 / -0.5, fluid at rest plus a seeded +-1e-3 perturbation, CFL-limited dt (CFLMAX 1.2,
+DT 1e-4 for the first two steps as main.F90:288-296 does).  A step is one main-loop iteration
+(CalcMaxCFL -> dt rule -> TimeMarcher, three substeps) of the whole 37.7 M-cell domain.
+
+value : Mcell-RK3-steps/s with the state resident in HBM (CUDA events on the solver stream,
+        max over ranks; ranks are independent replicas).
+e2e   : the same metric through the C ABI from pinned host buffers: upload of the five state
+        fields, K steps each reading back the CFL and the Nusselt/kinetic-energy metrics, and
+        download of the five fields, all inside the timed region.
+--impl reference : the CPU restatement of the same path (C + OpenMP, oracle/afid_cpu.c) on all
+        host cores, a bounded number of steps of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import math
+import os
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "afid-murphfi_b200"))
+
+WORKLOADS = {
+    "rbc3d": dict(nxm=256, nym=384, nzm=384, rayt=1e9, prat=1.0, ylen=1.0, zlen=1.0, precision=0,
+                  idtv=1, dt=1e-4, cflmax=1.2, dtmax=1e-2,
+                  name="rbc3d_384x384x256_fp64_ra1e9"),
+    "rbc3d_mixed": dict(nxm=384, nym=512, nzm=512, rayt=1e10, prat=1.0, ylen=1.0, zlen=1.0, precision=1,
+                        idtv=1, dt=1e-4, cflmax=1.2, dtmax=1e-2,
+                        name="rbc3d_512x512x384_mixed_ra1e10"),
+    # same kernels at 1/9 of the cells (4.2 M, ~0.6 GB per K1 launch > L2) for ncu captures
+    "rbc3d_small": dict(nxm=256, nym=128, nzm=128, rayt=1e9, prat=1.0, ylen=1.0, zlen=1.0, precision=0,
+                        idtv=1, dt=1e-4, cflmax=1.2, dtmax=1e-2,
+                        name="rbc3d_128x128x256_fp64_ra1e9"),
+    "rbc2d": dict(nxm=128, nym=256, nzm=1, rayt=1e8, prat=1.0, ylen=2.0, zlen=0.01, precision=0,
+                  idtv=0, dt=5e-4, cflmax=1.2, dtmax=5e-4,
+                  name="rbc2d_256x128_fp64_ra1e8"),
+}
+
+# Algorithmic HBM bytes per cell of the fused explicit + RHS + CN kernel (FP64): read vx, vy,
+# vz, T, p, rux, ruy, ruz, rutemp and write vx, vy, vz, T, rux, ruy, ruz, rutemp = 17 x 8 B.
+K1_BYTES_PER_CELL = 136
+# Algorithmic HBM bytes per cell per RK3 step of the whole path (one compulsory pass per
+# operator): 3 x 328 B per substep + 24 B for CalcMaxCFL.
+STEP_BYTES_PER_CELL = 1008
+
+
+def bou_text(w: dict, ntst: int) -> str:
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from helpers import bou_text as _bt  # noqa: E402  (shared bou.in template)
+    return _bt(w["nxm"], w["nym"], w["nzm"], rayt=w["rayt"], prat=w["prat"], ylen=w["ylen"],
+               zlen=w["zlen"], istr3=4, str3=2.0, idtv=w["idtv"], dt=w["dt"], cflmax=w["cflmax"],
+               dtmax=w["dtmax"], ntst=ntst, resid=1e-3)
+
+
+def measured_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def committed_traffic(workload: str):
+    """DRAM bytes per launch of the fused explicit/implicit kernel from the committed ncu
+    summary for this workload (profiles/), or None."""
+    p = os.path.join(ROOT, "profiles", f"k_explicit_implicit_{workload}.md")
+    if not os.path.exists(p):
+        return None
+    for line in open(p):
+        if line.startswith("traffic_bytes_per_launch:"):
+            return float(line.split(":")[1])
+    return None
+
+
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.dev = device_index
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.dev), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            out, _ = self.proc.communicate(timeout=5)
+        except Exception:
+            self.proc.kill()
+            out, _ = self.proc.communicate()
+        sm, smax, reasons = [], None, set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for line in out.splitlines():
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        if not sm:
+            return None
+        sm.sort()
+        return {"sm_mhz": sm[len(sm) // 2], "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_setup():
+    import torch
+    import torch.distributed as dist
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        from datetime import timedelta
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+    else:
+        torch.cuda.set_device(0)
+    return world, rank, local
+
+
+def reduce_max(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world: int):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def run_gpu(args):
+    import numpy as np
+    import torch
+    import afid_gpu as ag
+
+    world, rank, local = dist_setup()
+    w = WORKLOADS[args.config]
+    cells = w["nxm"] * w["nym"] * w["nzm"]
+    inp = ag.parse_bou_in(bou_text(w, args.steps + args.warmup))
+    tables = ag.Tables(inp, w["precision"])
+    stream = torch.cuda.Stream()
+    solver = ag.Solver(tables.grid, tables.params)
+    solver.set_stream(stream.cuda_stream)
+    temp0 = tables.initial_temperature(20261203)
+    nx, nym, nzm = w["nxm"] + 1, w["nym"], w["nzm"]
+    zeros = np.zeros((nzm, nym, nx))
+    solver.upload(zeros, zeros, zeros, temp0, zeros)
+    ra_pr = w["prat"] * abs(w["rayt"])
+
+    dt_box = [inp.dt]
+    dtc = ctypes.c_double()
+
+    def step(ntime: int):
+        cflm = solver.calc_max_cfl()
+        dtc.value = dt_box[0]
+        err = ag.lib().afid_next_dt(ctypes.byref(inp), ntime, ctypes.byref(dtc), cflm, None)
+        dt_box[0] = dtc.value
+        solver.time_marcher(dt_box[0], ntime)
+        return err
+
+    # ---- device-resident throughput ---------------------------------------------------------
+    ntime = 0
+    for _ in range(args.warmup):
+        step(ntime)
+        ntime += 1
+    solver.synchronize()
+    solver.profile_report()  # drop warm-up records
+    solver.profile(True)
+    launches0 = solver.launch_count()
+    clocks = ClockSampler(torch.cuda.current_device())
+    barrier(world)
+    torch.cuda.synchronize()
+    clocks.start()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(args.steps):
+        step(ntime)
+        ntime += 1
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    barrier(world)
+    clk = clocks.stop()
+    ms = ev0.elapsed_time(ev1)
+    prof = solver.profile_report()
+    solver.profile(False)
+    launches = solver.launch_count() - launches0
+    ms_max = reduce_max(ms, world)
+    value = world * cells * args.steps / (ms_max * 1e-3) / 1e6
+
+    k1_ms, k1_n = prof["explicit_implicit"]
+    k1_avg_s = (k1_ms / k1_n) * 1e-3 if k1_n else float("nan")
+    peak, peak_kind = measured_peak()
+    k1_bytes = K1_BYTES_PER_CELL * cells
+    achieved = k1_bytes / k1_avg_s / 1e9
+    traffic = committed_traffic(w["name"])
+
+    # ---- end to end through the C ABI with host buffers -----------------------------------
+    pin = lambda: torch.empty((nzm, nym, nx), dtype=torch.float64, pin_memory=True).numpy()  # noqa: E731
+    h_in = {k: pin() for k in ("vx", "vy", "vz", "temp", "pr")}
+    for k in ("vx", "vy", "vz", "pr"):
+        h_in[k][...] = 0.0
+    h_in["temp"][...] = temp0
+    h_out = {k: pin() for k in ("vx", "vy", "vz", "temp", "pr")}
+    dp = ctypes.POINTER(ctypes.c_double)
+    ptr = lambda a: a.ctypes.data_as(dp)  # noqa: E731
+    lib = ag.lib()
+    barrier(world)
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    rc = lib.afid_gpu_upload(solver._h, *(ptr(h_in[k]) for k in ("vx", "vy", "vz", "temp", "pr")), nx, nym)
+    assert rc == 0, rc
+    dt_box[0] = inp.dt
+    nu = ke = None
+    for n in range(args.steps):
+        step(n)
+        nu, ke, _ = solver.global_quantities(ra_pr)
+    rc = lib.afid_gpu_download(solver._h, *(ptr(h_out[k]) for k in ("vx", "vy", "vz", "temp", "pr")), nx, nym)
+    assert rc == 0, rc
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = reduce_max(e0.elapsed_time(e1), world)
+    e2e_value = world * cells * args.steps / (e2e_ms * 1e-3) / 1e6
+    field_bytes = 5 * nx * nym * nzm * 8
+    h2d = field_bytes / args.steps
+    d2h = field_bytes / args.steps + 8 + 3 * 8
+
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(w, args.cpu_steps)
+
+    solver.close()
+    tables.close()
+    if rank == 0:
+        line = {
+            "metric": "Mcell-RK3-steps/s",
+            "value": round(value, 3),
+            "unit": "Mcell-RK3-steps/s",
+            "n_gpus": world,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": round(ms_max / args.steps, 4),
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f64" if w["precision"] == 0 else "f32+f64",
+            "data": "synthetic: conductive RBC state + Philox-seeded +-1e-3 temperature perturbation",
+            "config": {"workload": w["name"], "grid_xyz": [w["nxm"], w["nym"], w["nzm"]],
+                       "cells": cells, "Ra": w["rayt"], "Pr": w["prat"],
+                       "dt": "CFL-limited (CFLMAX 1.2, DTMAX 1e-2)" if w["idtv"] else f"fixed {w['dt']}",
+                       "l2": "inputs larger than L2 (~%.1f GB resident state)" % (cells * 8 * 17 / 1e9),
+                       "parallelism": "replicas" if world > 1 else "single GPU"},
+            "roofline": {"bound": "hbm", "kernel": "k_explicit_implicit",
+                         "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                         "frac": round(achieved / peak, 4), "peak_kind": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)",
+                         "algorithmic_bytes_per_launch": k1_bytes,
+                         "avg_launch_ms": round(k1_avg_s * 1e3, 4),
+                         "traffic": traffic,
+                         "step_frac": round(value * 1e6 * STEP_BYTES_PER_CELL / (peak * 1e9 * world), 4)},
+            "kernels_ms_per_step": {k: round(v[0] / args.steps, 4) for k, v in prof.items() if v[1]},
+            "e2e": {"value": round(e2e_value, 3), "unit": "Mcell-RK3-steps/s",
+                    "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+                    "note": "upload 5 fields, K steps with CFL + Nu/KE read back, download 5 fields"},
+            "gpu_launches": int(launches),
+            "clocks": clk,
+            "nu_vol_end": nu,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def cpu_baseline(w: dict, steps: int):
+    """The CPU restatement (C + OpenMP, oracle/afid_cpu.c) on the same workload."""
+    try:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        from oracle import cpu_port
+    except Exception as e:  # pragma: no cover
+        return {"unavailable": f"CPU port not importable: {e}"}
+    text = bou_text(w, steps)
+    res = cpu_port.time_steps(text, steps, seed=20261203, mixed=False)
+    return {"value": round(res["mcells_per_s"], 4), "unit": "Mcell-RK3-steps/s",
+            "cores": res["threads"], "kind": "port",
+            "sample": f"{steps} full steps of {w['name']} (C+OpenMP restatement)",
+            "seconds": round(res["seconds"], 2)}
+
+
+def run_reference(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    w = WORKLOADS[args.config]
+    steps = args.cpu_steps
+    cpu = cpu_baseline(w, steps)
+    if "unavailable" in cpu:
+        print(json.dumps({"impl": "reference", "unavailable": cpu["unavailable"]}), flush=True)
+        return
+    line = {
+        "impl": "reference",
+        "metric": "Mcell-RK3-steps/s",
+        "value": cpu["value"],
+        "unit": "Mcell-RK3-steps/s",
+        "n_gpus": world,
+        "steps": steps,
+        "warmup": 0,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic: conductive RBC state + Philox-seeded +-1e-3 temperature perturbation",
+        "config": {"workload": w["name"], "grid_xyz": [w["nxm"], w["nym"], w["nzm"]]},
+        "cpu_baseline": cpu,
+        "e2e": {"value": cpu["value"], "unit": "Mcell-RK3-steps/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="afid", choices=["afid", "reference"])
+    ap.add_argument("--config", default="rbc3d", choices=sorted(WORKLOADS))
+    ap.add_argument("--cpu-steps", type=int, default=2)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_gpu(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -128,6 +128,15 @@ int afid_gpu_cuda_error(afid_ctx_t *ctx);   /* last cudaError_t seen by this con
 int afid_gpu_field_device_ptr(afid_ctx_t *ctx, int which, void **dptr, int *ldx);
 /* Kernels launched by this context since creation (all are this library's own kernels). */
 long long afid_gpu_launch_count(afid_ctx_t *ctx);
+/* Per-kernel device timing with CUDA events recorded on the context stream around every
+ * launch (no counterpart in the reference, which times whole steps with MPI_WTIME,
+ * main.F90:282,363-371).  Classes: 0 CN factor tables, 1 explicit+implicit, 2 divergence +
+ * y FFT, 3 z FFT forward, 4 Poisson tridiagonal, 5 z FFT backward, 6 y FFT backward,
+ * 7 projection + pressure update, 8 reductions (CFL, divergence, volume sums). */
+#define AFID_PROF_CLASSES 9
+int afid_gpu_profile_enable(afid_ctx_t *ctx, int enable);
+/* Milliseconds and launch counts per class since the last report; synchronises the stream. */
+int afid_gpu_profile_report(afid_ctx_t *ctx, double *ms, long long *count, int n);
 
 #ifdef __cplusplus
 }
