@@ -87,6 +87,7 @@ EXPORTS = [
     "afid_gpu_substep", "afid_gpu_cfl", "afid_gpu_divmax", "afid_gpu_globals",
     "afid_gpu_status_string", "afid_gpu_cuda_error", "afid_gpu_field_device_ptr",
     "afid_gpu_launch_count", "afid_gpu_profile_enable", "afid_gpu_profile_report",
+    "afid_gpu_globals_noalloc",
     "afid_parse_bou_in", "afid_read_bou_in", "afid_tables_create", "afid_tables_destroy",
     "afid_tables_grid", "afid_tables_params", "afid_tables_array", "afid_philox_uniform",
     "afid_initial_temperature", "afid_next_dt", "afid_run",
@@ -119,6 +120,7 @@ def load_library(path: str = _LIB_PATH) -> C.CDLL:
         "afid_gpu_launch_count": (C.c_longlong, [vp]),
         "afid_gpu_profile_enable": (i, [vp, i]),
         "afid_gpu_profile_report": (i, [vp, _dp, C.POINTER(C.c_longlong), i]),
+        "afid_gpu_globals_noalloc": (i, [i, i, i, i, d, d, vp, vp, vp, vp, vp, vp, vp]),
         "afid_parse_bou_in": (i, [C.c_char_p, C.POINTER(InputT)]),
         "afid_read_bou_in": (i, [C.c_char_p, C.POINTER(InputT)]),
         "afid_tables_create": (i, [C.POINTER(InputT), i, C.POINTER(vp)]),

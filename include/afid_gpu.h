@@ -42,7 +42,7 @@ extern "C" {
 #define AFID_E_TIMEOUT 602       /* a bounded device-side wait ran out                        */
 #define AFID_E_INVALID 603       /* bad argument / unsupported configuration                  */
 #define AFID_E_CUDA 604          /* CUDA runtime error (afid_gpu_cuda_error gives the code)   */
-#define AFID_E_CAPACITY 605      /* batch / server slot or HBM budget exhausted               */
+#define AFID_E_CAPACITY 605      /* batch/server slots, HBM budget or a fixed scratch array exhausted */
 
 /* precision of the explicit terms and transforms (the implicit solves are always FP64) */
 #define AFID_PREC_FP64 0
@@ -137,6 +137,23 @@ long long afid_gpu_launch_count(afid_ctx_t *ctx);
 int afid_gpu_profile_enable(afid_ctx_t *ctx, int enable);
 /* Milliseconds and launch counts per class since the last report; synchronises the stream. */
 int afid_gpu_profile_report(afid_ctx_t *ctx, double *ms, long long *count, int n);
+
+/* ---- statistics without allocation -------------------------------------------------------
+ * No counterpart in the reference.  For callers that cannot let a library allocate device
+ * memory (a host code with its own device pool or a capped allocator, a monitor attached to
+ * someone else's run): the same {nu_vol, ke, tmean} as afid_gpu_globals, computed from device
+ * fields the caller owns (x-fastest, x-stride ldx >= nxm+1, nym rows per z-plane; g3rc is a
+ * device array of nxm values), written to the caller's device array out3[3], stream-ordered on
+ * `stream` (cudaStream_t as void*, NULL = legacy default stream).  It calls no allocator: its
+ * partial sums live in a static device array of AFID_NOALLOC_SCRATCH_BYTES that every GPU
+ * loading this library holds until exit, which limits it to nym*nzm <= 174762 columns
+ * (AFID_E_CAPACITY beyond).  The first call on each device looks up that array's address (do
+ * it before any stream capture).  Calls share the array and it keeps the last call's
+ * contents; calls that overlap on the GPU race. */
+#define AFID_NOALLOC_SCRATCH_BYTES (4u << 20)
+int afid_gpu_globals_noalloc(int nxm, int nym, int nzm, int ldx, double alx3, double ra_pr,
+                             const double *vx, const double *vy, const double *vz,
+                             const double *temp, const double *g3rc, double *out3, void *stream);
 
 #ifdef __cplusplus
 }
