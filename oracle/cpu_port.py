@@ -1,0 +1,115 @@
+"""ctypes driver of the C + OpenMP restatement (oracle/afid_cpu.c).  TEST INFRASTRUCTURE ONLY:
+used by tests/ as a second checker and by bench.py as the timed CPU baseline."""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import time
+
+import numpy as np
+
+from oracle import afid_oracle as o
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        from oracle import build_oracle
+        path = build_oracle.build()
+        _lib = C.CDLL(path)
+        _lib.afid_cpu_create.restype = C.c_void_p
+        _lib.afid_cpu_create.argtypes = [C.c_int, C.c_int, C.c_int, C.c_double, C.c_double,
+                                         C.POINTER(C.c_void_p), C.POINTER(C.c_double), C.POINTER(C.c_int)]
+        _lib.afid_cpu_destroy.argtypes = [C.c_void_p]
+        _lib.afid_cpu_set.argtypes = [C.c_void_p, C.c_int, C.c_void_p]
+        _lib.afid_cpu_get.argtypes = [C.c_void_p, C.c_int, C.c_void_p]
+        _lib.afid_cpu_timemarcher.argtypes = [C.c_void_p, C.c_double]
+        _lib.afid_cpu_cfl.restype = C.c_double
+        _lib.afid_cpu_cfl.argtypes = [C.c_void_p]
+        _lib.afid_cpu_threads.restype = C.c_int
+    return _lib
+
+
+class CpuSolver:
+    NAMES = ("vx", "vy", "vz", "temp", "pr")
+
+    def __init__(self, g: o.Grid, s: o.State):
+        p = g.p
+        self.g = g
+        nx = g.nx
+        tempbp, temptp = s.tempbp, s.temptp
+
+        def pad(a, n):
+            b = np.zeros(max(n, 1))
+            b[:min(a.size, n)] = a[:min(a.size, n)]
+            return b
+        self._keep = [pad(g.udx3c, nx), pad(g.udx3m, nx), pad(g.ap3ck, nx), pad(g.ac3ck, nx), pad(g.am3ck, nx),
+                      pad(g.ap3sk, nx), pad(g.ac3sk, nx), pad(g.am3sk, nx), pad(g.ap3ssk, nx), pad(g.ac3ssk, nx),
+                      pad(g.am3ssk, nx), pad(g.amphk, nx), pad(g.acphk, nx), pad(g.apphk, nx),
+                      np.ascontiguousarray(g.ak1), np.ascontiguousarray(g.ak2),
+                      np.ascontiguousarray(tempbp).ravel(), np.ascontiguousarray(temptp).ravel(),
+                      pad(g.g3rc, nx)]
+        tabs = (C.c_void_p * 19)(*[a.ctypes.data for a in self._keep])
+        prm = (C.c_double * 6)(g.ren, g.pect, g.byct, p.xplusu, p.xminusu, p.dpdy)
+        ipr = (C.c_int * 7)(p.active_t, p.gaxis, p.inslws, p.inslwn, p.tfixs, p.tfixn, p.nsst)
+        self._h = lib().afid_cpu_create(p.nxm, p.nym, p.nzm, p.ylen, p.zlen, tabs, prm, ipr)
+        if not self._h:
+            raise ValueError("unsupported FFT size")
+        for w, n in enumerate(self.NAMES):
+            a = np.ascontiguousarray(getattr(s, n))
+            lib().afid_cpu_set(self._h, w, a.ctypes.data)
+
+    def time_marcher(self, dt):
+        lib().afid_cpu_timemarcher(self._h, dt)
+
+    def cfl(self):
+        return lib().afid_cpu_cfl(self._h)
+
+    def get(self):
+        p = self.g.p
+        out = {}
+        for w, n in enumerate(self.NAMES):
+            a = np.zeros((p.nzm, p.nym, self.g.nx))
+            lib().afid_cpu_get(self._h, w, a.ctypes.data)
+            out[n] = a
+        return out
+
+    def close(self):
+        if self._h:
+            lib().afid_cpu_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def time_steps(bou_text: str, steps: int, seed: int = 20261203, mixed: bool = False,
+               budget_s: float = 1e30) -> dict:
+    """Main-loop steps (CFL -> dt rule -> TimeMarcher) of the C restatement on all host cores,
+    from the seeded initial state, stopping early once ``budget_s`` seconds have been spent;
+    returns the throughput in Mcell-RK3-steps/s and the steps actually timed."""
+    p = o.parse_bou_in(bou_text)
+    g = o.create_grid(p)
+    s = o.initial_state(g, seed)
+    cpu = CpuSolver(g, s)
+    dt = p.dt
+    t0 = time.perf_counter()
+    done = 0
+    for n in range(steps):
+        cflm = cpu.cfl()
+        dt, _, _ = o.next_dt(p, n, dt, cflm)
+        cpu.time_marcher(dt)
+        done += 1
+        if time.perf_counter() - t0 > budget_s:
+            break
+    sec = time.perf_counter() - t0
+    cells = p.nxm * p.nym * p.nzm
+    cpu.close()
+    return {"seconds": sec, "steps": done, "mcells_per_s": cells * done / sec / 1e6,
+            "threads": lib().afid_cpu_threads()}

@@ -190,3 +190,28 @@ def test_launch_count_positive():
     with case.solver() as gpu:
         gpu.time_marcher(1e-3)
         assert gpu.launch_count() == 1 + 3 * 7
+
+
+@pytest.mark.parametrize("name", ["rbc3d_16x12x8_rv", "rbc3d_40x10x6_rv", "rbc2d_32x48x1"])
+def test_golden_fixture(name):
+    """The GPU path from a committed fixture's initial state against its stored oracle steps."""
+    import os
+    d = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", name + ".npz"))
+    text = str(d["bou_in"])
+    inp = ag.parse_bou_in(text)
+    tab = ag.Tables(inp)
+    nxm = inp.nxm
+    with ag.Solver(tab.grid, tab.params) as gpu:
+        gpu.upload(*(d["init_" + f] for f in ("vx", "vy", "vz", "temp", "pr")))
+        for n in range(3):
+            gpu.time_marcher(float(d["dt"]), n)
+            if n in (0, 2):
+                out = gpu.download()
+                for f in ("vx", "vy", "vz", "temp"):
+                    ref = d[f"step{n + 1}_{f}"][..., :nxm + (f == "vx")]
+                    got = out[f][..., :nxm + (f == "vx")]
+                    err = rel_l2(got, ref) if np.any(ref) else float(np.abs(got).max())
+                    assert err <= TOL_FP64, (name, n, f, err)
+                assert rel_l2_mod_mean(out["pr"][..., :nxm], d[f"step{n + 1}_pr"][..., :nxm]) <= TOL_FP64
+        assert gpu.calc_max_cfl() == pytest.approx(float(d["step3_cfl"]), rel=1e-10)
+        assert gpu.global_quantities(inp.prat * abs(inp.rayt))[0] == pytest.approx(float(d["step3_nu"]), rel=1e-10)
