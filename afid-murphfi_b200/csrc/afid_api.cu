@@ -449,6 +449,7 @@ int afid_gpu_create(const afid_grid_t *grid, const afid_params_t *prm, afid_ctx_
     afid_gpu_destroy(ctx);
     return AFID_E_INVALID;
   }
+  L.warp_fft = true;
   L.plan_y = py;
   L.plan_z = pz;
   L.twy = twy;

@@ -196,6 +196,158 @@ __device__ typename Cplx<T>::type *fft_block(typename Cplx<T>::type *buf0,
 }
 
 // ------------------------------------------------------------------------------------------
+// Register-resident warp FFT for N = 32*N1 (N1 in {1,2,3,4,6,8,12,16,24,32}).
+// Element n = lane + 32*m sits in lane `lane`, register m.  Step 1: an N1-point DFT over the
+// lane's registers (compile-time Stockham passes of radix 4/2/3/5); step 2: twiddle register
+// k1 by w_N^(lane*k1); step 3: a 32-point DFT across the lanes (5 decimation-in-frequency
+// stages on xor shuffles).  Afterwards lane l, register k1 holds X[k1 + N1*bitrev5(l)].
+// Twiddles come from the length-N table tw[m] = exp(-2 pi i m/N) (conjugated for INV).
+// ------------------------------------------------------------------------------------------
+struct RadixList {
+  int n;
+  int r[8];
+};
+__host__ __device__ constexpr RadixList radix_list(int N) {
+  RadixList L{0, {0, 0, 0, 0, 0, 0, 0, 0}};
+  int m = N;
+  while (m % 4 == 0) { L.r[L.n++] = 4; m /= 4; }
+  while (m % 2 == 0) { L.r[L.n++] = 2; m /= 2; }
+  while (m % 3 == 0) { L.r[L.n++] = 3; m /= 3; }
+  while (m % 5 == 0) { L.r[L.n++] = 5; m /= 5; }
+  return L;
+}
+
+template <int R, bool INV, typename T>
+__device__ __forceinline__ void dft_small(typename Cplx<T>::type (&a)[R]) {
+  using C = typename Cplx<T>::type;
+  if constexpr (R == 2) {
+    C t = a[0];
+    a[0] = cadd(t, a[1]);
+    a[1] = csub(t, a[1]);
+  } else if constexpr (R == 4) {
+    C t0 = cadd(a[0], a[2]), t1 = csub(a[0], a[2]);
+    C t2 = cadd(a[1], a[3]), t3 = mul_mi<INV>(csub(a[1], a[3]));
+    a[0] = cadd(t0, t2);
+    a[1] = cadd(t1, t3);
+    a[2] = csub(t0, t2);
+    a[3] = csub(t1, t3);
+  } else if constexpr (R == 3) {
+    const T s3 = (T)0.86602540378443864676;
+    C t1 = cadd(a[1], a[2]);
+    C t2;
+    t2.x = a[0].x - (T)0.5 * t1.x;
+    t2.y = a[0].y - (T)0.5 * t1.y;
+    C t3 = mul_mi<INV>(csub(a[1], a[2]));
+    t3.x *= s3;
+    t3.y *= s3;
+    a[0] = cadd(a[0], t1);
+    a[1] = cadd(t2, t3);
+    a[2] = csub(t2, t3);
+  } else if constexpr (R == 5) {
+    const T c1 = (T)0.30901699437494742410, c2 = (T)-0.80901699437494742410;
+    const T s1 = (T)0.95105651629515357212, s2 = (T)0.58778525229247312917;
+    C b1 = cadd(a[1], a[4]), b4 = csub(a[1], a[4]);
+    C b2 = cadd(a[2], a[3]), b3 = csub(a[2], a[3]);
+    C r1, r2, i1, i2, y0;
+    r1.x = a[0].x + c1 * b1.x + c2 * b2.x;
+    r1.y = a[0].y + c1 * b1.y + c2 * b2.y;
+    r2.x = a[0].x + c2 * b1.x + c1 * b2.x;
+    r2.y = a[0].y + c2 * b1.y + c1 * b2.y;
+    i1.x = s1 * b4.x + s2 * b3.x;
+    i1.y = s1 * b4.y + s2 * b3.y;
+    i2.x = s2 * b4.x - s1 * b3.x;
+    i2.y = s2 * b4.y - s1 * b3.y;
+    i1 = mul_mi<INV>(i1);
+    i2 = mul_mi<INV>(i2);
+    y0.x = a[0].x + b1.x + b2.x;
+    y0.y = a[0].y + b1.y + b2.y;
+    a[0] = y0;
+    a[1] = cadd(r1, i1);
+    a[4] = csub(r1, i1);
+    a[2] = cadd(r2, i2);
+    a[3] = csub(r2, i2);
+  }
+}
+
+template <bool INV, typename T>
+__device__ __forceinline__ typename Cplx<T>::type twiddle(const typename Cplx<T>::type *__restrict__ tw,
+                                                           int m) {
+  typename Cplx<T>::type w = tw[m];
+  if (INV) w.y = -w.y;
+  return w;
+}
+
+// One Stockham pass of radix R over N1 registers (input x, output y); NS = product of earlier radices.
+template <bool INV, typename T, int N1, int R, int NS>
+__device__ __forceinline__ void reg_pass(const typename Cplx<T>::type (&x)[N1], typename Cplx<T>::type (&y)[N1],
+                                         const typename Cplx<T>::type *__restrict__ tw) {
+  using C = typename Cplx<T>::type;
+  constexpr int NR = N1 / R;
+#pragma unroll
+  for (int jj = 0; jj < NR; ++jj) {
+    const int k = jj % NS;
+    C a[R];
+#pragma unroll
+    for (int q = 0; q < R; ++q) a[q] = x[jj + q * NR];
+    if constexpr (NS > 1) {
+#pragma unroll
+      for (int q = 1; q < R; ++q) {
+        // w_{NS*R}^(q*k) = w_N^(32 * q*k*N1/(NS*R)) for N = 32*N1
+        if (k != 0) a[q] = cmul(a[q], twiddle<INV, T>(tw, 32 * q * k * (N1 / (NS * R))));
+      }
+    }
+    dft_small<R, INV, T>(a);
+#pragma unroll
+    for (int q = 0; q < R; ++q) y[(jj / NS) * NS * R + k + q * NS] = a[q];
+  }
+}
+
+template <bool INV, typename T, int N1, int P, int NS>
+__device__ __forceinline__ void reg_fft_rec(typename Cplx<T>::type (&x)[N1],
+                                            const typename Cplx<T>::type *__restrict__ tw) {
+  using C = typename Cplx<T>::type;
+  constexpr RadixList L = radix_list(N1);
+  if constexpr (P < L.n) {
+    constexpr int R = L.r[P];
+    C y[N1];
+    reg_pass<INV, T, N1, R, NS>(x, y, tw);
+#pragma unroll
+    for (int q = 0; q < N1; ++q) x[q] = y[q];
+    reg_fft_rec<INV, T, N1, P + 1, NS * R>(x, tw);
+  }
+}
+
+__device__ __forceinline__ int bitrev5(int l) { return (int)(__brev((unsigned)l) >> 27); }
+
+template <bool INV, typename T, int N1>
+__device__ __forceinline__ void warp_fft(typename Cplx<T>::type (&x)[N1], int lane,
+                                         const typename Cplx<T>::type *__restrict__ tw) {
+  using C = typename Cplx<T>::type;
+  reg_fft_rec<INV, T, N1, 0, 1>(x, tw);
+#pragma unroll
+  for (int k1 = 1; k1 < N1; ++k1)
+    if (lane != 0) x[k1] = cmul(x[k1], twiddle<INV, T>(tw, lane * k1));
+  C w5[5];
+#pragma unroll
+  for (int s = 0; s < 5; ++s) {
+    const int h = 16 >> s;
+    w5[s] = twiddle<INV, T>(tw, ((lane & (h - 1)) * (16 / h)) * N1);  // w_{2h}^(lane mod h)
+  }
+#pragma unroll
+  for (int s = 0; s < 5; ++s) {
+    const int h = 16 >> s;
+    const bool bottom = (lane & h) != 0;
+#pragma unroll
+    for (int q = 0; q < N1; ++q) {
+      C o;
+      o.x = __shfl_xor_sync(0xffffffffu, x[q].x, h);
+      o.y = __shfl_xor_sync(0xffffffffu, x[q].y, h);
+      x[q] = bottom ? cmul(csub(o, x[q]), w5[s]) : cadd(x[q], o);
+    }
+  }
+}
+
+// ------------------------------------------------------------------------------------------
 // Bounded device-side waits: every spin in this library counts iterations and gives up with
 // an error flag instead of hanging (no trap, no unbounded loop).
 // ------------------------------------------------------------------------------------------

@@ -13,7 +13,8 @@ struct LaunchCtx {
   cudaStream_t stream;
   int M;           // rows per lane of the partitioned x-solves (32*M >= nxm)
   bool mixed;      // FP32 explicit terms / transforms
-  int tx_y, tx_z;  // x-tile widths of the y and z FFT kernels
+  int tx_y, tx_z;  // x-tile widths of the shared-memory (fallback) FFT kernels
+  bool warp_fft;   // register-resident warp FFT when N = 32*{1,2,3,4,6,8,12,16,24,32}
   FftPlan plan_y, plan_z;
   const void *twy, *twz;  // twiddle tables (double2 or float2)
 };

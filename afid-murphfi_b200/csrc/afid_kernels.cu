@@ -908,6 +908,181 @@ __global__ void k_sum_partials(const double *__restrict__ partial, int nblocks, 
   }
 }
 
+// ------------------------------------------------------------------------------------------
+// Warp-FFT variants of K2, K3/K5, K6 (N = 32*N1).  Shared memory only transposes between the
+// coalesced HBM layout and the per-warp sequences (each warp owns one sequence); after the
+// transform lane l, register k1 holds element k1 + N1*bitrev5(l).
+// ------------------------------------------------------------------------------------------
+// Column swizzle of the z-transform tile [row][8 x points] (16-byte elements): element (r, w)
+// sits at r*8 + (w ^ zsw(r)).  Keeps the coalesced row accesses, the per-warp column reads and
+// the bit-reversed per-warp writes at most 2-way bank conflicted for every supported N1.
+__device__ __forceinline__ int zsw(int r) { return (r ^ (r >> 2) ^ (r >> 6)) & 7; }
+
+// K2w: divergence + forward y r2c.  Block: TX x points (TX/2 warps) at one z index i.
+template <int N1, int TX, typename TS>
+__global__ void __launch_bounds__(TX * 16)
+    k_div_fft_y_w(Geom g, Tables t, const StepCoef *__restrict__ sc_all, int ns,
+                  const double *__restrict__ vx, const double *__restrict__ vy,
+                  const double *__restrict__ vz, typename Cplx<TS>::type *__restrict__ spec,
+                  const typename Cplx<TS>::type *__restrict__ tw) {
+  using C = typename Cplx<TS>::type;
+  constexpr int N = 32 * N1, LDT = TX + 1;
+  extern __shared__ __align__(16) unsigned char smem_k2w[];
+  TS *s_re = reinterpret_cast<TS *>(smem_k2w);  // [N][TX+1] real tile
+  C *s_z = reinterpret_cast<C *>(smem_k2w);     // [TX/2][N] complex, reuses the tile
+  const int k0 = blockIdx.x * TX, i = blockIdx.y;
+  const int ip = wrap_inc(i, g.nzm);
+  const StepCoef sc = sc_all[ns];
+  const double usdtal = 1.0 / (sc.dt * sc.al);
+  const int tx = threadIdx.x % TX, k = k0 + tx;
+  const double ux = (k < g.nxm) ? __ldg(t.udx3m + k) : 0.0;
+#pragma unroll 4
+  for (int j = threadIdx.x / TX; j < N; j += blockDim.x / TX) {
+    double dv = 0.0;
+    if (k < g.nxm) {
+      const int jp = wrap_inc(j, N);
+      const size_t c = col_off(g, j, i), cjp = col_off(g, jp, i), cip = col_off(g, j, ip);
+      const double dqcap = (__ldg(vz + cip + k) - __ldg(vz + c + k)) * g.dz +
+                           (__ldg(vy + cjp + k) - __ldg(vy + c + k)) * g.dy +
+                           (__ldg(vx + c + k + 1) - __ldg(vx + c + k)) * ux;
+      dv = dqcap * usdtal;
+    }
+    s_re[j * LDT + tx] = (TS)dv;
+  }
+  __syncthreads();
+  const int lane = threadIdx.x & 31, p = threadIdx.x >> 5;
+  C x[N1];
+#pragma unroll
+  for (int m = 0; m < N1; ++m) {
+    x[m].x = s_re[(lane + 32 * m) * LDT + 2 * p];
+    x[m].y = s_re[(lane + 32 * m) * LDT + 2 * p + 1];
+  }
+  warp_fft<false, TS, N1>(x, lane, tw);
+  __syncthreads();
+  const int rl = bitrev5(lane);
+#pragma unroll
+  for (int k1 = 0; k1 < N1; ++k1) s_z[p * N + k1 + N1 * rl] = x[k1];
+  __syncthreads();
+  const TS norm = (TS)(1.0 / ((double)g.nzm * (double)g.nym));
+  const TS half = (TS)0.5;
+  for (int e = threadIdx.x; e < g.nyh * TX; e += blockDim.x) {
+    const int ex = e % TX, ky = e / TX;
+    const int kk = k0 + ex;
+    if (kk >= g.nxm) continue;
+    const int q = ex >> 1;
+    const C zk = s_z[q * N + ky];
+    const C zn = s_z[q * N + (ky == 0 ? 0 : N - ky)];
+    C X;
+    if ((ex & 1) == 0) {
+      X.x = (zk.x + zn.x) * half;
+      X.y = (zk.y - zn.y) * half;
+    } else {
+      X.x = (zk.y + zn.y) * half;
+      X.y = (zn.x - zk.x) * half;
+    }
+    X.x *= norm;
+    X.y *= norm;
+    spec[(size_t)(ky + (size_t)g.nyh * i) * g.ldxc + kk] = X;
+  }
+}
+
+// K3w / K5w: z c2c in place.  Block: 8 x points (8 warps) at one ky.
+template <int N1, bool INV, typename TS>
+__global__ void __launch_bounds__(256)
+    k_fft_z_w(Geom g, typename Cplx<TS>::type *__restrict__ spec,
+              const typename Cplx<TS>::type *__restrict__ tw) {
+  using C = typename Cplx<TS>::type;
+  constexpr int N = 32 * N1;
+  extern __shared__ __align__(16) unsigned char smem_k3w[];
+  C *s = reinterpret_cast<C *>(smem_k3w);  // [N][8], swizzled columns
+  const int k0 = blockIdx.x * 8, ky = blockIdx.y;
+  const size_t zstride = (size_t)g.nyh * g.ldxc;
+  C *base = spec + (size_t)ky * g.ldxc + k0;
+  const int nvalid = min(8, g.nxm - k0);
+#pragma unroll 4
+  for (int e = threadIdx.x; e < N * 8; e += blockDim.x) {
+    const int ex = e & 7, iz = e >> 3;
+    C v;
+    v.x = 0;
+    v.y = 0;
+    if (ex < nvalid) v = base[(size_t)iz * zstride + ex];
+    s[iz * 8 + (ex ^ zsw(iz))] = v;
+  }
+  __syncthreads();
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  C x[N1];
+#pragma unroll
+  for (int m = 0; m < N1; ++m) {
+    const int r = lane + 32 * m;
+    x[m] = s[r * 8 + (w ^ zsw(r))];
+  }
+  warp_fft<INV, TS, N1>(x, lane, tw);
+  __syncthreads();
+  const int rl = bitrev5(lane);
+#pragma unroll
+  for (int k1 = 0; k1 < N1; ++k1) {
+    const int r = k1 + N1 * rl;
+    s[r * 8 + (w ^ zsw(r))] = x[k1];
+  }
+  __syncthreads();
+#pragma unroll 4
+  for (int e = threadIdx.x; e < N * 8; e += blockDim.x) {
+    const int ex = e & 7, iz = e >> 3;
+    if (ex < nvalid) base[(size_t)iz * zstride + ex] = s[iz * 8 + (ex ^ zsw(iz))];
+  }
+}
+
+// K6w: backward y c2r.  Block: TX x points (TX/2 warps) at one z index i.
+template <int N1, int TX, typename TS>
+__global__ void __launch_bounds__(TX * 16)
+    k_ifft_y_w(Geom g, const typename Cplx<TS>::type *__restrict__ spec, TS *__restrict__ phi,
+               const typename Cplx<TS>::type *__restrict__ tw) {
+  using C = typename Cplx<TS>::type;
+  constexpr int N = 32 * N1, LDT = TX + 1, B = TX / 2;
+  extern __shared__ __align__(16) unsigned char smem_k6w[];
+  C *s_z = reinterpret_cast<C *>(smem_k6w);     // [B][N]
+  TS *s_re = reinterpret_cast<TS *>(smem_k6w);  // [N][TX+1], reuses the buffer
+  const int k0 = blockIdx.x * TX, i = blockIdx.y;
+#pragma unroll 4
+  for (int e = threadIdx.x; e < N * B; e += blockDim.x) {
+    const int p = e % B, j = e / B;
+    const bool cj = (2 * j > N);
+    const int jj = cj ? N - j : j;
+    const int ka = k0 + 2 * p, kb = ka + 1;
+    const C *src = spec + (size_t)(jj + (size_t)g.nyh * i) * g.ldxc;
+    C X, Y;
+    X.x = 0; X.y = 0; Y.x = 0; Y.y = 0;
+    if (ka < g.nxm) X = src[ka];
+    if (kb < g.nxm) Y = src[kb];
+    if (cj) { X.y = -X.y; Y.y = -Y.y; }
+    if (jj == 0 || 2 * jj == N) { X.y = 0; Y.y = 0; }
+    C Z;
+    Z.x = X.x - Y.y;
+    Z.y = X.y + Y.x;
+    s_z[p * N + j] = Z;
+  }
+  __syncthreads();
+  const int lane = threadIdx.x & 31, p = threadIdx.x >> 5;
+  C x[N1];
+#pragma unroll
+  for (int m = 0; m < N1; ++m) x[m] = s_z[p * N + lane + 32 * m];
+  warp_fft<true, TS, N1>(x, lane, tw);
+  __syncthreads();
+  const int rl = bitrev5(lane);
+#pragma unroll
+  for (int k1 = 0; k1 < N1; ++k1) {
+    s_re[(k1 + N1 * rl) * LDT + 2 * p] = x[k1].x;
+    s_re[(k1 + N1 * rl) * LDT + 2 * p + 1] = x[k1].y;
+  }
+  __syncthreads();
+#pragma unroll 4
+  for (int e = threadIdx.x; e < N * TX; e += blockDim.x) {
+    const int ex = e % TX, j = e / TX;
+    const int k = k0 + ex;
+    if (k < g.nxm) phi[col_off(g, j, i) + k] = s_re[j * LDT + ex];
+  }
+}
+
 // ==========================================================================================
 // Host-side launchers
 // ==========================================================================================
@@ -1015,6 +1190,58 @@ static cudaError_t launch_k4_T(const LaunchCtx &L, void *spec, int *err) {
   return cudaErrorInvalidValue;
 }
 
+// Launch helpers for the warp-FFT kernels.  y transforms: 16 x points (8 warps) per block when
+// the tile fits in 64 KB, else 8 (4 warps); z transforms: 8 x points (8 warps).
+template <typename TS, int N1>
+static cudaError_t launch_w_n1(const LaunchCtx &L, const SubstepBuffers &b, int ns, Stage st) {
+  using C = typename Cplx<TS>::type;
+  const Geom &g = L.g;
+  C *spec = (C *)b.spec;
+  constexpr int N = 32 * N1;
+  if (st == Stage::DivFftY || st == Stage::IfftY) {
+    const bool big = (size_t)N * 17 * sizeof(TS) <= 64 * 1024;
+    const int TX = big ? 16 : 8;
+    const size_t sm = (size_t)N * (TX + 1) * sizeof(TS);
+    dim3 grid((g.nxm + TX - 1) / TX, g.nzm);
+    if (st == Stage::DivFftY) {
+      auto kern = big ? k_div_fft_y_w<N1, 16, TS> : k_div_fft_y_w<N1, 8, TS>;
+      cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+      kern<<<grid, TX * 16, sm, L.stream>>>(g, L.t, b.sc, ns, b.vx_o, b.vy_o, b.vz_o, spec, (const C *)L.twy);
+    } else {
+      auto kern = big ? k_ifft_y_w<N1, 16, TS> : k_ifft_y_w<N1, 8, TS>;
+      cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+      kern<<<grid, TX * 16, sm, L.stream>>>(g, spec, (TS *)b.phi, (const C *)L.twy);
+    }
+    return cudaGetLastError();
+  }
+  const size_t sm = (size_t)N * 8 * sizeof(C);
+  dim3 grid((g.nxm + 7) / 8, g.nyh);
+  auto kern = (st == Stage::FftZFwd) ? k_fft_z_w<N1, false, TS> : k_fft_z_w<N1, true, TS>;
+  cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  kern<<<grid, 256, sm, L.stream>>>(g, spec, (const C *)L.twz);
+  return cudaGetLastError();
+}
+
+// The warp FFT handles N = 32*{1,2,3,4,6,8,12,16,24,32}; returns false otherwise.
+template <typename TS>
+static bool launch_warp_fft(const LaunchCtx &L, const SubstepBuffers &b, int ns, Stage st, cudaError_t *err) {
+  const int N = (st == Stage::FftZFwd || st == Stage::FftZInv) ? L.g.nzm : L.g.nym;
+  if (N % 32 != 0) return false;
+  switch (N / 32) {
+    case 1: *err = launch_w_n1<TS, 1>(L, b, ns, st); return true;
+    case 2: *err = launch_w_n1<TS, 2>(L, b, ns, st); return true;
+    case 3: *err = launch_w_n1<TS, 3>(L, b, ns, st); return true;
+    case 4: *err = launch_w_n1<TS, 4>(L, b, ns, st); return true;
+    case 6: *err = launch_w_n1<TS, 6>(L, b, ns, st); return true;
+    case 8: *err = launch_w_n1<TS, 8>(L, b, ns, st); return true;
+    case 12: *err = launch_w_n1<TS, 12>(L, b, ns, st); return true;
+    case 16: *err = launch_w_n1<TS, 16>(L, b, ns, st); return true;
+    case 24: *err = launch_w_n1<TS, 24>(L, b, ns, st); return true;
+    case 32: *err = launch_w_n1<TS, 32>(L, b, ns, st); return true;
+  }
+  return false;
+}
+
 template <typename TS>
 static cudaError_t launch_stage_T(const LaunchCtx &L, const SubstepBuffers &b, int ns, Stage st) {
   using C = typename Cplx<TS>::type;
@@ -1022,6 +1249,11 @@ static cudaError_t launch_stage_T(const LaunchCtx &L, const SubstepBuffers &b, i
   C *spec = (C *)b.spec;
   const C *twy = (const C *)L.twy;
   const C *twz = (const C *)L.twz;
+  if (L.warp_fft && (st == Stage::DivFftY || st == Stage::IfftY ||
+                     ((st == Stage::FftZFwd || st == Stage::FftZInv) && g.nzm > 1))) {
+    cudaError_t e = cudaSuccess;
+    if (launch_warp_fft<TS>(L, b, ns, st, &e)) return e;
+  }
   switch (st) {
     case Stage::DivFftY: {  // K2 divergence + forward y FFT
       const int TX = L.tx_y;

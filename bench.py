@@ -46,9 +46,10 @@ WORKLOADS = {
                   name="rbc2d_256x128_fp64_ra1e8"),
 }
 
-# Algorithmic HBM bytes per cell of the fused explicit + RHS + CN kernel (FP64): read vx, vy,
-# vz, T, p, rux, ruy, ruz, rutemp and write vx, vy, vz, T, rux, ruy, ruz, rutemp = 17 x 8 B.
-K1_BYTES_PER_CELL = 136
+# Algorithmic HBM bytes per cell of the fused explicit + RHS + CN kernel: read vx, vy, vz, T, p
+# and the RK3 histories rux, ruy, ruz, rutemp, write vx, vy, vz, T and the histories.  FP64:
+# 17 x 8 B; mixed (FP32 histories): 9 x 8 + 8 x 4 B.
+K1_BYTES_PER_CELL = {0: 136, 1: 104}
 # Algorithmic HBM bytes per cell per RK3 step of the whole path (one compulsory pass per
 # operator): 3 x 328 B per substep + 24 B for CalcMaxCFL.
 STEP_BYTES_PER_CELL = 1008
@@ -97,7 +98,7 @@ class ClockSampler:
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.dev), f"--query-gpu={self.FIELDS}",
-                 "--format=csv,noheader,nounits", "-lms", "200"],
+                 "--format=csv,noheader,nounits", "-lms", "50"],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
         except Exception:
             self.proc = None
@@ -226,7 +227,7 @@ def run_gpu(args):
     k1_ms, k1_n = prof["explicit_implicit"]
     k1_avg_s = (k1_ms / k1_n) * 1e-3 if k1_n else float("nan")
     peak, peak_kind = measured_peak()
-    k1_bytes = K1_BYTES_PER_CELL * cells
+    k1_bytes = K1_BYTES_PER_CELL[w["precision"]] * cells
     achieved = k1_bytes / k1_avg_s / 1e9
     traffic = committed_traffic(w["name"])
 
@@ -359,7 +360,7 @@ def run_reference(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=30)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="afid", choices=["afid", "reference"])
     ap.add_argument("--config", default="rbc3d", choices=sorted(WORKLOADS))

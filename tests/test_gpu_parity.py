@@ -52,6 +52,10 @@ def _run_both(case, nsteps, seed=1234, random_velocity=0.0, dt=None):
     ((64, 32, 16), 10, 0.0),    # RBC from rest, 10 steps
     ((48, 64, 1), 10, 0.0),     # 2-D (nzm = 1)
     ((48, 64, 1), 3, 0.2),      # 2-D with random velocity
+    ((8, 384, 64), 2, 0.2),     # warp FFT: y N = 32*12, z N = 32*2
+    ((8, 64, 384), 2, 0.2),     # warp FFT: z N = 32*12
+    ((20, 96, 96), 2, 0.2),     # warp FFT N = 32*3 both ways
+    ((21, 128, 32), 2, 0.2),    # odd nxm: the last x pair of the y transform has one point
 ])
 def test_timemarcher_parity(shape, steps, rv):
     case = Case(*shape, rayt=1e6, dt=2e-3)
