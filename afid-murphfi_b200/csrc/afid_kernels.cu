@@ -918,26 +918,30 @@ __global__ void k_sum_partials(const double *__restrict__ partial, int nblocks, 
 // the bit-reversed per-warp writes at most 2-way bank conflicted for every supported N1.
 __device__ __forceinline__ int zsw(int r) { return (r ^ (r >> 2) ^ (r >> 6)) & 7; }
 
-// K2w: divergence + forward y r2c.  Block: TX x points (TX/2 warps) at one z index i.
-template <int N1, int TX, typename TS>
-__global__ void __launch_bounds__(TX * 16)
+// Tile of 8 complex columns per row, swizzled: element (r, c) at r*8 + (c ^ zsw(r)).
+__device__ __forceinline__ int tsw(int r, int c) { return r * 8 + (c ^ zsw(r)); }
+
+// K2w: divergence + forward y r2c.  Block: 16 x points = 8 pairs (8 warps, one pair per warp)
+// at one z index i.  The real tile is the complex tile read as (re, im) = (x point 2c, 2c+1).
+template <int N1, typename TS>
+__global__ void __launch_bounds__(256)
     k_div_fft_y_w(Geom g, Tables t, const StepCoef *__restrict__ sc_all, int ns,
                   const double *__restrict__ vx, const double *__restrict__ vy,
                   const double *__restrict__ vz, typename Cplx<TS>::type *__restrict__ spec,
                   const typename Cplx<TS>::type *__restrict__ tw) {
   using C = typename Cplx<TS>::type;
-  constexpr int N = 32 * N1, LDT = TX + 1;
+  constexpr int N = 32 * N1;
   extern __shared__ __align__(16) unsigned char smem_k2w[];
-  TS *s_re = reinterpret_cast<TS *>(smem_k2w);  // [N][TX+1] real tile
-  C *s_z = reinterpret_cast<C *>(smem_k2w);     // [TX/2][N] complex, reuses the tile
-  const int k0 = blockIdx.x * TX, i = blockIdx.y;
+  C *T = reinterpret_cast<C *>(smem_k2w);  // [N][8] swizzled
+  TS *Tr = reinterpret_cast<TS *>(smem_k2w);
+  const int k0 = blockIdx.x * 16, i = blockIdx.y;
   const int ip = wrap_inc(i, g.nzm);
   const StepCoef sc = sc_all[ns];
   const double usdtal = 1.0 / (sc.dt * sc.al);
-  const int tx = threadIdx.x % TX, k = k0 + tx;
+  const int tx = threadIdx.x & 15, k = k0 + tx;
   const double ux = (k < g.nxm) ? __ldg(t.udx3m + k) : 0.0;
 #pragma unroll 4
-  for (int j = threadIdx.x / TX; j < N; j += blockDim.x / TX) {
+  for (int j = threadIdx.x >> 4; j < N; j += 16) {
     double dv = 0.0;
     if (k < g.nxm) {
       const int jp = wrap_inc(j, N);
@@ -947,31 +951,28 @@ __global__ void __launch_bounds__(TX * 16)
                            (__ldg(vx + c + k + 1) - __ldg(vx + c + k)) * ux;
       dv = dqcap * usdtal;
     }
-    s_re[j * LDT + tx] = (TS)dv;
+    Tr[2 * tsw(j, tx >> 1) + (tx & 1)] = (TS)dv;
   }
   __syncthreads();
   const int lane = threadIdx.x & 31, p = threadIdx.x >> 5;
   C x[N1];
 #pragma unroll
-  for (int m = 0; m < N1; ++m) {
-    x[m].x = s_re[(lane + 32 * m) * LDT + 2 * p];
-    x[m].y = s_re[(lane + 32 * m) * LDT + 2 * p + 1];
-  }
+  for (int m = 0; m < N1; ++m) x[m] = T[tsw(lane + 32 * m, p)];
   warp_fft<false, TS, N1>(x, lane, tw);
   __syncthreads();
   const int rl = bitrev5(lane);
 #pragma unroll
-  for (int k1 = 0; k1 < N1; ++k1) s_z[p * N + k1 + N1 * rl] = x[k1];
+  for (int k1 = 0; k1 < N1; ++k1) T[tsw(k1 + N1 * rl, p)] = x[k1];
   __syncthreads();
   const TS norm = (TS)(1.0 / ((double)g.nzm * (double)g.nym));
   const TS half = (TS)0.5;
-  for (int e = threadIdx.x; e < g.nyh * TX; e += blockDim.x) {
-    const int ex = e % TX, ky = e / TX;
+  for (int e = threadIdx.x; e < g.nyh * 16; e += blockDim.x) {
+    const int ex = e & 15, ky = e >> 4;
     const int kk = k0 + ex;
     if (kk >= g.nxm) continue;
     const int q = ex >> 1;
-    const C zk = s_z[q * N + ky];
-    const C zn = s_z[q * N + (ky == 0 ? 0 : N - ky)];
+    const C zk = T[tsw(ky, q)];
+    const C zn = T[tsw(ky == 0 ? 0 : N - ky, q)];
     C X;
     if ((ex & 1) == 0) {
       X.x = (zk.x + zn.x) * half;
@@ -1032,20 +1033,20 @@ __global__ void __launch_bounds__(256)
   }
 }
 
-// K6w: backward y c2r.  Block: TX x points (TX/2 warps) at one z index i.
-template <int N1, int TX, typename TS>
-__global__ void __launch_bounds__(TX * 16)
+// K6w: backward y c2r.  Block: 16 x points = 8 pairs (8 warps) at one z index i.
+template <int N1, typename TS>
+__global__ void __launch_bounds__(256)
     k_ifft_y_w(Geom g, const typename Cplx<TS>::type *__restrict__ spec, TS *__restrict__ phi,
                const typename Cplx<TS>::type *__restrict__ tw) {
   using C = typename Cplx<TS>::type;
-  constexpr int N = 32 * N1, LDT = TX + 1, B = TX / 2;
+  constexpr int N = 32 * N1;
   extern __shared__ __align__(16) unsigned char smem_k6w[];
-  C *s_z = reinterpret_cast<C *>(smem_k6w);     // [B][N]
-  TS *s_re = reinterpret_cast<TS *>(smem_k6w);  // [N][TX+1], reuses the buffer
-  const int k0 = blockIdx.x * TX, i = blockIdx.y;
+  C *T = reinterpret_cast<C *>(smem_k6w);  // [N][8] swizzled
+  const TS *Tr = reinterpret_cast<const TS *>(smem_k6w);
+  const int k0 = blockIdx.x * 16, i = blockIdx.y;
 #pragma unroll 4
-  for (int e = threadIdx.x; e < N * B; e += blockDim.x) {
-    const int p = e % B, j = e / B;
+  for (int e = threadIdx.x; e < N * 8; e += blockDim.x) {
+    const int p = e & 7, j = e >> 3;
     const bool cj = (2 * j > N);
     const int jj = cj ? N - j : j;
     const int ka = k0 + 2 * p, kb = ka + 1;
@@ -1059,27 +1060,24 @@ __global__ void __launch_bounds__(TX * 16)
     C Z;
     Z.x = X.x - Y.y;
     Z.y = X.y + Y.x;
-    s_z[p * N + j] = Z;
+    T[tsw(j, p)] = Z;
   }
   __syncthreads();
   const int lane = threadIdx.x & 31, p = threadIdx.x >> 5;
   C x[N1];
 #pragma unroll
-  for (int m = 0; m < N1; ++m) x[m] = s_z[p * N + lane + 32 * m];
+  for (int m = 0; m < N1; ++m) x[m] = T[tsw(lane + 32 * m, p)];
   warp_fft<true, TS, N1>(x, lane, tw);
   __syncthreads();
   const int rl = bitrev5(lane);
 #pragma unroll
-  for (int k1 = 0; k1 < N1; ++k1) {
-    s_re[(k1 + N1 * rl) * LDT + 2 * p] = x[k1].x;
-    s_re[(k1 + N1 * rl) * LDT + 2 * p + 1] = x[k1].y;
-  }
+  for (int k1 = 0; k1 < N1; ++k1) T[tsw(k1 + N1 * rl, p)] = x[k1];
   __syncthreads();
 #pragma unroll 4
-  for (int e = threadIdx.x; e < N * TX; e += blockDim.x) {
-    const int ex = e % TX, j = e / TX;
+  for (int e = threadIdx.x; e < N * 16; e += blockDim.x) {
+    const int ex = e & 15, j = e >> 4;
     const int k = k0 + ex;
-    if (k < g.nxm) phi[col_off(g, j, i) + k] = s_re[j * LDT + ex];
+    if (k < g.nxm) phi[col_off(g, j, i) + k] = Tr[2 * tsw(j, ex >> 1) + (ex & 1)];
   }
 }
 
@@ -1190,8 +1188,8 @@ static cudaError_t launch_k4_T(const LaunchCtx &L, void *spec, int *err) {
   return cudaErrorInvalidValue;
 }
 
-// Launch helpers for the warp-FFT kernels.  y transforms: 16 x points (8 warps) per block when
-// the tile fits in 64 KB, else 8 (4 warps); z transforms: 8 x points (8 warps).
+// Launch helpers for the warp-FFT kernels: 8 warps per block, a [N][8] complex tile each
+// (y transforms: 16 x points as 8 pairs; z transforms: 8 x points).
 template <typename TS, int N1>
 static cudaError_t launch_w_n1(const LaunchCtx &L, const SubstepBuffers &b, int ns, Stage st) {
   using C = typename Cplx<TS>::type;
@@ -1199,18 +1197,16 @@ static cudaError_t launch_w_n1(const LaunchCtx &L, const SubstepBuffers &b, int 
   C *spec = (C *)b.spec;
   constexpr int N = 32 * N1;
   if (st == Stage::DivFftY || st == Stage::IfftY) {
-    const bool big = (size_t)N * 17 * sizeof(TS) <= 64 * 1024;
-    const int TX = big ? 16 : 8;
-    const size_t sm = (size_t)N * (TX + 1) * sizeof(TS);
-    dim3 grid((g.nxm + TX - 1) / TX, g.nzm);
+    const size_t sm = (size_t)N * 8 * sizeof(C);
+    dim3 grid((g.nxm + 15) / 16, g.nzm);
     if (st == Stage::DivFftY) {
-      auto kern = big ? k_div_fft_y_w<N1, 16, TS> : k_div_fft_y_w<N1, 8, TS>;
+      auto kern = k_div_fft_y_w<N1, TS>;
       cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-      kern<<<grid, TX * 16, sm, L.stream>>>(g, L.t, b.sc, ns, b.vx_o, b.vy_o, b.vz_o, spec, (const C *)L.twy);
+      kern<<<grid, 256, sm, L.stream>>>(g, L.t, b.sc, ns, b.vx_o, b.vy_o, b.vz_o, spec, (const C *)L.twy);
     } else {
-      auto kern = big ? k_ifft_y_w<N1, 16, TS> : k_ifft_y_w<N1, 8, TS>;
+      auto kern = k_ifft_y_w<N1, TS>;
       cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-      kern<<<grid, TX * 16, sm, L.stream>>>(g, spec, (TS *)b.phi, (const C *)L.twy);
+      kern<<<grid, 256, sm, L.stream>>>(g, spec, (TS *)b.phi, (const C *)L.twy);
     }
     return cudaGetLastError();
   }
