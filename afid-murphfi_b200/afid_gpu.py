@@ -80,7 +80,12 @@ class RunStatsT(C.Structure):
                 ("nu_vol", C.c_double), ("ke", C.c_double), ("seconds", C.c_double)]
 
 
-# Every symbol declared in include/afid_gpu.h and include/afid_host.h
+class BatchStatT(C.Structure):
+    _fields_ = [("ntime", C.c_int), ("errorcode", C.c_int), ("time", C.c_double),
+                ("dt", C.c_double), ("cfl", C.c_double)]
+
+
+# Every symbol declared in include/afid_gpu.h, include/afid_host.h and include/afid_batch.h
 EXPORTS = [
     "afid_gpu_create", "afid_gpu_destroy", "afid_gpu_set_stream", "afid_gpu_get_stream",
     "afid_gpu_synchronize", "afid_gpu_upload", "afid_gpu_download", "afid_gpu_timemarcher",
@@ -91,6 +96,10 @@ EXPORTS = [
     "afid_parse_bou_in", "afid_read_bou_in", "afid_tables_create", "afid_tables_destroy",
     "afid_tables_grid", "afid_tables_params", "afid_tables_array", "afid_philox_uniform",
     "afid_initial_temperature", "afid_next_dt", "afid_run",
+    "afid_batch_create", "afid_batch_destroy", "afid_batch_set_stream", "afid_batch_configure",
+    "afid_batch_seed", "afid_batch_upload", "afid_batch_download", "afid_batch_set_active",
+    "afid_batch_step", "afid_batch_synchronize", "afid_batch_stats", "afid_batch_num_slots",
+    "afid_batch_device_bytes", "afid_batch_launch_count",
 ]
 
 
@@ -132,6 +141,20 @@ def load_library(path: str = _LIB_PATH) -> C.CDLL:
         "afid_initial_temperature": (i, [vp, C.c_uint64, d, _dp, i, i]),
         "afid_next_dt": (i, [C.POINTER(InputT), i, _dp, d, _dp]),
         "afid_run": (i, [C.POINTER(InputT), i, C.c_uint64, i, i, vp, vp, C.POINTER(RunStatsT)]),
+        "afid_batch_create": (i, [C.POINTER(InputT), i, i, C.POINTER(vp)]),
+        "afid_batch_destroy": (i, [vp]),
+        "afid_batch_set_stream": (i, [vp, vp]),
+        "afid_batch_configure": (i, [vp, i, C.POINTER(InputT)]),
+        "afid_batch_seed": (i, [vp, i, C.c_uint64]),
+        "afid_batch_upload": (i, [vp, i, _dp, _dp, _dp, _dp, _dp, i, i]),
+        "afid_batch_download": (i, [vp, i, _dp, _dp, _dp, _dp, _dp, i, i]),
+        "afid_batch_set_active": (i, [vp, C.POINTER(C.c_ubyte)]),
+        "afid_batch_step": (i, [vp, i]),
+        "afid_batch_synchronize": (i, [vp]),
+        "afid_batch_stats": (i, [vp, C.POINTER(BatchStatT), _dp, _dp]),
+        "afid_batch_num_slots": (i, [vp]),
+        "afid_batch_device_bytes": (C.c_longlong, [vp]),
+        "afid_batch_launch_count": (C.c_longlong, [vp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -308,6 +331,94 @@ class Solver:
     def close(self):
         if self._h:
             lib().afid_gpu_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Batch:
+    """Independent 2-D instances of one size class advanced together (include/afid_batch.h).
+
+    Slot state crosses the boundary as numpy (nym, nx) arrays, x fastest.  Each slot carries
+    its own bou.in (Ra, Pr, YLEN, dt rule); ``step`` runs the reference's main-loop step
+    (CFL, dt rule, TimeMarcher) for every active slot.
+    """
+
+    FIELDS = ("vx", "vy", "vz", "temp", "pr")
+
+    def __init__(self, proto: InputT, nslots: int, precision: int = PREC_FP64):
+        self.nxm, self.nym, self.nslots = proto.nxm, proto.nym, nslots
+        self.nx = self.nxm + 1
+        self._h = C.c_void_p()
+        _check(lib().afid_batch_create(C.byref(proto), nslots, precision, C.byref(self._h)),
+               "afid_batch_create")
+
+    @property
+    def shape(self):
+        return (self.nym, self.nx)
+
+    def configure(self, slot: int, inp: InputT) -> None:
+        _check(lib().afid_batch_configure(self._h, slot, C.byref(inp)), "afid_batch_configure")
+
+    def seed(self, slot: int, seed: int) -> None:
+        _check(lib().afid_batch_seed(self._h, slot, seed), "afid_batch_seed")
+
+    def upload(self, slot: int, vx=None, vy=None, vz=None, temp=None, pr=None) -> None:
+        arrs = [None if a is None else np.ascontiguousarray(a, dtype=np.float64).reshape(self.shape)
+                for a in (vx, vy, vz, temp, pr)]
+        ptrs = [(_ptr(a) if a is not None else None) for a in arrs]
+        _check(lib().afid_batch_upload(self._h, slot, *ptrs, self.nx, self.nym), "afid_batch_upload")
+
+    def download(self, slot: int) -> dict:
+        out = {f: np.zeros(self.shape) for f in self.FIELDS}
+        _check(lib().afid_batch_download(self._h, slot, *(_ptr(out[f]) for f in self.FIELDS),
+                                         self.nx, self.nym), "afid_batch_download")
+        return out
+
+    def set_active(self, active) -> None:
+        a = np.ascontiguousarray(np.asarray(active, dtype=np.uint8).reshape(self.nslots))
+        _check(lib().afid_batch_set_active(self._h, a.ctypes.data_as(C.POINTER(C.c_ubyte))),
+               "afid_batch_set_active")
+
+    def step(self, nsteps: int = 1) -> None:
+        _check(lib().afid_batch_step(self._h, nsteps), "afid_batch_step")
+
+    def synchronize(self) -> None:
+        _check(lib().afid_batch_synchronize(self._h), "afid_batch_synchronize")
+
+    def set_stream(self, stream_handle: int | None) -> None:
+        _check(lib().afid_batch_set_stream(self._h, stream_handle), "afid_batch_set_stream")
+
+    def stats(self, globals_: bool = True) -> dict:
+        st = (BatchStatT * self.nslots)()
+        nu = np.zeros(self.nslots)
+        ke = np.zeros(self.nslots)
+        _check(lib().afid_batch_stats(self._h, st, _ptr(nu) if globals_ else None,
+                                      _ptr(ke) if globals_ else None), "afid_batch_stats")
+        out = {k: np.array([getattr(x, k) for x in st]) for k in ("ntime", "errorcode", "time", "dt", "cfl")}
+        if globals_:
+            out["nu_vol"], out["ke"] = nu, ke
+        return out
+
+    def device_bytes(self) -> int:
+        return int(lib().afid_batch_device_bytes(self._h))
+
+    def launch_count(self) -> int:
+        return int(lib().afid_batch_launch_count(self._h))
+
+    def close(self):
+        if self._h:
+            lib().afid_batch_destroy(self._h)
             self._h = C.c_void_p()
 
     def __enter__(self):

@@ -14,37 +14,6 @@
 
 using namespace afid;
 
-struct afid_ctx {
-  int dev = 0;
-  cudaStream_t own_stream = nullptr;
-  cudaStream_t stream = nullptr;
-  cudaError_t last_cuda = cudaSuccess;
-  long long launches = 0;
-  int nsst = 3;
-  double alx3 = 1.0;
-  LaunchCtx L{};
-  // device allocations
-  std::vector<void *> allocs;
-  double *vx = nullptr, *vy = nullptr, *vz = nullptr, *temp = nullptr, *pr = nullptr;
-  double *vx_o = nullptr, *vy_o = nullptr, *vz_o = nullptr, *temp_o = nullptr;
-  void *rux = nullptr, *ruy = nullptr, *ruz = nullptr, *rut = nullptr;
-  void *spec = nullptr, *phi = nullptr;
-  double *cn_tab = nullptr;
-  StepCoef *sc = nullptr;
-  int *err = nullptr;
-  unsigned long long *red = nullptr;
-  double *partial = nullptr, *gsum = nullptr;
-  double *host_scratch = nullptr;  // pinned, 8 doubles
-  // device tables for the CN builder
-  const double *am[3], *ac[3], *ap[3];
-  size_t field_elems = 0;
-  // optional per-kernel event timing
-  bool prof = false;
-  std::vector<cudaEvent_t> ev_pool;
-  size_t ev_used = 0;
-  struct Rec { int cls; size_t a, b; };
-  std::vector<Rec> recs;
-};
 
 namespace {
 
@@ -91,6 +60,7 @@ cudaError_t dalloc(afid_ctx_t *ctx, T **p, size_t count) {
   cudaError_t e = cudaMalloc(&q, std::max<size_t>(count, 1) * sizeof(T));
   if (e != cudaSuccess) return e;
   ctx->allocs.push_back(q);
+  ctx->dev_bytes += (long long)(std::max<size_t>(count, 1) * sizeof(T));
   *p = static_cast<T *>(q);
   return cudaMemset(q, 0, std::max<size_t>(count, 1) * sizeof(T));
 }
@@ -218,7 +188,7 @@ int run_substep(afid_ctx_t *ctx, int ns) {
   SubstepBuffers b = buffers(ctx);
   for (int st = 0; st < kNumStages; ++st) {
     const Stage stage = static_cast<Stage>(st);
-    if (ctx->L.g.nzm == 1 && (stage == Stage::FftZFwd || stage == Stage::FftZInv)) continue;
+    if ((ctx->L.g.nzm == 1 || ctx->L.g.batch) && (stage == Stage::FftZFwd || stage == Stage::FftZInv)) continue;
     AFID_CUDA(ctx, timed(ctx, 1 + st, [&] { return launch_stage(ctx->L, b, ns, stage); }));
     ctx->launches += 1;
   }
@@ -260,6 +230,14 @@ const char *afid_gpu_status_string(int s) {
 }
 
 int afid_gpu_create(const afid_grid_t *grid, const afid_params_t *prm, afid_ctx_t **out) {
+  return ctx_create(grid, prm, nullptr, out);
+}
+
+}  // extern "C"
+
+namespace afid {
+
+int ctx_create(const afid_grid_t *grid, const afid_params_t *prm, const BatchSpec *bs, afid_ctx_t **out) {
   if (!grid || !prm || !out) return AFID_E_INVALID;
   *out = nullptr;
   const int nxm = grid->nxm, nym = grid->nym, nzm = grid->nzm;
@@ -269,8 +247,15 @@ int afid_gpu_create(const afid_grid_t *grid, const afid_params_t *prm, afid_ctx_
   if (prm->precision != AFID_PREC_FP64 && prm->precision != AFID_PREC_MIXED) return AFID_E_INVALID;
   const int M = cn_choose_M(nxm);
   if (M < 0) return AFID_E_INVALID;
+  if (bs && (bs->ninst != nzm || !bs->inst || !bs->ak2)) return AFID_E_INVALID;
   FftPlan py, pz;
-  if (!make_plan(nym, &py) || !make_plan(nzm, &pz)) return AFID_E_FFTSIZE;
+  if (!make_plan(nym, &py)) return AFID_E_FFTSIZE;
+  if (bs) {
+    pz.n = 1;  // instances do not couple along z: no z transform
+    pz.npass = 0;
+  } else if (!make_plan(nzm, &pz)) {
+    return AFID_E_FFTSIZE;
+  }
 
   afid_ctx_t *ctx = new (std::nothrow) afid_ctx_t();
   if (!ctx) return AFID_E_ALLOC;
@@ -342,8 +327,9 @@ int afid_gpu_create(const afid_grid_t *grid, const afid_params_t *prm, afid_ctx_
   unsigned char *sp = nullptr;
   chk(dalloc(ctx, &sp, nspec * 2 * tsz));
   ctx->spec = sp;
-  chk(dalloc(ctx, &ctx->cn_tab, cn_tab_doubles(M, 3)));
-  chk(dalloc(ctx, &ctx->sc, 3));
+  const size_t nsets = bs ? (size_t)bs->ninst : 1;  // batch mode: one table set per instance
+  chk(dalloc(ctx, &ctx->cn_tab, cn_tab_doubles(M, 3) * nsets));
+  chk(dalloc(ctx, &ctx->sc, 3 * nsets));
   chk(dalloc(ctx, &ctx->err, 1));
   chk(dalloc(ctx, &ctx->red, 1));
   const int nb = globals_partial_blocks(g);
@@ -369,11 +355,13 @@ int afid_gpu_create(const afid_grid_t *grid, const afid_params_t *prm, afid_ctx_
   size_t o_ap3ssk = put(grid->ap3ssk, nxm, L1), o_ac3ssk = put(grid->ac3ssk, nxm, L1),
          o_am3ssk = put(grid->am3ssk, nxm, L1);
   size_t o_amphk = put(grid->amphk, nxm, L1), o_acphk = put(grid->acphk, nxm, L1), o_apphk = put(grid->apphk, nxm, L1);
-  size_t o_ak1 = put(grid->ak1, nzm, nzm), o_ak2 = put(grid->ak2, nym, nym);
+  size_t o_ak1 = bs ? put(nullptr, 0, nzm) : put(grid->ak1, nzm, nzm);
+  size_t o_ak2 = bs ? put(bs->ak2, nym * nzm, nym * nzm) : put(grid->ak2, nym, nym);
   size_t o_g3rc = put(grid->g3rc, nx, L1);
   std::vector<double> tbp((size_t)nym * nzm, 0.5), ttp((size_t)nym * nzm, -0.5);
-  if (prm->tempbp) std::memcpy(tbp.data(), prm->tempbp, tbp.size() * sizeof(double));
-  if (prm->temptp) std::memcpy(ttp.data(), prm->temptp, ttp.size() * sizeof(double));
+  const double *src_bp = bs ? bs->tempbp : prm->tempbp, *src_tp = bs ? bs->temptp : prm->temptp;
+  if (src_bp) std::memcpy(tbp.data(), src_bp, tbp.size() * sizeof(double));
+  if (src_tp) std::memcpy(ttp.data(), src_tp, ttp.size() * sizeof(double));
   size_t o_tbp = put(tbp.data(), (int)tbp.size(), (int)tbp.size());
   size_t o_ttp = put(ttp.data(), (int)ttp.size(), (int)ttp.size());
   double *dtab = nullptr;
@@ -445,9 +433,25 @@ int afid_gpu_create(const afid_grid_t *grid, const afid_params_t *prm, afid_ctx_
   while (L.tx_y > 2 && (size_t)L.tx_y * nym * csz > smem_cap) L.tx_y /= 2;
   L.tx_z = 8;
   while (L.tx_z > 2 && (size_t)2 * L.tx_z * nzm * csz > smem_cap) L.tx_z /= 2;
-  if ((size_t)L.tx_y * nym * csz > 200 * 1024 || (size_t)2 * L.tx_z * nzm * csz > 200 * 1024) {
+  if ((size_t)L.tx_y * nym * csz > 200 * 1024 || (!bs && (size_t)2 * L.tx_z * nzm * csz > 200 * 1024)) {
     afid_gpu_destroy(ctx);
     return AFID_E_INVALID;
+  }
+  if (bs) {
+    ctx->ninst = bs->ninst;
+    cudaError_t eb = dalloc(ctx, &ctx->inst_dev, (size_t)bs->ninst);
+    if (eb == cudaSuccess)
+      eb = cudaMemcpy(ctx->inst_dev, bs->inst, sizeof(InstScal) * bs->ninst, cudaMemcpyHostToDevice);
+    if (eb == cudaSuccess) eb = dalloc(ctx, &ctx->active_dev, (size_t)bs->ninst);
+    if (eb == cudaSuccess) eb = cudaMemset(ctx->active_dev, 1, bs->ninst);
+    if (eb != cudaSuccess) {
+      ctx->last_cuda = eb;
+      afid_gpu_destroy(ctx);
+      return eb == cudaErrorMemoryAllocation ? AFID_E_ALLOC : AFID_E_CUDA;
+    }
+    L.g.batch = 1;
+    L.g.inst = ctx->inst_dev;
+    L.g.active = ctx->active_dev;
   }
   L.warp_fft = true;
   L.plan_y = py;
@@ -457,6 +461,54 @@ int afid_gpu_create(const afid_grid_t *grid, const afid_params_t *prm, afid_ctx_
   *out = ctx;
   return AFID_OK;
 }
+
+SubstepBuffers ctx_buffers(afid_ctx_t *ctx) { return buffers(ctx); }
+int ctx_run_substep(afid_ctx_t *ctx, int ns) { return run_substep(ctx, ns); }
+int ctx_fail(afid_ctx_t *ctx, cudaError_t e) { return fail_cuda(ctx, e); }
+
+// CN tables and RK3 coefficients of all substeps for every instance of a batch, dt from the device.
+int ctx_build_cn_batch(afid_ctx_t *ctx, const double *dt_dev) {
+  const Geom &g = ctx->L.g;
+  CnInputs in;
+  for (int m = 0; m < 3; ++m) {
+    in.am[m] = ctx->am[m];
+    in.ac[m] = ctx->ac[m];
+    in.ap[m] = ctx->ap[m];
+  }
+  in.off[0] = 1;
+  in.n[0] = g.nxm - 1;
+  in.off[1] = 0;
+  in.n[1] = g.nxm;
+  in.off[2] = 0;
+  in.n[2] = g.nxm;
+  double gam[3], rom[3], alm[3];
+  rk3(ctx->nsst, gam, rom, alm);
+  for (int s2 = 0; s2 < 3; ++s2) {
+    in.al[s2] = alm[s2];
+    in.ga[s2] = gam[s2];
+    in.ro[s2] = rom[s2];
+  }
+  in.dt = 0.0;
+  in.beta = 0.0;
+  in.pect = g.pect;
+  in.ren = g.ren;
+  in.ns0 = 0;
+  in.nsub = ctx->nsst;
+  in.M = ctx->L.M;
+  in.tab = ctx->cn_tab;
+  in.sc = ctx->sc;
+  in.dt_dev = dt_dev;
+  in.inst = ctx->inst_dev;
+  in.active = ctx->active_dev;
+  in.ninst = ctx->ninst;
+  AFID_CUDA(ctx, timed(ctx, 0, [&] { return launch_cn_tables(ctx->L, in); }));
+  ctx->launches += 1;
+  return AFID_OK;
+}
+
+}  // namespace afid
+
+extern "C" {
 
 int afid_gpu_destroy(afid_ctx_t *ctx) {
   if (!ctx) return AFID_OK;

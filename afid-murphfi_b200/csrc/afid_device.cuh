@@ -27,6 +27,17 @@ struct Geom {
   double udyq_re, udzq_re, udyq_pe, udzq_pe;  // dyq/ren, dzq/ren, dyq/pect, dzq/pect
   double xplusu, xminusu;
   int active_t, gaxis, inslws, inslwn, tfixs, tfixn;
+  // Batch mode (batch != 0): the z index numbers independent 2-D instances of one size class;
+  // they do not couple along z and each has its own scalars, RK3 coefficients, CN tables,
+  // wavenumbers and an active flag.
+  int batch;
+  const struct InstScal *inst;   // [nzm] per-instance scalars (batch mode), else nullptr
+  const unsigned char *active;   // [nzm] 1 = advance this instance (batch mode), else nullptr
+};
+
+// Scalars that differ between the instances of a batch (aspect ratio, Ra, Pr).
+struct InstScal {
+  double dy, dyq, ren, pect, rren, rpect, udyq_re, udyq_pe;
 };
 
 // Device-resident per-substep scalars (written by the coefficient kernel, read by every
@@ -56,6 +67,29 @@ struct FftPlan {
 
 __device__ __forceinline__ int wrap_inc(int a, int n) { return (a + 1 == n) ? 0 : a + 1; }
 __device__ __forceinline__ int wrap_dec(int a, int n) { return (a == 0) ? n - 1 : a - 1; }
+
+// z neighbours: periodic for one domain, the instance itself in batch mode (2-D instances).
+__device__ __forceinline__ int zinc(const Geom &g, int i) { return g.batch ? i : wrap_inc(i, g.nzm); }
+__device__ __forceinline__ int zdec(const Geom &g, int i) { return g.batch ? i : wrap_dec(i, g.nzm); }
+__device__ __forceinline__ bool inst_active(const Geom &g, int i) { return !g.active || g.active[i] != 0; }
+// Load the scalars of instance i into a block-local copy of the geometry (batch mode).
+__device__ __forceinline__ void bind_instance(Geom &g, int i) {
+  if (g.inst) {
+    const InstScal s = g.inst[i];
+    g.dy = s.dy;
+    g.dyq = s.dyq;
+    g.ren = s.ren;
+    g.pect = s.pect;
+    g.rren = s.rren;
+    g.rpect = s.rpect;
+    g.udyq_re = s.udyq_re;
+    g.udyq_pe = s.udyq_pe;
+  }
+}
+// Index of the RK3 coefficients of substep ns (per instance in batch mode).
+__device__ __forceinline__ int sc_slot(const Geom &g, int i, int ns) { return (g.batch ? 3 * i : 0) + ns; }
+// z extent that the FFT normalisation 1/(nym*nzm) uses.
+__device__ __forceinline__ double nz_norm(const Geom &g) { return g.batch ? 1.0 : (double)g.nzm; }
 
 __device__ __forceinline__ size_t col_off(const Geom &g, int j, int i) {
   return (size_t)(j + (size_t)g.nym * i) * (size_t)g.ldx;

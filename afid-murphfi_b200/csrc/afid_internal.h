@@ -2,6 +2,8 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <vector>
+
 #include "afid_device.cuh"
 
 namespace afid {
@@ -41,6 +43,11 @@ struct CnInputs {
   int ns0, nsub, M;
   double *tab;
   StepCoef *sc;
+  // batch mode (else nullptr / 0): per-instance dt on the device, scalars, active flags
+  const double *dt_dev = nullptr;
+  const InstScal *inst = nullptr;
+  const unsigned char *active = nullptr;
+  int ninst = 0;
 };
 
 int cn_choose_M(int nxm);
@@ -58,3 +65,63 @@ cudaError_t launch_globals(const LaunchCtx &L, const double *vx, const double *v
 int globals_partial_blocks(const Geom &g);
 
 }  // namespace afid
+
+#include "afid_gpu.h"
+
+// The context behind afid_ctx_t (include/afid_gpu.h).
+struct afid_ctx {
+  int dev = 0;
+  cudaStream_t own_stream = nullptr;
+  cudaStream_t stream = nullptr;
+  cudaError_t last_cuda = cudaSuccess;
+  long long launches = 0;
+  int nsst = 3;
+  double alx3 = 1.0;
+  afid::LaunchCtx L{};
+  // device allocations
+  std::vector<void *> allocs;
+  long long dev_bytes = 0;  // sum of the allocations above
+  double *vx = nullptr, *vy = nullptr, *vz = nullptr, *temp = nullptr, *pr = nullptr;
+  double *vx_o = nullptr, *vy_o = nullptr, *vz_o = nullptr, *temp_o = nullptr;
+  void *rux = nullptr, *ruy = nullptr, *ruz = nullptr, *rut = nullptr;
+  void *spec = nullptr, *phi = nullptr;
+  double *cn_tab = nullptr;
+  afid::StepCoef *sc = nullptr;
+  int *err = nullptr;
+  unsigned long long *red = nullptr;
+  double *partial = nullptr, *gsum = nullptr;
+  double *host_scratch = nullptr;  // pinned, 8 doubles
+  // device tables for the CN builder
+  const double *am[3], *ac[3], *ap[3];
+  size_t field_elems = 0;
+  // optional per-kernel event timing
+  bool prof = false;
+  std::vector<cudaEvent_t> ev_pool;
+  size_t ev_used = 0;
+  struct Rec { int cls; size_t a, b; };
+  std::vector<Rec> recs;
+  // batch mode: instance scalars and active flags on the device (see afid::BatchSpec)
+  int ninst = 0;
+  afid::InstScal *inst_dev = nullptr;
+  unsigned char *active_dev = nullptr;
+};
+
+namespace afid {
+
+// A batch of independent 2-D instances of one size class, stacked along z (Geom::batch).
+struct BatchSpec {
+  int ninst;
+  const InstScal *inst;   // [ninst] host
+  const double *ak2;      // [ninst * nym] host, per-instance modified wavenumbers in y
+  const double *tempbp;   // [ninst * nym] host plate values
+  const double *temptp;
+};
+
+int ctx_create(const afid_grid_t *grid, const afid_params_t *prm, const BatchSpec *bs, afid_ctx_t **out);
+SubstepBuffers ctx_buffers(afid_ctx_t *ctx);
+int ctx_run_substep(afid_ctx_t *ctx, int ns);
+int ctx_build_cn_batch(afid_ctx_t *ctx, const double *dt_dev);
+int ctx_fail(afid_ctx_t *ctx, cudaError_t e);
+
+}  // namespace afid
+

@@ -50,29 +50,45 @@ struct CnBuildArgs {
   double al[3], ga[3], ro[3];
   double dt, beta, pect, ren;
   int ns0, nsub;       // substeps ns0 .. ns0+nsub-1 are built
+  // batch mode: one table set per instance, dt from dt_dev[instance] (beta = dt/ren/2),
+  // ren/pect from inst[instance]; idle instances are skipped
+  const double *dt_dev;
+  const InstScal *inst;
+  const unsigned char *active;
 };
 
 __global__ void k_cn_tables(CnBuildArgs args, int M, double *__restrict__ tab,
                             StepCoef *__restrict__ sc) {
   const int lane = threadIdx.x;
   const int m = blockIdx.x % 3;
-  const int sub = blockIdx.x / 3;
+  const int sub = (blockIdx.x / 3) % args.nsub;
+  const int b = blockIdx.x / (3 * args.nsub);  // instance (batch mode), else 0
   const int ns = args.ns0 + sub;
   const double al = args.al[sub];
+  double dt = args.dt, beta = args.beta, ren = args.ren, pect = args.pect;
+  int slot = ns;
+  if (args.dt_dev) {
+    if (args.active && !args.active[b]) return;
+    dt = args.dt_dev[b];
+    ren = args.inst[b].ren;
+    pect = args.inst[b].pect;
+    beta = dt / ren * 0.5;  // TimeMarcher.F90:28
+    slot = 3 * b + ns;
+  }
   if (m == 0 && lane == 0) {
     StepCoef c;
     c.al = al;
     c.ga = args.ga[sub];
     c.ro = args.ro[sub];
-    c.dt = args.dt;
-    c.beta = args.beta;
-    c.alre = al / args.ren;
-    c.alpec = al / args.pect;
-    sc[ns] = c;
+    c.dt = dt;
+    c.beta = beta;
+    c.alre = al / ren;
+    c.alpec = al / pect;
+    sc[slot] = c;
   }
   const CnMatrixDesc d = args.mat[m];
-  const double betadx = d.temperature ? 0.5 * al * args.dt / args.pect : args.beta * al;
-  double *T = tab + (size_t)(ns * 3 + m) * cn_table_size(M);
+  const double betadx = d.temperature ? 0.5 * al * dt / pect : beta * al;
+  double *T = tab + (size_t)(slot * 3 + m) * cn_table_size(M);
   double *Tsc = T, *Ta = T + 32 * M, *Tinv = T + 64 * M, *Tcp = T + 96 * M, *Tv = T + 128 * M,
          *Tw = T + 160 * M, *Tl = T + 192 * M;
   const int n = d.n;
@@ -368,7 +384,7 @@ __host__ __device__ inline size_t k1_stage_bytes(int ldx, size_t te_size) {
 // the increments to the staged centre values and stores the intermediate fields.
 template <int M, int TPC, int RPT, typename TE>
 __global__ void __launch_bounds__(TPC)
-    k_explicit_implicit(Geom g, Tables t, const StepCoef *__restrict__ sc_all, int ns,
+    k_explicit_implicit(Geom g0, Tables t, const StepCoef *__restrict__ sc_all, int ns,
                         const double *__restrict__ cn_tab, const double *__restrict__ vx,
                         const double *__restrict__ vy, const double *__restrict__ vz,
                         const double *__restrict__ temp, const double *__restrict__ pr,
@@ -379,6 +395,7 @@ __global__ void __launch_bounds__(TPC)
   constexpr int FLD = LD * M;
   extern __shared__ __align__(128) unsigned char smem_k1[];
   __shared__ uint64_t bar;
+  Geom g = g0;
   const int ldx = g.ldx;
   double *cols = reinterpret_cast<double *>(smem_k1);
   TE *rcols = reinterpret_cast<TE *>(cols + (size_t)kK1StateCols * ldx);
@@ -386,8 +403,15 @@ __global__ void __launch_bounds__(TPC)
   const int tc = threadIdx.x;
   const int colid = blockIdx.x;
   const int j = colid % g.nym, i = colid / g.nym;
+  if (!inst_active(g, i)) {
+    // An idle batch slot keeps its state: the temperature moves buffers every substep.
+    const size_t c = col_off(g, j, i);
+    for (int k = tc; k < g.nx; k += TPC) temp_o[c + k] = temp[c + k];
+    return;
+  }
+  bind_instance(g, i);
   const int jp = wrap_inc(j, g.nym), jm = wrap_dec(j, g.nym);
-  const int ip = wrap_inc(i, g.nzm), im = wrap_dec(i, g.nzm);
+  const int ip = zinc(g, i), im = zdec(g, i);
   const size_t c0 = col_off(g, j, i);
   if (tc == 0) {
     mbar_init(&bar, 1);
@@ -423,11 +447,12 @@ __global__ void __launch_bounds__(TPC)
   const ColV Z{C(11), C(12), C(13), C(14), C(15), C(16)};
   const ColV T{C(17), C(18), C(19), C(20), C(21), nullptr};
   const ColV P{C(22), nullptr, C(23), nullptr, C(24), nullptr};
-  const StepCoef sc = sc_all[ns];
+  const int slot = sc_slot(g, i, ns);
+  const StepCoef sc = sc_all[slot];
   const size_t tsz = cn_table_size(M);
-  const double *TX = cn_tab + (size_t)(ns * 3 + 0) * tsz;
-  const double *TY = cn_tab + (size_t)(ns * 3 + 1) * tsz;
-  const double *TT = cn_tab + (size_t)(ns * 3 + 2) * tsz;
+  const double *TX = cn_tab + (size_t)(slot * 3 + 0) * tsz;
+  const double *TY = cn_tab + (size_t)(slot * 3 + 1) * tsz;
+  const double *TT = cn_tab + (size_t)(slot * 3 + 2) * tsz;
   const int nxm = g.nxm;
   const size_t pl = (size_t)j + (size_t)g.nym * i;
   const double tbp = __ldg(t.tempbp + pl), ttp = __ldg(t.temptp + pl);
@@ -499,18 +524,21 @@ __global__ void __launch_bounds__(TPC)
 // ------------------------------------------------------------------------------------------
 template <int TX, typename TS>
 __global__ void __launch_bounds__(256)
-    k_div_fft_y(Geom g, Tables t, const StepCoef *__restrict__ sc_all, int ns,
+    k_div_fft_y(Geom g0, Tables t, const StepCoef *__restrict__ sc_all, int ns,
                 const double *__restrict__ vx, const double *__restrict__ vy,
                 const double *__restrict__ vz, typename Cplx<TS>::type *__restrict__ spec,
                 FftPlan pl, const typename Cplx<TS>::type *__restrict__ tw) {
   using C = typename Cplx<TS>::type;
   extern __shared__ __align__(16) unsigned char smem_raw_k2[];
   C *b0 = reinterpret_cast<C *>(smem_raw_k2);
+  const int k0 = blockIdx.x * TX, i = blockIdx.y;
+  Geom g = g0;
   const int N = g.nym, B = TX / 2;
   C *b1 = b0 + (size_t)B * N;
-  const int k0 = blockIdx.x * TX, i = blockIdx.y;
-  const int ip = wrap_inc(i, g.nzm);
-  const StepCoef sc = sc_all[ns];
+  if (!inst_active(g, i)) return;
+  bind_instance(g, i);
+  const int ip = zinc(g, i);
+  const StepCoef sc = sc_all[sc_slot(g, i, ns)];
   const double usdtal = 1.0 / (sc.dt * sc.al);
   const int tx = threadIdx.x % TX;
   const int k = k0 + tx;
@@ -530,7 +558,7 @@ __global__ void __launch_bounds__(256)
   }
   __syncthreads();
   C *res = fft_block<false, TS>(b0, b1, B, pl, tw);
-  const TS norm = (TS)(1.0 / ((double)g.nzm * (double)g.nym));
+  const TS norm = (TS)(1.0 / (nz_norm(g) * (double)g.nym));
   const TS half = (TS)0.5;
   for (int e = threadIdx.x; e < g.nyh * TX; e += blockDim.x) {
     const int ex = e % TX, ky = e / TX;
@@ -602,12 +630,15 @@ __global__ void __launch_bounds__(WPB * 32)
   const int sys = blockIdx.x * WPB + warp;
   if (sys >= g.nyh * g.nzm) return;
   const int ky = sys % g.nyh, kz = sys / g.nyh;
-  const bool pin = (ky == 0 && kz == 0);
+  if (!inst_active(g, kz)) return;  // whole warp (batch mode: kz numbers the instance)
+  // the singular (0,0) mode; in batch mode every instance's ky = 0 mode (nzm = 1 each)
+  const bool pin = (ky == 0 && (kz == 0 || g.batch));
   double *sa = smem_k4 + warp * (4 * 32 * M);
   double *sc_ = sa + 32 * M, *sdr = sa + 64 * M, *sdi = sa + 96 * M;
   C *colp = spec + (size_t)sys * g.ldxc;
   const int n = g.nxm;
-  const double akj = __ldg(t.ak2 + ky), aki = __ldg(t.ak1 + kz);
+  const double akj = __ldg(t.ak2 + (g.batch ? (size_t)kz * g.nym : 0) + ky);
+  const double aki = g.batch ? 0.0 : __ldg(t.ak1 + kz);
 #pragma unroll
   for (int tt = 0; tt < M; ++tt) {
     const int r = lane + 32 * tt;
@@ -737,6 +768,7 @@ __global__ void __launch_bounds__(256)
   const int N = g.nym, B = TX / 2;
   C *b1 = b0 + (size_t)B * N;
   const int k0 = blockIdx.x * TX, i = blockIdx.y;
+  if (!inst_active(g, i)) return;
 #pragma unroll 4
   for (int e = threadIdx.x; e < N * B; e += blockDim.x) {
     const int p = e % B, j = e / B;
@@ -770,17 +802,19 @@ __global__ void __launch_bounds__(256)
 // and CorrectPressure (pressure.F90:276-300) in place.  Thread per (k, j, i).
 template <typename TS>
 __global__ void __launch_bounds__(256)
-    k_correct(Geom g, Tables t, const StepCoef *__restrict__ sc_all, int ns,
+    k_correct(Geom g0, Tables t, const StepCoef *__restrict__ sc_all, int ns,
               const double *__restrict__ vxh, const double *__restrict__ vyh,
               const double *__restrict__ vzh, double *__restrict__ vx, double *__restrict__ vy,
               double *__restrict__ vz, double *__restrict__ pr, const TS *__restrict__ phi) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
   const int i = blockIdx.z;
-  if (k >= g.nxm || j >= g.nym) return;
-  const StepCoef sc = sc_all[ns];
+  Geom g = g0;
+  if (k >= g.nxm || j >= g.nym || !inst_active(g, i)) return;
+  bind_instance(g, i);
+  const StepCoef sc = sc_all[sc_slot(g, i, ns)];
   const int jm = wrap_dec(j, g.nym), jp = wrap_inc(j, g.nym);
-  const int im = wrap_dec(i, g.nzm), ip = wrap_inc(i, g.nzm);
+  const int im = zdec(g, i), ip = zinc(g, i);
   const int km = (k == 0) ? 0 : k - 1;
   const int kp = (k == g.nxm - 1) ? k : k + 1;
   const size_t c = col_off(g, j, i);
@@ -828,7 +862,7 @@ __global__ void __launch_bounds__(256)
   const int wstride = gridDim.x * (blockDim.x >> 5);
   for (int cidx = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); cidx < ncol; cidx += wstride) {
     const int j = cidx % g.nym, i = cidx / g.nym;
-    const int jp = wrap_inc(j, g.nym), ip = wrap_inc(i, g.nzm);
+    const int jp = wrap_inc(j, g.nym), ip = zinc(g, i);
     const size_t c = col_off(g, j, i), cjp = col_off(g, jp, i), cip = col_off(g, j, ip);
     for (int k = lane; k < g.nxm; k += 32) {
       double q;
@@ -925,7 +959,7 @@ __device__ __forceinline__ int tsw(int r, int c) { return r * 8 + (c ^ zsw(r)); 
 // at one z index i.  The real tile is the complex tile read as (re, im) = (x point 2c, 2c+1).
 template <int N1, typename TS>
 __global__ void __launch_bounds__(256)
-    k_div_fft_y_w(Geom g, Tables t, const StepCoef *__restrict__ sc_all, int ns,
+    k_div_fft_y_w(Geom g0, Tables t, const StepCoef *__restrict__ sc_all, int ns,
                   const double *__restrict__ vx, const double *__restrict__ vy,
                   const double *__restrict__ vz, typename Cplx<TS>::type *__restrict__ spec,
                   const typename Cplx<TS>::type *__restrict__ tw) {
@@ -935,8 +969,11 @@ __global__ void __launch_bounds__(256)
   C *T = reinterpret_cast<C *>(smem_k2w);  // [N][8] swizzled
   TS *Tr = reinterpret_cast<TS *>(smem_k2w);
   const int k0 = blockIdx.x * 16, i = blockIdx.y;
-  const int ip = wrap_inc(i, g.nzm);
-  const StepCoef sc = sc_all[ns];
+  Geom g = g0;
+  if (!inst_active(g, i)) return;
+  bind_instance(g, i);
+  const int ip = zinc(g, i);
+  const StepCoef sc = sc_all[sc_slot(g, i, ns)];
   const double usdtal = 1.0 / (sc.dt * sc.al);
   const int tx = threadIdx.x & 15, k = k0 + tx;
   const double ux = (k < g.nxm) ? __ldg(t.udx3m + k) : 0.0;
@@ -964,7 +1001,7 @@ __global__ void __launch_bounds__(256)
 #pragma unroll
   for (int k1 = 0; k1 < N1; ++k1) T[tsw(k1 + N1 * rl, p)] = x[k1];
   __syncthreads();
-  const TS norm = (TS)(1.0 / ((double)g.nzm * (double)g.nym));
+  const TS norm = (TS)(1.0 / (nz_norm(g) * (double)g.nym));
   const TS half = (TS)0.5;
   for (int e = threadIdx.x; e < g.nyh * 16; e += blockDim.x) {
     const int ex = e & 15, ky = e >> 4;
@@ -1044,6 +1081,7 @@ __global__ void __launch_bounds__(256)
   C *T = reinterpret_cast<C *>(smem_k6w);  // [N][8] swizzled
   const TS *Tr = reinterpret_cast<const TS *>(smem_k6w);
   const int k0 = blockIdx.x * 16, i = blockIdx.y;
+  if (!inst_active(g, i)) return;
 #pragma unroll 4
   for (int e = threadIdx.x; e < N * 8; e += blockDim.x) {
     const int p = e & 7, j = e >> 3;
@@ -1116,7 +1154,11 @@ cudaError_t launch_cn_tables(const LaunchCtx &L, const CnInputs &in) {
   a.ren = in.ren;
   a.ns0 = in.ns0;
   a.nsub = in.nsub;
-  k_cn_tables<<<3 * in.nsub, 32, 0, L.stream>>>(a, in.M, in.tab, in.sc);
+  a.dt_dev = in.dt_dev;
+  a.inst = in.inst;
+  a.active = in.active;
+  const int nb = in.dt_dev ? in.ninst : 1;
+  k_cn_tables<<<3 * in.nsub * nb, 32, 0, L.stream>>>(a, in.M, in.tab, in.sc);
   return cudaGetLastError();
 }
 
@@ -1246,7 +1288,7 @@ static cudaError_t launch_stage_T(const LaunchCtx &L, const SubstepBuffers &b, i
   const C *twy = (const C *)L.twy;
   const C *twz = (const C *)L.twz;
   if (L.warp_fft && (st == Stage::DivFftY || st == Stage::IfftY ||
-                     ((st == Stage::FftZFwd || st == Stage::FftZInv) && g.nzm > 1))) {
+                     ((st == Stage::FftZFwd || st == Stage::FftZInv) && g.nzm > 1 && !g.batch))) {
     cudaError_t e = cudaSuccess;
     if (launch_warp_fft<TS>(L, b, ns, st, &e)) return e;
   }
@@ -1271,8 +1313,8 @@ static cudaError_t launch_stage_T(const LaunchCtx &L, const SubstepBuffers &b, i
       return cudaGetLastError();
     }
     case Stage::FftZFwd:
-    case Stage::FftZInv: {  // K3 / K5 z FFT
-      if (g.nzm == 1) return cudaSuccess;
+    case Stage::FftZInv: {  // K3 / K5 z FFT (none for one 2-D domain or a batch of them)
+      if (g.nzm == 1 || g.batch) return cudaSuccess;
       const int TXZ = L.tx_z;
       const size_t smem = (size_t)2 * TXZ * g.nzm * sizeof(C);
       dim3 grid((g.nxm + TXZ - 1) / TXZ, g.nyh);

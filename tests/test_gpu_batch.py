@@ -1,0 +1,155 @@
+"""Batched 2-D instances (include/afid_batch.h).
+
+Gates:
+- alone == in-mix: a slot's fields after N steps are bitwise identical whether it ran alone or
+  next to other active slots with different Ra, Pr, aspect ratio and seeds (both precisions);
+- an idle slot keeps its state bit for bit while the others step;
+- a slot agrees with the same case run as its own context through the single-domain API with
+  the main-loop dt rule driven from the host (main.F90:285-313);
+- an instance that raises an error code (fixed dt, CFL > CFLMAX) stops; the others go on.
+"""
+import ctypes
+
+import numpy as np
+import pytest
+
+import afid_gpu as ag
+from helpers import Case, bou_text, rel_l2
+
+pytestmark = pytest.mark.gpu
+
+NXM, NYM = 32, 64
+SLOTS = [dict(rayt=1e6, prat=1.0, ylen=2.0), dict(rayt=3e7, prat=0.7, ylen=1.0),
+         dict(rayt=2e5, prat=4.4, ylen=4.0), dict(rayt=1e8, prat=1.0, ylen=2.0),
+         dict(rayt=5e6, prat=0.7, ylen=1.0)]
+STEP = dict(zlen=1.0, idtv=1, dt=1e-3, cflmax=1.2, dtmax=2e-3)
+
+
+def _inp(**kw):
+    v = dict(STEP)
+    v.update(kw)
+    return ag.parse_bou_in(bou_text(NXM, NYM, 1, **v))
+
+
+def _batch(precision, nslots=len(SLOTS)):
+    b = ag.Batch(_inp(**SLOTS[0]), nslots, precision)
+    for s in range(nslots):
+        b.configure(s, _inp(**SLOTS[s % len(SLOTS)]))
+        b.seed(s, 100 + s)
+    return b
+
+
+def _perturb(b, slot, amp=0.05):
+    """Non-zero velocity so the flow terms and the CFL rule are exercised from step 1."""
+    rng = np.random.default_rng(slot)
+    f = b.download(slot)
+    for k in ("vx", "vy"):
+        f[k][...] = amp * rng.standard_normal(f[k].shape)
+    f["vx"][:, 0] = 0.0
+    f["vx"][:, NXM] = 0.0
+    f["vy"][:, NXM] = 0.0
+    b.upload(slot, f["vx"], f["vy"], f["vz"], f["temp"], f["pr"])
+
+
+@pytest.mark.parametrize("precision", [ag.PREC_FP64, ag.PREC_MIXED])
+def test_alone_equals_in_mix(precision):
+    target, nsteps = 2, 40
+    out = {}
+    for mix in ("alone", "all", "odd_out"):
+        with _batch(precision) as b:
+            for s in range(b.nslots):
+                _perturb(b, s)
+            act = np.zeros(b.nslots, np.uint8)
+            if mix == "alone":
+                act[target] = 1
+            elif mix == "all":
+                act[:] = 1
+            else:
+                act[[0, 2, 3]] = 1
+            b.set_active(act)
+            b.step(nsteps // 2)
+            if mix == "odd_out":  # change the mix halfway: slot 4 joins, slot 0 leaves
+                act[0], act[4] = 0, 1
+                b.set_active(act)
+            b.step(nsteps - nsteps // 2)
+            st = b.stats()
+            out[mix] = (b.download(target), st)
+    ref, st_ref = out["alone"]
+    assert st_ref["ntime"][target] == nsteps and st_ref["errorcode"][target] == 0
+    for mix in ("all", "odd_out"):
+        f, st = out[mix]
+        for k in ag.Batch.FIELDS:
+            assert np.array_equal(f[k][:, :NXM], ref[k][:, :NXM]), (mix, k)
+        assert st["dt"][target] == st_ref["dt"][target]
+        assert st["time"][target] == st_ref["time"][target]
+        assert st["nu_vol"][target] == st_ref["nu_vol"][target]
+
+
+def test_idle_slot_keeps_state():
+    with _batch(ag.PREC_FP64) as b:
+        for s in range(b.nslots):
+            _perturb(b, s)
+        before = b.download(1)
+        act = np.ones(b.nslots, np.uint8)
+        act[1] = 0
+        b.set_active(act)
+        b.step(7)  # odd step count: the temperature buffers end swapped
+        after = b.download(1)
+        st = b.stats()
+    for k in ag.Batch.FIELDS:
+        assert np.array_equal(after[k][:, :NXM], before[k][:, :NXM]), k
+    assert st["ntime"][1] == 0 and st["ntime"][0] == 7
+
+
+@pytest.mark.parametrize("precision", [ag.PREC_FP64, ag.PREC_MIXED])
+def test_slot_matches_single_domain(precision):
+    slot, nsteps = 3, 30
+    with _batch(precision) as b:
+        for s in range(b.nslots):
+            _perturb(b, s)
+        init = b.download(slot)
+        b.set_active(np.ones(b.nslots, np.uint8))
+        b.step(nsteps)
+        got = b.download(slot)
+        st = b.stats()
+    case = Case(NXM, NYM, 1, precision=precision, **dict(STEP, **SLOTS[slot]))
+    dt = ctypes.c_double(case.p.dt)
+    with case.solver() as g:
+        g.upload(*(init[k][None] for k in ag.Solver.FIELDS))
+        t = 0.0
+        for n in range(nsteps):
+            cfl = g.calc_max_cfl()
+            assert ag.lib().afid_next_dt(ctypes.byref(case.inp), n, ctypes.byref(dt), cfl, None) == 0
+            g.time_marcher(dt.value, n)
+            t += dt.value
+        ref = g.download()
+        nu, ke, _ = g.global_quantities(case.p.prat * abs(case.p.rayt))
+    tol = 1e-11 if precision == ag.PREC_FP64 else 1e-5
+    for k in ("vx", "vy", "temp"):
+        assert rel_l2(got[k][:, :NXM], ref[k][0][:, :NXM]) < tol, k
+    assert abs(st["time"][slot] - t) < 1e-12 * t
+    assert abs(st["nu_vol"][slot] - nu) < 1e-9 * abs(nu)
+    assert abs(st["ke"][slot] - ke) < 1e-9 * abs(ke) + 1e-300
+
+
+def test_error_stops_only_that_instance():
+    with ag.Batch(_inp(**SLOTS[0]), 3, ag.PREC_FP64) as b:
+        for s in range(3):
+            b.configure(s, _inp(**SLOTS[s]) if s != 1 else _inp(**dict(SLOTS[1], idtv=0, dt=0.1)))
+            b.seed(s, 7 + s)
+            _perturb(b, s, amp=1.0)
+        b.set_active(np.ones(3, np.uint8))
+        b.step(5)
+        st = b.stats()
+    assert st["errorcode"][1] == 165
+    assert st["ntime"][1] == 1  # the step that raised the code completes, then the instance stops
+    assert st["ntime"][0] == 5 and st["ntime"][2] == 5
+    assert st["errorcode"][0] == 0 and st["errorcode"][2] == 0
+
+
+def test_configure_rejects_other_size_class():
+    with ag.Batch(_inp(**SLOTS[0]), 2, ag.PREC_FP64) as b:
+        other = ag.parse_bou_in(bou_text(NXM, 2 * NYM, 1, **STEP))
+        with pytest.raises(ag.AfidError):
+            b.configure(0, other)
+        assert b.device_bytes() > 0
