@@ -298,6 +298,13 @@ int ctx_create(const afid_grid_t *grid, const afid_params_t *prm, const BatchSpe
   g.tfixs = prm->tfixs;
   g.tfixn = prm->tfixn;
 
+  // One wall-normal column set must fit the shared memory of one block (3-D FP64: nxm <= ~850).
+  int smem_optin = 0;
+  cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx->dev);
+  if (smem_optin > 0 && k1_smem_bytes(g.ldx, M, mixed, bs != nullptr || nzm == 1) + 64 > (size_t)smem_optin) {
+    afid_gpu_destroy(ctx);
+    return AFID_E_INVALID;
+  }
   const size_t nf = (size_t)g.ldx * nym * nzm;
   ctx->field_elems = nf;
   const size_t nspec = (size_t)g.ldxc * g.nyh * nzm;

@@ -51,6 +51,8 @@ struct CnInputs {
 };
 
 int cn_choose_M(int nxm);
+// Dynamic shared memory of the fused explicit/implicit kernel (29 staged x-columns + solve rows).
+size_t k1_smem_bytes(int ldx, int M, bool mixed, bool two_d);
 size_t cn_tab_doubles(int M, int nsst);
 cudaError_t launch_cn_tables(const LaunchCtx &L, const CnInputs &in);
 cudaError_t launch_explicit_implicit(const LaunchCtx &L, const SubstepBuffers &b, int ns);

@@ -368,12 +368,15 @@ __device__ __forceinline__ double rhs_temp(const Geom &g, const Tables &t, const
 }
 
 // Number of x-columns K1 stages per (j,i) column: vx 5, vy 6, vz 6, temp 5, pr 3 (FP64) + 4 RK3
-// histories (TE).
+// histories (TE).  In 2-D (nzm = 1, or a batch of 2-D instances) the z neighbours are the
+// column itself, leaving vx, vy, vz, temp at (j, j+1, j-1) and pr at (j, j-1): 14 columns.
 constexpr int kK1StateCols = 25;
+constexpr int kK1StateCols2D = 14;
 constexpr int kK1RuCols = 4;
 
-__host__ __device__ inline size_t k1_stage_bytes(int ldx, size_t te_size) {
-  return (size_t)kK1StateCols * ldx * sizeof(double) + (size_t)kK1RuCols * ldx * te_size;
+__host__ __device__ inline size_t k1_stage_bytes(int ldx, size_t te_size, bool two_d) {
+  return (size_t)(two_d ? kK1StateCols2D : kK1StateCols) * ldx * sizeof(double) +
+         (size_t)kK1RuCols * ldx * te_size;
 }
 
 // K1: a block owns one (j,i) column.  One thread issues 1-D TMA bulk copies of the 29 needed
@@ -382,7 +385,7 @@ __host__ __device__ inline size_t k1_stage_bytes(int ldx, size_t te_size) {
 // memory, write the new RK3 histories, and put the scaled RHS in the solver's chunk layout
 // (row r at (r%M)*33 + r/M).  Four warps run the partitioned CN solves, and every thread adds
 // the increments to the staged centre values and stores the intermediate fields.
-template <int M, int TPC, int RPT, typename TE>
+template <int M, int TPC, int RPT, typename TE, bool TWO_D>
 __global__ void __launch_bounds__(TPC)
     k_explicit_implicit(Geom g0, Tables t, const StepCoef *__restrict__ sc_all, int ns,
                         const double *__restrict__ cn_tab, const double *__restrict__ vx,
@@ -398,8 +401,9 @@ __global__ void __launch_bounds__(TPC)
   Geom g = g0;
   const int ldx = g.ldx;
   double *cols = reinterpret_cast<double *>(smem_k1);
-  TE *rcols = reinterpret_cast<TE *>(cols + (size_t)kK1StateCols * ldx);
-  double *s_rhs = reinterpret_cast<double *>(smem_k1 + k1_stage_bytes(ldx, sizeof(TE)));
+  constexpr int NS = TWO_D ? kK1StateCols2D : kK1StateCols;
+  TE *rcols = reinterpret_cast<TE *>(cols + (size_t)NS * ldx);
+  double *s_rhs = reinterpret_cast<double *>(smem_k1 + k1_stage_bytes(ldx, sizeof(TE), TWO_D));
   const int tc = threadIdx.x;
   const int colid = blockIdx.x;
   const int j = colid % g.nym, i = colid / g.nym;
@@ -422,14 +426,24 @@ __global__ void __launch_bounds__(TPC)
     const size_t oc = c0, ojp = col_off(g, jp, i), ojm = col_off(g, jm, i), oip = col_off(g, j, ip),
                  oim = col_off(g, j, im), ojpim = col_off(g, jp, im), ojmip = col_off(g, jm, ip);
     const uint32_t cb = (uint32_t)ldx * sizeof(double), rb = (uint32_t)ldx * sizeof(TE);
-    mbar_arrive_expect_tx(&bar, (uint32_t)k1_stage_bytes(ldx, sizeof(TE)));
-    const double *src[kK1StateCols] = {vx + oc,   vx + ojp, vx + ojm, vx + oip, vx + oim,  // 0-4
-                                       vy + oc,   vy + ojp, vy + ojm, vy + oip, vy + oim, vy + ojpim,  // 5-10
-                                       vz + oc,   vz + ojp, vz + ojm, vz + oip, vz + oim, vz + ojmip,  // 11-16
-                                       temp + oc, temp + ojp, temp + ojm, temp + oip, temp + oim,      // 17-21
-                                       pr + oc,   pr + ojm, pr + oim};                                // 22-24
+    mbar_arrive_expect_tx(&bar, (uint32_t)k1_stage_bytes(ldx, sizeof(TE), TWO_D));
+    if constexpr (TWO_D) {
+      const double *src[kK1StateCols2D] = {vx + oc,   vx + ojp,   vx + ojm,    // 0-2
+                                           vy + oc,   vy + ojp,   vy + ojm,    // 3-5
+                                           vz + oc,   vz + ojp,   vz + ojm,    // 6-8
+                                           temp + oc, temp + ojp, temp + ojm,  // 9-11
+                                           pr + oc,   pr + ojm};               // 12-13
 #pragma unroll
-    for (int q = 0; q < kK1StateCols; ++q) bulk_g2s(cols + (size_t)q * ldx, src[q], cb, &bar);
+      for (int q = 0; q < kK1StateCols2D; ++q) bulk_g2s(cols + (size_t)q * ldx, src[q], cb, &bar);
+    } else {
+      const double *src[kK1StateCols] = {vx + oc,   vx + ojp, vx + ojm, vx + oip, vx + oim,  // 0-4
+                                         vy + oc,   vy + ojp, vy + ojm, vy + oip, vy + oim, vy + ojpim,  // 5-10
+                                         vz + oc,   vz + ojp, vz + ojm, vz + oip, vz + oim, vz + ojmip,  // 11-16
+                                         temp + oc, temp + ojp, temp + ojm, temp + oip, temp + oim,      // 17-21
+                                         pr + oc,   pr + ojm, pr + oim};                                // 22-24
+#pragma unroll
+      for (int q = 0; q < kK1StateCols; ++q) bulk_g2s(cols + (size_t)q * ldx, src[q], cb, &bar);
+    }
     bulk_g2s(rcols, rux + oc, rb, &bar);
     bulk_g2s(rcols + ldx, ruy + oc, rb, &bar);
     bulk_g2s(rcols + 2 * ldx, ruz + oc, rb, &bar);
@@ -442,11 +456,12 @@ __global__ void __launch_bounds__(TPC)
     return;
   }
   auto C = [&](int q) { return (const double *)(cols + (size_t)q * ldx); };
-  const ColV X{C(0), C(1), C(2), C(3), C(4), nullptr};
-  const ColV Y{C(5), C(6), C(7), C(8), C(9), C(10)};
-  const ColV Z{C(11), C(12), C(13), C(14), C(15), C(16)};
-  const ColV T{C(17), C(18), C(19), C(20), C(21), nullptr};
-  const ColV P{C(22), nullptr, C(23), nullptr, C(24), nullptr};
+  // {centre, j+1, j-1, i+1, i-1, diagonal}; in 2-D the i+-1 columns are the centre's
+  const ColV X = TWO_D ? ColV{C(0), C(1), C(2), C(0), C(0), nullptr} : ColV{C(0), C(1), C(2), C(3), C(4), nullptr};
+  const ColV Y = TWO_D ? ColV{C(3), C(4), C(5), C(3), C(3), C(4)} : ColV{C(5), C(6), C(7), C(8), C(9), C(10)};
+  const ColV Z = TWO_D ? ColV{C(6), C(7), C(8), C(6), C(6), C(8)} : ColV{C(11), C(12), C(13), C(14), C(15), C(16)};
+  const ColV T = TWO_D ? ColV{C(9), C(10), C(11), C(9), C(9), nullptr} : ColV{C(17), C(18), C(19), C(20), C(21), nullptr};
+  const ColV P = TWO_D ? ColV{C(12), nullptr, C(13), nullptr, C(12), nullptr} : ColV{C(22), nullptr, C(23), nullptr, C(24), nullptr};
   const int slot = sc_slot(g, i, ns);
   const StepCoef sc = sc_all[slot];
   const size_t tsz = cn_table_size(M);
@@ -1131,6 +1146,9 @@ static int pick_M(int nxm) {
 }
 
 int cn_choose_M(int nxm) { return pick_M(nxm); }
+size_t k1_smem_bytes(int ldx, int M, bool mixed, bool two_d) {
+  return k1_stage_bytes(ldx, mixed ? sizeof(float) : sizeof(double), two_d) + (size_t)4 * 33 * M * sizeof(double);
+}
 size_t cn_tab_doubles(int M, int nsst) { return cn_table_size(M) * 3 * (size_t)nsst; }
 
 cudaError_t launch_cn_tables(const LaunchCtx &L, const CnInputs &in) {
@@ -1162,11 +1180,11 @@ cudaError_t launch_cn_tables(const LaunchCtx &L, const CnInputs &in) {
   return cudaGetLastError();
 }
 
-template <int M, int TPC, int RPT, typename TE>
+template <int M, int TPC, int RPT, typename TE, bool TWO_D>
 static cudaError_t launch_k1_cfg(const LaunchCtx &L, const SubstepBuffers &b, int ns) {
   const int ncol = L.g.nym * L.g.nzm;
-  const size_t smem = k1_stage_bytes(L.g.ldx, sizeof(TE)) + (size_t)4 * 33 * M * sizeof(double);
-  auto kern = k_explicit_implicit<M, TPC, RPT, TE>;
+  const size_t smem = k1_stage_bytes(L.g.ldx, sizeof(TE), TWO_D) + (size_t)4 * 33 * M * sizeof(double);
+  auto kern = k_explicit_implicit<M, TPC, RPT, TE, TWO_D>;
   cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   kern<<<ncol, TPC, smem, L.stream>>>(L.g, L.t, b.sc, ns, b.cn_tab, b.vx, b.vy, b.vz, b.temp, b.pr,
                                       (TE *)b.rux, (TE *)b.ruy, (TE *)b.ruz, (TE *)b.rut, b.vx_o, b.vy_o,
@@ -1175,14 +1193,19 @@ static cudaError_t launch_k1_cfg(const LaunchCtx &L, const SubstepBuffers &b, in
 }
 
 // M = ceil(nxm/32) rounded to {1,2,4,8,12,16,24,32}; TPC threads cover nxm in RPT rows each.
+template <int M, typename TE, bool TWO_D>
+static cudaError_t launch_k1_M(const LaunchCtx &L, const SubstepBuffers &b, int ns) {
+  if constexpr (M <= 1) return launch_k1_cfg<M, 32, 1, TE, TWO_D>(L, b, ns);          // nxm <= 32
+  else if constexpr (M <= 2) return launch_k1_cfg<M, 64, 1, TE, TWO_D>(L, b, ns);     // <= 64
+  else if constexpr (M <= 4) return launch_k1_cfg<M, 128, 1, TE, TWO_D>(L, b, ns);    // <= 128
+  else if constexpr (M <= 8) return launch_k1_cfg<M, 256, 1, TE, TWO_D>(L, b, ns);    // <= 256
+  else if constexpr (M <= 16) return launch_k1_cfg<M, 256, 2, TE, TWO_D>(L, b, ns);   // <= 512
+  else return launch_k1_cfg<M, 256, 4, TE, TWO_D>(L, b, ns);                          // <= 1024
+}
+
 template <int M, typename TE>
 static cudaError_t launch_k1_M(const LaunchCtx &L, const SubstepBuffers &b, int ns) {
-  if constexpr (M <= 1) return launch_k1_cfg<M, 32, 1, TE>(L, b, ns);          // nxm <= 32
-  else if constexpr (M <= 2) return launch_k1_cfg<M, 64, 1, TE>(L, b, ns);     // <= 64
-  else if constexpr (M <= 4) return launch_k1_cfg<M, 128, 1, TE>(L, b, ns);    // <= 128
-  else if constexpr (M <= 8) return launch_k1_cfg<M, 256, 1, TE>(L, b, ns);    // <= 256
-  else if constexpr (M <= 16) return launch_k1_cfg<M, 256, 2, TE>(L, b, ns);   // <= 512
-  else return launch_k1_cfg<M, 256, 4, TE>(L, b, ns);                          // <= 1024
+  return (L.g.nzm == 1 || L.g.batch) ? launch_k1_M<M, TE, true>(L, b, ns) : launch_k1_M<M, TE, false>(L, b, ns);
 }
 
 template <typename TE>

@@ -310,6 +310,181 @@ def run_gpu(args):
         dist.destroy_process_group()
 
 
+# ---- batched sweep: independent 2-D instances of four size classes ------------------------
+BATCH_SEED = 20261203
+BATCH_SIZES = [(128, 64), (256, 128), (512, 256), (1024, 512)]  # (horizontal nym, wall-normal nxm)
+BATCH_PR = [0.7, 1.0, 4.4]
+BATCH_ASPECT = [1.0, 2.0, 4.0]
+
+
+def batch_instances(n: int = 256, seed: int = BATCH_SEED):
+    """Instance b draws size class, log10 Ra ~ U[6, 10], Pr and aspect ratio from the Philox
+    stream keyed by ``seed`` at counters 4b .. 4b+3."""
+    import afid_gpu as ag
+    u = lambda b, d: ag.lib().afid_philox_uniform(seed, 4 * b + d)  # noqa: E731
+    out = []
+    for b in range(n):
+        nym, nxm = BATCH_SIZES[min(int(u(b, 0) * 4), 3)]
+        out.append(dict(index=b, nxm=nxm, nym=nym, rayt=10.0 ** (6.0 + 4.0 * u(b, 1)),
+                        prat=BATCH_PR[min(int(u(b, 2) * 3), 2)], ylen=BATCH_ASPECT[min(int(u(b, 3) * 3), 2)]))
+    return out
+
+
+def diffusive_dtmax(nym: int, ylen: float, rayt: float, prat: float, cap: float = 1e-2) -> float:
+    """DTMAX of an instance: AFiD integrates the horizontal diffusion explicitly (ExplicitTerms*),
+    so RK3 needs dt < 0.63 dy^2 min(Re, Pe) (the real-axis stability bound 2.51 over the largest
+    eigenvalue 4 / (dy^2 Re)); the main-loop dt rule has only the CFL bound.  Half of it, capped
+    at 1e-2."""
+    dy = ylen / nym
+    re, pe = math.sqrt(rayt / prat), math.sqrt(rayt * prat)
+    return min(cap, 0.5 * dy * dy * min(re, pe))
+
+
+def batch_bou(inst: dict) -> str:
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from helpers import bou_text as _bt  # noqa: E402
+    dtmax = diffusive_dtmax(inst["nym"], inst["ylen"], inst["rayt"], inst["prat"])
+    return _bt(inst["nxm"], inst["nym"], 1, rayt=inst["rayt"], prat=inst["prat"], ylen=inst["ylen"],
+               zlen=1.0, istr3=4, str3=2.0, idtv=1, dt=min(1e-4, dtmax), cflmax=1.2, dtmax=dtmax,
+               ntst=1000000, resid=1e-3)
+
+
+class BatchSet:
+    """One ag.Batch per size class, each on its own stream; a step forks from and joins to a
+    master stream so the classes overlap on the device."""
+
+    def __init__(self, instances, precision: int):
+        import torch
+        import afid_gpu as ag
+        self.classes = {}
+        for inst in instances:
+            self.classes.setdefault((inst["nxm"], inst["nym"]), []).append(inst)
+        self.master = torch.cuda.Stream()
+        self.batches, self.streams = [], []
+        for key in sorted(self.classes):
+            members = self.classes[key]
+            b = ag.Batch(ag.parse_bou_in(batch_bou(members[0])), len(members), precision)
+            s = torch.cuda.Stream()
+            b.set_stream(s.cuda_stream)
+            for slot, inst in enumerate(members):
+                b.configure(slot, ag.parse_bou_in(batch_bou(inst)))
+                b.seed(slot, BATCH_SEED + 1 + inst["index"])
+            b.set_active([1] * len(members))
+            self.batches.append(b)
+            self.streams.append(s)
+        self.cells = sum(i["nxm"] * i["nym"] for i in instances)
+
+    def step(self, n: int = 1):
+        import torch
+        fork = torch.cuda.Event()
+        fork.record(self.master)
+        joins = []
+        for b, s in zip(self.batches, self.streams):
+            s.wait_event(fork)
+            b.step(n)
+            e = torch.cuda.Event()
+            e.record(s)
+            joins.append(e)
+        for e in joins:
+            self.master.wait_event(e)
+
+    def stats(self):
+        return [b.stats() for b in self.batches]
+
+    def launches(self):
+        return sum(b.launch_count() for b in self.batches)
+
+    def device_bytes(self):
+        return sum(b.device_bytes() for b in self.batches)
+
+    def close(self):
+        for b in self.batches:
+            b.close()
+
+
+def run_batched(args):
+    import numpy as np
+    import torch
+
+    world, rank, local = dist_setup()
+    insts = batch_instances()
+    precision = 1 if args.config == "batched" else 0
+    bs = BatchSet(insts, precision)
+    for _ in range(args.warmup):
+        bs.step()
+    torch.cuda.synchronize()
+    l0 = bs.launches()
+    clocks = ClockSampler(torch.cuda.current_device())
+    barrier(world)
+    torch.cuda.synchronize()
+    clocks.start()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(bs.master)
+    for _ in range(args.steps):
+        bs.step()
+    ev1.record(bs.master)
+    torch.cuda.synchronize()
+    barrier(world)
+    clk = clocks.stop()
+    ms = reduce_max(ev0.elapsed_time(ev1), world)
+    launches = bs.launches() - l0
+    value = world * bs.cells * args.steps / (ms * 1e-3) / 1e6
+    st = bs.stats()
+    nsteps_done = int(min(int(s["ntime"].min()) for s in st))
+    errors = int(sum(int((s["errorcode"] != 0).sum()) for s in st))
+    nu = np.concatenate([s["nu_vol"] for s in st])
+    bs_bytes = bs.device_bytes()
+    bs.close()
+
+    # Nusselt of the same instances and steps on the FP64 path (untimed) for the error gate
+    nu_err = None
+    if precision == 1 and not args.no_nu_check:
+        ref = BatchSet(insts, 0)
+        for _ in range(args.warmup + args.steps):
+            ref.step()
+        torch.cuda.synchronize()
+        nu64 = np.concatenate([s["nu_vol"] for s in ref.stats()])
+        ref.close()
+        ok = np.isfinite(nu) & np.isfinite(nu64)
+        rel = np.abs(nu[ok] - nu64[ok]) / np.abs(nu64[ok])
+        nu_err = {"max": float(rel.max()), "median": float(np.median(rel)),
+                  "within_0.5pct": int((rel <= 5e-3).sum()), "compared": int(ok.sum()),
+                  "note": "instantaneous Nu_vol after the timed steps, mixed vs FP64 batch"}
+
+    if rank == 0:
+        counts = {f"{k[1]}x{k[0]}": len(v) for k, v in sorted(bs.classes.items())}
+        line = {
+            "metric": "Mcell-RK3-steps/s",
+            "value": round(value, 3),
+            "unit": "Mcell-RK3-steps/s",
+            "n_gpus": world,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": round(ms / args.steps, 4),
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f32+f64" if precision else "f64",
+            "data": "synthetic: 256 Philox-drawn 2-D RBC instances, conductive state + seeded +-1e-3 perturbation",
+            "config": {"workload": "batched_256x2d_" + ("mixed" if precision else "fp64"),
+                       "instances": len(insts), "cells": bs.cells, "classes_nymxnxm": counts,
+                       "dt": "CFL-limited per instance (CFLMAX 1.2; DTMAX = min(1e-2, 0.5 dy^2 min(Re, Pe)))",
+                       "l2": "inputs larger than L2 (%.1f GB resident)" % (bs_bytes / 1e9),
+                       "parallelism": "replicas" if world > 1 else "single GPU"},
+            "gpu_launches": int(launches),
+            "clocks": clk,
+            "steps_done_min": nsteps_done,
+            "instances_with_error": errors,
+            "instances_nonfinite": int((~np.isfinite(nu)).sum()),
+            "nu_rel_err_max_vs_fp64": nu_err,
+            "device_bytes": int(bs_bytes),
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
 def cpu_baseline(w: dict, steps: int, budget_s: float = 60.0):
     """The CPU restatement (C + OpenMP, oracle/afid_cpu.c) on the same workload: up to
     ``steps`` full main-loop steps, stopping once ``budget_s`` seconds have been spent."""
@@ -363,7 +538,8 @@ def main():
     ap.add_argument("--steps", type=int, default=30)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="afid", choices=["afid", "reference"])
-    ap.add_argument("--config", default="rbc3d", choices=sorted(WORKLOADS))
+    ap.add_argument("--config", default="rbc3d", choices=sorted(WORKLOADS) + ["batched", "batched_fp64"])
+    ap.add_argument("--no-nu-check", action="store_true")
     ap.add_argument("--cpu-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
@@ -371,6 +547,8 @@ def main():
         args.warmup = 3
     if args.impl == "reference":
         run_reference(args)
+    elif args.config.startswith("batched"):
+        run_batched(args)
     else:
         run_gpu(args)
 

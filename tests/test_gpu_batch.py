@@ -153,3 +153,33 @@ def test_configure_rejects_other_size_class():
         with pytest.raises(ag.AfidError):
             b.configure(0, other)
         assert b.device_bytes() > 0
+
+
+def test_batched_mixed_nusselt_within_half_percent():
+    """Eight 2-D instances (Ra 1e6 .. 1e7, three Pr, three aspect ratios) from the seeded
+    conductive state through the onset of convection, CFL-limited dt; Nu_vol averaged over the
+    last third of 3000 steps, mixed against FP64, per instance."""
+    cases = [dict(rayt=ra, prat=pr, ylen=asp) for ra, pr, asp in
+             [(1e6, 1.0, 2.0), (2e6, 0.7, 1.0), (3e6, 4.4, 2.0), (5e6, 1.0, 4.0),
+              (1e6, 0.7, 4.0), (7e6, 1.0, 1.0), (1e7, 4.4, 2.0), (4e6, 0.7, 2.0)]]
+    step = dict(zlen=1.0, idtv=1, dt=1e-4, cflmax=1.2, dtmax=1e-2)
+    nus = {}
+    for prec in (ag.PREC_FP64, ag.PREC_MIXED):
+        inp = [ag.parse_bou_in(bou_text(64, 128, 1, **dict(step, **c))) for c in cases]
+        with ag.Batch(inp[0], len(cases), prec) as b:
+            for s, x in enumerate(inp):
+                b.configure(s, x)
+                b.seed(s, 2026 + s)
+            b.set_active(np.ones(len(cases), np.uint8))
+            series = []
+            for _ in range(300):
+                b.step(10)
+                series.append(b.stats()["nu_vol"])
+            st = b.stats()
+        assert (st["errorcode"] == 0).all() and (st["ntime"] == 3000).all()
+        nus[prec] = np.array(series)
+    tail = 200
+    n64 = nus[ag.PREC_FP64][tail:].mean(axis=0)
+    n32 = nus[ag.PREC_MIXED][tail:].mean(axis=0)
+    assert (n64 > 2.0).sum() >= 4, n64
+    assert np.all(np.abs(n32 - n64) / n64 < 5e-3), (n32, n64)

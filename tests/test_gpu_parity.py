@@ -56,6 +56,13 @@ def _run_both(case, nsteps, seed=1234, random_velocity=0.0, dt=None):
     ((8, 64, 384), 2, 0.2),     # warp FFT: z N = 32*12
     ((20, 96, 96), 2, 0.2),     # warp FFT N = 32*3 both ways
     ((21, 128, 32), 2, 0.2),    # odd nxm: the last x pair of the y transform has one point
+    ((512, 32, 1), 2, 0.1),     # M=16, two rows per thread
+    ((700, 8, 1), 2, 0.1),      # M=24, four rows per thread
+    ((8, 512, 1), 2, 0.2),      # warp FFT y N = 32*16
+    ((6, 768, 1), 2, 0.2),      # warp FFT y N = 32*24
+    ((8, 1024, 1), 2, 0.2),     # warp FFT y N = 32*32
+    ((4, 32, 512), 2, 0.2),     # warp FFT z N = 32*16
+    ((4, 16, 1024), 1, 0.2),    # warp FFT z N = 32*32
 ])
 def test_timemarcher_parity(shape, steps, rv):
     case = Case(*shape, rayt=1e6, dt=2e-3)
@@ -219,3 +226,29 @@ def test_golden_fixture(name):
                 assert rel_l2_mod_mean(out["pr"][..., :nxm], d[f"step{n + 1}_pr"][..., :nxm]) <= TOL_FP64
         assert gpu.calc_max_cfl() == pytest.approx(float(d["step3_cfl"]), rel=1e-10)
         assert gpu.global_quantities(inp.prat * abs(inp.rayt))[0] == pytest.approx(float(d["step3_nu"]), rel=1e-10)
+
+
+def test_timemarcher_parity_m32_exact_zero_mode():
+    """nxm = 800 (M = 32).  The reference solves the singular (0,0) Poisson mode through a
+    1+1e-15 diagonal; at this wall-normal size that moves pr by ~4e-9 relative to the exact
+    discrete solution (CorrectPressure applies the stiff wall-normal operator to phi), so pr is
+    compared with the oracle's exact (pinned) zero-mode solve; the velocities and temperature
+    are compared with the reference behaviour as well."""
+    case = Case(800, 8, 1, rayt=1e6, dt=2e-3)
+    s_ref, out = _run_both(case, 1, random_velocity=0.1)
+    nxm = case.p.nxm
+    for k in ("vx", "vy", "temp"):
+        assert rel_l2(out[k][..., :nxm + (k == "vx")], getattr(s_ref, k)[..., :nxm + (k == "vx")]) <= TOL_FP64, k
+    assert rel_l2_mod_mean(out["pr"][..., :nxm], s_ref.pr[..., :nxm]) <= 1e-8
+    case.g.pin_zero_mode = True
+    s_pin = case.oracle_state(seed=1234, random_velocity=0.1)
+    o.time_marcher(case.g, s_pin, 2e-3)
+    _compare(case, s_pin, out, TOL_FP64)
+
+
+def test_wall_normal_size_beyond_shared_memory_is_rejected():
+    """A wall-normal column set larger than one block's shared memory is refused at creation
+    (AFID_E_INVALID), not at the first launch."""
+    with pytest.raises(ag.AfidError) as e:
+        Case(1000, 8, 4).solver()
+    assert e.value.status == 603
