@@ -85,7 +85,31 @@ class BatchStatT(C.Structure):
                 ("dt", C.c_double), ("cfl", C.c_double)]
 
 
-# Every symbol declared in include/afid_gpu.h, include/afid_host.h and include/afid_batch.h
+class ServeConfigT(C.Structure):
+    _fields_ = [("precision", C.c_int), ("hbm_budget_bytes", C.c_longlong), ("slots_per_pool", C.c_int),
+                ("chunk_steps", C.c_int), ("max_cells_in_flight", C.c_longlong), ("policy", C.c_int)]
+
+
+class ServeJobT(C.Structure):
+    _fields_ = [("inp", InputT), ("seed", C.c_uint64), ("nsteps", C.c_int), ("tag", C.c_uint64),
+                ("temp_out", C.POINTER(C.c_double))]
+
+
+class ServeResultT(C.Structure):
+    _fields_ = [("tag", C.c_uint64), ("errorcode", C.c_int), ("steps_done", C.c_int),
+                ("time", C.c_double), ("dt", C.c_double), ("cfl", C.c_double), ("nu_vol", C.c_double),
+                ("ke", C.c_double), ("t_submit", C.c_double), ("t_admit", C.c_double), ("t_done", C.c_double)]
+
+
+class ServeStatusT(C.Structure):
+    _fields_ = [("queued", C.c_int), ("running", C.c_int), ("pools", C.c_int),
+                ("device_bytes", C.c_longlong), ("cells_in_flight", C.c_longlong),
+                ("cell_steps_done", C.c_longlong), ("jobs_done", C.c_longlong)]
+
+
+SERVE_FIFO, SERVE_SHORTEST_FIRST = 0, 1
+
+# Every symbol declared in include/afid_gpu.h, afid_host.h, afid_batch.h and afid_serve.h
 EXPORTS = [
     "afid_gpu_create", "afid_gpu_destroy", "afid_gpu_set_stream", "afid_gpu_get_stream",
     "afid_gpu_synchronize", "afid_gpu_upload", "afid_gpu_download", "afid_gpu_timemarcher",
@@ -99,7 +123,10 @@ EXPORTS = [
     "afid_batch_create", "afid_batch_destroy", "afid_batch_set_stream", "afid_batch_configure",
     "afid_batch_seed", "afid_batch_upload", "afid_batch_download", "afid_batch_set_active",
     "afid_batch_step", "afid_batch_synchronize", "afid_batch_stats", "afid_batch_num_slots",
+    "afid_batch_set_limit",
     "afid_batch_device_bytes", "afid_batch_launch_count",
+    "afid_serve_create", "afid_serve_destroy", "afid_serve_submit", "afid_serve_pump", "afid_serve_poll",
+    "afid_serve_status", "afid_serve_now",
 ]
 
 
@@ -149,6 +176,14 @@ def load_library(path: str = _LIB_PATH) -> C.CDLL:
         "afid_batch_upload": (i, [vp, i, _dp, _dp, _dp, _dp, _dp, i, i]),
         "afid_batch_download": (i, [vp, i, _dp, _dp, _dp, _dp, _dp, i, i]),
         "afid_batch_set_active": (i, [vp, C.POINTER(C.c_ubyte)]),
+        "afid_batch_set_limit": (i, [vp, i, i]),
+        "afid_serve_create": (i, [C.POINTER(ServeConfigT), C.POINTER(vp)]),
+        "afid_serve_destroy": (i, [vp]),
+        "afid_serve_submit": (i, [vp, C.POINTER(ServeJobT)]),
+        "afid_serve_pump": (i, [vp]),
+        "afid_serve_poll": (i, [vp, C.POINTER(ServeResultT), i, C.POINTER(i)]),
+        "afid_serve_status": (i, [vp, C.POINTER(ServeStatusT)]),
+        "afid_serve_now": (d, [vp]),
         "afid_batch_step": (i, [vp, i]),
         "afid_batch_synchronize": (i, [vp]),
         "afid_batch_stats": (i, [vp, C.POINTER(BatchStatT), _dp, _dp]),
@@ -357,7 +392,7 @@ class Batch:
     FIELDS = ("vx", "vy", "vz", "temp", "pr")
 
     def __init__(self, proto: InputT, nslots: int, precision: int = PREC_FP64):
-        self.nxm, self.nym, self.nslots = proto.nxm, proto.nym, nslots
+        self.nxm, self.nym, self.nzm, self.nslots = proto.nxm, proto.nym, proto.nzm, nslots
         self.nx = self.nxm + 1
         self._h = C.c_void_p()
         _check(lib().afid_batch_create(C.byref(proto), nslots, precision, C.byref(self._h)),
@@ -365,7 +400,10 @@ class Batch:
 
     @property
     def shape(self):
-        return (self.nym, self.nx)
+        return (self.nym, self.nx) if self.nzm == 1 else (self.nzm, self.nym, self.nx)
+
+    def set_limit(self, slot: int, nsteps: int) -> None:
+        _check(lib().afid_batch_set_limit(self._h, slot, nsteps), "afid_batch_set_limit")
 
     def configure(self, slot: int, inp: InputT) -> None:
         _check(lib().afid_batch_configure(self._h, slot, C.byref(inp)), "afid_batch_configure")
@@ -419,6 +457,63 @@ class Batch:
     def close(self):
         if self._h:
             lib().afid_batch_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Server:
+    """Request loop for simulation jobs (include/afid_serve.h)."""
+
+    def __init__(self, precision: int = PREC_MIXED, hbm_budget_bytes: int = 64 << 30, slots_per_pool: int = 32,
+                 chunk_steps: int = 50, max_cells_in_flight: int = 0, policy: int = SERVE_FIFO):
+        cfg = ServeConfigT(precision, hbm_budget_bytes, slots_per_pool, chunk_steps, max_cells_in_flight, policy)
+        self._h = C.c_void_p()
+        self._keep = {}
+        _check(lib().afid_serve_create(C.byref(cfg), C.byref(self._h)), "afid_serve_create")
+
+    def submit(self, inp: InputT, seed: int, nsteps: int, tag: int, temp_out: np.ndarray | None = None) -> None:
+        job = ServeJobT(inp, seed, nsteps, tag, None)
+        if temp_out is not None:
+            assert temp_out.dtype == np.float64 and temp_out.flags.c_contiguous
+            job.temp_out = _ptr(temp_out)
+            self._keep[tag] = temp_out
+        _check(lib().afid_serve_submit(self._h, C.byref(job)), "afid_serve_submit")
+
+    def pump(self) -> None:
+        _check(lib().afid_serve_pump(self._h), "afid_serve_pump")
+
+    def poll(self, max_results: int = 1024) -> list:
+        buf = (ServeResultT * max_results)()
+        n = C.c_int()
+        _check(lib().afid_serve_poll(self._h, buf, max_results, C.byref(n)), "afid_serve_poll")
+        out = []
+        for r in buf[:n.value]:
+            out.append({k: getattr(r, k) for k, _ in ServeResultT._fields_})
+            self._keep.pop(r.tag, None)
+        return out
+
+    def status(self) -> dict:
+        st = ServeStatusT()
+        _check(lib().afid_serve_status(self._h, C.byref(st)), "afid_serve_status")
+        return {k: getattr(st, k) for k, _ in ServeStatusT._fields_}
+
+    def now(self) -> float:
+        return float(lib().afid_serve_now(self._h))
+
+    def close(self):
+        if self._h:
+            lib().afid_serve_destroy(self._h)
             self._h = C.c_void_p()
 
     def __enter__(self):

@@ -22,7 +22,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 CUFLAGS = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", "-I" + INC, "-I" + CSRC] + ARCH
 CXXFLAGS = ["-std=c++17", "-O2", "-fPIC", "-I" + INC, "-I/usr/local/cuda/include"]
 
-SOURCES = ["afid_kernels.cu", "afid_api.cu", "afid_noalloc.cu", "afid_batch.cu", "afid_host.cpp"]
+SOURCES = ["afid_kernels.cu", "afid_api.cu", "afid_noalloc.cu", "afid_batch.cu", "afid_host.cpp", "afid_serve.cpp"]
 
 
 def _newer(target: str, deps) -> bool:

@@ -54,6 +54,35 @@ std::vector<C> twiddles(int n) {
 
 int round_up(int a, int b) { return (a + b - 1) / b * b; }
 
+// Spacings and physics scalars of the geometry (everything but the sizes).
+void geom_physics(Geom &g, const afid_grid_t *grid, const afid_params_t *prm) {
+  g.dx = (double)g.nxm / grid->alx3;  // CreateGrid.F90:100-106
+  g.dy = (double)g.nym / grid->ylen;
+  g.dz = (double)g.nzm / grid->zlen;
+  g.dyq = g.dy * g.dy;
+  g.dzq = g.dz * g.dz;
+  g.ren = prm->ren;
+  g.pect = prm->pect;
+  g.byct = prm->byct;
+  g.rren = 1.0 / prm->ren;
+  g.rpect = 1.0 / prm->pect;
+  g.udyq_re = g.dyq / prm->ren;  // ExplicitTermsVX.F90:191-192
+  g.udzq_re = g.dzq / prm->ren;
+  g.udyq_pe = g.dyq / prm->pect;  // ExplicitTermsTemp.F90:24-25
+  g.udzq_pe = g.dzq / prm->pect;
+  // ExplicitTermsVY.F90:30-34
+  g.gy = (prm->inslwn == 0 || prm->inslws == 0) ? prm->dpdy * prm->dpdy / (prm->ren * prm->ren)
+                                                 : 8.0 * (prm->dpdy * prm->dpdy) / (prm->ren * prm->ren);
+  g.xplusu = prm->xplusu;
+  g.xminusu = prm->xminusu;
+  g.active_t = prm->active_t;
+  g.gaxis = prm->gaxis;
+  g.inslws = prm->inslws;
+  g.inslwn = prm->inslwn;
+  g.tfixs = prm->tfixs;
+  g.tfixn = prm->tfixn;
+}
+
 template <typename T>
 cudaError_t dalloc(afid_ctx_t *ctx, T **p, size_t count) {
   void *q = nullptr;
@@ -272,31 +301,7 @@ int ctx_create(const afid_grid_t *grid, const afid_params_t *prm, const BatchSpe
   g.ldx = round_up(g.nx, 8);
   g.nyh = nym / 2 + 1;
   g.ldxc = round_up(nxm, 4);
-  g.dx = (double)nxm / grid->alx3;  // CreateGrid.F90:100-106
-  g.dy = (double)nym / grid->ylen;
-  g.dz = (double)nzm / grid->zlen;
-  g.dyq = g.dy * g.dy;
-  g.dzq = g.dz * g.dz;
-  g.ren = prm->ren;
-  g.pect = prm->pect;
-  g.byct = prm->byct;
-  g.rren = 1.0 / prm->ren;
-  g.rpect = 1.0 / prm->pect;
-  g.udyq_re = g.dyq / prm->ren;  // ExplicitTermsVX.F90:191-192
-  g.udzq_re = g.dzq / prm->ren;
-  g.udyq_pe = g.dyq / prm->pect;  // ExplicitTermsTemp.F90:24-25
-  g.udzq_pe = g.dzq / prm->pect;
-  // ExplicitTermsVY.F90:30-34
-  g.gy = (prm->inslwn == 0 || prm->inslws == 0) ? prm->dpdy * prm->dpdy / (prm->ren * prm->ren)
-                                                 : 8.0 * (prm->dpdy * prm->dpdy) / (prm->ren * prm->ren);
-  g.xplusu = prm->xplusu;
-  g.xminusu = prm->xminusu;
-  g.active_t = prm->active_t;
-  g.gaxis = prm->gaxis;
-  g.inslws = prm->inslws;
-  g.inslwn = prm->inslwn;
-  g.tfixs = prm->tfixs;
-  g.tfixn = prm->tfixn;
+  geom_physics(g, grid, prm);
 
   // One wall-normal column set must fit the shared memory of one block (3-D FP64: nxm <= ~850).
   int smem_optin = 0;
@@ -472,6 +477,28 @@ int ctx_create(const afid_grid_t *grid, const afid_params_t *prm, const BatchSpe
 SubstepBuffers ctx_buffers(afid_ctx_t *ctx) { return buffers(ctx); }
 int ctx_run_substep(afid_ctx_t *ctx, int ns) { return run_substep(ctx, ns); }
 int ctx_fail(afid_ctx_t *ctx, cudaError_t e) { return fail_cuda(ctx, e); }
+
+// New physics for a single-domain context of the same grid (sizes and wall-normal tables
+// unchanged): scalars, wavenumbers and plate temperatures.  Launches captured before this call
+// keep the old scalars.
+int ctx_update_params(afid_ctx_t *ctx, const afid_grid_t *grid, const afid_params_t *prm) {
+  Geom &g = ctx->L.g;
+  if (g.batch || grid->nxm != g.nxm || grid->nym != g.nym || grid->nzm != g.nzm || grid->alx3 != ctx->alx3)
+    return AFID_E_INVALID;
+  if (prm->dpdz != 0.0 || (prm->gaxis == 2 && prm->inslwn == 1)) return AFID_E_INVALID;
+  const Tables &t = ctx->L.t;
+  const size_t ny = (size_t)g.nym, nz = (size_t)g.nzm;
+  std::vector<double> bp(ny * nz, 0.5), tp(ny * nz, -0.5);
+  if (prm->tempbp) std::memcpy(bp.data(), prm->tempbp, bp.size() * sizeof(double));
+  if (prm->temptp) std::memcpy(tp.data(), prm->temptp, tp.size() * sizeof(double));
+  AFID_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  AFID_CUDA(ctx, cudaMemcpy(const_cast<double *>(t.ak1), grid->ak1, nz * sizeof(double), cudaMemcpyHostToDevice));
+  AFID_CUDA(ctx, cudaMemcpy(const_cast<double *>(t.ak2), grid->ak2, ny * sizeof(double), cudaMemcpyHostToDevice));
+  AFID_CUDA(ctx, cudaMemcpy(const_cast<double *>(t.tempbp), bp.data(), bp.size() * sizeof(double), cudaMemcpyHostToDevice));
+  AFID_CUDA(ctx, cudaMemcpy(const_cast<double *>(t.temptp), tp.data(), tp.size() * sizeof(double), cudaMemcpyHostToDevice));
+  geom_physics(g, grid, prm);
+  return AFID_OK;
+}
 
 // CN tables and RK3 coefficients of all substeps for every instance of a batch, dt from the device.
 int ctx_build_cn_batch(afid_ctx_t *ctx, const double *dt_dev) {

@@ -75,12 +75,15 @@ __global__ void k_batch_dt(int nslots, unsigned char *__restrict__ active, const
   dt[i] = d;
 }
 
-__global__ void k_batch_advance(int nslots, const unsigned char *__restrict__ active, const double *__restrict__ dt,
-                                double *__restrict__ time, int *__restrict__ ntime) {
+// time += dt (main.F90:313), step counter; a slot that reached its step limit switches off.
+__global__ void k_batch_advance(int nslots, unsigned char *__restrict__ active, const double *__restrict__ dt,
+                                double *__restrict__ time, int *__restrict__ ntime, const int *__restrict__ limit) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= nslots || !active[i]) return;
-  time[i] += dt[i];  // main.F90:313
-  ntime[i] += 1;
+  time[i] += dt[i];
+  const int n = ntime[i] + 1;
+  ntime[i] = n;
+  if (limit[i] > 0 && n >= limit[i]) active[i] = 0;
 }
 
 // Volume sums of GlobalQuantities.F90:31-47 per instance: partial[(i*chunks + chunk)*3 + q].
@@ -139,6 +142,8 @@ struct afid_batch {
   afid_input_t proto{};
   int nslots = 0;
   int precision = 0;
+  bool three_d = false;  // one 3-D domain (nslots = 1) with the step control on the device
+  int planes = 1;        // z planes per slot
   afid_tables_t *proto_tables = nullptr;
   std::vector<afid_input_t> cfg;
   std::vector<InstScal> inst_h;
@@ -148,7 +153,7 @@ struct afid_batch {
   std::vector<void *> allocs;
   InstCtl *ctl = nullptr;
   double *dt = nullptr, *time = nullptr, *cfl = nullptr, *partial = nullptr, *gsum = nullptr;
-  int *ntime = nullptr, *err = nullptr;
+  int *ntime = nullptr, *err = nullptr, *limit = nullptr;
   unsigned long long *cfl_bits = nullptr;
   double *host = nullptr;  // pinned staging for stats
   long long bytes = 0;
@@ -171,25 +176,16 @@ cudaError_t balloc(afid_batch_t *b, T **p, size_t n) {
   return cudaMemset(q, 0, (n ? n : 1) * sizeof(T));
 }
 
+// Inputs that must agree between the slots of one batch (sizes and wall-normal grid, the
+// scheme and the boundary-condition switches); Ra, Pr, YLEN/ZLEN and the dt rule may differ.
 bool same_class(const afid_input_t &a, const afid_input_t &p) {
-  return a.nxm == p.nxm && a.nym == p.nym && a.nzm == 1 && a.alx3 == p.alx3 && a.istr3 == p.istr3 &&
+  return a.nxm == p.nxm && a.nym == p.nym && a.nzm == p.nzm && a.alx3 == p.alx3 && a.istr3 == p.istr3 &&
          a.str3 == p.str3 && a.nsst == p.nsst && a.active_t == p.active_t && a.gaxis == p.gaxis &&
          a.inslws == p.inslws && a.inslwn == p.inslwn && a.tfixs == p.tfixs && a.tfixn == p.tfixn &&
          a.xplusu == p.xplusu && a.xminusu == p.xminusu && a.dpdy == p.dpdy && a.dpdz == 0.0;
 }
 
-// Scalars, wavenumbers and plates of one slot from its bou.in (ReadInputFile/CreateGrid/SetTempBCs).
-int slot_tables(const afid_input_t &in, InstScal *s, std::vector<double> *ak2, std::vector<double> *bp,
-                std::vector<double> *tp, InstCtl *c) {
-  afid_tables_t *t = nullptr;
-  int st = afid_tables_create(&in, AFID_PREC_FP64, &t);
-  if (st != AFID_OK) return st;
-  const afid_params_t *p = afid_tables_params(t);
-  int n = 0;
-  const double *a = afid_tables_array(t, "ak2", &n);
-  ak2->assign(a, a + n);
-  bp->assign(p->tempbp, p->tempbp + in.nym);
-  tp->assign(p->temptp, p->temptp + in.nym);
+void scal_ctl(const afid_input_t &in, const afid_params_t *p, InstScal *s, InstCtl *c) {
   s->dy = (double)in.nym / in.ylen;
   s->dyq = s->dy * s->dy;
   s->ren = p->ren;
@@ -203,18 +199,41 @@ int slot_tables(const afid_input_t &in, InstScal *s, std::vector<double> *ak2, s
   c->dtmin = in.dtmin;
   c->dtmax = in.dtmax;
   c->idtv = in.idtv;
+}
+
+// Scalars, wavenumbers and plates of one 2-D slot from its bou.in (ReadInputFile/CreateGrid/SetTempBCs).
+int slot_tables(const afid_input_t &in, InstScal *s, std::vector<double> *ak2, std::vector<double> *bp,
+                std::vector<double> *tp, InstCtl *c) {
+  afid_tables_t *t = nullptr;
+  int st = afid_tables_create(&in, AFID_PREC_FP64, &t);
+  if (st != AFID_OK) return st;
+  const afid_params_t *p = afid_tables_params(t);
+  int n = 0;
+  const double *a = afid_tables_array(t, "ak2", &n);
+  ak2->assign(a, a + n);
+  bp->assign(p->tempbp, p->tempbp + in.nym);
+  tp->assign(p->temptp, p->temptp + in.nym);
+  scal_ctl(in, p, s, c);
   afid_tables_destroy(t);
   return AFID_OK;
+}
+
+void drop_graphs(afid_batch_t *b) {
+  for (int p = 0; p < 2; ++p) {
+    if (b->graph[p]) cudaGraphExecDestroy(b->graph[p]);
+    b->graph[p] = nullptr;
+    b->graph_temp[p] = nullptr;
+  }
 }
 
 int reset_slot(afid_batch_t *b, int slot) {
   afid_ctx_t *ctx = b->ctx;
   cudaStream_t st = ctx->stream;
   const Geom &g = ctx->L.g;
-  const size_t plane = (size_t)g.ldx * g.nym;
+  const size_t n = (size_t)g.ldx * g.nym * b->planes;
   const size_t tsz = ctx->L.mixed ? sizeof(float) : sizeof(double);
   for (void *r : {ctx->rux, ctx->ruy, ctx->ruz, ctx->rut})
-    if (cudaMemsetAsync((char *)r + plane * slot * tsz, 0, plane * tsz, st) != cudaSuccess) return AFID_E_CUDA;
+    if (cudaMemsetAsync((char *)r + n * slot * tsz, 0, n * tsz, st) != cudaSuccess) return AFID_E_CUDA;
   const double dt0 = b->ctl_h[slot].dt0, zero = 0.0;
   const int izero = 0;
   if (cudaMemcpyAsync(b->dt + slot, &dt0, sizeof(double), cudaMemcpyHostToDevice, st) != cudaSuccess ||
@@ -230,8 +249,13 @@ int enqueue_step(afid_batch_t *b) {
   afid_ctx_t *ctx = b->ctx;
   const LaunchCtx &L = ctx->L;
   cudaStream_t st = ctx->stream;
-  if (cudaMemsetAsync(b->cfl_bits, 0, sizeof(unsigned long long) * b->nslots, st) != cudaSuccess) return AFID_E_CUDA;
-  k_batch_cfl<<<dim3(kChunks, b->nslots), 256, 0, st>>>(L.g, L.t, ctx->vx, ctx->vy, ctx->vz, b->cfl_bits);
+  if (b->three_d) {
+    if (launch_max_reduce(L, false, ctx->vx, ctx->vy, ctx->vz, b->cfl_bits) != cudaSuccess) return AFID_E_CUDA;
+  } else {
+    if (cudaMemsetAsync(b->cfl_bits, 0, sizeof(unsigned long long) * b->nslots, st) != cudaSuccess)
+      return AFID_E_CUDA;
+    k_batch_cfl<<<dim3(kChunks, b->nslots), 256, 0, st>>>(L.g, L.t, ctx->vx, ctx->vy, ctx->vz, b->cfl_bits);
+  }
   k_batch_dt<<<(b->nslots + 127) / 128, 128, 0, st>>>(b->nslots, ctx->active_dev, b->ctl, b->cfl_bits, b->ntime,
                                                       b->dt, b->cfl, b->err);
   ctx->launches += 3;  // with k_batch_advance below
@@ -239,8 +263,33 @@ int enqueue_step(afid_batch_t *b) {
   int s = ctx_build_cn_batch(ctx, b->dt);
   for (int ns = 0; s == AFID_OK && ns < ctx->nsst; ++ns) s = ctx_run_substep(ctx, ns);
   if (s != AFID_OK) return s;
-  k_batch_advance<<<(b->nslots + 127) / 128, 128, 0, st>>>(b->nslots, ctx->active_dev, b->dt, b->time, b->ntime);
+  k_batch_advance<<<(b->nslots + 127) / 128, 128, 0, st>>>(b->nslots, ctx->active_dev, b->dt, b->time, b->ntime,
+                                                           b->limit);
   return cudaGetLastError() == cudaSuccess ? AFID_OK : AFID_E_CUDA;
+}
+
+// Copy one slot's fields between host (ld_x, ld_y, planes) and device (ldx, nym, planes).
+int copy_slot(afid_batch_t *b, int slot, double *const dev[5], const double *const hsrc[5], double *const hdst[5],
+              int ld_x, int ld_y) {
+  afid_ctx_t *ctx = b->ctx;
+  const Geom &g = ctx->L.g;
+  const size_t plane = (size_t)g.ldx * g.nym, hplane = (size_t)ld_x * ld_y;
+  const size_t dpitch = (size_t)g.ldx * sizeof(double), hpitch = (size_t)ld_x * sizeof(double);
+  const size_t w = (size_t)g.nx * sizeof(double);
+  const bool whole = (ld_y == g.nym);  // host planes back to back: one 2-D copy per field
+  for (int f = 0; f < 5; ++f) {
+    if (!(hsrc ? hsrc[f] : hdst[f])) continue;
+    for (int p = 0; p < (whole ? 1 : b->planes); ++p) {
+      double *d = dev[f] + plane * ((size_t)slot * b->planes + p);
+      const size_t rows = whole ? (size_t)g.nym * b->planes : (size_t)g.nym;
+      cudaError_t e = hsrc ? cudaMemcpy2DAsync(d, dpitch, hsrc[f] + hplane * p, hpitch, w, rows,
+                                               cudaMemcpyHostToDevice, ctx->stream)
+                           : cudaMemcpy2DAsync(hdst[f] + hplane * p, hpitch, d, dpitch, w, rows,
+                                               cudaMemcpyDeviceToHost, ctx->stream);
+      if (e != cudaSuccess) return ctx_fail(ctx, e);
+    }
+  }
+  return AFID_OK;
 }
 
 }  // namespace
@@ -253,8 +302,7 @@ int afid_batch_destroy(afid_batch_t *b) {
     cudaSetDevice(b->ctx->dev);
     cudaStreamSynchronize(b->ctx->stream);
   }
-  for (cudaGraphExec_t &g : b->graph)
-    if (g) cudaGraphExecDestroy(g);
+  drop_graphs(b);
   for (void *p : b->allocs) cudaFree(p);
   if (b->host) cudaFreeHost(b->host);
   if (b->ctx) afid_gpu_destroy(b->ctx);
@@ -264,13 +312,16 @@ int afid_batch_destroy(afid_batch_t *b) {
 }
 
 int afid_batch_create(const afid_input_t *proto, int nslots, int precision, afid_batch_t **out) {
-  if (!proto || !out || nslots < 1 || proto->nzm != 1 || proto->dpdz != 0.0) return AFID_E_INVALID;
+  if (!proto || !out || nslots < 1 || proto->nzm < 1 || proto->dpdz != 0.0) return AFID_E_INVALID;
+  if (proto->nzm > 1 && nslots != 1) return AFID_E_INVALID;  // a 3-D domain is a batch of one
   *out = nullptr;
   afid_batch_t *b = new (std::nothrow) afid_batch_t();
   if (!b) return AFID_E_ALLOC;
   b->proto = *proto;
   b->nslots = nslots;
   b->precision = precision;
+  b->three_d = proto->nzm > 1;
+  b->planes = proto->nzm;
   int s = afid_tables_create(proto, precision, &b->proto_tables);
   if (s != AFID_OK) {
     afid_batch_destroy(b);
@@ -279,40 +330,58 @@ int afid_batch_create(const afid_input_t *proto, int nslots, int precision, afid
   const int nym = proto->nym;
   InstScal sc{};
   InstCtl cc{};
-  std::vector<double> ak2, bp, tp;
-  if ((s = slot_tables(*proto, &sc, &ak2, &bp, &tp, &cc)) != AFID_OK || (int)ak2.size() < nym) {
-    afid_batch_destroy(b);
-    return s != AFID_OK ? s : AFID_E_INVALID;
-  }
+  scal_ctl(*proto, afid_tables_params(b->proto_tables), &sc, &cc);
   b->cfg.assign(nslots, *proto);
   b->inst_h.assign(nslots, sc);
   b->ctl_h.assign(nslots, cc);
   b->active_h.assign(nslots, 0);
-  std::vector<double> ak2_all((size_t)nslots * nym), bp_all((size_t)nslots * nym), tp_all((size_t)nslots * nym);
-  for (int i = 0; i < nslots; ++i) {
-    std::memcpy(&ak2_all[(size_t)i * nym], ak2.data(), nym * sizeof(double));
-    std::memcpy(&bp_all[(size_t)i * nym], bp.data(), nym * sizeof(double));
-    std::memcpy(&tp_all[(size_t)i * nym], tp.data(), nym * sizeof(double));
-  }
-  // The stacked geometry: z numbers the instances.
   afid_grid_t grid = *afid_tables_grid(b->proto_tables);
-  grid.nzm = nslots;
-  grid.zlen = (double)nslots;
   afid_params_t prm = *afid_tables_params(b->proto_tables);
   prm.precision = precision;
-  BatchSpec bs{nslots, b->inst_h.data(), ak2_all.data(), bp_all.data(), tp_all.data()};
-  if ((s = ctx_create(&grid, &prm, &bs, &b->ctx)) != AFID_OK) {
+  if (b->three_d) {
+    s = ctx_create(&grid, &prm, nullptr, &b->ctx);
+  } else {
+    std::vector<double> ak2, bp, tp;
+    if ((s = slot_tables(*proto, &sc, &ak2, &bp, &tp, &cc)) != AFID_OK || (int)ak2.size() < nym) {
+      afid_batch_destroy(b);
+      return s != AFID_OK ? s : AFID_E_INVALID;
+    }
+    std::vector<double> ak2_all((size_t)nslots * nym), bp_all((size_t)nslots * nym), tp_all((size_t)nslots * nym);
+    for (int i = 0; i < nslots; ++i) {
+      std::memcpy(&ak2_all[(size_t)i * nym], ak2.data(), nym * sizeof(double));
+      std::memcpy(&bp_all[(size_t)i * nym], bp.data(), nym * sizeof(double));
+      std::memcpy(&tp_all[(size_t)i * nym], tp.data(), nym * sizeof(double));
+    }
+    // The stacked geometry: z numbers the instances.
+    grid.nzm = nslots;
+    grid.zlen = (double)nslots;
+    BatchSpec bs{nslots, b->inst_h.data(), ak2_all.data(), bp_all.data(), tp_all.data()};
+    s = ctx_create(&grid, &prm, &bs, &b->ctx);
+  }
+  if (s != AFID_OK) {
     afid_batch_destroy(b);
     return s;
   }
-  cudaError_t e = cudaMemset(b->ctx->active_dev, 0, nslots);
+  cudaError_t e = cudaSuccess;
   auto chk = [&](cudaError_t r) { if (e == cudaSuccess) e = r; };
+  if (b->three_d) {
+    // device-side step control for the single domain: its scalars and one active flag
+    afid_ctx_t *ctx = b->ctx;
+    chk(balloc(b, &ctx->inst_dev, 1));
+    chk(balloc(b, &ctx->active_dev, 1));
+    if (e == cudaSuccess) e = cudaMemcpy(ctx->inst_dev, &sc, sizeof(InstScal), cudaMemcpyHostToDevice);
+    ctx->ninst = 1;
+    ctx->L.g.active = ctx->active_dev;
+  } else {
+    chk(cudaMemset(b->ctx->active_dev, 0, nslots));
+  }
   chk(balloc(b, &b->ctl, nslots));
   chk(balloc(b, &b->dt, nslots));
   chk(balloc(b, &b->time, nslots));
   chk(balloc(b, &b->cfl, nslots));
   chk(balloc(b, &b->ntime, nslots));
   chk(balloc(b, &b->err, nslots));
+  chk(balloc(b, &b->limit, nslots));
   chk(balloc(b, &b->cfl_bits, nslots));
   chk(balloc(b, &b->partial, (size_t)nslots * kChunks * 3));
   chk(balloc(b, &b->gsum, (size_t)nslots * 3));
@@ -343,21 +412,37 @@ int afid_batch_configure(afid_batch_t *b, int slot, const afid_input_t *in) {
   cudaSetDevice(ctx->dev);
   InstScal sc{};
   InstCtl cc{};
-  std::vector<double> ak2, bp, tp;
-  int s = slot_tables(*in, &sc, &ak2, &bp, &tp, &cc);
-  if (s != AFID_OK) return s;
-  const int nym = in->nym;
-  if ((int)ak2.size() < nym) return AFID_E_INVALID;
   if (cudaStreamSynchronize(ctx->stream) != cudaSuccess) return AFID_E_CUDA;
-  const Tables &t = ctx->L.t;
-  const size_t off = (size_t)slot * nym;
-  cudaError_t e = cudaMemcpy(ctx->inst_dev + slot, &sc, sizeof(InstScal), cudaMemcpyHostToDevice);
-  if (e == cudaSuccess)
-    e = cudaMemcpy(const_cast<double *>(t.ak2) + off, ak2.data(), nym * sizeof(double), cudaMemcpyHostToDevice);
-  if (e == cudaSuccess)
-    e = cudaMemcpy(const_cast<double *>(t.tempbp) + off, bp.data(), nym * sizeof(double), cudaMemcpyHostToDevice);
-  if (e == cudaSuccess)
-    e = cudaMemcpy(const_cast<double *>(t.temptp) + off, tp.data(), nym * sizeof(double), cudaMemcpyHostToDevice);
+  cudaError_t e = cudaSuccess;
+  if (b->three_d) {
+    // the domain's scalars are launch arguments: update them and re-capture the step
+    afid_tables_t *t = nullptr;
+    int s = afid_tables_create(in, b->precision, &t);
+    if (s != AFID_OK) return s;
+    afid_params_t prm = *afid_tables_params(t);
+    prm.precision = b->precision;
+    s = ctx_update_params(ctx, afid_tables_grid(t), &prm);
+    scal_ctl(*in, &prm, &sc, &cc);
+    afid_tables_destroy(t);
+    if (s != AFID_OK) return s;
+    drop_graphs(b);
+    e = cudaMemcpy(ctx->inst_dev, &sc, sizeof(InstScal), cudaMemcpyHostToDevice);
+  } else {
+    std::vector<double> ak2, bp, tp;
+    int s = slot_tables(*in, &sc, &ak2, &bp, &tp, &cc);
+    if (s != AFID_OK) return s;
+    const int nym = in->nym;
+    if ((int)ak2.size() < nym) return AFID_E_INVALID;
+    const Tables &t = ctx->L.t;
+    const size_t off = (size_t)slot * nym;
+    e = cudaMemcpy(ctx->inst_dev + slot, &sc, sizeof(InstScal), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess)
+      e = cudaMemcpy(const_cast<double *>(t.ak2) + off, ak2.data(), nym * sizeof(double), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess)
+      e = cudaMemcpy(const_cast<double *>(t.tempbp) + off, bp.data(), nym * sizeof(double), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess)
+      e = cudaMemcpy(const_cast<double *>(t.temptp) + off, tp.data(), nym * sizeof(double), cudaMemcpyHostToDevice);
+  }
   if (e == cudaSuccess) e = cudaMemcpy(b->ctl + slot, &cc, sizeof(InstCtl), cudaMemcpyHostToDevice);
   if (e != cudaSuccess) return ctx_fail(ctx, e);
   b->cfg[slot] = *in;
@@ -370,40 +455,24 @@ int afid_batch_upload(afid_batch_t *b, int slot, const double *vx, const double 
                       const double *temp, const double *pr, int ld_x, int ld_y) {
   if (!b || slot < 0 || slot >= b->nslots) return AFID_E_INVALID;
   afid_ctx_t *ctx = b->ctx;
-  const Geom &g = ctx->L.g;
-  if (ld_x < g.nx || ld_y < g.nym) return AFID_E_INVALID;
+  if (ld_x < ctx->L.g.nx || ld_y < ctx->L.g.nym) return AFID_E_INVALID;
   cudaSetDevice(ctx->dev);
-  const size_t plane = (size_t)g.ldx * g.nym * slot;
-  const double *src[5] = {vx, vy, vz, temp, pr};
-  double *dst[5] = {ctx->vx, ctx->vy, ctx->vz, ctx->temp, ctx->pr};
-  for (int f = 0; f < 5; ++f) {
-    if (!src[f]) continue;
-    cudaError_t e = cudaMemcpy2DAsync(dst[f] + plane, (size_t)g.ldx * sizeof(double), src[f],
-                                      (size_t)ld_x * sizeof(double), (size_t)g.nx * sizeof(double), g.nym,
-                                      cudaMemcpyHostToDevice, ctx->stream);
-    if (e != cudaSuccess) return ctx_fail(ctx, e);
-  }
-  return reset_slot(b, slot);
+  double *const dev[5] = {ctx->vx, ctx->vy, ctx->vz, ctx->temp, ctx->pr};
+  const double *const src[5] = {vx, vy, vz, temp, pr};
+  int s = copy_slot(b, slot, dev, src, nullptr, ld_x, ld_y);
+  return s != AFID_OK ? s : reset_slot(b, slot);
 }
 
 int afid_batch_download(afid_batch_t *b, int slot, double *vx, double *vy, double *vz, double *temp,
                         double *pr, int ld_x, int ld_y) {
   if (!b || slot < 0 || slot >= b->nslots) return AFID_E_INVALID;
   afid_ctx_t *ctx = b->ctx;
-  const Geom &g = ctx->L.g;
-  if (ld_x < g.nx || ld_y < g.nym) return AFID_E_INVALID;
+  if (ld_x < ctx->L.g.nx || ld_y < ctx->L.g.nym) return AFID_E_INVALID;
   cudaSetDevice(ctx->dev);
-  const size_t plane = (size_t)g.ldx * g.nym * slot;
-  double *dst[5] = {vx, vy, vz, temp, pr};
-  const double *src[5] = {ctx->vx, ctx->vy, ctx->vz, ctx->temp, ctx->pr};
-  for (int f = 0; f < 5; ++f) {
-    if (!dst[f]) continue;
-    cudaError_t e = cudaMemcpy2DAsync(dst[f], (size_t)ld_x * sizeof(double), src[f] + plane,
-                                      (size_t)g.ldx * sizeof(double), (size_t)g.nx * sizeof(double), g.nym,
-                                      cudaMemcpyDeviceToHost, ctx->stream);
-    if (e != cudaSuccess) return ctx_fail(ctx, e);
-  }
-  return afid_batch_synchronize(b);
+  double *const dev[5] = {ctx->vx, ctx->vy, ctx->vz, ctx->temp, ctx->pr};
+  double *const dst[5] = {vx, vy, vz, temp, pr};
+  int s = copy_slot(b, slot, dev, nullptr, dst, ld_x, ld_y);
+  return s != AFID_OK ? s : afid_batch_synchronize(b);
 }
 
 int afid_batch_seed(afid_batch_t *b, int slot, uint64_t seed) {
@@ -412,11 +481,21 @@ int afid_batch_seed(afid_batch_t *b, int slot, uint64_t seed) {
   int s = afid_tables_create(&b->cfg[slot], AFID_PREC_FP64, &t);
   if (s != AFID_OK) return s;
   const int nx = b->proto.nxm + 1, nym = b->proto.nym;
-  std::vector<double> temp((size_t)nx * nym, 0.0), zero((size_t)nx * nym, 0.0);
+  const size_t n = (size_t)nx * nym * b->planes;
+  std::vector<double> temp(n, 0.0), zero(n, 0.0);
   s = afid_initial_temperature(t, seed, 1e-3, temp.data(), nx, nym);
   afid_tables_destroy(t);
   if (s != AFID_OK) return s;
   return afid_batch_upload(b, slot, zero.data(), zero.data(), zero.data(), temp.data(), zero.data(), nx, nym);
+}
+
+int afid_batch_set_limit(afid_batch_t *b, int slot, int nsteps) {
+  if (!b || slot < 0 || slot >= b->nslots || nsteps < 0) return AFID_E_INVALID;
+  afid_ctx_t *ctx = b->ctx;
+  cudaSetDevice(ctx->dev);
+  cudaError_t e = cudaStreamSynchronize(ctx->stream);
+  if (e == cudaSuccess) e = cudaMemcpy(b->limit + slot, &nsteps, sizeof(int), cudaMemcpyHostToDevice);
+  return e == cudaSuccess ? AFID_OK : ctx_fail(ctx, e);
 }
 
 int afid_batch_set_active(afid_batch_t *b, const unsigned char *active) {
@@ -436,8 +515,9 @@ int afid_batch_step(afid_batch_t *b, int nsteps) {
   for (int n = 0; n < nsteps; ++n) {
     int p = (b->graph[0] && b->graph_temp[0] == ctx->temp) ? 0 : (b->graph[1] && b->graph_temp[1] == ctx->temp) ? 1 : -1;
     if (p < 0) {
-      // Capture the step for this temperature-buffer parity; the host pointers swap during the
-      // capture exactly as the replay will swap the device state.
+      // Capture the step for this temperature-buffer parity.  The capture swaps the host-side
+      // buffer pointers as the substeps do; they are put back, and swapped again below when
+      // the replay is issued.
       p = b->graph[0] ? 1 : 0;
       double *temp0 = ctx->temp, *tempo0 = ctx->temp_o;
       const long long l0 = ctx->launches;
@@ -446,7 +526,6 @@ int afid_batch_step(afid_batch_t *b, int nsteps) {
       if (e != cudaSuccess) return ctx_fail(ctx, e);
       int s = enqueue_step(b);
       e = cudaStreamEndCapture(ctx->stream, &graph);
-      // the capture advanced the host-side buffer parity; the replay below is what runs it
       ctx->temp = temp0;
       ctx->temp_o = tempo0;
       if (s != AFID_OK || e != cudaSuccess) {
@@ -485,14 +564,18 @@ int afid_batch_stats(afid_batch_t *b, afid_batch_stat_t *stats, double *nu_vol, 
   const int n = b->nslots;
   cudaStream_t st = ctx->stream;
   const LaunchCtx &L = ctx->L;
-  double *h = b->host;  // [dt | time | cfl | gsum(3) | ntime,err as ints]
+  double *h = b->host;  // [dt | time | cfl | gsum(3) | ntime, err as ints]
   cudaError_t e = cudaSuccess;
   if (nu_vol || ke) {
-    k_batch_globals<<<dim3(kChunks, n), 256, 0, st>>>(L.g, L.t, ctx->vx, ctx->vy, ctx->vz, ctx->temp, b->partial);
-    k_batch_gsum<<<n, 32, 0, st>>>(b->partial, kChunks, b->gsum);
+    if (b->three_d) {
+      e = launch_globals(L, ctx->vx, ctx->vy, ctx->vz, ctx->temp, ctx->partial, b->gsum);
+    } else {
+      k_batch_globals<<<dim3(kChunks, n), 256, 0, st>>>(L.g, L.t, ctx->vx, ctx->vy, ctx->vz, ctx->temp, b->partial);
+      k_batch_gsum<<<n, 32, 0, st>>>(b->partial, kChunks, b->gsum);
+      e = cudaGetLastError();
+    }
     b->launches += 2;
     ctx->launches += 2;
-    e = cudaGetLastError();
     if (e == cudaSuccess)
       e = cudaMemcpyAsync(h + 3 * (size_t)n, b->gsum, 3 * n * sizeof(double), cudaMemcpyDeviceToHost, st);
   }
@@ -505,8 +588,8 @@ int afid_batch_stats(afid_batch_t *b, afid_batch_stat_t *stats, double *nu_vol, 
   if (e != cudaSuccess) return ctx_fail(ctx, e);
   int s = afid_gpu_synchronize(ctx);
   if (s != AFID_OK) return s;
-  // GlobalQuantities.F90:27,63-74 with nzm = 1 per instance
-  const double vol = 1.0 / ((double)b->proto.nxm * (double)b->proto.nym);
+  // GlobalQuantities.F90:27,63-74
+  const double vol = 1.0 / ((double)b->proto.nxm * (double)b->proto.nym * (double)b->planes);
   for (int i = 0; i < n; ++i) {
     if (stats) {
       stats[i].dt = h[i];

@@ -71,7 +71,11 @@ __device__ __forceinline__ int wrap_dec(int a, int n) { return (a == 0) ? n - 1 
 // z neighbours: periodic for one domain, the instance itself in batch mode (2-D instances).
 __device__ __forceinline__ int zinc(const Geom &g, int i) { return g.batch ? i : wrap_inc(i, g.nzm); }
 __device__ __forceinline__ int zdec(const Geom &g, int i) { return g.batch ? i : wrap_dec(i, g.nzm); }
-__device__ __forceinline__ bool inst_active(const Geom &g, int i) { return !g.active || g.active[i] != 0; }
+// Batch mode: active[i] per instance (i = z index).  A single 3-D domain with step control on
+// the device uses active[0] for the whole domain.
+__device__ __forceinline__ bool inst_active(const Geom &g, int i) {
+  return !g.active || g.active[g.batch ? i : 0] != 0;
+}
 // Load the scalars of instance i into a block-local copy of the geometry (batch mode).
 __device__ __forceinline__ void bind_instance(Geom &g, int i) {
   if (g.inst) {

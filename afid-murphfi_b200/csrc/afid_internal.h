@@ -124,6 +124,7 @@ SubstepBuffers ctx_buffers(afid_ctx_t *ctx);
 int ctx_run_substep(afid_ctx_t *ctx, int ns);
 int ctx_build_cn_batch(afid_ctx_t *ctx, const double *dt_dev);
 int ctx_fail(afid_ctx_t *ctx, cudaError_t e);
+int ctx_update_params(afid_ctx_t *ctx, const afid_grid_t *grid, const afid_params_t *prm);
 
 }  // namespace afid
 

@@ -1,0 +1,350 @@
+// afid_serve.cpp — the request loop of include/afid_serve.h: pools of batches per size class,
+// admission by device-memory footprint, chunked replay, harvest of finished slots.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cstring>
+#include <deque>
+#include <new>
+#include <vector>
+
+#include "afid_batch.h"
+#include "afid_serve.h"
+
+namespace {
+
+// The inputs that decide which jobs can share a pool (afid_batch same-class rule).
+struct ClassKey {
+  int nxm, nym, nzm, istr3, nsst, active_t, gaxis, inslws, inslwn, tfixs, tfixn;
+  double alx3, str3, xplusu, xminusu, dpdy;
+  bool operator==(const ClassKey &o) const {
+    return nxm == o.nxm && nym == o.nym && nzm == o.nzm && istr3 == o.istr3 && nsst == o.nsst &&
+           active_t == o.active_t && gaxis == o.gaxis && inslws == o.inslws && inslwn == o.inslwn &&
+           tfixs == o.tfixs && tfixn == o.tfixn && alx3 == o.alx3 && str3 == o.str3 && xplusu == o.xplusu &&
+           xminusu == o.xminusu && dpdy == o.dpdy;
+  }
+};
+
+ClassKey key_of(const afid_input_t &in) {
+  ClassKey k{};
+  k.nxm = in.nxm;
+  k.nym = in.nym;
+  k.nzm = in.nzm;
+  k.istr3 = in.istr3;
+  k.nsst = in.nsst;
+  k.active_t = in.active_t;
+  k.gaxis = in.gaxis;
+  k.inslws = in.inslws;
+  k.inslwn = in.inslwn;
+  k.tfixs = in.tfixs;
+  k.tfixn = in.tfixn;
+  k.alx3 = in.alx3;
+  k.str3 = in.str3;
+  k.xplusu = in.xplusu;
+  k.xminusu = in.xminusu;
+  k.dpdy = in.dpdy;
+  return k;
+}
+
+struct Job {
+  afid_serve_job_t spec;
+  double t_submit = 0.0, t_admit = 0.0;
+  long long cells = 0;
+  long long order = 0;  // submission number
+};
+
+struct Pool {
+  ClassKey key;
+  afid_batch_t *b = nullptr;
+  cudaStream_t stream = nullptr;
+  int nslots = 0;
+  std::vector<int> job;  // index into Server::running per slot, -1 = free
+  std::vector<unsigned char> active;
+  long long bytes = 0;
+  long long cells_per_slot = 0;
+  bool dirty = false;  // active flags changed since the last upload
+  int busy() const { return (int)std::count_if(job.begin(), job.end(), [](int j) { return j >= 0; }); }
+};
+
+}  // namespace
+
+struct afid_server {
+  afid_serve_config_t cfg{};
+  std::chrono::steady_clock::time_point t0;
+  std::deque<Job> queue;
+  std::vector<Job> running;  // slots refer to entries here; freed entries are reused
+  std::vector<int> free_running;
+  std::vector<Pool *> pools;
+  std::vector<afid_serve_result_t> done;
+  long long submitted = 0;
+  long long cells_in_flight = 0;
+  long long cell_steps_done = 0;
+  long long jobs_done = 0;
+  std::vector<afid_batch_stat_t> st;
+  std::vector<double> nu, ke;
+};
+
+namespace {
+
+double now_s(const afid_server_t *s) {
+  return std::chrono::duration<double>(std::chrono::steady_clock::now() - s->t0).count();
+}
+
+long long pool_bytes(const afid_server_t *s) {
+  long long b = 0;
+  for (const Pool *p : s->pools) b += p->bytes;
+  return b;
+}
+
+void drop_pool(afid_server_t *s, size_t i) {
+  Pool *p = s->pools[i];
+  afid_batch_destroy(p->b);
+  if (p->stream) cudaStreamDestroy(p->stream);
+  delete p;
+  s->pools.erase(s->pools.begin() + (long)i);
+}
+
+// Create a pool for `in`'s class; AFID_E_CAPACITY when it does not fit the budget even after
+// releasing idle pools of other classes.
+int new_pool(afid_server_t *s, const afid_input_t &in, Pool **out) {
+  const int nslots = in.nzm > 1 ? 1 : std::max(1, s->cfg.slots_per_pool);
+  Pool *p = new (std::nothrow) Pool();
+  if (!p) return AFID_E_ALLOC;
+  p->key = key_of(in);
+  int st = afid_batch_create(&in, nslots, s->cfg.precision, &p->b);
+  if (st != AFID_OK) {
+    delete p;
+    return st;
+  }
+  p->bytes = afid_batch_device_bytes(p->b);
+  // release idle pools while over budget
+  while (pool_bytes(s) + p->bytes > s->cfg.hbm_budget_bytes) {
+    size_t victim = s->pools.size();
+    for (size_t i = 0; i < s->pools.size(); ++i)
+      if (s->pools[i]->busy() == 0) {
+        victim = i;
+        break;
+      }
+    if (victim == s->pools.size()) {
+      afid_batch_destroy(p->b);
+      delete p;
+      return AFID_E_CAPACITY;
+    }
+    drop_pool(s, victim);
+  }
+  if (cudaStreamCreateWithFlags(&p->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      afid_batch_set_stream(p->b, p->stream) != AFID_OK) {
+    afid_batch_destroy(p->b);
+    if (p->stream) cudaStreamDestroy(p->stream);
+    delete p;
+    return AFID_E_CUDA;
+  }
+  p->nslots = nslots;
+  p->job.assign(nslots, -1);
+  p->active.assign(nslots, 0);
+  p->cells_per_slot = (long long)in.nxm * in.nym * in.nzm;
+  s->pools.push_back(p);
+  *out = p;
+  return AFID_OK;
+}
+
+// Place job j into a free slot of its class (creating a pool if needed).
+int admit(afid_server_t *s, Job &j) {
+  const ClassKey k = key_of(j.spec.in);
+  Pool *pool = nullptr;
+  int slot = -1;
+  for (Pool *p : s->pools) {
+    if (!(p->key == k)) continue;
+    for (int i = 0; i < p->nslots; ++i)
+      if (p->job[i] < 0) {
+        pool = p;
+        slot = i;
+        break;
+      }
+    if (pool) break;
+  }
+  if (!pool) {
+    int st = new_pool(s, j.spec.in, &pool);
+    if (st != AFID_OK) return st;
+    slot = 0;
+  }
+  int st = afid_batch_configure(pool->b, slot, &j.spec.in);
+  if (st == AFID_OK) st = afid_batch_seed(pool->b, slot, j.spec.seed);
+  if (st == AFID_OK) st = afid_batch_set_limit(pool->b, slot, j.spec.nsteps);
+  if (st != AFID_OK) return st;
+  int idx;
+  if (!s->free_running.empty()) {
+    idx = s->free_running.back();
+    s->free_running.pop_back();
+  } else {
+    idx = (int)s->running.size();
+    s->running.emplace_back();
+  }
+  j.t_admit = now_s(s);
+  s->running[idx] = j;
+  pool->job[slot] = idx;
+  pool->active[slot] = 1;
+  pool->dirty = true;
+  s->cells_in_flight += j.cells;
+  return AFID_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int afid_serve_create(const afid_serve_config_t *cfg, afid_server_t **out) {
+  if (!cfg || !out || cfg->hbm_budget_bytes <= 0 || cfg->chunk_steps < 1 ||
+      (cfg->precision != AFID_PREC_FP64 && cfg->precision != AFID_PREC_MIXED))
+    return AFID_E_INVALID;
+  afid_server_t *s = new (std::nothrow) afid_server_t();
+  if (!s) return AFID_E_ALLOC;
+  s->cfg = *cfg;
+  if (s->cfg.slots_per_pool < 1) s->cfg.slots_per_pool = 1;
+  s->t0 = std::chrono::steady_clock::now();
+  *out = s;
+  return AFID_OK;
+}
+
+int afid_serve_destroy(afid_server_t *s) {
+  if (!s) return AFID_OK;
+  while (!s->pools.empty()) drop_pool(s, s->pools.size() - 1);
+  delete s;
+  return AFID_OK;
+}
+
+int afid_serve_submit(afid_server_t *s, const afid_serve_job_t *job) {
+  if (!s || !job || job->nsteps < 1 || job->in.nxm < 2 || job->in.nym < 1 || job->in.nzm < 1 ||
+      job->in.dpdz != 0.0)
+    return AFID_E_INVALID;
+  Job j;
+  j.spec = *job;
+  j.t_submit = now_s(s);
+  j.cells = (long long)job->in.nxm * job->in.nym * job->in.nzm;
+  j.order = s->submitted++;
+  s->queue.push_back(j);
+  return AFID_OK;
+}
+
+int afid_serve_pump(afid_server_t *s) {
+  if (!s) return AFID_E_INVALID;
+  // 1. admission in policy order
+  std::vector<size_t> order(s->queue.size());
+  for (size_t i = 0; i < order.size(); ++i) order[i] = i;
+  const bool fifo = s->cfg.policy != AFID_SERVE_SHORTEST_FIRST;
+  if (!fifo)
+    std::stable_sort(order.begin(), order.end(), [&](size_t a, size_t b) {
+      return (double)s->queue[a].cells * s->queue[a].spec.nsteps < (double)s->queue[b].cells * s->queue[b].spec.nsteps;
+    });
+  std::vector<char> taken(s->queue.size(), 0);
+  for (size_t q : order) {
+    Job &j = s->queue[q];
+    if (s->cfg.max_cells_in_flight > 0 && s->cells_in_flight > 0 &&
+        s->cells_in_flight + j.cells > s->cfg.max_cells_in_flight) {
+      if (fifo) break;
+      continue;
+    }
+    const int st = admit(s, j);
+    const bool no_room = (st == AFID_E_CAPACITY || st == AFID_E_ALLOC);
+    if (no_room && !s->pools.empty()) {  // wait for running jobs to release memory
+      if (fifo) break;
+      continue;
+    }
+    if (st != AFID_OK) {
+      // malformed, or larger than the whole budget: the job completes with the status
+      afid_serve_result_t r{};
+      r.tag = j.spec.tag;
+      r.errorcode = st;
+      r.t_submit = j.t_submit;
+      r.t_admit = r.t_done = now_s(s);
+      s->done.push_back(r);
+    }
+    taken[q] = 1;
+  }
+  std::deque<Job> rest;
+  for (size_t i = 0; i < s->queue.size(); ++i)
+    if (!taken[i]) rest.push_back(s->queue[i]);
+  s->queue.swap(rest);
+
+  // 2. one chunk of steps on every pool with running jobs (each pool on its own stream)
+  for (Pool *p : s->pools) {
+    if (p->busy() == 0) continue;
+    int st = AFID_OK;
+    if (p->dirty) {
+      st = afid_batch_set_active(p->b, p->active.data());
+      p->dirty = false;
+    }
+    if (st == AFID_OK) st = afid_batch_step(p->b, s->cfg.chunk_steps);
+    if (st != AFID_OK) return st;
+  }
+
+  // 3. harvest the slots that reached their step count or stopped on an error code
+  for (Pool *p : s->pools) {
+    if (p->busy() == 0) continue;
+    s->st.resize(p->nslots);
+    s->nu.resize(p->nslots);
+    s->ke.resize(p->nslots);
+    int st = afid_batch_stats(p->b, s->st.data(), s->nu.data(), s->ke.data());
+    if (st != AFID_OK) return st;
+    for (int i = 0; i < p->nslots; ++i) {
+      const int idx = p->job[i];
+      if (idx < 0) continue;
+      Job &j = s->running[idx];
+      const afid_batch_stat_t &x = s->st[i];
+      if (x.ntime < j.spec.nsteps && x.errorcode == 0) continue;
+      if (j.spec.temp_out) {
+        const int nx = j.spec.in.nxm + 1;
+        st = afid_batch_download(p->b, i, nullptr, nullptr, nullptr, j.spec.temp_out, nullptr, nx, j.spec.in.nym);
+        if (st != AFID_OK) return st;
+      }
+      afid_serve_result_t r{};
+      r.tag = j.spec.tag;
+      r.errorcode = x.errorcode;
+      r.steps_done = x.ntime;
+      r.time = x.time;
+      r.dt = x.dt;
+      r.cfl = x.cfl;
+      r.nu_vol = s->nu[i];
+      r.ke = s->ke[i];
+      r.t_submit = j.t_submit;
+      r.t_admit = j.t_admit;
+      r.t_done = now_s(s);
+      s->done.push_back(r);
+      s->cells_in_flight -= j.cells;
+      s->cell_steps_done += j.cells * (long long)x.ntime;
+      s->jobs_done += 1;
+      p->job[i] = -1;
+      p->active[i] = 0;
+      p->dirty = true;
+      s->free_running.push_back(idx);
+    }
+  }
+  return AFID_OK;
+}
+
+int afid_serve_poll(afid_server_t *s, afid_serve_result_t *out, int max, int *n) {
+  if (!s || !n || (max > 0 && !out)) return AFID_E_INVALID;
+  const int k = std::min<int>(max, (int)s->done.size());
+  for (int i = 0; i < k; ++i) out[i] = s->done[i];
+  s->done.erase(s->done.begin(), s->done.begin() + k);
+  *n = k;
+  return AFID_OK;
+}
+
+int afid_serve_status(const afid_server_t *s, afid_serve_status_t *st) {
+  if (!s || !st) return AFID_E_INVALID;
+  st->queued = (int)s->queue.size();
+  st->running = 0;
+  for (const Pool *p : s->pools) st->running += p->busy();
+  st->pools = (int)s->pools.size();
+  st->device_bytes = pool_bytes(s);
+  st->cells_in_flight = s->cells_in_flight;
+  st->cell_steps_done = s->cell_steps_done;
+  st->jobs_done = s->jobs_done;
+  return AFID_OK;
+}
+
+double afid_serve_now(const afid_server_t *s) { return s ? now_s(s) : 0.0; }
+
+}  // extern "C"

@@ -485,6 +485,131 @@ def run_batched(args):
         dist.destroy_process_group()
 
 
+# ---- served stream: Poisson arrivals of 2-D and 3-D jobs -----------------------------------
+SERVE_SEED = BATCH_SEED + 1
+
+
+def serve_jobs(n: int, rate: float = 50.0, seed: int = SERVE_SEED):
+    """Job j draws from the Philox stream keyed by ``seed`` at counters 8j .. 8j+7: exponential
+    inter-arrival at ``rate``/s, 2-D (90%, sizes/Ra/Pr/aspect as the batched sweep) or 3-D
+    (96 x 128 x 128 wall-normal x horizontal, log10 Ra ~ U[6, 8], Pr 1), steps ~ U[500, 5000]."""
+    import afid_gpu as ag
+    u = lambda j, d: ag.lib().afid_philox_uniform(seed, 8 * j + d)  # noqa: E731
+    jobs, t = [], 0.0
+    for j in range(n):
+        t += -math.log(1.0 - u(j, 0)) / rate
+        nsteps = 500 + min(int(u(j, 1) * 4501), 4500)
+        if u(j, 2) < 0.9:
+            nym, nxm = BATCH_SIZES[min(int(u(j, 3) * 4), 3)]
+            job = dict(nxm=nxm, nym=nym, nzm=1, rayt=10.0 ** (6.0 + 4.0 * u(j, 4)),
+                       prat=BATCH_PR[min(int(u(j, 5) * 3), 2)], ylen=BATCH_ASPECT[min(int(u(j, 6) * 3), 2)],
+                       zlen=1.0)
+        else:
+            job = dict(nxm=96, nym=128, nzm=128, rayt=10.0 ** (6.0 + 2.0 * u(j, 4)), prat=1.0, ylen=1.0, zlen=1.0)
+        job.update(index=j, arrival=t, nsteps=nsteps, seed=SERVE_SEED + 1 + j)
+        jobs.append(job)
+    return jobs
+
+
+def serve_bou(job: dict) -> str:
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from helpers import bou_text as _bt  # noqa: E402
+    dtmax = diffusive_dtmax(job["nym"], job["ylen"], job["rayt"], job["prat"])
+    if job["nzm"] > 1:
+        dtmax = min(dtmax, diffusive_dtmax(job["nzm"], job["zlen"], job["rayt"], job["prat"]))
+    return _bt(job["nxm"], job["nym"], job["nzm"], rayt=job["rayt"], prat=job["prat"], ylen=job["ylen"],
+               zlen=job["zlen"], istr3=4, str3=2.0, idtv=1, dt=min(1e-4, dtmax), cflmax=1.2, dtmax=dtmax,
+               ntst=1000000, resid=1e-3)
+
+
+def run_served(args):
+    import numpy as np
+    import torch
+    import afid_gpu as ag
+
+    world, rank, local = dist_setup()
+    jobs = serve_jobs(args.jobs)
+    inputs = [ag.parse_bou_in(serve_bou(j)) for j in jobs]
+    policy = ag.SERVE_SHORTEST_FIRST if args.policy == "shortest" else ag.SERVE_FIFO
+    free, _ = torch.cuda.mem_get_info()
+    budget = int(min(free * 0.8, 120e9))
+    srv = ag.Server(ag.PREC_MIXED, hbm_budget_bytes=budget, slots_per_pool=args.slots, chunk_steps=args.chunk,
+                    max_cells_in_flight=args.max_cells, policy=policy)
+    # warm-up: a few 3-step jobs (device context, allocator, first captures)
+    for k, inp in enumerate(inputs[: min(4, len(inputs))]):
+        srv.submit(inp, 1, 3, 10_000_000 + k)
+    while True:
+        srv.pump()
+        srv.poll()
+        st = srv.status()
+        if st["running"] + st["queued"] == 0:
+            break
+    clocks = ClockSampler(torch.cuda.current_device())
+    barrier(world)
+    torch.cuda.synchronize()
+    clocks.start()
+    t0 = srv.now()
+    nxt, results = 0, {}
+    while len(results) < len(jobs):
+        now = srv.now() - t0
+        while nxt < len(jobs) and jobs[nxt]["arrival"] <= now:
+            srv.submit(inputs[nxt], jobs[nxt]["seed"], jobs[nxt]["nsteps"], nxt)
+            nxt += 1
+        st = srv.status()
+        if st["running"] == 0 and st["queued"] == 0 and nxt < len(jobs):
+            time.sleep(max(0.0, jobs[nxt]["arrival"] - (srv.now() - t0)))
+            continue
+        srv.pump()
+        for r in srv.poll():
+            results[r["tag"]] = r
+    t_end = srv.now() - t0
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    status = srv.status()
+    srv.close()
+    lat = np.array([results[j["index"]]["t_done"] - t0 - j["arrival"] for j in jobs])
+    wait = np.array([results[j["index"]]["t_admit"] - t0 - j["arrival"] for j in jobs])
+    cell_steps = sum(j["nxm"] * j["nym"] * j["nzm"] * results[j["index"]]["steps_done"] for j in jobs)
+    value = cell_steps / t_end / 1e6
+    errors = sum(1 for r in results.values() if r["errorcode"] != 0)
+    offered = sum(j["nxm"] * j["nym"] * j["nzm"] * j["nsteps"] for j in jobs) / jobs[-1]["arrival"] / 1e6
+    if rank == 0:
+        line = {
+            "metric": "Mcell-RK3-steps/s; p50/p99 job latency",
+            "value": round(value, 3),
+            "unit": "Mcell-RK3-steps/s",
+            "n_gpus": world,
+            "steps": len(jobs),
+            "warmup": 4,
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f32+f64",
+            "data": "synthetic: Poisson arrivals (50/s), Philox-drawn 2-D/3-D RBC jobs, seeded conductive IC",
+            "config": {"workload": f"served_{len(jobs)}jobs_poisson50", "jobs": len(jobs),
+                       "mix": {"2d": sum(1 for j in jobs if j["nzm"] == 1), "3d_96x128x128": sum(1 for j in jobs if j["nzm"] > 1)},
+                       "policy": args.policy, "chunk_steps": args.chunk, "slots_per_pool": args.slots,
+                       "max_cells_in_flight": args.max_cells, "hbm_budget_bytes": budget,
+                       "offered_load_mcell_steps_per_s": round(offered, 1),
+                       "l2": "resident state larger than L2",
+                       "parallelism": "replicas" if world > 1 else "single GPU"},
+            "latency_s": {"p50": round(float(np.percentile(lat, 50)), 3), "p99": round(float(np.percentile(lat, 99)), 3),
+                          "mean": round(float(lat.mean()), 3), "max": round(float(lat.max()), 3)},
+            "queue_wait_s": {"p50": round(float(np.percentile(wait, 50)), 3), "p99": round(float(np.percentile(wait, 99)), 3)},
+            "horizon_s": round(t_end, 3),
+            "e2e": {"value": round(value, 3), "unit": "Mcell-RK3-steps/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0,
+                    "note": "served loop: host submission -> result on host; initial states built on the host and uploaded per job"},
+            "jobs_with_error": errors,
+            "peak_device_bytes": status["device_bytes"],
+            "clocks": clk,
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
 def cpu_baseline(w: dict, steps: int, budget_s: float = 60.0):
     """The CPU restatement (C + OpenMP, oracle/afid_cpu.c) on the same workload: up to
     ``steps`` full main-loop steps, stopping once ``budget_s`` seconds have been spent."""
@@ -538,8 +663,13 @@ def main():
     ap.add_argument("--steps", type=int, default=30)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="afid", choices=["afid", "reference"])
-    ap.add_argument("--config", default="rbc3d", choices=sorted(WORKLOADS) + ["batched", "batched_fp64"])
+    ap.add_argument("--config", default="rbc3d", choices=sorted(WORKLOADS) + ["batched", "batched_fp64", "served"])
     ap.add_argument("--no-nu-check", action="store_true")
+    ap.add_argument("--jobs", type=int, default=100, help="served: number of jobs")
+    ap.add_argument("--chunk", type=int, default=50, help="served: steps per pump")
+    ap.add_argument("--slots", type=int, default=32, help="served: 2-D slots per pool")
+    ap.add_argument("--max-cells", type=int, default=0, help="served: cells-in-flight cap (0 = memory only)")
+    ap.add_argument("--policy", default="fifo", choices=["fifo", "shortest"])
     ap.add_argument("--cpu-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
@@ -549,6 +679,8 @@ def main():
         run_reference(args)
     elif args.config.startswith("batched"):
         run_batched(args)
+    elif args.config == "served":
+        run_served(args)
     else:
         run_gpu(args)
 

@@ -1,5 +1,6 @@
 /*
- * afid_batch.h — many independent 2-D convection instances of one size class on one GPU.
+ * afid_batch.h — many independent 2-D convection instances of one size class on one GPU
+ * (or one 3-D domain) with the main-loop step control on the device.
  *
  * The reference runs one domain per MPI job (main.F90); there is no batched form in it.  This
  * API advances up to thousands of 2-D Rayleigh-Benard instances together: instances that share
@@ -10,6 +11,9 @@
  * (CFL -> dt) runs on the device, so a step is a fixed launch sequence captured once in a CUDA
  * graph and replayed.  Instances never exchange data: an instance's result does not depend on
  * which other instances are active in the same batch.
+ *
+ * A batch created from a bou.in with NZM > 1 holds one 3-D domain (nslots = 1): the same
+ * device-side CFL -> dt rule and captured step, so served 3-D jobs run like 2-D slots.
  *
  * Slots: a batch has a fixed number of instance slots; idle slots cost no work.  A slot is
  * (re)configured with afid_batch_configure, loaded with afid_batch_seed or afid_batch_upload,
@@ -37,8 +41,8 @@ typedef struct afid_batch_stat {
   double cfl;       /* last CFL number (CalcMaxCFL) */
 } afid_batch_stat_t;
 
-/* nslots instance slots of the size class of `proto` (nxm, nym, alx3, istr3, str3; nzm must be 1).
- * All slots start configured from `proto`, zero state, inactive. */
+/* nslots instance slots of the size class of `proto` (nxm, nym, nzm, alx3, istr3, str3); nzm > 1
+ * requires nslots = 1.  All slots start configured from `proto`, zero state, inactive, no limit. */
 int afid_batch_create(const afid_input_t *proto, int nslots, int precision, afid_batch_t **out);
 int afid_batch_destroy(afid_batch_t *b);
 int afid_batch_set_stream(afid_batch_t *b, void *stream);
@@ -52,6 +56,9 @@ int afid_batch_upload(afid_batch_t *b, int slot, const double *vx, const double 
                       const double *temp, const double *pr, int ld_x, int ld_y);
 int afid_batch_download(afid_batch_t *b, int slot, double *vx, double *vy, double *vz, double *temp,
                         double *pr, int ld_x, int ld_y);
+/* The slot switches itself off after `nsteps` steps counted from its last load (seed/upload);
+ * 0 = no limit.  Lets slots with different step budgets share replayed multi-step chunks. */
+int afid_batch_set_limit(afid_batch_t *b, int slot, int nsteps);
 /* active[nslots]: nonzero = advance.  Takes effect for the next step. */
 int afid_batch_set_active(afid_batch_t *b, const unsigned char *active);
 /* nsteps main-loop steps (CFL, dt rule, TimeMarcher) of every active slot; asynchronous on the

@@ -183,3 +183,69 @@ def test_batched_mixed_nusselt_within_half_percent():
     n32 = nus[ag.PREC_MIXED][tail:].mean(axis=0)
     assert (n64 > 2.0).sum() >= 4, n64
     assert np.all(np.abs(n32 - n64) / n64 < 5e-3), (n32, n64)
+
+
+@pytest.mark.parametrize("precision", [ag.PREC_FP64, ag.PREC_MIXED])
+def test_three_d_batch_of_one_matches_single_domain(precision):
+    """A 3-D domain as a batch of one (device-side dt rule, captured step), reconfigured to a
+    second Ra/Pr/aspect, against the single-domain API with the dt rule on the host."""
+    shape, nsteps = (24, 32, 16), 12
+    first = dict(rayt=1e5, prat=1.0, ylen=1.0, zlen=1.0)
+    second = dict(rayt=4e6, prat=0.7, ylen=2.0, zlen=1.0)
+    step = dict(idtv=1, dt=1e-3, cflmax=1.2, dtmax=2e-3)
+    inp1 = ag.parse_bou_in(bou_text(*shape, **dict(step, **first)))
+    inp2 = ag.parse_bou_in(bou_text(*shape, **dict(step, **second)))
+    with ag.Batch(inp1, 1, precision) as b:
+        b.seed(0, 5)  # run the first configuration, then switch: the step graph is re-captured
+        b.set_active([1])
+        b.step(3)
+        b.configure(0, inp2)
+        b.seed(0, 77)
+        rng = np.random.default_rng(3)
+        f = b.download(0)
+        f["vy"][..., :shape[0]] = 0.05 * rng.standard_normal(f["vy"][..., :shape[0]].shape)
+        b.upload(0, f["vx"], f["vy"], f["vz"], f["temp"], f["pr"])
+        init = b.download(0)
+        b.set_active([1])
+        b.step(nsteps)
+        got = b.download(0)
+        st = b.stats()
+    case = Case(*shape, precision=precision, **dict(step, **second))
+    dt = ctypes.c_double(case.p.dt)
+    with case.solver() as g:
+        g.upload(*(init[k] for k in ag.Solver.FIELDS))
+        for n in range(nsteps):
+            cfl = g.calc_max_cfl()
+            ag.lib().afid_next_dt(ctypes.byref(case.inp), n, ctypes.byref(dt), cfl, None)
+            g.time_marcher(dt.value, n)
+        ref = g.download()
+        nu, ke, _ = g.global_quantities(case.p.prat * abs(case.p.rayt))
+    nxm = shape[0]
+    for k in ("vx", "vy", "vz", "temp"):
+        assert np.array_equal(got[k][..., :nxm], ref[k][..., :nxm]), k
+    assert st["ntime"][0] == nsteps
+    assert st["nu_vol"][0] == nu and st["ke"][0] == ke
+
+
+def test_step_limit_stops_slot_exactly():
+    with _batch(ag.PREC_FP64) as b:
+        for s in range(b.nslots):
+            _perturb(b, s)
+        b.set_limit(1, 7)
+        b.set_active(np.ones(b.nslots, np.uint8))
+        b.step(20)
+        got = b.download(1)
+        st = b.stats()
+    with _batch(ag.PREC_FP64) as b:
+        for s in range(b.nslots):
+            _perturb(b, s)
+        act = np.zeros(b.nslots, np.uint8)
+        act[1] = 1
+        b.set_active(act)
+        b.step(7)
+        ref = b.download(1)
+        st_ref = b.stats()
+    assert st["ntime"][1] == 7 and st["ntime"][0] == 20
+    for k in ag.Batch.FIELDS:
+        assert np.array_equal(got[k][:, :NXM], ref[k][:, :NXM]), k
+    assert st["time"][1] == st_ref["time"][1]
