@@ -85,6 +85,15 @@ class BatchStatT(C.Structure):
                 ("dt", C.c_double), ("cfl", C.c_double)]
 
 
+class TuneInfoT(C.Structure):
+    _fields_ = [("ncand", C.c_int), ("chosen", C.c_int), ("sample_columns", C.c_int),
+                ("threads", C.c_int * 3), ("rows", C.c_int * 3), ("us", C.c_double * 3)]
+
+    def as_dict(self) -> dict:
+        return {"ncand": self.ncand, "chosen": self.chosen, "sample_columns": self.sample_columns,
+                "shapes": [[self.threads[v], self.rows[v], round(self.us[v], 2)] for v in range(self.ncand)]}
+
+
 class ServeConfigT(C.Structure):
     _fields_ = [("precision", C.c_int), ("hbm_budget_bytes", C.c_longlong), ("slots_per_pool", C.c_int),
                 ("chunk_steps", C.c_int), ("max_cells_in_flight", C.c_longlong), ("policy", C.c_int)]
@@ -126,7 +135,8 @@ EXPORTS = [
     "afid_batch_set_limit",
     "afid_batch_device_bytes", "afid_batch_launch_count",
     "afid_serve_create", "afid_serve_destroy", "afid_serve_submit", "afid_serve_pump", "afid_serve_poll",
-    "afid_serve_status", "afid_serve_now",
+    "afid_serve_status", "afid_serve_now", "afid_gpu_autotune", "afid_batch_autotune",
+    "afid_gpu_set_k1_shape",
 ]
 
 
@@ -184,6 +194,9 @@ def load_library(path: str = _LIB_PATH) -> C.CDLL:
         "afid_serve_poll": (i, [vp, C.POINTER(ServeResultT), i, C.POINTER(i)]),
         "afid_serve_status": (i, [vp, C.POINTER(ServeStatusT)]),
         "afid_serve_now": (d, [vp]),
+        "afid_gpu_autotune": (i, [vp, i, C.POINTER(TuneInfoT)]),
+        "afid_gpu_set_k1_shape": (i, [vp, i]),
+        "afid_batch_autotune": (i, [vp, i, C.POINTER(TuneInfoT)]),
         "afid_batch_step": (i, [vp, i]),
         "afid_batch_synchronize": (i, [vp]),
         "afid_batch_stats": (i, [vp, C.POINTER(BatchStatT), _dp, _dp]),
@@ -348,6 +361,14 @@ class Solver:
     PROFILE_CLASSES = ("cn_tables", "explicit_implicit", "div_fft_y", "fft_z_fwd", "tridiag_pressure",
                        "fft_z_inv", "ifft_y", "correct", "reductions")
 
+    def autotune(self, force: bool = False) -> dict:
+        info = TuneInfoT()
+        _check(lib().afid_gpu_autotune(self._h, int(force), C.byref(info)), "afid_gpu_autotune")
+        return info.as_dict()
+
+    def set_k1_shape(self, index: int) -> None:
+        _check(lib().afid_gpu_set_k1_shape(self._h, index), "afid_gpu_set_k1_shape")
+
     def profile(self, enable: bool = True) -> None:
         _check(lib().afid_gpu_profile_enable(self._h, int(enable)), "afid_gpu_profile_enable")
 
@@ -450,6 +471,11 @@ class Batch:
 
     def device_bytes(self) -> int:
         return int(lib().afid_batch_device_bytes(self._h))
+
+    def autotune(self, force: bool = False) -> dict:
+        info = TuneInfoT()
+        _check(lib().afid_batch_autotune(self._h, int(force), C.byref(info)), "afid_batch_autotune")
+        return info.as_dict()
 
     def launch_count(self) -> int:
         return int(lib().afid_batch_launch_count(self._h))

@@ -5,6 +5,7 @@ the outputs next to this file, so they travel with the source tree.
 """
 from __future__ import annotations
 
+import concurrent.futures
 import os
 import subprocess
 import sys
@@ -22,7 +23,8 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 CUFLAGS = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", "-I" + INC, "-I" + CSRC] + ARCH
 CXXFLAGS = ["-std=c++17", "-O2", "-fPIC", "-I" + INC, "-I/usr/local/cuda/include"]
 
-SOURCES = ["afid_kernels.cu", "afid_api.cu", "afid_noalloc.cu", "afid_batch.cu", "afid_host.cpp", "afid_serve.cpp"]
+SOURCES = ["afid_k1_fp64.cu", "afid_k1_mixed.cu", "afid_kernels.cu", "afid_api.cu", "afid_noalloc.cu",
+           "afid_batch.cu", "afid_host.cpp", "afid_serve.cpp"]
 
 
 def _newer(target: str, deps) -> bool:
@@ -47,7 +49,7 @@ def _run(cmd, verbose):
 def build(verbose: bool = False, force: bool = False) -> str:
     os.makedirs(BUILD, exist_ok=True)
     headers = _headers()
-    objs = []
+    objs, jobs = [], []
     for src in SOURCES:
         s = os.path.join(CSRC, src)
         o = os.path.join(BUILD, src + ".o")
@@ -55,9 +57,13 @@ def build(verbose: bool = False, force: bool = False) -> str:
         if not force and _newer(o, [s] + headers):
             continue
         if src.endswith(".cu"):
-            _run([NVCC] + CUFLAGS + ["-c", s, "-o", o], verbose)
+            jobs.append([NVCC] + CUFLAGS + ["-c", s, "-o", o])
         else:
-            _run(["g++"] + CXXFLAGS + ["-c", s, "-o", o], verbose)
+            jobs.append(["g++"] + CXXFLAGS + ["-c", s, "-o", o])
+    # translation units compile independently: run them side by side
+    with concurrent.futures.ThreadPoolExecutor(max_workers=max(1, min(len(jobs), os.cpu_count() or 1))) as ex:
+        for f in [ex.submit(_run, cmd, verbose) for cmd in jobs]:
+            f.result()
     if force or not _newer(LIB, objs):
         _run([NVCC] + ARCH + ["-shared", "-o", LIB] + objs + ["-cudart", "static"], verbose)
     run_src = os.path.join(CSRC, "afid_run.cpp")

@@ -466,6 +466,7 @@ int ctx_create(const afid_grid_t *grid, const afid_params_t *prm, const BatchSpe
     L.g.active = ctx->active_dev;
   }
   L.warp_fft = true;
+  L.k1_var = 0;
   L.plan_y = py;
   L.plan_z = pz;
   L.twy = twy;
@@ -477,6 +478,74 @@ int ctx_create(const afid_grid_t *grid, const afid_params_t *prm, const BatchSpe
 SubstepBuffers ctx_buffers(afid_ctx_t *ctx) { return buffers(ctx); }
 int ctx_run_substep(afid_ctx_t *ctx, int ns) { return run_substep(ctx, ns); }
 int ctx_fail(afid_ctx_t *ctx, cudaError_t e) { return fail_cuda(ctx, e); }
+
+// Time every K1 thread shape on the first `sample` columns and keep the fastest.  The RK3
+// histories point at scratch memory for these launches (K1 updates them in place); the other
+// outputs are intermediates of the next substep or the idle temperature buffer, which the next
+// K1 overwrites, so the state is untouched.  Idle batch slots are timed as active.
+int ctx_autotune(afid_ctx_t *ctx, bool force) {
+  if (ctx->tuned && !force) return AFID_OK;
+  LaunchCtx L = ctx->L;
+  int tpc[AFID_TUNE_MAX] = {0}, rpt[AFID_TUNE_MAX] = {0};
+  const int n = k1_shapes(L.M, tpc, rpt);
+  afid_tune_info_t info{};
+  info.ncand = n;
+  const int ncol = L.g.nym * L.g.nzm;
+  const int sample = std::min(ncol, 148 * 24);
+  info.sample_columns = sample;
+  for (int v = 0; v < AFID_TUNE_MAX; ++v) {
+    info.threads[v] = v < n ? tpc[v] : 0;
+    info.rows[v] = v < n ? rpt[v] : 0;
+    info.us[v] = -1.0;
+  }
+  if (n > 1) {
+    const size_t tsz = L.mixed ? sizeof(float) : sizeof(double);
+    const size_t per = (size_t)sample * L.g.ldx * tsz;
+    char *scratch = nullptr;
+    AFID_CUDA(ctx, cudaMalloc(&scratch, 4 * per));
+    SubstepBuffers b = buffers(ctx);
+    b.rux = scratch;
+    b.ruy = scratch + per;
+    b.ruz = scratch + 2 * per;
+    b.rut = scratch + 3 * per;
+    L.g.active = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    cudaError_t e = cudaMemsetAsync(scratch, 0, 4 * per, ctx->stream);
+    if (e == cudaSuccess) e = cudaEventCreate(&e0);
+    if (e == cudaSuccess) e = cudaEventCreate(&e1);
+    double best = 1e300;
+    constexpr int kReps = 5;
+    for (int v = 0; v < n && e == cudaSuccess; ++v) {
+      auto run = [&] { return L.mixed ? launch_k1_mixed(L, b, 0, v, sample) : launch_k1_fp64(L, b, 0, v, sample); };
+      if (run() != cudaSuccess) {  // this shape does not fit the device: skip it
+        cudaGetLastError();
+        continue;
+      }
+      ctx->launches += 1 + kReps;
+      cudaEventRecord(e0, ctx->stream);
+      for (int r = 0; r < kReps; ++r) run();
+      cudaEventRecord(e1, ctx->stream);
+      e = cudaEventSynchronize(e1);
+      float ms = 0.f;
+      if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+      if (e != cudaSuccess) break;
+      info.us[v] = 1e3 * ms / kReps;
+      if (info.us[v] < best) {
+        best = info.us[v];
+        info.chosen = v;
+      }
+    }
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    cudaError_t ef = cudaFree(scratch);
+    if (e == cudaSuccess) e = ef;
+    if (e != cudaSuccess) return fail_cuda(ctx, e);
+  }
+  ctx->L.k1_var = info.chosen;
+  ctx->tune = info;
+  ctx->tuned = true;
+  return check_err_flag(ctx);
+}
 
 // New physics for a single-domain context of the same grid (sizes and wall-normal tables
 // unchanged): scalars, wavenumbers and plate temperatures.  Launches captured before this call
@@ -613,6 +682,7 @@ int afid_gpu_timemarcher(afid_ctx_t *ctx, double dt, int ntime) {
   const double beta = dt / ctx->L.g.ren * 0.5;  // TimeMarcher.F90:28
   int s;
   if ((s = build_cn(ctx, 0, ctx->nsst, alm, gam, rom, dt, beta)) != AFID_OK) return s;
+  if ((s = ctx_autotune(ctx, false)) != AFID_OK) return s;
   for (int ns = 0; ns < ctx->nsst; ++ns)
     if ((s = run_substep(ctx, ns)) != AFID_OK) return s;
   return AFID_OK;
@@ -623,6 +693,7 @@ int afid_gpu_substep(afid_ctx_t *ctx, int ns, double al, double ga, double ro, d
   cudaSetDevice(ctx->dev);
   int s;
   if ((s = build_cn(ctx, ns, 1, &al, &ga, &ro, dt, beta)) != AFID_OK) return s;
+  if ((s = ctx_autotune(ctx, false)) != AFID_OK) return s;
   return run_substep(ctx, ns);
 }
 
@@ -687,6 +758,33 @@ int afid_gpu_field_device_ptr(afid_ctx_t *ctx, int which, void **dptr, int *ldx)
 }
 
 long long afid_gpu_launch_count(afid_ctx_t *ctx) { return ctx ? ctx->launches : 0; }
+
+int afid_gpu_set_k1_shape(afid_ctx_t *ctx, int index) {
+  if (!ctx) return AFID_E_INVALID;
+  int tpc[AFID_TUNE_MAX], rpt[AFID_TUNE_MAX];
+  const int n = k1_shapes(ctx->L.M, tpc, rpt);
+  if (index < 0 || index >= n) return AFID_E_INVALID;
+  afid_tune_info_t info{};
+  info.ncand = n;
+  info.chosen = index;
+  for (int v = 0; v < AFID_TUNE_MAX; ++v) {
+    info.threads[v] = v < n ? tpc[v] : 0;
+    info.rows[v] = v < n ? rpt[v] : 0;
+    info.us[v] = -1.0;
+  }
+  ctx->tune = info;
+  ctx->L.k1_var = index;
+  ctx->tuned = true;
+  return AFID_OK;
+}
+
+int afid_gpu_autotune(afid_ctx_t *ctx, int force, afid_tune_info_t *info) {
+  if (!ctx) return AFID_E_INVALID;
+  cudaSetDevice(ctx->dev);
+  const int s = ctx_autotune(ctx, force != 0);
+  if (info) *info = ctx->tune;
+  return s;
+}
 
 int afid_gpu_profile_enable(afid_ctx_t *ctx, int enable) {
   if (!ctx) return AFID_E_INVALID;

@@ -512,6 +512,10 @@ int afid_batch_step(afid_batch_t *b, int nsteps) {
   if (!b || nsteps < 0) return AFID_E_INVALID;
   afid_ctx_t *ctx = b->ctx;
   cudaSetDevice(ctx->dev);
+  if (!ctx->tuned) {  // before the first capture: the tuner's launches must not be recorded
+    const int s = ctx_autotune(ctx, false);
+    if (s != AFID_OK) return s;
+  }
   for (int n = 0; n < nsteps; ++n) {
     int p = (b->graph[0] && b->graph_temp[0] == ctx->temp) ? 0 : (b->graph[1] && b->graph_temp[1] == ctx->temp) ? 1 : -1;
     if (p < 0) {
@@ -610,5 +614,15 @@ int afid_batch_num_slots(const afid_batch_t *b) { return b ? b->nslots : 0; }
 long long afid_batch_device_bytes(const afid_batch_t *b) { return b ? b->bytes + b->ctx->dev_bytes : 0; }
 
 long long afid_batch_launch_count(const afid_batch_t *b) { return b ? b->launches : 0; }
+
+int afid_batch_autotune(afid_batch_t *b, int force, afid_tune_info_t *info) {
+  if (!b) return AFID_E_INVALID;
+  cudaSetDevice(b->ctx->dev);
+  if (cudaStreamSynchronize(b->ctx->stream) != cudaSuccess) return AFID_E_CUDA;
+  const int s = ctx_autotune(b->ctx, force != 0);
+  if (s == AFID_OK && force) drop_graphs(b);  // the captured step holds the old shape
+  if (info) *info = b->ctx->tune;
+  return s;
+}
 
 }  // extern "C"

@@ -17,6 +17,7 @@ struct LaunchCtx {
   bool mixed;      // FP32 explicit terms / transforms
   int tx_y, tx_z;  // x-tile widths of the shared-memory (fallback) FFT kernels
   bool warp_fft;   // register-resident warp FFT when N = 32*{1,2,3,4,6,8,12,16,24,32}
+  int k1_var;      // K1 thread shape (index into the shapes of k1_shapes(M)), set by the autotuner
   FftPlan plan_y, plan_z;
   const void *twy, *twz;  // twiddle tables (double2 or float2)
 };
@@ -56,6 +57,11 @@ size_t k1_smem_bytes(int ldx, int M, bool mixed, bool two_d);
 size_t cn_tab_doubles(int M, int nsst);
 cudaError_t launch_cn_tables(const LaunchCtx &L, const CnInputs &in);
 cudaError_t launch_explicit_implicit(const LaunchCtx &L, const SubstepBuffers &b, int ns);
+// K1 over the first ncol columns with thread shape `var` (autotuner samples use ncol < all).
+cudaError_t launch_k1_fp64(const LaunchCtx &L, const SubstepBuffers &b, int ns, int var, int ncol);
+cudaError_t launch_k1_mixed(const LaunchCtx &L, const SubstepBuffers &b, int ns, int var, int ncol);
+// Thread shapes of K1 for M: fills tpc[]/rpt[] (up to 3) and returns their number.
+int k1_shapes(int M, int *tpc, int *rpt);
 // The kernels of one substep, in launch order (K1 .. K7).
 enum class Stage { ExplicitImplicit = 0, DivFftY, FftZFwd, Tridiag, FftZInv, IfftY, Correct };
 constexpr int kNumStages = 7;
@@ -102,6 +108,9 @@ struct afid_ctx {
   size_t ev_used = 0;
   struct Rec { int cls; size_t a, b; };
   std::vector<Rec> recs;
+  // K1 thread-shape autotuner
+  bool tuned = false;
+  afid_tune_info_t tune{};
   // batch mode: instance scalars and active flags on the device (see afid::BatchSpec)
   int ninst = 0;
   afid::InstScal *inst_dev = nullptr;
@@ -125,6 +134,7 @@ int ctx_run_substep(afid_ctx_t *ctx, int ns);
 int ctx_build_cn_batch(afid_ctx_t *ctx, const double *dt_dev);
 int ctx_fail(afid_ctx_t *ctx, cudaError_t e);
 int ctx_update_params(afid_ctx_t *ctx, const afid_grid_t *grid, const afid_params_t *prm);
+int ctx_autotune(afid_ctx_t *ctx, bool force);
 
 }  // namespace afid
 

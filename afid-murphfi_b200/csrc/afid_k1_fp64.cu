@@ -1,0 +1,20 @@
+// afid_k1_fp64.cu — K1 instantiations with FP64 explicit terms and RK3 histories.
+#include "afid_k1.cuh"
+
+namespace afid {
+
+cudaError_t launch_k1_fp64(const LaunchCtx &L, const SubstepBuffers &b, int ns, int var, int ncol) {
+  const bool two_d = (L.g.nzm == 1 || L.g.batch);  // z neighbours are the column itself
+  return two_d ? launch_k1_T<double, true>(L, b, ns, var, ncol) : launch_k1_T<double, false>(L, b, ns, var, ncol);
+}
+
+int k1_shapes(int M, int *tpc, int *rpt) {
+  const int mi = k1_m_index(M);
+  for (int v = 0; v < kK1ShapeCount[mi]; ++v) {
+    if (tpc) tpc[v] = kK1Shapes[mi][v].tpc;
+    if (rpt) rpt[v] = kK1Shapes[mi][v].rpt;
+  }
+  return kK1ShapeCount[mi];
+}
+
+}  // namespace afid

@@ -20,6 +20,7 @@
 // state (vx, vy, vz, temp, pr), the RHS assembly and every tridiagonal solve are FP64.
 #include "afid_device.cuh"
 #include "afid_internal.h"
+#include "afid_k1.cuh"
 
 namespace afid {
 
@@ -37,7 +38,6 @@ namespace afid {
 // system in PCR form.  Layout (doubles): [sc 32M][a 32M][inv 32M][cp 32M][v 32M][w 32M]
 // [as 32][cs 32][rinvB 32][pa 5x32][pg 5x32][pn 5x32], interior arrays as [q][lane].
 // ------------------------------------------------------------------------------------------
-__host__ __device__ inline size_t cn_table_size(int M) { return 192 * (size_t)M + 18 * 32; }
 
 struct CnMatrixDesc {
   const double *am, *ac, *ap;
@@ -161,375 +161,7 @@ __global__ void k_cn_tables(CnBuildArgs args, int M, double *__restrict__ tab,
   }
 }
 
-// Solve one column whose scaled RHS sits in s[q*32 + lane] (chunk layout); the solution
-// overwrites it.  Constant-matrix version using the tables above.
-template <int M, int LD = 32>
-__device__ __forceinline__ void cn_solve_chunk(double *__restrict__ s, const double *__restrict__ T,
-                                               int lane) {
-  const double *Ta = T + 32 * M, *Tinv = T + 64 * M, *Tcp = T + 96 * M, *Tv = T + 128 * M,
-               *Tw = T + 160 * M, *Tl = T + 192 * M;
-  double y[M];
-#pragma unroll
-  for (int q = 0; q < M; ++q) y[q] = s[q * LD + lane];
-  if constexpr (M > 1) {
-    y[1] = y[1] * __ldg(Tinv + 32 + lane);
-#pragma unroll
-    for (int q = 2; q < M; ++q)
-      y[q] = (y[q] - __ldg(Ta + q * 32 + lane) * y[q - 1]) * __ldg(Tinv + q * 32 + lane);
-#pragma unroll
-    for (int q = M - 2; q >= 1; --q) y[q] = y[q] - __ldg(Tcp + q * 32 + lane) * y[q + 1];
-  }
-  double D;
-  if constexpr (M > 1) {
-    double yprev = __shfl_up_sync(0xffffffffu, y[M - 1], 1);
-    if (lane == 0) yprev = 0.0;
-    D = y[0] - __ldg(Tl + lane) * yprev - __ldg(Tl + 32 + lane) * y[1];
-  } else {
-    D = y[0];
-  }
-  double delta = D * __ldg(Tl + 64 + lane);
-#pragma unroll
-  for (int lev = 0, h = 1; lev < 5; ++lev, h <<= 1) {
-    double dm = __shfl_up_sync(0xffffffffu, delta, h);
-    double dp = __shfl_down_sync(0xffffffffu, delta, h);
-    if (lane < h) dm = 0.0;
-    if (lane + h >= 32) dp = 0.0;
-    delta = (delta - __ldg(Tl + 96 + lev * 32 + lane) * dm - __ldg(Tl + 256 + lev * 32 + lane) * dp) *
-            __ldg(Tl + 416 + lev * 32 + lane);
-  }
-  double xnext = __shfl_down_sync(0xffffffffu, delta, 1);
-  if (lane == 31) xnext = 0.0;
-  s[lane] = delta;
-#pragma unroll
-  for (int q = 1; q < M; ++q)
-    s[q * LD + lane] = y[q] + __ldg(Tv + q * 32 + lane) * delta + __ldg(Tw + q * 32 + lane) * xnext;
-}
-
-// ------------------------------------------------------------------------------------------
-// Explicit terms + RHS, one (k, j, i) point each.  Expressions follow the reference loop
-// bodies term by term; TE is the arithmetic type of the explicit terms.  The operands are
-// x-columns staged in shared memory: c = (j,i), jp/jm = (j+-1,i), ip/im = (j,i+-1),
-// d = the diagonal neighbour (j+1,i-1) for vy and (j-1,i+1) for vz.
-// ------------------------------------------------------------------------------------------
-struct ColV {
-  const double *c, *jp, *jm, *ip, *im, *d;
-};
-
-template <typename TE> __device__ __forceinline__ TE cv(double v) { return (TE)v; }
-
-// ExplicitTermsVX.F90:194-291 + ImplicitAndUpdateVX.F90:124-150, k = 1..nxm-1 (0-based)
-template <typename TE>
-__device__ __forceinline__ double rhs_vx(const Geom &g, const Tables &t, const StepCoef &sc, int k,
-                                         const ColV &X, const ColV &Y, const ColV &Z, const ColV &T,
-                                         const ColV &P, double ru, TE &qout) {
-  const int km = k - 1, kp = k + 1;
-  const TE udy = (TE)(g.dy * 0.25), udz = (TE)(g.dz * 0.25);
-  const TE udyq = (TE)g.udyq_re, udzq = (TE)g.udzq_re;
-  const TE idxm = cv<TE>(__ldg(t.idx + km)), idxc = cv<TE>(__ldg(t.idx + k));
-  const TE udx3c = cv<TE>(__ldg(t.udx3c + k));
-  const TE vxc = cv<TE>(X.c[k]);
-  const TE vxkp = cv<TE>(X.c[kp]), vxkm = cv<TE>(X.c[km]);
-  const TE vxip = cv<TE>(X.ip[k]), vxim = cv<TE>(X.im[k]);
-  const TE vxjp = cv<TE>(X.jp[k]), vxjm = cv<TE>(X.jm[k]);
-  const TE hxz = udx3c * udz *
-                 ((idxm * cv<TE>(Z.ip[km]) + idxc * cv<TE>(Z.ip[k])) * (vxip + vxc) -
-                  (idxm * cv<TE>(Z.c[km]) + idxc * cv<TE>(Z.c[k])) * (vxc + vxim));
-  const TE hxy = udx3c * udy *
-                 ((idxm * cv<TE>(Y.jp[km]) + idxc * cv<TE>(Y.jp[k])) * (vxjp + vxc) -
-                  (idxm * cv<TE>(Y.c[km]) + idxc * cv<TE>(Y.c[k])) * (vxc + vxjm));
-  const TE hxx = ((vxkp + vxc) * (vxkp + vxc) - (vxc + vxkm) * (vxc + vxkm)) * udx3c * (TE)0.25;
-  const TE dzzvx = (vxim - (TE)2.0 * vxc + vxip) * udzq;
-  const TE dyyvx = (vxjm - (TE)2.0 * vxc + vxjp) * udyq;
-  TE qcap = -(hxx + hxy + hxz) + dyyvx + dzzvx;
-  if (g.gaxis == 1) {
-    const TE tempit = (TE)g.active_t * (TE)0.5 * (cv<TE>(T.c[k]) + cv<TE>(T.c[km]));
-    qcap = qcap + (TE)g.byct * tempit;
-  }
-  const double alre = sc.alre;
-  const double udx3 = sc.al * __ldg(t.udx3c + k);
-  const double dxxvx = X.c[kp] * __ldg(t.ap3ck + k) + X.c[k] * __ldg(t.ac3ck + k) + X.c[km] * __ldg(t.am3ck + k);
-  const double dxp = (P.c[k] - P.c[km]) * udx3;
-  qout = qcap;
-  return (sc.ga * (double)qcap + sc.ro * ru + alre * dxxvx - dxp) * sc.dt;
-}
-
-// ExplicitTermsVY.F90:23-122 + ImplicitAndUpdateVY.F90:28-80, k = 0..nxm-1
-template <typename TE>
-__device__ __forceinline__ double rhs_vy(const Geom &g, const Tables &t, const StepCoef &sc, int k,
-                                         const ColV &X, const ColV &Y, const ColV &Z, const ColV &T,
-                                         const ColV &P, double ru, TE &qout) {
-  const int kmm = (k == 0) ? 0 : k - 1;
-  const int kpp = (k == g.nxm - 1) ? k : k + 1;
-  const int kp = k + 1;
-  const TE udy = (TE)(g.dy * 0.25), udz = (TE)(g.dz * 0.25);
-  const TE udyq = (TE)g.udyq_re, udzq = (TE)g.udzq_re;
-  const TE c = cv<TE>(Y.c[k]);
-  const TE vyjp = cv<TE>(Y.jp[k]), vyjm = cv<TE>(Y.jm[k]);
-  const TE vyip = cv<TE>(Y.ip[k]), vyim = cv<TE>(Y.im[k]);
-  const TE hyx = ((cv<TE>(X.c[kp]) + cv<TE>(X.jm[kp])) * (cv<TE>(Y.c[kpp]) + c) -
-                  (cv<TE>(X.c[k]) + cv<TE>(X.jm[k])) * (c + cv<TE>(Y.c[kmm]))) *
-                 cv<TE>(__ldg(t.udx3m + k)) * (TE)0.25;
-  const TE hyy = ((vyjp + c) * (vyjp + c) - (vyjm + c) * (vyjm + c)) * udy;
-  const TE hyz = ((vyip + c) * (cv<TE>(Z.ip[k]) + cv<TE>(Z.d[k])) - (c + vyim) * (cv<TE>(Z.c[k]) + cv<TE>(Z.jm[k]))) *
-                 udz;
-  const TE dyyvy = (vyjp - (TE)2.0 * c + vyjm) * udyq;
-  const TE dzzvy = (vyip - (TE)2.0 * c + vyim) * udzq;
-  TE dph = -(hyx + hyy + hyz) + dyyvy + dzzvy + (TE)g.gy;
-  if (g.gaxis == 2) {
-    const TE tempit = (TE)g.active_t * (TE)0.5 * (cv<TE>(T.c[k]) + cv<TE>(T.jm[k]));
-    dph = dph + (TE)g.byct * tempit;
-  }
-  const double alre = sc.alre;
-  const double udyp = g.dy * sc.al;
-  const double amm = __ldg(t.am3sk + k), acc = __ldg(t.ac3sk + k), app = __ldg(t.ap3sk + k);
-  const double cd = Y.c[k];
-  double dxxvy;
-  if (k == 0)
-    dxxvy = Y.c[kpp] * app + cd * acc - (acc + app) * g.xminusu * g.inslws;
-  else if (k == g.nxm - 1)
-    dxxvy = -(acc + amm) * g.xplusu * g.inslwn + cd * acc + Y.c[kmm] * amm;
-  else
-    dxxvy = Y.c[kpp] * app + cd * acc + Y.c[kmm] * amm;
-  const double dyp = (P.c[k] - P.jm[k]) * udyp;
-  qout = dph;
-  return (sc.ga * (double)dph + sc.ro * ru + alre * dxxvy - dyp) * sc.dt;
-}
-
-// ExplicitTermsVZ.F90:149-244 + ImplicitAndUpdateVZ.F90:121-161, k = 0..nxm-1
-template <typename TE>
-__device__ __forceinline__ double rhs_vz(const Geom &g, const Tables &t, const StepCoef &sc, int k,
-                                         const ColV &X, const ColV &Y, const ColV &Z, const ColV &T,
-                                         const ColV &P, double ru, TE &qout) {
-  const int kmm = (k == 0) ? 0 : k - 1;
-  const int kpp = (k == g.nxm - 1) ? k : k + 1;
-  const int kp = k + 1;
-  const TE udy = (TE)(g.dy * 0.25), udz = (TE)(g.dz * 0.25);
-  const TE udyq = (TE)g.udyq_re, udzq = (TE)g.udzq_re;
-  const TE c = cv<TE>(Z.c[k]);
-  const TE vzip = cv<TE>(Z.ip[k]), vzim = cv<TE>(Z.im[k]);
-  const TE vzjp = cv<TE>(Z.jp[k]), vzjm = cv<TE>(Z.jm[k]);
-  const TE hzz = ((vzip + c) * (vzip + c) - (vzim + c) * (vzim + c)) * udz;
-  const TE hzy = ((cv<TE>(Y.jp[k]) + cv<TE>(Y.d[k])) * (vzjp + c) - (cv<TE>(Y.c[k]) + cv<TE>(Y.im[k])) * (c + vzjm)) *
-                 udy;
-  const TE hzx = ((cv<TE>(X.c[kp]) + cv<TE>(X.im[kp])) * (cv<TE>(Z.c[kpp]) + c) -
-                  (cv<TE>(X.c[k]) + cv<TE>(X.im[k])) * (c + cv<TE>(Z.c[kmm]))) *
-                 cv<TE>(__ldg(t.udx3m + k)) * (TE)0.25;
-  const TE dzzvz = (vzip - (TE)2.0 * c + vzim) * udzq;
-  const TE dyyvz = (vzjp - (TE)2.0 * c + vzjm) * udyq;
-  TE dq = -(hzx + hzy + hzz) + dyyvz + dzzvz;
-  if (g.gaxis == 3) {
-    const TE tempit = (TE)g.active_t * (TE)0.5 * (cv<TE>(T.c[k]) + cv<TE>(T.im[k]));
-    dq = dq + (TE)g.byct * tempit;
-  }
-  const double alre = sc.alre;
-  const double amm = __ldg(t.am3sk + k), acc = __ldg(t.ac3sk + k), app = __ldg(t.ap3sk + k);
-  const double dxxvz = Z.c[kpp] * app + Z.c[k] * acc + Z.c[kmm] * amm;
-  const double dzp = (P.c[k] - P.im[k]) * g.dz * sc.al;
-  qout = dq;
-  return (sc.ga * (double)dq + sc.ro * ru + alre * dxxvz - dzp) * sc.dt;
-}
-
-// ExplicitTermsTemp.F90:22-77 + ImplicitAndUpdateTemp.F90:197-237, k = 0..nxm-1
-template <typename TE>
-__device__ __forceinline__ double rhs_temp(const Geom &g, const Tables &t, const StepCoef &sc, int k,
-                                           const ColV &X, const ColV &Y, const ColV &Z, const ColV &T,
-                                           double tbp, double ttp, double ru, TE &qout) {
-  const TE udz = (TE)(g.dz * 0.5), udy = (TE)(g.dy * 0.5);
-  const TE udzq = (TE)g.udzq_pe, udyq = (TE)g.udyq_pe;
-  const TE tc = cv<TE>(T.c[k]);
-  const TE ux = cv<TE>(__ldg(t.udx3m + k));
-  TE htx;
-  if (k == 0)
-    htx = (cv<TE>(X.c[1]) * (cv<TE>(T.c[1]) + tc) - cv<TE>(X.c[0]) * (TE)2.0 * (TE)tbp) * (TE)0.5 * ux;
-  else if (k == g.nxm - 1)
-    htx = (cv<TE>(X.c[k + 1]) * (TE)2.0 * (TE)ttp - cv<TE>(X.c[k]) * (tc + cv<TE>(T.c[k - 1]))) * (TE)0.5 * ux;
-  else
-    htx = (cv<TE>(X.c[k + 1]) * (cv<TE>(T.c[k + 1]) + tc) - cv<TE>(X.c[k]) * (tc + cv<TE>(T.c[k - 1]))) *
-          (TE)0.5 * ux;
-  const TE tip = cv<TE>(T.ip[k]), tim = cv<TE>(T.im[k]);
-  const TE tjp = cv<TE>(T.jp[k]), tjm = cv<TE>(T.jm[k]);
-  const TE htz = (cv<TE>(Z.ip[k]) * (tip + tc) - cv<TE>(Z.c[k]) * (tc + tim)) * udz;
-  const TE hty = (cv<TE>(Y.jp[k]) * (tjp + tc) - cv<TE>(Y.c[k]) * (tc + tjm)) * udy;
-  const TE dzzt = (tip - (TE)2.0 * tc + tim) * udzq;
-  const TE dyyt = (tjp - (TE)2.0 * tc + tjm) * udyq;
-  const TE hro = -(htx + hty + htz) + dyyt + dzzt;
-  const double alpec = sc.alpec;
-  const double tcd = T.c[k];
-  double dxxt;
-  if (k == 0)
-    dxxt = T.c[1] * __ldg(t.ap3ssk) + tcd * __ldg(t.ac3ssk) - (__ldg(t.ap3ssk) + __ldg(t.ac3ssk)) * tbp * g.tfixs;
-  else if (k == g.nxm - 1)
-    dxxt = tcd * __ldg(t.ac3ssk + k) + T.c[k - 1] * __ldg(t.am3ssk + k) -
-           (__ldg(t.am3ssk + k) + __ldg(t.ac3ssk + k)) * ttp * g.tfixn;
-  else
-    dxxt = T.c[k + 1] * __ldg(t.ap3ssk + k) + tcd * __ldg(t.ac3ssk + k) + T.c[k - 1] * __ldg(t.am3ssk + k);
-  qout = hro;
-  return (sc.ga * (double)hro + sc.ro * ru + alpec * dxxt) * sc.dt;
-}
-
-// Number of x-columns K1 stages per (j,i) column: vx 5, vy 6, vz 6, temp 5, pr 3 (FP64) + 4 RK3
-// histories (TE).  In 2-D (nzm = 1, or a batch of 2-D instances) the z neighbours are the
-// column itself, leaving vx, vy, vz, temp at (j, j+1, j-1) and pr at (j, j-1): 14 columns.
-constexpr int kK1StateCols = 25;
-constexpr int kK1StateCols2D = 14;
-constexpr int kK1RuCols = 4;
-
-__host__ __device__ inline size_t k1_stage_bytes(int ldx, size_t te_size, bool two_d) {
-  return (size_t)(two_d ? kK1StateCols2D : kK1StateCols) * ldx * sizeof(double) +
-         (size_t)kK1RuCols * ldx * te_size;
-}
-
-// K1: a block owns one (j,i) column.  One thread issues 1-D TMA bulk copies of the 29 needed
-// x-columns (contiguous runs of ldx elements) into shared memory, completing on an mbarrier;
-// then TPC threads each compute the four explicit terms and RHS of RPT cells from shared
-// memory, write the new RK3 histories, and put the scaled RHS in the solver's chunk layout
-// (row r at (r%M)*33 + r/M).  Four warps run the partitioned CN solves, and every thread adds
-// the increments to the staged centre values and stores the intermediate fields.
-template <int M, int TPC, int RPT, typename TE, bool TWO_D>
-__global__ void __launch_bounds__(TPC)
-    k_explicit_implicit(Geom g0, Tables t, const StepCoef *__restrict__ sc_all, int ns,
-                        const double *__restrict__ cn_tab, const double *__restrict__ vx,
-                        const double *__restrict__ vy, const double *__restrict__ vz,
-                        const double *__restrict__ temp, const double *__restrict__ pr,
-                        TE *__restrict__ rux, TE *__restrict__ ruy, TE *__restrict__ ruz,
-                        TE *__restrict__ rut, double *__restrict__ vx_o, double *__restrict__ vy_o,
-                        double *__restrict__ vz_o, double *__restrict__ temp_o, int *__restrict__ err) {
-  constexpr int LD = 33;
-  constexpr int FLD = LD * M;
-  extern __shared__ __align__(128) unsigned char smem_k1[];
-  __shared__ uint64_t bar;
-  Geom g = g0;
-  const int ldx = g.ldx;
-  double *cols = reinterpret_cast<double *>(smem_k1);
-  constexpr int NS = TWO_D ? kK1StateCols2D : kK1StateCols;
-  TE *rcols = reinterpret_cast<TE *>(cols + (size_t)NS * ldx);
-  double *s_rhs = reinterpret_cast<double *>(smem_k1 + k1_stage_bytes(ldx, sizeof(TE), TWO_D));
-  const int tc = threadIdx.x;
-  const int colid = blockIdx.x;
-  const int j = colid % g.nym, i = colid / g.nym;
-  if (!inst_active(g, i)) {
-    // An idle batch slot keeps its state: the temperature moves buffers every substep.
-    const size_t c = col_off(g, j, i);
-    for (int k = tc; k < g.nx; k += TPC) temp_o[c + k] = temp[c + k];
-    return;
-  }
-  bind_instance(g, i);
-  const int jp = wrap_inc(j, g.nym), jm = wrap_dec(j, g.nym);
-  const int ip = zinc(g, i), im = zdec(g, i);
-  const size_t c0 = col_off(g, j, i);
-  if (tc == 0) {
-    mbar_init(&bar, 1);
-    fence_mbar_init();
-  }
-  __syncthreads();
-  if (tc == 0) {
-    const size_t oc = c0, ojp = col_off(g, jp, i), ojm = col_off(g, jm, i), oip = col_off(g, j, ip),
-                 oim = col_off(g, j, im), ojpim = col_off(g, jp, im), ojmip = col_off(g, jm, ip);
-    const uint32_t cb = (uint32_t)ldx * sizeof(double), rb = (uint32_t)ldx * sizeof(TE);
-    mbar_arrive_expect_tx(&bar, (uint32_t)k1_stage_bytes(ldx, sizeof(TE), TWO_D));
-    if constexpr (TWO_D) {
-      const double *src[kK1StateCols2D] = {vx + oc,   vx + ojp,   vx + ojm,    // 0-2
-                                           vy + oc,   vy + ojp,   vy + ojm,    // 3-5
-                                           vz + oc,   vz + ojp,   vz + ojm,    // 6-8
-                                           temp + oc, temp + ojp, temp + ojm,  // 9-11
-                                           pr + oc,   pr + ojm};               // 12-13
-#pragma unroll
-      for (int q = 0; q < kK1StateCols2D; ++q) bulk_g2s(cols + (size_t)q * ldx, src[q], cb, &bar);
-    } else {
-      const double *src[kK1StateCols] = {vx + oc,   vx + ojp, vx + ojm, vx + oip, vx + oim,  // 0-4
-                                         vy + oc,   vy + ojp, vy + ojm, vy + oip, vy + oim, vy + ojpim,  // 5-10
-                                         vz + oc,   vz + ojp, vz + ojm, vz + oip, vz + oim, vz + ojmip,  // 11-16
-                                         temp + oc, temp + ojp, temp + ojm, temp + oip, temp + oim,      // 17-21
-                                         pr + oc,   pr + ojm, pr + oim};                                // 22-24
-#pragma unroll
-      for (int q = 0; q < kK1StateCols; ++q) bulk_g2s(cols + (size_t)q * ldx, src[q], cb, &bar);
-    }
-    bulk_g2s(rcols, rux + oc, rb, &bar);
-    bulk_g2s(rcols + ldx, ruy + oc, rb, &bar);
-    bulk_g2s(rcols + 2 * ldx, ruz + oc, rb, &bar);
-    bulk_g2s(rcols + 3 * ldx, rut + oc, rb, &bar);
-  }
-  const bool ok = mbar_wait(&bar, 0, kSpinLimit);
-  if (!__syncthreads_and(ok)) {
-    if (tc == 0) atomicOr(err, 2);
-    mbar_wait(&bar, 0, kSpinLimit);  // let copies in flight land before the block exits
-    return;
-  }
-  auto C = [&](int q) { return (const double *)(cols + (size_t)q * ldx); };
-  // {centre, j+1, j-1, i+1, i-1, diagonal}; in 2-D the i+-1 columns are the centre's
-  const ColV X = TWO_D ? ColV{C(0), C(1), C(2), C(0), C(0), nullptr} : ColV{C(0), C(1), C(2), C(3), C(4), nullptr};
-  const ColV Y = TWO_D ? ColV{C(3), C(4), C(5), C(3), C(3), C(4)} : ColV{C(5), C(6), C(7), C(8), C(9), C(10)};
-  const ColV Z = TWO_D ? ColV{C(6), C(7), C(8), C(6), C(6), C(8)} : ColV{C(11), C(12), C(13), C(14), C(15), C(16)};
-  const ColV T = TWO_D ? ColV{C(9), C(10), C(11), C(9), C(9), nullptr} : ColV{C(17), C(18), C(19), C(20), C(21), nullptr};
-  const ColV P = TWO_D ? ColV{C(12), nullptr, C(13), nullptr, C(12), nullptr} : ColV{C(22), nullptr, C(23), nullptr, C(24), nullptr};
-  const int slot = sc_slot(g, i, ns);
-  const StepCoef sc = sc_all[slot];
-  const size_t tsz = cn_table_size(M);
-  const double *TX = cn_tab + (size_t)(slot * 3 + 0) * tsz;
-  const double *TY = cn_tab + (size_t)(slot * 3 + 1) * tsz;
-  const double *TT = cn_tab + (size_t)(slot * 3 + 2) * tsz;
-  const int nxm = g.nxm;
-  const size_t pl = (size_t)j + (size_t)g.nym * i;
-  const double tbp = __ldg(t.tempbp + pl), ttp = __ldg(t.temptp + pl);
-#pragma unroll
-  for (int p = 0; p < RPT; ++p) {
-    const int k = tc + TPC * p;
-    if (k < nxm) {
-      const double syz = __ldg(TY + k);
-      const int sk = (k % M) * LD + k / M;
-      TE q;
-      if (k >= 1) {
-        const int r = k - 1;
-        s_rhs[(r % M) * LD + r / M] = rhs_vx<TE>(g, t, sc, k, X, Y, Z, T, P, (double)rcols[k], q) * __ldg(TX + r);
-        rux[c0 + k] = q;
-      }
-      s_rhs[FLD + sk] = rhs_vy<TE>(g, t, sc, k, X, Y, Z, T, P, (double)rcols[ldx + k], q) * syz;
-      ruy[c0 + k] = q;
-      s_rhs[2 * FLD + sk] = rhs_vz<TE>(g, t, sc, k, X, Y, Z, T, P, (double)rcols[2 * ldx + k], q) * syz;
-      ruz[c0 + k] = q;
-      s_rhs[3 * FLD + sk] = rhs_temp<TE>(g, t, sc, k, X, Y, Z, T, tbp, ttp, (double)rcols[3 * ldx + k], q) *
-                            __ldg(TT + k);
-      rut[c0 + k] = q;
-    }
-  }
-  // identity padding rows: vx rows nxm-1 .. 32M-1, the others nxm .. 32M-1
-  for (int r = nxm - 1 + tc; r < 32 * M; r += TPC) {
-    const int sr = (r % M) * LD + r / M;
-    s_rhs[sr] = 0.0;
-    if (r >= nxm) {
-      s_rhs[FLD + sr] = 0.0;
-      s_rhs[2 * FLD + sr] = 0.0;
-      s_rhs[3 * FLD + sr] = 0.0;
-    }
-  }
-  __syncthreads();
-  {
-    const int warp = tc >> 5, lane = tc & 31;
-    constexpr int NW = TPC / 32;
-    for (int f = warp; f < 4; f += NW) {
-      const double *Tb = (f == 0) ? TX : ((f == 3) ? TT : TY);
-      cn_solve_chunk<M, LD>(s_rhs + f * FLD, Tb, lane);
-    }
-  }
-  __syncthreads();
-#pragma unroll
-  for (int p = 0; p < RPT; ++p) {
-    const int k = tc + TPC * p;
-    if (k < nxm) {
-      const int sk = (k % M) * LD + k / M;
-      if (k >= 1) {
-        const int r = k - 1;
-        vx_o[c0 + k] = X.c[k] + s_rhs[(r % M) * LD + r / M];
-      } else {
-        vx_o[c0] = 0.0;  // ImplicitAndUpdateVX.F90:171-172: vx(1) = vx(nx) = 0
-        vx_o[c0 + nxm] = 0.0;
-      }
-      vy_o[c0 + k] = Y.c[k] + s_rhs[FLD + sk];
-      vz_o[c0 + k] = Z.c[k] + s_rhs[2 * FLD + sk];
-      temp_o[c0 + k] = T.c[k] + s_rhs[3 * FLD + sk];
-    }
-  }
-}
+// K1 (explicit terms + RHS + CN solves) lives in afid_k1.cuh.
 
 // ------------------------------------------------------------------------------------------
 // K2: divergence (pressure.F90:147-158) fused with the forward y r2c FFT (pressure.F90:174)
@@ -1180,51 +812,9 @@ cudaError_t launch_cn_tables(const LaunchCtx &L, const CnInputs &in) {
   return cudaGetLastError();
 }
 
-template <int M, int TPC, int RPT, typename TE, bool TWO_D>
-static cudaError_t launch_k1_cfg(const LaunchCtx &L, const SubstepBuffers &b, int ns) {
-  const int ncol = L.g.nym * L.g.nzm;
-  const size_t smem = k1_stage_bytes(L.g.ldx, sizeof(TE), TWO_D) + (size_t)4 * 33 * M * sizeof(double);
-  auto kern = k_explicit_implicit<M, TPC, RPT, TE, TWO_D>;
-  cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  kern<<<ncol, TPC, smem, L.stream>>>(L.g, L.t, b.sc, ns, b.cn_tab, b.vx, b.vy, b.vz, b.temp, b.pr,
-                                      (TE *)b.rux, (TE *)b.ruy, (TE *)b.ruz, (TE *)b.rut, b.vx_o, b.vy_o,
-                                      b.vz_o, b.temp_o, b.err);
-  return cudaGetLastError();
-}
-
-// M = ceil(nxm/32) rounded to {1,2,4,8,12,16,24,32}; TPC threads cover nxm in RPT rows each.
-template <int M, typename TE, bool TWO_D>
-static cudaError_t launch_k1_M(const LaunchCtx &L, const SubstepBuffers &b, int ns) {
-  if constexpr (M <= 1) return launch_k1_cfg<M, 32, 1, TE, TWO_D>(L, b, ns);          // nxm <= 32
-  else if constexpr (M <= 2) return launch_k1_cfg<M, 64, 1, TE, TWO_D>(L, b, ns);     // <= 64
-  else if constexpr (M <= 4) return launch_k1_cfg<M, 128, 1, TE, TWO_D>(L, b, ns);    // <= 128
-  else if constexpr (M <= 8) return launch_k1_cfg<M, 256, 1, TE, TWO_D>(L, b, ns);    // <= 256
-  else if constexpr (M <= 16) return launch_k1_cfg<M, 256, 2, TE, TWO_D>(L, b, ns);   // <= 512
-  else return launch_k1_cfg<M, 256, 4, TE, TWO_D>(L, b, ns);                          // <= 1024
-}
-
-template <int M, typename TE>
-static cudaError_t launch_k1_M(const LaunchCtx &L, const SubstepBuffers &b, int ns) {
-  return (L.g.nzm == 1 || L.g.batch) ? launch_k1_M<M, TE, true>(L, b, ns) : launch_k1_M<M, TE, false>(L, b, ns);
-}
-
-template <typename TE>
-static cudaError_t launch_k1_T(const LaunchCtx &L, const SubstepBuffers &b, int ns) {
-  switch (L.M) {
-    case 1: return launch_k1_M<1, TE>(L, b, ns);
-    case 2: return launch_k1_M<2, TE>(L, b, ns);
-    case 4: return launch_k1_M<4, TE>(L, b, ns);
-    case 8: return launch_k1_M<8, TE>(L, b, ns);
-    case 12: return launch_k1_M<12, TE>(L, b, ns);
-    case 16: return launch_k1_M<16, TE>(L, b, ns);
-    case 24: return launch_k1_M<24, TE>(L, b, ns);
-    case 32: return launch_k1_M<32, TE>(L, b, ns);
-  }
-  return cudaErrorInvalidValue;
-}
-
 cudaError_t launch_explicit_implicit(const LaunchCtx &L, const SubstepBuffers &b, int ns) {
-  return L.mixed ? launch_k1_T<float>(L, b, ns) : launch_k1_T<double>(L, b, ns);
+  const int ncol = L.g.nym * L.g.nzm;
+  return L.mixed ? launch_k1_mixed(L, b, ns, L.k1_var, ncol) : launch_k1_fp64(L, b, ns, L.k1_var, ncol);
 }
 
 template <int M, typename TS>
@@ -1382,7 +972,7 @@ static cudaError_t launch_stage_T(const LaunchCtx &L, const SubstepBuffers &b, i
       return cudaGetLastError();
     }
     case Stage::ExplicitImplicit:
-      return L.mixed ? launch_k1_T<float>(L, b, ns) : launch_k1_T<double>(L, b, ns);
+      return launch_explicit_implicit(L, b, ns);
   }
   return cudaErrorInvalidValue;
 }

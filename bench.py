@@ -200,6 +200,7 @@ def run_gpu(args):
         step(ntime)
         ntime += 1
     solver.synchronize()
+    tune = solver.autotune()  # the shape the autotuner picked during the first step
     solver.profile_report()  # drop warm-up records
     solver.profile(True)
     launches0 = solver.launch_count()
@@ -300,6 +301,7 @@ def run_gpu(args):
                     "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
                     "note": "upload 5 fields, K steps with CFL + Nu/KE read back, download 5 fields"},
             "gpu_launches": int(launches),
+            "k1_autotune": tune,
             "clocks": clk,
             "nu_vol_end": nu,
             "cpu_baseline": cpu,
@@ -413,6 +415,7 @@ def run_batched(args):
     for _ in range(args.warmup):
         bs.step()
     torch.cuda.synchronize()
+    tune = {f"{k[1]}x{k[0]}": b.autotune() for k, b in zip(sorted(bs.classes), bs.batches)}
     l0 = bs.launches()
     clocks = ClockSampler(torch.cuda.current_device())
     barrier(world)
@@ -472,6 +475,7 @@ def run_batched(args):
                        "l2": "inputs larger than L2 (%.1f GB resident)" % (bs_bytes / 1e9),
                        "parallelism": "replicas" if world > 1 else "single GPU"},
             "gpu_launches": int(launches),
+            "k1_autotune": tune,
             "clocks": clk,
             "steps_done_min": nsteps_done,
             "instances_with_error": errors,

@@ -71,6 +71,9 @@ int afid_batch_num_slots(const afid_batch_t *b);
 /* Device bytes the batch holds (for admission control by HBM footprint). */
 long long afid_batch_device_bytes(const afid_batch_t *b);
 long long afid_batch_launch_count(const afid_batch_t *b);
+/* The autotuner of include/afid_gpu.h on this batch's stacked domain (runs by itself before the
+ * first captured step). */
+int afid_batch_autotune(afid_batch_t *b, int force, afid_tune_info_t *info);
 
 #ifdef __cplusplus
 }

@@ -128,6 +128,25 @@ int afid_gpu_cuda_error(afid_ctx_t *ctx);   /* last cudaError_t seen by this con
 int afid_gpu_field_device_ptr(afid_ctx_t *ctx, int which, void **dptr, int *ldx);
 /* Kernels launched by this context since creation (all are this library's own kernels). */
 long long afid_gpu_launch_count(afid_ctx_t *ctx);
+
+/* Autotuner of the fused explicit/implicit kernel: every thread shape available for this
+ * wall-normal size (threads per x-column block x rows per thread) is timed on a sample of
+ * columns, with the RK3 histories redirected to scratch memory so the state is untouched, and
+ * the fastest is kept.  It runs by itself before the first step; force = 1 repeats it.  The
+ * shape changes the schedule only: results are bitwise the same for every shape. */
+#define AFID_TUNE_MAX 3
+typedef struct afid_tune_info {
+  int ncand;                    /* shapes available (1 = nothing to choose)                  */
+  int chosen;                   /* index of the shape in use                                 */
+  int sample_columns;           /* x-columns per timed sample launch                         */
+  int threads[AFID_TUNE_MAX];   /* threads per column block                                  */
+  int rows[AFID_TUNE_MAX];      /* rows per thread                                           */
+  double us[AFID_TUNE_MAX];     /* mean time per sample launch in microseconds (-1: not run) */
+} afid_tune_info_t;
+int afid_gpu_autotune(afid_ctx_t *ctx, int force, afid_tune_info_t *info);
+/* Use shape `index` (0 .. ncand-1) from now on without timing, e.g. one saved from an earlier
+ * afid_gpu_autotune on the same device and sizes. */
+int afid_gpu_set_k1_shape(afid_ctx_t *ctx, int index);
 /* Per-kernel device timing with CUDA events recorded on the context stream around every
  * launch (no counterpart in the reference, which times whole steps with MPI_WTIME,
  * main.F90:282,363-371).  Classes: 0 CN factor tables, 1 explicit+implicit, 2 divergence +

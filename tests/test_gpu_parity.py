@@ -252,3 +252,26 @@ def test_wall_normal_size_beyond_shared_memory_is_rejected():
     with pytest.raises(ag.AfidError) as e:
         Case(1000, 8, 4).solver()
     assert e.value.status == 603
+
+
+@pytest.mark.parametrize("shape,precision", [((100, 16, 8), ag.PREC_FP64), ((384, 8, 4), ag.PREC_MIXED),
+                                             ((500, 16, 1), ag.PREC_FP64), ((700, 8, 1), ag.PREC_FP64)])
+def test_k1_shapes_bitwise_identical(shape, precision):
+    """Every thread shape the autotuner may pick gives the same fields bit for bit, and the
+    autotuner reports a timing for each."""
+    case = Case(*shape, precision=precision, rayt=1e6, dt=2e-3)
+    s = case.oracle_state(random_velocity=0.1)
+    outs = []
+    with case.solver() as g:
+        info = g.autotune()
+    assert info["ncand"] >= 2 and all(us > 0 for _, _, us in info["shapes"])
+    for v in range(info["ncand"]):
+        with case.solver() as g:
+            g.set_k1_shape(v)
+            g.upload(s.vx, s.vy, s.vz, s.temp, s.pr)
+            for n in range(2):
+                g.time_marcher(2e-3, n)
+            outs.append(g.download())
+    for o in outs[1:]:
+        for k in ag.Solver.FIELDS:
+            assert np.array_equal(o[k], outs[0][k]), k

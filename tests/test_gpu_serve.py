@@ -98,7 +98,7 @@ def test_admission_by_footprint():
         # FIFO: the small-class job could only start after the large-class pool drained
         assert res[9]["t_admit"] >= max(res[k]["t_done"] for k in (0, 1, 2)) - 1e-9
         assert srv.status()["device_bytes"] <= budget
-    with ag.Server(ag.PREC_MIXED, hbm_budget_bytes=1 << 20, slots_per_pool=2) as srv:
+    with ag.Server(ag.PREC_MIXED, hbm_budget_bytes=4096, slots_per_pool=2) as srv:
         srv.submit(a, 1, 10, 1)
         r = _run_to_completion(srv, 1)[1]
         assert r["errorcode"] == 605 and r["steps_done"] == 0
