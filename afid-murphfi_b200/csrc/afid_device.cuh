@@ -35,6 +35,13 @@ struct Geom {
   const unsigned char *active;   // [nzm] 1 = advance this instance (batch mode), else nullptr
 };
 
+// Shared-memory stride of the chunked tridiagonal layout (row r of a 32-chunk system at
+// (r % M) * LD + r / M, chunk q of lane l at q * LD + l): the smallest stride >= 32 that makes
+// the row-ordered accesses of a half-warp hit distinct 8-byte banks (2-way for M = 12, 24).
+__host__ __device__ constexpr int chunk_ld(int M) {
+  return M == 1 ? 32 : M == 2 ? 40 : M == 4 ? 36 : M == 8 ? 34 : 33;
+}
+
 // Scalars that differ between the instances of a batch (aspect ratio, Ra, Pr).
 struct InstScal {
   double dy, dyq, ren, pect, rren, rpect, udyq_re, udyq_pe;

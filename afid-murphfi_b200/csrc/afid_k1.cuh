@@ -244,7 +244,7 @@ __global__ void __launch_bounds__(TPC)
                         TE *__restrict__ rux, TE *__restrict__ ruy, TE *__restrict__ ruz,
                         TE *__restrict__ rut, double *__restrict__ vx_o, double *__restrict__ vy_o,
                         double *__restrict__ vz_o, double *__restrict__ temp_o, int *__restrict__ err) {
-  constexpr int LD = 33;
+  constexpr int LD = chunk_ld(M);
   constexpr int FLD = LD * M;
   extern __shared__ __align__(128) unsigned char smem_k1[];
   __shared__ uint64_t bar;
@@ -384,7 +384,7 @@ __global__ void __launch_bounds__(TPC)
 
 template <int M, int TPC, int RPT, typename TE, bool TWO_D>
 cudaError_t launch_k1_cfg(const LaunchCtx &L, const SubstepBuffers &b, int ns, int ncol) {
-  const size_t smem = k1_stage_bytes(L.g.ldx, sizeof(TE), TWO_D) + (size_t)4 * 33 * M * sizeof(double);
+  const size_t smem = k1_stage_bytes(L.g.ldx, sizeof(TE), TWO_D) + (size_t)4 * chunk_ld(M) * M * sizeof(double);
   auto kern = k_explicit_implicit<M, TPC, RPT, TE, TWO_D>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;

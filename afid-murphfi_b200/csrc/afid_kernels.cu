@@ -280,8 +280,9 @@ __global__ void __launch_bounds__(WPB * 32)
   if (!inst_active(g, kz)) return;  // whole warp (batch mode: kz numbers the instance)
   // the singular (0,0) mode; in batch mode every instance's ky = 0 mode (nzm = 1 each)
   const bool pin = (ky == 0 && (kz == 0 || g.batch));
-  double *sa = smem_k4 + warp * (4 * 32 * M);
-  double *sc_ = sa + 32 * M, *sdr = sa + 64 * M, *sdi = sa + 96 * M;
+  constexpr int LD = chunk_ld(M);
+  double *sa = smem_k4 + warp * (4 * LD * M);
+  double *sc_ = sa + LD * M, *sdr = sa + 2 * LD * M, *sdi = sa + 3 * LD * M;
   C *colp = spec + (size_t)sys * g.ldxc;
   const int n = g.nxm;
   const double akj = __ldg(t.ak2 + (g.batch ? (size_t)kz * g.nym : 0) + ky);
@@ -289,7 +290,7 @@ __global__ void __launch_bounds__(WPB * 32)
 #pragma unroll
   for (int tt = 0; tt < M; ++tt) {
     const int r = lane + 32 * tt;
-    const int s = (r % M) * 32 + r / M;
+    const int s = (r % M) * LD + r / M;
     double a = 0.0, c = 0.0, dr = 0.0, di = 0.0;
     if (r < n) {
       const double f = 1.0 / (__ldg(t.acphk + r) - akj - aki);
@@ -313,12 +314,12 @@ __global__ void __launch_bounds__(WPB * 32)
   cp[0] = 0.0; yr[0] = 0.0; yi[0] = 0.0; v[0] = 0.0; w[0] = 0.0;
 #pragma unroll
   for (int q = 1; q < M; ++q) {
-    const double a = sa[q * 32 + lane], c = sc_[q * 32 + lane];
+    const double a = sa[q * LD + lane], c = sc_[q * LD + lane];
     const double den = (q > 1) ? diag(s0 + q) - a * cp[q - 1] : diag(s0 + q);
     bad |= (den == 0.0);
     const double inv = 1.0 / den;
     cp[q] = c * inv;
-    const double dr = sdr[q * 32 + lane], di = sdi[q * 32 + lane];
+    const double dr = sdr[q * LD + lane], di = sdi[q * LD + lane];
     if (q > 1) {
       yr[q] = (dr - a * yr[q - 1]) * inv;
       yi[q] = (di - a * yi[q - 1]) * inv;
@@ -383,8 +384,8 @@ __global__ void __launch_bounds__(WPB * 32)
   sdi[lane] = ei;
 #pragma unroll
   for (int q = 1; q < M; ++q) {
-    sdr[q * 32 + lane] = yr[q] + v[q] * er + w[q] * xnr;
-    sdi[q * 32 + lane] = yi[q] + v[q] * ei + w[q] * xni;
+    sdr[q * LD + lane] = yr[q] + v[q] * er + w[q] * xnr;
+    sdi[q * LD + lane] = yi[q] + v[q] * ei + w[q] * xni;
   }
   if (bad) atomicOr(err, 1);
   __syncwarp();
@@ -392,7 +393,7 @@ __global__ void __launch_bounds__(WPB * 32)
   for (int tt = 0; tt < M; ++tt) {
     const int r = lane + 32 * tt;
     if (r < n) {
-      const int s = (r % M) * 32 + r / M;
+      const int s = (r % M) * LD + r / M;
       C o;
       o.x = (TS)sdr[s];
       o.y = (TS)sdi[s];
@@ -779,7 +780,7 @@ static int pick_M(int nxm) {
 
 int cn_choose_M(int nxm) { return pick_M(nxm); }
 size_t k1_smem_bytes(int ldx, int M, bool mixed, bool two_d) {
-  return k1_stage_bytes(ldx, mixed ? sizeof(float) : sizeof(double), two_d) + (size_t)4 * 33 * M * sizeof(double);
+  return k1_stage_bytes(ldx, mixed ? sizeof(float) : sizeof(double), two_d) + (size_t)4 * chunk_ld(M) * M * sizeof(double);
 }
 size_t cn_tab_doubles(int M, int nsst) { return cn_table_size(M) * 3 * (size_t)nsst; }
 
@@ -821,7 +822,7 @@ template <int M, typename TS>
 static cudaError_t launch_k4_M(const LaunchCtx &L, void *spec, int *err) {
   constexpr int W = (M >= 16) ? 2 : 4;
   const int nsys = L.g.nyh * L.g.nzm;
-  const size_t smem = (size_t)W * 4 * 32 * M * sizeof(double);
+  const size_t smem = (size_t)W * 4 * chunk_ld(M) * M * sizeof(double);
   auto kern = k_tridiag_pressure<M, W, TS>;
   cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   kern<<<(nsys + W - 1) / W, W * 32, smem, L.stream>>>(L.g, L.t, (typename Cplx<TS>::type *)spec, err);
