@@ -325,21 +325,26 @@ __global__ void __launch_bounds__(TPC)
   for (int p = 0; p < RPT; ++p) {
     const int k = tc + TPC * p;
     if (k < nxm) {
+      // all four right-hand sides first: no shared-memory store separates their operand loads,
+      // so the compiler reuses them across the four fields
+      TE q0 = (TE)0, q1, q2, q3;
+      const double r0 = (k >= 1) ? rhs_vx<TE>(g, t, sc, k, X, Y, Z, T, P, (double)rcols[k], q0) : 0.0;
+      const double r1 = rhs_vy<TE>(g, t, sc, k, X, Y, Z, T, P, (double)rcols[ldx + k], q1);
+      const double r2 = rhs_vz<TE>(g, t, sc, k, X, Y, Z, T, P, (double)rcols[2 * ldx + k], q2);
+      const double r3 = rhs_temp<TE>(g, t, sc, k, X, Y, Z, T, tbp, ttp, (double)rcols[3 * ldx + k], q3);
       const double syz = __ldg(TY + k);
       const int sk = (k % M) * LD + k / M;
-      TE q;
       if (k >= 1) {
         const int r = k - 1;
-        s_rhs[(r % M) * LD + r / M] = rhs_vx<TE>(g, t, sc, k, X, Y, Z, T, P, (double)rcols[k], q) * __ldg(TX + r);
-        rux[c0 + k] = q;
+        s_rhs[(r % M) * LD + r / M] = r0 * __ldg(TX + r);
+        rux[c0 + k] = q0;
       }
-      s_rhs[FLD + sk] = rhs_vy<TE>(g, t, sc, k, X, Y, Z, T, P, (double)rcols[ldx + k], q) * syz;
-      ruy[c0 + k] = q;
-      s_rhs[2 * FLD + sk] = rhs_vz<TE>(g, t, sc, k, X, Y, Z, T, P, (double)rcols[2 * ldx + k], q) * syz;
-      ruz[c0 + k] = q;
-      s_rhs[3 * FLD + sk] = rhs_temp<TE>(g, t, sc, k, X, Y, Z, T, tbp, ttp, (double)rcols[3 * ldx + k], q) *
-                            __ldg(TT + k);
-      rut[c0 + k] = q;
+      s_rhs[FLD + sk] = r1 * syz;
+      ruy[c0 + k] = q1;
+      s_rhs[2 * FLD + sk] = r2 * syz;
+      ruz[c0 + k] = q2;
+      s_rhs[3 * FLD + sk] = r3 * __ldg(TT + k);
+      rut[c0 + k] = q3;
     }
   }
   // identity padding rows: vx rows nxm-1 .. 32M-1, the others nxm .. 32M-1
