@@ -217,24 +217,32 @@ __device__ __forceinline__ double rhs_temp(const Geom &g, const Tables &t, const
   return (sc.ga * (double)hro + sc.ro * ru + alpec * dxxt) * sc.dt;
 }
 
-// Number of x-columns K1 stages per (j,i) column: vx 5, vy 6, vz 6, temp 5, pr 3 (FP64) + 4 RK3
-// histories (TE).  In 2-D (nzm = 1, or a batch of 2-D instances) the z neighbours are the
-// column itself, leaving vx, vy, vz, temp at (j, j+1, j-1) and pr at (j, j-1): 14 columns.
+// Number of x-columns K1 stages per (j,i) column (FP64 state): vx 5, vy 6, vz 6, temp 5, pr 3.
+// In 2-D (nzm = 1, or a batch of 2-D instances) the z neighbours are the column itself, leaving
+// vx, vy, vz, temp at (j, j+1, j-1) and pr at (j, j-1): 14 columns.  The four centre columns come
+// first; after the explicit phase the others are dead and hold the CN right-hand sides.
 constexpr int kK1StateCols = 25;
 constexpr int kK1StateCols2D = 14;
-constexpr int kK1RuCols = 4;
+constexpr int kK1Centre = 4;
 
-__host__ __device__ inline size_t k1_stage_bytes(int ldx, size_t te_size, bool two_d) {
-  return (size_t)(two_d ? kK1StateCols2D : kK1StateCols) * ldx * sizeof(double) +
-         (size_t)kK1RuCols * ldx * te_size;
+__host__ __device__ inline size_t k1_stage_bytes(int ldx, bool two_d) {
+  return (size_t)(two_d ? kK1StateCols2D : kK1StateCols) * ldx * sizeof(double);
+}
+// Dynamic shared memory of K1: the staged columns, or the centre columns plus the four RHS
+// arrays in chunk layout, whichever is larger.
+__host__ __device__ inline size_t k1_smem(int ldx, int M, bool two_d) {
+  const size_t rhs = (size_t)kK1Centre * ldx * sizeof(double) + (size_t)4 * chunk_ld(M) * M * sizeof(double);
+  const size_t st = k1_stage_bytes(ldx, two_d);
+  return st > rhs ? st : rhs;
 }
 
-// K1: a block owns one (j,i) column.  One thread issues 1-D TMA bulk copies of the 29 needed
-// x-columns (contiguous runs of ldx elements) into shared memory, completing on an mbarrier;
-// then TPC threads each compute the four explicit terms and RHS of RPT cells from shared
-// memory, write the new RK3 histories, and put the scaled RHS in the solver's chunk layout
-// (row r at (r%M)*33 + r/M).  Four warps run the partitioned CN solves, and every thread adds
-// the increments to the staged centre values and stores the intermediate fields.
+// K1: a block owns one (j,i) column.  One thread issues 1-D TMA bulk copies of the needed
+// x-columns (contiguous runs of ldx doubles) into shared memory, completing on an mbarrier;
+// then TPC threads each compute the four explicit terms and RHS of RPT cells from shared memory
+// (the RK3 histories come straight from global memory and are updated in place), and, after a
+// barrier, put the scaled RHS into the chunk layout (row r at (r%M)*LD + r/M) over the dead
+// neighbour columns.  Four warps run the partitioned CN solves, and every thread adds the
+// increments to the staged centre values and stores the intermediate fields.
 template <int M, int TPC, int RPT, typename TE, bool TWO_D>
 __global__ void __launch_bounds__(TPC)
     k_explicit_implicit(Geom g0, Tables t, const StepCoef *__restrict__ sc_all, int ns,
@@ -251,9 +259,7 @@ __global__ void __launch_bounds__(TPC)
   Geom g = g0;
   const int ldx = g.ldx;
   double *cols = reinterpret_cast<double *>(smem_k1);
-  constexpr int NS = TWO_D ? kK1StateCols2D : kK1StateCols;
-  TE *rcols = reinterpret_cast<TE *>(cols + (size_t)NS * ldx);
-  double *s_rhs = reinterpret_cast<double *>(smem_k1 + k1_stage_bytes(ldx, sizeof(TE), TWO_D));
+  double *s_rhs = cols + (size_t)kK1Centre * ldx;  // over the neighbour columns, after they are used
   const int tc = threadIdx.x;
   const int colid = blockIdx.x;
   const int j = colid % g.nym, i = colid / g.nym;
@@ -275,29 +281,38 @@ __global__ void __launch_bounds__(TPC)
   if (tc == 0) {
     const size_t oc = c0, ojp = col_off(g, jp, i), ojm = col_off(g, jm, i), oip = col_off(g, j, ip),
                  oim = col_off(g, j, im), ojpim = col_off(g, jp, im), ojmip = col_off(g, jm, ip);
-    const uint32_t cb = (uint32_t)ldx * sizeof(double), rb = (uint32_t)ldx * sizeof(TE);
-    mbar_arrive_expect_tx(&bar, (uint32_t)k1_stage_bytes(ldx, sizeof(TE), TWO_D));
+    const uint32_t cb = (uint32_t)ldx * sizeof(double);
+    mbar_arrive_expect_tx(&bar, (uint32_t)k1_stage_bytes(ldx, TWO_D));
     if constexpr (TWO_D) {
-      const double *src[kK1StateCols2D] = {vx + oc,   vx + ojp,   vx + ojm,    // 0-2
-                                           vy + oc,   vy + ojp,   vy + ojm,    // 3-5
-                                           vz + oc,   vz + ojp,   vz + ojm,    // 6-8
-                                           temp + oc, temp + ojp, temp + ojm,  // 9-11
-                                           pr + oc,   pr + ojm};               // 12-13
+      const double *src[kK1StateCols2D] = {vx + oc,   vy + oc,    vz + oc, temp + oc,  // 0-3 centre
+                                           vx + ojp,  vx + ojm,                        // 4-5
+                                           vy + ojp,  vy + ojm,                        // 6-7
+                                           vz + ojp,  vz + ojm,                        // 8-9
+                                           temp + ojp, temp + ojm,                     // 10-11
+                                           pr + oc,   pr + ojm};                       // 12-13
 #pragma unroll
       for (int q = 0; q < kK1StateCols2D; ++q) bulk_g2s(cols + (size_t)q * ldx, src[q], cb, &bar);
     } else {
-      const double *src[kK1StateCols] = {vx + oc,   vx + ojp, vx + ojm, vx + oip, vx + oim,  // 0-4
-                                         vy + oc,   vy + ojp, vy + ojm, vy + oip, vy + oim, vy + ojpim,  // 5-10
-                                         vz + oc,   vz + ojp, vz + ojm, vz + oip, vz + oim, vz + ojmip,  // 11-16
-                                         temp + oc, temp + ojp, temp + ojm, temp + oip, temp + oim,      // 17-21
-                                         pr + oc,   pr + ojm, pr + oim};                                // 22-24
+      const double *src[kK1StateCols] = {vx + oc,    vy + oc,    vz + oc,    temp + oc,               // 0-3
+                                         vx + ojp,   vx + ojm,   vx + oip,   vx + oim,                // 4-7
+                                         vy + ojp,   vy + ojm,   vy + oip,   vy + oim,   vy + ojpim,  // 8-12
+                                         vz + ojp,   vz + ojm,   vz + oip,   vz + oim,   vz + ojmip,  // 13-17
+                                         temp + ojp, temp + ojm, temp + oip, temp + oim,              // 18-21
+                                         pr + oc,    pr + ojm,   pr + oim};                           // 22-24
 #pragma unroll
       for (int q = 0; q < kK1StateCols; ++q) bulk_g2s(cols + (size_t)q * ldx, src[q], cb, &bar);
     }
-    bulk_g2s(rcols, rux + oc, rb, &bar);
-    bulk_g2s(rcols + ldx, ruy + oc, rb, &bar);
-    bulk_g2s(rcols + 2 * ldx, ruz + oc, rb, &bar);
-    bulk_g2s(rcols + 3 * ldx, rut + oc, rb, &bar);
+  }
+  // the RK3 histories go straight to registers; their loads overlap the staging copies
+  double uu[RPT][4];
+#pragma unroll
+  for (int p = 0; p < RPT; ++p) {
+    const int k = tc + TPC * p;
+    const bool in = k < g.nxm;
+    uu[p][0] = (in && k >= 1) ? (double)rux[c0 + k] : 0.0;
+    uu[p][1] = in ? (double)ruy[c0 + k] : 0.0;
+    uu[p][2] = in ? (double)ruz[c0 + k] : 0.0;
+    uu[p][3] = in ? (double)rut[c0 + k] : 0.0;
   }
   const bool ok = mbar_wait(&bar, 0, kSpinLimit);
   if (!__syncthreads_and(ok)) {
@@ -307,10 +322,10 @@ __global__ void __launch_bounds__(TPC)
   }
   auto C = [&](int q) { return (const double *)(cols + (size_t)q * ldx); };
   // {centre, j+1, j-1, i+1, i-1, diagonal}; in 2-D the i+-1 columns are the centre's
-  const ColV X = TWO_D ? ColV{C(0), C(1), C(2), C(0), C(0), nullptr} : ColV{C(0), C(1), C(2), C(3), C(4), nullptr};
-  const ColV Y = TWO_D ? ColV{C(3), C(4), C(5), C(3), C(3), C(4)} : ColV{C(5), C(6), C(7), C(8), C(9), C(10)};
-  const ColV Z = TWO_D ? ColV{C(6), C(7), C(8), C(6), C(6), C(8)} : ColV{C(11), C(12), C(13), C(14), C(15), C(16)};
-  const ColV T = TWO_D ? ColV{C(9), C(10), C(11), C(9), C(9), nullptr} : ColV{C(17), C(18), C(19), C(20), C(21), nullptr};
+  const ColV X = TWO_D ? ColV{C(0), C(4), C(5), C(0), C(0), nullptr} : ColV{C(0), C(4), C(5), C(6), C(7), nullptr};
+  const ColV Y = TWO_D ? ColV{C(1), C(6), C(7), C(1), C(1), C(6)} : ColV{C(1), C(8), C(9), C(10), C(11), C(12)};
+  const ColV Z = TWO_D ? ColV{C(2), C(8), C(9), C(2), C(2), C(9)} : ColV{C(2), C(13), C(14), C(15), C(16), C(17)};
+  const ColV T = TWO_D ? ColV{C(3), C(10), C(11), C(3), C(3), nullptr} : ColV{C(3), C(18), C(19), C(20), C(21), nullptr};
   const ColV P = TWO_D ? ColV{C(12), nullptr, C(13), nullptr, C(12), nullptr} : ColV{C(22), nullptr, C(23), nullptr, C(24), nullptr};
   const int slot = sc_slot(g, i, ns);
   const StepCoef sc = sc_all[slot];
@@ -321,30 +336,37 @@ __global__ void __launch_bounds__(TPC)
   const int nxm = g.nxm;
   const size_t pl = (size_t)j + (size_t)g.nym * i;
   const double tbp = __ldg(t.tempbp + pl), ttp = __ldg(t.temptp + pl);
+  double rr[RPT][4];
 #pragma unroll
   for (int p = 0; p < RPT; ++p) {
     const int k = tc + TPC * p;
     if (k < nxm) {
-      // all four right-hand sides first: no shared-memory store separates their operand loads,
-      // so the compiler reuses them across the four fields
       TE q0 = (TE)0, q1, q2, q3;
-      const double r0 = (k >= 1) ? rhs_vx<TE>(g, t, sc, k, X, Y, Z, T, P, (double)rcols[k], q0) : 0.0;
-      const double r1 = rhs_vy<TE>(g, t, sc, k, X, Y, Z, T, P, (double)rcols[ldx + k], q1);
-      const double r2 = rhs_vz<TE>(g, t, sc, k, X, Y, Z, T, P, (double)rcols[2 * ldx + k], q2);
-      const double r3 = rhs_temp<TE>(g, t, sc, k, X, Y, Z, T, tbp, ttp, (double)rcols[3 * ldx + k], q3);
-      const double syz = __ldg(TY + k);
+      const double u0 = uu[p][0], u1 = uu[p][1], u2 = uu[p][2], u3 = uu[p][3];
+      // all four right-hand sides from the staged columns before anything is stored
+      rr[p][0] = (k >= 1) ? rhs_vx<TE>(g, t, sc, k, X, Y, Z, T, P, u0, q0) * __ldg(TX + k - 1) : 0.0;
+      rr[p][1] = rhs_vy<TE>(g, t, sc, k, X, Y, Z, T, P, u1, q1) * __ldg(TY + k);
+      rr[p][2] = rhs_vz<TE>(g, t, sc, k, X, Y, Z, T, P, u2, q2) * __ldg(TY + k);
+      rr[p][3] = rhs_temp<TE>(g, t, sc, k, X, Y, Z, T, tbp, ttp, u3, q3) * __ldg(TT + k);
+      if (k >= 1) rux[c0 + k] = q0;
+      ruy[c0 + k] = q1;
+      ruz[c0 + k] = q2;
+      rut[c0 + k] = q3;
+    }
+  }
+  __syncthreads();  // the neighbour columns are dead from here on
+#pragma unroll
+  for (int p = 0; p < RPT; ++p) {
+    const int k = tc + TPC * p;
+    if (k < nxm) {
       const int sk = (k % M) * LD + k / M;
       if (k >= 1) {
         const int r = k - 1;
-        s_rhs[(r % M) * LD + r / M] = r0 * __ldg(TX + r);
-        rux[c0 + k] = q0;
+        s_rhs[(r % M) * LD + r / M] = rr[p][0];
       }
-      s_rhs[FLD + sk] = r1 * syz;
-      ruy[c0 + k] = q1;
-      s_rhs[2 * FLD + sk] = r2 * syz;
-      ruz[c0 + k] = q2;
-      s_rhs[3 * FLD + sk] = r3 * __ldg(TT + k);
-      rut[c0 + k] = q3;
+      s_rhs[FLD + sk] = rr[p][1];
+      s_rhs[2 * FLD + sk] = rr[p][2];
+      s_rhs[3 * FLD + sk] = rr[p][3];
     }
   }
   // identity padding rows: vx rows nxm-1 .. 32M-1, the others nxm .. 32M-1
@@ -386,10 +408,9 @@ __global__ void __launch_bounds__(TPC)
   }
 }
 
-
 template <int M, int TPC, int RPT, typename TE, bool TWO_D>
 cudaError_t launch_k1_cfg(const LaunchCtx &L, const SubstepBuffers &b, int ns, int ncol) {
-  const size_t smem = k1_stage_bytes(L.g.ldx, sizeof(TE), TWO_D) + (size_t)4 * chunk_ld(M) * M * sizeof(double);
+  const size_t smem = k1_smem(L.g.ldx, M, TWO_D);
   auto kern = k_explicit_implicit<M, TPC, RPT, TE, TWO_D>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;

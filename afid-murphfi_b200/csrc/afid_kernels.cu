@@ -780,7 +780,8 @@ static int pick_M(int nxm) {
 
 int cn_choose_M(int nxm) { return pick_M(nxm); }
 size_t k1_smem_bytes(int ldx, int M, bool mixed, bool two_d) {
-  return k1_stage_bytes(ldx, mixed ? sizeof(float) : sizeof(double), two_d) + (size_t)4 * chunk_ld(M) * M * sizeof(double);
+  (void)mixed;  // the RK3 histories are not staged
+  return k1_smem(ldx, M, two_d);
 }
 size_t cn_tab_doubles(int M, int nsst) { return cn_table_size(M) * 3 * (size_t)nsst; }
 
