@@ -87,11 +87,13 @@ class BatchStatT(C.Structure):
 
 class TuneInfoT(C.Structure):
     _fields_ = [("ncand", C.c_int), ("chosen", C.c_int), ("sample_columns", C.c_int),
-                ("threads", C.c_int * 3), ("rows", C.c_int * 3), ("us", C.c_double * 3)]
+                ("threads", C.c_int * 4), ("rows", C.c_int * 4), ("regcap", C.c_int * 4), ("us", C.c_double * 4)]
 
     def as_dict(self) -> dict:
+        """shapes: [threads per column, rows per thread, register cap, microseconds per sample]"""
         return {"ncand": self.ncand, "chosen": self.chosen, "sample_columns": self.sample_columns,
-                "shapes": [[self.threads[v], self.rows[v], round(self.us[v], 2)] for v in range(self.ncand)]}
+                "shapes": [[self.threads[v], self.rows[v], self.regcap[v], round(self.us[v], 2)]
+                           for v in range(self.ncand)]}
 
 
 class ServeConfigT(C.Structure):

@@ -60,8 +60,8 @@ cudaError_t launch_explicit_implicit(const LaunchCtx &L, const SubstepBuffers &b
 // K1 over the first ncol columns with thread shape `var` (autotuner samples use ncol < all).
 cudaError_t launch_k1_fp64(const LaunchCtx &L, const SubstepBuffers &b, int ns, int var, int ncol);
 cudaError_t launch_k1_mixed(const LaunchCtx &L, const SubstepBuffers &b, int ns, int var, int ncol);
-// Thread shapes of K1 for M: fills tpc[]/rpt[] (up to 3) and returns their number.
-int k1_shapes(int M, int *tpc, int *rpt);
+// Thread shapes of K1 for M: fills tpc[]/rpt[]/cap[] (up to AFID_TUNE_MAX) and returns their number.
+int k1_shapes(int M, int *tpc, int *rpt, int *cap);
 // The kernels of one substep, in launch order (K1 .. K7).
 enum class Stage { ExplicitImplicit = 0, DivFftY, FftZFwd, Tridiag, FftZInv, IfftY, Correct };
 constexpr int kNumStages = 7;

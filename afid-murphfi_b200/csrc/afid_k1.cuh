@@ -59,7 +59,8 @@ __device__ __forceinline__ void cn_solve_chunk(double *__restrict__ s, const dou
 // Explicit terms + RHS, one (k, j, i) point each.  Expressions follow the reference loop
 // bodies term by term; TE is the arithmetic type of the explicit terms.  The operands are
 // x-columns staged in shared memory: c = (j,i), jp/jm = (j+-1,i), ip/im = (j,i+-1),
-// d = the diagonal neighbour (j+1,i-1) for vy and (j-1,i+1) for vz.
+// The diagonal neighbours (vy at (j+1,i-1), vz at (j-1,i+1)) and the pressure at (j-1,i) and
+// (j,i-1) are read at row k only, so they arrive as values (zd, yd, pjm, pim), not columns.
 // ------------------------------------------------------------------------------------------
 struct ColV {
   const double *c, *jp, *jm, *ip, *im, *d;
@@ -107,7 +108,7 @@ __device__ __forceinline__ double rhs_vx(const Geom &g, const Tables &t, const S
 template <typename TE>
 __device__ __forceinline__ double rhs_vy(const Geom &g, const Tables &t, const StepCoef &sc, int k,
                                          const ColV &X, const ColV &Y, const ColV &Z, const ColV &T,
-                                         const ColV &P, double ru, TE &qout) {
+                                         const ColV &P, double zd, double pjm, double ru, TE &qout) {
   const int kmm = (k == 0) ? 0 : k - 1;
   const int kpp = (k == g.nxm - 1) ? k : k + 1;
   const int kp = k + 1;
@@ -120,7 +121,7 @@ __device__ __forceinline__ double rhs_vy(const Geom &g, const Tables &t, const S
                   (cv<TE>(X.c[k]) + cv<TE>(X.jm[k])) * (c + cv<TE>(Y.c[kmm]))) *
                  cv<TE>(__ldg(t.udx3m + k)) * (TE)0.25;
   const TE hyy = ((vyjp + c) * (vyjp + c) - (vyjm + c) * (vyjm + c)) * udy;
-  const TE hyz = ((vyip + c) * (cv<TE>(Z.ip[k]) + cv<TE>(Z.d[k])) - (c + vyim) * (cv<TE>(Z.c[k]) + cv<TE>(Z.jm[k]))) *
+  const TE hyz = ((vyip + c) * (cv<TE>(Z.ip[k]) + cv<TE>(zd)) - (c + vyim) * (cv<TE>(Z.c[k]) + cv<TE>(Z.jm[k]))) *
                  udz;
   const TE dyyvy = (vyjp - (TE)2.0 * c + vyjm) * udyq;
   const TE dzzvy = (vyip - (TE)2.0 * c + vyim) * udzq;
@@ -140,7 +141,7 @@ __device__ __forceinline__ double rhs_vy(const Geom &g, const Tables &t, const S
     dxxvy = -(acc + amm) * g.xplusu * g.inslwn + cd * acc + Y.c[kmm] * amm;
   else
     dxxvy = Y.c[kpp] * app + cd * acc + Y.c[kmm] * amm;
-  const double dyp = (P.c[k] - P.jm[k]) * udyp;
+  const double dyp = (P.c[k] - pjm) * udyp;
   qout = dph;
   return (sc.ga * (double)dph + sc.ro * ru + alre * dxxvy - dyp) * sc.dt;
 }
@@ -149,7 +150,7 @@ __device__ __forceinline__ double rhs_vy(const Geom &g, const Tables &t, const S
 template <typename TE>
 __device__ __forceinline__ double rhs_vz(const Geom &g, const Tables &t, const StepCoef &sc, int k,
                                          const ColV &X, const ColV &Y, const ColV &Z, const ColV &T,
-                                         const ColV &P, double ru, TE &qout) {
+                                         const ColV &P, double yd, double pim, double ru, TE &qout) {
   const int kmm = (k == 0) ? 0 : k - 1;
   const int kpp = (k == g.nxm - 1) ? k : k + 1;
   const int kp = k + 1;
@@ -159,7 +160,7 @@ __device__ __forceinline__ double rhs_vz(const Geom &g, const Tables &t, const S
   const TE vzip = cv<TE>(Z.ip[k]), vzim = cv<TE>(Z.im[k]);
   const TE vzjp = cv<TE>(Z.jp[k]), vzjm = cv<TE>(Z.jm[k]);
   const TE hzz = ((vzip + c) * (vzip + c) - (vzim + c) * (vzim + c)) * udz;
-  const TE hzy = ((cv<TE>(Y.jp[k]) + cv<TE>(Y.d[k])) * (vzjp + c) - (cv<TE>(Y.c[k]) + cv<TE>(Y.im[k])) * (c + vzjm)) *
+  const TE hzy = ((cv<TE>(Y.jp[k]) + cv<TE>(yd)) * (vzjp + c) - (cv<TE>(Y.c[k]) + cv<TE>(Y.im[k])) * (c + vzjm)) *
                  udy;
   const TE hzx = ((cv<TE>(X.c[kp]) + cv<TE>(X.im[kp])) * (cv<TE>(Z.c[kpp]) + c) -
                   (cv<TE>(X.c[k]) + cv<TE>(X.im[k])) * (c + cv<TE>(Z.c[kmm]))) *
@@ -174,7 +175,7 @@ __device__ __forceinline__ double rhs_vz(const Geom &g, const Tables &t, const S
   const double alre = sc.alre;
   const double amm = __ldg(t.am3sk + k), acc = __ldg(t.ac3sk + k), app = __ldg(t.ap3sk + k);
   const double dxxvz = Z.c[kpp] * app + Z.c[k] * acc + Z.c[kmm] * amm;
-  const double dzp = (P.c[k] - P.im[k]) * g.dz * sc.al;
+  const double dzp = (P.c[k] - pim) * g.dz * sc.al;
   qout = dq;
   return (sc.ga * (double)dq + sc.ro * ru + alre * dxxvz - dzp) * sc.dt;
 }
@@ -217,12 +218,14 @@ __device__ __forceinline__ double rhs_temp(const Geom &g, const Tables &t, const
   return (sc.ga * (double)hro + sc.ro * ru + alpec * dxxt) * sc.dt;
 }
 
-// Number of x-columns K1 stages per (j,i) column (FP64 state): vx 5, vy 6, vz 6, temp 5, pr 3.
-// In 2-D (nzm = 1, or a batch of 2-D instances) the z neighbours are the column itself, leaving
-// vx, vy, vz, temp at (j, j+1, j-1) and pr at (j, j-1): 14 columns.  The four centre columns come
-// first; after the explicit phase the others are dead and hold the CN right-hand sides.
-constexpr int kK1StateCols = 25;
-constexpr int kK1StateCols2D = 14;
+// Number of x-columns K1 stages per (j,i) column (FP64 state): vx 5, vy 5, vz 5, temp 5, pr 1
+// (the diagonal vy/vz neighbours and the pressure neighbours are read at one row each and go
+// straight to registers).  In 2-D (nzm = 1, or a batch of 2-D instances) the z neighbours are the
+// column itself, leaving vx, vy, vz, temp at (j, j+1, j-1) and pr at j: 13 columns.  The four
+// centre columns come first; after the explicit phase the others are dead and hold the CN
+// right-hand sides.
+constexpr int kK1StateCols = 21;
+constexpr int kK1StateCols2D = 13;
 constexpr int kK1Centre = 4;
 
 __host__ __device__ inline size_t k1_stage_bytes(int ldx, bool two_d) {
@@ -243,8 +246,10 @@ __host__ __device__ inline size_t k1_smem(int ldx, int M, bool two_d) {
 // barrier, put the scaled RHS into the chunk layout (row r at (r%M)*LD + r/M) over the dead
 // neighbour columns.  Four warps run the partitioned CN solves, and every thread adds the
 // increments to the staged centre values and stores the intermediate fields.
-template <int M, int TPC, int RPT, typename TE, bool TWO_D>
-__global__ void __launch_bounds__(TPC)
+// CAP: at least 16 resident warps per SM (<= 128 registers a thread for blocks of up to 256
+// threads); without it the compiler may use more registers for fewer resident blocks.
+template <int M, int TPC, int RPT, typename TE, bool TWO_D, bool CAP>
+__global__ void __launch_bounds__(TPC, (CAP && TPC < 512) ? 512 / TPC : 1)
     k_explicit_implicit(Geom g0, Tables t, const StepCoef *__restrict__ sc_all, int ns,
                         const double *__restrict__ cn_tab, const double *__restrict__ vx,
                         const double *__restrict__ vy, const double *__restrict__ vz,
@@ -283,28 +288,33 @@ __global__ void __launch_bounds__(TPC)
                  oim = col_off(g, j, im), ojpim = col_off(g, jp, im), ojmip = col_off(g, jm, ip);
     const uint32_t cb = (uint32_t)ldx * sizeof(double);
     mbar_arrive_expect_tx(&bar, (uint32_t)k1_stage_bytes(ldx, TWO_D));
+    (void)ojpim;
+    (void)ojmip;
     if constexpr (TWO_D) {
       const double *src[kK1StateCols2D] = {vx + oc,   vy + oc,    vz + oc, temp + oc,  // 0-3 centre
                                            vx + ojp,  vx + ojm,                        // 4-5
                                            vy + ojp,  vy + ojm,                        // 6-7
                                            vz + ojp,  vz + ojm,                        // 8-9
                                            temp + ojp, temp + ojm,                     // 10-11
-                                           pr + oc,   pr + ojm};                       // 12-13
+                                           pr + oc};                                   // 12
 #pragma unroll
       for (int q = 0; q < kK1StateCols2D; ++q) bulk_g2s(cols + (size_t)q * ldx, src[q], cb, &bar);
     } else {
-      const double *src[kK1StateCols] = {vx + oc,    vy + oc,    vz + oc,    temp + oc,               // 0-3
-                                         vx + ojp,   vx + ojm,   vx + oip,   vx + oim,                // 4-7
-                                         vy + ojp,   vy + ojm,   vy + oip,   vy + oim,   vy + ojpim,  // 8-12
-                                         vz + ojp,   vz + ojm,   vz + oip,   vz + oim,   vz + ojmip,  // 13-17
-                                         temp + ojp, temp + ojm, temp + oip, temp + oim,              // 18-21
-                                         pr + oc,    pr + ojm,   pr + oim};                           // 22-24
+      const double *src[kK1StateCols] = {vx + oc,    vy + oc,    vz + oc,    temp + oc,   // 0-3
+                                         vx + ojp,   vx + ojm,   vx + oip,   vx + oim,    // 4-7
+                                         vy + ojp,   vy + ojm,   vy + oip,   vy + oim,    // 8-11
+                                         vz + ojp,   vz + ojm,   vz + oip,   vz + oim,    // 12-15
+                                         temp + ojp, temp + ojm, temp + oip, temp + oim,  // 16-19
+                                         pr + oc};                                        // 20
 #pragma unroll
       for (int q = 0; q < kK1StateCols; ++q) bulk_g2s(cols + (size_t)q * ldx, src[q], cb, &bar);
     }
   }
+  // single-row operands: diagonal neighbours (3-D) and pressure neighbours, to registers
+  const size_t o_jm = col_off(g, jm, i), o_im = col_off(g, j, im);
+  const size_t o_jpim = col_off(g, jp, im), o_jmip = col_off(g, jm, ip);
   // the RK3 histories go straight to registers; their loads overlap the staging copies
-  double uu[RPT][4];
+  double uu[RPT][4], vv[RPT][4];  // RK3 histories; {vz(j-1,i+1), vy(j+1,i-1), pr(j-1), pr(i-1)}
 #pragma unroll
   for (int p = 0; p < RPT; ++p) {
     const int k = tc + TPC * p;
@@ -313,6 +323,16 @@ __global__ void __launch_bounds__(TPC)
     uu[p][1] = in ? (double)ruy[c0 + k] : 0.0;
     uu[p][2] = in ? (double)ruz[c0 + k] : 0.0;
     uu[p][3] = in ? (double)rut[c0 + k] : 0.0;
+    if constexpr (TWO_D) {
+      vv[p][0] = 0.0;  // taken from the staged vz(j-1) / vy(j+1) columns below
+      vv[p][1] = 0.0;
+      vv[p][3] = 0.0;  // pr(i-1) is the centre column
+    } else {
+      vv[p][0] = in ? __ldg(vz + o_jmip + k) : 0.0;
+      vv[p][1] = in ? __ldg(vy + o_jpim + k) : 0.0;
+      vv[p][3] = in ? __ldg(pr + o_im + k) : 0.0;
+    }
+    vv[p][2] = in ? __ldg(pr + o_jm + k) : 0.0;
   }
   const bool ok = mbar_wait(&bar, 0, kSpinLimit);
   if (!__syncthreads_and(ok)) {
@@ -323,10 +343,11 @@ __global__ void __launch_bounds__(TPC)
   auto C = [&](int q) { return (const double *)(cols + (size_t)q * ldx); };
   // {centre, j+1, j-1, i+1, i-1, diagonal}; in 2-D the i+-1 columns are the centre's
   const ColV X = TWO_D ? ColV{C(0), C(4), C(5), C(0), C(0), nullptr} : ColV{C(0), C(4), C(5), C(6), C(7), nullptr};
-  const ColV Y = TWO_D ? ColV{C(1), C(6), C(7), C(1), C(1), C(6)} : ColV{C(1), C(8), C(9), C(10), C(11), C(12)};
-  const ColV Z = TWO_D ? ColV{C(2), C(8), C(9), C(2), C(2), C(9)} : ColV{C(2), C(13), C(14), C(15), C(16), C(17)};
-  const ColV T = TWO_D ? ColV{C(3), C(10), C(11), C(3), C(3), nullptr} : ColV{C(3), C(18), C(19), C(20), C(21), nullptr};
-  const ColV P = TWO_D ? ColV{C(12), nullptr, C(13), nullptr, C(12), nullptr} : ColV{C(22), nullptr, C(23), nullptr, C(24), nullptr};
+  const ColV Y = TWO_D ? ColV{C(1), C(6), C(7), C(1), C(1), nullptr} : ColV{C(1), C(8), C(9), C(10), C(11), nullptr};
+  const ColV Z = TWO_D ? ColV{C(2), C(8), C(9), C(2), C(2), nullptr} : ColV{C(2), C(12), C(13), C(14), C(15), nullptr};
+  const ColV T = TWO_D ? ColV{C(3), C(10), C(11), C(3), C(3), nullptr} : ColV{C(3), C(16), C(17), C(18), C(19), nullptr};
+  const ColV P = TWO_D ? ColV{C(12), nullptr, nullptr, nullptr, nullptr, nullptr}
+                       : ColV{C(20), nullptr, nullptr, nullptr, nullptr, nullptr};
   const int slot = sc_slot(g, i, ns);
   const StepCoef sc = sc_all[slot];
   const size_t tsz = cn_table_size(M);
@@ -343,10 +364,14 @@ __global__ void __launch_bounds__(TPC)
     if (k < nxm) {
       TE q0 = (TE)0, q1, q2, q3;
       const double u0 = uu[p][0], u1 = uu[p][1], u2 = uu[p][2], u3 = uu[p][3];
+      // 2-D: vz(j-1,i+1) = vz(j-1), vy(j+1,i-1) = vy(j+1), pr(i-1) = pr
+      const double zd = TWO_D ? Z.jm[k] : vv[p][0];
+      const double yd = TWO_D ? Y.jp[k] : vv[p][1];
+      const double pim = TWO_D ? P.c[k] : vv[p][3];
       // all four right-hand sides from the staged columns before anything is stored
       rr[p][0] = (k >= 1) ? rhs_vx<TE>(g, t, sc, k, X, Y, Z, T, P, u0, q0) * __ldg(TX + k - 1) : 0.0;
-      rr[p][1] = rhs_vy<TE>(g, t, sc, k, X, Y, Z, T, P, u1, q1) * __ldg(TY + k);
-      rr[p][2] = rhs_vz<TE>(g, t, sc, k, X, Y, Z, T, P, u2, q2) * __ldg(TY + k);
+      rr[p][1] = rhs_vy<TE>(g, t, sc, k, X, Y, Z, T, P, zd, vv[p][2], u1, q1) * __ldg(TY + k);
+      rr[p][2] = rhs_vz<TE>(g, t, sc, k, X, Y, Z, T, P, yd, pim, u2, q2) * __ldg(TY + k);
       rr[p][3] = rhs_temp<TE>(g, t, sc, k, X, Y, Z, T, tbp, ttp, u3, q3) * __ldg(TT + k);
       if (k >= 1) rux[c0 + k] = q0;
       ruy[c0 + k] = q1;
@@ -408,10 +433,10 @@ __global__ void __launch_bounds__(TPC)
   }
 }
 
-template <int M, int TPC, int RPT, typename TE, bool TWO_D>
+template <int M, int TPC, int RPT, typename TE, bool TWO_D, bool CAP>
 cudaError_t launch_k1_cfg(const LaunchCtx &L, const SubstepBuffers &b, int ns, int ncol) {
   const size_t smem = k1_smem(L.g.ldx, M, TWO_D);
-  auto kern = k_explicit_implicit<M, TPC, RPT, TE, TWO_D>;
+  auto kern = k_explicit_implicit<M, TPC, RPT, TE, TWO_D, CAP>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   kern<<<ncol, TPC, smem, L.stream>>>(L.g, L.t, b.sc, ns, b.cn_tab, b.vx, b.vy, b.vz, b.temp, b.pr,
@@ -421,24 +446,25 @@ cudaError_t launch_k1_cfg(const LaunchCtx &L, const SubstepBuffers &b, int ns, i
 }
 
 // Thread shapes of K1 per M = {1, 2, 4, 8, 12, 16, 24, 32} (rows per lane of the CN solves):
-// {threads per column, rows per thread}, threads x rows >= 32 M.  The first is the default.
+// {threads per column, rows per thread, register cap}, threads x rows >= 32 M.  The first is the
+// default.
 struct K1Shape {
-  int tpc, rpt;
+  int tpc, rpt, cap;
 };
-constexpr int kK1MaxShapes = 3;
+constexpr int kK1MaxShapes = 4;
 constexpr int k1_m_index(int M) {
   return M == 1 ? 0 : M == 2 ? 1 : M == 4 ? 2 : M == 8 ? 3 : M == 12 ? 4 : M == 16 ? 5 : M == 24 ? 6 : 7;
 }
-constexpr int kK1ShapeCount[8] = {1, 2, 2, 2, 3, 3, 3, 2};
+constexpr int kK1ShapeCount[8] = {1, 2, 2, 3, 4, 4, 3, 2};
 constexpr K1Shape kK1Shapes[8][kK1MaxShapes] = {
-    {{32, 1}, {0, 0}, {0, 0}},       // M = 1   (nxm <= 32)
-    {{64, 1}, {32, 2}, {0, 0}},      // M = 2   (<= 64)
-    {{128, 1}, {64, 2}, {0, 0}},     // M = 4   (<= 128)
-    {{256, 1}, {128, 2}, {0, 0}},    // M = 8   (<= 256)
-    {{256, 2}, {384, 1}, {128, 3}},  // M = 12  (<= 384)
-    {{256, 2}, {512, 1}, {128, 4}},  // M = 16  (<= 512)
-    {{256, 4}, {384, 2}, {256, 3}},  // M = 24  (<= 768)
-    {{256, 4}, {512, 2}, {0, 0}},    // M = 32  (<= 1024)
+    {{32, 1, 0}, {0, 0, 0}, {0, 0, 0}, {0, 0, 0}},        // M = 1   (nxm <= 32)
+    {{64, 1, 0}, {32, 2, 1}, {0, 0, 0}, {0, 0, 0}},       // M = 2   (<= 64)
+    {{128, 1, 0}, {64, 2, 1}, {0, 0, 0}, {0, 0, 0}},      // M = 4   (<= 128)
+    {{128, 2, 1}, {256, 1, 0}, {128, 2, 0}, {0, 0, 0}},   // M = 8   (<= 256)
+    {{128, 3, 1}, {256, 2, 1}, {384, 1, 0}, {128, 3, 0}}, // M = 12  (<= 384)
+    {{128, 4, 1}, {256, 2, 1}, {512, 1, 0}, {128, 4, 0}}, // M = 16  (<= 512)
+    {{256, 3, 1}, {384, 2, 0}, {256, 4, 1}, {0, 0, 0}},   // M = 24  (<= 768)
+    {{256, 4, 1}, {512, 2, 0}, {0, 0, 0}, {0, 0, 0}},     // M = 32  (<= 1024)
 };
 
 template <int M, int V, typename TE, bool TWO_D>
@@ -446,8 +472,9 @@ cudaError_t launch_k1_v(const LaunchCtx &L, const SubstepBuffers &b, int ns, int
   constexpr int mi = k1_m_index(M);
   if constexpr (V < kK1ShapeCount[mi]) {
     constexpr int TPC = kK1Shapes[mi][V].tpc, RPT = kK1Shapes[mi][V].rpt;
+    constexpr bool CAP = kK1Shapes[mi][V].cap != 0;
     static_assert(TPC * RPT >= 32 * M, "K1 shape must cover 32*M rows");
-    return launch_k1_cfg<M, TPC, RPT, TE, TWO_D>(L, b, ns, ncol);
+    return launch_k1_cfg<M, TPC, RPT, TE, TWO_D, CAP>(L, b, ns, ncol);
   } else {
     return cudaErrorInvalidValue;
   }
@@ -459,6 +486,7 @@ cudaError_t launch_k1_M(const LaunchCtx &L, const SubstepBuffers &b, int ns, int
     case 0: return launch_k1_v<M, 0, TE, TWO_D>(L, b, ns, ncol);
     case 1: return launch_k1_v<M, 1, TE, TWO_D>(L, b, ns, ncol);
     case 2: return launch_k1_v<M, 2, TE, TWO_D>(L, b, ns, ncol);
+    case 3: return launch_k1_v<M, 3, TE, TWO_D>(L, b, ns, ncol);
   }
   return cudaErrorInvalidValue;
 }

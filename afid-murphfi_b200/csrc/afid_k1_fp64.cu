@@ -8,11 +8,12 @@ cudaError_t launch_k1_fp64(const LaunchCtx &L, const SubstepBuffers &b, int ns, 
   return two_d ? launch_k1_T<double, true>(L, b, ns, var, ncol) : launch_k1_T<double, false>(L, b, ns, var, ncol);
 }
 
-int k1_shapes(int M, int *tpc, int *rpt) {
+int k1_shapes(int M, int *tpc, int *rpt, int *cap) {
   const int mi = k1_m_index(M);
   for (int v = 0; v < kK1ShapeCount[mi]; ++v) {
     if (tpc) tpc[v] = kK1Shapes[mi][v].tpc;
     if (rpt) rpt[v] = kK1Shapes[mi][v].rpt;
+    if (cap) cap[v] = kK1Shapes[mi][v].cap;
   }
   return kK1ShapeCount[mi];
 }

@@ -265,7 +265,7 @@ def test_k1_shapes_bitwise_identical(shape, precision):
     outs = []
     with case.solver() as g:
         info = g.autotune()
-    assert info["ncand"] >= 2 and all(us > 0 for _, _, us in info["shapes"])
+    assert info["ncand"] >= 2 and all(us > 0 for _, _, _, us in info["shapes"])
     for v in range(info["ncand"]):
         with case.solver() as g:
             g.set_k1_shape(v)
