@@ -177,6 +177,8 @@ def run_gpu(args):
     stream = torch.cuda.Stream()
     solver = ag.Solver(tables.grid, tables.params)
     solver.set_stream(stream.cuda_stream)
+    if args.k1_shape >= 0:  # a saved autotuner pick (profiling runs use the bench's pick)
+        solver.set_k1_shape(args.k1_shape)
     temp0 = tables.initial_temperature(20261203)
     nx, nym, nzm = w["nxm"] + 1, w["nym"], w["nzm"]
     zeros = np.zeros((nzm, nym, nx))
@@ -669,6 +671,7 @@ def main():
     ap.add_argument("--impl", default="afid", choices=["afid", "reference"])
     ap.add_argument("--config", default="rbc3d", choices=sorted(WORKLOADS) + ["batched", "batched_fp64", "served"])
     ap.add_argument("--no-nu-check", action="store_true")
+    ap.add_argument("--k1-shape", type=int, default=-1, help="fixed K1 thread shape instead of autotuning")
     ap.add_argument("--jobs", type=int, default=100, help="served: number of jobs")
     ap.add_argument("--chunk", type=int, default=50, help="served: steps per pump")
     ap.add_argument("--slots", type=int, default=32, help="served: 2-D slots per pool")
