@@ -120,6 +120,10 @@ class ServeStatusT(C.Structure):
 
 SERVE_FIFO, SERVE_SHORTEST_FIRST = 0, 1
 
+# afid_gpu_mean_profiles order (the means.h5 dataset names of CalcMeanProfiles.F90)
+PROFILE_NAMES = ("Tbar", "vybar", "vzbar", "vxT", "vyT", "vzT", "Trms", "vxrms", "vyrms", "vzrms",
+                 "vxvy", "vxvz", "vyvz", "chiT", "epsilon")
+
 # Every symbol declared in include/afid_gpu.h, afid_host.h, afid_batch.h and afid_serve.h
 EXPORTS = [
     "afid_gpu_create", "afid_gpu_destroy", "afid_gpu_set_stream", "afid_gpu_get_stream",
@@ -138,7 +142,7 @@ EXPORTS = [
     "afid_batch_device_bytes", "afid_batch_launch_count",
     "afid_serve_create", "afid_serve_destroy", "afid_serve_submit", "afid_serve_pump", "afid_serve_poll",
     "afid_serve_status", "afid_serve_now", "afid_gpu_autotune", "afid_batch_autotune",
-    "afid_gpu_set_k1_shape",
+    "afid_gpu_set_k1_shape", "afid_gpu_mean_profiles", "afid_batch_mean_profiles",
 ]
 
 
@@ -198,6 +202,8 @@ def load_library(path: str = _LIB_PATH) -> C.CDLL:
         "afid_serve_now": (d, [vp]),
         "afid_gpu_autotune": (i, [vp, i, C.POINTER(TuneInfoT)]),
         "afid_gpu_set_k1_shape": (i, [vp, i]),
+        "afid_gpu_mean_profiles": (i, [vp, _dp]),
+        "afid_batch_mean_profiles": (i, [vp, i, _dp]),
         "afid_batch_autotune": (i, [vp, i, C.POINTER(TuneInfoT)]),
         "afid_batch_step": (i, [vp, i]),
         "afid_batch_synchronize": (i, [vp]),
@@ -368,6 +374,12 @@ class Solver:
         _check(lib().afid_gpu_autotune(self._h, int(force), C.byref(info)), "afid_gpu_autotune")
         return info.as_dict()
 
+    def mean_profiles(self) -> dict:
+        """CalcMeanProfiles.F90 profiles (means.h5 dataset names) from the device state."""
+        out = np.zeros((len(PROFILE_NAMES), self.nxm))
+        _check(lib().afid_gpu_mean_profiles(self._h, _ptr(out)), "afid_gpu_mean_profiles")
+        return dict(zip(PROFILE_NAMES, out))
+
     def set_k1_shape(self, index: int) -> None:
         _check(lib().afid_gpu_set_k1_shape(self._h, index), "afid_gpu_set_k1_shape")
 
@@ -473,6 +485,11 @@ class Batch:
 
     def device_bytes(self) -> int:
         return int(lib().afid_batch_device_bytes(self._h))
+
+    def mean_profiles(self, slot: int) -> dict:
+        out = np.zeros((len(PROFILE_NAMES), self.nxm))
+        _check(lib().afid_batch_mean_profiles(self._h, slot, _ptr(out)), "afid_batch_mean_profiles")
+        return dict(zip(PROFILE_NAMES, out))
 
     def autotune(self, force: bool = False) -> dict:
         info = TuneInfoT()

@@ -370,6 +370,13 @@ int ctx_create(const afid_grid_t *grid, const afid_params_t *prm, const BatchSpe
   size_t o_ak1 = bs ? put(nullptr, 0, nzm) : put(grid->ak1, nzm, nzm);
   size_t o_ak2 = bs ? put(bs->ak2, nym * nzm, nym * nzm) : put(grid->ak2, nym, nym);
   size_t o_g3rc = put(grid->g3rc, nx, L1);
+  // g3rm from the cell centres as CreateGrid.F90 builds it (xm[nx-1] is the ghost centre)
+  std::vector<double> g3rm(nx, 0.0);
+  if (grid->xm && grid->xc) {
+    for (int kc = 1; kc < nxm; ++kc) g3rm[kc] = (grid->xm[kc + 1] - grid->xm[kc - 1]) * g.dx * 0.5;
+    g3rm[0] = (grid->xm[1] - (2 * grid->xc[0] - grid->xm[0])) * g.dx * 0.5;
+  }
+  size_t o_g3rm = put(g3rm.data(), nx, L1);
   std::vector<double> tbp((size_t)nym * nzm, 0.5), ttp((size_t)nym * nzm, -0.5);
   const double *src_bp = bs ? bs->tempbp : prm->tempbp, *src_tp = bs ? bs->temptp : prm->temptp;
   if (src_bp) std::memcpy(tbp.data(), src_bp, tbp.size() * sizeof(double));
@@ -399,6 +406,7 @@ int ctx_create(const afid_grid_t *grid, const afid_params_t *prm, const BatchSpe
     t.ak1 = dtab + o_ak1;
     t.ak2 = dtab + o_ak2;
     t.g3rc = dtab + o_g3rc;
+    t.g3rm = dtab + o_g3rm;
     t.tempbp = dtab + o_tbp;
     t.temptp = dtab + o_ttp;
     ctx->am[0] = t.am3ck; ctx->ac[0] = t.ac3ck; ctx->ap[0] = t.ap3ck;
@@ -625,6 +633,7 @@ int afid_gpu_destroy(afid_ctx_t *ctx) {
   cudaSetDevice(ctx->dev);
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   for (void *p : ctx->allocs) cudaFree(p);
+  if (ctx->stats_buf) cudaFree(ctx->stats_buf);
   for (cudaEvent_t e : ctx->ev_pool) cudaEventDestroy(e);
   if (ctx->host_scratch) cudaFreeHost(ctx->host_scratch);
   if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);

@@ -615,6 +615,17 @@ long long afid_batch_device_bytes(const afid_batch_t *b) { return b ? b->bytes +
 
 long long afid_batch_launch_count(const afid_batch_t *b) { return b ? b->launches : 0; }
 
+int afid_batch_mean_profiles(afid_batch_t *b, int slot, double *out) {
+  if (!b || !out || slot < 0 || slot >= b->nslots) return AFID_E_INVALID;
+  afid_ctx_t *ctx = b->ctx;
+  cudaSetDevice(ctx->dev);
+  const Geom &g = ctx->L.g;
+  const InstScal &sc = b->inst_h[slot];
+  if (b->three_d)
+    return ctx_mean_profiles(ctx, 0, g.nym * g.nzm, (double)g.nym * (double)g.nzm, g.ren, g.pect, out);
+  return ctx_mean_profiles(ctx, slot * g.nym, g.nym, (double)g.nym, sc.ren, sc.pect, out);
+}
+
 int afid_batch_autotune(afid_batch_t *b, int force, afid_tune_info_t *info) {
   if (!b) return AFID_E_INVALID;
   cudaSetDevice(b->ctx->dev);

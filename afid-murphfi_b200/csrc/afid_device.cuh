@@ -63,6 +63,7 @@ struct Tables {
   const double *amphk, *acphk, *apphk;
   const double *ak1, *ak2;
   const double *g3rc;
+  const double *g3rm;  // cell-centre metric (CreateGrid.F90), for the profile gradients
   const double *tempbp, *temptp;  // nym*nzm, y fastest
 };
 

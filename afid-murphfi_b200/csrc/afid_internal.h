@@ -108,6 +108,9 @@ struct afid_ctx {
   size_t ev_used = 0;
   struct Rec { int cls; size_t a, b; };
   std::vector<Rec> recs;
+  // scratch of the profile reductions (afid_stats.cu), allocated on first use
+  double *stats_buf = nullptr;
+  size_t stats_elems = 0;
   // K1 thread-shape autotuner
   bool tuned = false;
   afid_tune_info_t tune{};
@@ -135,6 +138,7 @@ int ctx_build_cn_batch(afid_ctx_t *ctx, const double *dt_dev);
 int ctx_fail(afid_ctx_t *ctx, cudaError_t e);
 int ctx_update_params(afid_ctx_t *ctx, const afid_grid_t *grid, const afid_params_t *prm);
 int ctx_autotune(afid_ctx_t *ctx, bool force);
+int ctx_mean_profiles(afid_ctx_t *ctx, int col0, int ncols, double ny_nz, double ren, double pect, double *out);
 
 }  // namespace afid
 

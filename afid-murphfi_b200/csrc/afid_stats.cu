@@ -1,0 +1,177 @@
+// afid_stats.cu — wall-normal profiles of CalcMeanProfiles.F90 on the device.
+//
+// The fifteen y-z averages written to means.h5 (Tbar, vybar, vzbar, vxT, vyT, vzT, Trms, vxrms,
+// vyrms, vzrms, vxvy, vxvz, vyvz, chiT, epsilon) are reduced in two passes: every block walks a
+// strided set of x-columns with one thread per wall-normal row k and keeps the fifteen running
+// sums in registers, writes them as one partial row per block, and a second kernel adds the
+// partials in block order (deterministic, no atomics).  The host applies the reference's
+// normalisation (CalcMeanProfiles.F90:88-102, 203-207).
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <vector>
+
+#include "afid_internal.h"
+
+namespace afid {
+
+constexpr int kNumProfiles = 15;
+
+// Sums over the columns [col0, col0 + ncols) of the fifteen integrands of
+// CalcMeanProfiles.F90:48-72 (means and second moments), :104-128 (chiT) and :164-199
+// (epsilon).  Block = one thread per row k (blockDim.x >= nxm); partial[(b*15 + q)*nxm + k].
+__global__ void __launch_bounds__(1024)
+    k_mean_partial(Geom g0, Tables t, const double *__restrict__ vx, const double *__restrict__ vy,
+                   const double *__restrict__ vz, const double *__restrict__ temp, int col0, int ncols,
+                   double *__restrict__ partial) {
+  const int k = threadIdx.x;
+  const int nxm = g0.nxm;
+  double acc[kNumProfiles];
+#pragma unroll
+  for (int q = 0; q < kNumProfiles; ++q) acc[q] = 0.0;
+  if (k < nxm) {
+    const int kp = k + 1, km = k - 1;
+    const bool lo = (k == 0), hi = (k == nxm - 1);
+    const double udx3m = __ldg(t.udx3m + k);
+    const double tdx = 0.5 * g0.dx / __ldg(t.g3rm + k);                       // :113-126
+    const double tdx2 = 0.125 * (g0.dx / __ldg(t.g3rm + k)) * (g0.dx / __ldg(t.g3rm + k));  // :182-197
+    for (int cc = blockIdx.x; cc < ncols; cc += gridDim.x) {
+      const int col = col0 + cc;
+      const int j = col % g0.nym, i = col / g0.nym;
+      Geom g = g0;
+      bind_instance(g, i);
+      const int jp = wrap_inc(j, g.nym), jm = wrap_dec(j, g.nym);
+      const int ip = zinc(g, i), im = zdec(g, i);
+      const size_t c = col_off(g, j, i), cjp = col_off(g, jp, i), cjm = col_off(g, jm, i);
+      const size_t cip = col_off(g, j, ip), cim = col_off(g, j, im);
+      const size_t cjpip = col_off(g, jp, ip), cjpim = col_off(g, jp, im), cjmip = col_off(g, jm, ip);
+      const double tc = temp[c + k];
+      const double vxc = vx[c + k], vxp = vx[c + kp];
+      const double vyc = vy[c + k], vyjp = vy[cjp + k];
+      const double vzc = vz[c + k], vzip = vz[cip + k];
+      const double vxm = 0.5 * (vxc + vxp), vym = 0.5 * (vyc + vyjp), vzm = 0.5 * (vzc + vzip);
+      acc[0] += tc;
+      acc[1] += vym;
+      acc[2] += vzm;
+      acc[3] += vxm * tc;
+      acc[4] += vym * tc;
+      acc[5] += vzm * tc;
+      acc[6] += tc * tc;
+      acc[7] += 0.5 * (vxc * vxc + vxp * vxp);
+      acc[8] += 0.5 * (vyc * vyc + vyjp * vyjp);
+      acc[9] += 0.5 * (vzc * vzc + vzip * vzip);
+      acc[10] += 0.25 * (vxc + vxp) * (vyc + vyjp);
+      acc[11] += 0.25 * (vxc + vxp) * (vzc + vzip);
+      acc[12] += 0.25 * (vyc + vyjp) * (vzc + vzip);
+      // chiT: horizontal gradients, then the wall-normal one with the plate values at the walls
+      const double tz = (temp[cip + k] - temp[cim + k]) * 0.5 * g.dz;
+      const double ty = (temp[cjp + k] - temp[cjm + k]) * 0.5 * g.dy;
+      double tx;
+      const size_t pl = (size_t)j + (size_t)g.nym * i;
+      if (lo)
+        tx = temp[c + 1] - tc + 2.0 * g.tfixs * (tc - __ldg(t.tempbp + pl));
+      else if (hi)
+        tx = tc - temp[c + km] + 2.0 * g.tfixn * (__ldg(t.temptp + pl) - tc);
+      else
+        tx = temp[c + kp] - temp[c + km];
+      acc[13] += tz * tz + ty * ty + (tx * tdx) * (tx * tdx);
+      // epsilon: the seven interior terms, then the wall-normal derivatives of vz and vy
+      const double dz = g.dz, dy = g.dy;
+      const double e1 = (vzip - vzc) * dz;
+      const double a2 = vy[cjpip + k] - vy[cjpim + k], b2 = vy[cip + k] - vy[cim + k];
+      const double a3 = vx[cip + kp] - vx[cim + kp], b3 = vx[cip + k] - vx[cim + k];
+      const double a4 = vz[cjpip + k] - vz[cjmip + k], b4 = vz[cjp + k] - vz[cjm + k];
+      const double e5 = (vyjp - vyc) * dy;
+      const double a6 = vx[cjp + kp] - vx[cjm + kp], b6 = vx[cjp + k] - vx[cjm + k];
+      const double e7 = (vxp - vxc) * udx3m;
+      double eps = e1 * e1 + 0.125 * dz * dz * (a2 * a2 + b2 * b2) + 0.125 * dz * dz * (a3 * a3 + b3 * b3) +
+                   0.125 * dy * dy * (a4 * a4 + b4 * b4) + e5 * e5 + 0.125 * dy * dy * (a6 * a6 + b6 * b6) + e7 * e7;
+      double zxi, zxc, yxj, yxc;  // d/dx of vz at (j, i+1), (j, i) and vy at (j+1, i), (j, i)
+      const double vzip0 = vz[cip + k], vyjp0 = vy[cjp + k];
+      if (lo) {
+        zxi = vz[cip + 1] - vzip0 + g.inslws * 2.0 * (vzip0 - 0.0);
+        zxc = vz[c + 1] - vzc + g.inslws * 2.0 * (vzc - 0.0);
+        yxj = vy[cjp + 1] - vyjp0 + g.inslws * 2.0 * (vyjp0 - g.xminusu);
+        yxc = vy[c + 1] - vyc + g.inslws * 2.0 * (vyc - g.xminusu);
+      } else if (hi) {
+        zxi = vzip0 - vz[cip + km] + g.inslwn * 2.0 * (0.0 - vzip0);
+        zxc = vzc - vz[c + km] + g.inslwn * 2.0 * (0.0 - vzc);
+        yxj = vyjp0 - vy[cjp + km] + g.inslwn * 2.0 * (g.xplusu - vyjp0);
+        yxc = vyc - vy[c + km] + g.inslwn * 2.0 * (g.xplusu - vyc);
+      } else {
+        zxi = vz[cip + kp] - vz[cip + km];
+        zxc = vz[c + kp] - vz[c + km];
+        yxj = vy[cjp + kp] - vy[cjp + km];
+        yxc = vy[c + kp] - vy[c + km];
+      }
+      eps += tdx2 * (zxi * zxi + zxc * zxc) + tdx2 * (yxj * yxj + yxc * yxc);
+      acc[14] += eps;
+    }
+  }
+  if (k < nxm) {
+#pragma unroll
+    for (int q = 0; q < kNumProfiles; ++q) partial[((size_t)blockIdx.x * kNumProfiles + q) * nxm + k] = acc[q];
+  }
+}
+
+__global__ void k_mean_reduce(const double *__restrict__ partial, int nblocks, int nxm, double *__restrict__ out) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;  // e = q*nxm + k
+  if (e >= kNumProfiles * nxm) return;
+  double s = 0.0;
+  for (int b = 0; b < nblocks; ++b) s += partial[(size_t)b * kNumProfiles * nxm + e];
+  out[e] = s;
+}
+
+}  // namespace afid
+
+using namespace afid;
+
+namespace afid {
+
+// Profiles of the columns [col0, col0 + ncols) into host out[15 * nxm], normalised by ny_nz
+// (the number of y-z points averaged over) with the instance's ren / pect.
+int ctx_mean_profiles(afid_ctx_t *ctx, int col0, int ncols, double ny_nz, double ren, double pect, double *out) {
+  const Geom &g = ctx->L.g;
+  const int nxm = g.nxm;
+  const int nb = std::min(ncols, 148 * 4);
+  const size_t need = (size_t)nb * kNumProfiles * nxm + (size_t)kNumProfiles * nxm;
+  if (ctx->stats_elems < need) {
+    if (ctx->stats_buf) cudaFree(ctx->stats_buf);
+    ctx->stats_buf = nullptr;
+    ctx->stats_elems = 0;
+    if (cudaMalloc(&ctx->stats_buf, need * sizeof(double)) != cudaSuccess) return AFID_E_ALLOC;
+    ctx->stats_elems = need;
+  }
+  double *partial = ctx->stats_buf, *sums = ctx->stats_buf + (size_t)nb * kNumProfiles * nxm;
+  const int threads = (nxm + 31) / 32 * 32;
+  k_mean_partial<<<nb, threads, 0, ctx->stream>>>(g, ctx->L.t, ctx->vx, ctx->vy, ctx->vz, ctx->temp, col0, ncols,
+                                                  partial);
+  k_mean_reduce<<<(kNumProfiles * nxm + 255) / 256, 256, 0, ctx->stream>>>(partial, nb, nxm, sums);
+  ctx->launches += 2;
+  cudaError_t e = cudaGetLastError();
+  std::vector<double> h((size_t)kNumProfiles * nxm);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(h.data(), sums, h.size() * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+  if (e != cudaSuccess) return ctx_fail(ctx, e);
+  // CalcMeanProfiles.F90:88-102 (x inym x inzm), square roots of the rms rows, :203-207
+  const double inv = 1.0 / ny_nz;
+  for (int q = 0; q < kNumProfiles; ++q)
+    for (int k = 0; k < nxm; ++k) {
+      double v = h[(size_t)q * nxm + k] * inv;
+      if (q >= 6 && q <= 9) v = std::sqrt(v);
+      if (q == 13) v /= pect;
+      if (q == 14) v /= ren;
+      out[(size_t)q * nxm + k] = v;
+    }
+  return AFID_OK;
+}
+
+}  // namespace afid
+
+extern "C" int afid_gpu_mean_profiles(afid_ctx_t *ctx, double *out) {
+  if (!ctx || !out || ctx->L.g.batch) return AFID_E_INVALID;
+  cudaSetDevice(ctx->dev);
+  const Geom &g = ctx->L.g;
+  return ctx_mean_profiles(ctx, 0, g.nym * g.nzm, (double)g.nym * (double)g.nzm, g.ren, g.pect, out);
+}

@@ -74,6 +74,8 @@ long long afid_batch_launch_count(const afid_batch_t *b);
 /* The autotuner of include/afid_gpu.h on this batch's stacked domain (runs by itself before the
  * first captured step). */
 int afid_batch_autotune(afid_batch_t *b, int force, afid_tune_info_t *info);
+/* CalcMeanProfiles.F90 profiles of one slot (layout of afid_gpu_mean_profiles). */
+int afid_batch_mean_profiles(afid_batch_t *b, int slot, double *out);
 
 #ifdef __cplusplus
 }

@@ -129,6 +129,12 @@ int afid_gpu_field_device_ptr(afid_ctx_t *ctx, int which, void **dptr, int *ldx)
 /* Kernels launched by this context since creation (all are this library's own kernels). */
 long long afid_gpu_launch_count(afid_ctx_t *ctx);
 
+/* Wall-normal profiles of CalcMeanProfiles.F90 (the means.h5 datasets), computed on the device
+ * from the resident state: out[AFID_NUM_PROFILES * nxm], profile q at out + q*nxm, in the order
+ * Tbar, vybar, vzbar, vxT, vyT, vzT, Trms, vxrms, vyrms, vzrms, vxvy, vxvz, vyvz, chiT, epsilon. */
+#define AFID_NUM_PROFILES 15
+int afid_gpu_mean_profiles(afid_ctx_t *ctx, double *out);
+
 /* Autotuner of the fused explicit/implicit kernel: every thread shape available for this
  * wall-normal size (threads per x-column block x rows per thread) is timed on a sample of
  * columns, with the RK3 histories redirected to scratch memory so the state is untouched, and

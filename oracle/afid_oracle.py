@@ -984,3 +984,87 @@ def run(g: Grid, s: State, nsteps: int, callback=None):
         if err:
             break
     return time, dt, err
+
+
+# ----------------------------------------------------------------------------------------------
+# Wall-normal profiles (CalcMeanProfiles.F90)
+# ----------------------------------------------------------------------------------------------
+MEAN_PROFILE_NAMES = ("Tbar", "vybar", "vzbar", "vxT", "vyT", "vzT", "Trms", "vxrms", "vyrms", "vzrms",
+                      "vxvy", "vxvz", "vyvz", "chiT", "epsilon")
+
+
+def mean_profiles(g: Grid, s: State) -> dict:
+    """``CalcMeanProfiles.F90:37-208``: the fifteen y-z averaged profiles written to means.h5,
+    each of length nxm (names as the datasets, order of ``MEAN_PROFILE_NAMES``)."""
+    p = g.p
+    nxm = p.nxm
+    inym, inzm = 1.0 / p.nym, 1.0 / p.nzm
+    vx, vy, vz, t = s.vx, s.vy, s.vz, s.temp
+    K = np.arange(nxm)
+    vxc, vxp = vx[..., K], vx[..., K + 1]
+    vyc, vyjp = vy[..., :nxm], _jp(vy)[..., :nxm]
+    vzc, vzip = vz[..., :nxm], _ip(vz)[..., :nxm]
+    tc = t[..., :nxm]
+
+    def sums(a):
+        return a.sum(axis=(0, 1))
+
+    out = {}
+    # :48-72 sums, :88-102 normalisation
+    out["Tbar"] = sums(tc) * inym * inzm
+    out["vybar"] = sums(0.5 * (vyc + vyjp)) * inym * inzm
+    out["vzbar"] = sums(0.5 * (vzc + vzip)) * inym * inzm
+    out["vxT"] = sums(0.5 * (vxc + vxp) * tc) * inym * inzm
+    out["vyT"] = sums(0.5 * (vyc + vyjp) * tc) * inym * inzm
+    out["vzT"] = sums(0.5 * (vzc + vzip) * tc) * inym * inzm
+    out["Trms"] = np.sqrt(sums(tc ** 2) * inym * inzm)
+    out["vxrms"] = np.sqrt(sums(0.5 * (vxc ** 2 + vxp ** 2)) * inym * inzm)
+    out["vyrms"] = np.sqrt(sums(0.5 * (vyc ** 2 + vyjp ** 2)) * inym * inzm)
+    out["vzrms"] = np.sqrt(sums(0.5 * (vzc ** 2 + vzip ** 2)) * inym * inzm)
+    out["vxvy"] = sums(0.25 * (vxc + vxp) * (vyc + vyjp)) * inym * inzm
+    out["vxvz"] = sums(0.25 * (vxc + vxp) * (vzc + vzip)) * inym * inzm
+    out["vyvz"] = sums(0.25 * (vyc + vyjp) * (vzc + vzip)) * inym * inzm
+
+    # :104-128 thermal dissipation
+    dy, dz, dx = g.dy, g.dz, g.dx
+    chi = ((_ip(t) - _im(t))[..., :nxm] * 0.5 * dz) ** 2 + ((_jp(t) - _jm(t))[..., :nxm] * 0.5 * dy) ** 2
+    tdx = 0.5 * dx / g.g3rm[:nxm]
+    dT = np.empty_like(tc)
+    dT[..., 0] = t[..., 1] - t[..., 0] + 2.0 * p.tfixs * (t[..., 0] - s.tempbp)
+    dT[..., 1:nxm - 1] = t[..., 2:nxm] - t[..., 0:nxm - 2]
+    dT[..., nxm - 1] = t[..., nxm - 1] - t[..., nxm - 2] + 2.0 * p.tfixn * (s.temptp - t[..., nxm - 1])
+    chi = chi + (dT * tdx) ** 2
+    out["chiT"] = sums(chi) * inym * inzm / g.pect  # :203-207
+
+    # :164-199 viscous dissipation
+    vzip_, vyip_, vyim_, vxip_, vxim_ = _ip(vz), _ip(vy), _im(vy), _ip(vx), _im(vx)
+    eps = (((vzip_ - vz)[..., :nxm] * dz) ** 2
+           + 0.125 * dz ** 2 * ((_jp(vyip_) - _jp(vyim_))[..., :nxm] ** 2 + (vyip_ - vyim_)[..., :nxm] ** 2)
+           + 0.125 * dz ** 2 * ((vxip_ - vxim_)[..., K + 1] ** 2 + (vxip_ - vxim_)[..., K] ** 2)
+           + 0.125 * dy ** 2 * ((_jp(vzip_) - _jm(vzip_))[..., :nxm] ** 2 + (_jp(vz) - _jm(vz))[..., :nxm] ** 2)
+           + ((_jp(vy) - vy)[..., :nxm] * dy) ** 2
+           + 0.125 * dy ** 2 * ((_jp(vx) - _jm(vx))[..., K + 1] ** 2 + (_jp(vx) - _jm(vx))[..., K] ** 2)
+           + ((vxp - vxc) * g.udx3m[:nxm]) ** 2)
+    tdx2 = 0.125 * (dx / g.g3rm[:nxm]) ** 2
+    vyjp_ = _jp(vy)
+    dzx = np.empty_like(tc)
+    dzx_i = np.empty_like(tc)
+    dyx = np.empty_like(tc)
+    dyx_j = np.empty_like(tc)
+    # wall rows with the no-slip / moving-wall ghost values, interior central differences
+    dzx[..., 0] = vzip_[..., 1] - vzip_[..., 0] + p.inslws * 2.0 * (vzip_[..., 0] - 0.0)
+    dzx_i[..., 0] = vz[..., 1] - vz[..., 0] + p.inslws * 2.0 * (vz[..., 0] - 0.0)
+    dyx[..., 0] = vyjp_[..., 1] - vyjp_[..., 0] + p.inslws * 2.0 * (vyjp_[..., 0] - p.xminusu)
+    dyx_j[..., 0] = vy[..., 1] - vy[..., 0] + p.inslws * 2.0 * (vy[..., 0] - p.xminusu)
+    dzx[..., 1:nxm - 1] = vzip_[..., 2:nxm] - vzip_[..., 0:nxm - 2]
+    dzx_i[..., 1:nxm - 1] = vz[..., 2:nxm] - vz[..., 0:nxm - 2]
+    dyx[..., 1:nxm - 1] = vyjp_[..., 2:nxm] - vyjp_[..., 0:nxm - 2]
+    dyx_j[..., 1:nxm - 1] = vy[..., 2:nxm] - vy[..., 0:nxm - 2]
+    n1 = nxm - 1
+    dzx[..., n1] = vzip_[..., n1] - vzip_[..., n1 - 1] + p.inslwn * 2.0 * (0.0 - vzip_[..., n1])
+    dzx_i[..., n1] = vz[..., n1] - vz[..., n1 - 1] + p.inslwn * 2.0 * (0.0 - vz[..., n1])
+    dyx[..., n1] = vyjp_[..., n1] - vyjp_[..., n1 - 1] + p.inslwn * 2.0 * (p.xplusu - vyjp_[..., n1])
+    dyx_j[..., n1] = vy[..., n1] - vy[..., n1 - 1] + p.inslwn * 2.0 * (p.xplusu - vy[..., n1])
+    eps = eps + tdx2 * (dzx ** 2 + dzx_i ** 2) + tdx2 * (dyx ** 2 + dyx_j ** 2)
+    out["epsilon"] = sums(eps) * inym * inzm / g.ren
+    return out

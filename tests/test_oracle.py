@@ -167,3 +167,21 @@ def test_oracle_reproduces_golden_fixture(path):
             for f in ("vx", "vy", "vz", "temp"):
                 np.testing.assert_allclose(getattr(s, f), d[f"step{n + 1}_{f}"], rtol=0, atol=1e-13)
     assert o.nusselt_volume(g, s) == pytest.approx(float(d["step3_nu"]), rel=1e-13)
+
+
+@pytest.mark.parametrize("istr3,nxm", [(4, 32), (0, 24), (6, 40)])
+def test_mean_profiles_conduction_pin(istr3, nxm):
+    """CalcMeanProfiles.F90 on the conductive state: Tbar is the linear profile, every velocity
+    moment and epsilon vanish, and the thermal-dissipation Nusselt number Pe * int chiT dx is 1
+    (discrete identity of the one-sided wall gradients with the plate values)."""
+    from helpers import Case
+    c = Case(nxm, 16, 8, rayt=1e6, istr3=istr3)
+    s = o.initial_state(c.g, 1, eps=0.0)
+    m = o.mean_profiles(c.g, s)
+    assert set(m) == set(o.MEAN_PROFILE_NAMES)
+    xm = c.g.xm[:nxm]
+    assert np.allclose(m["Tbar"], 0.5 - xm / c.p.alx3, atol=1e-14)
+    for k in ("vybar", "vzbar", "vxT", "vyT", "vzT", "vxrms", "vyrms", "vzrms", "vxvy", "vxvz", "vyvz", "epsilon"):
+        assert np.abs(m[k]).max() == 0.0, k
+    dxk = c.g.xc[1:nxm + 1] - c.g.xc[:nxm]
+    assert abs(c.g.pect * np.sum(m["chiT"] * dxk) - 1.0) < 1e-12
