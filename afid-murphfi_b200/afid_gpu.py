@@ -87,7 +87,7 @@ class BatchStatT(C.Structure):
 
 class TuneInfoT(C.Structure):
     _fields_ = [("ncand", C.c_int), ("chosen", C.c_int), ("sample_columns", C.c_int),
-                ("threads", C.c_int * 4), ("rows", C.c_int * 4), ("regcap", C.c_int * 4), ("us", C.c_double * 4)]
+                ("threads", C.c_int * 5), ("rows", C.c_int * 5), ("regcap", C.c_int * 5), ("us", C.c_double * 5)]
 
     def as_dict(self) -> dict:
         """shapes: [threads per column, rows per thread, register cap, microseconds per sample]"""

@@ -246,10 +246,15 @@ __host__ __device__ inline size_t k1_smem(int ldx, int M, bool two_d) {
 // barrier, put the scaled RHS into the chunk layout (row r at (r%M)*LD + r/M) over the dead
 // neighbour columns.  Four warps run the partitioned CN solves, and every thread adds the
 // increments to the staged centre values and stores the intermediate fields.
-// CAP: at least 16 resident warps per SM (<= 128 registers a thread for blocks of up to 256
-// threads); without it the compiler may use more registers for fewer resident blocks.
-template <int M, int TPC, int RPT, typename TE, bool TWO_D, bool CAP>
-__global__ void __launch_bounds__(TPC, (CAP && TPC < 512) ? 512 / TPC : 1)
+// CAP: register cap for at least 16 (CAP = 1) or 32 (CAP = 2) resident warps per SM, i.e. <= 128
+// or <= 64 registers a thread; with CAP = 0 the compiler may use more registers for fewer
+// resident blocks.
+template <int CAP, int TPC>
+constexpr int k1_min_blocks() {
+  return CAP == 0 ? 1 : ((CAP == 1 ? 512 : 1024) / TPC > 1 ? (CAP == 1 ? 512 : 1024) / TPC : 1);
+}
+template <int M, int TPC, int RPT, typename TE, bool TWO_D, int CAP>
+__global__ void __launch_bounds__(TPC, k1_min_blocks<CAP, TPC>())
     k_explicit_implicit(Geom g0, Tables t, const StepCoef *__restrict__ sc_all, int ns,
                         const double *__restrict__ cn_tab, const double *__restrict__ vx,
                         const double *__restrict__ vy, const double *__restrict__ vz,
@@ -433,7 +438,7 @@ __global__ void __launch_bounds__(TPC, (CAP && TPC < 512) ? 512 / TPC : 1)
   }
 }
 
-template <int M, int TPC, int RPT, typename TE, bool TWO_D, bool CAP>
+template <int M, int TPC, int RPT, typename TE, bool TWO_D, int CAP>
 cudaError_t launch_k1_cfg(const LaunchCtx &L, const SubstepBuffers &b, int ns, int ncol) {
   const size_t smem = k1_smem(L.g.ldx, M, TWO_D);
   auto kern = k_explicit_implicit<M, TPC, RPT, TE, TWO_D, CAP>;
@@ -446,25 +451,25 @@ cudaError_t launch_k1_cfg(const LaunchCtx &L, const SubstepBuffers &b, int ns, i
 }
 
 // Thread shapes of K1 per M = {1, 2, 4, 8, 12, 16, 24, 32} (rows per lane of the CN solves):
-// {threads per column, rows per thread, register cap}, threads x rows >= 32 M.  The first is the
-// default.
+// {threads per column, rows per thread, register cap level}, threads x rows >= 32 M.  The first
+// is the default.
 struct K1Shape {
   int tpc, rpt, cap;
 };
-constexpr int kK1MaxShapes = 4;
+constexpr int kK1MaxShapes = 5;
 constexpr int k1_m_index(int M) {
   return M == 1 ? 0 : M == 2 ? 1 : M == 4 ? 2 : M == 8 ? 3 : M == 12 ? 4 : M == 16 ? 5 : M == 24 ? 6 : 7;
 }
-constexpr int kK1ShapeCount[8] = {1, 2, 2, 3, 4, 4, 3, 2};
+constexpr int kK1ShapeCount[8] = {1, 2, 3, 4, 5, 5, 3, 2};
 constexpr K1Shape kK1Shapes[8][kK1MaxShapes] = {
-    {{32, 1, 0}, {0, 0, 0}, {0, 0, 0}, {0, 0, 0}},        // M = 1   (nxm <= 32)
-    {{64, 1, 0}, {32, 2, 1}, {0, 0, 0}, {0, 0, 0}},       // M = 2   (<= 64)
-    {{128, 1, 0}, {64, 2, 1}, {0, 0, 0}, {0, 0, 0}},      // M = 4   (<= 128)
-    {{128, 2, 1}, {256, 1, 0}, {128, 2, 0}, {0, 0, 0}},   // M = 8   (<= 256)
-    {{128, 3, 1}, {256, 2, 1}, {384, 1, 0}, {128, 3, 0}}, // M = 12  (<= 384)
-    {{128, 4, 1}, {256, 2, 1}, {512, 1, 0}, {128, 4, 0}}, // M = 16  (<= 512)
-    {{256, 3, 1}, {384, 2, 0}, {256, 4, 1}, {0, 0, 0}},   // M = 24  (<= 768)
-    {{256, 4, 1}, {512, 2, 0}, {0, 0, 0}, {0, 0, 0}},     // M = 32  (<= 1024)
+    {{32, 1, 0}, {0, 0, 0}, {0, 0, 0}, {0, 0, 0}, {0, 0, 0}},          // M = 1   (nxm <= 32)
+    {{64, 1, 0}, {32, 2, 1}, {0, 0, 0}, {0, 0, 0}, {0, 0, 0}},         // M = 2   (<= 64)
+    {{128, 1, 0}, {64, 2, 1}, {128, 1, 2}, {0, 0, 0}, {0, 0, 0}},      // M = 4   (<= 128)
+    {{128, 2, 1}, {256, 1, 0}, {128, 2, 0}, {256, 1, 2}, {0, 0, 0}},   // M = 8   (<= 256)
+    {{128, 3, 1}, {256, 2, 1}, {384, 1, 0}, {128, 3, 0}, {384, 1, 2}}, // M = 12  (<= 384)
+    {{128, 4, 1}, {256, 2, 1}, {512, 1, 0}, {128, 4, 0}, {512, 1, 2}}, // M = 16  (<= 512)
+    {{256, 3, 1}, {384, 2, 0}, {256, 4, 1}, {0, 0, 0}, {0, 0, 0}},     // M = 24  (<= 768)
+    {{256, 4, 1}, {512, 2, 0}, {0, 0, 0}, {0, 0, 0}, {0, 0, 0}},       // M = 32  (<= 1024)
 };
 
 template <int M, int V, typename TE, bool TWO_D>
@@ -472,7 +477,7 @@ cudaError_t launch_k1_v(const LaunchCtx &L, const SubstepBuffers &b, int ns, int
   constexpr int mi = k1_m_index(M);
   if constexpr (V < kK1ShapeCount[mi]) {
     constexpr int TPC = kK1Shapes[mi][V].tpc, RPT = kK1Shapes[mi][V].rpt;
-    constexpr bool CAP = kK1Shapes[mi][V].cap != 0;
+    constexpr int CAP = kK1Shapes[mi][V].cap;
     static_assert(TPC * RPT >= 32 * M, "K1 shape must cover 32*M rows");
     return launch_k1_cfg<M, TPC, RPT, TE, TWO_D, CAP>(L, b, ns, ncol);
   } else {
@@ -487,6 +492,7 @@ cudaError_t launch_k1_M(const LaunchCtx &L, const SubstepBuffers &b, int ns, int
     case 1: return launch_k1_v<M, 1, TE, TWO_D>(L, b, ns, ncol);
     case 2: return launch_k1_v<M, 2, TE, TWO_D>(L, b, ns, ncol);
     case 3: return launch_k1_v<M, 3, TE, TWO_D>(L, b, ns, ncol);
+    case 4: return launch_k1_v<M, 4, TE, TWO_D>(L, b, ns, ncol);
   }
   return cudaErrorInvalidValue;
 }

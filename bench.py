@@ -41,6 +41,10 @@ WORKLOADS = {
     "rbc3d_small": dict(nxm=256, nym=128, nzm=128, rayt=1e9, prat=1.0, ylen=1.0, zlen=1.0, precision=0,
                         idtv=1, dt=1e-4, cflmax=1.2, dtmax=1e-2,
                         name="rbc3d_128x128x256_fp64_ra1e9"),
+    # 16.8 M cells (2.3 GB): state and spectrum larger than L2, small enough for multi-pass ncu
+    "rbc3d_medium": dict(nxm=256, nym=256, nzm=256, rayt=1e9, prat=1.0, ylen=1.0, zlen=1.0, precision=0,
+                         idtv=1, dt=1e-4, cflmax=1.2, dtmax=1e-2,
+                         name="rbc3d_256x256x256_fp64_ra1e9"),
     "rbc2d": dict(nxm=128, nym=256, nzm=1, rayt=1e8, prat=1.0, ylen=2.0, zlen=0.01, precision=0,
                   idtv=0, dt=5e-4, cflmax=1.2, dtmax=5e-4,
                   name="rbc2d_256x128_fp64_ra1e8"),
@@ -666,7 +670,7 @@ def run_reference(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=30)
+    ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="afid", choices=["afid", "reference"])
     ap.add_argument("--config", default="rbc3d", choices=sorted(WORKLOADS) + ["batched", "batched_fp64", "served"])
@@ -677,7 +681,7 @@ def main():
     ap.add_argument("--slots", type=int, default=32, help="served: 2-D slots per pool")
     ap.add_argument("--max-cells", type=int, default=0, help="served: cells-in-flight cap (0 = memory only)")
     ap.add_argument("--policy", default="fifo", choices=["fifo", "shortest"])
-    ap.add_argument("--cpu-steps", type=int, default=2)
+    ap.add_argument("--cpu-steps", type=int, default=10)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3:

@@ -140,14 +140,14 @@ int afid_gpu_mean_profiles(afid_ctx_t *ctx, double *out);
  * columns, with the RK3 histories redirected to scratch memory so the state is untouched, and
  * the fastest is kept.  It runs by itself before the first step; force = 1 repeats it.  The
  * shape changes the schedule only: results are bitwise the same for every shape. */
-#define AFID_TUNE_MAX 4
+#define AFID_TUNE_MAX 5
 typedef struct afid_tune_info {
   int ncand;                    /* shapes available (1 = nothing to choose)                  */
   int chosen;                   /* index of the shape in use                                 */
   int sample_columns;           /* x-columns per timed sample launch                         */
   int threads[AFID_TUNE_MAX];   /* threads per column block                                  */
   int rows[AFID_TUNE_MAX];      /* rows per thread                                           */
-  int regcap[AFID_TUNE_MAX];    /* 1: registers capped for >= 16 resident warps per SM        */
+  int regcap[AFID_TUNE_MAX];    /* registers capped for >= 16 (1) or >= 32 (2) warps per SM  */
   double us[AFID_TUNE_MAX];     /* mean time per sample launch in microseconds (-1: not run) */
 } afid_tune_info_t;
 int afid_gpu_autotune(afid_ctx_t *ctx, int force, afid_tune_info_t *info);
