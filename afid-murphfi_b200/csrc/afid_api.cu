@@ -353,6 +353,7 @@ int ctx_create(const afid_grid_t *grid, const afid_params_t *prm, const BatchSpe
   const int nx = g.nx;
   std::vector<double> h;
   auto put = [&](const double *src, int n, int len) -> size_t {
+    while (h.size() % 8) h.push_back(0.0);  // 64-byte aligned tables (vector loads)
     size_t off = h.size();
     for (int k = 0; k < len; ++k) h.push_back((src && k < n) ? src[k] : 0.0);
     return off;

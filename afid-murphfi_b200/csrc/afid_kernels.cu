@@ -448,40 +448,102 @@ __global__ void __launch_bounds__(256)
 
 // K7: RemoveDivergence (pressure.F90:245-266) out of place (intermediate velocities -> state)
 // and CorrectPressure (pressure.F90:276-300) in place.  Thread per (k, j, i).
+__device__ __forceinline__ double2 make_v2(double a, double b) { return make_double2(a, b); }
+__device__ __forceinline__ float2 make_v2(float a, float b) { return make_float2(a, b); }
+
+template <typename TS>
+struct Vec2;
+template <>
+struct Vec2<double> {
+  using type = double2;
+};
+template <>
+struct Vec2<float> {
+  using type = float2;
+};
+
+// K7: RemoveDivergence (pressure.F90:240-267) + CorrectPressure (pressure.F90:270-301).  Each
+// thread updates the two x-neighbours k0 = 2*tx and k0+1 with 16-byte (8-byte for FP32 phi)
+// vector loads and stores; the x-neighbours of the pair come from the adjacent threads.
 template <typename TS>
 __global__ void __launch_bounds__(256)
     k_correct(Geom g0, Tables t, const StepCoef *__restrict__ sc_all, int ns,
               const double *__restrict__ vxh, const double *__restrict__ vyh,
               const double *__restrict__ vzh, double *__restrict__ vx, double *__restrict__ vy,
               double *__restrict__ vz, double *__restrict__ pr, const TS *__restrict__ phi) {
-  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  using V = typename Vec2<TS>::type;
+  const int k0 = 2 * (blockIdx.x * blockDim.x + threadIdx.x);
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
   const int i = blockIdx.z;
   Geom g = g0;
-  if (k >= g.nxm || j >= g.nym || !inst_active(g, i)) return;
+  // threads past the end of the row still take part in the neighbour exchange below
+  const bool row_ok = (j < g.nym) && inst_active(g, i);
+  if (!row_ok) return;  // whole warps share j (blockDim.x is a multiple of 32)
   bind_instance(g, i);
+  const int nxm = g.nxm;
+  const bool in0 = k0 < nxm, in1 = k0 + 1 < nxm;
   const StepCoef sc = sc_all[sc_slot(g, i, ns)];
   const int jm = wrap_dec(j, g.nym), jp = wrap_inc(j, g.nym);
   const int im = zdec(g, i), ip = zinc(g, i);
-  const int km = (k == 0) ? 0 : k - 1;
-  const int kp = (k == g.nxm - 1) ? k : k + 1;
   const size_t c = col_off(g, j, i);
-  const double ph = (double)phi[c + k];
-  const double phkm = (double)phi[c + km], phkp = (double)phi[c + kp];
-  const double phjm = (double)phi[col_off(g, jm, i) + k], phjp = (double)phi[col_off(g, jp, i) + k];
-  const double phim = (double)phi[col_off(g, j, im) + k], phip = (double)phi[col_off(g, j, ip) + k];
+  // pairs (k0, k0+1): k0 even and every column starts on a multiple of 8 elements
+  V ph2 = make_v2(TS(0), TS(0)), pjm2 = ph2, pjp2 = ph2, pim2 = ph2, pip2 = ph2;
+  double2 uxh = make_double2(0.0, 0.0), uyh = uxh, uzh = uxh, upr = uxh;
+  if (in0) {
+    ph2 = *reinterpret_cast<const V *>(phi + c + k0);
+    pjm2 = *reinterpret_cast<const V *>(phi + col_off(g, jm, i) + k0);
+    pjp2 = *reinterpret_cast<const V *>(phi + col_off(g, jp, i) + k0);
+    pim2 = *reinterpret_cast<const V *>(phi + col_off(g, j, im) + k0);
+    pip2 = *reinterpret_cast<const V *>(phi + col_off(g, j, ip) + k0);
+    uxh = __ldg(reinterpret_cast<const double2 *>(vxh + c + k0));
+    uyh = __ldg(reinterpret_cast<const double2 *>(vyh + c + k0));
+    uzh = __ldg(reinterpret_cast<const double2 *>(vzh + c + k0));
+    upr = *reinterpret_cast<const double2 *>(pr + c + k0);
+  }
+  // x-neighbours: phi(k0-1) is the left thread's second value, phi(k0+2) the right thread's
+  // first; the lanes at the ends of a warp load theirs
+  const int lane = threadIdx.x & 31;
+  double left = __shfl_up_sync(0xffffffffu, (double)ph2.y, 1);
+  double right = __shfl_down_sync(0xffffffffu, (double)ph2.x, 1);
+  if (!in0) return;
+  if (lane == 0) left = (k0 > 0) ? (double)phi[c + k0 - 1] : 0.0;
+  if (lane == 31 || k0 + 2 >= nxm) right = (k0 + 2 < nxm) ? (double)phi[c + k0 + 2] : 0.0;
+  const double ph0 = (double)ph2.x, ph1 = (double)ph2.y;
+  const double phkm0 = (k0 == 0) ? ph0 : left;           // kmv(1) = 1
+  const double phkp1 = (k0 + 1 == nxm - 1) ? ph1 : right;  // kpv(nxm) = nxm
   const double aldt = sc.al * sc.dt;
   const double udy = aldt * g.dy, udz = aldt * g.dz;
-  const double usukm = aldt * __ldg(t.udx3c + k);
-  vx[c + k] = __ldg(vxh + c + k) - (ph - phkm) * usukm;
-  vy[c + k] = __ldg(vyh + c + k) - (ph - phjm) * udy;
-  vz[c + k] = __ldg(vzh + c + k) - (ph - phim) * udz;
-  if (k == g.nxm - 1) vx[c + k + 1] = __ldg(vxh + c + k + 1);
   const double be = sc.al * sc.beta;
-  const double amm = __ldg(t.amphk + k), acc = __ldg(t.acphk + k), app = __ldg(t.apphk + k);
-  pr[c + k] = pr[c + k] + ph -
-              be * ((phip - 2.0 * ph + phim) * g.dzq + (phjp - 2.0 * ph + phjm) * g.dyq +
-                    (phkp * app + ph * acc + phkm * amm));
+  const double2 ud = __ldg(reinterpret_cast<const double2 *>(t.udx3c + k0));
+  const double2 am = __ldg(reinterpret_cast<const double2 *>(t.amphk + k0));
+  const double2 ac = __ldg(reinterpret_cast<const double2 *>(t.acphk + k0));
+  const double2 ap = __ldg(reinterpret_cast<const double2 *>(t.apphk + k0));
+  double2 ox, oy, oz, op;
+  // cell k0
+  ox.x = uxh.x - (ph0 - phkm0) * (aldt * ud.x);
+  oy.x = uyh.x - (ph0 - (double)pjm2.x) * udy;
+  oz.x = uzh.x - (ph0 - (double)pim2.x) * udz;
+  op.x = upr.x + ph0 -
+         be * (((double)pip2.x - 2.0 * ph0 + (double)pim2.x) * g.dzq +
+               ((double)pjp2.x - 2.0 * ph0 + (double)pjm2.x) * g.dyq + ((in1 ? ph1 : ph0) * ap.x + ph0 * ac.x + phkm0 * am.x));
+  if (in1) {
+    ox.y = uxh.y - (ph1 - ph0) * (aldt * ud.y);
+    oy.y = uyh.y - (ph1 - (double)pjm2.y) * udy;
+    oz.y = uzh.y - (ph1 - (double)pim2.y) * udz;
+    op.y = upr.y + ph1 -
+           be * (((double)pip2.y - 2.0 * ph1 + (double)pim2.y) * g.dzq +
+                 ((double)pjp2.y - 2.0 * ph1 + (double)pjm2.y) * g.dyq + (phkp1 * ap.y + ph1 * ac.y + ph0 * am.y));
+    *reinterpret_cast<double2 *>(vx + c + k0) = ox;
+    *reinterpret_cast<double2 *>(vy + c + k0) = oy;
+    *reinterpret_cast<double2 *>(vz + c + k0) = oz;
+    *reinterpret_cast<double2 *>(pr + c + k0) = op;
+  } else {
+    vx[c + k0] = ox.x;
+    vy[c + k0] = oy.x;
+    vz[c + k0] = oz.x;
+    pr[c + k0] = op.x;
+  }
+  if (k0 + 1 >= nxm - 1) vx[c + nxm] = __ldg(vxh + c + nxm);  // the upper wall value is copied
 }
 
 // ------------------------------------------------------------------------------------------
@@ -964,11 +1026,12 @@ static cudaError_t launch_stage_T(const LaunchCtx &L, const SubstepBuffers &b, i
       }
       return cudaGetLastError();
     }
-    case Stage::Correct: {  // K7 projection + pressure update
-      const int bx = (g.nxm >= 256) ? 256 : ((g.nxm + 31) / 32) * 32;
+    case Stage::Correct: {  // K7 projection + pressure update, two x points a thread
+      const int pairs = (g.nxm + 1) / 2;
+      const int bx = (pairs >= 128) ? 128 : ((pairs + 31) / 32) * 32;
       const int by = 256 / bx;
       dim3 block(bx, by);
-      dim3 grid((g.nxm + bx - 1) / bx, (g.nym + by - 1) / by, g.nzm);
+      dim3 grid((pairs + bx - 1) / bx, (g.nym + by - 1) / by, g.nzm);
       k_correct<TS><<<grid, block, 0, L.stream>>>(g, L.t, b.sc, ns, b.vx_o, b.vy_o, b.vz_o, b.vx, b.vy,
                                                   b.vz, b.pr, (const TS *)b.phi);
       return cudaGetLastError();
