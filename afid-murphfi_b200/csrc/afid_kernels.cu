@@ -685,20 +685,33 @@ __global__ void __launch_bounds__(256)
   const int ip = zinc(g, i);
   const StepCoef sc = sc_all[sc_slot(g, i, ns)];
   const double usdtal = 1.0 / (sc.dt * sc.al);
-  const int tx = threadIdx.x & 15, k = k0 + tx;
-  const double ux = (k < g.nxm) ? __ldg(t.udx3m + k) : 0.0;
+  // thread pair q holds the x points (kk, kk+1) = (k0 + 2q, k0 + 2q + 1), loaded with 16-byte
+  // vector loads, and stores them as the packed complex column q
+  const int q = threadIdx.x & 7, kk = k0 + 2 * q;
+  const int nxm = g.nxm;
+  const double2 ux = (kk < nxm) ? __ldg(reinterpret_cast<const double2 *>(t.udx3m + kk)) : make_double2(0.0, 0.0);
+  (void)Tr;
 #pragma unroll 4
-  for (int j = threadIdx.x >> 4; j < N; j += 16) {
-    double dv = 0.0;
-    if (k < g.nxm) {
+  for (int j = threadIdx.x >> 3; j < N; j += 32) {
+    double dv0 = 0.0, dv1 = 0.0;
+    if (kk < nxm) {
       const int jp = wrap_inc(j, N);
       const size_t c = col_off(g, j, i), cjp = col_off(g, jp, i), cip = col_off(g, j, ip);
-      const double dqcap = (__ldg(vz + cip + k) - __ldg(vz + c + k)) * g.dz +
-                           (__ldg(vy + cjp + k) - __ldg(vy + c + k)) * g.dy +
-                           (__ldg(vx + c + k + 1) - __ldg(vx + c + k)) * ux;
-      dv = dqcap * usdtal;
+      const double2 zi = __ldg(reinterpret_cast<const double2 *>(vz + cip + kk));
+      const double2 zc = __ldg(reinterpret_cast<const double2 *>(vz + c + kk));
+      const double2 yj = __ldg(reinterpret_cast<const double2 *>(vy + cjp + kk));
+      const double2 yc = __ldg(reinterpret_cast<const double2 *>(vy + c + kk));
+      const double2 xc = __ldg(reinterpret_cast<const double2 *>(vx + c + kk));
+      dv0 = ((zi.x - zc.x) * g.dz + (yj.x - yc.x) * g.dy + (xc.y - xc.x) * ux.x) * usdtal;
+      if (kk + 1 < nxm) {
+        const double x2 = __ldg(vx + c + kk + 2);
+        dv1 = ((zi.y - zc.y) * g.dz + (yj.y - yc.y) * g.dy + (x2 - xc.y) * ux.y) * usdtal;
+      }
     }
-    Tr[2 * tsw(j, tx >> 1) + (tx & 1)] = (TS)dv;
+    C z;
+    z.x = (TS)dv0;
+    z.y = (TS)dv1;
+    T[tsw(j, q)] = z;
   }
   __syncthreads();
   const int lane = threadIdx.x & 31, p = threadIdx.x >> 5;
@@ -821,12 +834,22 @@ __global__ void __launch_bounds__(256)
 #pragma unroll
   for (int k1 = 0; k1 < N1; ++k1) T[tsw(k1 + N1 * rl, p)] = x[k1];
   __syncthreads();
+  // the packed pair (re, im) of column p is phi at (k0 + 2p, k0 + 2p + 1): one vector store
+  using V = typename Vec2<TS>::type;
 #pragma unroll 4
-  for (int e = threadIdx.x; e < N * 16; e += blockDim.x) {
-    const int ex = e & 15, j = e >> 4;
-    const int k = k0 + ex;
-    if (k < g.nxm) phi[col_off(g, j, i) + k] = Tr[2 * tsw(j, ex >> 1) + (ex & 1)];
+  for (int e = threadIdx.x; e < N * 8; e += blockDim.x) {
+    const int q = e & 7, j = e >> 3;
+    const int k = k0 + 2 * q;
+    if (k < g.nxm) {
+      const C v = T[tsw(j, q)];
+      TS *dst = phi + col_off(g, j, i) + k;
+      if (k + 1 < g.nxm)
+        *reinterpret_cast<V *>(dst) = make_v2(v.x, v.y);
+      else
+        dst[0] = v.x;
+    }
   }
+  (void)Tr;
 }
 
 // ==========================================================================================
