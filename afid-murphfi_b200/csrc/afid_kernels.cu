@@ -259,10 +259,11 @@ __global__ void __launch_bounds__(256)
 }
 
 // ------------------------------------------------------------------------------------------
-// K4: per (ky, kz) mode, the normalised complex tridiagonal of pressure.F90:209-232:
-// a_k = amphk(k)/(acphk(k)-ak2(j)-ak1(i)), c_k = apphk(k)/(...), diagonal 1+1e-15, RHS scaled
-// by the same factor.  One warp per mode; rows are split into 32 chunks of M (partition +
-// PCR as in the CN solve, with factors computed per mode).  The (0,0) mode is singular up to
+// K4: per (ky, kz) mode, the complex tridiagonal of pressure.F90:209-232.  The reference scales
+// row k by 1/(acphk(k)-ak2(j)-ak1(i)) and puts 1+1e-15 on the diagonal; the same system is
+// solved here unscaled (amphk, (acphk-ak2-ak1)(1+1e-15), apphk), which saves a reciprocal per
+// row.  One warp per mode; rows are split into 32 chunks of M (partition + PCR as in the CN
+// solve, with factors computed per mode).  The (0,0) mode is singular up to
 // the 1e-15 shift (the reference lets LAPACK return an arbitrary constant); here its last
 // equation is replaced by phi = 0, which fixes that constant without changing gradients.
 // A zero pivot sets AFID_E_SINGULAR (the reference aborts, pressure.F90:225-229).
@@ -281,8 +282,11 @@ __global__ void __launch_bounds__(WPB * 32)
   // the singular (0,0) mode; in batch mode every instance's ky = 0 mode (nzm = 1 each)
   const bool pin = (ky == 0 && (kz == 0 || g.batch));
   constexpr int LD = chunk_ld(M);
-  double *sa = smem_k4 + warp * (4 * LD * M);
-  double *sc_ = sa + LD * M, *sdr = sa + 2 * LD * M, *sdi = sa + 3 * LD * M;
+  // M <= 8: the diagonal is kept in shared memory too (a fifth array costs no resident block)
+  constexpr bool kStoreB = (M <= 8);
+  constexpr int NA = kStoreB ? 5 : 4;
+  double *sa = smem_k4 + warp * (NA * LD * M);
+  double *sc_ = sa + LD * M, *sdr = sa + 2 * LD * M, *sdi = sa + 3 * LD * M, *sb = sa + 4 * LD * M;
   C *colp = spec + (size_t)sys * g.ldxc;
   const int n = g.nxm;
   const double akj = __ldg(t.ak2 + (g.batch ? (size_t)kz * g.nym : 0) + ky);
@@ -291,31 +295,39 @@ __global__ void __launch_bounds__(WPB * 32)
   for (int tt = 0; tt < M; ++tt) {
     const int r = lane + 32 * tt;
     const int s = (r % M) * LD + r / M;
-    double a = 0.0, c = 0.0, dr = 0.0, di = 0.0;
+    // the rows unnormalised: the reference's row scaling 1/(acphk - ak2 - ak1) with unit-plus-
+    // 1e-15 diagonal is the same system as diagonal (acphk - ak2 - ak1)(1 + 1e-15)
+    double a = 0.0, c = 0.0, dr = 0.0, di = 0.0, b = 1.0;
     if (r < n) {
-      const double f = 1.0 / (__ldg(t.acphk + r) - akj - aki);
-      a = (r > 0) ? __ldg(t.amphk + r) * f : 0.0;
-      c = (r < n - 1) ? __ldg(t.apphk + r) * f : 0.0;
+      a = (r > 0) ? __ldg(t.amphk + r) : 0.0;
+      c = (r < n - 1) ? __ldg(t.apphk + r) : 0.0;
+      if (kStoreB) b = (__ldg(t.acphk + r) - akj - aki) * (1.0 + 1.0e-15);
       const C v = colp[r];
-      dr = (double)v.x * f;
-      di = (double)v.y * f;
-      if (pin && r == n - 1) { a = 0.0; dr = 0.0; di = 0.0; }
+      dr = (double)v.x;
+      di = (double)v.y;
+      if (pin && r == n - 1) { a = 0.0; dr = 0.0; di = 0.0; b = 1.0; }
     }
     sa[s] = a;
     sc_[s] = c;
     sdr[s] = dr;
     sdi[s] = di;
+    if (kStoreB) sb[s] = b;
   }
   __syncwarp();
   const int s0 = lane * M;
-  auto diag = [&](int r) -> double { return (r < n && !(pin && r == n - 1)) ? 1.0 + 1.0e-15 : 1.0; };
+  // diagonal of row s0 + q (identity for padding rows and the pinned row)
+  auto diag = [&](int q) -> double {
+    if constexpr (kStoreB) return sb[q * LD + lane];
+    const int r = s0 + q;
+    return (r < n && !(pin && r == n - 1)) ? (__ldg(t.acphk + r) - akj - aki) * (1.0 + 1.0e-15) : 1.0;
+  };
   double cp[M], yr[M], yi[M], v[M], w[M];
   bool bad = false;
   cp[0] = 0.0; yr[0] = 0.0; yi[0] = 0.0; v[0] = 0.0; w[0] = 0.0;
 #pragma unroll
   for (int q = 1; q < M; ++q) {
     const double a = sa[q * LD + lane], c = sc_[q * LD + lane];
-    const double den = (q > 1) ? diag(s0 + q) - a * cp[q - 1] : diag(s0 + q);
+    const double den = (q > 1) ? diag(q) - a * cp[q - 1] : diag(q);
     bad |= (den == 0.0);
     const double inv = 1.0 / den;
     cp[q] = c * inv;
@@ -342,7 +354,7 @@ __global__ void __launch_bounds__(WPB * 32)
   double A, B, Cc, Dr, Di;
   if constexpr (M == 1) {
     A = as_;
-    B = diag(s0);
+    B = diag(0);
     Cc = cs_;
     Dr = sdr[lane];
     Di = sdi[lane];
@@ -353,7 +365,7 @@ __global__ void __launch_bounds__(WPB * 32)
     double yl_i = __shfl_up_sync(0xffffffffu, yi[M - 1], 1);
     if (lane == 0) { vl = 0.0; wl = 0.0; yl_r = 0.0; yl_i = 0.0; }
     A = as_ * vl;
-    B = diag(s0) + as_ * wl + cs_ * v[1];
+    B = diag(0) + as_ * wl + cs_ * v[1];
     Cc = (lane == 31) ? 0.0 : cs_ * w[1];
     Dr = sdr[lane] - as_ * yl_r - cs_ * yr[1];
     Di = sdi[lane] - as_ * yl_i - cs_ * yi[1];
@@ -908,7 +920,7 @@ template <int M, typename TS>
 static cudaError_t launch_k4_M(const LaunchCtx &L, void *spec, int *err) {
   constexpr int W = (M >= 16) ? 2 : 4;
   const int nsys = L.g.nyh * L.g.nzm;
-  const size_t smem = (size_t)W * 4 * chunk_ld(M) * M * sizeof(double);
+  const size_t smem = (size_t)W * (M <= 8 ? 5 : 4) * chunk_ld(M) * M * sizeof(double);
   auto kern = k_tridiag_pressure<M, W, TS>;
   cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   kern<<<(nsys + W - 1) / W, W * 32, smem, L.stream>>>(L.g, L.t, (typename Cplx<TS>::type *)spec, err);
