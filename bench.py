@@ -153,11 +153,13 @@ def dist_setup():
 
 
 def reduce_max(x: float, world: int) -> float:
+    """Max over the ranks (timing is the slowest replica's); NCCL on GPUs, gloo on CPU."""
     if world == 1:
         return x
     import torch
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 
