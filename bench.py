@@ -679,10 +679,10 @@ def main():
     ap.add_argument("--no-nu-check", action="store_true")
     ap.add_argument("--k1-shape", type=int, default=-1, help="fixed K1 thread shape instead of autotuning")
     ap.add_argument("--jobs", type=int, default=100, help="served: number of jobs")
-    ap.add_argument("--chunk", type=int, default=50, help="served: steps per pump")
+    ap.add_argument("--chunk", type=int, default=25, help="served: steps per pump")
     ap.add_argument("--slots", type=int, default=32, help="served: 2-D slots per pool")
-    ap.add_argument("--max-cells", type=int, default=0, help="served: cells-in-flight cap (0 = memory only)")
-    ap.add_argument("--policy", default="fifo", choices=["fifo", "shortest"])
+    ap.add_argument("--max-cells", type=int, default=16_000_000, help="served: cells-in-flight cap (0 = memory only)")
+    ap.add_argument("--policy", default="shortest", choices=["fifo", "shortest"])
     ap.add_argument("--cpu-steps", type=int, default=10)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
