@@ -143,6 +143,7 @@ EXPORTS = [
     "afid_serve_create", "afid_serve_destroy", "afid_serve_submit", "afid_serve_pump", "afid_serve_poll",
     "afid_serve_status", "afid_serve_now", "afid_gpu_autotune", "afid_batch_autotune",
     "afid_gpu_set_k1_shape", "afid_gpu_mean_profiles", "afid_batch_mean_profiles",
+    "afid_gpu_spectra_reset", "afid_gpu_spectra_update", "afid_gpu_spectra_read", "afid_gpu_slice",
 ]
 
 
@@ -203,6 +204,10 @@ def load_library(path: str = _LIB_PATH) -> C.CDLL:
         "afid_gpu_autotune": (i, [vp, i, C.POINTER(TuneInfoT)]),
         "afid_gpu_set_k1_shape": (i, [vp, i]),
         "afid_gpu_mean_profiles": (i, [vp, _dp]),
+        "afid_gpu_spectra_reset": (i, [vp]),
+        "afid_gpu_spectra_update": (i, [vp, d]),
+        "afid_gpu_spectra_read": (i, [vp, i, _dp, _dp]),
+        "afid_gpu_slice": (i, [vp, i, i, i, _dp]),
         "afid_batch_mean_profiles": (i, [vp, i, _dp]),
         "afid_batch_autotune": (i, [vp, i, C.POINTER(TuneInfoT)]),
         "afid_batch_step": (i, [vp, i]),
@@ -379,6 +384,29 @@ class Solver:
         out = np.zeros((len(PROFILE_NAMES), self.nxm))
         _check(lib().afid_gpu_mean_profiles(self._h, _ptr(out)), "afid_gpu_mean_profiles")
         return dict(zip(PROFILE_NAMES, out))
+
+    def spectra_reset(self) -> None:
+        _check(lib().afid_gpu_spectra_reset(self._h), "afid_gpu_spectra_reset")
+
+    def spectra_update(self, dt: float) -> None:
+        _check(lib().afid_gpu_spectra_update(self._h, dt), "afid_gpu_spectra_update")
+
+    def spectra(self) -> dict:
+        """Time-averaged spectra {vx, vy, vz, temp}: arrays (nzm, nym//2+1, nxm) (Fortran
+        (nxm, nyh, nzm)), and the averaging interval under 'tav'."""
+        out, tav = {}, C.c_double()
+        for w, name in enumerate(("vx", "vy", "vz", "temp")):
+            a = np.zeros((self.nzm, self.nym // 2 + 1, self.nxm))
+            _check(lib().afid_gpu_spectra_read(self._h, w, _ptr(a), C.byref(tav)), "afid_gpu_spectra_read")
+            out[name] = a
+        out["tav"] = tav.value
+        return out
+
+    def slice(self, which: int, axis: int, index: int) -> np.ndarray:
+        shape = {0: (self.nzm, self.nym), 1: (self.nzm, self.nx), 2: (self.nym, self.nx)}[axis]
+        a = np.zeros(shape)
+        _check(lib().afid_gpu_slice(self._h, which, axis, index, _ptr(a)), "afid_gpu_slice")
+        return a
 
     def set_k1_shape(self, index: int) -> None:
         _check(lib().afid_gpu_set_k1_shape(self._h, index), "afid_gpu_set_k1_shape")

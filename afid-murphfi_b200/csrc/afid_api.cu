@@ -635,6 +635,7 @@ int afid_gpu_destroy(afid_ctx_t *ctx) {
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   for (void *p : ctx->allocs) cudaFree(p);
   if (ctx->stats_buf) cudaFree(ctx->stats_buf);
+  if (ctx->spec_acc) cudaFree(ctx->spec_acc);
   for (cudaEvent_t e : ctx->ev_pool) cudaEventDestroy(e);
   if (ctx->host_scratch) cudaFreeHost(ctx->host_scratch);
   if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);

@@ -34,6 +34,8 @@ struct SubstepBuffers {
   void *spec;                   // complex spectrum (double2 or float2)
   void *phi;                    // pressure correction (double or float)
   int *err;
+  // K2 input: nullptr = the divergence of (vx_o, vy_o, vz_o); else this field (spectra)
+  const double *fft_field = nullptr;
 };
 
 struct CnInputs {
@@ -111,6 +113,9 @@ struct afid_ctx {
   // scratch of the profile reductions (afid_stats.cu), allocated on first use
   double *stats_buf = nullptr;
   size_t stats_elems = 0;
+  // spectra accumulators (vx, vy, vz, temp; nxm x nyh x nzm each) and the averaged interval
+  double *spec_acc = nullptr;
+  double spec_tav = 0.0;
   // K1 thread-shape autotuner
   bool tuned = false;
   afid_tune_info_t tune{};

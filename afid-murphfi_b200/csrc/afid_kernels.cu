@@ -174,7 +174,7 @@ __global__ void __launch_bounds__(256)
     k_div_fft_y(Geom g0, Tables t, const StepCoef *__restrict__ sc_all, int ns,
                 const double *__restrict__ vx, const double *__restrict__ vy,
                 const double *__restrict__ vz, typename Cplx<TS>::type *__restrict__ spec,
-                FftPlan pl, const typename Cplx<TS>::type *__restrict__ tw) {
+                FftPlan pl, const typename Cplx<TS>::type *__restrict__ tw, const double *__restrict__ field) {
   using C = typename Cplx<TS>::type;
   extern __shared__ __align__(16) unsigned char smem_raw_k2[];
   C *b0 = reinterpret_cast<C *>(smem_raw_k2);
@@ -192,7 +192,9 @@ __global__ void __launch_bounds__(256)
 #pragma unroll 4
   for (int j = threadIdx.x / TX; j < N; j += blockDim.x / TX) {
     double dv = 0.0;
-    if (k < g.nxm) {
+    if (k < g.nxm && field) {
+      dv = __ldg(field + col_off(g, j, i) + k);
+    } else if (k < g.nxm) {
       const int jp = wrap_inc(j, N);
       const size_t c = col_off(g, j, i), cjp = col_off(g, jp, i), cip = col_off(g, j, ip);
       const double dqcap = (__ldg(vz + cip + k) - __ldg(vz + c + k)) * g.dz +
@@ -684,7 +686,7 @@ __global__ void __launch_bounds__(256)
     k_div_fft_y_w(Geom g0, Tables t, const StepCoef *__restrict__ sc_all, int ns,
                   const double *__restrict__ vx, const double *__restrict__ vy,
                   const double *__restrict__ vz, typename Cplx<TS>::type *__restrict__ spec,
-                  const typename Cplx<TS>::type *__restrict__ tw) {
+                  const typename Cplx<TS>::type *__restrict__ tw, const double *__restrict__ field) {
   using C = typename Cplx<TS>::type;
   constexpr int N = 32 * N1;
   extern __shared__ __align__(16) unsigned char smem_k2w[];
@@ -706,7 +708,11 @@ __global__ void __launch_bounds__(256)
 #pragma unroll 4
   for (int j = threadIdx.x >> 3; j < N; j += 32) {
     double dv0 = 0.0, dv1 = 0.0;
-    if (kk < nxm) {
+    if (kk < nxm && field) {  // spectra: the field itself
+      const double2 f = __ldg(reinterpret_cast<const double2 *>(field + col_off(g, j, i) + kk));
+      dv0 = f.x;
+      dv1 = (kk + 1 < nxm) ? f.y : 0.0;
+    } else if (kk < nxm) {
       const int jp = wrap_inc(j, N);
       const size_t c = col_off(g, j, i), cjp = col_off(g, jp, i), cip = col_off(g, j, ip);
       const double2 zi = __ldg(reinterpret_cast<const double2 *>(vz + cip + kk));
@@ -956,7 +962,8 @@ static cudaError_t launch_w_n1(const LaunchCtx &L, const SubstepBuffers &b, int 
     if (st == Stage::DivFftY) {
       auto kern = k_div_fft_y_w<N1, TS>;
       cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-      kern<<<grid, 256, sm, L.stream>>>(g, L.t, b.sc, ns, b.vx_o, b.vy_o, b.vz_o, spec, (const C *)L.twy);
+      kern<<<grid, 256, sm, L.stream>>>(g, L.t, b.sc, ns, b.vx_o, b.vy_o, b.vz_o, spec, (const C *)L.twy,
+                                        b.fft_field);
     } else {
       auto kern = k_ifft_y_w<N1, TS>;
       cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
@@ -1012,15 +1019,15 @@ static cudaError_t launch_stage_T(const LaunchCtx &L, const SubstepBuffers &b, i
       if (TX == 8) {
         cudaFuncSetAttribute(k_div_fft_y<8, TS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         k_div_fft_y<8, TS><<<grid, 256, smem, L.stream>>>(g, L.t, b.sc, ns, b.vx_o, b.vy_o, b.vz_o, spec,
-                                                          L.plan_y, twy);
+                                                          L.plan_y, twy, b.fft_field);
       } else if (TX == 4) {
         cudaFuncSetAttribute(k_div_fft_y<4, TS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         k_div_fft_y<4, TS><<<grid, 256, smem, L.stream>>>(g, L.t, b.sc, ns, b.vx_o, b.vy_o, b.vz_o, spec,
-                                                          L.plan_y, twy);
+                                                          L.plan_y, twy, b.fft_field);
       } else {
         cudaFuncSetAttribute(k_div_fft_y<2, TS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         k_div_fft_y<2, TS><<<grid, 256, smem, L.stream>>>(g, L.t, b.sc, ns, b.vx_o, b.vy_o, b.vz_o, spec,
-                                                          L.plan_y, twy);
+                                                          L.plan_y, twy, b.fft_field);
       }
       return cudaGetLastError();
     }

@@ -1,4 +1,5 @@
-// afid_stats.cu — wall-normal profiles of CalcMeanProfiles.F90 on the device.
+// afid_stats.cu — on-device statistics and outputs: the wall-normal profiles of
+// CalcMeanProfiles.F90, the spectra of spectra.F90 and the movie planes of MakeMovie*Cut.F90.
 //
 // The fifteen y-z averages written to means.h5 (Tbar, vybar, vzbar, vxT, vyT, vzT, Trms, vxrms,
 // vyrms, vzrms, vxvy, vxvz, vyvz, chiT, epsilon) are reduced in two passes: every block walks a
@@ -174,4 +175,143 @@ extern "C" int afid_gpu_mean_profiles(afid_ctx_t *ctx, double *out) {
   cudaSetDevice(ctx->dev);
   const Geom &g = ctx->L.g;
   return ctx_mean_profiles(ctx, 0, g.nym * g.nzm, (double)g.nym * (double)g.nzm, g.ren, g.pect, out);
+}
+
+// ------------------------------------------------------------------------------------------
+// Spectra (spectra.F90): the y r2c + z c2c Fourier coefficients of vx, vy, vz and temp at
+// k = 1..nxm, normalised by 1/(nym*nzm) (CalcFourierCoef, :70-96), accumulated as dt*|F|^2
+// (AddRealSpectrum, :101-114) and divided by the averaging interval when read (WriteSpectra).
+// The transforms are the Poisson solver's forward kernels with the field as their input.
+// ------------------------------------------------------------------------------------------
+namespace afid {
+
+template <typename C>
+__global__ void k_spec_acc(const C *__restrict__ spec, int nxm, int nyh, int nzm, int ldxc, double dt,
+                           double *__restrict__ acc) {
+  const size_t n = (size_t)nxm * nyh * nzm;
+  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
+    const int k = (int)(e % nxm);
+    const size_t m = e / nxm;  // ky + nyh*kz
+    const C v = spec[m * ldxc + k];
+    const double re = (double)v.x, im = (double)v.y;
+    acc[e] += dt * (re * re + im * im);
+  }
+}
+
+}  // namespace afid
+
+extern "C" {
+
+int afid_gpu_spectra_reset(afid_ctx_t *ctx) {
+  if (!ctx || ctx->L.g.batch) return AFID_E_INVALID;
+  cudaSetDevice(ctx->dev);
+  const Geom &g = ctx->L.g;
+  const size_t n = (size_t)4 * g.nxm * g.nyh * g.nzm;
+  if (!ctx->spec_acc) {
+    if (cudaMalloc(&ctx->spec_acc, n * sizeof(double)) != cudaSuccess) {
+      ctx->spec_acc = nullptr;
+      return AFID_E_ALLOC;
+    }
+  }
+  ctx->spec_tav = 0.0;
+  cudaError_t e = cudaMemsetAsync(ctx->spec_acc, 0, n * sizeof(double), ctx->stream);
+  return e == cudaSuccess ? AFID_OK : ctx_fail(ctx, e);
+}
+
+int afid_gpu_spectra_update(afid_ctx_t *ctx, double dt) {
+  if (!ctx || ctx->L.g.batch || !(dt > 0.0)) return AFID_E_INVALID;
+  if (!ctx->spec_acc) {
+    const int s = afid_gpu_spectra_reset(ctx);
+    if (s != AFID_OK) return s;
+  }
+  cudaSetDevice(ctx->dev);
+  const Geom &g = ctx->L.g;
+  const size_t n = (size_t)g.nxm * g.nyh * g.nzm;
+  SubstepBuffers b = ctx_buffers(ctx);
+  const double *fields[4] = {ctx->vx, ctx->vy, ctx->vz, ctx->temp};
+  for (int f = 0; f < 4; ++f) {
+    b.fft_field = fields[f];
+    cudaError_t e = launch_stage(ctx->L, b, 0, Stage::DivFftY);
+    if (e == cudaSuccess && g.nzm > 1) e = launch_stage(ctx->L, b, 0, Stage::FftZFwd);
+    if (e != cudaSuccess) return ctx_fail(ctx, e);
+    double *acc = ctx->spec_acc + (size_t)f * n;
+    const int nb = (int)std::min<size_t>((n + 255) / 256, 148 * 16);
+    if (ctx->L.mixed)
+      k_spec_acc<<<nb, 256, 0, ctx->stream>>>((const float2 *)ctx->spec, g.nxm, g.nyh, g.nzm, g.ldxc, dt, acc);
+    else
+      k_spec_acc<<<nb, 256, 0, ctx->stream>>>((const double2 *)ctx->spec, g.nxm, g.nyh, g.nzm, g.ldxc, dt, acc);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return ctx_fail(ctx, e);
+    ctx->launches += (g.nzm > 1) ? 3 : 2;
+  }
+  ctx->spec_tav += dt;
+  return AFID_OK;
+}
+
+int afid_gpu_spectra_read(afid_ctx_t *ctx, int which, double *out, double *tav) {
+  if (!ctx || !out || which < 0 || which > 3 || !ctx->spec_acc || !(ctx->spec_tav > 0.0)) return AFID_E_INVALID;
+  cudaSetDevice(ctx->dev);
+  const Geom &g = ctx->L.g;
+  const size_t n = (size_t)g.nxm * g.nyh * g.nzm;
+  cudaError_t e = cudaMemcpyAsync(out, ctx->spec_acc + (size_t)which * n, n * sizeof(double), cudaMemcpyDeviceToHost,
+                                  ctx->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+  if (e != cudaSuccess) return ctx_fail(ctx, e);
+  const double inv = 1.0 / ctx->spec_tav;  // WriteSpectra: divide by the averaging interval
+  for (size_t q = 0; q < n; ++q) out[q] *= inv;
+  if (tav) *tav = ctx->spec_tav;
+  return AFID_OK;
+}
+
+}  // extern "C"
+
+// ------------------------------------------------------------------------------------------
+// Planes of a field (MakeMovie{X,Y,Z}Cut.F90): a wall-parallel plane at k gathered by a kernel,
+// the others as strided 2-D copies.
+// ------------------------------------------------------------------------------------------
+namespace afid {
+
+__global__ void k_xcut(const double *__restrict__ f, int ldx, int nym, int nzm, int k, double *__restrict__ out) {
+  const size_t n = (size_t)nym * nzm;
+  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x)
+    out[e] = f[k + (size_t)ldx * e];
+}
+
+}  // namespace afid
+
+extern "C" int afid_gpu_slice(afid_ctx_t *ctx, int which, int axis, int index, double *out) {
+  if (!ctx || !out || which < 0 || which > 4 || ctx->L.g.batch) return AFID_E_INVALID;
+  cudaSetDevice(ctx->dev);
+  const Geom &g = ctx->L.g;
+  const double *f = (which == 0) ? ctx->vx : (which == 1) ? ctx->vy : (which == 2) ? ctx->vz
+                  : (which == 3) ? ctx->temp : ctx->pr;
+  const size_t dp = (size_t)g.ldx * sizeof(double), w = (size_t)g.nx * sizeof(double);
+  cudaError_t e = cudaSuccess;
+  if (axis == 0) {  // x = const: out[i][j], nzm x nym
+    if (index < 0 || index >= g.nx) return AFID_E_INVALID;
+    const size_t n = (size_t)g.nym * g.nzm;
+    if (ctx->stats_elems < n) {
+      if (ctx->stats_buf) cudaFree(ctx->stats_buf);
+      ctx->stats_buf = nullptr;
+      ctx->stats_elems = 0;
+      if (cudaMalloc(&ctx->stats_buf, n * sizeof(double)) != cudaSuccess) return AFID_E_ALLOC;
+      ctx->stats_elems = n;
+    }
+    k_xcut<<<(int)std::min<size_t>((n + 255) / 256, 148 * 8), 256, 0, ctx->stream>>>(f, g.ldx, g.nym, g.nzm, index,
+                                                                                      ctx->stats_buf);
+    ctx->launches += 1;
+    e = cudaGetLastError();
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(out, ctx->stats_buf, n * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream);
+  } else if (axis == 1) {  // y = const: out[i][k], nzm x nx
+    if (index < 0 || index >= g.nym) return AFID_E_INVALID;
+    e = cudaMemcpy2DAsync(out, w, f + (size_t)g.ldx * index, dp * g.nym, w, g.nzm, cudaMemcpyDeviceToHost, ctx->stream);
+  } else if (axis == 2) {  // z = const: out[j][k], nym x nx
+    if (index < 0 || index >= g.nzm) return AFID_E_INVALID;
+    e = cudaMemcpy2DAsync(out, w, f + (size_t)g.ldx * g.nym * index, dp, w, g.nym, cudaMemcpyDeviceToHost, ctx->stream);
+  } else {
+    return AFID_E_INVALID;
+  }
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+  return e == cudaSuccess ? AFID_OK : ctx_fail(ctx, e);
 }

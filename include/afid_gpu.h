@@ -135,6 +135,20 @@ long long afid_gpu_launch_count(afid_ctx_t *ctx);
 #define AFID_NUM_PROFILES 15
 int afid_gpu_mean_profiles(afid_ctx_t *ctx, double *out);
 
+/* Spectra of spectra.F90: per (k, ky, kz) the time average of |F|^2, F the y r2c + z c2c
+ * Fourier coefficients of vx, vy, vz, temp at k = 1..nxm normalised by 1/(nym nzm).
+ * afid_gpu_spectra_update(dt) adds dt*|F|^2 of the resident state (UpdateSpectra, after each
+ * TimeMarcher while averaging); afid_gpu_spectra_read(which = 0 vx, 1 vy, 2 vz, 3 temp) gives
+ * out[nxm * (nym/2+1) * nzm] (x fastest, then ky, then kz) divided by the accumulated interval
+ * (WriteSpectra), *tav = that interval; afid_gpu_spectra_reset starts a new average. */
+int afid_gpu_spectra_reset(afid_ctx_t *ctx);
+int afid_gpu_spectra_update(afid_ctx_t *ctx, double dt);
+int afid_gpu_spectra_read(afid_ctx_t *ctx, int which, double *out, double *tav);
+/* One plane of a resident field (which: 0 vx, 1 vy, 2 vz, 3 temp, 4 pr), as the movie cuts
+ * write them: axis 0 = x (wall-parallel plane at x index `index`): out[nzm][nym]; axis 1 = y:
+ * out[nzm][nx]; axis 2 = z: out[nym][nx]. */
+int afid_gpu_slice(afid_ctx_t *ctx, int which, int axis, int index, double *out);
+
 /* Autotuner of the fused explicit/implicit kernel: every thread shape available for this
  * wall-normal size (threads per x-column block x rows per thread) is timed on a sample of
  * columns, with the RK3 histories redirected to scratch memory so the state is untouched, and

@@ -1068,3 +1068,23 @@ def mean_profiles(g: Grid, s: State) -> dict:
     eps = eps + tdx2 * (dzx ** 2 + dzx_i ** 2) + tdx2 * (dyx ** 2 + dyx_j ** 2)
     out["epsilon"] = sums(eps) * inym * inzm / g.ren
     return out
+
+
+# ----------------------------------------------------------------------------------------------
+# Spectra (spectra.F90)
+# ----------------------------------------------------------------------------------------------
+def fourier_coef(g: Grid, var: np.ndarray) -> np.ndarray:
+    """``CalcFourierCoef`` (spectra.F90:70-96): y r2c then z c2c of var (nzm, nym, nxm), scaled by
+    1/(nzm*nym).  Returns (nzm, nym//2+1, nxm)."""
+    cy = np.fft.rfft(var, axis=1)
+    cz = np.fft.fft(cy, axis=0)
+    return cz * (1.0 / (g.p.nzm * g.p.nym))
+
+
+def spectra_update(g: Grid, s: State, dt: float, acc: dict) -> None:
+    """``UpdateSpectra`` / ``AddRealSpectrum`` (spectra.F90:101-114, 139-144): acc[name] += dt*|F|^2
+    for vx, vy, vz, temp at k = 1..nxm (no interpolation)."""
+    nxm = g.p.nxm
+    for name in ("vx", "vy", "vz", "temp"):
+        f = fourier_coef(g, getattr(s, name)[..., :nxm])
+        acc[name] = acc.get(name, 0.0) + dt * np.abs(f) ** 2
