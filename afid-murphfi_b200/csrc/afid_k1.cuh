@@ -68,8 +68,11 @@ struct ColV {
 
 template <typename TE> __device__ __forceinline__ TE cv(double v) { return (TE)v; }
 
+// In 2-D (TWO_D: the z neighbours are the cell itself) every z-difference term is zero by
+// construction; those terms are left out instead of being evaluated to zero.
+
 // ExplicitTermsVX.F90:194-291 + ImplicitAndUpdateVX.F90:124-150, k = 1..nxm-1 (0-based)
-template <typename TE>
+template <typename TE, bool TWO_D>
 __device__ __forceinline__ double rhs_vx(const Geom &g, const Tables &t, const StepCoef &sc, int k,
                                          const ColV &X, const ColV &Y, const ColV &Z, const ColV &T,
                                          const ColV &P, double ru, TE &qout) {
@@ -82,16 +85,19 @@ __device__ __forceinline__ double rhs_vx(const Geom &g, const Tables &t, const S
   const TE vxkp = cv<TE>(X.c[kp]), vxkm = cv<TE>(X.c[km]);
   const TE vxip = cv<TE>(X.ip[k]), vxim = cv<TE>(X.im[k]);
   const TE vxjp = cv<TE>(X.jp[k]), vxjm = cv<TE>(X.jm[k]);
-  const TE hxz = udx3c * udz *
-                 ((idxm * cv<TE>(Z.ip[km]) + idxc * cv<TE>(Z.ip[k])) * (vxip + vxc) -
-                  (idxm * cv<TE>(Z.c[km]) + idxc * cv<TE>(Z.c[k])) * (vxc + vxim));
+  TE hxz = (TE)0, dzzvx = (TE)0;
+  if constexpr (!TWO_D) {
+    hxz = udx3c * udz *
+          ((idxm * cv<TE>(Z.ip[km]) + idxc * cv<TE>(Z.ip[k])) * (vxip + vxc) -
+           (idxm * cv<TE>(Z.c[km]) + idxc * cv<TE>(Z.c[k])) * (vxc + vxim));
+    dzzvx = (vxim - (TE)2.0 * vxc + vxip) * udzq;
+  }
   const TE hxy = udx3c * udy *
                  ((idxm * cv<TE>(Y.jp[km]) + idxc * cv<TE>(Y.jp[k])) * (vxjp + vxc) -
                   (idxm * cv<TE>(Y.c[km]) + idxc * cv<TE>(Y.c[k])) * (vxc + vxjm));
   const TE hxx = ((vxkp + vxc) * (vxkp + vxc) - (vxc + vxkm) * (vxc + vxkm)) * udx3c * (TE)0.25;
-  const TE dzzvx = (vxim - (TE)2.0 * vxc + vxip) * udzq;
   const TE dyyvx = (vxjm - (TE)2.0 * vxc + vxjp) * udyq;
-  TE qcap = -(hxx + hxy + hxz) + dyyvx + dzzvx;
+  TE qcap = TWO_D ? (-(hxx + hxy) + dyyvx) : (-(hxx + hxy + hxz) + dyyvx + dzzvx);
   if (g.gaxis == 1) {
     const TE tempit = (TE)g.active_t * (TE)0.5 * (cv<TE>(T.c[k]) + cv<TE>(T.c[km]));
     qcap = qcap + (TE)g.byct * tempit;
@@ -105,7 +111,7 @@ __device__ __forceinline__ double rhs_vx(const Geom &g, const Tables &t, const S
 }
 
 // ExplicitTermsVY.F90:23-122 + ImplicitAndUpdateVY.F90:28-80, k = 0..nxm-1
-template <typename TE>
+template <typename TE, bool TWO_D>
 __device__ __forceinline__ double rhs_vy(const Geom &g, const Tables &t, const StepCoef &sc, int k,
                                          const ColV &X, const ColV &Y, const ColV &Z, const ColV &T,
                                          const ColV &P, double zd, double pjm, double ru, TE &qout) {
@@ -121,11 +127,16 @@ __device__ __forceinline__ double rhs_vy(const Geom &g, const Tables &t, const S
                   (cv<TE>(X.c[k]) + cv<TE>(X.jm[k])) * (c + cv<TE>(Y.c[kmm]))) *
                  cv<TE>(__ldg(t.udx3m + k)) * (TE)0.25;
   const TE hyy = ((vyjp + c) * (vyjp + c) - (vyjm + c) * (vyjm + c)) * udy;
-  const TE hyz = ((vyip + c) * (cv<TE>(Z.ip[k]) + cv<TE>(zd)) - (c + vyim) * (cv<TE>(Z.c[k]) + cv<TE>(Z.jm[k]))) *
-                 udz;
   const TE dyyvy = (vyjp - (TE)2.0 * c + vyjm) * udyq;
-  const TE dzzvy = (vyip - (TE)2.0 * c + vyim) * udzq;
-  TE dph = -(hyx + hyy + hyz) + dyyvy + dzzvy + (TE)g.gy;
+  TE dph;
+  if constexpr (TWO_D) {
+    dph = -(hyx + hyy) + dyyvy + (TE)g.gy;
+  } else {
+    const TE hyz = ((vyip + c) * (cv<TE>(Z.ip[k]) + cv<TE>(zd)) - (c + vyim) * (cv<TE>(Z.c[k]) + cv<TE>(Z.jm[k]))) *
+                   udz;
+    const TE dzzvy = (vyip - (TE)2.0 * c + vyim) * udzq;
+    dph = -(hyx + hyy + hyz) + dyyvy + dzzvy + (TE)g.gy;
+  }
   if (g.gaxis == 2) {
     const TE tempit = (TE)g.active_t * (TE)0.5 * (cv<TE>(T.c[k]) + cv<TE>(T.jm[k]));
     dph = dph + (TE)g.byct * tempit;
@@ -147,7 +158,7 @@ __device__ __forceinline__ double rhs_vy(const Geom &g, const Tables &t, const S
 }
 
 // ExplicitTermsVZ.F90:149-244 + ImplicitAndUpdateVZ.F90:121-161, k = 0..nxm-1
-template <typename TE>
+template <typename TE, bool TWO_D>
 __device__ __forceinline__ double rhs_vz(const Geom &g, const Tables &t, const StepCoef &sc, int k,
                                          const ColV &X, const ColV &Y, const ColV &Z, const ColV &T,
                                          const ColV &P, double yd, double pim, double ru, TE &qout) {
@@ -159,15 +170,20 @@ __device__ __forceinline__ double rhs_vz(const Geom &g, const Tables &t, const S
   const TE c = cv<TE>(Z.c[k]);
   const TE vzip = cv<TE>(Z.ip[k]), vzim = cv<TE>(Z.im[k]);
   const TE vzjp = cv<TE>(Z.jp[k]), vzjm = cv<TE>(Z.jm[k]);
-  const TE hzz = ((vzip + c) * (vzip + c) - (vzim + c) * (vzim + c)) * udz;
   const TE hzy = ((cv<TE>(Y.jp[k]) + cv<TE>(yd)) * (vzjp + c) - (cv<TE>(Y.c[k]) + cv<TE>(Y.im[k])) * (c + vzjm)) *
                  udy;
   const TE hzx = ((cv<TE>(X.c[kp]) + cv<TE>(X.im[kp])) * (cv<TE>(Z.c[kpp]) + c) -
                   (cv<TE>(X.c[k]) + cv<TE>(X.im[k])) * (c + cv<TE>(Z.c[kmm]))) *
                  cv<TE>(__ldg(t.udx3m + k)) * (TE)0.25;
-  const TE dzzvz = (vzip - (TE)2.0 * c + vzim) * udzq;
   const TE dyyvz = (vzjp - (TE)2.0 * c + vzjm) * udyq;
-  TE dq = -(hzx + hzy + hzz) + dyyvz + dzzvz;
+  TE dq;
+  if constexpr (TWO_D) {
+    dq = -(hzx + hzy) + dyyvz;
+  } else {
+    const TE hzz = ((vzip + c) * (vzip + c) - (vzim + c) * (vzim + c)) * udz;
+    const TE dzzvz = (vzip - (TE)2.0 * c + vzim) * udzq;
+    dq = -(hzx + hzy + hzz) + dyyvz + dzzvz;
+  }
   if (g.gaxis == 3) {
     const TE tempit = (TE)g.active_t * (TE)0.5 * (cv<TE>(T.c[k]) + cv<TE>(T.im[k]));
     dq = dq + (TE)g.byct * tempit;
@@ -175,13 +191,17 @@ __device__ __forceinline__ double rhs_vz(const Geom &g, const Tables &t, const S
   const double alre = sc.alre;
   const double amm = __ldg(t.am3sk + k), acc = __ldg(t.ac3sk + k), app = __ldg(t.ap3sk + k);
   const double dxxvz = Z.c[kpp] * app + Z.c[k] * acc + Z.c[kmm] * amm;
-  const double dzp = (P.c[k] - pim) * g.dz * sc.al;
   qout = dq;
-  return (sc.ga * (double)dq + sc.ro * ru + alre * dxxvz - dzp) * sc.dt;
+  if constexpr (TWO_D) {
+    return (sc.ga * (double)dq + sc.ro * ru + alre * dxxvz) * sc.dt;
+  } else {
+    const double dzp = (P.c[k] - pim) * g.dz * sc.al;
+    return (sc.ga * (double)dq + sc.ro * ru + alre * dxxvz - dzp) * sc.dt;
+  }
 }
 
 // ExplicitTermsTemp.F90:22-77 + ImplicitAndUpdateTemp.F90:197-237, k = 0..nxm-1
-template <typename TE>
+template <typename TE, bool TWO_D>
 __device__ __forceinline__ double rhs_temp(const Geom &g, const Tables &t, const StepCoef &sc, int k,
                                            const ColV &X, const ColV &Y, const ColV &Z, const ColV &T,
                                            double tbp, double ttp, double ru, TE &qout) {
@@ -199,11 +219,16 @@ __device__ __forceinline__ double rhs_temp(const Geom &g, const Tables &t, const
           (TE)0.5 * ux;
   const TE tip = cv<TE>(T.ip[k]), tim = cv<TE>(T.im[k]);
   const TE tjp = cv<TE>(T.jp[k]), tjm = cv<TE>(T.jm[k]);
-  const TE htz = (cv<TE>(Z.ip[k]) * (tip + tc) - cv<TE>(Z.c[k]) * (tc + tim)) * udz;
   const TE hty = (cv<TE>(Y.jp[k]) * (tjp + tc) - cv<TE>(Y.c[k]) * (tc + tjm)) * udy;
-  const TE dzzt = (tip - (TE)2.0 * tc + tim) * udzq;
   const TE dyyt = (tjp - (TE)2.0 * tc + tjm) * udyq;
-  const TE hro = -(htx + hty + htz) + dyyt + dzzt;
+  TE hro;
+  if constexpr (TWO_D) {
+    hro = -(htx + hty) + dyyt;
+  } else {
+    const TE htz = (cv<TE>(Z.ip[k]) * (tip + tc) - cv<TE>(Z.c[k]) * (tc + tim)) * udz;
+    const TE dzzt = (tip - (TE)2.0 * tc + tim) * udzq;
+    hro = -(htx + hty + htz) + dyyt + dzzt;
+  }
   const double alpec = sc.alpec;
   const double tcd = T.c[k];
   double dxxt;
@@ -374,10 +399,10 @@ __global__ void __launch_bounds__(TPC, k1_min_blocks<CAP, TPC>())
       const double yd = TWO_D ? Y.jp[k] : vv[p][1];
       const double pim = TWO_D ? P.c[k] : vv[p][3];
       // all four right-hand sides from the staged columns before anything is stored
-      rr[p][0] = (k >= 1) ? rhs_vx<TE>(g, t, sc, k, X, Y, Z, T, P, u0, q0) * __ldg(TX + k - 1) : 0.0;
-      rr[p][1] = rhs_vy<TE>(g, t, sc, k, X, Y, Z, T, P, zd, vv[p][2], u1, q1) * __ldg(TY + k);
-      rr[p][2] = rhs_vz<TE>(g, t, sc, k, X, Y, Z, T, P, yd, pim, u2, q2) * __ldg(TY + k);
-      rr[p][3] = rhs_temp<TE>(g, t, sc, k, X, Y, Z, T, tbp, ttp, u3, q3) * __ldg(TT + k);
+      rr[p][0] = (k >= 1) ? rhs_vx<TE, TWO_D>(g, t, sc, k, X, Y, Z, T, P, u0, q0) * __ldg(TX + k - 1) : 0.0;
+      rr[p][1] = rhs_vy<TE, TWO_D>(g, t, sc, k, X, Y, Z, T, P, zd, vv[p][2], u1, q1) * __ldg(TY + k);
+      rr[p][2] = rhs_vz<TE, TWO_D>(g, t, sc, k, X, Y, Z, T, P, yd, pim, u2, q2) * __ldg(TY + k);
+      rr[p][3] = rhs_temp<TE, TWO_D>(g, t, sc, k, X, Y, Z, T, tbp, ttp, u3, q3) * __ldg(TT + k);
       if (k >= 1) rux[c0 + k] = q0;
       ruy[c0 + k] = q1;
       ruz[c0 + k] = q2;
