@@ -101,6 +101,21 @@ int copy_field(afid_ctx_t *ctx, double *dst, const double *src, int ld_x, int ld
   const Geom &g = ctx->L.g;
   const size_t w = (size_t)g.nx * sizeof(double);
   cudaMemcpyKind kind = to_dev ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToHost;
+  if (ld_x == g.nx && ld_y == g.nym && g.nx != g.ldx && !g.batch) {
+    // packed host array: one linear transfer through an intermediate buffer (free between
+    // steps), repacked on the device; pitched copies of 2 KB rows run far below the link rate
+    const size_t rows = (size_t)g.nym * g.nzm, bytes = rows * w;
+    double *stage = ctx->vx_o;
+    if (to_dev) {
+      AFID_CUDA(ctx, cudaMemcpyAsync(stage, src, bytes, cudaMemcpyHostToDevice, ctx->stream));
+      AFID_CUDA(ctx, launch_repack(ctx->stream, stage, g.nx, dst, g.ldx, g.nx, rows));
+    } else {
+      AFID_CUDA(ctx, launch_repack(ctx->stream, dst, g.ldx, stage, g.nx, g.nx, rows));
+      AFID_CUDA(ctx, cudaMemcpyAsync(hdst, stage, bytes, cudaMemcpyDeviceToHost, ctx->stream));
+    }
+    ctx->launches += 1;
+    return AFID_OK;
+  }
   if (ld_y == g.nym) {
     if (to_dev)
       AFID_CUDA(ctx, cudaMemcpy2DAsync(dst, (size_t)g.ldx * sizeof(double), src, (size_t)ld_x * sizeof(double),

@@ -73,6 +73,8 @@ cudaError_t launch_max_reduce(const LaunchCtx &L, bool div, const double *vx, co
 cudaError_t launch_globals(const LaunchCtx &L, const double *vx, const double *vy,
                            const double *vz, const double *temp, double *partial, double *out3);
 int globals_partial_blocks(const Geom &g);
+cudaError_t launch_repack(cudaStream_t st, const double *src, int sld, double *dst, int dld, int width,
+                          size_t rows);
 
 }  // namespace afid
 

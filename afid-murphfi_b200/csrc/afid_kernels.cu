@@ -18,6 +18,8 @@
 // Template parameter TE is the type of the explicit terms and of the stored RK3 history
 // (double, or float for the mixed path); TS is the type of the spectral transforms.  The
 // state (vx, vy, vz, temp, pr), the RHS assembly and every tridiagonal solve are FP64.
+#include <algorithm>
+
 #include "afid_device.cuh"
 #include "afid_internal.h"
 #include "afid_k1.cuh"
@@ -1087,6 +1089,26 @@ static cudaError_t launch_stage_T(const LaunchCtx &L, const SubstepBuffers &b, i
 cudaError_t launch_stage(const LaunchCtx &L, const SubstepBuffers &b, int ns, Stage st) {
   if (st == Stage::ExplicitImplicit) return launch_explicit_implicit(L, b, ns);
   return L.mixed ? launch_stage_T<float>(L, b, ns, st) : launch_stage_T<double>(L, b, ns, st);
+}
+
+// dst[r*dld + k] = src[r*sld + k], k < width: between the padded device layout and a packed
+// staging copy (host transfers then run as one linear copy per field).
+__global__ void k_repack(const double *__restrict__ src, int sld, double *__restrict__ dst, int dld, int width,
+                         size_t rows) {
+  const size_t n = rows * (size_t)width;
+  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
+    const size_t r = e / width;
+    const int k = (int)(e - r * width);
+    dst[r * dld + k] = src[r * sld + k];
+  }
+}
+
+cudaError_t launch_repack(cudaStream_t st, const double *src, int sld, double *dst, int dld, int width,
+                          size_t rows) {
+  const size_t n = rows * (size_t)width;
+  const int nb = (int)std::min<size_t>((n + 255) / 256, (size_t)148 * 16);
+  k_repack<<<nb, 256, 0, st>>>(src, sld, dst, dld, width, rows);
+  return cudaGetLastError();
 }
 
 static int reduce_blocks(const Geom &g) {
