@@ -256,11 +256,17 @@ constexpr int kK1Centre = 4;
 __host__ __device__ inline size_t k1_stage_bytes(int ldx, bool two_d) {
   return (size_t)(two_d ? kK1StateCols2D : kK1StateCols) * ldx * sizeof(double);
 }
+// Staged columns sit at a compile-time stride of 32 M + 8 doubles (>= ldx = round_up(nxm+1, 8)
+// because nxm <= 32 M, and equal to it when nxm = 32 M), so every operand address is one base
+// register plus an immediate offset.
+__host__ __device__ constexpr int k1_col_stride(int M) { return 32 * M + 8; }
 // Dynamic shared memory of K1: the staged columns, or the centre columns plus the four RHS
 // arrays in chunk layout, whichever is larger.
 __host__ __device__ inline size_t k1_smem(int ldx, int M, bool two_d) {
-  const size_t rhs = (size_t)kK1Centre * ldx * sizeof(double) + (size_t)4 * chunk_ld(M) * M * sizeof(double);
-  const size_t st = k1_stage_bytes(ldx, two_d);
+  (void)ldx;
+  const int cs = k1_col_stride(M);
+  const size_t rhs = (size_t)kK1Centre * cs * sizeof(double) + (size_t)4 * chunk_ld(M) * M * sizeof(double);
+  const size_t st = (size_t)(two_d ? kK1StateCols2D : kK1StateCols) * cs * sizeof(double);
   return st > rhs ? st : rhs;
 }
 
@@ -294,7 +300,8 @@ __global__ void __launch_bounds__(TPC, k1_min_blocks<CAP, TPC>())
   Geom g = g0;
   const int ldx = g.ldx;
   double *cols = reinterpret_cast<double *>(smem_k1);
-  double *s_rhs = cols + (size_t)kK1Centre * ldx;  // over the neighbour columns, after they are used
+  constexpr int CS = k1_col_stride(M);
+  double *s_rhs = cols + (size_t)kK1Centre * CS;  // over the neighbour columns, after they are used
   const int tc = threadIdx.x;
   const int colid = blockIdx.x;
   const int j = colid % g.nym, i = colid / g.nym;
@@ -328,7 +335,7 @@ __global__ void __launch_bounds__(TPC, k1_min_blocks<CAP, TPC>())
                                            temp + ojp, temp + ojm,                     // 10-11
                                            pr + oc};                                   // 12
 #pragma unroll
-      for (int q = 0; q < kK1StateCols2D; ++q) bulk_g2s(cols + (size_t)q * ldx, src[q], cb, &bar);
+      for (int q = 0; q < kK1StateCols2D; ++q) bulk_g2s(cols + (size_t)q * CS, src[q], cb, &bar);
     } else {
       const double *src[kK1StateCols] = {vx + oc,    vy + oc,    vz + oc,    temp + oc,   // 0-3
                                          vx + ojp,   vx + ojm,   vx + oip,   vx + oim,    // 4-7
@@ -337,7 +344,7 @@ __global__ void __launch_bounds__(TPC, k1_min_blocks<CAP, TPC>())
                                          temp + ojp, temp + ojm, temp + oip, temp + oim,  // 16-19
                                          pr + oc};                                        // 20
 #pragma unroll
-      for (int q = 0; q < kK1StateCols; ++q) bulk_g2s(cols + (size_t)q * ldx, src[q], cb, &bar);
+      for (int q = 0; q < kK1StateCols; ++q) bulk_g2s(cols + (size_t)q * CS, src[q], cb, &bar);
     }
   }
   // single-row operands: diagonal neighbours (3-D) and pressure neighbours, to registers
@@ -370,7 +377,7 @@ __global__ void __launch_bounds__(TPC, k1_min_blocks<CAP, TPC>())
     mbar_wait(&bar, 0, kSpinLimit);  // let copies in flight land before the block exits
     return;
   }
-  auto C = [&](int q) { return (const double *)(cols + (size_t)q * ldx); };
+  auto C = [&](int q) { return (const double *)(cols + q * CS); };
   // {centre, j+1, j-1, i+1, i-1, diagonal}; in 2-D the i+-1 columns are the centre's
   const ColV X = TWO_D ? ColV{C(0), C(4), C(5), C(0), C(0), nullptr} : ColV{C(0), C(4), C(5), C(6), C(7), nullptr};
   const ColV Y = TWO_D ? ColV{C(1), C(6), C(7), C(1), C(1), nullptr} : ColV{C(1), C(8), C(9), C(10), C(11), nullptr};
