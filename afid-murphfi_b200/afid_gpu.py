@@ -143,7 +143,7 @@ EXPORTS = [
     "afid_serve_create", "afid_serve_destroy", "afid_serve_submit", "afid_serve_pump", "afid_serve_poll",
     "afid_serve_status", "afid_serve_now", "afid_gpu_autotune", "afid_batch_autotune",
     "afid_gpu_set_k1_shape", "afid_gpu_mean_profiles", "afid_batch_mean_profiles",
-    "afid_gpu_spectra_reset", "afid_gpu_spectra_update", "afid_gpu_spectra_read", "afid_gpu_slice",
+    "afid_batch_divmax", "afid_gpu_spectra_reset", "afid_gpu_spectra_update", "afid_gpu_spectra_read", "afid_gpu_slice",
 ]
 
 
@@ -209,6 +209,7 @@ def load_library(path: str = _LIB_PATH) -> C.CDLL:
         "afid_gpu_spectra_read": (i, [vp, i, _dp, _dp]),
         "afid_gpu_slice": (i, [vp, i, i, i, _dp]),
         "afid_batch_mean_profiles": (i, [vp, i, _dp]),
+        "afid_batch_divmax": (i, [vp, _dp]),
         "afid_batch_autotune": (i, [vp, i, C.POINTER(TuneInfoT)]),
         "afid_batch_step": (i, [vp, i]),
         "afid_batch_synchronize": (i, [vp]),
@@ -513,6 +514,11 @@ class Batch:
 
     def device_bytes(self) -> int:
         return int(lib().afid_batch_device_bytes(self._h))
+
+    def divmax(self) -> np.ndarray:
+        out = np.zeros(self.nslots)
+        _check(lib().afid_batch_divmax(self._h, _ptr(out)), "afid_batch_divmax")
+        return out
 
     def mean_profiles(self, slot: int) -> dict:
         out = np.zeros((len(PROFILE_NAMES), self.nxm))

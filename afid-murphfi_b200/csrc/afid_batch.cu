@@ -47,6 +47,28 @@ __global__ void __launch_bounds__(256)
   if (lane == 0) atomicMax(out + i, (unsigned long long)__double_as_longlong(m));
 }
 
+// Maximum |div u| of each instance (CheckDivergence.F90:36-39), same layout as k_batch_cfl.
+__global__ void __launch_bounds__(256)
+    k_batch_div(Geom g, Tables t, const double *__restrict__ vx, const double *__restrict__ vy,
+                const double *__restrict__ vz, unsigned long long *__restrict__ out) {
+  const int i = blockIdx.y;
+  bind_instance(g, i);
+  const int lane = threadIdx.x & 31;
+  double m = 0.0;
+  for (int j = blockIdx.x * 8 + (threadIdx.x >> 5); j < g.nym; j += gridDim.x * 8) {
+    const int jp = wrap_inc(j, g.nym);
+    const size_t c = col_off(g, j, i), cjp = col_off(g, jp, i), cip = col_off(g, j, zinc(g, i));
+    for (int k = lane; k < g.nxm; k += 32) {
+      const double dq = (vz[cip + k] - vz[c + k]) * g.dz + (vy[cjp + k] - vy[c + k]) * g.dy +
+                        (vx[c + k + 1] - vx[c + k]) * t.udx3m[k];
+      m = fmax(m, fabs(dq));
+    }
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if (lane == 0) atomicMax(out + i, (unsigned long long)__double_as_longlong(m));
+}
+
 // dt rule of main.F90:287-304 per instance.  An instance whose previous step raised an error
 // code is switched off before this step (the reference exits after the step that set it).
 __global__ void k_batch_dt(int nslots, unsigned char *__restrict__ active, const InstCtl *__restrict__ ctl,
@@ -624,6 +646,37 @@ int afid_batch_mean_profiles(afid_batch_t *b, int slot, double *out) {
   if (b->three_d)
     return ctx_mean_profiles(ctx, 0, g.nym * g.nzm, (double)g.nym * (double)g.nzm, g.ren, g.pect, out);
   return ctx_mean_profiles(ctx, slot * g.nym, g.nym, (double)g.nym, sc.ren, sc.pect, out);
+}
+
+int afid_batch_divmax(afid_batch_t *b, double *dmax) {
+  if (!b || !dmax) return AFID_E_INVALID;
+  afid_ctx_t *ctx = b->ctx;
+  cudaSetDevice(ctx->dev);
+  const LaunchCtx &L = ctx->L;
+  cudaStream_t st = ctx->stream;
+  cudaError_t e;
+  if (b->three_d) {
+    e = launch_max_reduce(L, true, ctx->vx, ctx->vy, ctx->vz, b->cfl_bits);
+  } else {
+    e = cudaMemsetAsync(b->cfl_bits, 0, sizeof(unsigned long long) * b->nslots, st);
+    if (e == cudaSuccess) {
+      k_batch_div<<<dim3(kChunks, b->nslots), 256, 0, st>>>(L.g, L.t, ctx->vx, ctx->vy, ctx->vz, b->cfl_bits);
+      e = cudaGetLastError();
+    }
+  }
+  b->launches += 1;
+  ctx->launches += 1;
+  std::vector<unsigned long long> h(b->nslots);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(h.data(), b->cfl_bits, sizeof(unsigned long long) * b->nslots, cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return ctx_fail(ctx, e);
+  for (int i = 0; i < b->nslots; ++i) {
+    double v;
+    std::memcpy(&v, &h[i], sizeof(double));
+    dmax[i] = v;
+  }
+  return AFID_OK;
 }
 
 int afid_batch_autotune(afid_batch_t *b, int force, afid_tune_info_t *info) {

@@ -249,3 +249,20 @@ def test_step_limit_stops_slot_exactly():
     for k in ag.Batch.FIELDS:
         assert np.array_equal(got[k][:, :NXM], ref[k][:, :NXM]), k
     assert st["time"][1] == st_ref["time"][1]
+
+
+def test_divergence_check_per_slot():
+    """CheckDivergence per slot: after steps the projected fields are divergence-free to
+    round-off; a slot given a divergent field reports it, the others do not."""
+    with _batch(ag.PREC_FP64) as b:
+        for s in range(b.nslots):
+            _perturb(b, s)
+        b.set_active(np.ones(b.nslots, np.uint8))
+        b.step(3)
+        d = b.divmax()
+        assert np.all(d < 1e-9), d
+        f = b.download(2)
+        f["vy"][5, 3] += 1.0  # one cell, no longer divergence-free
+        b.upload(2, f["vx"], f["vy"], f["vz"], f["temp"], f["pr"])
+        d2 = b.divmax()
+    assert d2[2] > 1.0 and np.all(np.delete(d2, 2) < 1e-9)
