@@ -95,6 +95,15 @@ class Params:
     dpdz: float = 0.0
     tout: float = 1e30
     tmax: float = 1e30
+    # multi-resolution salinity (MULTIRES NXMR NYMR NZMR, ISTR3R, SfixS SfixN, active_S)
+    multires: int = 0
+    nxmr: int = 0
+    nymr: int = 0
+    nzmr: int = 0
+    istr3r: int = 4
+    sfixs: int = 1
+    sfixn: int = 1
+    active_s: int = 0
 
     @property
     def nx(self) -> int:
@@ -112,6 +121,13 @@ class Params:
         pect = ren * self.prat
         pi = 2.0 * math.asin(1.0)
         return ren, pect, byct, pi
+
+    def derived_salinity(self):
+        """pecs and bycs of ``ReadInputFile.F90:109-122``."""
+        ren, _, _, _ = self.derived()
+        rrho = abs(self.rayt) * self.pras / (abs(self.rays) * self.prat)
+        bycs = 1.0 if (self.salinity and self.ffscales == 1) else 1.0 / rrho
+        return ren * self.pras, bycs
 
 
 def parse_bou_in(text: str) -> Params:
@@ -133,7 +149,7 @@ def parse_bou_in(text: str) -> Params:
     skip(2)
     nxm, nym, nzm, nsst = (int(float(x)) for x in vals()[:4])
     skip(3)
-    vals()  # MULTIRES NXMR NYMR NZMR (refined grid: not on this path)
+    multires, nxmr, nymr, nzmr = (int(float(x)) for x in vals()[:4])
     skip(3)
     flagsal, _flagpf = (int(float(x)) for x in vals()[:2])
     skip(3)
@@ -150,6 +166,7 @@ def parse_bou_in(text: str) -> Params:
     skip(3)
     v = vals()
     istr3, str3 = int(float(v[0])), float(v[1])
+    istr3r = int(float(v[2])) if len(v) > 2 else istr3
     skip(3)
     v = vals()
     rayt, prat, rays, pras = (float(x) for x in v[:4])
@@ -161,9 +178,10 @@ def parse_bou_in(text: str) -> Params:
     skip(3)
     v = vals()
     inslws, inslwn, tfixs, tfixn = (int(float(x)) for x in v[:4])
+    sfixs, sfixn = (int(float(x)) for x in v[4:6]) if len(v) >= 6 else (1, 1)
     skip(3)
     v = vals()
-    active_t, _active_s, gaxis = (int(float(x)) for x in v[:3])
+    active_t, active_s, gaxis = (int(float(x)) for x in v[:3])
     skip(3)
     v = vals()
     xplusu, xminusu, dpdy, dpdz = (float(x) for x in v[:4])
@@ -172,7 +190,9 @@ def parse_bou_in(text: str) -> Params:
                   ffscales=ffscales, salinity=bool(flagsal), idtv=idtv, dt=dt, resid=resid,
                   limit_cfl=limit_cfl, dtmin=dtmin, dtmax=dtmax, inslws=inslws, inslwn=inslwn,
                   tfixs=tfixs, tfixn=tfixn, active_t=active_t, gaxis=gaxis, xplusu=xplusu,
-                  xminusu=xminusu, dpdy=dpdy, dpdz=dpdz, tout=tout, tmax=tmax)
+                  xminusu=xminusu, dpdy=dpdy, dpdz=dpdz, tout=tout, tmax=tmax,
+                  multires=multires, nxmr=nxmr, nymr=nymr, nzmr=nzmr, istr3r=istr3r,
+                  sfixs=sfixs, sfixn=sfixn, active_s=active_s)
 
 
 def rk3_coefficients(nsst: int = 3):

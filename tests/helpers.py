@@ -12,11 +12,11 @@ NXM     NYM     NZM     NSST(>1=RK,else AB)
 
 Refined grid: on/off and grid size
 MULTIRES    NXMR    NYMR    NZMR
-0           {nxm}     {nym}     {nzm}
+{multires}           {nxmr}     {nymr}     {nzmr}
 
 Salinity and Phase-field (on/off)
 FLAGSAL     FLAGPF
-0           0
+{flagsal}           0
 
 Read flow / Reset logs
 NREAD       IRESET
@@ -36,11 +36,11 @@ ALX3   YLEN   ZLEN
 
 Grid stretching parameters
 ISTR3   STR3    ISTR3R
-{istr3}       {str3}     0
+{istr3}       {str3}     {istr3r}
 
 Physical flow parameters / Free-fall timescale
 RAYT    PRAT    RAYS    PRAS    FFscaleS
-{rayt}     {prat}     1e8     1.0     0
+{rayt}     {prat}     {rays}     {pras}     {ffscales}
 
 Time stepping parameters
 IDTV    DT      RESID   CFLMAX  DTMIN   DTMAX
@@ -48,11 +48,11 @@ IDTV    DT      RESID   CFLMAX  DTMIN   DTMAX
 
 Dirichlet/Neumann BC flag on upper(N) and lower(S) walls
 inslwS  inslwN  TfixS   TfixN   SfixS   SfixN
-{inslws}       {inslwn}       {tfixs}       {tfixn}       1       1
+{inslws}       {inslwn}       {tfixs}       {tfixn}       {sfixs}       {sfixn}
 
 Active/passive scalar flags / Gravitational axis (x=1,y=2,z=3)
 active_T    active_S    gAxis
-{active_t}           0           {gaxis}
+{active_t}           {active_s}           {gaxis}
 
 Wall velocity / Pressure gradient / Melt boundary condition
 xplusU  xminusU     dPdy    dPdz    MELT
@@ -66,11 +66,13 @@ pf_D(*Pe)   pf_A    pf_S    pf_Tm   IBM     pf_IC
 DEFAULTS = dict(nsst=3, ntst=9, tmax=1e30, tout=1e30, alx3=1.0, ylen=1.0, zlen=1.0, istr3=4,
                 str3=2.0, rayt=1e6, prat=1.0, idtv=0, dt=1e-3, resid=1e-3, cflmax=10.0,
                 dtmax=1e-2, inslws=1, inslwn=1, tfixs=1, tfixn=1, active_t=1, gaxis=1,
-                xplusu=0.0, xminusu=0.0, dpdy=0.0)
+                xplusu=0.0, xminusu=0.0, dpdy=0.0, multires=0, flagsal=0, istr3r=0, rays=1e8,
+                pras=1.0, ffscales=0, sfixs=1, sfixn=1, active_s=0)
 
 
 def bou_text(nxm, nym, nzm, **kw) -> str:
     v = dict(DEFAULTS)
+    v.update(nxmr=nxm, nymr=nym, nzmr=nzm)
     v.update(kw)
     return BOU_TEMPLATE.format(nxm=nxm, nym=nym, nzm=nzm, **v)
 
