@@ -120,11 +120,32 @@ class ServeStatusT(C.Structure):
 
 SERVE_FIFO, SERVE_SHORTEST_FIRST = 0, 1
 
+
+class StencilT(C.Structure):
+    _fields_ = [("n", C.c_int), ("start", C.POINTER(C.c_int)), ("w", C.POINTER(C.c_double))]
+
+
+class SalGridT(C.Structure):
+    _fields_ = [("nxmr", C.c_int), ("nymr", C.c_int), ("nzmr", C.c_int),
+                ("dxr", C.c_double), ("dyr", C.c_double), ("dzr", C.c_double),
+                ("pecs", C.c_double), ("bycs", C.c_double),
+                ("active_s", C.c_int), ("sfixs", C.c_int), ("sfixn", C.c_int),
+                ("xcr", C.POINTER(C.c_double)), ("udx3mr", C.POINTER(C.c_double)), ("g3rmr", C.POINTER(C.c_double)),
+                ("ap3sskr", C.POINTER(C.c_double)), ("ac3sskr", C.POINTER(C.c_double)),
+                ("am3sskr", C.POINTER(C.c_double)),
+                ("salbp", C.POINTER(C.c_double)), ("saltp", C.POINTER(C.c_double)),
+                ("to_ref", StencilT * 3), ("to_coarse", StencilT * 3)]
+
+
+# afid_gpu_sal_profiles order (the means.h5 dataset names of CalcSalStats)
+SAL_PROFILE_NAMES = ("Sbar", "Srms", "vxS", "vyS", "vzS", "chiS")
+
 # afid_gpu_mean_profiles order (the means.h5 dataset names of CalcMeanProfiles.F90)
 PROFILE_NAMES = ("Tbar", "vybar", "vzbar", "vxT", "vyT", "vzT", "Trms", "vxrms", "vyrms", "vzrms",
                  "vxvy", "vxvz", "vyvz", "chiT", "epsilon")
 
-# Every symbol declared in include/afid_gpu.h, afid_host.h, afid_batch.h and afid_serve.h
+# Every symbol declared in include/afid_gpu.h, afid_host.h, afid_batch.h, afid_serve.h and
+# afid_salinity.h
 EXPORTS = [
     "afid_gpu_create", "afid_gpu_destroy", "afid_gpu_set_stream", "afid_gpu_get_stream",
     "afid_gpu_synchronize", "afid_gpu_upload", "afid_gpu_download", "afid_gpu_timemarcher",
@@ -144,6 +165,9 @@ EXPORTS = [
     "afid_serve_status", "afid_serve_now", "afid_gpu_autotune", "afid_batch_autotune",
     "afid_gpu_set_k1_shape", "afid_gpu_mean_profiles", "afid_batch_mean_profiles",
     "afid_batch_divmax", "afid_gpu_spectra_reset", "afid_gpu_spectra_update", "afid_gpu_spectra_read", "afid_gpu_slice",
+    "afid_mgrd_create", "afid_mgrd_destroy", "afid_mgrd_view", "afid_mgrd_fast", "afid_mgrd_array",
+    "afid_initial_salinity", "afid_gpu_sal_create", "afid_gpu_sal_upload", "afid_gpu_sal_download",
+    "afid_gpu_sal_interpolate", "afid_gpu_sal_cfl", "afid_gpu_sal_profiles", "afid_gpu_sal_download_aux",
 ]
 
 
@@ -217,6 +241,19 @@ def load_library(path: str = _LIB_PATH) -> C.CDLL:
         "afid_batch_num_slots": (i, [vp]),
         "afid_batch_device_bytes": (C.c_longlong, [vp]),
         "afid_batch_launch_count": (C.c_longlong, [vp]),
+        "afid_mgrd_create": (i, [vp, C.POINTER(vp)]),
+        "afid_mgrd_destroy": (None, [vp]),
+        "afid_mgrd_view": (C.POINTER(SalGridT), [vp]),
+        "afid_mgrd_fast": (i, [vp]),
+        "afid_mgrd_array": (_dp, [vp, C.c_char_p, C.POINTER(i)]),
+        "afid_initial_salinity": (i, [vp, C.c_uint64, d, _dp, i, i]),
+        "afid_gpu_sal_create": (i, [vp, C.POINTER(SalGridT)]),
+        "afid_gpu_sal_upload": (i, [vp, _dp, i, i]),
+        "afid_gpu_sal_download": (i, [vp, _dp, i, i]),
+        "afid_gpu_sal_interpolate": (i, [vp]),
+        "afid_gpu_sal_cfl": (i, [vp, _dp]),
+        "afid_gpu_sal_profiles": (i, [vp, _dp]),
+        "afid_gpu_sal_download_aux": (i, [vp, _dp, _dp, _dp, i, i, _dp, i, i]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -290,6 +327,53 @@ class Tables:
     def close(self):
         if self._h:
             lib().afid_tables_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Mgrd:
+    """Refined salinity grid and stencils (CreateMgrdGrid + CreateMgrdStencil) built by the C++
+    host code from the coarse ``Tables`` of a bou.in with MULTIRES = FLAGSAL = 1."""
+
+    def __init__(self, tables: Tables):
+        self.tables = tables
+        self._h = C.c_void_p()
+        _check(lib().afid_mgrd_create(tables._h, C.byref(self._h)), "afid_mgrd_create")
+
+    @property
+    def view(self) -> SalGridT:
+        return lib().afid_mgrd_view(self._h).contents
+
+    @property
+    def fast(self) -> bool:
+        return bool(lib().afid_mgrd_fast(self._h))
+
+    @property
+    def shape(self):
+        v = self.view
+        return (v.nzmr, v.nymr, v.nxmr)
+
+    def array(self, name: str) -> np.ndarray:
+        n = C.c_int()
+        p = lib().afid_mgrd_array(self._h, name.encode(), C.byref(n))
+        if not p:
+            raise KeyError(name)
+        return np.ctypeslib.as_array(p, shape=(n.value,)).copy()
+
+    def initial_salinity(self, seed: int, amp: float = 5e-3) -> np.ndarray:
+        nz, ny, nx = self.shape
+        out = np.zeros((nz, ny, nx))
+        _check(lib().afid_initial_salinity(self._h, seed, amp, _ptr(out), nx, ny), "afid_initial_salinity")
+        return out
+
+    def close(self):
+        if self._h:
+            lib().afid_mgrd_destroy(self._h)
             self._h = C.c_void_p()
 
     def __del__(self):
@@ -408,6 +492,48 @@ class Solver:
         a = np.zeros(shape)
         _check(lib().afid_gpu_slice(self._h, which, axis, index, _ptr(a)), "afid_gpu_slice")
         return a
+
+    # ---- multi-resolution salinity (include/afid_salinity.h) ----
+    def sal_create(self, mgrd: "Mgrd") -> None:
+        _check(lib().afid_gpu_sal_create(self._h, C.byref(mgrd.view)), "afid_gpu_sal_create")
+        self._sal_shape = mgrd.shape
+
+    def sal_upload(self, sal: np.ndarray) -> None:
+        nz, ny, nx = self._sal_shape
+        a = np.ascontiguousarray(sal, dtype=np.float64)
+        if a.shape != (nz, ny, nx):
+            raise ValueError(f"salinity shape {a.shape} != {(nz, ny, nx)}")
+        _check(lib().afid_gpu_sal_upload(self._h, _ptr(a), nx, ny), "afid_gpu_sal_upload")
+
+    def sal_download(self) -> np.ndarray:
+        nz, ny, nx = self._sal_shape
+        out = np.zeros((nz, ny, nx))
+        _check(lib().afid_gpu_sal_download(self._h, _ptr(out), nx, ny), "afid_gpu_sal_download")
+        return out
+
+    def sal_interpolate(self) -> None:
+        _check(lib().afid_gpu_sal_interpolate(self._h), "afid_gpu_sal_interpolate")
+
+    def sal_cfl(self) -> float:
+        v = C.c_double()
+        _check(lib().afid_gpu_sal_cfl(self._h, C.byref(v)), "afid_gpu_sal_cfl")
+        return v.value
+
+    def sal_profiles(self) -> dict:
+        nxmr = self._sal_shape[2]
+        out = np.zeros(6 * nxmr)
+        _check(lib().afid_gpu_sal_profiles(self._h, _ptr(out)), "afid_gpu_sal_profiles")
+        return {n: out[q * nxmr:(q + 1) * nxmr].copy() for q, n in enumerate(SAL_PROFILE_NAMES)}
+
+    def sal_aux(self) -> dict:
+        """vxr (nzmr, nymr, nxmr+1), vyr / vzr (.., nxmr+1, last row unused) and salc (nzm, nym, nxm)."""
+        nz, ny, nx = self._sal_shape
+        nzm, nym, nxc = self.shape
+        vxr, vyr, vzr = (np.zeros((nz, ny, nx + 1)) for _ in range(3))
+        salc = np.zeros((nzm, nym, nxc - 1))
+        _check(lib().afid_gpu_sal_download_aux(self._h, _ptr(vxr), _ptr(vyr), _ptr(vzr), nx + 1, ny, _ptr(salc),
+                                               nxc - 1, nym), "afid_gpu_sal_download_aux")
+        return dict(vxr=vxr, vyr=vyr[..., :nx], vzr=vzr[..., :nx], salc=salc)
 
     def set_k1_shape(self, index: int) -> None:
         _check(lib().afid_gpu_set_k1_shape(self._h, index), "afid_gpu_set_k1_shape")

@@ -11,6 +11,7 @@
 
 #include "afid_gpu.h"
 #include "afid_internal.h"
+#include "afid_salinity.h"
 
 using namespace afid;
 
@@ -225,11 +226,42 @@ int build_cn(afid_ctx_t *ctx, int ns0, int nsub, const double *al, const double 
   in.sc = ctx->sc;
   AFID_CUDA(ctx, timed(ctx, 0, [&] { return launch_cn_tables(ctx->L, in); }));
   ctx->launches += 1;
+  if (ctx->sal) {
+    // SolveImpEqnUpdate_Sal (salinity.F90:408-425): one temperature-like matrix on the refined
+    // rows with betadx = 0.5 al dt / pecs; its StepCoef carries alpec = al / pecs
+    const SalCtx &S = *ctx->sal;
+    CnInputs si = in;
+    si.nmat = 1;
+    si.am[0] = S.am_d;
+    si.ac[0] = S.ac_d;
+    si.ap[0] = S.ap_d;
+    si.off[0] = 0;
+    si.n[0] = S.sg.nxmr;
+    si.pect = S.sg.pecs;
+    si.M = S.sg.MR;
+    si.tab = S.cn_tab;
+    si.sc = S.sc;
+    AFID_CUDA(ctx, timed(ctx, 0, [&] { return launch_cn_tables(ctx->L, si); }));
+    ctx->launches += 1;
+  }
+  return AFID_OK;
+}
+
+// InterpVelMgrd + InterpSalMultigrid (TimeMarcher.F90:138-144) from the resident state.
+int sal_interp(afid_ctx_t *ctx) {
+  AFID_CUDA(ctx, timed(ctx, 10, [&] { return launch_sal_interp(ctx->L, *ctx->sal, ctx->vx, ctx->vy, ctx->vz); }));
+  ctx->launches += kSalLaunchesInterp;
   return AFID_OK;
 }
 
 int run_substep(afid_ctx_t *ctx, int ns) {
   SubstepBuffers b = buffers(ctx);
+  if (ctx->sal) {
+    // ExplicitSalinity + ImplicitSalinity read the refined velocities and salc of the previous
+    // substep only, so the salinity update goes first (TimeMarcher.F90:50-51, 95)
+    AFID_CUDA(ctx, timed(ctx, 9, [&] { return launch_sal_step(ctx->L, *ctx->sal, ns); }));
+    ctx->launches += 1;
+  }
   for (int st = 0; st < kNumStages; ++st) {
     const Stage stage = static_cast<Stage>(st);
     if ((ctx->L.g.nzm == 1 || ctx->L.g.batch) && (stage == Stage::FftZFwd || stage == Stage::FftZInv)) continue;
@@ -237,6 +269,10 @@ int run_substep(afid_ctx_t *ctx, int ns) {
     ctx->launches += 1;
   }
   std::swap(ctx->temp, ctx->temp_o);  // temperature is final after K1; the state moves buffers
+  if (ctx->sal) {
+    std::swap(ctx->sal->sal, ctx->sal->sal_o);
+    return sal_interp(ctx);
+  }
   return AFID_OK;
 }
 
@@ -649,6 +685,7 @@ int afid_gpu_destroy(afid_ctx_t *ctx) {
   cudaSetDevice(ctx->dev);
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   for (void *p : ctx->allocs) cudaFree(p);
+  delete ctx->sal;
   if (ctx->stats_buf) cudaFree(ctx->stats_buf);
   if (ctx->spec_acc) cudaFree(ctx->spec_acc);
   for (cudaEvent_t e : ctx->ev_pool) cudaEventDestroy(e);
@@ -687,6 +724,7 @@ int afid_gpu_upload(afid_ctx_t *ctx, const double *vx, const double *vy, const d
   if (pr && (s = copy_field(ctx, ctx->pr, pr, ld_x, ld_y, true)) != AFID_OK) return s;
   const size_t tsz = ctx->L.mixed ? sizeof(float) : sizeof(double);
   AFID_CUDA(ctx, cudaMemsetAsync(ctx->rux, 0, 4 * ctx->field_elems * tsz, ctx->stream));
+  if (ctx->sal && (s = sal_interp(ctx)) != AFID_OK) return s;  // the refined velocities follow
   AFID_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   return AFID_OK;
 }
@@ -844,6 +882,216 @@ int afid_gpu_profile_report(afid_ctx_t *ctx, double *ms, long long *count, int n
   ctx->recs.clear();
   ctx->ev_used = 0;
   return AFID_OK;
+}
+
+}  // extern "C"
+
+// ==========================================================================================
+// Multi-resolution salinity (include/afid_salinity.h)
+// ==========================================================================================
+namespace {
+
+bool stencil_ok(const afid_stencil_t &s, int n, int lo, int hi) {
+  if (s.n != n || !s.start || !s.w) return false;
+  for (int t = 0; t < n; ++t)
+    if (s.start[t] < lo || s.start[t] > hi) return false;
+  return true;
+}
+
+// Refined field <-> Fortran-layout host array (rows x nymr x nzmr, leading dims ld_x, ld_y).
+int sal_copy(afid_ctx_t *ctx, double *dev, int rows, const double *src, double *hdst, int ld_x, int ld_y,
+             bool to_dev) {
+  const SalGeom &sg = ctx->sal->sg;
+  const size_t w = (size_t)rows * sizeof(double), dp = (size_t)sg.ldr * sizeof(double);
+  const size_t hp = (size_t)ld_x * sizeof(double);
+  for (int i = 0; i < sg.nzmr; ++i) {
+    const size_t hoff = (size_t)i * ld_x * ld_y, doff = (size_t)i * sg.ldr * sg.nymr;
+    if (to_dev)
+      AFID_CUDA(ctx, cudaMemcpy2DAsync(dev + doff, dp, src + hoff, hp, w, sg.nymr, cudaMemcpyHostToDevice, ctx->stream));
+    else
+      AFID_CUDA(ctx, cudaMemcpy2DAsync(hdst + hoff, hp, dev + doff, dp, w, sg.nymr, cudaMemcpyDeviceToHost, ctx->stream));
+  }
+  return AFID_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int afid_gpu_sal_create(afid_ctx_t *ctx, const afid_sal_grid_t *sg) {
+  if (!ctx || !sg || ctx->sal) return AFID_E_INVALID;
+  Geom &g = ctx->L.g;
+  if (g.batch) return AFID_E_INVALID;
+  const int nxmr = sg->nxmr, nymr = sg->nymr, nzmr = sg->nzmr;
+  if (nxmr < 3 || nymr < 1 || nzmr < 1 || (g.nzm == 1) != (nzmr == 1)) return AFID_E_INVALID;
+  const int MR = cn_choose_M(nxmr);
+  if (MR < 0) return AFID_E_INVALID;
+  if (!sg->xcr || !sg->udx3mr || !sg->g3rmr || !sg->ap3sskr || !sg->ac3sskr || !sg->am3sskr || !sg->salbp ||
+      !sg->saltp || !(sg->pecs > 0.0))
+    return AFID_E_INVALID;
+  // every source row the kernels read stays inside the (wall-extended) columns
+  if (!stencil_ok(sg->to_ref[0], nxmr, -2, g.nxm - 2) || !stencil_ok(sg->to_ref[1], nymr, -2 * nymr, 2 * nymr) ||
+      !stencil_ok(sg->to_ref[2], nzmr, -2 * nzmr, 2 * nzmr) || !stencil_ok(sg->to_coarse[0], g.nxm, -2, nxmr - 2) ||
+      !stencil_ok(sg->to_coarse[1], g.nym, -2 * g.nym, 2 * g.nym) ||
+      !stencil_ok(sg->to_coarse[2], g.nzm, -2 * g.nzm, 2 * g.nzm))
+    return AFID_E_INVALID;
+  const bool two_d = nzmr == 1;
+  const size_t smem_step = sal_step_smem_bytes(MR, two_d);
+  const size_t smem_ref = (size_t)(3 * (g.nxm + 4) + nxmr) * sizeof(double);
+  if (smem_step > 227 * 1024 || smem_ref > 227 * 1024) return AFID_E_INVALID;
+  cudaSetDevice(ctx->dev);
+  SalCtx *S = new (std::nothrow) SalCtx();
+  if (!S) return AFID_E_ALLOC;
+  SalGeom &q = S->sg;
+  q.nxmr = nxmr;
+  q.nymr = nymr;
+  q.nzmr = nzmr;
+  q.ldr = (nxmr + 1 + 7) / 8 * 8;
+  q.MR = MR;
+  q.dxr = sg->dxr;
+  q.dyr = sg->dyr;
+  q.dzr = sg->dzr;
+  q.udyr = 0.5 * sg->dyr;  // salinity.F90:279-283
+  q.udzr = 0.5 * sg->dzr;
+  q.udyrq = sg->dyr * sg->dyr / sg->pecs;
+  q.udzrq = sg->dzr * sg->dzr / sg->pecs;
+  q.lya = 1. / sg->dyr;  // InterpVelMgrd.F90:120, 204
+  q.lza = 1. / sg->dzr;
+  q.pecs = sg->pecs;
+  q.sfixs = sg->sfixs;
+  q.sfixn = sg->sfixn;
+  S->active_s = sg->active_s;
+  S->bycs = sg->bycs;
+  S->relems = (size_t)q.ldr * nymr * nzmr;
+  S->err = ctx->err;
+  auto fail = [&](cudaError_t e) {
+    delete S;
+    return fail_cuda(ctx, e);
+  };
+  cudaError_t e = cudaSuccess;
+  double **rf[8] = {&S->sal, &S->sal_o, &S->rusal, &S->vxr, &S->vyr, &S->vzr, &S->gyr, &S->gzr};
+  for (double **p : rf)
+    if ((e = dalloc(ctx, p, S->relems)) != cudaSuccess) return fail(e);
+  double **cf[4] = {&S->gx, &S->gy, &S->gz, &S->salc};
+  for (double **p : cf)
+    if ((e = dalloc(ctx, p, ctx->field_elems)) != cudaSuccess) return fail(e);
+  // 1-D tables
+  std::vector<double> lxa(nxmr), tdxr(nxmr);
+  for (int k = 0; k < nxmr; ++k) {
+    lxa[k] = sg->xcr[k + 1] - sg->xcr[k];         // InterpVelMgrd.F90:53
+    tdxr[k] = 0.5 * sg->dxr / sg->g3rmr[k];       // salinity.F90:605-607
+  }
+  auto up = [&](const double *h, size_t n, const double **d) -> cudaError_t {
+    double *p = nullptr;
+    cudaError_t r = dalloc(ctx, &p, n);
+    if (r == cudaSuccess) r = cudaMemcpy(p, h, n * sizeof(double), cudaMemcpyHostToDevice);
+    *d = p;
+    return r;
+  };
+  SalTables &st = S->st;
+  const size_t npl = (size_t)nymr * nzmr;
+  if ((e = up(lxa.data(), nxmr, &st.lxa)) != cudaSuccess || (e = up(sg->udx3mr, nxmr, &st.udx3mr)) != cudaSuccess ||
+      (e = up(tdxr.data(), nxmr, &st.tdxr)) != cudaSuccess || (e = up(sg->ap3sskr, nxmr, &st.ap)) != cudaSuccess ||
+      (e = up(sg->ac3sskr, nxmr, &st.ac)) != cudaSuccess || (e = up(sg->am3sskr, nxmr, &st.am)) != cudaSuccess ||
+      (e = up(sg->salbp, npl, &st.salbp)) != cudaSuccess || (e = up(sg->saltp, npl, &st.saltp)) != cudaSuccess)
+    return fail(e);
+  S->ap_d = st.ap;
+  S->ac_d = st.ac;
+  S->am_d = st.am;
+  const afid_stencil_t *sts[6] = {&sg->to_ref[0], &sg->to_ref[1], &sg->to_ref[2],
+                                  &sg->to_coarse[0], &sg->to_coarse[1], &sg->to_coarse[2]};
+  for (int d = 0; d < 6; ++d) {
+    int *pi = nullptr;
+    if ((e = dalloc(ctx, &pi, (size_t)sts[d]->n)) != cudaSuccess) return fail(e);
+    if ((e = cudaMemcpy(pi, sts[d]->start, sts[d]->n * sizeof(int), cudaMemcpyHostToDevice)) != cudaSuccess)
+      return fail(e);
+    st.st[d] = pi;
+    if ((e = up(sts[d]->w, (size_t)4 * sts[d]->n, &st.w[d])) != cudaSuccess) return fail(e);
+  }
+  if ((e = dalloc(ctx, &S->cn_tab, cn_tab_doubles(MR, 1))) != cudaSuccess ||  // 3 substeps x 1 matrix
+      (e = dalloc(ctx, &S->sc, 3)) != cudaSuccess || (e = dalloc(ctx, &S->red, 1)) != cudaSuccess)
+    return fail(e);
+  S->prof_blocks = sal_prof_blocks(q);
+  if ((e = dalloc(ctx, &S->partial, (size_t)S->prof_blocks * 6 * nxmr)) != cudaSuccess ||
+      (e = dalloc(ctx, &S->prof_out, (size_t)6 * nxmr)) != cudaSuccess)
+    return fail(e);
+  ctx->sal = S;
+  g.salc = sg->active_s == 1 ? S->salc : nullptr;  // AddSalBuoyancy only for an active scalar
+  g.bycs = sg->bycs;
+  return AFID_OK;
+}
+
+int afid_gpu_sal_upload(afid_ctx_t *ctx, const double *sal, int ld_x, int ld_y) {
+  if (!ctx || !ctx->sal || !sal) return AFID_E_INVALID;
+  SalCtx &S = *ctx->sal;
+  if (ld_x < S.sg.nxmr || ld_y < S.sg.nymr) return AFID_E_INVALID;
+  cudaSetDevice(ctx->dev);
+  int s;
+  if ((s = sal_copy(ctx, S.sal, S.sg.nxmr, sal, nullptr, ld_x, ld_y, true)) != AFID_OK) return s;
+  AFID_CUDA(ctx, cudaMemsetAsync(S.rusal, 0, S.relems * sizeof(double), ctx->stream));
+  if ((s = sal_interp(ctx)) != AFID_OK) return s;  // main.F90:206-208
+  return check_err_flag(ctx);
+}
+
+int afid_gpu_sal_download(afid_ctx_t *ctx, double *sal, int ld_x, int ld_y) {
+  if (!ctx || !ctx->sal || !sal) return AFID_E_INVALID;
+  SalCtx &S = *ctx->sal;
+  if (ld_x < S.sg.nxmr || ld_y < S.sg.nymr) return AFID_E_INVALID;
+  cudaSetDevice(ctx->dev);
+  int s;
+  if ((s = sal_copy(ctx, S.sal, S.sg.nxmr, nullptr, sal, ld_x, ld_y, false)) != AFID_OK) return s;
+  return check_err_flag(ctx);
+}
+
+int afid_gpu_sal_interpolate(afid_ctx_t *ctx) {
+  if (!ctx || !ctx->sal) return AFID_E_INVALID;
+  cudaSetDevice(ctx->dev);
+  int s;
+  if ((s = sal_interp(ctx)) != AFID_OK) return s;
+  return check_err_flag(ctx);
+}
+
+int afid_gpu_sal_cfl(afid_ctx_t *ctx, double *cflmr) {
+  if (!ctx || !ctx->sal || !cflmr) return AFID_E_INVALID;
+  cudaSetDevice(ctx->dev);
+  AFID_CUDA(ctx, timed(ctx, 8, [&] { return launch_sal_cfl(ctx->L, *ctx->sal); }));
+  ctx->launches += 1;
+  AFID_CUDA(ctx, cudaMemcpyAsync(ctx->host_scratch, ctx->sal->red, sizeof(double), cudaMemcpyDeviceToHost,
+                                 ctx->stream));
+  const int s = check_err_flag(ctx);
+  *cflmr = std::max(1.0e-8, ctx->host_scratch[0]);  // CalcMaxCFL.F90:50
+  return s;
+}
+
+int afid_gpu_sal_profiles(afid_ctx_t *ctx, double *out) {
+  if (!ctx || !ctx->sal || !out) return AFID_E_INVALID;
+  cudaSetDevice(ctx->dev);
+  SalCtx &S = *ctx->sal;
+  AFID_CUDA(ctx, timed(ctx, 8, [&] { return launch_sal_profiles(ctx->L, S, S.prof_out); }));
+  ctx->launches += 2;
+  AFID_CUDA(ctx, cudaMemcpyAsync(out, S.prof_out, (size_t)6 * S.sg.nxmr * sizeof(double), cudaMemcpyDeviceToHost,
+                                 ctx->stream));
+  return check_err_flag(ctx);
+}
+
+int afid_gpu_sal_download_aux(afid_ctx_t *ctx, double *vxr, double *vyr, double *vzr, int ldr_x, int ldr_y,
+                              double *salc, int ldc_x, int ldc_y) {
+  if (!ctx || !ctx->sal) return AFID_E_INVALID;
+  SalCtx &S = *ctx->sal;
+  const Geom &g = ctx->L.g;
+  if ((vxr || vyr || vzr) && (ldr_x < S.sg.nxmr + 1 || ldr_y < S.sg.nymr)) return AFID_E_INVALID;
+  if (salc && (ldc_x < g.nxm || ldc_y < g.nym)) return AFID_E_INVALID;
+  cudaSetDevice(ctx->dev);
+  int s;
+  if (vxr && (s = sal_copy(ctx, S.vxr, S.sg.nxmr + 1, nullptr, vxr, ldr_x, ldr_y, false)) != AFID_OK) return s;
+  if (vyr && (s = sal_copy(ctx, S.vyr, S.sg.nxmr, nullptr, vyr, ldr_x, ldr_y, false)) != AFID_OK) return s;
+  if (vzr && (s = sal_copy(ctx, S.vzr, S.sg.nxmr, nullptr, vzr, ldr_x, ldr_y, false)) != AFID_OK) return s;
+  if (salc)
+    for (int i = 0; i < g.nzm; ++i)
+      AFID_CUDA(ctx, cudaMemcpy2DAsync(salc + (size_t)i * ldc_x * ldc_y, (size_t)ldc_x * sizeof(double),
+                                       S.salc + (size_t)i * g.ldx * g.nym, (size_t)g.ldx * sizeof(double),
+                                       (size_t)g.nxm * sizeof(double), g.nym, cudaMemcpyDeviceToHost, ctx->stream));
+  return check_err_flag(ctx);
 }
 
 }  // extern "C"

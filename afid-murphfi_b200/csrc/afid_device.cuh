@@ -33,6 +33,10 @@ struct Geom {
   int batch;
   const struct InstScal *inst;   // [nzm] per-instance scalars (batch mode), else nullptr
   const unsigned char *active;   // [nzm] 1 = advance this instance (batch mode), else nullptr
+  // Salinity buoyancy (AddSalBuoyancy, salinity.F90:494-506): the forcing along gaxis loses
+  // bycs * salc at rows 0..nxm-1; nullptr when no active salinity is coupled.
+  const double *salc;
+  double bycs;
 };
 
 // Shared-memory stride of the chunked tridiagonal layout (row r of a 32-chunk system at

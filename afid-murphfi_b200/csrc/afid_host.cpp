@@ -1,6 +1,8 @@
 // afid_host.cpp — host-side set-up and step control around the GPU substep (include/afid_host.h).
 #include "afid_host.h"
 
+#include "afid_host_internal.h"
+
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -46,6 +48,11 @@ struct LineReader {
   }
 };
 
+}  // namespace
+
+
+namespace afid_hostd {
+
 double philox_u(uint64_t seed, uint64_t n) {
   // Philox4x32-10 (Salmon et al., SC'11): counter (n lo, n hi, 0, 0), key (seed lo, seed hi)
   uint32_t c0 = (uint32_t)n, c1 = (uint32_t)(n >> 32), c2 = 0, c3 = 0;
@@ -67,16 +74,135 @@ double philox_u(uint64_t seed, uint64_t n) {
   return (double)bits * (1.0 / 9007199254740992.0);
 }
 
-}  // namespace
+void uniform_grid(std::vector<double> &c, std::vector<double> &m, int nm, double len) {
+  c.assign(nm + 1, 0.0);
+  m.assign(nm, 0.0);
+  for (int i = 1; i <= nm + 1; ++i) c[i - 1] = len * (double)(i - 1) / (double)nm;  // grid.F90:19-21
+  for (int i = 1; i <= nm; ++i) m[i - 1] = 0.5 * (c[i - 1] + c[i]);
+}
 
-struct afid_tables {
-  afid_input_t in;
-  std::map<std::string, std::vector<double>> arr;
-  std::vector<double> tempbp, temptp;
-  afid_grid_t grid;
-  afid_params_t params;
-  double ren, pect, byct, pi, dx, dy, dz;
-};
+void second_derivative_coeff(std::vector<double> &ap3, std::vector<double> &ac3,
+                                    std::vector<double> &am3, const double *x, int n, double xlen,
+                                    int fix_up, int fix_low) {
+  // grid.F90:264-307
+  ap3.assign(n, 0.0);
+  ac3.assign(n, 0.0);
+  am3.assign(n, 0.0);
+  int k = 0;
+  double a33 = 2.0 / (x[k] + x[k + 1]);
+  ap3[k] = a33 / (x[k + 1] - x[k]);
+  am3[k] = 0.0;
+  if (x[k] == 0.0) {
+    ap3[k] = 0.0;
+    ac3[k] = 1.0;
+  } else {
+    ac3[k] = -ap3[k] - fix_low * a33 / x[k];
+  }
+  for (k = 1; k < n - 1; ++k) {
+    a33 = 2.0 / (x[k + 1] - x[k - 1]);
+    ap3[k] = a33 / (x[k + 1] - x[k]);
+    am3[k] = a33 / (x[k] - x[k - 1]);
+    ac3[k] = -ap3[k] - am3[k];
+  }
+  k = n - 1;
+  a33 = 2.0 / (2.0 * xlen - x[k] - x[k - 1]);
+  ap3[k] = 0.0;
+  am3[k] = a33 / (x[k] - x[k - 1]);
+  if (x[k] == xlen) {
+    am3[k] = 0.0;
+    ac3[k] = 1.0;
+  } else {
+    ac3[k] = -am3[k] - fix_up * a33 / (xlen - x[k]);
+  }
+}
+
+// Wall-normal faces xc[0..nxm] of grid type istr3 (grid.F90); schmidt enters ISTR3 = 3 only
+// (1 on the coarse grid, CreateGrid.F90:70; PraS on the refined grid, CreateMgrdGrid.F90:64).
+int x_grid(int istr3, int nxm, double L, double s, double pi, double schmidt, std::vector<double> &xc) {
+  const int nx = nxm + 1;
+  switch (istr3) {
+    case 0: {
+      std::vector<double> xmv;
+      uniform_grid(xc, xmv, nxm, L);
+      break;
+    }
+    case 1: {  // grid.F90:133-151
+      xc.assign(nx, 0.0);
+      for (int i = 2; i <= nxm; ++i) {
+        const double q = 2.0 * (i - 1) / nxm - 1;
+        xc[i - 1] = L / 2.0 * (s * std::pow(q, 7) + 2.0 * (i - 1) / nxm - 1) / (s + 1) + L / 2.0;
+      }
+      xc[nxm] = L;
+      break;
+    }
+    case 2:
+    case 3: {  // grid.F90:153-213 (natural boundary-layer stretching)
+      const double jb = 16.0, c_eta = 0.8, alpha = 1.5, dyw = 0.1;
+      xc.assign(nx, 0.0);
+      if (istr3 == 2) {
+        for (int j = 1; j <= nxm + 1; ++j) {
+          const double jm = j - 1;
+          xc[j - 1] = 1 / (1.0 + (jm / jb) * (jm / jb)) *
+                      (dyw * jm + std::pow(0.75 * alpha * c_eta * jm, 4.0 / 3.0) * (jm / jb) * (jm / jb));
+        }
+      } else {
+        const int nh = nxm / 2;
+        for (int j = 1; j <= nh + 1; ++j) {
+          const double jm = j - 1;
+          xc[j - 1] = 1 / (1.0 + (jm / jb) * (jm / jb)) *
+                      (dyw * jm + std::pow(0.75 * alpha * c_eta * jm / std::pow(schmidt, 0.5), 4.0 / 3.0) *
+                                      (jm / jb) * (jm / jb));
+        }
+        const double lh = 2.0 * xc[nh];
+        for (int j = 1; j <= nh; ++j) xc[nxm + 1 - j] = lh - xc[j - 1];
+      }
+      const double top = xc[nxm];
+      for (auto &v : xc) v = v / top * L;
+      break;
+    }
+    case 4: {  // grid.F90:29-53
+      const double tstr = std::tanh(s);
+      xc.assign(nx, 0.0);
+      for (int i = 2; i <= nxm + 1; ++i) {
+        const double z2 = (double)(2 * (i - 1) - nxm) / (double)nxm;
+        xc[i - 1] = 0.5 * (1 + std::tanh(s * z2) / tstr) * L;
+        if (xc[i - 1] < 0.0 || xc[i - 1] > L) return AFID_E_INVALID;
+      }
+      break;
+    }
+    case 6:
+    case 7: {  // grid.F90:55-131 (clipped Chebyshev)
+      const int nclip = (int)s;
+      const int n_ext = (istr3 == 6) ? nxm + 1 + 2 * nclip : nxm + 1 + nclip;
+      std::vector<double> etazm(n_ext), etaz(nx);
+      for (int i = 1; i <= n_ext; ++i)
+        etazm[i - 1] = (istr3 == 6) ? std::cos(pi * ((double)i - 0.5) / (double)n_ext)
+                                        : std::cos(pi * (double)i / (double)n_ext / 2.0);
+      for (int i = 1; i <= nx; ++i) etaz[i - 1] = etazm[i + nclip - 1];
+      xc.assign(nx, 0.0);
+      if (istr3 == 6) {
+        const double delet = etaz[0] - etaz[nxm];
+        for (auto &v : etaz) v = 2.0 * v / delet;
+        for (int i = 2; i <= nxm; ++i) xc[i - 1] = 0.5 * L * (1.0 - etaz[i - 1]);
+      } else {
+        const double delet = etaz[0];
+        for (auto &v : etaz) v = v / delet;
+        for (int i = 2; i <= nxm; ++i) xc[i - 1] = L * (1.0 - etaz[i - 1]);
+      }
+      xc[nxm] = L;
+      break;
+    }
+    default:
+      return AFID_E_INVALID;
+  }
+  return AFID_OK;
+}
+
+}  // namespace afid_hostd
+
+using afid_hostd::philox_u;
+using afid_hostd::second_derivative_coeff;
+using afid_hostd::uniform_grid;
 
 extern "C" {
 
@@ -141,48 +267,6 @@ int afid_read_bou_in(const char *path, afid_input_t *out) {
   return afid_parse_bou_in(s.c_str(), out);
 }
 
-static void uniform_grid(std::vector<double> &c, std::vector<double> &m, int nm, double len) {
-  c.assign(nm + 1, 0.0);
-  m.assign(nm, 0.0);
-  for (int i = 1; i <= nm + 1; ++i) c[i - 1] = len * (double)(i - 1) / (double)nm;  // grid.F90:19-21
-  for (int i = 1; i <= nm; ++i) m[i - 1] = 0.5 * (c[i - 1] + c[i]);
-}
-
-static void second_derivative_coeff(std::vector<double> &ap3, std::vector<double> &ac3,
-                                    std::vector<double> &am3, const double *x, int n, double xlen,
-                                    int fix_up, int fix_low) {
-  // grid.F90:264-307
-  ap3.assign(n, 0.0);
-  ac3.assign(n, 0.0);
-  am3.assign(n, 0.0);
-  int k = 0;
-  double a33 = 2.0 / (x[k] + x[k + 1]);
-  ap3[k] = a33 / (x[k + 1] - x[k]);
-  am3[k] = 0.0;
-  if (x[k] == 0.0) {
-    ap3[k] = 0.0;
-    ac3[k] = 1.0;
-  } else {
-    ac3[k] = -ap3[k] - fix_low * a33 / x[k];
-  }
-  for (k = 1; k < n - 1; ++k) {
-    a33 = 2.0 / (x[k + 1] - x[k - 1]);
-    ap3[k] = a33 / (x[k + 1] - x[k]);
-    am3[k] = a33 / (x[k] - x[k - 1]);
-    ac3[k] = -ap3[k] - am3[k];
-  }
-  k = n - 1;
-  a33 = 2.0 / (2.0 * xlen - x[k] - x[k - 1]);
-  ap3[k] = 0.0;
-  am3[k] = a33 / (x[k] - x[k - 1]);
-  if (x[k] == xlen) {
-    am3[k] = 0.0;
-    ac3[k] = 1.0;
-  } else {
-    ac3[k] = -am3[k] - fix_up * a33 / (xlen - x[k]);
-  }
-}
-
 int afid_tables_create(const afid_input_t *in, int precision, afid_tables_t **out) {
   if (!in || !out) return AFID_E_INVALID;
   *out = nullptr;
@@ -204,81 +288,12 @@ int afid_tables_create(const afid_input_t *in, int precision, afid_tables_t **ou
   t->pi = 2.0 * std::asin(1.0);
   const double pi = t->pi;
 
-  std::vector<double> zc, zm, yc, ym, xc, xmv;
+  std::vector<double> zc, zm, yc, ym, xc;
   uniform_grid(zc, zm, nzm, in->zlen);
   uniform_grid(yc, ym, nym, in->ylen);
-  const double L = in->alx3, s = in->str3;
-  switch (in->istr3) {
-    case 0: uniform_grid(xc, xmv, nxm, L); break;
-    case 1: {  // grid.F90:133-151
-      xc.assign(nx, 0.0);
-      for (int i = 2; i <= nxm; ++i) {
-        const double q = 2.0 * (i - 1) / nxm - 1;
-        xc[i - 1] = L / 2.0 * (s * std::pow(q, 7) + 2.0 * (i - 1) / nxm - 1) / (s + 1) + L / 2.0;
-      }
-      xc[nxm] = L;
-      break;
-    }
-    case 2:
-    case 3: {  // grid.F90:153-213 (natural boundary-layer stretching)
-      const double jb = 16.0, c_eta = 0.8, alpha = 1.5, dyw = 0.1;
-      xc.assign(nx, 0.0);
-      if (in->istr3 == 2) {
-        for (int j = 1; j <= nxm + 1; ++j) {
-          const double jm = j - 1;
-          xc[j - 1] = 1 / (1.0 + (jm / jb) * (jm / jb)) *
-                      (dyw * jm + std::pow(0.75 * alpha * c_eta * jm, 4.0 / 3.0) * (jm / jb) * (jm / jb));
-        }
-      } else {
-        const int nh = nxm / 2;
-        for (int j = 1; j <= nh + 1; ++j) {
-          const double jm = j - 1;
-          xc[j - 1] = 1 / (1.0 + (jm / jb) * (jm / jb)) *
-                      (dyw * jm + std::pow(0.75 * alpha * c_eta * jm / std::pow(1.0, 0.5), 4.0 / 3.0) *
-                                      (jm / jb) * (jm / jb));
-        }
-        const double lh = 2.0 * xc[nh];
-        for (int j = 1; j <= nh; ++j) xc[nxm + 1 - j] = lh - xc[j - 1];
-      }
-      const double top = xc[nxm];
-      for (auto &v : xc) v = v / top * L;
-      break;
-    }
-    case 4: {  // grid.F90:29-53
-      const double tstr = std::tanh(s);
-      xc.assign(nx, 0.0);
-      for (int i = 2; i <= nxm + 1; ++i) {
-        const double z2 = (double)(2 * (i - 1) - nxm) / (double)nxm;
-        xc[i - 1] = 0.5 * (1 + std::tanh(s * z2) / tstr) * L;
-        if (xc[i - 1] < 0.0 || xc[i - 1] > L) { delete t; return AFID_E_INVALID; }
-      }
-      break;
-    }
-    case 6:
-    case 7: {  // grid.F90:55-131 (clipped Chebyshev)
-      const int nclip = (int)s;
-      const int n_ext = (in->istr3 == 6) ? nxm + 1 + 2 * nclip : nxm + 1 + nclip;
-      std::vector<double> etazm(n_ext), etaz(nx);
-      for (int i = 1; i <= n_ext; ++i)
-        etazm[i - 1] = (in->istr3 == 6) ? std::cos(pi * ((double)i - 0.5) / (double)n_ext)
-                                        : std::cos(pi * (double)i / (double)n_ext / 2.0);
-      for (int i = 1; i <= nx; ++i) etaz[i - 1] = etazm[i + nclip - 1];
-      xc.assign(nx, 0.0);
-      if (in->istr3 == 6) {
-        const double delet = etaz[0] - etaz[nxm];
-        for (auto &v : etaz) v = 2.0 * v / delet;
-        for (int i = 2; i <= nxm; ++i) xc[i - 1] = 0.5 * L * (1.0 - etaz[i - 1]);
-      } else {
-        const double delet = etaz[0];
-        for (auto &v : etaz) v = v / delet;
-        for (int i = 2; i <= nxm; ++i) xc[i - 1] = L * (1.0 - etaz[i - 1]);
-      }
-      xc[nxm] = L;
-      break;
-    }
-    default:
-      delete t;
-      return AFID_E_INVALID;  // ISTR3=5 (scallop, channel-flow specific) is not on this path
+  if (afid_hostd::x_grid(in->istr3, nxm, in->alx3, in->str3, pi, 1.0, xc) != AFID_OK) {
+    delete t;
+    return AFID_E_INVALID;  // ISTR3=5 (scallop, channel-flow specific) is not on this path
   }
   // CreateGrid.F90:100-138
   const double dx = (double)nxm / in->alx3, dy = (double)nym / in->ylen, dz = (double)nzm / in->zlen;

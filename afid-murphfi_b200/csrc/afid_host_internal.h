@@ -1,0 +1,34 @@
+// afid_host_internal.h — host-side pieces shared by afid_host.cpp and afid_mgrd.cpp.
+#pragma once
+#include <stdint.h>
+
+#include <map>
+#include <string>
+#include <vector>
+
+#include "afid_host.h"
+
+// The tables behind afid_tables_t (include/afid_host.h).
+struct afid_tables {
+  afid_input_t in;
+  std::map<std::string, std::vector<double>> arr;
+  std::vector<double> tempbp, temptp;
+  afid_grid_t grid;
+  afid_params_t params;
+  double ren, pect, byct, pi, dx, dy, dz;
+};
+
+namespace afid_hostd {
+
+// Philox4x32-10 uniform in [0, 1) for counter n and key seed.
+double philox_u(uint64_t seed, uint64_t n);
+// grid.F90:12-27: faces c[0..nm] and centres m[0..nm-1] of a uniform grid of length len.
+void uniform_grid(std::vector<double> &c, std::vector<double> &m, int nm, double len);
+// grid.F90:264-307: second-derivative coefficients at the n points x with Dirichlet (fix = 1)
+// or Neumann (fix = 0) walls.
+void second_derivative_coeff(std::vector<double> &ap3, std::vector<double> &ac3, std::vector<double> &am3,
+                             const double *x, int n, double xlen, int fix_up, int fix_low);
+// Wall-normal faces of grid type istr3 (0, 1, 2, 3, 4, 6, 7); AFID_E_INVALID otherwise.
+int x_grid(int istr3, int nxm, double L, double s, double pi, double schmidt, std::vector<double> &xc);
+
+}  // namespace afid_hostd

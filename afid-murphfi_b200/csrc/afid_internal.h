@@ -39,6 +39,7 @@ struct SubstepBuffers {
 };
 
 struct CnInputs {
+  int nmat = 3;  // matrices per substep: vx, vy/vz, temp (3), or one temperature-like matrix (1)
   const double *am[3], *ac[3], *ap[3];
   int off[3], n[3];
   double al[3], ga[3], ro[3];
@@ -73,6 +74,55 @@ cudaError_t launch_max_reduce(const LaunchCtx &L, bool div, const double *vx, co
 cudaError_t launch_globals(const LaunchCtx &L, const double *vx, const double *vy,
                            const double *vz, const double *temp, double *partial, double *out3);
 int globals_partial_blocks(const Geom &g);
+
+// ---- multi-resolution salinity (afid_salinity.cu) ----------------------------------------
+struct SalGeom {
+  int nxmr, nymr, nzmr, ldr;       // refined cells and x stride (>= nxmr + 1, multiple of 8)
+  int MR;                          // rows per lane of the refined CN solve (32 MR >= nxmr)
+  double dxr, dyr, dzr;
+  double udyr, udzr;               // 0.5 dyr, 0.5 dzr        (ExplicitSalinity advection)
+  double udyrq, udzrq;             // dyr^2/pecs, dzr^2/pecs  (ExplicitSalinity diffusion)
+  double lya, lza;                 // 1/dyr, 1/dzr            (InterpVelMgrd integration)
+  double pecs;
+  int sfixs, sfixn;
+};
+struct SalTables {
+  const double *lxa;               // [nxmr] xcr(k+1) - xcr(k)
+  const double *udx3mr, *tdxr;     // [nxmr] dxr/d3xcr, 0.5 dxr/g3rmr
+  const double *ap, *ac, *am;      // [nxmr] ap3sskr, ac3sskr, am3sskr
+  const double *salbp, *saltp;     // [nymr*nzmr]
+  const int *st[6];                // to_ref x, y, z; to_coarse x, y, z: first source row
+  const double *w[6];              //   and the 4 weights of every target
+};
+struct SalCtx {
+  SalGeom sg{};
+  SalTables st{};
+  int active_s = 0;
+  double bycs = 0.0;
+  size_t relems = 0;               // elements of one refined field
+  double *sal = nullptr, *sal_o = nullptr, *rusal = nullptr;
+  double *vxr = nullptr, *vyr = nullptr, *vzr = nullptr;
+  double *gyr = nullptr, *gzr = nullptr;         // refined y/z velocity gradients (scratch)
+  double *gx = nullptr, *gy = nullptr, *gz = nullptr, *salc = nullptr;  // coarse
+  double *cn_tab = nullptr;
+  StepCoef *sc = nullptr;
+  double *partial = nullptr, *prof_out = nullptr;
+  int prof_blocks = 0;
+  unsigned long long *red = nullptr;
+  int *err = nullptr;                            // the context's error word
+  const double *am_d = nullptr, *ac_d = nullptr, *ap_d = nullptr;
+};
+// ExplicitSalinity + ImplicitSalinity + SolveImpEqnUpdate_Sal: sal -> sal_o, rusal in place.
+cudaError_t launch_sal_step(const LaunchCtx &L, const SalCtx &S, int ns);
+// InterpVelMgrd + InterpSalMultigrid from the state (vx, vy, vz) and S.sal.
+cudaError_t launch_sal_interp(const LaunchCtx &L, const SalCtx &S, const double *vx, const double *vy,
+                              const double *vz);
+cudaError_t launch_sal_cfl(const LaunchCtx &L, const SalCtx &S);
+// Six profiles (Sbar, Srms, vxS, vyS, vzS, chiS) into out[6 * nxmr] (device).
+cudaError_t launch_sal_profiles(const LaunchCtx &L, const SalCtx &S, double *out);
+int sal_prof_blocks(const SalGeom &sg);
+size_t sal_step_smem_bytes(int MR, bool two_d);
+constexpr int kSalLaunchesInterp = 5;
 cudaError_t launch_repack(cudaStream_t st, const double *src, int sld, double *dst, int dld, int width,
                           size_t rows);
 
@@ -125,6 +175,8 @@ struct afid_ctx {
   int ninst = 0;
   afid::InstScal *inst_dev = nullptr;
   unsigned char *active_dev = nullptr;
+  // multi-resolution salinity (include/afid_salinity.h), nullptr when off
+  afid::SalCtx *sal = nullptr;
 };
 
 namespace afid {

@@ -75,7 +75,7 @@ template <typename TE> __device__ __forceinline__ TE cv(double v) { return (TE)v
 template <typename TE, bool TWO_D>
 __device__ __forceinline__ double rhs_vx(const Geom &g, const Tables &t, const StepCoef &sc, int k,
                                          const ColV &X, const ColV &Y, const ColV &Z, const ColV &T,
-                                         const ColV &P, double ru, TE &qout) {
+                                         const ColV &P, double ru, TE &qout, double sb) {
   const int km = k - 1, kp = k + 1;
   const TE udy = (TE)(g.dy * 0.25), udz = (TE)(g.dz * 0.25);
   const TE udyq = (TE)g.udyq_re, udzq = (TE)g.udzq_re;
@@ -101,6 +101,7 @@ __device__ __forceinline__ double rhs_vx(const Geom &g, const Tables &t, const S
   if (g.gaxis == 1) {
     const TE tempit = (TE)g.active_t * (TE)0.5 * (cv<TE>(T.c[k]) + cv<TE>(T.c[km]));
     qcap = qcap + (TE)g.byct * tempit;
+    if (g.salc) qcap = qcap - (TE)sb;  // AddSalBuoyancy(qcap)
   }
   const double alre = sc.alre;
   const double udx3 = sc.al * __ldg(t.udx3c + k);
@@ -114,7 +115,8 @@ __device__ __forceinline__ double rhs_vx(const Geom &g, const Tables &t, const S
 template <typename TE, bool TWO_D>
 __device__ __forceinline__ double rhs_vy(const Geom &g, const Tables &t, const StepCoef &sc, int k,
                                          const ColV &X, const ColV &Y, const ColV &Z, const ColV &T,
-                                         const ColV &P, double zd, double pjm, double ru, TE &qout) {
+                                         const ColV &P, double zd, double pjm, double ru, TE &qout,
+                                         double sb) {
   const int kmm = (k == 0) ? 0 : k - 1;
   const int kpp = (k == g.nxm - 1) ? k : k + 1;
   const int kp = k + 1;
@@ -140,6 +142,7 @@ __device__ __forceinline__ double rhs_vy(const Geom &g, const Tables &t, const S
   if (g.gaxis == 2) {
     const TE tempit = (TE)g.active_t * (TE)0.5 * (cv<TE>(T.c[k]) + cv<TE>(T.jm[k]));
     dph = dph + (TE)g.byct * tempit;
+    if (g.salc) dph = dph - (TE)sb;  // AddSalBuoyancy(dph)
   }
   const double alre = sc.alre;
   const double udyp = g.dy * sc.al;
@@ -161,7 +164,8 @@ __device__ __forceinline__ double rhs_vy(const Geom &g, const Tables &t, const S
 template <typename TE, bool TWO_D>
 __device__ __forceinline__ double rhs_vz(const Geom &g, const Tables &t, const StepCoef &sc, int k,
                                          const ColV &X, const ColV &Y, const ColV &Z, const ColV &T,
-                                         const ColV &P, double yd, double pim, double ru, TE &qout) {
+                                         const ColV &P, double yd, double pim, double ru, TE &qout,
+                                         double sb) {
   const int kmm = (k == 0) ? 0 : k - 1;
   const int kpp = (k == g.nxm - 1) ? k : k + 1;
   const int kp = k + 1;
@@ -187,6 +191,7 @@ __device__ __forceinline__ double rhs_vz(const Geom &g, const Tables &t, const S
   if (g.gaxis == 3) {
     const TE tempit = (TE)g.active_t * (TE)0.5 * (cv<TE>(T.c[k]) + cv<TE>(T.im[k]));
     dq = dq + (TE)g.byct * tempit;
+    if (g.salc) dq = dq - (TE)sb;  // AddSalBuoyancy(dq)
   }
   const double alre = sc.alre;
   const double amm = __ldg(t.am3sk + k), acc = __ldg(t.ac3sk + k), app = __ldg(t.ap3sk + k);
@@ -405,10 +410,12 @@ __global__ void __launch_bounds__(TPC, k1_min_blocks<CAP, TPC>())
       const double zd = TWO_D ? Z.jm[k] : vv[p][0];
       const double yd = TWO_D ? Y.jp[k] : vv[p][1];
       const double pim = TWO_D ? P.c[k] : vv[p][3];
+      // salinity buoyancy bycs * salc at this row, for the gravity component
+      const double sb = g.salc ? g.bycs * __ldg(g.salc + c0 + k) : 0.0;
       // all four right-hand sides from the staged columns before anything is stored
-      rr[p][0] = (k >= 1) ? rhs_vx<TE, TWO_D>(g, t, sc, k, X, Y, Z, T, P, u0, q0) * __ldg(TX + k - 1) : 0.0;
-      rr[p][1] = rhs_vy<TE, TWO_D>(g, t, sc, k, X, Y, Z, T, P, zd, vv[p][2], u1, q1) * __ldg(TY + k);
-      rr[p][2] = rhs_vz<TE, TWO_D>(g, t, sc, k, X, Y, Z, T, P, yd, pim, u2, q2) * __ldg(TY + k);
+      rr[p][0] = (k >= 1) ? rhs_vx<TE, TWO_D>(g, t, sc, k, X, Y, Z, T, P, u0, q0, sb) * __ldg(TX + k - 1) : 0.0;
+      rr[p][1] = rhs_vy<TE, TWO_D>(g, t, sc, k, X, Y, Z, T, P, zd, vv[p][2], u1, q1, sb) * __ldg(TY + k);
+      rr[p][2] = rhs_vz<TE, TWO_D>(g, t, sc, k, X, Y, Z, T, P, yd, pim, u2, q2, sb) * __ldg(TY + k);
       rr[p][3] = rhs_temp<TE, TWO_D>(g, t, sc, k, X, Y, Z, T, tbp, ttp, u3, q3) * __ldg(TT + k);
       if (k >= 1) rux[c0 + k] = q0;
       ruy[c0 + k] = q1;

@@ -52,6 +52,7 @@ struct CnBuildArgs {
   double al[3], ga[3], ro[3];
   double dt, beta, pect, ren;
   int ns0, nsub;       // substeps ns0 .. ns0+nsub-1 are built
+  int nmat;            // matrices per substep (tables at (slot * nmat + m))
   // batch mode: one table set per instance, dt from dt_dev[instance] (beta = dt/ren/2),
   // ren/pect from inst[instance]; idle instances are skipped
   const double *dt_dev;
@@ -62,9 +63,9 @@ struct CnBuildArgs {
 __global__ void k_cn_tables(CnBuildArgs args, int M, double *__restrict__ tab,
                             StepCoef *__restrict__ sc) {
   const int lane = threadIdx.x;
-  const int m = blockIdx.x % 3;
-  const int sub = (blockIdx.x / 3) % args.nsub;
-  const int b = blockIdx.x / (3 * args.nsub);  // instance (batch mode), else 0
+  const int m = blockIdx.x % args.nmat;
+  const int sub = (blockIdx.x / args.nmat) % args.nsub;
+  const int b = blockIdx.x / (args.nmat * args.nsub);  // instance (batch mode), else 0
   const int ns = args.ns0 + sub;
   const double al = args.al[sub];
   double dt = args.dt, beta = args.beta, ren = args.ren, pect = args.pect;
@@ -90,7 +91,7 @@ __global__ void k_cn_tables(CnBuildArgs args, int M, double *__restrict__ tab,
   }
   const CnMatrixDesc d = args.mat[m];
   const double betadx = d.temperature ? 0.5 * al * dt / pect : beta * al;
-  double *T = tab + (size_t)(slot * 3 + m) * cn_table_size(M);
+  double *T = tab + (size_t)(slot * args.nmat + m) * cn_table_size(M);
   double *Tsc = T, *Ta = T + 32 * M, *Tinv = T + 64 * M, *Tcp = T + 96 * M, *Tv = T + 128 * M,
          *Tw = T + 160 * M, *Tl = T + 192 * M;
   const int n = d.n;
@@ -898,8 +899,9 @@ cudaError_t launch_cn_tables(const LaunchCtx &L, const CnInputs &in) {
     a.mat[m].ap = in.ap[m];
     a.mat[m].off = in.off[m];
     a.mat[m].n = in.n[m];
-    a.mat[m].temperature = (m == 2);
+    a.mat[m].temperature = (in.nmat == 3) ? (m == 2) : 1;
   }
+  a.nmat = in.nmat;
   for (int s = 0; s < 3; ++s) {
     a.al[s] = in.al[s];
     a.ga[s] = in.ga[s];
@@ -915,7 +917,7 @@ cudaError_t launch_cn_tables(const LaunchCtx &L, const CnInputs &in) {
   a.inst = in.inst;
   a.active = in.active;
   const int nb = in.dt_dev ? in.ninst : 1;
-  k_cn_tables<<<3 * in.nsub * nb, 32, 0, L.stream>>>(a, in.M, in.tab, in.sc);
+  k_cn_tables<<<in.nmat * in.nsub * nb, 32, 0, L.stream>>>(a, in.M, in.tab, in.sc);
   return cudaGetLastError();
 }
 

@@ -1,0 +1,603 @@
+// afid_salinity.cu — the multi-resolution salinity scalar on the device (include/afid_salinity.h).
+//
+// Per substep (TimeMarcher.F90:50-63, 95, 138-144):
+//   k_sal_step       ExplicitSalinity + ImplicitSalinity + SolveImpEqnUpdate_Sal fused per refined
+//                    x-column (salinity.F90:268-453): staged columns, RHS, CN solve, update
+//   (K1 subtracts bycs * salc from the forcing along gAxis: AddSalBuoyancy, salinity.F90:494-506)
+// after the projection:
+//   k_sal_grad       dvx/dx, dvy/dy, dvz/dz at the coarse cell centres (InterpVelMgrd.F90:33-158)
+//   k_sal_to_ref     the three gradients interpolated to the refined cell centres
+//                    (interpolate_xyz_to_refined, HermiteInterpolations.F90:168-200); vxr is
+//                    integrated along the column in the same block (InterpVelMgrd.F90:49-57)
+//   k_sal_scan_y     first-guess plane at y = 0 (vy interpolated in x-z) + integration along y
+//   k_sal_scan_z     first-guess plane at z = 0 (vz in x-y, when nzm > 1) + integration along z
+//   k_sal_to_coarse  salc from the wall-extended refined salinity (InterpSalMultigrid,
+//                    salinity.F90:455-492, per-target form of either coarse interpolation)
+// Diagnostics: k_sal_cfl (CalcMaxCFL.F90:48-65), k_sal_prof_* (CalcSalStats, salinity.F90:508-667).
+//
+// Layout: refined fields are x-fastest like the coarse ones, (k, j, i) at k + ldr (j + nymr i),
+// ldr = round_up(nxmr + 1, 8); vxr uses rows 0..nxmr (nxr faces), the others rows 0..nxmr-1.
+// Every stencil is a per-target table (first source row + 4 weights); along x the sources are
+// wall-extended columns whose ghost rows are formed on the fly.
+#include <cuda_runtime.h>
+
+#include "afid_device.cuh"
+#include "afid_internal.h"
+#include "afid_k1.cuh"
+
+namespace afid {
+
+namespace {
+
+__device__ __forceinline__ int wrapmod(int a, int n) {
+  a %= n;
+  return a < 0 ? a + n : a;
+}
+
+// Wall-extended coarse column (InterpVelMgrd.F90:40-41, 75-76, 107-108): row -1 is
+// (1 - 2 inslwS) row 0, row nxm is (1 - 2 inslwN) row nxm-1, rows -2 and nxm+1 are zero.
+__device__ __forceinline__ double coarse_ext(const double *__restrict__ col, int r, int nxm, double fs, double fn) {
+  if (r >= 0 && r < nxm) return __ldg(col + r);
+  if (r == -1) return fs * __ldg(col);
+  if (r == nxm) return fn * __ldg(col + nxm - 1);
+  return 0.0;
+}
+
+// Wall-extended refined salinity (salinity.F90:462-481): row -1 is 2 salbp - sal(0) with SfixS
+// (else sal(0)), row nxmr is 2 saltp - sal(nxmr-1) with SfixN (else sal(nxmr-1)); -2 and nxmr+1
+// are zero.
+__device__ __forceinline__ double sal_ext(const double *__restrict__ col, int r, int n, int sfixs, int sfixn,
+                                          double bp, double tp) {
+  if (r >= 0 && r < n) return __ldg(col + r);
+  if (r == -1) return sfixs ? 2.0 * bp - __ldg(col) : __ldg(col);
+  if (r == n) return sfixn ? 2.0 * tp - __ldg(col + n - 1) : __ldg(col + n - 1);
+  return 0.0;
+}
+
+// ------------------------------------------------------------------------------------------
+// k_sal_grad: one thread per coarse cell (k < nxm) of the padded field.
+// ------------------------------------------------------------------------------------------
+__global__ void __launch_bounds__(256)
+    k_sal_grad(Geom g, Tables t, const double *__restrict__ vx, const double *__restrict__ vy,
+               const double *__restrict__ vz, double *__restrict__ gx, double *__restrict__ gy,
+               double *__restrict__ gz) {
+  const size_t n = (size_t)g.ldx * g.nym * g.nzm;
+  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
+    const int k = (int)(e % g.ldx);
+    if (k >= g.nxm) continue;
+    const size_t col = e / g.ldx;
+    const int j = (int)(col % g.nym), i = (int)(col / g.nym);
+    const size_t ojp = col_off(g, wrap_inc(j, g.nym), i) + k, oip = col_off(g, j, wrap_inc(i, g.nzm)) + k;
+    gx[e] = (vx[e + 1] - vx[e]) * __ldg(t.udx3m + k);  // InterpVelMgrd.F90:37
+    gy[e] = (vy[ojp] - vy[e]) * g.dy;                   // :72
+    gz[e] = (vz[oip] - vz[e]) * g.dz;                   // :156
+  }
+}
+
+// ------------------------------------------------------------------------------------------
+// k_sal_to_ref: block per refined column (jr, ir).  The y-z contraction of the 16 coarse
+// columns around it (z first, then y: qv2 / qv1 of HermiteInterpolations.F90:186-192) gives one
+// wall-extended coarse column per gradient in shared memory; the x contraction then yields the
+// refined gradients.  dvx/dx is integrated along the column (vxr(1) = 0), dvy/dy and dvz/dz go
+// to scratch for the y and z integrations.
+// ------------------------------------------------------------------------------------------
+constexpr int kToRefThreads = 256;
+
+__global__ void __launch_bounds__(kToRefThreads)
+    k_sal_to_ref(Geom g, SalGeom sg, SalTables st, const double *__restrict__ gx, const double *__restrict__ gy,
+                 const double *__restrict__ gz, double *__restrict__ vxr, double *__restrict__ gyr,
+                 double *__restrict__ gzr) {
+  extern __shared__ __align__(16) double sm_to_ref[];
+  const int nxm = g.nxm, L = nxm + 4;  // extended rows -2 .. nxm+1 at 0 .. nxm+3
+  double *qx = sm_to_ref, *qy = qx + L, *qz = qy + L, *d = qz + L;
+  __shared__ double warp_tot[kToRefThreads / 32];
+  const int tid = threadIdx.x;
+  const int jr = blockIdx.x % sg.nymr, ir = blockIdx.x / sg.nymr;
+  const int sy = __ldg(st.st[1] + jr), sz = __ldg(st.st[2] + ir);
+  double wy[4], wz[4];
+  size_t co[4][4];  // coarse column offsets [b][c]
+#pragma unroll
+  for (int a = 0; a < 4; ++a) {
+    wy[a] = __ldg(st.w[1] + 4 * jr + a);
+    wz[a] = __ldg(st.w[2] + 4 * ir + a);
+  }
+#pragma unroll
+  for (int b = 0; b < 4; ++b)
+#pragma unroll
+    for (int c = 0; c < 4; ++c) co[b][c] = col_off(g, wrapmod(sy + b, g.nym), wrapmod(sz + c, g.nzm));
+  for (int r = tid; r < nxm; r += kToRefThreads) {
+    double q[3];
+    const double *src[3] = {gx, gy, gz};
+#pragma unroll
+    for (int f = 0; f < 3; ++f) {
+      double q2[4];
+#pragma unroll
+      for (int b = 0; b < 4; ++b)
+        q2[b] = __ldg(src[f] + co[b][0] + r) * wz[0] + __ldg(src[f] + co[b][1] + r) * wz[1] +
+                __ldg(src[f] + co[b][2] + r) * wz[2] + __ldg(src[f] + co[b][3] + r) * wz[3];
+      q[f] = q2[0] * wy[0] + q2[1] * wy[1] + q2[2] * wy[2] + q2[3] * wy[3];
+    }
+    qx[r + 2] = q[0];
+    qy[r + 2] = q[1];
+    qz[r + 2] = q[2];
+  }
+  __syncthreads();
+  if (tid < 3) {
+    // ghost rows: the wall rule commutes with the (linear) y-z contraction
+    double *q = tid == 0 ? qx : (tid == 1 ? qy : qz);
+    q[0] = 0.0;
+    q[1] = (double)(1 - 2 * g.inslws) * q[2];
+    q[nxm + 2] = (double)(1 - 2 * g.inslwn) * q[nxm + 1];
+    q[nxm + 3] = 0.0;
+  }
+  __syncthreads();
+  const size_t roff = ((size_t)jr + (size_t)sg.nymr * ir) * sg.ldr;
+  const int nxmr = sg.nxmr;
+  for (int kr = tid; kr < nxmr; kr += kToRefThreads) {
+    const int p = __ldg(st.st[0] + kr) + 2;
+    const double w0 = __ldg(st.w[0] + 4 * kr), w1 = __ldg(st.w[0] + 4 * kr + 1), w2 = __ldg(st.w[0] + 4 * kr + 2),
+                 w3 = __ldg(st.w[0] + 4 * kr + 3);
+    const double vxg = qx[p] * w0 + qx[p + 1] * w1 + qx[p + 2] * w2 + qx[p + 3] * w3;
+    gyr[roff + kr] = qy[p] * w0 + qy[p + 1] * w1 + qy[p + 2] * w2 + qy[p + 3] * w3;
+    gzr[roff + kr] = qz[p] * w0 + qz[p + 1] * w1 + qz[p + 2] * w2 + qz[p + 3] * w3;
+    d[kr] = vxg * __ldg(st.lxa + kr);  // InterpVelMgrd.F90:53-54
+  }
+  __syncthreads();
+  // vxr(kr+1) = sum_{q <= kr} d(q): each thread scans a contiguous chunk, the chunk totals are
+  // scanned across the block
+  const int chunk = (nxmr + kToRefThreads - 1) / kToRefThreads;
+  const int lo = tid * chunk, hi = min(lo + chunk, nxmr);
+  double tot = 0.0;
+  for (int q = lo; q < hi; ++q) tot += d[q];
+  const int lane = tid & 31, warp = tid >> 5;
+  double incl = tot;
+#pragma unroll
+  for (int h = 1; h < 32; h <<= 1) {
+    const double o = __shfl_up_sync(0xffffffffu, incl, h);
+    if (lane >= h) incl += o;
+  }
+  if (lane == 31) warp_tot[warp] = incl;
+  __syncthreads();
+  double base = incl - tot;
+  for (int w = 0; w < warp; ++w) base += warp_tot[w];
+  double run = base;
+  if (tid == 0) vxr[roff] = 0.0;  // InterpVelMgrd.F90:48
+  for (int q = lo; q < hi; ++q) {
+    run += d[q];
+    vxr[roff + q + 1] = run;
+  }
+}
+
+// ------------------------------------------------------------------------------------------
+// k_sal_scan_y: thread per (kr, ir).  vyr at the plane y = 0 (jcr0 = 1) is vy(:, 1, :)
+// interpolated in x-z (InterpVelMgrd.F90:99-116: z contracted first, then x); then
+// vyr(jr+1) = vyr(jr) + dvy/dy(jr) / dyr (:124-131).  One rank: the MPI_SCAN correction is zero.
+// ------------------------------------------------------------------------------------------
+__global__ void __launch_bounds__(128)
+    k_sal_scan_y(Geom g, SalGeom sg, SalTables st, const double *__restrict__ vy, const double *__restrict__ gyr,
+                 double *__restrict__ vyr) {
+  const int kr = blockIdx.x * blockDim.x + threadIdx.x, ir = blockIdx.y;
+  if (kr >= sg.nxmr) return;
+  const int sx = __ldg(st.st[0] + kr), sz = __ldg(st.st[2] + ir);
+  const double fs = (double)(1 - 2 * g.inslws), fn = (double)(1 - 2 * g.inslwn);
+  double v = 0.0;
+#pragma unroll
+  for (int a = 0; a < 4; ++a) {
+    double q1 = 0.0;
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      const double *col = vy + col_off(g, 0, wrapmod(sz + c, g.nzm));
+      const double e = coarse_ext(col, sx + a, g.nxm, fs, fn) * __ldg(st.w[2] + 4 * ir + c);
+      q1 = (c == 0) ? e : q1 + e;
+    }
+    const double e = q1 * __ldg(st.w[0] + 4 * kr + a);
+    v = (a == 0) ? e : v + e;
+  }
+  size_t o = (size_t)sg.nymr * ir * sg.ldr + kr;
+  vyr[o] = v;
+  for (int jr = 0; jr + 1 < sg.nymr; ++jr) {
+    v = v + __ldg(gyr + o) * sg.lya;
+    o += sg.ldr;
+    vyr[o] = v;
+  }
+}
+
+// ------------------------------------------------------------------------------------------
+// k_sal_scan_z: thread per (kr, jr).  vzr at the plane z = 0 (icr0 = 1) is vz(:, :, 1)
+// interpolated in x-y (InterpVelMgrd.F90:181-198: y first, then x), only when nzm > 1 (the
+// reference's `ic0 < xend(3)`); then vzr(ir+1) = vzr(ir) + dvz/dz(ir) / dzr (:206-213).
+// ------------------------------------------------------------------------------------------
+__global__ void __launch_bounds__(128)
+    k_sal_scan_z(Geom g, SalGeom sg, SalTables st, const double *__restrict__ vz, const double *__restrict__ gzr,
+                 double *__restrict__ vzr) {
+  const int kr = blockIdx.x * blockDim.x + threadIdx.x, jr = blockIdx.y;
+  if (kr >= sg.nxmr) return;
+  double v = 0.0;
+  if (g.nzm > 1) {
+    const int sx = __ldg(st.st[0] + kr), sy = __ldg(st.st[1] + jr);
+    const double fs = (double)(1 - 2 * g.inslws), fn = (double)(1 - 2 * g.inslwn);
+#pragma unroll
+    for (int a = 0; a < 4; ++a) {
+      double q1 = 0.0;
+#pragma unroll
+      for (int b = 0; b < 4; ++b) {
+        const double *col = vz + col_off(g, wrapmod(sy + b, g.nym), 0);
+        const double e = coarse_ext(col, sx + a, g.nxm, fs, fn) * __ldg(st.w[1] + 4 * jr + b);
+        q1 = (b == 0) ? e : q1 + e;
+      }
+      const double e = q1 * __ldg(st.w[0] + 4 * kr + a);
+      v = (a == 0) ? e : v + e;
+    }
+  }
+  const size_t plane = (size_t)sg.nymr * sg.ldr;
+  size_t o = (size_t)jr * sg.ldr + kr;
+  vzr[o] = v;
+  for (int ir = 0; ir + 1 < sg.nzmr; ++ir) {
+    v = v + __ldg(gzr + o) * sg.lza;
+    o += plane;
+    vzr[o] = v;
+  }
+}
+
+// ------------------------------------------------------------------------------------------
+// k_sal_to_coarse: thread per coarse point (k < nxm) of the padded field: salc =
+// sum_a wx_a sum_b wy_b sum_c wz_c S_ext (z, then y, then x as qv2 / qv1 of
+// HermiteInterpolations.F90:270-284).
+// ------------------------------------------------------------------------------------------
+__global__ void __launch_bounds__(256)
+    k_sal_to_coarse(Geom g, SalGeom sg, SalTables st, const double *__restrict__ sal, double *__restrict__ salc) {
+  const size_t n = (size_t)g.ldx * g.nym * g.nzm;
+  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
+    const int k = (int)(e % g.ldx);
+    if (k >= g.nxm) continue;
+    const size_t col = e / g.ldx;
+    const int j = (int)(col % g.nym), i = (int)(col / g.nym);
+    const int sx = __ldg(st.st[3] + k), sy = __ldg(st.st[4] + j), sz = __ldg(st.st[5] + i);
+    double wz[4], wy[4];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      wz[c] = __ldg(st.w[5] + 4 * i + c);
+      wy[c] = __ldg(st.w[4] + 4 * j + c);
+    }
+    int jj[4], ii[4];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      jj[c] = wrapmod(sy + c, sg.nymr);
+      ii[c] = wrapmod(sz + c, sg.nzmr);
+    }
+    double out = 0.0;
+#pragma unroll
+    for (int a = 0; a < 4; ++a) {
+      const int r = sx + a;
+      double q1 = 0.0;
+#pragma unroll
+      for (int b = 0; b < 4; ++b) {
+        double q2 = 0.0;
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+          const size_t pl = (size_t)jj[b] + (size_t)sg.nymr * ii[c];
+          const double *colr = sal + pl * sg.ldr;
+          const double s = sal_ext(colr, r, sg.nxmr, sg.sfixs, sg.sfixn, __ldg(st.salbp + pl), __ldg(st.saltp + pl));
+          q2 = (c == 0) ? s * wz[c] : q2 + s * wz[c];
+        }
+        q1 = (b == 0) ? q2 * wy[b] : q1 + q2 * wy[b];
+      }
+      const double wx = __ldg(st.w[3] + 4 * k + a);
+      out = (a == 0) ? q1 * wx : out + q1 * wx;
+    }
+    salc[e] = out;
+  }
+}
+
+// ------------------------------------------------------------------------------------------
+// k_sal_step: block per refined column (j, i).  One thread stages the x-columns the salinity
+// terms read (sal at the column and its four neighbours, vxr, vyr at j and j+1, vzr at i and
+// i+1; in 2-D the z neighbours are the column itself and those terms vanish) into shared memory
+// with 1-D TMA bulk copies on an mbarrier.  Every thread forms the explicit terms and the RHS of
+// its rows (ExplicitSalinity, salinity.F90:309-364; ImplicitSalinity :375-402), updates rusal in
+// place and puts the RHS, scaled by 1/(1 - ac betadx), into the chunk layout; one warp solves
+// the CN system with the factor tables of k_cn_tables (SolveImpEqnUpdate_Sal :408-452) and the
+// block writes sal_o = sal + increment.
+// ------------------------------------------------------------------------------------------
+constexpr int kSalCols3D = 10;
+constexpr int kSalCols2D = 6;
+
+template <int MR>
+struct SalShape {
+  static constexpr int tpc = MR == 1 ? 32 : MR == 2 ? 64 : MR == 4 ? 128 : MR == 12 ? 128 : 256;
+  static constexpr int rpt = (32 * MR + tpc - 1) / tpc;
+};
+
+__host__ __device__ inline size_t sal_step_smem(int MR, bool two_d) {
+  const int cs = 32 * MR + 8;
+  return ((size_t)(two_d ? kSalCols2D : kSalCols3D) * cs + (size_t)chunk_ld(MR) * MR) * sizeof(double);
+}
+
+template <int MR, bool TWO_D>
+__global__ void __launch_bounds__(SalShape<MR>::tpc)
+    k_sal_step(SalGeom sg, SalTables st, const StepCoef *__restrict__ sc_all, int ns, const double *__restrict__ cn_tab,
+               const double *__restrict__ sal, const double *__restrict__ vxr, const double *__restrict__ vyr,
+               const double *__restrict__ vzr, double *__restrict__ rusal, double *__restrict__ sal_o,
+               int *__restrict__ err) {
+  constexpr int TPC = SalShape<MR>::tpc, RPT = SalShape<MR>::rpt;
+  constexpr int CS = 32 * MR + 8;
+  constexpr int NC = TWO_D ? kSalCols2D : kSalCols3D;
+  constexpr int LD = chunk_ld(MR);
+  extern __shared__ __align__(128) unsigned char smem_sal[];
+  __shared__ uint64_t bar;
+  double *cols = reinterpret_cast<double *>(smem_sal);
+  double *s_rhs = cols + (size_t)NC * CS;
+  const int tc = threadIdx.x;
+  const int nymr = sg.nymr, nzmr = sg.nzmr, n = sg.nxmr;
+  const int j = blockIdx.x % nymr, i = blockIdx.x / nymr;
+  const int jp = wrap_inc(j, nymr), jm = wrap_dec(j, nymr);
+  const int ip = wrap_inc(i, nzmr), im = wrap_dec(i, nzmr);
+  auto off = [&](int jj, int ii) { return ((size_t)jj + (size_t)nymr * ii) * sg.ldr; };
+  const size_t c0 = off(j, i);
+  if (tc == 0) {
+    mbar_init(&bar, 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+  if (tc == 0) {
+    const uint32_t cb = (uint32_t)sg.ldr * sizeof(double);
+    mbar_arrive_expect_tx(&bar, cb * NC);
+    if constexpr (TWO_D) {
+      const double *src[kSalCols2D] = {sal + c0, vxr + c0, vyr + c0, sal + off(jp, i), sal + off(jm, i), vyr + off(jp, i)};
+#pragma unroll
+      for (int q = 0; q < NC; ++q) bulk_g2s(cols + (size_t)q * CS, src[q], cb, &bar);
+    } else {
+      const double *src[kSalCols3D] = {sal + c0,         vxr + c0,         vyr + c0,         vzr + c0,
+                                       sal + off(jp, i), sal + off(jm, i), sal + off(j, ip), sal + off(j, im),
+                                       vyr + off(jp, i), vzr + off(j, ip)};
+#pragma unroll
+      for (int q = 0; q < NC; ++q) bulk_g2s(cols + (size_t)q * CS, src[q], cb, &bar);
+    }
+  }
+  double ru[RPT];
+#pragma unroll
+  for (int p = 0; p < RPT; ++p) {
+    const int k = tc + TPC * p;
+    ru[p] = k < n ? rusal[c0 + k] : 0.0;
+  }
+  const bool ok = mbar_wait(&bar, 0, kSpinLimit);
+  if (!__syncthreads_and(ok)) {
+    if (tc == 0) atomicOr(err, 2);
+    mbar_wait(&bar, 0, kSpinLimit);  // let copies in flight land before the block exits
+    return;
+  }
+  const double *S = cols, *VX = cols + CS, *VY = cols + 2 * CS;
+  const double *SJP = cols + (TWO_D ? 3 : 4) * CS, *SJM = cols + (TWO_D ? 4 : 5) * CS;
+  const double *VYJP = cols + (TWO_D ? 5 : 8) * CS;
+  const double *VZ = cols + 3 * CS, *SIP = cols + 6 * CS, *SIM = cols + 7 * CS, *VZIP = cols + 9 * CS;
+  const StepCoef sc = sc_all[ns];
+  const double *T = cn_tab + (size_t)ns * cn_table_size(MR);
+  const size_t pl = (size_t)j + (size_t)nymr * i;
+  const double bp = __ldg(st.salbp + pl), tp = __ldg(st.saltp + pl);
+  const double alpec = sc.alpec;  // al / pecs (salinity.F90:374)
+#pragma unroll
+  for (int p = 0; p < RPT; ++p) {
+    const int k = tc + TPC * p;
+    if (k < n) {
+      const double sc_ = S[k];
+      const double ux = __ldg(st.udx3mr + k);
+      double hsx;
+      if (k == 0)
+        hsx = (VX[1] * (S[1] + sc_) - VX[0] * 2.0 * bp) * ux * 0.5;
+      else if (k == n - 1)
+        hsx = (VX[k + 1] * 2.0 * tp - VX[k] * (sc_ + S[k - 1])) * ux * 0.5;
+      else
+        hsx = (VX[k + 1] * (S[k + 1] + sc_) - VX[k] * (sc_ + S[k - 1])) * ux * 0.5;
+      const double hsy = (VYJP[k] * (SJP[k] + sc_) - VY[k] * (sc_ + SJM[k])) * sg.udyr;
+      const double dyys = (SJP[k] - 2.0 * sc_ + SJM[k]) * sg.udyrq;
+      double hsal;
+      if constexpr (TWO_D) {
+        hsal = -(hsx + hsy) + dyys;
+      } else {
+        const double hsz = (VZIP[k] * (SIP[k] + sc_) - VZ[k] * (sc_ + SIM[k])) * sg.udzr;
+        const double dzzs = (SIP[k] - 2.0 * sc_ + SIM[k]) * sg.udzrq;
+        hsal = -(hsx + hsy + hsz) + dyys + dzzs;
+      }
+      double dxxs;
+      const double a_p = __ldg(st.ap + k), a_c = __ldg(st.ac + k), a_m = __ldg(st.am + k);
+      if (k == 0)
+        dxxs = S[1] * a_p + sc_ * a_c - (a_p + a_c) * bp * sg.sfixs;
+      else if (k == n - 1)
+        dxxs = sc_ * a_c + S[k - 1] * a_m - (a_m + a_c) * tp * sg.sfixn;
+      else
+        dxxs = S[k + 1] * a_p + sc_ * a_c + S[k - 1] * a_m;
+      const double rhs = (sc.ga * hsal + sc.ro * ru[p] + alpec * dxxs) * sc.dt;
+      rusal[c0 + k] = hsal;
+      s_rhs[(k % MR) * LD + k / MR] = rhs * __ldg(T + k);
+    }
+  }
+  for (int r = n + tc; r < 32 * MR; r += TPC) s_rhs[(r % MR) * LD + r / MR] = 0.0;  // identity rows
+  __syncthreads();
+  if (tc < 32) cn_solve_chunk<MR, LD>(s_rhs, T, tc);
+  __syncthreads();
+#pragma unroll
+  for (int p = 0; p < RPT; ++p) {
+    const int k = tc + TPC * p;
+    if (k < n) sal_o[c0 + k] = S[k] + s_rhs[(k % MR) * LD + k / MR];
+  }
+}
+
+template <int MR>
+cudaError_t launch_sal_step_M(const SalCtx &S, cudaStream_t stream, int ns, int *err) {
+  const bool two_d = S.sg.nzmr == 1;
+  const size_t smem = sal_step_smem(MR, two_d);
+  const int nblk = S.sg.nymr * S.sg.nzmr;
+  if (two_d) {
+    auto kern = k_sal_step<MR, true>;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    kern<<<nblk, SalShape<MR>::tpc, smem, stream>>>(S.sg, S.st, S.sc, ns, S.cn_tab, S.sal, S.vxr, S.vyr, S.vzr,
+                                                    S.rusal, S.sal_o, err);
+  } else {
+    auto kern = k_sal_step<MR, false>;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    kern<<<nblk, SalShape<MR>::tpc, smem, stream>>>(S.sg, S.st, S.sc, ns, S.cn_tab, S.sal, S.vxr, S.vyr, S.vzr,
+                                                    S.rusal, S.sal_o, err);
+  }
+  return cudaGetLastError();
+}
+
+// ------------------------------------------------------------------------------------------
+// Diagnostics
+// ------------------------------------------------------------------------------------------
+// CalcMaxCFL.F90:48-65: max over refined cells of |vz|/dz + |vy|/dy + |vx|/dx at the centre.
+// Non-negative doubles order like their bit patterns, so the maximum is an integer atomicMax.
+__global__ void __launch_bounds__(256)
+    k_sal_cfl(SalGeom sg, SalTables st, const double *__restrict__ vxr, const double *__restrict__ vyr,
+              const double *__restrict__ vzr, unsigned long long *__restrict__ out) {
+  const size_t n = (size_t)sg.ldr * sg.nymr * sg.nzmr;
+  double m = 0.0;
+  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
+    const int k = (int)(e % sg.ldr);
+    if (k >= sg.nxmr) continue;
+    const size_t col = e / sg.ldr;
+    const int j = (int)(col % sg.nymr), i = (int)(col / sg.nymr);
+    const size_t ojp = ((size_t)wrap_inc(j, sg.nymr) + (size_t)sg.nymr * i) * sg.ldr + k;
+    const size_t oip = ((size_t)j + (size_t)sg.nymr * wrap_inc(i, sg.nzmr)) * sg.ldr + k;
+    const double q = fabs((vzr[e] + vzr[oip]) * 0.5 * sg.dzr) + fabs((vyr[e] + vyr[ojp]) * 0.5 * sg.dyr) +
+                     fabs((vxr[e] + vxr[e + 1]) * 0.5 * __ldg(st.udx3mr + k));
+    m = fmax(m, q);
+  }
+#pragma unroll
+  for (int h = 16; h > 0; h >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, h));
+  __shared__ double wm[8];
+  if ((threadIdx.x & 31) == 0) wm[threadIdx.x >> 5] = m;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int w = 1; w < (int)(blockDim.x >> 5); ++w) m = fmax(m, wm[w]);
+    atomicMax(out, (unsigned long long)__double_as_longlong(m));
+  }
+}
+
+// CalcSalStats / CalcDissipationSal (salinity.F90:537-566, 621-655): block b sums columns
+// b, b + nb, ... for every row k; partial[(b * 6 + q) * nxmr + k].
+__global__ void __launch_bounds__(256)
+    k_sal_prof_partial(SalGeom sg, SalTables st, const double *__restrict__ sal, const double *__restrict__ vxr,
+                       const double *__restrict__ vyr, const double *__restrict__ vzr, double *__restrict__ partial) {
+  const int n = sg.nxmr, ncol = sg.nymr * sg.nzmr;
+  for (int k = threadIdx.x; k < n; k += blockDim.x) {
+    double a[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+    const double tdx = __ldg(st.tdxr + k);
+    for (int col = blockIdx.x; col < ncol; col += gridDim.x) {
+      const int j = col % sg.nymr, i = col / sg.nymr;
+      const size_t o = (size_t)col * sg.ldr;
+      const size_t ojp = ((size_t)wrap_inc(j, sg.nymr) + (size_t)sg.nymr * i) * sg.ldr;
+      const size_t ojm = ((size_t)wrap_dec(j, sg.nymr) + (size_t)sg.nymr * i) * sg.ldr;
+      const size_t oip = ((size_t)j + (size_t)sg.nymr * wrap_inc(i, sg.nzmr)) * sg.ldr;
+      const size_t oim = ((size_t)j + (size_t)sg.nymr * wrap_dec(i, sg.nzmr)) * sg.ldr;
+      const double s = sal[o + k];
+      a[0] += s;
+      a[1] += s * s;
+      a[2] += 0.5 * (vxr[o + k] + vxr[o + k + 1]) * s;
+      a[3] += 0.5 * (vyr[o + k] + vyr[ojp + k]) * s;
+      a[4] += 0.5 * (vzr[o + k] + vzr[oip + k]) * s;
+      const double dz_ = (sal[oip + k] - sal[oim + k]) * 0.5 * sg.dzr;
+      const double dy_ = (sal[ojp + k] - sal[ojm + k]) * 0.5 * sg.dyr;
+      double dx_;
+      if (k == 0) {
+        const double bp = __ldg(st.salbp + col);
+        dx_ = (sal[o + 1] - s + 2.0 * sg.sfixs * (s - bp)) * tdx;
+      } else if (k == n - 1) {
+        const double tp = __ldg(st.saltp + col);
+        dx_ = (s - sal[o + k - 1] + 2.0 * sg.sfixn * (tp - s)) * tdx;
+      } else {
+        dx_ = (sal[o + k + 1] - sal[o + k - 1]) * tdx;
+      }
+      a[5] += dz_ * dz_;
+      a[5] += dy_ * dy_;
+      a[5] += dx_ * dx_;
+    }
+#pragma unroll
+    for (int q = 0; q < 6; ++q) partial[((size_t)blockIdx.x * 6 + q) * n + k] = a[q];
+  }
+}
+
+// Sum the block partials in block order and turn sums into averages (salinity.F90:578-587).
+__global__ void k_sal_prof_reduce(SalGeom sg, const double *__restrict__ partial, int nb, double *__restrict__ out) {
+  const int n = sg.nxmr;
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= 6 * n) return;
+  const int q = e / n, k = e % n;
+  double s = 0.0;
+  for (int b = 0; b < nb; ++b) s += partial[((size_t)b * 6 + q) * n + k];
+  const double inyz = 1.0 / sg.nymr / sg.nzmr;
+  if (q == 1)
+    s = sqrt(s * inyz);
+  else if (q == 5)
+    s = s / sg.pecs * inyz;
+  else
+    s = s * inyz;
+  out[e] = s;
+}
+
+int grid_for(size_t n, int tpb) {
+  const size_t b = (n + tpb - 1) / tpb;
+  return (int)(b < (size_t)148 * 16 ? b : (size_t)148 * 16);
+}
+
+}  // namespace
+
+int sal_prof_blocks(const SalGeom &sg) {
+  const int ncol = sg.nymr * sg.nzmr;
+  return ncol < 148 * 4 ? ncol : 148 * 4;
+}
+
+cudaError_t launch_sal_step(const LaunchCtx &L, const SalCtx &S, int ns) {
+  int *err = S.err;
+  switch (S.sg.MR) {
+    case 1: return launch_sal_step_M<1>(S, L.stream, ns, err);
+    case 2: return launch_sal_step_M<2>(S, L.stream, ns, err);
+    case 4: return launch_sal_step_M<4>(S, L.stream, ns, err);
+    case 8: return launch_sal_step_M<8>(S, L.stream, ns, err);
+    case 12: return launch_sal_step_M<12>(S, L.stream, ns, err);
+    case 16: return launch_sal_step_M<16>(S, L.stream, ns, err);
+    case 24: return launch_sal_step_M<24>(S, L.stream, ns, err);
+    case 32: return launch_sal_step_M<32>(S, L.stream, ns, err);
+  }
+  return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_sal_interp(const LaunchCtx &L, const SalCtx &S, const double *vx, const double *vy,
+                              const double *vz) {
+  const Geom &g = L.g;
+  const size_t nc = (size_t)g.ldx * g.nym * g.nzm;
+  k_sal_grad<<<grid_for(nc, 256), 256, 0, L.stream>>>(g, L.t, vx, vy, vz, S.gx, S.gy, S.gz);
+  const size_t smem = (size_t)(3 * (g.nxm + 4) + S.sg.nxmr) * sizeof(double);
+  if (smem > 48 * 1024) {
+    cudaError_t e = cudaFuncSetAttribute(k_sal_to_ref, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+  }
+  k_sal_to_ref<<<S.sg.nymr * S.sg.nzmr, kToRefThreads, smem, L.stream>>>(g, S.sg, S.st, S.gx, S.gy, S.gz, S.vxr,
+                                                                         S.gyr, S.gzr);
+  const dim3 gy((S.sg.nxmr + 127) / 128, S.sg.nzmr), gz((S.sg.nxmr + 127) / 128, S.sg.nymr);
+  k_sal_scan_y<<<gy, 128, 0, L.stream>>>(g, S.sg, S.st, vy, S.gyr, S.vyr);
+  k_sal_scan_z<<<gz, 128, 0, L.stream>>>(g, S.sg, S.st, vz, S.gzr, S.vzr);
+  k_sal_to_coarse<<<grid_for(nc, 256), 256, 0, L.stream>>>(g, S.sg, S.st, S.sal, S.salc);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_sal_cfl(const LaunchCtx &L, const SalCtx &S) {
+  cudaError_t e = cudaMemsetAsync(S.red, 0, sizeof(unsigned long long), L.stream);
+  if (e != cudaSuccess) return e;
+  const size_t n = (size_t)S.sg.ldr * S.sg.nymr * S.sg.nzmr;
+  k_sal_cfl<<<grid_for(n, 256), 256, 0, L.stream>>>(S.sg, S.st, S.vxr, S.vyr, S.vzr, S.red);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_sal_profiles(const LaunchCtx &L, const SalCtx &S, double *out) {
+  const int nb = sal_prof_blocks(S.sg);
+  k_sal_prof_partial<<<nb, 256, 0, L.stream>>>(S.sg, S.st, S.sal, S.vxr, S.vyr, S.vzr, S.partial);
+  const int ne = 6 * S.sg.nxmr;
+  k_sal_prof_reduce<<<(ne + 255) / 256, 256, 0, L.stream>>>(S.sg, S.partial, nb, out);
+  return cudaGetLastError();
+}
+
+size_t sal_step_smem_bytes(int MR, bool two_d) { return sal_step_smem(MR, two_d); }
+
+}  // namespace afid

@@ -18,7 +18,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 def _declared_functions():
     names = set()
-    for h in ("afid_gpu.h", "afid_host.h", "afid_batch.h", "afid_serve.h"):
+    for h in ("afid_gpu.h", "afid_host.h", "afid_batch.h", "afid_serve.h", "afid_salinity.h"):
         text = open(os.path.join(ROOT, "include", h)).read()
         text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
         names |= set(re.findall(r"\b(afid_\w+)\s*\(", text))
