@@ -930,10 +930,11 @@ int afid_gpu_sal_create(afid_ctx_t *ctx, const afid_sal_grid_t *sg) {
       !sg->saltp || !(sg->pecs > 0.0))
     return AFID_E_INVALID;
   // every source row the kernels read stays inside the (wall-extended) columns
-  if (!stencil_ok(sg->to_ref[0], nxmr, -2, g.nxm - 2) || !stencil_ok(sg->to_ref[1], nymr, -2 * nymr, 2 * nymr) ||
-      !stencil_ok(sg->to_ref[2], nzmr, -2 * nzmr, 2 * nzmr) || !stencil_ok(sg->to_coarse[0], g.nxm, -2, nxmr - 2) ||
-      !stencil_ok(sg->to_coarse[1], g.nym, -2 * g.nym, 2 * g.nym) ||
-      !stencil_ok(sg->to_coarse[2], g.nzm, -2 * g.nzm, 2 * g.nzm))
+  // (x: inside the wall-extended source column; y/z: within two periods of the source grid)
+  if (!stencil_ok(sg->to_ref[0], nxmr, -2, g.nxm - 2) || !stencil_ok(sg->to_ref[1], nymr, -2 * g.nym, 2 * g.nym) ||
+      !stencil_ok(sg->to_ref[2], nzmr, -2 * g.nzm, 2 * g.nzm) || !stencil_ok(sg->to_coarse[0], g.nxm, -2, nxmr - 2) ||
+      !stencil_ok(sg->to_coarse[1], g.nym, -2 * nymr, 2 * nymr) ||
+      !stencil_ok(sg->to_coarse[2], g.nzm, -2 * nzmr, 2 * nzmr))
     return AFID_E_INVALID;
   const bool two_d = nzmr == 1;
   const size_t smem_step = sal_step_smem_bytes(MR, two_d);
