@@ -457,7 +457,7 @@ class Solver:
         return int(lib().afid_gpu_launch_count(self._h))
 
     PROFILE_CLASSES = ("cn_tables", "explicit_implicit", "div_fft_y", "fft_z_fwd", "tridiag_pressure",
-                       "fft_z_inv", "ifft_y", "correct", "reductions")
+                       "fft_z_inv", "ifft_y", "correct", "reductions", "sal_step", "sal_interp")
 
     def autotune(self, force: bool = False) -> dict:
         info = TuneInfoT()

@@ -336,6 +336,7 @@ int afid_batch_destroy(afid_batch_t *b) {
 int afid_batch_create(const afid_input_t *proto, int nslots, int precision, afid_batch_t **out) {
   if (!proto || !out || nslots < 1 || proto->nzm < 1 || proto->dpdz != 0.0) return AFID_E_INVALID;
   if (proto->nzm > 1 && nslots != 1) return AFID_E_INVALID;  // a 3-D domain is a batch of one
+  if (proto->flagsal) return AFID_E_INVALID;                   // batches carry no salinity
   *out = nullptr;
   afid_batch_t *b = new (std::nothrow) afid_batch_t();
   if (!b) return AFID_E_ALLOC;

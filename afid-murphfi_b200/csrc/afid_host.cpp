@@ -2,6 +2,7 @@
 #include "afid_host.h"
 
 #include "afid_host_internal.h"
+#include "afid_salinity.h"
 
 #include <chrono>
 #include <cmath>
@@ -503,6 +504,19 @@ int afid_run(const afid_input_t *in, int precision, uint64_t seed, int nsteps, i
   afid_initial_temperature(t, seed, 1e-3, temp.data(), nx, nym);
   std::vector<double> zero(temp.size(), 0.0);
   s = afid_gpu_upload(ctx, zero.data(), zero.data(), zero.data(), temp.data(), zero.data(), nx, nym);
+  // multi-resolution salinity (MULTIRES = FLAGSAL = 1): refined grid, CreateInitialSalinity with
+  // Philox key seed + 1, and the refined-grid CFL number for the dt rule (main.F90:285-293)
+  afid_mgrd_t *mg = nullptr;
+  if (s == AFID_OK && in->flagsal) {
+    s = afid_mgrd_create(t, &mg);
+    if (s == AFID_OK) s = afid_gpu_sal_create(ctx, afid_mgrd_view(mg));
+    if (s == AFID_OK) {
+      const afid_sal_grid_t *v = afid_mgrd_view(mg);
+      std::vector<double> sal((size_t)v->nxmr * v->nymr * v->nzmr);
+      afid_initial_salinity(mg, seed + 1, 5e-3, sal.data(), v->nxmr, v->nymr);
+      s = afid_gpu_sal_upload(ctx, sal.data(), v->nxmr, v->nymr);
+    }
+  }
   afid_run_stats_t st{};
   const int total = (nsteps < 0) ? in->ntst + 1 : nsteps;
   double dt = in->dt, time = 0.0;
@@ -511,7 +525,7 @@ int afid_run(const afid_input_t *in, int precision, uint64_t seed, int nsteps, i
   int errorcode = 0;
   for (int ntime = 0; ntime < total && s == AFID_OK; ++ntime) {
     double cflm = 0.0;
-    if ((s = afid_gpu_cfl(ctx, &cflm)) != AFID_OK) break;
+    if ((s = mg ? afid_gpu_sal_cfl(ctx, &cflm) : afid_gpu_cfl(ctx, &cflm)) != AFID_OK) break;
     double cflr = 0.0;
     errorcode = afid_next_dt(in, ntime, &dt, cflm, &cflr);
     if ((s = afid_gpu_timemarcher(ctx, dt, ntime)) != AFID_OK) break;
@@ -543,6 +557,7 @@ int afid_run(const afid_input_t *in, int precision, uint64_t seed, int nsteps, i
   if (s == AFID_OK) afid_gpu_globals(ctx, ra_pr, &st.nu_vol, &st.ke, nullptr);
   if (stats) *stats = st;
   afid_gpu_destroy(ctx);
+  afid_mgrd_destroy(mg);
   afid_tables_destroy(t);
   return s;
 }

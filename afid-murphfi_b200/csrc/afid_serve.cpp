@@ -216,8 +216,8 @@ int afid_serve_destroy(afid_server_t *s) {
 
 int afid_serve_submit(afid_server_t *s, const afid_serve_job_t *job) {
   if (!s || !job || job->nsteps < 1 || job->in.nxm < 2 || job->in.nym < 1 || job->in.nzm < 1 ||
-      job->in.dpdz != 0.0)
-    return AFID_E_INVALID;
+      job->in.dpdz != 0.0 || job->in.flagsal)
+    return AFID_E_INVALID;  // served jobs carry no salinity
   Job j;
   j.spec = *job;
   j.t_submit = now_s(s);

@@ -77,6 +77,17 @@ def measured_peak():
         return 6650.0, "fallback"
 
 
+def committed_traffic_kernel(kernel: str, workload: str):
+    """DRAM bytes per launch of `kernel` from the committed ncu summary for this workload."""
+    p = os.path.join(ROOT, "profiles", f"{kernel}_{workload}.md")
+    if not os.path.exists(p):
+        return None
+    for line in open(p):
+        if line.startswith("traffic_bytes_per_launch:"):
+            return float(line.split(":")[1])
+    return None
+
+
 def committed_traffic(workload: str):
     """DRAM bytes per launch of the fused explicit/implicit kernel from the committed ncu
     summary for this workload (profiles/), or None."""
@@ -622,6 +633,213 @@ def run_served(args):
         dist.destroy_process_group()
 
 
+# ---- double-diffusive convection with the multi-resolution salinity scalar ------------------
+# Coarse flow + temperature grid as rbc3d, salinity on a grid refined 2x in every direction
+# (MULTIRES = FLAGSAL = 1), both scalars active along x, salinity free-fall scaling (FFscaleS = 1),
+# Le = PraS / Pr = 10; the reference's bounded double-diffusive initial salinity
+# 0.5 (2 (xmr - 0.5))^7 (salinity.F90:148-157) and the conductive temperature + noise.
+DDC_WORKLOADS = {
+    "ddc3d": dict(nxm=256, nym=384, nzm=384, nxmr=512, nymr=768, nzmr=768, rayt=1e8, prat=7.0, rays=1e9,
+                  pras=70.0, name="ddc3d_384x384x256_refined_768x768x512_fp64"),
+    # 1/8 of the refined cells (33.6 M, 2.2 GB of refined fields) for ncu captures
+    "ddc3d_small": dict(nxm=256, nym=128, nzm=128, nxmr=512, nymr=256, nzmr=256, rayt=1e8, prat=7.0, rays=1e9,
+                        pras=70.0, name="ddc3d_128x128x256_refined_256x256x512_fp64"),
+}
+# Algorithmic HBM bytes per refined cell of k_sal_step: read sal, vxr, vyr, vzr, rusal, write
+# sal_o, rusal (7 x 8 B).
+SAL_STEP_BYTES_PER_CELL = 56
+
+
+def ddc_bou_text(w: dict, ntst: int) -> str:
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from helpers import bou_text as _bt  # noqa: E402
+    return _bt(w["nxm"], w["nym"], w["nzm"], rayt=w["rayt"], prat=w["prat"], ylen=1.0, zlen=1.0, istr3=4,
+               str3=2.0, idtv=1, dt=1e-4, cflmax=1.2, dtmax=1e-2, ntst=ntst, resid=1e-3, multires=1,
+               nxmr=w["nxmr"], nymr=w["nymr"], nzmr=w["nzmr"], flagsal=1, istr3r=4, rays=w["rays"],
+               pras=w["pras"], ffscales=1, active_s=1)
+
+
+def ddc_cpu_baseline(budget_s: float = 30.0):
+    """The NumPy oracle (single thread) on a reduced double-diffusive case, one full step per
+    sample: the salinity path has no C restatement."""
+    from oracle import afid_oracle as o
+    from oracle import afid_salinity as sa
+    w = dict(nxm=64, nym=64, nzm=64, nxmr=128, nymr=128, nzmr=128, rayt=1e8, prat=7.0, rays=1e9, pras=70.0)
+    p = o.parse_bou_in(ddc_bou_text(w, 10))
+    g = o.create_grid(p)
+    m = sa.create_mgrd(g)
+    s = o.initial_state(g, 20261203)
+    ss = sa.new_sal_state(m, g, sa.initial_salinity(m, g, 20261204))
+    sa.interp_vel_mgrd(m, g, s, ss)
+    sa.interp_sal_multigrid(m, g, ss)
+    t0 = time.perf_counter()
+    n = 0
+    while n < 3 and (n == 0 or time.perf_counter() - t0 < budget_s):
+        sa.time_marcher(g, s, m, ss, 1e-4)
+        n += 1
+    sec = time.perf_counter() - t0
+    cells = w["nxm"] * w["nym"] * w["nzm"]
+    return {"value": round(cells * n / sec / 1e6, 4), "unit": "Mcell-RK3-steps/s", "cores": 1, "kind": "port",
+            "sample": f"{n} steps of a 64^3 coarse / 128^3 refined double-diffusive case (NumPy oracle)",
+            "steps": n, "seconds": round(sec, 2)}
+
+
+def run_ddc(args):
+    import numpy as np
+    import torch
+    import afid_gpu as ag
+
+    world, rank, local = dist_setup()
+    w = DDC_WORKLOADS[args.config]
+    cells = w["nxm"] * w["nym"] * w["nzm"]
+    rcells = w["nxmr"] * w["nymr"] * w["nzmr"]
+    inp = ag.parse_bou_in(ddc_bou_text(w, args.steps + args.warmup))
+    tables = ag.Tables(inp, ag.PREC_FP64)
+    mgrd = ag.Mgrd(tables)
+    stream = torch.cuda.Stream()
+    solver = ag.Solver(tables.grid, tables.params)
+    solver.set_stream(stream.cuda_stream)
+    if args.k1_shape >= 0:
+        solver.set_k1_shape(args.k1_shape)
+    solver.sal_create(mgrd)
+    temp0 = tables.initial_temperature(20261203)
+    sal0 = mgrd.initial_salinity(20261204)
+    nx, nym, nzm = w["nxm"] + 1, w["nym"], w["nzm"]
+    zeros = np.zeros((nzm, nym, nx))
+    solver.upload(zeros, zeros, zeros, temp0, zeros)
+    solver.sal_upload(sal0)
+    dt_box = [inp.dt]
+    dtc = ctypes.c_double()
+
+    def step(ntime: int):
+        cflmr = solver.sal_cfl()  # main.F90:285-293: the dt rule takes CFLmr with salinity on
+        dtc.value = dt_box[0]
+        err = ag.lib().afid_next_dt(ctypes.byref(inp), ntime, ctypes.byref(dtc), cflmr, None)
+        dt_box[0] = dtc.value
+        solver.time_marcher(dt_box[0], ntime)
+        return err
+
+    ntime = 0
+    for _ in range(args.warmup):
+        step(ntime)
+        ntime += 1
+    solver.synchronize()
+    tune = solver.autotune()
+    solver.profile_report()
+    solver.profile(True)
+    launches0 = solver.launch_count()
+    clocks = ClockSampler(torch.cuda.current_device())
+    barrier(world)
+    torch.cuda.synchronize()
+    clocks.start()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(args.steps):
+        step(ntime)
+        ntime += 1
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    barrier(world)
+    clk = clocks.stop()
+    ms_max = reduce_max(ev0.elapsed_time(ev1), world)
+    prof = solver.profile_report()
+    solver.profile(False)
+    launches = solver.launch_count() - launches0
+    value = world * cells * args.steps / (ms_max * 1e-3) / 1e6
+    s_ms, s_n = prof["sal_step"]
+    s_avg = (s_ms / s_n) * 1e-3 if s_n else float("nan")
+    peak, peak_kind = measured_peak()
+    s_bytes = SAL_STEP_BYTES_PER_CELL * rcells
+    achieved = s_bytes / s_avg / 1e9
+    prof_s = solver.sal_profiles()
+
+    # ---- end to end through the C ABI with host buffers -----------------------------------
+    pin = lambda shape: torch.empty(shape, dtype=torch.float64, pin_memory=True).numpy()  # noqa: E731
+    h_in = {k: pin((nzm, nym, nx)) for k in ("vx", "vy", "vz", "temp", "pr")}
+    for k in ("vx", "vy", "vz", "pr"):
+        h_in[k][...] = 0.0
+    h_in["temp"][...] = temp0
+    h_out = {k: pin((nzm, nym, nx)) for k in ("vx", "vy", "vz", "temp", "pr")}
+    rshape = (w["nzmr"], w["nymr"], w["nxmr"])
+    h_sal, h_sal_out = pin(rshape), pin(rshape)
+    h_sal[...] = sal0
+    dp = ctypes.POINTER(ctypes.c_double)
+    ptr = lambda a: a.ctypes.data_as(dp)  # noqa: E731
+    lib = ag.lib()
+    ra_pr = w["prat"] * abs(w["rayt"])
+    barrier(world)
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    assert lib.afid_gpu_upload(solver._h, *(ptr(h_in[k]) for k in ("vx", "vy", "vz", "temp", "pr")), nx, nym) == 0
+    assert lib.afid_gpu_sal_upload(solver._h, ptr(h_sal), w["nxmr"], w["nymr"]) == 0
+    dt_box[0] = inp.dt
+    nu = None
+    for n in range(args.steps):
+        step(n)
+        nu, _, _ = solver.global_quantities(ra_pr)
+    assert lib.afid_gpu_download(solver._h, *(ptr(h_out[k]) for k in ("vx", "vy", "vz", "temp", "pr")), nx, nym) == 0
+    assert lib.afid_gpu_sal_download(solver._h, ptr(h_sal_out), w["nxmr"], w["nymr"]) == 0
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = reduce_max(e0.elapsed_time(e1), world)
+    e2e_value = world * cells * args.steps / (e2e_ms * 1e-3) / 1e6
+    io_bytes = 5 * nx * nym * nzm * 8 + rcells * 8
+    finite = bool(np.isfinite(h_sal_out).all() and np.isfinite(h_out["vx"]).all())
+
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        cpu = ddc_cpu_baseline()
+    solver.close()
+    mgrd.close()
+    tables.close()
+    if rank == 0:
+        line = {
+            "metric": "Mcell-RK3-steps/s",
+            "value": round(value, 3),
+            "unit": "Mcell-RK3-steps/s",
+            "n_gpus": world,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": round(ms_max / args.steps, 4),
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f64",
+            "data": "synthetic: conductive temperature + Philox noise, double-diffusive salinity profile",
+            "config": {"workload": w["name"], "grid_xyz": [w["nxm"], w["nym"], w["nzm"]],
+                       "refined_xyz": [w["nxmr"], w["nymr"], w["nzmr"]], "cells": cells, "refined_cells": rcells,
+                       "refined_value": round(world * rcells * args.steps / (ms_max * 1e-3) / 1e6, 3),
+                       "RaT": w["rayt"], "Pr": w["prat"], "RaS": w["rays"], "PraS": w["pras"],
+                       "dt": "CFL-limited on the refined grid (CFLMAX 1.2, DTMAX 1e-2)",
+                       "l2": "inputs larger than L2 (~%.1f GB resident)" % ((cells * 21 + rcells * 8) * 8 / 1e9),
+                       "parallelism": "replicas" if world > 1 else "single GPU"},
+            "roofline": {"bound": "hbm", "kernel": "k_sal_step", "achieved": round(achieved, 1), "peak": peak,
+                         "unit": "GB/s", "frac": round(achieved / peak, 4),
+                         "peak_kind": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)",
+                         "algorithmic_bytes_per_launch": s_bytes, "avg_launch_ms": round(s_avg * 1e3, 4),
+                         "traffic": committed_traffic_kernel("k_sal_step", w["name"])},
+            "kernels_ms_per_step": {k: round(v[0] / args.steps, 4) for k, v in prof.items() if v[1]},
+            "e2e": {"value": round(e2e_value, 3), "unit": "Mcell-RK3-steps/s",
+                    "h2d_bytes_per_step": int(io_bytes / args.steps),
+                    "d2h_bytes_per_step": int(io_bytes / args.steps + 8 + 3 * 8),
+                    "note": "upload 5 fields + salinity, K steps with CFLmr + Nu/KE read back, download all"},
+            "gpu_launches": int(launches),
+            "k1_autotune": tune,
+            "clocks": clk,
+            "nu_vol_end": nu,
+            "sbar_range": [float(prof_s["Sbar"].min()), float(prof_s["Sbar"].max())],
+            "finite": finite,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
 def cpu_baseline(w: dict, steps: int, budget_s: float = 60.0):
     """The CPU restatement (C + OpenMP, oracle/afid_cpu.c) on the same workload: up to
     ``steps`` full main-loop steps, stopping once ``budget_s`` seconds have been spent."""
@@ -643,8 +861,16 @@ def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    w = WORKLOADS[args.config]
-    cpu = cpu_baseline(w, args.steps + args.warmup, budget_s=120.0)
+    if args.config in DDC_WORKLOADS:
+        w = DDC_WORKLOADS[args.config]
+        cpu = ddc_cpu_baseline(budget_s=120.0)
+    elif args.config in WORKLOADS:
+        w = WORKLOADS[args.config]
+        cpu = cpu_baseline(w, args.steps + args.warmup, budget_s=120.0)
+    else:
+        print(json.dumps({"impl": "reference", "unavailable": f"no CPU arm for the {args.config} workload"}),
+              flush=True)
+        return
     if "unavailable" in cpu:
         print(json.dumps({"impl": "reference", "unavailable": cpu["unavailable"]}), flush=True)
         return
@@ -675,7 +901,8 @@ def main():
     ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="afid", choices=["afid", "reference"])
-    ap.add_argument("--config", default="rbc3d", choices=sorted(WORKLOADS) + ["batched", "batched_fp64", "served"])
+    ap.add_argument("--config", default="rbc3d",
+                    choices=sorted(WORKLOADS) + sorted(DDC_WORKLOADS) + ["batched", "batched_fp64", "served"])
     ap.add_argument("--no-nu-check", action="store_true")
     ap.add_argument("--k1-shape", type=int, default=-1, help="fixed K1 thread shape instead of autotuning")
     ap.add_argument("--jobs", type=int, default=100, help="served: number of jobs")
@@ -694,6 +921,8 @@ def main():
         run_batched(args)
     elif args.config == "served":
         run_served(args)
+    elif args.config in DDC_WORKLOADS:
+        run_ddc(args)
     else:
         run_gpu(args)
 

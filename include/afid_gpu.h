@@ -172,8 +172,9 @@ int afid_gpu_set_k1_shape(afid_ctx_t *ctx, int index);
  * launch (no counterpart in the reference, which times whole steps with MPI_WTIME,
  * main.F90:282,363-371).  Classes: 0 CN factor tables, 1 explicit+implicit, 2 divergence +
  * y FFT, 3 z FFT forward, 4 Poisson tridiagonal, 5 z FFT backward, 6 y FFT backward,
- * 7 projection + pressure update, 8 reductions (CFL, divergence, volume sums). */
-#define AFID_PROF_CLASSES 9
+ * 7 projection + pressure update, 8 reductions (CFL, divergence, volume sums), 9 salinity step,
+ * 10 salinity interpolation (include/afid_salinity.h). */
+#define AFID_PROF_CLASSES 11
 int afid_gpu_profile_enable(afid_ctx_t *ctx, int enable);
 /* Milliseconds and launch counts per class since the last report; synchronises the stream. */
 int afid_gpu_profile_report(afid_ctx_t *ctx, double *ms, long long *count, int n);

@@ -161,3 +161,34 @@ def test_invalid_salinity_setups():
         with pytest.raises(ag.AfidError) as e:
             sv.sal_create(c2.mgrd)  # stencils built for another coarse grid
         assert e.value.status == ag.AFID_E_INVALID
+
+
+def test_host_driver_run_with_salinity_matches_oracle():
+    """afid_run with MULTIRES = FLAGSAL = 1: CreateInitialSalinity (Philox key seed + 1), the dt
+    rule on the refined CFL number, salinity coupled every substep; Nu and KE after 5 steps
+    against the oracle main loop."""
+    import ctypes
+    text = _text((32, 16, 8), (64, 32, 16), idtv=1, dt=1e-3, cflmax=1.0, dtmax=4e-3, ntst=4, active_t=1)
+    p = o.parse_bou_in(text)
+    g = o.create_grid(p)
+    m = sa.create_mgrd(g)
+    s = o.initial_state(g, 99)
+    ss = sa.new_sal_state(m, g, sa.initial_salinity(m, g, 100))
+    sa.interp_vel_mgrd(m, g, s, ss)
+    sa.interp_sal_multigrid(m, g, ss)
+    sa.run(g, s, m, ss, 5)
+    st = ag.RunStatsT()
+    inp = ag.parse_bou_in(text)
+    rc = ag.lib().afid_run(ctypes.byref(inp), ag.PREC_FP64, 99, 5, 0, None, None, ctypes.byref(st))
+    assert rc == 0 and st.steps_done == 5
+    assert st.nu_vol == pytest.approx(o.nusselt_volume(g, s), rel=1e-9)
+    assert st.ke == pytest.approx(o.kinetic_energy(g, s), rel=1e-6)
+    assert st.dt == pytest.approx(min(p.dtmax, p.limit_cfl / sa.calc_max_cfl_refined(m, ss)), rel=1e-6) or \
+        st.dt == pytest.approx(p.dtmax)
+
+
+def test_batches_and_jobs_refuse_salinity():
+    inp = ag.parse_bou_in(_text((16, 32, 1), (32, 64, 1)))
+    with pytest.raises(ag.AfidError) as e:
+        ag.Batch(inp, 2, ag.PREC_FP64)
+    assert e.value.status == ag.AFID_E_INVALID
