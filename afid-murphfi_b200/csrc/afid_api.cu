@@ -939,7 +939,7 @@ int afid_gpu_sal_create(afid_ctx_t *ctx, const afid_sal_grid_t *sg) {
   const bool two_d = nzmr == 1;
   const size_t smem_step = sal_step_smem_bytes(MR, two_d);
   const size_t smem_ref = (size_t)(3 * (g.nxm + 4) + nxmr) * sizeof(double);
-  if (smem_step > 227 * 1024 || smem_ref > 227 * 1024) return AFID_E_INVALID;
+  if (smem_step > 48 * 1024 || smem_ref > 227 * 1024) return AFID_E_INVALID;
   cudaSetDevice(ctx->dev);
   SalCtx *S = new (std::nothrow) SalCtx();
   if (!S) return AFID_E_ALLOC;
@@ -948,6 +948,7 @@ int afid_gpu_sal_create(afid_ctx_t *ctx, const afid_sal_grid_t *sg) {
   q.nymr = nymr;
   q.nzmr = nzmr;
   q.ldr = (nxmr + 1 + 7) / 8 * 8;
+  q.ldu = (nxmr + 4 + 7) / 8 * 8;
   q.MR = MR;
   q.dxr = sg->dxr;
   q.dyr = sg->dyr;
@@ -976,6 +977,8 @@ int afid_gpu_sal_create(afid_ctx_t *ctx, const afid_sal_grid_t *sg) {
   double **cf[4] = {&S->gx, &S->gy, &S->gz, &S->salc};
   for (double **p : cf)
     if ((e = dalloc(ctx, p, ctx->field_elems)) != cudaSuccess) return fail(e);
+  const size_t ntz = (size_t)3 * g.ldx * g.nym * nzmr, nu = (size_t)q.ldu * nymr * g.nzm;
+  if ((e = dalloc(ctx, &S->tmp, std::max(ntz, nu))) != cudaSuccess) return fail(e);
   // 1-D tables
   std::vector<double> lxa(nxmr), tdxr(nxmr);
   for (int k = 0; k < nxmr; ++k) {

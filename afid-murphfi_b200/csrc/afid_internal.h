@@ -78,6 +78,7 @@ int globals_partial_blocks(const Geom &g);
 // ---- multi-resolution salinity (afid_salinity.cu) ----------------------------------------
 struct SalGeom {
   int nxmr, nymr, nzmr, ldr;       // refined cells and x stride (>= nxmr + 1, multiple of 8)
+  int ldu;                         // x stride of wall-extended refined columns (>= nxmr + 4)
   int MR;                          // rows per lane of the refined CN solve (32 MR >= nxmr)
   double dxr, dyr, dzr;
   double udyr, udzr;               // 0.5 dyr, 0.5 dzr        (ExplicitSalinity advection)
@@ -103,6 +104,7 @@ struct SalCtx {
   double *sal = nullptr, *sal_o = nullptr, *rusal = nullptr;
   double *vxr = nullptr, *vyr = nullptr, *vzr = nullptr;
   double *gyr = nullptr, *gzr = nullptr;         // refined y/z velocity gradients (scratch)
+  double *tmp = nullptr;                         // z-contracted interpolation passes (scratch)
   double *gx = nullptr, *gy = nullptr, *gz = nullptr, *salc = nullptr;  // coarse
   double *cn_tab = nullptr;
   StepCoef *sc = nullptr;
@@ -122,7 +124,7 @@ cudaError_t launch_sal_cfl(const LaunchCtx &L, const SalCtx &S);
 cudaError_t launch_sal_profiles(const LaunchCtx &L, const SalCtx &S, double *out);
 int sal_prof_blocks(const SalGeom &sg);
 size_t sal_step_smem_bytes(int MR, bool two_d);
-constexpr int kSalLaunchesInterp = 5;
+constexpr int kSalLaunchesInterp = 7;
 cudaError_t launch_repack(cudaStream_t st, const double *src, int sld, double *dst, int dld, int width,
                           size_t rows);
 

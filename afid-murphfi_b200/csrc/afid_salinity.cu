@@ -2,17 +2,17 @@
 //
 // Per substep (TimeMarcher.F90:50-63, 95, 138-144):
 //   k_sal_step       ExplicitSalinity + ImplicitSalinity + SolveImpEqnUpdate_Sal fused per refined
-//                    x-column (salinity.F90:268-453): staged columns, RHS, CN solve, update
+//                    x-column (salinity.F90:268-453): one warp per column, RHS, CN solve, update
 //   (K1 subtracts bycs * salc from the forcing along gAxis: AddSalBuoyancy, salinity.F90:494-506)
 // after the projection:
 //   k_sal_grad       dvx/dx, dvy/dy, dvz/dz at the coarse cell centres (InterpVelMgrd.F90:33-158)
-//   k_sal_to_ref     the three gradients interpolated to the refined cell centres
-//                    (interpolate_xyz_to_refined, HermiteInterpolations.F90:168-200); vxr is
+//   k_sal_zint +     the three gradients interpolated to the refined cell centres
+//   k_sal_to_ref     (interpolate_xyz_to_refined, HermiteInterpolations.F90:168-200); vxr is
 //                    integrated along the column in the same block (InterpVelMgrd.F90:49-57)
 //   k_sal_scan_y     first-guess plane at y = 0 (vy interpolated in x-z) + integration along y
 //   k_sal_scan_z     first-guess plane at z = 0 (vz in x-y, when nzm > 1) + integration along z
-//   k_sal_to_coarse  salc from the wall-extended refined salinity (InterpSalMultigrid,
-//                    salinity.F90:455-492, per-target form of either coarse interpolation)
+//   k_sal_zc +       salc from the wall-extended refined salinity (InterpSalMultigrid,
+//   k_sal_to_coarse  salinity.F90:455-492, per-target form of either coarse interpolation)
 // Diagnostics: k_sal_cfl (CalcMaxCFL.F90:48-65), k_sal_prof_* (CalcSalStats, salinity.F90:508-667).
 //
 // Layout: refined fields are x-fastest like the coarse ones, (k, j, i) at k + ldr (j + nymr i),
@@ -75,47 +75,67 @@ __global__ void __launch_bounds__(256)
 }
 
 // ------------------------------------------------------------------------------------------
-// k_sal_to_ref: block per refined column (jr, ir).  The y-z contraction of the 16 coarse
-// columns around it (z first, then y: qv2 / qv1 of HermiteInterpolations.F90:186-192) gives one
-// wall-extended coarse column per gradient in shared memory; the x contraction then yields the
-// refined gradients.  dvx/dx is integrated along the column (vxr(1) = 0), dvy/dy and dvz/dz go
-// to scratch for the y and z integrations.
+// Coarse -> refined interpolation of the three velocity gradients in two passes, contracting z,
+// then y, then x exactly as qv2 / qv1 of HermiteInterpolations.F90:186-196:
+//   k_sal_zint   T_f(r, jc, ir) = sum_c wz_c(ir) g_f(r, jc, sz(ir) + c), one thread per point;
+//   k_sal_to_ref block per refined column (jr, ir): q_f(r) = sum_b wy_b(jr) T_f(r, sy(jr) + b, ir)
+//                gives a wall-extended coarse column per gradient in shared memory, the x
+//                contraction yields the refined gradients, and dvx/dx is integrated along the
+//                column (vxr(1) = 0, InterpVelMgrd.F90:48-57); dvy/dy and dvz/dz go to scratch
+//                for the y and z integrations.
 // ------------------------------------------------------------------------------------------
+__global__ void __launch_bounds__(256)
+    k_sal_zint(Geom g, SalGeom sg, SalTables st, const double *__restrict__ gx, const double *__restrict__ gy,
+               const double *__restrict__ gz, double *__restrict__ tz) {
+  const size_t plane = (size_t)g.ldx * g.nym;  // one z-plane of a coarse field
+  const size_t n = plane * sg.nzmr;
+  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
+    const int r = (int)(e % g.ldx);
+    if (r >= g.nxm) continue;
+    const int ir = (int)(e / plane);
+    const size_t off = e - (size_t)ir * plane;  // r + ldx * jc
+    const int sz = __ldg(st.st[2] + ir);
+    double w[4];
+    size_t o[4];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      w[c] = __ldg(st.w[2] + 4 * ir + c);
+      o[c] = off + plane * (size_t)wrapmod(sz + c, g.nzm);
+    }
+    const double *src[3] = {gx, gy, gz};
+#pragma unroll
+    for (int f = 0; f < 3; ++f)
+      tz[(size_t)f * n + e] = __ldg(src[f] + o[0]) * w[0] + __ldg(src[f] + o[1]) * w[1] + __ldg(src[f] + o[2]) * w[2] +
+                              __ldg(src[f] + o[3]) * w[3];
+  }
+}
+
 constexpr int kToRefThreads = 256;
 
 __global__ void __launch_bounds__(kToRefThreads)
-    k_sal_to_ref(Geom g, SalGeom sg, SalTables st, const double *__restrict__ gx, const double *__restrict__ gy,
-                 const double *__restrict__ gz, double *__restrict__ vxr, double *__restrict__ gyr,
-                 double *__restrict__ gzr) {
+    k_sal_to_ref(Geom g, SalGeom sg, SalTables st, const double *__restrict__ tz, double *__restrict__ vxr,
+                 double *__restrict__ gyr, double *__restrict__ gzr) {
   extern __shared__ __align__(16) double sm_to_ref[];
   const int nxm = g.nxm, L = nxm + 4;  // extended rows -2 .. nxm+1 at 0 .. nxm+3
   double *qx = sm_to_ref, *qy = qx + L, *qz = qy + L, *d = qz + L;
   __shared__ double warp_tot[kToRefThreads / 32];
   const int tid = threadIdx.x;
   const int jr = blockIdx.x % sg.nymr, ir = blockIdx.x / sg.nymr;
-  const int sy = __ldg(st.st[1] + jr), sz = __ldg(st.st[2] + ir);
-  double wy[4], wz[4];
-  size_t co[4][4];  // coarse column offsets [b][c]
+  const int sy = __ldg(st.st[1] + jr);
+  const size_t n = (size_t)g.ldx * g.nym * sg.nzmr;
+  double wy[4];
+  size_t co[4];  // T columns (sy + b, ir)
 #pragma unroll
-  for (int a = 0; a < 4; ++a) {
-    wy[a] = __ldg(st.w[1] + 4 * jr + a);
-    wz[a] = __ldg(st.w[2] + 4 * ir + a);
+  for (int b = 0; b < 4; ++b) {
+    wy[b] = __ldg(st.w[1] + 4 * jr + b);
+    co[b] = ((size_t)wrapmod(sy + b, g.nym) + (size_t)g.nym * ir) * g.ldx;
   }
-#pragma unroll
-  for (int b = 0; b < 4; ++b)
-#pragma unroll
-    for (int c = 0; c < 4; ++c) co[b][c] = col_off(g, wrapmod(sy + b, g.nym), wrapmod(sz + c, g.nzm));
   for (int r = tid; r < nxm; r += kToRefThreads) {
     double q[3];
-    const double *src[3] = {gx, gy, gz};
 #pragma unroll
     for (int f = 0; f < 3; ++f) {
-      double q2[4];
-#pragma unroll
-      for (int b = 0; b < 4; ++b)
-        q2[b] = __ldg(src[f] + co[b][0] + r) * wz[0] + __ldg(src[f] + co[b][1] + r) * wz[1] +
-                __ldg(src[f] + co[b][2] + r) * wz[2] + __ldg(src[f] + co[b][3] + r) * wz[3];
-      q[f] = q2[0] * wy[0] + q2[1] * wy[1] + q2[2] * wy[2] + q2[3] * wy[3];
+      const double *t = tz + (size_t)f * n + r;
+      q[f] = __ldg(t + co[0]) * wy[0] + __ldg(t + co[1]) * wy[1] + __ldg(t + co[2]) * wy[2] + __ldg(t + co[3]) * wy[3];
     }
     qx[r + 2] = q[0];
     qy[r + 2] = q[1];
@@ -123,7 +143,7 @@ __global__ void __launch_bounds__(kToRefThreads)
   }
   __syncthreads();
   if (tid < 3) {
-    // ghost rows: the wall rule commutes with the (linear) y-z contraction
+    // ghost rows: the wall rule (a factor +-1) commutes exactly with the y-z contraction
     double *q = tid == 0 ? qx : (tid == 1 ? qy : qz);
     q[0] = 0.0;
     q[1] = (double)(1 - 2 * g.inslws) * q[2];
@@ -240,209 +260,206 @@ __global__ void __launch_bounds__(128)
 }
 
 // ------------------------------------------------------------------------------------------
-// k_sal_to_coarse: thread per coarse point (k < nxm) of the padded field: salc =
-// sum_a wx_a sum_b wy_b sum_c wz_c S_ext (z, then y, then x as qv2 / qv1 of
-// HermiteInterpolations.F90:270-284).
+// Refined -> coarse interpolation of salinity (InterpSalMultigrid) in two passes, z, then y,
+// then x as HermiteInterpolations.F90:270-284:
+//   k_sal_zc         U(rr, jr, ic) = sum_c wz_c(ic) S_ext(rr, jr, sz(ic) + c) for the extended
+//                    refined rows rr = -2 .. nxmr+1 (stored at rr + 2, stride ldu), one thread
+//                    per point; the plate ghosts are formed per refined column as the reference
+//                    does before its contraction (salinity.F90:462-481);
+//   k_sal_to_coarse  block per coarse column (j, i): U2(rr) = sum_b wy_b(j) U(rr, sy(j) + b, i)
+//                    in shared memory, then salc(k) = sum_a wx_a(k) U2(sx(k) + a).
 // ------------------------------------------------------------------------------------------
 __global__ void __launch_bounds__(256)
-    k_sal_to_coarse(Geom g, SalGeom sg, SalTables st, const double *__restrict__ sal, double *__restrict__ salc) {
-  const size_t n = (size_t)g.ldx * g.nym * g.nzm;
+    k_sal_zc(Geom g, SalGeom sg, SalTables st, const double *__restrict__ sal, double *__restrict__ u) {
+  const int ldu = sg.ldu;
+  const size_t plane = (size_t)ldu * sg.nymr;
+  const size_t n = plane * g.nzm;
   for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
-    const int k = (int)(e % g.ldx);
-    if (k >= g.nxm) continue;
-    const size_t col = e / g.ldx;
-    const int j = (int)(col % g.nym), i = (int)(col / g.nym);
-    const int sx = __ldg(st.st[3] + k), sy = __ldg(st.st[4] + j), sz = __ldg(st.st[5] + i);
-    double wz[4], wy[4];
+    const int q = (int)(e % ldu);
+    if (q >= sg.nxmr + 4) continue;
+    const int rr = q - 2;
+    const size_t col = e / ldu;
+    const int jr = (int)(col % sg.nymr), ic = (int)(col / sg.nymr);
+    const int sz = __ldg(st.st[5] + ic);
+    double v = 0.0;
 #pragma unroll
     for (int c = 0; c < 4; ++c) {
-      wz[c] = __ldg(st.w[5] + 4 * i + c);
-      wy[c] = __ldg(st.w[4] + 4 * j + c);
+      const size_t pl = (size_t)jr + (size_t)sg.nymr * wrapmod(sz + c, sg.nzmr);
+      const double s = sal_ext(sal + pl * sg.ldr, rr, sg.nxmr, sg.sfixs, sg.sfixn, __ldg(st.salbp + pl),
+                               __ldg(st.saltp + pl)) *
+                       __ldg(st.w[5] + 4 * ic + c);
+      v = (c == 0) ? s : v + s;
     }
-    int jj[4], ii[4];
+    u[e] = v;
+  }
+}
+
+constexpr int kToCoarseThreads = 256;
+
+__global__ void __launch_bounds__(kToCoarseThreads)
+    k_sal_to_coarse(Geom g, SalGeom sg, SalTables st, const double *__restrict__ u, double *__restrict__ salc) {
+  extern __shared__ __align__(16) double sm_to_c[];
+  const int tid = threadIdx.x;
+  const int j = blockIdx.x % g.nym, i = blockIdx.x / g.nym;
+  const int sy = __ldg(st.st[4] + j);
+  double wy[4];
+  size_t co[4];
 #pragma unroll
-    for (int c = 0; c < 4; ++c) {
-      jj[c] = wrapmod(sy + c, sg.nymr);
-      ii[c] = wrapmod(sz + c, sg.nzmr);
-    }
-    double out = 0.0;
-#pragma unroll
-    for (int a = 0; a < 4; ++a) {
-      const int r = sx + a;
-      double q1 = 0.0;
-#pragma unroll
-      for (int b = 0; b < 4; ++b) {
-        double q2 = 0.0;
-#pragma unroll
-        for (int c = 0; c < 4; ++c) {
-          const size_t pl = (size_t)jj[b] + (size_t)sg.nymr * ii[c];
-          const double *colr = sal + pl * sg.ldr;
-          const double s = sal_ext(colr, r, sg.nxmr, sg.sfixs, sg.sfixn, __ldg(st.salbp + pl), __ldg(st.saltp + pl));
-          q2 = (c == 0) ? s * wz[c] : q2 + s * wz[c];
-        }
-        q1 = (b == 0) ? q2 * wy[b] : q1 + q2 * wy[b];
-      }
-      const double wx = __ldg(st.w[3] + 4 * k + a);
-      out = (a == 0) ? q1 * wx : out + q1 * wx;
-    }
-    salc[e] = out;
+  for (int b = 0; b < 4; ++b) {
+    wy[b] = __ldg(st.w[4] + 4 * j + b);
+    co[b] = ((size_t)wrapmod(sy + b, sg.nymr) + (size_t)sg.nymr * i) * sg.ldu;
+  }
+  const int nrows = sg.nxmr + 4;
+  for (int q = tid; q < nrows; q += kToCoarseThreads)
+    sm_to_c[q] = __ldg(u + co[0] + q) * wy[0] + __ldg(u + co[1] + q) * wy[1] + __ldg(u + co[2] + q) * wy[2] +
+                 __ldg(u + co[3] + q) * wy[3];
+  __syncthreads();
+  const size_t c0 = col_off(g, j, i);
+  for (int k = tid; k < g.nxm; k += kToCoarseThreads) {
+    const int p = __ldg(st.st[3] + k) + 2;
+    salc[c0 + k] = sm_to_c[p] * __ldg(st.w[3] + 4 * k) + sm_to_c[p + 1] * __ldg(st.w[3] + 4 * k + 1) +
+                   sm_to_c[p + 2] * __ldg(st.w[3] + 4 * k + 2) + sm_to_c[p + 3] * __ldg(st.w[3] + 4 * k + 3);
   }
 }
 
 // ------------------------------------------------------------------------------------------
-// k_sal_step: block per refined column (j, i).  One thread stages the x-columns the salinity
-// terms read (sal at the column and its four neighbours, vxr, vyr at j and j+1, vzr at i and
-// i+1; in 2-D the z neighbours are the column itself and those terms vanish) into shared memory
-// with 1-D TMA bulk copies on an mbarrier.  Every thread forms the explicit terms and the RHS of
-// its rows (ExplicitSalinity, salinity.F90:309-364; ImplicitSalinity :375-402), updates rusal in
-// place and puts the RHS, scaled by 1/(1 - ac betadx), into the chunk layout; one warp solves
-// the CN system with the factor tables of k_cn_tables (SolveImpEqnUpdate_Sal :408-452) and the
-// block writes sal_o = sal + increment.
+// k_sal_step: one warp per refined column (j, i), four columns per block, no block barriers.
+// Lane l owns rows l, l + 32, ...: it forms the explicit terms and the RHS of its rows
+// (ExplicitSalinity, salinity.F90:309-364; ImplicitAndUpdate :375-402) from coalesced loads of
+// the column and its neighbours (only the column itself is read at k +- 1), updates rusal in
+// place and puts the RHS, scaled by 1/(1 - ac betadx), into the warp's chunk-layout rows in
+// shared memory; the warp then solves the CN system with the factor tables of k_cn_tables
+// (SolveImpEqnUpdate_Sal :408-452) and writes sal_o = sal + increment.  In 2-D the z neighbours
+// are the column itself and those terms vanish; they are left out.
 // ------------------------------------------------------------------------------------------
-constexpr int kSalCols3D = 10;
-constexpr int kSalCols2D = 6;
-
-template <int MR>
-struct SalShape {
-  static constexpr int tpc = MR == 1 ? 32 : MR == 2 ? 64 : MR == 4 ? 128 : MR == 12 ? 128 : 256;
-  static constexpr int rpt = (32 * MR + tpc - 1) / tpc;
-};
+constexpr int kSalStepWarps = 4;
 
 __host__ __device__ inline size_t sal_step_smem(int MR, bool two_d) {
-  const int cs = 32 * MR + 8;
-  return ((size_t)(two_d ? kSalCols2D : kSalCols3D) * cs + (size_t)chunk_ld(MR) * MR) * sizeof(double);
+  (void)two_d;
+  return (size_t)kSalStepWarps * chunk_ld(MR) * MR * sizeof(double);
 }
 
 template <int MR, bool TWO_D>
-__global__ void __launch_bounds__(SalShape<MR>::tpc)
+__global__ void __launch_bounds__(32 * kSalStepWarps)
     k_sal_step(SalGeom sg, SalTables st, const StepCoef *__restrict__ sc_all, int ns, const double *__restrict__ cn_tab,
                const double *__restrict__ sal, const double *__restrict__ vxr, const double *__restrict__ vyr,
-               const double *__restrict__ vzr, double *__restrict__ rusal, double *__restrict__ sal_o,
-               int *__restrict__ err) {
-  constexpr int TPC = SalShape<MR>::tpc, RPT = SalShape<MR>::rpt;
-  constexpr int CS = 32 * MR + 8;
-  constexpr int NC = TWO_D ? kSalCols2D : kSalCols3D;
+               const double *__restrict__ vzr, double *__restrict__ rusal, double *__restrict__ sal_o) {
   constexpr int LD = chunk_ld(MR);
-  extern __shared__ __align__(128) unsigned char smem_sal[];
-  __shared__ uint64_t bar;
-  double *cols = reinterpret_cast<double *>(smem_sal);
-  double *s_rhs = cols + (size_t)NC * CS;
-  const int tc = threadIdx.x;
+  constexpr int B = MR < 4 ? MR : 4;  // rows per lane whose operands are loaded together
+  static_assert(MR % B == 0, "row batches must tile the column");
+  extern __shared__ __align__(16) double smem_sal[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int nymr = sg.nymr, nzmr = sg.nzmr, n = sg.nxmr;
-  const int j = blockIdx.x % nymr, i = blockIdx.x / nymr;
-  const int jp = wrap_inc(j, nymr), jm = wrap_dec(j, nymr);
-  const int ip = wrap_inc(i, nzmr), im = wrap_dec(i, nzmr);
+  const int col = blockIdx.x * kSalStepWarps + warp;
+  if (col >= nymr * nzmr) return;  // whole warps only: nothing below synchronises the block
+  double *s_rhs = smem_sal + (size_t)warp * LD * MR;
+  const int j = col % nymr, i = col / nymr;
   auto off = [&](int jj, int ii) { return ((size_t)jj + (size_t)nymr * ii) * sg.ldr; };
-  const size_t c0 = off(j, i);
-  if (tc == 0) {
-    mbar_init(&bar, 1);
-    fence_mbar_init();
-  }
-  __syncthreads();
-  if (tc == 0) {
-    const uint32_t cb = (uint32_t)sg.ldr * sizeof(double);
-    mbar_arrive_expect_tx(&bar, cb * NC);
-    if constexpr (TWO_D) {
-      const double *src[kSalCols2D] = {sal + c0, vxr + c0, vyr + c0, sal + off(jp, i), sal + off(jm, i), vyr + off(jp, i)};
-#pragma unroll
-      for (int q = 0; q < NC; ++q) bulk_g2s(cols + (size_t)q * CS, src[q], cb, &bar);
-    } else {
-      const double *src[kSalCols3D] = {sal + c0,         vxr + c0,         vyr + c0,         vzr + c0,
-                                       sal + off(jp, i), sal + off(jm, i), sal + off(j, ip), sal + off(j, im),
-                                       vyr + off(jp, i), vzr + off(j, ip)};
-#pragma unroll
-      for (int q = 0; q < NC; ++q) bulk_g2s(cols + (size_t)q * CS, src[q], cb, &bar);
-    }
-  }
-  double ru[RPT];
-#pragma unroll
-  for (int p = 0; p < RPT; ++p) {
-    const int k = tc + TPC * p;
-    ru[p] = k < n ? rusal[c0 + k] : 0.0;
-  }
-  const bool ok = mbar_wait(&bar, 0, kSpinLimit);
-  if (!__syncthreads_and(ok)) {
-    if (tc == 0) atomicOr(err, 2);
-    mbar_wait(&bar, 0, kSpinLimit);  // let copies in flight land before the block exits
-    return;
-  }
-  const double *S = cols, *VX = cols + CS, *VY = cols + 2 * CS;
-  const double *SJP = cols + (TWO_D ? 3 : 4) * CS, *SJM = cols + (TWO_D ? 4 : 5) * CS;
-  const double *VYJP = cols + (TWO_D ? 5 : 8) * CS;
-  const double *VZ = cols + 3 * CS, *SIP = cols + 6 * CS, *SIM = cols + 7 * CS, *VZIP = cols + 9 * CS;
+  const size_t c0 = off(j, i), ojp = off(wrap_inc(j, nymr), i), ojm = off(wrap_dec(j, nymr), i);
+  const size_t oip = off(j, wrap_inc(i, nzmr)), oim = off(j, wrap_dec(i, nzmr));
   const StepCoef sc = sc_all[ns];
   const double *T = cn_tab + (size_t)ns * cn_table_size(MR);
-  const size_t pl = (size_t)j + (size_t)nymr * i;
-  const double bp = __ldg(st.salbp + pl), tp = __ldg(st.saltp + pl);
+  const double bp = __ldg(st.salbp + col), tp = __ldg(st.saltp + col);
   const double alpec = sc.alpec;  // al / pecs (salinity.F90:374)
+  // operands of one row: sal(k), sal(k-1), sal(k+1), sal(j+-1), vxr(k), vxr(k+1), vyr(j), vyr(j+1),
+  // rusal, then (3-D) sal(i+-1), vzr(i), vzr(i+1)
+  constexpr int NV = TWO_D ? 9 : 13;
+#pragma unroll 1
+  for (int p0 = 0; p0 < MR; p0 += B) {
+    double v[B][NV];
 #pragma unroll
-  for (int p = 0; p < RPT; ++p) {
-    const int k = tc + TPC * p;
-    if (k < n) {
-      const double sc_ = S[k];
-      const double ux = __ldg(st.udx3mr + k);
-      double hsx;
-      if (k == 0)
-        hsx = (VX[1] * (S[1] + sc_) - VX[0] * 2.0 * bp) * ux * 0.5;
-      else if (k == n - 1)
-        hsx = (VX[k + 1] * 2.0 * tp - VX[k] * (sc_ + S[k - 1])) * ux * 0.5;
-      else
-        hsx = (VX[k + 1] * (S[k + 1] + sc_) - VX[k] * (sc_ + S[k - 1])) * ux * 0.5;
-      const double hsy = (VYJP[k] * (SJP[k] + sc_) - VY[k] * (sc_ + SJM[k])) * sg.udyr;
-      const double dyys = (SJP[k] - 2.0 * sc_ + SJM[k]) * sg.udyrq;
-      double hsal;
-      if constexpr (TWO_D) {
-        hsal = -(hsx + hsy) + dyys;
-      } else {
-        const double hsz = (VZIP[k] * (SIP[k] + sc_) - VZ[k] * (sc_ + SIM[k])) * sg.udzr;
-        const double dzzs = (SIP[k] - 2.0 * sc_ + SIM[k]) * sg.udzrq;
-        hsal = -(hsx + hsy + hsz) + dyys + dzzs;
+    for (int q = 0; q < B; ++q) {
+      const int k = lane + 32 * (p0 + q);
+      const int kk = k < n ? k : n - 1;  // rows past the column read a valid row and are discarded
+      v[q][0] = __ldg(sal + c0 + kk);
+      v[q][1] = kk > 0 ? __ldg(sal + c0 + kk - 1) : 0.0;
+      v[q][2] = kk < n - 1 ? __ldg(sal + c0 + kk + 1) : 0.0;
+      v[q][3] = __ldg(sal + ojp + kk);
+      v[q][4] = __ldg(sal + ojm + kk);
+      v[q][5] = __ldg(vxr + c0 + kk);
+      v[q][6] = __ldg(vxr + c0 + kk + 1);
+      v[q][7] = __ldg(vyr + c0 + kk);
+      v[q][8] = __ldg(vyr + ojp + kk);
+      if constexpr (!TWO_D) {
+        v[q][9] = __ldg(sal + oip + kk);
+        v[q][10] = __ldg(sal + oim + kk);
+        v[q][11] = __ldg(vzr + c0 + kk);
+        v[q][12] = __ldg(vzr + oip + kk);
       }
-      double dxxs;
-      const double a_p = __ldg(st.ap + k), a_c = __ldg(st.ac + k), a_m = __ldg(st.am + k);
-      if (k == 0)
-        dxxs = S[1] * a_p + sc_ * a_c - (a_p + a_c) * bp * sg.sfixs;
-      else if (k == n - 1)
-        dxxs = sc_ * a_c + S[k - 1] * a_m - (a_m + a_c) * tp * sg.sfixn;
-      else
-        dxxs = S[k + 1] * a_p + sc_ * a_c + S[k - 1] * a_m;
-      const double rhs = (sc.ga * hsal + sc.ro * ru[p] + alpec * dxxs) * sc.dt;
-      rusal[c0 + k] = hsal;
-      s_rhs[(k % MR) * LD + k / MR] = rhs * __ldg(T + k);
+    }
+    double ru[B];
+#pragma unroll
+    for (int q = 0; q < B; ++q) {
+      const int k = lane + 32 * (p0 + q);
+      ru[q] = rusal[c0 + (k < n ? k : n - 1)];
+    }
+#pragma unroll
+    for (int q = 0; q < B; ++q) {
+      const int k = lane + 32 * (p0 + q);
+      double rhs_s = 0.0;  // identity rows k >= n
+      if (k < n) {
+        const double sc_ = v[q][0], sm = v[q][1], sp = v[q][2], sjp = v[q][3], sjm = v[q][4];
+        const double vx0 = v[q][5], vx1 = v[q][6], vy0 = v[q][7], vy1 = v[q][8];
+        const double ux = __ldg(st.udx3mr + k);
+        double hsx;
+        if (k == 0)
+          hsx = (vx1 * (sp + sc_) - vx0 * 2.0 * bp) * ux * 0.5;
+        else if (k == n - 1)
+          hsx = (vx1 * 2.0 * tp - vx0 * (sc_ + sm)) * ux * 0.5;
+        else
+          hsx = (vx1 * (sp + sc_) - vx0 * (sc_ + sm)) * ux * 0.5;
+        const double hsy = (vy1 * (sjp + sc_) - vy0 * (sc_ + sjm)) * sg.udyr;
+        const double dyys = (sjp - 2.0 * sc_ + sjm) * sg.udyrq;
+        double hsal;
+        if constexpr (TWO_D) {
+          hsal = -(hsx + hsy) + dyys;
+        } else {
+          const double sip = v[q][9], sim = v[q][10], vz0 = v[q][11], vz1 = v[q][12];
+          const double hsz = (vz1 * (sip + sc_) - vz0 * (sc_ + sim)) * sg.udzr;
+          const double dzzs = (sip - 2.0 * sc_ + sim) * sg.udzrq;
+          hsal = -(hsx + hsy + hsz) + dyys + dzzs;
+        }
+        const double a_p = __ldg(st.ap + k), a_c = __ldg(st.ac + k), a_m = __ldg(st.am + k);
+        double dxxs;
+        if (k == 0)
+          dxxs = sp * a_p + sc_ * a_c - (a_p + a_c) * bp * sg.sfixs;
+        else if (k == n - 1)
+          dxxs = sc_ * a_c + sm * a_m - (a_m + a_c) * tp * sg.sfixn;
+        else
+          dxxs = sp * a_p + sc_ * a_c + sm * a_m;
+        const double rhs = (sc.ga * hsal + sc.ro * ru[q] + alpec * dxxs) * sc.dt;
+        rusal[c0 + k] = hsal;
+        rhs_s = rhs * __ldg(T + k);
+      }
+      s_rhs[(k % MR) * LD + k / MR] = rhs_s;
     }
   }
-  for (int r = n + tc; r < 32 * MR; r += TPC) s_rhs[(r % MR) * LD + r / MR] = 0.0;  // identity rows
-  __syncthreads();
-  if (tc < 32) cn_solve_chunk<MR, LD>(s_rhs, T, tc);
-  __syncthreads();
-#pragma unroll
-  for (int p = 0; p < RPT; ++p) {
-    const int k = tc + TPC * p;
-    if (k < n) sal_o[c0 + k] = S[k] + s_rhs[(k % MR) * LD + k / MR];
+  __syncwarp();
+  cn_solve_chunk<MR, LD>(s_rhs, T, lane);
+  __syncwarp();
+#pragma unroll 4
+  for (int p = 0; p < MR; ++p) {
+    const int k = lane + 32 * p;
+    if (k < n) sal_o[c0 + k] = __ldg(sal + c0 + k) + s_rhs[(k % MR) * LD + k / MR];  // column re-read hits L1/L2
   }
 }
 
 template <int MR>
-cudaError_t launch_sal_step_M(const SalCtx &S, cudaStream_t stream, int ns, int *err) {
+cudaError_t launch_sal_step_M(const SalCtx &S, cudaStream_t stream, int ns) {
   const bool two_d = S.sg.nzmr == 1;
   const size_t smem = sal_step_smem(MR, two_d);
-  const int nblk = S.sg.nymr * S.sg.nzmr;
-  if (two_d) {
-    auto kern = k_sal_step<MR, true>;
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
-    kern<<<nblk, SalShape<MR>::tpc, smem, stream>>>(S.sg, S.st, S.sc, ns, S.cn_tab, S.sal, S.vxr, S.vyr, S.vzr,
-                                                    S.rusal, S.sal_o, err);
-  } else {
-    auto kern = k_sal_step<MR, false>;
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
-    kern<<<nblk, SalShape<MR>::tpc, smem, stream>>>(S.sg, S.st, S.sc, ns, S.cn_tab, S.sal, S.vxr, S.vyr, S.vzr,
-                                                    S.rusal, S.sal_o, err);
-  }
+  const int ncol = S.sg.nymr * S.sg.nzmr;
+  const int nblk = (ncol + kSalStepWarps - 1) / kSalStepWarps;
+  if (two_d)
+    k_sal_step<MR, true><<<nblk, 32 * kSalStepWarps, smem, stream>>>(S.sg, S.st, S.sc, ns, S.cn_tab, S.sal, S.vxr,
+                                                                     S.vyr, S.vzr, S.rusal, S.sal_o);
+  else
+    k_sal_step<MR, false><<<nblk, 32 * kSalStepWarps, smem, stream>>>(S.sg, S.st, S.sc, ns, S.cn_tab, S.sal, S.vxr,
+                                                                      S.vyr, S.vzr, S.rusal, S.sal_o);
   return cudaGetLastError();
 }
 
+//                    salinity.F90:455-492, per-target form of either coarse interpolation)
 // ------------------------------------------------------------------------------------------
 // Diagnostics
 // ------------------------------------------------------------------------------------------
@@ -549,16 +566,15 @@ int sal_prof_blocks(const SalGeom &sg) {
 }
 
 cudaError_t launch_sal_step(const LaunchCtx &L, const SalCtx &S, int ns) {
-  int *err = S.err;
   switch (S.sg.MR) {
-    case 1: return launch_sal_step_M<1>(S, L.stream, ns, err);
-    case 2: return launch_sal_step_M<2>(S, L.stream, ns, err);
-    case 4: return launch_sal_step_M<4>(S, L.stream, ns, err);
-    case 8: return launch_sal_step_M<8>(S, L.stream, ns, err);
-    case 12: return launch_sal_step_M<12>(S, L.stream, ns, err);
-    case 16: return launch_sal_step_M<16>(S, L.stream, ns, err);
-    case 24: return launch_sal_step_M<24>(S, L.stream, ns, err);
-    case 32: return launch_sal_step_M<32>(S, L.stream, ns, err);
+    case 1: return launch_sal_step_M<1>(S, L.stream, ns);
+    case 2: return launch_sal_step_M<2>(S, L.stream, ns);
+    case 4: return launch_sal_step_M<4>(S, L.stream, ns);
+    case 8: return launch_sal_step_M<8>(S, L.stream, ns);
+    case 12: return launch_sal_step_M<12>(S, L.stream, ns);
+    case 16: return launch_sal_step_M<16>(S, L.stream, ns);
+    case 24: return launch_sal_step_M<24>(S, L.stream, ns);
+    case 32: return launch_sal_step_M<32>(S, L.stream, ns);
   }
   return cudaErrorInvalidValue;
 }
@@ -568,17 +584,21 @@ cudaError_t launch_sal_interp(const LaunchCtx &L, const SalCtx &S, const double 
   const Geom &g = L.g;
   const size_t nc = (size_t)g.ldx * g.nym * g.nzm;
   k_sal_grad<<<grid_for(nc, 256), 256, 0, L.stream>>>(g, L.t, vx, vy, vz, S.gx, S.gy, S.gz);
+  const size_t nt = (size_t)g.ldx * g.nym * S.sg.nzmr;
+  k_sal_zint<<<grid_for(nt, 256), 256, 0, L.stream>>>(g, S.sg, S.st, S.gx, S.gy, S.gz, S.tmp);
   const size_t smem = (size_t)(3 * (g.nxm + 4) + S.sg.nxmr) * sizeof(double);
   if (smem > 48 * 1024) {
     cudaError_t e = cudaFuncSetAttribute(k_sal_to_ref, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
   }
-  k_sal_to_ref<<<S.sg.nymr * S.sg.nzmr, kToRefThreads, smem, L.stream>>>(g, S.sg, S.st, S.gx, S.gy, S.gz, S.vxr,
-                                                                         S.gyr, S.gzr);
+  k_sal_to_ref<<<S.sg.nymr * S.sg.nzmr, kToRefThreads, smem, L.stream>>>(g, S.sg, S.st, S.tmp, S.vxr, S.gyr, S.gzr);
   const dim3 gy((S.sg.nxmr + 127) / 128, S.sg.nzmr), gz((S.sg.nxmr + 127) / 128, S.sg.nymr);
   k_sal_scan_y<<<gy, 128, 0, L.stream>>>(g, S.sg, S.st, vy, S.gyr, S.vyr);
   k_sal_scan_z<<<gz, 128, 0, L.stream>>>(g, S.sg, S.st, vz, S.gzr, S.vzr);
-  k_sal_to_coarse<<<grid_for(nc, 256), 256, 0, L.stream>>>(g, S.sg, S.st, S.sal, S.salc);
+  const size_t nu = (size_t)S.sg.ldu * S.sg.nymr * g.nzm;
+  k_sal_zc<<<grid_for(nu, 256), 256, 0, L.stream>>>(g, S.sg, S.st, S.sal, S.tmp);
+  const size_t smc = (size_t)(S.sg.nxmr + 4) * sizeof(double);
+  k_sal_to_coarse<<<g.nym * g.nzm, kToCoarseThreads, smc, L.stream>>>(g, S.sg, S.st, S.tmp, S.salc);
   return cudaGetLastError();
 }
 
