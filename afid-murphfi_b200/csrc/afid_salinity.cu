@@ -46,11 +46,12 @@ __device__ __forceinline__ double coarse_ext(const double *__restrict__ col, int
 // Wall-extended refined salinity (salinity.F90:462-481): row -1 is 2 salbp - sal(0) with SfixS
 // (else sal(0)), row nxmr is 2 saltp - sal(nxmr-1) with SfixN (else sal(nxmr-1)); -2 and nxmr+1
 // are zero.
+// The plate values are read only for the ghost rows.
 __device__ __forceinline__ double sal_ext(const double *__restrict__ col, int r, int n, int sfixs, int sfixn,
-                                          double bp, double tp) {
+                                          const double *__restrict__ bp, const double *__restrict__ tp) {
   if (r >= 0 && r < n) return __ldg(col + r);
-  if (r == -1) return sfixs ? 2.0 * bp - __ldg(col) : __ldg(col);
-  if (r == n) return sfixn ? 2.0 * tp - __ldg(col + n - 1) : __ldg(col + n - 1);
+  if (r == -1) return sfixs ? 2.0 * __ldg(bp) - __ldg(col) : __ldg(col);
+  if (r == n) return sfixn ? 2.0 * __ldg(tp) - __ldg(col + n - 1) : __ldg(col + n - 1);
   return 0.0;
 }
 
@@ -110,9 +111,9 @@ __global__ void __launch_bounds__(256)
   }
 }
 
-constexpr int kToRefThreads = 256;
+constexpr int kToRefThreads = 128;
 
-__global__ void __launch_bounds__(kToRefThreads)
+__global__ void __launch_bounds__(kToRefThreads, 8)
     k_sal_to_ref(Geom g, SalGeom sg, SalTables st, const double *__restrict__ tz, double *__restrict__ vxr,
                  double *__restrict__ gyr, double *__restrict__ gzr) {
   extern __shared__ __align__(16) double sm_to_ref[];
@@ -285,8 +286,7 @@ __global__ void __launch_bounds__(256)
 #pragma unroll
     for (int c = 0; c < 4; ++c) {
       const size_t pl = (size_t)jr + (size_t)sg.nymr * wrapmod(sz + c, sg.nzmr);
-      const double s = sal_ext(sal + pl * sg.ldr, rr, sg.nxmr, sg.sfixs, sg.sfixn, __ldg(st.salbp + pl),
-                               __ldg(st.saltp + pl)) *
+      const double s = sal_ext(sal + pl * sg.ldr, rr, sg.nxmr, sg.sfixs, sg.sfixn, st.salbp + pl, st.saltp + pl) *
                        __ldg(st.w[5] + 4 * ic + c);
       v = (c == 0) ? s : v + s;
     }
@@ -345,7 +345,7 @@ __global__ void __launch_bounds__(32 * kSalStepWarps)
                const double *__restrict__ sal, const double *__restrict__ vxr, const double *__restrict__ vyr,
                const double *__restrict__ vzr, double *__restrict__ rusal, double *__restrict__ sal_o) {
   constexpr int LD = chunk_ld(MR);
-  constexpr int B = MR < 4 ? MR : 4;  // rows per lane whose operands are loaded together
+  constexpr int B = MR < 2 ? MR : 2;  // rows per lane whose operands are loaded together
   static_assert(MR % B == 0, "row batches must tile the column");
   extern __shared__ __align__(16) double smem_sal[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
