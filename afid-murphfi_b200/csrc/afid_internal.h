@@ -63,6 +63,9 @@ cudaError_t launch_explicit_implicit(const LaunchCtx &L, const SubstepBuffers &b
 // K1 over the first ncol columns with thread shape `var` (autotuner samples use ncol < all).
 cudaError_t launch_k1_fp64(const LaunchCtx &L, const SubstepBuffers &b, int ns, int var, int ncol);
 cudaError_t launch_k1_mixed(const LaunchCtx &L, const SubstepBuffers &b, int ns, int var, int ncol);
+// The same with the salinity buoyancy in the explicit terms (L.g.salc set).
+cudaError_t launch_k1_fp64_sal(const LaunchCtx &L, const SubstepBuffers &b, int ns, int var, int ncol);
+cudaError_t launch_k1_mixed_sal(const LaunchCtx &L, const SubstepBuffers &b, int ns, int var, int ncol);
 // Thread shapes of K1 for M: fills tpc[]/rpt[]/cap[] (up to AFID_TUNE_MAX) and returns their number.
 int k1_shapes(int M, int *tpc, int *rpt, int *cap);
 // The kernels of one substep, in launch order (K1 .. K7).

@@ -72,7 +72,7 @@ template <typename TE> __device__ __forceinline__ TE cv(double v) { return (TE)v
 // construction; those terms are left out instead of being evaluated to zero.
 
 // ExplicitTermsVX.F90:194-291 + ImplicitAndUpdateVX.F90:124-150, k = 1..nxm-1 (0-based)
-template <typename TE, bool TWO_D>
+template <typename TE, bool TWO_D, bool SAL>
 __device__ __forceinline__ double rhs_vx(const Geom &g, const Tables &t, const StepCoef &sc, int k,
                                          const ColV &X, const ColV &Y, const ColV &Z, const ColV &T,
                                          const ColV &P, double ru, TE &qout, double sb) {
@@ -101,7 +101,7 @@ __device__ __forceinline__ double rhs_vx(const Geom &g, const Tables &t, const S
   if (g.gaxis == 1) {
     const TE tempit = (TE)g.active_t * (TE)0.5 * (cv<TE>(T.c[k]) + cv<TE>(T.c[km]));
     qcap = qcap + (TE)g.byct * tempit;
-    if (g.salc) qcap = qcap - (TE)sb;  // AddSalBuoyancy(qcap)
+    if constexpr (SAL) qcap = qcap - (TE)sb;  // AddSalBuoyancy(qcap)
   }
   const double alre = sc.alre;
   const double udx3 = sc.al * __ldg(t.udx3c + k);
@@ -112,7 +112,7 @@ __device__ __forceinline__ double rhs_vx(const Geom &g, const Tables &t, const S
 }
 
 // ExplicitTermsVY.F90:23-122 + ImplicitAndUpdateVY.F90:28-80, k = 0..nxm-1
-template <typename TE, bool TWO_D>
+template <typename TE, bool TWO_D, bool SAL>
 __device__ __forceinline__ double rhs_vy(const Geom &g, const Tables &t, const StepCoef &sc, int k,
                                          const ColV &X, const ColV &Y, const ColV &Z, const ColV &T,
                                          const ColV &P, double zd, double pjm, double ru, TE &qout,
@@ -142,7 +142,7 @@ __device__ __forceinline__ double rhs_vy(const Geom &g, const Tables &t, const S
   if (g.gaxis == 2) {
     const TE tempit = (TE)g.active_t * (TE)0.5 * (cv<TE>(T.c[k]) + cv<TE>(T.jm[k]));
     dph = dph + (TE)g.byct * tempit;
-    if (g.salc) dph = dph - (TE)sb;  // AddSalBuoyancy(dph)
+    if constexpr (SAL) dph = dph - (TE)sb;  // AddSalBuoyancy(dph)
   }
   const double alre = sc.alre;
   const double udyp = g.dy * sc.al;
@@ -161,7 +161,7 @@ __device__ __forceinline__ double rhs_vy(const Geom &g, const Tables &t, const S
 }
 
 // ExplicitTermsVZ.F90:149-244 + ImplicitAndUpdateVZ.F90:121-161, k = 0..nxm-1
-template <typename TE, bool TWO_D>
+template <typename TE, bool TWO_D, bool SAL>
 __device__ __forceinline__ double rhs_vz(const Geom &g, const Tables &t, const StepCoef &sc, int k,
                                          const ColV &X, const ColV &Y, const ColV &Z, const ColV &T,
                                          const ColV &P, double yd, double pim, double ru, TE &qout,
@@ -191,7 +191,7 @@ __device__ __forceinline__ double rhs_vz(const Geom &g, const Tables &t, const S
   if (g.gaxis == 3) {
     const TE tempit = (TE)g.active_t * (TE)0.5 * (cv<TE>(T.c[k]) + cv<TE>(T.im[k]));
     dq = dq + (TE)g.byct * tempit;
-    if (g.salc) dq = dq - (TE)sb;  // AddSalBuoyancy(dq)
+    if constexpr (SAL) dq = dq - (TE)sb;  // AddSalBuoyancy(dq)
   }
   const double alre = sc.alre;
   const double amm = __ldg(t.am3sk + k), acc = __ldg(t.ac3sk + k), app = __ldg(t.ap3sk + k);
@@ -289,7 +289,7 @@ template <int CAP, int TPC>
 constexpr int k1_min_blocks() {
   return CAP == 0 ? 1 : ((CAP == 1 ? 512 : 1024) / TPC > 1 ? (CAP == 1 ? 512 : 1024) / TPC : 1);
 }
-template <int M, int TPC, int RPT, typename TE, bool TWO_D, int CAP>
+template <int M, int TPC, int RPT, typename TE, bool TWO_D, int CAP, bool SAL>
 __global__ void __launch_bounds__(TPC, k1_min_blocks<CAP, TPC>())
     k_explicit_implicit(Geom g0, Tables t, const StepCoef *__restrict__ sc_all, int ns,
                         const double *__restrict__ cn_tab, const double *__restrict__ vx,
@@ -410,12 +410,12 @@ __global__ void __launch_bounds__(TPC, k1_min_blocks<CAP, TPC>())
       const double zd = TWO_D ? Z.jm[k] : vv[p][0];
       const double yd = TWO_D ? Y.jp[k] : vv[p][1];
       const double pim = TWO_D ? P.c[k] : vv[p][3];
-      // salinity buoyancy bycs * salc at this row, for the gravity component
-      const double sb = g.salc ? g.bycs * __ldg(g.salc + c0 + k) : 0.0;
+      // salinity buoyancy bycs * salc at this row, for the gravity component (SAL: salinity on)
+      const double sb = SAL ? g.bycs * __ldg(g.salc + c0 + k) : 0.0;
       // all four right-hand sides from the staged columns before anything is stored
-      rr[p][0] = (k >= 1) ? rhs_vx<TE, TWO_D>(g, t, sc, k, X, Y, Z, T, P, u0, q0, sb) * __ldg(TX + k - 1) : 0.0;
-      rr[p][1] = rhs_vy<TE, TWO_D>(g, t, sc, k, X, Y, Z, T, P, zd, vv[p][2], u1, q1, sb) * __ldg(TY + k);
-      rr[p][2] = rhs_vz<TE, TWO_D>(g, t, sc, k, X, Y, Z, T, P, yd, pim, u2, q2, sb) * __ldg(TY + k);
+      rr[p][0] = (k >= 1) ? rhs_vx<TE, TWO_D, SAL>(g, t, sc, k, X, Y, Z, T, P, u0, q0, sb) * __ldg(TX + k - 1) : 0.0;
+      rr[p][1] = rhs_vy<TE, TWO_D, SAL>(g, t, sc, k, X, Y, Z, T, P, zd, vv[p][2], u1, q1, sb) * __ldg(TY + k);
+      rr[p][2] = rhs_vz<TE, TWO_D, SAL>(g, t, sc, k, X, Y, Z, T, P, yd, pim, u2, q2, sb) * __ldg(TY + k);
       rr[p][3] = rhs_temp<TE, TWO_D>(g, t, sc, k, X, Y, Z, T, tbp, ttp, u3, q3) * __ldg(TT + k);
       if (k >= 1) rux[c0 + k] = q0;
       ruy[c0 + k] = q1;
@@ -477,10 +477,10 @@ __global__ void __launch_bounds__(TPC, k1_min_blocks<CAP, TPC>())
   }
 }
 
-template <int M, int TPC, int RPT, typename TE, bool TWO_D, int CAP>
+template <int M, int TPC, int RPT, typename TE, bool TWO_D, int CAP, bool SAL>
 cudaError_t launch_k1_cfg(const LaunchCtx &L, const SubstepBuffers &b, int ns, int ncol) {
   const size_t smem = k1_smem(L.g.ldx, M, TWO_D);
-  auto kern = k_explicit_implicit<M, TPC, RPT, TE, TWO_D, CAP>;
+  auto kern = k_explicit_implicit<M, TPC, RPT, TE, TWO_D, CAP, SAL>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   kern<<<ncol, TPC, smem, L.stream>>>(L.g, L.t, b.sc, ns, b.cn_tab, b.vx, b.vy, b.vz, b.temp, b.pr,
@@ -511,42 +511,42 @@ constexpr K1Shape kK1Shapes[8][kK1MaxShapes] = {
     {{256, 4, 1}, {512, 2, 0}, {0, 0, 0}, {0, 0, 0}, {0, 0, 0}},       // M = 32  (<= 1024)
 };
 
-template <int M, int V, typename TE, bool TWO_D>
+template <int M, int V, typename TE, bool TWO_D, bool SAL>
 cudaError_t launch_k1_v(const LaunchCtx &L, const SubstepBuffers &b, int ns, int ncol) {
   constexpr int mi = k1_m_index(M);
   if constexpr (V < kK1ShapeCount[mi]) {
     constexpr int TPC = kK1Shapes[mi][V].tpc, RPT = kK1Shapes[mi][V].rpt;
     constexpr int CAP = kK1Shapes[mi][V].cap;
     static_assert(TPC * RPT >= 32 * M, "K1 shape must cover 32*M rows");
-    return launch_k1_cfg<M, TPC, RPT, TE, TWO_D, CAP>(L, b, ns, ncol);
+    return launch_k1_cfg<M, TPC, RPT, TE, TWO_D, CAP, SAL>(L, b, ns, ncol);
   } else {
     return cudaErrorInvalidValue;
   }
 }
 
-template <int M, typename TE, bool TWO_D>
+template <int M, typename TE, bool TWO_D, bool SAL>
 cudaError_t launch_k1_M(const LaunchCtx &L, const SubstepBuffers &b, int ns, int var, int ncol) {
   switch (var) {
-    case 0: return launch_k1_v<M, 0, TE, TWO_D>(L, b, ns, ncol);
-    case 1: return launch_k1_v<M, 1, TE, TWO_D>(L, b, ns, ncol);
-    case 2: return launch_k1_v<M, 2, TE, TWO_D>(L, b, ns, ncol);
-    case 3: return launch_k1_v<M, 3, TE, TWO_D>(L, b, ns, ncol);
-    case 4: return launch_k1_v<M, 4, TE, TWO_D>(L, b, ns, ncol);
+    case 0: return launch_k1_v<M, 0, TE, TWO_D, SAL>(L, b, ns, ncol);
+    case 1: return launch_k1_v<M, 1, TE, TWO_D, SAL>(L, b, ns, ncol);
+    case 2: return launch_k1_v<M, 2, TE, TWO_D, SAL>(L, b, ns, ncol);
+    case 3: return launch_k1_v<M, 3, TE, TWO_D, SAL>(L, b, ns, ncol);
+    case 4: return launch_k1_v<M, 4, TE, TWO_D, SAL>(L, b, ns, ncol);
   }
   return cudaErrorInvalidValue;
 }
 
-template <typename TE, bool TWO_D>
+template <typename TE, bool TWO_D, bool SAL>
 cudaError_t launch_k1_T(const LaunchCtx &L, const SubstepBuffers &b, int ns, int var, int ncol) {
   switch (L.M) {
-    case 1: return launch_k1_M<1, TE, TWO_D>(L, b, ns, var, ncol);
-    case 2: return launch_k1_M<2, TE, TWO_D>(L, b, ns, var, ncol);
-    case 4: return launch_k1_M<4, TE, TWO_D>(L, b, ns, var, ncol);
-    case 8: return launch_k1_M<8, TE, TWO_D>(L, b, ns, var, ncol);
-    case 12: return launch_k1_M<12, TE, TWO_D>(L, b, ns, var, ncol);
-    case 16: return launch_k1_M<16, TE, TWO_D>(L, b, ns, var, ncol);
-    case 24: return launch_k1_M<24, TE, TWO_D>(L, b, ns, var, ncol);
-    case 32: return launch_k1_M<32, TE, TWO_D>(L, b, ns, var, ncol);
+    case 1: return launch_k1_M<1, TE, TWO_D, SAL>(L, b, ns, var, ncol);
+    case 2: return launch_k1_M<2, TE, TWO_D, SAL>(L, b, ns, var, ncol);
+    case 4: return launch_k1_M<4, TE, TWO_D, SAL>(L, b, ns, var, ncol);
+    case 8: return launch_k1_M<8, TE, TWO_D, SAL>(L, b, ns, var, ncol);
+    case 12: return launch_k1_M<12, TE, TWO_D, SAL>(L, b, ns, var, ncol);
+    case 16: return launch_k1_M<16, TE, TWO_D, SAL>(L, b, ns, var, ncol);
+    case 24: return launch_k1_M<24, TE, TWO_D, SAL>(L, b, ns, var, ncol);
+    case 32: return launch_k1_M<32, TE, TWO_D, SAL>(L, b, ns, var, ncol);
   }
   return cudaErrorInvalidValue;
 }
