@@ -938,7 +938,7 @@ int afid_gpu_sal_create(afid_ctx_t *ctx, const afid_sal_grid_t *sg) {
     return AFID_E_INVALID;
   const bool two_d = nzmr == 1;
   const size_t smem_step = sal_step_smem_bytes(MR, two_d);
-  const size_t smem_ref = (size_t)(3 * (g.nxm + 4) + nxmr) * sizeof(double);
+  const size_t smem_ref = (size_t)4 * 3 * (g.nxm + 4) * sizeof(double);  // four warps' rows
   if (smem_step > 48 * 1024 || smem_ref > 227 * 1024) return AFID_E_INVALID;
   cudaSetDevice(ctx->dev);
   SalCtx *S = new (std::nothrow) SalCtx();

@@ -78,50 +78,52 @@ __global__ void __launch_bounds__(256)
 // ------------------------------------------------------------------------------------------
 // Coarse -> refined interpolation of the three velocity gradients in two passes, contracting z,
 // then y, then x exactly as qv2 / qv1 of HermiteInterpolations.F90:186-196:
-//   k_sal_zint   T_f(r, jc, ir) = sum_c wz_c(ir) g_f(r, jc, sz(ir) + c), one thread per point;
-//   k_sal_to_ref block per refined column (jr, ir): q_f(r) = sum_b wy_b(jr) T_f(r, sy(jr) + b, ir)
+//   k_sal_zint   T_f(r, jc, ir) = sum_c wz_c(ir) g_f(r, jc, sz(ir) + c), block per column;
+//   k_sal_to_ref warp per refined column (jr, ir): q_f(r) = sum_b wy_b(jr) T_f(r, sy(jr) + b, ir)
 //                gives a wall-extended coarse column per gradient in shared memory, the x
 //                contraction yields the refined gradients, and dvx/dx is integrated along the
 //                column (vxr(1) = 0, InterpVelMgrd.F90:48-57); dvy/dy and dvz/dz go to scratch
 //                for the y and z integrations.
 // ------------------------------------------------------------------------------------------
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(128)
     k_sal_zint(Geom g, SalGeom sg, SalTables st, const double *__restrict__ gx, const double *__restrict__ gy,
                const double *__restrict__ gz, double *__restrict__ tz) {
-  const size_t plane = (size_t)g.ldx * g.nym;  // one z-plane of a coarse field
-  const size_t n = plane * sg.nzmr;
-  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
-    const int r = (int)(e % g.ldx);
-    if (r >= g.nxm) continue;
-    const int ir = (int)(e / plane);
-    const size_t off = e - (size_t)ir * plane;  // r + ldx * jc
-    const int sz = __ldg(st.st[2] + ir);
-    double w[4];
-    size_t o[4];
+  // block per output column (jc, ir): the four source columns and weights are block constants
+  const int jc = blockIdx.x % g.nym, ir = blockIdx.x / g.nym;
+  const size_t n = (size_t)g.ldx * g.nym * sg.nzmr;
+  const size_t out = ((size_t)jc + (size_t)g.nym * ir) * g.ldx;
+  const int sz = __ldg(st.st[2] + ir);
+  double w[4];
+  size_t o[4];
 #pragma unroll
-    for (int c = 0; c < 4; ++c) {
-      w[c] = __ldg(st.w[2] + 4 * ir + c);
-      o[c] = off + plane * (size_t)wrapmod(sz + c, g.nzm);
-    }
-    const double *src[3] = {gx, gy, gz};
+  for (int c = 0; c < 4; ++c) {
+    w[c] = __ldg(st.w[2] + 4 * ir + c);
+    o[c] = ((size_t)jc + (size_t)g.nym * wrapmod(sz + c, g.nzm)) * g.ldx;
+  }
+  const double *src[3] = {gx, gy, gz};
+  for (int r = threadIdx.x; r < g.nxm; r += blockDim.x) {
 #pragma unroll
     for (int f = 0; f < 3; ++f)
-      tz[(size_t)f * n + e] = __ldg(src[f] + o[0]) * w[0] + __ldg(src[f] + o[1]) * w[1] + __ldg(src[f] + o[2]) * w[2] +
-                              __ldg(src[f] + o[3]) * w[3];
+      tz[(size_t)f * n + out + r] = __ldg(src[f] + o[0] + r) * w[0] + __ldg(src[f] + o[1] + r) * w[1] +
+                                    __ldg(src[f] + o[2] + r) * w[2] + __ldg(src[f] + o[3] + r) * w[3];
   }
 }
 
-constexpr int kToRefThreads = 128;
+// Warp per refined column, four columns per block, no block barriers: the y contraction of the
+// four T columns goes to the warp's shared rows, then 32-row strips are contracted in x and dvx/dx
+// is integrated by a warp scan whose total carries to the next strip.
+constexpr int kToRefWarps = 4;
 
-__global__ void __launch_bounds__(kToRefThreads, 8)
+__global__ void __launch_bounds__(32 * kToRefWarps)
     k_sal_to_ref(Geom g, SalGeom sg, SalTables st, const double *__restrict__ tz, double *__restrict__ vxr,
                  double *__restrict__ gyr, double *__restrict__ gzr) {
   extern __shared__ __align__(16) double sm_to_ref[];
   const int nxm = g.nxm, L = nxm + 4;  // extended rows -2 .. nxm+1 at 0 .. nxm+3
-  double *qx = sm_to_ref, *qy = qx + L, *qz = qy + L, *d = qz + L;
-  __shared__ double warp_tot[kToRefThreads / 32];
-  const int tid = threadIdx.x;
-  const int jr = blockIdx.x % sg.nymr, ir = blockIdx.x / sg.nymr;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int col = blockIdx.x * kToRefWarps + warp;
+  if (col >= sg.nymr * sg.nzmr) return;  // whole warps only: nothing below synchronises the block
+  double *qx = sm_to_ref + (size_t)warp * 3 * L, *qy = qx + L, *qz = qy + L;
+  const int jr = col % sg.nymr, ir = col / sg.nymr;
   const int sy = __ldg(st.st[1] + jr);
   const size_t n = (size_t)g.ldx * g.nym * sg.nzmr;
   double wy[4];
@@ -131,7 +133,7 @@ __global__ void __launch_bounds__(kToRefThreads, 8)
     wy[b] = __ldg(st.w[1] + 4 * jr + b);
     co[b] = ((size_t)wrapmod(sy + b, g.nym) + (size_t)g.nym * ir) * g.ldx;
   }
-  for (int r = tid; r < nxm; r += kToRefThreads) {
+  for (int r = lane; r < nxm; r += 32) {
     double q[3];
 #pragma unroll
     for (int f = 0; f < 3; ++f) {
@@ -142,50 +144,41 @@ __global__ void __launch_bounds__(kToRefThreads, 8)
     qy[r + 2] = q[1];
     qz[r + 2] = q[2];
   }
-  __syncthreads();
-  if (tid < 3) {
+  __syncwarp();
+  if (lane < 3) {
     // ghost rows: the wall rule (a factor +-1) commutes exactly with the y-z contraction
-    double *q = tid == 0 ? qx : (tid == 1 ? qy : qz);
+    double *q = lane == 0 ? qx : (lane == 1 ? qy : qz);
     q[0] = 0.0;
     q[1] = (double)(1 - 2 * g.inslws) * q[2];
     q[nxm + 2] = (double)(1 - 2 * g.inslwn) * q[nxm + 1];
     q[nxm + 3] = 0.0;
   }
-  __syncthreads();
+  __syncwarp();
   const size_t roff = ((size_t)jr + (size_t)sg.nymr * ir) * sg.ldr;
   const int nxmr = sg.nxmr;
-  for (int kr = tid; kr < nxmr; kr += kToRefThreads) {
-    const int p = __ldg(st.st[0] + kr) + 2;
-    const double w0 = __ldg(st.w[0] + 4 * kr), w1 = __ldg(st.w[0] + 4 * kr + 1), w2 = __ldg(st.w[0] + 4 * kr + 2),
-                 w3 = __ldg(st.w[0] + 4 * kr + 3);
-    const double vxg = qx[p] * w0 + qx[p + 1] * w1 + qx[p + 2] * w2 + qx[p + 3] * w3;
-    gyr[roff + kr] = qy[p] * w0 + qy[p + 1] * w1 + qy[p + 2] * w2 + qy[p + 3] * w3;
-    gzr[roff + kr] = qz[p] * w0 + qz[p + 1] * w1 + qz[p + 2] * w2 + qz[p + 3] * w3;
-    d[kr] = vxg * __ldg(st.lxa + kr);  // InterpVelMgrd.F90:53-54
-  }
-  __syncthreads();
-  // vxr(kr+1) = sum_{q <= kr} d(q): each thread scans a contiguous chunk, the chunk totals are
-  // scanned across the block
-  const int chunk = (nxmr + kToRefThreads - 1) / kToRefThreads;
-  const int lo = tid * chunk, hi = min(lo + chunk, nxmr);
-  double tot = 0.0;
-  for (int q = lo; q < hi; ++q) tot += d[q];
-  const int lane = tid & 31, warp = tid >> 5;
-  double incl = tot;
+  double carry = 0.0;
+  if (lane == 0) vxr[roff] = 0.0;  // InterpVelMgrd.F90:48
+  for (int k0 = 0; k0 < nxmr; k0 += 32) {
+    const int kr = k0 + lane;
+    double d = 0.0;
+    if (kr < nxmr) {
+      const int p = __ldg(st.st[0] + kr) + 2;
+      const double2 w01 = __ldg(reinterpret_cast<const double2 *>(st.w[0] + 4 * kr));
+      const double2 w23 = __ldg(reinterpret_cast<const double2 *>(st.w[0] + 4 * kr + 2));
+      const double vxg = qx[p] * w01.x + qx[p + 1] * w01.y + qx[p + 2] * w23.x + qx[p + 3] * w23.y;
+      gyr[roff + kr] = qy[p] * w01.x + qy[p + 1] * w01.y + qy[p + 2] * w23.x + qy[p + 3] * w23.y;
+      gzr[roff + kr] = qz[p] * w01.x + qz[p + 1] * w01.y + qz[p + 2] * w23.x + qz[p + 3] * w23.y;
+      d = vxg * __ldg(st.lxa + kr);  // InterpVelMgrd.F90:53-54
+    }
+    // vxr(kr+1) = vxr(kr) + d(kr): inclusive scan of the strip plus the carried total
+    double incl = d;
 #pragma unroll
-  for (int h = 1; h < 32; h <<= 1) {
-    const double o = __shfl_up_sync(0xffffffffu, incl, h);
-    if (lane >= h) incl += o;
-  }
-  if (lane == 31) warp_tot[warp] = incl;
-  __syncthreads();
-  double base = incl - tot;
-  for (int w = 0; w < warp; ++w) base += warp_tot[w];
-  double run = base;
-  if (tid == 0) vxr[roff] = 0.0;  // InterpVelMgrd.F90:48
-  for (int q = lo; q < hi; ++q) {
-    run += d[q];
-    vxr[roff + q + 1] = run;
+    for (int h = 1; h < 32; h <<= 1) {
+      const double o = __shfl_up_sync(0xffffffffu, incl, h);
+      if (lane >= h) incl += o;
+    }
+    if (kr < nxmr) vxr[roff + kr + 1] = carry + incl;
+    carry += __shfl_sync(0xffffffffu, incl, 31);
   }
 }
 
@@ -264,33 +257,37 @@ __global__ void __launch_bounds__(128)
 // Refined -> coarse interpolation of salinity (InterpSalMultigrid) in two passes, z, then y,
 // then x as HermiteInterpolations.F90:270-284:
 //   k_sal_zc         U(rr, jr, ic) = sum_c wz_c(ic) S_ext(rr, jr, sz(ic) + c) for the extended
-//                    refined rows rr = -2 .. nxmr+1 (stored at rr + 2, stride ldu), one thread
-//                    per point; the plate ghosts are formed per refined column as the reference
+//                    refined rows rr = -2 .. nxmr+1 (stored at rr + 2, stride ldu), block per
+//                    column; the plate ghosts are formed per refined column as the reference
 //                    does before its contraction (salinity.F90:462-481);
 //   k_sal_to_coarse  block per coarse column (j, i): U2(rr) = sum_b wy_b(j) U(rr, sy(j) + b, i)
 //                    in shared memory, then salc(k) = sum_a wx_a(k) U2(sx(k) + a).
 // ------------------------------------------------------------------------------------------
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(128)
     k_sal_zc(Geom g, SalGeom sg, SalTables st, const double *__restrict__ sal, double *__restrict__ u) {
-  const int ldu = sg.ldu;
-  const size_t plane = (size_t)ldu * sg.nymr;
-  const size_t n = plane * g.nzm;
-  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
-    const int q = (int)(e % ldu);
-    if (q >= sg.nxmr + 4) continue;
+  // block per output column (jr, ic): the four refined source columns, their plates and the
+  // weights are block constants
+  const int jr = blockIdx.x % sg.nymr, ic = blockIdx.x / sg.nymr;
+  const int sz = __ldg(st.st[5] + ic);
+  double w[4];
+  const double *colp[4];
+  size_t pl[4];
+#pragma unroll
+  for (int c = 0; c < 4; ++c) {
+    w[c] = __ldg(st.w[5] + 4 * ic + c);
+    pl[c] = (size_t)jr + (size_t)sg.nymr * wrapmod(sz + c, sg.nzmr);
+    colp[c] = sal + pl[c] * sg.ldr;
+  }
+  double *out = u + ((size_t)jr + (size_t)sg.nymr * ic) * sg.ldu;
+  for (int q = threadIdx.x; q < sg.nxmr + 4; q += blockDim.x) {
     const int rr = q - 2;
-    const size_t col = e / ldu;
-    const int jr = (int)(col % sg.nymr), ic = (int)(col / sg.nymr);
-    const int sz = __ldg(st.st[5] + ic);
     double v = 0.0;
 #pragma unroll
     for (int c = 0; c < 4; ++c) {
-      const size_t pl = (size_t)jr + (size_t)sg.nymr * wrapmod(sz + c, sg.nzmr);
-      const double s = sal_ext(sal + pl * sg.ldr, rr, sg.nxmr, sg.sfixs, sg.sfixn, st.salbp + pl, st.saltp + pl) *
-                       __ldg(st.w[5] + 4 * ic + c);
+      const double s = sal_ext(colp[c], rr, sg.nxmr, sg.sfixs, sg.sfixn, st.salbp + pl[c], st.saltp + pl[c]) * w[c];
       v = (c == 0) ? s : v + s;
     }
-    u[e] = v;
+    out[q] = v;
   }
 }
 
@@ -584,19 +581,19 @@ cudaError_t launch_sal_interp(const LaunchCtx &L, const SalCtx &S, const double 
   const Geom &g = L.g;
   const size_t nc = (size_t)g.ldx * g.nym * g.nzm;
   k_sal_grad<<<grid_for(nc, 256), 256, 0, L.stream>>>(g, L.t, vx, vy, vz, S.gx, S.gy, S.gz);
-  const size_t nt = (size_t)g.ldx * g.nym * S.sg.nzmr;
-  k_sal_zint<<<grid_for(nt, 256), 256, 0, L.stream>>>(g, S.sg, S.st, S.gx, S.gy, S.gz, S.tmp);
-  const size_t smem = (size_t)(3 * (g.nxm + 4) + S.sg.nxmr) * sizeof(double);
+  k_sal_zint<<<g.nym * S.sg.nzmr, 128, 0, L.stream>>>(g, S.sg, S.st, S.gx, S.gy, S.gz, S.tmp);
+  const size_t smem = (size_t)kToRefWarps * 3 * (g.nxm + 4) * sizeof(double);
   if (smem > 48 * 1024) {
     cudaError_t e = cudaFuncSetAttribute(k_sal_to_ref, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
   }
-  k_sal_to_ref<<<S.sg.nymr * S.sg.nzmr, kToRefThreads, smem, L.stream>>>(g, S.sg, S.st, S.tmp, S.vxr, S.gyr, S.gzr);
+  const int ncr = S.sg.nymr * S.sg.nzmr;
+  k_sal_to_ref<<<(ncr + kToRefWarps - 1) / kToRefWarps, 32 * kToRefWarps, smem, L.stream>>>(g, S.sg, S.st, S.tmp,
+                                                                                            S.vxr, S.gyr, S.gzr);
   const dim3 gy((S.sg.nxmr + 127) / 128, S.sg.nzmr), gz((S.sg.nxmr + 127) / 128, S.sg.nymr);
   k_sal_scan_y<<<gy, 128, 0, L.stream>>>(g, S.sg, S.st, vy, S.gyr, S.vyr);
   k_sal_scan_z<<<gz, 128, 0, L.stream>>>(g, S.sg, S.st, vz, S.gzr, S.vzr);
-  const size_t nu = (size_t)S.sg.ldu * S.sg.nymr * g.nzm;
-  k_sal_zc<<<grid_for(nu, 256), 256, 0, L.stream>>>(g, S.sg, S.st, S.sal, S.tmp);
+  k_sal_zc<<<S.sg.nymr * g.nzm, 128, 0, L.stream>>>(g, S.sg, S.st, S.sal, S.tmp);
   const size_t smc = (size_t)(S.sg.nxmr + 4) * sizeof(double);
   k_sal_to_coarse<<<g.nym * g.nzm, kToCoarseThreads, smc, L.stream>>>(g, S.sg, S.st, S.tmp, S.salc);
   return cudaGetLastError();
