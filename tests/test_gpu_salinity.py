@@ -70,6 +70,9 @@ GEOMS = [
     ((24, 32, 1), (48, 64, 1), dict()),                               # 2-D
     ((16, 12, 12), (32, 24, 36), dict(istr3r=1, str3=2.0, gaxis=3)),  # gravity along z
     ((20, 16, 8), (40, 32, 16), dict(sfixs=0, sfixn=0, inslws=0)),    # zero-flux plates, free-slip bottom
+    ((16, 12, 12), (32, 36, 36), dict(gaxis=2, inslwn=0)),              # gravity along y (faces in y)
+    ((100, 32, 1), (300, 64, 1), dict()),                             # 12 refined rows per lane, padded
+    ((200, 16, 1), (700, 32, 1), dict(istr3r=0)),                     # 24 rows per lane, general path
 ]
 
 
