@@ -260,7 +260,7 @@ __global__ void __launch_bounds__(128)
 //                    refined rows rr = -2 .. nxmr+1 (stored at rr + 2, stride ldu), block per
 //                    column; the plate ghosts are formed per refined column as the reference
 //                    does before its contraction (salinity.F90:462-481);
-//   k_sal_to_coarse  block per coarse column (j, i): U2(rr) = sum_b wy_b(j) U(rr, sy(j) + b, i)
+//   k_sal_to_coarse  warp per coarse column (j, i): U2(rr) = sum_b wy_b(j) U(rr, sy(j) + b, i)
 //                    in shared memory, then salc(k) = sum_a wx_a(k) U2(sx(k) + a).
 // ------------------------------------------------------------------------------------------
 __global__ void __launch_bounds__(128)
@@ -291,13 +291,18 @@ __global__ void __launch_bounds__(128)
   }
 }
 
-constexpr int kToCoarseThreads = 256;
+constexpr int kToCoarseWarps = 4;
 
-__global__ void __launch_bounds__(kToCoarseThreads)
+__global__ void __launch_bounds__(32 * kToCoarseWarps)
     k_sal_to_coarse(Geom g, SalGeom sg, SalTables st, const double *__restrict__ u, double *__restrict__ salc) {
+  // warp per coarse column (j, i), four per block, no block barriers
   extern __shared__ __align__(16) double sm_to_c[];
-  const int tid = threadIdx.x;
-  const int j = blockIdx.x % g.nym, i = blockIdx.x / g.nym;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int col = blockIdx.x * kToCoarseWarps + warp;
+  if (col >= g.nym * g.nzm) return;
+  const int nrows = sg.nxmr + 4;
+  double *q = sm_to_c + (size_t)warp * nrows;
+  const int j = col % g.nym, i = col / g.nym;
   const int sy = __ldg(st.st[4] + j);
   double wy[4];
   size_t co[4];
@@ -306,16 +311,16 @@ __global__ void __launch_bounds__(kToCoarseThreads)
     wy[b] = __ldg(st.w[4] + 4 * j + b);
     co[b] = ((size_t)wrapmod(sy + b, sg.nymr) + (size_t)sg.nymr * i) * sg.ldu;
   }
-  const int nrows = sg.nxmr + 4;
-  for (int q = tid; q < nrows; q += kToCoarseThreads)
-    sm_to_c[q] = __ldg(u + co[0] + q) * wy[0] + __ldg(u + co[1] + q) * wy[1] + __ldg(u + co[2] + q) * wy[2] +
-                 __ldg(u + co[3] + q) * wy[3];
-  __syncthreads();
+  for (int r = lane; r < nrows; r += 32)
+    q[r] = __ldg(u + co[0] + r) * wy[0] + __ldg(u + co[1] + r) * wy[1] + __ldg(u + co[2] + r) * wy[2] +
+           __ldg(u + co[3] + r) * wy[3];
+  __syncwarp();
   const size_t c0 = col_off(g, j, i);
-  for (int k = tid; k < g.nxm; k += kToCoarseThreads) {
+  for (int k = lane; k < g.nxm; k += 32) {
     const int p = __ldg(st.st[3] + k) + 2;
-    salc[c0 + k] = sm_to_c[p] * __ldg(st.w[3] + 4 * k) + sm_to_c[p + 1] * __ldg(st.w[3] + 4 * k + 1) +
-                   sm_to_c[p + 2] * __ldg(st.w[3] + 4 * k + 2) + sm_to_c[p + 3] * __ldg(st.w[3] + 4 * k + 3);
+    const double2 w01 = __ldg(reinterpret_cast<const double2 *>(st.w[3] + 4 * k));
+    const double2 w23 = __ldg(reinterpret_cast<const double2 *>(st.w[3] + 4 * k + 2));
+    salc[c0 + k] = q[p] * w01.x + q[p + 1] * w01.y + q[p + 2] * w23.x + q[p + 3] * w23.y;
   }
 }
 
@@ -465,18 +470,20 @@ cudaError_t launch_sal_step_M(const SalCtx &S, cudaStream_t stream, int ns) {
 __global__ void __launch_bounds__(256)
     k_sal_cfl(SalGeom sg, SalTables st, const double *__restrict__ vxr, const double *__restrict__ vyr,
               const double *__restrict__ vzr, unsigned long long *__restrict__ out) {
-  const size_t n = (size_t)sg.ldr * sg.nymr * sg.nzmr;
+  // blocks walk whole refined columns; a thread per row
+  const int ncol = sg.nymr * sg.nzmr;
   double m = 0.0;
-  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
-    const int k = (int)(e % sg.ldr);
-    if (k >= sg.nxmr) continue;
-    const size_t col = e / sg.ldr;
-    const int j = (int)(col % sg.nymr), i = (int)(col / sg.nymr);
-    const size_t ojp = ((size_t)wrap_inc(j, sg.nymr) + (size_t)sg.nymr * i) * sg.ldr + k;
-    const size_t oip = ((size_t)j + (size_t)sg.nymr * wrap_inc(i, sg.nzmr)) * sg.ldr + k;
-    const double q = fabs((vzr[e] + vzr[oip]) * 0.5 * sg.dzr) + fabs((vyr[e] + vyr[ojp]) * 0.5 * sg.dyr) +
-                     fabs((vxr[e] + vxr[e + 1]) * 0.5 * __ldg(st.udx3mr + k));
-    m = fmax(m, q);
+  for (int col = blockIdx.x; col < ncol; col += gridDim.x) {
+    const int j = col % sg.nymr, i = col / sg.nymr;
+    const size_t o = (size_t)col * sg.ldr;
+    const size_t ojp = ((size_t)wrap_inc(j, sg.nymr) + (size_t)sg.nymr * i) * sg.ldr;
+    const size_t oip = ((size_t)j + (size_t)sg.nymr * wrap_inc(i, sg.nzmr)) * sg.ldr;
+    for (int k = threadIdx.x; k < sg.nxmr; k += blockDim.x) {
+      const double q = fabs((__ldg(vzr + o + k) + __ldg(vzr + oip + k)) * 0.5 * sg.dzr) +
+                       fabs((__ldg(vyr + o + k) + __ldg(vyr + ojp + k)) * 0.5 * sg.dyr) +
+                       fabs((__ldg(vxr + o + k) + __ldg(vxr + o + k + 1)) * 0.5 * __ldg(st.udx3mr + k));
+      m = fmax(m, q);
+    }
   }
 #pragma unroll
   for (int h = 16; h > 0; h >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, h));
@@ -594,16 +601,18 @@ cudaError_t launch_sal_interp(const LaunchCtx &L, const SalCtx &S, const double 
   k_sal_scan_y<<<gy, 128, 0, L.stream>>>(g, S.sg, S.st, vy, S.gyr, S.vyr);
   k_sal_scan_z<<<gz, 128, 0, L.stream>>>(g, S.sg, S.st, vz, S.gzr, S.vzr);
   k_sal_zc<<<S.sg.nymr * g.nzm, 128, 0, L.stream>>>(g, S.sg, S.st, S.sal, S.tmp);
-  const size_t smc = (size_t)(S.sg.nxmr + 4) * sizeof(double);
-  k_sal_to_coarse<<<g.nym * g.nzm, kToCoarseThreads, smc, L.stream>>>(g, S.sg, S.st, S.tmp, S.salc);
+  const size_t smc = (size_t)kToCoarseWarps * (S.sg.nxmr + 4) * sizeof(double);
+  const int ncc = g.nym * g.nzm;
+  k_sal_to_coarse<<<(ncc + kToCoarseWarps - 1) / kToCoarseWarps, 32 * kToCoarseWarps, smc, L.stream>>>(
+      g, S.sg, S.st, S.tmp, S.salc);
   return cudaGetLastError();
 }
 
 cudaError_t launch_sal_cfl(const LaunchCtx &L, const SalCtx &S) {
   cudaError_t e = cudaMemsetAsync(S.red, 0, sizeof(unsigned long long), L.stream);
   if (e != cudaSuccess) return e;
-  const size_t n = (size_t)S.sg.ldr * S.sg.nymr * S.sg.nzmr;
-  k_sal_cfl<<<grid_for(n, 256), 256, 0, L.stream>>>(S.sg, S.st, S.vxr, S.vyr, S.vzr, S.red);
+  const int ncol = S.sg.nymr * S.sg.nzmr;
+  k_sal_cfl<<<ncol < 148 * 8 ? ncol : 148 * 8, 256, 0, L.stream>>>(S.sg, S.st, S.vxr, S.vyr, S.vzr, S.red);
   return cudaGetLastError();
 }
 
