@@ -1,6 +1,8 @@
 """Multi-resolution salinity on the host (no GPU): the oracle's two forms of the Hermite
 interpolation agree, the C++ set-up (afid_mgrd_create) reproduces the oracle's refined grid,
-coefficients and per-target stencils, and the salinity CN step reduces to the temperature CN step
+coefficients and per-target stencils, the stencils follow the Hermite formula of the reference's
+docs/interpolation.md (and reproduce quadratics), interpolating a divergence-free coarse velocity
+gives a divergence-free refined one, and the salinity CN step reduces to the temperature CN step
 when both see the same grid, diffusivity and plates.
 
 Tolerances: stencil starts and the fast/general choice are exact; grid metrics and weights 1e-14
@@ -123,3 +125,94 @@ def test_salinity_diffusion_equals_temperature_diffusion():
     for _ in range(3):
         sa.time_marcher(g, s, m, ss, 2e-3)
     assert np.array_equal(ss.sal, s.temp[..., :p.nxm])
+
+
+def _docs_hermite_weights(xo, i, xn):
+    """Weights on (f_{i-1}, f_i, f_{i+1}, f_{i+2}) of the cubic Hermite interpolant at xn with the
+    second-order finite-difference derivatives stated in the reference's docs/interpolation.md
+    (h00 = (1+2t)(1-t)^2, h10 = t(1-t)^2, h01 = t^2(3-2t), h11 = t^2(t-1);
+    f'_k = [d-^2 (f_{k+1} - f_k) + d+^2 (f_k - f_{k-1})] / (d+ d- (d+ + d-)))."""
+    d = xo[i + 1] - xo[i]
+    t = (xn - xo[i]) / d
+
+    def fprime(k):  # coefficients of f'_k on (f_{k-1}, f_k, f_{k+1})
+        dp, dm = xo[k + 1] - xo[k], xo[k] - xo[k - 1]
+        den = dp * dm * (dp + dm)
+        return np.array([-dp * dp, dp * dp - dm * dm, dm * dm]) / den
+
+    h00, h10, h01, h11 = (1 + 2 * t) * (1 - t) ** 2, t * (1 - t) ** 2, t * t * (3 - 2 * t), t * t * (t - 1)
+    w = np.zeros(4)
+    w[1] += h00
+    w[2] += h01
+    w[0:3] += d * h10 * fprime(i)
+    w[1:4] += d * h11 * fprime(i + 1)
+    return w
+
+
+@pytest.mark.parametrize("coarse,refined,extra", CASES[:3])
+def test_stencils_follow_the_documented_hermite_formula(coarse, refined, extra):
+    """Interior weights of construct_stencil equal the formula of docs/interpolation.md, and the
+    interpolation reproduces quadratics exactly (the finite-difference derivatives are exact
+    for them) on the stretched wall-normal grids."""
+    txt = _case(coarse, refined, extra)
+    g = o.create_grid(o.parse_bou_in(txt))
+    m = sa.create_mgrd(g)
+    nxm = g.p.nxm
+    xm = g.xm[:nxm]
+    xmr = m.xmr[1:m.nxmr + 1]
+    st = m.to_ref[0]
+    checked = 0
+    for kr in range(m.nxmr):
+        i = st.start[kr] + 1  # coarse interval io - 1 (0-based), sources i-1 .. i+2
+        if i - 1 < 0 or i + 2 > nxm - 1:
+            continue          # wall intervals: linear, or ghost rows
+        w = _docs_hermite_weights(xm, i, xmr[kr])
+        assert np.abs(w - st.w[:, kr]).max() < 1e-13
+        f = 0.3 + 1.7 * xm - 2.2 * xm ** 2
+        val = float(np.dot(st.w[:, kr], f[i - 1:i + 3]))
+        assert abs(val - (0.3 + 1.7 * xmr[kr] - 2.2 * xmr[kr] ** 2)) < 1e-13
+        checked += 1
+    assert checked > m.nxmr // 2
+
+
+def _divergence_free_state(g, seed=4):
+    """A coarse velocity field projected to zero discrete divergence by one oracle substep."""
+    p = g.p
+    s = o.initial_state(g, 5)
+    rng = np.random.default_rng(seed)
+    for f in ("vx", "vy", "vz"):
+        getattr(s, f)[...] = 0.05 * rng.standard_normal(s.vx.shape)
+    s.vx[..., 0] = 0.0
+    s.vx[..., -1] = 0.0
+    div = o.calc_local_divergence(g, s, 1.0, 1.0)
+    phi = o.solve_pressure_correction(g, div)
+    o.remove_divergence(g, s, phi, 1.0, 1.0)
+    assert o.check_divergence(g, s) < 1e-12
+    return s
+
+
+def refined_divergence(m, ss):
+    """Discrete divergence of (vxr, vyr, vzr) at the refined cell centres, without the periodic
+    seam rows j = nymr-1 and i = nzmr-1 (where the reference's halo copy closes the
+    integrated field)."""
+    n = m.nxmr
+    dx = (ss.vxr[..., 1:n + 1] - ss.vxr[..., :n]) * m.udx3mr
+    dy = (np.roll(ss.vyr, -1, axis=1) - ss.vyr) * m.dyr
+    dz = (np.roll(ss.vzr, -1, axis=0) - ss.vzr) * m.dzr
+    d = dx + dy + dz
+    return d[:-1, :-1] if m.nzmr > 1 else d[:, :-1]
+
+
+@pytest.mark.parametrize("coarse,refined,extra", [CASES[0], CASES[1], CASES[3]])
+def test_velocity_interpolation_keeps_divergence_free(coarse, refined, extra):
+    """docs/interpolation.md: the velocity gradients are interpolated and integrated, so a
+    divergence-free coarse field gives a divergence-free refined one (up to rounding) away from
+    the periodic seam."""
+    txt = _case(coarse, refined, extra)
+    g = o.create_grid(o.parse_bou_in(txt))
+    m = sa.create_mgrd(g)
+    s = _divergence_free_state(g)
+    ss = sa.new_sal_state(m, g, sa.initial_salinity(m, g, 1))
+    sa.interp_vel_mgrd(m, g, s, ss)
+    scale = max(np.abs(ss.vxr).max() * m.udx3mr.max(), 1e-30)
+    assert np.abs(refined_divergence(m, ss)).max() < 1e-11 * scale
