@@ -357,6 +357,7 @@ __global__ void __launch_bounds__(TPC, k1_min_blocks<CAP, TPC>())
   const size_t o_jpim = col_off(g, jp, im), o_jmip = col_off(g, jm, ip);
   // the RK3 histories go straight to registers; their loads overlap the staging copies
   double uu[RPT][4], vv[RPT][4];  // RK3 histories; {vz(j-1,i+1), vy(j+1,i-1), pr(j-1), pr(i-1)}
+  double sbv[SAL ? RPT : 1];       // salinity buoyancy bycs * salc of each row (SAL only)
 #pragma unroll
   for (int p = 0; p < RPT; ++p) {
     const int k = tc + TPC * p;
@@ -375,6 +376,7 @@ __global__ void __launch_bounds__(TPC, k1_min_blocks<CAP, TPC>())
       vv[p][3] = in ? __ldg(pr + o_im + k) : 0.0;
     }
     vv[p][2] = in ? __ldg(pr + o_jm + k) : 0.0;
+    if constexpr (SAL) sbv[p] = in ? g.bycs * __ldg(g.salc + c0 + k) : 0.0;
   }
   const bool ok = mbar_wait(&bar, 0, kSpinLimit);
   if (!__syncthreads_and(ok)) {
@@ -411,7 +413,8 @@ __global__ void __launch_bounds__(TPC, k1_min_blocks<CAP, TPC>())
       const double yd = TWO_D ? Y.jp[k] : vv[p][1];
       const double pim = TWO_D ? P.c[k] : vv[p][3];
       // salinity buoyancy bycs * salc at this row, for the gravity component (SAL: salinity on)
-      const double sb = SAL ? g.bycs * __ldg(g.salc + c0 + k) : 0.0;
+      double sb = 0.0;
+      if constexpr (SAL) sb = sbv[p];
       // all four right-hand sides from the staged columns before anything is stored
       rr[p][0] = (k >= 1) ? rhs_vx<TE, TWO_D, SAL>(g, t, sc, k, X, Y, Z, T, P, u0, q0, sb) * __ldg(TX + k - 1) : 0.0;
       rr[p][1] = rhs_vy<TE, TWO_D, SAL>(g, t, sc, k, X, Y, Z, T, P, zd, vv[p][2], u1, q1, sb) * __ldg(TY + k);
