@@ -561,3 +561,349 @@ double afid_cpu_cfl(const afid_cpu_t *c) {
   }
   return m;
 }
+
+/* ============================================================================================
+ * Multi-resolution salinity (salinity.F90, multires/InterpVelMgrd.F90, HermiteInterpolations.F90):
+ * the same routines as oracle/afid_salinity.py, on the per-target stencils of afid_mgrd_create
+ * (first source row + 4 weights per target; x sources are wall-extended columns with rows
+ * -2 .. n+1, y/z sources wrap).  Refined fields are x fastest with stride nxr = nxmr + 1.
+ * ============================================================================================ */
+typedef struct {
+  afid_cpu_t *c;
+  int nxmr, nymr, nzmr, nxr, sfixs, sfixn, active_s;
+  double dxr, dyr, dzr, pecs, bycs;
+  double *lxa, *udx3mr, *tdxr, *ap, *ac, *am, *salbp, *saltp;
+  int *st[6];
+  double *w[6];
+  double *sal, *rusal, *vxr, *vyr, *vzr, *salc, *hsal;
+  double *tz;   /* z-contracted coarse gradients, 3 x nx*nym*nzmr */
+  double *u;    /* z-contracted extended refined salinity, (nxmr+4) * nymr * nzm */
+  double *gyr, *gzr;
+} afid_cpu_sal_t;
+
+static int wrapi(int a, int n) { a %= n; return a < 0 ? a + n : a; }
+
+/* tab: xcr[nxmr+1], udx3mr, g3rmr, ap3sskr, ac3sskr, am3sskr [nxmr], salbp, saltp [nymr*nzmr];
+   dprm: dxr dyr dzr pecs bycs; iprm: nxmr nymr nzmr active_s sfixs sfixn;
+   st/w: to_ref x y z, to_coarse x y z (sizes nxmr nymr nzmr nxm nym nzm). */
+afid_cpu_sal_t *afid_cpu_sal_create(afid_cpu_t *c, const double *tab[8], const double *dprm, const int *iprm,
+                                    const int *st[6], const double *w[6]) {
+  afid_cpu_sal_t *s = (afid_cpu_sal_t *)calloc(1, sizeof(afid_cpu_sal_t));
+  s->c = c;
+  s->nxmr = iprm[0]; s->nymr = iprm[1]; s->nzmr = iprm[2]; s->active_s = iprm[3]; s->sfixs = iprm[4]; s->sfixn = iprm[5];
+  s->nxr = s->nxmr + 1;
+  s->dxr = dprm[0]; s->dyr = dprm[1]; s->dzr = dprm[2]; s->pecs = dprm[3]; s->bycs = dprm[4];
+  const int n = s->nxmr, npl = s->nymr * s->nzmr;
+  s->lxa = (double *)malloc(8 * n); s->tdxr = (double *)malloc(8 * n);
+  for (int k = 0; k < n; ++k) { s->lxa[k] = tab[0][k + 1] - tab[0][k]; s->tdxr[k] = 0.5 * s->dxr / tab[2][k]; }
+  s->udx3mr = dup(tab[1], n); s->ap = dup(tab[3], n); s->ac = dup(tab[4], n); s->am = dup(tab[5], n);
+  s->salbp = dup(tab[6], npl); s->saltp = dup(tab[7], npl);
+  const int sizes[6] = {n, s->nymr, s->nzmr, c->nxm, c->nym, c->nzm};
+  for (int d = 0; d < 6; ++d) {
+    s->st[d] = (int *)malloc(sizeof(int) * sizes[d]);
+    memcpy(s->st[d], st[d], sizeof(int) * sizes[d]);
+    s->w[d] = dup(w[d], 4 * sizes[d]);
+  }
+  const size_t nr = (size_t)s->nxr * npl, ncs = (size_t)c->nx * c->nym * c->nzm;
+  double **f[] = {&s->sal, &s->rusal, &s->vxr, &s->vyr, &s->vzr, &s->hsal, &s->gyr, &s->gzr};
+  for (size_t q = 0; q < sizeof f / sizeof f[0]; ++q) *f[q] = (double *)calloc(nr, 8);
+  s->salc = (double *)calloc(ncs, 8);
+  s->tz = (double *)calloc(3 * (size_t)c->nx * c->nym * s->nzmr, 8);
+  s->u = (double *)calloc((size_t)(n + 4) * s->nymr * c->nzm, 8);
+  return s;
+}
+
+void afid_cpu_sal_destroy(afid_cpu_sal_t *s) {
+  if (!s) return;
+  double *a[] = {s->lxa, s->tdxr, s->udx3mr, s->ap, s->ac, s->am, s->salbp, s->saltp, s->sal, s->rusal, s->vxr,
+                 s->vyr, s->vzr, s->hsal, s->gyr, s->gzr, s->salc, s->tz, s->u};
+  for (size_t q = 0; q < sizeof a / sizeof a[0]; ++q) free(a[q]);
+  for (int d = 0; d < 6; ++d) { free(s->st[d]); free(s->w[d]); }
+  free(s);
+}
+
+static size_t RIDX(const afid_cpu_sal_t *s, int k, int j, int i) { return (size_t)k + (size_t)s->nxr * ((size_t)j + (size_t)s->nymr * i); }
+
+/* wall-extended coarse row r of a column (InterpVelMgrd.F90:40-41) */
+static double cext(const double *col, int r, int nxm, double fs, double fn) {
+  if (r >= 0 && r < nxm) return col[r];
+  if (r == -1) return fs * col[0];
+  if (r == nxm) return fn * col[nxm - 1];
+  return 0.0;
+}
+/* wall-extended refined salinity row r (salinity.F90:462-481) */
+static double sext(const afid_cpu_sal_t *s, const double *col, int r, int pl) {
+  const int n = s->nxmr;
+  if (r >= 0 && r < n) return col[r];
+  if (r == -1) return s->sfixs ? 2.0 * s->salbp[pl] - col[0] : col[0];
+  if (r == n) return s->sfixn ? 2.0 * s->saltp[pl] - col[n - 1] : col[n - 1];
+  return 0.0;
+}
+
+/* InterpVelMgrd (one rank) */
+static void sal_interp_vel(afid_cpu_sal_t *s) {
+  afid_cpu_t *c = s->c;
+  const int nxm = c->nxm, nym = c->nym, nzm = c->nzm, nx = c->nx;
+  const double fs = (double)(1 - 2 * c->inslws), fn = (double)(1 - 2 * c->inslwn);
+  const size_t nt = (size_t)nx * nym * s->nzmr;
+  /* gradients at the coarse centres, contracted in z (z first) */
+#pragma omp parallel for schedule(static)
+  for (int col = 0; col < nym * s->nzmr; ++col) {
+    const int jc = col % nym, ir = col / nym;
+    const int sz = s->st[2][ir];
+    const double *wz = s->w[2] + 4 * ir;
+    for (int r = 0; r < nxm; ++r) {
+      double t[3];
+      for (int cc = 0; cc < 4; ++cc) {
+        const int ic = wrapi(sz + cc, nzm);
+        const size_t e = IDX(c, r, jc, ic);
+        const double gx = (c->vx[e + 1] - c->vx[e]) * c->udx3m[r];
+        const double gy = (c->vy[IDX(c, r, wp(jc, nym), ic)] - c->vy[e]) * c->dy;
+        const double gz = (c->vz[IDX(c, r, jc, wp(ic, nzm))] - c->vz[e]) * c->dz;
+        if (cc == 0) { t[0] = gx * wz[0]; t[1] = gy * wz[0]; t[2] = gz * wz[0]; }
+        else { t[0] += gx * wz[cc]; t[1] += gy * wz[cc]; t[2] += gz * wz[cc]; }
+      }
+      const size_t o = (size_t)r + (size_t)nx * ((size_t)jc + (size_t)nym * ir);
+      s->tz[o] = t[0]; s->tz[nt + o] = t[1]; s->tz[2 * nt + o] = t[2];
+    }
+  }
+  /* y then x per refined column; vxr integrated along x (InterpVelMgrd.F90:48-57) */
+#pragma omp parallel
+  {
+    double *q = (double *)malloc(sizeof(double) * 3 * (nxm + 4));
+#pragma omp for schedule(static)
+    for (int col = 0; col < s->nymr * s->nzmr; ++col) {
+      const int jr = col % s->nymr, ir = col / s->nymr;
+      const int sy = s->st[1][jr];
+      const double *wy = s->w[1] + 4 * jr;
+      for (int f = 0; f < 3; ++f) {
+        double *qf = q + f * (nxm + 4);
+        for (int r = 0; r < nxm; ++r) {
+          double v = 0.0;
+          for (int b = 0; b < 4; ++b) {
+            const size_t o = (size_t)r + (size_t)nx * ((size_t)wrapi(sy + b, nym) + (size_t)nym * ir);
+            v = (b == 0) ? s->tz[f * nt + o] * wy[0] : v + s->tz[f * nt + o] * wy[b];
+          }
+          qf[r + 2] = v;
+        }
+        qf[0] = 0.0; qf[1] = fs * qf[2]; qf[nxm + 2] = fn * qf[nxm + 1]; qf[nxm + 3] = 0.0;
+      }
+      const size_t R = RIDX(s, 0, jr, ir);
+      s->vxr[R] = 0.0;
+      for (int kr = 0; kr < s->nxmr; ++kr) {
+        const int p = s->st[0][kr] + 2;
+        const double *wx = s->w[0] + 4 * kr;
+        double g[3];
+        for (int f = 0; f < 3; ++f) {
+          const double *qf = q + f * (nxm + 4);
+          g[f] = qf[p] * wx[0] + qf[p + 1] * wx[1] + qf[p + 2] * wx[2] + qf[p + 3] * wx[3];
+        }
+        s->vxr[R + kr + 1] = s->vxr[R + kr] + g[0] * s->lxa[kr];
+        s->gyr[R + kr] = g[1];
+        s->gzr[R + kr] = g[2];
+      }
+    }
+    free(q);
+  }
+  /* vyr: first guess at y = 0 (z, then x), integrated along y (:99-131) */
+  const double lya = 1. / s->dyr, lza = 1. / s->dzr;
+#pragma omp parallel for schedule(static)
+  for (int ir = 0; ir < s->nzmr; ++ir) {
+    const int sz = s->st[2][ir];
+    const double *wz = s->w[2] + 4 * ir;
+    for (int kr = 0; kr < s->nxmr; ++kr) {
+      const int sx = s->st[0][kr];
+      const double *wx = s->w[0] + 4 * kr;
+      double v = 0.0;
+      for (int a = 0; a < 4; ++a) {
+        double q1 = 0.0;
+        for (int cc = 0; cc < 4; ++cc) {
+          const double e = cext(c->vy + IDX(c, 0, 0, wrapi(sz + cc, nzm)), sx + a, nxm, fs, fn) * wz[cc];
+          q1 = (cc == 0) ? e : q1 + e;
+        }
+        v = (a == 0) ? q1 * wx[a] : v + q1 * wx[a];
+      }
+      s->vyr[RIDX(s, kr, 0, ir)] = v;
+      for (int jr = 0; jr + 1 < s->nymr; ++jr) {
+        v = v + s->gyr[RIDX(s, kr, jr, ir)] * lya;
+        s->vyr[RIDX(s, kr, jr + 1, ir)] = v;
+      }
+    }
+  }
+  /* vzr: first guess at z = 0 when nzm > 1 (y, then x), integrated along z (:181-213) */
+#pragma omp parallel for schedule(static)
+  for (int jr = 0; jr < s->nymr; ++jr) {
+    const int sy = s->st[1][jr];
+    const double *wy = s->w[1] + 4 * jr;
+    for (int kr = 0; kr < s->nxmr; ++kr) {
+      const int sx = s->st[0][kr];
+      const double *wx = s->w[0] + 4 * kr;
+      double v = 0.0;
+      if (nzm > 1)
+        for (int a = 0; a < 4; ++a) {
+          double q1 = 0.0;
+          for (int b = 0; b < 4; ++b) {
+            const double e = cext(c->vz + IDX(c, 0, wrapi(sy + b, nym), 0), sx + a, nxm, fs, fn) * wy[b];
+            q1 = (b == 0) ? e : q1 + e;
+          }
+          v = (a == 0) ? q1 * wx[a] : v + q1 * wx[a];
+        }
+      s->vzr[RIDX(s, kr, jr, 0)] = v;
+      for (int ir = 0; ir + 1 < s->nzmr; ++ir) {
+        v = v + s->gzr[RIDX(s, kr, jr, ir)] * lza;
+        s->vzr[RIDX(s, kr, jr, ir + 1)] = v;
+      }
+    }
+  }
+}
+
+/* InterpSalMultigrid: z, then y, then x on the wall-extended refined salinity */
+static void sal_interp_sal(afid_cpu_sal_t *s) {
+  afid_cpu_t *c = s->c;
+  const int nxm = c->nxm, nym = c->nym, nzm = c->nzm, n = s->nxmr, L = n + 4;
+#pragma omp parallel for schedule(static)
+  for (int col = 0; col < s->nymr * nzm; ++col) {
+    const int jr = col % s->nymr, ic = col / s->nymr;
+    const int sz = s->st[5][ic];
+    const double *wz = s->w[5] + 4 * ic;
+    double *uo = s->u + (size_t)L * col;
+    for (int q = 0; q < L; ++q) {
+      double v = 0.0;
+      for (int cc = 0; cc < 4; ++cc) {
+        const int ir = wrapi(sz + cc, s->nzmr), pl = jr + s->nymr * ir;
+        const double e = sext(s, s->sal + RIDX(s, 0, jr, ir), q - 2, pl) * wz[cc];
+        v = (cc == 0) ? e : v + e;
+      }
+      uo[q] = v;
+    }
+  }
+#pragma omp parallel
+  {
+    double *q2 = (double *)malloc(sizeof(double) * L);
+#pragma omp for schedule(static)
+    for (int col = 0; col < nym * nzm; ++col) {
+      const int j = col % nym, i = col / nym;
+      const int sy = s->st[4][j];
+      const double *wy = s->w[4] + 4 * j;
+      for (int q = 0; q < L; ++q) {
+        double v = 0.0;
+        for (int b = 0; b < 4; ++b) {
+          const double e = s->u[(size_t)L * (wrapi(sy + b, s->nymr) + (size_t)s->nymr * i) + q] * wy[b];
+          v = (b == 0) ? e : v + e;
+        }
+        q2[q] = v;
+      }
+      for (int k = 0; k < nxm; ++k) {
+        const int p = s->st[3][k] + 2;
+        const double *wx = s->w[3] + 4 * k;
+        s->salc[IDX(c, k, j, i)] = q2[p] * wx[0] + q2[p + 1] * wx[1] + q2[p + 2] * wx[2] + q2[p + 3] * wx[3];
+      }
+    }
+    free(q2);
+  }
+}
+
+/* ExplicitSalinity + ImplicitSalinity + SolveImpEqnUpdate_Sal (salinity.F90:268-453) */
+static void sal_step(afid_cpu_sal_t *s, double al, double ga, double ro, double dt) {
+  const int n = s->nxmr, nymr = s->nymr, nzmr = s->nzmr;
+  const double udyr = 0.5 * s->dyr, udzr = 0.5 * s->dzr, udyrq = s->dyr * s->dyr / s->pecs,
+               udzrq = s->dzr * s->dzr / s->pecs, alpec = al / s->pecs;
+  const double *sal = s->sal, *vxr = s->vxr, *vyr = s->vyr, *vzr = s->vzr;
+  /* explicit terms from the old salinity into hsal, then the per-column update */
+#pragma omp parallel for schedule(static)
+  for (int col = 0; col < nymr * nzmr; ++col) {
+    const int j = col % nymr, i = col / nymr;
+    const size_t C = RIDX(s, 0, j, i), JP = RIDX(s, 0, wp(j, nymr), i), JM = RIDX(s, 0, wm(j, nymr), i),
+                 IP = RIDX(s, 0, j, wp(i, nzmr)), IM = RIDX(s, 0, j, wm(i, nzmr));
+    const double bp = s->salbp[col], tp = s->saltp[col];
+    for (int k = 0; k < n; ++k) {
+      const double sc = sal[C + k];
+      double hsx;
+      if (k == 0) hsx = (vxr[C + 1] * (sal[C + 1] + sc) - vxr[C] * 2.0 * bp) * s->udx3mr[k] * 0.5;
+      else if (k == n - 1) hsx = (vxr[C + k + 1] * 2.0 * tp - vxr[C + k] * (sc + sal[C + k - 1])) * s->udx3mr[k] * 0.5;
+      else hsx = (vxr[C + k + 1] * (sal[C + k + 1] + sc) - vxr[C + k] * (sc + sal[C + k - 1])) * s->udx3mr[k] * 0.5;
+      const double hsy = (vyr[JP + k] * (sal[JP + k] + sc) - vyr[C + k] * (sc + sal[JM + k])) * udyr;
+      const double hsz = (vzr[IP + k] * (sal[IP + k] + sc) - vzr[C + k] * (sc + sal[IM + k])) * udzr;
+      const double dyys = (sal[JP + k] - 2.0 * sc + sal[JM + k]) * udyrq;
+      const double dzzs = (sal[IP + k] - 2.0 * sc + sal[IM + k]) * udzrq;
+      s->hsal[C + k] = -(hsx + hsy + hsz) + dyys + dzzs;
+    }
+  }
+  cnmat ms;
+  cn_build(&ms, n, 0, s->am, s->ac, s->ap, 0.5 * al * dt / s->pecs, 0);
+#pragma omp parallel
+  {
+    double *rhs = (double *)malloc(sizeof(double) * (n + 1));
+#pragma omp for schedule(static)
+    for (int col = 0; col < nymr * nzmr; ++col) {
+      const size_t C = RIDX(s, 0, col % nymr, col / nymr);
+      const double bp = s->salbp[col], tp = s->saltp[col];
+      double *sl = s->sal + C;
+      for (int k = 0; k < n; ++k) {
+        double dxx;
+        if (k == 0) dxx = sl[1] * s->ap[0] + sl[0] * s->ac[0] - (s->ap[0] + s->ac[0]) * bp * s->sfixs;
+        else if (k == n - 1) dxx = sl[k] * s->ac[k] + sl[k - 1] * s->am[k] - (s->am[k] + s->ac[k]) * tp * s->sfixn;
+        else dxx = sl[k + 1] * s->ap[k] + sl[k] * s->ac[k] + sl[k - 1] * s->am[k];
+        rhs[k] = (ga * s->hsal[C + k] + ro * s->rusal[C + k] + alpec * dxx) * dt * ms.sc[k];
+        s->rusal[C + k] = s->hsal[C + k];
+      }
+      gttrs_r(n, ms.dl, ms.d, ms.du, ms.du2, ms.ipiv, rhs);
+      for (int k = 0; k < n; ++k) sl[k] += rhs[k];
+    }
+    free(rhs);
+  }
+  cn_free(&ms);
+}
+
+void afid_cpu_sal_set(afid_cpu_sal_t *s, const double *sal) {
+  memcpy(s->sal, sal, sizeof(double) * (size_t)s->nxr * s->nymr * s->nzmr);
+  memset(s->rusal, 0, sizeof(double) * (size_t)s->nxr * s->nymr * s->nzmr);
+  sal_interp_vel(s);
+  sal_interp_sal(s);
+}
+void afid_cpu_sal_get(const afid_cpu_sal_t *s, double *sal) {
+  memcpy(sal, s->sal, sizeof(double) * (size_t)s->nxr * s->nymr * s->nzmr);
+}
+
+/* TimeMarcher.F90:28-150 with salinity */
+void afid_cpu_timemarcher_sal(afid_cpu_sal_t *s, double dt) {
+  afid_cpu_t *c = s->c;
+  double gam[3], rom[3];
+  if (c->nsst > 1) { gam[0] = 8.0 / 15.0; gam[1] = 5.0 / 12.0; gam[2] = 3.0 / 4.0; rom[0] = 0.0; rom[1] = -17.0 / 60.0; rom[2] = -5.0 / 12.0; }
+  else { gam[0] = 1.5; gam[1] = 0.0; gam[2] = 0.0; rom[0] = -0.5; rom[1] = 0.0; rom[2] = 0.0; }
+  const double beta = dt / c->ren * 0.5;
+  const int ns_n = c->nsst > 1 ? 3 : 1;
+  const size_t nc = (size_t)c->nx * c->nym * c->nzm;
+  for (int ns = 0; ns < ns_n; ++ns) {
+    const double al = gam[ns] + rom[ns];
+    explicit_terms(c);
+    if (s->active_s == 1) { /* AddSalBuoyancy (salinity.F90:494-506) */
+      double *tgt = c->gaxis == 1 ? c->qcap : (c->gaxis == 2 ? c->dph : c->dq);
+#pragma omp parallel for schedule(static)
+      for (size_t e = 0; e < nc; ++e)
+        if ((int)(e % c->nx) < c->nxm) tgt[e] = tgt[e] - s->bycs * s->salc[e];
+    }
+    sal_step(s, al, gam[ns], rom[ns], dt);
+    implicit_update(c, al, gam[ns], rom[ns], dt, beta);
+    pressure(c, al, dt, beta);
+    sal_interp_vel(s);
+    sal_interp_sal(s);
+  }
+}
+
+/* CalcMaxCFL.F90:48-65 (refined grid) */
+double afid_cpu_sal_cfl(const afid_cpu_sal_t *s) {
+  double m = 1.0e-8;
+#pragma omp parallel for reduction(max : m) schedule(static)
+  for (int col = 0; col < s->nymr * s->nzmr; ++col) {
+    const int j = col % s->nymr, i = col / s->nymr;
+    const size_t C = RIDX(s, 0, j, i), JP = RIDX(s, 0, wp(j, s->nymr), i), IP = RIDX(s, 0, j, wp(i, s->nzmr));
+    for (int k = 0; k < s->nxmr; ++k) {
+      const double q = fabs((s->vzr[C + k] + s->vzr[IP + k]) * 0.5 * s->dzr) +
+                       fabs((s->vyr[C + k] + s->vyr[JP + k]) * 0.5 * s->dyr) +
+                       fabs((s->vxr[C + k] + s->vxr[C + k + 1]) * 0.5 * s->udx3mr[k]);
+      if (q > m) m = q;
+    }
+  }
+  return m;
+}

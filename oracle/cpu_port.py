@@ -113,3 +113,97 @@ def time_steps(bou_text: str, steps: int, seed: int = 20261203, mixed: bool = Fa
     cpu.close()
     return {"seconds": sec, "steps": done, "mcells_per_s": cells * done / sec / 1e6,
             "threads": lib().afid_cpu_threads()}
+
+
+def _sal_lib():
+    L = lib()
+    if not hasattr(L, "_sal_ready"):
+        L.afid_cpu_sal_create.restype = C.c_void_p
+        L.afid_cpu_sal_create.argtypes = [C.c_void_p, C.POINTER(C.c_void_p), C.POINTER(C.c_double),
+                                          C.POINTER(C.c_int), C.POINTER(C.c_void_p), C.POINTER(C.c_void_p)]
+        L.afid_cpu_sal_destroy.argtypes = [C.c_void_p]
+        L.afid_cpu_sal_set.argtypes = [C.c_void_p, C.c_void_p]
+        L.afid_cpu_sal_get.argtypes = [C.c_void_p, C.c_void_p]
+        L.afid_cpu_timemarcher_sal.argtypes = [C.c_void_p, C.c_double]
+        L.afid_cpu_sal_cfl.restype = C.c_double
+        L.afid_cpu_sal_cfl.argtypes = [C.c_void_p]
+        L._sal_ready = True
+    return L
+
+
+class CpuSalSolver:
+    """The C restatement with the multi-resolution salinity scalar, on the oracle's refined grid
+    and per-target stencils (``oracle.afid_salinity.Mgrd``)."""
+
+    def __init__(self, g: o.Grid, s: o.State, m, sal: np.ndarray):
+        self.flow = CpuSolver(g, s)
+        self.m = m
+        nxr = m.nxmr + 1
+        planes = np.full((m.nzmr, m.nymr), 1.0)
+        self._keep = [np.ascontiguousarray(m.xcr), np.ascontiguousarray(m.udx3mr), np.ascontiguousarray(m.g3rmr),
+                      np.ascontiguousarray(m.ap3sskr), np.ascontiguousarray(m.ac3sskr),
+                      np.ascontiguousarray(m.am3sskr), (planes * m.salbp).ravel(), (planes * m.saltp).ravel()]
+        tabs = (C.c_void_p * 8)(*[a.ctypes.data for a in self._keep])
+        dprm = (C.c_double * 5)(m.dxr, m.dyr, m.dzr, m.pecs, m.bycs)
+        iprm = (C.c_int * 6)(m.nxmr, m.nymr, m.nzmr, m.active_s, m.sfixs, m.sfixn)
+        sts = list(m.to_ref) + list(m.to_coarse)
+        self._st = [np.ascontiguousarray(t.start, dtype=np.int32) for t in sts]
+        self._w = [np.ascontiguousarray(t.w.T) for t in sts]  # [target][4]
+        stp = (C.c_void_p * 6)(*[a.ctypes.data for a in self._st])
+        wp = (C.c_void_p * 6)(*[a.ctypes.data for a in self._w])
+        self._h = _sal_lib().afid_cpu_sal_create(self.flow._h, tabs, dprm, iprm, stp, wp)
+        full = np.zeros((m.nzmr, m.nymr, nxr))
+        full[..., :m.nxmr] = sal
+        _sal_lib().afid_cpu_sal_set(self._h, full.ctypes.data)
+
+    def time_marcher(self, dt):
+        _sal_lib().afid_cpu_timemarcher_sal(self._h, dt)
+
+    def cfl(self):
+        return _sal_lib().afid_cpu_sal_cfl(self._h)
+
+    def sal(self):
+        m = self.m
+        a = np.zeros((m.nzmr, m.nymr, m.nxmr + 1))
+        _sal_lib().afid_cpu_sal_get(self._h, a.ctypes.data)
+        return a[..., :m.nxmr]
+
+    def get(self):
+        return self.flow.get()
+
+    def close(self):
+        if self._h:
+            _sal_lib().afid_cpu_sal_destroy(self._h)
+            self._h = None
+        self.flow.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def time_steps_sal(bou_text: str, steps: int, seed: int = 20261203, budget_s: float = 1e30) -> dict:
+    """Main-loop steps with salinity (CFLmr -> dt rule -> TimeMarcher) of the C restatement on all
+    host cores from the seeded temperature and the reference's initial salinity."""
+    from oracle import afid_salinity as sa
+    p = o.parse_bou_in(bou_text)
+    g = o.create_grid(p)
+    m = sa.create_mgrd(g)
+    s = o.initial_state(g, seed)
+    cpu = CpuSalSolver(g, s, m, sa.initial_salinity(m, g, seed + 1))
+    dt = p.dt
+    t0 = time.perf_counter()
+    done = 0
+    for n in range(steps):
+        dt, _, _ = o.next_dt(p, n, dt, cpu.cfl())
+        cpu.time_marcher(dt)
+        done += 1
+        if time.perf_counter() - t0 > budget_s:
+            break
+    sec = time.perf_counter() - t0
+    cells = p.nxm * p.nym * p.nzm
+    cpu.close()
+    return {"seconds": sec, "steps": done, "mcells_per_s": cells * done / sec / 1e6,
+            "threads": lib().afid_cpu_threads()}

@@ -216,3 +216,36 @@ def test_velocity_interpolation_keeps_divergence_free(coarse, refined, extra):
     sa.interp_vel_mgrd(m, g, s, ss)
     scale = max(np.abs(ss.vxr).max() * m.udx3mr.max(), 1e-30)
     assert np.abs(refined_divergence(m, ss)).max() < 1e-11 * scale
+
+
+@pytest.mark.parametrize("coarse,refined,extra", [CASES[0], CASES[1], CASES[3], CASES[5]])
+def test_c_restatement_matches_numpy_oracle(coarse, refined, extra):
+    """The C + OpenMP restatement of the salinity path (the timed CPU baseline of the ddc3d
+    workload) against the NumPy oracle: refined CFL and all fields after 3 RK3 steps, 1e-13."""
+    from oracle import cpu_port
+    txt = _case(coarse, refined, extra, rayt=1e6, dt=1e-3)
+    g = o.create_grid(o.parse_bou_in(txt))
+    m = sa.create_mgrd(g)
+    s = o.initial_state(g, 5)
+    rng = np.random.default_rng(1)
+    for f in ("vx", "vy", "vz"):
+        getattr(s, f)[...] = 0.05 * rng.standard_normal(s.vx.shape)
+    s.vx[..., 0] = 0.0
+    s.vx[..., -1] = 0.0
+    for f in ("vy", "vz", "temp", "pr"):
+        getattr(s, f)[..., -1] = 0.0
+    sal = np.clip(sa.initial_salinity(m, g, 3) + 0.01 * rng.standard_normal((m.nzmr, m.nymr, m.nxmr)), -0.5, 0.5)
+    cpu = cpu_port.CpuSalSolver(g, s.copy(), m, sal)
+    ss = sa.new_sal_state(m, g, sal)
+    sa.interp_vel_mgrd(m, g, s, ss)
+    sa.interp_sal_multigrid(m, g, ss)
+    assert abs(cpu.cfl() - sa.calc_max_cfl_refined(m, ss)) < 1e-13 * sa.calc_max_cfl_refined(m, ss)
+    for _ in range(3):
+        cpu.time_marcher(1e-3)
+        sa.time_marcher(g, s, m, ss, 1e-3)
+    out = cpu.get()
+    for f in ("vx", "vy", "vz", "temp"):
+        ref = getattr(s, f)
+        assert np.linalg.norm(out[f] - ref) <= 1e-13 * np.linalg.norm(ref), f
+    assert np.linalg.norm(cpu.sal() - ss.sal) <= 1e-13 * np.linalg.norm(ss.sal)
+    cpu.close()
