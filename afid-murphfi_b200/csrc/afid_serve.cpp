@@ -64,6 +64,9 @@ struct Pool {
   long long bytes = 0;
   long long cells_per_slot = 0;
   bool dirty = false;  // active flags changed since the last upload
+  cudaEvent_t ev = nullptr;  // recorded after the pool's last chunk
+  bool in_flight = false;    // a chunk is queued or running on the pool's stream
+  long long launched = 0;    // pump launch order of that chunk
   int busy() const { return (int)std::count_if(job.begin(), job.end(), [](int j) { return j >= 0; }); }
 };
 
@@ -81,6 +84,7 @@ struct afid_server {
   long long cells_in_flight = 0;
   long long cell_steps_done = 0;
   long long jobs_done = 0;
+  long long launches = 0;  // chunks launched
   std::vector<afid_batch_stat_t> st;
   std::vector<double> nu, ke;
 };
@@ -99,7 +103,9 @@ long long pool_bytes(const afid_server_t *s) {
 
 void drop_pool(afid_server_t *s, size_t i) {
   Pool *p = s->pools[i];
+  if (p->stream) cudaStreamSynchronize(p->stream);
   afid_batch_destroy(p->b);
+  if (p->ev) cudaEventDestroy(p->ev);
   if (p->stream) cudaStreamDestroy(p->stream);
   delete p;
   s->pools.erase(s->pools.begin() + (long)i);
@@ -134,8 +140,10 @@ int new_pool(afid_server_t *s, const afid_input_t &in, Pool **out) {
     drop_pool(s, victim);
   }
   if (cudaStreamCreateWithFlags(&p->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&p->ev, cudaEventDisableTiming) != cudaSuccess ||
       afid_batch_set_stream(p->b, p->stream) != AFID_OK) {
     afid_batch_destroy(p->b);
+    if (p->ev) cudaEventDestroy(p->ev);
     if (p->stream) cudaStreamDestroy(p->stream);
     delete p;
     return AFID_E_CUDA;
@@ -149,21 +157,30 @@ int new_pool(afid_server_t *s, const afid_input_t &in, Pool **out) {
   return AFID_OK;
 }
 
-// Place job j into a free slot of its class (creating a pool if needed).
+// Place job j into a free slot of its class (creating a pool if needed).  A pool whose chunk is
+// still in flight takes no job (its slot set-up would wait for the chunk); kBusyPool
+// then keeps the job queued until that pool is harvested.
+constexpr int kBusyPool = -1;
 int admit(afid_server_t *s, Job &j) {
   const ClassKey k = key_of(j.spec.in);
   Pool *pool = nullptr;
   int slot = -1;
+  bool waiting = false;
   for (Pool *p : s->pools) {
     if (!(p->key == k)) continue;
     for (int i = 0; i < p->nslots; ++i)
       if (p->job[i] < 0) {
+        if (p->in_flight) {
+          waiting = true;
+          break;
+        }
         pool = p;
         slot = i;
         break;
       }
     if (pool) break;
   }
+  if (!pool && waiting) return kBusyPool;
   if (!pool) {
     int st = new_pool(s, j.spec.in, &pool);
     if (st != AFID_OK) return st;
@@ -187,6 +204,51 @@ int admit(afid_server_t *s, Job &j) {
   pool->active[slot] = 1;
   pool->dirty = true;
   s->cells_in_flight += j.cells;
+  return AFID_OK;
+}
+
+// Harvest one pool whose chunk has completed: results of the slots that reached their step
+// count or stopped on an error code.
+int harvest(afid_server_t *s, Pool *p) {
+  p->in_flight = false;
+  if (p->busy() == 0) return AFID_OK;
+  s->st.resize(p->nslots);
+  s->nu.resize(p->nslots);
+  s->ke.resize(p->nslots);
+  int st = afid_batch_stats(p->b, s->st.data(), s->nu.data(), s->ke.data());
+  if (st != AFID_OK) return st;
+  for (int i = 0; i < p->nslots; ++i) {
+    const int idx = p->job[i];
+    if (idx < 0) continue;
+    Job &j = s->running[idx];
+    const afid_batch_stat_t &x = s->st[i];
+    if (x.ntime < j.spec.nsteps && x.errorcode == 0) continue;
+    if (j.spec.temp_out) {
+      const int nx = j.spec.in.nxm + 1;
+      st = afid_batch_download(p->b, i, nullptr, nullptr, nullptr, j.spec.temp_out, nullptr, nx, j.spec.in.nym);
+      if (st != AFID_OK) return st;
+    }
+    afid_serve_result_t r{};
+    r.tag = j.spec.tag;
+    r.errorcode = x.errorcode;
+    r.steps_done = x.ntime;
+    r.time = x.time;
+    r.dt = x.dt;
+    r.cfl = x.cfl;
+    r.nu_vol = s->nu[i];
+    r.ke = s->ke[i];
+    r.t_submit = j.t_submit;
+    r.t_admit = j.t_admit;
+    r.t_done = now_s(s);
+    s->done.push_back(r);
+    s->cells_in_flight -= j.cells;
+    s->cell_steps_done += j.cells * (long long)x.ntime;
+    s->jobs_done += 1;
+    p->job[i] = -1;
+    p->active[i] = 0;
+    p->dirty = true;
+    s->free_running.push_back(idx);
+  }
   return AFID_OK;
 }
 
@@ -227,9 +289,25 @@ int afid_serve_submit(afid_server_t *s, const afid_serve_job_t *job) {
   return AFID_OK;
 }
 
+// One pass of the request loop, asynchronous per pool: pools whose chunk has completed are
+// harvested, queued jobs are admitted into pools that are not running, and every idle pool with
+// jobs gets its next chunk (each pool on its own stream, so a pool of small jobs does not wait
+// for a pool of large ones).  When a pass finds nothing to do it waits for the oldest running
+// chunk instead of spinning.
 int afid_serve_pump(afid_server_t *s) {
   if (!s) return AFID_E_INVALID;
-  // 1. admission in policy order
+  bool progress = false;
+  // 1. harvest the pools whose chunk completed
+  for (Pool *p : s->pools) {
+    if (!p->in_flight) continue;
+    const cudaError_t q = cudaEventQuery(p->ev);
+    if (q == cudaErrorNotReady) continue;
+    if (q != cudaSuccess) return AFID_E_CUDA;
+    const int st = harvest(s, p);
+    if (st != AFID_OK) return st;
+    progress = true;
+  }
+  // 2. admission in policy order
   std::vector<size_t> order(s->queue.size());
   for (size_t i = 0; i < order.size(); ++i) order[i] = i;
   const bool fifo = s->cfg.policy != AFID_SERVE_SHORTEST_FIRST;
@@ -246,6 +324,10 @@ int afid_serve_pump(afid_server_t *s) {
       continue;
     }
     const int st = admit(s, j);
+    if (st == kBusyPool) {  // its class's pool is running a chunk: retry after the harvest
+      if (fifo) break;
+      continue;
+    }
     const bool no_room = (st == AFID_E_CAPACITY || st == AFID_E_ALLOC);
     if (no_room && !s->pools.empty()) {  // wait for running jobs to release memory
       if (fifo) break;
@@ -261,15 +343,15 @@ int afid_serve_pump(afid_server_t *s) {
       s->done.push_back(r);
     }
     taken[q] = 1;
+    progress = true;
   }
   std::deque<Job> rest;
   for (size_t i = 0; i < s->queue.size(); ++i)
     if (!taken[i]) rest.push_back(s->queue[i]);
   s->queue.swap(rest);
-
-  // 2. one chunk of steps on every pool with running jobs (each pool on its own stream)
+  // 3. next chunk on every idle pool with running jobs
   for (Pool *p : s->pools) {
-    if (p->busy() == 0) continue;
+    if (p->in_flight || p->busy() == 0) continue;
     int st = AFID_OK;
     if (p->dirty) {
       st = afid_batch_set_active(p->b, p->active.data());
@@ -277,47 +359,19 @@ int afid_serve_pump(afid_server_t *s) {
     }
     if (st == AFID_OK) st = afid_batch_step(p->b, s->cfg.chunk_steps);
     if (st != AFID_OK) return st;
+    if (cudaEventRecord(p->ev, p->stream) != cudaSuccess) return AFID_E_CUDA;
+    p->in_flight = true;
+    p->launched = s->launches++;
+    progress = true;
   }
-
-  // 3. harvest the slots that reached their step count or stopped on an error code
-  for (Pool *p : s->pools) {
-    if (p->busy() == 0) continue;
-    s->st.resize(p->nslots);
-    s->nu.resize(p->nslots);
-    s->ke.resize(p->nslots);
-    int st = afid_batch_stats(p->b, s->st.data(), s->nu.data(), s->ke.data());
-    if (st != AFID_OK) return st;
-    for (int i = 0; i < p->nslots; ++i) {
-      const int idx = p->job[i];
-      if (idx < 0) continue;
-      Job &j = s->running[idx];
-      const afid_batch_stat_t &x = s->st[i];
-      if (x.ntime < j.spec.nsteps && x.errorcode == 0) continue;
-      if (j.spec.temp_out) {
-        const int nx = j.spec.in.nxm + 1;
-        st = afid_batch_download(p->b, i, nullptr, nullptr, nullptr, j.spec.temp_out, nullptr, nx, j.spec.in.nym);
-        if (st != AFID_OK) return st;
-      }
-      afid_serve_result_t r{};
-      r.tag = j.spec.tag;
-      r.errorcode = x.errorcode;
-      r.steps_done = x.ntime;
-      r.time = x.time;
-      r.dt = x.dt;
-      r.cfl = x.cfl;
-      r.nu_vol = s->nu[i];
-      r.ke = s->ke[i];
-      r.t_submit = j.t_submit;
-      r.t_admit = j.t_admit;
-      r.t_done = now_s(s);
-      s->done.push_back(r);
-      s->cells_in_flight -= j.cells;
-      s->cell_steps_done += j.cells * (long long)x.ntime;
-      s->jobs_done += 1;
-      p->job[i] = -1;
-      p->active[i] = 0;
-      p->dirty = true;
-      s->free_running.push_back(idx);
+  // 4. nothing happened: wait for the oldest running chunk
+  if (!progress) {
+    Pool *oldest = nullptr;
+    for (Pool *p : s->pools)
+      if (p->in_flight && (!oldest || p->launched < oldest->launched)) oldest = p;
+    if (oldest) {
+      if (cudaEventSynchronize(oldest->ev) != cudaSuccess) return AFID_E_CUDA;
+      return harvest(s, oldest);
     }
   }
   return AFID_OK;
