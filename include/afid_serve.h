@@ -14,9 +14,11 @@
  * make room), and, if max_cells_in_flight > 0, when the resident cells of running jobs stay
  * under that cap.  Queue order is FIFO, or shortest job (cells x steps) first.
  *
- * The caller drives the loop: afid_serve_submit as jobs arrive, afid_serve_pump to admit,
- * advance every pool by chunk_steps and harvest, afid_serve_poll for completed results.  One
- * host thread per server; the reference has no served mode (main.F90 runs one job).
+ * The caller drives the loop: afid_serve_submit as jobs arrive, afid_serve_pump to harvest the
+ * pools whose last chunk of chunk_steps has completed, admit queued jobs into pools that are not
+ * running, and start the next chunk on every idle pool with jobs (each pool on its own stream;
+ * a pump with nothing to do waits for the oldest running chunk), afid_serve_poll for completed
+ * results.  One host thread per server; the reference has no served mode (main.F90 runs one job).
  */
 #ifndef AFID_SERVE_H
 #define AFID_SERVE_H
@@ -72,7 +74,7 @@ int afid_serve_destroy(afid_server_t *s);
 /* Queue a job (AFID_E_INVALID if malformed).  A job that can never run comes back as a result
  * with its status in errorcode. */
 int afid_serve_submit(afid_server_t *s, const afid_serve_job_t *job);
-/* Admit queued jobs, advance every pool with running jobs by chunk_steps, harvest completions. */
+/* Harvest completed chunks, admit queued jobs, start the next chunk on idle pools with jobs. */
 int afid_serve_pump(afid_server_t *s);
 /* Move up to `max` completed results into out[]; *n = how many. */
 int afid_serve_poll(afid_server_t *s, afid_serve_result_t *out, int max, int *n);
