@@ -204,6 +204,7 @@ def run_gpu(args):
 
     dt_box = [inp.dt]
     dtc = ctypes.c_double()
+    dts = []  # dt of every step before the end-to-end run (replayed by the FP64 accuracy check)
 
     def step(ntime: int):
         cflm = solver.calc_max_cfl()
@@ -211,6 +212,7 @@ def run_gpu(args):
         err = ag.lib().afid_next_dt(ctypes.byref(inp), ntime, ctypes.byref(dtc), cflm, None)
         dt_box[0] = dtc.value
         solver.time_marcher(dt_box[0], ntime)
+        dts.append(dt_box[0])
         return err
 
     # ---- device-resident throughput ---------------------------------------------------------
@@ -250,6 +252,11 @@ def run_gpu(args):
     k1_bytes = K1_BYTES_PER_CELL[w["precision"]] * cells
     achieved = k1_bytes / k1_avg_s / 1e9
     traffic = committed_traffic(w["name"])
+
+    # ---- mixed precision: fields and Nu against an FP64 run with the same dt sequence --------
+    accuracy = None
+    if w["precision"] == 1 and not args.no_nu_check:
+        accuracy = mixed_vs_fp64(ag, w, inp, solver, temp0, list(dts), ra_pr)
 
     # ---- end to end through the C ABI with host buffers -----------------------------------
     pin = lambda: torch.empty((nzm, nym, nx), dtype=torch.float64, pin_memory=True).numpy()  # noqa: E731
@@ -325,10 +332,43 @@ def run_gpu(args):
             "nu_vol_end": nu,
             "cpu_baseline": cpu,
         }
+        if accuracy is not None:
+            line["accuracy_vs_fp64"] = accuracy
         print(json.dumps(line), flush=True)
     if world > 1:
         import torch.distributed as dist
         dist.destroy_process_group()
+
+
+def mixed_vs_fp64(ag, w, inp, solver, temp0, dts, ra_pr):
+    """Per-field relative L2 (pressure modulo its mean) and the Nusselt-number error of the
+    mixed-precision state after len(dts) steps against an FP64 solver advanced from the same
+    initial state with the same dt sequence (the configs[2] accuracy gate: Nu within 0.5%)."""
+    import numpy as np
+    got = solver.download()
+    nu_mx, _, _ = solver.global_quantities(ra_pr)
+    t64 = ag.Tables(inp, ag.PREC_FP64)
+    ref = ag.Solver(t64.grid, t64.params)
+    nx, nym, nzm = w["nxm"] + 1, w["nym"], w["nzm"]
+    zeros = np.zeros((nzm, nym, nx))
+    ref.upload(zeros, zeros, zeros, temp0, zeros)
+    for n, dt in enumerate(dts):
+        ref.time_marcher(dt, n)
+    exp = ref.download()
+    nu_64, _, _ = ref.global_quantities(ra_pr)
+    ref.close()
+    t64.close()
+    nxm = w["nxm"]
+
+    def rel(a, b):
+        return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+    out = {f: rel(got[f], exp[f]) for f in ("vx", "vy", "vz", "temp")}
+    pa, pb = got["pr"][..., :nxm], exp["pr"][..., :nxm]
+    out["pr_mod_mean"] = rel(pa - pa.mean(), pb - pb.mean())
+    return {"steps": len(dts), "rel_l2": out, "nu_vol_mixed": nu_mx, "nu_vol_fp64": nu_64,
+            "nu_rel_err": abs(nu_mx - nu_64) / abs(nu_64),
+            "note": "Nu - 1 is the signal while the flow is still near conduction: see nu_minus_1_rel_err",
+            "nu_minus_1_rel_err": abs(nu_mx - nu_64) / max(abs(nu_64 - 1.0), 1e-300)}
 
 
 # ---- batched sweep: independent 2-D instances of four size classes ------------------------
