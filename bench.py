@@ -291,8 +291,12 @@ def run_gpu(args):
     d2h = field_bytes / args.steps + 8 + 3 * 8
 
     cpu = None
+    parity = None
     if rank == 0 and not args.no_cpu_baseline:
-        cpu = cpu_baseline(w, args.cpu_steps)
+        cpu = cpu_baseline(w, args.cpu_steps, keep_state=w["precision"] == 0)
+        if "_state" in cpu:
+            solver.close()  # room for the replay
+            parity = parity_vs_cpu(ag, w, inp, temp0, cpu)
 
     solver.close()
     tables.close()
@@ -334,6 +338,8 @@ def run_gpu(args):
         }
         if accuracy is not None:
             line["accuracy_vs_fp64"] = accuracy
+        if parity is not None:
+            line["parity_vs_cpu_port"] = parity
         print(json.dumps(line), flush=True)
     if world > 1:
         import torch.distributed as dist
@@ -870,20 +876,50 @@ def run_ddc(args):
         dist.destroy_process_group()
 
 
-def cpu_baseline(w: dict, steps: int, budget_s: float = 60.0):
+def cpu_baseline(w: dict, steps: int, budget_s: float = 60.0, keep_state: bool = False):
     """The CPU restatement (C + OpenMP, oracle/afid_cpu.c) on the same workload: up to
-    ``steps`` full main-loop steps, stopping once ``budget_s`` seconds have been spent."""
+    ``steps`` full main-loop steps, stopping once ``budget_s`` seconds have been spent.  With
+    ``keep_state`` the final fields and dt sequence come back under "_state" / "_dts"."""
     try:
         sys.path.insert(0, os.path.join(ROOT, "oracle"))
         from oracle import cpu_port
     except Exception as e:  # pragma: no cover
         return {"unavailable": f"CPU port not importable: {e}"}
     text = bou_text(w, steps)
-    res = cpu_port.time_steps(text, steps, seed=20261203, mixed=False, budget_s=budget_s)
-    return {"value": round(res["mcells_per_s"], 4), "unit": "Mcell-RK3-steps/s",
-            "cores": res["threads"], "kind": "port",
-            "sample": f"{res['steps']} full steps of {w['name']} (C+OpenMP restatement)",
-            "steps": res["steps"], "seconds": round(res["seconds"], 2)}
+    res = cpu_port.time_steps(text, steps, seed=20261203, mixed=False, budget_s=budget_s, keep_state=keep_state)
+    out = {"value": round(res["mcells_per_s"], 4), "unit": "Mcell-RK3-steps/s",
+           "cores": res["threads"], "kind": "port",
+           "sample": f"{res['steps']} full steps of {w['name']} (C+OpenMP restatement)",
+           "steps": res["steps"], "seconds": round(res["seconds"], 2)}
+    if keep_state:
+        out["_state"], out["_dts"] = res["state"], res["dts"]
+    return out
+
+
+def parity_vs_cpu(ag, w, inp, temp0, cpu):
+    """configs[1] fields at full size: the GPU path replays the C restatement's dt sequence from
+    the same initial state; relative L2 per field (pressure modulo its mean)."""
+    import numpy as np
+    state, dts = cpu.pop("_state"), cpu.pop("_dts")
+    t = ag.Tables(inp, w["precision"])
+    sv = ag.Solver(t.grid, t.params)
+    nx, nym, nzm = w["nxm"] + 1, w["nym"], w["nzm"]
+    zeros = np.zeros((nzm, nym, nx))
+    sv.upload(zeros, zeros, zeros, temp0, zeros)
+    for n, dt in enumerate(dts):
+        sv.time_marcher(dt, n)
+    got = sv.download()
+    sv.close()
+    t.close()
+
+    def rel(a, b):
+        return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+    nxm = w["nxm"]
+    out = {f: rel(got[f], state[f]) for f in ("vx", "vy", "vz", "temp")}
+    pa, pb = got["pr"][..., :nxm], state["pr"][..., :nxm]
+    out["pr_mod_mean"] = rel(pa - pa.mean(), pb - pb.mean())
+    return {"steps": len(dts), "rel_l2": out, "tolerance": 1e-10,
+            "against": "C + OpenMP restatement (oracle/afid_cpu.c), same initial state and dt sequence"}
 
 
 def run_reference(args):

@@ -90,10 +90,11 @@ class CpuSolver:
 
 
 def time_steps(bou_text: str, steps: int, seed: int = 20261203, mixed: bool = False,
-               budget_s: float = 1e30) -> dict:
+               budget_s: float = 1e30, keep_state: bool = False) -> dict:
     """Main-loop steps (CFL -> dt rule -> TimeMarcher) of the C restatement on all host cores,
     from the seeded initial state, stopping early once ``budget_s`` seconds have been spent;
-    returns the throughput in Mcell-RK3-steps/s and the steps actually timed."""
+    returns the throughput in Mcell-RK3-steps/s and the steps actually timed (with
+    ``keep_state``, also the final fields and the dt of every step)."""
     p = o.parse_bou_in(bou_text)
     g = o.create_grid(p)
     s = o.initial_state(g, seed)
@@ -101,18 +102,24 @@ def time_steps(bou_text: str, steps: int, seed: int = 20261203, mixed: bool = Fa
     dt = p.dt
     t0 = time.perf_counter()
     done = 0
+    dts = []
     for n in range(steps):
         cflm = cpu.cfl()
         dt, _, _ = o.next_dt(p, n, dt, cflm)
         cpu.time_marcher(dt)
+        dts.append(dt)
         done += 1
         if time.perf_counter() - t0 > budget_s:
             break
     sec = time.perf_counter() - t0
     cells = p.nxm * p.nym * p.nzm
+    res = {"seconds": sec, "steps": done, "mcells_per_s": cells * done / sec / 1e6,
+           "threads": lib().afid_cpu_threads()}
+    if keep_state:
+        res["state"] = cpu.get()
+        res["dts"] = dts
     cpu.close()
-    return {"seconds": sec, "steps": done, "mcells_per_s": cells * done / sec / 1e6,
-            "threads": lib().afid_cpu_threads()}
+    return res
 
 
 def _sal_lib():
