@@ -246,6 +246,7 @@ def run_gpu(args):
     ms_max = reduce_max(ms, world)
     value = world * cells * args.steps / (ms_max * 1e-3) / 1e6
 
+    nusselt = nusselt_numbers(solver, tables, w, ra_pr)
     k1_ms, k1_n = prof["explicit_implicit"]
     k1_avg_s = (k1_ms / k1_n) * 1e-3 if k1_n else float("nan")
     peak, peak_kind = measured_peak()
@@ -334,6 +335,7 @@ def run_gpu(args):
             "k1_autotune": tune,
             "clocks": clk,
             "nu_vol_end": nu,
+            "nusselt_after_timed_steps": nusselt,
             "cpu_baseline": cpu,
         }
         if accuracy is not None:
@@ -344,6 +346,26 @@ def run_gpu(args):
     if world > 1:
         import torch.distributed as dist
         dist.destroy_process_group()
+
+
+def nusselt_numbers(solver, tables, w, ra_pr):
+    """Nusselt numbers of the resident state as the reference's post-processing defines them
+    (tools/afidtools/boundary_layers.py:41-62): the plate values from the first and last Tbar
+    rows, the dissipation value Pe * sum(chiT dx), and the volume value of GlobalQuantities."""
+    import numpy as np
+    prof = solver.mean_profiles()
+    xm, xc = tables.array("xm"), tables.array("xc")
+    nxm = w["nxm"]
+    tup, tlo = (-0.5, 0.5) if w["rayt"] > 0 else (0.5, -0.5)
+    lo = (prof["Tbar"][0] - tlo) / xm[0]
+    up = (tup - prof["Tbar"][nxm - 1]) / (1.0 - xm[nxm - 1])
+    if w["rayt"] > 0:
+        lo, up = -lo, -up
+    pect = np.sqrt(abs(w["rayt"]) / w["prat"]) * w["prat"]
+    diss = pect * float(np.sum(prof["chiT"] * (xc[1:nxm + 1] - xc[:nxm])))
+    nu_vol, ke, _ = solver.global_quantities(ra_pr)
+    return {"nu_plate_lower": float(lo), "nu_plate_upper": float(up), "nu_dissipation": diss,
+            "nu_volume": nu_vol, "kinetic_energy": ke}
 
 
 def mixed_vs_fp64(ag, w, inp, solver, temp0, dts, ra_pr):
@@ -789,6 +811,16 @@ def run_ddc(args):
     s_bytes = SAL_STEP_BYTES_PER_CELL * rcells
     achieved = s_bytes / s_avg / 1e9
     prof_s = solver.sal_profiles()
+    # solutal Nusselt numbers as tools/afidtools/boundary_layers.py:64-81 defines them
+    xmr, xcr = mgrd.array("xmr"), mgrd.array("xcr")
+    sup, slo = (0.5, -0.5) if w["rays"] > 0 else (-0.5, 0.5)
+    nus_lo = (prof_s["Sbar"][0] - slo) / xmr[0]
+    nus_up = (sup - prof_s["Sbar"][-1]) / (1.0 - xmr[-1])
+    if w["rays"] < 0:
+        nus_lo, nus_up = -nus_lo, -nus_up
+    ren = (abs(w["rays"]) / w["pras"]) ** 0.5  # FFscaleS = 1
+    nus = {"nu_s_plate_lower": float(nus_lo), "nu_s_plate_upper": float(nus_up),
+           "nu_s_dissipation": float(ren * w["pras"] * (prof_s["chiS"] * (xcr[1:] - xcr[:-1])).sum())}
 
     # ---- end to end through the C ABI with host buffers -----------------------------------
     pin = lambda shape: torch.empty(shape, dtype=torch.float64, pin_memory=True).numpy()  # noqa: E731
@@ -867,6 +899,7 @@ def run_ddc(args):
             "clocks": clk,
             "nu_vol_end": nu,
             "sbar_range": [float(prof_s["Sbar"].min()), float(prof_s["Sbar"].max())],
+            "solutal_nusselt_after_timed_steps": nus,
             "finite": finite,
             "cpu_baseline": cpu,
         }
