@@ -6,6 +6,9 @@ the salinity profiles 1e-12 relative to each field's largest magnitude (sums and
 different order); fields after whole RK3 steps 1e-10 relative L2 (pr after removing its mean), the
 bar of the flow path.
 """
+import glob
+import os
+
 import numpy as np
 import pytest
 
@@ -195,3 +198,26 @@ def test_batches_and_jobs_refuse_salinity():
     with pytest.raises(ag.AfidError) as e:
         ag.Batch(inp, 2, ag.PREC_FP64)
     assert e.value.status == ag.AFID_E_INVALID
+
+
+@pytest.mark.parametrize("path", sorted(glob.glob(os.path.join(os.path.dirname(__file__), "golden", "salinity",
+                                                               "*.npz"))))
+def test_gpu_matches_salinity_golden_fixture(path):
+    """Committed fixtures (tests/golden/salinity, from tests/golden/make_golden.py): the device
+    path after 1 and 3 steps, through the C ABI, at 1e-10 relative L2."""
+    d = np.load(path)
+    text = str(d["bou_in"])
+    tables = ag.Tables(ag.parse_bou_in(text))
+    mgrd = ag.Mgrd(tables)
+    with ag.Solver(tables.grid, tables.params) as sv:
+        sv.sal_create(mgrd)
+        sv.upload(*(d["init_" + f] for f in FIELDS))
+        sv.sal_upload(d["init_sal"])
+        for n in range(3):
+            sv.time_marcher(float(d["dt"]), n)
+            if n in (0, 2):
+                got = sv.download()
+                for f in ("vx", "vy", "vz", "temp"):
+                    assert rel_l2(got[f], d[f"step{n + 1}_{f}"]) < 1e-10, (n, f)
+                assert rel_l2(sv.sal_download(), d[f"step{n + 1}_sal"]) < 1e-10
+        assert abs(sv.sal_cfl() - float(d["step3_cflmr"])) < 1e-12 * float(d["step3_cflmr"])

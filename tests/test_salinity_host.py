@@ -9,6 +9,9 @@ Tolerances: stencil starts and the fast/general choice are exact; grid metrics a
 relative (the same expressions evaluated by C++ and NumPy); weights of every stencil sum to 1
 within 1e-13 (cubic Hermite reproduces constants).
 """
+import glob
+import os
+
 import numpy as np
 import pytest
 
@@ -249,3 +252,27 @@ def test_c_restatement_matches_numpy_oracle(coarse, refined, extra):
         assert np.linalg.norm(out[f] - ref) <= 1e-13 * np.linalg.norm(ref), f
     assert np.linalg.norm(cpu.sal() - ss.sal) <= 1e-13 * np.linalg.norm(ss.sal)
     cpu.close()
+
+
+@pytest.mark.parametrize("path", sorted(glob.glob(os.path.join(os.path.dirname(__file__), "golden", "salinity",
+                                                               "*.npz"))))
+def test_oracle_reproduces_salinity_golden_fixture(path):
+    """The committed salinity fixtures (tests/golden/make_golden.py) pin the oracle against later
+    changes: coarse fields and refined salinity after 1 and 3 steps to 1e-13."""
+    d = np.load(path)
+    p = o.parse_bou_in(str(d["bou_in"]))
+    g = o.create_grid(p)
+    m = sa.create_mgrd(g)
+    s = o.initial_state(g, 0)
+    for f in ("vx", "vy", "vz", "temp", "pr"):
+        getattr(s, f)[...] = d["init_" + f]
+    ss = sa.new_sal_state(m, g, d["init_sal"])
+    sa.interp_vel_mgrd(m, g, s, ss)
+    sa.interp_sal_multigrid(m, g, ss)
+    for n in range(3):
+        sa.time_marcher(g, s, m, ss, float(d["dt"]))
+        if n in (0, 2):
+            for f in ("vx", "vy", "vz", "temp"):
+                np.testing.assert_allclose(getattr(s, f), d[f"step{n + 1}_{f}"], rtol=0, atol=1e-13)
+            np.testing.assert_allclose(ss.sal, d[f"step{n + 1}_sal"], rtol=0, atol=1e-13)
+    assert sa.calc_max_cfl_refined(m, ss) == pytest.approx(float(d["step3_cflmr"]), rel=1e-13)
