@@ -371,7 +371,7 @@ def nusselt_numbers(solver, tables, w, ra_pr):
 def mixed_vs_fp64(ag, w, inp, solver, temp0, dts, ra_pr):
     """Per-field relative L2 (pressure modulo its mean) and the Nusselt-number error of the
     mixed-precision state after len(dts) steps against an FP64 solver advanced from the same
-    initial state with the same dt sequence (the configs[2] accuracy gate: Nu within 0.5%)."""
+    initial state with the same dt sequence (the mixed-precision accuracy gate: Nu within 0.5%)."""
     import numpy as np
     got = solver.download()
     nu_mx, _, _ = solver.global_quantities(ra_pr)
@@ -930,7 +930,7 @@ def cpu_baseline(w: dict, steps: int, budget_s: float = 60.0, keep_state: bool =
 
 
 def parity_vs_cpu(ag, w, inp, temp0, cpu):
-    """configs[1] fields at full size: the GPU path replays the C restatement's dt sequence from
+    """The default workload's fields at full size: the GPU path replays the C restatement's dt sequence from
     the same initial state; relative L2 per field (pressure modulo its mean)."""
     import numpy as np
     state, dts = cpu.pop("_state"), cpu.pop("_dts")
