@@ -1,6 +1,6 @@
 /*
  * afid_cpu.c — CPU restatement (C + OpenMP) of AFiD's RK3 flow + temperature substep.
- * TEST INFRASTRUCTURE ONLY: the timed CPU baseline of bench.py and a second checker for the
+ * TEST INFRASTRUCTURE ONLY: the timed CPU baseline of bench.py and a second oracle beside the
  * NumPy oracle (oracle/afid_oracle.py), which it is tested against.  Never part of the
  * product path.
  *

@@ -1,6 +1,6 @@
 """CPU oracle for the AFiD RK3 flow + temperature substep.  TEST INFRASTRUCTURE ONLY.
 
-This module is the checker, never the product: only ``tests/``, ``__graft_entry__.smoke()``
+This module is test infrastructure, never the product: only ``tests/``, ``__graft_entry__.smoke()``
 and ``bench.py`` (its CPU-baseline / reference arm) may import it.  The product path is the
 sm_100a CUDA library behind ``include/afid_gpu.h`` and fails loudly without it.
 
@@ -369,7 +369,7 @@ class Grid:
     pect: float
     byct: float
     pi: float
-    # Checker option, off for the reference behaviour: solve the singular (0,0) Poisson mode
+    # Test option, off for the reference behaviour: solve the singular (0,0) Poisson mode
     # exactly (last equation replaced by phi = 0) instead of through the 1+1e-15 diagonal.
     pin_zero_mode: bool = False
 

@@ -1,6 +1,6 @@
 """CPU oracle for the multi-resolution salinity scalar.  TEST INFRASTRUCTURE ONLY.
 
-This module is the checker, never the product: only ``tests/``, ``__graft_entry__.smoke()`` and
+This module is test infrastructure, never the product: only ``tests/``, ``__graft_entry__.smoke()`` and
 ``bench.py``'s CPU-baseline / reference arm may import it.  It is an FP64 NumPy restatement of
 the reference routines that evolve salinity on a refined grid and couple it to the flow:
 

@@ -1,6 +1,6 @@
 """Build recipe for the C restatement of the oracle (oracle/afid_cpu.c) -> oracle/libafid_cpu.so.
 
-Test infrastructure: the timed CPU baseline and a second checker.  gcc -O3 with OpenMP,
+Test infrastructure: the timed CPU baseline and a second oracle.  gcc -O3 with OpenMP,
 x86-64-v3 so the library built here also runs on the GPU hosts.
 """
 from __future__ import annotations

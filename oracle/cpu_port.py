@@ -1,5 +1,5 @@
 """ctypes driver of the C + OpenMP restatement (oracle/afid_cpu.c).  TEST INFRASTRUCTURE ONLY:
-used by tests/ as a second checker and by bench.py as the timed CPU baseline."""
+used by tests/ as a second oracle and by bench.py as the timed CPU baseline."""
 from __future__ import annotations
 
 import ctypes as C

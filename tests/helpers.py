@@ -1,4 +1,4 @@
-"""Shared helpers: build the same case for the oracle (CPU checker) and the CUDA library."""
+"""Shared helpers: build the same case for the oracle (CPU oracle) and the CUDA library."""
 from __future__ import annotations
 
 import numpy as np
