@@ -899,11 +899,25 @@ bool stencil_ok(const afid_stencil_t &s, int n, int lo, int hi) {
 }
 
 // Refined field <-> Fortran-layout host array (rows x nymr x nzmr, leading dims ld_x, ld_y).
+// A packed host array (ld_x == rows, ld_y == nymr) with a staging buffer travels as one linear
+// copy plus an on-device repack, as the coarse fields do; otherwise one pitched copy per z-plane.
 int sal_copy(afid_ctx_t *ctx, double *dev, int rows, const double *src, double *hdst, int ld_x, int ld_y,
-             bool to_dev) {
+             bool to_dev, double *stage = nullptr) {
   const SalGeom &sg = ctx->sal->sg;
   const size_t w = (size_t)rows * sizeof(double), dp = (size_t)sg.ldr * sizeof(double);
   const size_t hp = (size_t)ld_x * sizeof(double);
+  if (stage && ld_x == rows && ld_y == sg.nymr && rows < sg.ldr) {
+    const size_t nrow = (size_t)sg.nymr * sg.nzmr, bytes = nrow * w;
+    if (to_dev) {
+      AFID_CUDA(ctx, cudaMemcpyAsync(stage, src, bytes, cudaMemcpyHostToDevice, ctx->stream));
+      AFID_CUDA(ctx, launch_repack(ctx->stream, stage, rows, dev, sg.ldr, rows, nrow));
+    } else {
+      AFID_CUDA(ctx, launch_repack(ctx->stream, dev, sg.ldr, stage, rows, rows, nrow));
+      AFID_CUDA(ctx, cudaMemcpyAsync(hdst, stage, bytes, cudaMemcpyDeviceToHost, ctx->stream));
+    }
+    ctx->launches += 1;
+    return AFID_OK;
+  }
   for (int i = 0; i < sg.nzmr; ++i) {
     const size_t hoff = (size_t)i * ld_x * ld_y, doff = (size_t)i * sg.ldr * sg.nymr;
     if (to_dev)
@@ -1031,7 +1045,8 @@ int afid_gpu_sal_upload(afid_ctx_t *ctx, const double *sal, int ld_x, int ld_y) 
   if (ld_x < S.sg.nxmr || ld_y < S.sg.nymr) return AFID_E_INVALID;
   cudaSetDevice(ctx->dev);
   int s;
-  if ((s = sal_copy(ctx, S.sal, S.sg.nxmr, sal, nullptr, ld_x, ld_y, true)) != AFID_OK) return s;
+  // sal_o holds no state between substeps: it stages the transfer
+  if ((s = sal_copy(ctx, S.sal, S.sg.nxmr, sal, nullptr, ld_x, ld_y, true, S.sal_o)) != AFID_OK) return s;
   AFID_CUDA(ctx, cudaMemsetAsync(S.rusal, 0, S.relems * sizeof(double), ctx->stream));
   if ((s = sal_interp(ctx)) != AFID_OK) return s;  // main.F90:206-208
   return check_err_flag(ctx);
@@ -1043,7 +1058,7 @@ int afid_gpu_sal_download(afid_ctx_t *ctx, double *sal, int ld_x, int ld_y) {
   if (ld_x < S.sg.nxmr || ld_y < S.sg.nymr) return AFID_E_INVALID;
   cudaSetDevice(ctx->dev);
   int s;
-  if ((s = sal_copy(ctx, S.sal, S.sg.nxmr, nullptr, sal, ld_x, ld_y, false)) != AFID_OK) return s;
+  if ((s = sal_copy(ctx, S.sal, S.sg.nxmr, nullptr, sal, ld_x, ld_y, false, S.sal_o)) != AFID_OK) return s;
   return check_err_flag(ctx);
 }
 
