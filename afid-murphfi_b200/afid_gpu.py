@@ -31,6 +31,7 @@ AFID_E_TIMEOUT = 602
 AFID_E_INVALID = 603
 AFID_E_CUDA = 604
 AFID_E_CAPACITY = 605
+AFID_E_IO = 606
 PREC_FP64 = 0
 PREC_MIXED = 1
 
@@ -168,7 +169,26 @@ EXPORTS = [
     "afid_mgrd_create", "afid_mgrd_destroy", "afid_mgrd_view", "afid_mgrd_fast", "afid_mgrd_array",
     "afid_initial_salinity", "afid_gpu_sal_create", "afid_gpu_sal_upload", "afid_gpu_sal_download",
     "afid_gpu_sal_interpolate", "afid_gpu_sal_cfl", "afid_gpu_sal_profiles", "afid_gpu_sal_download_aux",
+    "afid_gpu_dims", "afid_h5_write", "afid_h5_info", "afid_h5_read_f64", "afid_continua_master_from_input",
+    "afid_write_flow_field", "afid_read_continua_master", "afid_read_flow_field", "afid_gpu_write_flow_field",
+    "afid_gpu_read_flow_field", "afid_run_io",
 ]
+
+
+H5_F64 = 1
+H5_I32 = 2
+H5_MAX_RANK = 4
+
+
+class H5DatasetT(C.Structure):
+    _fields_ = [("name", C.c_char_p), ("dtype", C.c_int), ("rank", C.c_int), ("dims", C.c_int64 * H5_MAX_RANK),
+                ("data", C.c_void_p)]
+
+
+class ContinuaMasterT(C.Structure):
+    _fields_ = [("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int), ("ylen", C.c_double), ("zlen", C.c_double),
+                ("time", C.c_double), ("istr3", C.c_int), ("str3", C.c_double), ("multires", C.c_int),
+                ("nxr", C.c_int), ("nyr", C.c_int), ("nzr", C.c_int), ("istr3r", C.c_int)]
 
 
 def load_library(path: str = _LIB_PATH) -> C.CDLL:
@@ -254,6 +274,18 @@ def load_library(path: str = _LIB_PATH) -> C.CDLL:
         "afid_gpu_sal_cfl": (i, [vp, _dp]),
         "afid_gpu_sal_profiles": (i, [vp, _dp]),
         "afid_gpu_sal_download_aux": (i, [vp, _dp, _dp, _dp, i, i, _dp, i, i]),
+        "afid_gpu_dims": (i, [vp, C.POINTER(i)]),
+        "afid_h5_write": (i, [C.c_char_p, i, C.POINTER(H5DatasetT)]),
+        "afid_h5_info": (i, [C.c_char_p, C.c_char_p, C.POINTER(i), C.POINTER(i), C.POINTER(C.c_int64)]),
+        "afid_h5_read_f64": (i, [C.c_char_p, C.c_char_p, _dp, C.c_int64]),
+        "afid_continua_master_from_input": (i, [C.POINTER(InputT), d, C.POINTER(ContinuaMasterT)]),
+        "afid_write_flow_field": (i, [C.c_char_p, i, d, C.POINTER(ContinuaMasterT), _dp, _dp, _dp, _dp, _dp, _dp]),
+        "afid_read_continua_master": (i, [C.c_char_p, i, C.POINTER(ContinuaMasterT)]),
+        "afid_read_flow_field": (i, [C.c_char_p, C.POINTER(ContinuaMasterT), _dp, _dp, _dp, _dp, _dp, _dp,
+                                     C.POINTER(i), _dp]),
+        "afid_gpu_write_flow_field": (i, [vp, C.c_char_p, i, d, C.POINTER(ContinuaMasterT)]),
+        "afid_gpu_read_flow_field": (i, [vp, C.c_char_p, C.POINTER(ContinuaMasterT), _dp]),
+        "afid_run_io": (i, [C.POINTER(InputT), i, C.c_uint64, i, i, vp, vp, C.c_char_p, C.POINTER(RunStatsT)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -535,6 +567,24 @@ class Solver:
                                                nxc - 1, nym), "afid_gpu_sal_download_aux")
         return dict(vxr=vxr, vyr=vyr[..., :nx], vzr=vzr[..., :nx], salc=salc)
 
+    def dims(self) -> tuple:
+        d = (C.c_int * 6)()
+        _check(lib().afid_gpu_dims(self._h, d), "afid_gpu_dims")
+        return tuple(d)
+
+    def write_flow_field(self, directory: str, master: "ContinuaMasterT", final: bool = True,
+                         save_3d: float = 1.0) -> None:
+        """WriteFlowField: the resident fields (and salinity) to directory's continua files."""
+        _check(lib().afid_gpu_write_flow_field(self._h, directory.encode(), int(final), save_3d, C.byref(master)),
+               "afid_gpu_write_flow_field")
+
+    def read_flow_field(self, directory: str, master: "ContinuaMasterT") -> float:
+        """Same-grid restart from directory's continua files; returns the master's time."""
+        t = C.c_double()
+        _check(lib().afid_gpu_read_flow_field(self._h, directory.encode(), C.byref(master), C.byref(t)),
+               "afid_gpu_read_flow_field")
+        return t.value
+
     def set_k1_shape(self, index: int) -> None:
         _check(lib().afid_gpu_set_k1_shape(self._h, index), "afid_gpu_set_k1_shape")
 
@@ -732,6 +782,79 @@ class Server:
             self.close()
         except Exception:
             pass
+
+
+def h5_write(path: str, datasets: dict) -> None:
+    """afid_h5_write: name -> array (float64 or int32, rank 1-4, C order)."""
+    keep, sets = [], (H5DatasetT * len(datasets))()
+    for i, (name, a) in enumerate(datasets.items()):
+        a = np.ascontiguousarray(a)
+        if a.dtype not in (np.float64, np.int32):
+            raise TypeError(f"{name}: dtype {a.dtype}")
+        keep.append(a)
+        sets[i].name = name.encode()
+        sets[i].dtype = H5_F64 if a.dtype == np.float64 else H5_I32
+        sets[i].rank = a.ndim
+        for r in range(a.ndim):
+            sets[i].dims[r] = a.shape[r]
+        sets[i].data = a.ctypes.data
+    _check(lib().afid_h5_write(path.encode(), len(datasets), sets), "afid_h5_write")
+
+
+def h5_info(path: str, name: str) -> tuple:
+    """(dtype class, shape) of one dataset."""
+    dt, rk, dims = C.c_int(), C.c_int(), (C.c_int64 * H5_MAX_RANK)()
+    _check(lib().afid_h5_info(path.encode(), name.encode(), C.byref(dt), C.byref(rk), dims), "afid_h5_info")
+    return dt.value, tuple(dims[i] for i in range(rk.value))
+
+
+def h5_read(path: str, name: str) -> np.ndarray:
+    """afid_h5_read_f64: the dataset converted to float64, in its own shape."""
+    _, shape = h5_info(path, name)
+    out = np.empty(shape, dtype=np.float64)
+    _check(lib().afid_h5_read_f64(path.encode(), name.encode(), _ptr(out), out.size), "afid_h5_read_f64")
+    return out
+
+
+def continua_master(inp: InputT, time: float = 0.0) -> ContinuaMasterT:
+    m = ContinuaMasterT()
+    _check(lib().afid_continua_master_from_input(C.byref(inp), time, C.byref(m)), "afid_continua_master_from_input")
+    return m
+
+
+def read_continua_master(directory: str, multires: bool = False) -> ContinuaMasterT:
+    m = ContinuaMasterT()
+    _check(lib().afid_read_continua_master(directory.encode(), int(multires), C.byref(m)), "afid_read_continua_master")
+    return m
+
+
+def write_flow_field(directory: str, master: ContinuaMasterT, fields: dict, final: bool = True,
+                     save_3d: float = 1.0) -> None:
+    """afid_write_flow_field from packed host arrays: vx, vy, vz, temp, pr of shape (nzm, nym, nx)
+    and optionally sal of shape (nzmr, nymr, nxmr)."""
+    arrs = {k: (np.ascontiguousarray(v, dtype=np.float64) if v is not None else None) for k, v in fields.items()}
+
+    def p(k):
+        a = arrs.get(k)
+        return _ptr(a) if a is not None else None
+    _check(lib().afid_write_flow_field(directory.encode(), int(final), save_3d, C.byref(master), p("vx"), p("vy"),
+                                       p("vz"), p("temp"), p("pr"), p("sal")), "afid_write_flow_field")
+
+
+def read_flow_field(directory: str, current: ContinuaMasterT, with_sal: bool = False) -> dict:
+    """afid_read_flow_field into packed arrays; pr is None when continua_pr.h5 is absent."""
+    shape = (current.nz - 1, current.ny - 1, current.nx)
+    f = {k: np.zeros(shape) for k in ("vx", "vy", "vz", "temp", "pr")}
+    sal = np.zeros((current.nzr - 1, current.nyr - 1, current.nxr - 1)) if with_sal else None
+    t, pr_read = C.c_double(), C.c_int()
+    _check(lib().afid_read_flow_field(directory.encode(), C.byref(current), C.byref(t), _ptr(f["vx"]), _ptr(f["vy"]),
+                                      _ptr(f["vz"]), _ptr(f["temp"]), _ptr(f["pr"]), C.byref(pr_read),
+                                      _ptr(sal) if sal is not None else None), "afid_read_flow_field")
+    if not pr_read.value:
+        f["pr"] = None
+    f["sal"] = sal
+    f["time"] = t.value
+    return f
 
 
 def grid_from_arrays(nxm, nym, nzm, alx3, ylen, zlen, arrays: dict, keep: list) -> GridT:

@@ -305,6 +305,7 @@ const char *afid_gpu_status_string(int s) {
     case AFID_E_INVALID: return "invalid argument or unsupported configuration";
     case AFID_E_CUDA: return "CUDA runtime error";
     case AFID_E_CAPACITY: return "capacity exhausted";
+    case AFID_E_IO: return "restart file missing, unreadable or unsupported";
   }
   return "unknown status";
 }
@@ -811,6 +812,17 @@ int afid_gpu_globals(afid_ctx_t *ctx, double ra_pr, double *nu_vol, double *ke, 
 }
 
 int afid_gpu_cuda_error(afid_ctx_t *ctx) { return ctx ? (int)ctx->last_cuda : 0; }
+
+int afid_gpu_dims(afid_ctx_t *ctx, int dims[6]) {
+  if (!ctx || !dims) return AFID_E_INVALID;
+  dims[0] = ctx->L.g.nxm;
+  dims[1] = ctx->L.g.nym;
+  dims[2] = ctx->L.g.nzm;
+  dims[3] = ctx->sal ? ctx->sal->sg.nxmr : 0;
+  dims[4] = ctx->sal ? ctx->sal->sg.nymr : 0;
+  dims[5] = ctx->sal ? ctx->sal->sg.nzmr : 0;
+  return AFID_OK;
+}
 
 int afid_gpu_field_device_ptr(afid_ctx_t *ctx, int which, void **dptr, int *ldx) {
   if (!ctx || !dptr) return AFID_E_INVALID;

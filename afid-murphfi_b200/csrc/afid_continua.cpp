@@ -1,0 +1,880 @@
+// Restart files in the reference's HDF5 layout, written and read without the HDF5 library.
+//
+// The container code implements the subset of the published HDF5 File Format Specification
+// (version 3.0, The HDF Group) that the reference's continua files use when its HDF5 library
+// runs with default property lists (h5tools/HdfRoutines.F90:11-96, :428-600): a version-0
+// superblock, a root group stored as a symbol table (version-1 B-tree of group nodes, symbol
+// table nodes, a local heap of names), and one version-1 object header per dataset with
+// dataspace, datatype, fill-value and contiguous data-layout messages.
+//
+// Writer layout (all addresses relative to byte 0, every object 8-byte aligned):
+//   superblock | root object header | local heap header + names | B-tree node | symbol table
+//   nodes | dataset object headers | raw data of each dataset
+// The B-tree node and the symbol table nodes are allocated at their full size (2K entries) as the
+// library reads them that way; the heap's free list is empty (head = 1, the library's end-of-list
+// value); entries in a symbol table node are sorted by name.
+#include <sys/stat.h>
+#include <sys/types.h>
+
+#include <algorithm>
+#include <cerrno>
+#include <cmath>
+#include <cstdint>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "afid_continua.h"
+#include "afid_salinity.h"
+
+namespace {
+
+constexpr uint64_t kUndef = ~0ull;
+constexpr uint8_t kSig[8] = {0x89, 'H', 'D', 'F', '\r', '\n', 0x1a, '\n'};
+constexpr int kLeafK = 4;          // symbol table node holds 2 * kLeafK entries
+constexpr int kInternalK = 16;     // group B-tree node holds 2 * kInternalK children
+constexpr size_t kEntrySize = 40;  // symbol table entry with 8-byte offsets
+constexpr size_t kSnodSize = 8 + 2 * kLeafK * kEntrySize;
+constexpr size_t kBtreeSize = 24 + (2 * kInternalK + 1) * 8 + 2 * kInternalK * 8;
+
+size_t pad8(size_t n) { return (n + 7) & ~size_t(7); }
+
+struct Out {
+  std::vector<uint8_t> b;
+  explicit Out(size_t n) : b(n, 0) {}
+  void put(size_t pos, uint64_t v, int bytes) {
+    for (int i = 0; i < bytes; ++i) b[pos + i] = (uint8_t)(v >> (8 * i));
+  }
+};
+
+// Object header version 1 with the given messages (type, body); returns its bytes.
+std::vector<uint8_t> object_header_v1(const std::vector<std::pair<int, std::vector<uint8_t>>> &msgs) {
+  size_t body = 0;
+  for (auto &m : msgs) body += 8 + pad8(m.second.size());
+  std::vector<uint8_t> h(16 + body, 0);
+  h[0] = 1;                                  // version
+  h[2] = (uint8_t)msgs.size();               // number of messages (2 bytes)
+  h[3] = (uint8_t)(msgs.size() >> 8);
+  h[4] = 1;                                  // reference count (4 bytes)
+  for (int i = 0; i < 4; ++i) h[8 + i] = (uint8_t)(body >> (8 * i));
+  size_t p = 16;
+  for (auto &m : msgs) {
+    const size_t sz = pad8(m.second.size());
+    h[p] = (uint8_t)m.first;
+    h[p + 1] = (uint8_t)(m.first >> 8);
+    h[p + 2] = (uint8_t)sz;
+    h[p + 3] = (uint8_t)(sz >> 8);
+    h[p + 4] = (m.first == 0x03 || m.first == 0x11) ? 1 : 0;  // datatype / symbol table: constant
+    std::memcpy(&h[p + 8], m.second.data(), m.second.size());
+    p += 8 + sz;
+  }
+  return h;
+}
+
+std::vector<uint8_t> le_bytes(std::initializer_list<std::pair<uint64_t, int>> fields) {
+  std::vector<uint8_t> v;
+  for (auto &f : fields)
+    for (int i = 0; i < f.second; ++i) v.push_back((uint8_t)(f.first >> (8 * i)));
+  return v;
+}
+
+std::vector<uint8_t> dataspace_msg(const afid_h5_dataset_t &d) {
+  std::vector<uint8_t> v = {1, (uint8_t)d.rank, 0, 0, 0, 0, 0, 0};  // version 1, no max dims
+  for (int r = 0; r < d.rank; ++r)
+    for (int i = 0; i < 8; ++i) v.push_back((uint8_t)((uint64_t)d.dims[r] >> (8 * i)));
+  return v;
+}
+
+std::vector<uint8_t> datatype_msg(int dtype) {
+  if (dtype == AFID_H5_F64)
+    // class 1 (floating point) version 1; little-endian, implied-MSB mantissa, sign bit 63;
+    // 8 bytes; offset 0, precision 64, exponent at 52 of 11 bits, mantissa at 0 of 52, bias 1023
+    return le_bytes({{0x11, 1}, {0x20, 1}, {63, 1}, {0, 1}, {8, 4}, {0, 2}, {64, 2}, {52, 1}, {11, 1},
+                     {0, 1}, {52, 1}, {1023, 4}});
+  // class 0 (fixed point) version 1; little-endian, signed; 4 bytes; offset 0, precision 32
+  return le_bytes({{0x10, 1}, {0x08, 1}, {0, 1}, {0, 1}, {4, 4}, {0, 2}, {32, 2}});
+}
+
+size_t elem_size(int dtype) { return dtype == AFID_H5_F64 ? 8 : 4; }
+
+int64_t elem_count(const afid_h5_dataset_t &d) {
+  int64_t n = 1;
+  for (int r = 0; r < d.rank; ++r) n *= d.dims[r];
+  return n;
+}
+
+bool write_all(FILE *f, const void *p, size_t n) { return n == 0 || std::fwrite(p, 1, n, f) == n; }
+
+}  // namespace
+
+extern "C" int afid_h5_write(const char *path, int n, const afid_h5_dataset_t *sets) {
+  if (!path || n < 1 || !sets) return AFID_E_INVALID;
+  std::vector<int> order(n);
+  for (int i = 0; i < n; ++i) {
+    const afid_h5_dataset_t &d = sets[i];
+    if (!d.name || !d.name[0] || std::strlen(d.name) > 255 || std::strchr(d.name, '/')) return AFID_E_INVALID;
+    if (d.rank < 1 || d.rank > AFID_H5_MAX_RANK || (d.dtype != AFID_H5_F64 && d.dtype != AFID_H5_I32))
+      return AFID_E_INVALID;
+    for (int r = 0; r < d.rank; ++r)
+      if (d.dims[r] < 0) return AFID_E_INVALID;
+    if (elem_count(d) > 0 && !d.data) return AFID_E_INVALID;
+    order[i] = i;
+  }
+  std::sort(order.begin(), order.end(), [&](int a, int b) { return std::strcmp(sets[a].name, sets[b].name) < 0; });
+  for (int i = 1; i < n; ++i)
+    if (std::strcmp(sets[order[i - 1]].name, sets[order[i]].name) == 0) return AFID_E_INVALID;
+  const int nsnod = (n + 2 * kLeafK - 1) / (2 * kLeafK);
+  if (nsnod > 2 * kInternalK) return AFID_E_INVALID;  // one B-tree leaf level is enough here
+
+  // local heap data: "" at 0, then each name NUL-terminated and padded to 8 bytes
+  std::vector<uint64_t> name_off(n);
+  size_t heap_data = 8;
+  for (int i = 0; i < n; ++i) {
+    name_off[order[i]] = heap_data;
+    heap_data += pad8(std::strlen(sets[order[i]].name) + 1);
+  }
+  const size_t a_super = 0, a_root = 96;
+  const size_t root_len = 16 + 8 + 16;                       // prefix + symbol table message
+  const size_t a_heap = a_root + root_len, heap_hdr = 32;
+  const size_t a_heapdata = a_heap + heap_hdr;
+  const size_t a_btree = a_heapdata + heap_data;
+  const size_t a_snod = a_btree + kBtreeSize;
+  size_t a = a_snod + nsnod * kSnodSize;
+  std::vector<size_t> a_oh(n), a_raw(n);
+  std::vector<std::vector<uint8_t>> oh(n);
+  for (int i = 0; i < n; ++i) {  // headers first (their size does not depend on the raw address)
+    oh[i] = object_header_v1({{0x01, dataspace_msg(sets[i])},
+                              {0x03, datatype_msg(sets[i].dtype)},
+                              {0x05, {2, 2, 2, 1, 0, 0, 0, 0}},   // fill value v2: late, if set, defined, size 0
+                              {0x08, std::vector<uint8_t>(18, 0)}});
+    a_oh[i] = a;
+    a += oh[i].size();
+  }
+  for (int i = 0; i < n; ++i) {
+    a_raw[i] = a;
+    a += pad8((size_t)elem_count(sets[i]) * elem_size(sets[i].dtype));
+  }
+  const size_t eof = a;
+  for (int i = 0; i < n; ++i) {  // fill in the layout message: version 3, contiguous, address, size
+    const size_t lay = 16 + (8 + pad8(dataspace_msg(sets[i]).size())) + (8 + pad8(datatype_msg(sets[i].dtype).size())) +
+                       (8 + 8) + 8;
+    const uint64_t bytes = (uint64_t)elem_count(sets[i]) * elem_size(sets[i].dtype);
+    oh[i][lay] = 3;
+    oh[i][lay + 1] = 1;
+    for (int k = 0; k < 8; ++k) {
+      oh[i][lay + 2 + k] = (uint8_t)((uint64_t)a_raw[i] >> (8 * k));
+      oh[i][lay + 10 + k] = (uint8_t)(bytes >> (8 * k));
+    }
+  }
+
+  Out m(a_snod + nsnod * kSnodSize);
+  // superblock version 0
+  std::memcpy(&m.b[a_super], kSig, 8);
+  m.put(13, 8, 1);                 // size of offsets
+  m.put(14, 8, 1);                 // size of lengths
+  m.put(16, kLeafK, 2);
+  m.put(18, kInternalK, 2);
+  m.put(24, 0, 8);                 // base address
+  m.put(32, kUndef, 8);            // free-space info
+  m.put(40, eof, 8);               // end of file
+  m.put(48, kUndef, 8);            // driver info
+  m.put(56, 0, 8);                 // root entry: link name offset
+  m.put(64, a_root, 8);            //   object header address
+  m.put(72, 1, 4);                 //   cache type 1: scratch holds B-tree and heap addresses
+  m.put(80, a_btree, 8);
+  m.put(88, a_heap, 8);
+  // root object header: one symbol table message
+  {
+    auto h = object_header_v1({{0x11, le_bytes({{a_btree, 8}, {a_heap, 8}})}});
+    std::memcpy(&m.b[a_root], h.data(), h.size());
+  }
+  // local heap
+  std::memcpy(&m.b[a_heap], "HEAP", 4);
+  m.put(a_heap + 8, heap_data, 8);
+  m.put(a_heap + 16, 1, 8);        // empty free list
+  m.put(a_heap + 24, a_heapdata, 8);
+  for (int i = 0; i < n; ++i) std::memcpy(&m.b[a_heapdata + name_off[i]], sets[i].name, std::strlen(sets[i].name));
+  // B-tree node (group, leaf level): keys are heap offsets of the largest name in each child
+  std::memcpy(&m.b[a_btree], "TREE", 4);
+  m.put(a_btree + 4, 0, 1);
+  m.put(a_btree + 5, 0, 1);
+  m.put(a_btree + 6, nsnod, 2);
+  m.put(a_btree + 8, kUndef, 8);
+  m.put(a_btree + 16, kUndef, 8);
+  size_t q = a_btree + 24;
+  m.put(q, 0, 8);
+  q += 8;
+  for (int c = 0; c < nsnod; ++c) {
+    const int last = std::min(n, (c + 1) * 2 * kLeafK) - 1;
+    m.put(q, a_snod + c * kSnodSize, 8);
+    m.put(q + 8, name_off[order[last]], 8);
+    q += 16;
+  }
+  // symbol table nodes
+  for (int c = 0; c < nsnod; ++c) {
+    const size_t s = a_snod + c * kSnodSize;
+    const int lo = c * 2 * kLeafK, hi = std::min(n, lo + 2 * kLeafK);
+    std::memcpy(&m.b[s], "SNOD", 4);
+    m.put(s + 4, 1, 1);
+    m.put(s + 6, hi - lo, 2);
+    for (int e = lo; e < hi; ++e) {
+      const size_t p = s + 8 + (e - lo) * kEntrySize;
+      m.put(p, name_off[order[e]], 8);
+      m.put(p + 8, a_oh[order[e]], 8);
+    }
+  }
+
+  FILE *f = std::fopen(path, "wb");
+  if (!f) return AFID_E_IO;
+  bool ok = write_all(f, m.b.data(), m.b.size());
+  for (int i = 0; i < n && ok; ++i) ok = write_all(f, oh[i].data(), oh[i].size());
+  static const uint8_t zeros[8] = {0};
+  for (int i = 0; i < n && ok; ++i) {
+    const size_t bytes = (size_t)elem_count(sets[i]) * elem_size(sets[i].dtype);
+    ok = write_all(f, sets[i].data, bytes) && write_all(f, zeros, pad8(bytes) - bytes);
+  }
+  ok = (std::fclose(f) == 0) && ok;
+  return ok ? AFID_OK : AFID_E_IO;
+}
+
+// ---- reader --------------------------------------------------------------------------------
+namespace {
+
+struct Msg {
+  int type;
+  std::vector<uint8_t> body;
+};
+
+struct DsInfo {
+  int rank = -1;
+  int64_t dims[AFID_H5_MAX_RANK] = {0, 0, 0, 0};
+  int cls = -1;          // 0 fixed point, 1 floating point
+  int size = 0;          // bytes per element
+  bool big_endian = false, is_signed = true;
+  bool compact = false, allocated = false;
+  uint64_t addr = 0;
+  std::vector<uint8_t> inline_data;
+};
+
+uint64_t le(const uint8_t *p, int n) {
+  uint64_t v = 0;
+  for (int i = 0; i < n; ++i) v |= (uint64_t)p[i] << (8 * i);
+  return v;
+}
+
+class Reader {
+ public:
+  ~Reader() {
+    if (f_) std::fclose(f_);
+  }
+  bool open(const char *path) {
+    f_ = std::fopen(path, "rb");
+    if (!f_) return false;
+    if (std::fseek(f_, 0, SEEK_END) != 0) return false;
+    const long end = std::ftell(f_);
+    if (end < 0) return false;
+    fsize_ = (uint64_t)end;
+    for (uint64_t pos = 0; pos + 8 <= fsize_; pos = pos ? pos * 2 : 512) {
+      uint8_t s[8];
+      if (!raw(pos, s, 8)) return false;
+      if (std::memcmp(s, kSig, 8) == 0) return superblock(pos);
+    }
+    return false;
+  }
+
+  bool find(const char *name, uint64_t *hdr) { return lookup(root_, name, hdr, 0); }
+
+  bool dataset(uint64_t hdr, DsInfo &d) {
+    std::vector<Msg> msgs;
+    if (!messages(hdr, msgs)) return false;
+    bool have_space = false, have_type = false, have_layout = false;
+    for (auto &m : msgs) {
+      const uint8_t *b = m.body.data();
+      const size_t n = m.body.size();
+      if (m.type == 0x01) {  // dataspace
+        if (n < 4) return false;
+        const int version = b[0], rank = b[1];
+        size_t r;
+        if (version == 1) r = 8;
+        else if (version == 2) {
+          r = 4;
+          if (b[3] == 0) { d.rank = 0; have_space = true; continue; }  // scalar
+          if (b[3] != 1) return false;                                  // null dataspace
+        } else return false;
+        if (rank > AFID_H5_MAX_RANK || n < r + (size_t)rank * sl_) return false;
+        d.rank = rank;
+        for (int i = 0; i < rank; ++i) d.dims[i] = (int64_t)le(b + r + i * sl_, sl_);
+        have_space = true;
+      } else if (m.type == 0x03) {  // datatype
+        if (n < 8) return false;
+        d.cls = b[0] & 0x0f;
+        d.big_endian = b[1] & 1;
+        d.is_signed = (b[1] & 0x08) != 0;
+        d.size = (int)le(b + 4, 4);
+        if (d.cls == 1 && d.size != 4 && d.size != 8) return false;
+        if (d.cls == 0 && d.size != 1 && d.size != 2 && d.size != 4 && d.size != 8) return false;
+        if (d.cls != 0 && d.cls != 1) return false;
+        have_type = true;
+      } else if (m.type == 0x08) {  // data layout
+        if (n < 2) return false;
+        const int version = b[0];
+        if (version == 3 || version == 4) {
+          const int cls = b[1];
+          if (cls == 0) {
+            const size_t len = (size_t)le(b + 2, 2);
+            if (n < 4 + len) return false;
+            d.compact = true;
+            d.inline_data.assign(b + 4, b + 4 + len);
+          } else if (cls == 1) {
+            if (n < 2 + (size_t)so_ + sl_) return false;
+            d.addr = le(b + 2, so_);
+          } else return false;  // chunked or virtual
+        } else if (version == 1 || version == 2) {
+          if (n < 8) return false;
+          const int rank = b[1], cls = b[2];
+          if (cls == 1) {
+            if (n < 8 + (size_t)so_) return false;
+            d.addr = le(b + 8, so_);
+          } else if (cls == 0) {
+            const size_t r = 8 + 4 * (size_t)rank;
+            if (n < r + 4) return false;
+            const size_t len = (size_t)le(b + r, 4);
+            if (n < r + 4 + len) return false;
+            d.compact = true;
+            d.inline_data.assign(b + r + 4, b + r + 4 + len);
+          } else return false;
+        } else return false;
+        have_layout = true;
+      } else if (m.type == 0x0b) {
+        return false;  // filter pipeline
+      }
+    }
+    d.allocated = d.compact || (d.addr != undef_addr());
+    return have_space && have_type && have_layout;
+  }
+
+  // Read count elements of dataset d converted to double.
+  bool read_f64(const DsInfo &d, double *out, int64_t count) {
+    const size_t es = (size_t)d.size;
+    const size_t chunk = 1 << 20;  // elements per pass
+    std::vector<uint8_t> buf;
+    for (int64_t i0 = 0; i0 < count; i0 += (int64_t)chunk) {
+      const size_t m = (size_t)std::min<int64_t>((int64_t)chunk, count - i0);
+      buf.resize(m * es);
+      if (d.compact) {
+        if ((i0 + (int64_t)m) * es > d.inline_data.size()) return false;
+        std::memcpy(buf.data(), d.inline_data.data() + i0 * es, m * es);
+      } else if (!d.allocated) {
+        std::fill(buf.begin(), buf.end(), 0);  // never written: the default fill value is zero
+      } else if (!raw(base_ + d.addr + (uint64_t)i0 * es, buf.data(), m * es)) {
+        return false;
+      }
+      for (size_t k = 0; k < m; ++k) {
+        uint8_t e[8];
+        for (size_t j = 0; j < es; ++j) e[j] = d.big_endian ? buf[k * es + es - 1 - j] : buf[k * es + j];
+        double v;
+        if (d.cls == 1) {
+          if (es == 8) std::memcpy(&v, e, 8);
+          else {
+            float x;
+            std::memcpy(&x, e, 4);
+            v = x;
+          }
+        } else {
+          uint64_t u = le(e, (int)es);
+          if (d.is_signed && es < 8 && (u >> (8 * es - 1)) & 1) u |= ~0ull << (8 * es);
+          v = d.is_signed ? (double)(int64_t)u : (double)u;
+        }
+        out[i0 + (int64_t)k] = v;
+      }
+    }
+    return true;
+  }
+
+ private:
+  FILE *f_ = nullptr;
+  uint64_t fsize_ = 0, base_ = 0, root_ = 0;
+  int so_ = 8, sl_ = 8;
+
+  uint64_t undef_addr() const { return so_ == 8 ? kUndef : ((1ull << (8 * so_)) - 1); }
+
+  bool raw(uint64_t pos, void *dst, size_t n) {
+    if (pos > fsize_ || n > fsize_ - pos) return false;
+    if (std::fseek(f_, (long)pos, SEEK_SET) != 0) return false;
+    return std::fread(dst, 1, n, f_) == n;
+  }
+  bool at(uint64_t addr, std::vector<uint8_t> &v, size_t n) {
+    v.resize(n);
+    return raw(base_ + addr, v.data(), n);
+  }
+
+  bool superblock(uint64_t pos) {
+    uint8_t s[256];
+    const size_t n = (size_t)std::min<uint64_t>(sizeof(s), fsize_ - pos);
+    if (n < 48 || !raw(pos, s, n)) return false;
+    const int version = s[8];
+    if (version == 0 || version == 1) {
+      so_ = s[13];
+      sl_ = s[14];
+      if ((so_ != 4 && so_ != 8) || (sl_ != 4 && sl_ != 8)) return false;
+      size_t q = 24 + (version == 1 ? 4 : 0);
+      if (q + 4 * so_ + 2 * so_ > n) return false;
+      base_ = le(s + q, so_);
+      q += 4 * so_;                  // base, free space, end of file, driver block
+      root_ = le(s + q + so_, so_);  // root entry: link name offset, object header address
+    } else if (version == 2 || version == 3) {
+      so_ = s[9];
+      sl_ = s[10];
+      if ((so_ != 4 && so_ != 8) || (sl_ != 4 && sl_ != 8)) return false;
+      const size_t q = 12;
+      if (q + 4 * so_ > n) return false;
+      base_ = le(s + q, so_);
+      root_ = le(s + q + 3 * so_, so_);  // base, extension, end of file, root object header
+    } else {
+      return false;
+    }
+    return true;
+  }
+
+  bool messages(uint64_t addr, std::vector<Msg> &out) {
+    std::vector<uint8_t> h;
+    if (!at(addr, h, 16)) return false;
+    struct Chunk { uint64_t addr, len; bool v2_cont; };
+    std::vector<Chunk> todo;
+    if (std::memcmp(h.data(), "OHDR", 4) == 0) {
+      const int flags = h[5];
+      size_t q = 6 + ((flags & 0x20) ? 16 : 0) + ((flags & 0x10) ? 4 : 0);
+      const int w = 1 << (flags & 3);
+      std::vector<uint8_t> pre;
+      if (!at(addr, pre, q + w)) return false;
+      const uint64_t len = le(pre.data() + q, w);
+      const bool order = flags & 0x04;
+      todo.push_back({addr + q + w, len, false});
+      for (size_t c = 0; c < todo.size() && c < 64; ++c) {
+        std::vector<uint8_t> b;
+        if (todo[c].len > (64u << 20) || !at(todo[c].addr, b, (size_t)todo[c].len)) return false;
+        size_t r = 0, end = b.size();
+        if (todo[c].v2_cont) {
+          if (end < 8 || std::memcmp(b.data(), "OCHK", 4) != 0) return false;
+          r = 4;
+          end -= 4;
+        }
+        const size_t mh = order ? 6 : 4;
+        while (r + mh <= end) {
+          const int type = b[r];
+          const size_t sz = (size_t)le(&b[r + 1], 2);
+          r += mh;
+          if (r + sz > end) break;  // gap at the end of the chunk
+          if (type == 0x10) {
+            if (sz < (size_t)so_ + sl_) return false;
+            todo.push_back({le(&b[r], so_), le(&b[r + so_], sl_), true});
+          } else {
+            out.push_back({type, std::vector<uint8_t>(b.begin() + r, b.begin() + r + sz)});
+          }
+          r += sz;
+        }
+      }
+      return true;
+    }
+    if (h[0] != 1) return false;
+    const size_t nmsg = (size_t)le(&h[2], 2);
+    todo.push_back({addr + 16, le(&h[8], 4), false});
+    for (size_t c = 0; c < todo.size() && c < 64 && out.size() < nmsg; ++c) {
+      std::vector<uint8_t> b;
+      if (todo[c].len > (64u << 20) || !at(todo[c].addr, b, (size_t)todo[c].len)) return false;
+      size_t r = 0;
+      while (r + 8 <= b.size()) {
+        const int type = (int)le(&b[r], 2);
+        const size_t sz = (size_t)le(&b[r + 2], 2);
+        r += 8;
+        if (r + sz > b.size()) return false;
+        if (type == 0x10) {
+          if (sz < (size_t)so_ + sl_) return false;
+          todo.push_back({le(&b[r], so_), le(&b[r + so_], sl_), false});
+        } else {
+          out.push_back({type, std::vector<uint8_t>(b.begin() + r, b.begin() + r + sz)});
+        }
+        r += sz;
+      }
+    }
+    return true;
+  }
+
+  bool heap_name(uint64_t heap_data, uint64_t off, std::string &s) {
+    s.clear();
+    char c[64];
+    for (uint64_t p = off;; p += sizeof(c)) {
+      const size_t n = (size_t)std::min<uint64_t>(sizeof(c), fsize_ - std::min(fsize_, base_ + heap_data + p));
+      if (n == 0 || !raw(base_ + heap_data + p, c, n)) return false;
+      for (size_t i = 0; i < n; ++i) {
+        if (c[i] == 0) return true;
+        s.push_back(c[i]);
+        if (s.size() > 4096) return false;
+      }
+    }
+  }
+
+  // Symbol table group: walk the B-tree of group nodes down to the symbol table nodes.
+  bool btree_find(uint64_t node, uint64_t heap_data, const char *name, uint64_t *hdr, int depth) {
+    if (depth > 16) return false;
+    std::vector<uint8_t> b;
+    if (!at(node, b, 8 + 2 * (size_t)so_)) return false;
+    if (std::memcmp(b.data(), "TREE", 4) != 0 || b[4] != 0) return false;
+    const int level = b[5];
+    const size_t used = (size_t)le(&b[6], 2);
+    const size_t body = 8 + 2 * (size_t)so_ + (used + 1) * sl_ + used * so_;
+    if (used > 4096 || !at(node, b, body)) return false;
+    size_t q = 8 + 2 * so_ + sl_;
+    for (size_t i = 0; i < used; ++i, q += so_ + sl_) {
+      const uint64_t child = le(&b[q], so_);
+      if (level > 0) {
+        if (btree_find(child, heap_data, name, hdr, depth + 1)) return true;
+        continue;
+      }
+      std::vector<uint8_t> s;
+      if (!at(child, s, 8)) return false;
+      if (std::memcmp(s.data(), "SNOD", 4) != 0) return false;
+      const size_t nsym = (size_t)le(&s[6], 2), es = 2 * (size_t)so_ + 24;
+      if (nsym > 4096 || !at(child, s, 8 + nsym * es)) return false;
+      for (size_t e = 0; e < nsym; ++e) {
+        std::string nm;
+        if (!heap_name(heap_data, le(&s[8 + e * es], so_), nm)) return false;
+        if (nm == name) {
+          *hdr = le(&s[8 + e * es + so_], so_);
+          return true;
+        }
+      }
+    }
+    return false;
+  }
+
+  bool lookup(uint64_t group, const char *name, uint64_t *hdr, int depth) {
+    std::vector<Msg> msgs;
+    if (depth > 0 || !messages(group, msgs)) return false;
+    for (auto &m : msgs) {
+      const uint8_t *b = m.body.data();
+      const size_t n = m.body.size();
+      if (m.type == 0x11) {  // symbol table: B-tree and local heap
+        if (n < 2 * (size_t)so_) return false;
+        const uint64_t btree = le(b, so_), heap = le(b + so_, so_);
+        std::vector<uint8_t> hh;
+        if (!at(heap, hh, 8 + 2 * (size_t)sl_ + so_) || std::memcmp(hh.data(), "HEAP", 4) != 0) return false;
+        const uint64_t heap_data = le(&hh[8 + 2 * sl_], so_);
+        return btree_find(btree, heap_data, name, hdr, 0);
+      }
+      if (m.type == 0x06) {  // link message (compact storage)
+        if (n < 2) continue;
+        const int flags = b[1];
+        size_t r = 2;
+        int ltype = 0;
+        if (flags & 0x08) ltype = b[r++];
+        if (flags & 0x04) r += 8;
+        if (flags & 0x10) r += 1;
+        const int w = 1 << (flags & 3);
+        if (r + w > n) continue;
+        const size_t len = (size_t)le(b + r, w);
+        r += w;
+        if (r + len + so_ > n) continue;
+        if (ltype == 0 && len == std::strlen(name) && std::memcmp(b + r, name, len) == 0) {
+          *hdr = le(b + r + len, so_);
+          return true;
+        }
+      }
+    }
+    return false;
+  }
+};
+
+int open_dataset(const char *path, const char *name, Reader &rd, DsInfo &d) {
+  if (!path || !name) return AFID_E_INVALID;
+  uint64_t hdr = 0;
+  if (!rd.open(path) || !rd.find(name, &hdr) || !rd.dataset(hdr, d)) return AFID_E_IO;
+  return AFID_OK;
+}
+
+}  // namespace
+
+extern "C" int afid_h5_info(const char *path, const char *name, int *dtype, int *rank,
+                            int64_t dims[AFID_H5_MAX_RANK]) {
+  Reader rd;
+  DsInfo d;
+  const int s = open_dataset(path, name, rd, d);
+  if (s != AFID_OK) return s;
+  if (dtype) *dtype = d.cls == 1 ? AFID_H5_F64 : AFID_H5_I32;
+  if (rank) *rank = d.rank;
+  if (dims)
+    for (int i = 0; i < AFID_H5_MAX_RANK; ++i) dims[i] = i < d.rank ? d.dims[i] : 0;
+  return AFID_OK;
+}
+
+extern "C" int afid_h5_read_f64(const char *path, const char *name, double *out, int64_t count) {
+  if (!out || count < 0) return AFID_E_INVALID;
+  Reader rd;
+  DsInfo d;
+  const int s = open_dataset(path, name, rd, d);
+  if (s != AFID_OK) return s;
+  int64_t n = 1;
+  for (int i = 0; i < d.rank; ++i) n *= d.dims[i];
+  if (n != count) return AFID_E_INVALID;
+  return rd.read_f64(d, out, count) ? AFID_OK : AFID_E_IO;
+}
+
+// ---- continua files --------------------------------------------------------------------------
+namespace {
+
+bool ensure_dir(const std::string &d) {
+  struct stat st;
+  if (stat(d.c_str(), &st) == 0) return S_ISDIR(st.st_mode);
+  return mkdir(d.c_str(), 0755) == 0 || errno == EEXIST;
+}
+
+bool file_exists(const std::string &p) {
+  struct stat st;
+  return stat(p.c_str(), &st) == 0 && S_ISREG(st.st_mode);
+}
+
+// One field file: dataset "var" with C-order dims (n3, n2, n1), from a packed host array whose x
+// extent is src_x (<= n1; the remaining x nodes are written as zero).
+int write_field(const std::string &path, const double *src, int src_x, int n1, int n2, int n3) {
+  const double *data = src;
+  std::vector<double> padded;
+  if (src_x != n1) {
+    padded.assign((size_t)n1 * n2 * n3, 0.0);
+    for (size_t c = 0; c < (size_t)n2 * n3; ++c)
+      std::memcpy(&padded[c * n1], src + c * src_x, sizeof(double) * src_x);
+    data = padded.data();
+  }
+  afid_h5_dataset_t d{};
+  d.name = "var";
+  d.dtype = AFID_H5_F64;
+  d.rank = 3;
+  d.dims[0] = n3;
+  d.dims[1] = n2;
+  d.dims[2] = n1;
+  d.data = data;
+  return afid_h5_write(path.c_str(), 1, &d);
+}
+
+// Read dataset "var" with C-order dims (n3, n2, n1) into a packed array of x extent dst_x <= n1.
+int read_field(const std::string &path, double *dst, int dst_x, int n1, int n2, int n3) {
+  int dtype = 0, rank = 0;
+  int64_t dims[AFID_H5_MAX_RANK];
+  int s = afid_h5_info(path.c_str(), "var", &dtype, &rank, dims);
+  if (s != AFID_OK) return s;
+  if (rank != 3 || dims[0] != n3 || dims[1] != n2 || dims[2] != n1) return AFID_E_INVALID;
+  const int64_t count = (int64_t)n1 * n2 * n3;
+  if (dst_x == n1) return afid_h5_read_f64(path.c_str(), "var", dst, count);
+  std::vector<double> full((size_t)count);
+  if ((s = afid_h5_read_f64(path.c_str(), "var", full.data(), count)) != AFID_OK) return s;
+  for (size_t c = 0; c < (size_t)n2 * n3; ++c) std::memcpy(dst + c * dst_x, &full[c * n1], sizeof(double) * dst_x);
+  return AFID_OK;
+}
+
+int read_scalar(const std::string &path, const char *name, double *v) {
+  int dtype = 0, rank = 0;
+  int64_t dims[AFID_H5_MAX_RANK];
+  int s = afid_h5_info(path.c_str(), name, &dtype, &rank, dims);
+  if (s != AFID_OK) return s;
+  int64_t n = 1;
+  for (int i = 0; i < rank; ++i) n *= dims[i];
+  if (n != 1) return AFID_E_IO;
+  return afid_h5_read_f64(path.c_str(), name, v, 1);
+}
+
+}  // namespace
+
+extern "C" int afid_continua_master_from_input(const afid_input_t *in, double time, afid_continua_master_t *m) {
+  if (!in || !m) return AFID_E_INVALID;
+  *m = afid_continua_master_t{};
+  m->nx = in->nxm + 1;
+  m->ny = in->nym + 1;
+  m->nz = in->nzm + 1;
+  m->ylen = in->ylen;
+  m->zlen = in->zlen;
+  m->time = time;
+  m->istr3 = in->istr3;
+  m->str3 = in->str3;
+  m->multires = in->multires ? 1 : 0;
+  if (m->multires) {
+    m->nxr = in->nxmr + 1;
+    m->nyr = in->nymr + 1;
+    m->nzr = in->nzmr + 1;
+    m->istr3r = in->istr3r;
+  }
+  return AFID_OK;
+}
+
+extern "C" int afid_write_flow_field(const char *dir, int final, double save_3d, const afid_continua_master_t *m,
+                                     const double *vx, const double *vy, const double *vz, const double *temp,
+                                     const double *pr, const double *sal) {
+  if (!dir || !m || !vx || !vy || !vz || !temp || (final && !pr)) return AFID_E_INVALID;
+  const int nx = m->nx, nym = m->ny - 1, nzm = m->nz - 1;
+  if (nx < 2 || nym < 1 || nzm < 1) return AFID_E_INVALID;
+  const bool with_sal = m->multires && sal;
+  if (with_sal && (m->nxr < 2 || m->nyr < 2 || m->nzr < 2)) return AFID_E_INVALID;
+  std::string base = dir;
+  if (!ensure_dir(base)) return AFID_E_IO;
+  if (final) {
+    base += "/continua";
+  } else {  // WriteFlowField.F90:22-26: frame = nint(time / save_3D), written as i5.5
+    if (!(save_3d > 0.0)) return AFID_E_INVALID;
+    const double fr = std::nearbyint(m->time / save_3d);
+    if (!(fr >= 0.0 && fr <= 99999.0)) return AFID_E_INVALID;
+    char frame[8];
+    std::snprintf(frame, sizeof(frame), "%05d", (int)fr);
+    base += "/fields";
+    if (!ensure_dir(base)) return AFID_E_IO;
+    base += std::string("/") + frame;
+  }
+  int s;
+  if ((s = write_field(base + "_temp.h5", temp, nx, nx, nym, nzm)) != AFID_OK) return s;
+  if ((s = write_field(base + "_vx.h5", vx, nx, nx, nym, nzm)) != AFID_OK) return s;
+  if ((s = write_field(base + "_vy.h5", vy, nx, nx, nym, nzm)) != AFID_OK) return s;
+  if ((s = write_field(base + "_vz.h5", vz, nx, nx, nym, nzm)) != AFID_OK) return s;
+  if (with_sal && (s = write_field(base + "_sal.h5", sal, m->nxr - 1, m->nxr, m->nyr - 1, m->nzr - 1)) != AFID_OK)
+    return s;
+  if (!final) return AFID_OK;
+  if ((s = write_field(base + "_pr.h5", pr, nx, nx, nym, nzm)) != AFID_OK) return s;
+  // continua_master.h5 (WriteFlowField.F90:51-82): one-element datasets
+  const int32_t ints[7] = {m->nx, m->ny, m->nz, m->istr3, m->nxr, m->nyr, m->nzr};
+  const int32_t istr3r = m->istr3r;
+  const double reals[4] = {m->ylen, m->zlen, m->time, m->str3};
+  afid_h5_dataset_t d[12];
+  int n = 0;
+  auto add = [&](const char *name, int dtype, const void *p) {
+    d[n] = afid_h5_dataset_t{};
+    d[n].name = name;
+    d[n].dtype = dtype;
+    d[n].rank = 1;
+    d[n].dims[0] = 1;
+    d[n].data = p;
+    ++n;
+  };
+  add("nx", AFID_H5_I32, &ints[0]);
+  add("ny", AFID_H5_I32, &ints[1]);
+  add("nz", AFID_H5_I32, &ints[2]);
+  add("ylen", AFID_H5_F64, &reals[0]);
+  add("zlen", AFID_H5_F64, &reals[1]);
+  add("time", AFID_H5_F64, &reals[2]);
+  add("istr3", AFID_H5_I32, &ints[3]);
+  add("str3", AFID_H5_F64, &reals[3]);
+  if (m->multires) {
+    add("nxr", AFID_H5_I32, &ints[4]);
+    add("nyr", AFID_H5_I32, &ints[5]);
+    add("nzr", AFID_H5_I32, &ints[6]);
+    add("istr3r", AFID_H5_I32, &istr3r);
+  }
+  return afid_h5_write((std::string(dir) + "/continua_master.h5").c_str(), n, d);
+}
+
+extern "C" int afid_read_continua_master(const char *dir, int multires, afid_continua_master_t *m) {
+  if (!dir || !m) return AFID_E_INVALID;
+  const std::string p = std::string(dir) + "/continua_master.h5";
+  if (!file_exists(p)) return AFID_E_IO;  // "Continuation files not found" (ReadFlowInterp.F90:25-29)
+  afid_continua_master_t r{};
+  double v[12];
+  const char *names[12] = {"nx", "ny", "nz", "time", "istr3", "str3", "ylen", "zlen", "nxr", "nyr", "nzr", "istr3r"};
+  const int count = multires ? 12 : 8;
+  for (int i = 0; i < count; ++i) {
+    const int s = read_scalar(p, names[i], &v[i]);
+    if (s != AFID_OK) return s;
+  }
+  r.nx = (int)v[0];
+  r.ny = (int)v[1];
+  r.nz = (int)v[2];
+  r.time = v[3];
+  r.istr3 = (int)v[4];
+  r.str3 = v[5];
+  r.ylen = v[6];
+  r.zlen = v[7];
+  r.multires = multires ? 1 : 0;
+  if (multires) {
+    r.nxr = (int)v[8];
+    r.nyr = (int)v[9];
+    r.nzr = (int)v[10];
+    r.istr3r = (int)v[11];
+  }
+  *m = r;
+  return AFID_OK;
+}
+
+extern "C" int afid_read_flow_field(const char *dir, const afid_continua_master_t *cur, double *time_out, double *vx,
+                                    double *vy, double *vz, double *temp, double *pr, int *pr_read, double *sal) {
+  if (!dir || !cur || !vx || !vy || !vz || !temp) return AFID_E_INVALID;
+  afid_continua_master_t old{};
+  int s = afid_read_continua_master(dir, cur->multires, &old);
+  if (s != AFID_OK) return s;
+  // ReadFlowInterp.F90:76-82: the domain size must match
+  if (std::fabs(cur->ylen - old.ylen) > 1e-8 || std::fabs(cur->zlen - old.zlen) > 1e-8) return AFID_E_INVALID;
+  // ReadFlowInterp.F90:85-89: a different grid needs the interpolating restart
+  if (cur->nx != old.nx || cur->ny != old.ny || cur->nz != old.nz || cur->istr3 != old.istr3 ||
+      std::fabs(cur->str3 - old.str3) > 1e-8 ||
+      (cur->multires && (cur->nxr != old.nxr || cur->nyr != old.nyr || cur->nzr != old.nzr || cur->istr3r != old.istr3r)))
+    return AFID_E_INVALID;
+  const std::string base = std::string(dir) + "/continua";
+  const int nx = cur->nx, nym = cur->ny - 1, nzm = cur->nz - 1;
+  if ((s = read_field(base + "_vx.h5", vx, nx, nx, nym, nzm)) != AFID_OK) return s;
+  if ((s = read_field(base + "_vy.h5", vy, nx, nx, nym, nzm)) != AFID_OK) return s;
+  if ((s = read_field(base + "_vz.h5", vz, nx, nx, nym, nzm)) != AFID_OK) return s;
+  if ((s = read_field(base + "_temp.h5", temp, nx, nx, nym, nzm)) != AFID_OK) return s;
+  if (cur->multires && sal &&
+      (s = read_field(base + "_sal.h5", sal, cur->nxr - 1, cur->nxr, cur->nyr - 1, cur->nzr - 1)) != AFID_OK)
+    return s;
+  int got_pr = 0;
+  if (pr && file_exists(base + "_pr.h5")) {  // ReadFlowInterp.F90:157-162
+    if ((s = read_field(base + "_pr.h5", pr, nx, nx, nym, nzm)) != AFID_OK) return s;
+    got_pr = 1;
+  }
+  if (pr_read) *pr_read = got_pr;
+  if (time_out) *time_out = old.time;
+  return AFID_OK;
+}
+
+extern "C" int afid_gpu_write_flow_field(afid_ctx_t *ctx, const char *dir, int final, double save_3d,
+                                         const afid_continua_master_t *m) {
+  if (!ctx || !dir || !m) return AFID_E_INVALID;
+  int dims[6];
+  int s = afid_gpu_dims(ctx, dims);
+  if (s != AFID_OK) return s;
+  if (m->nx != dims[0] + 1 || m->ny != dims[1] + 1 || m->nz != dims[2] + 1) return AFID_E_INVALID;
+  const bool with_sal = m->multires && dims[3] > 0;
+  if (with_sal && (m->nxr != dims[3] + 1 || m->nyr != dims[4] + 1 || m->nzr != dims[5] + 1)) return AFID_E_INVALID;
+  const int nx = m->nx, nym = dims[1], nzm = dims[2];
+  const size_t n = (size_t)nx * nym * nzm;
+  std::vector<double> f(5 * n);
+  double *vx = f.data(), *vy = vx + n, *vz = vy + n, *temp = vz + n, *pr = temp + n;
+  if ((s = afid_gpu_download(ctx, vx, vy, vz, temp, pr, nx, nym)) != AFID_OK) return s;
+  std::vector<double> sal;
+  if (with_sal) {
+    sal.resize((size_t)dims[3] * dims[4] * dims[5]);
+    if ((s = afid_gpu_sal_download(ctx, sal.data(), dims[3], dims[4])) != AFID_OK) return s;
+  }
+  return afid_write_flow_field(dir, final, save_3d, m, vx, vy, vz, temp, pr, with_sal ? sal.data() : nullptr);
+}
+
+extern "C" int afid_gpu_read_flow_field(afid_ctx_t *ctx, const char *dir, const afid_continua_master_t *cur,
+                                        double *time_out) {
+  if (!ctx || !dir || !cur) return AFID_E_INVALID;
+  int dims[6];
+  int s = afid_gpu_dims(ctx, dims);
+  if (s != AFID_OK) return s;
+  if (cur->nx != dims[0] + 1 || cur->ny != dims[1] + 1 || cur->nz != dims[2] + 1) return AFID_E_INVALID;
+  const bool with_sal = cur->multires && dims[3] > 0;
+  if (with_sal && (cur->nxr != dims[3] + 1 || cur->nyr != dims[4] + 1 || cur->nzr != dims[5] + 1))
+    return AFID_E_INVALID;
+  const int nx = cur->nx, nym = dims[1], nzm = dims[2];
+  const size_t n = (size_t)nx * nym * nzm;
+  std::vector<double> f(5 * n, 0.0);
+  double *vx = f.data(), *vy = vx + n, *vz = vy + n, *temp = vz + n, *pr = temp + n;
+  std::vector<double> sal(with_sal ? (size_t)dims[3] * dims[4] * dims[5] : 0);
+  int pr_read = 0;
+  double t = 0.0;
+  if ((s = afid_read_flow_field(dir, cur, &t, vx, vy, vz, temp, pr, &pr_read, with_sal ? sal.data() : nullptr)) !=
+      AFID_OK)
+    return s;
+  if ((s = afid_gpu_upload(ctx, vx, vy, vz, temp, pr, nx, nym)) != AFID_OK) return s;
+  if (with_sal && (s = afid_gpu_sal_upload(ctx, sal.data(), dims[3], dims[4])) != AFID_OK) return s;
+  if (time_out) *time_out = t;
+  return AFID_OK;
+}

@@ -1,6 +1,7 @@
 // afid_host.cpp — host-side set-up and step control around the GPU substep (include/afid_host.h).
 #include "afid_host.h"
 
+#include "afid_continua.h"
 #include "afid_host_internal.h"
 #include "afid_salinity.h"
 
@@ -492,6 +493,11 @@ int afid_next_dt(const afid_input_t *in, int ntime, double *dt, double cflm, dou
 
 int afid_run(const afid_input_t *in, int precision, uint64_t seed, int nsteps, int stats_every, afid_step_cb cb,
              void *user, afid_run_stats_t *stats) {
+  return afid_run_io(in, precision, seed, nsteps, stats_every, cb, user, nullptr, stats);
+}
+
+int afid_run_io(const afid_input_t *in, int precision, uint64_t seed, int nsteps, int stats_every, afid_step_cb cb,
+                void *user, const char *dir, afid_run_stats_t *stats) {
   if (!in) return AFID_E_INVALID;
   afid_tables_t *t = nullptr;
   int s = afid_tables_create(in, precision, &t);
@@ -500,26 +506,41 @@ int afid_run(const afid_input_t *in, int precision, uint64_t seed, int nsteps, i
   s = afid_gpu_create(&t->grid, &t->params, &ctx);
   if (s != AFID_OK) { afid_tables_destroy(t); return s; }
   const int nxm = in->nxm, nym = in->nym, nzm = in->nzm, nx = nxm + 1;
-  std::vector<double> temp((size_t)nx * nym * nzm, 0.0);
-  afid_initial_temperature(t, seed, 1e-3, temp.data(), nx, nym);
-  std::vector<double> zero(temp.size(), 0.0);
-  s = afid_gpu_upload(ctx, zero.data(), zero.data(), zero.data(), temp.data(), zero.data(), nx, nym);
   // multi-resolution salinity (MULTIRES = FLAGSAL = 1): refined grid, CreateInitialSalinity with
   // Philox key seed + 1, and the refined-grid CFL number for the dt rule (main.F90:285-293)
   afid_mgrd_t *mg = nullptr;
-  if (s == AFID_OK && in->flagsal) {
+  if (in->flagsal) {
     s = afid_mgrd_create(t, &mg);
     if (s == AFID_OK) s = afid_gpu_sal_create(ctx, afid_mgrd_view(mg));
-    if (s == AFID_OK) {
+  }
+  double time = 0.0;
+  afid_continua_master_t master{};
+  afid_continua_master_from_input(in, 0.0, &master);
+  if (s == AFID_OK && dir && in->nread) {  // ReadFlowInterp (main.F90:157-161), same grid
+    s = afid_gpu_read_flow_field(ctx, dir, &master, &time);
+    if (in->ireset) time = 0.0;           // ReadFlowInterp.F90:173
+  } else if (s == AFID_OK) {
+    std::vector<double> temp((size_t)nx * nym * nzm, 0.0);
+    afid_initial_temperature(t, seed, 1e-3, temp.data(), nx, nym);
+    std::vector<double> zero(temp.size(), 0.0);
+    s = afid_gpu_upload(ctx, zero.data(), zero.data(), zero.data(), temp.data(), zero.data(), nx, nym);
+    if (s == AFID_OK && mg) {
       const afid_sal_grid_t *v = afid_mgrd_view(mg);
       std::vector<double> sal((size_t)v->nxmr * v->nymr * v->nzmr);
       afid_initial_salinity(mg, seed + 1, 5e-3, sal.data(), v->nxmr, v->nymr);
       s = afid_gpu_sal_upload(ctx, sal.data(), v->nxmr, v->nymr);
     }
   }
+  // 3-D frames: at start-up (main.F90:241) and when mod(time, SAVE_3D) < dt past the first
+  // TFRAME (main.F90:376-381); skipped when SAVE_3D or TFRAME is not positive
+  const bool frames = dir && in->save_3d > 0.0 && in->tframe > 0.0;
+  if (s == AFID_OK && frames) {
+    master.time = time;
+    s = afid_gpu_write_flow_field(ctx, dir, 0, in->save_3d, &master);
+  }
   afid_run_stats_t st{};
   const int total = (nsteps < 0) ? in->ntst + 1 : nsteps;
-  double dt = in->dt, time = 0.0;
+  double dt = in->dt;
   const double ra_pr = std::fabs(in->rayt) * in->prat;
   auto t0 = std::chrono::steady_clock::now();
   int errorcode = 0;
@@ -544,6 +565,10 @@ int afid_run(const afid_input_t *in, int precision, uint64_t seed, int nsteps, i
       afid_gpu_globals(ctx, ra_pr, &nu, &ke, nullptr);
       cb(ntime, time, dt, nu, ke, user);
     }
+    if (frames && std::fmod(time, in->save_3d) < dt && std::floor(time / in->tframe) != 0.0) {
+      master.time = time;
+      if ((s = afid_gpu_write_flow_field(ctx, dir, 0, in->save_3d, &master)) != AFID_OK) break;
+    }
     if (time > in->tmax) errorcode = 333;
     if (errorcode == 0 && nsteps < 0 && ntime == in->ntst) errorcode = 555;
     if (errorcode != 0) break;
@@ -555,6 +580,11 @@ int afid_run(const afid_input_t *in, int precision, uint64_t seed, int nsteps, i
   st.dt = dt;
   st.errorcode = errorcode;
   if (s == AFID_OK) afid_gpu_globals(ctx, ra_pr, &st.nu_vol, &st.ke, nullptr);
+  // QuitRoutine.F90:37: the continua files on a normal exit
+  if (s == AFID_OK && dir && (errorcode == 0 || errorcode == 333 || errorcode == 334 || errorcode == 555)) {
+    master.time = time;
+    s = afid_gpu_write_flow_field(ctx, dir, 1, in->save_3d, &master);
+  }
   if (stats) *stats = st;
   afid_gpu_destroy(ctx);
   afid_mgrd_destroy(mg);

@@ -1,0 +1,119 @@
+/*
+ * afid_continua.h — restart files in the reference's HDF5 layout (C ABI, plain C types).
+ *
+ * The reference writes one file per field through the HDF5 library and a master file with the
+ * grid description; a run with NREAD = 1 reads them back.  These entry points produce and read
+ * the same files without the HDF5 library:
+ *
+ *   afid_write_flow_field        WriteFlowField.F90:11-86: <dir>/continua_{temp,vx,vy,vz,[sal],pr}.h5
+ *                                and <dir>/continua_master.h5 when final, otherwise
+ *                                <dir>/fields/NNNNN_{temp,vx,vy,vz,[sal]}.h5 with
+ *                                NNNNN = nint(time / save_3d)
+ *   afid_read_continua_master    ReadFlowInterp.F90:23-58 (the master datasets)
+ *   afid_read_flow_field         ReadFlowInterp.F90:76-171, same-grid branch: domain-size check,
+ *                                grid check, then HdfReadContinua (h5tools/HdfReadContinua.F90) per
+ *                                field; continua_pr.h5 is read only when it exists
+ *   afid_gpu_write_flow_field /  the same through a device context: download, write / read,
+ *   afid_gpu_read_flow_field     upload (salinity included when the context has it)
+ *   afid_run_io                  afid_run plus the main loop's restart and save points:
+ *                                ReadFlowInterp when NREAD = 1 (main.F90:157-161), the start-up
+ *                                frame (main.F90:241), the SAVE_3D frames (main.F90:376-381) and
+ *                                the final continua files on a normal exit (QuitRoutine.F90:37)
+ *
+ * Each field file holds one dataset "var" of little-endian IEEE doubles with C-order dims
+ * (nzm, nym, nx) — Fortran (nx, nym, nzm), h5tools/HdfRoutines.F90:467-471 — contiguous
+ * storage; the refined salinity file has (nzmr, nymr, nxmr + 1) (HdfRoutines.F90:562-566).
+ * The master file holds one-element datasets: nx, ny, nz, istr3 (32-bit integers), ylen, zlen,
+ * time, str3 (doubles), and nxr, nyr, nzr, istr3r when MULTIRES = 1 (WriteFlowField.F90:54-81).
+ * nx, ny, nz are nxm + 1, nym + 1, nzm + 1 as in param.F90; nxr, nyr, nzr likewise refined.
+ *
+ * Host arrays here are packed: vx, vy, vz, temp, pr with x extent nx (index nx - 1 is the upper
+ * wall node, zero for the cell-centred fields), salinity with x extent nxmr.  The salinity file's
+ * extra x node (nxmr + 1) is written as zero and dropped on reading.
+ *
+ * The container (afid_h5_*) is the subset of the HDF5 file format these files need: superblock
+ * version 0, version-1 object headers, a symbol-table root group, fixed-point and floating-point
+ * datasets with contiguous storage.  The reader also takes superblock versions 1-3, version-2
+ * object headers, compact link-message groups and compact storage; chunked storage, filters and
+ * dense link storage are refused with AFID_E_IO.
+ */
+#ifndef AFID_CONTINUA_H
+#define AFID_CONTINUA_H
+
+#include <stdint.h>
+
+#include "afid_gpu.h"
+#include "afid_host.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- the container ------------------------------------------------------------------------ */
+#define AFID_H5_F64 1          /* IEEE binary64, little-endian on disk                       */
+#define AFID_H5_I32 2          /* two's-complement 32-bit, little-endian on disk              */
+#define AFID_H5_MAX_RANK 4
+
+typedef struct afid_h5_dataset {
+  const char *name;            /* at most 255 bytes, no '/'                                    */
+  int dtype;                   /* AFID_H5_F64 / AFID_H5_I32                                    */
+  int rank;                    /* 1 .. AFID_H5_MAX_RANK                                        */
+  int64_t dims[AFID_H5_MAX_RANK];   /* C order: dims[rank - 1] varies fastest                  */
+  const void *data;            /* prod(dims) host values of the type                           */
+} afid_h5_dataset_t;
+
+/* Create (truncate) path holding the n datasets in its root group. */
+int afid_h5_write(const char *path, int n, const afid_h5_dataset_t *sets);
+/* Class and shape of one dataset: *dtype is AFID_H5_F64 for any floating-point type and
+ * AFID_H5_I32 for any integer type.  AFID_E_IO if the file or dataset is missing or unsupported. */
+int afid_h5_info(const char *path, const char *name, int *dtype, int *rank, int64_t dims[AFID_H5_MAX_RANK]);
+/* Read a whole dataset converted to double (count must equal its element count). */
+int afid_h5_read_f64(const char *path, const char *name, double *out, int64_t count);
+
+/* ---- continua files ----------------------------------------------------------------------- */
+typedef struct afid_continua_master {
+  int nx, ny, nz;              /* nxm + 1, nym + 1, nzm + 1                                    */
+  double ylen, zlen, time;
+  int istr3;
+  double str3;
+  int multires;                /* 1: nxr, nyr, nzr, istr3r are written / read                 */
+  int nxr, nyr, nzr, istr3r;   /* nxmr + 1, nymr + 1, nzmr + 1, ISTR3R                        */
+} afid_continua_master_t;
+
+/* The master record of a run described by in at the given time. */
+int afid_continua_master_from_input(const afid_input_t *in, double time, afid_continua_master_t *m);
+/* final != 0: continua_*.h5 including pr, and continua_master.h5; final == 0: a fields/ frame
+ * without pr (pr may be NULL then).  sal is written when m->multires and sal != NULL.
+ * Missing directories (dir, dir/fields) are created. */
+int afid_write_flow_field(const char *dir, int final, double save_3d, const afid_continua_master_t *m,
+                          const double *vx, const double *vy, const double *vz, const double *temp,
+                          const double *pr, const double *sal);
+/* Reads nx, ny, nz, time, istr3, str3, ylen, zlen, and the refined sizes when multires != 0. */
+int afid_read_continua_master(const char *dir, int multires, afid_continua_master_t *m);
+/* Same-grid restart into the current grid described by cur (time ignored): AFID_E_INVALID when
+ * |ylen - ylen_old| or |zlen - zlen_old| > 1e-8, or when any size, istr3, str3 (1e-8) or refined
+ * size differs (the reference interpolates then; that branch is not provided).  Fields are read
+ * into the packed host arrays; pr only when continua_pr.h5 exists (*pr_read = 1), salinity when
+ * cur->multires and sal != NULL.  *time_out gets the master's time. */
+int afid_read_flow_field(const char *dir, const afid_continua_master_t *cur, double *time_out, double *vx,
+                         double *vy, double *vz, double *temp, double *pr, int *pr_read, double *sal);
+
+/* Device context variants (salinity included when afid_gpu_sal_create was called). */
+int afid_gpu_write_flow_field(afid_ctx_t *ctx, const char *dir, int final, double save_3d,
+                              const afid_continua_master_t *m);
+/* Reads, uploads (RK3 history zeroed, salinity re-interpolated) and returns the master's time.
+ * When continua_pr.h5 is absent the pressure is uploaded as zero, as the reference leaves it. */
+int afid_gpu_read_flow_field(afid_ctx_t *ctx, const char *dir, const afid_continua_master_t *cur,
+                             double *time_out);
+
+/* afid_run with the restart and save points of the main loop in dir (NULL: same as afid_run).
+ * NREAD = 1 starts from dir's continua files (time from the master unless IRESET = 1); otherwise
+ * from the seeded initial condition.  Frames go to dir/fields, the final continua files to dir
+ * on a normal exit (steps done, 333 tmax, 555 ntst). */
+int afid_run_io(const afid_input_t *in, int precision, uint64_t seed, int nsteps, int stats_every,
+                afid_step_cb cb, void *user, const char *dir, afid_run_stats_t *stats);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* AFID_CONTINUA_H */

@@ -43,6 +43,7 @@ extern "C" {
 #define AFID_E_INVALID 603       /* bad argument / unsupported configuration                  */
 #define AFID_E_CUDA 604          /* CUDA runtime error (afid_gpu_cuda_error gives the code)   */
 #define AFID_E_CAPACITY 605      /* batch/server slots, HBM budget or a fixed scratch array exhausted */
+#define AFID_E_IO 606            /* restart file missing, unreadable or of an unsupported layout */
 
 /* precision of the explicit terms and transforms (the implicit solves are always FP64) */
 #define AFID_PREC_FP64 0
@@ -123,6 +124,8 @@ int afid_gpu_globals(afid_ctx_t *ctx, double ra_pr, double *nu_vol, double *ke, 
 /* ---- diagnostics ------------------------------------------------------------------------ */
 const char *afid_gpu_status_string(int status);
 int afid_gpu_cuda_error(afid_ctx_t *ctx);   /* last cudaError_t seen by this context */
+/* dims = {nxm, nym, nzm, nxmr, nymr, nzmr}; the refined sizes are 0 without salinity. */
+int afid_gpu_dims(afid_ctx_t *ctx, int dims[6]);
 /* Device pointer and x-stride (elements) of a resident field, for zero-copy interop.
  * which: 0 vx, 1 vy, 2 vz, 3 temp, 4 pr. */
 int afid_gpu_field_device_ptr(afid_ctx_t *ctx, int which, void **dptr, int *ldx);

@@ -20,7 +20,7 @@ FLAGSAL     FLAGPF
 
 Read flow / Reset logs
 NREAD       IRESET
-1           0
+{nread}           {ireset}
 
 Time steps / time limit (wall/flow)
 NTST        WALLTIMEMAX     TMAX
@@ -28,7 +28,7 @@ NTST        WALLTIMEMAX     TMAX
 
 Time interval for saving stats/movie frames
 TOUT    TFRAME  SAVE_3D
-{tout}     1.0     50.0
+{tout}     {tframe}     {save_3d}
 
 Domain size (keep ALX3 = 1.0)
 ALX3   YLEN   ZLEN
@@ -67,7 +67,8 @@ DEFAULTS = dict(nsst=3, ntst=9, tmax=1e30, tout=1e30, alx3=1.0, ylen=1.0, zlen=1
                 str3=2.0, rayt=1e6, prat=1.0, idtv=0, dt=1e-3, resid=1e-3, cflmax=10.0,
                 dtmax=1e-2, inslws=1, inslwn=1, tfixs=1, tfixn=1, active_t=1, gaxis=1,
                 xplusu=0.0, xminusu=0.0, dpdy=0.0, multires=0, flagsal=0, istr3r=0, rays=1e8,
-                pras=1.0, ffscales=0, sfixs=1, sfixn=1, active_s=0)
+                pras=1.0, ffscales=0, sfixs=1, sfixn=1, active_s=0, nread=1, ireset=0, tframe=1.0,
+                save_3d=50.0)
 
 
 def bou_text(nxm, nym, nzm, **kw) -> str:

@@ -1,0 +1,235 @@
+"""Restart files (include/afid_continua.h) on the CPU: the native HDF5 writer and reader against
+the oracle's restatement of the file format (oracle/afid_h5.py) and against a file written by the
+HDF5 library itself, and the continua file set of WriteFlowField.F90 / ReadFlowInterp.F90."""
+import os
+
+import numpy as np
+import pytest
+
+import afid_gpu as ag
+from helpers import bou_text
+from oracle import afid_h5 as h5
+
+SCIPY_DATA = None
+try:
+    import scipy.io.matlab as _m
+    SCIPY_DATA = os.path.join(os.path.dirname(_m.__file__), "tests", "data")
+except Exception:  # pragma: no cover
+    pass
+
+
+def _library_file():
+    if SCIPY_DATA is None:
+        pytest.skip("scipy test data not present")
+    path = os.path.join(SCIPY_DATA, "testhdf5_7.4_GLNX86.mat")
+    twin = os.path.join(SCIPY_DATA, "testdouble_7.1_GLNX86.mat")
+    if not (os.path.exists(path) and os.path.exists(twin)):
+        pytest.skip("scipy test data not present")
+    return path, twin
+
+
+def test_lookup3_known_answers():
+    """The self-test values of Bob Jenkins' lookup3.c (driver5)."""
+    assert h5.lookup3(b"") == 0xDEADBEEF
+    assert h5.lookup3(b"Four score and seven years ago") == 0x17770551
+    assert h5.lookup3(b"Four score and seven years ago", 1) == 0xCD628161
+
+
+def test_readers_match_a_file_written_by_the_hdf5_library():
+    """scipy's MATLAB 7.3 test file is an HDF5 file (512-byte user block, version-0 superblock)
+    written by the HDF5 library; its variable also ships in a MATLAB 5 file that scipy reads."""
+    from scipy.io import loadmat
+    path, twin = _library_file()
+    want = loadmat(twin)["testdouble"].astype(np.float64)        # (1, 9) in MATLAB's view
+    assert np.allclose(want.ravel(), np.pi / 4 * np.arange(9))
+    assert h5.names(path) == ["testdouble"]
+    got_oracle = h5.read(path, "testdouble")
+    assert got_oracle.shape == (9, 1)                             # column-major on disk
+    np.testing.assert_array_equal(got_oracle.ravel(), want.ravel())
+    assert ag.h5_info(path, "testdouble") == (ag.H5_F64, (9, 1))
+    np.testing.assert_array_equal(ag.h5_read(path, "testdouble").ravel(), want.ravel())
+    with pytest.raises(ag.AfidError) as e:
+        ag.h5_read(path, "nothere")
+    assert e.value.status == ag.AFID_E_IO
+
+
+def _datasets(rng):
+    d = {f"scalar_{c}": np.array([rng.integers(-2**31, 2**31 - 1)], dtype=np.int32) for c in "abcdefgh"}
+    d["time"] = np.array([0.125])
+    d["r1"] = rng.standard_normal(17)
+    d["r2"] = rng.standard_normal((5, 3))
+    d["r3"] = rng.standard_normal((4, 3, 9))
+    d["r4"] = rng.integers(-1000, 1000, (2, 3, 4, 5)).astype(np.int32)
+    d["empty"] = np.zeros((0, 4))
+    d["a_name_that_is_rather_long_for_a_dataset_" + "x" * 60] = np.array([1.0, -0.0, np.inf, np.nan])
+    return d
+
+
+def test_native_writer_output_reads_with_the_oracle(tmp_path):
+    """Sixteen datasets (two symbol table nodes under the B-tree), ranks 1-4, both types, an empty
+    dataset, special values; layout facts of the default HDF5 format checked on the bytes."""
+    rng = np.random.default_rng(3)
+    d = _datasets(rng)
+    path = str(tmp_path / "many.h5")
+    ag.h5_write(path, d)
+    f = h5.H5File(path)
+    assert (f.base, f.sb_version, f.so, f.sl) == (0, 0, 8, 8)
+    raw = open(path, "rb").read()
+    assert int.from_bytes(raw[40:48], "little") == len(raw)      # end-of-file address
+    assert sorted(f.root()) == sorted(d)
+    for k, v in d.items():
+        got = f.read(k)
+        assert got.dtype == v.dtype and got.shape == v.shape, k
+        np.testing.assert_array_equal(got, v)
+        nat = ag.h5_read(path, k)
+        assert nat.shape == v.shape
+        np.testing.assert_array_equal(nat, v.astype(np.float64))
+    # every dataset header is version 1 with dataspace, datatype, fill value and layout messages
+    for k, addr in f.root().items():
+        types = [t for t, _, _ in f.messages(addr)]
+        assert types == [0x01, 0x03, 0x05, 0x08], k
+
+
+def test_native_reader_takes_the_newer_layout(tmp_path):
+    """Superblock version 2, version-2 object headers, link-message root group, compact and
+    contiguous storage, big-endian and 32-bit types."""
+    rng = np.random.default_rng(4)
+    d = {"var": rng.standard_normal((3, 4, 5)), "small": np.arange(6, dtype=np.int32).reshape(2, 3),
+         "be": rng.standard_normal(7).astype(">f8"), "f32": rng.standard_normal(5).astype(np.float32),
+         "u16": np.arange(9, dtype=np.uint16), "i64": np.array([-3, 2**40], dtype=np.int64)}
+    path = str(tmp_path / "v2.h5")
+    h5.write_v2(path, d, compact=("small", "u16"))
+    f = h5.H5File(path)
+    assert f.sb_version == 2
+    for k, v in d.items():
+        np.testing.assert_array_equal(f.read(k), v)
+        np.testing.assert_array_equal(ag.h5_read(path, k), v.astype(np.float64))
+    assert ag.h5_info(path, "small") == (ag.H5_I32, (2, 3))
+
+
+def test_reader_refuses_damaged_files(tmp_path):
+    rng = np.random.default_rng(5)
+    path = str(tmp_path / "ok.h5")
+    ag.h5_write(path, {"var": rng.standard_normal((8, 8, 8))})
+    raw = open(path, "rb").read()
+    cases = {"truncated_meta": raw[:300], "truncated_data": raw[:len(raw) - 8], "garbage": bytes(rng.integers(0, 256, 4096, dtype=np.uint8)),
+             "empty": b""}
+    for name, blob in cases.items():
+        p = str(tmp_path / f"{name}.h5")
+        open(p, "wb").write(blob)
+        with pytest.raises(ag.AfidError) as e:
+            ag.h5_read(p, "var")
+        assert e.value.status == ag.AFID_E_IO, name
+    with pytest.raises(ag.AfidError) as e:
+        ag.h5_read(str(tmp_path / "missing.h5"), "var")
+    assert e.value.status == ag.AFID_E_IO
+    with pytest.raises(ag.AfidError) as e:
+        ag.h5_write(str(tmp_path / "dup.h5"), {"a/b": np.zeros(2)})
+    assert e.value.status == ag.AFID_E_INVALID
+
+
+def _input(**kw):
+    return ag.parse_bou_in(bou_text(16, 12, 8, **kw))
+
+
+def _fields(inp, rng, sal=False):
+    nx, nym, nzm = inp.nxm + 1, inp.nym, inp.nzm
+    f = {k: rng.standard_normal((nzm, nym, nx)) for k in ("vx", "vy", "vz", "temp", "pr")}
+    for k in ("vy", "vz", "temp", "pr"):
+        f[k][..., -1] = 0.0
+    if sal:
+        f["sal"] = rng.standard_normal((inp.nzmr, inp.nymr, inp.nxmr))
+    return f
+
+
+def test_continua_file_set_matches_the_reference_layout(tmp_path):
+    """WriteFlowField.F90(final=.true.): continua_{temp,vx,vy,vz,pr}.h5 with 'var' of dims
+    (nzm, nym, nx) and continua_master.h5 with the grid description; read back unchanged."""
+    inp = _input(multires=0)
+    rng = np.random.default_rng(6)
+    f = _fields(inp, rng)
+    m = ag.continua_master(inp, 1.25)
+    d = str(tmp_path / "outputdir")
+    ag.write_flow_field(d, m, f, final=True)
+    assert sorted(os.listdir(d)) == sorted(f"continua_{k}.h5" for k in ("master", "temp", "vx", "vy", "vz", "pr"))
+    for k in ("vx", "vy", "vz", "temp", "pr"):
+        p = os.path.join(d, f"continua_{k}.h5")
+        assert h5.names(p) == ["var"]
+        ds = h5.H5File(p).dataset("var")
+        assert ds.shape == (inp.nzm, inp.nym, inp.nxm + 1) and ds.dtype == np.dtype("<f8")
+        np.testing.assert_array_equal(h5.read(p, "var"), f[k])
+    mp = os.path.join(d, "continua_master.h5")
+    assert h5.names(mp) == sorted(["nx", "ny", "nz", "ylen", "zlen", "time", "istr3", "str3"])
+    want = dict(nx=inp.nxm + 1, ny=inp.nym + 1, nz=inp.nzm + 1, istr3=inp.istr3)
+    for k, v in want.items():
+        a = h5.read(mp, k)
+        assert a.dtype == np.dtype("<i4") and a.shape == (1,) and int(a[0]) == v, k
+    for k, v in dict(ylen=inp.ylen, zlen=inp.zlen, time=1.25, str3=inp.str3).items():
+        a = h5.read(mp, k)
+        assert a.dtype == np.dtype("<f8") and a.shape == (1,) and a[0] == v, k
+    back = ag.read_flow_field(d, ag.continua_master(inp))
+    assert back["time"] == 1.25
+    for k in ("vx", "vy", "vz", "temp", "pr"):
+        np.testing.assert_array_equal(back[k], f[k])
+
+
+def test_continua_with_refined_salinity(tmp_path):
+    """MULTIRES = 1: continua_sal.h5 on the refined grid with dims (nzmr, nymr, nxmr + 1), the
+    extra x node zero; nxr, nyr, nzr, istr3r in the master file."""
+    inp = _input(multires=1, nxmr=24, nymr=24, nzmr=16, flagsal=1, istr3r=4)
+    rng = np.random.default_rng(7)
+    f = _fields(inp, rng, sal=True)
+    m = ag.continua_master(inp, 0.5)
+    d = str(tmp_path / "out")
+    ag.write_flow_field(d, m, f, final=True)
+    sp = os.path.join(d, "continua_sal.h5")
+    s = h5.read(sp, "var")
+    assert s.shape == (16, 24, 25)
+    np.testing.assert_array_equal(s[..., :24], f["sal"])
+    assert np.all(s[..., 24] == 0.0)
+    mp = os.path.join(d, "continua_master.h5")
+    for k, v in dict(nxr=25, nyr=25, nzr=17, istr3r=4).items():
+        assert int(h5.read(mp, k)[0]) == v
+    back = ag.read_flow_field(d, ag.continua_master(inp), with_sal=True)
+    np.testing.assert_array_equal(back["sal"], f["sal"])
+    mm = ag.read_continua_master(d, multires=True)
+    assert (mm.nxr, mm.nyr, mm.nzr, mm.istr3r, mm.time) == (25, 25, 17, 4, 0.5)
+
+
+def test_frames_and_optional_pressure(tmp_path):
+    """final = .false. writes fields/NNNNN_* (NNNNN = nint(time/SAVE_3D)) without pr and without a
+    master; a restart without continua_pr.h5 leaves pr unread."""
+    inp = _input(multires=0)
+    rng = np.random.default_rng(8)
+    f = _fields(inp, rng)
+    d = str(tmp_path / "o")
+    m = ag.continua_master(inp, 2.6)
+    ag.write_flow_field(d, m, {k: f[k] for k in ("vx", "vy", "vz", "temp")}, final=False, save_3d=0.5)
+    assert sorted(os.listdir(os.path.join(d, "fields"))) == sorted(f"00005_{k}.h5" for k in ("temp", "vx", "vy", "vz"))
+    np.testing.assert_array_equal(h5.read(os.path.join(d, "fields", "00005_vz.h5"), "var"), f["vz"])
+    ag.write_flow_field(d, m, f, final=True)
+    os.remove(os.path.join(d, "continua_pr.h5"))
+    back = ag.read_flow_field(d, ag.continua_master(inp))
+    assert back["pr"] is None
+    np.testing.assert_array_equal(back["temp"], f["temp"])
+
+
+def test_restart_refuses_other_grids_and_domains(tmp_path):
+    """ReadFlowInterp.F90:76-89: a different Ly/Lz aborts; a different grid needs interpolation,
+    which this library does not provide (AFID_E_INVALID); no files: AFID_E_IO."""
+    inp = _input(multires=0)
+    rng = np.random.default_rng(9)
+    d = str(tmp_path / "o")
+    ag.write_flow_field(d, ag.continua_master(inp), _fields(inp, rng), final=True)
+    for kw in (dict(ylen=1.5), dict(zlen=0.5), dict(str3=3.0), dict(istr3=0)):
+        other = ag.parse_bou_in(bou_text(16, 12, 8, multires=0, **kw))
+        with pytest.raises(ag.AfidError) as e:
+            ag.read_flow_field(d, ag.continua_master(other))
+        assert e.value.status == ag.AFID_E_INVALID, kw
+    other = ag.parse_bou_in(bou_text(20, 12, 8, multires=0))
+    with pytest.raises(ag.AfidError) as e:
+        ag.read_flow_field(d, ag.continua_master(other))
+    assert e.value.status == ag.AFID_E_INVALID
+    with pytest.raises(ag.AfidError) as e:
+        ag.read_flow_field(str(tmp_path / "nothing"), ag.continua_master(inp))
+    assert e.value.status == ag.AFID_E_IO

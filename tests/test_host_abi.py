@@ -18,7 +18,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 def _declared_functions():
     names = set()
-    for h in ("afid_gpu.h", "afid_host.h", "afid_batch.h", "afid_serve.h", "afid_salinity.h"):
+    for h in ("afid_gpu.h", "afid_host.h", "afid_batch.h", "afid_serve.h", "afid_salinity.h", "afid_continua.h"):
         text = open(os.path.join(ROOT, "include", h)).read()
         text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
         names |= set(re.findall(r"\b(afid_\w+)\s*\(", text))
@@ -35,7 +35,7 @@ def test_library_exports_every_declared_symbol():
 
 
 def test_status_strings():
-    for s in (0, 8, 165, 166, 169, 444, 601, 602, 603, 604, 605):
+    for s in (0, 8, 165, 166, 169, 444, 601, 602, 603, 604, 605, 606):
         assert ag.lib().afid_gpu_status_string(s).decode() != "unknown status"
 
 
