@@ -1,11 +1,14 @@
 // afid_run — command-line drop-in for the reference's `afid` executable on the flow +
 // temperature path: reads bou.in from the working directory (ReadInputFile.F90:20) and runs
 // the main loop (main.F90:281-422) with the substep on the GPU.
-//   afid_run [--steps N] [--seed S] [--mixed] [--stats K] [bou.in]
+//   afid_run [--steps N] [--seed S] [--mixed] [--stats K] [--outputdir D] [bou.in]
+// With --outputdir the run reads D/continua_*.h5 when NREAD = 1 and writes the SAVE_3D frames and
+// the final continua files there, as the reference does in outputdir/.
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
 
+#include "afid_continua.h"
 #include "afid_host.h"
 
 static void on_step(int ntime, double time, double dt, double nu, double ke, void *) {
@@ -14,6 +17,7 @@ static void on_step(int ntime, double time, double dt, double nu, double ke, voi
 
 int main(int argc, char **argv) {
   const char *path = "bou.in";
+  const char *dir = nullptr;
   int steps = -1, stats = 0, prec = AFID_PREC_FP64;
   unsigned long long seed = 20261203ULL;
   for (int a = 1; a < argc; ++a) {
@@ -21,6 +25,7 @@ int main(int argc, char **argv) {
     else if (!std::strcmp(argv[a], "--seed") && a + 1 < argc) seed = std::strtoull(argv[++a], nullptr, 10);
     else if (!std::strcmp(argv[a], "--stats") && a + 1 < argc) stats = std::atoi(argv[++a]);
     else if (!std::strcmp(argv[a], "--mixed")) prec = AFID_PREC_MIXED;
+    else if (!std::strcmp(argv[a], "--outputdir") && a + 1 < argc) dir = argv[++a];
     else path = argv[a];
   }
   afid_input_t in;
@@ -30,7 +35,7 @@ int main(int argc, char **argv) {
     return 2;
   }
   afid_run_stats_t st;
-  s = afid_run(&in, prec, seed, steps, stats, stats > 0 ? on_step : nullptr, nullptr, &st);
+  s = afid_run_io(&in, prec, seed, steps, stats, stats > 0 ? on_step : nullptr, nullptr, dir, &st);
   if (s != AFID_OK) {
     std::fprintf(stderr, "afid_run: %s\n", afid_gpu_status_string(s));
     return 1;
