@@ -171,7 +171,7 @@ EXPORTS = [
     "afid_gpu_sal_interpolate", "afid_gpu_sal_cfl", "afid_gpu_sal_profiles", "afid_gpu_sal_download_aux",
     "afid_gpu_dims", "afid_h5_write", "afid_h5_info", "afid_h5_read_f64", "afid_continua_master_from_input",
     "afid_write_flow_field", "afid_read_continua_master", "afid_read_flow_field", "afid_gpu_write_flow_field",
-    "afid_gpu_read_flow_field", "afid_run_io",
+    "afid_gpu_read_flow_field", "afid_run_io", "afid_read_flow_interp", "afid_gpu_read_flow_interp",
 ]
 
 
@@ -286,6 +286,9 @@ def load_library(path: str = _LIB_PATH) -> C.CDLL:
         "afid_gpu_write_flow_field": (i, [vp, C.c_char_p, i, d, C.POINTER(ContinuaMasterT)]),
         "afid_gpu_read_flow_field": (i, [vp, C.c_char_p, C.POINTER(ContinuaMasterT), _dp]),
         "afid_run_io": (i, [C.POINTER(InputT), i, C.c_uint64, i, i, vp, vp, C.c_char_p, C.POINTER(RunStatsT)]),
+        "afid_read_flow_interp": (i, [C.c_char_p, C.POINTER(InputT), _dp, _dp, _dp, _dp, _dp, _dp, C.POINTER(i),
+                                      C.POINTER(i), _dp]),
+        "afid_gpu_read_flow_interp": (i, [vp, C.c_char_p, C.POINTER(InputT), _dp, C.POINTER(i)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -854,6 +857,20 @@ def read_flow_field(directory: str, current: ContinuaMasterT, with_sal: bool = F
         f["pr"] = None
     f["sal"] = sal
     f["time"] = t.value
+    return f
+
+
+def read_flow_interp(directory: str, inp: InputT) -> dict:
+    """afid_read_flow_interp (either branch of ReadFlowInterp) for the run described by inp."""
+    shape = (inp.nzm, inp.nym, inp.nxm + 1)
+    f = {k: np.zeros(shape) for k in ("vx", "vy", "vz", "temp", "pr")}
+    sal = np.zeros((inp.nzmr, inp.nymr, inp.nxmr)) if inp.multires else None
+    t, pr_read, interp = C.c_double(), C.c_int(), C.c_int()
+    _check(lib().afid_read_flow_interp(directory.encode(), C.byref(inp), C.byref(t), _ptr(f["vx"]), _ptr(f["vy"]),
+                                       _ptr(f["vz"]), _ptr(f["temp"]), _ptr(f["pr"]), C.byref(pr_read),
+                                       C.byref(interp), _ptr(sal) if sal is not None else None),
+           "afid_read_flow_interp")
+    f.update(sal=sal, time=t.value, pr_read=bool(pr_read.value), interpolated=bool(interp.value))
     return f
 
 

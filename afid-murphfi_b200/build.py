@@ -25,7 +25,7 @@ CXXFLAGS = ["-std=c++17", "-O2", "-fPIC", "-I" + INC, "-I/usr/local/cuda/include
 
 SOURCES = ["afid_k1_fp64.cu", "afid_k1_mixed.cu", "afid_k1_sal.cu", "afid_kernels.cu", "afid_api.cu", "afid_noalloc.cu",
            "afid_batch.cu", "afid_stats.cu", "afid_salinity.cu", "afid_host.cpp", "afid_mgrd.cpp",
-           "afid_serve.cpp", "afid_continua.cpp"]
+           "afid_serve.cpp", "afid_continua.cpp", "afid_restart.cpp"]
 
 
 def _newer(target: str, deps) -> bool:

@@ -516,8 +516,8 @@ int afid_run_io(const afid_input_t *in, int precision, uint64_t seed, int nsteps
   double time = 0.0;
   afid_continua_master_t master{};
   afid_continua_master_from_input(in, 0.0, &master);
-  if (s == AFID_OK && dir && in->nread) {  // ReadFlowInterp (main.F90:157-161), same grid
-    s = afid_gpu_read_flow_field(ctx, dir, &master, &time);
+  if (s == AFID_OK && dir && in->nread) {  // ReadFlowInterp (main.F90:157-161)
+    s = afid_gpu_read_flow_interp(ctx, dir, in, &time, nullptr);
     if (in->ireset) time = 0.0;           // ReadFlowInterp.F90:173
   } else if (s == AFID_OK) {
     std::vector<double> temp((size_t)nx * nym * nzm, 0.0);

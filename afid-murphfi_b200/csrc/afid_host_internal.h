@@ -31,4 +31,16 @@ void second_derivative_coeff(std::vector<double> &ap3, std::vector<double> &ac3,
 // Wall-normal faces of grid type istr3 (0, 1, 2, 3, 4, 6, 7); AFID_E_INVALID otherwise.
 int x_grid(int istr3, int nxm, double L, double s, double pi, double schmidt, std::vector<double> &xc);
 
+// Hermite stencils of multires/HermiteInterpolations.F90 (afid_mgrd.cpp).
+// :26-57: idx[io], io = 0 .. n_old+1 (Fortran values), the first new index at or past x_old(io).
+std::vector<int> interpolation_indices(const std::vector<double> &x_old, const std::vector<double> &x_new,
+                                       double x_len);
+// :105-164: weights cx[4*(in-1) + a] of every new point; axis 'x' (walls, linear at the ends),
+// 'y' or 'z' (periodic).
+std::vector<double> construct_stencil(const std::vector<double> &x_old, const std::vector<double> &x_new,
+                                      double x_len, const std::vector<int> &idx, char axis);
+// Per-target form of the interval loops io = io_lo .. io_hi: the 0-based first source row of every
+// new point (Fortran io - 1, less one).  False if a point is covered twice or not at all.
+bool starts_from_intervals(const std::vector<int> &idx, int n_new, int io_lo, int io_hi, std::vector<int> &start);
+
 }  // namespace afid_hostd

@@ -15,7 +15,7 @@
 
 using afid_hostd::philox_u;
 
-namespace {
+namespace afid_hostd {
 
 // HermiteInterpolations.F90:26-57: idx[io], io = 0 .. n_old+1 (Fortran values, 1-based), the
 // first new index whose coordinate is >= x_old(io).
@@ -124,7 +124,11 @@ bool starts_from_intervals(const std::vector<int> &idx, int n_new, int io_lo, in
   return true;
 }
 
-}  // namespace
+}  // namespace afid_hostd
+
+using afid_hostd::construct_stencil;
+using afid_hostd::interpolation_indices;
+using afid_hostd::starts_from_intervals;
 
 struct afid_mgrd {
   afid_sal_grid_t view{};

@@ -13,10 +13,12 @@
  *   afid_read_flow_field         ReadFlowInterp.F90:76-171, same-grid branch: domain-size check,
  *                                grid check, then HdfReadContinua (h5tools/HdfReadContinua.F90) per
  *                                field; continua_pr.h5 is read only when it exists
+ *   afid_read_flow_interp        ReadFlowInterp.F90 with both branches: on another grid the fields are
+ *                                interpolated (InterpInputVel.F90, InterpInputSal.F90)
  *   afid_gpu_write_flow_field /  the same through a device context: download, write / read,
  *   afid_gpu_read_flow_field     upload (salinity included when the context has it)
  *   afid_run_io                  afid_run plus the main loop's restart and save points:
- *                                ReadFlowInterp when NREAD = 1 (main.F90:157-161), the start-up
+ *                                ReadFlowInterp (either branch) when NREAD = 1 (main.F90:157-161), the start-up
  *                                frame (main.F90:241), the SAVE_3D frames (main.F90:376-381) and
  *                                the final continua files on a normal exit (QuitRoutine.F90:37)
  *
@@ -92,11 +94,22 @@ int afid_write_flow_field(const char *dir, int final, double save_3d, const afid
 int afid_read_continua_master(const char *dir, int multires, afid_continua_master_t *m);
 /* Same-grid restart into the current grid described by cur (time ignored): AFID_E_INVALID when
  * |ylen - ylen_old| or |zlen - zlen_old| > 1e-8, or when any size, istr3, str3 (1e-8) or refined
- * size differs (the reference interpolates then; that branch is not provided).  Fields are read
+ * size differs (afid_read_flow_interp takes the interpolating branch then).  Fields are read
  * into the packed host arrays; pr only when continua_pr.h5 exists (*pr_read = 1), salinity when
  * cur->multires and sal != NULL.  *time_out gets the master's time. */
 int afid_read_flow_field(const char *dir, const afid_continua_master_t *cur, double *time_out, double *vx,
                          double *vy, double *vz, double *temp, double *pr, int *pr_read, double *sal);
+
+/* ReadFlowInterp.F90 as a whole for the run described by in: the same-grid branch above when
+ * the stored grid matches (*interpolated = 0), otherwise the interpolating branch
+ * (ReadFlowInterp.F90:85-136, *interpolated = 1): the old grid rebuilt from the master record
+ * (CreateOldGrid.F90), cell-centre Hermite stencils old -> new (CreateNewInputStencil.F90),
+ * velocities rebuilt from their interpolated gradients and temperature interpolated with the plate
+ * ghosts (InterpInputVel.F90), the refined salinity interpolated likewise (InterpInputSal.F90);
+ * the pressure is set to zero (*pr_read = 0).  Ly/Lz must match as in the same-grid branch, and a
+ * 2-D file restarts a 2-D run only. */
+int afid_read_flow_interp(const char *dir, const afid_input_t *in, double *time_out, double *vx, double *vy,
+                          double *vz, double *temp, double *pr, int *pr_read, int *interpolated, double *sal);
 
 /* Device context variants (salinity included when afid_gpu_sal_create was called). */
 int afid_gpu_write_flow_field(afid_ctx_t *ctx, const char *dir, int final, double save_3d,
@@ -105,6 +118,10 @@ int afid_gpu_write_flow_field(afid_ctx_t *ctx, const char *dir, int final, doubl
  * When continua_pr.h5 is absent the pressure is uploaded as zero, as the reference leaves it. */
 int afid_gpu_read_flow_field(afid_ctx_t *ctx, const char *dir, const afid_continua_master_t *cur,
                              double *time_out);
+
+/* afid_read_flow_interp, then upload (RK3 history zeroed, salinity re-interpolated). */
+int afid_gpu_read_flow_interp(afid_ctx_t *ctx, const char *dir, const afid_input_t *in, double *time_out,
+                              int *interpolated);
 
 /* afid_run with the restart and save points of the main loop in dir (NULL: same as afid_run).
  * NREAD = 1 starts from dir's continua files (time from the master unless IRESET = 1); otherwise

@@ -233,3 +233,156 @@ def test_restart_refuses_other_grids_and_domains(tmp_path):
     with pytest.raises(ag.AfidError) as e:
         ag.read_flow_field(str(tmp_path / "nothing"), ag.continua_master(inp))
     assert e.value.status == ag.AFID_E_IO
+
+
+# ---- the interpolating restart (ReadFlowInterp.F90:85-136) --------------------------------------
+from oracle import afid_oracle as o  # noqa: E402
+from oracle import afid_restart as rs  # noqa: E402
+from oracle import afid_salinity as sa  # noqa: E402
+
+
+def _old_files(tmp_path, old_kw, rng, sal=False, fields=None):
+    text = bou_text(*old_kw.pop("dims"), **old_kw)
+    inp = ag.parse_bou_in(text)
+    f = fields if fields is not None else _fields(inp, rng, sal=sal)
+    d = str(tmp_path / "old")
+    ag.write_flow_field(d, ag.continua_master(inp, 0.75), f, final=True)
+    return d, f
+
+
+INTERP_CASES = [
+    # (old grid, new grid): finer, coarser, other stretching, 2-D, other wall conditions
+    (dict(dims=(16, 12, 8)), dict(dims=(24, 18, 12), str3=3.0)),
+    (dict(dims=(24, 16, 12), istr3=0), dict(dims=(16, 12, 8))),
+    (dict(dims=(32, 24, 1)), dict(dims=(48, 16, 1), istr3=1, str3=1.5)),
+    (dict(dims=(16, 12, 8)), dict(dims=(20, 24, 6), inslwn=0, tfixn=0, rayt=-1e6)),
+    (dict(dims=(16, 12, 8)), dict(dims=(20, 12, 8), inslws=0, tfixs=0)),
+]
+
+
+@pytest.mark.parametrize("old_kw,new_kw", INTERP_CASES)
+def test_interpolating_restart_matches_oracle(tmp_path, old_kw, new_kw):
+    """InterpInputVel on another grid: native C++ against the NumPy restatement, 1e-13 of each
+    field's scale; the pressure is zero and the time comes from the master file."""
+    rng = np.random.default_rng(10)
+    d, _ = _old_files(tmp_path, dict(old_kw), rng)
+    new_text = bou_text(*new_kw["dims"], **{k: v for k, v in new_kw.items() if k != "dims"})
+    inp = ag.parse_bou_in(new_text)
+    got = ag.read_flow_interp(d, inp)
+    assert got["interpolated"] and not got["pr_read"] and got["time"] == 0.75
+    assert np.all(got["pr"] == 0.0)
+    g = o.create_grid(o.parse_bou_in(new_text))
+    m = rs.read_master(d, False)
+    old = {k: h5.read(os.path.join(d, f"continua_{k}.h5"), "var") for k in ("vx", "vy", "vz", "temp")}
+    want = rs.interp_input_vel(old, m, g)
+    for k in ("vx", "vy", "vz", "temp"):
+        scale = max(np.abs(want[k]).max(), 1e-300)
+        assert np.abs(got[k] - want[k]).max() < 1e-13 * scale, k
+
+
+def test_interpolating_restart_of_refined_salinity(tmp_path):
+    """InterpInputSal: the refined salinity from another refined grid (and another coarse grid)."""
+    rng = np.random.default_rng(11)
+    old_kw = dict(dims=(16, 12, 8), multires=1, nxmr=32, nymr=24, nzmr=16, flagsal=1, istr3r=4, rays=1e6)
+    d, f = _old_files(tmp_path, dict(old_kw), rng, sal=True)
+    new_text = bou_text(16, 12, 8, multires=1, nxmr=40, nymr=36, nzmr=12, flagsal=1, istr3r=0, rays=-1e6,
+                        sfixn=0)
+    inp = ag.parse_bou_in(new_text)
+    got = ag.read_flow_interp(d, inp)
+    assert got["interpolated"]
+    g = o.create_grid(o.parse_bou_in(new_text))
+    mg = sa.create_mgrd(g)
+    m = rs.read_master(d, True)
+    salo = h5.read(os.path.join(d, "continua_sal.h5"), "var")[..., :m.nxr - 1]
+    want = rs.interp_input_sal(salo, m, g, mg)
+    assert got["sal"].shape == want.shape == (12, 36, 40)
+    assert np.abs(got["sal"] - want).max() < 1e-13 * np.abs(want).max()
+    # the coarse grid did not change: the flow fields come through the same interpolation as
+    # the identity map (Hermite weights (0, 1, 0, 0) on coinciding points)
+    for k in ("temp",):
+        np.testing.assert_allclose(got[k][..., :16], f[k][..., :16], rtol=0, atol=1e-14)
+
+
+def _solenoidal(inp, rng):
+    """vx, vy from a stream function at the cell corners (discrete divergence zero), vz = 0."""
+    g = o.create_grid(o.parse_bou_in(bou_text(inp.nxm, inp.nym, inp.nzm, istr3=inp.istr3, str3=inp.str3)))
+    nxm, nym, nzm = inp.nxm, inp.nym, inp.nzm
+    nx = nxm + 1
+    xc = g.xc[:nx]
+    yc = np.arange(nym) / nym * inp.ylen
+    zz = np.arange(nzm)[:, None, None]
+    X, Y = xc[None, None, :], yc[None, :, None]
+    psi = np.sin(np.pi * X) ** 2 * (np.cos(2 * np.pi * Y / inp.ylen) + 0.3 * np.sin(4 * np.pi * Y / inp.ylen)) \
+        * (1.0 + 0.2 * np.cos(2 * np.pi * zz / max(nzm, 1)))
+    psi = psi + 0.01 * rng.standard_normal(psi.shape) * np.sin(np.pi * X) ** 2
+    dy = nym / inp.ylen
+    vx = (np.roll(psi, -1, axis=1) - psi) * dy                         # at (xc_k, ym_j)
+    vy = np.zeros_like(vx)
+    vy[..., :nxm] = -(psi[..., 1:] - psi[..., :nxm]) / (xc[1:] - xc[:nxm])   # at (xm_k, yc_j)
+    return dict(vx=vx, vy=vy, vz=np.zeros_like(vx), temp=np.zeros_like(vx), pr=np.zeros_like(vx))
+
+
+def _divergence(f, inp, xc):
+    nxm = inp.nxm
+    dy, dz = inp.nym / inp.ylen, inp.nzm / inp.zlen
+    dvx = (f["vx"][..., 1:nxm + 1] - f["vx"][..., :nxm]) / (xc[1:] - xc[:nxm])
+    dvy = (np.roll(f["vy"], -1, axis=1) - f["vy"])[..., :nxm] * dy
+    dvz = (np.roll(f["vz"], -1, axis=0) - f["vz"])[..., :nxm] * dz
+    return dvx + dvy + dvz, np.abs(dvx).max()
+
+
+@pytest.mark.parametrize("dims_old,dims_new", [((16, 24, 4), (24, 36, 6)), ((32, 32, 1), (20, 48, 1))])
+def test_interpolating_restart_keeps_a_solenoidal_field_solenoidal(tmp_path, dims_old, dims_new):
+    """The velocity is rebuilt from interpolated gradients, so a discretely divergence-free field
+    stays divergence-free on the new grid away from the periodic seams (the last y row and z plane
+    close through the first one), to round-off of the gradient scale."""
+    rng = np.random.default_rng(12)
+    old_inp = ag.parse_bou_in(bou_text(*dims_old))
+    f = _solenoidal(old_inp, rng)
+    div_old, _ = _divergence(f, old_inp, o.create_grid(o.parse_bou_in(bou_text(*dims_old))).xc[:dims_old[0] + 1])
+    assert np.abs(div_old).max() < 1e-10
+    d = str(tmp_path / "old")
+    ag.write_flow_field(d, ag.continua_master(old_inp, 0.0), f, final=True)
+    new_inp = ag.parse_bou_in(bou_text(*dims_new))
+    got = ag.read_flow_interp(d, new_inp)
+    xc = o.create_grid(o.parse_bou_in(bou_text(*dims_new))).xc[:dims_new[0] + 1]
+    div, scale = _divergence(got, new_inp, xc)
+    inner = div[:max(dims_new[2] - 1, 1), :dims_new[1] - 1, :]
+    assert np.abs(inner).max() < 1e-11 * scale
+
+
+def test_interpolating_restart_resolves_smooth_fields(tmp_path):
+    """A smooth temperature onto a finer, differently stretched grid: cubic Hermite accuracy."""
+    old_inp = ag.parse_bou_in(bou_text(32, 32, 16))
+    g0 = o.create_grid(o.parse_bou_in(bou_text(32, 32, 16)))
+    new_text = bou_text(48, 40, 24, istr3=0)
+    g1 = o.create_grid(o.parse_bou_in(new_text))
+
+    def field(g, nxm, nym, nzm):
+        x = np.append(g.xm[:nxm], 0.0)[None, None, :]
+        y = g.ym[None, :, None]
+        z = g.zm[:, None, None]
+        t = 0.5 - x + 0.1 * np.sin(np.pi * x) * np.cos(2 * np.pi * y) * np.cos(2 * np.pi * z)
+        t[..., -1] = 0.0
+        return np.broadcast_to(t, (nzm, nym, nxm + 1)).copy()
+    rng = np.random.default_rng(13)
+    f = _fields(old_inp, rng)
+    f["temp"] = field(g0, 32, 32, 16)
+    d = str(tmp_path / "old")
+    ag.write_flow_field(d, ag.continua_master(old_inp, 0.0), f, final=True)
+    got = ag.read_flow_interp(d, ag.parse_bou_in(new_text))
+    want = field(g1, 48, 40, 24)
+    assert np.abs(got["temp"][..., :48] - want[..., :48]).max() < 2e-4
+
+
+def test_interpolating_restart_refusals(tmp_path):
+    rng = np.random.default_rng(14)
+    d, f = _old_files(tmp_path, dict(dims=(16, 12, 8)), rng)
+    same = ag.read_flow_interp(d, ag.parse_bou_in(bou_text(16, 12, 8)))
+    assert not same["interpolated"] and same["pr_read"]
+    for k in ("vx", "vy", "vz", "temp", "pr"):
+        np.testing.assert_array_equal(same[k], f[k])
+    for text in (bou_text(16, 12, 1), bou_text(16, 12, 8, ylen=2.0)):
+        with pytest.raises(ag.AfidError) as e:
+            ag.read_flow_interp(d, ag.parse_bou_in(text))
+        assert e.value.status == ag.AFID_E_INVALID
