@@ -588,6 +588,13 @@ class Solver:
                "afid_gpu_read_flow_field")
         return t.value
 
+    def read_flow_interp(self, directory: str, inp: "InputT") -> tuple:
+        """ReadFlowInterp (either branch) onto this context; returns (time, interpolated)."""
+        t, interp = C.c_double(), C.c_int()
+        _check(lib().afid_gpu_read_flow_interp(self._h, directory.encode(), C.byref(inp), C.byref(t),
+                                               C.byref(interp)), "afid_gpu_read_flow_interp")
+        return t.value, bool(interp.value)
+
     def set_k1_shape(self, index: int) -> None:
         _check(lib().afid_gpu_set_k1_shape(self._h, index), "afid_gpu_set_k1_shape")
 

@@ -115,3 +115,31 @@ def test_salinity_restart_through_files(tmp_path):
         assert rel_l2(fb[f], fa[f]) < 1e-12, f
     s = h5.read(os.path.join(d, "continua_sal.h5"), "var")
     assert s.shape == (16, 32, 33) and np.all(s[..., 32] == 0.0)
+
+
+def test_restart_on_another_grid(tmp_path):
+    """NREAD = 1 with continua files from a coarser grid: the interpolating restart uploads what
+    the host interpolation produces, and afid_run_io carries on from it."""
+    kw = dict(idtv=0, dt=1e-3, save_3d=1e30, tframe=1e30, ntst=1000)
+    d = str(tmp_path / "run")
+    first = ag.parse_bou_in(bou_text(16, 16, 8, nread=0, **kw))
+    st = ag.RunStatsT()
+    assert ag.lib().afid_run_io(ctypes.byref(first), ag.PREC_FP64, 9, 3, 0, None, None, d.encode(),
+                                ctypes.byref(st)) == 0
+    text = bou_text(24, 20, 12, nread=1, **kw)
+    second = ag.parse_bou_in(text)
+    host = ag.read_flow_interp(d, second)
+    assert host["interpolated"]
+    tables = ag.Tables(second)
+    with ag.Solver(tables.grid, tables.params) as sv:
+        t, interp = sv.read_flow_interp(d, second)
+        assert interp and t == st.time
+        got = sv.download()
+    for f in ("vx", "vy", "vz", "temp"):
+        np.testing.assert_array_equal(got[f][..., :24], host[f][..., :24])
+    assert np.all(got["pr"] == 0.0)
+    st2 = ag.RunStatsT()
+    assert ag.lib().afid_run_io(ctypes.byref(second), ag.PREC_FP64, 9, 2, 0, None, None, d.encode(),
+                                ctypes.byref(st2)) == 0
+    assert st2.steps_done == 2 and np.isfinite(st2.nu_vol) and np.isfinite(st2.ke) and st2.divmax < 1e-10
+    assert ag.read_continua_master(d).nx == 25
