@@ -425,6 +425,23 @@ __device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t by
       "l"(src), "r"(bytes), "r"(smem_u32(bar))
       : "memory");
 }
+// Per-thread asynchronous copy of one BYTES-sized element (4, 8 or 16) global -> shared, with
+// zero fill when `valid` is false (no byte is read then; src must still be a mapped address).
+// Completed by cp_async_wait_all() in the issuing thread; a barrier publishes it to the block.
+template <int BYTES>
+__device__ __forceinline__ void cp_async_zfill(void *dst, const void *src, bool valid) {
+  static_assert(BYTES == 4 || BYTES == 8 || BYTES == 16, "cp.async element size");
+  const int n = valid ? BYTES : 0;
+  if constexpr (BYTES == 16)
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(smem_u32(dst)), "l"(src), "r"(n)
+                 : "memory");
+  else
+    asm volatile("cp.async.ca.shared.global [%0], [%1], %2, %3;" ::"r"(smem_u32(dst)), "l"(src), "n"(BYTES),
+                 "r"(n)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
 // Wait for the given phase parity; gives up after `limit` polls and returns false.
 __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, long long limit) {
   const uint32_t addr = smem_u32(bar);

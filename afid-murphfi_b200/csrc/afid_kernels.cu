@@ -781,15 +781,18 @@ __global__ void __launch_bounds__(256)
   const size_t zstride = (size_t)g.nyh * g.ldxc;
   C *base = spec + (size_t)ky * g.ldxc + k0;
   const int nvalid = min(8, g.nxm - k0);
-#pragma unroll 4
-  for (int e = threadIdx.x; e < N * 8; e += blockDim.x) {
+  // the whole tile in flight at once: N1 asynchronous element copies per thread (256 threads,
+  // N * 8 = 256 * N1 elements), zero-filled past nxm
+#pragma unroll
+  for (int it = 0; it < N1; ++it) {
+    const int e = threadIdx.x + 256 * it;
     const int ex = e & 7, iz = e >> 3;
-    C v;
-    v.x = 0;
-    v.y = 0;
-    if (ex < nvalid) v = base[(size_t)iz * zstride + ex];
-    s[iz * 8 + (ex ^ zsw(iz))] = v;
+    const bool ok = ex < nvalid;
+    cp_async_zfill<(int)sizeof(C)>(&s[iz * 8 + (ex ^ zsw(iz))], ok ? (const void *)(base + (size_t)iz * zstride + ex)
+                                                                  : (const void *)base,
+                                   ok);
   }
+  cp_async_wait_all();
   __syncthreads();
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   C x[N1];
@@ -814,41 +817,53 @@ __global__ void __launch_bounds__(256)
   }
 }
 
-// K6w: backward y c2r.  Block: 16 x points = 8 pairs (8 warps) at one z index i.
+// K6w: backward y c2r.  Block: 16 x points = 8 pairs (8 warps) at one z index i.  The half
+// spectrum rows 0 .. N/2 of the 16 x points are staged with asynchronous copies (all in flight
+// at once); each warp then builds its packed sequence straight from them.
 template <int N1, typename TS>
 __global__ void __launch_bounds__(256)
     k_ifft_y_w(Geom g, const typename Cplx<TS>::type *__restrict__ spec, TS *__restrict__ phi,
                const typename Cplx<TS>::type *__restrict__ tw) {
   using C = typename Cplx<TS>::type;
   constexpr int N = 32 * N1;
+  constexpr int NH = N / 2 + 1;
   extern __shared__ __align__(16) unsigned char smem_k6w[];
-  C *T = reinterpret_cast<C *>(smem_k6w);  // [N][8] swizzled
+  C *T = reinterpret_cast<C *>(smem_k6w);  // [N][8] swizzled (output transposition)
+  C *R = T;                                 // [NH][16], element (jj, c) at jj*16 + (c ^ 2(jj & 7))
   const TS *Tr = reinterpret_cast<const TS *>(smem_k6w);
   const int k0 = blockIdx.x * 16, i = blockIdx.y;
   if (!inst_active(g, i)) return;
-#pragma unroll 4
-  for (int e = threadIdx.x; e < N * 8; e += blockDim.x) {
-    const int p = e & 7, j = e >> 3;
-    const bool cj = (2 * j > N);
-    const int jj = cj ? N - j : j;
-    const int ka = k0 + 2 * p, kb = ka + 1;
-    const C *src = spec + (size_t)(jj + (size_t)g.nyh * i) * g.ldxc;
-    C X, Y;
-    X.x = 0; X.y = 0; Y.x = 0; Y.y = 0;
-    if (ka < g.nxm) X = src[ka];
-    if (kb < g.nxm) Y = src[kb];
-    if (cj) { X.y = -X.y; Y.y = -Y.y; }
-    if (jj == 0 || 2 * jj == N) { X.y = 0; Y.y = 0; }
-    C Z;
-    Z.x = X.x - Y.y;
-    Z.y = X.y + Y.x;
-    T[tsw(j, p)] = Z;
+  const C *src0 = spec + (size_t)g.nyh * i * g.ldxc + k0;
+  const int nvalid = min(16, g.nxm - k0);
+  constexpr int kIt = (NH * 16 + 255) / 256;
+#pragma unroll
+  for (int it = 0; it < kIt; ++it) {
+    const int e = threadIdx.x + 256 * it;
+    if (e < NH * 16) {
+      const int c = e & 15, jj = e >> 4;
+      const bool ok = c < nvalid;
+      cp_async_zfill<(int)sizeof(C)>(&R[jj * 16 + (c ^ ((jj & 7) << 1))],
+                                     ok ? (const void *)(src0 + (size_t)jj * g.ldxc + c) : (const void *)src0, ok);
+    }
   }
+  cp_async_wait_all();
   __syncthreads();
   const int lane = threadIdx.x & 31, p = threadIdx.x >> 5;
   C x[N1];
 #pragma unroll
-  for (int m = 0; m < N1; ++m) x[m] = T[tsw(lane + 32 * m, p)];
+  for (int m = 0; m < N1; ++m) {
+    // row j of the full spectrum from row jj of the half spectrum (conjugate above N/2); the
+    // pair (x points k0 + 2p, k0 + 2p + 1) packed as X + iY
+    const int j = lane + 32 * m;
+    const bool cj = (2 * j > N);
+    const int jj = cj ? N - j : j;
+    const int sw = (jj & 7) << 1;
+    C X = R[jj * 16 + ((2 * p) ^ sw)], Y = R[jj * 16 + ((2 * p + 1) ^ sw)];
+    if (cj) { X.y = -X.y; Y.y = -Y.y; }
+    if (jj == 0 || 2 * jj == N) { X.y = 0; Y.y = 0; }
+    x[m].x = X.x - Y.y;
+    x[m].y = X.y + Y.x;
+  }
   warp_fft<true, TS, N1>(x, lane, tw);
   __syncthreads();
   const int rl = bitrev5(lane);
@@ -969,9 +984,11 @@ static cudaError_t launch_w_n1(const LaunchCtx &L, const SubstepBuffers &b, int 
       kern<<<grid, 256, sm, L.stream>>>(g, L.t, b.sc, ns, b.vx_o, b.vy_o, b.vz_o, spec, (const C *)L.twy,
                                         b.fft_field);
     } else {
+      // the staged half spectrum [N/2 + 1][16] is 16 elements larger than the [N][8] tile
+      const size_t sm6 = (size_t)(N * 8 + 16) * sizeof(C);
       auto kern = k_ifft_y_w<N1, TS>;
-      cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-      kern<<<grid, 256, sm, L.stream>>>(g, spec, (TS *)b.phi, (const C *)L.twy);
+      cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm6);
+      kern<<<grid, 256, sm6, L.stream>>>(g, spec, (TS *)b.phi, (const C *)L.twy);
     }
     return cudaGetLastError();
   }
