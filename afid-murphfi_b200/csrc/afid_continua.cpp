@@ -357,6 +357,10 @@ class Reader {
   // Read count elements of dataset d converted to double.
   bool read_f64(const DsInfo &d, double *out, int64_t count) {
     const size_t es = (size_t)d.size;
+    const uint16_t probe = 1;
+    const bool host_le = *reinterpret_cast<const uint8_t *>(&probe) == 1;
+    if (d.cls == 1 && es == 8 && !d.big_endian && host_le && d.allocated && !d.compact)
+      return raw(base_ + d.addr, out, (size_t)count * 8);  // the on-disk bytes are the host's doubles
     const size_t chunk = 1 << 20;  // elements per pass
     std::vector<uint8_t> buf;
     for (int64_t i0 = 0; i0 < count; i0 += (int64_t)chunk) {

@@ -291,6 +291,8 @@ def run_gpu(args):
     h2d = field_bytes / args.steps
     d2h = field_bytes / args.steps + 8 + 3 * 8
 
+    restart = restart_io(ag, solver, inp) if (args.restart_io and rank == 0) else None
+
     cpu = None
     parity = None
     if rank == 0 and not args.no_cpu_baseline:
@@ -342,6 +344,8 @@ def run_gpu(args):
             line["accuracy_vs_fp64"] = accuracy
         if parity is not None:
             line["parity_vs_cpu_port"] = parity
+        if restart is not None:
+            line["restart_io"] = restart
         print(json.dumps(line), flush=True)
     if world > 1:
         import torch.distributed as dist
@@ -929,6 +933,36 @@ def cpu_baseline(w: dict, steps: int, budget_s: float = 60.0, keep_state: bool =
     return out
 
 
+def restart_io(ag, solver, inp):
+    """The restart files of the resident state: WriteFlowField (download + HDF5 write of the five
+    continua files and the master file) and ReadFlowInterp's same-grid branch (HDF5 read +
+    upload), host wall clock; the state read back must equal the state written."""
+    import shutil
+    import tempfile
+
+    import numpy as np
+    d = tempfile.mkdtemp(prefix="afid_continua_")
+    try:
+        before = solver.download()
+        master = ag.continua_master(inp, 0.0)
+        t0 = time.perf_counter()
+        solver.write_flow_field(d, master, final=True)
+        t1 = time.perf_counter()
+        _, interpolated = solver.read_flow_interp(d, inp)
+        solver.synchronize()
+        t2 = time.perf_counter()
+        after = solver.download()
+        exact = all(np.array_equal(before[k], after[k]) for k in before)
+        nbytes = sum(os.path.getsize(os.path.join(d, f)) for f in os.listdir(d))
+    finally:
+        shutil.rmtree(d, ignore_errors=True)
+    return {"bytes": nbytes, "write_s": round(t1 - t0, 3), "read_s": round(t2 - t1, 3),
+            "write_GBps": round(nbytes / (t1 - t0) / 1e9, 2), "read_GBps": round(nbytes / (t2 - t1) / 1e9, 2),
+            "interpolated": interpolated, "roundtrip_exact": exact,
+            "note": "continua_{vx,vy,vz,temp,pr}.h5 + continua_master.h5 in a temporary directory on the "
+                    "host's local disk (page cache), via afid_gpu_write_flow_field / afid_gpu_read_flow_interp"}
+
+
 def parity_vs_cpu(ag, w, inp, temp0, cpu):
     """The default workload's fields at full size: the GPU path replays the C restatement's dt sequence from
     the same initial state; relative L2 per field (pressure modulo its mean)."""
@@ -1011,6 +1045,7 @@ def main():
     ap.add_argument("--policy", default="shortest", choices=["fifo", "shortest"])
     ap.add_argument("--cpu-steps", type=int, default=10)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--restart-io", action="store_true", help="rbc3d: time writing and reading the restart files")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
