@@ -723,7 +723,7 @@ extern "C" int afid_write_flow_field(const char *dir, int final, double save_3d,
     base += "/continua";
   } else {  // WriteFlowField.F90:22-26: frame = nint(time / save_3D), written as i5.5
     if (!(save_3d > 0.0)) return AFID_E_INVALID;
-    const double fr = std::nearbyint(m->time / save_3d);
+    const double fr = std::round(m->time / save_3d);  // nint: halves away from zero
     if (!(fr >= 0.0 && fr <= 99999.0)) return AFID_E_INVALID;
     char frame[8];
     std::snprintf(frame, sizeof(frame), "%05d", (int)fr);

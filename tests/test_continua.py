@@ -207,6 +207,11 @@ def test_frames_and_optional_pressure(tmp_path):
     ag.write_flow_field(d, m, {k: f[k] for k in ("vx", "vy", "vz", "temp")}, final=False, save_3d=0.5)
     assert sorted(os.listdir(os.path.join(d, "fields"))) == sorted(f"00005_{k}.h5" for k in ("temp", "vx", "vy", "vz"))
     np.testing.assert_array_equal(h5.read(os.path.join(d, "fields", "00005_vz.h5"), "var"), f["vz"])
+    # nint rounds halves away from zero: time / SAVE_3D = 2.5 is frame 00003, 4.5 is 00005
+    for t, frame in ((1.25, "00003"), (2.25, "00005")):
+        ag.write_flow_field(d, ag.continua_master(inp, t), {k: f[k] for k in ("vx", "vy", "vz", "temp")},
+                            final=False, save_3d=0.5)
+        assert os.path.exists(os.path.join(d, "fields", f"{frame}_temp.h5")), (t, frame)
     ag.write_flow_field(d, m, f, final=True)
     os.remove(os.path.join(d, "continua_pr.h5"))
     back = ag.read_flow_field(d, ag.continua_master(inp))

@@ -50,12 +50,13 @@ def test_restart_through_files_continues_the_run(tmp_path):
 
 def _replay_frames(t0, dt, nsteps, save_3d, tframe):
     """Frame numbers main.F90:241 and :376-381 produce for a fixed dt (same double arithmetic)."""
-    frames = [round(t0 / save_3d)]
+    nint = lambda v: int(math.floor(abs(v) + 0.5)) * (1 if v >= 0 else -1)  # noqa: E731  Fortran nint
+    frames = [nint(t0 / save_3d)]
     t = t0
     for _ in range(nsteps):
         t += dt
         if math.fmod(t, save_3d) < dt and math.floor(t / tframe) != 0:
-            frames.append(round(t / save_3d))
+            frames.append(nint(t / save_3d))
     return t, sorted(set(frames))
 
 
