@@ -913,17 +913,19 @@ def run_ddc(args):
         dist.destroy_process_group()
 
 
-def cpu_baseline(w: dict, steps: int, budget_s: float = 60.0, keep_state: bool = False):
-    """The CPU restatement (C + OpenMP, oracle/afid_cpu.c) on the same workload: up to
-    ``steps`` full main-loop steps, stopping once ``budget_s`` seconds have been spent.  With
-    ``keep_state`` the final fields and dt sequence come back under "_state" / "_dts"."""
+def cpu_baseline(w: dict, steps: int, budget_s: float = 60.0, keep_state: bool = False, warmup: int = 0):
+    """The CPU restatement (C + OpenMP, oracle/afid_cpu.c) on the same workload: ``warmup``
+    untimed main-loop steps, then up to ``steps`` timed ones, stopping once ``budget_s`` seconds
+    have been spent.  With ``keep_state`` the final fields and dt sequence come back under
+    "_state" / "_dts"."""
     try:
         sys.path.insert(0, os.path.join(ROOT, "oracle"))
         from oracle import cpu_port
     except Exception as e:  # pragma: no cover
         return {"unavailable": f"CPU port not importable: {e}"}
-    text = bou_text(w, steps)
-    res = cpu_port.time_steps(text, steps, seed=20261203, mixed=False, budget_s=budget_s, keep_state=keep_state)
+    text = bou_text(w, steps + warmup)
+    res = cpu_port.time_steps(text, steps, seed=20261203, mixed=False, budget_s=budget_s, keep_state=keep_state,
+                              warmup=warmup)
     out = {"value": round(res["mcells_per_s"], 4), "unit": "Mcell-RK3-steps/s",
            "cores": res["threads"], "kind": "port",
            "sample": f"{res['steps']} full steps of {w['name']} (C+OpenMP restatement)",
@@ -999,7 +1001,7 @@ def run_reference(args):
         cpu = ddc_cpu_baseline(budget_s=120.0)
     elif args.config in WORKLOADS:
         w = WORKLOADS[args.config]
-        cpu = cpu_baseline(w, args.steps + args.warmup, budget_s=120.0)
+        cpu = cpu_baseline(w, args.steps, budget_s=120.0, warmup=args.warmup)
     else:
         print(json.dumps({"impl": "reference", "unavailable": f"no CPU arm for the {args.config} workload"}),
               flush=True)
@@ -1014,7 +1016,8 @@ def run_reference(args):
         "unit": "Mcell-RK3-steps/s",
         "n_gpus": world,
         "steps": cpu.get("steps"),
-        "warmup": 0,
+        "steps_requested": args.steps if args.config in WORKLOADS else None,
+        "warmup": args.warmup if args.config in WORKLOADS else 0,
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,

@@ -90,20 +90,26 @@ class CpuSolver:
 
 
 def time_steps(bou_text: str, steps: int, seed: int = 20261203, mixed: bool = False,
-               budget_s: float = 1e30, keep_state: bool = False) -> dict:
+               budget_s: float = 1e30, keep_state: bool = False, warmup: int = 0) -> dict:
     """Main-loop steps (CFL -> dt rule -> TimeMarcher) of the C restatement on all host cores,
-    from the seeded initial state, stopping early once ``budget_s`` seconds have been spent;
-    returns the throughput in Mcell-RK3-steps/s and the steps actually timed (with
-    ``keep_state``, also the final fields and the dt of every step)."""
+    from the seeded initial state: ``warmup`` untimed steps, then up to ``steps`` timed ones,
+    stopping early once ``budget_s`` seconds of timed steps have been spent; returns the
+    throughput in Mcell-RK3-steps/s and the steps actually timed (with ``keep_state``, also the
+    final fields and the dt of every step, warm-up steps included)."""
     p = o.parse_bou_in(bou_text)
     g = o.create_grid(p)
     s = o.initial_state(g, seed)
     cpu = CpuSolver(g, s)
     dt = p.dt
+    dts = []
+    for n in range(warmup):
+        cflm = cpu.cfl()
+        dt, _, _ = o.next_dt(p, n, dt, cflm)
+        cpu.time_marcher(dt)
+        dts.append(dt)
     t0 = time.perf_counter()
     done = 0
-    dts = []
-    for n in range(steps):
+    for n in range(warmup, warmup + steps):
         cflm = cpu.cfl()
         dt, _, _ = o.next_dt(p, n, dt, cflm)
         cpu.time_marcher(dt)
