@@ -500,7 +500,7 @@ def run_batched(args):
     import torch
 
     world, rank, local = dist_setup()
-    insts = batch_instances()
+    insts = batch_instances(args.instances)
     precision = 1 if args.config == "batched" else 0
     bs = BatchSet(insts, precision)
     for _ in range(args.warmup):
@@ -560,7 +560,7 @@ def run_batched(args):
             "vs_baseline": None,
             "dtype": "f32+f64" if precision else "f64",
             "data": "synthetic: 256 Philox-drawn 2-D RBC instances, conductive state + seeded +-1e-3 perturbation",
-            "config": {"workload": "batched_256x2d_" + ("mixed" if precision else "fp64"),
+            "config": {"workload": f"batched_{len(insts)}x2d_" + ("mixed" if precision else "fp64"),
                        "instances": len(insts), "cells": bs.cells, "classes_nymxnxm": counts,
                        "dt": "CFL-limited per instance (CFLMAX 1.2; DTMAX = min(1e-2, 0.5 dy^2 min(Re, Pe)))",
                        "l2": "inputs larger than L2 (%.1f GB resident)" % (bs_bytes / 1e9),
@@ -1049,6 +1049,8 @@ def main():
     ap.add_argument("--cpu-steps", type=int, default=10)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--restart-io", action="store_true", help="rbc3d: time writing and reading the restart files")
+    ap.add_argument("--instances", type=int, default=256,
+                    help="batched: the first N instances of the 256-instance draw (profiling a smaller set)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
