@@ -351,7 +351,19 @@ class Reader {
       }
     }
     d.allocated = d.compact || (d.addr != undef_addr());
-    return have_space && have_type && have_layout;
+    if (!(have_space && have_type && have_layout)) return false;
+    // the shape must be non-negative, its element count must not overflow, and the data must
+    // lie inside the file (or inside the header, for compact storage)
+    uint64_t count = 1;
+    for (int i = 0; i < d.rank; ++i) {
+      if (d.dims[i] < 0 || (uint64_t)d.dims[i] > (1ull << 40)) return false;
+      if (d.dims[i] != 0 && count > (1ull << 48) / (uint64_t)d.dims[i]) return false;
+      count *= (uint64_t)d.dims[i];
+    }
+    const uint64_t bytes = count * (uint64_t)d.size;
+    if (d.compact) return bytes <= d.inline_data.size();
+    if (d.allocated) return d.addr <= fsize_ && base_ <= fsize_ - d.addr && bytes <= fsize_ - base_ - d.addr;
+    return true;
   }
 
   // Read count elements of dataset d converted to double.
