@@ -11,6 +11,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <map>
+#include <memory>
 #include <new>
 #include <sstream>
 #include <string>
@@ -269,11 +270,26 @@ int afid_read_bou_in(const char *path, afid_input_t *out) {
   return afid_parse_bou_in(s.c_str(), out);
 }
 
+static int tables_create(const afid_input_t *in, int precision, afid_tables_t **out);
+
 int afid_tables_create(const afid_input_t *in, int precision, afid_tables_t **out) {
   if (!in || !out) return AFID_E_INVALID;
   *out = nullptr;
-  if (in->nxm < 2 || in->nym < 1 || in->nzm < 1) return AFID_E_INVALID;
-  afid_tables_t *t = new (std::nothrow) afid_tables_t();
+  // sizes far beyond any grid one GPU can hold are input errors, not allocation requests (the
+  // host tables include two y-z planes of plate temperatures)
+  if (in->nxm < 2 || in->nym < 1 || in->nzm < 1 || in->nxm > (1 << 20) || in->nym > (1 << 20) ||
+      in->nzm > (1 << 20) || (long long)in->nym * in->nzm > (1LL << 28))
+    return AFID_E_INVALID;
+  try {
+    return tables_create(in, precision, out);
+  } catch (const std::bad_alloc &) {
+    return AFID_E_ALLOC;
+  }
+}
+
+static int tables_create(const afid_input_t *in, int precision, afid_tables_t **out) {
+  std::unique_ptr<afid_tables_t> holder(new (std::nothrow) afid_tables_t());  // freed on every early exit
+  afid_tables_t *t = holder.get();
   if (!t) return AFID_E_ALLOC;
   t->in = *in;
   const int nxm = in->nxm, nym = in->nym, nzm = in->nzm, nx = nxm + 1;
@@ -294,7 +310,6 @@ int afid_tables_create(const afid_input_t *in, int precision, afid_tables_t **ou
   uniform_grid(zc, zm, nzm, in->zlen);
   uniform_grid(yc, ym, nym, in->ylen);
   if (afid_hostd::x_grid(in->istr3, nxm, in->alx3, in->str3, pi, 1.0, xc) != AFID_OK) {
-    delete t;
     return AFID_E_INVALID;  // ISTR3=5 (scallop, channel-flow specific) is not on this path
   }
   // CreateGrid.F90:100-138
@@ -434,7 +449,7 @@ int afid_tables_create(const afid_input_t *in, int precision, afid_tables_t **ou
   p.precision = precision;
   p.tempbp = t->tempbp.data();
   p.temptp = t->temptp.data();
-  *out = t;
+  *out = holder.release();
   return AFID_OK;
 }
 

@@ -8,6 +8,7 @@
 #include <cmath>
 #include <cstring>
 #include <limits>
+#include <memory>
 #include <new>
 
 #include "afid_host_internal.h"
@@ -143,17 +144,30 @@ struct afid_mgrd {
 
 extern "C" {
 
+static int mgrd_create(const afid_tables_t *coarse, afid_mgrd_t **out);
+
 int afid_mgrd_create(const afid_tables_t *coarse, afid_mgrd_t **out) {
   if (!coarse || !out) return AFID_E_INVALID;
   *out = nullptr;
+  try {
+    return mgrd_create(coarse, out);
+  } catch (const std::bad_alloc &) {
+    return AFID_E_ALLOC;
+  }
+}
+
+static int mgrd_create(const afid_tables_t *coarse, afid_mgrd_t **out) {
   const afid_input_t &in = coarse->in;
   const int nxm = in.nxm, nym = in.nym, nzm = in.nzm;
   const int nxmr = in.nxmr, nymr = in.nymr, nzmr = in.nzmr;
   if (!in.multires || !in.flagsal || in.flagpf || in.melt) return AFID_E_INVALID;
-  if (nxmr < 3 || nymr < 1 || nzmr < 1 || nxmr > 1024) return AFID_E_INVALID;
+  if (nxmr < 3 || nymr < 1 || nzmr < 1 || nxmr > 1024 || nymr > (1 << 20) || nzmr > (1 << 20) ||
+      (long long)nymr * nzmr > (1LL << 28))
+    return AFID_E_INVALID;
   if ((nzm == 1) != (nzmr == 1)) return AFID_E_INVALID;
   if (in.gaxis < 1 || in.gaxis > 3) return AFID_E_INVALID;
-  afid_mgrd_t *m = new (std::nothrow) afid_mgrd_t();
+  std::unique_ptr<afid_mgrd_t> holder(new (std::nothrow) afid_mgrd_t());  // freed on every early exit
+  afid_mgrd_t *m = holder.get();
   if (!m) return AFID_E_ALLOC;
   const double pi = coarse->pi;
   // CreateMgrdGrid.F90:37-90: uniform y/z, wall-normal grid of type ISTR3R with STR3
@@ -161,7 +175,6 @@ int afid_mgrd_create(const afid_tables_t *coarse, afid_mgrd_t **out) {
   afid_hostd::uniform_grid(zcr, zmr, nzmr, in.zlen);
   afid_hostd::uniform_grid(ycr, ymr, nymr, in.ylen);
   if (afid_hostd::x_grid(in.istr3r, nxmr, in.alx3, in.str3, pi, in.pras, xcr) != AFID_OK || in.istr3r == 2) {
-    delete m;
     return AFID_E_INVALID;
   }
   const int nxr = nxmr + 1;
@@ -249,7 +262,6 @@ int afid_mgrd_create(const afid_tables_t *coarse, afid_mgrd_t **out) {
          starts_from_intervals(krangr, nzm, 0, nzmr, m->start[5]);
   }
   if (!ok) {
-    delete m;
     return AFID_E_INVALID;
   }
   m->arr["xcr"] = xcr;
@@ -294,7 +306,7 @@ int afid_mgrd_create(const afid_tables_t *coarse, afid_mgrd_t **out) {
     v.to_ref[d] = afid_stencil_t{(int)m->start[d].size(), m->start[d].data(), m->w[d].data()};
     v.to_coarse[d] = afid_stencil_t{(int)m->start[3 + d].size(), m->start[3 + d].data(), m->w[3 + d].data()};
   }
-  *out = m;
+  *out = holder.release();
   return AFID_OK;
 }
 

@@ -111,3 +111,16 @@ def test_next_dt_matches_oracle(idtv, ntime, cflm):
     assert err == erro
     assert dt.value == dto
     assert rep.value == repo
+
+
+def test_tables_refuse_absurd_sizes():
+    """Sizes far beyond what one GPU can hold are input errors answered with AFID_E_INVALID, not
+    host allocations that exhaust memory."""
+    import ctypes
+    for dims in ((2_000_000_000, 8, 8), (64, 2_000_000_000, 8), (64, 64, 2_000_000_000), (64, 30000, 30000),
+                 (-5, 8, 8), (64, 0, 8)):
+        inp = ag.parse_bou_in(bou_text(16, 12, 8))
+        inp.nxm, inp.nym, inp.nzm = dims
+        t = ctypes.c_void_p()
+        assert ag.lib().afid_tables_create(ctypes.byref(inp), 0, ctypes.byref(t)) == ag.AFID_E_INVALID, dims
+        assert not t.value
