@@ -26,6 +26,7 @@
 #include <vector>
 
 #include "afid_continua.h"
+#include "afid_host_internal.h"
 #include "afid_salinity.h"
 
 namespace {
@@ -109,133 +110,135 @@ bool write_all(FILE *f, const void *p, size_t n) { return n == 0 || std::fwrite(
 }  // namespace
 
 extern "C" int afid_h5_write(const char *path, int n, const afid_h5_dataset_t *sets) {
-  if (!path || n < 1 || !sets) return AFID_E_INVALID;
-  std::vector<int> order(n);
-  for (int i = 0; i < n; ++i) {
-    const afid_h5_dataset_t &d = sets[i];
-    if (!d.name || !d.name[0] || std::strlen(d.name) > 255 || std::strchr(d.name, '/')) return AFID_E_INVALID;
-    if (d.rank < 1 || d.rank > AFID_H5_MAX_RANK || (d.dtype != AFID_H5_F64 && d.dtype != AFID_H5_I32))
-      return AFID_E_INVALID;
-    for (int r = 0; r < d.rank; ++r)
-      if (d.dims[r] < 0) return AFID_E_INVALID;
-    if (elem_count(d) > 0 && !d.data) return AFID_E_INVALID;
-    order[i] = i;
-  }
-  std::sort(order.begin(), order.end(), [&](int a, int b) { return std::strcmp(sets[a].name, sets[b].name) < 0; });
-  for (int i = 1; i < n; ++i)
-    if (std::strcmp(sets[order[i - 1]].name, sets[order[i]].name) == 0) return AFID_E_INVALID;
-  const int nsnod = (n + 2 * kLeafK - 1) / (2 * kLeafK);
-  if (nsnod > 2 * kInternalK) return AFID_E_INVALID;  // one B-tree leaf level is enough here
-
-  // local heap data: "" at 0, then each name NUL-terminated and padded to 8 bytes
-  std::vector<uint64_t> name_off(n);
-  size_t heap_data = 8;
-  for (int i = 0; i < n; ++i) {
-    name_off[order[i]] = heap_data;
-    heap_data += pad8(std::strlen(sets[order[i]].name) + 1);
-  }
-  const size_t a_super = 0, a_root = 96;
-  const size_t root_len = 16 + 8 + 16;                       // prefix + symbol table message
-  const size_t a_heap = a_root + root_len, heap_hdr = 32;
-  const size_t a_heapdata = a_heap + heap_hdr;
-  const size_t a_btree = a_heapdata + heap_data;
-  const size_t a_snod = a_btree + kBtreeSize;
-  size_t a = a_snod + nsnod * kSnodSize;
-  std::vector<size_t> a_oh(n), a_raw(n);
-  std::vector<std::vector<uint8_t>> oh(n);
-  for (int i = 0; i < n; ++i) {  // headers first (their size does not depend on the raw address)
-    oh[i] = object_header_v1({{0x01, dataspace_msg(sets[i])},
-                              {0x03, datatype_msg(sets[i].dtype)},
-                              {0x05, {2, 2, 2, 1, 0, 0, 0, 0}},   // fill value v2: late, if set, defined, size 0
-                              {0x08, std::vector<uint8_t>(18, 0)}});
-    a_oh[i] = a;
-    a += oh[i].size();
-  }
-  for (int i = 0; i < n; ++i) {
-    a_raw[i] = a;
-    a += pad8((size_t)elem_count(sets[i]) * elem_size(sets[i].dtype));
-  }
-  const size_t eof = a;
-  for (int i = 0; i < n; ++i) {  // fill in the layout message: version 3, contiguous, address, size
-    const size_t lay = 16 + (8 + pad8(dataspace_msg(sets[i]).size())) + (8 + pad8(datatype_msg(sets[i].dtype).size())) +
-                       (8 + 8) + 8;
-    const uint64_t bytes = (uint64_t)elem_count(sets[i]) * elem_size(sets[i].dtype);
-    oh[i][lay] = 3;
-    oh[i][lay + 1] = 1;
-    for (int k = 0; k < 8; ++k) {
-      oh[i][lay + 2 + k] = (uint8_t)((uint64_t)a_raw[i] >> (8 * k));
-      oh[i][lay + 10 + k] = (uint8_t)(bytes >> (8 * k));
+  return afid_guard([&]() -> int {
+    if (!path || n < 1 || !sets) return AFID_E_INVALID;
+    std::vector<int> order(n);
+    for (int i = 0; i < n; ++i) {
+      const afid_h5_dataset_t &d = sets[i];
+      if (!d.name || !d.name[0] || std::strlen(d.name) > 255 || std::strchr(d.name, '/')) return AFID_E_INVALID;
+      if (d.rank < 1 || d.rank > AFID_H5_MAX_RANK || (d.dtype != AFID_H5_F64 && d.dtype != AFID_H5_I32))
+        return AFID_E_INVALID;
+      for (int r = 0; r < d.rank; ++r)
+        if (d.dims[r] < 0) return AFID_E_INVALID;
+      if (elem_count(d) > 0 && !d.data) return AFID_E_INVALID;
+      order[i] = i;
     }
-  }
+    std::sort(order.begin(), order.end(), [&](int a, int b) { return std::strcmp(sets[a].name, sets[b].name) < 0; });
+    for (int i = 1; i < n; ++i)
+      if (std::strcmp(sets[order[i - 1]].name, sets[order[i]].name) == 0) return AFID_E_INVALID;
+    const int nsnod = (n + 2 * kLeafK - 1) / (2 * kLeafK);
+    if (nsnod > 2 * kInternalK) return AFID_E_INVALID;  // one B-tree leaf level is enough here
 
-  Out m(a_snod + nsnod * kSnodSize);
-  // superblock version 0
-  std::memcpy(&m.b[a_super], kSig, 8);
-  m.put(13, 8, 1);                 // size of offsets
-  m.put(14, 8, 1);                 // size of lengths
-  m.put(16, kLeafK, 2);
-  m.put(18, kInternalK, 2);
-  m.put(24, 0, 8);                 // base address
-  m.put(32, kUndef, 8);            // free-space info
-  m.put(40, eof, 8);               // end of file
-  m.put(48, kUndef, 8);            // driver info
-  m.put(56, 0, 8);                 // root entry: link name offset
-  m.put(64, a_root, 8);            //   object header address
-  m.put(72, 1, 4);                 //   cache type 1: scratch holds B-tree and heap addresses
-  m.put(80, a_btree, 8);
-  m.put(88, a_heap, 8);
-  // root object header: one symbol table message
-  {
-    auto h = object_header_v1({{0x11, le_bytes({{a_btree, 8}, {a_heap, 8}})}});
-    std::memcpy(&m.b[a_root], h.data(), h.size());
-  }
-  // local heap
-  std::memcpy(&m.b[a_heap], "HEAP", 4);
-  m.put(a_heap + 8, heap_data, 8);
-  m.put(a_heap + 16, 1, 8);        // empty free list
-  m.put(a_heap + 24, a_heapdata, 8);
-  for (int i = 0; i < n; ++i) std::memcpy(&m.b[a_heapdata + name_off[i]], sets[i].name, std::strlen(sets[i].name));
-  // B-tree node (group, leaf level): keys are heap offsets of the largest name in each child
-  std::memcpy(&m.b[a_btree], "TREE", 4);
-  m.put(a_btree + 4, 0, 1);
-  m.put(a_btree + 5, 0, 1);
-  m.put(a_btree + 6, nsnod, 2);
-  m.put(a_btree + 8, kUndef, 8);
-  m.put(a_btree + 16, kUndef, 8);
-  size_t q = a_btree + 24;
-  m.put(q, 0, 8);
-  q += 8;
-  for (int c = 0; c < nsnod; ++c) {
-    const int last = std::min(n, (c + 1) * 2 * kLeafK) - 1;
-    m.put(q, a_snod + c * kSnodSize, 8);
-    m.put(q + 8, name_off[order[last]], 8);
-    q += 16;
-  }
-  // symbol table nodes
-  for (int c = 0; c < nsnod; ++c) {
-    const size_t s = a_snod + c * kSnodSize;
-    const int lo = c * 2 * kLeafK, hi = std::min(n, lo + 2 * kLeafK);
-    std::memcpy(&m.b[s], "SNOD", 4);
-    m.put(s + 4, 1, 1);
-    m.put(s + 6, hi - lo, 2);
-    for (int e = lo; e < hi; ++e) {
-      const size_t p = s + 8 + (e - lo) * kEntrySize;
-      m.put(p, name_off[order[e]], 8);
-      m.put(p + 8, a_oh[order[e]], 8);
+    // local heap data: "" at 0, then each name NUL-terminated and padded to 8 bytes
+    std::vector<uint64_t> name_off(n);
+    size_t heap_data = 8;
+    for (int i = 0; i < n; ++i) {
+      name_off[order[i]] = heap_data;
+      heap_data += pad8(std::strlen(sets[order[i]].name) + 1);
     }
-  }
+    const size_t a_super = 0, a_root = 96;
+    const size_t root_len = 16 + 8 + 16;                       // prefix + symbol table message
+    const size_t a_heap = a_root + root_len, heap_hdr = 32;
+    const size_t a_heapdata = a_heap + heap_hdr;
+    const size_t a_btree = a_heapdata + heap_data;
+    const size_t a_snod = a_btree + kBtreeSize;
+    size_t a = a_snod + nsnod * kSnodSize;
+    std::vector<size_t> a_oh(n), a_raw(n);
+    std::vector<std::vector<uint8_t>> oh(n);
+    for (int i = 0; i < n; ++i) {  // headers first (their size does not depend on the raw address)
+      oh[i] = object_header_v1({{0x01, dataspace_msg(sets[i])},
+                                {0x03, datatype_msg(sets[i].dtype)},
+                                {0x05, {2, 2, 2, 1, 0, 0, 0, 0}},   // fill value v2: late, if set, defined, size 0
+                                {0x08, std::vector<uint8_t>(18, 0)}});
+      a_oh[i] = a;
+      a += oh[i].size();
+    }
+    for (int i = 0; i < n; ++i) {
+      a_raw[i] = a;
+      a += pad8((size_t)elem_count(sets[i]) * elem_size(sets[i].dtype));
+    }
+    const size_t eof = a;
+    for (int i = 0; i < n; ++i) {  // fill in the layout message: version 3, contiguous, address, size
+      const size_t lay = 16 + (8 + pad8(dataspace_msg(sets[i]).size())) + (8 + pad8(datatype_msg(sets[i].dtype).size())) +
+                         (8 + 8) + 8;
+      const uint64_t bytes = (uint64_t)elem_count(sets[i]) * elem_size(sets[i].dtype);
+      oh[i][lay] = 3;
+      oh[i][lay + 1] = 1;
+      for (int k = 0; k < 8; ++k) {
+        oh[i][lay + 2 + k] = (uint8_t)((uint64_t)a_raw[i] >> (8 * k));
+        oh[i][lay + 10 + k] = (uint8_t)(bytes >> (8 * k));
+      }
+    }
 
-  FILE *f = std::fopen(path, "wb");
-  if (!f) return AFID_E_IO;
-  bool ok = write_all(f, m.b.data(), m.b.size());
-  for (int i = 0; i < n && ok; ++i) ok = write_all(f, oh[i].data(), oh[i].size());
-  static const uint8_t zeros[8] = {0};
-  for (int i = 0; i < n && ok; ++i) {
-    const size_t bytes = (size_t)elem_count(sets[i]) * elem_size(sets[i].dtype);
-    ok = write_all(f, sets[i].data, bytes) && write_all(f, zeros, pad8(bytes) - bytes);
-  }
-  ok = (std::fclose(f) == 0) && ok;
-  return ok ? AFID_OK : AFID_E_IO;
+    Out m(a_snod + nsnod * kSnodSize);
+    // superblock version 0
+    std::memcpy(&m.b[a_super], kSig, 8);
+    m.put(13, 8, 1);                 // size of offsets
+    m.put(14, 8, 1);                 // size of lengths
+    m.put(16, kLeafK, 2);
+    m.put(18, kInternalK, 2);
+    m.put(24, 0, 8);                 // base address
+    m.put(32, kUndef, 8);            // free-space info
+    m.put(40, eof, 8);               // end of file
+    m.put(48, kUndef, 8);            // driver info
+    m.put(56, 0, 8);                 // root entry: link name offset
+    m.put(64, a_root, 8);            //   object header address
+    m.put(72, 1, 4);                 //   cache type 1: scratch holds B-tree and heap addresses
+    m.put(80, a_btree, 8);
+    m.put(88, a_heap, 8);
+    // root object header: one symbol table message
+    {
+      auto h = object_header_v1({{0x11, le_bytes({{a_btree, 8}, {a_heap, 8}})}});
+      std::memcpy(&m.b[a_root], h.data(), h.size());
+    }
+    // local heap
+    std::memcpy(&m.b[a_heap], "HEAP", 4);
+    m.put(a_heap + 8, heap_data, 8);
+    m.put(a_heap + 16, 1, 8);        // empty free list
+    m.put(a_heap + 24, a_heapdata, 8);
+    for (int i = 0; i < n; ++i) std::memcpy(&m.b[a_heapdata + name_off[i]], sets[i].name, std::strlen(sets[i].name));
+    // B-tree node (group, leaf level): keys are heap offsets of the largest name in each child
+    std::memcpy(&m.b[a_btree], "TREE", 4);
+    m.put(a_btree + 4, 0, 1);
+    m.put(a_btree + 5, 0, 1);
+    m.put(a_btree + 6, nsnod, 2);
+    m.put(a_btree + 8, kUndef, 8);
+    m.put(a_btree + 16, kUndef, 8);
+    size_t q = a_btree + 24;
+    m.put(q, 0, 8);
+    q += 8;
+    for (int c = 0; c < nsnod; ++c) {
+      const int last = std::min(n, (c + 1) * 2 * kLeafK) - 1;
+      m.put(q, a_snod + c * kSnodSize, 8);
+      m.put(q + 8, name_off[order[last]], 8);
+      q += 16;
+    }
+    // symbol table nodes
+    for (int c = 0; c < nsnod; ++c) {
+      const size_t s = a_snod + c * kSnodSize;
+      const int lo = c * 2 * kLeafK, hi = std::min(n, lo + 2 * kLeafK);
+      std::memcpy(&m.b[s], "SNOD", 4);
+      m.put(s + 4, 1, 1);
+      m.put(s + 6, hi - lo, 2);
+      for (int e = lo; e < hi; ++e) {
+        const size_t p = s + 8 + (e - lo) * kEntrySize;
+        m.put(p, name_off[order[e]], 8);
+        m.put(p + 8, a_oh[order[e]], 8);
+      }
+    }
+
+    FILE *f = std::fopen(path, "wb");
+    if (!f) return AFID_E_IO;
+    bool ok = write_all(f, m.b.data(), m.b.size());
+    for (int i = 0; i < n && ok; ++i) ok = write_all(f, oh[i].data(), oh[i].size());
+    static const uint8_t zeros[8] = {0};
+    for (int i = 0; i < n && ok; ++i) {
+      const size_t bytes = (size_t)elem_count(sets[i]) * elem_size(sets[i].dtype);
+      ok = write_all(f, sets[i].data, bytes) && write_all(f, zeros, pad8(bytes) - bytes);
+    }
+    ok = (std::fclose(f) == 0) && ok;
+    return ok ? AFID_OK : AFID_E_IO;
+  });
 }
 
 // ---- reader --------------------------------------------------------------------------------
@@ -613,27 +616,31 @@ int open_dataset(const char *path, const char *name, Reader &rd, DsInfo &d) {
 
 extern "C" int afid_h5_info(const char *path, const char *name, int *dtype, int *rank,
                             int64_t dims[AFID_H5_MAX_RANK]) {
-  Reader rd;
-  DsInfo d;
-  const int s = open_dataset(path, name, rd, d);
-  if (s != AFID_OK) return s;
-  if (dtype) *dtype = d.cls == 1 ? AFID_H5_F64 : AFID_H5_I32;
-  if (rank) *rank = d.rank;
-  if (dims)
-    for (int i = 0; i < AFID_H5_MAX_RANK; ++i) dims[i] = i < d.rank ? d.dims[i] : 0;
-  return AFID_OK;
+  return afid_guard([&]() -> int {
+    Reader rd;
+    DsInfo d;
+    const int s = open_dataset(path, name, rd, d);
+    if (s != AFID_OK) return s;
+    if (dtype) *dtype = d.cls == 1 ? AFID_H5_F64 : AFID_H5_I32;
+    if (rank) *rank = d.rank;
+    if (dims)
+      for (int i = 0; i < AFID_H5_MAX_RANK; ++i) dims[i] = i < d.rank ? d.dims[i] : 0;
+    return AFID_OK;
+  });
 }
 
 extern "C" int afid_h5_read_f64(const char *path, const char *name, double *out, int64_t count) {
-  if (!out || count < 0) return AFID_E_INVALID;
-  Reader rd;
-  DsInfo d;
-  const int s = open_dataset(path, name, rd, d);
-  if (s != AFID_OK) return s;
-  int64_t n = 1;
-  for (int i = 0; i < d.rank; ++i) n *= d.dims[i];
-  if (n != count) return AFID_E_INVALID;
-  return rd.read_f64(d, out, count) ? AFID_OK : AFID_E_IO;
+  return afid_guard([&]() -> int {
+    if (!out || count < 0) return AFID_E_INVALID;
+    Reader rd;
+    DsInfo d;
+    const int s = open_dataset(path, name, rd, d);
+    if (s != AFID_OK) return s;
+    int64_t n = 1;
+    for (int i = 0; i < d.rank; ++i) n *= d.dims[i];
+    if (n != count) return AFID_E_INVALID;
+    return rd.read_f64(d, out, count) ? AFID_OK : AFID_E_IO;
+  });
 }
 
 // ---- continua files --------------------------------------------------------------------------
@@ -701,196 +708,208 @@ int read_scalar(const std::string &path, const char *name, double *v) {
 }  // namespace
 
 extern "C" int afid_continua_master_from_input(const afid_input_t *in, double time, afid_continua_master_t *m) {
-  if (!in || !m) return AFID_E_INVALID;
-  *m = afid_continua_master_t{};
-  m->nx = in->nxm + 1;
-  m->ny = in->nym + 1;
-  m->nz = in->nzm + 1;
-  m->ylen = in->ylen;
-  m->zlen = in->zlen;
-  m->time = time;
-  m->istr3 = in->istr3;
-  m->str3 = in->str3;
-  m->multires = in->multires ? 1 : 0;
-  if (m->multires) {
-    m->nxr = in->nxmr + 1;
-    m->nyr = in->nymr + 1;
-    m->nzr = in->nzmr + 1;
-    m->istr3r = in->istr3r;
-  }
-  return AFID_OK;
+  return afid_guard([&]() -> int {
+    if (!in || !m) return AFID_E_INVALID;
+    *m = afid_continua_master_t{};
+    m->nx = in->nxm + 1;
+    m->ny = in->nym + 1;
+    m->nz = in->nzm + 1;
+    m->ylen = in->ylen;
+    m->zlen = in->zlen;
+    m->time = time;
+    m->istr3 = in->istr3;
+    m->str3 = in->str3;
+    m->multires = in->multires ? 1 : 0;
+    if (m->multires) {
+      m->nxr = in->nxmr + 1;
+      m->nyr = in->nymr + 1;
+      m->nzr = in->nzmr + 1;
+      m->istr3r = in->istr3r;
+    }
+    return AFID_OK;
+  });
 }
 
 extern "C" int afid_write_flow_field(const char *dir, int final, double save_3d, const afid_continua_master_t *m,
                                      const double *vx, const double *vy, const double *vz, const double *temp,
                                      const double *pr, const double *sal) {
-  if (!dir || !m || !vx || !vy || !vz || !temp || (final && !pr)) return AFID_E_INVALID;
-  const int nx = m->nx, nym = m->ny - 1, nzm = m->nz - 1;
-  if (nx < 2 || nym < 1 || nzm < 1) return AFID_E_INVALID;
-  const bool with_sal = m->multires && sal;
-  if (with_sal && (m->nxr < 2 || m->nyr < 2 || m->nzr < 2)) return AFID_E_INVALID;
-  std::string base = dir;
-  if (!ensure_dir(base)) return AFID_E_IO;
-  if (final) {
-    base += "/continua";
-  } else {  // WriteFlowField.F90:22-26: frame = nint(time / save_3D), written as i5.5
-    if (!(save_3d > 0.0)) return AFID_E_INVALID;
-    const double fr = std::round(m->time / save_3d);  // nint: halves away from zero
-    if (!(fr >= 0.0 && fr <= 99999.0)) return AFID_E_INVALID;
-    char frame[8];
-    std::snprintf(frame, sizeof(frame), "%05d", (int)fr);
-    base += "/fields";
+  return afid_guard([&]() -> int {
+    if (!dir || !m || !vx || !vy || !vz || !temp || (final && !pr)) return AFID_E_INVALID;
+    const int nx = m->nx, nym = m->ny - 1, nzm = m->nz - 1;
+    if (nx < 2 || nym < 1 || nzm < 1) return AFID_E_INVALID;
+    const bool with_sal = m->multires && sal;
+    if (with_sal && (m->nxr < 2 || m->nyr < 2 || m->nzr < 2)) return AFID_E_INVALID;
+    std::string base = dir;
     if (!ensure_dir(base)) return AFID_E_IO;
-    base += std::string("/") + frame;
-  }
-  int s;
-  if ((s = write_field(base + "_temp.h5", temp, nx, nx, nym, nzm)) != AFID_OK) return s;
-  if ((s = write_field(base + "_vx.h5", vx, nx, nx, nym, nzm)) != AFID_OK) return s;
-  if ((s = write_field(base + "_vy.h5", vy, nx, nx, nym, nzm)) != AFID_OK) return s;
-  if ((s = write_field(base + "_vz.h5", vz, nx, nx, nym, nzm)) != AFID_OK) return s;
-  if (with_sal && (s = write_field(base + "_sal.h5", sal, m->nxr - 1, m->nxr, m->nyr - 1, m->nzr - 1)) != AFID_OK)
-    return s;
-  if (!final) return AFID_OK;
-  if ((s = write_field(base + "_pr.h5", pr, nx, nx, nym, nzm)) != AFID_OK) return s;
-  // continua_master.h5 (WriteFlowField.F90:51-82): one-element datasets
-  const int32_t ints[7] = {m->nx, m->ny, m->nz, m->istr3, m->nxr, m->nyr, m->nzr};
-  const int32_t istr3r = m->istr3r;
-  const double reals[4] = {m->ylen, m->zlen, m->time, m->str3};
-  afid_h5_dataset_t d[12];
-  int n = 0;
-  auto add = [&](const char *name, int dtype, const void *p) {
-    d[n] = afid_h5_dataset_t{};
-    d[n].name = name;
-    d[n].dtype = dtype;
-    d[n].rank = 1;
-    d[n].dims[0] = 1;
-    d[n].data = p;
-    ++n;
-  };
-  add("nx", AFID_H5_I32, &ints[0]);
-  add("ny", AFID_H5_I32, &ints[1]);
-  add("nz", AFID_H5_I32, &ints[2]);
-  add("ylen", AFID_H5_F64, &reals[0]);
-  add("zlen", AFID_H5_F64, &reals[1]);
-  add("time", AFID_H5_F64, &reals[2]);
-  add("istr3", AFID_H5_I32, &ints[3]);
-  add("str3", AFID_H5_F64, &reals[3]);
-  if (m->multires) {
-    add("nxr", AFID_H5_I32, &ints[4]);
-    add("nyr", AFID_H5_I32, &ints[5]);
-    add("nzr", AFID_H5_I32, &ints[6]);
-    add("istr3r", AFID_H5_I32, &istr3r);
-  }
-  return afid_h5_write((std::string(dir) + "/continua_master.h5").c_str(), n, d);
+    if (final) {
+      base += "/continua";
+    } else {  // WriteFlowField.F90:22-26: frame = nint(time / save_3D), written as i5.5
+      if (!(save_3d > 0.0)) return AFID_E_INVALID;
+      const double fr = std::round(m->time / save_3d);  // nint: halves away from zero
+      if (!(fr >= 0.0 && fr <= 99999.0)) return AFID_E_INVALID;
+      char frame[8];
+      std::snprintf(frame, sizeof(frame), "%05d", (int)fr);
+      base += "/fields";
+      if (!ensure_dir(base)) return AFID_E_IO;
+      base += std::string("/") + frame;
+    }
+    int s;
+    if ((s = write_field(base + "_temp.h5", temp, nx, nx, nym, nzm)) != AFID_OK) return s;
+    if ((s = write_field(base + "_vx.h5", vx, nx, nx, nym, nzm)) != AFID_OK) return s;
+    if ((s = write_field(base + "_vy.h5", vy, nx, nx, nym, nzm)) != AFID_OK) return s;
+    if ((s = write_field(base + "_vz.h5", vz, nx, nx, nym, nzm)) != AFID_OK) return s;
+    if (with_sal && (s = write_field(base + "_sal.h5", sal, m->nxr - 1, m->nxr, m->nyr - 1, m->nzr - 1)) != AFID_OK)
+      return s;
+    if (!final) return AFID_OK;
+    if ((s = write_field(base + "_pr.h5", pr, nx, nx, nym, nzm)) != AFID_OK) return s;
+    // continua_master.h5 (WriteFlowField.F90:51-82): one-element datasets
+    const int32_t ints[7] = {m->nx, m->ny, m->nz, m->istr3, m->nxr, m->nyr, m->nzr};
+    const int32_t istr3r = m->istr3r;
+    const double reals[4] = {m->ylen, m->zlen, m->time, m->str3};
+    afid_h5_dataset_t d[12];
+    int n = 0;
+    auto add = [&](const char *name, int dtype, const void *p) {
+      d[n] = afid_h5_dataset_t{};
+      d[n].name = name;
+      d[n].dtype = dtype;
+      d[n].rank = 1;
+      d[n].dims[0] = 1;
+      d[n].data = p;
+      ++n;
+    };
+    add("nx", AFID_H5_I32, &ints[0]);
+    add("ny", AFID_H5_I32, &ints[1]);
+    add("nz", AFID_H5_I32, &ints[2]);
+    add("ylen", AFID_H5_F64, &reals[0]);
+    add("zlen", AFID_H5_F64, &reals[1]);
+    add("time", AFID_H5_F64, &reals[2]);
+    add("istr3", AFID_H5_I32, &ints[3]);
+    add("str3", AFID_H5_F64, &reals[3]);
+    if (m->multires) {
+      add("nxr", AFID_H5_I32, &ints[4]);
+      add("nyr", AFID_H5_I32, &ints[5]);
+      add("nzr", AFID_H5_I32, &ints[6]);
+      add("istr3r", AFID_H5_I32, &istr3r);
+    }
+    return afid_h5_write((std::string(dir) + "/continua_master.h5").c_str(), n, d);
+  });
 }
 
 extern "C" int afid_read_continua_master(const char *dir, int multires, afid_continua_master_t *m) {
-  if (!dir || !m) return AFID_E_INVALID;
-  const std::string p = std::string(dir) + "/continua_master.h5";
-  if (!file_exists(p)) return AFID_E_IO;  // "Continuation files not found" (ReadFlowInterp.F90:25-29)
-  afid_continua_master_t r{};
-  double v[12];
-  const char *names[12] = {"nx", "ny", "nz", "time", "istr3", "str3", "ylen", "zlen", "nxr", "nyr", "nzr", "istr3r"};
-  const int count = multires ? 12 : 8;
-  for (int i = 0; i < count; ++i) {
-    const int s = read_scalar(p, names[i], &v[i]);
-    if (s != AFID_OK) return s;
-  }
-  r.nx = (int)v[0];
-  r.ny = (int)v[1];
-  r.nz = (int)v[2];
-  r.time = v[3];
-  r.istr3 = (int)v[4];
-  r.str3 = v[5];
-  r.ylen = v[6];
-  r.zlen = v[7];
-  r.multires = multires ? 1 : 0;
-  if (multires) {
-    r.nxr = (int)v[8];
-    r.nyr = (int)v[9];
-    r.nzr = (int)v[10];
-    r.istr3r = (int)v[11];
-  }
-  *m = r;
-  return AFID_OK;
+  return afid_guard([&]() -> int {
+    if (!dir || !m) return AFID_E_INVALID;
+    const std::string p = std::string(dir) + "/continua_master.h5";
+    if (!file_exists(p)) return AFID_E_IO;  // "Continuation files not found" (ReadFlowInterp.F90:25-29)
+    afid_continua_master_t r{};
+    double v[12];
+    const char *names[12] = {"nx", "ny", "nz", "time", "istr3", "str3", "ylen", "zlen", "nxr", "nyr", "nzr", "istr3r"};
+    const int count = multires ? 12 : 8;
+    for (int i = 0; i < count; ++i) {
+      const int s = read_scalar(p, names[i], &v[i]);
+      if (s != AFID_OK) return s;
+    }
+    r.nx = (int)v[0];
+    r.ny = (int)v[1];
+    r.nz = (int)v[2];
+    r.time = v[3];
+    r.istr3 = (int)v[4];
+    r.str3 = v[5];
+    r.ylen = v[6];
+    r.zlen = v[7];
+    r.multires = multires ? 1 : 0;
+    if (multires) {
+      r.nxr = (int)v[8];
+      r.nyr = (int)v[9];
+      r.nzr = (int)v[10];
+      r.istr3r = (int)v[11];
+    }
+    *m = r;
+    return AFID_OK;
+  });
 }
 
 extern "C" int afid_read_flow_field(const char *dir, const afid_continua_master_t *cur, double *time_out, double *vx,
                                     double *vy, double *vz, double *temp, double *pr, int *pr_read, double *sal) {
-  if (!dir || !cur || !vx || !vy || !vz || !temp) return AFID_E_INVALID;
-  afid_continua_master_t old{};
-  int s = afid_read_continua_master(dir, cur->multires, &old);
-  if (s != AFID_OK) return s;
-  // ReadFlowInterp.F90:76-82: the domain size must match
-  if (std::fabs(cur->ylen - old.ylen) > 1e-8 || std::fabs(cur->zlen - old.zlen) > 1e-8) return AFID_E_INVALID;
-  // ReadFlowInterp.F90:85-89: a different grid needs the interpolating restart
-  if (cur->nx != old.nx || cur->ny != old.ny || cur->nz != old.nz || cur->istr3 != old.istr3 ||
-      std::fabs(cur->str3 - old.str3) > 1e-8 ||
-      (cur->multires && (cur->nxr != old.nxr || cur->nyr != old.nyr || cur->nzr != old.nzr || cur->istr3r != old.istr3r)))
-    return AFID_E_INVALID;
-  const std::string base = std::string(dir) + "/continua";
-  const int nx = cur->nx, nym = cur->ny - 1, nzm = cur->nz - 1;
-  if ((s = read_field(base + "_vx.h5", vx, nx, nx, nym, nzm)) != AFID_OK) return s;
-  if ((s = read_field(base + "_vy.h5", vy, nx, nx, nym, nzm)) != AFID_OK) return s;
-  if ((s = read_field(base + "_vz.h5", vz, nx, nx, nym, nzm)) != AFID_OK) return s;
-  if ((s = read_field(base + "_temp.h5", temp, nx, nx, nym, nzm)) != AFID_OK) return s;
-  if (cur->multires && sal &&
-      (s = read_field(base + "_sal.h5", sal, cur->nxr - 1, cur->nxr, cur->nyr - 1, cur->nzr - 1)) != AFID_OK)
-    return s;
-  int got_pr = 0;
-  if (pr && file_exists(base + "_pr.h5")) {  // ReadFlowInterp.F90:157-162
-    if ((s = read_field(base + "_pr.h5", pr, nx, nx, nym, nzm)) != AFID_OK) return s;
-    got_pr = 1;
-  }
-  if (pr_read) *pr_read = got_pr;
-  if (time_out) *time_out = old.time;
-  return AFID_OK;
+  return afid_guard([&]() -> int {
+    if (!dir || !cur || !vx || !vy || !vz || !temp) return AFID_E_INVALID;
+    afid_continua_master_t old{};
+    int s = afid_read_continua_master(dir, cur->multires, &old);
+    if (s != AFID_OK) return s;
+    // ReadFlowInterp.F90:76-82: the domain size must match
+    if (std::fabs(cur->ylen - old.ylen) > 1e-8 || std::fabs(cur->zlen - old.zlen) > 1e-8) return AFID_E_INVALID;
+    // ReadFlowInterp.F90:85-89: a different grid needs the interpolating restart
+    if (cur->nx != old.nx || cur->ny != old.ny || cur->nz != old.nz || cur->istr3 != old.istr3 ||
+        std::fabs(cur->str3 - old.str3) > 1e-8 ||
+        (cur->multires && (cur->nxr != old.nxr || cur->nyr != old.nyr || cur->nzr != old.nzr || cur->istr3r != old.istr3r)))
+      return AFID_E_INVALID;
+    const std::string base = std::string(dir) + "/continua";
+    const int nx = cur->nx, nym = cur->ny - 1, nzm = cur->nz - 1;
+    if ((s = read_field(base + "_vx.h5", vx, nx, nx, nym, nzm)) != AFID_OK) return s;
+    if ((s = read_field(base + "_vy.h5", vy, nx, nx, nym, nzm)) != AFID_OK) return s;
+    if ((s = read_field(base + "_vz.h5", vz, nx, nx, nym, nzm)) != AFID_OK) return s;
+    if ((s = read_field(base + "_temp.h5", temp, nx, nx, nym, nzm)) != AFID_OK) return s;
+    if (cur->multires && sal &&
+        (s = read_field(base + "_sal.h5", sal, cur->nxr - 1, cur->nxr, cur->nyr - 1, cur->nzr - 1)) != AFID_OK)
+      return s;
+    int got_pr = 0;
+    if (pr && file_exists(base + "_pr.h5")) {  // ReadFlowInterp.F90:157-162
+      if ((s = read_field(base + "_pr.h5", pr, nx, nx, nym, nzm)) != AFID_OK) return s;
+      got_pr = 1;
+    }
+    if (pr_read) *pr_read = got_pr;
+    if (time_out) *time_out = old.time;
+    return AFID_OK;
+  });
 }
 
 extern "C" int afid_gpu_write_flow_field(afid_ctx_t *ctx, const char *dir, int final, double save_3d,
                                          const afid_continua_master_t *m) {
-  if (!ctx || !dir || !m) return AFID_E_INVALID;
-  int dims[6];
-  int s = afid_gpu_dims(ctx, dims);
-  if (s != AFID_OK) return s;
-  if (m->nx != dims[0] + 1 || m->ny != dims[1] + 1 || m->nz != dims[2] + 1) return AFID_E_INVALID;
-  const bool with_sal = m->multires && dims[3] > 0;
-  if (with_sal && (m->nxr != dims[3] + 1 || m->nyr != dims[4] + 1 || m->nzr != dims[5] + 1)) return AFID_E_INVALID;
-  const int nx = m->nx, nym = dims[1], nzm = dims[2];
-  const size_t n = (size_t)nx * nym * nzm;
-  std::vector<double> f(5 * n);
-  double *vx = f.data(), *vy = vx + n, *vz = vy + n, *temp = vz + n, *pr = temp + n;
-  if ((s = afid_gpu_download(ctx, vx, vy, vz, temp, pr, nx, nym)) != AFID_OK) return s;
-  std::vector<double> sal;
-  if (with_sal) {
-    sal.resize((size_t)dims[3] * dims[4] * dims[5]);
-    if ((s = afid_gpu_sal_download(ctx, sal.data(), dims[3], dims[4])) != AFID_OK) return s;
-  }
-  return afid_write_flow_field(dir, final, save_3d, m, vx, vy, vz, temp, pr, with_sal ? sal.data() : nullptr);
+  return afid_guard([&]() -> int {
+    if (!ctx || !dir || !m) return AFID_E_INVALID;
+    int dims[6];
+    int s = afid_gpu_dims(ctx, dims);
+    if (s != AFID_OK) return s;
+    if (m->nx != dims[0] + 1 || m->ny != dims[1] + 1 || m->nz != dims[2] + 1) return AFID_E_INVALID;
+    const bool with_sal = m->multires && dims[3] > 0;
+    if (with_sal && (m->nxr != dims[3] + 1 || m->nyr != dims[4] + 1 || m->nzr != dims[5] + 1)) return AFID_E_INVALID;
+    const int nx = m->nx, nym = dims[1], nzm = dims[2];
+    const size_t n = (size_t)nx * nym * nzm;
+    std::vector<double> f(5 * n);
+    double *vx = f.data(), *vy = vx + n, *vz = vy + n, *temp = vz + n, *pr = temp + n;
+    if ((s = afid_gpu_download(ctx, vx, vy, vz, temp, pr, nx, nym)) != AFID_OK) return s;
+    std::vector<double> sal;
+    if (with_sal) {
+      sal.resize((size_t)dims[3] * dims[4] * dims[5]);
+      if ((s = afid_gpu_sal_download(ctx, sal.data(), dims[3], dims[4])) != AFID_OK) return s;
+    }
+    return afid_write_flow_field(dir, final, save_3d, m, vx, vy, vz, temp, pr, with_sal ? sal.data() : nullptr);
+  });
 }
 
 extern "C" int afid_gpu_read_flow_field(afid_ctx_t *ctx, const char *dir, const afid_continua_master_t *cur,
                                         double *time_out) {
-  if (!ctx || !dir || !cur) return AFID_E_INVALID;
-  int dims[6];
-  int s = afid_gpu_dims(ctx, dims);
-  if (s != AFID_OK) return s;
-  if (cur->nx != dims[0] + 1 || cur->ny != dims[1] + 1 || cur->nz != dims[2] + 1) return AFID_E_INVALID;
-  const bool with_sal = cur->multires && dims[3] > 0;
-  if (with_sal && (cur->nxr != dims[3] + 1 || cur->nyr != dims[4] + 1 || cur->nzr != dims[5] + 1))
-    return AFID_E_INVALID;
-  const int nx = cur->nx, nym = dims[1], nzm = dims[2];
-  const size_t n = (size_t)nx * nym * nzm;
-  std::vector<double> f(5 * n, 0.0);
-  double *vx = f.data(), *vy = vx + n, *vz = vy + n, *temp = vz + n, *pr = temp + n;
-  std::vector<double> sal(with_sal ? (size_t)dims[3] * dims[4] * dims[5] : 0);
-  int pr_read = 0;
-  double t = 0.0;
-  if ((s = afid_read_flow_field(dir, cur, &t, vx, vy, vz, temp, pr, &pr_read, with_sal ? sal.data() : nullptr)) !=
-      AFID_OK)
-    return s;
-  if ((s = afid_gpu_upload(ctx, vx, vy, vz, temp, pr, nx, nym)) != AFID_OK) return s;
-  if (with_sal && (s = afid_gpu_sal_upload(ctx, sal.data(), dims[3], dims[4])) != AFID_OK) return s;
-  if (time_out) *time_out = t;
-  return AFID_OK;
+  return afid_guard([&]() -> int {
+    if (!ctx || !dir || !cur) return AFID_E_INVALID;
+    int dims[6];
+    int s = afid_gpu_dims(ctx, dims);
+    if (s != AFID_OK) return s;
+    if (cur->nx != dims[0] + 1 || cur->ny != dims[1] + 1 || cur->nz != dims[2] + 1) return AFID_E_INVALID;
+    const bool with_sal = cur->multires && dims[3] > 0;
+    if (with_sal && (cur->nxr != dims[3] + 1 || cur->nyr != dims[4] + 1 || cur->nzr != dims[5] + 1))
+      return AFID_E_INVALID;
+    const int nx = cur->nx, nym = dims[1], nzm = dims[2];
+    const size_t n = (size_t)nx * nym * nzm;
+    std::vector<double> f(5 * n, 0.0);
+    double *vx = f.data(), *vy = vx + n, *vz = vy + n, *temp = vz + n, *pr = temp + n;
+    std::vector<double> sal(with_sal ? (size_t)dims[3] * dims[4] * dims[5] : 0);
+    int pr_read = 0;
+    double t = 0.0;
+    if ((s = afid_read_flow_field(dir, cur, &t, vx, vy, vz, temp, pr, &pr_read, with_sal ? sal.data() : nullptr)) !=
+        AFID_OK)
+      return s;
+    if ((s = afid_gpu_upload(ctx, vx, vy, vz, temp, pr, nx, nym)) != AFID_OK) return s;
+    if (with_sal && (s = afid_gpu_sal_upload(ctx, sal.data(), dims[3], dims[4])) != AFID_OK) return s;
+    if (time_out) *time_out = t;
+    return AFID_OK;
+  });
 }

@@ -210,64 +210,68 @@ using afid_hostd::uniform_grid;
 extern "C" {
 
 int afid_parse_bou_in(const char *text, afid_input_t *o) {
-  if (!text || !o) return AFID_E_INVALID;
-  std::memset(o, 0, sizeof(*o));
-  LineReader r(text);
-  r.skip(2);
-  auto v = r.vals(4);
-  o->nxm = (int)v[0]; o->nym = (int)v[1]; o->nzm = (int)v[2]; o->nsst = (int)v[3];
-  r.skip(3);
-  v = r.vals(4);
-  o->multires = (int)v[0]; o->nxmr = (int)v[1]; o->nymr = (int)v[2]; o->nzmr = (int)v[3];
-  r.skip(3);
-  v = r.vals(2);
-  o->flagsal = (int)v[0]; o->flagpf = (int)v[1];
-  r.skip(3);
-  v = r.vals(2);
-  o->nread = (int)v[0]; o->ireset = (int)v[1];
-  r.skip(3);
-  v = r.vals(3);
-  o->ntst = (int)v[0]; o->walltimemax = v[1]; o->tmax = v[2];
-  r.skip(3);
-  v = r.vals(3);
-  o->tout = v[0]; o->tframe = v[1]; o->save_3d = v[2];
-  r.skip(3);
-  v = r.vals(3);
-  o->alx3 = v[0]; o->ylen = v[1]; o->zlen = v[2];
-  r.skip(3);
-  v = r.vals(3);
-  o->istr3 = (int)v[0]; o->str3 = v[1]; o->istr3r = (int)v[2];
-  r.skip(3);
-  v = r.vals(5);
-  o->rayt = v[0]; o->prat = v[1]; o->rays = v[2]; o->pras = v[3]; o->ffscales = (int)v[4];
-  r.skip(3);
-  v = r.vals(6);
-  o->idtv = (int)v[0]; o->dt = v[1]; o->resid = v[2]; o->limit_cfl = v[3]; o->dtmin = v[4]; o->dtmax = v[5];
-  r.skip(3);
-  v = r.vals(6);
-  o->inslws = (int)v[0]; o->inslwn = (int)v[1]; o->tfixs = (int)v[2]; o->tfixn = (int)v[3];
-  o->sfixs = (int)v[4]; o->sfixn = (int)v[5];
-  r.skip(3);
-  v = r.vals(3);
-  o->active_t = (int)v[0]; o->active_s = (int)v[1]; o->gaxis = (int)v[2];
-  r.skip(3);
-  v = r.vals(5);
-  o->xplusu = v[0]; o->xminusu = v[1]; o->dpdy = v[2]; o->dpdz = v[3]; o->melt = (int)v[4];
-  if (!r.ok) return AFID_E_INVALID;
-  if (o->nxm < 1 || o->nym < 1 || o->nzm < 1) return AFID_E_INVALID;
-  return AFID_OK;
+  return afid_guard([&]() -> int {
+    if (!text || !o) return AFID_E_INVALID;
+    std::memset(o, 0, sizeof(*o));
+    LineReader r(text);
+    r.skip(2);
+    auto v = r.vals(4);
+    o->nxm = (int)v[0]; o->nym = (int)v[1]; o->nzm = (int)v[2]; o->nsst = (int)v[3];
+    r.skip(3);
+    v = r.vals(4);
+    o->multires = (int)v[0]; o->nxmr = (int)v[1]; o->nymr = (int)v[2]; o->nzmr = (int)v[3];
+    r.skip(3);
+    v = r.vals(2);
+    o->flagsal = (int)v[0]; o->flagpf = (int)v[1];
+    r.skip(3);
+    v = r.vals(2);
+    o->nread = (int)v[0]; o->ireset = (int)v[1];
+    r.skip(3);
+    v = r.vals(3);
+    o->ntst = (int)v[0]; o->walltimemax = v[1]; o->tmax = v[2];
+    r.skip(3);
+    v = r.vals(3);
+    o->tout = v[0]; o->tframe = v[1]; o->save_3d = v[2];
+    r.skip(3);
+    v = r.vals(3);
+    o->alx3 = v[0]; o->ylen = v[1]; o->zlen = v[2];
+    r.skip(3);
+    v = r.vals(3);
+    o->istr3 = (int)v[0]; o->str3 = v[1]; o->istr3r = (int)v[2];
+    r.skip(3);
+    v = r.vals(5);
+    o->rayt = v[0]; o->prat = v[1]; o->rays = v[2]; o->pras = v[3]; o->ffscales = (int)v[4];
+    r.skip(3);
+    v = r.vals(6);
+    o->idtv = (int)v[0]; o->dt = v[1]; o->resid = v[2]; o->limit_cfl = v[3]; o->dtmin = v[4]; o->dtmax = v[5];
+    r.skip(3);
+    v = r.vals(6);
+    o->inslws = (int)v[0]; o->inslwn = (int)v[1]; o->tfixs = (int)v[2]; o->tfixn = (int)v[3];
+    o->sfixs = (int)v[4]; o->sfixn = (int)v[5];
+    r.skip(3);
+    v = r.vals(3);
+    o->active_t = (int)v[0]; o->active_s = (int)v[1]; o->gaxis = (int)v[2];
+    r.skip(3);
+    v = r.vals(5);
+    o->xplusu = v[0]; o->xminusu = v[1]; o->dpdy = v[2]; o->dpdz = v[3]; o->melt = (int)v[4];
+    if (!r.ok) return AFID_E_INVALID;
+    if (o->nxm < 1 || o->nym < 1 || o->nzm < 1) return AFID_E_INVALID;
+    return AFID_OK;
+  });
 }
 
 int afid_read_bou_in(const char *path, afid_input_t *out) {
-  if (!path) return AFID_E_INVALID;
-  FILE *f = std::fopen(path, "rb");
-  if (!f) return AFID_E_INVALID;
-  std::string s;
-  char buf[4096];
-  size_t n;
-  while ((n = std::fread(buf, 1, sizeof buf, f)) > 0) s.append(buf, n);
-  std::fclose(f);
-  return afid_parse_bou_in(s.c_str(), out);
+  return afid_guard([&]() -> int {
+    if (!path) return AFID_E_INVALID;
+    FILE *f = std::fopen(path, "rb");
+    if (!f) return AFID_E_INVALID;
+    std::string s;
+    char buf[4096];
+    size_t n;
+    while ((n = std::fread(buf, 1, sizeof buf, f)) > 0) s.append(buf, n);
+    std::fclose(f);
+    return afid_parse_bou_in(s.c_str(), out);
+  });
 }
 
 static int tables_create(const afid_input_t *in, int precision, afid_tables_t **out);
@@ -469,142 +473,150 @@ double afid_philox_uniform(uint64_t seed, uint64_t n) { return philox_u(seed, n)
 
 int afid_initial_temperature(const afid_tables_t *t, uint64_t seed, double eps, double *temp, int ld_x,
                              int ld_y) {
-  if (!t || !temp) return AFID_E_INVALID;
-  const int nxm = t->in.nxm, nym = t->in.nym, nzm = t->in.nzm, nx = nxm + 1;
-  if (ld_x < nx || ld_y < nym) return AFID_E_INVALID;
-  const std::vector<double> &xm = t->arr.at("xm");
-  for (int i = 0; i < nzm; ++i)
-    for (int j = 0; j < nym; ++j) {
-      const double tb = t->tempbp[(size_t)j + (size_t)nym * i], tt = t->temptp[(size_t)j + (size_t)nym * i];
-      double *col = temp + ((size_t)i * ld_y + j) * ld_x;
-      for (int k = 0; k < nxm; ++k) {
-        double v = tb + (tt - tb) * xm[k] / t->in.alx3;  // CreateInitialConditions.F90:178-185
-        const double u = philox_u(seed, (uint64_t)k + (uint64_t)nx * ((uint64_t)j + (uint64_t)nym * i));
-        const double dist = std::fabs(xm[k] - 0.5);
-        const double amp = (dist + eps > 0.5) ? 0.5 - dist : eps;  // :190-196
-        col[k] = v + amp * (2.0 * u - 1.0);
+  return afid_guard([&]() -> int {
+    if (!t || !temp) return AFID_E_INVALID;
+    const int nxm = t->in.nxm, nym = t->in.nym, nzm = t->in.nzm, nx = nxm + 1;
+    if (ld_x < nx || ld_y < nym) return AFID_E_INVALID;
+    const std::vector<double> &xm = t->arr.at("xm");
+    for (int i = 0; i < nzm; ++i)
+      for (int j = 0; j < nym; ++j) {
+        const double tb = t->tempbp[(size_t)j + (size_t)nym * i], tt = t->temptp[(size_t)j + (size_t)nym * i];
+        double *col = temp + ((size_t)i * ld_y + j) * ld_x;
+        for (int k = 0; k < nxm; ++k) {
+          double v = tb + (tt - tb) * xm[k] / t->in.alx3;  // CreateInitialConditions.F90:178-185
+          const double u = philox_u(seed, (uint64_t)k + (uint64_t)nx * ((uint64_t)j + (uint64_t)nym * i));
+          const double dist = std::fabs(xm[k] - 0.5);
+          const double amp = (dist + eps > 0.5) ? 0.5 - dist : eps;  // :190-196
+          col[k] = v + amp * (2.0 * u - 1.0);
+        }
       }
-    }
-  return AFID_OK;
+    return AFID_OK;
+  });
 }
 
 int afid_next_dt(const afid_input_t *in, int ntime, double *dt, double cflm, double *cfl_report) {
-  if (!in || !dt) return AFID_E_INVALID;
-  int err = 0;
-  if (in->idtv == 1) {  // main.F90:287-302
-    if (ntime > 1) {
-      *dt = (cflm < 1.0e-8) ? in->dtmax : in->limit_cfl / cflm;
-      if (*dt > in->dtmax) *dt = in->dtmax;
+  return afid_guard([&]() -> int {
+    if (!in || !dt) return AFID_E_INVALID;
+    int err = 0;
+    if (in->idtv == 1) {  // main.F90:287-302
+      if (ntime > 1) {
+        *dt = (cflm < 1.0e-8) ? in->dtmax : in->limit_cfl / cflm;
+        if (*dt > in->dtmax) *dt = in->dtmax;
+      }
+      if (*dt < in->dtmin) err = AFID_E_DTMIN;
+      if (cfl_report) *cfl_report = cflm;
+    } else {  // main.F90:297-298
+      const double c = cflm * (*dt);
+      if (c > in->limit_cfl) err = AFID_E_CFL;
+      if (cfl_report) *cfl_report = c;
     }
-    if (*dt < in->dtmin) err = AFID_E_DTMIN;
-    if (cfl_report) *cfl_report = cflm;
-  } else {  // main.F90:297-298
-    const double c = cflm * (*dt);
-    if (c > in->limit_cfl) err = AFID_E_CFL;
-    if (cfl_report) *cfl_report = c;
-  }
-  return err;
+    return err;
+  });
 }
 
 int afid_run(const afid_input_t *in, int precision, uint64_t seed, int nsteps, int stats_every, afid_step_cb cb,
              void *user, afid_run_stats_t *stats) {
-  return afid_run_io(in, precision, seed, nsteps, stats_every, cb, user, nullptr, stats);
+  return afid_guard([&]() -> int {
+    return afid_run_io(in, precision, seed, nsteps, stats_every, cb, user, nullptr, stats);
+  });
 }
 
 int afid_run_io(const afid_input_t *in, int precision, uint64_t seed, int nsteps, int stats_every, afid_step_cb cb,
                 void *user, const char *dir, afid_run_stats_t *stats) {
-  if (!in) return AFID_E_INVALID;
-  afid_tables_t *t = nullptr;
-  int s = afid_tables_create(in, precision, &t);
-  if (s != AFID_OK) return s;
-  afid_ctx_t *ctx = nullptr;
-  s = afid_gpu_create(&t->grid, &t->params, &ctx);
-  if (s != AFID_OK) { afid_tables_destroy(t); return s; }
-  const int nxm = in->nxm, nym = in->nym, nzm = in->nzm, nx = nxm + 1;
-  // multi-resolution salinity (MULTIRES = FLAGSAL = 1): refined grid, CreateInitialSalinity with
-  // Philox key seed + 1, and the refined-grid CFL number for the dt rule (main.F90:285-293)
-  afid_mgrd_t *mg = nullptr;
-  if (in->flagsal) {
-    s = afid_mgrd_create(t, &mg);
-    if (s == AFID_OK) s = afid_gpu_sal_create(ctx, afid_mgrd_view(mg));
-  }
-  double time = 0.0;
-  afid_continua_master_t master{};
-  afid_continua_master_from_input(in, 0.0, &master);
-  if (s == AFID_OK && dir && in->nread) {  // ReadFlowInterp (main.F90:157-161)
-    s = afid_gpu_read_flow_interp(ctx, dir, in, &time, nullptr);
-    if (in->ireset) time = 0.0;           // ReadFlowInterp.F90:173
-  } else if (s == AFID_OK) {
-    std::vector<double> temp((size_t)nx * nym * nzm, 0.0);
-    afid_initial_temperature(t, seed, 1e-3, temp.data(), nx, nym);
-    std::vector<double> zero(temp.size(), 0.0);
-    s = afid_gpu_upload(ctx, zero.data(), zero.data(), zero.data(), temp.data(), zero.data(), nx, nym);
-    if (s == AFID_OK && mg) {
-      const afid_sal_grid_t *v = afid_mgrd_view(mg);
-      std::vector<double> sal((size_t)v->nxmr * v->nymr * v->nzmr);
-      afid_initial_salinity(mg, seed + 1, 5e-3, sal.data(), v->nxmr, v->nymr);
-      s = afid_gpu_sal_upload(ctx, sal.data(), v->nxmr, v->nymr);
+  return afid_guard([&]() -> int {
+    if (!in) return AFID_E_INVALID;
+    afid_tables_t *t = nullptr;
+    int s = afid_tables_create(in, precision, &t);
+    if (s != AFID_OK) return s;
+    afid_ctx_t *ctx = nullptr;
+    s = afid_gpu_create(&t->grid, &t->params, &ctx);
+    if (s != AFID_OK) { afid_tables_destroy(t); return s; }
+    const int nxm = in->nxm, nym = in->nym, nzm = in->nzm, nx = nxm + 1;
+    // multi-resolution salinity (MULTIRES = FLAGSAL = 1): refined grid, CreateInitialSalinity with
+    // Philox key seed + 1, and the refined-grid CFL number for the dt rule (main.F90:285-293)
+    afid_mgrd_t *mg = nullptr;
+    if (in->flagsal) {
+      s = afid_mgrd_create(t, &mg);
+      if (s == AFID_OK) s = afid_gpu_sal_create(ctx, afid_mgrd_view(mg));
     }
-  }
-  // 3-D frames: at start-up (main.F90:241) and when mod(time, SAVE_3D) < dt past the first
-  // TFRAME (main.F90:376-381); skipped when SAVE_3D or TFRAME is not positive
-  const bool frames = dir && in->save_3d > 0.0 && in->tframe > 0.0;
-  if (s == AFID_OK && frames) {
-    master.time = time;
-    s = afid_gpu_write_flow_field(ctx, dir, 0, in->save_3d, &master);
-  }
-  afid_run_stats_t st{};
-  const int total = (nsteps < 0) ? in->ntst + 1 : nsteps;
-  double dt = in->dt;
-  const double ra_pr = std::fabs(in->rayt) * in->prat;
-  auto t0 = std::chrono::steady_clock::now();
-  int errorcode = 0;
-  for (int ntime = 0; ntime < total && s == AFID_OK; ++ntime) {
-    double cflm = 0.0;
-    if ((s = mg ? afid_gpu_sal_cfl(ctx, &cflm) : afid_gpu_cfl(ctx, &cflm)) != AFID_OK) break;
-    double cflr = 0.0;
-    errorcode = afid_next_dt(in, ntime, &dt, cflm, &cflr);
-    if ((s = afid_gpu_timemarcher(ctx, dt, ntime)) != AFID_OK) break;
-    time += dt;
-    st.steps_done = ntime + 1;
-    st.cfl = cflr;
-    // main.F90:346-358: divergence check on step 1 and every tout
-    if (ntime == 1 || std::fmod(time, in->tout) < dt) {
-      double dmax = 0.0;
-      if ((s = afid_gpu_divmax(ctx, &dmax)) != AFID_OK) break;
-      st.divmax = dmax;
-      if (std::fabs(dmax) > in->resid) errorcode = AFID_E_DIVERGENCE;
+    double time = 0.0;
+    afid_continua_master_t master{};
+    afid_continua_master_from_input(in, 0.0, &master);
+    if (s == AFID_OK && dir && in->nread) {  // ReadFlowInterp (main.F90:157-161)
+      s = afid_gpu_read_flow_interp(ctx, dir, in, &time, nullptr);
+      if (in->ireset) time = 0.0;           // ReadFlowInterp.F90:173
+    } else if (s == AFID_OK) {
+      std::vector<double> temp((size_t)nx * nym * nzm, 0.0);
+      afid_initial_temperature(t, seed, 1e-3, temp.data(), nx, nym);
+      std::vector<double> zero(temp.size(), 0.0);
+      s = afid_gpu_upload(ctx, zero.data(), zero.data(), zero.data(), temp.data(), zero.data(), nx, nym);
+      if (s == AFID_OK && mg) {
+        const afid_sal_grid_t *v = afid_mgrd_view(mg);
+        std::vector<double> sal((size_t)v->nxmr * v->nymr * v->nzmr);
+        afid_initial_salinity(mg, seed + 1, 5e-3, sal.data(), v->nxmr, v->nymr);
+        s = afid_gpu_sal_upload(ctx, sal.data(), v->nxmr, v->nymr);
+      }
     }
-    if (stats_every > 0 && cb && ((ntime + 1) % stats_every == 0)) {
-      double nu = 0, ke = 0;
-      afid_gpu_globals(ctx, ra_pr, &nu, &ke, nullptr);
-      cb(ntime, time, dt, nu, ke, user);
-    }
-    if (frames && std::fmod(time, in->save_3d) < dt && std::floor(time / in->tframe) != 0.0) {
+    // 3-D frames: at start-up (main.F90:241) and when mod(time, SAVE_3D) < dt past the first
+    // TFRAME (main.F90:376-381); skipped when SAVE_3D or TFRAME is not positive
+    const bool frames = dir && in->save_3d > 0.0 && in->tframe > 0.0;
+    if (s == AFID_OK && frames) {
       master.time = time;
-      if ((s = afid_gpu_write_flow_field(ctx, dir, 0, in->save_3d, &master)) != AFID_OK) break;
+      s = afid_gpu_write_flow_field(ctx, dir, 0, in->save_3d, &master);
     }
-    if (time > in->tmax) errorcode = 333;
-    if (errorcode == 0 && nsteps < 0 && ntime == in->ntst) errorcode = 555;
-    if (errorcode != 0) break;
-  }
-  if (s == AFID_OK) s = afid_gpu_synchronize(ctx);
-  auto t1 = std::chrono::steady_clock::now();
-  st.seconds = std::chrono::duration<double>(t1 - t0).count();
-  st.time = time;
-  st.dt = dt;
-  st.errorcode = errorcode;
-  if (s == AFID_OK) afid_gpu_globals(ctx, ra_pr, &st.nu_vol, &st.ke, nullptr);
-  // QuitRoutine.F90:37: the continua files on a normal exit
-  if (s == AFID_OK && dir && (errorcode == 0 || errorcode == 333 || errorcode == 334 || errorcode == 555)) {
-    master.time = time;
-    s = afid_gpu_write_flow_field(ctx, dir, 1, in->save_3d, &master);
-  }
-  if (stats) *stats = st;
-  afid_gpu_destroy(ctx);
-  afid_mgrd_destroy(mg);
-  afid_tables_destroy(t);
-  return s;
+    afid_run_stats_t st{};
+    const int total = (nsteps < 0) ? in->ntst + 1 : nsteps;
+    double dt = in->dt;
+    const double ra_pr = std::fabs(in->rayt) * in->prat;
+    auto t0 = std::chrono::steady_clock::now();
+    int errorcode = 0;
+    for (int ntime = 0; ntime < total && s == AFID_OK; ++ntime) {
+      double cflm = 0.0;
+      if ((s = mg ? afid_gpu_sal_cfl(ctx, &cflm) : afid_gpu_cfl(ctx, &cflm)) != AFID_OK) break;
+      double cflr = 0.0;
+      errorcode = afid_next_dt(in, ntime, &dt, cflm, &cflr);
+      if ((s = afid_gpu_timemarcher(ctx, dt, ntime)) != AFID_OK) break;
+      time += dt;
+      st.steps_done = ntime + 1;
+      st.cfl = cflr;
+      // main.F90:346-358: divergence check on step 1 and every tout
+      if (ntime == 1 || std::fmod(time, in->tout) < dt) {
+        double dmax = 0.0;
+        if ((s = afid_gpu_divmax(ctx, &dmax)) != AFID_OK) break;
+        st.divmax = dmax;
+        if (std::fabs(dmax) > in->resid) errorcode = AFID_E_DIVERGENCE;
+      }
+      if (stats_every > 0 && cb && ((ntime + 1) % stats_every == 0)) {
+        double nu = 0, ke = 0;
+        afid_gpu_globals(ctx, ra_pr, &nu, &ke, nullptr);
+        cb(ntime, time, dt, nu, ke, user);
+      }
+      if (frames && std::fmod(time, in->save_3d) < dt && std::floor(time / in->tframe) != 0.0) {
+        master.time = time;
+        if ((s = afid_gpu_write_flow_field(ctx, dir, 0, in->save_3d, &master)) != AFID_OK) break;
+      }
+      if (time > in->tmax) errorcode = 333;
+      if (errorcode == 0 && nsteps < 0 && ntime == in->ntst) errorcode = 555;
+      if (errorcode != 0) break;
+    }
+    if (s == AFID_OK) s = afid_gpu_synchronize(ctx);
+    auto t1 = std::chrono::steady_clock::now();
+    st.seconds = std::chrono::duration<double>(t1 - t0).count();
+    st.time = time;
+    st.dt = dt;
+    st.errorcode = errorcode;
+    if (s == AFID_OK) afid_gpu_globals(ctx, ra_pr, &st.nu_vol, &st.ke, nullptr);
+    // QuitRoutine.F90:37: the continua files on a normal exit
+    if (s == AFID_OK && dir && (errorcode == 0 || errorcode == 333 || errorcode == 334 || errorcode == 555)) {
+      master.time = time;
+      s = afid_gpu_write_flow_field(ctx, dir, 1, in->save_3d, &master);
+    }
+    if (stats) *stats = st;
+    afid_gpu_destroy(ctx);
+    afid_mgrd_destroy(mg);
+    afid_tables_destroy(t);
+    return s;
+  });
 }
 
 }  // extern "C"

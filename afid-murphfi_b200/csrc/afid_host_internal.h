@@ -1,12 +1,26 @@
-// afid_host_internal.h — host-side pieces shared by afid_host.cpp and afid_mgrd.cpp.
+// afid_host_internal.h — host-side pieces shared by the host-code translation units.
 #pragma once
 #include <stdint.h>
 
 #include <map>
+#include <new>
 #include <string>
 #include <vector>
 
 #include "afid_host.h"
+
+// Runs the body of a C entry point so that no C++ exception crosses the C ABI: a failed host
+// allocation becomes AFID_E_ALLOC, anything else AFID_E_INVALID.
+template <class F>
+int afid_guard(F &&body) noexcept {
+  try {
+    return body();
+  } catch (const std::bad_alloc &) {
+    return AFID_E_ALLOC;
+  } catch (...) {
+    return AFID_E_INVALID;
+  }
+}
 
 // The tables behind afid_tables_t (include/afid_host.h).
 struct afid_tables {

@@ -325,30 +325,32 @@ const double *afid_mgrd_array(const afid_mgrd_t *m, const char *name, int *len) 
 }
 
 int afid_initial_salinity(const afid_mgrd_t *m, uint64_t seed, double amp, double *sal, int ld_x, int ld_y) {
-  if (!m || !sal) return AFID_E_INVALID;
-  const afid_sal_grid_t &v = m->view;
-  if (ld_x < v.nxmr || ld_y < v.nymr) return AFID_E_INVALID;
-  const std::vector<double> &xmr = m->arr.at("xmr"), &xcr = m->arr.at("xcr");
-  const bool ddc = v.active_s == 1 && m->active_t == 1 && m->gaxis == 1;  // salinity.F90:148-157
-  const uint64_t nxr = (uint64_t)v.nxmr + 1;
-  for (int i = 0; i < v.nzmr; ++i)
-    for (int j = 0; j < v.nymr; ++j) {
-      double *col = sal + ((size_t)i * ld_y + j) * ld_x;
-      for (int k = 0; k < v.nxmr; ++k) {
-        if (ddc) {
-          col[k] = 0.5 * std::pow(2 * (xmr[k] - 0.5), 7);
-          continue;
+  return afid_guard([&]() -> int {
+    if (!m || !sal) return AFID_E_INVALID;
+    const afid_sal_grid_t &v = m->view;
+    if (ld_x < v.nxmr || ld_y < v.nymr) return AFID_E_INVALID;
+    const std::vector<double> &xmr = m->arr.at("xmr"), &xcr = m->arr.at("xcr");
+    const bool ddc = v.active_s == 1 && m->active_t == 1 && m->gaxis == 1;  // salinity.F90:148-157
+    const uint64_t nxr = (uint64_t)v.nxmr + 1;
+    for (int i = 0; i < v.nzmr; ++i)
+      for (int j = 0; j < v.nymr; ++j) {
+        double *col = sal + ((size_t)i * ld_y + j) * ld_x;
+        for (int k = 0; k < v.nxmr; ++k) {
+          if (ddc) {
+            col[k] = 0.5 * std::pow(2 * (xmr[k] - 0.5), 7);
+            continue;
+          }
+          // SetLinearSalinity + AddSalinityNoise(amp, localised = .false.) (salinity.F90:176-266)
+          const double s0 = m->salbp0 - (m->salbp0 - m->saltp0) * xmr[k] / xcr[v.nxmr];
+          const double u = philox_u(seed, (uint64_t)k + nxr * ((uint64_t)j + (uint64_t)v.nymr * i));
+          if (std::fabs(s0) + amp > 0.5)
+            col[k] = s0 + (0.5 - std::fabs(s0)) * (2.0 * u - 1.0);
+          else
+            col[k] = s0 + amp * (2.0 * u - 1.0);
         }
-        // SetLinearSalinity + AddSalinityNoise(amp, localised = .false.) (salinity.F90:176-266)
-        const double s0 = m->salbp0 - (m->salbp0 - m->saltp0) * xmr[k] / xcr[v.nxmr];
-        const double u = philox_u(seed, (uint64_t)k + nxr * ((uint64_t)j + (uint64_t)v.nymr * i));
-        if (std::fabs(s0) + amp > 0.5)
-          col[k] = s0 + (0.5 - std::fabs(s0)) * (2.0 * u - 1.0);
-        else
-          col[k] = s0 + amp * (2.0 * u - 1.0);
       }
-    }
-  return AFID_OK;
+    return AFID_OK;
+  });
 }
 
 }  // extern "C"

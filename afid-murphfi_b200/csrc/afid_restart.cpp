@@ -120,210 +120,214 @@ int read_var(const std::string &path, std::vector<double> &v, int n1, int n2, in
 extern "C" int afid_read_flow_interp(const char *dir, const afid_input_t *in, double *time_out, double *vx,
                                      double *vy, double *vz, double *temp, double *pr, int *pr_read,
                                      int *interpolated, double *sal) {
-  if (!dir || !in || !vx || !vy || !vz || !temp) return AFID_E_INVALID;
-  afid_continua_master_t cur{};
-  int s = afid_continua_master_from_input(in, 0.0, &cur);
-  if (s != AFID_OK) return s;
-  const bool want_sal = in->multires && sal;
-  cur.multires = in->multires ? 1 : 0;
-  afid_continua_master_t old{};
-  if ((s = afid_read_continua_master(dir, cur.multires, &old)) != AFID_OK) return s;
-  if (std::fabs(cur.ylen - old.ylen) > 1e-8 || std::fabs(cur.zlen - old.zlen) > 1e-8) return AFID_E_INVALID;
-  const bool same = cur.nx == old.nx && cur.ny == old.ny && cur.nz == old.nz && cur.istr3 == old.istr3 &&
-                    std::fabs(cur.str3 - old.str3) <= 1e-8 &&
-                    (!cur.multires || (cur.nxr == old.nxr && cur.nyr == old.nyr && cur.nzr == old.nzr &&
-                                       cur.istr3r == old.istr3r));
-  if (interpolated) *interpolated = same ? 0 : 1;
-  if (same)
-    return afid_read_flow_field(dir, &cur, time_out, vx, vy, vz, temp, pr, pr_read, want_sal ? sal : nullptr);
+  return afid_guard([&]() -> int {
+    if (!dir || !in || !vx || !vy || !vz || !temp) return AFID_E_INVALID;
+    afid_continua_master_t cur{};
+    int s = afid_continua_master_from_input(in, 0.0, &cur);
+    if (s != AFID_OK) return s;
+    const bool want_sal = in->multires && sal;
+    cur.multires = in->multires ? 1 : 0;
+    afid_continua_master_t old{};
+    if ((s = afid_read_continua_master(dir, cur.multires, &old)) != AFID_OK) return s;
+    if (std::fabs(cur.ylen - old.ylen) > 1e-8 || std::fabs(cur.zlen - old.zlen) > 1e-8) return AFID_E_INVALID;
+    const bool same = cur.nx == old.nx && cur.ny == old.ny && cur.nz == old.nz && cur.istr3 == old.istr3 &&
+                      std::fabs(cur.str3 - old.str3) <= 1e-8 &&
+                      (!cur.multires || (cur.nxr == old.nxr && cur.nyr == old.nyr && cur.nzr == old.nzr &&
+                                         cur.istr3r == old.istr3r));
+    if (interpolated) *interpolated = same ? 0 : 1;
+    if (same)
+      return afid_read_flow_field(dir, &cur, time_out, vx, vy, vz, temp, pr, pr_read, want_sal ? sal : nullptr);
 
-  // ---- CreateOldGrid / current grid ----
-  const int nxo = old.nx, nxmo = nxo - 1, nymo = old.ny - 1, nzmo = old.nz - 1;
-  if (nxmo < 2 || nymo < 1 || nzmo < 1 || (nzmo == 1) != (in->nzm == 1)) return AFID_E_INVALID;
-  const double pi = 2.0 * std::asin(1.0);
-  std::vector<double> xco, yco, ymo, zco, zmo, xc, yc, ym, zc, zm;
-  if (afid_hostd::x_grid(old.istr3, nxmo, in->alx3, old.str3, pi, 1.0, xco) != AFID_OK) return AFID_E_INVALID;
-  afid_hostd::uniform_grid(yco, ymo, nymo, in->ylen);
-  afid_hostd::uniform_grid(zco, zmo, nzmo, in->zlen);
-  const int nxm = in->nxm, nym = in->nym, nzm = in->nzm, nx = nxm + 1;
-  if (afid_hostd::x_grid(in->istr3, nxm, in->alx3, in->str3, pi, 1.0, xc) != AFID_OK) return AFID_E_INVALID;
-  afid_hostd::uniform_grid(yc, ym, nym, in->ylen);
-  afid_hostd::uniform_grid(zc, zm, nzm, in->zlen);
-  const std::vector<double> xmo = centres(xco), xm = centres(xc);
-  Axis ax, ay, az;  // CreateInputStencil: cell centres to cell centres
-  if (!make_axis(xmo, xm, in->alx3, 'x', ax) || !make_axis(ymo, ym, in->ylen, 'y', ay) ||
-      !make_axis(zmo, zm, in->zlen, 'z', az))
-    return AFID_E_INVALID;
+    // ---- CreateOldGrid / current grid ----
+    const int nxo = old.nx, nxmo = nxo - 1, nymo = old.ny - 1, nzmo = old.nz - 1;
+    if (nxmo < 2 || nymo < 1 || nzmo < 1 || (nzmo == 1) != (in->nzm == 1)) return AFID_E_INVALID;
+    const double pi = 2.0 * std::asin(1.0);
+    std::vector<double> xco, yco, ymo, zco, zmo, xc, yc, ym, zc, zm;
+    if (afid_hostd::x_grid(old.istr3, nxmo, in->alx3, old.str3, pi, 1.0, xco) != AFID_OK) return AFID_E_INVALID;
+    afid_hostd::uniform_grid(yco, ymo, nymo, in->ylen);
+    afid_hostd::uniform_grid(zco, zmo, nzmo, in->zlen);
+    const int nxm = in->nxm, nym = in->nym, nzm = in->nzm, nx = nxm + 1;
+    if (afid_hostd::x_grid(in->istr3, nxm, in->alx3, in->str3, pi, 1.0, xc) != AFID_OK) return AFID_E_INVALID;
+    afid_hostd::uniform_grid(yc, ym, nym, in->ylen);
+    afid_hostd::uniform_grid(zc, zm, nzm, in->zlen);
+    const std::vector<double> xmo = centres(xco), xm = centres(xc);
+    Axis ax, ay, az;  // CreateInputStencil: cell centres to cell centres
+    if (!make_axis(xmo, xm, in->alx3, 'x', ax) || !make_axis(ymo, ym, in->ylen, 'y', ay) ||
+        !make_axis(zmo, zm, in->zlen, 'z', az))
+      return AFID_E_INVALID;
 
-  const std::string base = std::string(dir) + "/continua";
-  std::vector<double> f;
-  const size_t plane = (size_t)nym * nx, ncell = plane * nzm;
-  std::fill(vx, vx + ncell, 0.0);
-  std::fill(vy, vy + ncell, 0.0);
-  std::fill(vz, vz + ncell, 0.0);
-  std::fill(temp, temp + ncell, 0.0);
-  std::vector<double> grad(ncell);  // tpdv on the new grid, x stride nx
-  Ext e(nzmo, nymo, nxmo);
-  auto wall_rows = [&](Ext &x) {  // rows 0 and nxo: (1 - 2 inslw) * rows 1 and nxmo
+    const std::string base = std::string(dir) + "/continua";
+    std::vector<double> f;
+    const size_t plane = (size_t)nym * nx, ncell = plane * nzm;
+    std::fill(vx, vx + ncell, 0.0);
+    std::fill(vy, vy + ncell, 0.0);
+    std::fill(vz, vz + ncell, 0.0);
+    std::fill(temp, temp + ncell, 0.0);
+    std::vector<double> grad(ncell);  // tpdv on the new grid, x stride nx
+    Ext e(nzmo, nymo, nxmo);
+    auto wall_rows = [&](Ext &x) {  // rows 0 and nxo: (1 - 2 inslw) * rows 1 and nxmo
+      for (int i = 0; i < nzmo; ++i)
+        for (int j = 0; j < nymo; ++j) {
+          double *c = x.col(i, j);
+          c[1] = (1 - 2 * in->inslws) * c[2];
+          c[nxmo + 2] = (1 - 2 * in->inslwn) * c[nxmo + 1];
+        }
+    };
+    // ---- vx: dvx/dx at the old centres, interpolated, integrated from vx(1) = 0 ----
+    if ((s = read_var(base + "_vx.h5", f, nxo, nymo, nzmo)) != AFID_OK) return s;
     for (int i = 0; i < nzmo; ++i)
       for (int j = 0; j < nymo; ++j) {
-        double *c = x.col(i, j);
+        const double *v = &f[((size_t)i * nymo + j) * nxo];
+        double *c = e.col(i, j);
+        for (int k = 0; k < nxmo; ++k) c[k + 2] = (v[k + 1] - v[k]) / (xco[k + 1] - xco[k]);
+      }
+    wall_rows(e);
+    interp3(e, ax, ay, az, grad.data(), nx);
+    for (size_t c = 0; c < (size_t)nym * nzm; ++c) {
+      double *v = vx + c * nx;
+      const double *g = &grad[c * nx];
+      v[0] = 0.0;
+      for (int k = 0; k < nxm; ++k) v[k + 1] = v[k] + g[k] * (xc[k + 1] - xc[k]);
+    }
+    // ---- vy: dvy/dy, the y = 0 plane interpolated in x-z, integrated along y ----
+    if ((s = read_var(base + "_vy.h5", f, nxo, nymo, nzmo)) != AFID_OK) return s;
+    const double dyo = 1.0 / (yco[1] - yco[0]), dzo = 1.0 / (zco[1] - zco[0]);
+    for (int i = 0; i < nzmo; ++i)
+      for (int j = 0; j < nymo; ++j) {
+        const double *v = &f[((size_t)i * nymo + j) * nxo], *vp = &f[((size_t)i * nymo + (j + 1) % nymo) * nxo];
+        double *c = e.col(i, j);
+        for (int k = 0; k < nxmo; ++k) c[k + 2] = (vp[k] - v[k]) * dyo;
+      }
+    wall_rows(e);
+    interp3(e, ax, ay, az, grad.data(), nx);
+    {
+      std::vector<double> pl((size_t)nzmo * (nxmo + 4), 0.0);
+      for (int i = 0; i < nzmo; ++i) {
+        const double *v = &f[((size_t)i * nymo) * nxo];
+        double *c = &pl[(size_t)i * (nxmo + 4)];
+        for (int k = 0; k < nxmo; ++k) c[k + 2] = v[k];
         c[1] = (1 - 2 * in->inslws) * c[2];
         c[nxmo + 2] = (1 - 2 * in->inslwn) * c[nxmo + 1];
       }
-  };
-  // ---- vx: dvx/dx at the old centres, interpolated, integrated from vx(1) = 0 ----
-  if ((s = read_var(base + "_vx.h5", f, nxo, nymo, nzmo)) != AFID_OK) return s;
-  for (int i = 0; i < nzmo; ++i)
-    for (int j = 0; j < nymo; ++j) {
-      const double *v = &f[((size_t)i * nymo + j) * nxo];
-      double *c = e.col(i, j);
-      for (int k = 0; k < nxmo; ++k) c[k + 2] = (v[k + 1] - v[k]) / (xco[k + 1] - xco[k]);
+      interp2(pl, nzmo, nxmo, ax, az, vy, plane);  // vy(:, 1, :) of every new z plane
     }
-  wall_rows(e);
-  interp3(e, ax, ay, az, grad.data(), nx);
-  for (size_t c = 0; c < (size_t)nym * nzm; ++c) {
-    double *v = vx + c * nx;
-    const double *g = &grad[c * nx];
-    v[0] = 0.0;
-    for (int k = 0; k < nxm; ++k) v[k + 1] = v[k] + g[k] * (xc[k + 1] - xc[k]);
-  }
-  // ---- vy: dvy/dy, the y = 0 plane interpolated in x-z, integrated along y ----
-  if ((s = read_var(base + "_vy.h5", f, nxo, nymo, nzmo)) != AFID_OK) return s;
-  const double dyo = 1.0 / (yco[1] - yco[0]), dzo = 1.0 / (zco[1] - zco[0]);
-  for (int i = 0; i < nzmo; ++i)
-    for (int j = 0; j < nymo; ++j) {
-      const double *v = &f[((size_t)i * nymo + j) * nxo], *vp = &f[((size_t)i * nymo + (j + 1) % nymo) * nxo];
-      double *c = e.col(i, j);
-      for (int k = 0; k < nxmo; ++k) c[k + 2] = (vp[k] - v[k]) * dyo;
-    }
-  wall_rows(e);
-  interp3(e, ax, ay, az, grad.data(), nx);
-  {
-    std::vector<double> pl((size_t)nzmo * (nxmo + 4), 0.0);
-    for (int i = 0; i < nzmo; ++i) {
-      const double *v = &f[((size_t)i * nymo) * nxo];
-      double *c = &pl[(size_t)i * (nxmo + 4)];
-      for (int k = 0; k < nxmo; ++k) c[k + 2] = v[k];
-      c[1] = (1 - 2 * in->inslws) * c[2];
-      c[nxmo + 2] = (1 - 2 * in->inslwn) * c[nxmo + 1];
-    }
-    interp2(pl, nzmo, nxmo, ax, az, vy, plane);  // vy(:, 1, :) of every new z plane
-  }
-  const double lya = 1.0 / ((double)nym / in->ylen), lza = 1.0 / ((double)nzm / in->zlen);
-  for (int i = 0; i < nzm; ++i)
-    for (int j = 0; j + 1 < nym; ++j) {
-      double *v = vy + (size_t)i * plane + (size_t)j * nx;
-      const double *g = &grad[(size_t)i * plane + (size_t)j * nx];
-      for (int k = 0; k < nxm; ++k) v[nx + k] = v[k] + g[k] * lya;
-    }
-  // ---- vz: dvz/dz, the z = 0 plane interpolated in x-y, integrated along z ----
-  if ((s = read_var(base + "_vz.h5", f, nxo, nymo, nzmo)) != AFID_OK) return s;
-  for (int i = 0; i < nzmo; ++i)
-    for (int j = 0; j < nymo; ++j) {
-      const double *v = &f[((size_t)i * nymo + j) * nxo], *vp = &f[((size_t)((i + 1) % nzmo) * nymo + j) * nxo];
-      double *c = e.col(i, j);
-      for (int k = 0; k < nxmo; ++k) c[k + 2] = (vp[k] - v[k]) * dzo;
-    }
-  wall_rows(e);
-  interp3(e, ax, ay, az, grad.data(), nx);
-  {
-    std::vector<double> pl((size_t)nymo * (nxmo + 4), 0.0);
-    for (int j = 0; j < nymo; ++j) {
-      const double *v = &f[(size_t)j * nxo];
-      double *c = &pl[(size_t)j * (nxmo + 4)];
-      for (int k = 0; k < nxmo; ++k) c[k + 2] = v[k];
-      c[1] = (1 - 2 * in->inslws) * c[2];
-      c[nxmo + 2] = (1 - 2 * in->inslwn) * c[nxmo + 1];
-    }
-    interp2(pl, nymo, nxmo, ax, ay, vz, nx);  // vz(:, :, 1)
-  }
-  for (int i = 0; i + 1 < nzm; ++i)
-    for (int j = 0; j < nym; ++j) {
-      double *v = vz + (size_t)i * plane + (size_t)j * nx;
-      const double *g = &grad[(size_t)i * plane + (size_t)j * nx];
-      for (int k = 0; k < nxm; ++k) v[plane + k] = v[k] + g[k] * lza;
-    }
-  // ---- temperature with the plate ghosts ----
-  if ((s = read_var(base + "_temp.h5", f, nxo, nymo, nzmo)) != AFID_OK) return s;
-  double tlo, tup;
-  if (in->rayt > 0) {
-    tup = in->inslwn == 0 ? 0.0 : -0.5;
-    tlo = in->inslwn == 0 ? 1.0 : 0.5;
-  } else {
-    tup = 0.5;
-    tlo = -0.5;
-  }
-  for (int i = 0; i < nzmo; ++i)
-    for (int j = 0; j < nymo; ++j) {
-      const double *v = &f[((size_t)i * nymo + j) * nxo];
-      double *c = e.col(i, j);
-      for (int k = 0; k < nxmo; ++k) c[k + 2] = v[k];
-      c[1] = in->tfixs == 1 ? 2.0 * tlo - v[0] : v[0];
-      c[nxmo + 2] = in->tfixn == 1 ? 2.0 * tup - v[nxmo - 1] : v[nxmo - 1];
-    }
-  interp3(e, ax, ay, az, temp, nx);
-  for (size_t c = 0; c < (size_t)nym * nzm; ++c) temp[c * nx + nxm] = 0.0;
-  // ---- refined salinity ----
-  if (want_sal) {
-    const int nxmro = old.nxr - 1, nymro = old.nyr - 1, nzmro = old.nzr - 1;
-    const int nxmr = in->nxmr, nymr = in->nymr, nzmr = in->nzmr;
-    if (nxmro < 2 || nymro < 1 || nzmro < 1) return AFID_E_INVALID;
-    std::vector<double> xcro, ycro, ymro, zcro, zmro, xcr, ycr, ymr, zcr, zmr;
-    // CreateOldGrid.F90: the old refined grid takes the old STR3 and Schmidt number 1
-    if (afid_hostd::x_grid(old.istr3r, nxmro, in->alx3, old.str3, pi, 1.0, xcro) != AFID_OK) return AFID_E_INVALID;
-    afid_hostd::uniform_grid(ycro, ymro, nymro, in->ylen);
-    afid_hostd::uniform_grid(zcro, zmro, nzmro, in->zlen);
-    // CreateMgrdGrid.F90: the current refined grid (as afid_mgrd_create builds it)
-    if (afid_hostd::x_grid(in->istr3r, nxmr, in->alx3, in->str3, pi, in->pras, xcr) != AFID_OK) return AFID_E_INVALID;
-    afid_hostd::uniform_grid(ycr, ymr, nymr, in->ylen);
-    afid_hostd::uniform_grid(zcr, zmr, nzmr, in->zlen);
-    Axis rx, ry, rz;
-    if (!make_axis(centres(xcro), centres(xcr), in->alx3, 'x', rx) || !make_axis(ymro, ymr, in->ylen, 'y', ry) ||
-        !make_axis(zmro, zmr, in->zlen, 'z', rz))
-      return AFID_E_INVALID;
-    if ((s = read_var(base + "_sal.h5", f, nxmro + 1, nymro, nzmro)) != AFID_OK) return s;
-    const double slo = in->rays > 0 ? -0.5 : 0.5, sup = in->rays > 0 ? 0.5 : -0.5;
-    Ext es(nzmro, nymro, nxmro);
-    for (int i = 0; i < nzmro; ++i)
-      for (int j = 0; j < nymro; ++j) {
-        const double *v = &f[((size_t)i * nymro + j) * (nxmro + 1)];
-        double *c = es.col(i, j);
-        for (int k = 0; k < nxmro; ++k) c[k + 2] = v[k];
-        c[1] = in->sfixs == 1 ? 2.0 * slo - v[0] : v[0];
-        c[nxmro + 2] = in->sfixn == 1 ? 2.0 * sup - v[nxmro - 1] : v[nxmro - 1];
+    const double lya = 1.0 / ((double)nym / in->ylen), lza = 1.0 / ((double)nzm / in->zlen);
+    for (int i = 0; i < nzm; ++i)
+      for (int j = 0; j + 1 < nym; ++j) {
+        double *v = vy + (size_t)i * plane + (size_t)j * nx;
+        const double *g = &grad[(size_t)i * plane + (size_t)j * nx];
+        for (int k = 0; k < nxm; ++k) v[nx + k] = v[k] + g[k] * lya;
       }
-    interp3(es, rx, ry, rz, sal, nxmr);
-  }
-  // the pressure is not read in this branch (it stays zero)
-  if (pr) std::fill(pr, pr + ncell, 0.0);
-  if (pr_read) *pr_read = 0;
-  if (time_out) *time_out = old.time;
-  return AFID_OK;
+    // ---- vz: dvz/dz, the z = 0 plane interpolated in x-y, integrated along z ----
+    if ((s = read_var(base + "_vz.h5", f, nxo, nymo, nzmo)) != AFID_OK) return s;
+    for (int i = 0; i < nzmo; ++i)
+      for (int j = 0; j < nymo; ++j) {
+        const double *v = &f[((size_t)i * nymo + j) * nxo], *vp = &f[((size_t)((i + 1) % nzmo) * nymo + j) * nxo];
+        double *c = e.col(i, j);
+        for (int k = 0; k < nxmo; ++k) c[k + 2] = (vp[k] - v[k]) * dzo;
+      }
+    wall_rows(e);
+    interp3(e, ax, ay, az, grad.data(), nx);
+    {
+      std::vector<double> pl((size_t)nymo * (nxmo + 4), 0.0);
+      for (int j = 0; j < nymo; ++j) {
+        const double *v = &f[(size_t)j * nxo];
+        double *c = &pl[(size_t)j * (nxmo + 4)];
+        for (int k = 0; k < nxmo; ++k) c[k + 2] = v[k];
+        c[1] = (1 - 2 * in->inslws) * c[2];
+        c[nxmo + 2] = (1 - 2 * in->inslwn) * c[nxmo + 1];
+      }
+      interp2(pl, nymo, nxmo, ax, ay, vz, nx);  // vz(:, :, 1)
+    }
+    for (int i = 0; i + 1 < nzm; ++i)
+      for (int j = 0; j < nym; ++j) {
+        double *v = vz + (size_t)i * plane + (size_t)j * nx;
+        const double *g = &grad[(size_t)i * plane + (size_t)j * nx];
+        for (int k = 0; k < nxm; ++k) v[plane + k] = v[k] + g[k] * lza;
+      }
+    // ---- temperature with the plate ghosts ----
+    if ((s = read_var(base + "_temp.h5", f, nxo, nymo, nzmo)) != AFID_OK) return s;
+    double tlo, tup;
+    if (in->rayt > 0) {
+      tup = in->inslwn == 0 ? 0.0 : -0.5;
+      tlo = in->inslwn == 0 ? 1.0 : 0.5;
+    } else {
+      tup = 0.5;
+      tlo = -0.5;
+    }
+    for (int i = 0; i < nzmo; ++i)
+      for (int j = 0; j < nymo; ++j) {
+        const double *v = &f[((size_t)i * nymo + j) * nxo];
+        double *c = e.col(i, j);
+        for (int k = 0; k < nxmo; ++k) c[k + 2] = v[k];
+        c[1] = in->tfixs == 1 ? 2.0 * tlo - v[0] : v[0];
+        c[nxmo + 2] = in->tfixn == 1 ? 2.0 * tup - v[nxmo - 1] : v[nxmo - 1];
+      }
+    interp3(e, ax, ay, az, temp, nx);
+    for (size_t c = 0; c < (size_t)nym * nzm; ++c) temp[c * nx + nxm] = 0.0;
+    // ---- refined salinity ----
+    if (want_sal) {
+      const int nxmro = old.nxr - 1, nymro = old.nyr - 1, nzmro = old.nzr - 1;
+      const int nxmr = in->nxmr, nymr = in->nymr, nzmr = in->nzmr;
+      if (nxmro < 2 || nymro < 1 || nzmro < 1) return AFID_E_INVALID;
+      std::vector<double> xcro, ycro, ymro, zcro, zmro, xcr, ycr, ymr, zcr, zmr;
+      // CreateOldGrid.F90: the old refined grid takes the old STR3 and Schmidt number 1
+      if (afid_hostd::x_grid(old.istr3r, nxmro, in->alx3, old.str3, pi, 1.0, xcro) != AFID_OK) return AFID_E_INVALID;
+      afid_hostd::uniform_grid(ycro, ymro, nymro, in->ylen);
+      afid_hostd::uniform_grid(zcro, zmro, nzmro, in->zlen);
+      // CreateMgrdGrid.F90: the current refined grid (as afid_mgrd_create builds it)
+      if (afid_hostd::x_grid(in->istr3r, nxmr, in->alx3, in->str3, pi, in->pras, xcr) != AFID_OK) return AFID_E_INVALID;
+      afid_hostd::uniform_grid(ycr, ymr, nymr, in->ylen);
+      afid_hostd::uniform_grid(zcr, zmr, nzmr, in->zlen);
+      Axis rx, ry, rz;
+      if (!make_axis(centres(xcro), centres(xcr), in->alx3, 'x', rx) || !make_axis(ymro, ymr, in->ylen, 'y', ry) ||
+          !make_axis(zmro, zmr, in->zlen, 'z', rz))
+        return AFID_E_INVALID;
+      if ((s = read_var(base + "_sal.h5", f, nxmro + 1, nymro, nzmro)) != AFID_OK) return s;
+      const double slo = in->rays > 0 ? -0.5 : 0.5, sup = in->rays > 0 ? 0.5 : -0.5;
+      Ext es(nzmro, nymro, nxmro);
+      for (int i = 0; i < nzmro; ++i)
+        for (int j = 0; j < nymro; ++j) {
+          const double *v = &f[((size_t)i * nymro + j) * (nxmro + 1)];
+          double *c = es.col(i, j);
+          for (int k = 0; k < nxmro; ++k) c[k + 2] = v[k];
+          c[1] = in->sfixs == 1 ? 2.0 * slo - v[0] : v[0];
+          c[nxmro + 2] = in->sfixn == 1 ? 2.0 * sup - v[nxmro - 1] : v[nxmro - 1];
+        }
+      interp3(es, rx, ry, rz, sal, nxmr);
+    }
+    // the pressure is not read in this branch (it stays zero)
+    if (pr) std::fill(pr, pr + ncell, 0.0);
+    if (pr_read) *pr_read = 0;
+    if (time_out) *time_out = old.time;
+    return AFID_OK;
+  });
 }
 
 extern "C" int afid_gpu_read_flow_interp(afid_ctx_t *ctx, const char *dir, const afid_input_t *in, double *time_out,
                                          int *interpolated) {
-  if (!ctx || !dir || !in) return AFID_E_INVALID;
-  int dims[6];
-  int s = afid_gpu_dims(ctx, dims);
-  if (s != AFID_OK) return s;
-  if (in->nxm != dims[0] || in->nym != dims[1] || in->nzm != dims[2]) return AFID_E_INVALID;
-  const bool with_sal = in->multires && dims[3] > 0;
-  if (with_sal && (in->nxmr != dims[3] || in->nymr != dims[4] || in->nzmr != dims[5])) return AFID_E_INVALID;
-  const int nx = dims[0] + 1, nym = dims[1], nzm = dims[2];
-  const size_t n = (size_t)nx * nym * nzm;
-  std::vector<double> fl(5 * n, 0.0);
-  double *vx = fl.data(), *vy = vx + n, *vz = vy + n, *temp = vz + n, *pr = temp + n;
-  std::vector<double> sal(with_sal ? (size_t)dims[3] * dims[4] * dims[5] : 0);
-  int pr_read = 0, interp = 0;
-  double t = 0.0;
-  if ((s = afid_read_flow_interp(dir, in, &t, vx, vy, vz, temp, pr, &pr_read, &interp,
-                                 with_sal ? sal.data() : nullptr)) != AFID_OK)
-    return s;
-  if ((s = afid_gpu_upload(ctx, vx, vy, vz, temp, pr, nx, nym)) != AFID_OK) return s;
-  if (with_sal && (s = afid_gpu_sal_upload(ctx, sal.data(), dims[3], dims[4])) != AFID_OK) return s;
-  if (time_out) *time_out = t;
-  if (interpolated) *interpolated = interp;
-  return AFID_OK;
+  return afid_guard([&]() -> int {
+    if (!ctx || !dir || !in) return AFID_E_INVALID;
+    int dims[6];
+    int s = afid_gpu_dims(ctx, dims);
+    if (s != AFID_OK) return s;
+    if (in->nxm != dims[0] || in->nym != dims[1] || in->nzm != dims[2]) return AFID_E_INVALID;
+    const bool with_sal = in->multires && dims[3] > 0;
+    if (with_sal && (in->nxmr != dims[3] || in->nymr != dims[4] || in->nzmr != dims[5])) return AFID_E_INVALID;
+    const int nx = dims[0] + 1, nym = dims[1], nzm = dims[2];
+    const size_t n = (size_t)nx * nym * nzm;
+    std::vector<double> fl(5 * n, 0.0);
+    double *vx = fl.data(), *vy = vx + n, *vz = vy + n, *temp = vz + n, *pr = temp + n;
+    std::vector<double> sal(with_sal ? (size_t)dims[3] * dims[4] * dims[5] : 0);
+    int pr_read = 0, interp = 0;
+    double t = 0.0;
+    if ((s = afid_read_flow_interp(dir, in, &t, vx, vy, vz, temp, pr, &pr_read, &interp,
+                                   with_sal ? sal.data() : nullptr)) != AFID_OK)
+      return s;
+    if ((s = afid_gpu_upload(ctx, vx, vy, vz, temp, pr, nx, nym)) != AFID_OK) return s;
+    if (with_sal && (s = afid_gpu_sal_upload(ctx, sal.data(), dims[3], dims[4])) != AFID_OK) return s;
+    if (time_out) *time_out = t;
+    if (interpolated) *interpolated = interp;
+    return AFID_OK;
+  });
 }

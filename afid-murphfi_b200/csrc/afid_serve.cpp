@@ -11,6 +11,7 @@
 
 #include "afid_batch.h"
 #include "afid_serve.h"
+#include "afid_host_internal.h"
 
 namespace {
 
@@ -257,36 +258,42 @@ int harvest(afid_server_t *s, Pool *p) {
 extern "C" {
 
 int afid_serve_create(const afid_serve_config_t *cfg, afid_server_t **out) {
-  if (!cfg || !out || cfg->hbm_budget_bytes <= 0 || cfg->chunk_steps < 1 ||
-      (cfg->precision != AFID_PREC_FP64 && cfg->precision != AFID_PREC_MIXED))
-    return AFID_E_INVALID;
-  afid_server_t *s = new (std::nothrow) afid_server_t();
-  if (!s) return AFID_E_ALLOC;
-  s->cfg = *cfg;
-  if (s->cfg.slots_per_pool < 1) s->cfg.slots_per_pool = 1;
-  s->t0 = std::chrono::steady_clock::now();
-  *out = s;
-  return AFID_OK;
+  return afid_guard([&]() -> int {
+    if (!cfg || !out || cfg->hbm_budget_bytes <= 0 || cfg->chunk_steps < 1 ||
+        (cfg->precision != AFID_PREC_FP64 && cfg->precision != AFID_PREC_MIXED))
+      return AFID_E_INVALID;
+    afid_server_t *s = new (std::nothrow) afid_server_t();
+    if (!s) return AFID_E_ALLOC;
+    s->cfg = *cfg;
+    if (s->cfg.slots_per_pool < 1) s->cfg.slots_per_pool = 1;
+    s->t0 = std::chrono::steady_clock::now();
+    *out = s;
+    return AFID_OK;
+  });
 }
 
 int afid_serve_destroy(afid_server_t *s) {
-  if (!s) return AFID_OK;
-  while (!s->pools.empty()) drop_pool(s, s->pools.size() - 1);
-  delete s;
-  return AFID_OK;
+  return afid_guard([&]() -> int {
+    if (!s) return AFID_OK;
+    while (!s->pools.empty()) drop_pool(s, s->pools.size() - 1);
+    delete s;
+    return AFID_OK;
+  });
 }
 
 int afid_serve_submit(afid_server_t *s, const afid_serve_job_t *job) {
-  if (!s || !job || job->nsteps < 1 || job->in.nxm < 2 || job->in.nym < 1 || job->in.nzm < 1 ||
-      job->in.dpdz != 0.0 || job->in.flagsal)
-    return AFID_E_INVALID;  // served jobs carry no salinity
-  Job j;
-  j.spec = *job;
-  j.t_submit = now_s(s);
-  j.cells = (long long)job->in.nxm * job->in.nym * job->in.nzm;
-  j.order = s->submitted++;
-  s->queue.push_back(j);
-  return AFID_OK;
+  return afid_guard([&]() -> int {
+    if (!s || !job || job->nsteps < 1 || job->in.nxm < 2 || job->in.nym < 1 || job->in.nzm < 1 ||
+        job->in.dpdz != 0.0 || job->in.flagsal)
+      return AFID_E_INVALID;  // served jobs carry no salinity
+    Job j;
+    j.spec = *job;
+    j.t_submit = now_s(s);
+    j.cells = (long long)job->in.nxm * job->in.nym * job->in.nzm;
+    j.order = s->submitted++;
+    s->queue.push_back(j);
+    return AFID_OK;
+  });
 }
 
 // One pass of the request loop, asynchronous per pool: pools whose chunk has completed are
@@ -295,108 +302,114 @@ int afid_serve_submit(afid_server_t *s, const afid_serve_job_t *job) {
 // for a pool of large ones).  When a pass finds nothing to do it waits for the oldest running
 // chunk instead of spinning.
 int afid_serve_pump(afid_server_t *s) {
-  if (!s) return AFID_E_INVALID;
-  bool progress = false;
-  // 1. harvest the pools whose chunk completed
-  for (Pool *p : s->pools) {
-    if (!p->in_flight) continue;
-    const cudaError_t q = cudaEventQuery(p->ev);
-    if (q == cudaErrorNotReady) continue;
-    if (q != cudaSuccess) return AFID_E_CUDA;
-    const int st = harvest(s, p);
-    if (st != AFID_OK) return st;
-    progress = true;
-  }
-  // 2. admission in policy order
-  std::vector<size_t> order(s->queue.size());
-  for (size_t i = 0; i < order.size(); ++i) order[i] = i;
-  const bool fifo = s->cfg.policy != AFID_SERVE_SHORTEST_FIRST;
-  if (!fifo)
-    std::stable_sort(order.begin(), order.end(), [&](size_t a, size_t b) {
-      return (double)s->queue[a].cells * s->queue[a].spec.nsteps < (double)s->queue[b].cells * s->queue[b].spec.nsteps;
-    });
-  std::vector<char> taken(s->queue.size(), 0);
-  for (size_t q : order) {
-    Job &j = s->queue[q];
-    if (s->cfg.max_cells_in_flight > 0 && s->cells_in_flight > 0 &&
-        s->cells_in_flight + j.cells > s->cfg.max_cells_in_flight) {
-      if (fifo) break;
-      continue;
+  return afid_guard([&]() -> int {
+    if (!s) return AFID_E_INVALID;
+    bool progress = false;
+    // 1. harvest the pools whose chunk completed
+    for (Pool *p : s->pools) {
+      if (!p->in_flight) continue;
+      const cudaError_t q = cudaEventQuery(p->ev);
+      if (q == cudaErrorNotReady) continue;
+      if (q != cudaSuccess) return AFID_E_CUDA;
+      const int st = harvest(s, p);
+      if (st != AFID_OK) return st;
+      progress = true;
     }
-    const int st = admit(s, j);
-    if (st == kBusyPool) {  // its class's pool is running a chunk: retry after the harvest
-      if (fifo) break;
-      continue;
+    // 2. admission in policy order
+    std::vector<size_t> order(s->queue.size());
+    for (size_t i = 0; i < order.size(); ++i) order[i] = i;
+    const bool fifo = s->cfg.policy != AFID_SERVE_SHORTEST_FIRST;
+    if (!fifo)
+      std::stable_sort(order.begin(), order.end(), [&](size_t a, size_t b) {
+        return (double)s->queue[a].cells * s->queue[a].spec.nsteps < (double)s->queue[b].cells * s->queue[b].spec.nsteps;
+      });
+    std::vector<char> taken(s->queue.size(), 0);
+    for (size_t q : order) {
+      Job &j = s->queue[q];
+      if (s->cfg.max_cells_in_flight > 0 && s->cells_in_flight > 0 &&
+          s->cells_in_flight + j.cells > s->cfg.max_cells_in_flight) {
+        if (fifo) break;
+        continue;
+      }
+      const int st = admit(s, j);
+      if (st == kBusyPool) {  // its class's pool is running a chunk: retry after the harvest
+        if (fifo) break;
+        continue;
+      }
+      const bool no_room = (st == AFID_E_CAPACITY || st == AFID_E_ALLOC);
+      if (no_room && !s->pools.empty()) {  // wait for running jobs to release memory
+        if (fifo) break;
+        continue;
+      }
+      if (st != AFID_OK) {
+        // malformed, or larger than the whole budget: the job completes with the status
+        afid_serve_result_t r{};
+        r.tag = j.spec.tag;
+        r.errorcode = st;
+        r.t_submit = j.t_submit;
+        r.t_admit = r.t_done = now_s(s);
+        s->done.push_back(r);
+      }
+      taken[q] = 1;
+      progress = true;
     }
-    const bool no_room = (st == AFID_E_CAPACITY || st == AFID_E_ALLOC);
-    if (no_room && !s->pools.empty()) {  // wait for running jobs to release memory
-      if (fifo) break;
-      continue;
+    std::deque<Job> rest;
+    for (size_t i = 0; i < s->queue.size(); ++i)
+      if (!taken[i]) rest.push_back(s->queue[i]);
+    s->queue.swap(rest);
+    // 3. next chunk on every idle pool with running jobs
+    for (Pool *p : s->pools) {
+      if (p->in_flight || p->busy() == 0) continue;
+      int st = AFID_OK;
+      if (p->dirty) {
+        st = afid_batch_set_active(p->b, p->active.data());
+        p->dirty = false;
+      }
+      if (st == AFID_OK) st = afid_batch_step(p->b, s->cfg.chunk_steps);
+      if (st != AFID_OK) return st;
+      if (cudaEventRecord(p->ev, p->stream) != cudaSuccess) return AFID_E_CUDA;
+      p->in_flight = true;
+      p->launched = s->launches++;
+      progress = true;
     }
-    if (st != AFID_OK) {
-      // malformed, or larger than the whole budget: the job completes with the status
-      afid_serve_result_t r{};
-      r.tag = j.spec.tag;
-      r.errorcode = st;
-      r.t_submit = j.t_submit;
-      r.t_admit = r.t_done = now_s(s);
-      s->done.push_back(r);
+    // 4. nothing happened: wait for the oldest running chunk
+    if (!progress) {
+      Pool *oldest = nullptr;
+      for (Pool *p : s->pools)
+        if (p->in_flight && (!oldest || p->launched < oldest->launched)) oldest = p;
+      if (oldest) {
+        if (cudaEventSynchronize(oldest->ev) != cudaSuccess) return AFID_E_CUDA;
+        return harvest(s, oldest);
+      }
     }
-    taken[q] = 1;
-    progress = true;
-  }
-  std::deque<Job> rest;
-  for (size_t i = 0; i < s->queue.size(); ++i)
-    if (!taken[i]) rest.push_back(s->queue[i]);
-  s->queue.swap(rest);
-  // 3. next chunk on every idle pool with running jobs
-  for (Pool *p : s->pools) {
-    if (p->in_flight || p->busy() == 0) continue;
-    int st = AFID_OK;
-    if (p->dirty) {
-      st = afid_batch_set_active(p->b, p->active.data());
-      p->dirty = false;
-    }
-    if (st == AFID_OK) st = afid_batch_step(p->b, s->cfg.chunk_steps);
-    if (st != AFID_OK) return st;
-    if (cudaEventRecord(p->ev, p->stream) != cudaSuccess) return AFID_E_CUDA;
-    p->in_flight = true;
-    p->launched = s->launches++;
-    progress = true;
-  }
-  // 4. nothing happened: wait for the oldest running chunk
-  if (!progress) {
-    Pool *oldest = nullptr;
-    for (Pool *p : s->pools)
-      if (p->in_flight && (!oldest || p->launched < oldest->launched)) oldest = p;
-    if (oldest) {
-      if (cudaEventSynchronize(oldest->ev) != cudaSuccess) return AFID_E_CUDA;
-      return harvest(s, oldest);
-    }
-  }
-  return AFID_OK;
+    return AFID_OK;
+  });
 }
 
 int afid_serve_poll(afid_server_t *s, afid_serve_result_t *out, int max, int *n) {
-  if (!s || !n || (max > 0 && !out)) return AFID_E_INVALID;
-  const int k = std::min<int>(max, (int)s->done.size());
-  for (int i = 0; i < k; ++i) out[i] = s->done[i];
-  s->done.erase(s->done.begin(), s->done.begin() + k);
-  *n = k;
-  return AFID_OK;
+  return afid_guard([&]() -> int {
+    if (!s || !n || (max > 0 && !out)) return AFID_E_INVALID;
+    const int k = std::min<int>(max, (int)s->done.size());
+    for (int i = 0; i < k; ++i) out[i] = s->done[i];
+    s->done.erase(s->done.begin(), s->done.begin() + k);
+    *n = k;
+    return AFID_OK;
+  });
 }
 
 int afid_serve_status(const afid_server_t *s, afid_serve_status_t *st) {
-  if (!s || !st) return AFID_E_INVALID;
-  st->queued = (int)s->queue.size();
-  st->running = 0;
-  for (const Pool *p : s->pools) st->running += p->busy();
-  st->pools = (int)s->pools.size();
-  st->device_bytes = pool_bytes(s);
-  st->cells_in_flight = s->cells_in_flight;
-  st->cell_steps_done = s->cell_steps_done;
-  st->jobs_done = s->jobs_done;
-  return AFID_OK;
+  return afid_guard([&]() -> int {
+    if (!s || !st) return AFID_E_INVALID;
+    st->queued = (int)s->queue.size();
+    st->running = 0;
+    for (const Pool *p : s->pools) st->running += p->busy();
+    st->pools = (int)s->pools.size();
+    st->device_bytes = pool_bytes(s);
+    st->cells_in_flight = s->cells_in_flight;
+    st->cell_steps_done = s->cell_steps_done;
+    st->jobs_done = s->jobs_done;
+    return AFID_OK;
+  });
 }
 
 double afid_serve_now(const afid_server_t *s) { return s ? now_s(s) : 0.0; }

@@ -391,3 +391,18 @@ def test_interpolating_restart_refusals(tmp_path):
         with pytest.raises(ag.AfidError) as e:
             ag.read_flow_interp(d, ag.parse_bou_in(text))
         assert e.value.status == ag.AFID_E_INVALID
+
+
+def test_allocation_failure_is_a_status_not_a_crash(tmp_path):
+    """No C++ exception crosses the C ABI: the padded copy the refined salinity file needs
+    (x extent nxmr + 1) cannot be allocated for an absurd refined grid, and the call answers
+    AFID_E_ALLOC (the caller's salinity array is never read, the allocation comes first)."""
+    inp = _input(multires=0)
+    rng = np.random.default_rng(15)
+    f = _fields(inp, rng)
+    m = ag.continua_master(inp, 0.0)
+    m.multires, m.nxr, m.nyr, m.nzr, m.istr3r = 1, 1 << 20, 1 << 20, 1 << 12, 0
+    f["sal"] = np.zeros(4)
+    with pytest.raises(ag.AfidError) as e:
+        ag.write_flow_field(str(tmp_path / "o"), m, f, final=True)
+    assert e.value.status == ag.AFID_E_ALLOC
