@@ -433,3 +433,86 @@ def write_v2(path: str, datasets: dict, compact: tuple = ()) -> None:
     assert len(out) == eof
     with open(path, "wb") as f:
         f.write(out)
+
+
+# --- writer of the version-0 layout (what the HDF5 library writes with default properties) ------
+# An independent restatement of the layout the library's native writer produces, byte for byte:
+# superblock v0 with the root symbol table entry (cache type 1), root object header v1 with a
+# symbol table message, a local heap ("" at 0, names padded to 8 bytes, empty free list = 1), one
+# group B-tree leaf node allocated at 2K = 32 children, symbol table nodes of 2K = 8 entries sorted
+# by name, dataset object headers v1 (dataspace v1, datatype v1, fill value v2, layout v3
+# contiguous), then the raw data of each dataset in header order, each padded to 8 bytes.
+
+def _pad8(n: int) -> int:
+    return (n + 7) & ~7
+
+
+def _ohdr_v1(msgs) -> bytes:
+    body = b""
+    for t, m in msgs:
+        flags = 1 if t in (0x03, 0x11) else 0
+        body += struct.pack("<HHB3x", t, _pad8(len(m)), flags) + m + bytes(_pad8(len(m)) - len(m))
+    return struct.pack("<BBHII", 1, 0, len(msgs), 1, len(body)) + bytes(4) + body
+
+
+def _dataset_msgs(a: np.ndarray, raw_addr: int) -> list:
+    space = bytes([1, a.ndim, 0, 0, 0, 0, 0, 0]) + b"".join(struct.pack("<Q", d) for d in a.shape)
+    fill = bytes([2, 2, 2, 1, 0, 0, 0, 0])
+    layout = bytes([3, 1]) + struct.pack("<QQ", raw_addr, a.nbytes)
+    return [(0x01, space), (0x03, _datatype_msg(a.dtype)), (0x05, fill), (0x08, layout)]
+
+
+def write_v0(path: str, datasets: dict) -> None:
+    """float64 / int32 datasets (little-endian), names sorted as C strcmp orders them."""
+    K_LEAF, K_INT = 4, 16
+    items = [(k, np.ascontiguousarray(v)) for k, v in datasets.items()]
+    for k, a in items:
+        assert a.dtype in (np.dtype("<f8"), np.dtype("<i4")), (k, a.dtype)
+    order = sorted(range(len(items)), key=lambda i: items[i][0].encode())
+    heap = bytearray(8)
+    name_off = {}
+    for i in order:
+        name_off[i] = len(heap)
+        nm = items[i][0].encode()
+        heap += nm + bytes(_pad8(len(nm) + 1) - len(nm))
+    nsnod = (len(items) + 2 * K_LEAF - 1) // (2 * K_LEAF)
+    snod_size = 8 + 2 * K_LEAF * 40
+    btree_size = 24 + (2 * K_INT + 1) * 8 + 2 * K_INT * 8
+    a_root = 96
+    a_heap = a_root + 40
+    a_heapdata = a_heap + 32
+    a_btree = a_heapdata + len(heap)
+    a_snod = a_btree + btree_size
+    pos = a_snod + nsnod * snod_size
+    a_oh = []
+    for k, a in items:
+        a_oh.append(pos)
+        pos += len(_ohdr_v1(_dataset_msgs(a, 0)))
+    a_raw = []
+    for k, a in items:
+        a_raw.append(pos)
+        pos += _pad8(a.nbytes)
+    eof = pos
+    out = bytearray(SIGNATURE + bytes([0, 0, 0, 0, 0, 8, 8, 0]) + struct.pack("<HHI", K_LEAF, K_INT, 0))
+    out += struct.pack("<QQQQ", 0, UNDEF, eof, UNDEF)
+    out += struct.pack("<QQII", 0, a_root, 1, 0) + struct.pack("<QQ", a_btree, a_heap)
+    assert len(out) == a_root
+    out += _ohdr_v1([(0x11, struct.pack("<QQ", a_btree, a_heap))])
+    out += b"HEAP" + bytes(4) + struct.pack("<QQQ", len(heap), 1, a_heapdata) + heap
+    bt = bytearray(b"TREE" + bytes([0, 0]) + struct.pack("<HQQ", nsnod, UNDEF, UNDEF) + struct.pack("<Q", 0))
+    for c in range(nsnod):
+        last = order[min(len(items), (c + 1) * 2 * K_LEAF) - 1]
+        bt += struct.pack("<QQ", a_snod + c * snod_size, name_off[last])
+    out += bt + bytes(btree_size - len(bt))
+    for c in range(nsnod):
+        sn = bytearray(b"SNOD" + bytes([1, 0]) + struct.pack("<H", min(len(items), (c + 1) * 2 * K_LEAF) - c * 2 * K_LEAF))
+        for i in order[c * 2 * K_LEAF:(c + 1) * 2 * K_LEAF]:
+            sn += struct.pack("<QQII", name_off[i], a_oh[i], 0, 0) + bytes(16)
+        out += sn + bytes(snod_size - len(sn))
+    for (k, a), r in zip(items, a_raw):
+        out += _ohdr_v1(_dataset_msgs(a, r))
+    for k, a in items:
+        out += a.tobytes() + bytes(_pad8(a.nbytes) - a.nbytes)
+    assert len(out) == eof
+    with open(path, "wb") as f:
+        f.write(out)

@@ -406,3 +406,24 @@ def test_allocation_failure_is_a_status_not_a_crash(tmp_path):
     with pytest.raises(ag.AfidError) as e:
         ag.write_flow_field(str(tmp_path / "o"), m, f, final=True)
     assert e.value.status == ag.AFID_E_ALLOC
+
+
+def test_native_writer_matches_the_golden_restart_set(tmp_path):
+    """tests/golden/continua/ holds a restart set written by the oracle's own version-0 writer
+    (tests/golden/make_continua_golden.py); the native writer must produce the same bytes from the
+    same arrays, and both readers must read the set back."""
+    gold = os.path.join(os.path.dirname(__file__), "golden", "continua")
+    inp = ag.parse_bou_in(bou_text(4, 3, 2, multires=1, nxmr=8, nymr=6, nzmr=4, flagsal=1, istr3r=4))
+    m = ag.continua_master(inp, 0.625)
+    f = {k: h5.read(os.path.join(gold, f"continua_{k}.h5"), "var") for k in ("vx", "vy", "vz", "temp", "pr")}
+    f["sal"] = h5.read(os.path.join(gold, "continua_sal.h5"), "var")[..., :8]
+    d = str(tmp_path / "out")
+    ag.write_flow_field(d, m, f, final=True)
+    names = sorted(os.listdir(gold))
+    assert sorted(os.listdir(d)) == names
+    for n in names:
+        assert open(os.path.join(d, n), "rb").read() == open(os.path.join(gold, n), "rb").read(), n
+    back = ag.read_flow_field(gold, m, with_sal=True)
+    assert back["time"] == 0.625
+    for k in ("vx", "vy", "vz", "temp", "pr", "sal"):
+        np.testing.assert_array_equal(back[k], f[k])
