@@ -172,11 +172,13 @@ EXPORTS = [
     "afid_gpu_dims", "afid_h5_write", "afid_h5_info", "afid_h5_read_f64", "afid_continua_master_from_input",
     "afid_write_flow_field", "afid_read_continua_master", "afid_read_flow_field", "afid_gpu_write_flow_field",
     "afid_gpu_read_flow_field", "afid_run_io", "afid_read_flow_interp", "afid_gpu_read_flow_interp",
+    "afid_write_means",
 ]
 
 
 H5_F64 = 1
 H5_I32 = 2
+H5_GROUP = 3
 H5_MAX_RANK = 4
 
 
@@ -289,6 +291,7 @@ def load_library(path: str = _LIB_PATH) -> C.CDLL:
         "afid_read_flow_interp": (i, [C.c_char_p, C.POINTER(InputT), _dp, _dp, _dp, _dp, _dp, _dp, C.POINTER(i),
                                       C.POINTER(i), _dp]),
         "afid_gpu_read_flow_interp": (i, [vp, C.c_char_p, C.POINTER(InputT), _dp, C.POINTER(i)]),
+        "afid_write_means": (i, [C.c_char_p, d, i, _dp, i, _dp, i, _dp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -795,9 +798,14 @@ class Server:
 
 
 def h5_write(path: str, datasets: dict) -> None:
-    """afid_h5_write: name -> array (float64 or int32, rank 1-4, C order)."""
+    """afid_h5_write: path -> array (float64 or int32, rank 1-4, C order), or None for a group;
+    '/' in a path nests groups."""
     keep, sets = [], (H5DatasetT * len(datasets))()
     for i, (name, a) in enumerate(datasets.items()):
+        if a is None:
+            sets[i].name = name.encode()
+            sets[i].dtype = H5_GROUP
+            continue
         a = np.ascontiguousarray(a)
         if a.dtype not in (np.float64, np.int32):
             raise TypeError(f"{name}: dtype {a.dtype}")
@@ -824,6 +832,20 @@ def h5_read(path: str, name: str) -> np.ndarray:
     out = np.empty(shape, dtype=np.float64)
     _check(lib().afid_h5_read_f64(path.encode(), name.encode(), _ptr(out), out.size), "afid_h5_read_f64")
     return out
+
+
+def write_means(directory: str, tout: float, times, profiles: np.ndarray, sal_profiles: np.ndarray = None) -> None:
+    """afid_write_means: profiles (nsamples, 15, nxm) as Solver.mean_profiles stacks them,
+    sal_profiles (nsamples, 6, nxmr) or None."""
+    times = np.ascontiguousarray(times, dtype=np.float64)
+    prof = np.ascontiguousarray(profiles, dtype=np.float64)
+    ns, nq, nxm = prof.shape
+    if nq != len(PROFILE_NAMES) or times.shape != (ns,):
+        raise ValueError("profiles must be (nsamples, 15, nxm) with one time per sample")
+    sal = None if sal_profiles is None else np.ascontiguousarray(sal_profiles, dtype=np.float64)
+    nxmr = 0 if sal is None else sal.shape[2]
+    _check(lib().afid_write_means(directory.encode(), tout, ns, _ptr(times), nxm, _ptr(prof), nxmr,
+                                  _ptr(sal) if sal is not None else None), "afid_write_means")
 
 
 def continua_master(inp: InputT, time: float = 0.0) -> ContinuaMasterT:

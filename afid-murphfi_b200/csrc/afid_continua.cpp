@@ -109,58 +109,189 @@ bool write_all(FILE *f, const void *p, size_t n) { return n == 0 || std::fwrite(
 
 }  // namespace
 
+namespace {
+
+// A group of the file being written: its members (sorted by name as C strcmp orders them) are
+// datasets (ds >= 0, index into the caller's array) or groups (ds < 0).
+struct GroupNode {
+  std::vector<std::pair<std::string, int>> members;  // name, dataset index or -1 - child group
+  std::vector<GroupNode> groups;
+  // layout
+  size_t a_oh = 0, a_heap = 0, a_heapdata = 0, heap_size = 0, a_snod = 0, nsnod = 0;
+  std::vector<uint64_t> name_off;                     // per member
+  std::vector<std::vector<size_t>> level_addr;        // B-tree node addresses per level (0 = leaves)
+  size_t a_btree_root = 0;
+};
+
+// Insert dataset `ds` (or, with ds < 0, a group) under its '/'-separated path, creating the
+// groups on the way; false on an empty component or a clash.
+bool insert_path(GroupNode &g, const char *path, int ds) {
+  const char *slash = std::strchr(path, '/');
+  const std::string head = slash ? std::string(path, slash - path) : std::string(path);
+  if (head.empty() || head.size() > 255) return false;
+  for (auto &m : g.members)
+    if (m.first == head) {
+      if (m.second >= 0) return false;           // a dataset used again, or used as a group
+      if (!slash) return ds < 0;                 // the group exists already: fine for a group entry
+      return insert_path(g.groups[(size_t)(-1 - m.second)], slash + 1, ds);
+    }
+  if (!slash && ds >= 0) {
+    g.members.emplace_back(head, ds);
+    return true;
+  }
+  g.groups.emplace_back();
+  g.members.emplace_back(head, -(int)g.groups.size());
+  return slash ? insert_path(g.groups.back(), slash + 1, ds) : true;
+}
+
+void sort_members(GroupNode &g) {
+  std::sort(g.members.begin(), g.members.end(), [](const std::pair<std::string, int> &a,
+                                                   const std::pair<std::string, int> &b) {
+    return std::strcmp(a.first.c_str(), b.first.c_str()) < 0;
+  });
+  for (auto &c : g.groups) sort_members(c);
+}
+
+// Addresses of a group's own structures: object header (symbol table message), local heap,
+// B-tree nodes (root first, then the lower levels), symbol table nodes; then its child groups.
+void place_group(GroupNode &g, size_t &a) {
+  const size_t n = g.members.size();
+  g.name_off.assign(n, 0);
+  size_t heap = 8;
+  for (size_t i = 0; i < n; ++i) {
+    g.name_off[i] = heap;
+    heap += pad8(g.members[i].first.size() + 1);
+  }
+  g.heap_size = heap;
+  g.nsnod = (n + 2 * kLeafK - 1) / (2 * kLeafK);
+  // B-tree levels: leaves over the symbol table nodes, each node up to 2K children
+  std::vector<size_t> count{std::max<size_t>(1, (g.nsnod + 2 * kInternalK - 1) / (2 * kInternalK))};
+  while (count.back() > 1) count.push_back((count.back() + 2 * kInternalK - 1) / (2 * kInternalK));
+  g.a_oh = a;
+  a += 16 + 8 + 16;
+  g.a_heap = a;
+  g.a_heapdata = a + 32;
+  a += 32 + heap;
+  g.level_addr.assign(count.size(), {});
+  for (size_t lev = count.size(); lev-- > 0;)
+    for (size_t c = 0; c < count[lev]; ++c) {
+      g.level_addr[lev].push_back(a);
+      a += kBtreeSize;
+    }
+  g.a_btree_root = g.level_addr.back()[0];
+  g.a_snod = a;
+  a += g.nsnod * kSnodSize;
+  for (auto &c : g.groups) place_group(c, a);
+}
+
+// Serialise a placed group into the image `m` (dataset object header addresses in a_ds).
+void emit_group(const GroupNode &g, Out &m, const std::vector<size_t> &a_ds) {
+  const size_t n = g.members.size();
+  {
+    auto h = object_header_v1({{0x11, le_bytes({{g.a_btree_root, 8}, {g.a_heap, 8}})}});
+    std::memcpy(&m.b[g.a_oh], h.data(), h.size());
+  }
+  std::memcpy(&m.b[g.a_heap], "HEAP", 4);
+  m.put(g.a_heap + 8, g.heap_size, 8);
+  m.put(g.a_heap + 16, 1, 8);  // empty free list
+  m.put(g.a_heap + 24, g.a_heapdata, 8);
+  for (size_t i = 0; i < n; ++i)
+    std::memcpy(&m.b[g.a_heapdata + g.name_off[i]], g.members[i].first.data(), g.members[i].first.size());
+  // symbol table nodes
+  for (size_t c = 0; c < g.nsnod; ++c) {
+    const size_t s = g.a_snod + c * kSnodSize, lo = c * 2 * kLeafK, hi = std::min(n, lo + 2 * kLeafK);
+    std::memcpy(&m.b[s], "SNOD", 4);
+    m.put(s + 4, 1, 1);
+    m.put(s + 6, hi - lo, 2);
+    for (size_t e = lo; e < hi; ++e) {
+      const size_t p = s + 8 + (e - lo) * kEntrySize;
+      const int id = g.members[e].second;
+      m.put(p, g.name_off[e], 8);
+      m.put(p + 8, id >= 0 ? a_ds[(size_t)id] : g.groups[(size_t)(-1 - id)].a_oh, 8);
+    }
+  }
+  // B-tree nodes: children of a leaf are symbol table nodes, of a level-l node the level l-1
+  // nodes; key 0 is the empty name, key c+1 the largest name under child c
+  std::vector<uint64_t> child_addr(g.nsnod), child_key(g.nsnod);
+  for (size_t c = 0; c < g.nsnod; ++c) {
+    child_addr[c] = g.a_snod + c * kSnodSize;
+    child_key[c] = g.name_off[std::min(n, (c + 1) * 2 * kLeafK) - 1];
+  }
+  for (size_t lev = 0; lev < g.level_addr.size(); ++lev) {
+    const auto &nodes = g.level_addr[lev];
+    std::vector<uint64_t> next_addr, next_key;
+    for (size_t k = 0; k < nodes.size(); ++k) {
+      const size_t b = nodes[k];
+      const size_t lo = k * 2 * kInternalK, hi = std::min(child_addr.size(), lo + 2 * kInternalK);
+      std::memcpy(&m.b[b], "TREE", 4);
+      m.put(b + 4, 0, 1);
+      m.put(b + 5, lev, 1);
+      m.put(b + 6, hi - lo, 2);
+      m.put(b + 8, k > 0 ? nodes[k - 1] : kUndef, 8);
+      m.put(b + 16, k + 1 < nodes.size() ? nodes[k + 1] : kUndef, 8);
+      size_t q = b + 24;
+      m.put(q, 0, 8);
+      q += 8;
+      for (size_t c = lo; c < hi; ++c) {
+        m.put(q, child_addr[c], 8);
+        m.put(q + 8, child_key[c], 8);
+        q += 16;
+      }
+      next_addr.push_back(b);
+      next_key.push_back(hi > lo ? child_key[hi - 1] : 0);
+    }
+    child_addr.swap(next_addr);
+    child_key.swap(next_key);
+  }
+  for (auto &c : g.groups) emit_group(c, m, a_ds);
+}
+
+}  // namespace
+
 extern "C" int afid_h5_write(const char *path, int n, const afid_h5_dataset_t *sets) {
   return afid_guard([&]() -> int {
-    if (!path || n < 1 || !sets) return AFID_E_INVALID;
-    std::vector<int> order(n);
+    if (!path || n < 0 || (n > 0 && !sets)) return AFID_E_INVALID;
+    GroupNode root;
     for (int i = 0; i < n; ++i) {
       const afid_h5_dataset_t &d = sets[i];
-      if (!d.name || !d.name[0] || std::strlen(d.name) > 255 || std::strchr(d.name, '/')) return AFID_E_INVALID;
+      if (!d.name || !d.name[0] || std::strlen(d.name) > 4095) return AFID_E_INVALID;
+      if (d.dtype == AFID_H5_GROUP) {
+        if (!insert_path(root, d.name, -1)) return AFID_E_INVALID;
+        continue;
+      }
       if (d.rank < 1 || d.rank > AFID_H5_MAX_RANK || (d.dtype != AFID_H5_F64 && d.dtype != AFID_H5_I32))
         return AFID_E_INVALID;
       for (int r = 0; r < d.rank; ++r)
         if (d.dims[r] < 0) return AFID_E_INVALID;
       if (elem_count(d) > 0 && !d.data) return AFID_E_INVALID;
-      order[i] = i;
+      if (!insert_path(root, d.name, i)) return AFID_E_INVALID;
     }
-    std::sort(order.begin(), order.end(), [&](int a, int b) { return std::strcmp(sets[a].name, sets[b].name) < 0; });
-    for (int i = 1; i < n; ++i)
-      if (std::strcmp(sets[order[i - 1]].name, sets[order[i]].name) == 0) return AFID_E_INVALID;
-    const int nsnod = (n + 2 * kLeafK - 1) / (2 * kLeafK);
-    if (nsnod > 2 * kInternalK) return AFID_E_INVALID;  // one B-tree leaf level is enough here
-
-    // local heap data: "" at 0, then each name NUL-terminated and padded to 8 bytes
-    std::vector<uint64_t> name_off(n);
-    size_t heap_data = 8;
-    for (int i = 0; i < n; ++i) {
-      name_off[order[i]] = heap_data;
-      heap_data += pad8(std::strlen(sets[order[i]].name) + 1);
-    }
-    const size_t a_super = 0, a_root = 96;
-    const size_t root_len = 16 + 8 + 16;                       // prefix + symbol table message
-    const size_t a_heap = a_root + root_len, heap_hdr = 32;
-    const size_t a_heapdata = a_heap + heap_hdr;
-    const size_t a_btree = a_heapdata + heap_data;
-    const size_t a_snod = a_btree + kBtreeSize;
-    size_t a = a_snod + nsnod * kSnodSize;
-    std::vector<size_t> a_oh(n), a_raw(n);
+    sort_members(root);
+    size_t a = 96;  // superblock
+    place_group(root, a);
+    const size_t meta_end = a;
+    std::vector<size_t> a_ds(n), a_raw(n);
     std::vector<std::vector<uint8_t>> oh(n);
+    auto is_ds = [&](int i) { return sets[i].dtype != AFID_H5_GROUP; };
     for (int i = 0; i < n; ++i) {  // headers first (their size does not depend on the raw address)
+      if (!is_ds(i)) continue;
       oh[i] = object_header_v1({{0x01, dataspace_msg(sets[i])},
                                 {0x03, datatype_msg(sets[i].dtype)},
-                                {0x05, {2, 2, 2, 1, 0, 0, 0, 0}},   // fill value v2: late, if set, defined, size 0
+                                {0x05, {2, 2, 2, 1, 0, 0, 0, 0}},  // fill value v2: late, if set, defined, size 0
                                 {0x08, std::vector<uint8_t>(18, 0)}});
-      a_oh[i] = a;
+      a_ds[i] = a;
       a += oh[i].size();
     }
     for (int i = 0; i < n; ++i) {
+      if (!is_ds(i)) continue;
       a_raw[i] = a;
       a += pad8((size_t)elem_count(sets[i]) * elem_size(sets[i].dtype));
     }
     const size_t eof = a;
-    for (int i = 0; i < n; ++i) {  // fill in the layout message: version 3, contiguous, address, size
-      const size_t lay = 16 + (8 + pad8(dataspace_msg(sets[i]).size())) + (8 + pad8(datatype_msg(sets[i].dtype).size())) +
-                         (8 + 8) + 8;
+    for (int i = 0; i < n; ++i) {  // the layout message: version 3, contiguous, address, size
+      if (!is_ds(i)) continue;
+      const size_t lay = 16 + (8 + pad8(dataspace_msg(sets[i]).size())) +
+                         (8 + pad8(datatype_msg(sets[i].dtype).size())) + (8 + 8) + 8;
       const uint64_t bytes = (uint64_t)elem_count(sets[i]) * elem_size(sets[i].dtype);
       oh[i][lay] = 3;
       oh[i][lay + 1] = 1;
@@ -170,62 +301,23 @@ extern "C" int afid_h5_write(const char *path, int n, const afid_h5_dataset_t *s
       }
     }
 
-    Out m(a_snod + nsnod * kSnodSize);
+    Out m(meta_end);
     // superblock version 0
-    std::memcpy(&m.b[a_super], kSig, 8);
-    m.put(13, 8, 1);                 // size of offsets
-    m.put(14, 8, 1);                 // size of lengths
+    std::memcpy(&m.b[0], kSig, 8);
+    m.put(13, 8, 1);  // size of offsets
+    m.put(14, 8, 1);  // size of lengths
     m.put(16, kLeafK, 2);
     m.put(18, kInternalK, 2);
-    m.put(24, 0, 8);                 // base address
-    m.put(32, kUndef, 8);            // free-space info
-    m.put(40, eof, 8);               // end of file
-    m.put(48, kUndef, 8);            // driver info
-    m.put(56, 0, 8);                 // root entry: link name offset
-    m.put(64, a_root, 8);            //   object header address
-    m.put(72, 1, 4);                 //   cache type 1: scratch holds B-tree and heap addresses
-    m.put(80, a_btree, 8);
-    m.put(88, a_heap, 8);
-    // root object header: one symbol table message
-    {
-      auto h = object_header_v1({{0x11, le_bytes({{a_btree, 8}, {a_heap, 8}})}});
-      std::memcpy(&m.b[a_root], h.data(), h.size());
-    }
-    // local heap
-    std::memcpy(&m.b[a_heap], "HEAP", 4);
-    m.put(a_heap + 8, heap_data, 8);
-    m.put(a_heap + 16, 1, 8);        // empty free list
-    m.put(a_heap + 24, a_heapdata, 8);
-    for (int i = 0; i < n; ++i) std::memcpy(&m.b[a_heapdata + name_off[i]], sets[i].name, std::strlen(sets[i].name));
-    // B-tree node (group, leaf level): keys are heap offsets of the largest name in each child
-    std::memcpy(&m.b[a_btree], "TREE", 4);
-    m.put(a_btree + 4, 0, 1);
-    m.put(a_btree + 5, 0, 1);
-    m.put(a_btree + 6, nsnod, 2);
-    m.put(a_btree + 8, kUndef, 8);
-    m.put(a_btree + 16, kUndef, 8);
-    size_t q = a_btree + 24;
-    m.put(q, 0, 8);
-    q += 8;
-    for (int c = 0; c < nsnod; ++c) {
-      const int last = std::min(n, (c + 1) * 2 * kLeafK) - 1;
-      m.put(q, a_snod + c * kSnodSize, 8);
-      m.put(q + 8, name_off[order[last]], 8);
-      q += 16;
-    }
-    // symbol table nodes
-    for (int c = 0; c < nsnod; ++c) {
-      const size_t s = a_snod + c * kSnodSize;
-      const int lo = c * 2 * kLeafK, hi = std::min(n, lo + 2 * kLeafK);
-      std::memcpy(&m.b[s], "SNOD", 4);
-      m.put(s + 4, 1, 1);
-      m.put(s + 6, hi - lo, 2);
-      for (int e = lo; e < hi; ++e) {
-        const size_t p = s + 8 + (e - lo) * kEntrySize;
-        m.put(p, name_off[order[e]], 8);
-        m.put(p + 8, a_oh[order[e]], 8);
-      }
-    }
+    m.put(24, 0, 8);        // base address
+    m.put(32, kUndef, 8);   // free-space info
+    m.put(40, eof, 8);      // end of file
+    m.put(48, kUndef, 8);   // driver info
+    m.put(56, 0, 8);        // root entry: link name offset
+    m.put(64, root.a_oh, 8);  //   object header address
+    m.put(72, 1, 4);        //   cache type 1: scratch holds B-tree and heap addresses
+    m.put(80, root.a_btree_root, 8);
+    m.put(88, root.a_heap, 8);
+    emit_group(root, m, a_ds);
 
     FILE *f = std::fopen(path, "wb");
     if (!f) return AFID_E_IO;
@@ -233,6 +325,7 @@ extern "C" int afid_h5_write(const char *path, int n, const afid_h5_dataset_t *s
     for (int i = 0; i < n && ok; ++i) ok = write_all(f, oh[i].data(), oh[i].size());
     static const uint8_t zeros[8] = {0};
     for (int i = 0; i < n && ok; ++i) {
+      if (!is_ds(i)) continue;
       const size_t bytes = (size_t)elem_count(sets[i]) * elem_size(sets[i].dtype);
       ok = write_all(f, sets[i].data, bytes) && write_all(f, zeros, pad8(bytes) - bytes);
     }
@@ -286,7 +379,22 @@ class Reader {
     return false;
   }
 
-  bool find(const char *name, uint64_t *hdr) { return lookup(root_, name, hdr, 0); }
+  // Object header of the '/'-separated path below the root group.
+  bool find(const char *name, uint64_t *hdr) {
+    uint64_t cur = root_;
+    const char *p = name;
+    for (int depth = 0; depth < 32; ++depth) {
+      const char *slash = std::strchr(p, '/');
+      const std::string comp = slash ? std::string(p, slash - p) : std::string(p);
+      if (comp.empty() || !lookup(cur, comp.c_str(), &cur, 0)) return false;
+      if (!slash) {
+        *hdr = cur;
+        return true;
+      }
+      p = slash + 1;
+    }
+    return false;
+  }
 
   bool dataset(uint64_t hdr, DsInfo &d) {
     std::vector<Msg> msgs;
@@ -414,6 +522,9 @@ class Reader {
  private:
   FILE *f_ = nullptr;
   uint64_t fsize_ = 0, base_ = 0, root_ = 0;
+  // B-tree and symbol-table nodes one lookup may visit: a damaged tree whose nodes point back at
+  // themselves would otherwise be walked an exponential number of times
+  long long node_budget_ = 0;
   int so_ = 8, sl_ = 8;
 
   uint64_t undef_addr() const { return so_ == 8 ? kUndef : ((1ull << (8 * so_)) - 1); }
@@ -536,7 +647,7 @@ class Reader {
 
   // Symbol table group: walk the B-tree of group nodes down to the symbol table nodes.
   bool btree_find(uint64_t node, uint64_t heap_data, const char *name, uint64_t *hdr, int depth) {
-    if (depth > 16) return false;
+    if (depth > 16 || --node_budget_ < 0) return false;
     std::vector<uint8_t> b;
     if (!at(node, b, 8 + 2 * (size_t)so_)) return false;
     if (std::memcmp(b.data(), "TREE", 4) != 0 || b[4] != 0) return false;
@@ -555,7 +666,7 @@ class Reader {
       if (!at(child, s, 8)) return false;
       if (std::memcmp(s.data(), "SNOD", 4) != 0) return false;
       const size_t nsym = (size_t)le(&s[6], 2), es = 2 * (size_t)so_ + 24;
-      if (nsym > 4096 || !at(child, s, 8 + nsym * es)) return false;
+      if (nsym > 4096 || (node_budget_ -= (long long)nsym + 1) < 0 || !at(child, s, 8 + nsym * es)) return false;
       for (size_t e = 0; e < nsym; ++e) {
         std::string nm;
         if (!heap_name(heap_data, le(&s[8 + e * es], so_), nm)) return false;
@@ -580,6 +691,7 @@ class Reader {
         std::vector<uint8_t> hh;
         if (!at(heap, hh, 8 + 2 * (size_t)sl_ + so_) || std::memcmp(hh.data(), "HEAP", 4) != 0) return false;
         const uint64_t heap_data = le(&hh[8 + 2 * sl_], so_);
+        node_budget_ = 1 << 20;
         return btree_find(btree, heap_data, name, hdr, 0);
       }
       if (m.type == 0x06) {  // link message (compact storage)
@@ -911,5 +1023,58 @@ extern "C" int afid_gpu_read_flow_field(afid_ctx_t *ctx, const char *dir, const 
     if (with_sal && (s = afid_gpu_sal_upload(ctx, sal.data(), dims[3], dims[4])) != AFID_OK) return s;
     if (time_out) *time_out = t;
     return AFID_OK;
+  });
+}
+
+// ---- mean profiles file ----------------------------------------------------------------------
+extern "C" int afid_write_means(const char *dir, double tout, int nsamples, const double *times, int nxm,
+                                const double *profiles, int nxmr, const double *sal_profiles) {
+  return afid_guard([&]() -> int {
+    static const char *const kNames[AFID_NUM_PROFILES] = {"Tbar",  "vybar", "vzbar", "vxT",  "vyT",
+                                                          "vzT",   "Trms",  "vxrms", "vyrms", "vzrms",
+                                                          "vxvy",  "vxvz",  "vyvz",  "chiT", "epsilon"};
+    static const char *const kSalNames[AFID_NUM_SAL_PROFILES] = {"Sbar", "Srms", "vxS", "vyS", "vzS", "chiS"};
+    if (!dir || nsamples < 0 || nxm < 1 || !(tout > 0.0)) return AFID_E_INVALID;
+    if (nsamples > 0 && (!times || !profiles)) return AFID_E_INVALID;
+    const bool sal = sal_profiles != nullptr;
+    if (sal && nxmr < 1) return AFID_E_INVALID;
+    if (!ensure_dir(dir)) return AFID_E_IO;
+    // sample names: nint(time / TOUT) as i5.5 (CalcMeanProfiles.F90:209), distinct
+    std::vector<std::string> stamp(nsamples);
+    std::vector<char> used(100000, 0);
+    for (int s = 0; s < nsamples; ++s) {
+      const double fr = std::round(times[s] / tout);
+      if (!(fr >= 0.0 && fr <= 99999.0)) return AFID_E_INVALID;
+      if (used[(size_t)fr]++) return AFID_E_INVALID;  // the reference cannot write a sample twice
+      char b[8];
+      std::snprintf(b, sizeof(b), "%05d", (int)fr);
+      stamp[s] = b;
+    }
+    const int ngroups = AFID_NUM_PROFILES + (sal ? AFID_NUM_SAL_PROFILES : 0);
+    std::vector<std::string> names;
+    names.reserve((size_t)ngroups * (nsamples + 1));
+    std::vector<afid_h5_dataset_t> sets;
+    sets.reserve(names.capacity());
+    auto add = [&](std::string name, int dtype, int64_t len, const double *data) {
+      names.push_back(std::move(name));
+      afid_h5_dataset_t d{};
+      d.dtype = dtype;
+      d.rank = 1;
+      d.dims[0] = len;
+      d.data = data;
+      sets.push_back(d);
+    };
+    for (int q = 0; q < ngroups; ++q) {  // HdfCreateMeansFile / CreateSalinityH5Groups: the groups
+      const bool sq = q >= AFID_NUM_PROFILES;
+      const char *g = sq ? kSalNames[q - AFID_NUM_PROFILES] : kNames[q];
+      add(g, AFID_H5_GROUP, 0, nullptr);
+      for (int s = 0; s < nsamples; ++s) {
+        const double *src = sq ? sal_profiles + ((size_t)s * AFID_NUM_SAL_PROFILES + (q - AFID_NUM_PROFILES)) * nxmr
+                               : profiles + ((size_t)s * AFID_NUM_PROFILES + q) * nxm;
+        add(std::string(g) + "/" + stamp[s], AFID_H5_F64, sq ? nxmr : nxm, src);
+      }
+    }
+    for (size_t i = 0; i < sets.size(); ++i) sets[i].name = names[i].c_str();
+    return afid_h5_write((std::string(dir) + "/means.h5").c_str(), (int)sets.size(), sets.data());
   });
 }

@@ -17,6 +17,7 @@
  *                                interpolated (InterpInputVel.F90, InterpInputSal.F90)
  *   afid_gpu_write_flow_field /  the same through a device context: download, write / read,
  *   afid_gpu_read_flow_field     upload (salinity included when the context has it)
+ *   afid_write_means             the mean-profile file means.h5 (CalcMeanProfiles.F90:209-334)
  *   afid_run_io                  afid_run plus the main loop's restart and save points:
  *                                ReadFlowInterp (either branch) when NREAD = 1 (main.F90:157-161), the start-up
  *                                frame (main.F90:241), the SAVE_3D frames (main.F90:376-381) and
@@ -34,8 +35,8 @@
  * extra x node (nxmr + 1) is written as zero and dropped on reading.
  *
  * The container (afid_h5_*) is the subset of the HDF5 file format these files need: superblock
- * version 0, version-1 object headers, a symbol-table root group, fixed-point and floating-point
- * datasets with contiguous storage.  The reader also takes superblock versions 1-3, version-2
+ * version 0, version-1 object headers, symbol-table groups (nested, any number of members),
+ * fixed-point and floating-point datasets with contiguous storage.  The reader also takes superblock versions 1-3, version-2
  * object headers, compact link-message groups and compact storage; chunked storage, filters and
  * dense link storage are refused with AFID_E_IO.
  */
@@ -54,17 +55,21 @@ extern "C" {
 /* ---- the container ------------------------------------------------------------------------ */
 #define AFID_H5_F64 1          /* IEEE binary64, little-endian on disk                       */
 #define AFID_H5_I32 2          /* two's-complement 32-bit, little-endian on disk              */
+#define AFID_H5_GROUP 3        /* an entry that only creates the (possibly empty) group `name` */
 #define AFID_H5_MAX_RANK 4
 
 typedef struct afid_h5_dataset {
-  const char *name;            /* at most 255 bytes, no '/'                                    */
-  int dtype;                   /* AFID_H5_F64 / AFID_H5_I32                                    */
+  const char *name;            /* path below the root group: components of at most 255 bytes
+                                  separated by '/'; the groups on the way are created         */
+  int dtype;                   /* AFID_H5_F64 / AFID_H5_I32, or AFID_H5_GROUP (rank, dims and
+                                  data ignored)                                               */
   int rank;                    /* 1 .. AFID_H5_MAX_RANK                                        */
   int64_t dims[AFID_H5_MAX_RANK];   /* C order: dims[rank - 1] varies fastest                  */
   const void *data;            /* prod(dims) host values of the type                           */
 } afid_h5_dataset_t;
 
-/* Create (truncate) path holding the n datasets in its root group. */
+/* Create (truncate) path holding the n datasets (and groups).  Groups are symbol-table groups
+ * whose B-trees grow extra levels as needed (more than 256 members per group are fine). */
 int afid_h5_write(const char *path, int n, const afid_h5_dataset_t *sets);
 /* Class and shape of one dataset: *dtype is AFID_H5_F64 for any floating-point type and
  * AFID_H5_I32 for any integer type.  AFID_E_IO if the file or dataset is missing or unsupported. */
@@ -110,6 +115,19 @@ int afid_read_flow_field(const char *dir, const afid_continua_master_t *cur, dou
  * 2-D file restarts a 2-D run only. */
 int afid_read_flow_interp(const char *dir, const afid_input_t *in, double *time_out, double *vx, double *vy,
                           double *vz, double *temp, double *pr, int *pr_read, int *interpolated, double *sal);
+
+/* ---- mean profiles file ------------------------------------------------------------------ */
+/* <dir>/means.h5 as CalcMeanProfiles.F90:209-270 (HdfCreateMeansFile :289-334) and
+ * CalcSalStats / CreateSalinityH5Groups (salinity.F90:592-603, :704-714) lay it out: one group per
+ * profile (Tbar, vybar, vzbar, vxT, vyT, vzT, Trms, vxrms, vyrms, vzrms, vxvy, vxvz, vyvz, chiT,
+ * epsilon; with salinity also Sbar, Srms, vxS, vyS, vzS, chiS), holding one dataset of nxm (nxmr)
+ * doubles per sample, named NNNNN = nint(time / TOUT).  profiles[s][q][k] is sample s as
+ * afid_gpu_mean_profiles returns it; sal_profiles[s][q][k] as afid_gpu_sal_profiles (NULL: no
+ * salinity groups).  The reference appends each sample to the file as it is taken; this call
+ * writes the whole file from the samples given (nsamples = 0: the empty groups).  Two samples
+ * with the same NNNNN are refused (AFID_E_INVALID), as the reference cannot create a dataset twice. */
+int afid_write_means(const char *dir, double tout, int nsamples, const double *times, int nxm,
+                     const double *profiles, int nxmr, const double *sal_profiles);
 
 /* Device context variants (salinity included when afid_gpu_sal_create was called). */
 int afid_gpu_write_flow_field(afid_ctx_t *ctx, const char *dir, int final, double save_3d,

@@ -123,9 +123,11 @@ def test_reader_refuses_damaged_files(tmp_path):
     with pytest.raises(ag.AfidError) as e:
         ag.h5_read(str(tmp_path / "missing.h5"), "var")
     assert e.value.status == ag.AFID_E_IO
-    with pytest.raises(ag.AfidError) as e:
-        ag.h5_write(str(tmp_path / "dup.h5"), {"a/b": np.zeros(2)})
-    assert e.value.status == ag.AFID_E_INVALID
+    for bad in ({"a//b": np.zeros(2)}, {"/a": np.zeros(2)}, {"a/": np.zeros(2)},
+                {"a": np.zeros(2), "a/b": np.zeros(2)}):   # empty path components; a dataset used as a group
+        with pytest.raises(ag.AfidError) as e:
+            ag.h5_write(str(tmp_path / "bad.h5"), bad)
+        assert e.value.status == ag.AFID_E_INVALID
 
 
 def _input(**kw):
@@ -427,3 +429,59 @@ def test_native_writer_matches_the_golden_restart_set(tmp_path):
     assert back["time"] == 0.625
     for k in ("vx", "vy", "vz", "temp", "pr", "sal"):
         np.testing.assert_array_equal(back[k], f[k])
+
+
+def test_nested_groups_and_large_groups(tmp_path):
+    """Groups nest through '/' paths; an empty group is an entry of its own; a group of 600
+    members needs a two-level group B-tree (75 symbol table nodes over three leaf nodes).  The
+    oracle reader and the native reader both find every dataset."""
+    rng = np.random.default_rng(16)
+    d = {f"big/{k:05d}": rng.standard_normal(3) for k in range(600)}
+    d.update({"g/a": np.arange(4, dtype=np.int32), "g/b/c": rng.standard_normal((2, 3)), "empty": None,
+              "top": np.array([2.5])})
+    path = str(tmp_path / "nested.h5")
+    ag.h5_write(path, d)
+    f = h5.H5File(path)
+    assert sorted(f.root()) == ["big", "empty", "g", "top"]
+    assert f.is_group("empty") and f.links(f.resolve("empty")) == {}
+    assert sorted(f.links(f.resolve("g"))) == ["a", "b"]
+    btree = [int.from_bytes(b[:8], "little") for t, _, b in f.messages(f.resolve("big")) if t == 0x11][0]
+    assert f.buf[f._abs(btree) + 5] == 1                       # root node one level above the leaves
+    assert len(f.links(f.resolve("big"))) == 600
+    for k, v in d.items():
+        if v is None:
+            continue
+        np.testing.assert_array_equal(f.read(k), v)
+        np.testing.assert_array_equal(ag.h5_read(path, k), v.astype(np.float64))
+    with pytest.raises(ag.AfidError) as e:
+        ag.h5_read(path, "g")                                    # a group is not a dataset
+    assert e.value.status == ag.AFID_E_IO
+
+
+def test_means_file_layout(tmp_path):
+    """means.h5 as CalcMeanProfiles / CalcSalStats lay it out: one group per profile, one dataset
+    per sample named nint(time / TOUT) as five digits."""
+    rng = np.random.default_rng(17)
+    times = np.array([0.5, 1.0, 1.5000000001])
+    prof = rng.standard_normal((3, 15, 16))
+    sal = rng.standard_normal((3, 6, 24))
+    d = str(tmp_path / "outputdir")
+    ag.write_means(d, 0.5, times, prof, sal)
+    p = os.path.join(d, "means.h5")
+    groups = list(ag.PROFILE_NAMES) + list(ag.SAL_PROFILE_NAMES)
+    assert sorted(h5.names(p)) == sorted(groups)
+    f = h5.H5File(p)
+    for q, g in enumerate(groups):
+        assert sorted(f.links(f.resolve(g))) == ["00001", "00002", "00003"], g
+        for s in range(3):
+            want = prof[s, q] if q < 15 else sal[s, q - 15]
+            np.testing.assert_array_equal(f.read(f"{g}/{s + 1:05d}"), want)
+            np.testing.assert_array_equal(ag.h5_read(p, f"{g}/{s + 1:05d}"), want)
+    # no samples yet: the empty groups HdfCreateMeansFile makes
+    ag.write_means(str(tmp_path / "empty"), 0.5, np.zeros(0), np.zeros((0, 15, 16)))
+    f0 = h5.H5File(str(tmp_path / "empty" / "means.h5"))
+    assert sorted(f0.root()) == sorted(ag.PROFILE_NAMES)
+    assert all(f0.links(f0.resolve(g)) == {} for g in ag.PROFILE_NAMES)
+    with pytest.raises(ag.AfidError) as e:   # two samples with the same NNNNN
+        ag.write_means(d, 0.5, np.array([0.5, 0.52]), prof[:2])
+    assert e.value.status == ag.AFID_E_INVALID
