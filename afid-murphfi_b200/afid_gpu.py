@@ -172,7 +172,7 @@ EXPORTS = [
     "afid_gpu_dims", "afid_h5_write", "afid_h5_info", "afid_h5_read_f64", "afid_continua_master_from_input",
     "afid_write_flow_field", "afid_read_continua_master", "afid_read_flow_field", "afid_gpu_write_flow_field",
     "afid_gpu_read_flow_field", "afid_run_io", "afid_read_flow_interp", "afid_gpu_read_flow_interp",
-    "afid_write_means",
+    "afid_write_means", "afid_write_movie",
 ]
 
 
@@ -292,6 +292,7 @@ def load_library(path: str = _LIB_PATH) -> C.CDLL:
                                       C.POINTER(i), _dp]),
         "afid_gpu_read_flow_interp": (i, [vp, C.c_char_p, C.POINTER(InputT), _dp, C.POINTER(i)]),
         "afid_write_means": (i, [C.c_char_p, d, i, _dp, i, _dp, i, _dp]),
+        "afid_write_movie": (i, [C.c_char_p, i, d, i, _dp, i, i, i, _dp, i, i, i, _dp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -846,6 +847,17 @@ def write_means(directory: str, tout: float, times, profiles: np.ndarray, sal_pr
     nxmr = 0 if sal is None else sal.shape[2]
     _check(lib().afid_write_means(directory.encode(), tout, ns, _ptr(times), nxm, _ptr(prof), nxmr,
                                   _ptr(sal) if sal is not None else None), "afid_write_means")
+
+
+def write_movie(directory: str, axis: int, tframe: float, times, planes: np.ndarray, nxm: int, nym: int,
+                nzm: int, sal_planes: np.ndarray = None, refined: tuple = (0, 0, 0)) -> None:
+    """afid_write_movie: planes (nframes, 4, rows, cols) in Solver.slice's layout for the axis,
+    sal_planes (nframes, rows_r, cols_r) or None with refined = (nxmr, nymr, nzmr)."""
+    times = np.ascontiguousarray(times, dtype=np.float64)
+    pl = np.ascontiguousarray(planes, dtype=np.float64)
+    sal = None if sal_planes is None else np.ascontiguousarray(sal_planes, dtype=np.float64)
+    _check(lib().afid_write_movie(directory.encode(), axis, tframe, times.size, _ptr(times), nxm, nym, nzm,
+                                  _ptr(pl), *refined, _ptr(sal) if sal is not None else None), "afid_write_movie")
 
 
 def continua_master(inp: InputT, time: float = 0.0) -> ContinuaMasterT:

@@ -1078,3 +1078,78 @@ extern "C" int afid_write_means(const char *dir, double tout, int nsamples, cons
     return afid_h5_write((std::string(dir) + "/means.h5").c_str(), (int)sets.size(), sets.data());
   });
 }
+
+// ---- movie planes --------------------------------------------------------------------------
+extern "C" int afid_write_movie(const char *dir, int axis, double tframe, int nframes, const double *times,
+                                int nxm, int nym, int nzm, const double *planes, int nxmr, int nymr, int nzmr,
+                                const double *sal_planes) {
+  return afid_guard([&]() -> int {
+    static const char *const kVars[4] = {"vx", "vy", "vz", "temp"};
+    static const char *const kFile[3] = {"movie_xcut.h5", "movie_ycut.h5", "movie_zcut.h5"};
+    if (!dir || axis < 0 || axis > 2 || nframes < 0 || !(tframe > 0.0) || nxm < 1 || nym < 1 || nzm < 1)
+      return AFID_E_INVALID;
+    if (nframes > 0 && (!times || !planes)) return AFID_E_INVALID;
+    const bool sal = sal_planes != nullptr;
+    if (sal && (nxmr < 1 || nymr < 1 || nzmr < 1)) return AFID_E_INVALID;
+    const int nx = nxm + 1;
+    // a plane as afid_gpu_slice returns it: (rows, cols) with cols the fastest index
+    const int rows = axis == 2 ? nym : nzm, cols = axis == 0 ? nym : nx;
+    const size_t plane = (size_t)rows * cols;
+    const int rrows = axis == 2 ? nymr : nzmr, rcols = axis == 0 ? nymr : nxmr;
+    const size_t rplane = (size_t)rrows * rcols;
+    std::string d = dir;
+    if (!ensure_dir(d) || !ensure_dir(d + "/flowmov")) return AFID_E_IO;
+    // frame numbers nint(time / TFRAME); a later frame with the same number replaces the earlier
+    // one, as the reference deletes an existing dataset before writing it (h5_tools.F90:117-118)
+    std::vector<int> frame(nframes), keep;
+    std::vector<int> last(100000, -1);
+    for (int f = 0; f < nframes; ++f) {
+      const double fr = std::round(times[f] / tframe);
+      if (!(fr >= 0.0 && fr <= 99999.0)) return AFID_E_INVALID;
+      frame[f] = (int)fr;
+      last[(size_t)fr] = f;
+    }
+    for (int f = 0; f < nframes; ++f)
+      if (last[(size_t)frame[f]] == f) keep.push_back(f);
+    // the files hold nxm rows of the cell-centred fields in the y and z cuts (nx for vx)
+    std::vector<std::vector<double>> trimmed;
+    trimmed.reserve(keep.size() * 3);
+    std::vector<std::string> names;
+    std::vector<afid_h5_dataset_t> sets;
+    const int ngroups = 4 + (sal ? 1 : 0);
+    names.reserve((size_t)ngroups * (keep.size() + 1));
+    sets.reserve(names.capacity());
+    auto add = [&](std::string name, int dtype, int64_t d0, int64_t d1, const double *data) {
+      names.push_back(std::move(name));
+      afid_h5_dataset_t e{};
+      e.dtype = dtype;
+      e.rank = 2;
+      e.dims[0] = d0;
+      e.dims[1] = d1;
+      e.data = data;
+      sets.push_back(e);
+    };
+    for (int v = 0; v < ngroups; ++v) {  // h5_add_slice_groups
+      const char *g = v < 4 ? kVars[v] : "sal";
+      add(g, AFID_H5_GROUP, 0, 0, nullptr);
+      for (int f : keep) {
+        char b[8];
+        std::snprintf(b, sizeof(b), "%05d", frame[f]);
+        const std::string name = std::string(g) + "/" + b;
+        if (v == 4) {
+          add(name, AFID_H5_F64, rrows, rcols, sal_planes + (size_t)f * rplane);
+        } else if (axis == 0 || v == 0) {
+          add(name, AFID_H5_F64, rows, cols, planes + ((size_t)f * 4 + v) * plane);
+        } else {  // vy, vz, temp of the y and z cuts: rows of nxm
+          const double *src = planes + ((size_t)f * 4 + v) * plane;
+          trimmed.emplace_back((size_t)rows * nxm);
+          for (int r = 0; r < rows; ++r)
+            std::memcpy(&trimmed.back()[(size_t)r * nxm], src + (size_t)r * cols, sizeof(double) * nxm);
+          add(name, AFID_H5_F64, rows, nxm, trimmed.back().data());
+        }
+      }
+    }
+    for (size_t i = 0; i < sets.size(); ++i) sets[i].name = names[i].c_str();
+    return afid_h5_write((d + "/flowmov/" + kFile[axis]).c_str(), (int)sets.size(), sets.data());
+  });
+}

@@ -18,6 +18,7 @@
  *   afid_gpu_write_flow_field /  the same through a device context: download, write / read,
  *   afid_gpu_read_flow_field     upload (salinity included when the context has it)
  *   afid_write_means             the mean-profile file means.h5 (CalcMeanProfiles.F90:209-334)
+ *   afid_write_movie             the movie-plane files flowmov/movie_{x,y,z}cut.h5 (MakeMovie*Cut.F90)
  *   afid_run_io                  afid_run plus the main loop's restart and save points:
  *                                ReadFlowInterp (either branch) when NREAD = 1 (main.F90:157-161), the start-up
  *                                frame (main.F90:241), the SAVE_3D frames (main.F90:376-381) and
@@ -128,6 +129,20 @@ int afid_read_flow_interp(const char *dir, const afid_input_t *in, double *time_
  * with the same NNNNN are refused (AFID_E_INVALID), as the reference cannot create a dataset twice. */
 int afid_write_means(const char *dir, double tout, int nsamples, const double *times, int nxm,
                      const double *profiles, int nxmr, const double *sal_profiles);
+
+/* ---- movie planes ------------------------------------------------------------------------ */
+/* <dir>/flowmov/movie_{x,y,z}cut.h5 (axis 0, 1, 2) as h5tools/MakeMovie{X,Y,Z}Cut.F90 and
+ * h5tools/h5_tools.F90:33-135 lay them out: groups vx, vy, vz, temp (and sal), one 2-D dataset
+ * per frame named NNNNN = nint(time / TFRAME).  planes[f][4][...] holds, per frame, the four planes
+ * in afid_gpu_slice's layout for the axis (x: nzm x nym; y: nzm x nx; z: nym x nx; the y and z
+ * cuts of vy, vz, temp are stored with their nxm cell rows, as the reference writes them);
+ * sal_planes[f][...] the refined salinity planes (x: nzmr x nymr; y: nzmr x nxmr; z: nymr x nxmr)
+ * or NULL.  The reference cuts at x index 1 (vx: 2), y index nym/2 + 1 and z index nzm/2 + 1
+ * (1-based).  A later frame with the same number replaces an earlier one, as the reference
+ * deletes and rewrites an existing dataset.  The whole file is written from the frames given. */
+int afid_write_movie(const char *dir, int axis, double tframe, int nframes, const double *times, int nxm,
+                     int nym, int nzm, const double *planes, int nxmr, int nymr, int nzmr,
+                     const double *sal_planes);
 
 /* Device context variants (salinity included when afid_gpu_sal_create was called). */
 int afid_gpu_write_flow_field(afid_ctx_t *ctx, const char *dir, int final, double save_3d,

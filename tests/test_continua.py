@@ -485,3 +485,35 @@ def test_means_file_layout(tmp_path):
     with pytest.raises(ag.AfidError) as e:   # two samples with the same NNNNN
         ag.write_means(d, 0.5, np.array([0.5, 0.52]), prof[:2])
     assert e.value.status == ag.AFID_E_INVALID
+
+
+@pytest.mark.parametrize("axis", [0, 1, 2])
+def test_movie_file_layout(tmp_path, axis):
+    """flowmov/movie_{x,y,z}cut.h5 as MakeMovie*Cut.F90 / h5_tools.F90 lay them out: groups vx, vy,
+    vz, temp, sal; one plane per frame named nint(time / TFRAME); the y and z cuts keep nx rows for
+    vx and nxm for the cell-centred fields; a later frame with the same number replaces the
+    earlier one."""
+    rng = np.random.default_rng(18 + axis)
+    nxm, nym, nzm, nxmr, nymr, nzmr = 6, 8, 4, 12, 16, 8
+    nx = nxm + 1
+    rows, cols = [(nzm, nym), (nzm, nx), (nym, nx)][axis]
+    rrows, rcols = [(nzmr, nymr), (nzmr, nxmr), (nymr, nxmr)][axis]
+    times = np.array([0.1, 0.2, 0.2 + 1e-9, 0.4])          # frames 1, 2, 2 (replaces), 4
+    planes = rng.standard_normal((4, 4, rows, cols))
+    sal = rng.standard_normal((4, rrows, rcols))
+    d = str(tmp_path / "outputdir")
+    ag.write_movie(d, axis, 0.1, times, planes, nxm, nym, nzm, sal, (nxmr, nymr, nzmr))
+    p = os.path.join(d, "flowmov", ["movie_xcut.h5", "movie_ycut.h5", "movie_zcut.h5"][axis])
+    f = h5.H5File(p)
+    assert sorted(f.root()) == sorted(["vx", "vy", "vz", "temp", "sal"])
+    for v, g in enumerate(("vx", "vy", "vz", "temp", "sal")):
+        assert sorted(f.links(f.resolve(g))) == ["00001", "00002", "00004"], g
+        for frame, src in (("00001", 0), ("00002", 2), ("00004", 3)):
+            got = f.read(f"{g}/{frame}")
+            if g == "sal":
+                want = sal[src]
+            elif axis == 0 or g == "vx":
+                want = planes[src, v]
+            else:
+                want = planes[src, v][:, :nxm]
+            np.testing.assert_array_equal(got, want)
