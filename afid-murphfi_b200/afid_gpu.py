@@ -172,7 +172,7 @@ EXPORTS = [
     "afid_gpu_dims", "afid_h5_write", "afid_h5_info", "afid_h5_read_f64", "afid_continua_master_from_input",
     "afid_write_flow_field", "afid_read_continua_master", "afid_read_flow_field", "afid_gpu_write_flow_field",
     "afid_gpu_read_flow_field", "afid_run_io", "afid_read_flow_interp", "afid_gpu_read_flow_interp",
-    "afid_write_means", "afid_write_movie",
+    "afid_write_means", "afid_write_movie", "afid_write_grid_info",
 ]
 
 
@@ -293,6 +293,7 @@ def load_library(path: str = _LIB_PATH) -> C.CDLL:
         "afid_gpu_read_flow_interp": (i, [vp, C.c_char_p, C.POINTER(InputT), _dp, C.POINTER(i)]),
         "afid_write_means": (i, [C.c_char_p, d, i, _dp, i, _dp, i, _dp]),
         "afid_write_movie": (i, [C.c_char_p, i, d, i, _dp, i, i, i, _dp, i, i, i, _dp]),
+        "afid_write_grid_info": (i, [C.c_char_p, vp, vp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -833,6 +834,12 @@ def h5_read(path: str, name: str) -> np.ndarray:
     out = np.empty(shape, dtype=np.float64)
     _check(lib().afid_h5_read_f64(path.encode(), name.encode(), _ptr(out), out.size), "afid_h5_read_f64")
     return out
+
+
+def write_grid_info(directory: str, tables: "Tables", mgrd: "Mgrd" = None) -> None:
+    """afid_write_grid_info: cordin_info.h5 of the grid (and the refined grid)."""
+    _check(lib().afid_write_grid_info(directory.encode(), tables._h, mgrd._h if mgrd is not None else None),
+           "afid_write_grid_info")
 
 
 def write_means(directory: str, tout: float, times, profiles: np.ndarray, sal_profiles: np.ndarray = None) -> None:

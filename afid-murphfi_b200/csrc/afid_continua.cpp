@@ -1153,3 +1153,43 @@ extern "C" int afid_write_movie(const char *dir, int axis, double tframe, int nf
     return afid_h5_write((d + "/flowmov/" + kFile[axis]).c_str(), (int)sets.size(), sets.data());
   });
 }
+
+// ---- grid coordinates ----------------------------------------------------------------------
+extern "C" int afid_write_grid_info(const char *dir, const afid_tables_t *t, const afid_mgrd_t *m) {
+  return afid_guard([&]() -> int {
+    if (!dir || !t) return AFID_E_INVALID;
+    const afid_grid_t *g = afid_tables_grid(t);
+    if (!g) return AFID_E_INVALID;
+    const int nxm = g->nxm, nym = g->nym, nzm = g->nzm;
+    struct Item {
+      const char *name;
+      const char *table;
+      int count;
+      bool refined;
+    };
+    std::vector<Item> items = {{"xm", "xm", nxm, false}, {"xc", "xc", nxm + 1, false},
+                               {"ym", "ym", nym, false}, {"zm", "zm", nzm, false}};
+    if (m) {
+      const afid_sal_grid_t *v = afid_mgrd_view(m);
+      items.push_back({"xmr", "xmr", v->nxmr, true});
+      items.push_back({"xcr", "xcr", v->nxmr + 1, true});
+      items.push_back({"ymr", "ymr", v->nymr, true});
+      items.push_back({"zmr", "zmr", v->nzmr, true});
+    }
+    std::vector<afid_h5_dataset_t> sets;
+    for (const Item &it : items) {
+      int len = 0;
+      const double *a = it.refined ? afid_mgrd_array(m, it.table, &len) : afid_tables_array(t, it.table, &len);
+      if (!a || len < it.count) return AFID_E_INVALID;
+      afid_h5_dataset_t d{};
+      d.name = it.name;
+      d.dtype = AFID_H5_F64;
+      d.rank = 1;
+      d.dims[0] = it.count;
+      d.data = a;
+      sets.push_back(d);
+    }
+    if (!ensure_dir(dir)) return AFID_E_IO;
+    return afid_h5_write((std::string(dir) + "/cordin_info.h5").c_str(), (int)sets.size(), sets.data());
+  });
+}

@@ -17,6 +17,7 @@
  *                                interpolated (InterpInputVel.F90, InterpInputSal.F90)
  *   afid_gpu_write_flow_field /  the same through a device context: download, write / read,
  *   afid_gpu_read_flow_field     upload (salinity included when the context has it)
+ *   afid_write_grid_info         the coordinates file cordin_info.h5 (WriteGridInfo.F90)
  *   afid_write_means             the mean-profile file means.h5 (CalcMeanProfiles.F90:209-334)
  *   afid_write_movie             the movie-plane files flowmov/movie_{x,y,z}cut.h5 (MakeMovie*Cut.F90)
  *   afid_run_io                  afid_run plus the main loop's restart and save points:
@@ -48,6 +49,7 @@
 
 #include "afid_gpu.h"
 #include "afid_host.h"
+#include "afid_salinity.h"
 
 #ifdef __cplusplus
 extern "C" {
@@ -129,6 +131,12 @@ int afid_read_flow_interp(const char *dir, const afid_input_t *in, double *time_
  * with the same NNNNN are refused (AFID_E_INVALID), as the reference cannot create a dataset twice. */
 int afid_write_means(const char *dir, double tout, int nsamples, const double *times, int nxm,
                      const double *profiles, int nxmr, const double *sal_profiles);
+
+/* ---- grid coordinates --------------------------------------------------------------------- */
+/* <dir>/cordin_info.h5 as WriteGridInfo.F90:20-45 writes it: xm (nxm), xc (nx), ym (nym), zm
+ * (nzm) of the grid in t and, when m is given (MULTIRES), xmr (nxmr), xcr (nxmr + 1), ymr (nymr),
+ * zmr (nzmr) of the refined grid; the post-processing reads the coordinates from here. */
+int afid_write_grid_info(const char *dir, const afid_tables_t *t, const afid_mgrd_t *m);
 
 /* ---- movie planes ------------------------------------------------------------------------ */
 /* <dir>/flowmov/movie_{x,y,z}cut.h5 (axis 0, 1, 2) as h5tools/MakeMovie{X,Y,Z}Cut.F90 and

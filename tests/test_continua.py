@@ -517,3 +517,23 @@ def test_movie_file_layout(tmp_path, axis):
             else:
                 want = planes[src, v][:, :nxm]
             np.testing.assert_array_equal(got, want)
+
+
+def test_grid_info_file(tmp_path):
+    """cordin_info.h5 as WriteGridInfo.F90 writes it, against the oracle's grids."""
+    text = bou_text(16, 12, 8, multires=1, nxmr=24, nymr=18, nzmr=16, flagsal=1, istr3r=4)
+    tables = ag.Tables(ag.parse_bou_in(text))
+    mgrd = ag.Mgrd(tables)
+    d = str(tmp_path / "outputdir")
+    ag.write_grid_info(d, tables, mgrd)
+    g = o.create_grid(o.parse_bou_in(text))
+    m = sa.create_mgrd(g)
+    p = os.path.join(d, "cordin_info.h5")
+    assert sorted(h5.names(p)) == sorted(["xm", "xc", "ym", "zm", "xmr", "xcr", "ymr", "zmr"])
+    want = dict(xm=g.xm[:16], xc=g.xc[:17], ym=g.ym, zm=g.zm, xmr=m.xmr[1:25], xcr=m.xcr, ymr=m.ymr, zmr=m.zmr)
+    for k, v in want.items():
+        got = h5.read(p, k)
+        assert got.shape == v.shape, k
+        np.testing.assert_allclose(got, v, rtol=0, atol=1e-15, err_msg=k)
+    ag.write_grid_info(str(tmp_path / "flat"), ag.Tables(ag.parse_bou_in(bou_text(16, 12, 8))))
+    assert sorted(h5.names(str(tmp_path / "flat" / "cordin_info.h5"))) == ["xc", "xm", "ym", "zm"]
