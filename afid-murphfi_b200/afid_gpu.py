@@ -867,6 +867,69 @@ def write_movie(directory: str, axis: int, tframe: float, times, planes: np.ndar
                                   _ptr(pl), *refined, _ptr(sal) if sal is not None else None), "afid_write_movie")
 
 
+class Recorder:
+    """The outputs the reference's main loop writes besides the restart files, for a run driven
+    from Python: cordin_info.h5 at construction (WriteGridInfo), a mean-profile sample per
+    ``profiles(time)`` call (CalcMeanProfiles / CalcSalStats at TOUT), the three movie cuts per
+    ``frame(time)`` call (Mkmov_xcut / Mkmov_ycut / Mkmov_zcut at TFRAME), and ``flush()`` writing
+    means.h5 and flowmov/movie_{x,y,z}cut.h5 from everything sampled so far.
+
+    The cuts sit where the reference puts them (0-based here): x at index 0 (vx at 1; index
+    nxm/2 - 1, vx max(nxm/2, 2) - 1, when RAYS and RAYT are both negative), y at nym/2, z at nzm/2;
+    the refined salinity likewise on its own grid, cut on the host from a download of the field."""
+
+    def __init__(self, solver, inp: InputT, directory: str, tables: "Tables", mgrd: "Mgrd" = None):
+        self.solver, self.inp, self.dir, self.sal = solver, inp, directory, mgrd is not None
+        write_grid_info(directory, tables, mgrd)
+        self.ptimes, self.prof, self.salprof = [], [], []
+        self.ftimes, self.planes, self.salplanes = [], {0: [], 1: [], 2: []}, {0: [], 1: [], 2: []}
+        both_neg = inp.rays < 0 and inp.rayt < 0
+        ic = inp.nxm // 2 if both_neg else 1                      # 1-based, MakeMovieXCut.F90
+        self.xcut = (max(ic, 2) - 1, ic - 1)                       # (vx, the others)
+        self.ycut, self.zcut = inp.nym // 2, inp.nzm // 2         # nym/2 + 1, nzm/2 + 1 (1-based)
+        if self.sal:
+            icr = inp.nxmr // 2 if both_neg else 1
+            self.salcut = (icr - 1, inp.nymr // 2, inp.nzmr // 2)
+
+    def profiles(self, time: float) -> None:
+        p = self.solver.mean_profiles()
+        self.ptimes.append(time)
+        self.prof.append(np.stack([p[n] for n in PROFILE_NAMES]))
+        if self.sal:
+            q = self.solver.sal_profiles()
+            self.salprof.append(np.stack([q[n] for n in SAL_PROFILE_NAMES]))
+
+    def frame(self, time: float) -> None:
+        self.ftimes.append(time)
+        for axis in (0, 1, 2):
+            planes = []
+            for which in range(4):
+                idx = (self.xcut[0] if which == 0 else self.xcut[1]) if axis == 0 else \
+                    (self.ycut if axis == 1 else self.zcut)
+                planes.append(self.solver.slice(which, axis, idx))
+            self.planes[axis].append(np.stack(planes))
+        if self.sal:
+            sal = self.solver.sal_download()                       # (nzmr, nymr, nxmr)
+            ix, iy, iz = self.salcut
+            self.salplanes[0].append(np.ascontiguousarray(sal[:, :, ix]))
+            self.salplanes[1].append(np.ascontiguousarray(sal[:, iy, :]))
+            self.salplanes[2].append(np.ascontiguousarray(sal[iz, :, :]))
+
+    def flush(self) -> None:
+        inp = self.inp
+        nxm = inp.nxm
+        prof = np.stack(self.prof) if self.prof else np.zeros((0, len(PROFILE_NAMES), nxm))
+        salprof = (np.stack(self.salprof) if self.salprof else np.zeros((0, 6, inp.nxmr))) if self.sal else None
+        write_means(self.dir, inp.tout, np.array(self.ptimes, dtype=np.float64), prof, salprof)
+        if not self.ftimes:
+            return
+        refined = (inp.nxmr, inp.nymr, inp.nzmr) if self.sal else (0, 0, 0)
+        for axis in (0, 1, 2):
+            sp = np.stack(self.salplanes[axis]) if self.sal else None
+            write_movie(self.dir, axis, inp.tframe, np.array(self.ftimes, dtype=np.float64),
+                        np.stack(self.planes[axis]), nxm, inp.nym, inp.nzm, sp, refined)
+
+
 def continua_master(inp: InputT, time: float = 0.0) -> ContinuaMasterT:
     m = ContinuaMasterT()
     _check(lib().afid_continua_master_from_input(C.byref(inp), time, C.byref(m)), "afid_continua_master_from_input")

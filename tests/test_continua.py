@@ -537,3 +537,65 @@ def test_grid_info_file(tmp_path):
         np.testing.assert_allclose(got, v, rtol=0, atol=1e-15, err_msg=k)
     ag.write_grid_info(str(tmp_path / "flat"), ag.Tables(ag.parse_bou_in(bou_text(16, 12, 8))))
     assert sorted(h5.names(str(tmp_path / "flat" / "cordin_info.h5"))) == ["xc", "xm", "ym", "zm"]
+
+
+class _FakeSolver:
+    """Stands in for ag.Solver on the CPU: every array it returns encodes what was asked for."""
+
+    def __init__(self, nxm, nym, nzm, refined=None):
+        self.nxm, self.nym, self.nzm, self.nx = nxm, nym, nzm, nxm + 1
+        self.refined = refined
+        self.calls = 0
+
+    def mean_profiles(self):
+        self.calls += 1
+        return {n: np.full(self.nxm, 100.0 * self.calls + q) for q, n in enumerate(ag.PROFILE_NAMES)}
+
+    def sal_profiles(self):
+        return {n: np.full(self.refined[0], -100.0 * self.calls - q) for q, n in enumerate(ag.SAL_PROFILE_NAMES)}
+
+    def slice(self, which, axis, index):
+        shape = {0: (self.nzm, self.nym), 1: (self.nzm, self.nx), 2: (self.nym, self.nx)}[axis]
+        return np.full(shape, 1000.0 * which + 100.0 * axis + index)
+
+    def sal_download(self):
+        nxmr, nymr, nzmr = self.refined
+        k = np.arange(nxmr)[None, None, :]
+        j = np.arange(nymr)[None, :, None]
+        i = np.arange(nzmr)[:, None, None]
+        return (1e4 * i + 1e2 * j + k).astype(np.float64)
+
+
+def test_recorder_writes_the_reference_outputs(tmp_path):
+    """ag.Recorder: cordin_info.h5 at start, a means.h5 sample per TOUT call, the three movie cuts
+    per TFRAME call at the reference's cut positions (0-based: x at 0 and vx at 1, y at nym/2,
+    z at nzm/2; salinity on its own grid)."""
+    text = bou_text(6, 8, 4, multires=1, nxmr=12, nymr=16, nzmr=8, flagsal=1, istr3r=4, tout=0.5, tframe=0.25)
+    inp = ag.parse_bou_in(text)
+    tables = ag.Tables(inp)
+    mgrd = ag.Mgrd(tables)
+    fake = _FakeSolver(6, 8, 4, refined=(12, 16, 8))
+    d = str(tmp_path / "outputdir")
+    rec = ag.Recorder(fake, inp, d, tables, mgrd)
+    assert os.path.exists(os.path.join(d, "cordin_info.h5"))
+    for t in (0.0, 0.5):
+        rec.profiles(t)
+    for t in (0.25, 0.5):
+        rec.frame(t)
+    rec.flush()
+    m = h5.H5File(os.path.join(d, "means.h5"))
+    assert sorted(m.links(m.resolve("Tbar"))) == ["00000", "00001"]
+    np.testing.assert_array_equal(m.read("vxT/00001"), np.full(6, 203.0))
+    np.testing.assert_array_equal(m.read("chiS/00000"), np.full(12, -105.0))
+    x = h5.H5File(os.path.join(d, "flowmov", "movie_xcut.h5"))
+    assert sorted(x.links(x.resolve("vx"))) == ["00001", "00002"]
+    assert x.read("vx/00001")[0, 0] == 0 * 1000 + 0 * 100 + 1          # vx at x index 1
+    assert x.read("temp/00002")[0, 0] == 3 * 1000 + 0 * 100 + 0        # the others at 0
+    y = h5.H5File(os.path.join(d, "flowmov", "movie_ycut.h5"))
+    assert y.read("vy/00001").shape == (4, 6) and y.read("vx/00001").shape == (4, 7)
+    assert y.read("vz/00001")[0, 0] == 2 * 1000 + 1 * 100 + 4          # y index nym/2 = 4
+    z = h5.H5File(os.path.join(d, "flowmov", "movie_zcut.h5"))
+    assert z.read("vx/00002")[0, 0] == 0 * 1000 + 2 * 100 + 2          # z index nzm/2 = 2
+    np.testing.assert_array_equal(x.read("sal/00001"), fake.sal_download()[:, :, 0])
+    np.testing.assert_array_equal(y.read("sal/00001"), fake.sal_download()[:, 8, :])
+    np.testing.assert_array_equal(z.read("sal/00001"), fake.sal_download()[4, :, :])
