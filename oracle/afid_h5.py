@@ -231,9 +231,19 @@ class H5File:
     def root(self) -> dict:
         return self.links(self.root_header)
 
+    def resolve(self, path: str) -> int:
+        """Object header address of a '/'-separated path below the root group."""
+        addr = self.root_header
+        for comp in path.split("/"):
+            addr = self.links(addr)[comp]
+        return addr
+
+    def is_group(self, path: str) -> bool:
+        return any(t in (0x11, 0x02, 0x06) for t, _, _ in self.messages(self.resolve(path)))
+
     # --- datasets --------------------------------------------------------------------------
     def dataset(self, name: str) -> Dataset:
-        addr = self.root()[name]
+        addr = self.resolve(name)
         shape, dtype, ds = None, None, Dataset(name, (), np.dtype("f8"))
         for mtype, _, b in self.messages(addr):
             if mtype == 0x01:
@@ -460,6 +470,134 @@ def _dataset_msgs(a: np.ndarray, raw_addr: int) -> list:
     fill = bytes([2, 2, 2, 1, 0, 0, 0, 0])
     layout = bytes([3, 1]) + struct.pack("<QQ", raw_addr, a.nbytes)
     return [(0x01, space), (0x03, _datatype_msg(a.dtype)), (0x05, fill), (0x08, layout)]
+
+
+def write_v0_tree(path: str, datasets: dict) -> None:
+    """write_v0 with nested groups: '/' in a name nests, a None value is an (empty) group.  Per
+    group, in depth-first order from the root: object header, local heap, B-tree nodes (root
+    level first; a level-l node has up to 32 level l-1 children), symbol table nodes; then every
+    dataset header and every dataset's raw data in the order given."""
+    K_LEAF, K_INT = 4, 16
+    items = list(datasets.items())
+
+    def new_group():
+        return {"members": {}, "groups": {}}
+
+    root = new_group()
+    for i, (name, a) in enumerate(items):      # the groups, in order of first appearance
+        g = root
+        for comp in name.split("/")[:-1]:
+            g = g["groups"].setdefault(comp, new_group())
+
+    def register(g):                             # a group is a member of its parent
+        for comp, child in g["groups"].items():
+            g["members"][comp] = ("g", child)
+            register(child)
+    for i, (name, a) in enumerate(items):
+        parts = name.split("/")
+        g = root
+        for comp in parts[:-1]:
+            g = g["groups"][comp]
+        if a is None:
+            g["groups"].setdefault(parts[-1], new_group())
+        else:
+            g["members"][parts[-1]] = ("d", i)
+    register(root)
+
+    snod_size = 8 + 2 * K_LEAF * 40
+    btree_size = 24 + (2 * K_INT + 1) * 8 + 2 * K_INT * 8
+    order = []          # groups in placement order
+
+    def place(g, pos):
+        g["names"] = sorted(g["members"], key=lambda k: k.encode())
+        heap = bytearray(8)
+        g["off"] = {}
+        for nm in g["names"]:
+            g["off"][nm] = len(heap)
+            b = nm.encode()
+            heap += b + bytes(_pad8(len(b) + 1) - len(b))
+        g["heap"] = heap
+        nsnod = (len(g["names"]) + 2 * K_LEAF - 1) // (2 * K_LEAF)
+        counts = [max(1, (nsnod + 2 * K_INT - 1) // (2 * K_INT))]
+        while counts[-1] > 1:
+            counts.append((counts[-1] + 2 * K_INT - 1) // (2 * K_INT))
+        g["a_oh"] = pos
+        pos += 40
+        g["a_heap"] = pos
+        pos += 32 + len(heap)
+        g["levels"] = [[] for _ in counts]
+        for lev in range(len(counts) - 1, -1, -1):
+            for _ in range(counts[lev]):
+                g["levels"][lev].append(pos)
+                pos += btree_size
+        g["a_snod"] = pos
+        g["nsnod"] = nsnod
+        pos += nsnod * snod_size
+        order.append(g)
+        for comp in g["groups"]:
+            pos = place(g["groups"][comp], pos)
+        return pos
+
+    pos = place(root, 96)
+    a_ds = {}
+    for i, (k, a) in enumerate(items):
+        if a is None:
+            continue
+        a_ds[i] = pos
+        pos += len(_ohdr_v1(_dataset_msgs(np.ascontiguousarray(a), 0)))
+    a_raw = {}
+    for i, (k, a) in enumerate(items):
+        if a is None:
+            continue
+        a_raw[i] = pos
+        pos += _pad8(np.ascontiguousarray(a).nbytes)
+    eof = pos
+    out = bytearray(SIGNATURE + bytes([0, 0, 0, 0, 0, 8, 8, 0]) + struct.pack("<HHI", K_LEAF, K_INT, 0))
+    out += struct.pack("<QQQQ", 0, UNDEF, eof, UNDEF)
+    out += struct.pack("<QQII", 0, root["a_oh"], 1, 0) + struct.pack("<QQ", root["levels"][-1][0], root["a_heap"])
+    for g in order:
+        assert len(out) == g["a_oh"]
+        out += _ohdr_v1([(0x11, struct.pack("<QQ", g["levels"][-1][0], g["a_heap"]))])
+        out += b"HEAP" + bytes(4) + struct.pack("<QQQ", len(g["heap"]), 1, g["a_heap"] + 32) + g["heap"]
+        names = g["names"]
+        n = len(names)
+        child_addr = [g["a_snod"] + c * snod_size for c in range(g["nsnod"])]
+        child_key = [g["off"][names[min(n, (c + 1) * 2 * K_LEAF) - 1]] for c in range(g["nsnod"])]
+        nodes_bytes = {}
+        for lev, nodes in enumerate(g["levels"]):
+            nxt_addr, nxt_key = [], []
+            for k_, b in enumerate(nodes):
+                lo, hi = k_ * 2 * K_INT, min(len(child_addr), (k_ + 1) * 2 * K_INT)
+                left = nodes[k_ - 1] if k_ > 0 else UNDEF
+                right = nodes[k_ + 1] if k_ + 1 < len(nodes) else UNDEF
+                bt = bytearray(b"TREE" + bytes([0, lev]) + struct.pack("<HQQ", hi - lo, left, right))
+                bt += struct.pack("<Q", 0)
+                for c in range(lo, hi):
+                    bt += struct.pack("<QQ", child_addr[c], child_key[c])
+                nodes_bytes[b] = bytes(bt) + bytes(btree_size - len(bt))
+                nxt_addr.append(b)
+                nxt_key.append(child_key[hi - 1] if hi > lo else 0)
+            child_addr, child_key = nxt_addr, nxt_key
+        for b in sorted(nodes_bytes):
+            out += nodes_bytes[b]
+        for c in range(g["nsnod"]):
+            lo, hi = c * 2 * K_LEAF, min(n, (c + 1) * 2 * K_LEAF)
+            sn = bytearray(b"SNOD" + bytes([1, 0]) + struct.pack("<H", hi - lo))
+            for nm in names[lo:hi]:
+                kind, ref = g["members"][nm]
+                addr = a_ds[ref] if kind == "d" else ref["a_oh"]
+                sn += struct.pack("<QQII", g["off"][nm], addr, 0, 0) + bytes(16)
+            out += sn + bytes(snod_size - len(sn))
+    for i, (k, a) in enumerate(items):
+        if a is not None:
+            out += _ohdr_v1(_dataset_msgs(np.ascontiguousarray(a), a_raw[i]))
+    for i, (k, a) in enumerate(items):
+        if a is not None:
+            b = np.ascontiguousarray(a)
+            out += b.tobytes() + bytes(_pad8(b.nbytes) - b.nbytes)
+    assert len(out) == eof, (len(out), eof)
+    with open(path, "wb") as f:
+        f.write(out)
 
 
 def write_v0(path: str, datasets: dict) -> None:

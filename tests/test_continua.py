@@ -599,3 +599,27 @@ def test_recorder_writes_the_reference_outputs(tmp_path):
     np.testing.assert_array_equal(x.read("sal/00001"), fake.sal_download()[:, :, 0])
     np.testing.assert_array_equal(y.read("sal/00001"), fake.sal_download()[:, 8, :])
     np.testing.assert_array_equal(z.read("sal/00001"), fake.sal_download()[4, :, :])
+
+
+def test_nested_layout_matches_the_oracle_writer_byte_for_byte(tmp_path):
+    """The oracle's own nested-group writer (oracle/afid_h5.py write_v0_tree) and the native
+    writer produce the same bytes: a two-level group B-tree, nested and empty groups, and the
+    means.h5 written by afid_write_means."""
+    rng = np.random.default_rng(19)
+    tree = {f"big/{k:05d}": rng.standard_normal(3) for k in range(600)}
+    tree.update({"g/a": np.arange(4, dtype=np.int32), "g/b/c": rng.standard_normal((2, 3)), "empty": None,
+                 "top": np.array([2.5])})
+    a, b = str(tmp_path / "oracle.h5"), str(tmp_path / "native.h5")
+    h5.write_v0_tree(a, tree)
+    ag.h5_write(b, tree)
+    assert open(a, "rb").read() == open(b, "rb").read()
+    # means.h5: groups in the library's order, each followed by its samples
+    times, prof = np.array([0.5, 1.0]), rng.standard_normal((2, 15, 8))
+    ag.write_means(str(tmp_path / "m"), 0.5, times, prof)
+    want = {}
+    for q, g in enumerate(ag.PROFILE_NAMES):
+        want[g] = None
+        for s in range(2):
+            want[f"{g}/{s + 1:05d}"] = prof[s, q]
+    h5.write_v0_tree(str(tmp_path / "means_oracle.h5"), want)
+    assert open(tmp_path / "m" / "means.h5", "rb").read() == open(tmp_path / "means_oracle.h5", "rb").read()
