@@ -57,5 +57,9 @@ def test_reference_arm_prints_on_rank_zero_only(rank):
         d = json.loads(lines[0])
         assert d["impl"] == "reference" and d["value"] > 0 and d["cpu_baseline"]["kind"] == "port"
         assert d["e2e"]["value"] == d["value"]
+        # the warm-up steps run untimed; the timed count and the requested count are reported
+        assert d["warmup"] == 3 and d["steps"] == 1 and d["steps_requested"] == 1
+        for k in ("metric", "unit", "n_gpus", "higher_is_better", "scaling", "vs_baseline", "dtype", "config"):
+            assert k in d, k
     else:
         assert lines == []
