@@ -5,6 +5,7 @@
 #include "afid_host_internal.h"
 #include "afid_salinity.h"
 
+#include <algorithm>
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -206,6 +207,102 @@ int x_grid(int istr3, int nxm, double L, double s, double pi, double schmidt, st
 using afid_hostd::philox_u;
 using afid_hostd::second_derivative_coeff;
 using afid_hostd::uniform_grid;
+
+namespace {
+
+// The mean-profile samples and movie cuts afid_run_io collects for means.h5 and flowmov/.
+struct Samples {
+  std::vector<double> ptimes, prof, salprof, ftimes;
+  std::vector<double> planes[3], salplanes[3];
+
+  int profiles(afid_ctx_t *ctx, const afid_input_t *in, const afid_mgrd_t *mg, double time) {
+    const size_t off = prof.size();
+    prof.resize(off + (size_t)AFID_NUM_PROFILES * in->nxm);
+    int r = afid_gpu_mean_profiles(ctx, prof.data() + off);
+    if (r == AFID_OK && mg) {
+      const size_t o2 = salprof.size();
+      salprof.resize(o2 + (size_t)AFID_NUM_SAL_PROFILES * afid_mgrd_view(mg)->nxmr);
+      r = afid_gpu_sal_profiles(ctx, salprof.data() + o2);
+    }
+    ptimes.push_back(time);
+    return r;
+  }
+
+  // The cut positions of MakeMovie{X,Y,Z}Cut.F90 (0-based): x at 0 (vx at 1; nxm/2 - 1 and
+  // max(nxm/2, 2) - 1 when RAYS and RAYT are both negative), y at nym/2, z at nzm/2; the refined
+  // salinity likewise, cut on the host from a download of the field.
+  // The planes are kept in host memory until the run ends; past kMovieBytes further frames are
+  // not collected (the reference appends each frame to its files instead).
+  static constexpr size_t kMovieBytes = size_t(2) << 30;
+
+  int movie(afid_ctx_t *ctx, const afid_input_t *in, const afid_mgrd_t *mg, double time) {
+    const bool both_neg = in->rays < 0 && in->rayt < 0;
+    const int icx = both_neg ? in->nxm / 2 : 1, nx = in->nxm + 1;
+    const size_t psz[3] = {(size_t)in->nzm * in->nym, (size_t)in->nzm * nx, (size_t)in->nym * nx};
+    size_t frame_bytes = 4 * (psz[0] + psz[1] + psz[2]) * sizeof(double);
+    if (mg) {
+      const afid_sal_grid_t *v = afid_mgrd_view(mg);
+      frame_bytes += ((size_t)v->nzmr * v->nymr + (size_t)v->nzmr * v->nxmr + (size_t)v->nymr * v->nxmr) * sizeof(double);
+    }
+    if ((ftimes.size() + 1) * frame_bytes > kMovieBytes) return AFID_OK;
+    for (int axis = 0; axis < 3; ++axis)
+      for (int which = 0; which < 4; ++which) {
+        const int idx = axis == 0 ? (which == 0 ? std::max(icx, 2) - 1 : icx - 1) : axis == 1 ? in->nym / 2 : in->nzm / 2;
+        const size_t off = planes[axis].size();
+        planes[axis].resize(off + psz[axis]);
+        const int r = afid_gpu_slice(ctx, which, axis, idx, planes[axis].data() + off);
+        if (r != AFID_OK) return r;
+      }
+    if (mg) {
+      const afid_sal_grid_t *v = afid_mgrd_view(mg);
+      const int nxmr = v->nxmr, nymr = v->nymr, nzmr = v->nzmr;
+      std::vector<double> sal((size_t)nxmr * nymr * nzmr);
+      const int r = afid_gpu_sal_download(ctx, sal.data(), nxmr, nymr);
+      if (r != AFID_OK) return r;
+      const int ix = (both_neg ? nxmr / 2 : 1) - 1, iy = nymr / 2, iz = nzmr / 2;
+      for (int i = 0; i < nzmr; ++i)
+        for (int j = 0; j < nymr; ++j) salplanes[0].push_back(sal[((size_t)i * nymr + j) * nxmr + ix]);
+      for (int i = 0; i < nzmr; ++i)
+        for (int k = 0; k < nxmr; ++k) salplanes[1].push_back(sal[((size_t)i * nymr + iy) * nxmr + k]);
+      for (int j = 0; j < nymr; ++j)
+        for (int k = 0; k < nxmr; ++k) salplanes[2].push_back(sal[((size_t)iz * nymr + j) * nxmr + k]);
+    }
+    ftimes.push_back(time);
+    return AFID_OK;
+  }
+
+  int write(const char *dir, const afid_input_t *in, const afid_mgrd_t *mg) const {
+    const afid_sal_grid_t *v = mg ? afid_mgrd_view(mg) : nullptr;
+    int r = AFID_OK;
+    if (in->tout > 0.0 && !ptimes.empty()) {
+      // a sample whose number nint(time / TOUT) was taken already is dropped: the reference's
+      // second dataset creation under that name fails and the first sample stays
+      std::vector<double> t, p, q;
+      std::vector<char> seen(100000, 0);
+      const size_t np = (size_t)AFID_NUM_PROFILES * in->nxm, nq = v ? (size_t)AFID_NUM_SAL_PROFILES * v->nxmr : 0;
+      for (size_t k = 0; k < ptimes.size(); ++k) {
+        const double fr = std::round(ptimes[k] / in->tout);
+        if (!(fr >= 0.0 && fr <= 99999.0) || seen[(size_t)fr]) continue;
+        seen[(size_t)fr] = 1;
+        t.push_back(ptimes[k]);
+        p.insert(p.end(), prof.begin() + k * np, prof.begin() + (k + 1) * np);
+        if (v) q.insert(q.end(), salprof.begin() + k * nq, salprof.begin() + (k + 1) * nq);
+      }
+      r = afid_write_means(dir, in->tout, (int)t.size(), t.data(), in->nxm, p.data(), v ? v->nxmr : 0,
+                           v ? q.data() : nullptr);
+    }
+    if (r != AFID_OK || !(in->tframe > 0.0) || ftimes.empty()) return r;
+    for (size_t f = 0; f < ftimes.size(); ++f)
+      if (!(std::round(ftimes[f] / in->tframe) >= 0.0 && std::round(ftimes[f] / in->tframe) <= 99999.0)) return r;
+    for (int axis = 0; axis < 3 && r == AFID_OK; ++axis)
+      r = afid_write_movie(dir, axis, in->tframe, (int)ftimes.size(), ftimes.data(), in->nxm, in->nym, in->nzm,
+                           planes[axis].data(), v ? v->nxmr : 0, v ? v->nymr : 0, v ? v->nzmr : 0,
+                           v ? salplanes[axis].data() : nullptr);
+    return r;
+  }
+};
+
+}  // namespace
 
 extern "C" {
 
@@ -557,6 +654,17 @@ int afid_run_io(const afid_input_t *in, int precision, uint64_t seed, int nsteps
         s = afid_gpu_sal_upload(ctx, sal.data(), v->nxmr, v->nymr);
       }
     }
+    // Outputs besides the restart files (dir only): cordin_info.h5 (WriteGridInfo), a mean-profile
+    // sample at start-up and at TOUT (CalcMeanProfiles, main.F90:227, 315-320) and the three movie
+    // cuts at start-up and at TFRAME (Mkmov_*, main.F90:230-232, 333-341), collected here and
+    // written when the run ends
+    Samples out;
+    const bool outputs = dir != nullptr;
+    if (s == AFID_OK && outputs) {
+      s = afid_write_grid_info(dir, t, mg);
+      if (s == AFID_OK) s = out.profiles(ctx, in, mg, time);
+      if (s == AFID_OK) s = out.movie(ctx, in, mg, time);
+    }
     // 3-D frames: at start-up (main.F90:241) and when mod(time, SAVE_3D) < dt past the first
     // TFRAME (main.F90:376-381); skipped when SAVE_3D or TFRAME is not positive
     const bool frames = dir && in->save_3d > 0.0 && in->tframe > 0.0;
@@ -591,6 +699,12 @@ int afid_run_io(const afid_input_t *in, int precision, uint64_t seed, int nsteps
         afid_gpu_globals(ctx, ra_pr, &nu, &ke, nullptr);
         cb(ntime, time, dt, nu, ke, user);
       }
+      if (outputs && in->tout > 0.0 && std::fmod(time, in->tout) < dt &&
+          (s = out.profiles(ctx, in, mg, time)) != AFID_OK)
+        break;
+      if (outputs && in->tframe > 0.0 && std::fmod(time, in->tframe) < dt && std::floor(time / in->tframe) != 0.0 &&
+          (s = out.movie(ctx, in, mg, time)) != AFID_OK)
+        break;
       if (frames && std::fmod(time, in->save_3d) < dt && std::floor(time / in->tframe) != 0.0) {
         master.time = time;
         if ((s = afid_gpu_write_flow_field(ctx, dir, 0, in->save_3d, &master)) != AFID_OK) break;
@@ -611,6 +725,8 @@ int afid_run_io(const afid_input_t *in, int precision, uint64_t seed, int nsteps
       master.time = time;
       s = afid_gpu_write_flow_field(ctx, dir, 1, in->save_3d, &master);
     }
+    // means.h5 and the movie files hold every sample taken, as the reference's files would
+    if (s == AFID_OK && outputs) s = out.write(dir, in, mg);
     if (stats) *stats = st;
     afid_gpu_destroy(ctx);
     afid_mgrd_destroy(mg);
