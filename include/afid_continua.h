@@ -168,7 +168,8 @@ int afid_gpu_read_flow_interp(afid_ctx_t *ctx, const char *dir, const afid_input
  * Besides the restart files it writes cordin_info.h5, means.h5 (a sample at start-up and whenever
  * mod(time, TOUT) < dt) and flowmov/movie_{x,y,z}cut.h5 (the cuts at start-up and whenever
  * mod(time, TFRAME) < dt past the first TFRAME), as the reference's main loop does; the samples
- * are written when the run ends, the movie planes kept up to 2 GiB per run.
+ * are written when the run ends, the movie planes kept up to 2 GiB per run.  A restarted run
+ * rewrites means.h5 and the movie files with its own samples, where the reference appends to them.
  * NREAD = 1 starts from dir's continua files (time from the master unless IRESET = 1); otherwise
  * from the seeded initial condition.  Frames go to dir/fields, the final continua files to dir
  * on a normal exit (steps done, 333 tmax, 555 ntst). */
