@@ -67,7 +67,7 @@ void geom_physics(Geom &g, const afid_grid_t *grid, const afid_params_t *prm) {
   g.byct = prm->byct;
   g.rren = 1.0 / prm->ren;
   g.rpect = 1.0 / prm->pect;
-  g.udyq_re = g.dyq / prm->ren;  // ExplicitTermsVX.F90:191-192
+  g.udyq_re = g.dyq / prm->ren;  // ExplicitTermsVX.F90:27-28
   g.udzq_re = g.dzq / prm->ren;
   g.udyq_pe = g.dyq / prm->pect;  // ExplicitTermsTemp.F90:24-25
   g.udzq_pe = g.dzq / prm->pect;
@@ -413,7 +413,7 @@ int ctx_create(const afid_grid_t *grid, const afid_params_t *prm, const BatchSpe
   const int L1 = nx + 8;
   size_t o_udx3c = put(grid->udx3c, nx, L1), o_udx3m = put(grid->udx3m, nxm, L1);
   std::vector<double> idx(nxm);
-  for (int k = 0; k < nxm; ++k) idx[k] = 1.0 / grid->udx3m[k];  // ExplicitTermsVX.F90:194-196
+  for (int k = 0; k < nxm; ++k) idx[k] = 1.0 / grid->udx3m[k];  // ExplicitTermsVX.F90:30-32
   size_t o_idx = put(idx.data(), nxm, L1);
   size_t o_ap3ck = put(grid->ap3ck, nx, L1), o_ac3ck = put(grid->ac3ck, nx, L1), o_am3ck = put(grid->am3ck, nx, L1);
   size_t o_ap3sk = put(grid->ap3sk, nxm, L1), o_ac3sk = put(grid->ac3sk, nxm, L1), o_am3sk = put(grid->am3sk, nxm, L1);

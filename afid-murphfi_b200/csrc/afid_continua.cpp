@@ -1039,20 +1039,24 @@ extern "C" int afid_write_means(const char *dir, double tout, int nsamples, cons
     const bool sal = sal_profiles != nullptr;
     if (sal && nxmr < 1) return AFID_E_INVALID;
     if (!ensure_dir(dir)) return AFID_E_IO;
-    // sample names: nint(time / TOUT) as i5.5 (CalcMeanProfiles.F90:209), distinct
+    // sample names: nint(time / TOUT) as i5.5 (CalcMeanProfiles.F90:209).  A later sample with
+    // the same number replaces the earlier one: HdfSerialWriteReal1D deletes an existing dataset
+    // of that name before it writes (h5tools/HdfRoutines.F90:159-161).
     std::vector<std::string> stamp(nsamples);
-    std::vector<char> used(100000, 0);
+    std::vector<int> last(100000, -1), keep;
     for (int s = 0; s < nsamples; ++s) {
       const double fr = std::round(times[s] / tout);
       if (!(fr >= 0.0 && fr <= 99999.0)) return AFID_E_INVALID;
-      if (used[(size_t)fr]++) return AFID_E_INVALID;  // the reference cannot write a sample twice
+      last[(size_t)fr] = s;
       char b[8];
       std::snprintf(b, sizeof(b), "%05d", (int)fr);
       stamp[s] = b;
     }
+    for (int s = 0; s < nsamples; ++s)
+      if (last[(size_t)std::round(times[s] / tout)] == s) keep.push_back(s);
     const int ngroups = AFID_NUM_PROFILES + (sal ? AFID_NUM_SAL_PROFILES : 0);
     std::vector<std::string> names;
-    names.reserve((size_t)ngroups * (nsamples + 1));
+    names.reserve((size_t)ngroups * (keep.size() + 1));
     std::vector<afid_h5_dataset_t> sets;
     sets.reserve(names.capacity());
     auto add = [&](std::string name, int dtype, int64_t len, const double *data) {
@@ -1068,7 +1072,7 @@ extern "C" int afid_write_means(const char *dir, double tout, int nsamples, cons
       const bool sq = q >= AFID_NUM_PROFILES;
       const char *g = sq ? kSalNames[q - AFID_NUM_PROFILES] : kNames[q];
       add(g, AFID_H5_GROUP, 0, nullptr);
-      for (int s = 0; s < nsamples; ++s) {
+      for (int s : keep) {
         const double *src = sq ? sal_profiles + ((size_t)s * AFID_NUM_SAL_PROFILES + (q - AFID_NUM_PROFILES)) * nxmr
                                : profiles + ((size_t)s * AFID_NUM_PROFILES + q) * nxm;
         add(std::string(g) + "/" + stamp[s], AFID_H5_F64, sq ? nxmr : nxm, src);

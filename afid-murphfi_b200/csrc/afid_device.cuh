@@ -55,12 +55,12 @@ struct InstScal {
 // kernel of the substep, so a captured step graph does not depend on dt).
 struct StepCoef {
   double al, ga, ro, dt, beta;
-  double alre, alpec;  // al/ren (ImplicitAndUpdateVX.F90:111), al/pect (ImplicitAndUpdateTemp.F90:197)
+  double alre, alpec;  // al/ren (ImplicitAndUpdateVX.F90:26), al/pect (ImplicitAndUpdateTemp.F90:22)
 };
 
 // 1-D metric tables on the device (0-based copies of the reference's arrays).
 struct Tables {
-  const double *udx3c, *udx3m, *idx;  // idx = 1/udx3m (ExplicitTermsVX.F90:194-196)
+  const double *udx3c, *udx3m, *idx;  // idx = 1/udx3m (ExplicitTermsVX.F90:30-32)
   const double *ap3ck, *ac3ck, *am3ck;
   const double *ap3sk, *ac3sk, *am3sk;
   const double *ap3ssk, *ac3ssk, *am3ssk;

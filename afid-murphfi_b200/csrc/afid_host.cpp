@@ -213,6 +213,7 @@ namespace {
 // The mean-profile samples and movie cuts afid_run_io collects for means.h5 and flowmov/.
 struct Samples {
   std::vector<double> ptimes, prof, salprof, ftimes;
+  size_t dropped = 0;  // movie frames left out once the plane buffer is full
   std::vector<double> planes[3], salplanes[3];
 
   int profiles(afid_ctx_t *ctx, const afid_input_t *in, const afid_mgrd_t *mg, double time) {
@@ -244,7 +245,15 @@ struct Samples {
       const afid_sal_grid_t *v = afid_mgrd_view(mg);
       frame_bytes += ((size_t)v->nzmr * v->nymr + (size_t)v->nzmr * v->nxmr + (size_t)v->nymr * v->nxmr) * sizeof(double);
     }
-    if ((ftimes.size() + 1) * frame_bytes > kMovieBytes) return AFID_OK;
+    if ((ftimes.size() + 1) * frame_bytes > kMovieBytes) {
+      // the frame is not kept: say so once, and count the frames left out
+      if (dropped++ == 0)
+        std::fprintf(stderr,
+                     "afid_run_io: movie planes exceed %zu bytes at time %.6g; this and later frames "
+                     "are not written to flowmov/\n",
+                     kMovieBytes, time);
+      return AFID_OK;
+    }
     for (int axis = 0; axis < 3; ++axis)
       for (int which = 0; which < 4; ++which) {
         const int idx = axis == 0 ? (which == 0 ? std::max(icx, 2) - 1 : icx - 1) : axis == 1 ? in->nym / 2 : in->nzm / 2;
@@ -275,15 +284,14 @@ struct Samples {
     const afid_sal_grid_t *v = mg ? afid_mgrd_view(mg) : nullptr;
     int r = AFID_OK;
     if (in->tout > 0.0 && !ptimes.empty()) {
-      // a sample whose number nint(time / TOUT) was taken already is dropped: the reference's
-      // second dataset creation under that name fails and the first sample stays
+      // samples whose number nint(time / TOUT) is out of the five-digit range are dropped; of
+      // two samples with the same number afid_write_means keeps the later one, as the
+      // reference's writer deletes and rewrites the dataset
       std::vector<double> t, p, q;
-      std::vector<char> seen(100000, 0);
       const size_t np = (size_t)AFID_NUM_PROFILES * in->nxm, nq = v ? (size_t)AFID_NUM_SAL_PROFILES * v->nxmr : 0;
       for (size_t k = 0; k < ptimes.size(); ++k) {
         const double fr = std::round(ptimes[k] / in->tout);
-        if (!(fr >= 0.0 && fr <= 99999.0) || seen[(size_t)fr]) continue;
-        seen[(size_t)fr] = 1;
+        if (!(fr >= 0.0 && fr <= 99999.0)) continue;
         t.push_back(ptimes[k]);
         p.insert(p.end(), prof.begin() + k * np, prof.begin() + (k + 1) * np);
         if (v) q.insert(q.end(), salprof.begin() + k * nq, salprof.begin() + (k + 1) * nq);
@@ -291,6 +299,8 @@ struct Samples {
       r = afid_write_means(dir, in->tout, (int)t.size(), t.data(), in->nxm, p.data(), v ? v->nxmr : 0,
                            v ? q.data() : nullptr);
     }
+    if (dropped)
+      std::fprintf(stderr, "afid_run_io: %zu movie frames were left out of flowmov/ (plane buffer full)\n", dropped);
     if (r != AFID_OK || !(in->tframe > 0.0) || ftimes.empty()) return r;
     for (size_t f = 0; f < ftimes.size(); ++f)
       if (!(std::round(ftimes[f] / in->tframe) >= 0.0 && std::round(ftimes[f] / in->tframe) <= 99999.0)) return r;

@@ -71,7 +71,7 @@ template <typename TE> __device__ __forceinline__ TE cv(double v) { return (TE)v
 // In 2-D (TWO_D: the z neighbours are the cell itself) every z-difference term is zero by
 // construction; those terms are left out instead of being evaluated to zero.
 
-// ExplicitTermsVX.F90:194-291 + ImplicitAndUpdateVX.F90:124-150, k = 1..nxm-1 (0-based)
+// ExplicitTermsVX.F90:30-127 + ImplicitAndUpdateVX.F90:39-66, k = 1..nxm-1 (0-based)
 template <typename TE, bool TWO_D, bool SAL>
 __device__ __forceinline__ double rhs_vx(const Geom &g, const Tables &t, const StepCoef &sc, int k,
                                          const ColV &X, const ColV &Y, const ColV &Z, const ColV &T,
@@ -160,7 +160,7 @@ __device__ __forceinline__ double rhs_vy(const Geom &g, const Tables &t, const S
   return (sc.ga * (double)dph + sc.ro * ru + alre * dxxvy - dyp) * sc.dt;
 }
 
-// ExplicitTermsVZ.F90:149-244 + ImplicitAndUpdateVZ.F90:121-161, k = 0..nxm-1
+// ExplicitTermsVZ.F90:23-118 + ImplicitAndUpdateVZ.F90:38-69, k = 0..nxm-1
 template <typename TE, bool TWO_D, bool SAL>
 __device__ __forceinline__ double rhs_vz(const Geom &g, const Tables &t, const StepCoef &sc, int k,
                                          const ColV &X, const ColV &Y, const ColV &Z, const ColV &T,
@@ -205,7 +205,7 @@ __device__ __forceinline__ double rhs_vz(const Geom &g, const Tables &t, const S
   }
 }
 
-// ExplicitTermsTemp.F90:22-77 + ImplicitAndUpdateTemp.F90:197-237, k = 0..nxm-1
+// ExplicitTermsTemp.F90:22-77 + ImplicitAndUpdateTemp.F90:33-66, k = 0..nxm-1
 template <typename TE, bool TWO_D>
 __device__ __forceinline__ double rhs_temp(const Geom &g, const Tables &t, const StepCoef &sc, int k,
                                            const ColV &X, const ColV &Y, const ColV &Z, const ColV &T,
@@ -470,7 +470,7 @@ __global__ void __launch_bounds__(TPC, k1_min_blocks<CAP, TPC>())
         const int r = k - 1;
         vx_o[c0 + k] = X.c[k] + s_rhs[(r % M) * LD + r / M];
       } else {
-        vx_o[c0] = 0.0;  // ImplicitAndUpdateVX.F90:171-172: vx(1) = vx(nx) = 0
+        vx_o[c0] = 0.0;  // ImplicitAndUpdateVX.F90:86-87: vx(1) = vx(nx) = 0
         vx_o[c0 + nxm] = 0.0;
       }
       vy_o[c0 + k] = Y.c[k] + s_rhs[FLD + sk];

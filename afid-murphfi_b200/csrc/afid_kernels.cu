@@ -29,8 +29,8 @@ namespace afid {
 // ------------------------------------------------------------------------------------------
 // CN tridiagonal factor tables.
 //
-// The matrices of SolveImpEqnUpdate_X.F90:27-42, SolveImpEqnUpdate_YZ.F90:96-105 and
-// SolveImpEqnUpdate_Temp.F90:154-165 are identical for every (j,i) column: rows normalised by
+// The matrices of SolveImpEqnUpdate_X.F90:27-42, SolveImpEqnUpdate_YZ.F90:25-36 and
+// SolveImpEqnUpdate_Temp.F90:25-36 are identical for every (j,i) column: rows normalised by
 // ackl_b = 1/(1 - ac*betadx), unit diagonal, a = -am*betadx*ackl_b, c = -ap*betadx*ackl_b.
 // For vx the identity rows 1 and nx (whose RHS is zeroed, SolveImpEqnUpdate_X.F90:56-57) are
 // eliminated, leaving rows k = 2..nxm.  Rows are split into 32 chunks of M (lane l owns rows

@@ -27,6 +27,7 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[AFID_NOALLOC_SC
 constexpr int kMaxDevices = 64;
 std::mutex g_mu;
 void *g_scratch_addr[kMaxDevices] = {};  // device address of g_noalloc_scratch, per device
+void *g_scratch_ctx[kMaxDevices] = {};   // the context each address was looked up in
 
 // One warp per (j,i) column: the three g3rc-weighted sums of GlobalQuantities.F90:31-47 for
 // that column go to partial[3*col + q], so every partial is rewritten on every call.
@@ -90,16 +91,41 @@ __global__ void __launch_bounds__(256)
   }
 }
 
-// Device address of the scratch array on the current device, looked up once per device.
+// Handle of the calling thread's current context (driver API cuCtxGetCurrent, reached through the
+// runtime's entry-point query so that no driver library is linked), or null when unavailable.
+using CtxGetCurrentFn = int (*)(void **);
+void *current_context() {
+  static CtxGetCurrentFn fn = []() -> CtxGetCurrentFn {
+    void *f = nullptr;
+    cudaDriverEntryPointQueryResult q{};
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      return nullptr;
+    return reinterpret_cast<CtxGetCurrentFn>(f);
+  }();
+  void *ctx = nullptr;
+  if (!fn || fn(&ctx) != 0) return nullptr;
+  return ctx;
+}
+
+// Device address of the scratch array on the current device.  It is looked up once per device
+// and context: a device reset (or any new context on the device) loads the module again, so the
+// cached address is dropped when the current context handle differs from the one it was taken
+// in.  Without a context handle the lookup runs on every call.
 int scratch_for_current_device(void **out) {
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return AFID_E_CUDA;
+  void *ctx = current_context();
   std::lock_guard<std::mutex> lk(g_mu);
-  if (!g_scratch_addr[dev]) {
+  if (!g_scratch_addr[dev] || !ctx || g_scratch_ctx[dev] != ctx) {
     void *p = nullptr;
     const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-    if (e != cudaSuccess || !p) return AFID_E_CUDA;
+    if (e != cudaSuccess || !p) {
+      g_scratch_addr[dev] = nullptr;
+      return AFID_E_CUDA;
+    }
     g_scratch_addr[dev] = p;
+    g_scratch_ctx[dev] = ctx;
   }
   *out = g_scratch_addr[dev];
   return AFID_OK;
@@ -111,7 +137,7 @@ extern "C" int afid_gpu_globals_noalloc(int nxm, int nym, int nzm, int ldx, doub
                                         const double *vx, const double *vy, const double *vz,
                                         const double *temp, const double *g3rc, double *out3,
                                         void *stream) {
-  if (nxm < 1 || nym < 1 || nzm < 1 || ldx < nxm + 1 || !(alx3 > 0.0) || ra_pr < 0.0) return AFID_E_INVALID;
+  if (nxm < 1 || nym < 1 || nzm < 1 || ldx < nxm + 1 || !(alx3 > 0.0) || !(ra_pr >= 0.0)) return AFID_E_INVALID;
   if (!vx || !vy || !vz || !temp || !g3rc || !out3) return AFID_E_INVALID;
   const long long ncol = (long long)nym * nzm;
   const long long need = (3 * ncol) * (long long)sizeof(double);
@@ -123,8 +149,15 @@ extern "C" int afid_gpu_globals_noalloc(int nxm, int nym, int nzm, int ldx, doub
   double *partial = static_cast<double *>(scratch);
   const double dx = (double)nxm / alx3;
   const double vol = 1.0 / (alx3 * dx * (double)nzm * (double)nym);  // GlobalQuantities.F90:27
-  const int blocks = (int)((ncol + 7) / 8);
-  k_noalloc_column_sums<<<blocks, 256, 0, st>>>(nxm, nym, nzm, ldx, vx, vy, vz, temp, g3rc, partial);
-  k_noalloc_finish<<<1, 256, 0, st>>>(partial, ncol, vol, std::sqrt(ra_pr), out3);
-  return (cudaGetLastError() == cudaSuccess) ? AFID_OK : AFID_E_CUDA;
+  const double sqrt_ra_pr = std::sqrt(ra_pr);
+  // each launch reports its own status (cudaLaunchKernel's return value), so an error left
+  // behind by the caller's earlier, unrelated CUDA calls is neither returned nor cleared here
+  const dim3 grid1((unsigned)((ncol + 7) / 8)), block(256), one(1);
+  void *a1[] = {&nxm, &nym, &nzm, &ldx, &vx, &vy, &vz, &temp, &g3rc, &partial};
+  cudaError_t e = cudaLaunchKernel((const void *)k_noalloc_column_sums, grid1, block, a1, 0, st);
+  if (e == cudaSuccess) {
+    void *a2[] = {(void *)&partial, (void *)&ncol, (void *)&vol, (void *)&sqrt_ra_pr, (void *)&out3};
+    e = cudaLaunchKernel((const void *)k_noalloc_finish, one, block, a2, 0, st);
+  }
+  return e == cudaSuccess ? AFID_OK : AFID_E_CUDA;
 }

@@ -9,8 +9,8 @@
  * builds the metric tables exactly as the reference does (CreateGrid.F90, InitPressureSolver
  * in pressure.F90:61-114); the library owns device buffers and keeps the state resident on
  * the GPU between calls.  The precedent for binding C from the reference is its FFTW
- * interface block (src/flow_solver/param.F90:184-226); INTEGRATION.md shows the
- * ISO_C_BINDING interface a maintainer adds.
+ * interface block (src/flow_solver/param.F90:184-226); a Fortran caller binds these entry
+ * points the same way, with an ISO_C_BINDING interface block of bind(C) functions.
  *
  * Array conventions: all 1-D tables are 0-based copies of the reference's 1-based arrays
  * (table[k-1] == fortran(k)).  3-D host arrays are Fortran column-major (x fastest, then y,
@@ -192,8 +192,10 @@ int afid_gpu_profile_report(afid_ctx_t *ctx, double *ms, long long *count, int n
  * partial sums live in a static device array of AFID_NOALLOC_SCRATCH_BYTES that every GPU
  * loading this library holds until exit, which limits it to nym*nzm <= 174762 columns
  * (AFID_E_CAPACITY beyond).  The first call on each device looks up that array's address (do
- * it before any stream capture).  Calls share the array and it keeps the last call's
- * contents; calls that overlap on the GPU race. */
+ * it before any stream capture); a device reset or a new context on the device invalidates the
+ * address, and the first call after it looks it up again.  Calls share the array and it keeps
+ * the last call's contents; calls that overlap on the GPU race.  Each launch's own status is
+ * returned (AFID_E_CUDA); errors left by the caller's earlier CUDA calls are not consumed. */
 #define AFID_NOALLOC_SCRATCH_BYTES (4u << 20)
 int afid_gpu_globals_noalloc(int nxm, int nym, int nzm, int ldx, double alx3, double ra_pr,
                              const double *vx, const double *vy, const double *vz,

@@ -262,7 +262,7 @@ static void explicit_terms(afid_cpu_t *c) {
     const int jp = wp(j, nym), jm = wm(j, nym), ip = wp(i, nzm), im = wm(i, nzm);
     const size_t C = IDX(c, 0, j, i), JP = IDX(c, 0, jp, i), JM = IDX(c, 0, jm, i), IP = IDX(c, 0, j, ip),
                  IM = IDX(c, 0, j, im), JMIP = IDX(c, 0, jm, ip), JPIM = IDX(c, 0, jp, im);
-    /* ExplicitTermsVX.F90:206-291 */
+    /* ExplicitTermsVX.F90:42-127 */
     for (int k = 1; k < nxm; ++k) {
       const int km = k - 1, kp = k + 1;
       const double *idx = c->idx;
@@ -294,7 +294,7 @@ static void explicit_terms(afid_cpu_t *c) {
       double dph = -(hyx + hyy + hyz) + dyyvy + dzzvy + c->gy;
       if (c->gaxis == 2) dph = dph + c->byct * (c->active_t * 0.5 * (t[C + k] + t[JM + k]));
       c->dph[C + k] = dph;
-      /* ExplicitTermsVZ.F90:164-244 */
+      /* ExplicitTermsVZ.F90:38-118 */
       cc = vz[C + k];
       double hzz = ((vz[IP + k] + cc) * (vz[IP + k] + cc) - (vz[IM + k] + cc) * (vz[IM + k] + cc)) * udz;
       double hzy = ((vy[JP + k] + vy[JPIM + k]) * (vz[JP + k] + cc) - (vy[C + k] + vy[IM + k]) * (cc + vz[JM + k])) * udy;
@@ -366,7 +366,7 @@ static void implicit_update(afid_cpu_t *c, double al, double ga, double ro, doub
       const int j = col % nym, i = col / nym, jm = wm(j, nym), im = wm(i, nzm);
       const size_t C = IDX(c, 0, j, i), JM = IDX(c, 0, jm, i), IM = IDX(c, 0, j, im);
       double *vx = c->vx, *vy = c->vy, *vz = c->vz, *t = c->temp, *pr = c->pr;
-      /* ImplicitAndUpdateVX.F90:122-172 */
+      /* ImplicitAndUpdateVX.F90:37-87 */
       rhs[0] = 0.0; rhs[nx - 1] = 0.0;
       for (int k = 1; k < nxm; ++k) {
         double dxx = vx[C + k + 1] * c->ap3ck[k] + vx[C + k] * c->ac3ck[k] + vx[C + k - 1] * c->am3ck[k];
@@ -390,7 +390,7 @@ static void implicit_update(afid_cpu_t *c, double al, double ga, double ro, doub
       }
       gttrs_r(nxm, my.dl, my.d, my.du, my.du2, my.ipiv, rhs);
       for (int k = 0; k < nxm; ++k) vy[C + k] += rhs[k];
-      /* ImplicitAndUpdateVZ.F90:133-173 */
+      /* ImplicitAndUpdateVZ.F90:38-77 */
       for (int k = 0; k < nxm; ++k) {
         const int kmm = k == 0 ? 0 : k - 1, kpp = k == nxm - 1 ? k : k + 1;
         double dxx = vz[C + kpp] * c->ap3sk[k] + vz[C + k] * c->ac3sk[k] + vz[C + kmm] * c->am3sk[k];
@@ -400,7 +400,7 @@ static void implicit_update(afid_cpu_t *c, double al, double ga, double ro, doub
       }
       gttrs_r(nxm, my.dl, my.d, my.du, my.du2, my.ipiv, rhs);
       for (int k = 0; k < nxm; ++k) vz[C + k] += rhs[k];
-      /* ImplicitAndUpdateTemp.F90:208-250 */
+      /* ImplicitAndUpdateTemp.F90:33-74 */
       const double tbp = c->tempbp[j + nym * i], ttp = c->temptp[j + nym * i];
       for (int k = 0; k < nxm; ++k) {
         double dxx;

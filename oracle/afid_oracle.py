@@ -548,7 +548,7 @@ def _im(a):
 # Explicit terms
 # ----------------------------------------------------------------------------------------------
 def explicit_terms_vx(g: Grid, s: State, qcap: np.ndarray) -> None:
-    """``ExplicitTermsVX.F90:188-291``: qcap(k=2..nxm) = -(hxx+hxy+hxz) + dyy vx + dzz vx
+    """``ExplicitTermsVX.F90:24-127``: qcap(k=2..nxm) = -(hxx+hxy+hxz) + dyy vx + dzz vx
     (+ byct*T buoyancy for gAxis=1)."""
     p = g.p
     nxm = p.nxm
@@ -615,7 +615,7 @@ def explicit_terms_vy(g: Grid, s: State, dph: np.ndarray) -> None:
 
 
 def explicit_terms_vz(g: Grid, s: State, dq: np.ndarray) -> None:
-    """``ExplicitTermsVZ.F90:149-244``: dq(k=1..nxm) for vz (+ buoyancy for gAxis=3)."""
+    """``ExplicitTermsVZ.F90:23-118``: dq(k=1..nxm) for vz (+ buoyancy for gAxis=3)."""
     p = g.p
     nxm = p.nxm
     udyq = g.dyq / g.ren
@@ -696,7 +696,7 @@ def _dgttrs_columns(dl, d, du, rhs_cols):
 
 
 def implicit_and_update_vx(g: Grid, s: State, qcap, al, ga, ro, dt, beta) -> None:
-    """``ImplicitAndUpdateVX.F90:111-172`` + ``SolveImpEqnUpdate_X.F90:25-67``."""
+    """``ImplicitAndUpdateVX.F90:26-87`` + ``SolveImpEqnUpdate_X.F90:25-67``."""
     p = g.p
     nxm, nx = p.nxm, g.nx
     alre = al / g.ren
@@ -731,7 +731,7 @@ def implicit_and_update_vx(g: Grid, s: State, qcap, al, ga, ro, dt, beta) -> Non
 
 
 def _solve_yz_like(g: Grid, q, rhs, ap, ac, am, betadx):
-    """``SolveImpEqnUpdate_YZ.F90:94-127`` / ``SolveImpEqnUpdate_Temp.F90:154-190``."""
+    """``SolveImpEqnUpdate_YZ.F90:25-58`` / ``SolveImpEqnUpdate_Temp.F90:25-61``."""
     nxm = g.p.nxm
     amkl = np.zeros(nxm)
     apkl = np.zeros(nxm)
@@ -775,7 +775,7 @@ def implicit_and_update_vy(g: Grid, s: State, dph, al, ga, ro, dt, beta) -> None
 
 
 def implicit_and_update_vz(g: Grid, s: State, dq, al, ga, ro, dt, beta) -> None:
-    """``ImplicitAndUpdateVZ.F90:121-173``."""
+    """``ImplicitAndUpdateVZ.F90:26-77``."""
     p = g.p
     nxm = p.nxm
     alre = al / g.ren
@@ -791,7 +791,7 @@ def implicit_and_update_vz(g: Grid, s: State, dq, al, ga, ro, dt, beta) -> None:
 
 
 def implicit_and_update_temp(g: Grid, s: State, hro, al, ga, ro, dt) -> None:
-    """``ImplicitAndUpdateTemp.F90:197-250`` + ``SolveImpEqnUpdate_Temp.F90:154-190``."""
+    """``ImplicitAndUpdateTemp.F90:22-74`` + ``SolveImpEqnUpdate_Temp.F90:25-61``."""
     p = g.p
     nxm = p.nxm
     alpec = al / g.pect

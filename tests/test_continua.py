@@ -482,9 +482,33 @@ def test_means_file_layout(tmp_path):
     f0 = h5.H5File(str(tmp_path / "empty" / "means.h5"))
     assert sorted(f0.root()) == sorted(ag.PROFILE_NAMES)
     assert all(f0.links(f0.resolve(g)) == {} for g in ag.PROFILE_NAMES)
-    with pytest.raises(ag.AfidError) as e:   # two samples with the same NNNNN
-        ag.write_means(d, 0.5, np.array([0.5, 0.52]), prof[:2])
-    assert e.value.status == ag.AFID_E_INVALID
+    # two samples with the same NNNNN: the later one is stored, as HdfSerialWriteReal1D deletes
+    # the existing dataset before it writes (h5tools/HdfRoutines.F90:159-161)
+    ag.write_means(str(tmp_path / "twice"), 0.5, np.array([0.5, 0.52, 1.0]), prof)
+    f2 = h5.H5File(str(tmp_path / "twice" / "means.h5"))
+    for q, g in enumerate(ag.PROFILE_NAMES):
+        assert sorted(f2.links(f2.resolve(g))) == ["00001", "00002"], g
+        np.testing.assert_array_equal(f2.read(f"{g}/00001"), prof[1, q])
+        np.testing.assert_array_equal(f2.read(f"{g}/00002"), prof[2, q])
+
+
+def test_means_samples_closer_than_half_tout_keep_the_later(tmp_path):
+    """With dt > TOUT/2 two main-loop sample points can round to the same nint(time / TOUT); the
+    reference's writer then replaces the first profile by the second.  The Recorder (and
+    afid_run_io's sample list, which goes through the same afid_write_means) store the later one."""
+    text = bou_text(6, 8, 4, tout=0.5, tframe=0.0)
+    inp = ag.parse_bou_in(text)
+    fake = _FakeSolver(6, 8, 4)
+    d = str(tmp_path / "outputdir")
+    rec = ag.Recorder(fake, inp, d, ag.Tables(inp))
+    for t in (0.0, 0.3, 0.7, 1.0):            # numbers 0, 1, 1, 2: the 0.7 sample replaces 0.3
+        rec.profiles(t)
+    rec.flush()
+    m = h5.H5File(os.path.join(d, "means.h5"))
+    assert sorted(m.links(m.resolve("Tbar"))) == ["00000", "00001", "00002"]
+    np.testing.assert_array_equal(m.read("Tbar/00000"), np.full(6, 100.0))
+    np.testing.assert_array_equal(m.read("Tbar/00001"), np.full(6, 300.0))   # the third call
+    np.testing.assert_array_equal(m.read("vxT/00002"), np.full(6, 403.0))
 
 
 @pytest.mark.parametrize("axis", [0, 1, 2])

@@ -5,9 +5,10 @@ Some callers cannot let a library allocate device memory (host codes with their 
 pool or a capped allocator, monitors attached to another program's run); this entry point
 serves them from a static device array instead.  The check: on two calls in a row, on the
 state of a running solver, it returns the same Nusselt number, kinetic energy and mean
-temperature as the regular entry point, within the 1e-12 relative tolerance the other
-statistics tests use.  This file is collected last so that a run that stops at its first
-failure has run every other test before it.
+temperature as the regular entry point, and the same Nusselt number and kinetic energy as the
+CPU oracle's GlobalQuantities restatement stepped alongside, within the 1e-12 relative
+tolerance the other statistics tests use.  This file is collected last so that a run that
+stops at its first failure has run every other test before it.
 """
 import ctypes
 
@@ -16,6 +17,7 @@ import pytest
 
 import afid_gpu as ag
 from helpers import Case
+from oracle import afid_oracle as o
 
 pytestmark = pytest.mark.gpu
 
@@ -46,7 +48,19 @@ def test_globals_noalloc_matches_regular_entry_point():
             got = out3.cpu().numpy().copy()
             ref = np.array(gpu.global_quantities(ra_pr))
             np.testing.assert_allclose(got, ref, rtol=1e-12, atol=0.0, err_msg=f"call {call}")
+            assert got[0] == pytest.approx(o.nusselt_volume(case.g, s), rel=1e-12), call
+            assert got[1] == pytest.approx(o.kinetic_energy(case.g, s), rel=1e-12), call
             gpu.time_marcher(1e-3, call)  # a different state for the second call
+            o.time_marcher(case.g, s, 1e-3)
+
+
+def test_globals_noalloc_rejects_bad_arguments():
+    lib = ag.lib()
+    ptrs = (ctypes.c_void_p(8),) * 7
+    # a NaN Rayleigh-Prandtl product is refused like a negative one
+    assert lib.afid_gpu_globals_noalloc(8, 4, 4, 16, 1.0, float("nan"), *ptrs, None) == ag.AFID_E_INVALID
+    assert lib.afid_gpu_globals_noalloc(8, 4, 4, 16, 1.0, -1.0, *ptrs, None) == ag.AFID_E_INVALID
+    assert lib.afid_gpu_globals_noalloc(8, 4, 4, 8, 1.0, 1.0, *ptrs, None) == ag.AFID_E_INVALID  # ldx < nxm+1
 
 
 def test_globals_noalloc_rejects_oversized_grid():
