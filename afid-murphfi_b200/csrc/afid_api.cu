@@ -803,7 +803,7 @@ int afid_gpu_globals(afid_ctx_t *ctx, double ra_pr, double *nu_vol, double *ke, 
   AFID_CUDA(ctx, cudaMemcpyAsync(ctx->host_scratch, ctx->gsum, 3 * sizeof(double), cudaMemcpyDeviceToHost,
                                  ctx->stream));
   int s = check_err_flag(ctx);
-  // GlobalQuantities.F90:27,63-74
+  // GlobalQuantities.F90:35,79,87-91
   const double vol = 1.0 / (ctx->alx3 * g.dx * (double)g.nzm * (double)g.nym);
   if (nu_vol) *nu_vol = 1.0 + std::sqrt(ra_pr) * ctx->host_scratch[0] * vol;
   if (ke) *ke = 0.5 * ctx->host_scratch[1] * vol;

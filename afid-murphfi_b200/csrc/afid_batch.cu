@@ -108,7 +108,7 @@ __global__ void k_batch_advance(int nslots, unsigned char *__restrict__ active, 
   if (limit[i] > 0 && n >= limit[i]) active[i] = 0;
 }
 
-// Volume sums of GlobalQuantities.F90:31-47 per instance: partial[(i*chunks + chunk)*3 + q].
+// Volume sums of GlobalQuantities.F90:39-60 per instance: partial[(i*chunks + chunk)*3 + q].
 __global__ void __launch_bounds__(256)
     k_batch_globals(Geom g, Tables t, const double *__restrict__ vx, const double *__restrict__ vy,
                     const double *__restrict__ vz, const double *__restrict__ temp, double *__restrict__ partial) {
@@ -615,7 +615,7 @@ int afid_batch_stats(afid_batch_t *b, afid_batch_stat_t *stats, double *nu_vol, 
   if (e != cudaSuccess) return ctx_fail(ctx, e);
   int s = afid_gpu_synchronize(ctx);
   if (s != AFID_OK) return s;
-  // GlobalQuantities.F90:27,63-74
+  // GlobalQuantities.F90:35,79,87-91
   const double vol = 1.0 / ((double)b->proto.nxm * (double)b->proto.nym * (double)b->planes);
   for (int i = 0; i < n; ++i) {
     if (stats) {

@@ -614,7 +614,7 @@ __global__ void __launch_bounds__(256)
   }
 }
 
-// Volume sums of GlobalQuantities.F90:31-47 per block, written to partial[block*3 + {0,1,2}]
+// Volume sums of GlobalQuantities.F90:39-60 per block, written to partial[block*3 + {0,1,2}]
 // (T*vx_centre*g3rc, (vx^2+vy^2+vz^2)*g3rc, T*g3rc) and summed in fixed order afterwards.
 __global__ void __launch_bounds__(256)
     k_globals_partial(Geom g, Tables t, const double *__restrict__ vx, const double *__restrict__ vy,

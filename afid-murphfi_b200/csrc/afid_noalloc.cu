@@ -29,7 +29,7 @@ std::mutex g_mu;
 void *g_scratch_addr[kMaxDevices] = {};  // device address of g_noalloc_scratch, per device
 void *g_scratch_ctx[kMaxDevices] = {};   // the context each address was looked up in
 
-// One warp per (j,i) column: the three g3rc-weighted sums of GlobalQuantities.F90:31-47 for
+// One warp per (j,i) column: the three g3rc-weighted sums of GlobalQuantities.F90:39-60 for
 // that column go to partial[3*col + q], so every partial is rewritten on every call.
 __global__ void __launch_bounds__(256)
     k_noalloc_column_sums(int nxm, int nym, int nzm, int ldx, const double *__restrict__ vx,
@@ -63,7 +63,7 @@ __global__ void __launch_bounds__(256)
 }
 
 // Single block: sums the column partials in a fixed order and writes
-// out3 = {1 + sqrt(ra_pr) * vol * sum0, 0.5 * vol * sum1, vol * sum2} (GlobalQuantities.F90:63-74).
+// out3 = {1 + sqrt(ra_pr) * vol * sum0, 0.5 * vol * sum1, vol * sum2} (GlobalQuantities.F90:79, 87-91).
 __global__ void __launch_bounds__(256)
     k_noalloc_finish(const double *__restrict__ partial, long long ncol, double vol, double sqrt_ra_pr,
                      double *__restrict__ out3) {
@@ -148,7 +148,7 @@ extern "C" int afid_gpu_globals_noalloc(int nxm, int nym, int nzm, int ldx, doub
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   double *partial = static_cast<double *>(scratch);
   const double dx = (double)nxm / alx3;
-  const double vol = 1.0 / (alx3 * dx * (double)nzm * (double)nym);  // GlobalQuantities.F90:27
+  const double vol = 1.0 / (alx3 * dx * (double)nzm * (double)nym);  // GlobalQuantities.F90:35
   const double sqrt_ra_pr = std::sqrt(ra_pr);
   // each launch reports its own status (cudaLaunchKernel's return value), so an error left
   // behind by the caller's earlier, unrelated CUDA calls is neither returned nor cleared here

@@ -257,6 +257,10 @@ def run_gpu(args):
     # ---- mixed precision: fields and Nu against an FP64 run with the same dt sequence --------
     accuracy = None
     if w["precision"] == 1 and not args.no_nu_check:
+        # the run continues (untimed) to the workload's full length before the comparison
+        while len(dts) < args.accuracy_steps:
+            step(ntime)
+            ntime += 1
         accuracy = mixed_vs_fp64(ag, w, inp, solver, temp0, list(dts), ra_pr)
 
     # ---- end to end through the C ABI with host buffers -----------------------------------
@@ -296,7 +300,7 @@ def run_gpu(args):
     cpu = None
     parity = None
     if rank == 0 and not args.no_cpu_baseline:
-        cpu = cpu_baseline(w, args.cpu_steps, keep_state=w["precision"] == 0)
+        cpu = cpu_baseline(w, args.cpu_steps, budget_s=args.cpu_budget, keep_state=w["precision"] == 0)
         if "_state" in cpu:
             solver.close()  # room for the replay
             parity = parity_vs_cpu(ag, w, inp, temp0, cpu)
@@ -378,7 +382,7 @@ def mixed_vs_fp64(ag, w, inp, solver, temp0, dts, ra_pr):
     initial state with the same dt sequence (the mixed-precision accuracy gate: Nu within 0.5%)."""
     import numpy as np
     got = solver.download()
-    nu_mx, _, _ = solver.global_quantities(ra_pr)
+    nu_mx, ke_mx, _ = solver.global_quantities(ra_pr)
     t64 = ag.Tables(inp, ag.PREC_FP64)
     ref = ag.Solver(t64.grid, t64.params)
     nx, nym, nzm = w["nxm"] + 1, w["nym"], w["nzm"]
@@ -387,7 +391,7 @@ def mixed_vs_fp64(ag, w, inp, solver, temp0, dts, ra_pr):
     for n, dt in enumerate(dts):
         ref.time_marcher(dt, n)
     exp = ref.download()
-    nu_64, _, _ = ref.global_quantities(ra_pr)
+    nu_64, ke_64, _ = ref.global_quantities(ra_pr)
     ref.close()
     t64.close()
     nxm = w["nxm"]
@@ -398,7 +402,8 @@ def mixed_vs_fp64(ag, w, inp, solver, temp0, dts, ra_pr):
     pa, pb = got["pr"][..., :nxm], exp["pr"][..., :nxm]
     out["pr_mod_mean"] = rel(pa - pa.mean(), pb - pb.mean())
     return {"steps": len(dts), "rel_l2": out, "nu_vol_mixed": nu_mx, "nu_vol_fp64": nu_64,
-            "nu_rel_err": abs(nu_mx - nu_64) / abs(nu_64),
+            "nu_rel_err": abs(nu_mx - nu_64) / abs(nu_64), "ke_mixed": ke_mx, "ke_fp64": ke_64,
+            "ke_rel_err": abs(ke_mx - ke_64) / max(abs(ke_64), 1e-300), "nu_within_half_pct": abs(nu_mx - nu_64) <= 0.005 * abs(nu_64),
             "note": "Nu - 1 is the signal while the flow is still near conduction: see nu_minus_1_rel_err",
             "nu_minus_1_rel_err": abs(nu_mx - nu_64) / max(abs(nu_64 - 1.0), 1e-300)}
 
@@ -931,7 +936,7 @@ def cpu_baseline(w: dict, steps: int, budget_s: float = 60.0, keep_state: bool =
            "sample": f"{res['steps']} full steps of {w['name']} (C+OpenMP restatement)",
            "steps": res["steps"], "seconds": round(res["seconds"], 2)}
     if keep_state:
-        out["_state"], out["_dts"] = res["state"], res["dts"]
+        out["_state"], out["_dts"], out["_stats"] = res["state"], res["dts"], res["stats"]
     return out
 
 
@@ -966,20 +971,41 @@ def restart_io(ag, solver, inp):
 
 
 def parity_vs_cpu(ag, w, inp, temp0, cpu):
-    """The default workload's fields at full size: the GPU path replays the C restatement's dt sequence from
-    the same initial state; relative L2 per field (pressure modulo its mean)."""
+    """The default workload at full size against the C restatement: the GPU path replays its dt
+    sequence from the same initial state.  Fields after the last step: relative L2 per field
+    (pressure modulo its mean).  Over the run: Nu_vol, the plate Nusselt numbers and the kinetic
+    energy after every step (GlobalQuantities; boundary_layers.py:41-54 from the Tbar rows), their
+    largest relative difference and the relative difference of their run averages (gate 1%)."""
     import numpy as np
-    state, dts = cpu.pop("_state"), cpu.pop("_dts")
+    from oracle.cpu_port import plate_and_volume_stats
+    from oracle import afid_oracle as o
+    state, dts, cstats = cpu.pop("_state"), cpu.pop("_dts"), cpu.pop("_stats")
+    p = o.parse_bou_in(bou_text(w, len(dts)))
+    xm = o.create_grid(p).xm
+    ra_pr = w["prat"] * abs(w["rayt"])
     t = ag.Tables(inp, w["precision"])
     sv = ag.Solver(t.grid, t.params)
     nx, nym, nzm = w["nxm"] + 1, w["nym"], w["nzm"]
     zeros = np.zeros((nzm, nym, nx))
     sv.upload(zeros, zeros, zeros, temp0, zeros)
+    gstats = []
     for n, dt in enumerate(dts):
         sv.time_marcher(dt, n)
+        nu, ke, _ = sv.global_quantities(ra_pr)
+        tbar = sv.mean_profiles()["Tbar"]
+        gstats.append(plate_and_volume_stats(p, xm, nu, ke, tbar[0], tbar[w["nxm"] - 1]))
     got = sv.download()
     sv.close()
     t.close()
+    series = {}
+    for k in ("nu_vol", "nu_plate_lower", "nu_plate_upper", "ke"):
+        a = np.array([g[k] for g in gstats])
+        b = np.array([c[k] for c in cstats])
+        series[k] = {"gpu_mean": float(a.mean()), "cpu_mean": float(b.mean()),
+                     "mean_rel_diff": float(abs(a.mean() - b.mean()) / abs(b.mean())),
+                     "max_rel_diff": float(np.max(np.abs(a - b) / np.abs(b))),
+                     "cpu_last": float(b[-1])}
+    series["within_1pct"] = all(v["mean_rel_diff"] <= 0.01 for v in series.values())
 
     def rel(a, b):
         return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
@@ -987,7 +1013,7 @@ def parity_vs_cpu(ag, w, inp, temp0, cpu):
     out = {f: rel(got[f], state[f]) for f in ("vx", "vy", "vz", "temp")}
     pa, pb = got["pr"][..., :nxm], state["pr"][..., :nxm]
     out["pr_mod_mean"] = rel(pa - pa.mean(), pb - pb.mean())
-    return {"steps": len(dts), "rel_l2": out, "tolerance": 1e-10,
+    return {"steps": len(dts), "rel_l2": out, "tolerance": 1e-10, "nu_ke_over_run": series,
             "against": "C + OpenMP restatement (oracle/afid_cpu.c), same initial state and dt sequence"}
 
 
@@ -1040,13 +1066,17 @@ def main():
     ap.add_argument("--config", default="rbc3d",
                     choices=sorted(WORKLOADS) + sorted(DDC_WORKLOADS) + ["batched", "batched_fp64", "served"])
     ap.add_argument("--no-nu-check", action="store_true")
+    ap.add_argument("--accuracy-steps", type=int, default=500,
+                    help="rbc3d_mixed: steps of the mixed run compared with the FP64 replay (500 = the full run)")
     ap.add_argument("--k1-shape", type=int, default=-1, help="fixed K1 thread shape instead of autotuning")
     ap.add_argument("--jobs", type=int, default=100, help="served: number of jobs")
     ap.add_argument("--chunk", type=int, default=25, help="served: steps per pump")
     ap.add_argument("--slots", type=int, default=32, help="served: 2-D slots per pool")
     ap.add_argument("--max-cells", type=int, default=16_000_000, help="served: cells-in-flight cap (0 = memory only)")
     ap.add_argument("--policy", default="shortest", choices=["fifo", "shortest"])
-    ap.add_argument("--cpu-steps", type=int, default=10)
+    ap.add_argument("--cpu-steps", type=int, default=10,
+                    help="steps of the CPU baseline (and of the GPU replay compared with it)")
+    ap.add_argument("--cpu-budget", type=float, default=60.0, help="seconds of CPU-baseline steps at most")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--restart-io", action="store_true", help="rbc3d: time writing and reading the restart files")
     ap.add_argument("--instances", type=int, default=256,

@@ -28,7 +28,7 @@ typedef struct {
   int active_t, gaxis, inslws, inslwn, tfixs, tfixn;
   /* tables (0-based copies of the reference arrays) */
   double *udx3c, *udx3m, *idx, *ap3ck, *ac3ck, *am3ck, *ap3sk, *ac3sk, *am3sk, *ap3ssk, *ac3ssk,
-      *am3ssk, *amphk, *acphk, *apphk, *ak1, *ak2, *tempbp, *temptp;
+      *am3ssk, *amphk, *acphk, *apphk, *ak1, *ak2, *tempbp, *temptp, *g3rc;
   /* state */
   double *vx, *vy, *vz, *temp, *pr, *rux, *ruy, *ruz, *rut;
   double *qcap, *dph, *dq, *hro, *phi;
@@ -203,6 +203,7 @@ afid_cpu_t *afid_cpu_create(int nxm, int nym, int nzm, double ylen, double zlen,
   c->amphk = dup(tab[11], nx); c->acphk = dup(tab[12], nx); c->apphk = dup(tab[13], nx);
   c->ak1 = dup(tab[14], nzm); c->ak2 = dup(tab[15], nym);
   c->tempbp = dup(tab[16], nym * nzm); c->temptp = dup(tab[17], nym * nzm);
+  c->g3rc = dup(tab[18], nx);
   c->idx = (double *)malloc(sizeof(double) * nx);
   for (int k = 0; k < nxm; ++k) c->idx[k] = 1.0 / c->udx3m[k];
   size_t n = (size_t)nx * nym * nzm;
@@ -222,7 +223,7 @@ void afid_cpu_destroy(afid_cpu_t *c) {
   if (!c) return;
   double *a[] = {c->udx3c, c->udx3m, c->idx, c->ap3ck, c->ac3ck, c->am3ck, c->ap3sk, c->ac3sk, c->am3sk,
                  c->ap3ssk, c->ac3ssk, c->am3ssk, c->amphk, c->acphk, c->apphk, c->ak1, c->ak2,
-                 c->tempbp, c->temptp, c->vx, c->vy, c->vz, c->temp, c->pr, c->rux, c->ruy, c->ruz,
+                 c->tempbp, c->temptp, c->g3rc, c->vx, c->vy, c->vz, c->temp, c->pr, c->rux, c->ruy, c->ruz,
                  c->rut, c->qcap, c->dph, c->dq, c->hro, c->phi};
   for (size_t q = 0; q < sizeof a / sizeof a[0]; ++q) free(a[q]);
   free(c->spec); free(c->twy); free(c->twz);
@@ -560,6 +561,38 @@ double afid_cpu_cfl(const afid_cpu_t *c) {
     }
   }
   return m;
+}
+
+/* GlobalQuantities.F90:35-79, 87-91 and the first and last rows of CalcMeanProfiles' Tbar
+ * (CalcMeanProfiles.F90:48-50, 88): out = {Nu_vol, kinetic energy 0.5 <|u|^2> (g3rc-weighted),
+ * Tbar(1), Tbar(nxm)}; ra_pr = Pr*|Ra|.  Column sums are accumulated in column order. */
+void afid_cpu_stats(const afid_cpu_t *c, double ra_pr, double *out) {
+  const int nxm = c->nxm, nym = c->nym, nzm = c->nzm, ncol = nym * nzm;
+  double *part = (double *)calloc((size_t)ncol * 4, sizeof(double));
+#pragma omp parallel for schedule(static)
+  for (int col = 0; col < ncol; ++col) {
+    const int j = col % nym, i = col / nym;
+    double anu = 0.0, ke = 0.0;
+    for (int k = 0; k < nxm; ++k) {
+      const size_t q = IDX(c, k, j, i);
+      const double fac2 = c->g3rc[k];
+      anu += c->temp[q] * ((c->vx[q] + c->vx[q + 1]) * 0.5) * fac2;
+      ke += fac2 * (c->vz[q] * c->vz[q] + c->vy[q] * c->vy[q] + c->vx[q] * c->vx[q]);
+    }
+    part[4 * col + 0] = anu;
+    part[4 * col + 1] = ke;
+    part[4 * col + 2] = c->temp[IDX(c, 0, j, i)];
+    part[4 * col + 3] = c->temp[IDX(c, nxm - 1, j, i)];
+  }
+  double sum[4] = {0.0, 0.0, 0.0, 0.0};
+  for (int col = 0; col < ncol; ++col)
+    for (int q = 0; q < 4; ++q) sum[q] += part[4 * col + q];
+  free(part);
+  const double vol = 1.0 / ((double)nxm * (double)nzm * (double)nym);  /* alx3 * dx = nxm */
+  out[0] = 1.0 + sqrt(ra_pr) * sum[0] * vol;
+  out[1] = 0.5 * sum[1] * vol;
+  out[2] = sum[2] / ((double)nym * (double)nzm);
+  out[3] = sum[3] / ((double)nym * (double)nzm);
 }
 
 /* ============================================================================================

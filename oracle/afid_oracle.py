@@ -920,7 +920,7 @@ def check_divergence(g: Grid, s: State) -> float:
 
 
 def nusselt_volume(g: Grid, s: State) -> float:
-    """Volume Nusselt number of ``GlobalQuantities.F90:27-67``:
+    """Volume Nusselt number of ``GlobalQuantities.F90:35-79``:
     1 + sqrt(Pr*|Ra|) * vol * sum(T * (vx_k + vx_{k+1})/2 * g3rc_k)."""
     p = g.p
     nxm = p.nxm
@@ -931,7 +931,7 @@ def nusselt_volume(g: Grid, s: State) -> float:
 
 
 def kinetic_energy(g: Grid, s: State) -> float:
-    """Volume-mean 0.5*(vx^2+vy^2+vz^2), g3rc-weighted as ``GlobalQuantities.F90:40-50``."""
+    """Volume-mean 0.5*(vx^2+vy^2+vz^2), g3rc-weighted as ``GlobalQuantities.F90:53-57, 91``."""
     p = g.p
     nxm = p.nxm
     vol = 1.0 / (p.alx3 * g.dx * float(p.nzm) * float(p.nym))

@@ -30,6 +30,7 @@ def lib():
         _lib.afid_cpu_cfl.restype = C.c_double
         _lib.afid_cpu_cfl.argtypes = [C.c_void_p]
         _lib.afid_cpu_threads.restype = C.c_int
+        _lib.afid_cpu_stats.argtypes = [C.c_void_p, C.c_double, C.POINTER(C.c_double)]
     return _lib
 
 
@@ -68,6 +69,15 @@ class CpuSolver:
     def cfl(self):
         return lib().afid_cpu_cfl(self._h)
 
+    def stats(self) -> dict:
+        """Volume Nusselt number and kinetic energy (GlobalQuantities) and the plate Nusselt
+        numbers from the first and last Tbar rows, as the reference's post-processing forms
+        them (tools/afidtools/boundary_layers.py:41-54)."""
+        p, g = self.g.p, self.g
+        out = (C.c_double * 4)()
+        lib().afid_cpu_stats(self._h, p.prat * abs(p.rayt), out)
+        return plate_and_volume_stats(p, g.xm, out[0], out[1], out[2], out[3])
+
     def get(self):
         p = self.g.p
         out = {}
@@ -89,41 +99,61 @@ class CpuSolver:
             pass
 
 
+def plate_and_volume_stats(p, xm, nu_vol: float, ke: float, tbar_lo: float, tbar_up: float) -> dict:
+    """Nu_vol and KE as given; the plate Nusselt numbers of boundary_layers.py:41-54 from the
+    first and last Tbar rows (plates at T = +-0.5, the sign flipped for Ra > 0; a zero-flux
+    plate gives 0)."""
+    nxm = p.nxm
+    tup, tlo = (-0.5, 0.5) if p.rayt > 0 else (0.5, -0.5)
+    lo = (tbar_lo - tlo) / xm[0] if p.tfixs else 0.0
+    up = (tup - tbar_up) / (1.0 - xm[nxm - 1]) if p.tfixn else 0.0
+    if p.rayt > 0:
+        lo, up = -lo, -up
+    return {"nu_vol": float(nu_vol), "ke": float(ke), "nu_plate_lower": float(lo), "nu_plate_upper": float(up)}
+
+
 def time_steps(bou_text: str, steps: int, seed: int = 20261203, mixed: bool = False,
                budget_s: float = 1e30, keep_state: bool = False, warmup: int = 0) -> dict:
     """Main-loop steps (CFL -> dt rule -> TimeMarcher) of the C restatement on all host cores,
     from the seeded initial state: ``warmup`` untimed steps, then up to ``steps`` timed ones,
     stopping early once ``budget_s`` seconds of timed steps have been spent; returns the
     throughput in Mcell-RK3-steps/s and the steps actually timed (with ``keep_state``, also the
-    final fields and the dt of every step, warm-up steps included)."""
+    final fields, the dt of every step and the Nusselt numbers and kinetic energy after every
+    step, warm-up steps included; the statistics are taken outside the timed interval)."""
     p = o.parse_bou_in(bou_text)
     g = o.create_grid(p)
     s = o.initial_state(g, seed)
     cpu = CpuSolver(g, s)
     dt = p.dt
-    dts = []
+    dts, stats = [], []
     for n in range(warmup):
         cflm = cpu.cfl()
         dt, _, _ = o.next_dt(p, n, dt, cflm)
         cpu.time_marcher(dt)
         dts.append(dt)
-    t0 = time.perf_counter()
+        if keep_state:
+            stats.append(cpu.stats())
+    sec = 0.0
     done = 0
     for n in range(warmup, warmup + steps):
+        t0 = time.perf_counter()
         cflm = cpu.cfl()
         dt, _, _ = o.next_dt(p, n, dt, cflm)
         cpu.time_marcher(dt)
+        sec += time.perf_counter() - t0
         dts.append(dt)
         done += 1
-        if time.perf_counter() - t0 > budget_s:
+        if keep_state:
+            stats.append(cpu.stats())
+        if sec > budget_s:
             break
-    sec = time.perf_counter() - t0
     cells = p.nxm * p.nym * p.nzm
     res = {"seconds": sec, "steps": done, "mcells_per_s": cells * done / sec / 1e6,
            "threads": lib().afid_cpu_threads()}
     if keep_state:
         res["state"] = cpu.get()
         res["dts"] = dts
+        res["stats"] = stats
     cpu.close()
     return res
 

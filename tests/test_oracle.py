@@ -151,6 +151,12 @@ def test_c_restatement_matches_numpy_oracle(shape):
     assert rel_l2(out["temp"][..., :nxm], s.temp[..., :nxm]) < 1e-13
     assert rel_l2_mod_mean(out["pr"][..., :nxm], s.pr[..., :nxm]) < 1e-11
     assert cpu.cfl() == pytest.approx(o.calc_max_cfl(g, s), rel=1e-13)
+    st = cpu.stats()
+    assert st["nu_vol"] == pytest.approx(o.nusselt_volume(g, s), rel=1e-13)
+    assert st["ke"] == pytest.approx(o.kinetic_energy(g, s), rel=1e-13)
+    tbar = o.mean_profiles(g, s)["Tbar"]
+    assert st["nu_plate_lower"] == pytest.approx(-(tbar[0] - 0.5) / g.xm[0], rel=1e-13)
+    assert st["nu_plate_upper"] == pytest.approx(-(-0.5 - tbar[nxm - 1]) / (1.0 - g.xm[nxm - 1]), rel=1e-13)
 
 
 @pytest.mark.parametrize("path", sorted(glob.glob(os.path.join(HERE, "golden", "*.npz"))))
