@@ -32,6 +32,7 @@ AFID_E_INVALID = 603
 AFID_E_CUDA = 604
 AFID_E_CAPACITY = 605
 AFID_E_IO = 606
+AFID_E_CANCELLED = 607
 PREC_FP64 = 0
 PREC_MIXED = 1
 
@@ -163,8 +164,9 @@ EXPORTS = [
     "afid_batch_set_limit",
     "afid_batch_device_bytes", "afid_batch_launch_count",
     "afid_serve_create", "afid_serve_destroy", "afid_serve_submit", "afid_serve_pump", "afid_serve_poll",
+    "afid_serve_cancel",
     "afid_serve_status", "afid_serve_now", "afid_gpu_autotune", "afid_batch_autotune",
-    "afid_gpu_set_k1_shape", "afid_gpu_mean_profiles", "afid_batch_mean_profiles",
+    "afid_gpu_set_k1_shape", "afid_gpu_set_wait_test", "afid_gpu_mean_profiles", "afid_batch_mean_profiles",
     "afid_batch_divmax", "afid_gpu_spectra_reset", "afid_gpu_spectra_update", "afid_gpu_spectra_read", "afid_gpu_slice",
     "afid_mgrd_create", "afid_mgrd_destroy", "afid_mgrd_view", "afid_mgrd_fast", "afid_mgrd_array",
     "afid_initial_salinity", "afid_gpu_sal_create", "afid_gpu_sal_upload", "afid_gpu_sal_download",
@@ -244,11 +246,13 @@ def load_library(path: str = _LIB_PATH) -> C.CDLL:
         "afid_serve_destroy": (i, [vp]),
         "afid_serve_submit": (i, [vp, C.POINTER(ServeJobT)]),
         "afid_serve_pump": (i, [vp]),
+        "afid_serve_cancel": (i, [vp, C.c_uint64]),
         "afid_serve_poll": (i, [vp, C.POINTER(ServeResultT), i, C.POINTER(i)]),
         "afid_serve_status": (i, [vp, C.POINTER(ServeStatusT)]),
         "afid_serve_now": (d, [vp]),
         "afid_gpu_autotune": (i, [vp, i, C.POINTER(TuneInfoT)]),
         "afid_gpu_set_k1_shape": (i, [vp, i]),
+        "afid_gpu_set_wait_test": (i, [vp, C.c_longlong]),
         "afid_gpu_mean_profiles": (i, [vp, _dp]),
         "afid_gpu_spectra_reset": (i, [vp]),
         "afid_gpu_spectra_update": (i, [vp, d]),
@@ -603,6 +607,10 @@ class Solver:
     def set_k1_shape(self, index: int) -> None:
         _check(lib().afid_gpu_set_k1_shape(self._h, index), "afid_gpu_set_k1_shape")
 
+    def set_wait_test(self, polls: int) -> None:
+        """Test hook: make the bounded staging wait run out after `polls` polls (0 = off)."""
+        _check(lib().afid_gpu_set_wait_test(self._h, polls), "afid_gpu_set_wait_test")
+
     def profile(self, enable: bool = True) -> None:
         _check(lib().afid_gpu_profile_enable(self._h, int(enable)), "afid_gpu_profile_enable")
 
@@ -762,6 +770,10 @@ class Server:
 
     def pump(self) -> None:
         _check(lib().afid_serve_pump(self._h), "afid_serve_pump")
+
+    def cancel(self, tag: int) -> None:
+        """afid_serve_cancel: the job comes back as a result with errorcode AFID_E_CANCELLED."""
+        _check(lib().afid_serve_cancel(self._h, C.c_uint64(tag)), "afid_serve_cancel")
 
     def poll(self, max_results: int = 1024) -> list:
         buf = (ServeResultT * max_results)()

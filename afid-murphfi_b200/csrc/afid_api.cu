@@ -306,6 +306,7 @@ const char *afid_gpu_status_string(int s) {
     case AFID_E_CUDA: return "CUDA runtime error";
     case AFID_E_CAPACITY: return "capacity exhausted";
     case AFID_E_IO: return "restart file missing, unreadable or unsupported";
+    case AFID_E_CANCELLED: return "job cancelled";
   }
   return "unknown status";
 }
@@ -704,6 +705,12 @@ int afid_gpu_set_stream(afid_ctx_t *ctx, void *stream) {
 }
 
 void *afid_gpu_get_stream(afid_ctx_t *ctx) { return ctx ? (void *)ctx->stream : nullptr; }
+
+int afid_gpu_set_wait_test(afid_ctx_t *ctx, long long polls) {
+  if (!ctx || polls < 0 || polls > (1LL << 24)) return AFID_E_INVALID;
+  ctx->L.g.wait_test_polls = polls;
+  return AFID_OK;
+}
 
 int afid_gpu_synchronize(afid_ctx_t *ctx) {
   if (!ctx) return AFID_E_INVALID;

@@ -39,11 +39,11 @@ __global__ void __launch_bounds__(256)
     for (int k = lane; k < g.nxm; k += 32) {
       const double q = fabs((vz[c + k] + vz[cip + k]) * 0.5 * g.dz) + fabs((vy[c + k] + vy[cjp + k]) * 0.5 * g.dy) +
                        fabs((vx[c + k] + vx[c + k + 1]) * 0.5 * t.udx3m[k]);
-      m = fmax(m, q);
+      m = nan_max(m, q);
     }
   }
 #pragma unroll
-  for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+  for (int o = 16; o > 0; o >>= 1) m = nan_max(m, __shfl_xor_sync(0xffffffffu, m, o));
   if (lane == 0) atomicMax(out + i, (unsigned long long)__double_as_longlong(m));
 }
 
@@ -61,11 +61,11 @@ __global__ void __launch_bounds__(256)
     for (int k = lane; k < g.nxm; k += 32) {
       const double dq = (vz[cip + k] - vz[c + k]) * g.dz + (vy[cjp + k] - vy[c + k]) * g.dy +
                         (vx[c + k + 1] - vx[c + k]) * t.udx3m[k];
-      m = fmax(m, fabs(dq));
+      m = nan_max(m, fabs(dq));
     }
   }
 #pragma unroll
-  for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+  for (int o = 16; o > 0; o >>= 1) m = nan_max(m, __shfl_xor_sync(0xffffffffu, m, o));
   if (lane == 0) atomicMax(out + i, (unsigned long long)__double_as_longlong(m));
 }
 
@@ -80,7 +80,7 @@ __global__ void k_batch_dt(int nslots, unsigned char *__restrict__ active, const
     active[i] = 0;
     return;
   }
-  const double cflm = fmax(0.00000001, __longlong_as_double((long long)cfl_bits[i]));  // CalcMaxCFL.F90:22
+  const double cflm = nan_max(0.00000001, __longlong_as_double((long long)cfl_bits[i]));  // CalcMaxCFL.F90:22
   const InstCtl c = ctl[i];
   double d = dt[i];
   if (c.idtv == 1) {
@@ -88,10 +88,10 @@ __global__ void k_batch_dt(int nslots, unsigned char *__restrict__ active, const
       d = (cflm < 1.0e-8) ? c.dtmax : c.limit_cfl / cflm;
       if (d > c.dtmax) d = c.dtmax;
     }
-    if (d < c.dtmin) err[i] = AFID_E_DTMIN;
+    if (!(d >= c.dtmin)) err[i] = AFID_E_DTMIN;  // a NaN CFL gives a NaN dt: refused too
     cfl[i] = cflm;
   } else {
-    if (cflm * d > c.limit_cfl) err[i] = AFID_E_CFL;
+    if (!(cflm * d <= c.limit_cfl)) err[i] = AFID_E_CFL;
     cfl[i] = cflm * d;
   }
   dt[i] = d;

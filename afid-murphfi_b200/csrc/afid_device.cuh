@@ -37,6 +37,10 @@ struct Geom {
   // bycs * salc at rows 0..nxm-1; nullptr when no active salinity is coupled.
   const double *salc;
   double bycs;
+  // Test hook of the bounded waits (afid_gpu_set_wait_test): when non-zero, K1's staging wait
+  // also waits for an mbarrier phase that nothing completes, for at most this many polls, so
+  // the timeout path runs; 0 in normal operation.
+  long long wait_test_polls;
 };
 
 // Shared-memory stride of the chunked tridiagonal layout (row r of a 32-chunk system at
@@ -399,9 +403,15 @@ __device__ __forceinline__ void warp_fft(typename Cplx<T>::type (&x)[N1], int la
 
 // ------------------------------------------------------------------------------------------
 // Bounded device-side waits: every spin in this library counts iterations and gives up with
-// an error flag instead of hanging (no trap, no unbounded loop).
+// an error flag instead of hanging (no trap, no unbounded loop).  A wait that gave up drains
+// the copies still in flight with kDrainLimit polls before its block exits.
 // ------------------------------------------------------------------------------------------
 constexpr long long kSpinLimit = 1LL << 22;
+constexpr long long kDrainLimit = 1LL << 28;
+
+// Maximum that propagates NaN (fmax drops it): a NaN anywhere in a CFL or divergence
+// reduction makes the result NaN, which the main-loop checks turn into an error code.
+__device__ __forceinline__ double nan_max(double a, double b) { return (b > a || b != b) ? b : a; }
 
 // 1-D TMA bulk copies global -> shared, completed on an mbarrier (sm_90+ PTX, no tensor map,
 // no multicast).  Source and destination must be 16-byte aligned, size a multiple of 16.

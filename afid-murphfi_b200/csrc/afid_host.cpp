@@ -610,11 +610,11 @@ int afid_next_dt(const afid_input_t *in, int ntime, double *dt, double cflm, dou
         *dt = (cflm < 1.0e-8) ? in->dtmax : in->limit_cfl / cflm;
         if (*dt > in->dtmax) *dt = in->dtmax;
       }
-      if (*dt < in->dtmin) err = AFID_E_DTMIN;
+      if (!(*dt >= in->dtmin)) err = AFID_E_DTMIN;  // also a NaN dt from a NaN CFL
       if (cfl_report) *cfl_report = cflm;
     } else {  // main.F90:297-298
       const double c = cflm * (*dt);
-      if (c > in->limit_cfl) err = AFID_E_CFL;
+      if (!(c <= in->limit_cfl)) err = AFID_E_CFL;  // also a NaN CFL
       if (cfl_report) *cfl_report = c;
     }
     return err;
@@ -702,7 +702,7 @@ int afid_run_io(const afid_input_t *in, int precision, uint64_t seed, int nsteps
         double dmax = 0.0;
         if ((s = afid_gpu_divmax(ctx, &dmax)) != AFID_OK) break;
         st.divmax = dmax;
-        if (std::fabs(dmax) > in->resid) errorcode = AFID_E_DIVERGENCE;
+        if (!(std::fabs(dmax) <= in->resid)) errorcode = AFID_E_DIVERGENCE;  // NaN included
       }
       if (stats_every > 0 && cb && ((ntime + 1) % stats_every == 0)) {
         double nu = 0, ke = 0;

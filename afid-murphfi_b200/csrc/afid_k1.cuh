@@ -378,10 +378,12 @@ __global__ void __launch_bounds__(TPC, k1_min_blocks<CAP, TPC>())
     vv[p][2] = in ? __ldg(pr + o_jm + k) : 0.0;
     if constexpr (SAL) sbv[p] = in ? g.bycs * __ldg(g.salc + c0 + k) : 0.0;
   }
-  const bool ok = mbar_wait(&bar, 0, kSpinLimit);
+  bool ok = mbar_wait(&bar, 0, kSpinLimit);
+  // test hook: phase 1 of the barrier is never completed, so this wait always runs out
+  if (g.wait_test_polls > 0) ok = ok && mbar_wait(&bar, 1, g.wait_test_polls);
   if (!__syncthreads_and(ok)) {
     if (tc == 0) atomicOr(err, 2);
-    mbar_wait(&bar, 0, kSpinLimit);  // let copies in flight land before the block exits
+    mbar_wait(&bar, 0, kDrainLimit);  // let copies in flight land before the block exits
     return;
   }
   auto C = [&](int q) { return (const double *)(cols + q * CS); };

@@ -569,7 +569,7 @@ __global__ void __launch_bounds__(256)
 // ------------------------------------------------------------------------------------------
 __device__ __forceinline__ double warp_max(double v) {
 #pragma unroll
-  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+  for (int o = 16; o > 0; o >>= 1) v = nan_max(v, __shfl_xor_sync(0xffffffffu, v, o));
   return v;
 }
 __device__ __forceinline__ double warp_sum(double v) {
@@ -601,7 +601,7 @@ __global__ void __launch_bounds__(256)
         q = fabs((vz[c + k] + vz[cip + k]) * 0.5 * g.dz) + fabs((vy[c + k] + vy[cjp + k]) * 0.5 * g.dy) +
             fabs((vx[c + k] + vx[c + k + 1]) * 0.5 * t.udx3m[k]);
       }
-      m = fmax(m, q);
+      m = nan_max(m, q);
     }
   }
   m = warp_max(m);

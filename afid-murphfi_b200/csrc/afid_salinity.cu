@@ -482,16 +482,16 @@ __global__ void __launch_bounds__(256)
       const double q = fabs((__ldg(vzr + o + k) + __ldg(vzr + oip + k)) * 0.5 * sg.dzr) +
                        fabs((__ldg(vyr + o + k) + __ldg(vyr + ojp + k)) * 0.5 * sg.dyr) +
                        fabs((__ldg(vxr + o + k) + __ldg(vxr + o + k + 1)) * 0.5 * __ldg(st.udx3mr + k));
-      m = fmax(m, q);
+      m = nan_max(m, q);
     }
   }
 #pragma unroll
-  for (int h = 16; h > 0; h >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, h));
+  for (int h = 16; h > 0; h >>= 1) m = nan_max(m, __shfl_xor_sync(0xffffffffu, m, h));
   __shared__ double wm[8];
   if ((threadIdx.x & 31) == 0) wm[threadIdx.x >> 5] = m;
   __syncthreads();
   if (threadIdx.x == 0) {
-    for (int w = 1; w < (int)(blockDim.x >> 5); ++w) m = fmax(m, wm[w]);
+    for (int w = 1; w < (int)(blockDim.x >> 5); ++w) m = nan_max(m, wm[w]);
     atomicMax(out, (unsigned long long)__double_as_longlong(m));
   }
 }

@@ -53,6 +53,7 @@ struct Job {
   double t_submit = 0.0, t_admit = 0.0;
   long long cells = 0;
   long long order = 0;  // submission number
+  bool cancelled = false;  // afid_serve_cancel on a running job: finish at the next harvest
 };
 
 struct Pool {
@@ -223,7 +224,7 @@ int harvest(afid_server_t *s, Pool *p) {
     if (idx < 0) continue;
     Job &j = s->running[idx];
     const afid_batch_stat_t &x = s->st[i];
-    if (x.ntime < j.spec.nsteps && x.errorcode == 0) continue;
+    if (x.ntime < j.spec.nsteps && x.errorcode == 0 && !j.cancelled) continue;
     if (j.spec.temp_out) {
       const int nx = j.spec.in.nxm + 1;
       st = afid_batch_download(p->b, i, nullptr, nullptr, nullptr, j.spec.temp_out, nullptr, nx, j.spec.in.nym);
@@ -231,7 +232,7 @@ int harvest(afid_server_t *s, Pool *p) {
     }
     afid_serve_result_t r{};
     r.tag = j.spec.tag;
-    r.errorcode = x.errorcode;
+    r.errorcode = j.cancelled ? AFID_E_CANCELLED : x.errorcode;
     r.steps_done = x.ntime;
     r.time = x.time;
     r.dt = x.dt;
@@ -248,9 +249,29 @@ int harvest(afid_server_t *s, Pool *p) {
     p->job[i] = -1;
     p->active[i] = 0;
     p->dirty = true;
+    j.cancelled = false;
     s->free_running.push_back(idx);
   }
   return AFID_OK;
+}
+
+bool has_cancelled(const afid_server_t *s, const Pool *p) {
+  for (int idx : p->job)
+    if (idx >= 0 && s->running[idx].cancelled) return true;
+  return false;
+}
+
+// Device bytes of a pool's state arrays for a job of this input: nine FP64 field arrays (state
+// and intermediates), four RK3 histories and phi at the explicit-term width, and the complex half
+// spectrum (the layout afid_batch_create allocates; its 1-D tables and per-slot records come on
+// top).  A lower bound of the pool's footprint.
+long long pool_state_bytes(const afid_server_t *s, const afid_input_t &in) {
+  const long long slots = in.nzm > 1 ? 1 : std::max(1, s->cfg.slots_per_pool);
+  const long long planes = in.nzm > 1 ? in.nzm : slots;
+  const long long ldx = (in.nxm + 1 + 7) / 8 * 8, ldxc = (in.nxm + 3) / 4 * 4;
+  const long long tsz = s->cfg.precision == AFID_PREC_MIXED ? 4 : 8;
+  const long long nf = ldx * in.nym * planes, nspec = ldxc * (in.nym / 2 + 1) * planes;
+  return nf * (9 * 8 + 5 * tsz) + nspec * 2 * tsz;
 }
 
 }  // namespace
@@ -286,6 +307,8 @@ int afid_serve_submit(afid_server_t *s, const afid_serve_job_t *job) {
     if (!s || !job || job->nsteps < 1 || job->in.nxm < 2 || job->in.nym < 1 || job->in.nzm < 1 ||
         job->in.dpdz != 0.0 || job->in.flagsal)
       return AFID_E_INVALID;  // served jobs carry no salinity
+    // a job whose pool cannot fit the budget even empty is refused here, not queued
+    if (pool_state_bytes(s, job->in) > s->cfg.hbm_budget_bytes) return AFID_E_CAPACITY;
     Job j;
     j.spec = *job;
     j.t_submit = now_s(s);
@@ -357,9 +380,15 @@ int afid_serve_pump(afid_server_t *s) {
     for (size_t i = 0; i < s->queue.size(); ++i)
       if (!taken[i]) rest.push_back(s->queue[i]);
     s->queue.swap(rest);
-    // 3. next chunk on every idle pool with running jobs
+    // 3. next chunk on every idle pool with running jobs (cancelled jobs leave first)
     for (Pool *p : s->pools) {
       if (p->in_flight || p->busy() == 0) continue;
+      if (has_cancelled(s, p)) {
+        const int hs = harvest(s, p);
+        if (hs != AFID_OK) return hs;
+        progress = true;
+        if (p->busy() == 0) continue;
+      }
       int st = AFID_OK;
       if (p->dirty) {
         st = afid_batch_set_active(p->b, p->active.data());
@@ -383,6 +412,30 @@ int afid_serve_pump(afid_server_t *s) {
       }
     }
     return AFID_OK;
+  });
+}
+
+int afid_serve_cancel(afid_server_t *s, uint64_t tag) {
+  return afid_guard([&]() -> int {
+    if (!s) return AFID_E_INVALID;
+    for (auto it = s->queue.begin(); it != s->queue.end(); ++it)
+      if (it->spec.tag == tag) {
+        afid_serve_result_t r{};
+        r.tag = tag;
+        r.errorcode = AFID_E_CANCELLED;
+        r.t_submit = it->t_submit;
+        r.t_admit = r.t_done = now_s(s);
+        s->done.push_back(r);
+        s->queue.erase(it);
+        return AFID_OK;
+      }
+    for (const Pool *p : s->pools)
+      for (int idx : p->job)
+        if (idx >= 0 && s->running[idx].spec.tag == tag && !s->running[idx].cancelled) {
+          s->running[idx].cancelled = true;  // finished at the pool's next harvest
+          return AFID_OK;
+        }
+    return AFID_E_INVALID;
   });
 }
 

@@ -628,7 +628,7 @@ def run_served(args):
     import afid_gpu as ag
 
     world, rank, local = dist_setup()
-    jobs = serve_jobs(args.jobs)
+    jobs = serve_jobs(args.jobs, rate=args.rate)
     inputs = [ag.parse_bou_in(serve_bou(j)) for j in jobs]
     policy = ag.SERVE_SHORTEST_FIRST if args.policy == "shortest" else ag.SERVE_FIFO
     free, _ = torch.cuda.mem_get_info()
@@ -685,8 +685,9 @@ def run_served(args):
             "scaling": "weak",
             "vs_baseline": None,
             "dtype": "f32+f64",
-            "data": "synthetic: Poisson arrivals (50/s), Philox-drawn 2-D/3-D RBC jobs, seeded conductive IC",
-            "config": {"workload": f"served_{len(jobs)}jobs_poisson50", "jobs": len(jobs),
+            "data": f"synthetic: Poisson arrivals ({args.rate:g}/s), Philox-drawn 2-D/3-D RBC jobs, seeded conductive IC",
+            "config": {"workload": f"served_{len(jobs)}jobs_poisson{args.rate:g}", "jobs": len(jobs),
+                       "arrival_rate_per_s": args.rate,
                        "mix": {"2d": sum(1 for j in jobs if j["nzm"] == 1), "3d_96x128x128": sum(1 for j in jobs if j["nzm"] > 1)},
                        "policy": args.policy, "chunk_steps": args.chunk, "slots_per_pool": args.slots,
                        "max_cells_in_flight": args.max_cells, "hbm_budget_bytes": budget,
@@ -1070,6 +1071,9 @@ def main():
                     help="rbc3d_mixed: steps of the mixed run compared with the FP64 replay (500 = the full run)")
     ap.add_argument("--k1-shape", type=int, default=-1, help="fixed K1 thread shape instead of autotuning")
     ap.add_argument("--jobs", type=int, default=100, help="served: number of jobs")
+    ap.add_argument("--rate", type=float, default=50.0,
+                    help="served: Poisson arrival rate per second (50 = the benchmark's stream, ~16x capacity; "
+                         "2 offers ~0.6 of capacity)")
     ap.add_argument("--chunk", type=int, default=25, help="served: steps per pump")
     ap.add_argument("--slots", type=int, default=32, help="served: 2-D slots per pool")
     ap.add_argument("--max-cells", type=int, default=16_000_000, help="served: cells-in-flight cap (0 = memory only)")

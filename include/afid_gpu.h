@@ -34,8 +34,8 @@ extern "C" {
 /* ---- status codes: the reference's errorcode values where one matches ----------------- */
 #define AFID_OK 0
 #define AFID_E_ALLOC 8           /* allocation failure (AuxiliaryRoutines.F90:88-91)          */
-#define AFID_E_CFL 165           /* CFL*dt > CFLMAX with fixed dt (main.F90:297-298)          */
-#define AFID_E_DTMIN 166         /* dt < dtmin with variable dt (main.F90:302)                */
+#define AFID_E_CFL 165           /* CFL*dt > CFLMAX with fixed dt (main.F90:300-302)          */
+#define AFID_E_DTMIN 166         /* dt < dtmin with variable dt (main.F90:298)                */
 #define AFID_E_DIVERGENCE 169    /* max|div u| > resid (main.F90:357)                         */
 #define AFID_E_FFTSIZE 444       /* nym/nzm with a prime factor > 5 (main.F90:272-279)        */
 #define AFID_E_SINGULAR 601      /* zero pivot in a Poisson mode (pressure.F90:225-229)       */
@@ -44,6 +44,7 @@ extern "C" {
 #define AFID_E_CUDA 604          /* CUDA runtime error (afid_gpu_cuda_error gives the code)   */
 #define AFID_E_CAPACITY 605      /* batch/server slots, HBM budget or a fixed scratch array exhausted */
 #define AFID_E_IO 606            /* restart file missing, unreadable or of an unsupported layout */
+#define AFID_E_CANCELLED 607     /* a served job cancelled by the caller (afid_serve_cancel)   */
 
 /* precision of the explicit terms and transforms (the implicit solves are always FP64) */
 #define AFID_PREC_FP64 0
@@ -171,6 +172,13 @@ int afid_gpu_autotune(afid_ctx_t *ctx, int force, afid_tune_info_t *info);
 /* Use shape `index` (0 .. ncand-1) from now on without timing, e.g. one saved from an earlier
  * afid_gpu_autotune on the same device and sizes. */
 int afid_gpu_set_k1_shape(afid_ctx_t *ctx, int index);
+/* Test hook of the bounded device waits (no counterpart in the reference).  With polls > 0
+ * (at most 2^24), the fused explicit/implicit kernel's staging wait, after its copies have
+ * landed, also waits at most `polls` polls for an mbarrier phase that nothing completes: every
+ * block gives up, sets the error flag and exits, and the call returns AFID_E_TIMEOUT.  No
+ * fault, no hang; the flag stays set for the life of the context (as the reference stops at
+ * its first error code).  polls = 0 restores normal operation. */
+int afid_gpu_set_wait_test(afid_ctx_t *ctx, long long polls);
 /* Per-kernel device timing with CUDA events recorded on the context stream around every
  * launch (no counterpart in the reference, which times whole steps with MPI_WTIME,
  * main.F90:282,363-371).  Classes: 0 CN factor tables, 1 explicit+implicit, 2 divergence +

@@ -54,8 +54,9 @@ typedef struct afid_serve_job {
 
 typedef struct afid_serve_result {
   uint64_t tag;
-  int errorcode;      /* 0, 165 or 166 (the job stopped at the step that raised it), or the
-                         status that kept it from running (605 larger than the budget, 603, 444) */
+  int errorcode;      /* 0, 165 or 166 (the job stopped at the step that raised it), 607 when
+                         cancelled (afid_serve_cancel), or the status that kept it from running
+                         (603, 444, or 605 when its pool outgrew the budget after submission) */
   int steps_done;
   double time, dt, cfl, nu_vol, ke;   /* simulated time, last dt and CFL, GlobalQuantities      */
   double t_submit, t_admit, t_done;   /* seconds on the server clock (afid_serve_now)           */
@@ -71,9 +72,17 @@ typedef struct afid_serve_status {
 
 int afid_serve_create(const afid_serve_config_t *cfg, afid_server_t **out);
 int afid_serve_destroy(afid_server_t *s);
-/* Queue a job (AFID_E_INVALID if malformed).  A job that can never run comes back as a result
- * with its status in errorcode. */
+/* Queue a job.  Refused at once, with nothing queued: AFID_E_INVALID if malformed, and
+ * AFID_E_CAPACITY if its pool's state arrays alone (the nine FP64 field arrays, the RK3
+ * histories, phi and the half spectrum, for 1 slot in 3-D or slots_per_pool slots in 2-D)
+ * exceed hbm_budget_bytes.  A queued job that still cannot run comes back as a result with its
+ * status in errorcode. */
 int afid_serve_submit(afid_server_t *s, const afid_serve_job_t *job);
+/* Cancel the job with this tag.  A queued job leaves the queue; a running job stops at the end
+ * of its pool's current chunk (its slot is freed; the other jobs of the pool are unaffected).
+ * Either way it comes back from afid_serve_poll with errorcode AFID_E_CANCELLED and the steps it
+ * ran.  AFID_E_INVALID if no queued or running job has the tag. */
+int afid_serve_cancel(afid_server_t *s, uint64_t tag);
 /* Harvest completed chunks, admit queued jobs, start the next chunk on idle pools with jobs. */
 int afid_serve_pump(afid_server_t *s);
 /* Move up to `max` completed results into out[]; *n = how many. */

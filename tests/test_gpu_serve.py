@@ -6,8 +6,10 @@ Gates:
   size classes (2-D and 3-D);
 - every job stops at exactly its requested step count;
 - admission by device-memory footprint: with room for one pool, jobs of a second class wait
-  for the first class's pool to drain and be released; a job larger than the budget returns
-  AFID_E_CAPACITY; shortest-first ordering under a cells-in-flight cap.
+  for the first class's pool to drain and be released; a job larger than the budget is refused
+  at submit with AFID_E_CAPACITY; shortest-first ordering under a cells-in-flight cap;
+- cancellation: a queued job leaves the queue, a running job leaves its pool at the end of the
+  chunk, both come back with AFID_E_CANCELLED, and the other jobs' results do not change.
 """
 import numpy as np
 import pytest
@@ -99,9 +101,10 @@ def test_admission_by_footprint():
         assert res[9]["t_admit"] >= max(res[k]["t_done"] for k in (0, 1, 2)) - 1e-9
         assert srv.status()["device_bytes"] <= budget
     with ag.Server(ag.PREC_MIXED, hbm_budget_bytes=4096, slots_per_pool=2) as srv:
-        srv.submit(a, 1, 10, 1)
-        r = _run_to_completion(srv, 1)[1]
-        assert r["errorcode"] == 605 and r["steps_done"] == 0
+        with pytest.raises(ag.AfidError) as e:      # larger than the whole budget: refused at submit
+            srv.submit(a, 1, 10, 1)
+        assert e.value.status == ag.AFID_E_CAPACITY
+        assert srv.status()["queued"] == 0
 
 
 def test_shortest_first_under_cell_cap():
@@ -114,3 +117,28 @@ def test_shortest_first_under_cell_cap():
         res = _run_to_completion(srv, 3)
     order = sorted(res, key=lambda t: res[t]["t_done"])
     assert order == [2, 3, 1]
+
+
+def test_cancel_queued_and_running_jobs():
+    inp = _inp(32, 64, rayt=2e6)
+    with ag.Server(ag.PREC_FP64, slots_per_pool=2, chunk_steps=6) as srv:
+        srv.submit(inp, 2, 30, 2)
+        alone = _run_to_completion(srv, 1)[2]
+    with ag.Server(ag.PREC_FP64, slots_per_pool=2, chunk_steps=6, policy=ag.SERVE_FIFO) as srv:
+        for tag in (1, 2, 3, 4):
+            srv.submit(inp, tag, 30, tag)
+        srv.pump()                       # jobs 1 and 2 run, 3 and 4 wait for a slot
+        st = srv.status()
+        assert st["running"] == 2 and st["queued"] == 2
+        srv.cancel(3)                    # queued: leaves at once
+        srv.cancel(1)                    # running: leaves at the end of its chunk
+        with pytest.raises(ag.AfidError) as e:
+            srv.cancel(99)
+        assert e.value.status == ag.AFID_E_INVALID
+        res = _run_to_completion(srv, 4)
+    assert res[3]["errorcode"] == ag.AFID_E_CANCELLED and res[3]["steps_done"] == 0
+    assert res[1]["errorcode"] == ag.AFID_E_CANCELLED and 0 < res[1]["steps_done"] < 30
+    for tag in (2, 4):
+        assert res[tag]["errorcode"] == 0 and res[tag]["steps_done"] == 30
+    for k in ("nu_vol", "ke", "time", "dt"):
+        assert res[2][k] == alone[k], k

@@ -35,7 +35,7 @@ def test_library_exports_every_declared_symbol():
 
 
 def test_status_strings():
-    for s in (0, 8, 165, 166, 169, 444, 601, 602, 603, 604, 605, 606):
+    for s in (0, 8, 165, 166, 169, 444, 601, 602, 603, 604, 605, 606, 607):
         assert ag.lib().afid_gpu_status_string(s).decode() != "unknown status"
 
 
@@ -124,3 +124,37 @@ def test_tables_refuse_absurd_sizes():
         t = ctypes.c_void_p()
         assert ag.lib().afid_tables_create(ctypes.byref(inp), 0, ctypes.byref(t)) == ag.AFID_E_INVALID, dims
         assert not t.value
+
+
+def test_next_dt_refuses_nan_cfl():
+    """A NaN CFL maximum (a blown-up field) is never a valid step: 166 with variable dt, 165 with
+    fixed dt.  Finite values follow main.F90:287-302 (test_next_dt_matches_oracle)."""
+    for idtv, want in ((1, ag.AFID_E_DTMIN), (0, ag.AFID_E_CFL)):
+        inp = ag.parse_bou_in(bou_text(16, 8, 4, idtv=idtv, dt=1e-3, cflmax=1.2))
+        dtc = ctypes.c_double(1e-3)
+        assert ag.lib().afid_next_dt(ctypes.byref(inp), 5, ctypes.byref(dtc), float("nan"), None) == want
+
+
+def test_serve_refuses_oversized_job_at_submit_and_cancels_queued_job():
+    """Host side of the request loop (no pump, so no device work): a job whose pool cannot fit
+    the budget is refused by afid_serve_submit itself; a queued job cancelled by its tag comes
+    back from afid_serve_poll with AFID_E_CANCELLED and no steps; an unknown tag is an error."""
+    small = ag.parse_bou_in(bou_text(16, 32, 1))
+    big = ag.parse_bou_in(bou_text(256, 512, 1))
+    # 32 slots of 257x512 FP64 cells need ~400 MB of state arrays; a 64 MB budget cannot hold them
+    with ag.Server(ag.PREC_FP64, hbm_budget_bytes=64 << 20, slots_per_pool=32) as srv:
+        with pytest.raises(ag.AfidError) as e:
+            srv.submit(big, 1, 10, 1)
+        assert e.value.status == ag.AFID_E_CAPACITY
+        srv.submit(small, 2, 10, 2)
+        srv.submit(small, 3, 10, 3)
+        assert srv.status()["queued"] == 2
+        srv.cancel(2)
+        with pytest.raises(ag.AfidError) as e:
+            srv.cancel(2)
+        assert e.value.status == ag.AFID_E_INVALID
+        st = srv.status()
+        assert st["queued"] == 1 and st["running"] == 0
+        res = srv.poll()
+    assert len(res) == 1 and res[0]["tag"] == 2
+    assert res[0]["errorcode"] == ag.AFID_E_CANCELLED and res[0]["steps_done"] == 0
