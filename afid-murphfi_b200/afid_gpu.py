@@ -174,7 +174,8 @@ EXPORTS = [
     "afid_gpu_dims", "afid_h5_write", "afid_h5_info", "afid_h5_read_f64", "afid_continua_master_from_input",
     "afid_write_flow_field", "afid_read_continua_master", "afid_read_flow_field", "afid_gpu_write_flow_field",
     "afid_gpu_read_flow_field", "afid_run_io", "afid_read_flow_interp", "afid_gpu_read_flow_interp",
-    "afid_write_means", "afid_write_movie", "afid_write_grid_info",
+    "afid_write_means", "afid_write_movie", "afid_write_grid_info", "afid_write_movie_mean",
+    "afid_write_spectrum", "afid_gpu_write_spectra", "afid_gpu_mean_plane", "afid_gpu_sal_mean_plane",
 ]
 
 
@@ -297,6 +298,11 @@ def load_library(path: str = _LIB_PATH) -> C.CDLL:
         "afid_gpu_read_flow_interp": (i, [vp, C.c_char_p, C.POINTER(InputT), _dp, C.POINTER(i)]),
         "afid_write_means": (i, [C.c_char_p, d, i, _dp, i, _dp, i, _dp]),
         "afid_write_movie": (i, [C.c_char_p, i, d, i, _dp, i, i, i, _dp, i, i, i, _dp]),
+        "afid_write_movie_mean": (i, [C.c_char_p, i, d, i, _dp, i, i, i, _dp, i, i, i, _dp]),
+        "afid_write_spectrum": (i, [C.c_char_p, i, i, i, _dp]),
+        "afid_gpu_write_spectra": (i, [vp, C.c_char_p]),
+        "afid_gpu_mean_plane": (i, [vp, i, i, _dp]),
+        "afid_gpu_sal_mean_plane": (i, [vp, i, _dp]),
         "afid_write_grid_info": (i, [C.c_char_p, vp, vp]),
     }
     for name, (res, args) in sig.items():
@@ -530,6 +536,22 @@ class Solver:
             out[name] = a
         out["tav"] = tav.value
         return out
+
+    def mean_plane(self, which: int, axis: int) -> np.ndarray:
+        """afid_gpu_mean_plane: the y-mean (axis 1, (nzm, nx)) or z-mean (axis 2, (nym, nx)) of
+        vx, vy, vz or temp (which 0..3)."""
+        a = np.zeros((self.nzm, self.nx) if axis == 1 else (self.nym, self.nx))
+        _check(lib().afid_gpu_mean_plane(self._h, which, axis, _ptr(a)), "afid_gpu_mean_plane")
+        return a
+
+    def sal_mean_plane(self, axis: int) -> np.ndarray:
+        nzmr, nymr, nxmr = self._sal_shape
+        a = np.zeros((nzmr, nxmr) if axis == 1 else (nymr, nxmr))
+        _check(lib().afid_gpu_sal_mean_plane(self._h, axis, _ptr(a)), "afid_gpu_sal_mean_plane")
+        return a
+
+    def write_spectra(self, directory: str) -> None:
+        _check(lib().afid_gpu_write_spectra(self._h, directory.encode()), "afid_gpu_write_spectra")
 
     def slice(self, which: int, axis: int, index: int) -> np.ndarray:
         shape = {0: (self.nzm, self.nym), 1: (self.nzm, self.nx), 2: (self.nym, self.nx)}[axis]
@@ -879,12 +901,36 @@ def write_movie(directory: str, axis: int, tframe: float, times, planes: np.ndar
                                   _ptr(pl), *refined, _ptr(sal) if sal is not None else None), "afid_write_movie")
 
 
+def write_movie_mean(directory: str, axis: int, tframe: float, times, planes: np.ndarray, nxm: int, nym: int,
+                     nzm: int, sal_planes: np.ndarray = None, refined: tuple = (0, 0, 0)) -> None:
+    """afid_write_movie_mean: flowmov/movie_ymean.h5 (axis 1) or movie_zmean.h5 (axis 2) from
+    planes (nframes, 4, rows, nx) in Solver.mean_plane's layout, sal_planes (nframes, rows_r,
+    nxmr) or None."""
+    times = np.ascontiguousarray(times, dtype=np.float64)
+    pl = np.ascontiguousarray(planes, dtype=np.float64)
+    sal = None if sal_planes is None else np.ascontiguousarray(sal_planes, dtype=np.float64)
+    _check(lib().afid_write_movie_mean(directory.encode(), axis, tframe, times.size, _ptr(times), nxm, nym, nzm,
+                                       _ptr(pl), *refined, _ptr(sal) if sal is not None else None),
+           "afid_write_movie_mean")
+
+
+def write_spectrum_file(path: str, half: np.ndarray, nym: int) -> None:
+    """afid_write_spectrum: the half spectrum (nzm, nym//2 + 1, nxm) as the 'var' dataset
+    (nzm, nym, nxm) of write_3D_spectrum, the rows past nym//2 at 0."""
+    a = np.ascontiguousarray(half, dtype=np.float64)
+    nzm, nyh, nxm = a.shape
+    if nyh != nym // 2 + 1:
+        raise ValueError(f"half spectrum has {nyh} rows, nym = {nym} needs {nym // 2 + 1}")
+    _check(lib().afid_write_spectrum(path.encode(), nxm, nym, nzm, _ptr(a)), "afid_write_spectrum")
+
+
 class Recorder:
     """The outputs the reference's main loop writes besides the restart files, for a run driven
     from Python: cordin_info.h5 at construction (WriteGridInfo), a mean-profile sample per
     ``profiles(time)`` call (CalcMeanProfiles / CalcSalStats at TOUT), the three movie cuts per
-    ``frame(time)`` call (Mkmov_xcut / Mkmov_ycut / Mkmov_zcut at TFRAME), and ``flush()`` writing
-    means.h5 and flowmov/movie_{x,y,z}cut.h5 from everything sampled so far.
+    ``frame(time)`` call (Mkmov_xcut / Mkmov_ycut / Mkmov_zcut at TFRAME, and mean_yplane /
+    mean_zplane when nym > 1 and nzm > 1, main.F90:42, 340-343), and ``flush()`` writing means.h5,
+    flowmov/movie_{x,y,z}cut.h5 and flowmov/movie_{y,z}mean.h5 from everything sampled so far.
 
     The cuts sit where the reference puts them (0-based here): x at index 0 (vx at 1; index
     nxm/2 - 1, vx max(nxm/2, 2) - 1, when RAYS and RAYT are both negative), y at nym/2, z at nzm/2;
@@ -895,6 +941,8 @@ class Recorder:
         write_grid_info(directory, tables, mgrd)
         self.ptimes, self.prof, self.salprof = [], [], []
         self.ftimes, self.planes, self.salplanes = [], {0: [], 1: [], 2: []}, {0: [], 1: [], 2: []}
+        self.mean_planes = inp.nym > 1 and inp.nzm > 1          # write_mean_planes (main.F90:42)
+        self.mplanes, self.salmplanes = {1: [], 2: []}, {1: [], 2: []}
         both_neg = inp.rays < 0 and inp.rayt < 0
         ic = inp.nxm // 2 if both_neg else 1                      # 1-based, MakeMovieXCut.F90
         self.xcut = (max(ic, 2) - 1, ic - 1)                       # (vx, the others)
@@ -920,6 +968,11 @@ class Recorder:
                     (self.ycut if axis == 1 else self.zcut)
                 planes.append(self.solver.slice(which, axis, idx))
             self.planes[axis].append(np.stack(planes))
+        if self.mean_planes:
+            for axis in (1, 2):
+                self.mplanes[axis].append(np.stack([self.solver.mean_plane(w, axis) for w in range(4)]))
+                if self.sal:
+                    self.salmplanes[axis].append(self.solver.sal_mean_plane(axis))
         if self.sal:
             sal = self.solver.sal_download()                       # (nzmr, nymr, nxmr)
             ix, iy, iz = self.salcut
@@ -940,6 +993,11 @@ class Recorder:
             sp = np.stack(self.salplanes[axis]) if self.sal else None
             write_movie(self.dir, axis, inp.tframe, np.array(self.ftimes, dtype=np.float64),
                         np.stack(self.planes[axis]), nxm, inp.nym, inp.nzm, sp, refined)
+        if self.mean_planes:
+            for axis in (1, 2):
+                sp = np.stack(self.salmplanes[axis]) if self.sal else None
+                write_movie_mean(self.dir, axis, inp.tframe, np.array(self.ftimes, dtype=np.float64),
+                                 np.stack(self.mplanes[axis]), nxm, inp.nym, inp.nzm, sp, refined)
 
 
 def continua_master(inp: InputT, time: float = 0.0) -> ContinuaMasterT:

@@ -998,6 +998,29 @@ extern "C" int afid_gpu_write_flow_field(afid_ctx_t *ctx, const char *dir, int f
   });
 }
 
+// WriteSpectra (spectra.F90:169-196): the time-averaged power spectra of vx, vy, vz and temp as
+// <dir>/{vx,vy,vz,te}_spectrum.h5 (afid_gpu_spectra_read gives each divided by the averaging
+// interval, as the reference divides by time - tav_start).
+extern "C" int afid_gpu_write_spectra(afid_ctx_t *ctx, const char *dir) {
+  return afid_guard([&]() -> int {
+    static const char *const kFile[4] = {"vx_spectrum.h5", "vy_spectrum.h5", "vz_spectrum.h5", "te_spectrum.h5"};
+    if (!ctx || !dir) return AFID_E_INVALID;
+    int dims[6];
+    int s = afid_gpu_dims(ctx, dims);
+    if (s != AFID_OK) return s;
+    const int nxm = dims[0], nym = dims[1], nzm = dims[2];
+    if (!ensure_dir(dir)) return AFID_E_IO;
+    std::vector<double> half((size_t)nxm * (nym / 2 + 1) * nzm);
+    for (int w = 0; w < 4; ++w) {
+      double tav = 0.0;
+      if ((s = afid_gpu_spectra_read(ctx, w, half.data(), &tav)) != AFID_OK) return s;
+      if ((s = afid_write_spectrum((std::string(dir) + "/" + kFile[w]).c_str(), nxm, nym, nzm, half.data())) != AFID_OK)
+        return s;
+    }
+    return AFID_OK;
+  });
+}
+
 extern "C" int afid_gpu_read_flow_field(afid_ctx_t *ctx, const char *dir, const afid_continua_master_t *cur,
                                         double *time_out) {
   return afid_guard([&]() -> int {
@@ -1084,12 +1107,14 @@ extern "C" int afid_write_means(const char *dir, double tout, int nsamples, cons
 }
 
 // ---- movie planes --------------------------------------------------------------------------
-extern "C" int afid_write_movie(const char *dir, int axis, double tframe, int nframes, const double *times,
-                                int nxm, int nym, int nzm, const double *planes, int nxmr, int nymr, int nzmr,
-                                const double *sal_planes) {
+namespace {
+// The frame files of write_H5_plane (h5tools/h5_tools.F90:67-136) for one plane orientation
+// (axis 0: x = const, 1: y = const or y-mean, 2: z = const or z-mean), into <dir>/flowmov/<file>.
+int write_plane_frames(const char *dir, const char *file, int axis, double tframe, int nframes, const double *times,
+                       int nxm, int nym, int nzm, const double *planes, int nxmr, int nymr, int nzmr,
+                       const double *sal_planes) {
   return afid_guard([&]() -> int {
     static const char *const kVars[4] = {"vx", "vy", "vz", "temp"};
-    static const char *const kFile[3] = {"movie_xcut.h5", "movie_ycut.h5", "movie_zcut.h5"};
     if (!dir || axis < 0 || axis > 2 || nframes < 0 || !(tframe > 0.0) || nxm < 1 || nym < 1 || nzm < 1)
       return AFID_E_INVALID;
     if (nframes > 0 && (!times || !planes)) return AFID_E_INVALID;
@@ -1154,7 +1179,49 @@ extern "C" int afid_write_movie(const char *dir, int axis, double tframe, int nf
       }
     }
     for (size_t i = 0; i < sets.size(); ++i) sets[i].name = names[i].c_str();
-    return afid_h5_write((d + "/flowmov/" + kFile[axis]).c_str(), (int)sets.size(), sets.data());
+    return afid_h5_write((d + "/flowmov/" + file).c_str(), (int)sets.size(), sets.data());
+  });
+}
+}  // namespace
+
+extern "C" int afid_write_movie(const char *dir, int axis, double tframe, int nframes, const double *times,
+                                int nxm, int nym, int nzm, const double *planes, int nxmr, int nymr, int nzmr,
+                                const double *sal_planes) {
+  static const char *const kFile[3] = {"movie_xcut.h5", "movie_ycut.h5", "movie_zcut.h5"};
+  if (axis < 0 || axis > 2) return AFID_E_INVALID;
+  return write_plane_frames(dir, kFile[axis], axis, tframe, nframes, times, nxm, nym, nzm, planes, nxmr, nymr,
+                            nzmr, sal_planes);
+}
+
+// mean_yplane / mean_zplane (h5tools/mean_zplane.F90:131-258 / 2-129): the same layout as the
+// y and z cuts, in flowmov/movie_ymean.h5 and flowmov/movie_zmean.h5.
+extern "C" int afid_write_movie_mean(const char *dir, int axis, double tframe, int nframes, const double *times,
+                                     int nxm, int nym, int nzm, const double *planes, int nxmr, int nymr, int nzmr,
+                                     const double *sal_planes) {
+  if (axis != 1 && axis != 2) return AFID_E_INVALID;
+  return write_plane_frames(dir, axis == 1 ? "movie_ymean.h5" : "movie_zmean.h5", axis, tframe, nframes, times, nxm,
+                            nym, nzm, planes, nxmr, nymr, nzmr, sal_planes);
+}
+
+// write_3D_spectrum (h5tools/h5_tools.F90:229-302): dataset 'var' declared (nxm, nym, nzm) in
+// Fortran order; the nym/2 + 1 computed wavenumber rows fill its first rows (the hyperslab of
+// the spectral decomposition) and the rest keep the fill value 0.
+extern "C" int afid_write_spectrum(const char *path, int nxm, int nym, int nzm, const double *half) {
+  return afid_guard([&]() -> int {
+    if (!path || !half || nxm < 1 || nym < 2 || nzm < 1) return AFID_E_INVALID;
+    const int nyh = nym / 2 + 1;
+    std::vector<double> full((size_t)nzm * nym * nxm, 0.0);
+    for (int i = 0; i < nzm; ++i)
+      std::memcpy(&full[(size_t)i * nym * nxm], half + (size_t)i * nyh * nxm, sizeof(double) * (size_t)nyh * nxm);
+    afid_h5_dataset_t d{};
+    d.name = "var";
+    d.dtype = AFID_H5_F64;
+    d.rank = 3;
+    d.dims[0] = nzm;
+    d.dims[1] = nym;
+    d.dims[2] = nxm;
+    d.data = full.data();
+    return afid_h5_write(path, 1, &d);
   });
 }
 

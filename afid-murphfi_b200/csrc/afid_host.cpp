@@ -215,6 +215,7 @@ struct Samples {
   std::vector<double> ptimes, prof, salprof, ftimes;
   size_t dropped = 0;  // movie frames left out once the plane buffer is full
   std::vector<double> planes[3], salplanes[3];
+  std::vector<double> mplanes[3], salmplanes[3];  // mean_yplane / mean_zplane (axis 1, 2)
 
   int profiles(afid_ctx_t *ctx, const afid_input_t *in, const afid_mgrd_t *mg, double time) {
     const size_t off = prof.size();
@@ -240,10 +241,12 @@ struct Samples {
     const bool both_neg = in->rays < 0 && in->rayt < 0;
     const int icx = both_neg ? in->nxm / 2 : 1, nx = in->nxm + 1;
     const size_t psz[3] = {(size_t)in->nzm * in->nym, (size_t)in->nzm * nx, (size_t)in->nym * nx};
-    size_t frame_bytes = 4 * (psz[0] + psz[1] + psz[2]) * sizeof(double);
+    const bool means = in->nym > 1 && in->nzm > 1;  // write_mean_planes (main.F90:42)
+    size_t frame_bytes = 4 * (psz[0] + psz[1] + psz[2] + (means ? psz[1] + psz[2] : 0)) * sizeof(double);
     if (mg) {
       const afid_sal_grid_t *v = afid_mgrd_view(mg);
       frame_bytes += ((size_t)v->nzmr * v->nymr + (size_t)v->nzmr * v->nxmr + (size_t)v->nymr * v->nxmr) * sizeof(double);
+      if (means) frame_bytes += ((size_t)v->nzmr * v->nxmr + (size_t)v->nymr * v->nxmr) * sizeof(double);
     }
     if ((ftimes.size() + 1) * frame_bytes > kMovieBytes) {
       // the frame is not kept: say so once, and count the frames left out
@@ -262,6 +265,22 @@ struct Samples {
         const int r = afid_gpu_slice(ctx, which, axis, idx, planes[axis].data() + off);
         if (r != AFID_OK) return r;
       }
+    // mean_yplane / mean_zplane beside the cuts (main.F90:340-343)
+    for (int axis = 1; means && axis <= 2; ++axis) {
+      for (int which = 0; which < 4; ++which) {
+        const size_t off = mplanes[axis].size();
+        mplanes[axis].resize(off + psz[axis]);
+        const int r = afid_gpu_mean_plane(ctx, which, axis, mplanes[axis].data() + off);
+        if (r != AFID_OK) return r;
+      }
+      if (mg) {
+        const afid_sal_grid_t *v = afid_mgrd_view(mg);
+        const size_t off = salmplanes[axis].size();
+        salmplanes[axis].resize(off + (size_t)(axis == 1 ? v->nzmr : v->nymr) * v->nxmr);
+        const int r = afid_gpu_sal_mean_plane(ctx, axis, salmplanes[axis].data() + off);
+        if (r != AFID_OK) return r;
+      }
+    }
     if (mg) {
       const afid_sal_grid_t *v = afid_mgrd_view(mg);
       const int nxmr = v->nxmr, nymr = v->nymr, nzmr = v->nzmr;
@@ -308,6 +327,10 @@ struct Samples {
       r = afid_write_movie(dir, axis, in->tframe, (int)ftimes.size(), ftimes.data(), in->nxm, in->nym, in->nzm,
                            planes[axis].data(), v ? v->nxmr : 0, v ? v->nymr : 0, v ? v->nzmr : 0,
                            v ? salplanes[axis].data() : nullptr);
+    for (int axis = 1; axis <= 2 && r == AFID_OK && in->nym > 1 && in->nzm > 1; ++axis)
+      r = afid_write_movie_mean(dir, axis, in->tframe, (int)ftimes.size(), ftimes.data(), in->nxm, in->nym,
+                                in->nzm, mplanes[axis].data(), v ? v->nxmr : 0, v ? v->nymr : 0, v ? v->nzmr : 0,
+                                v ? salmplanes[axis].data() : nullptr);
     return r;
   }
 };

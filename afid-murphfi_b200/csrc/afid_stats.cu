@@ -315,3 +315,59 @@ extern "C" int afid_gpu_slice(afid_ctx_t *ctx, int which, int axis, int index, d
   if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
   return e == cudaSuccess ? AFID_OK : ctx_fail(ctx, e);
 }
+
+// ---- plane means (h5tools/means.F90 ymean / zmean / ymeanr / zmeanr) ----------------------
+// Mean over y (axis 1: out[i][k], planes x rows of nxc) or over z (axis 2: out[j][k]) of a
+// field stored x-fastest with stride ld, ny rows per z-plane, nz planes.  The sum runs in the
+// reference's order (the averaged index ascending) and is divided once at the end.
+__global__ void k_plane_mean(const double *__restrict__ f, int ld, int ny, int nz, int nxc, int axis,
+                             double *__restrict__ out) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  const int r = blockIdx.y;  // i (y-mean) or j (z-mean)
+  if (k >= nxc) return;
+  double acc = 0.0;
+  if (axis == 1) {
+    const double *p = f + (size_t)ld * ny * r + k;
+    for (int j = 0; j < ny; ++j) acc += p[(size_t)ld * j];
+    out[(size_t)r * nxc + k] = acc / (double)ny;
+  } else {
+    const double *p = f + (size_t)ld * r + k;
+    for (int i = 0; i < nz; ++i) acc += p[(size_t)ld * ny * i];
+    out[(size_t)r * nxc + k] = acc / (double)nz;
+  }
+}
+
+namespace {
+int plane_mean(afid_ctx_t *ctx, const double *f, int ld, int ny, int nz, int nxc, int axis, double *out) {
+  const size_t n = (size_t)(axis == 1 ? nz : ny) * nxc;
+  if (ctx->stats_elems < n) {
+    if (ctx->stats_buf) cudaFree(ctx->stats_buf);
+    ctx->stats_buf = nullptr;
+    ctx->stats_elems = 0;
+    if (cudaMalloc(&ctx->stats_buf, n * sizeof(double)) != cudaSuccess) return AFID_E_ALLOC;
+    ctx->stats_elems = n;
+  }
+  const dim3 grid((unsigned)((nxc + 127) / 128), (unsigned)(axis == 1 ? nz : ny));
+  k_plane_mean<<<grid, 128, 0, ctx->stream>>>(f, ld, ny, nz, nxc, axis, ctx->stats_buf);
+  ctx->launches += 1;
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaMemcpyAsync(out, ctx->stats_buf, n * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+  return e == cudaSuccess ? AFID_OK : ctx_fail(ctx, e);
+}
+}  // namespace
+
+extern "C" int afid_gpu_mean_plane(afid_ctx_t *ctx, int which, int axis, double *out) {
+  if (!ctx || !out || which < 0 || which > 3 || (axis != 1 && axis != 2) || ctx->L.g.batch) return AFID_E_INVALID;
+  cudaSetDevice(ctx->dev);
+  const Geom &g = ctx->L.g;
+  const double *f = (which == 0) ? ctx->vx : (which == 1) ? ctx->vy : (which == 2) ? ctx->vz : ctx->temp;
+  return plane_mean(ctx, f, g.ldx, g.nym, g.nzm, g.nx, axis, out);
+}
+
+extern "C" int afid_gpu_sal_mean_plane(afid_ctx_t *ctx, int axis, double *out) {
+  if (!ctx || !out || !ctx->sal || (axis != 1 && axis != 2)) return AFID_E_INVALID;
+  cudaSetDevice(ctx->dev);
+  const SalGeom &sg = ctx->sal->sg;
+  return plane_mean(ctx, ctx->sal->sal, sg.ldr, sg.nymr, sg.nzmr, sg.nxmr, axis, out);
+}

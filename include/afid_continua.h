@@ -20,6 +20,9 @@
  *   afid_write_grid_info         the coordinates file cordin_info.h5 (WriteGridInfo.F90)
  *   afid_write_means             the mean-profile file means.h5 (CalcMeanProfiles.F90:209-334)
  *   afid_write_movie             the movie-plane files flowmov/movie_{x,y,z}cut.h5 (MakeMovie*Cut.F90)
+ *   afid_write_movie_mean        the plane-mean files flowmov/movie_{y,z}mean.h5 (mean_zplane.F90)
+ *   afid_write_spectrum /        the spectrum files {vx,vy,vz,te}_spectrum.h5 (spectra.F90:169-196)
+ *   afid_gpu_write_spectra
  *   afid_run_io                  afid_run plus the main loop's restart and save points:
  *                                ReadFlowInterp (either branch) when NREAD = 1 (main.F90:157-161), the start-up
  *                                frame (main.F90:241), the SAVE_3D frames (main.F90:376-381) and
@@ -151,6 +154,27 @@ int afid_write_grid_info(const char *dir, const afid_tables_t *t, const afid_mgr
 int afid_write_movie(const char *dir, int axis, double tframe, int nframes, const double *times, int nxm,
                      int nym, int nzm, const double *planes, int nxmr, int nymr, int nzmr,
                      const double *sal_planes);
+/* <dir>/flowmov/movie_ymean.h5 (axis 1) or movie_zmean.h5 (axis 2): the plane means of
+ * mean_yplane / mean_zplane (h5tools/mean_zplane.F90:131-258 / 2-129, averaging by
+ * h5tools/means.F90 ymean / zmean / ymeanr / zmeanr), written like the y and z cuts above:
+ * planes in afid_gpu_mean_plane's layout (y-mean: nzm x nx; z-mean: nym x nx; vy, vz, temp stored
+ * with their nxm rows), sal_planes from afid_gpu_sal_mean_plane (nzmr x nxmr, nymr x nxmr) or
+ * NULL.  The reference writes them beside the cuts when nym > 1 and nzm > 1 (main.F90:42,
+ * 233-235, 340-343). */
+int afid_write_movie_mean(const char *dir, int axis, double tframe, int nframes, const double *times, int nxm,
+                          int nym, int nzm, const double *planes, int nxmr, int nymr, int nzmr,
+                          const double *sal_planes);
+
+/* ---- spectra ----------------------------------------------------------------------------- */
+/* One spectrum file of write_3D_spectrum (h5tools/h5_tools.F90:229-302): dataset 'var' declared
+ * with the Fortran dims (nxm, nym, nzm) (C order nzm x nym x nxm); the half spectrum
+ * half[nzm][nym/2+1][nxm] (afid_gpu_spectra_read's layout) fills the first nym/2 + 1 wavenumber
+ * rows of each z plane and the remaining rows hold 0, the fill value of the reference's
+ * hyperslab write. */
+int afid_write_spectrum(const char *path, int nxm, int nym, int nzm, const double *half);
+/* WriteSpectra (spectra.F90:169-196) through a device context: <dir>/vx_spectrum.h5,
+ * vy_spectrum.h5, vz_spectrum.h5, te_spectrum.h5 from the averages of afid_gpu_spectra_update. */
+int afid_gpu_write_spectra(afid_ctx_t *ctx, const char *dir);
 
 /* Device context variants (salinity included when afid_gpu_sal_create was called). */
 int afid_gpu_write_flow_field(afid_ctx_t *ctx, const char *dir, int final, double save_3d,

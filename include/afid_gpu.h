@@ -152,6 +152,10 @@ int afid_gpu_spectra_read(afid_ctx_t *ctx, int which, double *out, double *tav);
  * write them: axis 0 = x (wall-parallel plane at x index `index`): out[nzm][nym]; axis 1 = y:
  * out[nzm][nx]; axis 2 = z: out[nym][nx]. */
 int afid_gpu_slice(afid_ctx_t *ctx, int which, int axis, int index, double *out);
+/* Plane mean of a resident field (which: 0 vx, 1 vy, 2 vz, 3 temp) over y (axis 1: out[nzm][nx],
+ * ymean of h5tools/means.F90:10-45) or over z (axis 2: out[nym][nx], zmean, means.F90:47-82):
+ * the sum over the averaged index in ascending order divided by nym (nzm), on the device. */
+int afid_gpu_mean_plane(afid_ctx_t *ctx, int which, int axis, double *out);
 
 /* Autotuner of the fused explicit/implicit kernel: every thread shape available for this
  * wall-normal size (threads per x-column block x rows per thread) is timed on a sample of

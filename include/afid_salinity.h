@@ -92,6 +92,9 @@ int afid_gpu_sal_interpolate(afid_ctx_t *ctx);
 int afid_gpu_sal_cfl(afid_ctx_t *ctx, double *cflmr);
 /* out[AFID_NUM_SAL_PROFILES * nxmr]: Sbar, Srms, vxS, vyS, vzS, chiS (CalcSalStats). */
 int afid_gpu_sal_profiles(afid_ctx_t *ctx, double *out);
+/* Plane mean of the refined salinity over y (axis 1: out[nzmr][nxmr], ymeanr of
+ * h5tools/means.F90:84-157 without IBM) or over z (axis 2: out[nymr][nxmr], zmeanr). */
+int afid_gpu_sal_mean_plane(afid_ctx_t *ctx, int axis, double *out);
 /* The interpolated fields: vxr [nxmr+1 rows], vyr, vzr [nxmr rows] with leading dims
  * ldr_x >= nxmr+1, ldr_y >= nymr; salc [nxm rows] with ldc_x >= nxm, ldc_y >= nym.  NULL skips. */
 int afid_gpu_sal_download_aux(afid_ctx_t *ctx, double *vxr, double *vyr, double *vzr, int ldr_x,

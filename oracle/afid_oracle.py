@@ -1108,3 +1108,26 @@ def spectra_update(g: Grid, s: State, dt: float, acc: dict) -> None:
     for name in ("vx", "vy", "vz", "temp"):
         f = fourier_coef(g, getattr(s, name)[..., :nxm])
         acc[name] = acc.get(name, 0.0) + dt * np.abs(f) ** 2
+
+
+# ----------------------------------------------------------------------------------------------
+# Plane means (h5tools/mean_zplane.F90, h5tools/means.F90)
+# ----------------------------------------------------------------------------------------------
+def mean_plane(field: np.ndarray, axis: int) -> np.ndarray:
+    """``ymean`` (axis 1, ``means.F90:10-45``) or ``zmean`` (axis 2, ``means.F90:47-82``) of a
+    field stored (nz, ny, nx_rows): plane(k, i) = sum_j var(k, j, i) / nym, or plane(k, j) =
+    sum_i var(k, j, i) / nzm, summed in ascending order as the reference's loops do (one rank,
+    so the MPI_REDUCE adds nothing), then divided once.  Returns (nz, nx_rows) or (ny, nx_rows).
+    The refined-grid versions ``ymeanr`` / ``zmeanr`` (``means.F90:84-157`` and on) are the same
+    without IBM."""
+    f = np.asarray(field, dtype=np.float64)
+    nz, ny, _ = f.shape
+    if axis == 1:
+        acc = np.zeros((nz, f.shape[2]))
+        for j in range(ny):
+            acc = acc + f[:, j, :]
+        return acc / float(ny)
+    acc = np.zeros((ny, f.shape[2]))
+    for i in range(nz):
+        acc = acc + f[i, :, :]
+    return acc / float(nz)

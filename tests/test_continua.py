@@ -543,6 +543,66 @@ def test_movie_file_layout(tmp_path, axis):
             np.testing.assert_array_equal(got, want)
 
 
+@pytest.mark.parametrize("axis", [1, 2])
+def test_movie_mean_file_layout(tmp_path, axis):
+    """flowmov/movie_ymean.h5 and movie_zmean.h5 (mean_zplane.F90 through write_H5_plane): the
+    layout of the y and z cuts, under the plane-mean file names."""
+    rng = np.random.default_rng(28 + axis)
+    nxm, nym, nzm, nxmr, nymr, nzmr = 6, 8, 4, 12, 16, 8
+    nx = nxm + 1
+    rows = nzm if axis == 1 else nym
+    rrows = nzmr if axis == 1 else nymr
+    times = np.array([0.0, 0.1, 0.2])
+    planes = rng.standard_normal((3, 4, rows, nx))
+    sal = rng.standard_normal((3, rrows, nxmr))
+    d = str(tmp_path / "outputdir")
+    ag.write_movie_mean(d, axis, 0.1, times, planes, nxm, nym, nzm, sal, (nxmr, nymr, nzmr))
+    p = os.path.join(d, "flowmov", "movie_ymean.h5" if axis == 1 else "movie_zmean.h5")
+    f = h5.H5File(p)
+    assert sorted(f.root()) == sorted(["vx", "vy", "vz", "temp", "sal"])
+    for v, g in enumerate(("vx", "vy", "vz", "temp")):
+        assert sorted(f.links(f.resolve(g))) == ["00000", "00001", "00002"]
+        for fr in range(3):
+            want = planes[fr, v] if g == "vx" else planes[fr, v][:, :nxm]
+            np.testing.assert_array_equal(f.read(f"{g}/{fr:05d}"), want)
+    np.testing.assert_array_equal(f.read("sal/00002"), sal[2])
+    with pytest.raises(ag.AfidError):
+        ag.write_movie_mean(d, 0, 0.1, times, planes, nxm, nym, nzm)   # no x-mean file
+
+
+def test_spectrum_file_layout(tmp_path):
+    """{vx,vy,vz,te}_spectrum.h5 (write_3D_spectrum, h5_tools.F90:229-302): dataset 'var' with the
+    declared (nxm, nym, nzm) extent, the nym/2 + 1 computed wavenumber rows first, zeros after."""
+    rng = np.random.default_rng(30)
+    nxm, nym, nzm = 5, 12, 4
+    half = rng.random((nzm, nym // 2 + 1, nxm))
+    p = str(tmp_path / "vx_spectrum.h5")
+    ag.write_spectrum_file(p, half, nym)
+    assert h5.names(p) == ["var"]
+    got = h5.read(p, "var")
+    assert got.shape == (nzm, nym, nxm)
+    np.testing.assert_array_equal(got[:, :nym // 2 + 1, :], half)
+    assert np.all(got[:, nym // 2 + 1:, :] == 0.0)
+    with pytest.raises(ValueError):
+        ag.write_spectrum_file(p, half, nym + 4)
+
+
+def test_oracle_mean_plane_is_the_loop_sum():
+    """The oracle's ymean / zmean: ascending-order sums divided once (checked against an
+    explicit triple loop) on a small field."""
+    rng = np.random.default_rng(31)
+    f = rng.standard_normal((3, 4, 5))
+    y = np.zeros((3, 5))
+    z = np.zeros((4, 5))
+    for i in range(3):
+        for j in range(4):
+            for k in range(5):
+                y[i, k] += f[i, j, k]
+                z[j, k] += f[i, j, k]
+    np.testing.assert_array_equal(o.mean_plane(f, 1), y / 4.0)
+    np.testing.assert_array_equal(o.mean_plane(f, 2), z / 3.0)
+
+
 def test_grid_info_file(tmp_path):
     """cordin_info.h5 as WriteGridInfo.F90 writes it, against the oracle's grids."""
     text = bou_text(16, 12, 8, multires=1, nxmr=24, nymr=18, nzmr=16, flagsal=1, istr3r=4)
@@ -577,6 +637,14 @@ class _FakeSolver:
 
     def sal_profiles(self):
         return {n: np.full(self.refined[0], -100.0 * self.calls - q) for q, n in enumerate(ag.SAL_PROFILE_NAMES)}
+
+    def mean_plane(self, which, axis):
+        shape = {1: (self.nzm, self.nx), 2: (self.nym, self.nx)}[axis]
+        return np.full(shape, -(1000.0 * which + 10.0 * axis))
+
+    def sal_mean_plane(self, axis):
+        nxmr, nymr, nzmr = self.refined
+        return np.full((nzmr, nxmr) if axis == 1 else (nymr, nxmr), -7.0 * axis)
 
     def slice(self, which, axis, index):
         shape = {0: (self.nzm, self.nym), 1: (self.nzm, self.nx), 2: (self.nym, self.nx)}[axis]
@@ -618,6 +686,12 @@ def test_recorder_writes_the_reference_outputs(tmp_path):
     y = h5.H5File(os.path.join(d, "flowmov", "movie_ycut.h5"))
     assert y.read("vy/00001").shape == (4, 6) and y.read("vx/00001").shape == (4, 7)
     assert y.read("vz/00001")[0, 0] == 2 * 1000 + 1 * 100 + 4          # y index nym/2 = 4
+    for name, axis in (("movie_ymean.h5", 1), ("movie_zmean.h5", 2)):   # mean_yplane / mean_zplane
+        mf = h5.H5File(os.path.join(d, "flowmov", name))
+        assert sorted(mf.links(mf.resolve("temp"))) == ["00001", "00002"]
+        assert mf.read("vx/00001").shape == ((4, 7) if axis == 1 else (8, 7))
+        assert mf.read("vy/00002")[0, 0] == -(1000 * 1 + 10 * axis)
+        assert mf.read("sal/00001").shape == ((8, 12) if axis == 1 else (16, 12))
     z = h5.H5File(os.path.join(d, "flowmov", "movie_zcut.h5"))
     assert z.read("vx/00002")[0, 0] == 0 * 1000 + 2 * 100 + 2          # z index nzm/2 = 2
     np.testing.assert_array_equal(x.read("sal/00001"), fake.sal_download()[:, :, 0])

@@ -87,6 +87,11 @@ def test_run_io_restart_matches_an_uninterrupted_run(tmp_path, sal):
     want = sorted(f"{fr:05d}_{k}.h5" for fr in set(frames1) | set(frames2) for k in names)
     assert sorted(os.listdir(os.path.join(d, "fields"))) == want
     assert ag.read_continua_master(d, multires=sal).time == t2
+    # the plane means sit beside the cuts, frame for frame (main.F90:233-235, 337-343)
+    for mean, cut in (("movie_ymean.h5", "movie_ycut.h5"), ("movie_zmean.h5", "movie_zcut.h5")):
+        fm, fc = h5.H5File(os.path.join(d, "flowmov", mean)), h5.H5File(os.path.join(d, "flowmov", cut))
+        assert sorted(fm.links(fm.resolve("temp"))) == sorted(fc.links(fc.resolve("temp")))
+        assert sorted(fm.root()) == sorted(fc.root())
     ref = ag.RunStatsT()
     assert ag.lib().afid_run(ctypes.byref(first), ag.PREC_FP64, 5, 7, 0, None, None, ctypes.byref(ref)) == 0
     assert st2.nu_vol == pytest.approx(ref.nu_vol, rel=1e-11)
