@@ -179,9 +179,10 @@ int afid_gpu_set_k1_shape(afid_ctx_t *ctx, int index);
 /* Test hook of the bounded device waits (no counterpart in the reference).  With polls > 0
  * (at most 2^24), the fused explicit/implicit kernel's staging wait, after its copies have
  * landed, also waits at most `polls` polls for an mbarrier phase that nothing completes: every
- * block gives up, sets the error flag and exits, and the call returns AFID_E_TIMEOUT.  No
- * fault, no hang; the flag stays set for the life of the context (as the reference stops at
- * its first error code).  polls = 0 restores normal operation. */
+ * block gives up, sets the error flag and exits, and the next call that synchronises with the
+ * stream (afid_gpu_synchronize, afid_gpu_cfl, afid_gpu_divmax, afid_gpu_globals, ...) returns
+ * AFID_E_TIMEOUT.  No fault, no hang; the flag stays set for the life of the context (as the
+ * reference stops at its first error code).  polls = 0 restores normal operation. */
 int afid_gpu_set_wait_test(afid_ctx_t *ctx, long long polls);
 /* Per-kernel device timing with CUDA events recorded on the context stream around every
  * launch (no counterpart in the reference, which times whole steps with MPI_WTIME,

@@ -3,8 +3,9 @@
 * Bounded device waits: the fused explicit/implicit kernel's staging wait is made to run out
   (afid_gpu_set_wait_test: after its copies land it also waits for an mbarrier phase that
   nothing completes, at most a few thousand polls).  Every block gives up, drains, sets the
-  error flag and exits; the call returns AFID_E_TIMEOUT, the flag stays set on that context,
-  and the device stays usable: a new context on the same GPU steps and matches the oracle.
+  error flag and exits; the next synchronising call returns AFID_E_TIMEOUT, the flag stays set
+  on that context, and the device stays usable: a new context on the same GPU steps and matches
+  the oracle.
 * Blown-up fields: a NaN in the velocity propagates through the CFL and divergence maxima
   (CalcMaxCFL.F90:22-43, CheckDivergence.F90:22-42), and the main-loop rules of
   main.F90:287-302, 357 turn it into 166 (variable dt), 165 (fixed dt) and 169 (divergence);
@@ -29,11 +30,12 @@ def test_bounded_wait_runs_out_with_timeout_status():
         gpu.upload(s.vx, s.vy, s.vz, s.temp, s.pr)
         gpu.set_wait_test(4096)
         with pytest.raises(ag.AfidError) as e:
-            gpu.time_marcher(1e-3, 0)
+            gpu.time_marcher(1e-3, 0)               # stream-ordered: returns before the kernels end
+            gpu.synchronize()                       # the next synchronising call reports it
         assert e.value.status == ag.AFID_E_TIMEOUT
         gpu.set_wait_test(0)
         with pytest.raises(ag.AfidError) as e:      # the flag stays set on this context
-            gpu.synchronize()
+            gpu.calc_max_cfl()
         assert e.value.status == ag.AFID_E_TIMEOUT
     # the GPU itself is fine: a new context steps and matches the oracle
     with case.solver() as gpu:
