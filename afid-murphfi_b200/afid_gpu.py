@@ -87,14 +87,19 @@ class BatchStatT(C.Structure):
                 ("dt", C.c_double), ("cfl", C.c_double)]
 
 
+TUNE_MAX = 8
+
+
 class TuneInfoT(C.Structure):
     _fields_ = [("ncand", C.c_int), ("chosen", C.c_int), ("sample_columns", C.c_int),
-                ("threads", C.c_int * 5), ("rows", C.c_int * 5), ("regcap", C.c_int * 5), ("us", C.c_double * 5)]
+                ("threads", C.c_int * TUNE_MAX), ("rows", C.c_int * TUNE_MAX), ("regcap", C.c_int * TUNE_MAX),
+                ("policy", C.c_int * TUNE_MAX), ("us", C.c_double * TUNE_MAX)]
 
     def as_dict(self) -> dict:
-        """shapes: [threads per column, rows per thread, register cap, microseconds per sample]"""
+        """shapes: [threads per column, rows per thread, register cap, memory policy,
+        microseconds per sample]"""
         return {"ncand": self.ncand, "chosen": self.chosen, "sample_columns": self.sample_columns,
-                "shapes": [[self.threads[v], self.rows[v], self.regcap[v], round(self.us[v], 2)]
+                "shapes": [[self.threads[v], self.rows[v], self.regcap[v], self.policy[v], round(self.us[v], 2)]
                            for v in range(self.ncand)]}
 
 

@@ -548,8 +548,8 @@ int ctx_fail(afid_ctx_t *ctx, cudaError_t e) { return fail_cuda(ctx, e); }
 int ctx_autotune(afid_ctx_t *ctx, bool force) {
   if (ctx->tuned && !force) return AFID_OK;
   LaunchCtx L = ctx->L;
-  int tpc[AFID_TUNE_MAX] = {0}, rpt[AFID_TUNE_MAX] = {0}, cap[AFID_TUNE_MAX] = {0};
-  const int n = k1_shapes(L.M, tpc, rpt, cap);
+  int tpc[AFID_TUNE_MAX] = {0}, rpt[AFID_TUNE_MAX] = {0}, cap[AFID_TUNE_MAX] = {0}, pol[AFID_TUNE_MAX] = {0};
+  const int n = k1_shapes(L.M, tpc, rpt, cap, pol);
   afid_tune_info_t info{};
   info.ncand = n;
   const int ncol = L.g.nym * L.g.nzm;
@@ -559,6 +559,7 @@ int ctx_autotune(afid_ctx_t *ctx, bool force) {
     info.threads[v] = v < n ? tpc[v] : 0;
     info.rows[v] = v < n ? rpt[v] : 0;
     info.regcap[v] = v < n ? cap[v] : 0;
+    info.policy[v] = v < n ? pol[v] : 0;
     info.us[v] = -1.0;
   }
   if (n > 1) {
@@ -851,8 +852,8 @@ long long afid_gpu_launch_count(afid_ctx_t *ctx) { return ctx ? ctx->launches : 
 
 int afid_gpu_set_k1_shape(afid_ctx_t *ctx, int index) {
   if (!ctx) return AFID_E_INVALID;
-  int tpc[AFID_TUNE_MAX], rpt[AFID_TUNE_MAX], cap[AFID_TUNE_MAX];
-  const int n = k1_shapes(ctx->L.M, tpc, rpt, cap);
+  int tpc[AFID_TUNE_MAX], rpt[AFID_TUNE_MAX], cap[AFID_TUNE_MAX], pol[AFID_TUNE_MAX];
+  const int n = k1_shapes(ctx->L.M, tpc, rpt, cap, pol);
   if (index < 0 || index >= n) return AFID_E_INVALID;
   afid_tune_info_t info{};
   info.ncand = n;
@@ -861,6 +862,7 @@ int afid_gpu_set_k1_shape(afid_ctx_t *ctx, int index) {
     info.threads[v] = v < n ? tpc[v] : 0;
     info.rows[v] = v < n ? rpt[v] : 0;
     info.regcap[v] = v < n ? cap[v] : 0;
+    info.policy[v] = v < n ? pol[v] : 0;
     info.us[v] = -1.0;
   }
   ctx->tune = info;

@@ -66,8 +66,8 @@ cudaError_t launch_k1_mixed(const LaunchCtx &L, const SubstepBuffers &b, int ns,
 // The same with the salinity buoyancy in the explicit terms (L.g.salc set).
 cudaError_t launch_k1_fp64_sal(const LaunchCtx &L, const SubstepBuffers &b, int ns, int var, int ncol);
 cudaError_t launch_k1_mixed_sal(const LaunchCtx &L, const SubstepBuffers &b, int ns, int var, int ncol);
-// Thread shapes of K1 for M: fills tpc[]/rpt[]/cap[] (up to AFID_TUNE_MAX) and returns their number.
-int k1_shapes(int M, int *tpc, int *rpt, int *cap);
+// Thread shapes of K1 for M: fills tpc[]/rpt[]/cap[]/pol[] (up to AFID_TUNE_MAX) and returns their number.
+int k1_shapes(int M, int *tpc, int *rpt, int *cap, int *pol);
 // The kernels of one substep, in launch order (K1 .. K7).
 enum class Stage { ExplicitImplicit = 0, DivFftY, FftZFwd, Tridiag, FftZInv, IfftY, Correct };
 constexpr int kNumStages = 7;

@@ -8,12 +8,55 @@
 
 namespace afid {
 
+// Loads by cache policy.  H = 0: read-only data through the non-coherent path (__ldg) and the
+// RK3 histories by plain loads.  H = 1: the tables every block reads (metric coefficients, CN
+// factors) are kept in L1 with the evict_last priority, and the data each block reads once (RK3
+// histories, single-row neighbours) bypasses L1 (no_allocate), so the streaming data does not
+// evict the tables.
+template <int H> __device__ __forceinline__ double tld(const double *p) {
+  if constexpr (H != 0) {
+    double v;
+    asm("ld.global.nc.L1::evict_last.f64 %0, [%1];" : "=d"(v) : "l"(p));
+    return v;
+  } else {
+    return __ldg(p);
+  }
+}
+template <int H> __device__ __forceinline__ double nld(const double *p) {
+  if constexpr (H != 0) {
+    double v;
+    asm("ld.global.nc.L1::no_allocate.f64 %0, [%1];" : "=d"(v) : "l"(p));
+    return v;
+  } else {
+    return __ldg(p);
+  }
+}
+// Read-write streaming data (the histories, rewritten later by the same thread): coherent loads.
+template <int H> __device__ __forceinline__ double sld(const double *p) {
+  if constexpr (H != 0) {
+    double v;
+    asm volatile("ld.global.L1::no_allocate.f64 %0, [%1];" : "=d"(v) : "l"(p) : "memory");
+    return v;
+  } else {
+    return *p;
+  }
+}
+template <int H> __device__ __forceinline__ double sld(const float *p) {
+  if constexpr (H != 0) {
+    float v;
+    asm volatile("ld.global.L1::no_allocate.f32 %0, [%1];" : "=f"(v) : "l"(p) : "memory");
+    return (double)v;
+  } else {
+    return (double)*p;
+  }
+}
+
 // Doubles per CN factor table (one matrix, one substep); layout in afid_kernels.cu.
 __host__ __device__ inline size_t cn_table_size(int M) { return 192 * (size_t)M + 18 * 32; }
 
 // Solve one column whose scaled RHS sits in s[q*32 + lane] (chunk layout); the solution
 // overwrites it.  Constant-matrix version using the tables above.
-template <int M, int LD = 32>
+template <int M, int LD = 32, int H = 0>
 __device__ __forceinline__ void cn_solve_chunk(double *__restrict__ s, const double *__restrict__ T,
                                                int lane) {
   const double *Ta = T + 32 * M, *Tinv = T + 64 * M, *Tcp = T + 96 * M, *Tv = T + 128 * M,
@@ -22,37 +65,37 @@ __device__ __forceinline__ void cn_solve_chunk(double *__restrict__ s, const dou
 #pragma unroll
   for (int q = 0; q < M; ++q) y[q] = s[q * LD + lane];
   if constexpr (M > 1) {
-    y[1] = y[1] * __ldg(Tinv + 32 + lane);
+    y[1] = y[1] * tld<H>(Tinv + 32 + lane);
 #pragma unroll
     for (int q = 2; q < M; ++q)
-      y[q] = (y[q] - __ldg(Ta + q * 32 + lane) * y[q - 1]) * __ldg(Tinv + q * 32 + lane);
+      y[q] = (y[q] - tld<H>(Ta + q * 32 + lane) * y[q - 1]) * tld<H>(Tinv + q * 32 + lane);
 #pragma unroll
-    for (int q = M - 2; q >= 1; --q) y[q] = y[q] - __ldg(Tcp + q * 32 + lane) * y[q + 1];
+    for (int q = M - 2; q >= 1; --q) y[q] = y[q] - tld<H>(Tcp + q * 32 + lane) * y[q + 1];
   }
   double D;
   if constexpr (M > 1) {
     double yprev = __shfl_up_sync(0xffffffffu, y[M - 1], 1);
     if (lane == 0) yprev = 0.0;
-    D = y[0] - __ldg(Tl + lane) * yprev - __ldg(Tl + 32 + lane) * y[1];
+    D = y[0] - tld<H>(Tl + lane) * yprev - tld<H>(Tl + 32 + lane) * y[1];
   } else {
     D = y[0];
   }
-  double delta = D * __ldg(Tl + 64 + lane);
+  double delta = D * tld<H>(Tl + 64 + lane);
 #pragma unroll
   for (int lev = 0, h = 1; lev < 5; ++lev, h <<= 1) {
     double dm = __shfl_up_sync(0xffffffffu, delta, h);
     double dp = __shfl_down_sync(0xffffffffu, delta, h);
     if (lane < h) dm = 0.0;
     if (lane + h >= 32) dp = 0.0;
-    delta = (delta - __ldg(Tl + 96 + lev * 32 + lane) * dm - __ldg(Tl + 256 + lev * 32 + lane) * dp) *
-            __ldg(Tl + 416 + lev * 32 + lane);
+    delta = (delta - tld<H>(Tl + 96 + lev * 32 + lane) * dm - tld<H>(Tl + 256 + lev * 32 + lane) * dp) *
+            tld<H>(Tl + 416 + lev * 32 + lane);
   }
   double xnext = __shfl_down_sync(0xffffffffu, delta, 1);
   if (lane == 31) xnext = 0.0;
   s[lane] = delta;
 #pragma unroll
   for (int q = 1; q < M; ++q)
-    s[q * LD + lane] = y[q] + __ldg(Tv + q * 32 + lane) * delta + __ldg(Tw + q * 32 + lane) * xnext;
+    s[q * LD + lane] = y[q] + tld<H>(Tv + q * 32 + lane) * delta + tld<H>(Tw + q * 32 + lane) * xnext;
 }
 
 // ------------------------------------------------------------------------------------------
@@ -72,15 +115,15 @@ template <typename TE> __device__ __forceinline__ TE cv(double v) { return (TE)v
 // construction; those terms are left out instead of being evaluated to zero.
 
 // ExplicitTermsVX.F90:30-127 + ImplicitAndUpdateVX.F90:39-66, k = 1..nxm-1 (0-based)
-template <typename TE, bool TWO_D, bool SAL>
+template <typename TE, bool TWO_D, bool SAL, int H = 0>
 __device__ __forceinline__ double rhs_vx(const Geom &g, const Tables &t, const StepCoef &sc, int k,
                                          const ColV &X, const ColV &Y, const ColV &Z, const ColV &T,
                                          const ColV &P, double ru, TE &qout, double sb) {
   const int km = k - 1, kp = k + 1;
   const TE udy = (TE)(g.dy * 0.25), udz = (TE)(g.dz * 0.25);
   const TE udyq = (TE)g.udyq_re, udzq = (TE)g.udzq_re;
-  const TE idxm = cv<TE>(__ldg(t.idx + km)), idxc = cv<TE>(__ldg(t.idx + k));
-  const TE udx3c = cv<TE>(__ldg(t.udx3c + k));
+  const TE idxm = cv<TE>(tld<H>(t.idx + km)), idxc = cv<TE>(tld<H>(t.idx + k));
+  const TE udx3c = cv<TE>(tld<H>(t.udx3c + k));
   const TE vxc = cv<TE>(X.c[k]);
   const TE vxkp = cv<TE>(X.c[kp]), vxkm = cv<TE>(X.c[km]);
   const TE vxip = cv<TE>(X.ip[k]), vxim = cv<TE>(X.im[k]);
@@ -104,15 +147,15 @@ __device__ __forceinline__ double rhs_vx(const Geom &g, const Tables &t, const S
     if constexpr (SAL) qcap = qcap - (TE)sb;  // AddSalBuoyancy(qcap)
   }
   const double alre = sc.alre;
-  const double udx3 = sc.al * __ldg(t.udx3c + k);
-  const double dxxvx = X.c[kp] * __ldg(t.ap3ck + k) + X.c[k] * __ldg(t.ac3ck + k) + X.c[km] * __ldg(t.am3ck + k);
+  const double udx3 = sc.al * tld<H>(t.udx3c + k);
+  const double dxxvx = X.c[kp] * tld<H>(t.ap3ck + k) + X.c[k] * tld<H>(t.ac3ck + k) + X.c[km] * tld<H>(t.am3ck + k);
   const double dxp = (P.c[k] - P.c[km]) * udx3;
   qout = qcap;
   return (sc.ga * (double)qcap + sc.ro * ru + alre * dxxvx - dxp) * sc.dt;
 }
 
 // ExplicitTermsVY.F90:23-122 + ImplicitAndUpdateVY.F90:28-80, k = 0..nxm-1
-template <typename TE, bool TWO_D, bool SAL>
+template <typename TE, bool TWO_D, bool SAL, int H = 0>
 __device__ __forceinline__ double rhs_vy(const Geom &g, const Tables &t, const StepCoef &sc, int k,
                                          const ColV &X, const ColV &Y, const ColV &Z, const ColV &T,
                                          const ColV &P, double zd, double pjm, double ru, TE &qout,
@@ -127,7 +170,7 @@ __device__ __forceinline__ double rhs_vy(const Geom &g, const Tables &t, const S
   const TE vyip = cv<TE>(Y.ip[k]), vyim = cv<TE>(Y.im[k]);
   const TE hyx = ((cv<TE>(X.c[kp]) + cv<TE>(X.jm[kp])) * (cv<TE>(Y.c[kpp]) + c) -
                   (cv<TE>(X.c[k]) + cv<TE>(X.jm[k])) * (c + cv<TE>(Y.c[kmm]))) *
-                 cv<TE>(__ldg(t.udx3m + k)) * (TE)0.25;
+                 cv<TE>(tld<H>(t.udx3m + k)) * (TE)0.25;
   const TE hyy = ((vyjp + c) * (vyjp + c) - (vyjm + c) * (vyjm + c)) * udy;
   const TE dyyvy = (vyjp - (TE)2.0 * c + vyjm) * udyq;
   TE dph;
@@ -146,7 +189,7 @@ __device__ __forceinline__ double rhs_vy(const Geom &g, const Tables &t, const S
   }
   const double alre = sc.alre;
   const double udyp = g.dy * sc.al;
-  const double amm = __ldg(t.am3sk + k), acc = __ldg(t.ac3sk + k), app = __ldg(t.ap3sk + k);
+  const double amm = tld<H>(t.am3sk + k), acc = tld<H>(t.ac3sk + k), app = tld<H>(t.ap3sk + k);
   const double cd = Y.c[k];
   double dxxvy;
   if (k == 0)
@@ -161,7 +204,7 @@ __device__ __forceinline__ double rhs_vy(const Geom &g, const Tables &t, const S
 }
 
 // ExplicitTermsVZ.F90:23-118 + ImplicitAndUpdateVZ.F90:38-69, k = 0..nxm-1
-template <typename TE, bool TWO_D, bool SAL>
+template <typename TE, bool TWO_D, bool SAL, int H = 0>
 __device__ __forceinline__ double rhs_vz(const Geom &g, const Tables &t, const StepCoef &sc, int k,
                                          const ColV &X, const ColV &Y, const ColV &Z, const ColV &T,
                                          const ColV &P, double yd, double pim, double ru, TE &qout,
@@ -178,7 +221,7 @@ __device__ __forceinline__ double rhs_vz(const Geom &g, const Tables &t, const S
                  udy;
   const TE hzx = ((cv<TE>(X.c[kp]) + cv<TE>(X.im[kp])) * (cv<TE>(Z.c[kpp]) + c) -
                   (cv<TE>(X.c[k]) + cv<TE>(X.im[k])) * (c + cv<TE>(Z.c[kmm]))) *
-                 cv<TE>(__ldg(t.udx3m + k)) * (TE)0.25;
+                 cv<TE>(tld<H>(t.udx3m + k)) * (TE)0.25;
   const TE dyyvz = (vzjp - (TE)2.0 * c + vzjm) * udyq;
   TE dq;
   if constexpr (TWO_D) {
@@ -194,7 +237,7 @@ __device__ __forceinline__ double rhs_vz(const Geom &g, const Tables &t, const S
     if constexpr (SAL) dq = dq - (TE)sb;  // AddSalBuoyancy(dq)
   }
   const double alre = sc.alre;
-  const double amm = __ldg(t.am3sk + k), acc = __ldg(t.ac3sk + k), app = __ldg(t.ap3sk + k);
+  const double amm = tld<H>(t.am3sk + k), acc = tld<H>(t.ac3sk + k), app = tld<H>(t.ap3sk + k);
   const double dxxvz = Z.c[kpp] * app + Z.c[k] * acc + Z.c[kmm] * amm;
   qout = dq;
   if constexpr (TWO_D) {
@@ -206,14 +249,14 @@ __device__ __forceinline__ double rhs_vz(const Geom &g, const Tables &t, const S
 }
 
 // ExplicitTermsTemp.F90:22-77 + ImplicitAndUpdateTemp.F90:33-66, k = 0..nxm-1
-template <typename TE, bool TWO_D>
+template <typename TE, bool TWO_D, int H = 0>
 __device__ __forceinline__ double rhs_temp(const Geom &g, const Tables &t, const StepCoef &sc, int k,
                                            const ColV &X, const ColV &Y, const ColV &Z, const ColV &T,
                                            double tbp, double ttp, double ru, TE &qout) {
   const TE udz = (TE)(g.dz * 0.5), udy = (TE)(g.dy * 0.5);
   const TE udzq = (TE)g.udzq_pe, udyq = (TE)g.udyq_pe;
   const TE tc = cv<TE>(T.c[k]);
-  const TE ux = cv<TE>(__ldg(t.udx3m + k));
+  const TE ux = cv<TE>(tld<H>(t.udx3m + k));
   TE htx;
   if (k == 0)
     htx = (cv<TE>(X.c[1]) * (cv<TE>(T.c[1]) + tc) - cv<TE>(X.c[0]) * (TE)2.0 * (TE)tbp) * (TE)0.5 * ux;
@@ -238,12 +281,12 @@ __device__ __forceinline__ double rhs_temp(const Geom &g, const Tables &t, const
   const double tcd = T.c[k];
   double dxxt;
   if (k == 0)
-    dxxt = T.c[1] * __ldg(t.ap3ssk) + tcd * __ldg(t.ac3ssk) - (__ldg(t.ap3ssk) + __ldg(t.ac3ssk)) * tbp * g.tfixs;
+    dxxt = T.c[1] * tld<H>(t.ap3ssk) + tcd * tld<H>(t.ac3ssk) - (tld<H>(t.ap3ssk) + tld<H>(t.ac3ssk)) * tbp * g.tfixs;
   else if (k == g.nxm - 1)
-    dxxt = tcd * __ldg(t.ac3ssk + k) + T.c[k - 1] * __ldg(t.am3ssk + k) -
-           (__ldg(t.am3ssk + k) + __ldg(t.ac3ssk + k)) * ttp * g.tfixn;
+    dxxt = tcd * tld<H>(t.ac3ssk + k) + T.c[k - 1] * tld<H>(t.am3ssk + k) -
+           (tld<H>(t.am3ssk + k) + tld<H>(t.ac3ssk + k)) * ttp * g.tfixn;
   else
-    dxxt = T.c[k + 1] * __ldg(t.ap3ssk + k) + tcd * __ldg(t.ac3ssk + k) + T.c[k - 1] * __ldg(t.am3ssk + k);
+    dxxt = T.c[k + 1] * tld<H>(t.ap3ssk + k) + tcd * tld<H>(t.ac3ssk + k) + T.c[k - 1] * tld<H>(t.am3ssk + k);
   qout = hro;
   return (sc.ga * (double)hro + sc.ro * ru + alpec * dxxt) * sc.dt;
 }
@@ -289,7 +332,7 @@ template <int CAP, int TPC>
 constexpr int k1_min_blocks() {
   return CAP == 0 ? 1 : ((CAP == 1 ? 512 : 1024) / TPC > 1 ? (CAP == 1 ? 512 : 1024) / TPC : 1);
 }
-template <int M, int TPC, int RPT, typename TE, bool TWO_D, int CAP, bool SAL>
+template <int M, int TPC, int RPT, typename TE, bool TWO_D, int CAP, bool SAL, int POL>
 __global__ void __launch_bounds__(TPC, k1_min_blocks<CAP, TPC>())
     k_explicit_implicit(Geom g0, Tables t, const StepCoef *__restrict__ sc_all, int ns,
                         const double *__restrict__ cn_tab, const double *__restrict__ vx,
@@ -300,6 +343,7 @@ __global__ void __launch_bounds__(TPC, k1_min_blocks<CAP, TPC>())
                         double *__restrict__ vz_o, double *__restrict__ temp_o, int *__restrict__ err) {
   constexpr int LD = chunk_ld(M);
   constexpr int FLD = LD * M;
+  constexpr int H = POL & 1;  // cache policy of the global loads (tld / nld / sld above)
   extern __shared__ __align__(128) unsigned char smem_k1[];
   __shared__ uint64_t bar;
   Geom g = g0;
@@ -362,21 +406,21 @@ __global__ void __launch_bounds__(TPC, k1_min_blocks<CAP, TPC>())
   for (int p = 0; p < RPT; ++p) {
     const int k = tc + TPC * p;
     const bool in = k < g.nxm;
-    uu[p][0] = (in && k >= 1) ? (double)rux[c0 + k] : 0.0;
-    uu[p][1] = in ? (double)ruy[c0 + k] : 0.0;
-    uu[p][2] = in ? (double)ruz[c0 + k] : 0.0;
-    uu[p][3] = in ? (double)rut[c0 + k] : 0.0;
+    uu[p][0] = (in && k >= 1) ? sld<H>(rux + c0 + k) : 0.0;
+    uu[p][1] = in ? sld<H>(ruy + c0 + k) : 0.0;
+    uu[p][2] = in ? sld<H>(ruz + c0 + k) : 0.0;
+    uu[p][3] = in ? sld<H>(rut + c0 + k) : 0.0;
     if constexpr (TWO_D) {
       vv[p][0] = 0.0;  // taken from the staged vz(j-1) / vy(j+1) columns below
       vv[p][1] = 0.0;
       vv[p][3] = 0.0;  // pr(i-1) is the centre column
     } else {
-      vv[p][0] = in ? __ldg(vz + o_jmip + k) : 0.0;
-      vv[p][1] = in ? __ldg(vy + o_jpim + k) : 0.0;
-      vv[p][3] = in ? __ldg(pr + o_im + k) : 0.0;
+      vv[p][0] = in ? nld<H>(vz + o_jmip + k) : 0.0;
+      vv[p][1] = in ? nld<H>(vy + o_jpim + k) : 0.0;
+      vv[p][3] = in ? nld<H>(pr + o_im + k) : 0.0;
     }
-    vv[p][2] = in ? __ldg(pr + o_jm + k) : 0.0;
-    if constexpr (SAL) sbv[p] = in ? g.bycs * __ldg(g.salc + c0 + k) : 0.0;
+    vv[p][2] = in ? nld<H>(pr + o_jm + k) : 0.0;
+    if constexpr (SAL) sbv[p] = in ? g.bycs * nld<H>(g.salc + c0 + k) : 0.0;
   }
   bool ok = mbar_wait(&bar, 0, kSpinLimit);
   // test hook: phase 1 of the barrier is never completed, so this wait always runs out
@@ -402,7 +446,7 @@ __global__ void __launch_bounds__(TPC, k1_min_blocks<CAP, TPC>())
   const double *TT = cn_tab + (size_t)(slot * 3 + 2) * tsz;
   const int nxm = g.nxm;
   const size_t pl = (size_t)j + (size_t)g.nym * i;
-  const double tbp = __ldg(t.tempbp + pl), ttp = __ldg(t.temptp + pl);
+  const double tbp = nld<H>(t.tempbp + pl), ttp = nld<H>(t.temptp + pl);
   double rr[RPT][4];
 #pragma unroll
   for (int p = 0; p < RPT; ++p) {
@@ -418,10 +462,10 @@ __global__ void __launch_bounds__(TPC, k1_min_blocks<CAP, TPC>())
       double sb = 0.0;
       if constexpr (SAL) sb = sbv[p];
       // all four right-hand sides from the staged columns before anything is stored
-      rr[p][0] = (k >= 1) ? rhs_vx<TE, TWO_D, SAL>(g, t, sc, k, X, Y, Z, T, P, u0, q0, sb) * __ldg(TX + k - 1) : 0.0;
-      rr[p][1] = rhs_vy<TE, TWO_D, SAL>(g, t, sc, k, X, Y, Z, T, P, zd, vv[p][2], u1, q1, sb) * __ldg(TY + k);
-      rr[p][2] = rhs_vz<TE, TWO_D, SAL>(g, t, sc, k, X, Y, Z, T, P, yd, pim, u2, q2, sb) * __ldg(TY + k);
-      rr[p][3] = rhs_temp<TE, TWO_D>(g, t, sc, k, X, Y, Z, T, tbp, ttp, u3, q3) * __ldg(TT + k);
+      rr[p][0] = (k >= 1) ? rhs_vx<TE, TWO_D, SAL, H>(g, t, sc, k, X, Y, Z, T, P, u0, q0, sb) * tld<H>(TX + k - 1) : 0.0;
+      rr[p][1] = rhs_vy<TE, TWO_D, SAL, H>(g, t, sc, k, X, Y, Z, T, P, zd, vv[p][2], u1, q1, sb) * tld<H>(TY + k);
+      rr[p][2] = rhs_vz<TE, TWO_D, SAL, H>(g, t, sc, k, X, Y, Z, T, P, yd, pim, u2, q2, sb) * tld<H>(TY + k);
+      rr[p][3] = rhs_temp<TE, TWO_D, H>(g, t, sc, k, X, Y, Z, T, tbp, ttp, u3, q3) * tld<H>(TT + k);
       if (k >= 1) rux[c0 + k] = q0;
       ruy[c0 + k] = q1;
       ruz[c0 + k] = q2;
@@ -459,7 +503,7 @@ __global__ void __launch_bounds__(TPC, k1_min_blocks<CAP, TPC>())
     constexpr int NW = TPC / 32;
     for (int f = warp; f < 4; f += NW) {
       const double *Tb = (f == 0) ? TX : ((f == 3) ? TT : TY);
-      cn_solve_chunk<M, LD>(s_rhs + f * FLD, Tb, lane);
+      cn_solve_chunk<M, LD, H>(s_rhs + f * FLD, Tb, lane);
     }
   }
   __syncthreads();
@@ -482,12 +526,26 @@ __global__ void __launch_bounds__(TPC, k1_min_blocks<CAP, TPC>())
   }
 }
 
-template <int M, int TPC, int RPT, typename TE, bool TWO_D, int CAP, bool SAL>
+// Shared-memory carve-out (percent of the SM's 228 KB) that holds `blocks` resident blocks of
+// K1 with `smem` bytes each (1 KB per block reserved by the system): fewer blocks than the
+// default leave more of the SM's 256 KB of L1/shared storage to L1.
+inline int k1_carveout_pct(size_t smem, int blocks) {
+  const size_t need = (size_t)blocks * (smem + 1024);
+  const int pct = (int)((need * 100 + 233471) / 233472);
+  return pct > 100 ? 100 : pct;
+}
+
+template <int M, int TPC, int RPT, typename TE, bool TWO_D, int CAP, bool SAL, int POL>
 cudaError_t launch_k1_cfg(const LaunchCtx &L, const SubstepBuffers &b, int ns, int ncol) {
   const size_t smem = k1_smem(L.g.ldx, M, TWO_D);
-  auto kern = k_explicit_implicit<M, TPC, RPT, TE, TWO_D, CAP, SAL>;
+  auto kern = k_explicit_implicit<M, TPC, RPT, TE, TWO_D, CAP, SAL, POL>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
+  if constexpr ((POL >> 1) != 0) {  // a carve-out for POL >> 1 resident blocks per SM
+    e = cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout,
+                             k1_carveout_pct(smem, POL >> 1));
+    if (e != cudaSuccess) return e;
+  }
   kern<<<ncol, TPC, smem, L.stream>>>(L.g, L.t, b.sc, ns, b.cn_tab, b.vx, b.vy, b.vz, b.temp, b.pr,
                                       (TE *)b.rux, (TE *)b.ruy, (TE *)b.ruz, (TE *)b.rut, b.vx_o, b.vy_o,
                                       b.vz_o, b.temp_o, b.err);
@@ -495,25 +553,31 @@ cudaError_t launch_k1_cfg(const LaunchCtx &L, const SubstepBuffers &b, int ns, i
 }
 
 // Thread shapes of K1 per M = {1, 2, 4, 8, 12, 16, 24, 32} (rows per lane of the CN solves):
-// {threads per column, rows per thread, register cap level}, threads x rows >= 32 M.  The first
-// is the default.
+// {threads per column, rows per thread, register cap level, memory policy}, threads x rows >=
+// 32 M.  Memory policy: bit 0 = the cache hints of tld / nld / sld; the bits above = resident
+// blocks per SM that the shared-memory carve-out is sized for (0: the driver's default, which
+// packs as many blocks as shared memory allows and leaves the rest to L1).  The first entry is
+// the default.
 struct K1Shape {
-  int tpc, rpt, cap;
+  int tpc, rpt, cap, pol;
 };
-constexpr int kK1MaxShapes = 5;
+constexpr int kK1MaxShapes = 8;
 constexpr int k1_m_index(int M) {
   return M == 1 ? 0 : M == 2 ? 1 : M == 4 ? 2 : M == 8 ? 3 : M == 12 ? 4 : M == 16 ? 5 : M == 24 ? 6 : 7;
 }
-constexpr int kK1ShapeCount[8] = {1, 2, 3, 4, 5, 5, 3, 2};
+constexpr int kK1ShapeCount[8] = {2, 3, 4, 8, 7, 7, 5, 4};
 constexpr K1Shape kK1Shapes[8][kK1MaxShapes] = {
-    {{32, 1, 0}, {0, 0, 0}, {0, 0, 0}, {0, 0, 0}, {0, 0, 0}},          // M = 1   (nxm <= 32)
-    {{64, 1, 0}, {32, 2, 1}, {0, 0, 0}, {0, 0, 0}, {0, 0, 0}},         // M = 2   (<= 64)
-    {{128, 1, 0}, {64, 2, 1}, {128, 1, 2}, {0, 0, 0}, {0, 0, 0}},      // M = 4   (<= 128)
-    {{128, 2, 1}, {256, 1, 0}, {128, 2, 0}, {256, 1, 2}, {0, 0, 0}},   // M = 8   (<= 256)
-    {{128, 3, 1}, {256, 2, 1}, {384, 1, 0}, {128, 3, 0}, {384, 1, 2}}, // M = 12  (<= 384)
-    {{128, 4, 1}, {256, 2, 1}, {512, 1, 0}, {128, 4, 0}, {512, 1, 2}}, // M = 16  (<= 512)
-    {{256, 3, 1}, {384, 2, 0}, {256, 4, 1}, {0, 0, 0}, {0, 0, 0}},     // M = 24  (<= 768)
-    {{256, 4, 1}, {512, 2, 0}, {0, 0, 0}, {0, 0, 0}, {0, 0, 0}},       // M = 32  (<= 1024)
+    {{32, 1, 0, 0}, {32, 1, 0, 1}},                                                    // M = 1   (nxm <= 32)
+    {{64, 1, 0, 0}, {32, 2, 1, 0}, {64, 1, 0, 1}},                                     // M = 2   (<= 64)
+    {{128, 1, 0, 0}, {64, 2, 1, 0}, {128, 1, 2, 0}, {128, 1, 0, 1}},                   // M = 4   (<= 128)
+    {{128, 2, 1, 0}, {256, 1, 0, 0}, {128, 2, 0, 0}, {256, 1, 2, 0},                   // M = 8   (<= 256)
+     {128, 2, 1, 1}, {128, 2, 1, 6}, {128, 2, 1, 7}, {128, 2, 0, 7}},
+    {{128, 3, 1, 0}, {256, 2, 1, 0}, {384, 1, 0, 0}, {128, 3, 0, 0}, {384, 1, 2, 0},   // M = 12  (<= 384)
+     {384, 1, 0, 1}, {128, 3, 1, 1}},
+    {{128, 4, 1, 0}, {256, 2, 1, 0}, {512, 1, 0, 0}, {128, 4, 0, 0}, {512, 1, 2, 0},   // M = 16  (<= 512)
+     {128, 4, 1, 1}, {512, 1, 0, 1}},
+    {{256, 3, 1, 0}, {384, 2, 0, 0}, {256, 4, 1, 0}, {256, 3, 1, 1}, {384, 2, 0, 1}},  // M = 24  (<= 768)
+    {{256, 4, 1, 0}, {512, 2, 0, 0}, {256, 4, 1, 1}, {512, 2, 0, 1}},                  // M = 32  (<= 1024)
 };
 
 template <int M, int V, typename TE, bool TWO_D, bool SAL>
@@ -521,9 +585,9 @@ cudaError_t launch_k1_v(const LaunchCtx &L, const SubstepBuffers &b, int ns, int
   constexpr int mi = k1_m_index(M);
   if constexpr (V < kK1ShapeCount[mi]) {
     constexpr int TPC = kK1Shapes[mi][V].tpc, RPT = kK1Shapes[mi][V].rpt;
-    constexpr int CAP = kK1Shapes[mi][V].cap;
+    constexpr int CAP = kK1Shapes[mi][V].cap, POL = kK1Shapes[mi][V].pol;
     static_assert(TPC * RPT >= 32 * M, "K1 shape must cover 32*M rows");
-    return launch_k1_cfg<M, TPC, RPT, TE, TWO_D, CAP, SAL>(L, b, ns, ncol);
+    return launch_k1_cfg<M, TPC, RPT, TE, TWO_D, CAP, SAL, POL>(L, b, ns, ncol);
   } else {
     return cudaErrorInvalidValue;
   }
@@ -537,6 +601,9 @@ cudaError_t launch_k1_M(const LaunchCtx &L, const SubstepBuffers &b, int ns, int
     case 2: return launch_k1_v<M, 2, TE, TWO_D, SAL>(L, b, ns, ncol);
     case 3: return launch_k1_v<M, 3, TE, TWO_D, SAL>(L, b, ns, ncol);
     case 4: return launch_k1_v<M, 4, TE, TWO_D, SAL>(L, b, ns, ncol);
+    case 5: return launch_k1_v<M, 5, TE, TWO_D, SAL>(L, b, ns, ncol);
+    case 6: return launch_k1_v<M, 6, TE, TWO_D, SAL>(L, b, ns, ncol);
+    case 7: return launch_k1_v<M, 7, TE, TWO_D, SAL>(L, b, ns, ncol);
   }
   return cudaErrorInvalidValue;
 }

@@ -10,12 +10,14 @@ cudaError_t launch_k1_fp64(const LaunchCtx &L, const SubstepBuffers &b, int ns, 
                : launch_k1_T<double, false, false>(L, b, ns, var, ncol);
 }
 
-int k1_shapes(int M, int *tpc, int *rpt, int *cap) {
+int k1_shapes(int M, int *tpc, int *rpt, int *cap, int *pol) {
   const int mi = k1_m_index(M);
+  static_assert(kK1MaxShapes <= AFID_TUNE_MAX, "the tune record must hold every K1 shape");
   for (int v = 0; v < kK1ShapeCount[mi]; ++v) {
     if (tpc) tpc[v] = kK1Shapes[mi][v].tpc;
     if (rpt) rpt[v] = kK1Shapes[mi][v].rpt;
     if (cap) cap[v] = kK1Shapes[mi][v].cap;
+    if (pol) pol[v] = kK1Shapes[mi][v].pol;
   }
   return kK1ShapeCount[mi];
 }
