@@ -785,7 +785,7 @@ int afid_gpu_cfl(afid_ctx_t *ctx, double *cflm) {
   AFID_CUDA(ctx, cudaMemcpyAsync(ctx->host_scratch, ctx->red, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
   int s = check_err_flag(ctx);
   const double v = ctx->host_scratch[0];
-  *cflm = std::max(0.00000001, v);  // CalcMaxCFL.F90:22
+  *cflm = (v != v) ? v : std::max(0.00000001, v);  // CalcMaxCFL.F90:22; a NaN maximum is passed on
   return s;
 }
 
@@ -1099,7 +1099,8 @@ int afid_gpu_sal_cfl(afid_ctx_t *ctx, double *cflmr) {
   AFID_CUDA(ctx, cudaMemcpyAsync(ctx->host_scratch, ctx->sal->red, sizeof(double), cudaMemcpyDeviceToHost,
                                  ctx->stream));
   const int s = check_err_flag(ctx);
-  *cflmr = std::max(1.0e-8, ctx->host_scratch[0]);  // CalcMaxCFL.F90:50
+  const double v = ctx->host_scratch[0];
+  *cflmr = (v != v) ? v : std::max(1.0e-8, v);  // CalcMaxCFL.F90:50; a NaN maximum is passed on
   return s;
 }
 

@@ -98,6 +98,74 @@ __device__ __forceinline__ void cn_solve_chunk(double *__restrict__ s, const dou
     s[q * LD + lane] = y[q] + tld<H>(Tv + q * 32 + lane) * delta + tld<H>(Tw + q * 32 + lane) * xnext;
 }
 
+// Two columns with the same matrix (s0, s1: chunk layout as above) solved by one warp: every
+// factor is loaded once and applied to both right-hand sides, in the same operation order as
+// cn_solve_chunk (so each solution is bitwise the same as a single solve).
+template <int M, int LD = 32, int H = 0>
+__device__ __forceinline__ void cn_solve_chunk2(double *__restrict__ s0, double *__restrict__ s1,
+                                                const double *__restrict__ T, int lane) {
+  const double *Ta = T + 32 * M, *Tinv = T + 64 * M, *Tcp = T + 96 * M, *Tv = T + 128 * M,
+               *Tw = T + 160 * M, *Tl = T + 192 * M;
+  double y[M], z[M];
+#pragma unroll
+  for (int q = 0; q < M; ++q) {
+    y[q] = s0[q * LD + lane];
+    z[q] = s1[q * LD + lane];
+  }
+  if constexpr (M > 1) {
+    const double i1 = tld<H>(Tinv + 32 + lane);
+    y[1] = y[1] * i1;
+    z[1] = z[1] * i1;
+#pragma unroll
+    for (int q = 2; q < M; ++q) {
+      const double a = tld<H>(Ta + q * 32 + lane), iv = tld<H>(Tinv + q * 32 + lane);
+      y[q] = (y[q] - a * y[q - 1]) * iv;
+      z[q] = (z[q] - a * z[q - 1]) * iv;
+    }
+#pragma unroll
+    for (int q = M - 2; q >= 1; --q) {
+      const double cp = tld<H>(Tcp + q * 32 + lane);
+      y[q] = y[q] - cp * y[q + 1];
+      z[q] = z[q] - cp * z[q + 1];
+    }
+  }
+  double Dy, Dz;
+  if constexpr (M > 1) {
+    double yprev = __shfl_up_sync(0xffffffffu, y[M - 1], 1);
+    double zprev = __shfl_up_sync(0xffffffffu, z[M - 1], 1);
+    if (lane == 0) yprev = zprev = 0.0;
+    const double l0 = tld<H>(Tl + lane), l1 = tld<H>(Tl + 32 + lane);
+    Dy = y[0] - l0 * yprev - l1 * y[1];
+    Dz = z[0] - l0 * zprev - l1 * z[1];
+  } else {
+    Dy = y[0];
+    Dz = z[0];
+  }
+  const double l2 = tld<H>(Tl + 64 + lane);
+  double dy = Dy * l2, dz = Dz * l2;
+#pragma unroll
+  for (int lev = 0, h = 1; lev < 5; ++lev, h <<= 1) {
+    double ym = __shfl_up_sync(0xffffffffu, dy, h), yp = __shfl_down_sync(0xffffffffu, dy, h);
+    double zm = __shfl_up_sync(0xffffffffu, dz, h), zp = __shfl_down_sync(0xffffffffu, dz, h);
+    if (lane < h) ym = zm = 0.0;
+    if (lane + h >= 32) yp = zp = 0.0;
+    const double lm = tld<H>(Tl + 96 + lev * 32 + lane), lp = tld<H>(Tl + 256 + lev * 32 + lane),
+                 li = tld<H>(Tl + 416 + lev * 32 + lane);
+    dy = (dy - lm * ym - lp * yp) * li;
+    dz = (dz - lm * zm - lp * zp) * li;
+  }
+  double ynext = __shfl_down_sync(0xffffffffu, dy, 1), znext = __shfl_down_sync(0xffffffffu, dz, 1);
+  if (lane == 31) ynext = znext = 0.0;
+  s0[lane] = dy;
+  s1[lane] = dz;
+#pragma unroll
+  for (int q = 1; q < M; ++q) {
+    const double v = tld<H>(Tv + q * 32 + lane), w = tld<H>(Tw + q * 32 + lane);
+    s0[q * LD + lane] = y[q] + v * dy + w * ynext;
+    s1[q * LD + lane] = z[q] + v * dz + w * znext;
+  }
+}
+
 // ------------------------------------------------------------------------------------------
 // Explicit terms + RHS, one (k, j, i) point each.  Expressions follow the reference loop
 // bodies term by term; TE is the arithmetic type of the explicit terms.  The operands are
@@ -526,13 +594,260 @@ __global__ void __launch_bounds__(TPC, k1_min_blocks<CAP, TPC>())
   }
 }
 
-// Shared-memory carve-out (percent of the SM's 228 KB) that holds `blocks` resident blocks of
-// K1 with `smem` bytes each (1 KB per block reserved by the system): fewer blocks than the
-// default leave more of the SM's 256 KB of L1/shared storage to L1.
-inline int k1_carveout_pct(size_t smem, int blocks) {
-  const size_t need = (size_t)blocks * (smem + 1024);
-  const int pct = (int)((need * 100 + 233471) / 233472);
-  return pct > 100 ? 100 : pct;
+// K1 on a tile of two neighbouring columns along y, (j0, i) and (j0 + 1, i), j0 even: a thread
+// owns the same rows of both columns, so every metric coefficient it loads serves two cells, and
+// warp f solves field f of both columns with one load of each CN factor (cn_solve_chunk2).  The
+// staged set: vx, vy, vz, temp at j0 - 1 .. j0 + 2 (the y line) and at i +- 1 for both columns
+// (in 3-D), and pr at both columns: 34 columns for two (17 a column instead of 21); in 2-D 18.
+// The single-row operands left are vz(j0-1, i+1), vy(j0+2, i-1), pr(j0-1) and pr(i-1).
+// Layout of the staged columns: centres F*2 + c (F = vx, vy, vz, temp; c = column 0, 1), the
+// y-line ends 8 + F*2 + {0: j0-1, 1: j0+2}, then (3-D) z+ 16 + F*2 + c, z- 24 + F*2 + c, then pr.
+constexpr int kK1Y2Cols = 34;
+constexpr int kK1Y2Cols2D = 18;
+__host__ __device__ inline size_t k1y2_smem(int M, bool two_d) {
+  const int cs = k1_col_stride(M);
+  const size_t st = (size_t)(two_d ? kK1Y2Cols2D : kK1Y2Cols) * cs * sizeof(double);
+  const size_t rhs = (size_t)8 * cs * sizeof(double) + (size_t)8 * chunk_ld(M) * M * sizeof(double);
+  return st > rhs ? st : rhs;
+}
+
+template <int M, int TPC, int RPT, typename TE, bool TWO_D, int CAP, bool SAL, int POL>
+__global__ void __launch_bounds__(TPC, k1_min_blocks<CAP, TPC>())
+    k_explicit_implicit_y2(Geom g0, Tables t, const StepCoef *__restrict__ sc_all, int ns,
+                           const double *__restrict__ cn_tab, const double *__restrict__ vx,
+                           const double *__restrict__ vy, const double *__restrict__ vz,
+                           const double *__restrict__ temp, const double *__restrict__ pr,
+                           TE *__restrict__ rux, TE *__restrict__ ruy, TE *__restrict__ ruz,
+                           TE *__restrict__ rut, double *__restrict__ vx_o, double *__restrict__ vy_o,
+                           double *__restrict__ vz_o, double *__restrict__ temp_o, int *__restrict__ err) {
+  constexpr int LD = chunk_ld(M);
+  constexpr int FLD = LD * M;
+  constexpr int H = POL & 1;
+  constexpr int NS = TWO_D ? kK1Y2Cols2D : kK1Y2Cols;
+  constexpr int PRC = TWO_D ? 16 : 32;  // first pr column
+  extern __shared__ __align__(128) unsigned char smem_k1[];
+  __shared__ uint64_t bar;
+  Geom g = g0;
+  const int ldx = g.ldx;
+  double *cols = reinterpret_cast<double *>(smem_k1);
+  constexpr int CS = k1_col_stride(M);
+  double *s_rhs = cols + (size_t)8 * CS;  // over the non-centre columns, after they are used
+  const int tc = threadIdx.x;
+  const int nyt = g.nym >> 1;
+  const int j0 = 2 * (blockIdx.x % nyt), i = blockIdx.x / nyt;
+  if (!inst_active(g, i)) {
+    for (int c = 0; c < 2; ++c) {
+      const size_t o = col_off(g, j0 + c, i);
+      for (int k = tc; k < g.nx; k += TPC) temp_o[o + k] = temp[o + k];
+    }
+    return;
+  }
+  bind_instance(g, i);
+  const int jm = wrap_dec(j0, g.nym), jp2 = wrap_inc(j0 + 1, g.nym);
+  const int ip = zinc(g, i), im = zdec(g, i);
+  size_t oc[2];
+  oc[0] = col_off(g, j0, i);
+  oc[1] = col_off(g, j0 + 1, i);
+  if (tc == 0) {
+    mbar_init(&bar, 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+  if (tc == 0) {
+    const uint32_t cb = (uint32_t)ldx * sizeof(double);
+    mbar_arrive_expect_tx(&bar, (uint32_t)((size_t)NS * cb));
+    const double *f4[4] = {vx, vy, vz, temp};
+    const size_t ojm = col_off(g, jm, i), ojp2 = col_off(g, jp2, i);
+#pragma unroll
+    for (int F = 0; F < 4; ++F) {
+      bulk_g2s(cols + (size_t)(F * 2 + 0) * CS, f4[F] + oc[0], cb, &bar);
+      bulk_g2s(cols + (size_t)(F * 2 + 1) * CS, f4[F] + oc[1], cb, &bar);
+      bulk_g2s(cols + (size_t)(8 + F * 2 + 0) * CS, f4[F] + ojm, cb, &bar);
+      bulk_g2s(cols + (size_t)(8 + F * 2 + 1) * CS, f4[F] + ojp2, cb, &bar);
+      if constexpr (!TWO_D) {
+        bulk_g2s(cols + (size_t)(16 + F * 2 + 0) * CS, f4[F] + col_off(g, j0, ip), cb, &bar);
+        bulk_g2s(cols + (size_t)(16 + F * 2 + 1) * CS, f4[F] + col_off(g, j0 + 1, ip), cb, &bar);
+        bulk_g2s(cols + (size_t)(24 + F * 2 + 0) * CS, f4[F] + col_off(g, j0, im), cb, &bar);
+        bulk_g2s(cols + (size_t)(24 + F * 2 + 1) * CS, f4[F] + col_off(g, j0 + 1, im), cb, &bar);
+      }
+    }
+    bulk_g2s(cols + (size_t)(PRC + 0) * CS, pr + oc[0], cb, &bar);
+    bulk_g2s(cols + (size_t)(PRC + 1) * CS, pr + oc[1], cb, &bar);
+  }
+  // single-row operands and the RK3 histories straight to registers, before the wait
+  const size_t o_pjm = col_off(g, jm, i);                    // pr(j0 - 1)
+  const size_t o_zd0 = col_off(g, jm, ip);                   // vz(j0 - 1, i + 1)
+  const size_t o_yd1 = col_off(g, jp2, im);                  // vy(j0 + 2, i - 1)
+  const size_t o_pim0 = col_off(g, j0, im), o_pim1 = col_off(g, j0 + 1, im);  // pr(., i - 1)
+  double uu[RPT][2][4];
+  double sv[RPT][5];  // {pr(j0-1), vz(j0-1,i+1), vy(j0+2,i-1), pr(j0,i-1), pr(j0+1,i-1)}
+  double sbv[SAL ? RPT : 1][2];
+#pragma unroll
+  for (int p = 0; p < RPT; ++p) {
+    const int k = tc + TPC * p;
+    const bool in = k < g.nxm;
+#pragma unroll
+    for (int c = 0; c < 2; ++c) {
+      uu[p][c][0] = (in && k >= 1) ? sld<H>(rux + oc[c] + k) : 0.0;
+      uu[p][c][1] = in ? sld<H>(ruy + oc[c] + k) : 0.0;
+      uu[p][c][2] = in ? sld<H>(ruz + oc[c] + k) : 0.0;
+      uu[p][c][3] = in ? sld<H>(rut + oc[c] + k) : 0.0;
+      if constexpr (SAL) sbv[p][c] = in ? g.bycs * nld<H>(g.salc + oc[c] + k) : 0.0;
+    }
+    sv[p][0] = in ? nld<H>(pr + o_pjm + k) : 0.0;
+    if constexpr (!TWO_D) {
+      sv[p][1] = in ? nld<H>(vz + o_zd0 + k) : 0.0;
+      sv[p][2] = in ? nld<H>(vy + o_yd1 + k) : 0.0;
+      sv[p][3] = in ? nld<H>(pr + o_pim0 + k) : 0.0;
+      sv[p][4] = in ? nld<H>(pr + o_pim1 + k) : 0.0;
+    } else {
+      sv[p][1] = sv[p][2] = sv[p][3] = sv[p][4] = 0.0;
+    }
+  }
+  bool ok = mbar_wait(&bar, 0, kSpinLimit);
+  if (g.wait_test_polls > 0) ok = ok && mbar_wait(&bar, 1, g.wait_test_polls);
+  if (!__syncthreads_and(ok)) {
+    if (tc == 0) atomicOr(err, 2);
+    mbar_wait(&bar, 0, kDrainLimit);
+    return;
+  }
+  auto C = [&](int q) { return (const double *)(cols + q * CS); };
+  // column c of field F: {centre, j+1, j-1, i+1, i-1, -}
+  auto colv = [&](int F, int c) {
+    const double *ctr = C(F * 2 + c);
+    const double *jpc = c == 0 ? C(F * 2 + 1) : C(8 + F * 2 + 1);
+    const double *jmc = c == 0 ? C(8 + F * 2) : C(F * 2);
+    if constexpr (TWO_D) return ColV{ctr, jpc, jmc, ctr, ctr, nullptr};
+    return ColV{ctr, jpc, jmc, C(16 + F * 2 + c), C(24 + F * 2 + c), nullptr};
+  };
+  const int slot = sc_slot(g, i, ns);
+  const StepCoef sc = sc_all[slot];
+  const size_t tsz = cn_table_size(M);
+  const double *TX = cn_tab + (size_t)(slot * 3 + 0) * tsz;
+  const double *TY = cn_tab + (size_t)(slot * 3 + 1) * tsz;
+  const double *TT = cn_tab + (size_t)(slot * 3 + 2) * tsz;
+  const int nxm = g.nxm;
+  double rr[RPT][2][4];
+#pragma unroll
+  for (int c = 0; c < 2; ++c) {
+    const ColV X = colv(0, c), Y = colv(1, c), Z = colv(2, c), T = colv(3, c);
+    const ColV P{C(PRC + c), nullptr, nullptr, nullptr, nullptr, nullptr};
+    const size_t pl = (size_t)(j0 + c) + (size_t)g.nym * i;
+    const double tbp = nld<H>(t.tempbp + pl), ttp = nld<H>(t.temptp + pl);
+#pragma unroll
+    for (int p = 0; p < RPT; ++p) {
+      const int k = tc + TPC * p;
+      if (k < nxm) {
+        TE q0 = (TE)0, q1, q2, q3;
+        // vz(j-1, i+1), vy(j+1, i-1), pr(j-1), pr(i-1) of column c
+        double zd, yd, pjm, pim;
+        if constexpr (TWO_D) {
+          zd = c == 0 ? C(8 + 2 * 2)[k] : C(2 * 2)[k];        // vz(j-1)
+          yd = c == 0 ? C(1 * 2 + 1)[k] : C(8 + 1 * 2 + 1)[k];  // vy(j+1)
+          pim = P.c[k];
+        } else {
+          zd = c == 0 ? sv[p][1] : C(16 + 2 * 2 + 0)[k];        // vz(j0, i+1) staged for column 1
+          yd = c == 0 ? C(24 + 1 * 2 + 1)[k] : sv[p][2];        // vy(j0+1, i-1) staged for column 0
+          pim = c == 0 ? sv[p][3] : sv[p][4];
+        }
+        pjm = c == 0 ? sv[p][0] : C(PRC)[k];
+        double sb = 0.0;
+        if constexpr (SAL) sb = sbv[p][c];
+        rr[p][c][0] = (k >= 1) ? rhs_vx<TE, TWO_D, SAL, H>(g, t, sc, k, X, Y, Z, T, P, uu[p][c][0], q0, sb) *
+                                     tld<H>(TX + k - 1)
+                               : 0.0;
+        rr[p][c][1] = rhs_vy<TE, TWO_D, SAL, H>(g, t, sc, k, X, Y, Z, T, P, zd, pjm, uu[p][c][1], q1, sb) *
+                      tld<H>(TY + k);
+        rr[p][c][2] = rhs_vz<TE, TWO_D, SAL, H>(g, t, sc, k, X, Y, Z, T, P, yd, pim, uu[p][c][2], q2, sb) *
+                      tld<H>(TY + k);
+        rr[p][c][3] = rhs_temp<TE, TWO_D, H>(g, t, sc, k, X, Y, Z, T, tbp, ttp, uu[p][c][3], q3) * tld<H>(TT + k);
+        if (k >= 1) rux[oc[c] + k] = q0;
+        ruy[oc[c] + k] = q1;
+        ruz[oc[c] + k] = q2;
+        rut[oc[c] + k] = q3;
+      }
+    }
+  }
+  __syncthreads();  // every non-centre column is dead from here on
+  // system s = c * 4 + F over the dead columns; padding rows as in the one-column kernel
+#pragma unroll
+  for (int p = 0; p < RPT; ++p) {
+    const int k = tc + TPC * p;
+    if (k < nxm) {
+      const int sk = (k % M) * LD + k / M;
+#pragma unroll
+      for (int c = 0; c < 2; ++c) {
+        double *sr = s_rhs + (size_t)c * 4 * FLD;
+        if (k >= 1) {
+          const int r = k - 1;
+          sr[(r % M) * LD + r / M] = rr[p][c][0];
+        }
+        sr[FLD + sk] = rr[p][c][1];
+        sr[2 * FLD + sk] = rr[p][c][2];
+        sr[3 * FLD + sk] = rr[p][c][3];
+      }
+    }
+  }
+  for (int r = nxm - 1 + tc; r < 32 * M; r += TPC) {
+    const int sr = (r % M) * LD + r / M;
+#pragma unroll
+    for (int c = 0; c < 2; ++c) {
+      double *b = s_rhs + (size_t)c * 4 * FLD;
+      b[sr] = 0.0;
+      if (r >= nxm) {
+        b[FLD + sr] = 0.0;
+        b[2 * FLD + sr] = 0.0;
+        b[3 * FLD + sr] = 0.0;
+      }
+    }
+  }
+  __syncthreads();
+  {
+    const int warp = tc >> 5, lane = tc & 31;
+    constexpr int NW = TPC / 32;
+    for (int f = warp; f < 4; f += NW) {
+      const double *Tb = (f == 0) ? TX : ((f == 3) ? TT : TY);
+      cn_solve_chunk2<M, LD, H>(s_rhs + f * FLD, s_rhs + (4 + f) * FLD, Tb, lane);
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int c = 0; c < 2; ++c) {
+    const double *sr = s_rhs + (size_t)c * 4 * FLD;
+    const double *Xc = C(0 * 2 + c), *Yc = C(1 * 2 + c), *Zc = C(2 * 2 + c), *Tc = C(3 * 2 + c);
+#pragma unroll
+    for (int p = 0; p < RPT; ++p) {
+      const int k = tc + TPC * p;
+      if (k < nxm) {
+        const int sk = (k % M) * LD + k / M;
+        if (k >= 1) {
+          const int r = k - 1;
+          vx_o[oc[c] + k] = Xc[k] + sr[(r % M) * LD + r / M];
+        } else {
+          vx_o[oc[c]] = 0.0;  // ImplicitAndUpdateVX.F90:86-87: vx(1) = vx(nx) = 0
+          vx_o[oc[c] + nxm] = 0.0;
+        }
+        vy_o[oc[c] + k] = Yc[k] + sr[FLD + sk];
+        vz_o[oc[c] + k] = Zc[k] + sr[2 * FLD + sk];
+        temp_o[oc[c] + k] = Tc[k] + sr[3 * FLD + sk];
+      }
+    }
+  }
+}
+
+// The two-column tile: ncol / 2 blocks; needs an even nym (every x-column pair within a row of
+// the y-z plane) and an even ncol.
+template <int M, int TPC, int RPT, typename TE, bool TWO_D, int CAP, bool SAL, int POL>
+cudaError_t launch_k1y2_cfg(const LaunchCtx &L, const SubstepBuffers &b, int ns, int ncol) {
+  if ((L.g.nym & 1) || (ncol & 1)) return cudaErrorInvalidValue;
+  const size_t smem = k1y2_smem(M, TWO_D);
+  auto kern = k_explicit_implicit_y2<M, TPC, RPT, TE, TWO_D, CAP, SAL, POL>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  kern<<<ncol / 2, TPC, smem, L.stream>>>(L.g, L.t, b.sc, ns, b.cn_tab, b.vx, b.vy, b.vz, b.temp, b.pr,
+                                          (TE *)b.rux, (TE *)b.ruy, (TE *)b.ruz, (TE *)b.rut, b.vx_o, b.vy_o,
+                                          b.vz_o, b.temp_o, b.err);
+  return cudaGetLastError();
 }
 
 template <int M, int TPC, int RPT, typename TE, bool TWO_D, int CAP, bool SAL, int POL>
@@ -541,43 +856,39 @@ cudaError_t launch_k1_cfg(const LaunchCtx &L, const SubstepBuffers &b, int ns, i
   auto kern = k_explicit_implicit<M, TPC, RPT, TE, TWO_D, CAP, SAL, POL>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
-  if constexpr ((POL >> 1) != 0) {  // a carve-out for POL >> 1 resident blocks per SM
-    e = cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout,
-                             k1_carveout_pct(smem, POL >> 1));
-    if (e != cudaSuccess) return e;
-  }
   kern<<<ncol, TPC, smem, L.stream>>>(L.g, L.t, b.sc, ns, b.cn_tab, b.vx, b.vy, b.vz, b.temp, b.pr,
                                       (TE *)b.rux, (TE *)b.ruy, (TE *)b.ruz, (TE *)b.rut, b.vx_o, b.vy_o,
                                       b.vz_o, b.temp_o, b.err);
   return cudaGetLastError();
 }
 
-// Thread shapes of K1 per M = {1, 2, 4, 8, 12, 16, 24, 32} (rows per lane of the CN solves):
-// {threads per column, rows per thread, register cap level, memory policy}, threads x rows >=
-// 32 M.  Memory policy: bit 0 = the cache hints of tld / nld / sld; the bits above = resident
-// blocks per SM that the shared-memory carve-out is sized for (0: the driver's default, which
-// packs as many blocks as shared memory allows and leaves the rest to L1).  The first entry is
-// the default.
+// Launch shapes of K1 per M = {1, 2, 4, 8, 12, 16, 24, 32} (rows per lane of the CN solves):
+// {threads per block, rows per thread, register cap level, cache policy (1: the hints of tld /
+// nld / sld), columns per block along y (1 or 2, the tile of k_explicit_implicit_y2)}, threads x
+// rows >= 32 M.  The first entry is the default.
 struct K1Shape {
-  int tpc, rpt, cap, pol;
+  int tpc, rpt, cap, pol, ny;
 };
 constexpr int kK1MaxShapes = 8;
 constexpr int k1_m_index(int M) {
   return M == 1 ? 0 : M == 2 ? 1 : M == 4 ? 2 : M == 8 ? 3 : M == 12 ? 4 : M == 16 ? 5 : M == 24 ? 6 : 7;
 }
-constexpr int kK1ShapeCount[8] = {2, 3, 4, 8, 7, 7, 5, 4};
+constexpr int kK1ShapeCount[8] = {3, 4, 6, 8, 8, 8, 6, 5};
 constexpr K1Shape kK1Shapes[8][kK1MaxShapes] = {
-    {{32, 1, 0, 0}, {32, 1, 0, 1}},                                                    // M = 1   (nxm <= 32)
-    {{64, 1, 0, 0}, {32, 2, 1, 0}, {64, 1, 0, 1}},                                     // M = 2   (<= 64)
-    {{128, 1, 0, 0}, {64, 2, 1, 0}, {128, 1, 2, 0}, {128, 1, 0, 1}},                   // M = 4   (<= 128)
-    {{128, 2, 1, 0}, {256, 1, 0, 0}, {128, 2, 0, 0}, {256, 1, 2, 0},                   // M = 8   (<= 256)
-     {128, 2, 1, 1}, {128, 2, 1, 6}, {128, 2, 1, 7}, {128, 2, 0, 7}},
-    {{128, 3, 1, 0}, {256, 2, 1, 0}, {384, 1, 0, 0}, {128, 3, 0, 0}, {384, 1, 2, 0},   // M = 12  (<= 384)
-     {384, 1, 0, 1}, {128, 3, 1, 1}},
-    {{128, 4, 1, 0}, {256, 2, 1, 0}, {512, 1, 0, 0}, {128, 4, 0, 0}, {512, 1, 2, 0},   // M = 16  (<= 512)
-     {128, 4, 1, 1}, {512, 1, 0, 1}},
-    {{256, 3, 1, 0}, {384, 2, 0, 0}, {256, 4, 1, 0}, {256, 3, 1, 1}, {384, 2, 0, 1}},  // M = 24  (<= 768)
-    {{256, 4, 1, 0}, {512, 2, 0, 0}, {256, 4, 1, 1}, {512, 2, 0, 1}},                  // M = 32  (<= 1024)
+    {{32, 1, 0, 0, 1}, {32, 1, 0, 1, 1}, {32, 1, 0, 1, 2}},                               // M = 1   (nxm <= 32)
+    {{64, 1, 0, 0, 1}, {32, 2, 1, 0, 1}, {64, 1, 0, 1, 1}, {64, 1, 0, 1, 2}},             // M = 2   (<= 64)
+    {{128, 1, 0, 0, 1}, {64, 2, 1, 0, 1}, {128, 1, 2, 0, 1}, {128, 1, 0, 1, 1},           // M = 4   (<= 128)
+     {128, 1, 1, 1, 2}, {128, 1, 0, 1, 2}},
+    {{128, 2, 1, 0, 1}, {256, 1, 0, 0, 1}, {128, 2, 0, 0, 1}, {256, 1, 2, 0, 1},          // M = 8   (<= 256)
+     {128, 2, 1, 1, 1}, {256, 1, 1, 1, 2}, {256, 1, 1, 0, 2}, {256, 1, 0, 1, 2}},
+    {{128, 3, 1, 0, 1}, {256, 2, 1, 0, 1}, {384, 1, 0, 0, 1}, {128, 3, 0, 0, 1},          // M = 12  (<= 384)
+     {384, 1, 2, 0, 1}, {384, 1, 0, 1, 1}, {128, 3, 1, 1, 1}, {384, 1, 0, 1, 2}},
+    {{128, 4, 1, 0, 1}, {256, 2, 1, 0, 1}, {512, 1, 0, 0, 1}, {128, 4, 0, 0, 1},          // M = 16  (<= 512)
+     {512, 1, 2, 0, 1}, {128, 4, 1, 1, 1}, {512, 1, 0, 1, 1}, {512, 1, 0, 1, 2}},
+    {{256, 3, 1, 0, 1}, {384, 2, 0, 0, 1}, {256, 4, 1, 0, 1}, {256, 3, 1, 1, 1},          // M = 24  (<= 768)
+     {384, 2, 0, 1, 1}, {384, 2, 0, 1, 2}},
+    {{256, 4, 1, 0, 1}, {512, 2, 0, 0, 1}, {256, 4, 1, 1, 1}, {512, 2, 0, 1, 1},          // M = 32  (<= 1024)
+     {512, 2, 0, 1, 2}},
 };
 
 template <int M, int V, typename TE, bool TWO_D, bool SAL>
@@ -587,7 +898,10 @@ cudaError_t launch_k1_v(const LaunchCtx &L, const SubstepBuffers &b, int ns, int
     constexpr int TPC = kK1Shapes[mi][V].tpc, RPT = kK1Shapes[mi][V].rpt;
     constexpr int CAP = kK1Shapes[mi][V].cap, POL = kK1Shapes[mi][V].pol;
     static_assert(TPC * RPT >= 32 * M, "K1 shape must cover 32*M rows");
-    return launch_k1_cfg<M, TPC, RPT, TE, TWO_D, CAP, SAL, POL>(L, b, ns, ncol);
+    if constexpr (kK1Shapes[mi][V].ny == 2)
+      return launch_k1y2_cfg<M, TPC, RPT, TE, TWO_D, CAP, SAL, POL>(L, b, ns, ncol);
+    else
+      return launch_k1_cfg<M, TPC, RPT, TE, TWO_D, CAP, SAL, POL>(L, b, ns, ncol);
   } else {
     return cudaErrorInvalidValue;
   }

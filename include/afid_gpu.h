@@ -158,7 +158,8 @@ int afid_gpu_slice(afid_ctx_t *ctx, int which, int axis, int index, double *out)
 int afid_gpu_mean_plane(afid_ctx_t *ctx, int which, int axis, double *out);
 
 /* Autotuner of the fused explicit/implicit kernel: every launch shape available for this
- * wall-normal size (threads per x-column block x rows per thread, register cap, memory policy)
+ * wall-normal size (threads per block x rows per thread, register cap, cache policy, columns
+ * per block)
  * is timed on a sample of columns, with the RK3 histories redirected to scratch memory so the
  * state is untouched, and the fastest is kept.  It runs by itself before the first step;
  * force = 1 repeats it.  The shape changes the schedule only: results are bitwise the same for
@@ -172,8 +173,7 @@ typedef struct afid_tune_info {
   int rows[AFID_TUNE_MAX];      /* rows per thread                                           */
   int regcap[AFID_TUNE_MAX];    /* registers capped for >= 16 (1) or >= 32 (2) warps per SM  */
   int policy[AFID_TUNE_MAX];    /* bit 0: L1 cache hints (tables kept, streaming data not
-                                   allocated); bits 1+: resident blocks per SM the shared-memory
-                                   carve-out is sized for (0 = driver default)                 */
+                                   allocated); bit 1: two neighbouring columns per block        */
   double us[AFID_TUNE_MAX];     /* mean time per sample launch in microseconds (-1: not run) */
 } afid_tune_info_t;
 int afid_gpu_autotune(afid_ctx_t *ctx, int force, afid_tune_info_t *info);
