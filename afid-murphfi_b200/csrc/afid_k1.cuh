@@ -412,6 +412,9 @@ __global__ void __launch_bounds__(TPC, k1_min_blocks<CAP, TPC>())
   constexpr int LD = chunk_ld(M);
   constexpr int FLD = LD * M;
   constexpr int H = POL & 1;  // cache policy of the global loads (tld / nld / sld above)
+  // rows of a thread: tc + TPC p (strided), or RPT tc + p (adjacent, POL bit 2), so that the
+  // k - 1 / k + 1 operands of one row are the centre operands of the next
+  constexpr bool ADJ = (POL & 4) != 0;
   extern __shared__ __align__(128) unsigned char smem_k1[];
   __shared__ uint64_t bar;
   Geom g = g0;
@@ -472,7 +475,7 @@ __global__ void __launch_bounds__(TPC, k1_min_blocks<CAP, TPC>())
   double sbv[SAL ? RPT : 1];       // salinity buoyancy bycs * salc of each row (SAL only)
 #pragma unroll
   for (int p = 0; p < RPT; ++p) {
-    const int k = tc + TPC * p;
+    const int k = ADJ ? RPT * tc + p : tc + TPC * p;
     const bool in = k < g.nxm;
     uu[p][0] = (in && k >= 1) ? sld<H>(rux + c0 + k) : 0.0;
     uu[p][1] = in ? sld<H>(ruy + c0 + k) : 0.0;
@@ -518,7 +521,7 @@ __global__ void __launch_bounds__(TPC, k1_min_blocks<CAP, TPC>())
   double rr[RPT][4];
 #pragma unroll
   for (int p = 0; p < RPT; ++p) {
-    const int k = tc + TPC * p;
+    const int k = ADJ ? RPT * tc + p : tc + TPC * p;
     if (k < nxm) {
       TE q0 = (TE)0, q1, q2, q3;
       const double u0 = uu[p][0], u1 = uu[p][1], u2 = uu[p][2], u3 = uu[p][3];
@@ -543,7 +546,7 @@ __global__ void __launch_bounds__(TPC, k1_min_blocks<CAP, TPC>())
   __syncthreads();  // the neighbour columns are dead from here on
 #pragma unroll
   for (int p = 0; p < RPT; ++p) {
-    const int k = tc + TPC * p;
+    const int k = ADJ ? RPT * tc + p : tc + TPC * p;
     if (k < nxm) {
       const int sk = (k % M) * LD + k / M;
       if (k >= 1) {
@@ -577,7 +580,7 @@ __global__ void __launch_bounds__(TPC, k1_min_blocks<CAP, TPC>())
   __syncthreads();
 #pragma unroll
   for (int p = 0; p < RPT; ++p) {
-    const int k = tc + TPC * p;
+    const int k = ADJ ? RPT * tc + p : tc + TPC * p;
     if (k < nxm) {
       const int sk = (k % M) * LD + k / M;
       if (k >= 1) {
@@ -805,9 +808,17 @@ __global__ void __launch_bounds__(TPC, k1_min_blocks<CAP, TPC>())
   {
     const int warp = tc >> 5, lane = tc & 31;
     constexpr int NW = TPC / 32;
-    for (int f = warp; f < 4; f += NW) {
-      const double *Tb = (f == 0) ? TX : ((f == 3) ? TT : TY);
-      cn_solve_chunk2<M, LD, H>(s_rhs + f * FLD, s_rhs + (4 + f) * FLD, Tb, lane);
+    if constexpr (NW >= 8) {  // a warp per system: no warp idles through the solves
+      for (int sidx = warp; sidx < 8; sidx += NW) {
+        const int f = sidx & 3;
+        const double *Tb = (f == 0) ? TX : ((f == 3) ? TT : TY);
+        cn_solve_chunk<M, LD, H>(s_rhs + (size_t)((sidx >> 2) * 4 + f) * FLD, Tb, lane);
+      }
+    } else {  // fewer warps: a warp per field, both columns with one load of each factor
+      for (int f = warp; f < 4; f += NW) {
+        const double *Tb = (f == 0) ? TX : ((f == 3) ? TT : TY);
+        cn_solve_chunk2<M, LD, H>(s_rhs + f * FLD, s_rhs + (4 + f) * FLD, Tb, lane);
+      }
     }
   }
   __syncthreads();
@@ -863,9 +874,9 @@ cudaError_t launch_k1_cfg(const LaunchCtx &L, const SubstepBuffers &b, int ns, i
 }
 
 // Launch shapes of K1 per M = {1, 2, 4, 8, 12, 16, 24, 32} (rows per lane of the CN solves):
-// {threads per block, rows per thread, register cap level, cache policy (1: the hints of tld /
-// nld / sld), columns per block along y (1 or 2, the tile of k_explicit_implicit_y2)}, threads x
-// rows >= 32 M.  The first entry is the default.
+// {threads per block, rows per thread, register cap level, policy (bit 0: the cache hints of
+// tld / nld / sld; bit 2: adjacent rows per thread), columns per block along y (1 or 2, the tile
+// of k_explicit_implicit_y2)}, threads x rows >= 32 M.  The first entry is the default.
 struct K1Shape {
   int tpc, rpt, cap, pol, ny;
 };
@@ -873,14 +884,14 @@ constexpr int kK1MaxShapes = 8;
 constexpr int k1_m_index(int M) {
   return M == 1 ? 0 : M == 2 ? 1 : M == 4 ? 2 : M == 8 ? 3 : M == 12 ? 4 : M == 16 ? 5 : M == 24 ? 6 : 7;
 }
-constexpr int kK1ShapeCount[8] = {3, 4, 6, 8, 8, 8, 6, 5};
+constexpr int kK1ShapeCount[8] = {3, 4, 6, 7, 8, 8, 6, 5};
 constexpr K1Shape kK1Shapes[8][kK1MaxShapes] = {
     {{32, 1, 0, 0, 1}, {32, 1, 0, 1, 1}, {32, 1, 0, 1, 2}},                               // M = 1   (nxm <= 32)
     {{64, 1, 0, 0, 1}, {32, 2, 1, 0, 1}, {64, 1, 0, 1, 1}, {64, 1, 0, 1, 2}},             // M = 2   (<= 64)
     {{128, 1, 0, 0, 1}, {64, 2, 1, 0, 1}, {128, 1, 2, 0, 1}, {128, 1, 0, 1, 1},           // M = 4   (<= 128)
      {128, 1, 1, 1, 2}, {128, 1, 0, 1, 2}},
-    {{128, 2, 1, 0, 1}, {256, 1, 0, 0, 1}, {128, 2, 0, 0, 1}, {256, 1, 2, 0, 1},          // M = 8   (<= 256)
-     {128, 2, 1, 1, 1}, {256, 1, 1, 1, 2}, {256, 1, 1, 0, 2}, {256, 1, 0, 1, 2}},
+    {{128, 2, 1, 0, 1}, {256, 1, 2, 0, 1}, {128, 2, 1, 1, 1}, {128, 2, 1, 5, 1},          // M = 8   (<= 256)
+     {128, 2, 1, 4, 1}, {256, 1, 1, 1, 2}, {128, 2, 1, 1, 2}},
     {{128, 3, 1, 0, 1}, {256, 2, 1, 0, 1}, {384, 1, 0, 0, 1}, {128, 3, 0, 0, 1},          // M = 12  (<= 384)
      {384, 1, 2, 0, 1}, {384, 1, 0, 1, 1}, {128, 3, 1, 1, 1}, {384, 1, 0, 1, 2}},
     {{128, 4, 1, 0, 1}, {256, 2, 1, 0, 1}, {512, 1, 0, 0, 1}, {128, 4, 0, 0, 1},          // M = 16  (<= 512)

@@ -17,7 +17,7 @@ int k1_shapes(int M, int *tpc, int *rpt, int *cap, int *pol) {
     if (tpc) tpc[v] = kK1Shapes[mi][v].tpc;
     if (rpt) rpt[v] = kK1Shapes[mi][v].rpt;
     if (cap) cap[v] = kK1Shapes[mi][v].cap;
-    if (pol) pol[v] = kK1Shapes[mi][v].pol | (kK1Shapes[mi][v].ny == 2 ? 2 : 0);
+    if (pol) pol[v] = kK1Shapes[mi][v].pol | (kK1Shapes[mi][v].ny == 2 ? 2 : 0);  // bit 1: two columns
   }
   return kK1ShapeCount[mi];
 }

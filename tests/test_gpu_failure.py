@@ -91,7 +91,7 @@ def test_nan_in_one_batch_instance_stops_only_that_instance():
         for slot in range(3):
             b.seed(slot, 40 + slot)
         f = b.download(1)
-        f["vy"][0, 9, 4] = np.nan
+        f["vy"][9, 4] = np.nan                      # a 2-D slot comes back as (nym, nx)
         b.upload(1, f["vx"], f["vy"], f["vz"], f["temp"], f["pr"])
         dm = b.divmax()
         assert np.isnan(dm[1]) and np.isfinite(dm[0]) and np.isfinite(dm[2])
