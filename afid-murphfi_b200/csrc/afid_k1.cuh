@@ -884,9 +884,9 @@ constexpr int kK1MaxShapes = 8;
 constexpr int k1_m_index(int M) {
   return M == 1 ? 0 : M == 2 ? 1 : M == 4 ? 2 : M == 8 ? 3 : M == 12 ? 4 : M == 16 ? 5 : M == 24 ? 6 : 7;
 }
-constexpr int kK1ShapeCount[8] = {3, 4, 6, 7, 8, 8, 6, 5};
+constexpr int kK1ShapeCount[8] = {1, 4, 6, 7, 8, 8, 6, 5};
 constexpr K1Shape kK1Shapes[8][kK1MaxShapes] = {
-    {{32, 1, 0, 0, 1}, {32, 1, 0, 1, 1}, {32, 1, 0, 1, 2}},                               // M = 1   (nxm <= 32)
+    {{32, 1, 0, 0, 1}},                                                                  // M = 1   (nxm <= 32)
     {{64, 1, 0, 0, 1}, {32, 2, 1, 0, 1}, {64, 1, 0, 1, 1}, {64, 1, 0, 1, 2}},             // M = 2   (<= 64)
     {{128, 1, 0, 0, 1}, {64, 2, 1, 0, 1}, {128, 1, 2, 0, 1}, {128, 1, 0, 1, 1},           // M = 4   (<= 128)
      {128, 1, 1, 1, 2}, {128, 1, 0, 1, 2}},
