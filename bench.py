@@ -449,42 +449,68 @@ def batch_bou(inst: dict) -> str:
 
 class BatchSet:
     """One ag.Batch per size class, each on its own stream; a step forks from and joins to a
-    master stream so the classes overlap on the device."""
+    master stream so the classes overlap on the device.
 
-    def __init__(self, instances, precision: int):
+    With ``group_bytes`` > 0 each class is split into groups whose device state stays under that
+    many bytes (so that a group fits the L2 cache), one ag.Batch per group, and a step of ``n``
+    runs group after group, each group ``n`` steps in a row, consecutive groups alternating
+    between ``lanes`` streams: the state of a group stays in L2 across its steps instead of
+    streaming through HBM every step.  Instances are independent, so the grouping changes the
+    schedule only."""
+
+    def __init__(self, instances, precision: int, group_bytes: int = 0, lanes: int = 2):
         import torch
         import afid_gpu as ag
         self.classes = {}
         for inst in instances:
             self.classes.setdefault((inst["nxm"], inst["nym"]), []).append(inst)
         self.master = torch.cuda.Stream()
-        self.batches, self.streams = [], []
+        self.batches, self.class_of = [], []
+        grouped = group_bytes > 0
         for key in sorted(self.classes):
             members = self.classes[key]
-            b = ag.Batch(ag.parse_bou_in(batch_bou(members[0])), len(members), precision)
-            s = torch.cuda.Stream()
-            b.set_stream(s.cuda_stream)
-            for slot, inst in enumerate(members):
-                b.configure(slot, ag.parse_bou_in(batch_bou(inst)))
-                b.seed(slot, BATCH_SEED + 1 + inst["index"])
-            b.set_active([1] * len(members))
-            self.batches.append(b)
-            self.streams.append(s)
+            if grouped:
+                # device bytes of one slot, from a batch of one of this class
+                with ag.Batch(ag.parse_bou_in(batch_bou(members[0])), 1, precision) as probe:
+                    per = max(1, probe.device_bytes())
+                size = max(1, int(group_bytes // per))
+                parts = [members[i:i + size] for i in range(0, len(members), size)]
+            else:
+                parts = [members]
+            for part in parts:
+                b = ag.Batch(ag.parse_bou_in(batch_bou(part[0])), len(part), precision)
+                for slot, inst in enumerate(part):
+                    b.configure(slot, ag.parse_bou_in(batch_bou(inst)))
+                    b.seed(slot, BATCH_SEED + 1 + inst["index"])
+                b.set_active([1] * len(part))
+                self.batches.append(b)
+                self.class_of.append(key)
+        nstreams = lanes if grouped else len(self.batches)
+        self.streams = [torch.cuda.Stream() for _ in range(nstreams)]
+        for q, b in enumerate(self.batches):
+            b.set_stream(self.streams[q % nstreams].cuda_stream)
         self.cells = sum(i["nxm"] * i["nym"] for i in instances)
 
     def step(self, n: int = 1):
         import torch
         fork = torch.cuda.Event()
         fork.record(self.master)
-        joins = []
-        for b, s in zip(self.batches, self.streams):
+        for s in self.streams:
             s.wait_event(fork)
+        for b in self.batches:
             b.step(n)
+        for s in self.streams:
             e = torch.cuda.Event()
             e.record(s)
-            joins.append(e)
-        for e in joins:
             self.master.wait_event(e)
+
+    def autotune(self):
+        out = {}
+        for key, b in zip(self.class_of, self.batches):
+            name = f"{key[1]}x{key[0]}"
+            if name not in out:
+                out[name] = b.autotune()
+        return out
 
     def stats(self):
         return [b.stats() for b in self.batches]
@@ -507,11 +533,15 @@ def run_batched(args):
     world, rank, local = dist_setup()
     insts = batch_instances(args.instances)
     precision = 1 if args.config == "batched" else 0
-    bs = BatchSet(insts, precision)
+    group_bytes = int(args.l2_group_mb * 1e6)
+    chunk = max(1, args.group_steps) if group_bytes else 1
+    if args.steps % chunk:
+        args.steps += chunk - args.steps % chunk  # whole visits of every group
+    bs = BatchSet(insts, precision, group_bytes)
     for _ in range(args.warmup):
         bs.step()
     torch.cuda.synchronize()
-    tune = {f"{k[1]}x{k[0]}": b.autotune() for k, b in zip(sorted(bs.classes), bs.batches)}
+    tune = bs.autotune()
     l0 = bs.launches()
     clocks = ClockSampler(torch.cuda.current_device())
     barrier(world)
@@ -519,8 +549,8 @@ def run_batched(args):
     clocks.start()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     ev0.record(bs.master)
-    for _ in range(args.steps):
-        bs.step()
+    for _ in range(args.steps // chunk):
+        bs.step(chunk)
     ev1.record(bs.master)
     torch.cuda.synchronize()
     barrier(world)
@@ -567,6 +597,8 @@ def run_batched(args):
             "data": "synthetic: 256 Philox-drawn 2-D RBC instances, conductive state + seeded +-1e-3 perturbation",
             "config": {"workload": f"batched_{len(insts)}x2d_" + ("mixed" if precision else "fp64"),
                        "instances": len(insts), "cells": bs.cells, "classes_nymxnxm": counts,
+                       "schedule": (f"L2 groups of <= {args.l2_group_mb:g} MB, {chunk} steps per group visit, "
+                                    f"{len(bs.batches)} groups" if group_bytes else "one batch per class, stepped together"),
                        "dt": "CFL-limited per instance (CFLMAX 1.2; DTMAX = min(1e-2, 0.5 dy^2 min(Re, Pe)))",
                        "l2": "inputs larger than L2 (%.1f GB resident)" % (bs_bytes / 1e9),
                        "parallelism": "replicas" if world > 1 else "single GPU"},
@@ -1083,6 +1115,10 @@ def main():
     ap.add_argument("--cpu-budget", type=float, default=60.0, help="seconds of CPU-baseline steps at most")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--restart-io", action="store_true", help="rbc3d: time writing and reading the restart files")
+    ap.add_argument("--l2-group-mb", type=float, default=0.0,
+                    help="batched: split each class into groups of at most this many MB of device state, stepped "
+                         "group after group (0 = one batch per class)")
+    ap.add_argument("--group-steps", type=int, default=10, help="batched: steps per group visit with --l2-group-mb")
     ap.add_argument("--instances", type=int, default=256,
                     help="batched: the first N instances of the 256-instance draw (profiling a smaller set)")
     args = ap.parse_args()
