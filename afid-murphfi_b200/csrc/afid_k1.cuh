@@ -3,6 +3,8 @@
 // terms in afid_k1_mixed.cu).  Thread shapes per M (threads per column x rows per thread) are
 // listed in kK1Shapes; the autotuner picks one per context.
 #pragma once
+#include <algorithm>
+
 #include "afid_device.cuh"
 #include "afid_internal.h"
 
@@ -12,9 +14,11 @@ namespace afid {
 // RK3 histories by plain loads.  H = 1: the tables every block reads (metric coefficients, CN
 // factors) are kept in L1 with the evict_last priority, and the data each block reads once (RK3
 // histories, single-row neighbours) bypasses L1 (no_allocate), so the streaming data does not
-// evict the tables.
+// evict the tables.  H = 2 (tld only): the tables sit in shared memory; plain loads.
 template <int H> __device__ __forceinline__ double tld(const double *p) {
-  if constexpr (H != 0) {
+  if constexpr (H == 2) {  // tables staged in shared memory (k_explicit_implicit_p)
+    return *p;
+  } else if constexpr (H != 0) {
     double v;
     asm("ld.global.nc.L1::evict_last.f64 %0, [%1];" : "=d"(v) : "l"(p));
     return v;
@@ -861,6 +865,288 @@ cudaError_t launch_k1y2_cfg(const LaunchCtx &L, const SubstepBuffers &b, int ns,
   return cudaGetLastError();
 }
 
+// ------------------------------------------------------------------------------------------
+// K1, persistent form: one block per SM, G groups of TPC threads.  The block stages the tables
+// every column reads (the 12 metric arrays and the substep's three CN factor sets) into shared
+// memory once, then each group works through columns blockIdx.x*G + grp, + gridDim.x*G, ... with
+// its own staging slot and mbarrier, exactly as the one-column kernel does per block; table
+// reads are shared-memory loads instead of L1/L2 hits.  Groups synchronise on named barriers
+// (id 1 + grp) and never wait for one another.  Single domains only (a batch has CN tables per
+// instance).
+// ------------------------------------------------------------------------------------------
+__host__ __device__ constexpr int k1p_cn_doubles(int M) { return 192 * M + 576; }
+__host__ __device__ constexpr size_t k1p_slot_doubles(int M, bool two_d) {
+  const size_t st = (size_t)(two_d ? kK1StateCols2D : kK1StateCols) * k1_col_stride(M);
+  const size_t rhs = (size_t)kK1Centre * k1_col_stride(M) + (size_t)4 * chunk_ld(M) * M;
+  const size_t d = st > rhs ? st : rhs;
+  return (d + 15) / 16 * 16;  // 128-byte aligned slots
+}
+__host__ __device__ constexpr size_t k1p_table_doubles(int M) {
+  return (size_t)12 * k1_col_stride(M) + (size_t)3 * k1p_cn_doubles(M);
+}
+// Groups per block: as many staging slots as fit beside the tables in 227 KB, at most 4.
+__host__ __device__ constexpr int k1p_groups(int M, bool two_d) {
+  const size_t avail = (size_t)232448 - 512 - k1p_table_doubles(M) * 8;
+  const size_t g = avail / (k1p_slot_doubles(M, two_d) * 8);
+  return g > 4 ? 4 : (int)g;
+}
+__device__ __forceinline__ void group_sync(int id, int nthreads) {
+  asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(nthreads) : "memory");
+}
+__device__ __forceinline__ bool group_and(int id, int nthreads, bool v) {
+  uint32_t r;
+  asm volatile(
+      "{\n\t.reg .pred p, q;\n\tsetp.ne.u32 p, %1, 0;\n\tbar.red.and.pred q, %2, %3, p;\n\t"
+      "selp.u32 %0, 1, 0, q;\n\t}"
+      : "=r"(r)
+      : "r"((uint32_t)v), "r"(id), "r"(nthreads)
+      : "memory");
+  return r != 0;
+}
+__device__ __forceinline__ void fence_proxy_async_smem() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+template <int M, int TPC, int RPT, typename TE, bool TWO_D, bool SAL, int G>
+__global__ void __launch_bounds__(TPC * G, 1)
+    k_explicit_implicit_p(Geom g0, Tables t, const StepCoef *__restrict__ sc_all, int ns,
+                          const double *__restrict__ cn_tab, const double *__restrict__ vx,
+                          const double *__restrict__ vy, const double *__restrict__ vz,
+                          const double *__restrict__ temp, const double *__restrict__ pr,
+                          TE *__restrict__ rux, TE *__restrict__ ruy, TE *__restrict__ ruz,
+                          TE *__restrict__ rut, double *__restrict__ vx_o, double *__restrict__ vy_o,
+                          double *__restrict__ vz_o, double *__restrict__ temp_o, int *__restrict__ err,
+                          int ncol) {
+  constexpr int LD = chunk_ld(M);
+  constexpr int FLD = LD * M;
+  constexpr int CS = k1_col_stride(M);
+  constexpr int TSZ = k1p_cn_doubles(M);
+  constexpr size_t SLOT = k1p_slot_doubles(M, TWO_D);
+  constexpr int NT = TPC * G;
+  extern __shared__ __align__(128) unsigned char smem_k1p[];
+  __shared__ uint64_t tbar, bars[G];
+  double *tm = reinterpret_cast<double *>(smem_k1p);  // 12 metric arrays at stride CS
+  double *tcn = tm + 12 * CS;                          // CN factors of vx, vy/vz, temp
+  const int tid = threadIdx.x, grp = tid / TPC, tc = tid % TPC;
+  const int slot = ns;  // single domain: one table set per substep
+  if (tid == 0) {
+    mbar_init(&tbar, 1);
+#pragma unroll
+    for (int q = 0; q < G; ++q) mbar_init(&bars[q], 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+  if (tid == 0) {
+    const uint32_t mb = (uint32_t)(((g0.nx + 1) & ~1) * sizeof(double));  // rows rounded to 16 bytes
+    mbar_arrive_expect_tx(&tbar, 12 * mb + 3 * (uint32_t)TSZ * (uint32_t)sizeof(double));
+    const double *src[12] = {t.idx,   t.udx3c, t.udx3m, t.ap3ck,  t.ac3ck,  t.am3ck,
+                             t.ap3sk, t.ac3sk, t.am3sk, t.ap3ssk, t.ac3ssk, t.am3ssk};
+#pragma unroll
+    for (int q = 0; q < 12; ++q) bulk_g2s(tm + (size_t)q * CS, src[q], mb, &tbar);
+#pragma unroll
+    for (int m = 0; m < 3; ++m)
+      bulk_g2s(tcn + (size_t)m * TSZ, cn_tab + (size_t)(slot * 3 + m) * TSZ, (uint32_t)TSZ * sizeof(double), &tbar);
+  }
+  const bool tok = mbar_wait(&tbar, 0, kSpinLimit);
+  if (!__syncthreads_and(tok)) {
+    if (tid == 0) atomicOr(err, 2);
+    mbar_wait(&tbar, 0, kDrainLimit);
+    return;
+  }
+  Tables ts = t;  // the metric arrays from shared memory
+  ts.idx = tm;
+  ts.udx3c = tm + CS;
+  ts.udx3m = tm + 2 * CS;
+  ts.ap3ck = tm + 3 * CS;
+  ts.ac3ck = tm + 4 * CS;
+  ts.am3ck = tm + 5 * CS;
+  ts.ap3sk = tm + 6 * CS;
+  ts.ac3sk = tm + 7 * CS;
+  ts.am3sk = tm + 8 * CS;
+  ts.ap3ssk = tm + 9 * CS;
+  ts.ac3ssk = tm + 10 * CS;
+  ts.am3ssk = tm + 11 * CS;
+  const double *TX = tcn, *TY = tcn + TSZ, *TT = tcn + 2 * TSZ;
+  const StepCoef sc = sc_all[slot];
+  double *cols = tcn + 3 * TSZ + (size_t)grp * SLOT;
+  double *s_rhs = cols + (size_t)kK1Centre * CS;
+  uint64_t *bar = &bars[grp];
+  const int gid = 1 + grp;
+  const int ldx = g0.ldx, nxm = g0.nxm;
+  uint32_t ph = 0;
+  for (int colid = blockIdx.x * G + grp; colid < ncol; colid += gridDim.x * G) {
+    Geom g = g0;
+    const int j = colid % g.nym, i = colid / g.nym;
+    const size_t c0 = col_off(g, j, i);
+    if (!inst_active(g, i)) {
+      for (int k = tc; k < g.nx; k += TPC) temp_o[c0 + k] = temp[c0 + k];
+      continue;
+    }
+    const int jp = wrap_inc(j, g.nym), jm = wrap_dec(j, g.nym);
+    const int ip = zinc(g, i), im = zdec(g, i);
+    if (tc == 0) {
+      const size_t oc = c0, ojp = col_off(g, jp, i), ojm = col_off(g, jm, i), oip = col_off(g, j, ip),
+                   oim = col_off(g, j, im);
+      const uint32_t cb = (uint32_t)ldx * sizeof(double);
+      mbar_arrive_expect_tx(bar, (uint32_t)k1_stage_bytes(ldx, TWO_D));
+      if constexpr (TWO_D) {
+        const double *src[kK1StateCols2D] = {vx + oc,   vy + oc,    vz + oc, temp + oc, vx + ojp, vx + ojm, vy + ojp,
+                                             vy + ojm,  vz + ojp,   vz + ojm, temp + ojp, temp + ojm, pr + oc};
+#pragma unroll
+        for (int q = 0; q < kK1StateCols2D; ++q) bulk_g2s(cols + (size_t)q * CS, src[q], cb, bar);
+      } else {
+        const double *src[kK1StateCols] = {vx + oc,    vy + oc,    vz + oc,    temp + oc,  vx + ojp,   vx + ojm,
+                                           vx + oip,   vx + oim,   vy + ojp,   vy + ojm,   vy + oip,   vy + oim,
+                                           vz + ojp,   vz + ojm,   vz + oip,   vz + oim,   temp + ojp, temp + ojm,
+                                           temp + oip, temp + oim, pr + oc};
+#pragma unroll
+        for (int q = 0; q < kK1StateCols; ++q) bulk_g2s(cols + (size_t)q * CS, src[q], cb, bar);
+      }
+    }
+    const size_t o_jm = col_off(g, jm, i), o_im = col_off(g, j, im);
+    const size_t o_jpim = col_off(g, jp, im), o_jmip = col_off(g, jm, ip);
+    double uu[RPT][4], vv[RPT][4];
+    double sbv[SAL ? RPT : 1];
+#pragma unroll
+    for (int p = 0; p < RPT; ++p) {
+      const int k = tc + TPC * p;
+      const bool in = k < nxm;
+      uu[p][0] = (in && k >= 1) ? sld<1>(rux + c0 + k) : 0.0;
+      uu[p][1] = in ? sld<1>(ruy + c0 + k) : 0.0;
+      uu[p][2] = in ? sld<1>(ruz + c0 + k) : 0.0;
+      uu[p][3] = in ? sld<1>(rut + c0 + k) : 0.0;
+      if constexpr (TWO_D) {
+        vv[p][0] = vv[p][1] = vv[p][3] = 0.0;
+      } else {
+        vv[p][0] = in ? nld<1>(vz + o_jmip + k) : 0.0;
+        vv[p][1] = in ? nld<1>(vy + o_jpim + k) : 0.0;
+        vv[p][3] = in ? nld<1>(pr + o_im + k) : 0.0;
+      }
+      vv[p][2] = in ? nld<1>(pr + o_jm + k) : 0.0;
+      if constexpr (SAL) sbv[p] = in ? g.bycs * nld<1>(g.salc + c0 + k) : 0.0;
+    }
+    bool ok = mbar_wait(bar, ph & 1, kSpinLimit);
+    if (g.wait_test_polls > 0) ok = ok && mbar_wait(bar, (ph & 1) ^ 1, g.wait_test_polls);
+    if (!group_and(gid, TPC, ok)) {
+      if (tc == 0) atomicOr(err, 2);
+      mbar_wait(bar, ph & 1, kDrainLimit);
+      break;  // the whole group leaves; the other groups are not affected
+    }
+    ++ph;
+    auto C = [&](int q) { return (const double *)(cols + q * CS); };
+    const ColV X = TWO_D ? ColV{C(0), C(4), C(5), C(0), C(0), nullptr} : ColV{C(0), C(4), C(5), C(6), C(7), nullptr};
+    const ColV Y = TWO_D ? ColV{C(1), C(6), C(7), C(1), C(1), nullptr} : ColV{C(1), C(8), C(9), C(10), C(11), nullptr};
+    const ColV Z = TWO_D ? ColV{C(2), C(8), C(9), C(2), C(2), nullptr} : ColV{C(2), C(12), C(13), C(14), C(15), nullptr};
+    const ColV T = TWO_D ? ColV{C(3), C(10), C(11), C(3), C(3), nullptr} : ColV{C(3), C(16), C(17), C(18), C(19), nullptr};
+    const ColV P = TWO_D ? ColV{C(12), nullptr, nullptr, nullptr, nullptr, nullptr}
+                         : ColV{C(20), nullptr, nullptr, nullptr, nullptr, nullptr};
+    const size_t pl = (size_t)j + (size_t)g.nym * i;
+    const double tbp = nld<1>(t.tempbp + pl), ttp = nld<1>(t.temptp + pl);
+    double rr[RPT][4];
+#pragma unroll
+    for (int p = 0; p < RPT; ++p) {
+      const int k = tc + TPC * p;
+      if (k < nxm) {
+        TE q0 = (TE)0, q1, q2, q3;
+        const double zd = TWO_D ? Z.jm[k] : vv[p][0];
+        const double yd = TWO_D ? Y.jp[k] : vv[p][1];
+        const double pim = TWO_D ? P.c[k] : vv[p][3];
+        double sb = 0.0;
+        if constexpr (SAL) sb = sbv[p];
+        rr[p][0] = (k >= 1) ? rhs_vx<TE, TWO_D, SAL, 2>(g, ts, sc, k, X, Y, Z, T, P, uu[p][0], q0, sb) * TX[k - 1] : 0.0;
+        rr[p][1] = rhs_vy<TE, TWO_D, SAL, 2>(g, ts, sc, k, X, Y, Z, T, P, zd, vv[p][2], uu[p][1], q1, sb) * TY[k];
+        rr[p][2] = rhs_vz<TE, TWO_D, SAL, 2>(g, ts, sc, k, X, Y, Z, T, P, yd, pim, uu[p][2], q2, sb) * TY[k];
+        rr[p][3] = rhs_temp<TE, TWO_D, 2>(g, ts, sc, k, X, Y, Z, T, tbp, ttp, uu[p][3], q3) * TT[k];
+        if (k >= 1) rux[c0 + k] = q0;
+        ruy[c0 + k] = q1;
+        ruz[c0 + k] = q2;
+        rut[c0 + k] = q3;
+      }
+    }
+    group_sync(gid, TPC);  // the neighbour columns are dead from here on
+#pragma unroll
+    for (int p = 0; p < RPT; ++p) {
+      const int k = tc + TPC * p;
+      if (k < nxm) {
+        const int sk = (k % M) * LD + k / M;
+        if (k >= 1) {
+          const int r = k - 1;
+          s_rhs[(r % M) * LD + r / M] = rr[p][0];
+        }
+        s_rhs[FLD + sk] = rr[p][1];
+        s_rhs[2 * FLD + sk] = rr[p][2];
+        s_rhs[3 * FLD + sk] = rr[p][3];
+      }
+    }
+    for (int r = nxm - 1 + tc; r < 32 * M; r += TPC) {
+      const int sr = (r % M) * LD + r / M;
+      s_rhs[sr] = 0.0;
+      if (r >= nxm) {
+        s_rhs[FLD + sr] = 0.0;
+        s_rhs[2 * FLD + sr] = 0.0;
+        s_rhs[3 * FLD + sr] = 0.0;
+      }
+    }
+    group_sync(gid, TPC);
+    {
+      const int warp = tc >> 5, lane = tc & 31;
+      constexpr int NW = TPC / 32;
+      for (int f = warp; f < 4; f += NW) {
+        const double *Tb = (f == 0) ? TX : ((f == 3) ? TT : TY);
+        cn_solve_chunk<M, LD, 2>(s_rhs + f * FLD, Tb, lane);
+      }
+    }
+    group_sync(gid, TPC);
+#pragma unroll
+    for (int p = 0; p < RPT; ++p) {
+      const int k = tc + TPC * p;
+      if (k < nxm) {
+        const int sk = (k % M) * LD + k / M;
+        if (k >= 1) {
+          const int r = k - 1;
+          vx_o[c0 + k] = X.c[k] + s_rhs[(r % M) * LD + r / M];
+        } else {
+          vx_o[c0] = 0.0;  // ImplicitAndUpdateVX.F90:86-87: vx(1) = vx(nx) = 0
+          vx_o[c0 + nxm] = 0.0;
+        }
+        vy_o[c0 + k] = Y.c[k] + s_rhs[FLD + sk];
+        vz_o[c0 + k] = Z.c[k] + s_rhs[2 * FLD + sk];
+        temp_o[c0 + k] = T.c[k] + s_rhs[3 * FLD + sk];
+      }
+    }
+    // the slot is rewritten by the next column's bulk copies (async proxy): order this group's
+    // shared-memory reads and writes before them
+    fence_proxy_async_smem();
+    group_sync(gid, TPC);
+  }
+  (void)NT;
+}
+
+template <int M, int TPC, int RPT, typename TE, bool TWO_D, bool SAL>
+cudaError_t launch_k1p_cfg(const LaunchCtx &L, const SubstepBuffers &b, int ns, int ncol) {
+  constexpr int G = k1p_groups(M, TWO_D);
+  if constexpr (G < 2) {
+    return cudaErrorInvalidValue;  // the tables leave room for fewer than two groups
+  } else {
+    if (L.g.batch) return cudaErrorInvalidValue;  // CN tables per instance
+    static int nsm = 0;
+    if (nsm == 0) {
+      int dev = 0;
+      cudaGetDevice(&dev);
+      if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || nsm < 1) nsm = 148;
+    }
+    const size_t smem = (k1p_table_doubles(M) + (size_t)G * k1p_slot_doubles(M, TWO_D)) * sizeof(double);
+    auto kern = k_explicit_implicit_p<M, TPC, RPT, TE, TWO_D, SAL, G>;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    const int grid = std::min(nsm, (ncol + G - 1) / G);
+    kern<<<grid, TPC * G, smem, L.stream>>>(L.g, L.t, b.sc, ns, b.cn_tab, b.vx, b.vy, b.vz, b.temp, b.pr,
+                                            (TE *)b.rux, (TE *)b.ruy, (TE *)b.ruz, (TE *)b.rut, b.vx_o, b.vy_o,
+                                            b.vz_o, b.temp_o, b.err, ncol);
+    return cudaGetLastError();
+  }
+}
+
 template <int M, int TPC, int RPT, typename TE, bool TWO_D, int CAP, bool SAL, int POL>
 cudaError_t launch_k1_cfg(const LaunchCtx &L, const SubstepBuffers &b, int ns, int ncol) {
   const size_t smem = k1_smem(L.g.ldx, M, TWO_D);
@@ -874,9 +1160,11 @@ cudaError_t launch_k1_cfg(const LaunchCtx &L, const SubstepBuffers &b, int ns, i
 }
 
 // Launch shapes of K1 per M = {1, 2, 4, 8, 12, 16, 24, 32} (rows per lane of the CN solves):
-// {threads per block, rows per thread, register cap level, policy (bit 0: the cache hints of
-// tld / nld / sld; bit 2: adjacent rows per thread), columns per block along y (1 or 2, the tile
-// of k_explicit_implicit_y2)}, threads x rows >= 32 M.  The first entry is the default.
+// {threads per column, rows per thread, register cap level, policy (bit 0: the cache hints of
+// tld / nld / sld; bit 1: tables in shared memory; bit 2: adjacent rows per thread), columns per
+// block along y (1, or 2 for the tile of k_explicit_implicit_y2; 0 for the persistent
+// k_explicit_implicit_p with its groups of `threads` threads)}, threads x rows >= 32 M.  The
+// first entry is the default.
 struct K1Shape {
   int tpc, rpt, cap, pol, ny;
 };
@@ -884,14 +1172,14 @@ constexpr int kK1MaxShapes = 8;
 constexpr int k1_m_index(int M) {
   return M == 1 ? 0 : M == 2 ? 1 : M == 4 ? 2 : M == 8 ? 3 : M == 12 ? 4 : M == 16 ? 5 : M == 24 ? 6 : 7;
 }
-constexpr int kK1ShapeCount[8] = {1, 4, 6, 7, 8, 8, 6, 5};
+constexpr int kK1ShapeCount[8] = {1, 4, 7, 8, 8, 8, 6, 5};
 constexpr K1Shape kK1Shapes[8][kK1MaxShapes] = {
     {{32, 1, 0, 0, 1}},                                                                  // M = 1   (nxm <= 32)
     {{64, 1, 0, 0, 1}, {32, 2, 1, 0, 1}, {64, 1, 0, 1, 1}, {64, 1, 0, 1, 2}},             // M = 2   (<= 64)
     {{128, 1, 0, 0, 1}, {64, 2, 1, 0, 1}, {128, 1, 2, 0, 1}, {128, 1, 0, 1, 1},           // M = 4   (<= 128)
-     {128, 1, 1, 1, 2}, {128, 1, 0, 1, 2}},
+     {128, 1, 1, 1, 2}, {128, 1, 0, 1, 2}, {128, 1, 0, 2, 0}},
     {{128, 2, 1, 0, 1}, {256, 1, 2, 0, 1}, {128, 2, 1, 1, 1}, {128, 2, 1, 5, 1},          // M = 8   (<= 256)
-     {128, 2, 1, 4, 1}, {256, 1, 1, 1, 2}, {128, 2, 1, 1, 2}},
+     {128, 2, 1, 4, 1}, {256, 1, 1, 1, 2}, {128, 2, 1, 1, 2}, {128, 2, 0, 2, 0}},
     {{128, 3, 1, 0, 1}, {256, 2, 1, 0, 1}, {384, 1, 0, 0, 1}, {128, 3, 0, 0, 1},          // M = 12  (<= 384)
      {384, 1, 2, 0, 1}, {384, 1, 0, 1, 1}, {128, 3, 1, 1, 1}, {384, 1, 0, 1, 2}},
     {{128, 4, 1, 0, 1}, {256, 2, 1, 0, 1}, {512, 1, 0, 0, 1}, {128, 4, 0, 0, 1},          // M = 16  (<= 512)
@@ -911,6 +1199,8 @@ cudaError_t launch_k1_v(const LaunchCtx &L, const SubstepBuffers &b, int ns, int
     static_assert(TPC * RPT >= 32 * M, "K1 shape must cover 32*M rows");
     if constexpr (kK1Shapes[mi][V].ny == 2)
       return launch_k1y2_cfg<M, TPC, RPT, TE, TWO_D, CAP, SAL, POL>(L, b, ns, ncol);
+    else if constexpr (kK1Shapes[mi][V].ny == 0)
+      return launch_k1p_cfg<M, TPC, RPT, TE, TWO_D, SAL>(L, b, ns, ncol);
     else
       return launch_k1_cfg<M, TPC, RPT, TE, TWO_D, CAP, SAL, POL>(L, b, ns, ncol);
   } else {

@@ -17,7 +17,9 @@ int k1_shapes(int M, int *tpc, int *rpt, int *cap, int *pol) {
     if (tpc) tpc[v] = kK1Shapes[mi][v].tpc;
     if (rpt) rpt[v] = kK1Shapes[mi][v].rpt;
     if (cap) cap[v] = kK1Shapes[mi][v].cap;
-    if (pol) pol[v] = kK1Shapes[mi][v].pol | (kK1Shapes[mi][v].ny == 2 ? 2 : 0);  // bit 1: two columns
+    // reported policy: bit 0 cache hints, bit 1 two columns per block, bit 2 adjacent rows,
+    // bit 3 the persistent kernel with its tables in shared memory
+    if (pol) pol[v] = (kK1Shapes[mi][v].pol & 5) | (kK1Shapes[mi][v].ny == 2 ? 2 : 0) | (kK1Shapes[mi][v].ny == 0 ? 8 : 0);
   }
   return kK1ShapeCount[mi];
 }

@@ -174,7 +174,8 @@ typedef struct afid_tune_info {
   int regcap[AFID_TUNE_MAX];    /* registers capped for >= 16 (1) or >= 32 (2) warps per SM  */
   int policy[AFID_TUNE_MAX];    /* bit 0: L1 cache hints (tables kept, streaming data not
                                    allocated); bit 1: two neighbouring columns per block;
-                                   bit 2: adjacent rows per thread                              */
+                                   bit 2: adjacent rows per thread; bit 3: one persistent block
+                                   per SM with the tables in shared memory                     */
   double us[AFID_TUNE_MAX];     /* mean time per sample launch in microseconds (-1: not run) */
 } afid_tune_info_t;
 int afid_gpu_autotune(afid_ctx_t *ctx, int force, afid_tune_info_t *info);
