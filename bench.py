@@ -78,13 +78,18 @@ def measured_peak():
 
 
 def committed_traffic_kernel(kernel: str, workload: str):
-    """DRAM bytes per launch of `kernel` from the committed ncu summary for this workload."""
-    p = os.path.join(ROOT, "profiles", f"{kernel}_{workload}.md")
-    if not os.path.exists(p):
-        return None
-    for line in open(p):
-        if line.startswith("traffic_bytes_per_launch:"):
-            return float(line.split(":")[1])
+    """DRAM bytes per launch of `kernel` from the committed ncu summary that covers this workload
+    (profiles/<kernel>_<workload>.md, or a summary of a smaller capture whose `covers:` line names
+    the workload and whose traffic is scaled to it)."""
+    import glob
+    for p in sorted(glob.glob(os.path.join(ROOT, "profiles", f"{kernel}_*.md"))):
+        lines = open(p).read().splitlines()
+        named = os.path.basename(p) == f"{kernel}_{workload}.md"
+        covers = any(line.strip() == f"covers: {workload}" for line in lines)
+        if named or covers:
+            for line in lines:
+                if line.startswith("traffic_bytes_per_launch:"):
+                    return float(line.split(":")[1])
     return None
 
 
