@@ -956,6 +956,99 @@ def run_ddc(args):
         dist.destroy_process_group()
 
 
+# ---- the reference's published Rayleigh-Benard example -------------------------------------
+# docs/examples/rbc.md: Ra = 1e8, Pr = 10, 128^3 cells for the velocity and 384^3 refined cells for
+# the scalar that plays the temperature (the salinity field, active_S = 1, with the temperature
+# switched off as a buoyancy source, active_T = 0), free-fall units of the scalar (FFscaleS = 1);
+# grids and time stepping of examples/RayleighBenardConvection/bou.in (clipped Chebyshev
+# wall-normal coarse grid ISTR3 = 6, STR3 = 12, uniform refined grid ISTR3R = 0, CFLMAX 1,
+# DTMAX 1e-2).  The reference publishes the five Nusselt numbers of tools/plot_time_series.py over
+# t = 0 .. 200 (docs/figures/Nusselt.svg, digitised in tests/golden/).
+PUBLISHED = dict(nxm=128, nym=128, nzm=128, nxmr=384, nymr=384, nzmr=384, rays=1e8, pras=10.0,
+                 name="rbc3d_sal_128cubed_refined_384cubed_ra1e8_pr10")
+
+
+def published_bou_text(t_end: float) -> str:
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from helpers import bou_text as _bt  # noqa: E402
+    w = PUBLISHED
+    return _bt(w["nxm"], w["nym"], w["nzm"], rayt=1e8, prat=1.0, ylen=1.0, zlen=1.0, istr3=6, str3=12.0,
+               idtv=1, dt=1e-2, cflmax=1.0, dtmax=1e-2, ntst=10_000_000, tmax=t_end, resid=1e-3, multires=1,
+               nxmr=w["nxmr"], nymr=w["nymr"], nzmr=w["nzmr"], flagsal=1, istr3r=0, rays=w["rays"],
+               pras=w["pras"], ffscales=1, active_s=1, active_t=0, tout=0.2, tframe=1.0)
+
+
+def run_published(args):
+    """The published example on the device from a seeded start to t = args.t_end: the main loop
+    (CFLmr -> dt rule -> TimeMarcher) with the five Nusselt numbers of tools/plot_time_series.py
+    sampled every args.sample_dt, their averages from t = 75 against the digitised figure."""
+    import numpy as np
+    import torch
+    import afid_gpu as ag
+
+    world, rank, local = dist_setup()
+    w = PUBLISHED
+    inp = ag.parse_bou_in(published_bou_text(args.t_end))
+    tables = ag.Tables(inp, ag.PREC_FP64)
+    mgrd = ag.Mgrd(tables)
+    solver = ag.Solver(tables.grid, tables.params)
+    solver.sal_create(mgrd)
+    nx, nym, nzm = w["nxm"] + 1, w["nym"], w["nzm"]
+    zeros = np.zeros((nzm, nym, nx))
+    solver.upload(zeros, zeros, zeros, tables.initial_temperature(20261203), zeros)
+    solver.sal_upload(mgrd.initial_salinity(20261204))
+    xmr, xcr, xc = mgrd.array("xmr"), mgrd.array("xcr"), tables.array("xc")
+    dxr, dxc = xcr[1:] - xcr[:-1], xc[1:w["nxm"] + 1] - xc[:w["nxm"]]
+    pec = (w["rays"] * w["pras"]) ** 0.5
+
+    def nusselt():  # tools/plot_time_series.py:17-35
+        ps, pf = solver.sal_profiles(), solver.mean_profiles()
+        return {"nu_pl": (0.5 + ps["Sbar"][0]) / xmr[0], "nu_pu": (0.5 - ps["Sbar"][-1]) / (1.0 - xmr[-1]),
+                "nu_chi": float((ps["chiS"] * dxr).sum()) * pec,
+                "nu_eps": 1.0 + float((pf["epsilon"] * dxc).sum()) * pec,
+                "nu_vol": 1.0 - float((ps["vxS"] * dxr).sum()) * pec}
+
+    dtc = ctypes.c_double(inp.dt)
+    t, n, err = 0.0, 0, 0
+    times, series = [], {k: [] for k in ("nu_pl", "nu_pu", "nu_chi", "nu_eps", "nu_vol")}
+    next_sample = args.sample_dt
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    while t < args.t_end and err == 0:
+        err = ag.lib().afid_next_dt(ctypes.byref(inp), n, ctypes.byref(dtc), solver.sal_cfl(), None)
+        solver.time_marcher(dtc.value, n)
+        t += dtc.value
+        n += 1
+        if t >= next_sample - 1e-12:
+            for k, v in nusselt().items():
+                series[k].append(float(v))
+            times.append(t)
+            next_sample += args.sample_dt
+    solver.synchronize()
+    wall = time.perf_counter() - t0
+    solver.close()
+    tables.close()
+    with open(os.path.join(ROOT, "tests", "golden", "published_nusselt_rbc_ra1e8_pr10.json")) as f:
+        pub = json.load(f)
+    tt = np.array(times)
+    ours = {}
+    for k, v in series.items():
+        v = np.array(v)
+        m = tt >= 75.0
+        ours[k] = float(np.trapezoid(v[m], tt[m]) / (tt[m][-1] - tt[m][0])) if m.sum() > 1 else float("nan")
+    ref = pub["mean_from_75"]
+    line = {"metric": "Nusselt numbers of the reference's published RBC example, averaged over t >= 75",
+            "config": {"workload": w["name"], "t_end": args.t_end, "steps": n, "sample_dt": args.sample_dt,
+                       "data": "synthetic seeded start (the statistically steady state is what is compared)"},
+            "errorcode": err, "wall_s": round(wall, 1), "mean_from_75": {k: round(v, 3) for k, v in ours.items()},
+            "published_mean_from_75": ref,
+            "rel_diff": {k: round(abs(ours[k] - ref[k]) / ref[k], 4) for k in ref},
+            "series_every": args.sample_dt,
+            "series": {"t": [round(x, 3) for x in times], **{k: [round(x, 3) for x in v] for k, v in series.items()}}}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 def cpu_baseline(w: dict, steps: int, budget_s: float = 60.0, keep_state: bool = False, warmup: int = 0):
     """The CPU restatement (C + OpenMP, oracle/afid_cpu.c) on the same workload: ``warmup``
     untimed main-loop steps, then up to ``steps`` timed ones, stopping once ``budget_s`` seconds
@@ -1102,7 +1195,10 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="afid", choices=["afid", "reference"])
     ap.add_argument("--config", default="rbc3d",
-                    choices=sorted(WORKLOADS) + sorted(DDC_WORKLOADS) + ["batched", "batched_fp64", "served"])
+                    choices=sorted(WORKLOADS) + sorted(DDC_WORKLOADS) + ["batched", "batched_fp64", "served",
+                                                                         "published_rbc"])
+    ap.add_argument("--t-end", type=float, default=200.0, help="published_rbc: simulated time to reach")
+    ap.add_argument("--sample-dt", type=float, default=0.5, help="published_rbc: time between Nusselt samples")
     ap.add_argument("--no-nu-check", action="store_true")
     ap.add_argument("--accuracy-steps", type=int, default=500,
                     help="rbc3d_mixed: steps of the mixed run compared with the FP64 replay (500 = the full run)")
@@ -1137,6 +1233,8 @@ def main():
         run_served(args)
     elif args.config in DDC_WORKLOADS:
         run_ddc(args)
+    elif args.config == "published_rbc":
+        run_published(args)
     else:
         run_gpu(args)
 
