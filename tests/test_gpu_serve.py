@@ -124,10 +124,12 @@ def test_cancel_queued_and_running_jobs():
     with ag.Server(ag.PREC_FP64, slots_per_pool=2, chunk_steps=6) as srv:
         srv.submit(inp, 2, 30, 2)
         alone = _run_to_completion(srv, 1)[2]
-    with ag.Server(ag.PREC_FP64, slots_per_pool=2, chunk_steps=6, policy=ag.SERVE_FIFO) as srv:
+    # room for two jobs at a time (cells in flight), so jobs 3 and 4 wait in the queue
+    with ag.Server(ag.PREC_FP64, slots_per_pool=2, chunk_steps=6, policy=ag.SERVE_FIFO,
+                   max_cells_in_flight=2 * 32 * 64) as srv:
         for tag in (1, 2, 3, 4):
             srv.submit(inp, tag, 30, tag)
-        srv.pump()                       # jobs 1 and 2 run, 3 and 4 wait for a slot
+        srv.pump()                       # jobs 1 and 2 run, 3 and 4 wait
         st = srv.status()
         assert st["running"] == 2 and st["queued"] == 2
         srv.cancel(3)                    # queued: leaves at once
