@@ -529,6 +529,7 @@ int ctx_create(const afid_grid_t *grid, const afid_params_t *prm, const BatchSpe
   }
   L.warp_fft = true;
   L.k1_var = 0;
+  L.k4_var = 0;
   L.plan_y = py;
   L.plan_z = pz;
   L.twy = twy;
@@ -612,6 +613,38 @@ int ctx_autotune(afid_ctx_t *ctx, bool force) {
     if (e != cudaSuccess) return fail_cuda(ctx, e);
   }
   ctx->L.k1_var = info.chosen;
+  // The Poisson tridiagonal (FP64 spectra): both forms timed on full launches over the spectrum
+  // buffer, whose contents are dead between substeps (K2 rewrites all of it).
+  info.k4_chosen = 0;
+  info.k4_us[0] = info.k4_us[1] = -1.0;
+  if (!L.mixed) {
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    cudaError_t e = cudaEventCreate(&e0);
+    if (e == cudaSuccess) e = cudaEventCreate(&e1);
+    SubstepBuffers b = buffers(ctx);
+    LaunchCtx L4 = ctx->L;
+    L4.g.active = ctx->L.g.active;
+    constexpr int kReps = 3;
+    for (int round = 0; round < 2 && e == cudaSuccess; ++round)
+      for (int v = 0; v < 2 && e == cudaSuccess; ++v) {
+        L4.k4_var = v;
+        if ((e = launch_stage(L4, b, 0, Stage::Tridiag)) != cudaSuccess) break;
+        cudaEventRecord(e0, ctx->stream);
+        for (int r = 0; r < kReps && e == cudaSuccess; ++r) e = launch_stage(L4, b, 0, Stage::Tridiag);
+        cudaEventRecord(e1, ctx->stream);
+        if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+        float ms = 0.f;
+        if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+        ctx->launches += 1 + kReps;
+        const double us = 1e3 * ms / kReps;
+        if (e == cudaSuccess && (info.k4_us[v] < 0.0 || us < info.k4_us[v])) info.k4_us[v] = us;
+      }
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    if (e != cudaSuccess) return fail_cuda(ctx, e);
+    if (info.k4_us[1] >= 0.0 && info.k4_us[1] < info.k4_us[0]) info.k4_chosen = 1;
+  }
+  ctx->L.k4_var = info.k4_chosen;
   ctx->tune = info;
   ctx->tuned = true;
   return check_err_flag(ctx);
@@ -868,6 +901,13 @@ int afid_gpu_set_k1_shape(afid_ctx_t *ctx, int index) {
   ctx->tune = info;
   ctx->L.k1_var = index;
   ctx->tuned = true;
+  return AFID_OK;
+}
+
+int afid_gpu_set_k4_form(afid_ctx_t *ctx, int form) {
+  if (!ctx || form < 0 || form > 1 || (form == 1 && ctx->L.mixed)) return AFID_E_INVALID;
+  ctx->L.k4_var = form;
+  ctx->tune.k4_chosen = form;
   return AFID_OK;
 }
 

@@ -18,6 +18,7 @@ struct LaunchCtx {
   int tx_y, tx_z;  // x-tile widths of the shared-memory (fallback) FFT kernels
   bool warp_fft;   // register-resident warp FFT when N = 32*{1,2,3,4,6,8,12,16,24,32}
   int k1_var;      // K1 thread shape (index into the shapes of k1_shapes(M)), set by the autotuner
+  int k4_var;      // K4 form: 0 one mode a warp, 1 persistent with the next mode prefetched (FP64)
   FftPlan plan_y, plan_z;
   const void *twy, *twz;  // twiddle tables (double2 or float2)
 };

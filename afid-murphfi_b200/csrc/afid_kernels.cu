@@ -941,6 +941,193 @@ cudaError_t launch_explicit_implicit(const LaunchCtx &L, const SubstepBuffers &b
   return L.mixed ? launch_k1_mixed(L, b, ns, L.k1_var, ncol) : launch_k1_fp64(L, b, ns, L.k1_var, ncol);
 }
 
+// ------------------------------------------------------------------------------------------
+// K4, persistent form (FP64): each warp solves modes sys, sys + gridDim.x*W, ... and brings the
+// next mode's right-hand side into shared memory with asynchronous copies (cp.async) while it
+// solves the current one (two buffers a warp).  The mode-independent rows (amphk, apphk, acphk in
+// chunk layout) are staged once a block and shared by its warps; the diagonal of a mode is formed
+// from acphk as the one-mode kernel forms it, and the pinned (0,0) row is applied on the fly.
+// Same arithmetic, in the same order, as k_tridiag_pressure.
+// ------------------------------------------------------------------------------------------
+template <int M, int WPB>
+__global__ void __launch_bounds__(WPB * 32)
+    k_tridiag_pressure_p(Geom g, Tables t, double2 *__restrict__ spec, int *__restrict__ err) {
+  extern __shared__ double smem_k4p[];
+  constexpr int LD = chunk_ld(M);
+  constexpr int FL = LD * M;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int n = g.nxm;
+  double *sa = smem_k4p, *sc_ = sa + FL, *sacp = sa + 2 * FL;  // shared by the block
+  double *buf = sa + 3 * FL + (size_t)warp * 4 * FL;          // [2][dr, di] of this warp
+  for (int r = threadIdx.x; r < 32 * M; r += WPB * 32) {
+    const int s = (r % M) * LD + r / M;
+    sa[s] = (r < n && r > 0) ? __ldg(t.amphk + r) : 0.0;
+    sc_[s] = (r < n - 1) ? __ldg(t.apphk + r) : 0.0;
+    sacp[s] = (r < n) ? __ldg(t.acphk + r) : 0.0;
+  }
+  __syncthreads();
+  const int nsys = g.nyh * g.nzm;
+  const int stride = gridDim.x * WPB;
+  int sys = blockIdx.x * WPB + warp;
+  // the right-hand side of mode `m` into buffer `b`: rows r = lane + 32 tt, zero past nxm
+  auto fetch = [&](int m, int b) {
+    const double2 *colp = spec + (size_t)m * g.ldxc;
+    double *dr = buf + b * 2 * FL, *di = dr + FL;
+#pragma unroll
+    for (int tt = 0; tt < M; ++tt) {
+      const int r = lane + 32 * tt;
+      const int s = (r % M) * LD + r / M;
+      const bool ok = r < n;
+      const double *src = ok ? &colp[r].x : &colp[0].x;
+      cp_async_zfill<8>(&dr[s], src, ok);
+      cp_async_zfill<8>(&di[s], src + 1, ok);
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
+  };
+  if (sys < nsys) fetch(sys, 0);
+  bool bad = false;
+  for (int it = 0; sys < nsys; ++it, sys += stride) {
+    const int nxt = sys + stride;
+    if (nxt < nsys) {
+      fetch(nxt, (it + 1) & 1);
+      asm volatile("cp.async.wait_group 1;" ::: "memory");
+    } else {
+      asm volatile("cp.async.wait_group 0;" ::: "memory");
+    }
+    __syncwarp();
+    double *sdr = buf + (it & 1) * 2 * FL, *sdi = sdr + FL;
+    const int ky = sys % g.nyh, kz = sys / g.nyh;
+    const bool active = inst_active(g, kz);
+    if (active) {
+      const bool pin = (ky == 0 && (kz == 0 || g.batch));
+      const double akj = __ldg(t.ak2 + (g.batch ? (size_t)kz * g.nym : 0) + ky);
+      const double aki = g.batch ? 0.0 : __ldg(t.ak1 + kz);
+      const int s0 = lane * M;
+      // row s0 + q of this lane's chunk: the pinned row is phi = 0 (a = 0, b = 1, rhs 0)
+      auto pinrow = [&](int q) { return pin && (s0 + q == n - 1); };
+      auto diag = [&](int q) -> double {
+        const int r = s0 + q;
+        return (r < n && !pinrow(q)) ? (sacp[q * LD + lane] - akj - aki) * (1.0 + 1.0e-15) : 1.0;
+      };
+      auto aa = [&](int q) { return pinrow(q) ? 0.0 : sa[q * LD + lane]; };
+      auto rr = [&](const double *d, int q) { return pinrow(q) ? 0.0 : d[q * LD + lane]; };
+      double cp[M], yr[M], yi[M], v[M], w[M];
+      cp[0] = 0.0; yr[0] = 0.0; yi[0] = 0.0; v[0] = 0.0; w[0] = 0.0;
+#pragma unroll
+      for (int q = 1; q < M; ++q) {
+        const double a = aa(q), c = sc_[q * LD + lane];
+        const double den = (q > 1) ? diag(q) - a * cp[q - 1] : diag(q);
+        bad |= (den == 0.0);
+        const double inv = 1.0 / den;
+        cp[q] = c * inv;
+        const double dr = rr(sdr, q), di = rr(sdi, q);
+        if (q > 1) {
+          yr[q] = (dr - a * yr[q - 1]) * inv;
+          yi[q] = (di - a * yi[q - 1]) * inv;
+          v[q] = -a * v[q - 1] * inv;
+        } else {
+          yr[q] = dr * inv;
+          yi[q] = di * inv;
+          v[q] = -a * inv;
+        }
+        w[q] = (q == M - 1) ? -c * inv : 0.0;
+      }
+#pragma unroll
+      for (int q = M - 2; q >= 1; --q) {
+        yr[q] -= cp[q] * yr[q + 1];
+        yi[q] -= cp[q] * yi[q + 1];
+        v[q] -= cp[q] * v[q + 1];
+        w[q] -= cp[q] * w[q + 1];
+      }
+      const double as_ = aa(0), cs_ = sc_[lane];
+      double A, B, Cc, Dr, Di;
+      if constexpr (M == 1) {
+        A = as_;
+        B = diag(0);
+        Cc = cs_;
+        Dr = rr(sdr, 0);
+        Di = rr(sdi, 0);
+      } else {
+        double vl = __shfl_up_sync(0xffffffffu, v[M - 1], 1);
+        double wl = __shfl_up_sync(0xffffffffu, w[M - 1], 1);
+        double yl_r = __shfl_up_sync(0xffffffffu, yr[M - 1], 1);
+        double yl_i = __shfl_up_sync(0xffffffffu, yi[M - 1], 1);
+        if (lane == 0) { vl = 0.0; wl = 0.0; yl_r = 0.0; yl_i = 0.0; }
+        A = as_ * vl;
+        B = diag(0) + as_ * wl + cs_ * v[1];
+        Cc = (lane == 31) ? 0.0 : cs_ * w[1];
+        Dr = rr(sdr, 0) - as_ * yl_r - cs_ * yr[1];
+        Di = rr(sdi, 0) - as_ * yl_i - cs_ * yi[1];
+      }
+      bad |= (B == 0.0);
+      const double rB = 1.0 / B;
+      double al_ = A * rB, ga_ = Cc * rB, er = Dr * rB, ei = Di * rB;
+#pragma unroll
+      for (int h = 1; h < 32; h <<= 1) {
+        double am = __shfl_up_sync(0xffffffffu, al_, h), gm = __shfl_up_sync(0xffffffffu, ga_, h);
+        double ap = __shfl_down_sync(0xffffffffu, al_, h), gp = __shfl_down_sync(0xffffffffu, ga_, h);
+        double erm = __shfl_up_sync(0xffffffffu, er, h), eim = __shfl_up_sync(0xffffffffu, ei, h);
+        double erp = __shfl_down_sync(0xffffffffu, er, h), eip = __shfl_down_sync(0xffffffffu, ei, h);
+        if (lane < h) { am = 0.0; gm = 0.0; erm = 0.0; eim = 0.0; }
+        if (lane + h >= 32) { ap = 0.0; gp = 0.0; erp = 0.0; eip = 0.0; }
+        const double dd = 1.0 - al_ * gm - ga_ * ap;
+        bad |= (dd == 0.0);
+        const double nrm = 1.0 / dd;
+        er = (er - al_ * erm - ga_ * erp) * nrm;
+        ei = (ei - al_ * eim - ga_ * eip) * nrm;
+        const double na = -al_ * am * nrm, ng = -ga_ * gp * nrm;
+        al_ = na;
+        ga_ = ng;
+      }
+      double xnr = __shfl_down_sync(0xffffffffu, er, 1), xni = __shfl_down_sync(0xffffffffu, ei, 1);
+      if (lane == 31) { xnr = 0.0; xni = 0.0; }
+      __syncwarp();  // every lane has read its rows before any is overwritten
+      sdr[lane] = er;
+      sdi[lane] = ei;
+#pragma unroll
+      for (int q = 1; q < M; ++q) {
+        sdr[q * LD + lane] = yr[q] + v[q] * er + w[q] * xnr;
+        sdi[q * LD + lane] = yi[q] + v[q] * ei + w[q] * xni;
+      }
+      __syncwarp();
+      double2 *colp = spec + (size_t)sys * g.ldxc;
+#pragma unroll 1
+      for (int tt = 0; tt < M; ++tt) {
+        const int r = lane + 32 * tt;
+        if (r < n) {
+          const int s = (r % M) * LD + r / M;
+          colp[r] = make_double2(sdr[s], sdi[s]);
+        }
+      }
+    }
+    __syncwarp();  // this buffer is refilled two modes from now
+  }
+  asm volatile("cp.async.wait_group 0;" ::: "memory");
+  if (bad) atomicOr(err, 1);
+}
+
+static int k4p_grid(int nsys, int wpb) {
+  static int nsm = 0;
+  if (nsm == 0) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || nsm < 1) nsm = 148;
+  }
+  return std::max(1, std::min((nsys + wpb - 1) / wpb, nsm * 16 / wpb * 2));
+}
+
+template <int M>
+static cudaError_t launch_k4p_M(const LaunchCtx &L, void *spec, int *err) {
+  constexpr int W = (M >= 16) ? 2 : 4;
+  const int nsys = L.g.nyh * L.g.nzm;
+  const size_t smem = (size_t)(3 + 4 * W) * chunk_ld(M) * M * sizeof(double);
+  auto kern = k_tridiag_pressure_p<M, W>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  kern<<<k4p_grid(nsys, W), W * 32, smem, L.stream>>>(L.g, L.t, (double2 *)spec, err);
+  return cudaGetLastError();
+}
+
 template <int M, typename TS>
 static cudaError_t launch_k4_M(const LaunchCtx &L, void *spec, int *err) {
   constexpr int W = (M >= 16) ? 2 : 4;
@@ -954,6 +1141,21 @@ static cudaError_t launch_k4_M(const LaunchCtx &L, void *spec, int *err) {
 
 template <typename TS>
 static cudaError_t launch_k4_T(const LaunchCtx &L, void *spec, int *err) {
+  if constexpr (sizeof(TS) == sizeof(double)) {
+    if (L.k4_var == 1) {  // the persistent prefetching form (the autotuner's pick, FP64 spectra)
+      switch (L.M) {
+        case 1: return launch_k4p_M<1>(L, spec, err);
+        case 2: return launch_k4p_M<2>(L, spec, err);
+        case 4: return launch_k4p_M<4>(L, spec, err);
+        case 8: return launch_k4p_M<8>(L, spec, err);
+        case 12: return launch_k4p_M<12>(L, spec, err);
+        case 16: return launch_k4p_M<16>(L, spec, err);
+        case 24: return launch_k4p_M<24>(L, spec, err);
+        case 32: return launch_k4p_M<32>(L, spec, err);
+      }
+      return cudaErrorInvalidValue;
+    }
+  }
   switch (L.M) {
     case 1: return launch_k4_M<1, TS>(L, spec, err);
     case 2: return launch_k4_M<2, TS>(L, spec, err);
