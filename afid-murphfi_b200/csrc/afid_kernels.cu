@@ -950,7 +950,7 @@ cudaError_t launch_explicit_implicit(const LaunchCtx &L, const SubstepBuffers &b
 // Same arithmetic, in the same order, as k_tridiag_pressure.
 // ------------------------------------------------------------------------------------------
 template <int M, int WPB>
-__global__ void __launch_bounds__(WPB * 32)
+__global__ void __launch_bounds__(WPB * 32, (WPB == 4) ? 4 : 2)
     k_tridiag_pressure_p(Geom g, Tables t, double2 *__restrict__ spec, int *__restrict__ err) {
   extern __shared__ double smem_k4p[];
   constexpr int LD = chunk_ld(M);
@@ -1106,14 +1106,14 @@ __global__ void __launch_bounds__(WPB * 32)
   if (bad) atomicOr(err, 1);
 }
 
-static int k4p_grid(int nsys, int wpb) {
-  static int nsm = 0;
-  if (nsm == 0) {
-    int dev = 0;
-    cudaGetDevice(&dev);
-    if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || nsm < 1) nsm = 148;
-  }
-  return std::max(1, std::min((nsys + wpb - 1) / wpb, nsm * 16 / wpb * 2));
+// Persistent grid: as many blocks as can be resident at once, no more than there are modes.
+template <typename K>
+static int k4p_grid(K kern, int nsys, int wpb, size_t smem) {
+  int dev = 0, nsm = 148, per = 1;
+  cudaGetDevice(&dev);
+  if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || nsm < 1) nsm = 148;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, wpb * 32, smem) != cudaSuccess || per < 1) per = 1;
+  return std::max(1, std::min((nsys + wpb - 1) / wpb, nsm * per));
 }
 
 template <int M>
@@ -1124,7 +1124,7 @@ static cudaError_t launch_k4p_M(const LaunchCtx &L, void *spec, int *err) {
   auto kern = k_tridiag_pressure_p<M, W>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
-  kern<<<k4p_grid(nsys, W), W * 32, smem, L.stream>>>(L.g, L.t, (double2 *)spec, err);
+  kern<<<k4p_grid(kern, nsys, W, smem), W * 32, smem, L.stream>>>(L.g, L.t, (double2 *)spec, err);
   return cudaGetLastError();
 }
 
