@@ -980,8 +980,9 @@ def published_bou_text(t_end: float) -> str:
 
 def run_published(args):
     """The published example on the device from a seeded start to t = args.t_end: the main loop
-    (CFLmr -> dt rule -> TimeMarcher) with the five Nusselt numbers of tools/plot_time_series.py
-    sampled every args.sample_dt, their averages from t = 75 against the digitised figure."""
+    (CFLmr -> dt rule -> TimeMarcher) with the Nusselt and Reynolds numbers of
+    tools/plot_time_series.py sampled every args.sample_dt, their averages from t = 75 against the
+    digitised figures."""
     import numpy as np
     import torch
     import afid_gpu as ag
@@ -1001,16 +1002,21 @@ def run_published(args):
     dxr, dxc = xcr[1:] - xcr[:-1], xc[1:w["nxm"] + 1] - xc[:w["nxm"]]
     pec = (w["rays"] * w["pras"]) ** 0.5
 
-    def nusselt():  # tools/plot_time_series.py:17-35
+    inu = (w["rays"] / w["pras"]) ** 0.5
+
+    def sample():  # tools/plot_time_series.py:17-35 (Nusselt), :50-61 (Reynolds)
         ps, pf = solver.sal_profiles(), solver.mean_profiles()
+        re_v = float((pf["vxrms"] ** 2 * dxc).sum()) ** 0.5 * inu
+        re_h = float(((pf["vyrms"] ** 2 + pf["vzrms"] ** 2) * dxc).sum()) ** 0.5 * inu
         return {"nu_pl": (0.5 + ps["Sbar"][0]) / xmr[0], "nu_pu": (0.5 - ps["Sbar"][-1]) / (1.0 - xmr[-1]),
                 "nu_chi": float((ps["chiS"] * dxr).sum()) * pec,
                 "nu_eps": 1.0 + float((pf["epsilon"] * dxc).sum()) * pec,
-                "nu_vol": 1.0 - float((ps["vxS"] * dxr).sum()) * pec}
+                "nu_vol": 1.0 - float((ps["vxS"] * dxr).sum()) * pec,
+                "re_v": re_v, "re_h": re_h, "re_t": (re_v ** 2 + re_h ** 2) ** 0.5}
 
     dtc = ctypes.c_double(inp.dt)
     t, n, err = 0.0, 0, 0
-    times, series = [], {k: [] for k in ("nu_pl", "nu_pu", "nu_chi", "nu_eps", "nu_vol")}
+    times, series = [], {k: [] for k in ("nu_pl", "nu_pu", "nu_chi", "nu_eps", "nu_vol", "re_v", "re_h", "re_t")}
     next_sample = args.sample_dt
     torch.cuda.synchronize()
     t0 = time.perf_counter()
@@ -1020,7 +1026,7 @@ def run_published(args):
         t += dtc.value
         n += 1
         if t >= next_sample - 1e-12:
-            for k, v in nusselt().items():
+            for k, v in sample().items():
                 series[k].append(float(v))
             times.append(t)
             next_sample += args.sample_dt
@@ -1028,7 +1034,7 @@ def run_published(args):
     wall = time.perf_counter() - t0
     solver.close()
     tables.close()
-    with open(os.path.join(ROOT, "tests", "golden", "published_nusselt_rbc_ra1e8_pr10.json")) as f:
+    with open(os.path.join(ROOT, "tests", "golden", "published_rbc_ra1e8_pr10.json")) as f:
         pub = json.load(f)
     tt = np.array(times)
     ours = {}
@@ -1036,8 +1042,8 @@ def run_published(args):
         v = np.array(v)
         m = tt >= 75.0
         ours[k] = float(np.trapezoid(v[m], tt[m]) / (tt[m][-1] - tt[m][0])) if m.sum() > 1 else float("nan")
-    ref = pub["mean_from_75"]
-    line = {"metric": "Nusselt numbers of the reference's published RBC example, averaged over t >= 75",
+    ref = dict(pub["nusselt"]["mean_from_75"], **pub["reynolds"]["mean_from_75"])
+    line = {"metric": "Nusselt and Reynolds numbers of the reference's published RBC example, averaged over t >= 75",
             "config": {"workload": w["name"], "t_end": args.t_end, "steps": n, "sample_dt": args.sample_dt,
                        "data": "synthetic seeded start (the statistically steady state is what is compared)"},
             "errorcode": err, "wall_s": round(wall, 1), "mean_from_75": {k: round(v, 3) for k, v in ours.items()},
