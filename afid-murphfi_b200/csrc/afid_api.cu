@@ -530,6 +530,7 @@ int ctx_create(const afid_grid_t *grid, const afid_params_t *prm, const BatchSpe
   L.warp_fft = true;
   L.k1_var = 0;
   L.k4_var = 0;
+  L.fftz_var = 0;
   L.plan_y = py;
   L.plan_z = pz;
   L.twy = twy;
@@ -645,6 +646,37 @@ int ctx_autotune(afid_ctx_t *ctx, bool force) {
     if (info.k4_us[1] >= 0.0 && info.k4_us[1] < info.k4_us[0]) info.k4_chosen = 1;
   }
   ctx->L.k4_var = info.k4_chosen;
+  // The z transforms (3-D single domains): one tile per block, or persistent blocks with the next
+  // tile's copies in flight; timed the same way (the spectrum's contents are dead here too).
+  info.fftz_chosen = 0;
+  info.fftz_us[0] = info.fftz_us[1] = -1.0;
+  if (ctx->L.g.nzm > 1 && !ctx->L.g.batch) {
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    cudaError_t e = cudaEventCreate(&e0);
+    if (e == cudaSuccess) e = cudaEventCreate(&e1);
+    SubstepBuffers b = buffers(ctx);
+    LaunchCtx Lz = ctx->L;
+    constexpr int kReps = 3;
+    for (int round = 0; round < 2 && e == cudaSuccess; ++round)
+      for (int v = 0; v < 2 && e == cudaSuccess; ++v) {
+        Lz.fftz_var = v;
+        if ((e = launch_stage(Lz, b, 0, Stage::FftZFwd)) != cudaSuccess) break;
+        cudaEventRecord(e0, ctx->stream);
+        for (int r = 0; r < kReps && e == cudaSuccess; ++r) e = launch_stage(Lz, b, 0, Stage::FftZFwd);
+        cudaEventRecord(e1, ctx->stream);
+        if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+        float ms = 0.f;
+        if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+        ctx->launches += 1 + kReps;
+        const double us = 1e3 * ms / kReps;
+        if (e == cudaSuccess && (info.fftz_us[v] < 0.0 || us < info.fftz_us[v])) info.fftz_us[v] = us;
+      }
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    if (e != cudaSuccess) return fail_cuda(ctx, e);
+    if (info.fftz_us[1] >= 0.0 && info.fftz_us[1] < info.fftz_us[0]) info.fftz_chosen = 1;
+  }
+  ctx->L.fftz_var = info.fftz_chosen;
   ctx->tune = info;
   ctx->tuned = true;
   return check_err_flag(ctx);
@@ -908,6 +940,13 @@ int afid_gpu_set_k4_form(afid_ctx_t *ctx, int form) {
   if (!ctx || form < 0 || form > 1 || (form == 1 && ctx->L.mixed)) return AFID_E_INVALID;
   ctx->L.k4_var = form;
   ctx->tune.k4_chosen = form;
+  return AFID_OK;
+}
+
+int afid_gpu_set_fftz_form(afid_ctx_t *ctx, int form) {
+  if (!ctx || form < 0 || form > 1) return AFID_E_INVALID;
+  ctx->L.fftz_var = form;
+  ctx->tune.fftz_chosen = form;
   return AFID_OK;
 }
 

@@ -817,6 +817,75 @@ __global__ void __launch_bounds__(256)
   }
 }
 
+// K3w / K5w, persistent form: each block transforms tiles t = blockIdx.x, + gridDim.x, ... (8 x
+// points at one ky each, as k_fft_z_w) with two tile buffers: the next tile's asynchronous copies
+// are in flight while the current tile is transformed and stored.  Same arithmetic as k_fft_z_w.
+template <int N1, bool INV, typename TS>
+__global__ void __launch_bounds__(256)
+    k_fft_z_wp(Geom g, typename Cplx<TS>::type *__restrict__ spec,
+               const typename Cplx<TS>::type *__restrict__ tw) {
+  using C = typename Cplx<TS>::type;
+  constexpr int N = 32 * N1;
+  extern __shared__ __align__(16) unsigned char smem_k3p[];
+  C *sb = reinterpret_cast<C *>(smem_k3p);  // [2][N][8], swizzled columns
+  const size_t zstride = (size_t)g.nyh * g.ldxc;
+  const int ntx = (g.nxm + 7) / 8;
+  const int ntiles = ntx * g.nyh;
+  auto issue = [&](int tile, int b) {
+    const int k0 = (tile % ntx) * 8, ky = tile / ntx;
+    const C *base = spec + (size_t)ky * g.ldxc + k0;
+    const int nvalid = min(8, g.nxm - k0);
+    C *s = sb + (size_t)b * N * 8;
+#pragma unroll
+    for (int it = 0; it < N1; ++it) {
+      const int e = threadIdx.x + 256 * it;
+      const int ex = e & 7, iz = e >> 3;
+      const bool ok = ex < nvalid;
+      cp_async_zfill<(int)sizeof(C)>(&s[iz * 8 + (ex ^ zsw(iz))],
+                                     ok ? (const void *)(base + (size_t)iz * zstride + ex) : (const void *)base, ok);
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
+  };
+  int tile = blockIdx.x;
+  if (tile < ntiles) issue(tile, 0);
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  for (int it = 0; tile < ntiles; ++it, tile += gridDim.x) {
+    const int nt = tile + gridDim.x;
+    if (nt < ntiles) {
+      issue(nt, (it + 1) & 1);
+      asm volatile("cp.async.wait_group 1;" ::: "memory");
+    } else {
+      asm volatile("cp.async.wait_group 0;" ::: "memory");
+    }
+    __syncthreads();
+    C *s = sb + (size_t)(it & 1) * N * 8;
+    C x[N1];
+#pragma unroll
+    for (int m = 0; m < N1; ++m) {
+      const int r = lane + 32 * m;
+      x[m] = s[r * 8 + (w ^ zsw(r))];
+    }
+    warp_fft<INV, TS, N1>(x, lane, tw);
+    __syncthreads();
+    const int rl = bitrev5(lane);
+#pragma unroll
+    for (int k1 = 0; k1 < N1; ++k1) {
+      const int r = k1 + N1 * rl;
+      s[r * 8 + (w ^ zsw(r))] = x[k1];
+    }
+    __syncthreads();
+    const int k0 = (tile % ntx) * 8, ky = tile / ntx;
+    C *base = spec + (size_t)ky * g.ldxc + k0;
+    const int nvalid = min(8, g.nxm - k0);
+#pragma unroll 4
+    for (int e = threadIdx.x; e < N * 8; e += blockDim.x) {
+      const int ex = e & 7, iz = e >> 3;
+      if (ex < nvalid) base[(size_t)iz * zstride + ex] = s[iz * 8 + (ex ^ zsw(iz))];
+    }
+    __syncthreads();  // this buffer is refilled by the copies issued in the next iteration but one
+  }
+}
+
 // K6w: backward y c2r.  Block: 16 x points = 8 pairs (8 warps) at one z index i.  The half
 // spectrum rows 0 .. N/2 of the 16 x points are staged with asynchronous copies (all in flight
 // at once); each warp then builds its packed sequence straight from them.
@@ -1195,6 +1264,18 @@ static cudaError_t launch_w_n1(const LaunchCtx &L, const SubstepBuffers &b, int 
     return cudaGetLastError();
   }
   const size_t sm = (size_t)N * 8 * sizeof(C);
+  if (L.fftz_var == 1) {  // persistent, double-buffered tiles (the autotuner's pick)
+    auto kern = (st == Stage::FftZFwd) ? k_fft_z_wp<N1, false, TS> : k_fft_z_wp<N1, true, TS>;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(2 * sm));
+    if (e != cudaSuccess) return e;
+    int dev = 0, nsm = 148, per = 1;
+    cudaGetDevice(&dev);
+    if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || nsm < 1) nsm = 148;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, 256, 2 * sm) != cudaSuccess || per < 1) per = 1;
+    const int ntiles = ((g.nxm + 7) / 8) * g.nyh;
+    kern<<<std::max(1, std::min(ntiles, nsm * per)), 256, 2 * sm, L.stream>>>(g, spec, (const C *)L.twz);
+    return cudaGetLastError();
+  }
   dim3 grid((g.nxm + 7) / 8, g.nyh);
   auto kern = (st == Stage::FftZFwd) ? k_fft_z_w<N1, false, TS> : k_fft_z_w<N1, true, TS>;
   cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);

@@ -180,6 +180,9 @@ typedef struct afid_tune_info {
   int k4_chosen;                /* Poisson tridiagonal: 0 one mode per warp, 1 persistent warps
                                    with the next mode's right-hand side prefetched (FP64 only)  */
   double k4_us[2];              /* microseconds per full launch of each form (-1: not run)   */
+  int fftz_chosen;              /* z transforms: 0 one tile per block, 1 persistent blocks with
+                                   the next tile's copies in flight (3-D single domains)         */
+  double fftz_us[2];            /* microseconds per full forward z launch of each form         */
 } afid_tune_info_t;
 int afid_gpu_autotune(afid_ctx_t *ctx, int force, afid_tune_info_t *info);
 /* Use shape `index` (0 .. ncand-1) from now on without timing, e.g. one saved from an earlier
@@ -188,6 +191,8 @@ int afid_gpu_set_k1_shape(afid_ctx_t *ctx, int index);
 /* Use Poisson-tridiagonal form `form` (0 or 1 as in afid_tune_info_t.k4_chosen; 1 needs FP64
  * spectra) from now on; both forms give bitwise the same results. */
 int afid_gpu_set_k4_form(afid_ctx_t *ctx, int form);
+/* Use z-transform form `form` (0 or 1 as in afid_tune_info_t.fftz_chosen); bitwise the same. */
+int afid_gpu_set_fftz_form(afid_ctx_t *ctx, int form);
 /* Test hook of the bounded device waits (no counterpart in the reference).  With polls > 0
  * (at most 2^24), the fused explicit/implicit kernel's staging wait, after its copies have
  * landed, also waits at most `polls` polls for an mbarrier phase that nothing completes: every

@@ -205,10 +205,11 @@ def test_launch_count_positive():
         assert gpu.launch_count() - n0 == 1 + 3 * 7
 
 
-@pytest.mark.parametrize("shape", [(256, 24, 16), (100, 16, 8), (60, 16, 1), (500, 16, 4)])
-def test_k4_forms_bitwise_identical(shape):
+@pytest.mark.parametrize("shape", [(256, 24, 16), (100, 16, 8), (60, 16, 1), (500, 16, 4), (64, 32, 96)])
+def test_k4_and_fftz_forms_bitwise_identical(shape):
     """Both forms of the Poisson tridiagonal (a mode per warp; persistent warps with the next
-    mode prefetched) give the same fields bit for bit, so the autotuner's choice changes the
+    mode prefetched) and of the z transforms (a tile per block; persistent blocks with the next
+    tile prefetched) give the same fields bit for bit, so the autotuner's choices change the
     schedule only."""
     case = Case(*shape, rayt=1e6, dt=2e-3)
     s = case.oracle_state(random_velocity=0.1)
@@ -217,6 +218,7 @@ def test_k4_forms_bitwise_identical(shape):
         with case.solver() as g:
             g.autotune()
             g.set_k4_form(form)
+            g.set_fftz_form(form)
             g.upload(s.vx, s.vy, s.vz, s.temp, s.pr)
             for n in range(2):
                 g.time_marcher(2e-3, n)
