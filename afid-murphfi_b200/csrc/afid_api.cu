@@ -629,7 +629,10 @@ int ctx_autotune(afid_ctx_t *ctx, bool force) {
     for (int round = 0; round < 2 && e == cudaSuccess; ++round)
       for (int v = 0; v < 2 && e == cudaSuccess; ++v) {
         L4.k4_var = v;
-        if ((e = launch_stage(L4, b, 0, Stage::Tridiag)) != cudaSuccess) break;
+        if (launch_stage(L4, b, 0, Stage::Tridiag) != cudaSuccess) {  // this form does not fit: skip it
+          cudaGetLastError();
+          continue;
+        }
         cudaEventRecord(e0, ctx->stream);
         for (int r = 0; r < kReps && e == cudaSuccess; ++r) e = launch_stage(L4, b, 0, Stage::Tridiag);
         cudaEventRecord(e1, ctx->stream);
@@ -660,7 +663,10 @@ int ctx_autotune(afid_ctx_t *ctx, bool force) {
     for (int round = 0; round < 2 && e == cudaSuccess; ++round)
       for (int v = 0; v < 2 && e == cudaSuccess; ++v) {
         Lz.fftz_var = v;
-        if ((e = launch_stage(Lz, b, 0, Stage::FftZFwd)) != cudaSuccess) break;
+        if (launch_stage(Lz, b, 0, Stage::FftZFwd) != cudaSuccess) {  // this form does not fit: skip it
+          cudaGetLastError();
+          continue;
+        }
         cudaEventRecord(e0, ctx->stream);
         for (int r = 0; r < kReps && e == cudaSuccess; ++r) e = launch_stage(Lz, b, 0, Stage::FftZFwd);
         cudaEventRecord(e1, ctx->stream);

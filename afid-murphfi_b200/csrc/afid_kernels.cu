@@ -1265,6 +1265,7 @@ static cudaError_t launch_w_n1(const LaunchCtx &L, const SubstepBuffers &b, int 
   }
   const size_t sm = (size_t)N * 8 * sizeof(C);
   if (L.fftz_var == 1) {  // persistent, double-buffered tiles (the autotuner's pick)
+    if (2 * sm > (size_t)227 * 1024) return cudaErrorInvalidValue;  // two tiles do not fit
     auto kern = (st == Stage::FftZFwd) ? k_fft_z_wp<N1, false, TS> : k_fft_z_wp<N1, true, TS>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(2 * sm));
     if (e != cudaSuccess) return e;
