@@ -614,11 +614,11 @@ int ctx_autotune(afid_ctx_t *ctx, bool force) {
     if (e != cudaSuccess) return fail_cuda(ctx, e);
   }
   ctx->L.k1_var = info.chosen;
-  // The Poisson tridiagonal (FP64 spectra): both forms timed on full launches over the spectrum
-  // buffer, whose contents are dead between substeps (K2 rewrites all of it).
+  // The Poisson tridiagonal: both forms timed on full launches over the spectrum buffer, whose
+  // contents are dead between substeps (K2 rewrites all of it).
   info.k4_chosen = 0;
   info.k4_us[0] = info.k4_us[1] = -1.0;
-  if (!L.mixed) {
+  {
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     cudaError_t e = cudaEventCreate(&e0);
     if (e == cudaSuccess) e = cudaEventCreate(&e1);
@@ -943,7 +943,7 @@ int afid_gpu_set_k1_shape(afid_ctx_t *ctx, int index) {
 }
 
 int afid_gpu_set_k4_form(afid_ctx_t *ctx, int form) {
-  if (!ctx || form < 0 || form > 1 || (form == 1 && ctx->L.mixed)) return AFID_E_INVALID;
+  if (!ctx || form < 0 || form > 1) return AFID_E_INVALID;
   ctx->L.k4_var = form;
   ctx->tune.k4_chosen = form;
   return AFID_OK;

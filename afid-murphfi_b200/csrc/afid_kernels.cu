@@ -1018,16 +1018,17 @@ cudaError_t launch_explicit_implicit(const LaunchCtx &L, const SubstepBuffers &b
 // from acphk as the one-mode kernel forms it, and the pinned (0,0) row is applied on the fly.
 // Same arithmetic, in the same order, as k_tridiag_pressure.
 // ------------------------------------------------------------------------------------------
-template <int M, int WPB>
+template <int M, int WPB, typename TS>
 __global__ void __launch_bounds__(WPB * 32, (WPB == 4) ? 4 : 2)
-    k_tridiag_pressure_p(Geom g, Tables t, double2 *__restrict__ spec, int *__restrict__ err) {
+    k_tridiag_pressure_p(Geom g, Tables t, typename Cplx<TS>::type *__restrict__ spec, int *__restrict__ err) {
+  using C = typename Cplx<TS>::type;
   extern __shared__ double smem_k4p[];
   constexpr int LD = chunk_ld(M);
   constexpr int FL = LD * M;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int n = g.nxm;
   double *sa = smem_k4p, *sc_ = sa + FL, *sacp = sa + 2 * FL;  // shared by the block
-  double *buf = sa + 3 * FL + (size_t)warp * 4 * FL;          // [2][dr, di] of this warp
+  TS *buf = reinterpret_cast<TS *>(sa + 3 * FL) + (size_t)warp * 4 * FL;  // [2][dr, di] of this warp
   for (int r = threadIdx.x; r < 32 * M; r += WPB * 32) {
     const int s = (r % M) * LD + r / M;
     sa[s] = (r < n && r > 0) ? __ldg(t.amphk + r) : 0.0;
@@ -1040,16 +1041,16 @@ __global__ void __launch_bounds__(WPB * 32, (WPB == 4) ? 4 : 2)
   int sys = blockIdx.x * WPB + warp;
   // the right-hand side of mode `m` into buffer `b`: rows r = lane + 32 tt, zero past nxm
   auto fetch = [&](int m, int b) {
-    const double2 *colp = spec + (size_t)m * g.ldxc;
-    double *dr = buf + b * 2 * FL, *di = dr + FL;
+    const C *colp = spec + (size_t)m * g.ldxc;
+    TS *dr = buf + b * 2 * FL, *di = dr + FL;
 #pragma unroll
     for (int tt = 0; tt < M; ++tt) {
       const int r = lane + 32 * tt;
       const int s = (r % M) * LD + r / M;
       const bool ok = r < n;
-      const double *src = ok ? &colp[r].x : &colp[0].x;
-      cp_async_zfill<8>(&dr[s], src, ok);
-      cp_async_zfill<8>(&di[s], src + 1, ok);
+      const TS *src = ok ? &colp[r].x : &colp[0].x;
+      cp_async_zfill<(int)sizeof(TS)>(&dr[s], src, ok);
+      cp_async_zfill<(int)sizeof(TS)>(&di[s], src + 1, ok);
     }
     asm volatile("cp.async.commit_group;" ::: "memory");
   };
@@ -1064,7 +1065,7 @@ __global__ void __launch_bounds__(WPB * 32, (WPB == 4) ? 4 : 2)
       asm volatile("cp.async.wait_group 0;" ::: "memory");
     }
     __syncwarp();
-    double *sdr = buf + (it & 1) * 2 * FL, *sdi = sdr + FL;
+    TS *sdr = buf + (it & 1) * 2 * FL, *sdi = sdr + FL;
     const int ky = sys % g.nyh, kz = sys / g.nyh;
     const bool active = inst_active(g, kz);
     if (active) {
@@ -1079,7 +1080,7 @@ __global__ void __launch_bounds__(WPB * 32, (WPB == 4) ? 4 : 2)
         return (r < n && !pinrow(q)) ? (sacp[q * LD + lane] - akj - aki) * (1.0 + 1.0e-15) : 1.0;
       };
       auto aa = [&](int q) { return pinrow(q) ? 0.0 : sa[q * LD + lane]; };
-      auto rr = [&](const double *d, int q) { return pinrow(q) ? 0.0 : d[q * LD + lane]; };
+      auto rr = [&](const TS *d, int q) { return pinrow(q) ? 0.0 : (double)d[q * LD + lane]; };
       double cp[M], yr[M], yi[M], v[M], w[M];
       cp[0] = 0.0; yr[0] = 0.0; yi[0] = 0.0; v[0] = 0.0; w[0] = 0.0;
 #pragma unroll
@@ -1151,21 +1152,25 @@ __global__ void __launch_bounds__(WPB * 32, (WPB == 4) ? 4 : 2)
       double xnr = __shfl_down_sync(0xffffffffu, er, 1), xni = __shfl_down_sync(0xffffffffu, ei, 1);
       if (lane == 31) { xnr = 0.0; xni = 0.0; }
       __syncwarp();  // every lane has read its rows before any is overwritten
-      sdr[lane] = er;
-      sdi[lane] = ei;
+      // the results overwrite the inputs in the buffer, rounded to the spectrum's type once
+      sdr[lane] = (TS)er;
+      sdi[lane] = (TS)ei;
 #pragma unroll
       for (int q = 1; q < M; ++q) {
-        sdr[q * LD + lane] = yr[q] + v[q] * er + w[q] * xnr;
-        sdi[q * LD + lane] = yi[q] + v[q] * ei + w[q] * xni;
+        sdr[q * LD + lane] = (TS)(yr[q] + v[q] * er + w[q] * xnr);
+        sdi[q * LD + lane] = (TS)(yi[q] + v[q] * ei + w[q] * xni);
       }
       __syncwarp();
-      double2 *colp = spec + (size_t)sys * g.ldxc;
+      C *colp = spec + (size_t)sys * g.ldxc;
 #pragma unroll 1
       for (int tt = 0; tt < M; ++tt) {
         const int r = lane + 32 * tt;
         if (r < n) {
           const int s = (r % M) * LD + r / M;
-          colp[r] = make_double2(sdr[s], sdi[s]);
+          C o;
+          o.x = sdr[s];
+          o.y = sdi[s];
+          colp[r] = o;
         }
       }
     }
@@ -1185,15 +1190,15 @@ static int k4p_grid(K kern, int nsys, int wpb, size_t smem) {
   return std::max(1, std::min((nsys + wpb - 1) / wpb, nsm * per));
 }
 
-template <int M>
+template <int M, typename TS>
 static cudaError_t launch_k4p_M(const LaunchCtx &L, void *spec, int *err) {
   constexpr int W = (M >= 16) ? 2 : 4;
   const int nsys = L.g.nyh * L.g.nzm;
-  const size_t smem = (size_t)(3 + 4 * W) * chunk_ld(M) * M * sizeof(double);
-  auto kern = k_tridiag_pressure_p<M, W>;
+  const size_t smem = (size_t)3 * chunk_ld(M) * M * sizeof(double) + (size_t)4 * W * chunk_ld(M) * M * sizeof(TS);
+  auto kern = k_tridiag_pressure_p<M, W, TS>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
-  kern<<<k4p_grid(kern, nsys, W, smem), W * 32, smem, L.stream>>>(L.g, L.t, (double2 *)spec, err);
+  kern<<<k4p_grid(kern, nsys, W, smem), W * 32, smem, L.stream>>>(L.g, L.t, (typename Cplx<TS>::type *)spec, err);
   return cudaGetLastError();
 }
 
@@ -1210,20 +1215,18 @@ static cudaError_t launch_k4_M(const LaunchCtx &L, void *spec, int *err) {
 
 template <typename TS>
 static cudaError_t launch_k4_T(const LaunchCtx &L, void *spec, int *err) {
-  if constexpr (sizeof(TS) == sizeof(double)) {
-    if (L.k4_var == 1) {  // the persistent prefetching form (the autotuner's pick, FP64 spectra)
-      switch (L.M) {
-        case 1: return launch_k4p_M<1>(L, spec, err);
-        case 2: return launch_k4p_M<2>(L, spec, err);
-        case 4: return launch_k4p_M<4>(L, spec, err);
-        case 8: return launch_k4p_M<8>(L, spec, err);
-        case 12: return launch_k4p_M<12>(L, spec, err);
-        case 16: return launch_k4p_M<16>(L, spec, err);
-        case 24: return launch_k4p_M<24>(L, spec, err);
-        case 32: return launch_k4p_M<32>(L, spec, err);
-      }
-      return cudaErrorInvalidValue;
+  if (L.k4_var == 1) {  // the persistent prefetching form (the autotuner's pick)
+    switch (L.M) {
+      case 1: return launch_k4p_M<1, TS>(L, spec, err);
+      case 2: return launch_k4p_M<2, TS>(L, spec, err);
+      case 4: return launch_k4p_M<4, TS>(L, spec, err);
+      case 8: return launch_k4p_M<8, TS>(L, spec, err);
+      case 12: return launch_k4p_M<12, TS>(L, spec, err);
+      case 16: return launch_k4p_M<16, TS>(L, spec, err);
+      case 24: return launch_k4p_M<24, TS>(L, spec, err);
+      case 32: return launch_k4p_M<32, TS>(L, spec, err);
     }
+    return cudaErrorInvalidValue;
   }
   switch (L.M) {
     case 1: return launch_k4_M<1, TS>(L, spec, err);

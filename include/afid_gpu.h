@@ -178,7 +178,7 @@ typedef struct afid_tune_info {
                                    per SM with the tables in shared memory                     */
   double us[AFID_TUNE_MAX];     /* mean time per sample launch in microseconds (-1: not run) */
   int k4_chosen;                /* Poisson tridiagonal: 0 one mode per warp, 1 persistent warps
-                                   with the next mode's right-hand side prefetched (FP64 only)  */
+                                   with the next mode's right-hand side prefetched              */
   double k4_us[2];              /* microseconds per full launch of each form (-1: not run)   */
   int fftz_chosen;              /* z transforms: 0 one tile per block, 1 persistent blocks with
                                    the next tile's copies in flight (3-D single domains)         */
@@ -188,8 +188,8 @@ int afid_gpu_autotune(afid_ctx_t *ctx, int force, afid_tune_info_t *info);
 /* Use shape `index` (0 .. ncand-1) from now on without timing, e.g. one saved from an earlier
  * afid_gpu_autotune on the same device and sizes. */
 int afid_gpu_set_k1_shape(afid_ctx_t *ctx, int index);
-/* Use Poisson-tridiagonal form `form` (0 or 1 as in afid_tune_info_t.k4_chosen; 1 needs FP64
- * spectra) from now on; both forms give bitwise the same results. */
+/* Use Poisson-tridiagonal form `form` (0 or 1 as in afid_tune_info_t.k4_chosen) from now on;
+ * both forms give bitwise the same results. */
 int afid_gpu_set_k4_form(afid_ctx_t *ctx, int form);
 /* Use z-transform form `form` (0 or 1 as in afid_tune_info_t.fftz_chosen); bitwise the same. */
 int afid_gpu_set_fftz_form(afid_ctx_t *ctx, int form);

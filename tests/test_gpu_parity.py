@@ -205,13 +205,16 @@ def test_launch_count_positive():
         assert gpu.launch_count() - n0 == 1 + 3 * 7
 
 
-@pytest.mark.parametrize("shape", [(256, 24, 16), (100, 16, 8), (60, 16, 1), (500, 16, 4), (64, 32, 96)])
-def test_k4_and_fftz_forms_bitwise_identical(shape):
+@pytest.mark.parametrize("shape,precision", [((256, 24, 16), ag.PREC_FP64), ((100, 16, 8), ag.PREC_FP64),
+                                             ((60, 16, 1), ag.PREC_FP64), ((500, 16, 4), ag.PREC_FP64),
+                                             ((64, 32, 96), ag.PREC_FP64), ((100, 16, 8), ag.PREC_MIXED),
+                                             ((64, 32, 96), ag.PREC_MIXED)])
+def test_k4_and_fftz_forms_bitwise_identical(shape, precision):
     """Both forms of the Poisson tridiagonal (a mode per warp; persistent warps with the next
     mode prefetched) and of the z transforms (a tile per block; persistent blocks with the next
     tile prefetched) give the same fields bit for bit, so the autotuner's choices change the
     schedule only."""
-    case = Case(*shape, rayt=1e6, dt=2e-3)
+    case = Case(*shape, precision=precision, rayt=1e6, dt=2e-3)
     s = case.oracle_state(random_velocity=0.1)
     outs = []
     for form in (0, 1):
