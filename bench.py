@@ -201,6 +201,10 @@ def run_gpu(args):
     solver.set_stream(stream.cuda_stream)
     if args.k1_shape >= 0:  # a saved autotuner pick (profiling runs use the bench's pick)
         solver.set_k1_shape(args.k1_shape)
+        if args.k4_form >= 0:
+            solver.set_k4_form(args.k4_form)
+        if args.fftz_form >= 0:
+            solver.set_fftz_form(args.fftz_form)
     temp0 = tables.initial_temperature(20261203)
     nx, nym, nzm = w["nxm"] + 1, w["nym"], w["nzm"]
     zeros = np.zeros((nzm, nym, nx))
@@ -1209,6 +1213,8 @@ def main():
     ap.add_argument("--accuracy-steps", type=int, default=500,
                     help="rbc3d_mixed: steps of the mixed run compared with the FP64 replay (500 = the full run)")
     ap.add_argument("--k1-shape", type=int, default=-1, help="fixed K1 thread shape instead of autotuning")
+    ap.add_argument("--k4-form", type=int, default=-1, help="with --k1-shape: fixed Poisson tridiagonal form")
+    ap.add_argument("--fftz-form", type=int, default=-1, help="with --k1-shape: fixed z-transform form")
     ap.add_argument("--jobs", type=int, default=100, help="served: number of jobs")
     ap.add_argument("--rate", type=float, default=50.0,
                     help="served: Poisson arrival rate per second (50 = the benchmark's stream, ~16x capacity; "
