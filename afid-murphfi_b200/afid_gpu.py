@@ -173,7 +173,7 @@ EXPORTS = [
     "afid_batch_device_bytes", "afid_batch_launch_count",
     "afid_serve_create", "afid_serve_destroy", "afid_serve_submit", "afid_serve_pump", "afid_serve_poll",
     "afid_serve_cancel",
-    "afid_serve_status", "afid_serve_now", "afid_gpu_autotune", "afid_batch_autotune",
+    "afid_serve_status", "afid_serve_now", "afid_gpu_autotune", "afid_batch_autotune", "afid_batch_set_k1_shape",
     "afid_gpu_set_k1_shape", "afid_gpu_set_k4_form", "afid_gpu_set_fftz_form", "afid_gpu_set_wait_test", "afid_gpu_mean_profiles", "afid_batch_mean_profiles",
     "afid_batch_divmax", "afid_gpu_spectra_reset", "afid_gpu_spectra_update", "afid_gpu_spectra_read", "afid_gpu_slice",
     "afid_mgrd_create", "afid_mgrd_destroy", "afid_mgrd_view", "afid_mgrd_fast", "afid_mgrd_array",
@@ -272,6 +272,7 @@ def load_library(path: str = _LIB_PATH) -> C.CDLL:
         "afid_batch_mean_profiles": (i, [vp, i, _dp]),
         "afid_batch_divmax": (i, [vp, _dp]),
         "afid_batch_autotune": (i, [vp, i, C.POINTER(TuneInfoT)]),
+        "afid_batch_set_k1_shape": (i, [vp, i]),
         "afid_batch_step": (i, [vp, i]),
         "afid_batch_synchronize": (i, [vp]),
         "afid_batch_stats": (i, [vp, C.POINTER(BatchStatT), _dp, _dp]),
@@ -766,6 +767,10 @@ class Batch:
         info = TuneInfoT()
         _check(lib().afid_batch_autotune(self._h, int(force), C.byref(info)), "afid_batch_autotune")
         return info.as_dict()
+
+    def set_k1_shape(self, index: int) -> None:
+        """Use K1 shape `index` (as Solver.set_k1_shape) for this batch from now on."""
+        _check(lib().afid_batch_set_k1_shape(self._h, index), "afid_batch_set_k1_shape")
 
     def launch_count(self) -> int:
         return int(lib().afid_batch_launch_count(self._h))

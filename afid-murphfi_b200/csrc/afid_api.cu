@@ -586,6 +586,7 @@ int ctx_autotune(afid_ctx_t *ctx, bool force) {
     for (int round = 0; round < 2 && e == cudaSuccess; ++round) {
       for (int v = 0; v < n && e == cudaSuccess; ++v) {
         auto run = [&] { return L.mixed ? launch_k1_mixed(L, b, 0, v, sample) : launch_k1_fp64(L, b, 0, v, sample); };
+        if (!k1_shape_usable(L.M, v, L.g.batch != 0, L.g.nzm == 1 || L.g.batch)) continue;
         if (run() != cudaSuccess) {  // this shape does not fit the device: skip it
           cudaGetLastError();
           continue;
@@ -926,6 +927,8 @@ int afid_gpu_set_k1_shape(afid_ctx_t *ctx, int index) {
   int tpc[AFID_TUNE_MAX], rpt[AFID_TUNE_MAX], cap[AFID_TUNE_MAX], pol[AFID_TUNE_MAX];
   const int n = k1_shapes(ctx->L.M, tpc, rpt, cap, pol);
   if (index < 0 || index >= n) return AFID_E_INVALID;
+  const bool two_d = ctx->L.g.nzm == 1 || ctx->L.g.batch;
+  if (!k1_shape_usable(ctx->L.M, index, ctx->L.g.batch != 0, two_d)) return AFID_E_INVALID;
   afid_tune_info_t info{};
   info.ncand = n;
   info.chosen = index;

@@ -690,4 +690,13 @@ int afid_batch_autotune(afid_batch_t *b, int force, afid_tune_info_t *info) {
   return s;
 }
 
+int afid_batch_set_k1_shape(afid_batch_t *b, int index) {
+  if (!b) return AFID_E_INVALID;
+  cudaSetDevice(b->ctx->dev);
+  if (cudaStreamSynchronize(b->ctx->stream) != cudaSuccess) return AFID_E_CUDA;
+  const int s = afid_gpu_set_k1_shape(b->ctx, index);
+  if (s == AFID_OK) drop_graphs(b);  // the captured step holds the old shape
+  return s;
+}
+
 }  // extern "C"

@@ -70,6 +70,9 @@ cudaError_t launch_k1_fp64_sal(const LaunchCtx &L, const SubstepBuffers &b, int 
 cudaError_t launch_k1_mixed_sal(const LaunchCtx &L, const SubstepBuffers &b, int ns, int var, int ncol);
 // Thread shapes of K1 for M: fills tpc[]/rpt[]/cap[]/pol[] (up to AFID_TUNE_MAX) and returns their number.
 int k1_shapes(int M, int *tpc, int *rpt, int *cap, int *pol);
+// Whether K1 shape v of this M can run on a context (the forms that keep one substep's CN
+// factors per block do not take a batch, whose factors differ per instance).
+bool k1_shape_usable(int M, int v, bool batch, bool two_d);
 // The kernels of one substep, in launch order (K1 .. K7).
 enum class Stage { ExplicitImplicit = 0, DivFftY, FftZFwd, Tridiag, FftZInv, IfftY, Correct };
 constexpr int kNumStages = 7;

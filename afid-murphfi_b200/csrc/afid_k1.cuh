@@ -186,16 +186,39 @@ template <typename TE> __device__ __forceinline__ TE cv(double v) { return (TE)v
 // In 2-D (TWO_D: the z neighbours are the cell itself) every z-difference term is zero by
 // construction; those terms are left out instead of being evaluated to zero.
 
+// The per-row table operands of the four explicit terms (they depend on the row k only), loaded
+// together from global or shared memory before the terms that use them.
+struct RowTab {
+  double idxm, idxc, udx3c, udx3m, ap3ck, ac3ck, am3ck, ap3sk, ac3sk, am3sk, ap3ssk, ac3ssk, am3ssk;
+};
+template <int H> __device__ __forceinline__ RowTab row_tab(const Tables &t, int k) {
+  RowTab r;
+  r.idxm = (k >= 1) ? tld<H>(t.idx + k - 1) : 0.0;  // read by the vx terms only, k >= 1
+  r.idxc = tld<H>(t.idx + k);
+  r.udx3c = tld<H>(t.udx3c + k);
+  r.udx3m = tld<H>(t.udx3m + k);
+  r.ap3ck = tld<H>(t.ap3ck + k);
+  r.ac3ck = tld<H>(t.ac3ck + k);
+  r.am3ck = tld<H>(t.am3ck + k);
+  r.ap3sk = tld<H>(t.ap3sk + k);
+  r.ac3sk = tld<H>(t.ac3sk + k);
+  r.am3sk = tld<H>(t.am3sk + k);
+  r.ap3ssk = tld<H>(t.ap3ssk + k);
+  r.ac3ssk = tld<H>(t.ac3ssk + k);
+  r.am3ssk = tld<H>(t.am3ssk + k);
+  return r;
+}
+
 // ExplicitTermsVX.F90:30-127 + ImplicitAndUpdateVX.F90:39-66, k = 1..nxm-1 (0-based)
 template <typename TE, bool TWO_D, bool SAL, int H = 0>
-__device__ __forceinline__ double rhs_vx(const Geom &g, const Tables &t, const StepCoef &sc, int k,
+__device__ __forceinline__ double rhs_vx(const Geom &g, const RowTab &r, const StepCoef &sc, int k,
                                          const ColV &X, const ColV &Y, const ColV &Z, const ColV &T,
                                          const ColV &P, double ru, TE &qout, double sb) {
   const int km = k - 1, kp = k + 1;
   const TE udy = (TE)(g.dy * 0.25), udz = (TE)(g.dz * 0.25);
   const TE udyq = (TE)g.udyq_re, udzq = (TE)g.udzq_re;
-  const TE idxm = cv<TE>(tld<H>(t.idx + km)), idxc = cv<TE>(tld<H>(t.idx + k));
-  const TE udx3c = cv<TE>(tld<H>(t.udx3c + k));
+  const TE idxm = cv<TE>(r.idxm), idxc = cv<TE>(r.idxc);
+  const TE udx3c = cv<TE>(r.udx3c);
   const TE vxc = cv<TE>(X.c[k]);
   const TE vxkp = cv<TE>(X.c[kp]), vxkm = cv<TE>(X.c[km]);
   const TE vxip = cv<TE>(X.ip[k]), vxim = cv<TE>(X.im[k]);
@@ -219,8 +242,8 @@ __device__ __forceinline__ double rhs_vx(const Geom &g, const Tables &t, const S
     if constexpr (SAL) qcap = qcap - (TE)sb;  // AddSalBuoyancy(qcap)
   }
   const double alre = sc.alre;
-  const double udx3 = sc.al * tld<H>(t.udx3c + k);
-  const double dxxvx = X.c[kp] * tld<H>(t.ap3ck + k) + X.c[k] * tld<H>(t.ac3ck + k) + X.c[km] * tld<H>(t.am3ck + k);
+  const double udx3 = sc.al * r.udx3c;
+  const double dxxvx = X.c[kp] * r.ap3ck + X.c[k] * r.ac3ck + X.c[km] * r.am3ck;
   const double dxp = (P.c[k] - P.c[km]) * udx3;
   qout = qcap;
   return (sc.ga * (double)qcap + sc.ro * ru + alre * dxxvx - dxp) * sc.dt;
@@ -228,7 +251,7 @@ __device__ __forceinline__ double rhs_vx(const Geom &g, const Tables &t, const S
 
 // ExplicitTermsVY.F90:23-122 + ImplicitAndUpdateVY.F90:28-80, k = 0..nxm-1
 template <typename TE, bool TWO_D, bool SAL, int H = 0>
-__device__ __forceinline__ double rhs_vy(const Geom &g, const Tables &t, const StepCoef &sc, int k,
+__device__ __forceinline__ double rhs_vy(const Geom &g, const RowTab &r, const StepCoef &sc, int k,
                                          const ColV &X, const ColV &Y, const ColV &Z, const ColV &T,
                                          const ColV &P, double zd, double pjm, double ru, TE &qout,
                                          double sb) {
@@ -242,7 +265,7 @@ __device__ __forceinline__ double rhs_vy(const Geom &g, const Tables &t, const S
   const TE vyip = cv<TE>(Y.ip[k]), vyim = cv<TE>(Y.im[k]);
   const TE hyx = ((cv<TE>(X.c[kp]) + cv<TE>(X.jm[kp])) * (cv<TE>(Y.c[kpp]) + c) -
                   (cv<TE>(X.c[k]) + cv<TE>(X.jm[k])) * (c + cv<TE>(Y.c[kmm]))) *
-                 cv<TE>(tld<H>(t.udx3m + k)) * (TE)0.25;
+                 cv<TE>(r.udx3m) * (TE)0.25;
   const TE hyy = ((vyjp + c) * (vyjp + c) - (vyjm + c) * (vyjm + c)) * udy;
   const TE dyyvy = (vyjp - (TE)2.0 * c + vyjm) * udyq;
   TE dph;
@@ -261,7 +284,7 @@ __device__ __forceinline__ double rhs_vy(const Geom &g, const Tables &t, const S
   }
   const double alre = sc.alre;
   const double udyp = g.dy * sc.al;
-  const double amm = tld<H>(t.am3sk + k), acc = tld<H>(t.ac3sk + k), app = tld<H>(t.ap3sk + k);
+  const double amm = r.am3sk, acc = r.ac3sk, app = r.ap3sk;
   const double cd = Y.c[k];
   double dxxvy;
   if (k == 0)
@@ -277,7 +300,7 @@ __device__ __forceinline__ double rhs_vy(const Geom &g, const Tables &t, const S
 
 // ExplicitTermsVZ.F90:23-118 + ImplicitAndUpdateVZ.F90:38-69, k = 0..nxm-1
 template <typename TE, bool TWO_D, bool SAL, int H = 0>
-__device__ __forceinline__ double rhs_vz(const Geom &g, const Tables &t, const StepCoef &sc, int k,
+__device__ __forceinline__ double rhs_vz(const Geom &g, const RowTab &r, const StepCoef &sc, int k,
                                          const ColV &X, const ColV &Y, const ColV &Z, const ColV &T,
                                          const ColV &P, double yd, double pim, double ru, TE &qout,
                                          double sb) {
@@ -293,7 +316,7 @@ __device__ __forceinline__ double rhs_vz(const Geom &g, const Tables &t, const S
                  udy;
   const TE hzx = ((cv<TE>(X.c[kp]) + cv<TE>(X.im[kp])) * (cv<TE>(Z.c[kpp]) + c) -
                   (cv<TE>(X.c[k]) + cv<TE>(X.im[k])) * (c + cv<TE>(Z.c[kmm]))) *
-                 cv<TE>(tld<H>(t.udx3m + k)) * (TE)0.25;
+                 cv<TE>(r.udx3m) * (TE)0.25;
   const TE dyyvz = (vzjp - (TE)2.0 * c + vzjm) * udyq;
   TE dq;
   if constexpr (TWO_D) {
@@ -309,7 +332,7 @@ __device__ __forceinline__ double rhs_vz(const Geom &g, const Tables &t, const S
     if constexpr (SAL) dq = dq - (TE)sb;  // AddSalBuoyancy(dq)
   }
   const double alre = sc.alre;
-  const double amm = tld<H>(t.am3sk + k), acc = tld<H>(t.ac3sk + k), app = tld<H>(t.ap3sk + k);
+  const double amm = r.am3sk, acc = r.ac3sk, app = r.ap3sk;
   const double dxxvz = Z.c[kpp] * app + Z.c[k] * acc + Z.c[kmm] * amm;
   qout = dq;
   if constexpr (TWO_D) {
@@ -322,13 +345,13 @@ __device__ __forceinline__ double rhs_vz(const Geom &g, const Tables &t, const S
 
 // ExplicitTermsTemp.F90:22-77 + ImplicitAndUpdateTemp.F90:33-66, k = 0..nxm-1
 template <typename TE, bool TWO_D, int H = 0>
-__device__ __forceinline__ double rhs_temp(const Geom &g, const Tables &t, const StepCoef &sc, int k,
+__device__ __forceinline__ double rhs_temp(const Geom &g, const RowTab &r, const StepCoef &sc, int k,
                                            const ColV &X, const ColV &Y, const ColV &Z, const ColV &T,
                                            double tbp, double ttp, double ru, TE &qout) {
   const TE udz = (TE)(g.dz * 0.5), udy = (TE)(g.dy * 0.5);
   const TE udzq = (TE)g.udzq_pe, udyq = (TE)g.udyq_pe;
   const TE tc = cv<TE>(T.c[k]);
-  const TE ux = cv<TE>(tld<H>(t.udx3m + k));
+  const TE ux = cv<TE>(r.udx3m);
   TE htx;
   if (k == 0)
     htx = (cv<TE>(X.c[1]) * (cv<TE>(T.c[1]) + tc) - cv<TE>(X.c[0]) * (TE)2.0 * (TE)tbp) * (TE)0.5 * ux;
@@ -353,12 +376,11 @@ __device__ __forceinline__ double rhs_temp(const Geom &g, const Tables &t, const
   const double tcd = T.c[k];
   double dxxt;
   if (k == 0)
-    dxxt = T.c[1] * tld<H>(t.ap3ssk) + tcd * tld<H>(t.ac3ssk) - (tld<H>(t.ap3ssk) + tld<H>(t.ac3ssk)) * tbp * g.tfixs;
+    dxxt = T.c[1] * r.ap3ssk + tcd * r.ac3ssk - (r.ap3ssk + r.ac3ssk) * tbp * g.tfixs;
   else if (k == g.nxm - 1)
-    dxxt = tcd * tld<H>(t.ac3ssk + k) + T.c[k - 1] * tld<H>(t.am3ssk + k) -
-           (tld<H>(t.am3ssk + k) + tld<H>(t.ac3ssk + k)) * ttp * g.tfixn;
+    dxxt = tcd * r.ac3ssk + T.c[k - 1] * r.am3ssk - (r.am3ssk + r.ac3ssk) * ttp * g.tfixn;
   else
-    dxxt = T.c[k + 1] * tld<H>(t.ap3ssk + k) + tcd * tld<H>(t.ac3ssk + k) + T.c[k - 1] * tld<H>(t.am3ssk + k);
+    dxxt = T.c[k + 1] * r.ap3ssk + tcd * r.ac3ssk + T.c[k - 1] * r.am3ssk;
   qout = hro;
   return (sc.ga * (double)hro + sc.ro * ru + alpec * dxxt) * sc.dt;
 }
@@ -528,6 +550,7 @@ __global__ void __launch_bounds__(TPC, k1_min_blocks<CAP, TPC>())
     const int k = ADJ ? RPT * tc + p : tc + TPC * p;
     if (k < nxm) {
       TE q0 = (TE)0, q1, q2, q3;
+      const RowTab rt = row_tab<H>(t, k);
       const double u0 = uu[p][0], u1 = uu[p][1], u2 = uu[p][2], u3 = uu[p][3];
       // 2-D: vz(j-1,i+1) = vz(j-1), vy(j+1,i-1) = vy(j+1), pr(i-1) = pr
       const double zd = TWO_D ? Z.jm[k] : vv[p][0];
@@ -537,10 +560,10 @@ __global__ void __launch_bounds__(TPC, k1_min_blocks<CAP, TPC>())
       double sb = 0.0;
       if constexpr (SAL) sb = sbv[p];
       // all four right-hand sides from the staged columns before anything is stored
-      rr[p][0] = (k >= 1) ? rhs_vx<TE, TWO_D, SAL, H>(g, t, sc, k, X, Y, Z, T, P, u0, q0, sb) * tld<H>(TX + k - 1) : 0.0;
-      rr[p][1] = rhs_vy<TE, TWO_D, SAL, H>(g, t, sc, k, X, Y, Z, T, P, zd, vv[p][2], u1, q1, sb) * tld<H>(TY + k);
-      rr[p][2] = rhs_vz<TE, TWO_D, SAL, H>(g, t, sc, k, X, Y, Z, T, P, yd, pim, u2, q2, sb) * tld<H>(TY + k);
-      rr[p][3] = rhs_temp<TE, TWO_D, H>(g, t, sc, k, X, Y, Z, T, tbp, ttp, u3, q3) * tld<H>(TT + k);
+      rr[p][0] = (k >= 1) ? rhs_vx<TE, TWO_D, SAL, H>(g, rt, sc, k, X, Y, Z, T, P, u0, q0, sb) * tld<H>(TX + k - 1) : 0.0;
+      rr[p][1] = rhs_vy<TE, TWO_D, SAL, H>(g, rt, sc, k, X, Y, Z, T, P, zd, vv[p][2], u1, q1, sb) * tld<H>(TY + k);
+      rr[p][2] = rhs_vz<TE, TWO_D, SAL, H>(g, rt, sc, k, X, Y, Z, T, P, yd, pim, u2, q2, sb) * tld<H>(TY + k);
+      rr[p][3] = rhs_temp<TE, TWO_D, H>(g, rt, sc, k, X, Y, Z, T, tbp, ttp, u3, q3) * tld<H>(TT + k);
       if (k >= 1) rux[c0 + k] = q0;
       ruy[c0 + k] = q1;
       ruz[c0 + k] = q2;
@@ -746,6 +769,7 @@ __global__ void __launch_bounds__(TPC, k1_min_blocks<CAP, TPC>())
       const int k = tc + TPC * p;
       if (k < nxm) {
         TE q0 = (TE)0, q1, q2, q3;
+        const RowTab rt = row_tab<H>(t, k);
         // vz(j-1, i+1), vy(j+1, i-1), pr(j-1), pr(i-1) of column c
         double zd, yd, pjm, pim;
         if constexpr (TWO_D) {
@@ -760,14 +784,14 @@ __global__ void __launch_bounds__(TPC, k1_min_blocks<CAP, TPC>())
         pjm = c == 0 ? sv[p][0] : C(PRC)[k];
         double sb = 0.0;
         if constexpr (SAL) sb = sbv[p][c];
-        rr[p][c][0] = (k >= 1) ? rhs_vx<TE, TWO_D, SAL, H>(g, t, sc, k, X, Y, Z, T, P, uu[p][c][0], q0, sb) *
+        rr[p][c][0] = (k >= 1) ? rhs_vx<TE, TWO_D, SAL, H>(g, rt, sc, k, X, Y, Z, T, P, uu[p][c][0], q0, sb) *
                                      tld<H>(TX + k - 1)
                                : 0.0;
-        rr[p][c][1] = rhs_vy<TE, TWO_D, SAL, H>(g, t, sc, k, X, Y, Z, T, P, zd, pjm, uu[p][c][1], q1, sb) *
+        rr[p][c][1] = rhs_vy<TE, TWO_D, SAL, H>(g, rt, sc, k, X, Y, Z, T, P, zd, pjm, uu[p][c][1], q1, sb) *
                       tld<H>(TY + k);
-        rr[p][c][2] = rhs_vz<TE, TWO_D, SAL, H>(g, t, sc, k, X, Y, Z, T, P, yd, pim, uu[p][c][2], q2, sb) *
+        rr[p][c][2] = rhs_vz<TE, TWO_D, SAL, H>(g, rt, sc, k, X, Y, Z, T, P, yd, pim, uu[p][c][2], q2, sb) *
                       tld<H>(TY + k);
-        rr[p][c][3] = rhs_temp<TE, TWO_D, H>(g, t, sc, k, X, Y, Z, T, tbp, ttp, uu[p][c][3], q3) * tld<H>(TT + k);
+        rr[p][c][3] = rhs_temp<TE, TWO_D, H>(g, rt, sc, k, X, Y, Z, T, tbp, ttp, uu[p][c][3], q3) * tld<H>(TT + k);
         if (k >= 1) rux[oc[c] + k] = q0;
         ruy[oc[c] + k] = q1;
         ruz[oc[c] + k] = q2;
@@ -1048,15 +1072,16 @@ __global__ void __launch_bounds__(TPC * G, 1)
       const int k = tc + TPC * p;
       if (k < nxm) {
         TE q0 = (TE)0, q1, q2, q3;
+        const RowTab rt = row_tab<2>(ts, k);
         const double zd = TWO_D ? Z.jm[k] : vv[p][0];
         const double yd = TWO_D ? Y.jp[k] : vv[p][1];
         const double pim = TWO_D ? P.c[k] : vv[p][3];
         double sb = 0.0;
         if constexpr (SAL) sb = sbv[p];
-        rr[p][0] = (k >= 1) ? rhs_vx<TE, TWO_D, SAL, 2>(g, ts, sc, k, X, Y, Z, T, P, uu[p][0], q0, sb) * TX[k - 1] : 0.0;
-        rr[p][1] = rhs_vy<TE, TWO_D, SAL, 2>(g, ts, sc, k, X, Y, Z, T, P, zd, vv[p][2], uu[p][1], q1, sb) * TY[k];
-        rr[p][2] = rhs_vz<TE, TWO_D, SAL, 2>(g, ts, sc, k, X, Y, Z, T, P, yd, pim, uu[p][2], q2, sb) * TY[k];
-        rr[p][3] = rhs_temp<TE, TWO_D, 2>(g, ts, sc, k, X, Y, Z, T, tbp, ttp, uu[p][3], q3) * TT[k];
+        rr[p][0] = (k >= 1) ? rhs_vx<TE, TWO_D, SAL, 2>(g, rt, sc, k, X, Y, Z, T, P, uu[p][0], q0, sb) * TX[k - 1] : 0.0;
+        rr[p][1] = rhs_vy<TE, TWO_D, SAL, 2>(g, rt, sc, k, X, Y, Z, T, P, zd, vv[p][2], uu[p][1], q1, sb) * TY[k];
+        rr[p][2] = rhs_vz<TE, TWO_D, SAL, 2>(g, rt, sc, k, X, Y, Z, T, P, yd, pim, uu[p][2], q2, sb) * TY[k];
+        rr[p][3] = rhs_temp<TE, TWO_D, 2>(g, rt, sc, k, X, Y, Z, T, tbp, ttp, uu[p][3], q3) * TT[k];
         if (k >= 1) rux[c0 + k] = q0;
         ruy[c0 + k] = q1;
         ruz[c0 + k] = q2;

@@ -24,4 +24,13 @@ int k1_shapes(int M, int *tpc, int *rpt, int *cap, int *pol) {
   return kK1ShapeCount[mi];
 }
 
+bool k1_shape_usable(int M, int v, bool batch, bool two_d) {
+  const int mi = k1_m_index(M);
+  if (v < 0 || v >= kK1ShapeCount[mi]) return false;
+  const K1Shape &s = kK1Shapes[mi][v];
+  if (batch && s.ny == 0) return false;
+  if (s.ny == 0 && k1p_groups(M, two_d) < 2) return false;
+  return true;
+}
+
 }  // namespace afid

@@ -74,6 +74,9 @@ long long afid_batch_launch_count(const afid_batch_t *b);
 /* The autotuner of include/afid_gpu.h on this batch's stacked domain (runs by itself before the
  * first captured step). */
 int afid_batch_autotune(afid_batch_t *b, int force, afid_tune_info_t *info);
+/* Use K1 shape `index` for this batch from now on, as afid_gpu_set_k1_shape (bitwise the same
+ * results for every shape). */
+int afid_batch_set_k1_shape(afid_batch_t *b, int index);
 /* dmax[nslots]: max |div u| of every slot's resident state (CheckDivergence.F90), for the check
  * main.F90:346-358 makes every tout (errorcode 169 above RESID).  The cfl scratch of the step
  * control is reused: not while a step is in flight on the batch stream (it is stream-ordered). */

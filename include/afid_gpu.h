@@ -186,7 +186,8 @@ typedef struct afid_tune_info {
 } afid_tune_info_t;
 int afid_gpu_autotune(afid_ctx_t *ctx, int force, afid_tune_info_t *info);
 /* Use shape `index` (0 .. ncand-1) from now on without timing, e.g. one saved from an earlier
- * afid_gpu_autotune on the same device and sizes. */
+ * afid_gpu_autotune on the same device and sizes.  AFID_E_INVALID for a shape this context
+ * cannot run (those the autotuner reports with us = -1 for that reason). */
 int afid_gpu_set_k1_shape(afid_ctx_t *ctx, int index);
 /* Use Poisson-tridiagonal form `form` (0 or 1 as in afid_tune_info_t.k4_chosen) from now on;
  * both forms give bitwise the same results. */

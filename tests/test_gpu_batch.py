@@ -266,3 +266,60 @@ def test_divergence_check_per_slot():
         b.upload(2, f["vx"], f["vy"], f["vz"], f["temp"], f["pr"])
         d2 = b.divmax()
     assert d2[2] > 1.0 and np.all(np.delete(d2, 2) < 1e-9)
+
+
+@pytest.mark.parametrize("precision", [ag.PREC_FP64, ag.PREC_MIXED])
+def test_k1_shapes_bitwise_identical_in_batch(precision):
+    """Every K1 shape a batch of the 129..256 wall-normal class can take (one or two columns per
+    block, cache hints, adjacent rows) steps a batch with an idle slot to the same fields bit for
+    bit, and the idle slot keeps its state; the persistent form, which holds one substep's CN
+    factors per block, is refused for a batch with AFID_E_INVALID."""
+    nxm, nym, nslots, idle = 200, 32, 4, 1
+
+    def inp(**kw):
+        v = dict(STEP)
+        v.update(kw)
+        return ag.parse_bou_in(bou_text(nxm, nym, 1, **v))
+
+    def make():
+        b = ag.Batch(inp(**SLOTS[0]), nslots, precision)
+        for s in range(nslots):
+            b.configure(s, inp(**SLOTS[s]))
+            b.seed(s, 100 + s)
+            rng = np.random.default_rng(s)
+            f = b.download(s)
+            for k in ("vx", "vy"):
+                f[k][...] = 0.05 * rng.standard_normal(f[k].shape)
+            f["vx"][:, 0] = 0.0
+            f["vx"][:, nxm] = 0.0
+            f["vy"][:, nxm] = 0.0
+            b.upload(s, f["vx"], f["vy"], f["vz"], f["temp"], f["pr"])
+        return b
+
+    with make() as b:
+        info = b.autotune()
+        before = b.download(idle)
+        # the forms that hold one substep's CN factors per block cannot take a batch
+        usable = [v for v, (*_, us) in enumerate(info["shapes"]) if us > 0]
+        for v in set(range(info["ncand"])) - set(usable):
+            with pytest.raises(ag.AfidError) as e:
+                b.set_k1_shape(v)
+            assert e.value.status == ag.AFID_E_INVALID
+    assert len(usable) >= 2
+    outs = []
+    for v in usable:
+        with make() as b:
+            b.set_k1_shape(v)
+            act = np.ones(nslots, np.uint8)
+            act[idle] = 0
+            b.set_active(act)
+            b.step(5)
+            st = b.stats()
+            outs.append([b.download(s) for s in range(nslots)])
+        assert all(st["ntime"][s] == (0 if s == idle else 5) for s in range(nslots)), v
+        assert all(st["errorcode"][s] == 0 for s in range(nslots)), v
+    for v, o in zip(usable, outs):
+        for k in ag.Batch.FIELDS:
+            assert np.array_equal(o[idle][k], before[k]), (v, k)
+            for s in range(nslots):
+                assert np.array_equal(o[s][k], outs[0][s][k]), (v, s, k)

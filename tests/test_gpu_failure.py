@@ -47,6 +47,31 @@ def test_bounded_wait_runs_out_with_timeout_status():
     assert rel_l2(out["temp"][..., :case.p.nxm], s.temp[..., :case.p.nxm]) < 1e-10
 
 
+def test_bounded_wait_runs_out_in_every_k1_form():
+    """The same bounded wait in every K1 form of the 129..256 wall-normal class (one column per
+    block, two columns per block, the persistent form): each reports AFID_E_TIMEOUT at the next
+    synchronising call and leaves no copy in flight (the device steps on in a new context)."""
+    case = Case(200, 16, 8, rayt=1e6, dt=1e-3)
+    s = case.oracle_state(random_velocity=0.1)
+    with case.solver() as gpu:
+        ncand = gpu.autotune()["ncand"]
+    for v in range(ncand):
+        with case.solver() as gpu:
+            gpu.set_k1_shape(v)
+            gpu.upload(s.vx, s.vy, s.vz, s.temp, s.pr)
+            gpu.set_wait_test(4096)
+            with pytest.raises(ag.AfidError) as e:
+                gpu.time_marcher(1e-3, 0)
+                gpu.synchronize()
+            assert e.value.status == ag.AFID_E_TIMEOUT, v
+    with case.solver() as gpu:
+        gpu.upload(s.vx, s.vy, s.vz, s.temp, s.pr)
+        gpu.time_marcher(1e-3, 0)
+        out = gpu.download()
+    o.time_marcher(case.g, s, 1e-3)
+    assert rel_l2(out["vx"], s.vx) < 1e-10
+
+
 def test_wait_test_hook_rejects_out_of_range():
     case = Case(16, 8, 4)
     with case.solver() as gpu:

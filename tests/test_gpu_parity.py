@@ -284,7 +284,8 @@ def test_wall_normal_size_beyond_solver_is_rejected():
 
 @pytest.mark.parametrize("shape,precision", [((100, 16, 8), ag.PREC_FP64), ((384, 8, 4), ag.PREC_MIXED),
                                              ((500, 16, 1), ag.PREC_FP64), ((700, 8, 1), ag.PREC_FP64),
-                                             ((256, 16, 8), ag.PREC_FP64), ((60, 16, 8), ag.PREC_FP64)])
+                                             ((256, 16, 8), ag.PREC_FP64), ((60, 16, 8), ag.PREC_FP64),
+                                             ((256, 24, 1), ag.PREC_FP64), ((200, 16, 8), ag.PREC_MIXED)])
 def test_k1_shapes_bitwise_identical(shape, precision):
     """Every launch shape the autotuner may pick (threads, rows per thread, register cap, cache
     policy, one or two columns per block, the persistent form with shared-memory tables) gives

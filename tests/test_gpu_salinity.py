@@ -114,6 +114,27 @@ def test_steps_match_oracle(coarse, refined, kw):
         assert rel_l2(sal, sa.initial_salinity(c.m, c.g, 3)) > 1e-8
 
 
+def test_k1_shapes_bitwise_identical_with_salinity():
+    """The salinity-coupled K1 (buoyancy from the coarse salinity) gives the same fields and
+    salinity bit for bit on every launch shape of its wall-normal class, the two-column and
+    persistent forms among them."""
+    c = SalCase((150, 16, 8), (300, 32, 16))
+    with c.solver() as sv:
+        ncand = sv.autotune()["ncand"]
+    assert ncand >= 2
+    outs = []
+    for v in range(ncand):
+        with c.solver() as sv:
+            sv.set_k1_shape(v)
+            for n in range(2):
+                sv.time_marcher(1e-3, n)
+            outs.append((sv.download(), sv.sal_download()))
+    for got, sal in outs[1:]:
+        for f in FIELDS:
+            assert np.array_equal(got[f], outs[0][0][f]), f
+        assert np.array_equal(sal, outs[0][1])
+
+
 def test_cfl_and_profiles_match_oracle():
     c = SalCase((16, 16, 8), (32, 32, 16))
     with c.solver() as sv:
