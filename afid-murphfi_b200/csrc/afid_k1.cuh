@@ -519,6 +519,26 @@ __global__ void __launch_bounds__(TPC, k1_min_blocks<CAP, TPC>())
     vv[p][2] = in ? nld<H>(pr + o_jm + k) : 0.0;
     if constexpr (SAL) sbv[p] = in ? g.bycs * nld<H>(g.salc + c0 + k) : 0.0;
   }
+  const int slot = sc_slot(g, i, ns);
+  const size_t tsz = cn_table_size(M);
+  const double *TX = cn_tab + (size_t)(slot * 3 + 0) * tsz;
+  const double *TY = cn_tab + (size_t)(slot * 3 + 1) * tsz;
+  const double *TT = cn_tab + (size_t)(slot * 3 + 2) * tsz;
+  // POL bit 3: the first row's table operands and CN row scalings are loaded before the wait as
+  // well, so their latency overlaps the staging copies (all rows' would not fit the registers)
+  constexpr bool EARLY = (POL & 8) != 0;
+  RowTab rte;
+  double rse[3];
+  if constexpr (EARLY) {
+    const int k = ADJ ? RPT * tc : tc;
+    if (k < g.nxm) {
+      rte = row_tab<H>(t, k);
+      rse[0] = (k >= 1) ? tld<H>(TX + k - 1) : 0.0;
+      rse[1] = tld<H>(TY + k);
+      rse[2] = tld<H>(TT + k);
+    }
+  }
+
   bool ok = mbar_wait(&bar, 0, kSpinLimit);
   // test hook: phase 1 of the barrier is never completed, so this wait always runs out
   if (g.wait_test_polls > 0) ok = ok && mbar_wait(&bar, 1, g.wait_test_polls);
@@ -535,12 +555,7 @@ __global__ void __launch_bounds__(TPC, k1_min_blocks<CAP, TPC>())
   const ColV T = TWO_D ? ColV{C(3), C(10), C(11), C(3), C(3), nullptr} : ColV{C(3), C(16), C(17), C(18), C(19), nullptr};
   const ColV P = TWO_D ? ColV{C(12), nullptr, nullptr, nullptr, nullptr, nullptr}
                        : ColV{C(20), nullptr, nullptr, nullptr, nullptr, nullptr};
-  const int slot = sc_slot(g, i, ns);
   const StepCoef sc = sc_all[slot];
-  const size_t tsz = cn_table_size(M);
-  const double *TX = cn_tab + (size_t)(slot * 3 + 0) * tsz;
-  const double *TY = cn_tab + (size_t)(slot * 3 + 1) * tsz;
-  const double *TT = cn_tab + (size_t)(slot * 3 + 2) * tsz;
   const int nxm = g.nxm;
   const size_t pl = (size_t)j + (size_t)g.nym * i;
   const double tbp = nld<H>(t.tempbp + pl), ttp = nld<H>(t.temptp + pl);
@@ -550,7 +565,7 @@ __global__ void __launch_bounds__(TPC, k1_min_blocks<CAP, TPC>())
     const int k = ADJ ? RPT * tc + p : tc + TPC * p;
     if (k < nxm) {
       TE q0 = (TE)0, q1, q2, q3;
-      const RowTab rt = row_tab<H>(t, k);
+      const RowTab rt = (EARLY && p == 0) ? rte : row_tab<H>(t, k);
       const double u0 = uu[p][0], u1 = uu[p][1], u2 = uu[p][2], u3 = uu[p][3];
       // 2-D: vz(j-1,i+1) = vz(j-1), vy(j+1,i-1) = vy(j+1), pr(i-1) = pr
       const double zd = TWO_D ? Z.jm[k] : vv[p][0];
@@ -560,10 +575,13 @@ __global__ void __launch_bounds__(TPC, k1_min_blocks<CAP, TPC>())
       double sb = 0.0;
       if constexpr (SAL) sb = sbv[p];
       // all four right-hand sides from the staged columns before anything is stored
-      rr[p][0] = (k >= 1) ? rhs_vx<TE, TWO_D, SAL, H>(g, rt, sc, k, X, Y, Z, T, P, u0, q0, sb) * tld<H>(TX + k - 1) : 0.0;
-      rr[p][1] = rhs_vy<TE, TWO_D, SAL, H>(g, rt, sc, k, X, Y, Z, T, P, zd, vv[p][2], u1, q1, sb) * tld<H>(TY + k);
-      rr[p][2] = rhs_vz<TE, TWO_D, SAL, H>(g, rt, sc, k, X, Y, Z, T, P, yd, pim, u2, q2, sb) * tld<H>(TY + k);
-      rr[p][3] = rhs_temp<TE, TWO_D, H>(g, rt, sc, k, X, Y, Z, T, tbp, ttp, u3, q3) * tld<H>(TT + k);
+      const double sx = (EARLY && p == 0) ? rse[0] : ((k >= 1) ? tld<H>(TX + k - 1) : 0.0);
+      const double sy = (EARLY && p == 0) ? rse[1] : tld<H>(TY + k);
+      const double st = (EARLY && p == 0) ? rse[2] : tld<H>(TT + k);
+      rr[p][0] = (k >= 1) ? rhs_vx<TE, TWO_D, SAL, H>(g, rt, sc, k, X, Y, Z, T, P, u0, q0, sb) * sx : 0.0;
+      rr[p][1] = rhs_vy<TE, TWO_D, SAL, H>(g, rt, sc, k, X, Y, Z, T, P, zd, vv[p][2], u1, q1, sb) * sy;
+      rr[p][2] = rhs_vz<TE, TWO_D, SAL, H>(g, rt, sc, k, X, Y, Z, T, P, yd, pim, u2, q2, sb) * sy;
+      rr[p][3] = rhs_temp<TE, TWO_D, H>(g, rt, sc, k, X, Y, Z, T, tbp, ttp, u3, q3) * st;
       if (k >= 1) rux[c0 + k] = q0;
       ruy[c0 + k] = q1;
       ruz[c0 + k] = q2;
@@ -734,6 +752,24 @@ __global__ void __launch_bounds__(TPC, k1_min_blocks<CAP, TPC>())
       sv[p][1] = sv[p][2] = sv[p][3] = sv[p][4] = 0.0;
     }
   }
+  const int slot = sc_slot(g, i, ns);
+  const size_t tsz = cn_table_size(M);
+  const double *TX = cn_tab + (size_t)(slot * 3 + 0) * tsz;
+  const double *TY = cn_tab + (size_t)(slot * 3 + 1) * tsz;
+  const double *TT = cn_tab + (size_t)(slot * 3 + 2) * tsz;
+  // POL bit 3: the first row's table operands and CN row scalings before the wait (as in
+  // k_explicit_implicit); they serve both columns
+  constexpr bool EARLY = (POL & 8) != 0;
+  RowTab rte;
+  double rse[3];
+  if constexpr (EARLY) {
+    if (tc < g.nxm) {
+      rte = row_tab<H>(t, tc);
+      rse[0] = (tc >= 1) ? tld<H>(TX + tc - 1) : 0.0;
+      rse[1] = tld<H>(TY + tc);
+      rse[2] = tld<H>(TT + tc);
+    }
+  }
   bool ok = mbar_wait(&bar, 0, kSpinLimit);
   if (g.wait_test_polls > 0) ok = ok && mbar_wait(&bar, 1, g.wait_test_polls);
   if (!__syncthreads_and(ok)) {
@@ -750,12 +786,7 @@ __global__ void __launch_bounds__(TPC, k1_min_blocks<CAP, TPC>())
     if constexpr (TWO_D) return ColV{ctr, jpc, jmc, ctr, ctr, nullptr};
     return ColV{ctr, jpc, jmc, C(16 + F * 2 + c), C(24 + F * 2 + c), nullptr};
   };
-  const int slot = sc_slot(g, i, ns);
   const StepCoef sc = sc_all[slot];
-  const size_t tsz = cn_table_size(M);
-  const double *TX = cn_tab + (size_t)(slot * 3 + 0) * tsz;
-  const double *TY = cn_tab + (size_t)(slot * 3 + 1) * tsz;
-  const double *TT = cn_tab + (size_t)(slot * 3 + 2) * tsz;
   const int nxm = g.nxm;
   double rr[RPT][2][4];
 #pragma unroll
@@ -769,7 +800,7 @@ __global__ void __launch_bounds__(TPC, k1_min_blocks<CAP, TPC>())
       const int k = tc + TPC * p;
       if (k < nxm) {
         TE q0 = (TE)0, q1, q2, q3;
-        const RowTab rt = row_tab<H>(t, k);
+        const RowTab rt = (EARLY && p == 0) ? rte : row_tab<H>(t, k);
         // vz(j-1, i+1), vy(j+1, i-1), pr(j-1), pr(i-1) of column c
         double zd, yd, pjm, pim;
         if constexpr (TWO_D) {
@@ -784,14 +815,14 @@ __global__ void __launch_bounds__(TPC, k1_min_blocks<CAP, TPC>())
         pjm = c == 0 ? sv[p][0] : C(PRC)[k];
         double sb = 0.0;
         if constexpr (SAL) sb = sbv[p][c];
-        rr[p][c][0] = (k >= 1) ? rhs_vx<TE, TWO_D, SAL, H>(g, rt, sc, k, X, Y, Z, T, P, uu[p][c][0], q0, sb) *
-                                     tld<H>(TX + k - 1)
-                               : 0.0;
-        rr[p][c][1] = rhs_vy<TE, TWO_D, SAL, H>(g, rt, sc, k, X, Y, Z, T, P, zd, pjm, uu[p][c][1], q1, sb) *
-                      tld<H>(TY + k);
-        rr[p][c][2] = rhs_vz<TE, TWO_D, SAL, H>(g, rt, sc, k, X, Y, Z, T, P, yd, pim, uu[p][c][2], q2, sb) *
-                      tld<H>(TY + k);
-        rr[p][c][3] = rhs_temp<TE, TWO_D, H>(g, rt, sc, k, X, Y, Z, T, tbp, ttp, uu[p][c][3], q3) * tld<H>(TT + k);
+        const double sx = (EARLY && p == 0) ? rse[0] : ((k >= 1) ? tld<H>(TX + k - 1) : 0.0);
+        const double sy = (EARLY && p == 0) ? rse[1] : tld<H>(TY + k);
+        const double st = (EARLY && p == 0) ? rse[2] : tld<H>(TT + k);
+        rr[p][c][0] =
+            (k >= 1) ? rhs_vx<TE, TWO_D, SAL, H>(g, rt, sc, k, X, Y, Z, T, P, uu[p][c][0], q0, sb) * sx : 0.0;
+        rr[p][c][1] = rhs_vy<TE, TWO_D, SAL, H>(g, rt, sc, k, X, Y, Z, T, P, zd, pjm, uu[p][c][1], q1, sb) * sy;
+        rr[p][c][2] = rhs_vz<TE, TWO_D, SAL, H>(g, rt, sc, k, X, Y, Z, T, P, yd, pim, uu[p][c][2], q2, sb) * sy;
+        rr[p][c][3] = rhs_temp<TE, TWO_D, H>(g, rt, sc, k, X, Y, Z, T, tbp, ttp, uu[p][c][3], q3) * st;
         if (k >= 1) rux[oc[c] + k] = q0;
         ruy[oc[c] + k] = q1;
         ruz[oc[c] + k] = q2;
@@ -1186,7 +1217,8 @@ cudaError_t launch_k1_cfg(const LaunchCtx &L, const SubstepBuffers &b, int ns, i
 
 // Launch shapes of K1 per M = {1, 2, 4, 8, 12, 16, 24, 32} (rows per lane of the CN solves):
 // {threads per column, rows per thread, register cap level, policy (bit 0: the cache hints of
-// tld / nld / sld; bit 1: tables in shared memory; bit 2: adjacent rows per thread), columns per
+// tld / nld / sld; bit 1: tables in shared memory; bit 2: adjacent rows per thread; bit 3: the
+// row operands loaded before the staging wait), columns per
 // block along y (1, or 2 for the tile of k_explicit_implicit_y2; 0 for the persistent
 // k_explicit_implicit_p with its groups of `threads` threads)}, threads x rows >= 32 M.  The
 // first entry is the default.
@@ -1197,18 +1229,18 @@ constexpr int kK1MaxShapes = 8;
 constexpr int k1_m_index(int M) {
   return M == 1 ? 0 : M == 2 ? 1 : M == 4 ? 2 : M == 8 ? 3 : M == 12 ? 4 : M == 16 ? 5 : M == 24 ? 6 : 7;
 }
-constexpr int kK1ShapeCount[8] = {1, 4, 7, 8, 8, 8, 6, 5};
+constexpr int kK1ShapeCount[8] = {1, 5, 8, 8, 8, 8, 6, 5};
 constexpr K1Shape kK1Shapes[8][kK1MaxShapes] = {
     {{32, 1, 0, 0, 1}},                                                                  // M = 1   (nxm <= 32)
-    {{64, 1, 0, 0, 1}, {32, 2, 1, 0, 1}, {64, 1, 0, 1, 1}, {64, 1, 0, 1, 2}},             // M = 2   (<= 64)
+    {{64, 1, 0, 0, 1}, {32, 2, 1, 0, 1}, {64, 1, 0, 1, 1}, {64, 1, 0, 1, 2}, {64, 1, 0, 9, 2}},  // M = 2
     {{128, 1, 0, 0, 1}, {64, 2, 1, 0, 1}, {128, 1, 2, 0, 1}, {128, 1, 0, 1, 1},           // M = 4   (<= 128)
-     {128, 1, 1, 1, 2}, {128, 1, 0, 1, 2}, {128, 1, 0, 2, 0}},
-    {{128, 2, 1, 0, 1}, {256, 1, 2, 0, 1}, {128, 2, 1, 1, 1}, {128, 2, 1, 5, 1},          // M = 8   (<= 256)
-     {128, 2, 1, 4, 1}, {256, 1, 1, 1, 2}, {128, 2, 1, 1, 2}, {128, 2, 0, 2, 0}},
-    {{128, 3, 1, 0, 1}, {256, 2, 1, 0, 1}, {384, 1, 0, 0, 1}, {128, 3, 0, 0, 1},          // M = 12  (<= 384)
+     {128, 1, 1, 1, 2}, {128, 1, 0, 1, 2}, {128, 1, 0, 2, 0}, {128, 1, 1, 9, 2}},
+    {{128, 2, 1, 0, 1}, {256, 1, 2, 0, 1}, {128, 2, 1, 1, 1}, {128, 2, 1, 9, 2},          // M = 8   (<= 256)
+     {128, 2, 1, 9, 1}, {256, 1, 1, 1, 2}, {128, 2, 1, 1, 2}, {128, 2, 0, 2, 0}},
+    {{128, 3, 1, 0, 1}, {128, 3, 1, 9, 1}, {128, 3, 0, 9, 1}, {128, 3, 0, 0, 1},          // M = 12  (<= 384)
      {384, 1, 2, 0, 1}, {384, 1, 0, 1, 1}, {128, 3, 1, 1, 1}, {384, 1, 0, 1, 2}},
-    {{128, 4, 1, 0, 1}, {256, 2, 1, 0, 1}, {512, 1, 0, 0, 1}, {128, 4, 0, 0, 1},          // M = 16  (<= 512)
-     {512, 1, 2, 0, 1}, {128, 4, 1, 1, 1}, {512, 1, 0, 1, 1}, {512, 1, 0, 1, 2}},
+    {{128, 4, 1, 0, 1}, {256, 2, 1, 0, 1}, {128, 4, 1, 9, 1}, {128, 4, 0, 0, 1},          // M = 16  (<= 512)
+     {512, 1, 2, 0, 1}, {128, 4, 1, 1, 1}, {128, 4, 1, 8, 1}, {512, 1, 0, 1, 2}},
     {{256, 3, 1, 0, 1}, {384, 2, 0, 0, 1}, {256, 4, 1, 0, 1}, {256, 3, 1, 1, 1},          // M = 24  (<= 768)
      {384, 2, 0, 1, 1}, {384, 2, 0, 1, 2}},
     {{256, 4, 1, 0, 1}, {512, 2, 0, 0, 1}, {256, 4, 1, 1, 1}, {512, 2, 0, 1, 1},          // M = 32  (<= 1024)

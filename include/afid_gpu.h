@@ -175,7 +175,8 @@ typedef struct afid_tune_info {
   int policy[AFID_TUNE_MAX];    /* bit 0: L1 cache hints (tables kept, streaming data not
                                    allocated); bit 1: two neighbouring columns per block;
                                    bit 2: adjacent rows per thread; bit 3: one persistent block
-                                   per SM with the tables in shared memory                     */
+                                   per SM with the tables in shared memory; bit 4: the first
+                                   row's table operands loaded before the staging wait          */
   double us[AFID_TUNE_MAX];     /* mean time per sample launch in microseconds (-1: not run) */
   int k4_chosen;                /* Poisson tridiagonal: 0 one mode per warp, 1 persistent warps
                                    with the next mode's right-hand side prefetched              */
