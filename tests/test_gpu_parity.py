@@ -208,7 +208,8 @@ def test_launch_count_positive():
 @pytest.mark.parametrize("shape,precision", [((256, 24, 16), ag.PREC_FP64), ((100, 16, 8), ag.PREC_FP64),
                                              ((60, 16, 1), ag.PREC_FP64), ((500, 16, 4), ag.PREC_FP64),
                                              ((64, 32, 96), ag.PREC_FP64), ((100, 16, 8), ag.PREC_MIXED),
-                                             ((64, 32, 96), ag.PREC_MIXED)])
+                                             ((64, 32, 96), ag.PREC_MIXED), ((60, 64, 64), ag.PREC_FP64),
+                                             ((60, 64, 64), ag.PREC_MIXED)])
 def test_k4_and_fftz_forms_bitwise_identical(shape, precision):
     """Both forms of the Poisson tridiagonal (a mode per warp; persistent warps with the next
     mode prefetched) and of the z transforms (a tile per block; persistent blocks with the next
