@@ -121,6 +121,18 @@ def test_cfl_divergence_globals():
         assert o.check_divergence(case.g, s) < 1e-10
 
 
+def test_cfl_after_timemarcher_passes_nan_on():
+    """A NaN that a TimeMarcher spread through the state reaches the CFL maximum
+    (CalcMaxCFL.F90:22; the main loop then turns it into 166/165)."""
+    case = Case(40, 24, 8, rayt=1e6, dt=1e-3)
+    s = case.oracle_state(random_velocity=0.1)
+    s.vy[2, 3, 5] = np.nan
+    with case.solver() as gpu:
+        gpu.upload(s.vx, s.vy, s.vz, s.temp, s.pr)
+        gpu.time_marcher(1e-3, 0)
+        assert np.isnan(gpu.calc_max_cfl())
+
+
 def test_variable_dt_main_loop():
     """Main-loop dt rule (main.F90:285-304) with the CFL from the device reduction."""
     import ctypes
