@@ -58,21 +58,37 @@ template <int H> __device__ __forceinline__ double sld(const float *p) {
 // Doubles per CN factor table (one matrix, one substep); layout in afid_kernels.cu.
 __host__ __device__ inline size_t cn_table_size(int M) { return 192 * (size_t)M + 18 * 32; }
 
+// The forward-elimination factors of one lane (a_q, 1/b'_q for q < M), loaded ahead of the
+// solve by a caller that has a barrier to hide their latency behind (cn_solve_chunk with PRE).
+template <int M, int H = 0>
+struct CnFwd {
+  double a[M], inv[M];
+  __device__ __forceinline__ void load(const double *__restrict__ T, int lane) {
+#pragma unroll
+    for (int q = 1; q < M; ++q) {
+      inv[q] = tld<H>(T + 64 * M + q * 32 + lane);
+      if (q >= 2) a[q] = tld<H>(T + 32 * M + q * 32 + lane);
+    }
+  }
+};
+
 // Solve one column whose scaled RHS sits in s[q*32 + lane] (chunk layout); the solution
-// overwrites it.  Constant-matrix version using the tables above.
-template <int M, int LD = 32, int H = 0>
+// overwrites it.  Constant-matrix version using the tables above.  PRE: the forward factors
+// come from `fw` (loaded earlier) instead of from the table.
+template <int M, int LD = 32, int H = 0, bool PRE = false>
 __device__ __forceinline__ void cn_solve_chunk(double *__restrict__ s, const double *__restrict__ T,
-                                               int lane) {
+                                               int lane, const CnFwd<M, H> *fw = nullptr) {
   const double *Ta = T + 32 * M, *Tinv = T + 64 * M, *Tcp = T + 96 * M, *Tv = T + 128 * M,
                *Tw = T + 160 * M, *Tl = T + 192 * M;
   double y[M];
 #pragma unroll
   for (int q = 0; q < M; ++q) y[q] = s[q * LD + lane];
   if constexpr (M > 1) {
-    y[1] = y[1] * tld<H>(Tinv + 32 + lane);
+    y[1] = y[1] * (PRE ? fw->inv[1] : tld<H>(Tinv + 32 + lane));
 #pragma unroll
     for (int q = 2; q < M; ++q)
-      y[q] = (y[q] - tld<H>(Ta + q * 32 + lane) * y[q - 1]) * tld<H>(Tinv + q * 32 + lane);
+      y[q] = (y[q] - (PRE ? fw->a[q] : tld<H>(Ta + q * 32 + lane)) * y[q - 1]) *
+             (PRE ? fw->inv[q] : tld<H>(Tinv + q * 32 + lane));
 #pragma unroll
     for (int q = M - 2; q >= 1; --q) y[q] = y[q] - tld<H>(Tcp + q * 32 + lane) * y[q + 1];
   }
@@ -603,6 +619,14 @@ __global__ void __launch_bounds__(TPC, k1_min_blocks<CAP, TPC>())
       s_rhs[3 * FLD + sk] = rr[p][3];
     }
   }
+  // POL bit 4: each solving warp loads its field's forward-elimination factors before the
+  // barrier below, so their latency overlaps the barrier and the other warps' stores
+  constexpr bool PRE = (POL & 16) != 0 && (TPC / 32) == 4;
+  CnFwd<M, H> fw;
+  if constexpr (PRE) {
+    const int warp = tc >> 5;
+    fw.load((warp == 0) ? TX : ((warp == 3) ? TT : TY), tc & 31);
+  }
   // identity padding rows: vx rows nxm-1 .. 32M-1, the others nxm .. 32M-1
   for (int r = nxm - 1 + tc; r < 32 * M; r += TPC) {
     const int sr = (r % M) * LD + r / M;
@@ -619,7 +643,10 @@ __global__ void __launch_bounds__(TPC, k1_min_blocks<CAP, TPC>())
     constexpr int NW = TPC / 32;
     for (int f = warp; f < 4; f += NW) {
       const double *Tb = (f == 0) ? TX : ((f == 3) ? TT : TY);
-      cn_solve_chunk<M, LD, H>(s_rhs + f * FLD, Tb, lane);
+      if constexpr (PRE)
+        cn_solve_chunk<M, LD, H, true>(s_rhs + f * FLD, Tb, lane, &fw);
+      else
+        cn_solve_chunk<M, LD, H>(s_rhs + f * FLD, Tb, lane);
     }
   }
   __syncthreads();
@@ -1235,7 +1262,7 @@ constexpr K1Shape kK1Shapes[8][kK1MaxShapes] = {
     {{64, 1, 0, 0, 1}, {32, 2, 1, 0, 1}, {64, 1, 0, 1, 1}, {64, 1, 0, 1, 2}, {64, 1, 0, 9, 2}},  // M = 2
     {{128, 1, 0, 0, 1}, {64, 2, 1, 0, 1}, {128, 1, 2, 0, 1}, {128, 1, 0, 1, 1},           // M = 4   (<= 128)
      {128, 1, 1, 1, 2}, {128, 1, 0, 1, 2}, {128, 1, 0, 2, 0}, {128, 1, 1, 9, 2}},
-    {{128, 2, 1, 0, 1}, {256, 1, 2, 0, 1}, {128, 2, 1, 1, 1}, {128, 2, 1, 9, 2},          // M = 8   (<= 256)
+    {{128, 2, 1, 0, 1}, {128, 2, 1, 25, 1}, {128, 2, 1, 1, 1}, {128, 2, 1, 9, 2},         // M = 8   (<= 256)
      {128, 2, 1, 9, 1}, {256, 1, 1, 1, 2}, {128, 2, 1, 1, 2}, {128, 2, 0, 2, 0}},
     {{128, 3, 1, 0, 1}, {128, 3, 1, 9, 1}, {128, 3, 0, 9, 1}, {128, 3, 0, 0, 1},          // M = 12  (<= 384)
      {384, 1, 2, 0, 1}, {384, 1, 0, 1, 1}, {128, 3, 1, 1, 1}, {384, 1, 0, 1, 2}},
