@@ -1245,7 +1245,8 @@ cudaError_t launch_k1_cfg(const LaunchCtx &L, const SubstepBuffers &b, int ns, i
 // Launch shapes of K1 per M = {1, 2, 4, 8, 12, 16, 24, 32} (rows per lane of the CN solves):
 // {threads per column, rows per thread, register cap level, policy (bit 0: the cache hints of
 // tld / nld / sld; bit 1: tables in shared memory; bit 2: adjacent rows per thread; bit 3: the
-// row operands loaded before the staging wait), columns per
+// row operands loaded before the staging wait; bit 4: the solves' forward factors loaded before
+// the barrier that precedes the solves), columns per
 // block along y (1, or 2 for the tile of k_explicit_implicit_y2; 0 for the persistent
 // k_explicit_implicit_p with its groups of `threads` threads)}, threads x rows >= 32 M.  The
 // first entry is the default.

@@ -19,10 +19,11 @@ int k1_shapes(int M, int *tpc, int *rpt, int *cap, int *pol) {
     if (cap) cap[v] = kK1Shapes[mi][v].cap;
     // reported policy: bit 0 cache hints, bit 1 two columns per block, bit 2 adjacent rows,
     // bit 3 the persistent kernel with its tables in shared memory, bit 4 the first row's table
-    // operands loaded before the staging wait
+    // operands loaded before the staging wait, bit 5 the solves' forward factors loaded before
+    // the barrier that precedes them
     if (pol)
       pol[v] = (kK1Shapes[mi][v].pol & 5) | (kK1Shapes[mi][v].ny == 2 ? 2 : 0) | (kK1Shapes[mi][v].ny == 0 ? 8 : 0) |
-               ((kK1Shapes[mi][v].pol & 8) ? 16 : 0);
+               ((kK1Shapes[mi][v].pol & 8) ? 16 : 0) | ((kK1Shapes[mi][v].pol & 16) ? 32 : 0);
   }
   return kK1ShapeCount[mi];
 }

@@ -176,7 +176,8 @@ typedef struct afid_tune_info {
                                    allocated); bit 1: two neighbouring columns per block;
                                    bit 2: adjacent rows per thread; bit 3: one persistent block
                                    per SM with the tables in shared memory; bit 4: the first
-                                   row's table operands loaded before the staging wait          */
+                                   row's table operands loaded before the staging wait; bit 5:
+                                   the CN solves' forward factors loaded before their barrier  */
   double us[AFID_TUNE_MAX];     /* mean time per sample launch in microseconds (-1: not run) */
   int k4_chosen;                /* Poisson tridiagonal: 0 one mode per warp, 1 persistent warps
                                    with the next mode's right-hand side prefetched              */
