@@ -1268,7 +1268,7 @@ constexpr K1Shape kK1Shapes[8][kK1MaxShapes] = {
     {{128, 3, 1, 0, 1}, {128, 3, 1, 9, 1}, {128, 3, 0, 9, 1}, {128, 3, 0, 0, 1},          // M = 12  (<= 384)
      {384, 1, 2, 0, 1}, {384, 1, 0, 1, 1}, {128, 3, 1, 1, 1}, {384, 1, 0, 1, 2}},
     {{128, 4, 1, 0, 1}, {256, 2, 1, 0, 1}, {128, 4, 1, 9, 1}, {128, 4, 0, 0, 1},          // M = 16  (<= 512)
-     {512, 1, 2, 0, 1}, {128, 4, 1, 1, 1}, {128, 4, 1, 8, 1}, {512, 1, 0, 1, 2}},
+     {512, 1, 2, 0, 1}, {128, 4, 1, 1, 1}, {128, 4, 1, 8, 1}, {128, 4, 1, 24, 1}},
     {{256, 3, 1, 0, 1}, {384, 2, 0, 0, 1}, {256, 4, 1, 0, 1}, {256, 3, 1, 1, 1},          // M = 24  (<= 768)
      {384, 2, 0, 1, 1}, {384, 2, 0, 1, 2}},
     {{256, 4, 1, 0, 1}, {512, 2, 0, 0, 1}, {256, 4, 1, 1, 1}, {512, 2, 0, 1, 1},          // M = 32  (<= 1024)
