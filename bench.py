@@ -57,6 +57,30 @@ K1_BYTES_PER_CELL = {0: 136, 1: 104}
 # Algorithmic HBM bytes per cell per RK3 step of the whole path (one compulsory pass per
 # operator): 3 x 328 B per substep + 24 B for CalcMaxCFL.
 STEP_BYTES_PER_CELL = 1008
+# Algorithmic HBM bytes per cell of each kernel class of the profile (one launch), FP64 and mixed
+# (FP32 spectrum and phi): K2 reads vx, vy, vz and writes the half spectrum (nym/2+1 of nym rows
+# of complex values, counted as half a complex a cell); K3, K4, K5 read and write the spectrum;
+# K6 reads it and writes phi; K7 reads the intermediate velocities, pr and phi and writes the
+# velocities and pr; the CFL reduction reads vx, vy, vz.
+KERNEL_BYTES_PER_CELL = {
+    0: {"explicit_implicit": 136, "div_fft_y": 32, "fft_z_fwd": 16, "tridiag_pressure": 16, "fft_z_inv": 16,
+        "ifft_y": 16, "correct": 72, "reductions": 24},
+    1: {"explicit_implicit": 104, "div_fft_y": 28, "fft_z_fwd": 8, "tridiag_pressure": 8, "fft_z_inv": 8,
+        "ifft_y": 8, "correct": 68, "reductions": 24},
+}
+
+
+def kernels_roofline(prof: dict, cells: int, precision: int, peak: float) -> dict:
+    """Achieved GB/s and fraction of the copy peak of every kernel class, from its CUDA-event
+    time per launch and its algorithmic bytes per launch."""
+    out = {}
+    for k, b in KERNEL_BYTES_PER_CELL[precision].items():
+        ms, n = prof.get(k, (0.0, 0))
+        if n:
+            gbs = b * cells / (ms / n * 1e-3) / 1e9
+            out[k] = {"bytes_per_cell": b, "ms_per_launch": round(ms / n, 4), "gbs": round(gbs, 1),
+                      "frac": round(gbs / peak, 3)}
+    return out
 
 
 def bou_text(w: dict, ntst: int) -> str:
@@ -343,6 +367,7 @@ def run_gpu(args):
                          "traffic": traffic,
                          "step_frac": round(value * 1e6 * STEP_BYTES_PER_CELL / (peak * 1e9 * world), 4)},
             "kernels_ms_per_step": {k: round(v[0] / args.steps, 4) for k, v in prof.items() if v[1]},
+            "kernels_roofline": kernels_roofline(prof, cells, w["precision"], peak),
             "e2e": {"value": round(e2e_value, 3), "unit": "Mcell-RK3-steps/s",
                     "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
                     "note": "upload 5 fields, K steps with CFL + Nu/KE read back, download 5 fields"},
