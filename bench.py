@@ -1025,8 +1025,8 @@ def run_published(args):
     solver.sal_create(mgrd)
     nx, nym, nzm = w["nxm"] + 1, w["nym"], w["nzm"]
     zeros = np.zeros((nzm, nym, nx))
-    solver.upload(zeros, zeros, zeros, tables.initial_temperature(20261203), zeros)
-    solver.sal_upload(mgrd.initial_salinity(20261204))
+    solver.upload(zeros, zeros, zeros, tables.initial_temperature(args.seed), zeros)
+    solver.sal_upload(mgrd.initial_salinity(args.seed + 1))
     xmr, xcr, xc = mgrd.array("xmr"), mgrd.array("xcr"), tables.array("xc")
     dxr, dxc = xcr[1:] - xcr[:-1], xc[1:w["nxm"] + 1] - xc[:w["nxm"]]
     pec = (w["rays"] * w["pras"]) ** 0.5
@@ -1234,6 +1234,7 @@ def main():
                                                                          "published_rbc"])
     ap.add_argument("--t-end", type=float, default=200.0, help="published_rbc: simulated time to reach")
     ap.add_argument("--sample-dt", type=float, default=0.5, help="published_rbc: time between Nusselt samples")
+    ap.add_argument("--seed", type=int, default=20261203, help="published_rbc: seed of the initial perturbations")
     ap.add_argument("--no-nu-check", action="store_true")
     ap.add_argument("--accuracy-steps", type=int, default=500,
                     help="rbc3d_mixed: steps of the mixed run compared with the FP64 replay (500 = the full run)")
