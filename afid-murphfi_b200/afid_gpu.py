@@ -125,7 +125,8 @@ class ServeResultT(C.Structure):
 class ServeStatusT(C.Structure):
     _fields_ = [("queued", C.c_int), ("running", C.c_int), ("pools", C.c_int),
                 ("device_bytes", C.c_longlong), ("cells_in_flight", C.c_longlong),
-                ("cell_steps_done", C.c_longlong), ("jobs_done", C.c_longlong)]
+                ("cell_steps_done", C.c_longlong), ("jobs_done", C.c_longlong),
+                ("pool_failures", C.c_int), ("last_cuda_error", C.c_int)]
 
 
 SERVE_FIFO, SERVE_SHORTEST_FIRST = 0, 1
@@ -173,7 +174,7 @@ EXPORTS = [
     "afid_batch_device_bytes", "afid_batch_launch_count",
     "afid_serve_create", "afid_serve_destroy", "afid_serve_submit", "afid_serve_pump", "afid_serve_poll",
     "afid_serve_cancel",
-    "afid_serve_status", "afid_serve_now", "afid_gpu_autotune", "afid_batch_autotune", "afid_batch_set_k1_shape",
+    "afid_serve_status", "afid_serve_now", "afid_serve_set_fail_test", "afid_gpu_autotune", "afid_batch_autotune", "afid_batch_set_k1_shape",
     "afid_gpu_set_k1_shape", "afid_gpu_set_k4_form", "afid_gpu_set_fftz_form", "afid_gpu_set_wait_test", "afid_gpu_mean_profiles", "afid_batch_mean_profiles",
     "afid_batch_divmax", "afid_gpu_spectra_reset", "afid_gpu_spectra_update", "afid_gpu_spectra_read", "afid_gpu_slice",
     "afid_mgrd_create", "afid_mgrd_destroy", "afid_mgrd_view", "afid_mgrd_fast", "afid_mgrd_array",
@@ -258,6 +259,7 @@ def load_library(path: str = _LIB_PATH) -> C.CDLL:
         "afid_serve_cancel": (i, [vp, C.c_uint64]),
         "afid_serve_poll": (i, [vp, C.POINTER(ServeResultT), i, C.POINTER(i)]),
         "afid_serve_status": (i, [vp, C.POINTER(ServeStatusT)]),
+        "afid_serve_set_fail_test": (i, [vp, i]),
         "afid_serve_now": (d, [vp]),
         "afid_gpu_autotune": (i, [vp, i, C.POINTER(TuneInfoT)]),
         "afid_gpu_set_k1_shape": (i, [vp, i]),
@@ -835,6 +837,10 @@ class Server:
 
     def now(self) -> float:
         return float(lib().afid_serve_now(self._h))
+
+    def set_fail_test(self, nth: int) -> None:
+        """Test hook: the nth next chunk launch counts as failed (no CUDA call); 0 = off."""
+        _check(lib().afid_serve_set_fail_test(self._h, nth), "afid_serve_set_fail_test")
 
     def close(self):
         if self._h:

@@ -87,6 +87,9 @@ struct afid_server {
   long long cell_steps_done = 0;
   long long jobs_done = 0;
   long long launches = 0;  // chunks launched
+  int pool_failures = 0;    // pools taken out after a failed operation (their jobs completed)
+  int last_cuda_error = 0;  // the CUDA error seen at the last such failure, 0 if none
+  int fail_test = 0;        // test hook: the fail_test-th next chunk launch counts as failed
   std::vector<afid_batch_stat_t> st;
   std::vector<double> nu, ke;
 };
@@ -111,6 +114,39 @@ void drop_pool(afid_server_t *s, size_t i) {
   if (p->stream) cudaStreamDestroy(p->stream);
   delete p;
   s->pools.erase(s->pools.begin() + (long)i);
+}
+
+// A pool whose chunk, harvest or launch failed: its running jobs complete with `status` (their
+// steps are not read back: the pool's state may not be), the pool is released and the server
+// goes on with the others.  A CUDA error behind the failure is recorded and cleared, so a
+// transient one does not stop later calls; a lasting one makes the next pools fail the same way.
+void fail_pool(afid_server_t *s, Pool *p, int status) {
+  const cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) s->last_cuda_error = (int)e;
+  for (int i = 0; i < p->nslots; ++i) {
+    const int idx = p->job[i];
+    if (idx < 0) continue;
+    Job &j = s->running[idx];
+    afid_serve_result_t r{};
+    r.tag = j.spec.tag;
+    r.errorcode = status;
+    r.t_submit = j.t_submit;
+    r.t_admit = j.t_admit;
+    r.t_done = now_s(s);
+    s->done.push_back(r);
+    s->cells_in_flight -= j.cells;
+    s->jobs_done += 1;
+    p->job[i] = -1;
+    j.cancelled = false;
+    s->free_running.push_back(idx);
+  }
+  s->pool_failures += 1;
+  for (size_t i = 0; i < s->pools.size(); ++i)
+    if (s->pools[i] == p) {
+      drop_pool(s, i);
+      break;
+    }
+  cudaGetLastError();  // a failed synchronisation while releasing the pool is not carried on
 }
 
 // Create a pool for `in`'s class; AFID_E_CAPACITY when it does not fit the budget even after
@@ -328,16 +364,26 @@ int afid_serve_pump(afid_server_t *s) {
   return afid_guard([&]() -> int {
     if (!s) return AFID_E_INVALID;
     bool progress = false;
+    std::vector<std::pair<Pool *, int>> failed;  // taken out after each phase
+    auto take_out = [&]() {
+      for (auto &f : failed) fail_pool(s, f.first, f.second);
+      if (!failed.empty()) progress = true;
+      failed.clear();
+    };
     // 1. harvest the pools whose chunk completed
     for (Pool *p : s->pools) {
       if (!p->in_flight) continue;
       const cudaError_t q = cudaEventQuery(p->ev);
       if (q == cudaErrorNotReady) continue;
-      if (q != cudaSuccess) return AFID_E_CUDA;
-      const int st = harvest(s, p);
-      if (st != AFID_OK) return st;
+      const int st = (q == cudaSuccess) ? harvest(s, p) : AFID_E_CUDA;
+      if (st != AFID_OK) {
+        p->in_flight = false;
+        failed.emplace_back(p, st);
+        continue;
+      }
       progress = true;
     }
+    take_out();
     // 2. admission in policy order
     std::vector<size_t> order(s->queue.size());
     for (size_t i = 0; i < order.size(); ++i) order[i] = i;
@@ -385,7 +431,10 @@ int afid_serve_pump(afid_server_t *s) {
       if (p->in_flight || p->busy() == 0) continue;
       if (has_cancelled(s, p)) {
         const int hs = harvest(s, p);
-        if (hs != AFID_OK) return hs;
+        if (hs != AFID_OK) {
+          failed.emplace_back(p, hs);
+          continue;
+        }
         progress = true;
         if (p->busy() == 0) continue;
       }
@@ -394,21 +443,29 @@ int afid_serve_pump(afid_server_t *s) {
         st = afid_batch_set_active(p->b, p->active.data());
         p->dirty = false;
       }
+      if (st == AFID_OK && s->fail_test > 0 && --s->fail_test == 0) st = AFID_E_CUDA;  // test hook
       if (st == AFID_OK) st = afid_batch_step(p->b, s->cfg.chunk_steps);
-      if (st != AFID_OK) return st;
-      if (cudaEventRecord(p->ev, p->stream) != cudaSuccess) return AFID_E_CUDA;
+      if (st == AFID_OK && cudaEventRecord(p->ev, p->stream) != cudaSuccess) st = AFID_E_CUDA;
+      if (st != AFID_OK) {
+        failed.emplace_back(p, st);
+        continue;
+      }
       p->in_flight = true;
       p->launched = s->launches++;
       progress = true;
     }
+    take_out();
     // 4. nothing happened: wait for the oldest running chunk
     if (!progress) {
       Pool *oldest = nullptr;
       for (Pool *p : s->pools)
         if (p->in_flight && (!oldest || p->launched < oldest->launched)) oldest = p;
       if (oldest) {
-        if (cudaEventSynchronize(oldest->ev) != cudaSuccess) return AFID_E_CUDA;
-        return harvest(s, oldest);
+        const int st = (cudaEventSynchronize(oldest->ev) == cudaSuccess) ? harvest(s, oldest) : AFID_E_CUDA;
+        if (st != AFID_OK) {
+          oldest->in_flight = false;
+          fail_pool(s, oldest, st);
+        }
       }
     }
     return AFID_OK;
@@ -461,10 +518,18 @@ int afid_serve_status(const afid_server_t *s, afid_serve_status_t *st) {
     st->cells_in_flight = s->cells_in_flight;
     st->cell_steps_done = s->cell_steps_done;
     st->jobs_done = s->jobs_done;
+    st->pool_failures = s->pool_failures;
+    st->last_cuda_error = s->last_cuda_error;
     return AFID_OK;
   });
 }
 
 double afid_serve_now(const afid_server_t *s) { return s ? now_s(s) : 0.0; }
+
+int afid_serve_set_fail_test(afid_server_t *s, int nth) {
+  if (!s || nth < 0) return AFID_E_INVALID;
+  s->fail_test = nth;
+  return AFID_OK;
+}
 
 }  // extern "C"

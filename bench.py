@@ -738,6 +738,12 @@ def run_served(args):
     cell_steps = sum(j["nxm"] * j["nym"] * j["nzm"] * results[j["index"]]["steps_done"] for j in jobs)
     value = cell_steps / t_end / 1e6
     errors = sum(1 for r in results.values() if r["errorcode"] != 0)
+    error_codes = {}
+    for j in jobs:
+        c = int(results[j["index"]]["errorcode"])
+        if c:
+            key = f"{c} ({j['nym']}x{j['nxm']}x{j['nzm']})"
+            error_codes[key] = error_codes.get(key, 0) + 1
     offered = sum(j["nxm"] * j["nym"] * j["nzm"] * j["nsteps"] for j in jobs) / jobs[-1]["arrival"] / 1e6
     if rank == 0:
         line = {
@@ -768,6 +774,7 @@ def run_served(args):
                     "d2h_bytes_per_step": 0,
                     "note": "served loop: host submission -> result on host; initial states built on the host and uploaded per job"},
             "jobs_with_error": errors,
+            "error_codes": error_codes,
             "peak_device_bytes": status["device_bytes"],
             "clocks": clk,
         }

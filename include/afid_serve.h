@@ -68,6 +68,8 @@ typedef struct afid_serve_status {
   long long cells_in_flight;   /* cells of running jobs                                        */
   long long cell_steps_done;   /* sum over completed jobs of cells x steps                     */
   long long jobs_done;
+  int pool_failures;           /* pools taken out after a failed chunk, harvest or launch      */
+  int last_cuda_error;         /* cudaError_t behind the last such failure (0: none)           */
 } afid_serve_status_t;
 
 int afid_serve_create(const afid_serve_config_t *cfg, afid_server_t **out);
@@ -83,11 +85,18 @@ int afid_serve_submit(afid_server_t *s, const afid_serve_job_t *job);
  * Either way it comes back from afid_serve_poll with errorcode AFID_E_CANCELLED and the steps it
  * ran.  AFID_E_INVALID if no queued or running job has the tag. */
 int afid_serve_cancel(afid_server_t *s, uint64_t tag);
-/* Harvest completed chunks, admit queued jobs, start the next chunk on idle pools with jobs. */
+/* Harvest completed chunks, admit queued jobs, start the next chunk on idle pools with jobs.
+ * A pool whose chunk, harvest or launch fails is taken out on its own: its running jobs come
+ * back with the failure's status (AFID_E_CUDA, AFID_E_TIMEOUT, ...) and steps_done 0, the other
+ * pools go on, and afid_serve_status counts it (pool_failures, last_cuda_error). */
 int afid_serve_pump(afid_server_t *s);
 /* Move up to `max` completed results into out[]; *n = how many. */
 int afid_serve_poll(afid_server_t *s, afid_serve_result_t *out, int max, int *n);
 int afid_serve_status(const afid_server_t *s, afid_serve_status_t *st);
+/* Test hook (no counterpart in the reference): the nth next chunk launch of the pump counts as a
+ * failed launch (AFID_E_CUDA) without any CUDA call, so that the isolation of a failing pool can
+ * be tested without a GPU fault; 0 turns it off. */
+int afid_serve_set_fail_test(afid_server_t *s, int nth);
 double afid_serve_now(const afid_server_t *s);
 
 #ifdef __cplusplus

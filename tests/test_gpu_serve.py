@@ -144,3 +144,28 @@ def test_cancel_queued_and_running_jobs():
         assert res[tag]["errorcode"] == 0 and res[tag]["steps_done"] == 30
     for k in ("nu_vol", "ke", "time", "dt"):
         assert res[2][k] == alone[k], k
+
+
+def test_failing_pool_is_taken_out_alone():
+    """A pool whose chunk launch fails (injected on the host: no CUDA call is made, no GPU
+    fault) is taken out by itself: its job comes back with AFID_E_CUDA and steps_done 0, the
+    job of the other pool completes with the same result as on a server without the failure,
+    and a later job of the failed pool's class gets a new pool and completes."""
+    a = (_inp(32, 64, rayt=3e6), 31, 24)
+    b = (_inp(16, 32, rayt=2e5), 32, 40)
+    with ag.Server(ag.PREC_FP64, slots_per_pool=4, chunk_steps=8) as srv:
+        srv.submit(b[0], b[1], b[2], 2)
+        ref = _run_to_completion(srv, 1)[2]
+    with ag.Server(ag.PREC_FP64, slots_per_pool=4, chunk_steps=8) as srv:
+        srv.submit(a[0], a[1], a[2], 1)   # admitted first: its pool launches first and fails
+        srv.submit(b[0], b[1], b[2], 2)
+        srv.set_fail_test(1)
+        got = _run_to_completion(srv, 2)
+        st = srv.status()
+        assert st["pool_failures"] == 1 and st["last_cuda_error"] == 0   # no CUDA error behind it
+        srv.submit(a[0], a[1], a[2], 3)
+        got.update(_run_to_completion(srv, 1))
+    assert got[1]["errorcode"] == ag.AFID_E_CUDA and got[1]["steps_done"] == 0
+    for k in ("errorcode", "steps_done", "nu_vol", "ke", "time", "dt"):
+        assert got[2][k] == ref[k], k
+    assert got[3]["errorcode"] == 0 and got[3]["steps_done"] == a[2]
