@@ -775,6 +775,8 @@ def run_served(args):
                     "note": "served loop: host submission -> result on host; initial states built on the host and uploaded per job"},
             "jobs_with_error": errors,
             "error_codes": error_codes,
+            "pool_failures": status["pool_failures"],
+            "last_cuda_error": status["last_cuda_error"],
             "peak_device_bytes": status["device_bytes"],
             "clocks": clk,
         }
