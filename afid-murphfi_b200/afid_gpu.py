@@ -94,7 +94,7 @@ class TuneInfoT(C.Structure):
     _fields_ = [("ncand", C.c_int), ("chosen", C.c_int), ("sample_columns", C.c_int),
                 ("threads", C.c_int * TUNE_MAX), ("rows", C.c_int * TUNE_MAX), ("regcap", C.c_int * TUNE_MAX),
                 ("policy", C.c_int * TUNE_MAX), ("us", C.c_double * TUNE_MAX), ("k4_chosen", C.c_int),
-                ("k4_us", C.c_double * 2), ("fftz_chosen", C.c_int), ("fftz_us", C.c_double * 2)]
+                ("k4_us", C.c_double * 2), ("fftz_chosen", C.c_int), ("fftz_us", C.c_double * 3)]
 
     def as_dict(self) -> dict:
         """shapes: [threads per column, rows per thread, register cap, memory policy,

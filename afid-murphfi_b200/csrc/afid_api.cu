@@ -653,7 +653,7 @@ int ctx_autotune(afid_ctx_t *ctx, bool force) {
   // The z transforms (3-D single domains): one tile per block, or persistent blocks with the next
   // tile's copies in flight; timed the same way (the spectrum's contents are dead here too).
   info.fftz_chosen = 0;
-  info.fftz_us[0] = info.fftz_us[1] = -1.0;
+  info.fftz_us[0] = info.fftz_us[1] = info.fftz_us[2] = -1.0;
   if (ctx->L.g.nzm > 1 && !ctx->L.g.batch) {
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     cudaError_t e = cudaEventCreate(&e0);
@@ -662,7 +662,7 @@ int ctx_autotune(afid_ctx_t *ctx, bool force) {
     LaunchCtx Lz = ctx->L;
     constexpr int kReps = 3;
     for (int round = 0; round < 2 && e == cudaSuccess; ++round)
-      for (int v = 0; v < 2 && e == cudaSuccess; ++v) {
+      for (int v = 0; v < 3 && e == cudaSuccess; ++v) {
         Lz.fftz_var = v;
         if (launch_stage(Lz, b, 0, Stage::FftZFwd) != cudaSuccess) {  // this form does not fit: skip it
           cudaGetLastError();
@@ -681,7 +681,8 @@ int ctx_autotune(afid_ctx_t *ctx, bool force) {
     if (e0) cudaEventDestroy(e0);
     if (e1) cudaEventDestroy(e1);
     if (e != cudaSuccess) return fail_cuda(ctx, e);
-    if (info.fftz_us[1] >= 0.0 && info.fftz_us[1] < info.fftz_us[0]) info.fftz_chosen = 1;
+    for (int v = 1; v < 3; ++v)
+      if (info.fftz_us[v] >= 0.0 && info.fftz_us[v] < info.fftz_us[info.fftz_chosen]) info.fftz_chosen = v;
   }
   ctx->L.fftz_var = info.fftz_chosen;
   ctx->tune = info;
@@ -953,7 +954,12 @@ int afid_gpu_set_k4_form(afid_ctx_t *ctx, int form) {
 }
 
 int afid_gpu_set_fftz_form(afid_ctx_t *ctx, int form) {
-  if (!ctx || form < 0 || form > 1) return AFID_E_INVALID;
+  if (!ctx || form < 0 || form > 2 || (form == 2 && ctx->L.mixed)) return AFID_E_INVALID;
+  // the persistent forms hold two tiles of nzm rows of 8 elements in shared memory (the
+  // tensor-copy form with its barriers and 1024-byte alignment slack)
+  const size_t elem = ctx->L.mixed ? 8 : 16;
+  const size_t tiles = 2 * (size_t)ctx->L.g.nzm * 8 * elem + (form == 2 ? 16 + 1024 : 0);
+  if (form > 0 && tiles > (size_t)227 * 1024) return AFID_E_INVALID;
   ctx->L.fftz_var = form;
   ctx->tune.fftz_chosen = form;
   return AFID_OK;

@@ -435,6 +435,22 @@ __device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t by
       "l"(src), "r"(bytes), "r"(smem_u32(bar))
       : "memory");
 }
+// 1-D bulk copy shared -> global in the issuing thread's bulk group (same alignment rules).
+// The shared source must be published to the async proxy first (fence_proxy_async_shared after
+// the generic stores, then a barrier), and must not be overwritten before bulk_wait_read().
+__device__ __forceinline__ void bulk_s2g(void *dst, const void *src, uint32_t bytes) {
+  asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(dst), "r"(smem_u32(src)),
+               "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+// This thread's committed bulk stores have read their shared sources.
+__device__ __forceinline__ void bulk_wait_read() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
+// This thread's committed bulk stores are complete.
+__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
+__device__ __forceinline__ void fence_proxy_async_shared() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
 // Per-thread asynchronous copy of one BYTES-sized element (4, 8 or 16) global -> shared, with
 // zero fill when `valid` is false (no byte is read then; src must still be a mapped address).
 // Completed by cp_async_wait_all() in the issuing thread; a barrier publishes it to the block.

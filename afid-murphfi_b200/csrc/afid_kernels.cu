@@ -19,6 +19,9 @@
 // (double, or float for the mixed path); TS is the type of the spectral transforms.  The
 // state (vx, vy, vz, temp, pr), the RHS assembly and every tridiagonal solve are FP64.
 #include <algorithm>
+#include <type_traits>
+
+#include <cuda.h>
 
 #include "afid_device.cuh"
 #include "afid_internal.h"
@@ -886,6 +889,152 @@ __global__ void __launch_bounds__(256)
   }
 }
 
+// Shared-memory row of z index r = k1 + N1 * rl in k_fft_z_wt's output tile, where lane
+// bitrev5(rl) of a warp holds it in register k1 after the warp FFT: row q + 8 a for
+// r = a + 4 N1 q (q = rl >> 2, a = k1 + N1 (rl & 3)), the order in which the store tensor map
+// (dimensions x, q, a) lays the tile out.  The row's low three bits are q, which differ between
+// the eight lanes of a quarter warp, so with the 128-byte swizzle (16-byte chunk c of row R at
+// c ^ (R & 7)) the write-back of one register across the warp is free of bank conflicts.
+template <int N1>
+__device__ __forceinline__ int zslot(int k1, int rl) {
+  return ((rl >> 2) & 7) + 8 * (k1 + N1 * (rl & 3));
+}
+
+// 4-D tiled tensor copies (no multicast): global -> shared completing on an mbarrier, and
+// shared -> global in the issuing thread's bulk group.  `map` is a __grid_constant__ kernel
+// parameter; the innermost coordinate must be a multiple of 16 bytes.
+__device__ __forceinline__ void tma_load_4d(void *dst, const CUtensorMap *map, int c0, int c1, int c2, int c3,
+                                            uint64_t *bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, "
+      "%5}], [%6];" ::"r"(smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(smem_u32(bar))
+      : "memory");
+}
+__device__ __forceinline__ void tma_store_4d(const CUtensorMap *map, int c0, int c1, int c2, int c3, const void *src) {
+  asm volatile("cp.async.bulk.tensor.4d.global.shared::cta.tile.bulk_group [%0, {%1, %2, %3, %4}], [%5];" ::"l"(
+                   reinterpret_cast<uint64_t>(map)),
+               "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(smem_u32(src))
+               : "memory");
+}
+
+// K3w / K5w, tensor-copy persistent form (FP64 spectrum): a tile (8 x points at one ky, all nzm
+// z rows) comes in by one tiled TMA load and goes back by one tiled TMA store, so the load/store
+// pipe carries only the transform's own shared-memory traffic (the per-thread asynchronous copies
+// of k_fft_z_wp spend about a third of it, and one 1-D bulk copy per 128-byte row is bound by the
+// copy engine's operation rate instead).  The load map views z as (z mod 32, z / 32) and fills the
+// tile in z order; the store map views z as (z / 4 N1, z mod 4 N1) and reads the tile in zslot
+// order, into which each warp writes its column's results in place (its own swizzled chunks, so no
+// other warp is touched).  Both use the 128-byte swizzle; x points past nxm load as zeros and are
+// not stored.  Two tiles in flight as in k_fft_z_wp; the same arithmetic, so the same bits.  The
+// staging wait is bounded: a block that gives up sets bit 2 of *err, lets its copies land and
+// exits.
+template <int N1, bool INV>
+__global__ void __launch_bounds__(256)
+    k_fft_z_wt(Geom g, const __grid_constant__ CUtensorMap ld_map, const __grid_constant__ CUtensorMap st_map,
+               const double2 *__restrict__ tw, int *__restrict__ err) {
+  constexpr int N = 32 * N1;
+  extern __shared__ __align__(1024) unsigned char smem_k3t[];
+  // the 128-byte swizzle repeats every 1024 bytes: tiles start on such a boundary
+  unsigned char *base = smem_k3t + ((1024u - (smem_u32(smem_k3t) & 1023u)) & 1023u);
+  double2 *sb = reinterpret_cast<double2 *>(base);  // [2][N][8]
+  uint64_t *bar = reinterpret_cast<uint64_t *>(sb + 2 * N * 8);
+  const int ntx = (g.nxm + 7) / 8;
+  const int ntiles = ntx * g.nyh;
+  const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+  if (tid == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+  auto issue = [&](int tile, int b) {  // thread 0
+    const int k0 = (tile % ntx) * 8, ky = tile / ntx;
+    mbar_arrive_expect_tx(&bar[b], 128u * N);
+    tma_load_4d(sb + (size_t)b * N * 8, &ld_map, 2 * k0, 0, 0, ky, &bar[b]);
+  };
+  int tile = blockIdx.x;
+  if (tid == 0 && tile < ntiles) issue(tile, 0);
+  for (int it = 0; tile < ntiles; ++it, tile += gridDim.x) {
+    const int b = it & 1, nt = tile + gridDim.x;
+    if (nt < ntiles) {
+      // buffer b ^ 1 last held tile it - 1: its store must have read it before it is refilled
+      if (tid == 0) bulk_wait_read();
+      __syncthreads();
+      if (tid == 0) issue(nt, b ^ 1);
+    }
+    const uint32_t par = (uint32_t)(it >> 1) & 1u;
+    bool ok = mbar_wait(&bar[b], par, kSpinLimit);
+    // test hook: the opposite phase is never completed here, so this wait always runs out
+    if (g.wait_test_polls > 0) ok = ok && mbar_wait(&bar[b], par ^ 1u, g.wait_test_polls);
+    if (!__syncthreads_and(ok)) {
+      if (tid == 0) atomicOr(err, 2);
+      mbar_wait(&bar[b], par, kDrainLimit);  // copies in flight land before the block exits
+      if (nt < ntiles) mbar_wait(&bar[b ^ 1], (uint32_t)((it + 1) >> 1) & 1u, kDrainLimit);
+      break;
+    }
+    double2 *s = sb + (size_t)b * N * 8;
+    double2 x[N1];
+#pragma unroll
+    for (int m = 0; m < N1; ++m) {
+      const int r = lane + 32 * m;
+      x[m] = s[r * 8 + (w ^ (r & 7))];
+    }
+    __syncwarp();
+    warp_fft<INV, double, N1>(x, lane, tw);
+    const int rl = bitrev5(lane);
+#pragma unroll
+    for (int k1 = 0; k1 < N1; ++k1) {
+      const int r = zslot<N1>(k1, rl);
+      s[r * 8 + (w ^ (r & 7))] = x[k1];
+    }
+    fence_proxy_async_shared();
+    __syncthreads();
+    if (tid == 0) {
+      tma_store_4d(&st_map, 2 * ((tile % ntx) * 8), 0, 0, tile / ntx, s);
+      bulk_commit();
+    }
+  }
+  if (tid == 0) bulk_wait_all();
+}
+
+// The two tensor maps of k_fft_z_wt over an FP64 spectrum [nzm][nyh][ldxc] of double2, viewed
+// as doubles: x (2 nxm, the tile's 16 doubles a box row), two z dimensions, ky.  Encoded through
+// the driver's entry point (no driver library linked); false if that is unavailable or refuses.
+using TmapEncodeFn = CUresult (*)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                  const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+static TmapEncodeFn tmap_encoder() {
+  static TmapEncodeFn fn = []() -> TmapEncodeFn {
+    void *f = nullptr;
+    cudaDriverEntryPointQueryResult q{};
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      return nullptr;
+    return reinterpret_cast<TmapEncodeFn>(f);
+  }();
+  return fn;
+}
+
+static bool fftz_tmaps(const Geom &g, int N1, double2 *spec, CUtensorMap *ld, CUtensorMap *st) {
+  TmapEncodeFn enc = tmap_encoder();
+  if (!enc) return false;
+  const cuuint64_t zb = (cuuint64_t)g.nyh * g.ldxc * sizeof(double2);  // bytes between z rows
+  const cuuint32_t estr[4] = {1, 1, 1, 1};
+  const cuuint64_t ldim[4] = {(cuuint64_t)2 * g.nxm, 32, (cuuint64_t)N1, (cuuint64_t)g.nyh};
+  const cuuint64_t lstr[3] = {zb, 32 * zb, (cuuint64_t)g.ldxc * sizeof(double2)};
+  const cuuint32_t lbox[4] = {16, 32, (cuuint32_t)N1, 1};
+  const cuuint64_t sdim[4] = {(cuuint64_t)2 * g.nxm, 8, (cuuint64_t)4 * N1, (cuuint64_t)g.nyh};
+  const cuuint64_t sstr[3] = {(cuuint64_t)4 * N1 * zb, zb, (cuuint64_t)g.ldxc * sizeof(double2)};
+  const cuuint32_t sbox[4] = {16, 8, (cuuint32_t)(4 * N1), 1};
+  return enc(ld, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4, spec, ldim, lstr, lbox, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+             CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS &&
+         enc(st, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4, spec, sdim, sstr, sbox, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+             CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
 // K6w: backward y c2r.  Block: 16 x points = 8 pairs (8 warps) at one z index i.  The half
 // spectrum rows 0 .. N/2 of the 16 x points are staged with asynchronous copies (all in flight
 // at once); each warp then builds its packed sequence straight from them.
@@ -1267,7 +1416,29 @@ static cudaError_t launch_w_n1(const LaunchCtx &L, const SubstepBuffers &b, int 
     return cudaGetLastError();
   }
   const size_t sm = (size_t)N * 8 * sizeof(C);
-  if (L.fftz_var == 1) {  // persistent, double-buffered tiles (the autotuner's pick)
+  if (L.fftz_var == 2) {  // persistent, rows moved by bulk copies (FP64 spectrum only)
+    if constexpr (!std::is_same<TS, double>::value) {
+      return cudaErrorInvalidValue;
+    } else {
+      // two 1024-byte aligned tiles of N x 128 bytes, the barriers, the alignment slack
+      const size_t smb = (size_t)2 * N * 8 * sizeof(double2) + 2 * sizeof(uint64_t) + 1024;
+      if (smb > (size_t)227 * 1024 || 4 * N1 > 256) return cudaErrorInvalidValue;  // two tiles do not fit
+      CUtensorMap ld_map, st_map;
+      if (!fftz_tmaps(g, N1, spec, &ld_map, &st_map)) return cudaErrorInvalidValue;
+      auto kern = (st == Stage::FftZFwd) ? k_fft_z_wt<N1, false> : k_fft_z_wt<N1, true>;
+      cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smb);
+      if (e != cudaSuccess) return e;
+      int dev = 0, nsm = 148, per = 1;
+      cudaGetDevice(&dev);
+      if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || nsm < 1) nsm = 148;
+      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, 256, smb) != cudaSuccess || per < 1) per = 1;
+      const int ntiles = ((g.nxm + 7) / 8) * g.nyh;
+      kern<<<std::max(1, std::min(ntiles, nsm * per)), 256, smb, L.stream>>>(g, ld_map, st_map,
+                                                                              (const double2 *)L.twz, b.err);
+      return cudaGetLastError();
+    }
+  }
+  if (L.fftz_var == 1) {  // persistent, double-buffered tiles
     if (2 * sm > (size_t)227 * 1024) return cudaErrorInvalidValue;  // two tiles do not fit
     auto kern = (st == Stage::FftZFwd) ? k_fft_z_wp<N1, false, TS> : k_fft_z_wp<N1, true, TS>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(2 * sm));

@@ -183,8 +183,9 @@ typedef struct afid_tune_info {
                                    with the next mode's right-hand side prefetched              */
   double k4_us[2];              /* microseconds per full launch of each form (-1: not run)   */
   int fftz_chosen;              /* z transforms: 0 one tile per block, 1 persistent blocks with
-                                   the next tile's copies in flight (3-D single domains)         */
-  double fftz_us[2];            /* microseconds per full forward z launch of each form         */
+                                   the next tile's copies in flight, 2 the same with the tile
+                                   rows moved by bulk copies (FP64 only; 3-D single domains)    */
+  double fftz_us[3];            /* microseconds per full forward z launch of each form         */
 } afid_tune_info_t;
 int afid_gpu_autotune(afid_ctx_t *ctx, int force, afid_tune_info_t *info);
 /* Use shape `index` (0 .. ncand-1) from now on without timing, e.g. one saved from an earlier
@@ -194,11 +195,12 @@ int afid_gpu_set_k1_shape(afid_ctx_t *ctx, int index);
 /* Use Poisson-tridiagonal form `form` (0 or 1 as in afid_tune_info_t.k4_chosen) from now on;
  * both forms give bitwise the same results. */
 int afid_gpu_set_k4_form(afid_ctx_t *ctx, int form);
-/* Use z-transform form `form` (0 or 1 as in afid_tune_info_t.fftz_chosen); bitwise the same. */
+/* Use z-transform form `form` (0, 1 or 2 as in afid_tune_info_t.fftz_chosen); bitwise the same.
+ * AFID_E_INVALID for form 2 on a mixed-precision context (FP32 spectrum). */
 int afid_gpu_set_fftz_form(afid_ctx_t *ctx, int form);
 /* Test hook of the bounded device waits (no counterpart in the reference).  With polls > 0
- * (at most 2^24), the fused explicit/implicit kernel's staging wait, after its copies have
- * landed, also waits at most `polls` polls for an mbarrier phase that nothing completes: every
+ * (at most 2^24), the fused explicit/implicit kernel's staging wait (and that of z-transform
+ * form 2), after its copies have landed, also waits at most `polls` polls for an mbarrier phase that nothing completes: every
  * block gives up, sets the error flag and exits, and the next call that synchronises with the
  * stream (afid_gpu_synchronize, afid_gpu_cfl, afid_gpu_divmax, afid_gpu_globals, ...) returns
  * AFID_E_TIMEOUT.  No fault, no hang; the flag stays set for the life of the context (as the

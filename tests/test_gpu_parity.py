@@ -221,26 +221,35 @@ def test_launch_count_positive():
                                              ((60, 16, 1), ag.PREC_FP64), ((500, 16, 4), ag.PREC_FP64),
                                              ((64, 32, 96), ag.PREC_FP64), ((100, 16, 8), ag.PREC_MIXED),
                                              ((64, 32, 96), ag.PREC_MIXED), ((60, 64, 64), ag.PREC_FP64),
-                                             ((60, 64, 64), ag.PREC_MIXED)])
+                                             ((60, 64, 64), ag.PREC_MIXED), ((60, 16, 256), ag.PREC_FP64),
+                                             ((36, 8, 384), ag.PREC_FP64), ((64, 8, 512), ag.PREC_FP64)])
 def test_k4_and_fftz_forms_bitwise_identical(shape, precision):
     """Both forms of the Poisson tridiagonal (a mode per warp; persistent warps with the next
-    mode prefetched) and of the z transforms (a tile per block; persistent blocks with the next
-    tile prefetched) give the same fields bit for bit, so the autotuner's choices change the
-    schedule only."""
+    mode prefetched) and every form of the z transforms (a tile per block; persistent blocks
+    with the next tile prefetched by per-thread copies, or by bulk row copies with bulk stores,
+    FP64 only) give the same fields bit for bit, so the autotuner's choices change the schedule
+    only.  nxm = 60 and 36 leave a partial tile of x points."""
     case = Case(*shape, precision=precision, rayt=1e6, dt=2e-3)
     s = case.oracle_state(random_velocity=0.1)
+    forms = (0, 1, 2) if precision == ag.PREC_FP64 else (0, 1)
     outs = []
-    for form in (0, 1):
+    for form in forms:
         with case.solver() as g:
             g.autotune()
-            g.set_k4_form(form)
+            g.set_k4_form(min(form, 1))
             g.set_fftz_form(form)
             g.upload(s.vx, s.vy, s.vz, s.temp, s.pr)
             for n in range(2):
                 g.time_marcher(2e-3, n)
             outs.append(g.download())
-    for k in ag.Solver.FIELDS:
-        assert np.array_equal(outs[0][k], outs[1][k]), k
+    for o_ in outs[1:]:
+        for k in ag.Solver.FIELDS:
+            assert np.array_equal(outs[0][k], o_[k]), k
+    if precision != ag.PREC_FP64:
+        with case.solver() as g:
+            with pytest.raises(ag.AfidError) as e:
+                g.set_fftz_form(2)
+            assert e.value.status == ag.AFID_E_INVALID
 
 
 @pytest.mark.parametrize("name", ["rbc3d_16x12x8_rv", "rbc3d_40x10x6_rv", "rbc2d_32x48x1"])
