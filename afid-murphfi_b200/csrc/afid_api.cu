@@ -531,6 +531,7 @@ int ctx_create(const afid_grid_t *grid, const afid_params_t *prm, const BatchSpe
   L.k1_var = 0;
   L.k4_var = 0;
   L.fftz_var = 0;
+  L.ify_var = 0;
   L.plan_y = py;
   L.plan_z = pz;
   L.twy = twy;
@@ -685,6 +686,40 @@ int ctx_autotune(afid_ctx_t *ctx, bool force) {
       if (info.fftz_us[v] >= 0.0 && info.fftz_us[v] < info.fftz_us[info.fftz_chosen]) info.fftz_chosen = v;
   }
   ctx->L.fftz_var = info.fftz_chosen;
+  // The inverse y transform (FP64 single domains): per-thread copies or tensor copies, timed on
+  // full launches (phi and the spectrum are dead here: K6 rewrites phi from the spectrum).
+  info.ify_chosen = 0;
+  info.ify_us[0] = info.ify_us[1] = -1.0;
+  if (!ctx->L.mixed && !ctx->L.g.batch && ctx->L.warp_fft) {
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    cudaError_t e = cudaEventCreate(&e0);
+    if (e == cudaSuccess) e = cudaEventCreate(&e1);
+    SubstepBuffers b = buffers(ctx);
+    LaunchCtx L6 = ctx->L;
+    constexpr int kReps = 3;
+    for (int round = 0; round < 2 && e == cudaSuccess; ++round)
+      for (int v = 0; v < 2 && e == cudaSuccess; ++v) {
+        L6.ify_var = v;
+        if (launch_stage(L6, b, 0, Stage::IfftY) != cudaSuccess) {  // this form does not apply: skip it
+          cudaGetLastError();
+          continue;
+        }
+        cudaEventRecord(e0, ctx->stream);
+        for (int r = 0; r < kReps && e == cudaSuccess; ++r) e = launch_stage(L6, b, 0, Stage::IfftY);
+        cudaEventRecord(e1, ctx->stream);
+        if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+        float ms = 0.f;
+        if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+        ctx->launches += 1 + kReps;
+        const double us = 1e3 * ms / kReps;
+        if (e == cudaSuccess && (info.ify_us[v] < 0.0 || us < info.ify_us[v])) info.ify_us[v] = us;
+      }
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    if (e != cudaSuccess) return fail_cuda(ctx, e);
+    if (info.ify_us[1] >= 0.0 && info.ify_us[1] < info.ify_us[0]) info.ify_chosen = 1;
+  }
+  ctx->L.ify_var = info.ify_chosen;
   ctx->tune = info;
   ctx->tuned = true;
   return check_err_flag(ctx);
@@ -962,6 +997,18 @@ int afid_gpu_set_fftz_form(afid_ctx_t *ctx, int form) {
   if (form > 0 && tiles > (size_t)227 * 1024) return AFID_E_INVALID;
   ctx->L.fftz_var = form;
   ctx->tune.fftz_chosen = form;
+  return AFID_OK;
+}
+
+int afid_gpu_set_ify_form(afid_ctx_t *ctx, int form) {
+  if (!ctx || form < 0 || form > 1) return AFID_E_INVALID;
+  // the tensor-copy form: FP64 single domains whose y transform is a warp FFT of at most 384
+  // points (N = 32 x {1, 2, 3, 4, 6, 8, 12})
+  const int nym = ctx->L.g.nym, n1 = nym / 32;
+  const bool fits = nym % 32 == 0 && (n1 <= 4 || n1 == 6 || n1 == 8 || n1 == 12);
+  if (form == 1 && (ctx->L.mixed || ctx->L.g.batch || !ctx->L.warp_fft || !fits)) return AFID_E_INVALID;
+  ctx->L.ify_var = form;
+  ctx->tune.ify_chosen = form;
   return AFID_OK;
 }
 

@@ -37,9 +37,9 @@ struct Geom {
   // bycs * salc at rows 0..nxm-1; nullptr when no active salinity is coupled.
   const double *salc;
   double bycs;
-  // Test hook of the bounded waits (afid_gpu_set_wait_test): when non-zero, K1's staging wait
-  // also waits for an mbarrier phase that nothing completes, for at most this many polls, so
-  // the timeout path runs; 0 in normal operation.
+  // Test hook of the bounded waits (afid_gpu_set_wait_test): when non-zero, the staging waits of
+  // K1 and of the tensor-copy transforms also wait for an mbarrier phase that nothing
+  // completes, for at most this many polls, so the timeout path runs; 0 in normal operation.
   long long wait_test_polls;
 };
 
@@ -435,18 +435,12 @@ __device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t by
       "l"(src), "r"(bytes), "r"(smem_u32(bar))
       : "memory");
 }
-// 1-D bulk copy shared -> global in the issuing thread's bulk group (same alignment rules).
-// The shared source must be published to the async proxy first (fence_proxy_async_shared after
-// the generic stores, then a barrier), and must not be overwritten before bulk_wait_read().
-__device__ __forceinline__ void bulk_s2g(void *dst, const void *src, uint32_t bytes) {
-  asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(dst), "r"(smem_u32(src)),
-               "r"(bytes)
-               : "memory");
-}
+// Bulk-group bookkeeping of the issuing thread (tensor stores shared -> global): commit the
+// copies issued so far; wait until they have read their shared sources, or until complete.
+// A shared source must be published to the async proxy first (fence_proxy_async_shared after
+// the generic stores, then a barrier).
 __device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
-// This thread's committed bulk stores have read their shared sources.
 __device__ __forceinline__ void bulk_wait_read() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
-// This thread's committed bulk stores are complete.
 __device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
 __device__ __forceinline__ void fence_proxy_async_shared() {
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");

@@ -19,7 +19,9 @@ struct LaunchCtx {
   bool warp_fft;   // register-resident warp FFT when N = 32*{1,2,3,4,6,8,12,16,24,32}
   int k1_var;      // K1 thread shape (index into the shapes of k1_shapes(M)), set by the autotuner
   int k4_var;      // K4 form: 0 one mode a warp, 1 persistent with the next mode prefetched (FP64)
-  int fftz_var;    // z transforms (K3/K5): 0 a tile a block, 1 persistent with the next tile prefetched
+  int fftz_var;    // z transforms (K3/K5): 0 a tile a block, 1 persistent with the next tile
+                   // prefetched, 2 the same with tensor copies (FP64)
+  int ify_var;     // inverse y transform (K6): 0 per-thread copies, 1 tensor copies (FP64 single domain)
   FftPlan plan_y, plan_z;
   const void *twy, *twz;  // twiddle tables (double2 or float2)
 };

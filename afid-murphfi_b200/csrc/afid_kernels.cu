@@ -911,6 +911,13 @@ __device__ __forceinline__ void tma_load_4d(void *dst, const CUtensorMap *map, i
       "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(smem_u32(bar))
       : "memory");
 }
+__device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, int c0, int c1, int c2, uint64_t *bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
+      "[%5];" ::"r"(smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(smem_u32(bar))
+      : "memory");
+}
 __device__ __forceinline__ void tma_store_4d(const CUtensorMap *map, int c0, int c1, int c2, int c3, const void *src) {
   asm volatile("cp.async.bulk.tensor.4d.global.shared::cta.tile.bulk_group [%0, {%1, %2, %3, %4}], [%5];" ::"l"(
                    reinterpret_cast<uint64_t>(map)),
@@ -1104,6 +1111,128 @@ __global__ void __launch_bounds__(256)
     }
   }
   (void)Tr;
+}
+
+// K6w, tensor-copy persistent form (FP64 spectrum and phi, single domain, N <= 384): a tile
+// (16 x points at one z index) is the half spectrum rows 0 .. N/2, brought in by two tiled TMA
+// loads (8 x points each, 128-byte swizzle), and phi at its 16 x points of all N rows, sent out by
+// one tiled TMA store whose map views y as (j / 4 N1, j mod 4 N1): the warps write the output
+// tile over the staged input in zslot order, free of bank conflicts as in k_fft_z_wt.  The
+// load/store pipe then carries only the transform's own shared-memory traffic.  Each block walks
+// tiles blockIdx.x, + gridDim.x, ... with two tiles in flight.  The same arithmetic as
+// k_ifft_y_w, so the same bits; x points past nxm load as zeros and are not stored.  The staging
+// wait is bounded (bit 2 of *err, copies drained before the block exits).
+template <int N1>
+__global__ void __launch_bounds__(256)
+    k_ifft_y_wt(Geom g, const __grid_constant__ CUtensorMap ld_map, const __grid_constant__ CUtensorMap st_map,
+                const double2 *__restrict__ tw, int *__restrict__ err) {
+  constexpr int N = 32 * N1;
+  constexpr int NH = N / 2 + 1;
+  constexpr int HB = (NH * 128 + 1023) / 1024 * 1024;  // bytes of one staged half, 1024-aligned
+  static_assert(N * 128 <= 2 * HB, "the output tile fits over the staged halves");
+  if (!inst_active(g, 0)) return;  // a single domain stopped by its step control
+  extern __shared__ __align__(1024) unsigned char smem_k6t[];
+  unsigned char *base = smem_k6t + ((1024u - (smem_u32(smem_k6t) & 1023u)) & 1023u);  // [2][2][HB]
+  uint64_t *bar = reinterpret_cast<uint64_t *>(base + 4 * HB);
+  const int ntx = (g.nxm + 15) / 16;
+  const int ntiles = ntx * g.nzm;
+  const int tid = threadIdx.x, lane = tid & 31, p = tid >> 5;
+  if (tid == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+  auto issue = [&](int tile, int b) {  // thread 0
+    const int k0 = (tile % ntx) * 16, i = tile / ntx;
+    const bool two = k0 + 8 < g.nxm;  // the second 8 x points hold data
+    unsigned char *dst = base + (size_t)b * 2 * HB;
+    mbar_arrive_expect_tx(&bar[b], (two ? 2u : 1u) * 128u * NH);
+    tma_load_3d(dst, &ld_map, 2 * k0, 0, i, &bar[b]);
+    if (two) tma_load_3d(dst + HB, &ld_map, 2 * k0 + 16, 0, i, &bar[b]);
+  };
+  int tile = blockIdx.x;
+  if (tid == 0 && tile < ntiles) issue(tile, 0);
+  for (int it = 0; tile < ntiles; ++it, tile += gridDim.x) {
+    const int b = it & 1, nt = tile + gridDim.x;
+    if (nt < ntiles) {
+      // buffer b ^ 1 last held tile it - 1: its store must have read it before it is refilled
+      if (tid == 0) bulk_wait_read();
+      __syncthreads();
+      if (tid == 0) issue(nt, b ^ 1);
+    }
+    const uint32_t par = (uint32_t)(it >> 1) & 1u;
+    bool ok = mbar_wait(&bar[b], par, kSpinLimit);
+    // test hook: the opposite phase is never completed here, so this wait always runs out
+    if (g.wait_test_polls > 0) ok = ok && mbar_wait(&bar[b], par ^ 1u, g.wait_test_polls);
+    if (!__syncthreads_and(ok)) {
+      if (tid == 0) atomicOr(err, 2);
+      mbar_wait(&bar[b], par, kDrainLimit);  // copies in flight land before the block exits
+      if (nt < ntiles) mbar_wait(&bar[b ^ 1], (uint32_t)((it + 1) >> 1) & 1u, kDrainLimit);
+      break;
+    }
+    unsigned char *tb = base + (size_t)b * 2 * HB;
+    const double2 *Hp = reinterpret_cast<const double2 *>(tb + (p >> 2) * HB);  // the half of x point k0 + 2p
+    const int c0 = (2 * p) & 7;  // its chunk within that half
+    double2 x[N1];
+#pragma unroll
+    for (int m = 0; m < N1; ++m) {
+      // row j of the full spectrum from row jj of the half spectrum (conjugate above N/2); the
+      // pair (x points k0 + 2p, k0 + 2p + 1) packed as X + iY
+      const int j = lane + 32 * m;
+      const bool cj = (2 * j > N);
+      const int jj = cj ? N - j : j;
+      const int sw = jj & 7;
+      double2 X = Hp[jj * 8 + (c0 ^ sw)], Y = Hp[jj * 8 + ((c0 + 1) ^ sw)];
+      if (cj) {
+        X.y = -X.y;
+        Y.y = -Y.y;
+      }
+      if (jj == 0 || 2 * jj == N) {
+        X.y = 0;
+        Y.y = 0;
+      }
+      x[m].x = X.x - Y.y;
+      x[m].y = X.y + Y.x;
+    }
+    warp_fft<true, double, N1>(x, lane, tw);
+    __syncthreads();  // every warp has read its input before the tile is overwritten
+    double2 *T = reinterpret_cast<double2 *>(tb);  // [N][8] output tile
+    const int rl = bitrev5(lane);
+#pragma unroll
+    for (int k1 = 0; k1 < N1; ++k1) {
+      const int r = zslot<N1>(k1, rl);
+      T[r * 8 + (p ^ (r & 7))] = x[k1];  // chunk p of row r: phi at x points k0 + 2p, k0 + 2p + 1
+    }
+    fence_proxy_async_shared();
+    __syncthreads();
+    if (tid == 0) {
+      tma_store_4d(&st_map, (tile % ntx) * 16, 0, 0, tile / ntx, T);
+      bulk_commit();
+    }
+  }
+  if (tid == 0) bulk_wait_all();
+}
+
+// The tensor maps of k_ifft_y_wt: the half spectrum [nzm][nyh][ldxc] of double2 viewed as
+// doubles (x 2 nxm, ky, z; box 16 x nyh) and phi [nzm][nym][ldx] (x nxm, two y dimensions, z).
+static bool ify_tmaps(const Geom &g, int N1, double2 *spec, double *phi, CUtensorMap *ld, CUtensorMap *st) {
+  TmapEncodeFn enc = tmap_encoder();
+  if (!enc || g.nyh > 256) return false;
+  const cuuint32_t estr[4] = {1, 1, 1, 1};
+  const cuuint64_t ldim[3] = {(cuuint64_t)2 * g.nxm, (cuuint64_t)g.nyh, (cuuint64_t)g.nzm};
+  const cuuint64_t lstr[2] = {(cuuint64_t)g.ldxc * sizeof(double2), (cuuint64_t)g.nyh * g.ldxc * sizeof(double2)};
+  const cuuint32_t lbox[3] = {16, (cuuint32_t)g.nyh, 1};
+  const cuuint64_t yb = (cuuint64_t)g.ldx * sizeof(double);  // bytes between y rows of phi
+  const cuuint64_t sdim[4] = {(cuuint64_t)g.nxm, 8, (cuuint64_t)4 * N1, (cuuint64_t)g.nzm};
+  const cuuint64_t sstr[3] = {(cuuint64_t)4 * N1 * yb, yb, (cuuint64_t)g.nym * yb};
+  const cuuint32_t sbox[4] = {16, 8, (cuuint32_t)(4 * N1), 1};
+  return enc(ld, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, spec, ldim, lstr, lbox, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+             CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS &&
+         enc(st, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4, phi, sdim, sstr, sbox, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+             CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
 // ==========================================================================================
@@ -1406,6 +1535,27 @@ static cudaError_t launch_w_n1(const LaunchCtx &L, const SubstepBuffers &b, int 
       cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
       kern<<<grid, 256, sm, L.stream>>>(g, L.t, b.sc, ns, b.vx_o, b.vy_o, b.vz_o, spec, (const C *)L.twy,
                                         b.fft_field);
+    } else if (L.ify_var == 1) {  // tensor copies (FP64 single domain, N <= 384)
+      if constexpr (!std::is_same<TS, double>::value || N1 > 12) {
+        return cudaErrorInvalidValue;
+      } else {
+        if (g.batch) return cudaErrorInvalidValue;
+        constexpr int NH = N / 2 + 1;
+        const size_t hb = (size_t)(NH * 128 + 1023) / 1024 * 1024;
+        const size_t sm6 = 4 * hb + 2 * sizeof(uint64_t) + 1024;  // two tiles of two halves
+        CUtensorMap ld_map, st_map;
+        if (!ify_tmaps(g, N1, spec, (double *)b.phi, &ld_map, &st_map)) return cudaErrorInvalidValue;
+        auto kern = k_ifft_y_wt<N1>;
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm6);
+        if (e != cudaSuccess) return e;
+        int dev = 0, nsm = 148, per = 1;
+        cudaGetDevice(&dev);
+        if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || nsm < 1) nsm = 148;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, 256, sm6) != cudaSuccess || per < 1) per = 1;
+        const int ntiles = ((g.nxm + 15) / 16) * g.nzm;
+        kern<<<std::max(1, std::min(ntiles, nsm * per)), 256, sm6, L.stream>>>(g, ld_map, st_map,
+                                                                              (const double2 *)L.twy, b.err);
+      }
     } else {
       // the staged half spectrum [N/2 + 1][16] is 16 elements larger than the [N][8] tile
       const size_t sm6 = (size_t)(N * 8 + 16) * sizeof(C);

@@ -186,6 +186,9 @@ typedef struct afid_tune_info {
                                    the next tile's copies in flight, 2 the same with the tile
                                    rows moved by bulk copies (FP64 only; 3-D single domains)    */
   double fftz_us[3];            /* microseconds per full forward z launch of each form         */
+  int ify_chosen;               /* inverse y transform: 0 per-thread copies, 1 tensor copies
+                                   (FP64 single domains, nym = 32 x {1,2,3,4,6,8,12})           */
+  double ify_us[2];             /* microseconds per full launch of each form (-1: not run)    */
 } afid_tune_info_t;
 int afid_gpu_autotune(afid_ctx_t *ctx, int force, afid_tune_info_t *info);
 /* Use shape `index` (0 .. ncand-1) from now on without timing, e.g. one saved from an earlier
@@ -198,9 +201,12 @@ int afid_gpu_set_k4_form(afid_ctx_t *ctx, int form);
 /* Use z-transform form `form` (0, 1 or 2 as in afid_tune_info_t.fftz_chosen); bitwise the same.
  * AFID_E_INVALID for form 2 on a mixed-precision context (FP32 spectrum). */
 int afid_gpu_set_fftz_form(afid_ctx_t *ctx, int form);
+/* Use inverse-y-transform form `form` (0 or 1 as in afid_tune_info_t.ify_chosen); bitwise the
+ * same.  AFID_E_INVALID for form 1 where it does not apply (mixed precision, other nym). */
+int afid_gpu_set_ify_form(afid_ctx_t *ctx, int form);
 /* Test hook of the bounded device waits (no counterpart in the reference).  With polls > 0
- * (at most 2^24), the fused explicit/implicit kernel's staging wait (and that of z-transform
- * form 2), after its copies have landed, also waits at most `polls` polls for an mbarrier phase that nothing completes: every
+ * (at most 2^24), the fused explicit/implicit kernel's staging wait (and those of the
+ * tensor-copy transform forms), after its copies have landed, also waits at most `polls` polls for an mbarrier phase that nothing completes: every
  * block gives up, sets the error flag and exits, and the next call that synchronises with the
  * stream (afid_gpu_synchronize, afid_gpu_cfl, afid_gpu_divmax, afid_gpu_globals, ...) returns
  * AFID_E_TIMEOUT.  No fault, no hang; the flag stays set for the life of the context (as the

@@ -72,15 +72,17 @@ def test_bounded_wait_runs_out_in_every_k1_form():
     assert rel_l2(out["vx"], s.vx) < 1e-10
 
 
-def test_bounded_wait_runs_out_in_bulk_z_transform():
-    """The z transforms' bulk-copy form waits on an mbarrier for its rows too: with the hook set
-    its blocks give up, the next synchronising call reports AFID_E_TIMEOUT, and no copy is left
-    in flight (a new context on the same device steps and matches the oracle)."""
-    case = Case(60, 16, 256, rayt=1e6, dt=1e-3)
+def test_bounded_wait_runs_out_in_tensor_copy_transforms():
+    """The tensor-copy forms of the z transforms and of the inverse y transform wait on an
+    mbarrier for their tiles too: with the hook set their blocks give up, the next synchronising
+    call reports AFID_E_TIMEOUT, and no copy is left in flight (a new context on the same device
+    steps and matches the oracle)."""
+    case = Case(60, 64, 256, rayt=1e6, dt=1e-3)
     s = case.oracle_state(random_velocity=0.1)
     with case.solver() as gpu:
         gpu.autotune()
         gpu.set_fftz_form(2)
+        gpu.set_ify_form(1)
         gpu.upload(s.vx, s.vy, s.vz, s.temp, s.pr)
         gpu.set_wait_test(4096)
         with pytest.raises(ag.AfidError) as e:
@@ -90,6 +92,7 @@ def test_bounded_wait_runs_out_in_bulk_z_transform():
     with case.solver() as gpu:
         gpu.autotune()
         gpu.set_fftz_form(2)
+        gpu.set_ify_form(1)
         gpu.upload(s.vx, s.vy, s.vz, s.temp, s.pr)
         gpu.time_marcher(1e-3, 0)
         out = gpu.download()

@@ -222,22 +222,35 @@ def test_launch_count_positive():
                                              ((64, 32, 96), ag.PREC_FP64), ((100, 16, 8), ag.PREC_MIXED),
                                              ((64, 32, 96), ag.PREC_MIXED), ((60, 64, 64), ag.PREC_FP64),
                                              ((60, 64, 64), ag.PREC_MIXED), ((60, 16, 256), ag.PREC_FP64),
-                                             ((36, 8, 384), ag.PREC_FP64), ((64, 8, 512), ag.PREC_FP64)])
+                                             ((36, 8, 384), ag.PREC_FP64), ((64, 8, 512), ag.PREC_FP64),
+                                             ((36, 256, 8), ag.PREC_FP64), ((20, 384, 4), ag.PREC_FP64),
+                                             ((44, 96, 4), ag.PREC_FP64), ((40, 64, 1), ag.PREC_FP64)])
 def test_k4_and_fftz_forms_bitwise_identical(shape, precision):
     """Both forms of the Poisson tridiagonal (a mode per warp; persistent warps with the next
-    mode prefetched) and every form of the z transforms (a tile per block; persistent blocks
-    with the next tile prefetched by per-thread copies, or by bulk row copies with bulk stores,
-    FP64 only) give the same fields bit for bit, so the autotuner's choices change the schedule
-    only.  nxm = 60 and 36 leave a partial tile of x points."""
+    mode prefetched), every form of the z transforms (a tile per block; persistent blocks with
+    the next tile prefetched by per-thread copies, or by tensor copies, FP64 only) and both forms
+    of the inverse y transform (per-thread copies; tensor copies for FP64 single domains with
+    nym = 32 x {1, 2, 3, 4, 6, 8, 12}) give the same fields bit for bit, so the autotuner's
+    choices change the schedule only.  nxm = 60, 36, 20 and 44 leave partial tiles of x points."""
     case = Case(*shape, precision=precision, rayt=1e6, dt=2e-3)
     s = case.oracle_state(random_velocity=0.1)
-    forms = (0, 1, 2) if precision == ag.PREC_FP64 else (0, 1)
+    fp64 = precision == ag.PREC_FP64
+    forms = (0, 1, 2) if fp64 else (0, 1)
+    nym = shape[1]
+    ify_ok = fp64 and nym % 32 == 0 and nym // 32 in (1, 2, 3, 4, 6, 8, 12)
     outs = []
     for form in forms:
         with case.solver() as g:
             g.autotune()
             g.set_k4_form(min(form, 1))
             g.set_fftz_form(form)
+            if ify_ok:
+                g.set_ify_form(min(form, 1))
+            else:
+                with pytest.raises(ag.AfidError) as e:
+                    g.set_ify_form(1)
+                assert e.value.status == ag.AFID_E_INVALID
+                g.set_ify_form(0)
             g.upload(s.vx, s.vy, s.vz, s.temp, s.pr)
             for n in range(2):
                 g.time_marcher(2e-3, n)
