@@ -95,7 +95,8 @@ class TuneInfoT(C.Structure):
                 ("threads", C.c_int * TUNE_MAX), ("rows", C.c_int * TUNE_MAX), ("regcap", C.c_int * TUNE_MAX),
                 ("policy", C.c_int * TUNE_MAX), ("us", C.c_double * TUNE_MAX), ("k4_chosen", C.c_int),
                 ("k4_us", C.c_double * 2), ("fftz_chosen", C.c_int), ("fftz_us", C.c_double * 3),
-                ("ify_chosen", C.c_int), ("ify_us", C.c_double * 2)]
+                ("ify_chosen", C.c_int), ("ify_us", C.c_double * 2),
+                ("div_chosen", C.c_int), ("div_us", C.c_double * 2)]
 
     def as_dict(self) -> dict:
         """shapes: [threads per column, rows per thread, register cap, memory policy,
@@ -105,7 +106,8 @@ class TuneInfoT(C.Structure):
                            for v in range(self.ncand)],
                 "k4": {"chosen": self.k4_chosen, "us": [round(x, 2) for x in self.k4_us]},
                 "fft_z": {"chosen": self.fftz_chosen, "us": [round(x, 2) for x in self.fftz_us]},
-                "ifft_y": {"chosen": self.ify_chosen, "us": [round(x, 2) for x in self.ify_us]}}
+                "ifft_y": {"chosen": self.ify_chosen, "us": [round(x, 2) for x in self.ify_us]},
+                "div_fft_y": {"chosen": self.div_chosen, "us": [round(x, 2) for x in self.div_us]}}
 
 
 class ServeConfigT(C.Structure):
@@ -177,7 +179,7 @@ EXPORTS = [
     "afid_serve_create", "afid_serve_destroy", "afid_serve_submit", "afid_serve_pump", "afid_serve_poll",
     "afid_serve_cancel",
     "afid_serve_status", "afid_serve_now", "afid_serve_set_fail_test", "afid_gpu_autotune", "afid_batch_autotune", "afid_batch_set_k1_shape",
-    "afid_gpu_set_k1_shape", "afid_gpu_set_k4_form", "afid_gpu_set_fftz_form", "afid_gpu_set_ify_form", "afid_gpu_set_wait_test", "afid_gpu_mean_profiles", "afid_batch_mean_profiles",
+    "afid_gpu_set_k1_shape", "afid_gpu_set_k4_form", "afid_gpu_set_fftz_form", "afid_gpu_set_ify_form", "afid_gpu_set_div_form", "afid_gpu_set_wait_test", "afid_gpu_mean_profiles", "afid_batch_mean_profiles",
     "afid_batch_divmax", "afid_gpu_spectra_reset", "afid_gpu_spectra_update", "afid_gpu_spectra_read", "afid_gpu_slice",
     "afid_mgrd_create", "afid_mgrd_destroy", "afid_mgrd_view", "afid_mgrd_fast", "afid_mgrd_array",
     "afid_initial_salinity", "afid_gpu_sal_create", "afid_gpu_sal_upload", "afid_gpu_sal_download",
@@ -268,6 +270,7 @@ def load_library(path: str = _LIB_PATH) -> C.CDLL:
         "afid_gpu_set_k4_form": (i, [vp, i]),
         "afid_gpu_set_fftz_form": (i, [vp, i]),
         "afid_gpu_set_ify_form": (i, [vp, i]),
+        "afid_gpu_set_div_form": (i, [vp, i]),
         "afid_gpu_set_wait_test": (i, [vp, C.c_longlong]),
         "afid_gpu_mean_profiles": (i, [vp, _dp]),
         "afid_gpu_spectra_reset": (i, [vp]),
@@ -653,6 +656,9 @@ class Solver:
 
     def set_ify_form(self, form: int) -> None:
         _check(lib().afid_gpu_set_ify_form(self._h, form), "afid_gpu_set_ify_form")
+
+    def set_div_form(self, form: int) -> None:
+        _check(lib().afid_gpu_set_div_form(self._h, form), "afid_gpu_set_div_form")
 
     def set_wait_test(self, polls: int) -> None:
         """Test hook: make the bounded staging wait run out after `polls` polls (0 = off)."""

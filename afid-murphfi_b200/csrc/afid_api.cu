@@ -532,6 +532,7 @@ int ctx_create(const afid_grid_t *grid, const afid_params_t *prm, const BatchSpe
   L.k4_var = 0;
   L.fftz_var = 0;
   L.ify_var = 0;
+  L.div_var = 0;
   L.plan_y = py;
   L.plan_z = pz;
   L.twy = twy;
@@ -720,6 +721,40 @@ int ctx_autotune(afid_ctx_t *ctx, bool force) {
     if (info.ify_us[1] >= 0.0 && info.ify_us[1] < info.ify_us[0]) info.ify_chosen = 1;
   }
   ctx->L.ify_var = info.ify_chosen;
+  // The divergence + forward y transform (FP64 single domains): per-thread loads or tensor
+  // copies, timed on full launches (the spectrum is dead here: K2 rewrites it).
+  info.div_chosen = 0;
+  info.div_us[0] = info.div_us[1] = -1.0;
+  if (!ctx->L.mixed && !ctx->L.g.batch && ctx->L.warp_fft) {
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    cudaError_t e = cudaEventCreate(&e0);
+    if (e == cudaSuccess) e = cudaEventCreate(&e1);
+    SubstepBuffers b = buffers(ctx);
+    LaunchCtx L2 = ctx->L;
+    constexpr int kReps = 3;
+    for (int round = 0; round < 2 && e == cudaSuccess; ++round)
+      for (int v = 0; v < 2 && e == cudaSuccess; ++v) {
+        L2.div_var = v;
+        if (launch_stage(L2, b, 0, Stage::DivFftY) != cudaSuccess) {  // this form does not apply: skip it
+          cudaGetLastError();
+          continue;
+        }
+        cudaEventRecord(e0, ctx->stream);
+        for (int r = 0; r < kReps && e == cudaSuccess; ++r) e = launch_stage(L2, b, 0, Stage::DivFftY);
+        cudaEventRecord(e1, ctx->stream);
+        if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+        float ms = 0.f;
+        if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+        ctx->launches += 1 + kReps;
+        const double us = 1e3 * ms / kReps;
+        if (e == cudaSuccess && (info.div_us[v] < 0.0 || us < info.div_us[v])) info.div_us[v] = us;
+      }
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    if (e != cudaSuccess) return fail_cuda(ctx, e);
+    if (info.div_us[1] >= 0.0 && info.div_us[1] < info.div_us[0]) info.div_chosen = 1;
+  }
+  ctx->L.div_var = info.div_chosen;
   ctx->tune = info;
   ctx->tuned = true;
   return check_err_flag(ctx);
@@ -1009,6 +1044,16 @@ int afid_gpu_set_ify_form(afid_ctx_t *ctx, int form) {
   if (form == 1 && (ctx->L.mixed || ctx->L.g.batch || !ctx->L.warp_fft || !fits)) return AFID_E_INVALID;
   ctx->L.ify_var = form;
   ctx->tune.ify_chosen = form;
+  return AFID_OK;
+}
+
+int afid_gpu_set_div_form(afid_ctx_t *ctx, int form) {
+  if (!ctx || form < 0 || form > 1) return AFID_E_INVALID;
+  // the tensor-copy form: FP64 single domains whose y transform is a warp FFT (nym = 32 x N1)
+  if (form == 1 && (ctx->L.mixed || ctx->L.g.batch || !ctx->L.warp_fft || ctx->L.g.nym % 32 != 0))
+    return AFID_E_INVALID;
+  ctx->L.div_var = form;
+  ctx->tune.div_chosen = form;
   return AFID_OK;
 }
 

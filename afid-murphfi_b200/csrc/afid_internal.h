@@ -22,6 +22,8 @@ struct LaunchCtx {
   int fftz_var;    // z transforms (K3/K5): 0 a tile a block, 1 persistent with the next tile
                    // prefetched, 2 the same with tensor copies (FP64)
   int ify_var;     // inverse y transform (K6): 0 per-thread copies, 1 tensor copies (FP64 single domain)
+  int div_var;     // divergence + forward y transform (K2): 0 per-thread loads, 1 tensor copies (FP64
+                   // single domain)
   FftPlan plan_y, plan_z;
   const void *twy, *twz;  // twiddle tables (double2 or float2)
 };

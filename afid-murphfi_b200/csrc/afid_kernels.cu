@@ -771,6 +771,163 @@ __global__ void __launch_bounds__(256)
   }
 }
 
+// 3-D and 4-D tiled tensor copies (no multicast): global -> shared completing on an mbarrier,
+// and shared -> global in the issuing thread's bulk group.  `map` is a __grid_constant__ kernel
+// parameter; the innermost coordinate must be a multiple of 16 bytes.
+__device__ __forceinline__ void tma_load_4d(void *dst, const CUtensorMap *map, int c0, int c1, int c2, int c3,
+                                            uint64_t *bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, "
+      "%5}], [%6];" ::"r"(smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(smem_u32(bar))
+      : "memory");
+}
+__device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, int c0, int c1, int c2, uint64_t *bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
+      "[%5];" ::"r"(smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(smem_u32(bar))
+      : "memory");
+}
+__device__ __forceinline__ void tma_store_4d(const CUtensorMap *map, int c0, int c1, int c2, int c3, const void *src) {
+  asm volatile("cp.async.bulk.tensor.4d.global.shared::cta.tile.bulk_group [%0, {%1, %2, %3, %4}], [%5];" ::"l"(
+                   reinterpret_cast<uint64_t>(map)),
+               "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(smem_u32(src))
+               : "memory");
+}
+
+// K2w, tensor-copy persistent form (FP64, single domain): the same divergence and y r2c transform
+// of 16 x points at one z index (a tile), with the velocity rows staged by tiled TMA loads in
+// chunks of 32 rows (vx with the 17th x point, vy with the row after the chunk, vz at i and at
+// i + 1) instead of per-thread global loads, whose latency bounds k_div_fft_y_w.  Each block walks
+// tiles blockIdx.x, + gridDim.x, ... as one stream of chunks with two in flight, so the next
+// tile's first chunks load while the current tile is transformed and stored.  The divergence's
+// expression order, the packed tile, the transform and the output are those of k_div_fft_y_w, so
+// the same bits.  The staging wait is bounded (bit 2 of *err, copies drained before the block
+// exits).
+struct DivMaps {
+  CUtensorMap vx, vx2, vy, vyr, vz;  // 16 x 32 swizzled boxes; vx's 17th point; vy's next row
+};
+constexpr int kDivChunk = 32;                           // rows a chunk
+constexpr uint32_t kDivChunkTx = 4 * 4096 + 512 + 128;  // bytes a chunk brings
+constexpr int kDivChunkBytes = 17408;                   // a chunk buffer, 1024-aligned
+
+template <int N1>
+__global__ void __launch_bounds__(256, (N1 <= 8) ? 3 : (N1 <= 16) ? 2 : 1)
+    k_div_fft_y_wt(Geom g, Tables t, const StepCoef *__restrict__ sc_all, int ns, const __grid_constant__ DivMaps mp,
+                   double2 *__restrict__ spec, const double2 *__restrict__ tw, int *__restrict__ err) {
+  constexpr int N = 32 * N1;
+  if (!inst_active(g, 0)) return;  // a single domain stopped by its step control
+  extern __shared__ __align__(1024) unsigned char smem_k2t[];
+  unsigned char *base = smem_k2t + ((1024u - (smem_u32(smem_k2t) & 1023u)) & 1023u);
+  double2 *T = reinterpret_cast<double2 *>(base + 2 * kDivChunkBytes);  // [N][8] swizzled (tsw)
+  uint64_t *bar = reinterpret_cast<uint64_t *>(T + N * 8);
+  const int ntx = (g.nxm + 15) / 16;
+  const int ntiles = ntx * g.nzm;
+  const int mytiles = blockIdx.x < ntiles ? (ntiles - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
+  const int nchunks = mytiles * N1;  // this block's chunk stream
+  const int tid = threadIdx.x;
+  if (tid == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+  auto issue = [&](int sq) {  // thread 0: chunk sq of the stream into buffer sq & 1
+    const int tile = blockIdx.x + (sq / N1) * gridDim.x, c = sq % N1, b = sq & 1;
+    const int k0 = (tile % ntx) * 16, i = tile / ntx, ip = zinc(g, i);
+    unsigned char *cb = base + b * kDivChunkBytes;
+    const int j0 = kDivChunk * c;
+    mbar_arrive_expect_tx(&bar[b], kDivChunkTx);
+    tma_load_3d(cb, &mp.vx, k0, j0, i, &bar[b]);
+    tma_load_3d(cb + 4096, &mp.vy, k0, j0, i, &bar[b]);
+    tma_load_3d(cb + 8192, &mp.vz, k0, j0, i, &bar[b]);
+    tma_load_3d(cb + 12288, &mp.vz, k0, j0, ip, &bar[b]);
+    tma_load_3d(cb + 16384, &mp.vx2, k0 + 16, j0, i, &bar[b]);
+    tma_load_3d(cb + 16896, &mp.vyr, k0, (j0 + kDivChunk) % N, i, &bar[b]);
+  };
+  if (tid == 0) {
+    if (nchunks > 0) issue(0);
+    if (nchunks > 1) issue(1);
+  }
+  const StepCoef sc = sc_all[sc_slot(g, 0, ns)];
+  const double usdtal = 1.0 / (sc.dt * sc.al);
+  const double norm = 1.0 / (nz_norm(g) * (double)g.nym);
+  const int nxm = g.nxm;
+  // thread (jl, q): row jl of each chunk, x points (kk, kk + 1) = (k0 + 2q, k0 + 2q + 1)
+  const int q = tid & 7, jl = tid >> 3;
+  const int lane = tid & 31, p = tid >> 5;
+  for (int lt = 0; lt < mytiles; ++lt) {
+    const int tile = blockIdx.x + lt * gridDim.x;
+    const int k0 = (tile % ntx) * 16, i = tile / ntx;
+    const int kk = k0 + 2 * q;
+    const double2 ux = (kk < nxm) ? __ldg(reinterpret_cast<const double2 *>(t.udx3m + kk)) : make_double2(0.0, 0.0);
+    for (int c = 0; c < N1; ++c) {
+      const int sq = lt * N1 + c, b = sq & 1;
+      const uint32_t par = (uint32_t)(sq >> 1) & 1u;
+      bool ok = mbar_wait(&bar[b], par, kSpinLimit);
+      // test hook: the opposite phase is never completed here, so this wait always runs out
+      if (g.wait_test_polls > 0) ok = ok && mbar_wait(&bar[b], par ^ 1u, g.wait_test_polls);
+      if (!__syncthreads_and(ok)) {
+        if (tid == 0) atomicOr(err, 2);
+        mbar_wait(&bar[b], par, kDrainLimit);  // copies in flight land before the block exits
+        if (sq + 1 < nchunks) mbar_wait(&bar[b ^ 1], (uint32_t)((sq + 1) >> 1) & 1u, kDrainLimit);
+        return;
+      }
+      const unsigned char *cb = base + b * kDivChunkBytes;
+      // 16-byte chunk ch of row r of a swizzled 16 x 32 box at byte offset off
+      auto at = [&](int off, int r, int ch) {
+        return *reinterpret_cast<const double2 *>(cb + off + r * 128 + ((ch ^ (r & 7)) << 4));
+      };
+      double dv0 = 0.0, dv1 = 0.0;
+      if (kk < nxm) {
+        const double2 zi = at(12288, jl, q), zc = at(8192, jl, q);
+        const double2 yj =
+            (jl + 1 < kDivChunk) ? at(4096, jl + 1, q) : reinterpret_cast<const double2 *>(cb + 16896)[q];
+        const double2 yc = at(4096, jl, q);
+        const double2 xc = at(0, jl, q);
+        dv0 = ((zi.x - zc.x) * g.dz + (yj.x - yc.x) * g.dy + (xc.y - xc.x) * ux.x) * usdtal;
+        if (kk + 1 < nxm) {
+          const double x2 = (q < 7) ? at(0, jl, q + 1).x : reinterpret_cast<const double2 *>(cb + 16384)[jl].x;
+          dv1 = ((zi.y - zc.y) * g.dz + (yj.y - yc.y) * g.dy + (x2 - xc.y) * ux.y) * usdtal;
+        }
+      }
+      T[tsw(kDivChunk * c + jl, q)] = make_double2(dv0, dv1);
+      __syncthreads();  // chunk buffer b is free again
+      if (tid == 0 && sq + 2 < nchunks) issue(sq + 2);
+    }
+    double2 x[N1];
+#pragma unroll
+    for (int m = 0; m < N1; ++m) x[m] = T[tsw(lane + 32 * m, p)];
+    warp_fft<false, double, N1>(x, lane, tw);
+    __syncthreads();
+    const int rl = bitrev5(lane);
+#pragma unroll
+    for (int k1 = 0; k1 < N1; ++k1) T[tsw(k1 + N1 * rl, p)] = x[k1];
+    __syncthreads();
+    for (int e = tid; e < g.nyh * 16; e += blockDim.x) {
+      const int ex = e & 15, ky = e >> 4;
+      const int kx = k0 + ex;
+      if (kx >= nxm) continue;
+      const int qq = ex >> 1;
+      const double2 zk = T[tsw(ky, qq)];
+      const double2 zn = T[tsw(ky == 0 ? 0 : N - ky, qq)];
+      double2 X;
+      if ((ex & 1) == 0) {
+        X.x = (zk.x + zn.x) * 0.5;
+        X.y = (zk.y - zn.y) * 0.5;
+      } else {
+        X.x = (zk.y + zn.y) * 0.5;
+        X.y = (zn.x - zk.x) * 0.5;
+      }
+      X.x *= norm;
+      X.y *= norm;
+      spec[(size_t)(ky + (size_t)g.nyh * i) * g.ldxc + kx] = X;
+    }
+    __syncthreads();  // the tile is read out before the next tile's divergence overwrites it
+  }
+}
+
 // K3w / K5w: z c2c in place.  Block: 8 x points (8 warps) at one ky.
 template <int N1, bool INV, typename TS>
 __global__ void __launch_bounds__(256)
@@ -898,31 +1055,6 @@ __global__ void __launch_bounds__(256)
 template <int N1>
 __device__ __forceinline__ int zslot(int k1, int rl) {
   return ((rl >> 2) & 7) + 8 * (k1 + N1 * (rl & 3));
-}
-
-// 4-D tiled tensor copies (no multicast): global -> shared completing on an mbarrier, and
-// shared -> global in the issuing thread's bulk group.  `map` is a __grid_constant__ kernel
-// parameter; the innermost coordinate must be a multiple of 16 bytes.
-__device__ __forceinline__ void tma_load_4d(void *dst, const CUtensorMap *map, int c0, int c1, int c2, int c3,
-                                            uint64_t *bar) {
-  asm volatile(
-      "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, "
-      "%5}], [%6];" ::"r"(smem_u32(dst)),
-      "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(smem_u32(bar))
-      : "memory");
-}
-__device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, int c0, int c1, int c2, uint64_t *bar) {
-  asm volatile(
-      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
-      "[%5];" ::"r"(smem_u32(dst)),
-      "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(smem_u32(bar))
-      : "memory");
-}
-__device__ __forceinline__ void tma_store_4d(const CUtensorMap *map, int c0, int c1, int c2, int c3, const void *src) {
-  asm volatile("cp.async.bulk.tensor.4d.global.shared::cta.tile.bulk_group [%0, {%1, %2, %3, %4}], [%5];" ::"l"(
-                   reinterpret_cast<uint64_t>(map)),
-               "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(smem_u32(src))
-               : "memory");
 }
 
 // K3w / K5w, tensor-copy persistent form (FP64 spectrum): a tile (8 x points at one ky, all nzm
@@ -1519,6 +1651,28 @@ static cudaError_t launch_k4_T(const LaunchCtx &L, void *spec, int *err) {
   return cudaErrorInvalidValue;
 }
 
+// The tensor maps of k_div_fft_y_wt over the intermediate velocities [nzm][nym][ldx] (doubles):
+// 16 x 32 swizzled boxes of vx (x extent nx, so its 17th point is the wall value at nxm), vy and
+// vz (x extent nxm), two x points of vx past the tile, and one unswizzled row of vy.
+static bool div_tmaps(const Geom &g, const double *vx, const double *vy, const double *vz, DivMaps *m) {
+  TmapEncodeFn enc = tmap_encoder();
+  if (!enc || g.nym < kDivChunk) return false;
+  const cuuint32_t estr[3] = {1, 1, 1};
+  const cuuint64_t yb = (cuuint64_t)g.ldx * sizeof(double);
+  const cuuint64_t str[2] = {yb, (cuuint64_t)g.nym * yb};
+  const cuuint64_t dimx[3] = {(cuuint64_t)g.nx, (cuuint64_t)g.nym, (cuuint64_t)g.nzm};
+  const cuuint64_t dimm[3] = {(cuuint64_t)g.nxm, (cuuint64_t)g.nym, (cuuint64_t)g.nzm};
+  const cuuint32_t box[3] = {16, (cuuint32_t)kDivChunk, 1}, box2[3] = {2, (cuuint32_t)kDivChunk, 1},
+                   boxr[3] = {16, 1, 1};
+  auto one = [&](CUtensorMap *t, const double *f, const cuuint64_t *dim, const cuuint32_t *bx, bool swz) {
+    return enc(t, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, const_cast<double *>(f), dim, str, bx, estr,
+               CU_TENSOR_MAP_INTERLEAVE_NONE, swz ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_NONE,
+               CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+  };
+  return one(&m->vx, vx, dimx, box, true) && one(&m->vx2, vx, dimx, box2, false) && one(&m->vy, vy, dimm, box, true) &&
+         one(&m->vyr, vy, dimm, boxr, false) && one(&m->vz, vz, dimm, box, true);
+}
+
 // Launch helpers for the warp-FFT kernels: 8 warps per block, a [N][8] complex tile each
 // (y transforms: 16 x points as 8 pairs; z transforms: 8 x points).
 template <typename TS, int N1>
@@ -1530,7 +1684,27 @@ static cudaError_t launch_w_n1(const LaunchCtx &L, const SubstepBuffers &b, int 
   if (st == Stage::DivFftY || st == Stage::IfftY) {
     const size_t sm = (size_t)N * 8 * sizeof(C);
     dim3 grid((g.nxm + 15) / 16, g.nzm);
-    if (st == Stage::DivFftY) {
+    if (st == Stage::DivFftY && L.div_var == 1) {  // tensor copies (FP64 single domain)
+      if constexpr (!std::is_same<TS, double>::value) {
+        return cudaErrorInvalidValue;
+      } else {
+        if (g.batch || b.fft_field) return cudaErrorInvalidValue;
+        const size_t sm2 = 1024 + 2 * (size_t)kDivChunkBytes + (size_t)N * 8 * sizeof(double2) + 2 * sizeof(uint64_t);
+        if (sm2 > (size_t)227 * 1024) return cudaErrorInvalidValue;
+        DivMaps mp;
+        if (!div_tmaps(g, b.vx_o, b.vy_o, b.vz_o, &mp)) return cudaErrorInvalidValue;
+        auto kern = k_div_fft_y_wt<N1>;
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2);
+        if (e != cudaSuccess) return e;
+        int dev = 0, nsm = 148, per = 1;
+        cudaGetDevice(&dev);
+        if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || nsm < 1) nsm = 148;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, 256, sm2) != cudaSuccess || per < 1) per = 1;
+        const int ntiles = ((g.nxm + 15) / 16) * g.nzm;
+        kern<<<std::max(1, std::min(ntiles, nsm * per)), 256, sm2, L.stream>>>(g, L.t, b.sc, ns, mp, spec,
+                                                                              (const double2 *)L.twy, b.err);
+      }
+    } else if (st == Stage::DivFftY) {
       auto kern = k_div_fft_y_w<N1, TS>;
       cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
       kern<<<grid, 256, sm, L.stream>>>(g, L.t, b.sc, ns, b.vx_o, b.vy_o, b.vz_o, spec, (const C *)L.twy,

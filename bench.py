@@ -231,6 +231,8 @@ def run_gpu(args):
             solver.set_fftz_form(args.fftz_form)
         if args.ify_form >= 0:
             solver.set_ify_form(args.ify_form)
+        if args.div_form >= 0:
+            solver.set_div_form(args.div_form)
     temp0 = tables.initial_temperature(20261203)
     nx, nym, nzm = w["nxm"] + 1, w["nym"], w["nzm"]
     zeros = np.zeros((nzm, nym, nx))
@@ -1253,6 +1255,7 @@ def main():
     ap.add_argument("--k4-form", type=int, default=-1, help="with --k1-shape: fixed Poisson tridiagonal form")
     ap.add_argument("--fftz-form", type=int, default=-1, help="with --k1-shape: fixed z-transform form")
     ap.add_argument("--ify-form", type=int, default=-1, help="with --k1-shape: fixed inverse-y-transform form")
+    ap.add_argument("--div-form", type=int, default=-1, help="with --k1-shape: fixed divergence + y-transform form")
     ap.add_argument("--jobs", type=int, default=100, help="served: number of jobs")
     ap.add_argument("--rate", type=float, default=50.0,
                     help="served: Poisson arrival rate per second (50 = the benchmark's stream, ~16x capacity; "

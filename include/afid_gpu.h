@@ -189,6 +189,9 @@ typedef struct afid_tune_info {
   int ify_chosen;               /* inverse y transform: 0 per-thread copies, 1 tensor copies
                                    (FP64 single domains, nym = 32 x {1,2,3,4,6,8,12})           */
   double ify_us[2];             /* microseconds per full launch of each form (-1: not run)    */
+  int div_chosen;               /* divergence + forward y transform: 0 per-thread loads, 1
+                                   tensor copies of the velocity rows (FP64 single domains)      */
+  double div_us[2];             /* microseconds per full launch of each form (-1: not run)    */
 } afid_tune_info_t;
 int afid_gpu_autotune(afid_ctx_t *ctx, int force, afid_tune_info_t *info);
 /* Use shape `index` (0 .. ncand-1) from now on without timing, e.g. one saved from an earlier
@@ -204,6 +207,9 @@ int afid_gpu_set_fftz_form(afid_ctx_t *ctx, int form);
 /* Use inverse-y-transform form `form` (0 or 1 as in afid_tune_info_t.ify_chosen); bitwise the
  * same.  AFID_E_INVALID for form 1 where it does not apply (mixed precision, other nym). */
 int afid_gpu_set_ify_form(afid_ctx_t *ctx, int form);
+/* Use divergence + forward-y-transform form `form` (0 or 1 as in afid_tune_info_t.div_chosen);
+ * bitwise the same.  AFID_E_INVALID for form 1 where it does not apply (mixed precision). */
+int afid_gpu_set_div_form(afid_ctx_t *ctx, int form);
 /* Test hook of the bounded device waits (no counterpart in the reference).  With polls > 0
  * (at most 2^24), the fused explicit/implicit kernel's staging wait (and those of the
  * tensor-copy transform forms), after its copies have landed, also waits at most `polls` polls for an mbarrier phase that nothing completes: every

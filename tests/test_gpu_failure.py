@@ -73,8 +73,8 @@ def test_bounded_wait_runs_out_in_every_k1_form():
 
 
 def test_bounded_wait_runs_out_in_tensor_copy_transforms():
-    """The tensor-copy forms of the z transforms and of the inverse y transform wait on an
-    mbarrier for their tiles too: with the hook set their blocks give up, the next synchronising
+    """The tensor-copy forms of the z transforms and of both y transforms wait on an mbarrier
+    for their tiles too: with the hook set their blocks give up, the next synchronising
     call reports AFID_E_TIMEOUT, and no copy is left in flight (a new context on the same device
     steps and matches the oracle)."""
     case = Case(60, 64, 256, rayt=1e6, dt=1e-3)
@@ -83,6 +83,7 @@ def test_bounded_wait_runs_out_in_tensor_copy_transforms():
         gpu.autotune()
         gpu.set_fftz_form(2)
         gpu.set_ify_form(1)
+        gpu.set_div_form(1)
         gpu.upload(s.vx, s.vy, s.vz, s.temp, s.pr)
         gpu.set_wait_test(4096)
         with pytest.raises(ag.AfidError) as e:
@@ -93,6 +94,7 @@ def test_bounded_wait_runs_out_in_tensor_copy_transforms():
         gpu.autotune()
         gpu.set_fftz_form(2)
         gpu.set_ify_form(1)
+        gpu.set_div_form(1)
         gpu.upload(s.vx, s.vy, s.vz, s.temp, s.pr)
         gpu.time_marcher(1e-3, 0)
         out = gpu.download()

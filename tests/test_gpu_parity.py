@@ -230,7 +230,8 @@ def test_k4_and_fftz_forms_bitwise_identical(shape, precision):
     mode prefetched), every form of the z transforms (a tile per block; persistent blocks with
     the next tile prefetched by per-thread copies, or by tensor copies, FP64 only) and both forms
     of the inverse y transform (per-thread copies; tensor copies for FP64 single domains with
-    nym = 32 x {1, 2, 3, 4, 6, 8, 12}) give the same fields bit for bit, so the autotuner's
+    nym = 32 x {1, 2, 3, 4, 6, 8, 12}) and of the divergence + forward y transform (per-thread
+    loads; tensor copies of the velocity rows) give the same fields bit for bit, so the autotuner's
     choices change the schedule only.  nxm = 60, 36, 20 and 44 leave partial tiles of x points."""
     case = Case(*shape, precision=precision, rayt=1e6, dt=2e-3)
     s = case.oracle_state(random_velocity=0.1)
@@ -251,6 +252,12 @@ def test_k4_and_fftz_forms_bitwise_identical(shape, precision):
                     g.set_ify_form(1)
                 assert e.value.status == ag.AFID_E_INVALID
                 g.set_ify_form(0)
+            if fp64 and nym % 32 == 0:
+                g.set_div_form(min(form, 1))
+            else:
+                with pytest.raises(ag.AfidError) as e:
+                    g.set_div_form(1)
+                assert e.value.status == ag.AFID_E_INVALID
             g.upload(s.vx, s.vy, s.vz, s.temp, s.pr)
             for n in range(2):
                 g.time_marcher(2e-3, n)

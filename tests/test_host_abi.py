@@ -38,7 +38,7 @@ def test_tuning_setters_refuse_null_handles():
     """The autotuner overrides check their handle before any CUDA call (no GPU needed)."""
     lib = ag.lib()
     for fn in ("afid_gpu_set_k1_shape", "afid_gpu_set_k4_form", "afid_gpu_set_fftz_form", "afid_gpu_set_ify_form",
-               "afid_batch_set_k1_shape"):
+               "afid_gpu_set_div_form", "afid_batch_set_k1_shape"):
         assert getattr(lib, fn)(None, 0) == ag.AFID_E_INVALID, fn
     assert lib.afid_gpu_autotune(None, 0, None) == ag.AFID_E_INVALID
     assert lib.afid_batch_autotune(None, 0, None) == ag.AFID_E_INVALID
