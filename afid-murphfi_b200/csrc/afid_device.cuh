@@ -401,6 +401,54 @@ __device__ __forceinline__ void warp_fft(typename Cplx<T>::type (&x)[N1], int la
   }
 }
 
+// The lane-dependent twiddles of warp_fft for N = 32 N1 as a shared table [N1 + 4][32]: rows
+// k1 - 1 = 0 .. N1 - 2 hold w_N^(lane k1), rows N1 - 1 .. N1 + 3 the five radix-2 stage factors,
+// so a warp reads 32 consecutive entries (free of bank conflicts) instead of scattered global
+// loads.  Filled by the whole block from the global table (the same values, so the same bits);
+// the caller synchronises before use.
+template <typename T, int N1>
+__device__ __forceinline__ void fill_lane_twiddles(typename Cplx<T>::type *stw,
+                                                   const typename Cplx<T>::type *__restrict__ tw) {
+  for (int e = threadIdx.x; e < (N1 + 4) * 32; e += blockDim.x) {
+    const int row = e >> 5, lane = e & 31;
+    int m;
+    if (row < N1 - 1) {
+      m = lane * (row + 1);
+    } else {
+      const int h = 16 >> (row - (N1 - 1));
+      m = ((lane & (h - 1)) * (16 / h)) * N1;
+    }
+    stw[e] = tw[m];
+  }
+}
+
+// warp_fft with the lane-dependent twiddles read from a fill_lane_twiddles table.
+template <bool INV, typename T, int N1>
+__device__ __forceinline__ void warp_fft_lt(typename Cplx<T>::type (&x)[N1], int lane,
+                                            const typename Cplx<T>::type *__restrict__ tw,
+                                            const typename Cplx<T>::type *stw) {
+  using C = typename Cplx<T>::type;
+  reg_fft_rec<INV, T, N1, 0, 1>(x, tw);
+#pragma unroll
+  for (int k1 = 1; k1 < N1; ++k1)
+    if (lane != 0) x[k1] = cmul(x[k1], twiddle<INV, T>(stw, (k1 - 1) * 32 + lane));
+  C w5[5];
+#pragma unroll
+  for (int s = 0; s < 5; ++s) w5[s] = twiddle<INV, T>(stw, (N1 - 1 + s) * 32 + lane);
+#pragma unroll
+  for (int s = 0; s < 5; ++s) {
+    const int h = 16 >> s;
+    const bool bottom = (lane & h) != 0;
+#pragma unroll
+    for (int q = 0; q < N1; ++q) {
+      C o;
+      o.x = __shfl_xor_sync(0xffffffffu, x[q].x, h);
+      o.y = __shfl_xor_sync(0xffffffffu, x[q].y, h);
+      x[q] = bottom ? cmul(csub(o, x[q]), w5[s]) : cadd(x[q], o);
+    }
+  }
+}
+
 // ------------------------------------------------------------------------------------------
 // Bounded device-side waits: every spin in this library counts iterations and gives up with
 // an error flag instead of hanging (no trap, no unbounded loop).  A wait that gave up drains

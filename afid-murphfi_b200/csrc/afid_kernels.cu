@@ -771,6 +771,16 @@ __global__ void __launch_bounds__(256)
   }
 }
 
+// Whether a tensor-copy kernel of `bytes` dynamic shared memory a block keeps its blocks per SM
+// when the lane-twiddle table (`table` bytes) is added (228 KB an SM, 1 KB reserved a block).
+__host__ __device__ constexpr bool lane_table_fits(size_t bytes, size_t table) {
+  return bytes + table <= 227 * 1024 && (228 * 1024) / (bytes + table + 1024) >= (228 * 1024) / (bytes + 1024);
+}
+template <int N1>
+__host__ __device__ constexpr size_t lane_table_bytes() {
+  return (size_t)(N1 + 4) * 32 * sizeof(double2);
+}
+
 // 3-D and 4-D tiled tensor copies (no multicast): global -> shared completing on an mbarrier,
 // and shared -> global in the issuing thread's bulk group.  `map` is a __grid_constant__ kernel
 // parameter; the innermost coordinate must be a multiple of 16 bytes.
@@ -822,6 +832,9 @@ __global__ void __launch_bounds__(256, (N1 <= 8) ? 3 : (N1 <= 16) ? 2 : 1)
   unsigned char *base = smem_k2t + ((1024u - (smem_u32(smem_k2t) & 1023u)) & 1023u);
   double2 *T = reinterpret_cast<double2 *>(base + 2 * kDivChunkBytes);  // [N][8] swizzled (tsw)
   uint64_t *bar = reinterpret_cast<uint64_t *>(T + N * 8);
+  constexpr bool LT = lane_table_fits(1024 + 2 * kDivChunkBytes + N * 128 + 16, lane_table_bytes<N1>());
+  double2 *stw = reinterpret_cast<double2 *>(bar + 2);  // lane twiddles (when LT)
+  if constexpr (LT) fill_lane_twiddles<double, N1>(stw, tw);
   const int ntx = (g.nxm + 15) / 16;
   const int ntiles = ntx * g.nzm;
   const int mytiles = blockIdx.x < ntiles ? (ntiles - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
@@ -899,7 +912,10 @@ __global__ void __launch_bounds__(256, (N1 <= 8) ? 3 : (N1 <= 16) ? 2 : 1)
     double2 x[N1];
 #pragma unroll
     for (int m = 0; m < N1; ++m) x[m] = T[tsw(lane + 32 * m, p)];
-    warp_fft<false, double, N1>(x, lane, tw);
+    if constexpr (LT)
+      warp_fft_lt<false, double, N1>(x, lane, tw, stw);
+    else
+      warp_fft<false, double, N1>(x, lane, tw);
     __syncthreads();
     const int rl = bitrev5(lane);
 #pragma unroll
@@ -1078,6 +1094,9 @@ __global__ void __launch_bounds__(256)
   unsigned char *base = smem_k3t + ((1024u - (smem_u32(smem_k3t) & 1023u)) & 1023u);
   double2 *sb = reinterpret_cast<double2 *>(base);  // [2][N][8]
   uint64_t *bar = reinterpret_cast<uint64_t *>(sb + 2 * N * 8);
+  constexpr bool LT = lane_table_fits(2 * N * 128 + 16 + 1024, lane_table_bytes<N1>());
+  double2 *stw = reinterpret_cast<double2 *>(bar + 2);  // lane twiddles (when LT)
+  if constexpr (LT) fill_lane_twiddles<double, N1>(stw, tw);
   const int ntx = (g.nxm + 7) / 8;
   const int ntiles = ntx * g.nyh;
   const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
@@ -1120,7 +1139,10 @@ __global__ void __launch_bounds__(256)
       x[m] = s[r * 8 + (w ^ (r & 7))];
     }
     __syncwarp();
-    warp_fft<INV, double, N1>(x, lane, tw);
+    if constexpr (LT)
+      warp_fft_lt<INV, double, N1>(x, lane, tw, stw);
+    else
+      warp_fft<INV, double, N1>(x, lane, tw);
     const int rl = bitrev5(lane);
 #pragma unroll
     for (int k1 = 0; k1 < N1; ++k1) {
@@ -1266,6 +1288,9 @@ __global__ void __launch_bounds__(256)
   extern __shared__ __align__(1024) unsigned char smem_k6t[];
   unsigned char *base = smem_k6t + ((1024u - (smem_u32(smem_k6t) & 1023u)) & 1023u);  // [2][2][HB]
   uint64_t *bar = reinterpret_cast<uint64_t *>(base + 4 * HB);
+  constexpr bool LT = lane_table_fits(4 * HB + 16 + 1024, lane_table_bytes<N1>());
+  double2 *stw = reinterpret_cast<double2 *>(bar + 2);  // lane twiddles (when LT)
+  if constexpr (LT) fill_lane_twiddles<double, N1>(stw, tw);
   const int ntx = (g.nxm + 15) / 16;
   const int ntiles = ntx * g.nzm;
   const int tid = threadIdx.x, lane = tid & 31, p = tid >> 5;
@@ -1327,7 +1352,10 @@ __global__ void __launch_bounds__(256)
       x[m].x = X.x - Y.y;
       x[m].y = X.y + Y.x;
     }
-    warp_fft<true, double, N1>(x, lane, tw);
+    if constexpr (LT)
+      warp_fft_lt<true, double, N1>(x, lane, tw, stw);
+    else
+      warp_fft<true, double, N1>(x, lane, tw);
     __syncthreads();  // every warp has read its input before the tile is overwritten
     double2 *T = reinterpret_cast<double2 *>(tb);  // [N][8] output tile
     const int rl = bitrev5(lane);
@@ -1689,7 +1717,8 @@ static cudaError_t launch_w_n1(const LaunchCtx &L, const SubstepBuffers &b, int 
         return cudaErrorInvalidValue;
       } else {
         if (g.batch || b.fft_field) return cudaErrorInvalidValue;
-        const size_t sm2 = 1024 + 2 * (size_t)kDivChunkBytes + (size_t)N * 8 * sizeof(double2) + 2 * sizeof(uint64_t);
+        size_t sm2 = 1024 + 2 * (size_t)kDivChunkBytes + (size_t)N * 8 * sizeof(double2) + 2 * sizeof(uint64_t);
+        if (lane_table_fits(sm2, lane_table_bytes<N1>())) sm2 += lane_table_bytes<N1>();
         if (sm2 > (size_t)227 * 1024) return cudaErrorInvalidValue;
         DivMaps mp;
         if (!div_tmaps(g, b.vx_o, b.vy_o, b.vz_o, &mp)) return cudaErrorInvalidValue;
@@ -1716,7 +1745,8 @@ static cudaError_t launch_w_n1(const LaunchCtx &L, const SubstepBuffers &b, int 
         if (g.batch) return cudaErrorInvalidValue;
         constexpr int NH = N / 2 + 1;
         const size_t hb = (size_t)(NH * 128 + 1023) / 1024 * 1024;
-        const size_t sm6 = 4 * hb + 2 * sizeof(uint64_t) + 1024;  // two tiles of two halves
+        size_t sm6 = 4 * hb + 2 * sizeof(uint64_t) + 1024;  // two tiles of two halves
+        if (lane_table_fits(sm6, lane_table_bytes<N1>())) sm6 += lane_table_bytes<N1>();
         CUtensorMap ld_map, st_map;
         if (!ify_tmaps(g, N1, spec, (double *)b.phi, &ld_map, &st_map)) return cudaErrorInvalidValue;
         auto kern = k_ifft_y_wt<N1>;
@@ -1745,7 +1775,8 @@ static cudaError_t launch_w_n1(const LaunchCtx &L, const SubstepBuffers &b, int 
       return cudaErrorInvalidValue;
     } else {
       // two 1024-byte aligned tiles of N x 128 bytes, the barriers, the alignment slack
-      const size_t smb = (size_t)2 * N * 8 * sizeof(double2) + 2 * sizeof(uint64_t) + 1024;
+      size_t smb = (size_t)2 * N * 8 * sizeof(double2) + 2 * sizeof(uint64_t) + 1024;
+      if (lane_table_fits(smb, lane_table_bytes<N1>())) smb += lane_table_bytes<N1>();
       if (smb > (size_t)227 * 1024 || 4 * N1 > 256) return cudaErrorInvalidValue;  // two tiles do not fit
       CUtensorMap ld_map, st_map;
       if (!fftz_tmaps(g, N1, spec, &ld_map, &st_map)) return cudaErrorInvalidValue;
