@@ -422,6 +422,16 @@ __device__ __forceinline__ void fill_lane_twiddles(typename Cplx<T>::type *stw,
   }
 }
 
+// Bytes of that table, and whether a kernel of `bytes` dynamic shared memory a block keeps its
+// blocks per SM (228 KB an SM, 1 KB reserved a block; at most 227 KB a block) with it added.
+template <int N1, typename C = double2>
+__host__ __device__ constexpr size_t lane_table_bytes() {
+  return (size_t)(N1 + 4) * 32 * sizeof(C);
+}
+__host__ __device__ constexpr bool lane_table_fits(size_t bytes, size_t table) {
+  return bytes + table <= 227 * 1024 && (228 * 1024) / (bytes + table + 1024) >= (228 * 1024) / (bytes + 1024);
+}
+
 // warp_fft with the lane-dependent twiddles read from a fill_lane_twiddles table.
 template <bool INV, typename T, int N1>
 __device__ __forceinline__ void warp_fft_lt(typename Cplx<T>::type (&x)[N1], int lane,

@@ -698,9 +698,12 @@ __global__ void __launch_bounds__(256)
   extern __shared__ __align__(16) unsigned char smem_k2w[];
   C *T = reinterpret_cast<C *>(smem_k2w);  // [N][8] swizzled
   TS *Tr = reinterpret_cast<TS *>(smem_k2w);
+  constexpr bool LT = lane_table_fits((size_t)N * 8 * sizeof(C), lane_table_bytes<N1, C>());
+  C *stw = T + N * 8;  // lane twiddles (when LT)
   const int k0 = blockIdx.x * 16, i = blockIdx.y;
   Geom g = g0;
   if (!inst_active(g, i)) return;
+  if constexpr (LT) fill_lane_twiddles<TS, N1>(stw, tw);
   bind_instance(g, i);
   const int ip = zinc(g, i);
   const StepCoef sc = sc_all[sc_slot(g, i, ns)];
@@ -742,7 +745,10 @@ __global__ void __launch_bounds__(256)
   C x[N1];
 #pragma unroll
   for (int m = 0; m < N1; ++m) x[m] = T[tsw(lane + 32 * m, p)];
-  warp_fft<false, TS, N1>(x, lane, tw);
+  if constexpr (LT)
+    warp_fft_lt<false, TS, N1>(x, lane, tw, stw);
+  else
+    warp_fft<false, TS, N1>(x, lane, tw);
   __syncthreads();
   const int rl = bitrev5(lane);
 #pragma unroll
@@ -769,16 +775,6 @@ __global__ void __launch_bounds__(256)
     X.y *= norm;
     spec[(size_t)(ky + (size_t)g.nyh * i) * g.ldxc + kk] = X;
   }
-}
-
-// Whether a tensor-copy kernel of `bytes` dynamic shared memory a block keeps its blocks per SM
-// when the lane-twiddle table (`table` bytes) is added (228 KB an SM, 1 KB reserved a block).
-__host__ __device__ constexpr bool lane_table_fits(size_t bytes, size_t table) {
-  return bytes + table <= 227 * 1024 && (228 * 1024) / (bytes + table + 1024) >= (228 * 1024) / (bytes + 1024);
-}
-template <int N1>
-__host__ __device__ constexpr size_t lane_table_bytes() {
-  return (size_t)(N1 + 4) * 32 * sizeof(double2);
 }
 
 // 3-D and 4-D tiled tensor copies (no multicast): global -> shared completing on an mbarrier,
@@ -953,6 +949,9 @@ __global__ void __launch_bounds__(256)
   constexpr int N = 32 * N1;
   extern __shared__ __align__(16) unsigned char smem_k3w[];
   C *s = reinterpret_cast<C *>(smem_k3w);  // [N][8], swizzled columns
+  constexpr bool LT = lane_table_fits((size_t)N * 8 * sizeof(C), lane_table_bytes<N1, C>());
+  C *stw = s + N * 8;  // lane twiddles (when LT)
+  if constexpr (LT) fill_lane_twiddles<TS, N1>(stw, tw);
   const int k0 = blockIdx.x * 8, ky = blockIdx.y;
   const size_t zstride = (size_t)g.nyh * g.ldxc;
   C *base = spec + (size_t)ky * g.ldxc + k0;
@@ -977,7 +976,10 @@ __global__ void __launch_bounds__(256)
     const int r = lane + 32 * m;
     x[m] = s[r * 8 + (w ^ zsw(r))];
   }
-  warp_fft<INV, TS, N1>(x, lane, tw);
+  if constexpr (LT)
+    warp_fft_lt<INV, TS, N1>(x, lane, tw, stw);
+  else
+    warp_fft<INV, TS, N1>(x, lane, tw);
   __syncthreads();
   const int rl = bitrev5(lane);
 #pragma unroll
@@ -1004,6 +1006,9 @@ __global__ void __launch_bounds__(256)
   constexpr int N = 32 * N1;
   extern __shared__ __align__(16) unsigned char smem_k3p[];
   C *sb = reinterpret_cast<C *>(smem_k3p);  // [2][N][8], swizzled columns
+  constexpr bool LT = lane_table_fits((size_t)2 * N * 8 * sizeof(C), lane_table_bytes<N1, C>());
+  C *stw = sb + 2 * N * 8;  // lane twiddles (when LT)
+  if constexpr (LT) fill_lane_twiddles<TS, N1>(stw, tw);
   const size_t zstride = (size_t)g.nyh * g.ldxc;
   const int ntx = (g.nxm + 7) / 8;
   const int ntiles = ntx * g.nyh;
@@ -1041,7 +1046,10 @@ __global__ void __launch_bounds__(256)
       const int r = lane + 32 * m;
       x[m] = s[r * 8 + (w ^ zsw(r))];
     }
-    warp_fft<INV, TS, N1>(x, lane, tw);
+    if constexpr (LT)
+      warp_fft_lt<INV, TS, N1>(x, lane, tw, stw);
+    else
+      warp_fft<INV, TS, N1>(x, lane, tw);
     __syncthreads();
     const int rl = bitrev5(lane);
 #pragma unroll
@@ -1210,8 +1218,11 @@ __global__ void __launch_bounds__(256)
   C *T = reinterpret_cast<C *>(smem_k6w);  // [N][8] swizzled (output transposition)
   C *R = T;                                 // [NH][16], element (jj, c) at jj*16 + (c ^ 2(jj & 7))
   const TS *Tr = reinterpret_cast<const TS *>(smem_k6w);
+  constexpr bool LT = lane_table_fits((size_t)(N * 8 + 16) * sizeof(C), lane_table_bytes<N1, C>());
+  C *stw = T + N * 8 + 16;  // lane twiddles (when LT)
   const int k0 = blockIdx.x * 16, i = blockIdx.y;
   if (!inst_active(g, i)) return;
+  if constexpr (LT) fill_lane_twiddles<TS, N1>(stw, tw);
   const C *src0 = spec + (size_t)g.nyh * i * g.ldxc + k0;
   const int nvalid = min(16, g.nxm - k0);
   constexpr int kIt = (NH * 16 + 255) / 256;
@@ -1243,7 +1254,10 @@ __global__ void __launch_bounds__(256)
     x[m].x = X.x - Y.y;
     x[m].y = X.y + Y.x;
   }
-  warp_fft<true, TS, N1>(x, lane, tw);
+  if constexpr (LT)
+    warp_fft_lt<true, TS, N1>(x, lane, tw, stw);
+  else
+    warp_fft<true, TS, N1>(x, lane, tw);
   __syncthreads();
   const int rl = bitrev5(lane);
 #pragma unroll
@@ -1712,11 +1726,12 @@ static cudaError_t launch_w_n1(const LaunchCtx &L, const SubstepBuffers &b, int 
   if (st == Stage::DivFftY || st == Stage::IfftY) {
     const size_t sm = (size_t)N * 8 * sizeof(C);
     dim3 grid((g.nxm + 15) / 16, g.nzm);
-    if (st == Stage::DivFftY && L.div_var == 1) {  // tensor copies (FP64 single domain)
+    // tensor copies (FP64 single domain); a field's transform (spectra) takes the per-thread form
+    if (st == Stage::DivFftY && L.div_var == 1 && !b.fft_field) {
       if constexpr (!std::is_same<TS, double>::value) {
         return cudaErrorInvalidValue;
       } else {
-        if (g.batch || b.fft_field) return cudaErrorInvalidValue;
+        if (g.batch) return cudaErrorInvalidValue;
         size_t sm2 = 1024 + 2 * (size_t)kDivChunkBytes + (size_t)N * 8 * sizeof(double2) + 2 * sizeof(uint64_t);
         if (lane_table_fits(sm2, lane_table_bytes<N1>())) sm2 += lane_table_bytes<N1>();
         if (sm2 > (size_t)227 * 1024) return cudaErrorInvalidValue;
@@ -1734,10 +1749,11 @@ static cudaError_t launch_w_n1(const LaunchCtx &L, const SubstepBuffers &b, int 
                                                                               (const double2 *)L.twy, b.err);
       }
     } else if (st == Stage::DivFftY) {
+      const size_t smt = sm + (lane_table_fits(sm, lane_table_bytes<N1, C>()) ? lane_table_bytes<N1, C>() : 0);
       auto kern = k_div_fft_y_w<N1, TS>;
-      cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-      kern<<<grid, 256, sm, L.stream>>>(g, L.t, b.sc, ns, b.vx_o, b.vy_o, b.vz_o, spec, (const C *)L.twy,
-                                        b.fft_field);
+      cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smt);
+      kern<<<grid, 256, smt, L.stream>>>(g, L.t, b.sc, ns, b.vx_o, b.vy_o, b.vz_o, spec, (const C *)L.twy,
+                                         b.fft_field);
     } else if (L.ify_var == 1) {  // tensor copies (FP64 single domain, N <= 384)
       if constexpr (!std::is_same<TS, double>::value || N1 > 12) {
         return cudaErrorInvalidValue;
@@ -1762,7 +1778,8 @@ static cudaError_t launch_w_n1(const LaunchCtx &L, const SubstepBuffers &b, int 
       }
     } else {
       // the staged half spectrum [N/2 + 1][16] is 16 elements larger than the [N][8] tile
-      const size_t sm6 = (size_t)(N * 8 + 16) * sizeof(C);
+      size_t sm6 = (size_t)(N * 8 + 16) * sizeof(C);
+      if (lane_table_fits(sm6, lane_table_bytes<N1, C>())) sm6 += lane_table_bytes<N1, C>();
       auto kern = k_ifft_y_w<N1, TS>;
       cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm6);
       kern<<<grid, 256, sm6, L.stream>>>(g, spec, (TS *)b.phi, (const C *)L.twy);
@@ -1795,21 +1812,23 @@ static cudaError_t launch_w_n1(const LaunchCtx &L, const SubstepBuffers &b, int 
   }
   if (L.fftz_var == 1) {  // persistent, double-buffered tiles
     if (2 * sm > (size_t)227 * 1024) return cudaErrorInvalidValue;  // two tiles do not fit
+    const size_t smp = 2 * sm + (lane_table_fits(2 * sm, lane_table_bytes<N1, C>()) ? lane_table_bytes<N1, C>() : 0);
     auto kern = (st == Stage::FftZFwd) ? k_fft_z_wp<N1, false, TS> : k_fft_z_wp<N1, true, TS>;
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(2 * sm));
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smp);
     if (e != cudaSuccess) return e;
     int dev = 0, nsm = 148, per = 1;
     cudaGetDevice(&dev);
     if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || nsm < 1) nsm = 148;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, 256, 2 * sm) != cudaSuccess || per < 1) per = 1;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, 256, smp) != cudaSuccess || per < 1) per = 1;
     const int ntiles = ((g.nxm + 7) / 8) * g.nyh;
-    kern<<<std::max(1, std::min(ntiles, nsm * per)), 256, 2 * sm, L.stream>>>(g, spec, (const C *)L.twz);
+    kern<<<std::max(1, std::min(ntiles, nsm * per)), 256, smp, L.stream>>>(g, spec, (const C *)L.twz);
     return cudaGetLastError();
   }
   dim3 grid((g.nxm + 7) / 8, g.nyh);
+  const size_t smt = sm + (lane_table_fits(sm, lane_table_bytes<N1, C>()) ? lane_table_bytes<N1, C>() : 0);
   auto kern = (st == Stage::FftZFwd) ? k_fft_z_w<N1, false, TS> : k_fft_z_w<N1, true, TS>;
-  cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-  kern<<<grid, 256, sm, L.stream>>>(g, spec, (const C *)L.twz);
+  cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smt);
+  kern<<<grid, 256, smt, L.stream>>>(g, spec, (const C *)L.twz);
   return cudaGetLastError();
 }
 

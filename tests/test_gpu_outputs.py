@@ -41,6 +41,33 @@ def test_spectra_match_oracle(shape, precision):
         assert err < tol, (name, err)
 
 
+@pytest.mark.parametrize("shape", [(16, 96, 64), (24, 64, 32)])
+def test_spectra_with_tensor_copy_forms(shape):
+    """The spectra's field transforms take the per-thread y transform and the chosen z form
+    while the step runs the tensor-copy forms of K2, K3/K5 and K6 (FP64)."""
+    case = Case(*shape, rayt=1e6, dt=1e-3)
+    s = case.oracle_state(random_velocity=0.2)
+    acc = {}
+    with case.solver() as g:
+        g.autotune()
+        g.set_div_form(1)
+        g.set_fftz_form(2)
+        g.set_ify_form(1)
+        g.upload(s.vx, s.vy, s.vz, s.temp, s.pr)
+        g.spectra_reset()
+        g.spectra_update(0.3)
+        o.spectra_update(case.g, s, 0.3, acc)
+        g.time_marcher(1e-3, 0)
+        o.time_marcher(case.g, s, 1e-3)
+        g.spectra_update(0.2)
+        o.spectra_update(case.g, s, 0.2, acc)
+        got = g.spectra()
+    for name in ("vx", "vy", "vz", "temp"):
+        ref = acc[name] / 0.5
+        err = np.abs(got[name] - ref).max() / max(np.abs(ref).max(), 1e-300)
+        assert err < 1e-12, (name, err)
+
+
 def test_slices_are_planes_of_the_state():
     case = Case(20, 24, 12, rayt=1e6)
     s = case.oracle_state(random_velocity=0.2)
