@@ -818,18 +818,42 @@ constexpr int kDivChunk = 32;                           // rows a chunk
 constexpr uint32_t kDivChunkTx = 4 * 4096 + 512 + 128;  // bytes a chunk brings
 constexpr int kDivChunkBytes = 17408;                   // a chunk buffer, 1024-aligned
 
+// Blocks per SM that k_div_fft_y_wt's register cap allows, its dynamic shared memory with nb
+// chunk buffers (alignment slack, chunks, the [N][8] tile, barriers, the lane-twiddle table
+// where it keeps the blocks per SM), and the number of chunk buffers: a third where it costs no
+// block per SM (N = 384, two blocks by registers), so that more of the next tile is in flight
+// while a tile is transformed.
 template <int N1>
-__global__ void __launch_bounds__(256, (N1 <= 8) ? 3 : (N1 <= 16) ? 2 : 1)
+__host__ __device__ constexpr int div_blocks_by_regs() {
+  return (N1 <= 8) ? 3 : (N1 <= 16) ? 2 : 1;
+}
+template <int N1>
+__host__ __device__ constexpr size_t div_smem(int nb) {
+  const size_t core = 1024 + (size_t)nb * kDivChunkBytes + (size_t)32 * N1 * 128 + 32;  // 32: up to 4 barriers
+  return core + (lane_table_fits(core, lane_table_bytes<N1>()) ? lane_table_bytes<N1>() : 0);
+}
+__host__ __device__ constexpr size_t div_min(size_t a, size_t b) { return a < b ? a : b; }
+template <int N1>
+__host__ __device__ constexpr int div_nbuf() {
+  const size_t r = (size_t)div_blocks_by_regs<N1>(), b3 = div_smem<N1>(3), b2 = div_smem<N1>(2);
+  return (b3 <= 227 * 1024 && div_min(r, (228 * 1024) / (b3 + 1024)) >= div_min(r, (228 * 1024) / (b2 + 1024))) ? 3
+                                                                                                               : 2;
+}
+
+template <int N1>
+__global__ void __launch_bounds__(256, div_blocks_by_regs<N1>())
     k_div_fft_y_wt(Geom g, Tables t, const StepCoef *__restrict__ sc_all, int ns, const __grid_constant__ DivMaps mp,
                    double2 *__restrict__ spec, const double2 *__restrict__ tw, int *__restrict__ err) {
   constexpr int N = 32 * N1;
   if (!inst_active(g, 0)) return;  // a single domain stopped by its step control
   extern __shared__ __align__(1024) unsigned char smem_k2t[];
   unsigned char *base = smem_k2t + ((1024u - (smem_u32(smem_k2t) & 1023u)) & 1023u);
-  double2 *T = reinterpret_cast<double2 *>(base + 2 * kDivChunkBytes);  // [N][8] swizzled (tsw)
+  constexpr int NB = div_nbuf<N1>();  // chunk buffers
+  double2 *T = reinterpret_cast<double2 *>(base + NB * kDivChunkBytes);  // [N][8] swizzled (tsw)
   uint64_t *bar = reinterpret_cast<uint64_t *>(T + N * 8);
-  constexpr bool LT = lane_table_fits(1024 + 2 * kDivChunkBytes + N * 128 + 16, lane_table_bytes<N1>());
-  double2 *stw = reinterpret_cast<double2 *>(bar + 2);  // lane twiddles (when LT)
+  constexpr size_t kCore = 1024 + (size_t)NB * kDivChunkBytes + (size_t)N * 128 + 32;  // as div_smem
+  constexpr bool LT = lane_table_fits(kCore, lane_table_bytes<N1>());
+  double2 *stw = reinterpret_cast<double2 *>(base + kCore - 1024);  // lane twiddles (when LT)
   if constexpr (LT) fill_lane_twiddles<double, N1>(stw, tw);
   const int ntx = (g.nxm + 15) / 16;
   const int ntiles = ntx * g.nzm;
@@ -837,13 +861,12 @@ __global__ void __launch_bounds__(256, (N1 <= 8) ? 3 : (N1 <= 16) ? 2 : 1)
   const int nchunks = mytiles * N1;  // this block's chunk stream
   const int tid = threadIdx.x;
   if (tid == 0) {
-    mbar_init(&bar[0], 1);
-    mbar_init(&bar[1], 1);
+    for (int b = 0; b < NB; ++b) mbar_init(&bar[b], 1);
     fence_mbar_init();
   }
   __syncthreads();
-  auto issue = [&](int sq) {  // thread 0: chunk sq of the stream into buffer sq & 1
-    const int tile = blockIdx.x + (sq / N1) * gridDim.x, c = sq % N1, b = sq & 1;
+  auto issue = [&](int sq) {  // thread 0: chunk sq of the stream into buffer sq % NB
+    const int tile = blockIdx.x + (sq / N1) * gridDim.x, c = sq % N1, b = sq % NB;
     const int k0 = (tile % ntx) * 16, i = tile / ntx, ip = zinc(g, i);
     unsigned char *cb = base + b * kDivChunkBytes;
     const int j0 = kDivChunk * c;
@@ -855,10 +878,8 @@ __global__ void __launch_bounds__(256, (N1 <= 8) ? 3 : (N1 <= 16) ? 2 : 1)
     tma_load_3d(cb + 16384, &mp.vx2, k0 + 16, j0, i, &bar[b]);
     tma_load_3d(cb + 16896, &mp.vyr, k0, (j0 + kDivChunk) % N, i, &bar[b]);
   };
-  if (tid == 0) {
-    if (nchunks > 0) issue(0);
-    if (nchunks > 1) issue(1);
-  }
+  if (tid == 0)
+    for (int sq = 0; sq < NB && sq < nchunks; ++sq) issue(sq);
   const StepCoef sc = sc_all[sc_slot(g, 0, ns)];
   const double usdtal = 1.0 / (sc.dt * sc.al);
   const double norm = 1.0 / (nz_norm(g) * (double)g.nym);
@@ -872,15 +893,16 @@ __global__ void __launch_bounds__(256, (N1 <= 8) ? 3 : (N1 <= 16) ? 2 : 1)
     const int kk = k0 + 2 * q;
     const double2 ux = (kk < nxm) ? __ldg(reinterpret_cast<const double2 *>(t.udx3m + kk)) : make_double2(0.0, 0.0);
     for (int c = 0; c < N1; ++c) {
-      const int sq = lt * N1 + c, b = sq & 1;
-      const uint32_t par = (uint32_t)(sq >> 1) & 1u;
+      const int sq = lt * N1 + c, b = sq % NB;
+      const uint32_t par = (uint32_t)(sq / NB) & 1u;
       bool ok = mbar_wait(&bar[b], par, kSpinLimit);
       // test hook: the opposite phase is never completed here, so this wait always runs out
       if (g.wait_test_polls > 0) ok = ok && mbar_wait(&bar[b], par ^ 1u, g.wait_test_polls);
       if (!__syncthreads_and(ok)) {
         if (tid == 0) atomicOr(err, 2);
-        mbar_wait(&bar[b], par, kDrainLimit);  // copies in flight land before the block exits
-        if (sq + 1 < nchunks) mbar_wait(&bar[b ^ 1], (uint32_t)((sq + 1) >> 1) & 1u, kDrainLimit);
+        // copies in flight (this chunk and the next NB - 1) land before the block exits
+        for (int d = 0; d < NB && sq + d < nchunks; ++d)
+          mbar_wait(&bar[(sq + d) % NB], (uint32_t)((sq + d) / NB) & 1u, kDrainLimit);
         return;
       }
       const unsigned char *cb = base + b * kDivChunkBytes;
@@ -903,7 +925,7 @@ __global__ void __launch_bounds__(256, (N1 <= 8) ? 3 : (N1 <= 16) ? 2 : 1)
       }
       T[tsw(kDivChunk * c + jl, q)] = make_double2(dv0, dv1);
       __syncthreads();  // chunk buffer b is free again
-      if (tid == 0 && sq + 2 < nchunks) issue(sq + 2);
+      if (tid == 0 && sq + NB < nchunks) issue(sq + NB);
     }
     double2 x[N1];
 #pragma unroll
@@ -1732,8 +1754,7 @@ static cudaError_t launch_w_n1(const LaunchCtx &L, const SubstepBuffers &b, int 
         return cudaErrorInvalidValue;
       } else {
         if (g.batch) return cudaErrorInvalidValue;
-        size_t sm2 = 1024 + 2 * (size_t)kDivChunkBytes + (size_t)N * 8 * sizeof(double2) + 2 * sizeof(uint64_t);
-        if (lane_table_fits(sm2, lane_table_bytes<N1>())) sm2 += lane_table_bytes<N1>();
+        const size_t sm2 = div_smem<N1>(div_nbuf<N1>());
         if (sm2 > (size_t)227 * 1024) return cudaErrorInvalidValue;
         DivMaps mp;
         if (!div_tmaps(g, b.vx_o, b.vy_o, b.vz_o, &mp)) return cudaErrorInvalidValue;
