@@ -1024,11 +1024,11 @@ int afid_gpu_set_k4_form(afid_ctx_t *ctx, int form) {
 }
 
 int afid_gpu_set_fftz_form(afid_ctx_t *ctx, int form) {
-  if (!ctx || form < 0 || form > 2 || (form == 2 && ctx->L.mixed)) return AFID_E_INVALID;
-  // the persistent forms hold two tiles of nzm rows of 8 elements in shared memory (the
-  // tensor-copy form with its barriers and 1024-byte alignment slack)
+  if (!ctx || form < 0 || form > 2) return AFID_E_INVALID;
+  // the persistent forms hold two tiles of nzm rows in shared memory: 8 elements a row, or 128
+  // bytes a row for the tensor-copy form, with its barriers and 1024-byte alignment slack
   const size_t elem = ctx->L.mixed ? 8 : 16;
-  const size_t tiles = 2 * (size_t)ctx->L.g.nzm * 8 * elem + (form == 2 ? 16 + 1024 : 0);
+  const size_t tiles = form == 2 ? 2 * (size_t)ctx->L.g.nzm * 128 + 16 + 1024 : 2 * (size_t)ctx->L.g.nzm * 8 * elem;
   if (form > 0 && tiles > (size_t)227 * 1024) return AFID_E_INVALID;
   ctx->L.fftz_var = form;
   ctx->tune.fftz_chosen = form;

@@ -1114,20 +1114,23 @@ __device__ __forceinline__ int zslot(int k1, int rl) {
 // not stored.  Two tiles in flight as in k_fft_z_wp; the same arithmetic, so the same bits.  The
 // staging wait is bounded: a block that gives up sets bit 2 of *err, lets its copies land and
 // exits.
-template <int N1, bool INV>
+template <int N1, bool INV, typename TS>
 __global__ void __launch_bounds__(256)
     k_fft_z_wt(Geom g, const __grid_constant__ CUtensorMap ld_map, const __grid_constant__ CUtensorMap st_map,
-               const double2 *__restrict__ tw, int *__restrict__ err) {
+               const typename Cplx<TS>::type *__restrict__ tw, int *__restrict__ err) {
+  using C = typename Cplx<TS>::type;
   constexpr int N = 32 * N1;
+  // a tile row is 128 bytes: 8 x points of double2, or 16 of float2 (two columns a warp)
+  constexpr int CPW = 16 / (int)sizeof(C), XT = 8 * CPW;
   extern __shared__ __align__(1024) unsigned char smem_k3t[];
   // the 128-byte swizzle repeats every 1024 bytes: tiles start on such a boundary
   unsigned char *base = smem_k3t + ((1024u - (smem_u32(smem_k3t) & 1023u)) & 1023u);
-  double2 *sb = reinterpret_cast<double2 *>(base);  // [2][N][8]
+  uint4 *sb = reinterpret_cast<uint4 *>(base);  // [2][N][8] 16-byte chunks
   uint64_t *bar = reinterpret_cast<uint64_t *>(sb + 2 * N * 8);
-  constexpr bool LT = lane_table_fits(2 * N * 128 + 16 + 1024, lane_table_bytes<N1>());
-  double2 *stw = reinterpret_cast<double2 *>(bar + 2);  // lane twiddles (when LT)
-  if constexpr (LT) fill_lane_twiddles<double, N1>(stw, tw);
-  const int ntx = (g.nxm + 7) / 8;
+  constexpr bool LT = lane_table_fits(2 * N * 128 + 16 + 1024, lane_table_bytes<N1, C>());
+  C *stw = reinterpret_cast<C *>(bar + 2);  // lane twiddles (when LT)
+  if constexpr (LT) fill_lane_twiddles<TS, N1>(stw, tw);
+  const int ntx = (g.nxm + XT - 1) / XT;
   const int ntiles = ntx * g.nyh;
   const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
   if (tid == 0) {
@@ -1137,9 +1140,15 @@ __global__ void __launch_bounds__(256)
   }
   __syncthreads();
   auto issue = [&](int tile, int b) {  // thread 0
-    const int k0 = (tile % ntx) * 8, ky = tile / ntx;
+    const int k0 = (tile % ntx) * XT, ky = tile / ntx;
     mbar_arrive_expect_tx(&bar[b], 128u * N);
     tma_load_4d(sb + (size_t)b * N * 8, &ld_map, 2 * k0, 0, 0, ky, &bar[b]);
+  };
+  auto fft = [&](C(&x)[N1]) {
+    if constexpr (LT)
+      warp_fft_lt<INV, TS, N1>(x, lane, tw, stw);
+    else
+      warp_fft<INV, TS, N1>(x, lane, tw);
   };
   int tile = blockIdx.x;
   if (tid == 0 && tile < ntiles) issue(tile, 0);
@@ -1161,36 +1170,45 @@ __global__ void __launch_bounds__(256)
       if (nt < ntiles) mbar_wait(&bar[b ^ 1], (uint32_t)((it + 1) >> 1) & 1u, kDrainLimit);
       break;
     }
-    double2 *s = sb + (size_t)b * N * 8;
-    double2 x[N1];
+    uint4 *s = sb + (size_t)b * N * 8;
+    // chunk w of each row: the warp's column (FP64) or its two adjacent columns (FP32)
+    C x[CPW][N1];
 #pragma unroll
     for (int m = 0; m < N1; ++m) {
       const int r = lane + 32 * m;
-      x[m] = s[r * 8 + (w ^ (r & 7))];
+      if constexpr (CPW == 1) {
+        x[0][m] = reinterpret_cast<const C *>(s)[r * 8 + (w ^ (r & 7))];
+      } else {
+        const float4 v = reinterpret_cast<const float4 *>(s)[r * 8 + (w ^ (r & 7))];
+        x[0][m] = make_float2(v.x, v.y);
+        x[CPW - 1][m] = make_float2(v.z, v.w);
+      }
     }
     __syncwarp();
-    if constexpr (LT)
-      warp_fft_lt<INV, double, N1>(x, lane, tw, stw);
-    else
-      warp_fft<INV, double, N1>(x, lane, tw);
+#pragma unroll
+    for (int c = 0; c < CPW; ++c) fft(x[c]);
     const int rl = bitrev5(lane);
 #pragma unroll
     for (int k1 = 0; k1 < N1; ++k1) {
       const int r = zslot<N1>(k1, rl);
-      s[r * 8 + (w ^ (r & 7))] = x[k1];
+      if constexpr (CPW == 1)
+        reinterpret_cast<C *>(s)[r * 8 + (w ^ (r & 7))] = x[0][k1];
+      else
+        reinterpret_cast<float4 *>(s)[r * 8 + (w ^ (r & 7))] =
+            make_float4(x[0][k1].x, x[0][k1].y, x[CPW - 1][k1].x, x[CPW - 1][k1].y);
     }
     fence_proxy_async_shared();
     __syncthreads();
     if (tid == 0) {
-      tma_store_4d(&st_map, 2 * ((tile % ntx) * 8), 0, 0, tile / ntx, s);
+      tma_store_4d(&st_map, 2 * ((tile % ntx) * XT), 0, 0, tile / ntx, s);
       bulk_commit();
     }
   }
   if (tid == 0) bulk_wait_all();
 }
 
-// The two tensor maps of k_fft_z_wt over an FP64 spectrum [nzm][nyh][ldxc] of double2, viewed
-// as doubles: x (2 nxm, the tile's 16 doubles a box row), two z dimensions, ky.  Encoded through
+// The two tensor maps of k_fft_z_wt over a spectrum [nzm][nyh][ldxc] of complex TS, viewed as
+// TS: x (2 nxm, a 128-byte box row: 16 doubles or 32 floats), two z dimensions, ky.  Encoded through
 // the driver's entry point (no driver library linked); false if that is unavailable or refuses.
 using TmapEncodeFn = CUresult (*)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
                                   const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
@@ -1207,23 +1225,25 @@ static TmapEncodeFn tmap_encoder() {
   return fn;
 }
 
-static bool fftz_tmaps(const Geom &g, int N1, double2 *spec, CUtensorMap *ld, CUtensorMap *st) {
+template <typename TS>
+static bool fftz_tmaps(const Geom &g, int N1, typename Cplx<TS>::type *spec, CUtensorMap *ld, CUtensorMap *st) {
+  using C = typename Cplx<TS>::type;
   TmapEncodeFn enc = tmap_encoder();
   if (!enc) return false;
-  const cuuint64_t zb = (cuuint64_t)g.nyh * g.ldxc * sizeof(double2);  // bytes between z rows
+  const CUtensorMapDataType dt = sizeof(TS) == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
+  const cuuint32_t bx = 128 / sizeof(TS);  // a 128-byte box row
+  const cuuint64_t zb = (cuuint64_t)g.nyh * g.ldxc * sizeof(C);  // bytes between z rows
   const cuuint32_t estr[4] = {1, 1, 1, 1};
   const cuuint64_t ldim[4] = {(cuuint64_t)2 * g.nxm, 32, (cuuint64_t)N1, (cuuint64_t)g.nyh};
-  const cuuint64_t lstr[3] = {zb, 32 * zb, (cuuint64_t)g.ldxc * sizeof(double2)};
-  const cuuint32_t lbox[4] = {16, 32, (cuuint32_t)N1, 1};
+  const cuuint64_t lstr[3] = {zb, 32 * zb, (cuuint64_t)g.ldxc * sizeof(C)};
+  const cuuint32_t lbox[4] = {bx, 32, (cuuint32_t)N1, 1};
   const cuuint64_t sdim[4] = {(cuuint64_t)2 * g.nxm, 8, (cuuint64_t)4 * N1, (cuuint64_t)g.nyh};
-  const cuuint64_t sstr[3] = {(cuuint64_t)4 * N1 * zb, zb, (cuuint64_t)g.ldxc * sizeof(double2)};
-  const cuuint32_t sbox[4] = {16, 8, (cuuint32_t)(4 * N1), 1};
-  return enc(ld, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4, spec, ldim, lstr, lbox, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
-             CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS &&
-         enc(st, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4, spec, sdim, sstr, sbox, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
-             CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+  const cuuint64_t sstr[3] = {(cuuint64_t)4 * N1 * zb, zb, (cuuint64_t)g.ldxc * sizeof(C)};
+  const cuuint32_t sbox[4] = {bx, 8, (cuuint32_t)(4 * N1), 1};
+  return enc(ld, dt, 4, spec, ldim, lstr, lbox, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+             CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS &&
+         enc(st, dt, 4, spec, sdim, sstr, sbox, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+             CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
 // K6w: backward y c2r.  Block: 16 x points = 8 pairs (8 warps) at one z index i.  The half
@@ -1808,28 +1828,25 @@ static cudaError_t launch_w_n1(const LaunchCtx &L, const SubstepBuffers &b, int 
     return cudaGetLastError();
   }
   const size_t sm = (size_t)N * 8 * sizeof(C);
-  if (L.fftz_var == 2) {  // persistent, rows moved by bulk copies (FP64 spectrum only)
-    if constexpr (!std::is_same<TS, double>::value) {
-      return cudaErrorInvalidValue;
-    } else {
-      // two 1024-byte aligned tiles of N x 128 bytes, the barriers, the alignment slack
-      size_t smb = (size_t)2 * N * 8 * sizeof(double2) + 2 * sizeof(uint64_t) + 1024;
-      if (lane_table_fits(smb, lane_table_bytes<N1>())) smb += lane_table_bytes<N1>();
-      if (smb > (size_t)227 * 1024 || 4 * N1 > 256) return cudaErrorInvalidValue;  // two tiles do not fit
-      CUtensorMap ld_map, st_map;
-      if (!fftz_tmaps(g, N1, spec, &ld_map, &st_map)) return cudaErrorInvalidValue;
-      auto kern = (st == Stage::FftZFwd) ? k_fft_z_wt<N1, false> : k_fft_z_wt<N1, true>;
-      cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smb);
-      if (e != cudaSuccess) return e;
-      int dev = 0, nsm = 148, per = 1;
-      cudaGetDevice(&dev);
-      if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || nsm < 1) nsm = 148;
-      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, 256, smb) != cudaSuccess || per < 1) per = 1;
-      const int ntiles = ((g.nxm + 7) / 8) * g.nyh;
-      kern<<<std::max(1, std::min(ntiles, nsm * per)), 256, smb, L.stream>>>(g, ld_map, st_map,
-                                                                              (const double2 *)L.twz, b.err);
-      return cudaGetLastError();
-    }
+  if (L.fftz_var == 2) {  // persistent, tiles moved by tensor copies
+    // two 1024-byte aligned tiles of N x 128 bytes, the barriers, the alignment slack
+    size_t smb = (size_t)2 * N * 128 + 2 * sizeof(uint64_t) + 1024;
+    if (lane_table_fits(smb, lane_table_bytes<N1, C>())) smb += lane_table_bytes<N1, C>();
+    if (smb > (size_t)227 * 1024 || 4 * N1 > 256) return cudaErrorInvalidValue;  // two tiles do not fit
+    CUtensorMap ld_map, st_map;
+    if (!fftz_tmaps<TS>(g, N1, spec, &ld_map, &st_map)) return cudaErrorInvalidValue;
+    auto kern = (st == Stage::FftZFwd) ? k_fft_z_wt<N1, false, TS> : k_fft_z_wt<N1, true, TS>;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smb);
+    if (e != cudaSuccess) return e;
+    int dev = 0, nsm = 148, per = 1;
+    cudaGetDevice(&dev);
+    if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || nsm < 1) nsm = 148;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, 256, smb) != cudaSuccess || per < 1) per = 1;
+    constexpr int XT = 128 / (int)sizeof(C);  // x points a tile
+    const int ntiles = ((g.nxm + XT - 1) / XT) * g.nyh;
+    kern<<<std::max(1, std::min(ntiles, nsm * per)), 256, smb, L.stream>>>(g, ld_map, st_map, (const C *)L.twz,
+                                                                          b.err);
+    return cudaGetLastError();
   }
   if (L.fftz_var == 1) {  // persistent, double-buffered tiles
     if (2 * sm > (size_t)227 * 1024) return cudaErrorInvalidValue;  // two tiles do not fit

@@ -183,8 +183,8 @@ typedef struct afid_tune_info {
                                    with the next mode's right-hand side prefetched              */
   double k4_us[2];              /* microseconds per full launch of each form (-1: not run)   */
   int fftz_chosen;              /* z transforms: 0 one tile per block, 1 persistent blocks with
-                                   the next tile's copies in flight, 2 the same with the tile
-                                   rows moved by bulk copies (FP64 only; 3-D single domains)    */
+                                   the next tile's copies in flight, 2 the same with the tiles
+                                   moved by tensor copies (3-D single domains)                  */
   double fftz_us[3];            /* microseconds per full forward z launch of each form         */
   int ify_chosen;               /* inverse y transform: 0 per-thread copies, 1 tensor copies
                                    (FP64 single domains, nym = 32 x {1,2,3,4,6,8,12})           */
@@ -202,7 +202,7 @@ int afid_gpu_set_k1_shape(afid_ctx_t *ctx, int index);
  * both forms give bitwise the same results. */
 int afid_gpu_set_k4_form(afid_ctx_t *ctx, int form);
 /* Use z-transform form `form` (0, 1 or 2 as in afid_tune_info_t.fftz_chosen); bitwise the same.
- * AFID_E_INVALID for form 2 on a mixed-precision context (FP32 spectrum). */
+ * AFID_E_INVALID for a persistent form whose two tiles of nzm rows do not fit shared memory. */
 int afid_gpu_set_fftz_form(afid_ctx_t *ctx, int form);
 /* Use inverse-y-transform form `form` (0 or 1 as in afid_tune_info_t.ify_chosen); bitwise the
  * same.  AFID_E_INVALID for form 1 where it does not apply (mixed precision, other nym). */

@@ -104,6 +104,33 @@ def test_bounded_wait_runs_out_in_tensor_copy_transforms():
     assert rel_l2(out["temp"][..., :nxm], s.temp[..., :nxm]) < 1e-10
 
 
+def test_bounded_wait_runs_out_in_tensor_copy_z_transform_mixed():
+    """The same for the FP32 spectrum of the mixed path (two columns a warp): AFID_E_TIMEOUT at
+    the next synchronising call, and a new context on the device steps to the same fields as a
+    context that never ran out."""
+    case = Case(60, 16, 256, precision=ag.PREC_MIXED, rayt=1e6, dt=1e-3)
+    s = case.oracle_state(random_velocity=0.1)
+    with case.solver() as gpu:
+        gpu.autotune()
+        gpu.set_fftz_form(2)
+        gpu.upload(s.vx, s.vy, s.vz, s.temp, s.pr)
+        gpu.set_wait_test(4096)
+        with pytest.raises(ag.AfidError) as e:
+            gpu.time_marcher(1e-3, 0)
+            gpu.synchronize()
+        assert e.value.status == ag.AFID_E_TIMEOUT
+    outs = []
+    for form in (2, 1):
+        with case.solver() as gpu:
+            gpu.autotune()
+            gpu.set_fftz_form(form)
+            gpu.upload(s.vx, s.vy, s.vz, s.temp, s.pr)
+            gpu.time_marcher(1e-3, 0)
+            outs.append(gpu.download())
+    for k in ag.Solver.FIELDS:
+        assert np.array_equal(outs[0][k], outs[1][k]), k
+
+
 def test_wait_test_hook_rejects_out_of_range():
     case = Case(16, 8, 4)
     with case.solver() as gpu:

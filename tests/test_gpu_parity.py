@@ -221,14 +221,15 @@ def test_launch_count_positive():
                                              ((60, 16, 1), ag.PREC_FP64), ((500, 16, 4), ag.PREC_FP64),
                                              ((64, 32, 96), ag.PREC_FP64), ((100, 16, 8), ag.PREC_MIXED),
                                              ((64, 32, 96), ag.PREC_MIXED), ((60, 64, 64), ag.PREC_FP64),
-                                             ((60, 64, 64), ag.PREC_MIXED), ((60, 16, 256), ag.PREC_FP64),
+                                             ((60, 64, 64), ag.PREC_MIXED), ((60, 16, 256), ag.PREC_MIXED),
+                                             ((36, 8, 384), ag.PREC_MIXED), ((60, 16, 256), ag.PREC_FP64),
                                              ((36, 8, 384), ag.PREC_FP64), ((64, 8, 512), ag.PREC_FP64),
                                              ((36, 256, 8), ag.PREC_FP64), ((20, 384, 4), ag.PREC_FP64),
                                              ((44, 96, 4), ag.PREC_FP64), ((40, 64, 1), ag.PREC_FP64)])
 def test_k4_and_fftz_forms_bitwise_identical(shape, precision):
     """Both forms of the Poisson tridiagonal (a mode per warp; persistent warps with the next
     mode prefetched), every form of the z transforms (a tile per block; persistent blocks with
-    the next tile prefetched by per-thread copies, or by tensor copies, FP64 only) and both forms
+    the next tile prefetched by per-thread copies, or by tensor copies) and both forms
     of the inverse y transform (per-thread copies; tensor copies for FP64 single domains with
     nym = 32 x {1, 2, 3, 4, 6, 8, 12}) and of the divergence + forward y transform (per-thread
     loads; tensor copies of the velocity rows) give the same fields bit for bit, so the autotuner's
@@ -236,7 +237,7 @@ def test_k4_and_fftz_forms_bitwise_identical(shape, precision):
     case = Case(*shape, precision=precision, rayt=1e6, dt=2e-3)
     s = case.oracle_state(random_velocity=0.1)
     fp64 = precision == ag.PREC_FP64
-    forms = (0, 1, 2) if fp64 else (0, 1)
+    forms = (0, 1, 2)
     nym = shape[1]
     ify_ok = fp64 and nym % 32 == 0 and nym // 32 in (1, 2, 3, 4, 6, 8, 12)
     outs = []
@@ -265,11 +266,6 @@ def test_k4_and_fftz_forms_bitwise_identical(shape, precision):
     for o_ in outs[1:]:
         for k in ag.Solver.FIELDS:
             assert np.array_equal(outs[0][k], o_[k]), k
-    if precision != ag.PREC_FP64:
-        with case.solver() as g:
-            with pytest.raises(ag.AfidError) as e:
-                g.set_fftz_form(2)
-            assert e.value.status == ag.AFID_E_INVALID
 
 
 @pytest.mark.parametrize("name", ["rbc3d_16x12x8_rv", "rbc3d_40x10x6_rv", "rbc2d_32x48x1"])
