@@ -806,8 +806,9 @@ __device__ __forceinline__ void tma_store_4d(const CUtensorMap *map, int c0, int
 // of 16 x points at one z index (a tile), with the velocity rows staged by tiled TMA loads in
 // chunks of 32 rows (vx with the 17th x point, vy with the row after the chunk, vz at i and at
 // i + 1) instead of per-thread global loads, whose latency bounds k_div_fft_y_w.  Each block walks
-// tiles blockIdx.x, + gridDim.x, ... as one stream of chunks with two in flight, so the next
-// tile's first chunks load while the current tile is transformed and stored.  The divergence's
+// tiles blockIdx.x, + gridDim.x, ... as one stream of chunks with two or three in flight
+// (div_nbuf), so the next tile's first chunks load while the current tile is transformed and
+// stored.  The divergence's
 // expression order, the packed tile, the transform and the output are those of k_div_fft_y_w, so
 // the same bits.  The staging wait is bounded (bit 2 of *err, copies drained before the block
 // exits).
@@ -1103,8 +1104,9 @@ __device__ __forceinline__ int zslot(int k1, int rl) {
   return ((rl >> 2) & 7) + 8 * (k1 + N1 * (rl & 3));
 }
 
-// K3w / K5w, tensor-copy persistent form (FP64 spectrum): a tile (8 x points at one ky, all nzm
-// z rows) comes in by one tiled TMA load and goes back by one tiled TMA store, so the load/store
+// K3w / K5w, tensor-copy persistent form: a tile (128 bytes of x at one ky, i.e. 8 x points of an
+// FP64 spectrum or 16 of an FP32 one, whose warps then transform two adjacent columns each; all
+// nzm z rows) comes in by one tiled TMA load and goes back by one tiled TMA store, so the load/store
 // pipe carries only the transform's own shared-memory traffic (the per-thread asynchronous copies
 // of k_fft_z_wp spend about a third of it, and one 1-D bulk copy per 128-byte row is bound by the
 // copy engine's operation rate instead).  The load map views z as (z mod 32, z / 32) and fills the
